@@ -1,0 +1,141 @@
+/*
+ * kelp_cuda.h -- C ABI of the B200 (sm_100a) implementation of KELP's
+ * compiled time-stepping path.
+ *
+ * The library owns all device memory.  A context binds one CUDA device and
+ * one stream; it holds the resident mesh (node table, element table,
+ * node->element CSR, grid hash), a small ring of velocity snapshots, and the
+ * particle state.  Calls on one context are not thread-safe; callers
+ * serialise them.  Every function returns 0 on success or a KC_ERR_* code;
+ * kc_last_error() gives the message.  Invalid arguments are rejected on the
+ * host before any kernel runs.  Per-particle failures are data
+ * (status OUTSIDE + failure reason), as in the reference.
+ *
+ * Reference interfaces replaced (paths inside the KELP project):
+ *   kc_step / kc_run   <- integrators.rk2_step / rk4_step / euler_step
+ *                         (src/kelp/numerics/integrators.py:5611, :6013, :5150),
+ *                         the per-step call of tracking.run_single_realization
+ *                         (src/kelp/tracking.py:2643-2655)
+ *   kc_mesh_upload     <- the arrays of core.mesh.Mesh after build_search
+ *                         (src/kelp/core/mesh.py:40-166, :844-1001)
+ *   kc_field_upload    <- core.io.VelocityField snapshot arrays
+ *                         (src/kelp/core/io.py:180)
+ *   kc_particles_*     <- core.particles.ParticleState arrays
+ *                         (src/kelp/core/particles.py:153)
+ *   kc_node_xyz_fill   <- core.mesh._node_xyz_fill (src/kelp/core/mesh.py:712)
+ *   kc_find_nearest    <- core.mesh.find_nearest_nodes (src/kelp/core/mesh.py:1896)
+ */
+#ifndef KELP_CUDA_H
+#define KELP_CUDA_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KC_ABI_VERSION 1
+
+#define KC_OK 0
+#define KC_ERR_ARG 1      /* invalid argument or combination */
+#define KC_ERR_CUDA 2     /* CUDA runtime error */
+#define KC_ERR_STATE 3    /* call out of order (no mesh / field / particles) */
+#define KC_ERR_DEVICE 4   /* a device-side iteration cap was hit */
+
+/* field element types */
+#define KC_F32 0
+#define KC_F64 1
+
+/* integration schemes */
+#define KC_EULER 0
+#define KC_RK2 1
+#define KC_RK4 2
+
+typedef struct kc_ctx kc_ctx;
+
+typedef struct kc_mesh_desc {
+    long long n_nodes;
+    long long n_elems;
+    int max_v;                   /* 3 or 4 columns in elem_nodes */
+    int max_conn;                /* columns in node_to_elems */
+    const double* nodes_lon;     /* (N) degrees */
+    const double* nodes_lat;     /* (N) degrees */
+    const double* depth;         /* (N) metres positive down; may be NULL for 2-D */
+    const int* elem_nodes;       /* (E, max_v), -1 padded */
+    const int* node_to_elems;    /* (N, max_conn), -1 padded */
+    const int* node_to_elems_count; /* (N) */
+    const int* gh_offsets;       /* (gh_nx * gh_ny + 1) CSR offsets */
+    const int* gh_node_ids;      /* (N) node ids in hash order */
+    const double* node_xyz;      /* (N, 3) unit-sphere table */
+    double gh_cell_size, gh_lon_min, gh_lat_min;
+    int gh_nx, gh_ny, gh_wrap_lon, gh_far_rows;
+    int exact_nearest;           /* mesh.metadata["exact_nearest"] */
+    double r_earth;              /* mesh.r_earth */
+    const double* z_levels;      /* (n_levels) interfaces positive down, NULL for 2-D */
+    int n_levels;
+} kc_mesh_desc;
+
+typedef struct kc_step_args {
+    int scheme;                  /* KC_EULER / KC_RK2 / KC_RK4 */
+    int dims;                    /* 2 or 3 */
+    int slot_a, slot_b, slot_t;  /* bracket pair and stage target snapshots */
+    double alpha0;               /* bracket fraction at the step's start */
+    double alpha_k[4];           /* stage alphas c_k * dt / dt_to_next */
+    double dt;                   /* seconds, > 0 */
+    double time_dir;             /* +1 forward, -1 backward */
+    int w_code;                  /* 3-D W: 0 nearest, 1 barycentric */
+    int kick;                    /* split uniform-Kh random walk on/off */
+    double kh_x, kh_y;           /* m^2/s */
+    unsigned long long seed, real_id, step_i, pid_offset;
+    long long global_step;       /* delayed-release activation step, -1 for none */
+} kc_step_args;
+
+int kc_abi_version(void);
+
+/* Host routine: unit-sphere node table with the C library's cos/sin. */
+int kc_node_xyz_fill(const double* lon, const double* lat, long long n, double* xyz_out);
+
+int kc_create(int device, kc_ctx** out);
+void kc_destroy(kc_ctx* ctx);
+int kc_last_error(const kc_ctx* ctx, char* buf, int buflen);
+int kc_synchronize(kc_ctx* ctx);
+
+int kc_mesh_upload(kc_ctx* ctx, const kc_mesh_desc* desc);
+
+/* One snapshot into ring slot `slot` (0..7): u, v (n_uv_rows, n_nodes) and
+ * optional w (n_w_rows, n_nodes), all of element type `dtype`. */
+int kc_field_upload(kc_ctx* ctx, int slot, int dtype, long long n_nodes, int n_uv_rows,
+                    const void* u, const void* v, int n_w_rows, const void* w);
+
+/* Particle state.  Optional pointers may be NULL (z: zeros, fr: zeros,
+ * pid: the index, release_step: all released). */
+int kc_particles_upload(kc_ctx* ctx, long long P, const double* lon, const double* lat,
+                        const double* z, const int* status, const int* nearest_node,
+                        const signed char* failure_reason, const long long* pid,
+                        const int* release_step);
+int kc_particles_download(kc_ctx* ctx, long long P, double* lon, double* lat, double* z,
+                          int* status, int* nearest_node, signed char* failure_reason,
+                          double* u, double* v, double* w);
+
+/* One step of every resident particle; kc_run: n_steps steps in order,
+ * per-step arguments, no host round trip in between. */
+int kc_step(kc_ctx* ctx, const kc_step_args* args);
+int kc_run(kc_ctx* ctx, const kc_step_args* steps, int n_steps);
+
+/* Batch exact nearest node of P query points (host arrays). */
+int kc_find_nearest(kc_ctx* ctx, long long P, const double* lon, const double* lat, int* out);
+
+/* Device error word (bitmask of iteration caps hit since the last call). */
+int kc_device_errors(kc_ctx* ctx, int* word);
+
+/* Timing on the context's stream: record event `slot` (0..15), and the
+ * elapsed milliseconds between two recorded events. */
+int kc_event_record(kc_ctx* ctx, int slot);
+int kc_event_elapsed(kc_ctx* ctx, int slot_a, int slot_b, float* ms);
+
+/* Page-locked host buffers for the end-to-end path. */
+int kc_host_alloc(long long bytes, void** out);
+int kc_host_free(void* p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KELP_CUDA_H */

@@ -1,0 +1,120 @@
+"""ctypes binding of the native library (``libkelpcuda.so``, C ABI in
+``include/kelp_cuda.h``).
+
+There is no fallback: if the library is missing or a CUDA device cannot be
+opened, every entry point raises.  Loading the library needs no GPU (the host
+routine ``kc_node_xyz_fill`` runs anywhere); creating a context does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libkelpcuda.so")
+
+KC_OK, KC_ERR_ARG, KC_ERR_CUDA, KC_ERR_STATE, KC_ERR_DEVICE = 0, 1, 2, 3, 4
+KC_F32, KC_F64 = 0, 1
+KC_EULER, KC_RK2, KC_RK4 = 0, 1, 2
+
+#: every symbol include/kelp_cuda.h declares
+EXPORTS = ("kc_abi_version", "kc_node_xyz_fill", "kc_create", "kc_destroy", "kc_last_error",
+           "kc_synchronize", "kc_mesh_upload", "kc_field_upload", "kc_particles_upload",
+           "kc_particles_download", "kc_step", "kc_run", "kc_find_nearest", "kc_device_errors",
+           "kc_event_record", "kc_event_elapsed", "kc_host_alloc", "kc_host_free")
+
+
+class KcError(RuntimeError):
+    """A C-ABI call returned a non-zero code."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"kelp_cuda error {code}: {msg}")
+        self.code = code
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("n_nodes", C.c_longlong), ("n_elems", C.c_longlong),
+                ("max_v", C.c_int), ("max_conn", C.c_int),
+                ("nodes_lon", C.c_void_p), ("nodes_lat", C.c_void_p), ("depth", C.c_void_p),
+                ("elem_nodes", C.c_void_p), ("node_to_elems", C.c_void_p),
+                ("node_to_elems_count", C.c_void_p), ("gh_offsets", C.c_void_p),
+                ("gh_node_ids", C.c_void_p), ("node_xyz", C.c_void_p),
+                ("gh_cell_size", C.c_double), ("gh_lon_min", C.c_double), ("gh_lat_min", C.c_double),
+                ("gh_nx", C.c_int), ("gh_ny", C.c_int), ("gh_wrap_lon", C.c_int), ("gh_far_rows", C.c_int),
+                ("exact_nearest", C.c_int), ("r_earth", C.c_double),
+                ("z_levels", C.c_void_p), ("n_levels", C.c_int)]
+
+
+class StepArgs(C.Structure):
+    _fields_ = [("scheme", C.c_int), ("dims", C.c_int),
+                ("slot_a", C.c_int), ("slot_b", C.c_int), ("slot_t", C.c_int),
+                ("alpha0", C.c_double), ("alpha_k", C.c_double * 4),
+                ("dt", C.c_double), ("time_dir", C.c_double),
+                ("w_code", C.c_int), ("kick", C.c_int),
+                ("kh_x", C.c_double), ("kh_y", C.c_double),
+                ("seed", C.c_ulonglong), ("real_id", C.c_ulonglong),
+                ("step_i", C.c_ulonglong), ("pid_offset", C.c_ulonglong),
+                ("global_step", C.c_longlong)]
+
+
+_lib = None
+
+
+def lib():
+    """The loaded library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m kelp_b200.build` "
+                              "(the CUDA path has no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        vp, ll, i, d = C.c_void_p, C.c_longlong, C.c_int, C.c_double
+        L.kc_abi_version.restype = i
+        L.kc_node_xyz_fill.argtypes = [vp, vp, ll, vp]
+        L.kc_create.argtypes = [i, C.POINTER(vp)]
+        L.kc_destroy.argtypes = [vp]
+        L.kc_destroy.restype = None
+        L.kc_last_error.argtypes = [vp, C.c_char_p, i]
+        L.kc_synchronize.argtypes = [vp]
+        L.kc_mesh_upload.argtypes = [vp, C.POINTER(MeshDesc)]
+        L.kc_field_upload.argtypes = [vp, i, i, ll, i, vp, vp, i, vp]
+        L.kc_particles_upload.argtypes = [vp, ll, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.kc_particles_download.argtypes = [vp, ll, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.kc_step.argtypes = [vp, C.POINTER(StepArgs)]
+        L.kc_run.argtypes = [vp, C.POINTER(StepArgs), i]
+        L.kc_find_nearest.argtypes = [vp, ll, vp, vp, vp]
+        L.kc_device_errors.argtypes = [vp, C.POINTER(i)]
+        L.kc_event_record.argtypes = [vp, i]
+        L.kc_event_elapsed.argtypes = [vp, i, i, C.POINTER(C.c_float)]
+        L.kc_host_alloc.argtypes = [ll, C.POINTER(vp)]
+        L.kc_host_free.argtypes = [vp]
+        for name in EXPORTS:
+            fn = getattr(L, name)
+            if name != "kc_destroy" and fn.restype is not None and fn.restype != i:
+                fn.restype = i
+        _lib = L
+    return _lib
+
+
+def ptr(a):
+    """Data pointer of a C-contiguous numpy array (None passes NULL)."""
+    if a is None:
+        return None
+    if not a.flags.c_contiguous:
+        raise ValueError("array must be C-contiguous")
+    return a.ctypes.data
+
+
+def node_xyz_fill(lon: np.ndarray, lat: np.ndarray, out: np.ndarray) -> None:
+    rc = lib().kc_node_xyz_fill(ptr(lon), ptr(lat), lon.shape[0], ptr(out))
+    if rc:
+        raise KcError(rc, "kc_node_xyz_fill")
+
+
+def check(ctx, rc: int, what: str) -> None:
+    if rc:
+        buf = C.create_string_buffer(512)
+        if ctx:
+            lib().kc_last_error(ctx, buf, 512)
+        raise KcError(rc, f"{what}: {buf.value.decode(errors='replace')}")

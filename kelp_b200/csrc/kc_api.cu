@@ -1,0 +1,515 @@
+// C ABI of the B200 time-stepping path (declared in include/kelp_cuda.h):
+// context, resident mesh / snapshot ring / particle state, the step kernels'
+// launchers and the batch nearest-node query.
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <algorithm>
+#include <cuda_runtime.h>
+
+#include "../../include/kelp_cuda.h"
+#include "kc_step.cuh"
+
+namespace {
+
+constexpr int kSlots = 8;
+constexpr int kEvents = 16;
+constexpr int kBlock = 128;
+
+struct Slot {
+    void* u = nullptr;
+    void* v = nullptr;
+    void* w = nullptr;
+    long long n = 0;
+    int uv_rows = 0, w_rows = 0, dtype = -1;
+    size_t cap_uv = 0, cap_w = 0;
+};
+
+}  // namespace
+
+struct kc_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    // mesh
+    bool has_mesh = false;
+    long long N = 0, E = 0;
+    double2* d_ll = nullptr;
+    int4* d_en = nullptr;
+    int* d_n2e_off = nullptr;
+    int* d_n2e = nullptr;
+    int* d_gh_off = nullptr;
+    double4* d_gh_tab = nullptr;
+    double* d_xyz = nullptr;
+    double* d_depth = nullptr;
+    double* d_zlev = nullptr;
+    int* d_err = nullptr;
+    kc::DMesh dm{};
+    // snapshot ring
+    Slot slots[kSlots];
+    // particles
+    long long P = 0, cap = 0;
+    double *lon = nullptr, *lat = nullptr, *z = nullptr, *U = nullptr, *V = nullptr, *W = nullptr;
+    int *status = nullptr, *nn = nullptr, *rs = nullptr;
+    signed char* fr = nullptr;
+    long long* pid = nullptr;
+    bool has_pid = false, has_rs = false;
+    // query scratch of kc_find_nearest
+    double* q = nullptr;
+    int* qout = nullptr;
+    long long qcap = 0;
+    cudaEvent_t ev[kEvents] = {};
+};
+
+namespace {
+
+int fail(kc_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+#define KC_CUDA(c, call)                                                                         \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess)                                                                   \
+            return fail((c), KC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename P>
+void dfree(P*& p) {
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+}
+
+template <typename T>
+kc::DField<T> field_of(const Slot& s) {
+    return kc::DField<T>{(const T*)s.u, (const T*)s.v, (const T*)s.w};
+}
+
+kc::DState state_of(kc_ctx* c) {
+    kc::DState st;
+    st.lon = c->lon; st.lat = c->lat; st.z = c->z; st.status = c->status; st.nn = c->nn;
+    st.U = c->U; st.V = c->V; st.W = c->W; st.fr = c->fr;
+    st.pid = c->has_pid ? c->pid : nullptr;
+    st.release_step = c->has_rs ? c->rs : nullptr;
+    st.P = c->P;
+    return st;
+}
+
+kc::DStep step_of(const kc_step_args* a) {
+    kc::DStep s;
+    s.dt = a->dt; s.time_dir = a->time_dir;
+    for (int k = 0; k < 4; ++k) s.ak[k] = a->alpha_k[k];
+    s.w_code = a->w_code; s.kick = a->kick;
+    s.kh_x = a->kh_x; s.kh_y = a->kh_y;
+    s.seed = a->seed; s.real_id = a->real_id; s.step_i = a->step_i; s.pid_offset = a->pid_offset;
+    s.global_step = a->global_step;
+    return s;
+}
+
+// delayed release (release.py:112-129): NOT_RELEASED -> ALIVE at its step
+__device__ __forceinline__ void activate(const kc::DState& st, const kc::DStep& s, long long i) {
+    if (st.release_step && s.global_step >= 0 && st.status[i] == kc::NOT_RELEASED &&
+        s.global_step >= (long long)st.release_step[i])
+        st.status[i] = kc::ALIVE;
+}
+
+template <typename T, int SCHEME>
+__global__ void __launch_bounds__(kBlock) k_step2d(kc::DMesh m, kc::DBlend<T> f, kc::DState st, kc::DStep s) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= st.P) return;
+    activate(st, s, i);
+    kc::step2d_particle<T, SCHEME>(m, f, st, s, i);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBlock) k_step3d_rk2(kc::DMesh m, kc::DBlend<T> f, kc::DState st, kc::DStep s) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= st.P) return;
+    activate(st, s, i);
+    kc::step3d_rk2_particle<T>(m, f, st, s, i);
+}
+
+__global__ void __launch_bounds__(kBlock) k_nearest(kc::DMesh m, const double* q, long long P, int* out) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P) return;
+    out[i] = kc::site_anchor(m, q[i], q[P + i]);
+}
+
+unsigned grid_for(long long n) { return (unsigned)((n + kBlock - 1) / kBlock); }
+
+template <typename T>
+int launch_step(kc_ctx* c, const kc_step_args* a) {
+    kc::DBlend<T> f;
+    f.a = field_of<T>(c->slots[a->slot_a]);
+    f.b = field_of<T>(c->slots[a->slot_b]);
+    f.t = field_of<T>(c->slots[a->slot_t]);
+    f.alpha0 = a->alpha0;
+    f.n = c->N;
+    kc::DState st = state_of(c);
+    kc::DStep s = step_of(a);
+    if (c->P == 0) return KC_OK;
+    unsigned g = grid_for(c->P);
+    if (a->dims == 2) {
+        if (a->scheme == KC_EULER) k_step2d<T, 0><<<g, kBlock, 0, c->stream>>>(c->dm, f, st, s);
+        else if (a->scheme == KC_RK2) k_step2d<T, 1><<<g, kBlock, 0, c->stream>>>(c->dm, f, st, s);
+        else k_step2d<T, 2><<<g, kBlock, 0, c->stream>>>(c->dm, f, st, s);
+    } else {
+        k_step3d_rk2<T><<<g, kBlock, 0, c->stream>>>(c->dm, f, st, s);
+    }
+    KC_CUDA(c, cudaGetLastError());
+    return KC_OK;
+}
+
+int check_step(kc_ctx* c, const kc_step_args* a) {
+    if (!a) return fail(c, KC_ERR_ARG, "kc_step: null args");
+    if (!c->has_mesh) return fail(c, KC_ERR_STATE, "kc_step: no mesh uploaded");
+    if (!(a->scheme == KC_EULER || a->scheme == KC_RK2 || a->scheme == KC_RK4))
+        return fail(c, KC_ERR_ARG, "kc_step: unknown scheme");
+    if (!(a->dims == 2 || a->dims == 3)) return fail(c, KC_ERR_ARG, "kc_step: dims must be 2 or 3");
+    if (a->dims == 3 && a->scheme != KC_RK2)
+        return fail(c, KC_ERR_ARG, "kc_step: the 3-D step supports rk2 only in this build");
+    if (!(a->dt > 0.0)) return fail(c, KC_ERR_ARG, "kc_step: dt must be > 0");
+    if (!(a->time_dir == 1.0 || a->time_dir == -1.0)) return fail(c, KC_ERR_ARG, "kc_step: time_dir must be +-1");
+    if (a->w_code != 0 && a->w_code != 1) return fail(c, KC_ERR_ARG, "kc_step: w_code must be 0 or 1");
+    if (a->kick && !(a->kh_x >= 0.0 && a->kh_y >= 0.0)) return fail(c, KC_ERR_ARG, "kc_step: Kh must be >= 0");
+    int sl[3] = {a->slot_a, a->slot_b, a->slot_t};
+    int dtype = -1;
+    for (int k = 0; k < 3; ++k) {
+        if (sl[k] < 0 || sl[k] >= kSlots) return fail(c, KC_ERR_ARG, "kc_step: slot out of range");
+        const Slot& s = c->slots[sl[k]];
+        if (s.dtype < 0) return fail(c, KC_ERR_STATE, "kc_step: snapshot slot " + std::to_string(sl[k]) + " is empty");
+        if (s.n != c->N) return fail(c, KC_ERR_ARG, "kc_step: snapshot node count differs from the mesh");
+        if (dtype >= 0 && s.dtype != dtype) return fail(c, KC_ERR_ARG, "kc_step: snapshots of mixed element types");
+        dtype = s.dtype;
+        if (a->dims == 2 && s.uv_rows != 1) return fail(c, KC_ERR_ARG, "kc_step: 2-D step needs single-row u/v");
+        if (a->dims == 3) {
+            if (c->dm.K < 2) return fail(c, KC_ERR_STATE, "kc_step: 3-D step needs z-levels and depth");
+            if (s.uv_rows != c->dm.K - 1 || s.w_rows != c->dm.K)
+                return fail(c, KC_ERR_ARG, "kc_step: 3-D layer fields need u/v (K-1, N) and w (K, N)");
+        }
+    }
+    if (c->P > 0 && !c->lon) return fail(c, KC_ERR_STATE, "kc_step: no particles uploaded");
+    return KC_OK;
+}
+
+int do_step(kc_ctx* c, const kc_step_args* a) {
+    int rc = check_step(c, a);
+    if (rc) return rc;
+    if (c->slots[a->slot_a].dtype == KC_F32) return launch_step<float>(c, a);
+    return launch_step<double>(c, a);
+}
+
+template <typename T>
+int upload(kc_ctx* c, T** dst, const void* src, size_t count) {
+    KC_CUDA(c, cudaMalloc((void**)dst, std::max<size_t>(count, 1) * sizeof(T)));
+    if (count) KC_CUDA(c, cudaMemcpyAsync(*dst, src, count * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+    return KC_OK;
+}
+
+void free_mesh(kc_ctx* c) {
+    dfree(c->d_ll); dfree(c->d_en); dfree(c->d_n2e_off); dfree(c->d_n2e); dfree(c->d_gh_off);
+    dfree(c->d_gh_tab); dfree(c->d_xyz); dfree(c->d_depth); dfree(c->d_zlev);
+    c->has_mesh = false;
+}
+
+void free_particles(kc_ctx* c) {
+    dfree(c->lon); dfree(c->lat); dfree(c->z); dfree(c->U); dfree(c->V); dfree(c->W);
+    dfree(c->status); dfree(c->nn); dfree(c->fr); dfree(c->pid); dfree(c->rs);
+    c->P = c->cap = 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int kc_abi_version(void) { return KC_ABI_VERSION; }
+
+int kc_create(int device, kc_ctx** out) {
+    if (!out) return KC_ERR_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) return KC_ERR_CUDA;
+    if (cudaSetDevice(device) != cudaSuccess) return KC_ERR_CUDA;
+    kc_ctx* c = new kc_ctx();
+    c->device = device;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc((void**)&c->d_err, sizeof(int)) != cudaSuccess ||
+        cudaMemset(c->d_err, 0, sizeof(int)) != cudaSuccess) {
+        kc_destroy(c);
+        return KC_ERR_CUDA;
+    }
+    for (int k = 0; k < kEvents; ++k) cudaEventCreate(&c->ev[k]);
+    *out = c;
+    return KC_OK;
+}
+
+void kc_destroy(kc_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    free_mesh(c);
+    free_particles(c);
+    for (auto& s : c->slots) { dfree(s.u); dfree(s.v); dfree(s.w); }
+    dfree(c->q); dfree(c->qout); dfree(c->d_err);
+    for (int k = 0; k < kEvents; ++k) if (c->ev[k]) cudaEventDestroy(c->ev[k]);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+int kc_last_error(const kc_ctx* c, char* buf, int buflen) {
+    if (!c || !buf || buflen <= 0) return KC_ERR_ARG;
+    std::snprintf(buf, (size_t)buflen, "%s", c->err.c_str());
+    return KC_OK;
+}
+
+int kc_synchronize(kc_ctx* c) {
+    if (!c) return KC_ERR_ARG;
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KC_OK;
+}
+
+int kc_mesh_upload(kc_ctx* c, const kc_mesh_desc* d) {
+    if (!c || !d) return KC_ERR_ARG;
+    if (d->n_nodes <= 0 || d->n_elems <= 0) return fail(c, KC_ERR_ARG, "kc_mesh_upload: empty mesh");
+    if (d->max_v != 3 && d->max_v != 4) return fail(c, KC_ERR_ARG, "kc_mesh_upload: max_v must be 3 or 4");
+    if (!d->nodes_lon || !d->nodes_lat || !d->elem_nodes || !d->node_to_elems || !d->node_to_elems_count ||
+        !d->gh_offsets || !d->gh_node_ids || !d->node_xyz)
+        return fail(c, KC_ERR_ARG, "kc_mesh_upload: missing array");
+    if (d->gh_nx <= 0 || d->gh_ny <= 0 || !(d->gh_cell_size > 0.0))
+        return fail(c, KC_ERR_ARG, "kc_mesh_upload: invalid grid-hash geometry");
+    if (d->n_levels > 0 && (!d->z_levels || !d->depth))
+        return fail(c, KC_ERR_ARG, "kc_mesh_upload: 3-D mesh needs z_levels and depth");
+    KC_CUDA(c, cudaSetDevice(c->device));
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    free_mesh(c);
+    const long long N = d->n_nodes, E = d->n_elems;
+    const long long ncell = (long long)d->gh_nx * d->gh_ny;
+    // host-side validation of every index the kernels will follow
+    for (long long e = 0; e < E * d->max_v; ++e)
+        if (d->elem_nodes[e] >= N || d->elem_nodes[e] < -1)
+            return fail(c, KC_ERR_ARG, "kc_mesh_upload: elem_nodes index out of range");
+    if (d->gh_offsets[0] != 0 || d->gh_offsets[ncell] != N)
+        return fail(c, KC_ERR_ARG, "kc_mesh_upload: grid-hash offsets do not cover the nodes");
+    for (long long k = 0; k < ncell; ++k)
+        if (d->gh_offsets[k + 1] < d->gh_offsets[k]) return fail(c, KC_ERR_ARG, "kc_mesh_upload: offsets not monotone");
+    // repacked tables
+    std::vector<double2> ll((size_t)N);
+    for (long long i = 0; i < N; ++i) ll[i] = make_double2(d->nodes_lon[i], d->nodes_lat[i]);
+    std::vector<int4> en((size_t)E);
+    for (long long e = 0; e < E; ++e) {
+        const int* r = d->elem_nodes + e * d->max_v;
+        en[e] = make_int4(r[0], r[1], r[2], d->max_v == 4 ? r[3] : -1);
+    }
+    std::vector<int> off((size_t)N + 1);
+    std::vector<int> ids;
+    ids.reserve((size_t)N * 6);
+    off[0] = 0;
+    for (long long i = 0; i < N; ++i) {
+        int cnt = d->node_to_elems_count[i];
+        if (cnt < 0 || cnt > d->max_conn) return fail(c, KC_ERR_ARG, "kc_mesh_upload: node_to_elems_count out of range");
+        for (int k = 0; k < cnt; ++k) {
+            int el = d->node_to_elems[i * d->max_conn + k];
+            if (el >= E) return fail(c, KC_ERR_ARG, "kc_mesh_upload: node_to_elems index out of range");
+            if (el >= 0) ids.push_back(el);
+        }
+        off[i + 1] = (int)ids.size();
+    }
+    std::vector<double4> tab((size_t)N);
+    for (long long k = 0; k < N; ++k) {
+        int nd = d->gh_node_ids[k];
+        if (nd < 0 || nd >= N) return fail(c, KC_ERR_ARG, "kc_mesh_upload: gh_node_ids out of range");
+        tab[k] = make_double4(d->node_xyz[3 * (long long)nd], d->node_xyz[3 * (long long)nd + 1],
+                              d->node_xyz[3 * (long long)nd + 2], (double)nd);
+    }
+    int rc;
+    if ((rc = upload(c, &c->d_ll, ll.data(), ll.size()))) return rc;
+    if ((rc = upload(c, &c->d_en, en.data(), en.size()))) return rc;
+    if ((rc = upload(c, &c->d_n2e_off, off.data(), off.size()))) return rc;
+    if ((rc = upload(c, &c->d_n2e, ids.data(), ids.size()))) return rc;
+    if ((rc = upload(c, &c->d_gh_off, d->gh_offsets, (size_t)ncell + 1))) return rc;
+    if ((rc = upload(c, &c->d_gh_tab, tab.data(), tab.size()))) return rc;
+    if ((rc = upload(c, &c->d_xyz, d->node_xyz, (size_t)N * 3))) return rc;
+    if (d->depth && (rc = upload(c, &c->d_depth, d->depth, (size_t)N))) return rc;
+    if (d->n_levels > 0 && (rc = upload(c, &c->d_zlev, d->z_levels, (size_t)d->n_levels))) return rc;
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    kc::DMesh& m = c->dm;
+    m.ll = c->d_ll; m.en = c->d_en; m.n2e_off = c->d_n2e_off; m.n2e = c->d_n2e;
+    m.gh_off = c->d_gh_off; m.gh_tab = c->d_gh_tab; m.xyz = c->d_xyz;
+    m.depth = c->d_depth; m.zlev = c->d_zlev;
+    m.cell = d->gh_cell_size; m.lon_min = d->gh_lon_min; m.lat_min = d->gh_lat_min; m.r_earth = d->r_earth;
+    m.nx = d->gh_nx; m.ny = d->gh_ny; m.wrap = d->gh_wrap_lon ? 1 : 0; m.far_rows = d->gh_far_rows;
+    m.K = d->n_levels; m.exact = d->exact_nearest ? 1 : 0;
+    m.err = c->d_err;
+    c->N = N; c->E = E;
+    c->has_mesh = true;
+    return KC_OK;
+}
+
+int kc_field_upload(kc_ctx* c, int slot, int dtype, long long n_nodes, int n_uv_rows, const void* u,
+                    const void* v, int n_w_rows, const void* w) {
+    if (!c) return KC_ERR_ARG;
+    if (slot < 0 || slot >= kSlots) return fail(c, KC_ERR_ARG, "kc_field_upload: slot out of range");
+    if (dtype != KC_F32 && dtype != KC_F64) return fail(c, KC_ERR_ARG, "kc_field_upload: dtype");
+    if (n_nodes <= 0 || n_uv_rows <= 0 || !u || !v) return fail(c, KC_ERR_ARG, "kc_field_upload: empty u/v");
+    if (n_w_rows > 0 && !w) return fail(c, KC_ERR_ARG, "kc_field_upload: missing w");
+    KC_CUDA(c, cudaSetDevice(c->device));
+    Slot& s = c->slots[slot];
+    size_t es = dtype == KC_F32 ? 4 : 8;
+    size_t nuv = (size_t)n_nodes * n_uv_rows * es;
+    size_t nw = (size_t)n_nodes * (n_w_rows > 0 ? n_w_rows : 0) * es;
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (s.cap_uv < nuv) {
+        dfree(s.u); dfree(s.v);
+        KC_CUDA(c, cudaMalloc(&s.u, nuv));
+        KC_CUDA(c, cudaMalloc(&s.v, nuv));
+        s.cap_uv = nuv;
+    }
+    if (s.cap_w < nw) {
+        dfree(s.w);
+        KC_CUDA(c, cudaMalloc(&s.w, nw));
+        s.cap_w = nw;
+    }
+    KC_CUDA(c, cudaMemcpyAsync(s.u, u, nuv, cudaMemcpyHostToDevice, c->stream));
+    KC_CUDA(c, cudaMemcpyAsync(s.v, v, nuv, cudaMemcpyHostToDevice, c->stream));
+    if (nw) KC_CUDA(c, cudaMemcpyAsync(s.w, w, nw, cudaMemcpyHostToDevice, c->stream));
+    s.n = n_nodes; s.uv_rows = n_uv_rows; s.w_rows = n_w_rows > 0 ? n_w_rows : 0; s.dtype = dtype;
+    return KC_OK;
+}
+
+int kc_particles_upload(kc_ctx* c, long long P, const double* lon, const double* lat, const double* z,
+                        const int* status, const int* nn, const signed char* fr, const long long* pid,
+                        const int* rs) {
+    if (!c) return KC_ERR_ARG;
+    if (P < 0 || (P > 0 && (!lon || !lat || !status || !nn)))
+        return fail(c, KC_ERR_ARG, "kc_particles_upload: missing array");
+    KC_CUDA(c, cudaSetDevice(c->device));
+    if (P > c->cap) {
+        KC_CUDA(c, cudaStreamSynchronize(c->stream));
+        free_particles(c);
+        size_t n = (size_t)P;
+        KC_CUDA(c, cudaMalloc((void**)&c->lon, n * 8)); KC_CUDA(c, cudaMalloc((void**)&c->lat, n * 8));
+        KC_CUDA(c, cudaMalloc((void**)&c->z, n * 8)); KC_CUDA(c, cudaMalloc((void**)&c->U, n * 8));
+        KC_CUDA(c, cudaMalloc((void**)&c->V, n * 8)); KC_CUDA(c, cudaMalloc((void**)&c->W, n * 8));
+        KC_CUDA(c, cudaMalloc((void**)&c->status, n * 4)); KC_CUDA(c, cudaMalloc((void**)&c->nn, n * 4));
+        KC_CUDA(c, cudaMalloc((void**)&c->fr, n)); KC_CUDA(c, cudaMalloc((void**)&c->pid, n * 8));
+        KC_CUDA(c, cudaMalloc((void**)&c->rs, n * 4));
+        c->cap = P;
+    }
+    c->P = P;
+    if (P == 0) return KC_OK;
+    size_t n = (size_t)P;
+    cudaStream_t s = c->stream;
+    KC_CUDA(c, cudaMemcpyAsync(c->lon, lon, n * 8, cudaMemcpyHostToDevice, s));
+    KC_CUDA(c, cudaMemcpyAsync(c->lat, lat, n * 8, cudaMemcpyHostToDevice, s));
+    if (z) KC_CUDA(c, cudaMemcpyAsync(c->z, z, n * 8, cudaMemcpyHostToDevice, s));
+    else KC_CUDA(c, cudaMemsetAsync(c->z, 0, n * 8, s));
+    KC_CUDA(c, cudaMemcpyAsync(c->status, status, n * 4, cudaMemcpyHostToDevice, s));
+    KC_CUDA(c, cudaMemcpyAsync(c->nn, nn, n * 4, cudaMemcpyHostToDevice, s));
+    if (fr) KC_CUDA(c, cudaMemcpyAsync(c->fr, fr, n, cudaMemcpyHostToDevice, s));
+    else KC_CUDA(c, cudaMemsetAsync(c->fr, 0, n, s));
+    c->has_pid = pid != nullptr;
+    if (pid) KC_CUDA(c, cudaMemcpyAsync(c->pid, pid, n * 8, cudaMemcpyHostToDevice, s));
+    c->has_rs = rs != nullptr;
+    if (rs) KC_CUDA(c, cudaMemcpyAsync(c->rs, rs, n * 4, cudaMemcpyHostToDevice, s));
+    KC_CUDA(c, cudaMemsetAsync(c->U, 0, n * 8, s));
+    KC_CUDA(c, cudaMemsetAsync(c->V, 0, n * 8, s));
+    KC_CUDA(c, cudaMemsetAsync(c->W, 0, n * 8, s));
+    return KC_OK;
+}
+
+int kc_particles_download(kc_ctx* c, long long P, double* lon, double* lat, double* z, int* status, int* nn,
+                          signed char* fr, double* u, double* v, double* w) {
+    if (!c) return KC_ERR_ARG;
+    if (P != c->P) return fail(c, KC_ERR_ARG, "kc_particles_download: P differs from the resident count");
+    if (P == 0) return KC_OK;
+    KC_CUDA(c, cudaSetDevice(c->device));
+    size_t n = (size_t)P;
+    cudaStream_t s = c->stream;
+    if (lon) KC_CUDA(c, cudaMemcpyAsync(lon, c->lon, n * 8, cudaMemcpyDeviceToHost, s));
+    if (lat) KC_CUDA(c, cudaMemcpyAsync(lat, c->lat, n * 8, cudaMemcpyDeviceToHost, s));
+    if (z) KC_CUDA(c, cudaMemcpyAsync(z, c->z, n * 8, cudaMemcpyDeviceToHost, s));
+    if (status) KC_CUDA(c, cudaMemcpyAsync(status, c->status, n * 4, cudaMemcpyDeviceToHost, s));
+    if (nn) KC_CUDA(c, cudaMemcpyAsync(nn, c->nn, n * 4, cudaMemcpyDeviceToHost, s));
+    if (fr) KC_CUDA(c, cudaMemcpyAsync(fr, c->fr, n, cudaMemcpyDeviceToHost, s));
+    if (u) KC_CUDA(c, cudaMemcpyAsync(u, c->U, n * 8, cudaMemcpyDeviceToHost, s));
+    if (v) KC_CUDA(c, cudaMemcpyAsync(v, c->V, n * 8, cudaMemcpyDeviceToHost, s));
+    if (w) KC_CUDA(c, cudaMemcpyAsync(w, c->W, n * 8, cudaMemcpyDeviceToHost, s));
+    KC_CUDA(c, cudaStreamSynchronize(s));
+    return KC_OK;
+}
+
+int kc_step(kc_ctx* c, const kc_step_args* a) {
+    if (!c) return KC_ERR_ARG;
+    return do_step(c, a);
+}
+
+int kc_run(kc_ctx* c, const kc_step_args* steps, int n_steps) {
+    if (!c) return KC_ERR_ARG;
+    if (n_steps < 0 || (n_steps > 0 && !steps)) return fail(c, KC_ERR_ARG, "kc_run: bad step list");
+    for (int k = 0; k < n_steps; ++k) {
+        int rc = check_step(c, &steps[k]);
+        if (rc) return rc;
+    }
+    for (int k = 0; k < n_steps; ++k) {
+        int rc = do_step(c, &steps[k]);
+        if (rc) return rc;
+    }
+    return KC_OK;
+}
+
+int kc_find_nearest(kc_ctx* c, long long P, const double* lon, const double* lat, int* out) {
+    if (!c) return KC_ERR_ARG;
+    if (!c->has_mesh) return fail(c, KC_ERR_STATE, "kc_find_nearest: no mesh uploaded");
+    if (P < 0 || (P > 0 && (!lon || !lat || !out))) return fail(c, KC_ERR_ARG, "kc_find_nearest: arrays");
+    if (P == 0) return KC_OK;
+    KC_CUDA(c, cudaSetDevice(c->device));
+    if (P > c->qcap) {
+        KC_CUDA(c, cudaStreamSynchronize(c->stream));
+        dfree(c->q); dfree(c->qout);
+        KC_CUDA(c, cudaMalloc((void**)&c->q, (size_t)P * 16));
+        KC_CUDA(c, cudaMalloc((void**)&c->qout, (size_t)P * 4));
+        c->qcap = P;
+    }
+    KC_CUDA(c, cudaMemcpyAsync(c->q, lon, (size_t)P * 8, cudaMemcpyHostToDevice, c->stream));
+    KC_CUDA(c, cudaMemcpyAsync(c->q + P, lat, (size_t)P * 8, cudaMemcpyHostToDevice, c->stream));
+    k_nearest<<<grid_for(P), kBlock, 0, c->stream>>>(c->dm, c->q, P, c->qout);
+    KC_CUDA(c, cudaGetLastError());
+    KC_CUDA(c, cudaMemcpyAsync(out, c->qout, (size_t)P * 4, cudaMemcpyDeviceToHost, c->stream));
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KC_OK;
+}
+
+int kc_device_errors(kc_ctx* c, int* word) {
+    if (!c || !word) return KC_ERR_ARG;
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    KC_CUDA(c, cudaMemcpy(word, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    KC_CUDA(c, cudaMemset(c->d_err, 0, sizeof(int)));
+    return KC_OK;
+}
+
+int kc_event_record(kc_ctx* c, int slot) {
+    if (!c || slot < 0 || slot >= kEvents) return KC_ERR_ARG;
+    KC_CUDA(c, cudaEventRecord(c->ev[slot], c->stream));
+    return KC_OK;
+}
+
+int kc_event_elapsed(kc_ctx* c, int a, int b, float* ms) {
+    if (!c || !ms || a < 0 || b < 0 || a >= kEvents || b >= kEvents) return KC_ERR_ARG;
+    KC_CUDA(c, cudaEventSynchronize(c->ev[b]));
+    KC_CUDA(c, cudaEventElapsedTime(ms, c->ev[a], c->ev[b]));
+    return KC_OK;
+}
+
+int kc_host_alloc(long long bytes, void** out) {
+    if (!out || bytes < 0) return KC_ERR_ARG;
+    return cudaMallocHost(out, (size_t)std::max<long long>(bytes, 1)) == cudaSuccess ? KC_OK : KC_ERR_CUDA;
+}
+
+int kc_host_free(void* p) {
+    if (!p) return KC_OK;
+    return cudaFreeHost(p) == cudaSuccess ? KC_OK : KC_ERR_CUDA;
+}
+
+}  // extern "C"

@@ -1,0 +1,605 @@
+// Device-side geometry of the KELP time-stepping path: Python-semantics
+// modulo, grid-hash cell lookup, exact nearest-node search with its
+// certificate, element containment and vertex weights.
+//
+// Every routine restates a KELP Numba function (file:line in its comment)
+// with the same floating-point operation order.  This translation unit is
+// compiled with -fmad=false: Numba emits no fused multiply-adds, so a
+// contracted a*b+c here would round differently and could flip an anchor or
+// a containment verdict.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace kc {
+
+constexpr double DEG2RAD = 0.017453292519943295;   // pi / 180
+constexpr double RAD2DEG = 57.29577951308232;      // 180 / pi
+constexpr double SLM = 111120.0;                   // metres per degree of latitude
+constexpr double R_STD = 6371000.0;                // standard Earth radius
+constexpr double BARY_EPS = -1e-6;                 // mesh.py:33
+constexpr double AREA_TOL = 1e-10;                 // mesh.py:32
+constexpr double INF30 = 1.0e30;
+constexpr int SHORT_ROW_CELLS = 32;                // mesh.py:1608
+constexpr int ALIVE = 1, BEACHED = 2, OUTSIDE = 3, NOT_RELEASED = 4;
+constexpr int FR_INTERP = 1, FR_OOB = 2;
+
+// device error word bits (read back by the host)
+constexpr int ERR_SEARCH_CAP = 1;   // exact-search growth loop hit its cap
+constexpr int ERR_RING_CAP = 2;     // widened ring search hit its cap
+
+// Resident mesh: node table, element table, node->element CSR, grid hash.
+struct DMesh {
+    const double2* ll;        // (N) node lon, lat in degrees
+    const int4* en;           // (E) element nodes, -1 padded to 4
+    const int* n2e_off;       // (N+1) CSR offsets of the node->element table
+    const int* n2e;           // element ids, per node in the reference order
+    const int* gh_off;        // (nx*ny+1) CSR offsets of the grid hash
+    const double4* gh_tab;    // hash-ordered {x, y, z, node id} unit-sphere table
+    const double* xyz;        // (N, 3) unit-sphere table by node id
+    const double* depth;      // (N) bottom depth, positive down (3-D)
+    const double* zlev;       // (K) z-level interfaces, positive down (3-D)
+    double cell, lon_min, lat_min, r_earth;
+    int nx, ny, wrap, far_rows, K, exact;
+    int* err;                 // device error word
+};
+
+// Python float modulo for a positive divisor (CPython float_rem, Numba
+// real_divmod): the remainder carries the divisor's sign, zero is +0.
+__device__ __forceinline__ double pymod(double x, double m) {
+    double r = fmod(x, m);
+    if (r != 0.0) {
+        if (r < 0.0) r += m;
+    } else {
+        r = 0.0;
+    }
+    return r;
+}
+
+// ((x + 180) % 360) - 180
+__device__ __forceinline__ double wrap180(double x) { return pymod(x + 180.0, 360.0) - 180.0; }
+
+// Python integer modulo for a positive divisor.
+__device__ __forceinline__ int imod(int a, int n) {
+    int r = a % n;
+    return r < 0 ? r + n : r;
+}
+
+// mesh.py:1192-1207 _gh_fold_dlon
+__device__ __forceinline__ double gh_fold_dlon(const DMesh& m, double lon_p) {
+    double dlon = pymod(lon_p - m.lon_min, 360.0);
+    if (!m.wrap) {
+        double grid_span = (double)m.nx * m.cell;
+        if (dlon > grid_span && (dlon - grid_span) > (360.0 - dlon)) dlon -= 360.0;
+    }
+    return dlon;
+}
+
+// mesh.py:1210-1232 _gh_cell_of (int() truncates toward zero)
+__device__ __forceinline__ void gh_cell_of(const DMesh& m, double lon_p, double lat_p, int& ci, int& cj) {
+    double dlon = gh_fold_dlon(m, lon_p);
+    ci = (int)(dlon / m.cell);
+    cj = (int)((lat_p - m.lat_min) / m.cell);
+    if (ci < 0) ci = 0;
+    if (ci >= m.nx) ci = m.nx - 1;
+    if (cj < 0) cj = 0;
+    if (cj >= m.ny) cj = m.ny - 1;
+}
+
+// Query point on the unit sphere (mesh.py:1268-1273); also returns cos(lat).
+__device__ __forceinline__ void query_xyz(double lon_p, double lat_p, double& xp, double& yp, double& zp, double& cos_lat) {
+    double lat_r = lat_p * DEG2RAD;
+    double lon_r = lon_p * DEG2RAD;
+    double cl = cos(lat_r);
+    xp = cl * cos(lon_r);
+    yp = cl * sin(lon_r);
+    zp = sin(lat_r);
+    cos_lat = cl;
+}
+
+// Scan hash-table positions [s, e): strict '<' keeps the first node found
+// on a tie, which makes the CSR order part of the contract (mesh.py:1290-1301).
+__device__ __forceinline__ void scan_range(const double4* __restrict__ tab, int s, int e,
+                                           double xp, double yp, double zp, int& best, double& bd2) {
+    for (int k = s; k < e; ++k) {
+        const double2* p = reinterpret_cast<const double2*>(tab + k);
+        double2 t0 = __ldg(p), t1 = __ldg(p + 1);
+        double dx = t0.x - xp, dy = t0.y - yp, dz = t1.x - zp;
+        double d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 < bd2) { bd2 = d2; best = (int)t1.y; }
+    }
+}
+
+__device__ __forceinline__ void scan_cell(const DMesh& m, int cell, double xp, double yp, double zp, int& best, double& bd2) {
+    scan_range(m.gh_tab, __ldg(&m.gh_off[cell]), __ldg(&m.gh_off[cell + 1]), xp, yp, zp, best, bd2);
+}
+
+// mesh.py:1235-1303 _grid_hash_nearest_3x3.  Adjacent columns of one row are
+// adjacent in the CSR, so an unclipped, unwrapped row is one contiguous slice
+// (same nodes, same order as three cell scans).
+__device__ __forceinline__ int nearest_3x3(const DMesh& m, double lon_p, double lat_p,
+                                           double xp, double yp, double zp, double& bd2_out) {
+    int ci, cj;
+    gh_cell_of(m, lon_p, lat_p, ci, cj);
+    int best = -1;
+    double bd2 = 1e30;
+    for (int dj = -1; dj <= 1; ++dj) {
+        int cj2 = cj + dj;
+        if (cj2 < 0 || cj2 >= m.ny) continue;
+        int row = cj2 * m.nx;
+        if (ci >= 1 && ci + 1 < m.nx) {
+            scan_range(m.gh_tab, __ldg(&m.gh_off[row + ci - 1]), __ldg(&m.gh_off[row + ci + 2]), xp, yp, zp, best, bd2);
+        } else {
+            for (int di = -1; di <= 1; ++di) {
+                int ci2 = ci + di;
+                if (ci2 < 0) ci2 = m.wrap ? ci2 + m.nx : -1;
+                else if (ci2 >= m.nx) ci2 = m.wrap ? ci2 - m.nx : -1;
+                if (ci2 < 0) continue;
+                scan_cell(m, row + ci2, xp, yp, zp, best, bd2);
+            }
+        }
+    }
+    bd2_out = bd2;
+    return best;
+}
+
+// mesh.py:1306-1328 _cap_extents -> (theta_deg, ext_lon_deg)
+__device__ __forceinline__ void cap_extents(double lon_p, double lat_p, double lon_n, double lat_n,
+                                            double& theta_deg, double& ext) {
+    double lat_pr = lat_p * DEG2RAD;
+    double lat_nr = lat_n * DEG2RAD;
+    double cosd = sin(lat_pr) * sin(lat_nr) + cos(lat_pr) * cos(lat_nr) * cos((lon_p - lon_n) * DEG2RAD);
+    if (cosd > 1.0) cosd = 1.0;
+    if (cosd < -1.0) cosd = -1.0;
+    double theta = acos(cosd);
+    if (theta <= 0.0) { theta_deg = 0.0; ext = 0.0; return; }
+    theta_deg = theta * RAD2DEG;
+    if (fabs(lat_p) + theta_deg >= 90.0) { ext = 1.0e30; return; }
+    double r = sin(theta) / cos(lat_pr);
+    if (r >= 1.0) { ext = 1.0e30; return; }
+    ext = asin(r) * RAD2DEG;
+}
+
+// mesh.py:1475-1549 _anchor_provable_rect: 0 when `node` is provably the
+// nearest for the (2rx+1) x (2ry+1) window, else a deficit bitmask.
+__device__ __noinline__ int anchor_provable_rect(const DMesh& m, double lon_p, double lat_p, int node, int rx, int ry) {
+    double2 nl = __ldg(&m.ll[node]);
+    double theta_deg, ext_lon;
+    cap_extents(lon_p, lat_p, nl.x, nl.y, theta_deg, ext_lon);
+    if (theta_deg <= 0.0) return 0;
+    double dlon = gh_fold_dlon(m, lon_p);
+    double lon_q = m.lon_min + dlon;
+    int ci_raw = (int)floor(dlon / m.cell);
+    int cj_raw = (int)floor((lat_p - m.lat_min) / m.cell);
+    const double INF = 1.0e30;
+    int cj = cj_raw;
+    if (cj < 0) cj = 0;
+    if (cj > m.ny - 1) cj = m.ny - 1;
+    double cov_dn = (cj - ry >= 0) ? lat_p - (m.lat_min + (double)(cj - ry) * m.cell) : INF;
+    double cov_up = (cj + ry <= m.ny - 1) ? (m.lat_min + (double)(cj + ry + 1) * m.cell) - lat_p : INF;
+    int code = 0;
+    if (theta_deg > cov_dn || theta_deg > cov_up) code |= 1;
+    if (m.wrap) {
+        if (2 * rx + 1 >= m.nx) return code;
+        if (ext_lon >= INF) return code | 4;
+        double w_last = 360.0 - (double)(m.nx - 1) * m.cell;
+        int ci = imod(ci_raw, m.nx);
+        double left = m.lon_min + (double)(ci - rx) * m.cell;
+        if (ci - rx < 0) left += m.cell - w_last;
+        double right = m.lon_min + (double)(ci + rx + 1) * m.cell;
+        if (ci + rx >= m.nx - 1) right -= m.cell - w_last;
+        if (ext_lon > lon_q - left || ext_lon > right - lon_q) code |= 2;
+        return code;
+    }
+    int ci = ci_raw;
+    if (ci < 0) ci = 0;
+    if (ci > m.nx - 1) ci = m.nx - 1;
+    double cov_l = (ci - rx >= 0) ? lon_q - (m.lon_min + (double)(ci - rx) * m.cell) : INF;
+    double cov_r = (ci + rx <= m.nx - 1) ? (m.lon_min + (double)(ci + rx + 1) * m.cell) - lon_q : INF;
+    if (cov_l >= INF && cov_r >= INF) return code;
+    if (ext_lon >= INF) return code | 4;
+    if (ext_lon > cov_l || ext_lon > cov_r) code |= 2;
+    double n_lo = m.lon_min + m.cell;
+    double n_hi = m.lon_min + (double)(m.nx - 1) * m.cell;
+    for (int s = 0; s < 2; ++s) {
+        double shift = s == 0 ? -360.0 : 360.0;
+        double a = lon_q - ext_lon + shift;
+        double b = lon_q + ext_lon + shift;
+        if (b >= n_lo && a <= n_hi) return code | 4;
+    }
+    return code;
+}
+
+// mesh.py:1331-1442 _grid_hash_nearest_widened: the 3x3 window, and on an
+// empty window a ring-by-ring scan that stops one ring after the first hit.
+__device__ __noinline__ int nearest_widened(const DMesh& m, double lon_p, double lat_p) {
+    double xp, yp, zp, cl, bd2;
+    query_xyz(lon_p, lat_p, xp, yp, zp, cl);
+    int best = nearest_3x3(m, lon_p, lat_p, xp, yp, zp, bd2);
+    if (best >= 0) return best;
+    int ci, cj;
+    gh_cell_of(m, lon_p, lat_p, ci, cj);
+    bd2 = 1e30;
+    int max_ring = m.nx > m.ny ? m.nx : m.ny;
+    int found_ring = -1;
+    for (int r = 2; r <= max_ring; ++r) {
+        for (int dj = -r; dj <= r; ++dj) {
+            int cj2 = cj + dj;
+            if (cj2 < 0 || cj2 >= m.ny) continue;
+            int di_step = (dj == -r || dj == r) ? 1 : 2 * r;
+            for (int di = -r; di <= r; di += di_step) {
+                int ci2 = ci + di;
+                if (m.wrap) ci2 = imod(ci2, m.nx);
+                else if (ci2 < 0 || ci2 >= m.nx) continue;
+                scan_cell(m, cj2 * m.nx + ci2, xp, yp, zp, best, bd2);
+            }
+        }
+        if (best >= 0) {
+            if (found_ring < 0) found_ring = r;
+            else if (r > found_ring) break;
+        }
+    }
+    return best;
+}
+
+// mesh.py:1552-1605 row slices
+__device__ __forceinline__ void scan_row_range(const DMesh& m, int cj2, int c_lo, int c_hi,
+                                               double xp, double yp, double zp, int& best, double& bd2) {
+    scan_range(m.gh_tab, __ldg(&m.gh_off[cj2 * m.nx + c_lo]), __ldg(&m.gh_off[cj2 * m.nx + c_hi + 1]), xp, yp, zp, best, bd2);
+}
+
+__device__ __forceinline__ void scan_row_window(const DMesh& m, int cj2, int ci, int rx,
+                                                double xp, double yp, double zp, int& best, double& bd2) {
+    if (m.wrap && 2 * rx + 1 >= m.nx) { scan_row_range(m, cj2, 0, m.nx - 1, xp, yp, zp, best, bd2); return; }
+    int c_lo = ci - rx, c_hi = ci + rx;
+    if (m.wrap) {
+        if (c_lo < 0) {
+            scan_row_range(m, cj2, c_lo + m.nx, m.nx - 1, xp, yp, zp, best, bd2);
+            c_lo = 0;
+        } else if (c_hi > m.nx - 1) {
+            scan_row_range(m, cj2, 0, c_hi - m.nx, xp, yp, zp, best, bd2);
+            c_hi = m.nx - 1;
+        }
+    } else {
+        if (c_lo < 0) c_lo = 0;
+        if (c_hi > m.nx - 1) c_hi = m.nx - 1;
+    }
+    scan_row_range(m, cj2, c_lo, c_hi, xp, yp, zp, best, bd2);
+}
+
+
+// mesh.py:1611-1859 _grid_hash_nearest_exact: the 3x3 window accepted when
+// the certificate proves it, else a rectangle grown by the certificate's
+// deficits until the best node is provable, every cell is scanned, or the
+// row budget `far_rows` says the query is outside every element.
+__device__ __noinline__ int nearest_exact_slow(const DMesh& m, double lon_p, double lat_p, int best, int code);
+
+__device__ __forceinline__ int nearest_exact(const DMesh& m, double lon_p, double lat_p,
+                                             double xp, double yp, double zp) {
+    const double far = (double)m.far_rows * m.cell;
+    if (lat_p < m.lat_min - far || lat_p > m.lat_min + (double)m.ny * m.cell + far)
+        return nearest_widened(m, lon_p, lat_p);
+    double bd2;
+    int best = nearest_3x3(m, lon_p, lat_p, xp, yp, zp, bd2);
+    int code = 0;
+    if (best >= 0) {
+        code = anchor_provable_rect(m, lon_p, lat_p, best, 1, 1);
+        if (code == 0) return best;
+    }
+    return nearest_exact_slow(m, lon_p, lat_p, best, code);
+}
+
+__device__ __noinline__ int nearest_exact_slow(const DMesh& m, double lon_p, double lat_p, int best, int code) {
+    const double far = (double)m.far_rows * m.cell;
+    if (best >= 0) {
+        double2 nl = __ldg(&m.ll[best]);
+        double theta_deg, ext;
+        cap_extents(lon_p, lat_p, nl.x, nl.y, theta_deg, ext);
+        if (theta_deg > far) return best;
+    }
+    int ci, cj;
+    gh_cell_of(m, lon_p, lat_p, ci, cj);
+    double xp, yp, zp, cos_lat_p;
+    query_xyz(lon_p, lat_p, xp, yp, zp, cos_lat_p);
+    double best_d2 = 1.0e30;
+    if (best >= 0) {
+        double xn = m.xyz[3 * (long long)best], yn = m.xyz[3 * (long long)best + 1], zn = m.xyz[3 * (long long)best + 2];
+        double dx = xn - xp, dy = yn - yp, dz = zn - zp;
+        best_d2 = dx * dx + dy * dy + dz * dz;
+    }
+    int rx = 1, ry = 1;
+    bool short_row = 360.0 * cos_lat_p <= (double)SHORT_ROW_CELLS * m.cell;
+    int rx_max;
+    if (m.wrap) {
+        rx_max = m.nx / 2;
+        if (rx_max < 1) rx_max = 1;
+    } else {
+        rx_max = ci > m.nx - 1 - ci ? ci : m.nx - 1 - ci;
+    }
+    int ry_max = cj > m.ny - 1 - cj ? cj : m.ny - 1 - cj;
+    double abs_lat = lat_p >= 0.0 ? lat_p : -lat_p;
+    double dlon_q = gh_fold_dlon(m, lon_p);
+    const double INF = 1.0e30;
+    // each pass grows rx or ry by at least one, or returns
+    const int cap = 4 * (m.nx + m.ny) + 16;
+    for (int it = 0; it < cap; ++it) {
+        if (best >= 0 && code == 0) {
+            code = anchor_provable_rect(m, lon_p, lat_p, best, rx, ry);
+            if (code == 0) return best;
+        }
+        if (best < 0 || 2.0 * asin(0.5 * sqrt(best_d2)) * RAD2DEG > far) {
+            bool cols_full;
+            if (m.wrap) cols_full = 2 * rx + 1 >= m.nx;
+            else cols_full = ci - rx <= 0 && ci + rx >= m.nx - 1;
+            double clear = ry >= ry_max ? INF : (double)ry * m.cell;
+            if (!cols_full) {
+                double lat_edge = abs_lat + (double)(ry + 1) * m.cell;
+                double clear_lon;
+                if (lat_edge >= 90.0) {
+                    clear_lon = 0.0;
+                } else {
+                    double dl = (double)rx * m.cell;
+                    if (!m.wrap) {
+                        double x = dlon_q > 0.0 ? dlon_q : 0.0;
+                        double w = (double)m.nx * m.cell;
+                        if (x > w) x = w;
+                        double near_edge = x < w - x ? x : w - x;
+                        double dl_cut = 360.0 - w + near_edge;
+                        if (dl_cut < dl) dl = dl_cut;
+                    }
+                    if (dl > 180.0) dl = 180.0;
+                    clear_lon = asin(sin(dl * DEG2RAD) * cos(lat_edge * DEG2RAD)) * RAD2DEG;
+                }
+                if (clear_lon < clear) clear = clear_lon;
+            }
+            if (clear >= far) {
+                if (best >= 0) return best;
+                return nearest_widened(m, lon_p, lat_p);
+            }
+        }
+        bool grow_x, grow_y, all_x;
+        if (best >= 0) {
+            grow_x = (code & 2) != 0;
+            grow_y = (code & 1) != 0;
+            all_x = (code & 4) != 0;
+            code = 0;
+        } else if (short_row) {
+            grow_x = false; grow_y = true; all_x = true;
+        } else {
+            grow_x = true; grow_y = true; all_x = false;
+        }
+        if (rx >= rx_max) { grow_x = false; all_x = false; }
+        if (ry >= ry_max) grow_y = false;
+        if (!(grow_x || grow_y || all_x)) {
+            if (best >= 0) return best;
+            return nearest_widened(m, lon_p, lat_p);
+        }
+        int rx_new = all_x ? rx_max : (grow_x ? rx + 1 : rx);
+        int ry_new = grow_y ? ry + 1 : ry;
+        int j_lo = cj - ry > 0 ? cj - ry : 0;
+        int j_hi = cj + ry < m.ny - 1 ? cj + ry : m.ny - 1;
+        if (rx_new > rx) {
+            if (m.wrap && 2 * rx_new + 1 >= m.nx && rx_new - rx > 1) {
+                for (int cj2 = j_lo; cj2 <= j_hi; ++cj2) {
+                    int c_lo = imod(ci + rx + 1, m.nx);
+                    int c_hi = imod(ci - rx - 1, m.nx);
+                    if (c_lo <= c_hi) {
+                        scan_row_range(m, cj2, c_lo, c_hi, xp, yp, zp, best, best_d2);
+                    } else {
+                        scan_row_range(m, cj2, c_lo, m.nx - 1, xp, yp, zp, best, best_d2);
+                        scan_row_range(m, cj2, 0, c_hi, xp, yp, zp, best, best_d2);
+                    }
+                }
+            } else if (!m.wrap && rx_new - rx > 1) {
+                for (int cj2 = j_lo; cj2 <= j_hi; ++cj2) {
+                    if (ci - rx - 1 >= 0) {
+                        int c_lo = ci - rx_new > 0 ? ci - rx_new : 0;
+                        scan_row_range(m, cj2, c_lo, ci - rx - 1, xp, yp, zp, best, best_d2);
+                    }
+                    if (ci + rx + 1 <= m.nx - 1) {
+                        int c_hi = ci + rx_new < m.nx - 1 ? ci + rx_new : m.nx - 1;
+                        scan_row_range(m, cj2, ci + rx + 1, c_hi, xp, yp, zp, best, best_d2);
+                    }
+                }
+            } else {
+                for (int r = rx + 1; r <= rx_new; ++r) {
+                    if (m.wrap) {
+                        int c_left = imod(ci - r, m.nx);
+                        bool two = 2 * r + 1 <= m.nx;
+                        int c_right = imod(ci + r, m.nx);
+                        for (int cj2 = j_lo; cj2 <= j_hi; ++cj2) {
+                            scan_cell(m, cj2 * m.nx + c_left, xp, yp, zp, best, best_d2);
+                            if (two) scan_cell(m, cj2 * m.nx + c_right, xp, yp, zp, best, best_d2);
+                        }
+                    } else {
+                        for (int side = 0; side < 2; ++side) {
+                            int c2 = side == 0 ? ci - r : ci + r;
+                            if (c2 < 0 || c2 > m.nx - 1) continue;
+                            for (int cj2 = j_lo; cj2 <= j_hi; ++cj2)
+                                scan_cell(m, cj2 * m.nx + c2, xp, yp, zp, best, best_d2);
+                        }
+                    }
+                }
+            }
+        }
+        for (int r = ry + 1; r <= ry_new; ++r) {
+            for (int side = 0; side < 2; ++side) {
+                int cj2 = side == 0 ? cj - r : cj + r;
+                if (cj2 < 0 || cj2 > m.ny - 1) continue;
+                scan_row_window(m, cj2, ci, rx_new, xp, yp, zp, best, best_d2);
+            }
+        }
+        rx = rx_new;
+        ry = ry_new;
+    }
+    atomicOr(m.err, ERR_SEARCH_CAP);
+    return best;
+}
+
+// The anchor of one evaluation site (integrators.py:1470-1487).
+__device__ __forceinline__ int site_anchor(const DMesh& m, double lon_p, double lat_p) {
+    if (!m.exact) return nearest_widened(m, lon_p, lat_p);
+    double xp, yp, zp, cl;
+    query_xyz(lon_p, lat_p, xp, yp, zp, cl);
+    return nearest_exact(m, lon_p, lat_p, xp, yp, zp);
+}
+
+// ---------------------------------------------------------------------------
+// Containment and weights
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ int elem_node(const int4& e, int k) {
+    return k == 0 ? e.x : (k == 1 ? e.y : (k == 2 ? e.z : e.w));
+}
+
+// mesh.py:2054-2073 _barycentric_weights_tri; false on a degenerate triangle
+// (the reference's [-1, -1, -1] sentinel).
+__device__ __forceinline__ bool bary_tri(double px, double py, double ax, double ay, double bx, double by,
+                                         double cx, double cy, double& w1, double& w2, double& w3) {
+    double denom = (by - cy) * (ax - cx) + (cx - bx) * (ay - cy);
+    if (fabs(denom) < AREA_TOL) { w1 = w2 = w3 = -1.0; return false; }
+    w1 = ((by - cy) * (px - cx) + (cx - bx) * (py - cy)) / denom;
+    w2 = ((cy - ay) * (px - cx) + (ax - cx) * (py - cy)) / denom;
+    w3 = 1.0 - w1 - w2;
+    return true;
+}
+
+// mesh.py:2076-2116 _wachspress_weights_quad (product form)
+__device__ __forceinline__ void wachspress_quad(double px, double py, const double* x, const double* y, double* out) {
+    double A[4], C[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        int i1 = (k + 1) & 3, im = (k + 3) & 3;
+        A[k] = (x[k] - px) * (y[i1] - py) - (x[i1] - px) * (y[k] - py);
+        C[k] = (x[k] - x[im]) * (y[i1] - y[im]) - (x[i1] - x[im]) * (y[k] - y[im]);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        double w = C[k] * A[(k + 1) & 3] * A[(k + 2) & 3];
+        out[k] = w;
+        s += w;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) out[k] = out[k] / s;
+}
+
+// mesh.py:2119-2136 _polygon_weights; returns false only for the degenerate
+// triangle sentinel (w[0] == -1.0 is what the callers test).
+__device__ __forceinline__ bool polygon_weights(double px, double py, const double* x, const double* y, int nv, double* w) {
+    if (nv == 3) {
+        bary_tri(px, py, x[0], y[0], x[1], y[1], x[2], y[2], w[0], w[1], w[2]);
+        return !(w[0] == -1.0);
+    }
+    wachspress_quad(px, py, x, y, w);
+    return !(w[0] == -1.0);
+}
+
+// mesh.py:2210-2263 _element_contains with mesh.py:2006-2051
+// _project_to_local_xy and mesh.py:2139-2168 _polygon_contains_bool.
+__device__ __forceinline__ bool element_contains(const DMesh& m, int c, double lon_p, double lat_p) {
+    int4 e = __ldg(&m.en[c]);
+    int nodes[4] = {e.x, e.y, e.z, e.w};
+    bool mask[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) mask[k] = nodes[k] >= 0;
+    if (nodes[3] == nodes[0] && nodes[0] >= 0) mask[3] = false;
+    int n = 0;
+    double ln[4], la[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (mask[k]) {
+            double2 p = __ldg(&m.ll[nodes[k]]);
+            ln[n] = p.x;
+            la[n] = p.y;
+            ++n;
+        }
+    }
+    if (n < 3) return false;
+    // bbox prefilter in wrapped-delta space around the first valid vertex
+    double lon_ref = ln[0];
+    double dmin = 0.0, dmax = 0.0, lamin = la[0], lamax = la[0];
+    for (int k = 0; k < n; ++k) {
+        double d = wrap180(ln[k] - lon_ref);
+        if (k == 0) { dmin = d; dmax = d; }
+        else { if (d < dmin) dmin = d; if (d > dmax) dmax = d; }
+        if (la[k] > lamax) lamax = la[k];
+        if (la[k] < lamin) lamin = la[k];
+    }
+    double dlon_p = wrap180(lon_p - lon_ref);
+    if (dlon_p > dmax || dlon_p < dmin) return false;
+    if (lat_p > lamax || lat_p < lamin) return false;
+    // local projection: raw-mean origin unless the element spans > 180 deg
+    double lmin = ln[0], lmax = ln[0];
+    for (int k = 0; k < n; ++k) {
+        if (ln[k] < lmin) lmin = ln[k];
+        if (ln[k] > lmax) lmax = ln[k];
+    }
+    double lon0;
+    if (lmax - lmin > 180.0) {
+        double ref = ln[0], dsum = 0.0;
+        for (int k = 0; k < n; ++k) dsum += wrap180(ln[k] - ref);
+        lon0 = ref + dsum / (double)n;
+    } else {
+        double s = 0.0;
+        for (int k = 0; k < n; ++k) s += ln[k];
+        lon0 = s / (double)n;
+    }
+    double s = 0.0;
+    for (int k = 0; k < n; ++k) s += la[k];
+    double lat0 = s / (double)n;
+    double cos_lat0 = cos(lat0 * DEG2RAD);
+    double x[4], y[4];
+    for (int k = 0; k < n; ++k) {
+        x[k] = wrap180(ln[k] - lon0) * DEG2RAD * R_STD * cos_lat0;
+        y[k] = (la[k] - lat0) * DEG2RAD * R_STD;
+    }
+    double px = wrap180(lon_p - lon0) * DEG2RAD * R_STD * cos_lat0;
+    double py = (lat_p - lat0) * DEG2RAD * R_STD;
+    double w1, w2, w3;
+    if (n == 3) {
+        bary_tri(px, py, x[0], y[0], x[1], y[1], x[2], y[2], w1, w2, w3);
+        return w1 >= BARY_EPS && w2 >= BARY_EPS && w3 >= BARY_EPS;
+    }
+    for (int i = 1; i < n - 1; ++i) {
+        bary_tri(px, py, x[0], y[0], x[i], y[i], x[i + 1], y[i + 1], w1, w2, w3);
+        if (w1 >= BARY_EPS && w2 >= BARY_EPS && w3 >= BARY_EPS) return true;
+    }
+    return false;
+}
+
+__device__ __noinline__ int contain_two_ring(const DMesh& m, double lon_p, double lat_p, int nn);
+
+// mesh.py:2392-2470 _find_containing_element_local: the 1-ring of the anchor,
+// then its 2-ring; -1 when no element contains the point.
+__device__ __forceinline__ int contain_local(const DMesh& m, double lon_p, double lat_p, int nn) {
+    int s = __ldg(&m.n2e_off[nn]), e = __ldg(&m.n2e_off[nn + 1]);
+    if (e == s) return -1;
+    for (int k = s; k < e; ++k) {
+        int c = __ldg(&m.n2e[k]);
+        if (element_contains(m, c, lon_p, lat_p)) return c;
+    }
+    return contain_two_ring(m, lon_p, lat_p, nn);
+}
+
+__device__ __noinline__ int contain_two_ring(const DMesh& m, double lon_p, double lat_p, int nn) {
+    int s = m.n2e_off[nn], e = m.n2e_off[nn + 1];
+    for (int k = s; k < e; ++k) {
+        int el = m.n2e[k];
+        int4 en = m.en[el];
+        for (int j = 0; j < 4; ++j) {
+            int v = elem_node(en, j);
+            if (v < 0 || v == nn) continue;
+            int s2 = m.n2e_off[v], e2 = m.n2e_off[v + 1];
+            for (int kk = s2; kk < e2; ++kk) {
+                int c = m.n2e[kk];
+                int4 ce = m.en[c];
+                if (ce.x == nn || ce.y == nn || ce.z == nn || ce.w == nn) continue;
+                if (element_contains(m, c, lon_p, lat_p)) return c;
+            }
+        }
+    }
+    return -1;
+}
+
+}  // namespace kc

@@ -1,0 +1,241 @@
+"""Device-resident state behind the step functions: one CUDA context with the
+uploaded mesh, a ring of velocity snapshots and the particle arrays.
+
+Uploads are cached by object identity (a strong reference is kept, so an id
+is never reused while cached): a run that steps the same mesh and snapshots
+every step pays each upload once.  Particles travel every ``step()`` call
+(the reference's per-call contract returns fresh arrays); the multi-step
+driver in ``tracking`` keeps them resident instead.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from collections import OrderedDict
+from typing import Optional
+
+import numpy as np
+
+from . import _native as N
+
+N_SLOTS = 8
+
+
+def _c(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def mesh_desc(mesh, keep: list) -> N.MeshDesc:
+    """Fill the C mesh descriptor from a mesh (duck-typed: a kelp_b200 Mesh or
+    KELP's own ``kelp.core.mesh.Mesh`` after ``build_search``).  Arrays that
+    need a dtype conversion are appended to ``keep`` so they outlive the call."""
+    if getattr(mesh, "_gh_offsets", None) is None:
+        raise RuntimeError("mesh has no grid hash: call build_search(mesh) first")
+    xyz = getattr(mesh, "_node_xyz", None)
+    if xyz is None:
+        raise RuntimeError("grid hash without its node coordinate table: call build_search(mesh)")
+
+    def k(a, dt):
+        a = _c(a, dt)
+        keep.append(a)
+        return a
+
+    lon = k(mesh.nodes_lon, np.float64)
+    lat = k(mesh.nodes_lat, np.float64)
+    en = k(mesh.elem_nodes, np.int32)
+    n2e = k(mesh.node_to_elems, np.int32)
+    cnt = k(mesh.node_to_elems_count, np.int32)
+    off = k(mesh._gh_offsets, np.int32)
+    ids = k(mesh._gh_node_ids, np.int32)
+    xyz = k(xyz, np.float64)
+    depth = k(mesh.depth, np.float64) if getattr(mesh, "depth", None) is not None else None
+    sigma = np.asarray(getattr(mesh, "sigma", np.zeros(0)))
+    zl = None
+    if sigma.size > 0 and getattr(mesh, "vertical_coord", "zlevel") == "zlevel":
+        zl = k(np.abs(sigma), np.float64)
+    d = N.MeshDesc()
+    d.n_nodes = lon.shape[0]
+    d.n_elems = en.shape[0]
+    d.max_v = en.shape[1]
+    d.max_conn = n2e.shape[1] if n2e.ndim == 2 else 0
+    d.nodes_lon, d.nodes_lat = N.ptr(lon), N.ptr(lat)
+    d.depth = N.ptr(depth)
+    d.elem_nodes, d.node_to_elems, d.node_to_elems_count = N.ptr(en), N.ptr(n2e), N.ptr(cnt)
+    d.gh_offsets, d.gh_node_ids, d.node_xyz = N.ptr(off), N.ptr(ids), N.ptr(xyz)
+    d.gh_cell_size = float(mesh._gh_cell_size)
+    d.gh_lon_min = float(mesh._gh_lon_min)
+    d.gh_lat_min = float(mesh._gh_lat_min)
+    d.gh_nx, d.gh_ny = int(mesh._gh_nx), int(mesh._gh_ny)
+    d.gh_wrap_lon = 1 if mesh._gh_wrap_lon else 0
+    d.gh_far_rows = int(mesh._gh_far_rows)
+    d.exact_nearest = 1 if (getattr(mesh, "metadata", None) or {}).get("exact_nearest", False) else 0
+    d.r_earth = float(getattr(mesh, "r_earth", 6371000.0))
+    d.z_levels = N.ptr(zl)
+    d.n_levels = 0 if zl is None else int(zl.shape[0])
+    return d
+
+
+class DeviceContext:
+    """One CUDA device context of the native library."""
+
+    def __init__(self, device: int = 0):
+        L = N.lib()
+        p = C.c_void_p()
+        rc = L.kc_create(int(device), C.byref(p))
+        if rc:
+            raise N.KcError(rc, f"kc_create(device={device}) failed: no usable CUDA device")
+        self._ctx = p
+        self.device = device
+        self._mesh_ref = None
+        self._mesh_key = None
+        self._slots: "OrderedDict[int, tuple]" = OrderedDict()   # id(field) -> (slot, field)
+        self.P = 0
+
+    # -- plumbing ---------------------------------------------------------
+    def _chk(self, rc, what):
+        N.check(self._ctx, rc, what)
+
+    def close(self):
+        if self._ctx:
+            N.lib().kc_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._ctx
+
+    def synchronize(self):
+        self._chk(N.lib().kc_synchronize(self._ctx), "kc_synchronize")
+
+    # -- mesh ---------------------------------------------------------------
+    def ensure_mesh(self, mesh) -> None:
+        key = (id(mesh), id(mesh._gh_offsets), id(getattr(mesh, "_node_xyz", None)),
+               bool((mesh.metadata or {}).get("exact_nearest", False)))
+        if self._mesh_key == key and self._mesh_ref is mesh:
+            return
+        keep: list = []
+        d = mesh_desc(mesh, keep)
+        self._chk(N.lib().kc_mesh_upload(self._ctx, C.byref(d)), "kc_mesh_upload")
+        self._mesh_ref = mesh
+        self._mesh_key = key
+        self._slots.clear()
+
+    # -- snapshot ring --------------------------------------------------------
+    def upload_field(self, field, slot: int, dtype=None) -> None:
+        u = np.asarray(field.u)
+        v = np.asarray(field.v)
+        w = None if getattr(field, "w", None) is None else np.asarray(field.w)
+        if dtype is None:
+            dtype = np.float32 if (u.dtype == np.float32 and v.dtype == np.float32
+                                   and (w is None or w.dtype == np.float32)) else np.float64
+        u = _c(u, dtype)
+        v = _c(v, dtype)
+        w = None if w is None else _c(w, dtype)
+        n = u.shape[-1]
+        rows = 1 if u.ndim == 1 else u.shape[0]
+        wrows = 0 if w is None else (1 if w.ndim == 1 else w.shape[0])
+        code = N.KC_F32 if dtype == np.float32 else N.KC_F64
+        self._chk(N.lib().kc_field_upload(self._ctx, slot, code, n, rows, N.ptr(u), N.ptr(v), wrows, N.ptr(w)),
+                  "kc_field_upload")
+        self.synchronize()
+
+    def slots_for(self, fields) -> list:
+        """Ring slots holding ``fields`` (uploading the ones not resident).
+        All fields of one step share one element type: float32 only when every
+        one of them is float32."""
+        all32 = all(np.asarray(f.u).dtype == np.float32 and np.asarray(f.v).dtype == np.float32
+                    and (f.w is None or np.asarray(f.w).dtype == np.float32) for f in fields)
+        dtype = np.float32 if all32 else np.float64
+        out = []
+        pinned = set()
+        for f in fields:
+            key = (id(f), dtype)
+            if key in self._slots:
+                self._slots.move_to_end(key)
+                slot = self._slots[key][0]
+            else:
+                used = {s for s, _ in self._slots.values()}
+                free = [s for s in range(N_SLOTS) if s not in used]
+                if free:
+                    slot = free[0]
+                else:
+                    victim = next(k for k, (s, _) in self._slots.items() if s not in pinned)
+                    slot = self._slots.pop(victim)[0]
+                self.upload_field(f, slot, dtype)
+                self._slots[key] = (slot, f)
+            pinned.add(slot)
+            out.append(slot)
+        return out
+
+    # -- particles ------------------------------------------------------------
+    def upload_particles(self, lon, lat, z, status, nn, fr=None, pid=None, release_step=None):
+        lon = _c(lon, np.float64)
+        lat = _c(lat, np.float64)
+        z = None if z is None else _c(z, np.float64)
+        status = _c(status, np.int32)
+        nn = _c(nn, np.int32)
+        fr = None if fr is None else _c(fr, np.int8)
+        pid = None if pid is None else _c(pid, np.int64)
+        rs = None if release_step is None else _c(release_step, np.int32)
+        P = lon.shape[0]
+        self._chk(N.lib().kc_particles_upload(self._ctx, P, N.ptr(lon), N.ptr(lat), N.ptr(z), N.ptr(status),
+                                              N.ptr(nn), N.ptr(fr), N.ptr(pid), N.ptr(rs)),
+                  "kc_particles_upload")
+        self.P = P
+
+    def download_particles(self) -> dict:
+        P = self.P
+        out = {"lon": np.empty(P), "lat": np.empty(P), "z": np.empty(P),
+               "status": np.empty(P, np.int32), "nearest_node": np.empty(P, np.int32),
+               "failure_reason": np.empty(P, np.int8),
+               "u": np.empty(P), "v": np.empty(P), "w": np.empty(P)}
+        self._chk(N.lib().kc_particles_download(
+            self._ctx, P, N.ptr(out["lon"]), N.ptr(out["lat"]), N.ptr(out["z"]), N.ptr(out["status"]),
+            N.ptr(out["nearest_node"]), N.ptr(out["failure_reason"]), N.ptr(out["u"]), N.ptr(out["v"]),
+            N.ptr(out["w"])), "kc_particles_download")
+        return out
+
+    # -- work -------------------------------------------------------------------
+    def step(self, args: N.StepArgs) -> None:
+        self._chk(N.lib().kc_step(self._ctx, C.byref(args)), "kc_step")
+
+    def run(self, steps) -> None:
+        arr = (N.StepArgs * len(steps))(*steps)
+        self._chk(N.lib().kc_run(self._ctx, arr, len(steps)), "kc_run")
+
+    def find_nearest(self, lon, lat) -> np.ndarray:
+        lon = _c(lon, np.float64)
+        lat = _c(lat, np.float64)
+        out = np.empty(lon.shape[0], np.int32)
+        self._chk(N.lib().kc_find_nearest(self._ctx, lon.shape[0], N.ptr(lon), N.ptr(lat), N.ptr(out)),
+                  "kc_find_nearest")
+        return out
+
+    def device_errors(self) -> int:
+        w = C.c_int(0)
+        self._chk(N.lib().kc_device_errors(self._ctx, C.byref(w)), "kc_device_errors")
+        return int(w.value)
+
+    def record(self, slot: int) -> None:
+        self._chk(N.lib().kc_event_record(self._ctx, slot), "kc_event_record")
+
+    def elapsed_ms(self, a: int, b: int) -> float:
+        ms = C.c_float(0.0)
+        self._chk(N.lib().kc_event_elapsed(self._ctx, a, b, C.byref(ms)), "kc_event_elapsed")
+        return float(ms.value)
+
+
+_default: Optional[DeviceContext] = None
+
+
+def default_context() -> DeviceContext:
+    """The process-wide context on CUDA device 0 (created on first use)."""
+    global _default
+    if _default is None:
+        _default = DeviceContext(0)
+    return _default

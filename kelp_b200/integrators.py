@@ -1,0 +1,201 @@
+"""Step functions with KELP's integrator signature, running on the B200.
+
+``euler_step`` / ``rk2_step`` / ``rk4_step`` take and return the same objects
+as KELP's (``src/kelp/numerics/integrators.py:5150``, ``:5611``, ``:6013``):
+``step(state, vel, mesh, dt, time_dir, layer=0, *, w_interp, uv_interp,
+vel_next, dt_to_next, diffusion, ...) -> ParticleState``.  ``INTEGRATORS`` /
+``get_integrator`` mirror the registry (``integrators.py:6635-6660``), so the
+module is a drop-in at the plugin point.
+
+Every supported combination runs as one CUDA kernel launch per step; there is
+no CPU path.  Combinations this build does not implement raise
+``NotImplementedError`` before any device work, naming what is missing.
+Argument errors raise ``ValueError`` in Python, as in the reference.
+"""
+from __future__ import annotations
+
+from typing import Optional
+
+import numpy as np
+
+from . import _native as N
+from .device import default_context
+from .particles import ParticleState
+
+_RK2_C = (0.0, 0.5)
+_RK4_C = (0.0, 0.5, 0.5, 1.0)
+
+
+def _is_3d(vel) -> bool:
+    return getattr(vel, "w", None) is not None if not hasattr(vel, "vel_a") else (
+        vel.vel_a.w is not None and vel.vel_b.w is not None)
+
+
+def _zero_dead_velocity(state: ParticleState) -> ParticleState:
+    """integrators.py:272-281: nothing alive -> zero velocity diagnostics."""
+    if state.u is None:
+        return state
+    return state.replace(u=np.zeros_like(state.u), v=np.zeros_like(state.v),
+                         w=None if state.w is None else np.zeros_like(state.w))
+
+
+def _validate_time_aware(vel_next, dt_to_next, dt):
+    if (vel_next is None) != (dt_to_next is None):
+        raise ValueError("vel_next and dt_to_next must both be set or both be None")
+    if dt_to_next is not None and not float(dt_to_next) > 0:
+        raise ValueError(f"dt_to_next must be > 0, got {dt_to_next!r}")
+
+
+def _kick_args(diffusion) -> Optional[tuple]:
+    """(kh_x, kh_y, seed, real_id, step_i, pid_offset) of a split uniform kick,
+    or None when no kick applies (absent, or Kh = 0: ``integrators.py:719-720``)."""
+    if diffusion is None:
+        return None
+    if diffusion.scheme != "uniform":
+        raise NotImplementedError(f"diffusion.scheme={diffusion.scheme!r} (variable Kh) is not built "
+                                  "on the CUDA backend; only the uniform split kick is")
+    if diffusion.composition not in ("split",):
+        raise NotImplementedError(f"diffusion.composition={diffusion.composition!r} is not built on the "
+                                  "CUDA backend")
+    if getattr(diffusion, "az_enabled", False):
+        raise NotImplementedError("the vertical Az kick is not built on the CUDA backend")
+    if float(diffusion.kh_x) == 0.0 and float(diffusion.kh_y) == 0.0:
+        return None
+    if float(diffusion.kh_x) < 0 or float(diffusion.kh_y) < 0:
+        raise ValueError("Kh must be >= 0")
+    return (float(diffusion.kh_x), float(diffusion.kh_y), int(diffusion.seed), int(diffusion.real_id),
+            int(diffusion.step_i), int(getattr(diffusion, "pid_offset", 0)))
+
+
+def _fields(vel, vel_next):
+    """(vel_a, vel_b, target, alpha0) threading of the fused runners
+    (integrators.py:3367-3370, :4729-4745)."""
+    vel_a = getattr(vel, "vel_a", vel)
+    vel_b = getattr(vel, "vel_b", vel_next if vel_next is not None else vel_a)
+    alpha0 = float(getattr(vel, "alpha", 0.0))
+    target = vel_next if vel_next is not None else vel_a
+    return vel_a, vel_b, target, alpha0
+
+
+def _check_node_fields(mesh, fields, is3d):
+    n = mesh.nodes_lon.shape[0]
+    for f in fields:
+        if getattr(f, "uv_layout", "element") != "node":
+            raise NotImplementedError("element-layout u/v (leastsq / edge_leastsq) is not built on the "
+                                      "CUDA backend; node-layout barycentric is")
+        u = np.asarray(f.u)
+        if u.shape[-1] != n or np.asarray(f.v).shape != u.shape:
+            raise ValueError(f"u/v of shape {u.shape} do not match the mesh's {n} nodes")
+        if is3d:
+            zl = np.abs(np.asarray(mesh.sigma))
+            w = np.asarray(f.w)
+            if w.shape != (zl.shape[0], n) or u.shape != (zl.shape[0] - 1, n):
+                raise ValueError(f"3-D layer fields need u/v ({zl.shape[0] - 1}, {n}) and w "
+                                 f"({zl.shape[0]}, {n}); got {u.shape} and {w.shape}")
+
+
+def _run(state, vel, mesh, dt, time_dir, scheme, c_coeffs, kw, ctx=None) -> ParticleState:
+    if float(dt) <= 0:
+        raise ValueError(f"dt must be > 0, got {dt!r}")
+    if float(time_dir) not in (1.0, -1.0):
+        raise ValueError(f"time_dir must be +1 or -1, got {time_dir!r}")
+    if kw.get("uv_interp", "leastsq") == "nemo_cgrid":
+        raise NotImplementedError("the NEMO C-grid step is not built on the CUDA backend")
+    diffusion = kw.get("diffusion", None)
+    kick = _kick_args(diffusion)
+    if not np.any(state.alive_mask):
+        return _zero_dead_velocity(state)
+    uv_interp = kw.get("uv_interp", "leastsq")
+    if uv_interp != "barycentric":
+        raise NotImplementedError(f"uv_interp={uv_interp!r} is not built on the CUDA backend; "
+                                  "use 'barycentric' (node-layout velocities)")
+    if kw.get("recon") is not None:
+        raise NotImplementedError("PCHIP temporal reconstruction is not built on the CUDA backend")
+    if state.elem is not None:
+        raise NotImplementedError("elem_search: walk (carried elements) is not built on the CUDA backend")
+    if not (mesh.metadata or {}).get("exact_nearest", False):
+        raise NotImplementedError("the CUDA backend anchors with the exact nearest-node search only "
+                                  "(mesh.exact_nearest: true, the configuration default)")
+    vel_next = kw.get("vel_next", None)
+    dt_to_next = kw.get("dt_to_next", None)
+    _validate_time_aware(vel_next, dt_to_next, dt)
+    is3d = _is_3d(vel)
+    w_code = 0
+    if is3d:
+        if getattr(mesh, "vertical_coord", "zlevel") != "zlevel":
+            raise NotImplementedError("sigma meshes are not built on the CUDA backend")
+        if getattr(vel, "uv_vertical", "layer") != "layer":
+            raise NotImplementedError("depth-linear u/v placement is not built on the CUDA backend")
+        if scheme != N.KC_RK2:
+            raise NotImplementedError("3-D euler/rk4 are not built on the CUDA backend; rk2 is")
+        w_interp = kw.get("w_interp", "leastsq")
+        if w_interp not in ("nearest", "barycentric"):
+            raise NotImplementedError(f"w_interp={w_interp!r} is not built on the CUDA backend")
+        w_code = 0 if w_interp == "nearest" else 1
+        if hasattr(vel, "vel_a") and float(getattr(vel, "alpha", 1.0)) == 0.0:
+            raise NotImplementedError("an endpoint LazyLerpField (alpha 0) takes the reference's unfused "
+                                      "path, which is not built on the CUDA backend")
+    vel_a, vel_b, target, alpha0 = _fields(vel, vel_next)
+    _check_node_fields(mesh, [vel_a, vel_b, target], is3d)
+
+    ctx = ctx or default_context()
+    ctx.ensure_mesh(mesh)
+    sa, sb, st = ctx.slots_for([vel_a, vel_b, target])
+    fr_in = state.failure_reason
+    ctx.upload_particles(state.lon, state.lat, state.z, state.status, state.nearest_node,
+                         fr=fr_in)
+    a = N.StepArgs()
+    a.scheme = scheme
+    a.dims = 3 if is3d else 2
+    a.slot_a, a.slot_b, a.slot_t = sa, sb, st
+    a.alpha0 = alpha0
+    if vel_next is not None and scheme != N.KC_EULER:
+        for k, c in enumerate(c_coeffs):
+            a.alpha_k[k] = float(c) * float(dt) / float(dt_to_next)
+    a.dt = float(dt)
+    a.time_dir = float(time_dir)
+    a.w_code = w_code
+    if kick is not None:
+        a.kick = 1
+        a.kh_x, a.kh_y, a.seed, a.real_id, a.step_i, a.pid_offset = kick
+    a.global_step = -1
+    ctx.step(a)
+    out = ctx.download_particles()
+    if ctx.device_errors():
+        raise N.KcError(N.KC_ERR_DEVICE, "a device-side search iteration cap was hit")
+    return state.replace(
+        lon=out["lon"], lat=out["lat"], z=out["z"] if is3d else np.array(state.z, copy=True),
+        status=out["status"], nearest_node=out["nearest_node"],
+        u=out["u"], v=out["v"], w=out["w"] if is3d else None,
+        failure_reason=None if fr_in is None else out["failure_reason"],
+    )
+
+
+def euler_step(state, vel, mesh, dt, time_dir, layer: int = 0, **kwargs) -> ParticleState:
+    """Forward Euler (integrators.py:5150)."""
+    return _run(state, vel, mesh, dt, time_dir, N.KC_EULER, (0.0,), kwargs)
+
+
+def rk2_step(state, vel, mesh, dt, time_dir, layer: int = 0, **kwargs) -> ParticleState:
+    """RK2 midpoint (integrators.py:5611)."""
+    return _run(state, vel, mesh, dt, time_dir, N.KC_RK2, _RK2_C, kwargs)
+
+
+def rk4_step(state, vel, mesh, dt, time_dir, layer: int = 0, **kwargs) -> ParticleState:
+    """Classical RK4 (integrators.py:6013)."""
+    return _run(state, vel, mesh, dt, time_dir, N.KC_RK4, _RK4_C, kwargs)
+
+
+def _rk45_unavailable(*a, **k):
+    raise NotImplementedError("rk45 (adaptive, 2-D leastsq) is not built on the CUDA backend")
+
+
+INTEGRATORS = {"euler": euler_step, "rk2": rk2_step, "rk4": rk4_step, "rk45": _rk45_unavailable}
+
+
+def get_integrator(name: str):
+    """Registry lookup (integrators.py:6635-6660)."""
+    key = str(name).lower()
+    if key not in INTEGRATORS:
+        raise ValueError(f"Unknown integrator {name!r}. Choose from: {sorted(INTEGRATORS)}")
+    return INTEGRATORS[key]

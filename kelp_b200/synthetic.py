@@ -1,0 +1,182 @@
+"""Seeded synthetic meshes, velocity snapshots and particle releases.
+
+The reference measures on synthetic data only; these generators build inputs
+of the shapes its benchmark configurations name (no readers, no files):
+
+* ``lattice_mesh`` -- a jittered lon/lat lattice triangulated cell by cell
+  (the seam column joins back across +-180 deg like KELP's own band meshes in
+  ``tests/test_fused_bary_tinterp.py``), optionally with a fraction of cells
+  kept as convex quads, and a land mask from smooth spherical noise;
+* ``gyre_snapshots`` -- node-layout u/v (solid-body rotation plus a
+  double gyre) and, for 3-D, u/v per layer and w on the interfaces from the
+  continuity of the same stream-function flow;
+* ``release_uniform`` -- particles uniform in area over the wet elements
+  (and uniform in depth over the local column for 3-D).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .fields import VelocityField
+from .geometry import DEG2RAD
+from .mesh import make_mesh
+
+
+def _sphere_noise(lon, lat, n_modes=32, seed=2):
+    rng = np.random.default_rng(seed)
+    x = np.cos(lat * DEG2RAD) * np.cos(lon * DEG2RAD)
+    y = np.cos(lat * DEG2RAD) * np.sin(lon * DEG2RAD)
+    z = np.sin(lat * DEG2RAD)
+    f = np.zeros_like(lon)
+    for _ in range(n_modes):
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        k = rng.uniform(1.0, 6.0)
+        ph = rng.uniform(0, 2 * np.pi)
+        amp = rng.uniform(0.5, 1.0) / k
+        f += amp * np.cos(k * (d[0] * x + d[1] * y + d[2] * z) * np.pi + ph)
+    return f
+
+
+def lattice_mesh(spacing: float = 0.5625, lat_max: float = 80.0, *, lon_min: float = -180.0,
+                 lon_max: float = 180.0, jitter: float = 0.2, land_frac: float = 0.3,
+                 quad_frac: float = 0.0, seed_jitter: int = 1, seed_land: int = 2, seed_quad: int = 4,
+                 depth=None, sigma=None, cell_size: float = 0.0, name: str = "lattice"):
+    """Jittered lon/lat lattice mesh.  ``lon_max - lon_min == 360`` joins the
+    seam column.  Land (``land_frac`` of the nodes by smooth noise) removes
+    every element touching a land node, then orphaned nodes."""
+    glob = abs((lon_max - lon_min) - 360.0) < 1e-9
+    nlon = int(round((lon_max - lon_min) / spacing)) + (0 if glob else 1)
+    nlat = int(round(2 * lat_max / spacing)) + 1 if lat_max > 0 else 1
+    lon1 = lon_min + spacing * np.arange(nlon)
+    lat1 = -lat_max + spacing * np.arange(nlat)
+    gx, gy = np.meshgrid(lon1, lat1)
+    lon = gx.ravel().astype(np.float64)
+    lat = gy.ravel().astype(np.float64)
+    rng = np.random.default_rng(seed_jitter)
+    lon = lon + rng.uniform(-jitter, jitter, lon.size) * spacing
+    lat = lat + rng.uniform(-jitter, jitter, lat.size) * spacing
+    lat = np.clip(lat, -89.9, 89.9)
+    lon = ((lon + 180.0) % 360.0) - 180.0
+    ncx = nlon if glob else nlon - 1
+    jj, ii = np.meshgrid(np.arange(nlat - 1), np.arange(ncx), indexing="ij")
+    jj = jj.ravel()
+    ii = ii.ravel()
+    i2 = (ii + 1) % nlon
+    n0 = jj * nlon + ii
+    n1 = jj * nlon + i2
+    n2 = (jj + 1) * nlon + ii
+    n3 = (jj + 1) * nlon + i2
+    qrng = np.random.default_rng(seed_quad)
+    is_quad = qrng.uniform(size=n0.size) < quad_frac
+    tris_a = np.stack([n0, n1, n2, np.full_like(n0, -1)], 1)
+    tris_b = np.stack([n1, n3, n2, np.full_like(n0, -1)], 1)
+    quads = np.stack([n0, n1, n3, n2], 1)
+    elems = np.concatenate([quads[is_quad], tris_a[~is_quad], tris_b[~is_quad]])
+    if land_frac > 0:
+        noise = _sphere_noise(lon, lat, seed=seed_land)
+        land = noise < np.quantile(noise, land_frac)
+        valid = elems >= 0
+        touches = (land[np.where(valid, elems, 0)] & valid).any(axis=1)
+        elems = elems[~touches]
+    if quad_frac <= 0:
+        elems = elems[:, :3]
+    used = np.zeros(lon.size, bool)
+    used[elems[elems >= 0]] = True
+    remap = np.full(lon.size, -1, np.int64)
+    remap[used] = np.arange(used.sum())
+    elems = np.where(elems >= 0, remap[np.where(elems >= 0, elems, 0)], -1).astype(np.int32)
+    lon = lon[used]
+    lat = lat[used]
+    if depth is None:
+        d = np.full(lon.size, 4000.0)
+    elif callable(depth):
+        d = depth(lon, lat)
+    else:
+        d = np.asarray(depth)[used]
+    return make_mesh(name, lon, lat, d, elems, sigma=sigma, cell_size=cell_size)
+
+
+def stretched_levels(k_levels: int = 47, top: float = 5.0, bottom: float = 6000.0):
+    """0 then ``top * r**(k-1)`` up to ``bottom`` (positive down)."""
+    n = k_levels - 1
+    r = (bottom / top) ** (1.0 / (n - 1))
+    return np.concatenate([[0.0], top * r ** np.arange(n)])
+
+
+def smooth_bathymetry(lon, lat, dmin=50.0, dmax=6000.0, seed=5):
+    f = _sphere_noise(lon, lat, n_modes=16, seed=seed)
+    f = (f - f.min()) / (f.max() - f.min() + 1e-300)
+    return dmin + (dmax - dmin) * f
+
+
+def _gyre_uv(lon, lat, phase, amp):
+    """Solid-body rotation plus a double gyre (m/s), smooth on the sphere."""
+    la = lat * DEG2RAD
+    lo = lon * DEG2RAD
+    u_sb = 0.5 * amp * np.cos(la)
+    # stream function psi = sin(2 lo + phase) * sin(2 la)^2 ; u = -dpsi/dy, v = dpsi/dx
+    s = np.sin(2 * lo + phase)
+    c = np.cos(2 * lo + phase)
+    u_g = -amp * 0.5 * s * 2 * np.sin(2 * la) * np.cos(2 * la) * 2
+    v_g = amp * 0.5 * 2 * c * np.sin(2 * la) ** 2
+    return u_sb + u_g, v_g
+
+
+def gyre_snapshots(mesh, n_snap: int = 2, *, amp: float = 0.5, dtype=np.float32,
+                   z_levels=None, decay: float = 1000.0, w_scale: float = 1e-4):
+    """``n_snap`` node-layout snapshots, the phase advancing by 0.7 rad per
+    snapshot.  With ``z_levels`` (K interfaces): u/v (K-1, N) at the layer
+    mid-depths scaled by ``exp(-z / decay)``, and w (K, N) from continuity of
+    the divergent part (positive down, w = 0 at the surface)."""
+    lon = np.asarray(mesh.nodes_lon)
+    lat = np.asarray(mesh.nodes_lat)
+    out = []
+    for k in range(n_snap):
+        u, v = _gyre_uv(lon, lat, 0.7 * k, amp)
+        if z_levels is None:
+            out.append(VelocityField(u=u.astype(dtype), v=v.astype(dtype), eta=np.zeros(lon.size),
+                                     uv_layout="node"))
+            continue
+        zl = np.asarray(z_levels, dtype=np.float64)
+        zm = 0.5 * (zl[:-1] + zl[1:])
+        dec = np.exp(-zm / decay)[:, None]
+        div = np.sin(3 * lon * DEG2RAD + 0.7 * k) * np.cos(3 * lat * DEG2RAD)
+        uu = (u[None, :] * dec).astype(dtype)
+        vv = (v[None, :] * dec).astype(dtype)
+        # w(z) = -int_0^z div * f(z') dz', f = exp(-z/decay): closed form
+        ww = (w_scale * div[None, :] * (1.0 - np.exp(-zl / decay))[:, None]).astype(dtype)
+        out.append(VelocityField(u=uu, v=vv, w=ww, eta=np.zeros(lon.size), uv_layout="node",
+                                 uv_vertical="layer"))
+    return out
+
+
+def release_uniform(mesh, P: int, seed: int = 3, *, depth_uniform: bool = False):
+    """``P`` positions uniform in area over the mesh's elements (lon, lat, z)."""
+    rng = np.random.default_rng(seed)
+    en = np.asarray(mesh.elem_nodes)
+    lon = np.asarray(mesh.nodes_lon)
+    lat = np.asarray(mesh.nodes_lat)
+    # split every element into fan triangles (0, k, k+1)
+    tris = []
+    for k in range(1, en.shape[1] - 1):
+        t = np.stack([en[:, 0], en[:, k], en[:, k + 1]], 1)
+        tris.append(t[(t >= 0).all(1)])
+    t = np.concatenate(tris)
+    la = lat[t]
+    lo0 = lon[t[:, :1]]
+    lo = lo0 + (((lon[t] - lo0) + 180.0) % 360.0 - 180.0)
+    area = 0.5 * np.abs((lo[:, 1] - lo[:, 0]) * (la[:, 2] - la[:, 0]) - (lo[:, 2] - lo[:, 0]) * (la[:, 1] - la[:, 0]))
+    area *= np.cos(la.mean(1) * DEG2RAD)
+    pick = rng.choice(t.shape[0], size=P, p=area / area.sum())
+    r1 = np.sqrt(rng.uniform(size=P))
+    r2 = rng.uniform(size=P)
+    b = np.stack([1 - r1, r1 * (1 - r2), r1 * r2], 1)
+    plon = (b * lo[pick]).sum(1)
+    plat = (b * la[pick]).sum(1)
+    plon = ((plon + 180.0) % 360.0) - 180.0
+    z = np.zeros(P)
+    if depth_uniform:
+        dep = np.asarray(mesh.depth)[t[pick]].min(1)
+        z = rng.uniform(size=P) * dep
+    return plon, plat, z

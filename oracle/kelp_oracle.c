@@ -1,0 +1,982 @@
+/*
+ * kelp_oracle.c -- TEST INFRASTRUCTURE, NOT THE PRODUCT.
+ *
+ * A plain-C CPU restatement of KELP's compiled time-stepping path, used as the
+ * parity checker for the CUDA kernels (tests/, __graft_entry__.smoke()) and as
+ * the timed CPU baseline of bench.py.  Nothing in kelp_b200/ links or calls it.
+ *
+ * It works on the reference's own array layout (dense node_to_elems (N,
+ * max_conn), elem_nodes (E, max_v), node_xyz (N, 3), CSR grid hash) and follows
+ * the reference's Numba functions statement by statement, with the C
+ * library's math (the functions Numba lowers np.cos/np.sin/math.log to) and no
+ * floating-point contraction (-ffp-contract=off).  Each function cites the
+ * reference file:line it restates (paths inside the KELP project).
+ *
+ * Pinned against golden vectors produced by running the reference itself
+ * (tests/golden/make_golden.py -> tests/golden/*.npz; tests/test_oracle_golden.py).
+ */
+#include <math.h>
+#include <pthread.h>
+#include <unistd.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define DEG2RAD 0.017453292519943295
+#define RAD2DEG 57.29577951308232
+#define SLM 111120.0
+#define R_STD 6371000.0
+#define BARY_EPS (-1e-6)
+#define AREA_TOL 1e-10
+#define ALIVE 1
+#define OUTSIDE 3
+#define NOT_RELEASED 4
+
+typedef struct {
+    int64_t N, E;
+    int max_v, max_conn;
+    const double *lon, *lat, *depth, *xyz, *zlev;
+    const int32_t *en, *n2e, *n2e_cnt, *gh_off, *gh_ids;
+    double cell, lon_min, lat_min, r_earth;
+    int nx, ny, wrap, far_rows, exact, K;
+} OMesh;
+
+typedef struct {
+    const void *ua, *va, *wa, *ub, *vb, *wb, *ut, *vt, *wt;
+    int f32;
+    double alpha0;
+    int64_t n;
+} OField;
+
+static double fld(const void* p, int f32, int64_t i) {
+    return f32 ? (double)((const float*)p)[i] : ((const double*)p)[i];
+}
+
+/* Python float % for a positive divisor (CPython float_rem). */
+static double pymod(double x, double m) {
+    double r = fmod(x, m);
+    if (r != 0.0) {
+        if (r < 0.0) r += m;
+    } else {
+        r = 0.0;
+    }
+    return r;
+}
+static double wrap180(double x) { return pymod(x + 180.0, 360.0) - 180.0; }
+static int imod(int a, int n) { int r = a % n; return r < 0 ? r + n : r; }
+
+/* mesh.py:1192-1207 */
+static double fold_dlon(const OMesh* m, double lon_p) {
+    double dlon = pymod(lon_p - m->lon_min, 360.0);
+    if (!m->wrap) {
+        double grid_span = m->nx * m->cell;
+        if (dlon > grid_span && (dlon - grid_span) > (360.0 - dlon)) dlon -= 360.0;
+    }
+    return dlon;
+}
+
+/* mesh.py:1210-1232 */
+static void cell_of(const OMesh* m, double lon_p, double lat_p, int* ci, int* cj) {
+    double dlon = fold_dlon(m, lon_p);
+    int a = (int)(dlon / m->cell);
+    int b = (int)((lat_p - m->lat_min) / m->cell);
+    if (a < 0) a = 0;
+    if (a >= m->nx) a = m->nx - 1;
+    if (b < 0) b = 0;
+    if (b >= m->ny) b = m->ny - 1;
+    *ci = a;
+    *cj = b;
+}
+
+static void qxyz(double lon_p, double lat_p, double* xp, double* yp, double* zp, double* cl) {
+    double lat_r = lat_p * DEG2RAD, lon_r = lon_p * DEG2RAD;
+    double c = cos(lat_r);
+    *xp = c * cos(lon_r);
+    *yp = c * sin(lon_r);
+    *zp = sin(lat_r);
+    *cl = c;
+}
+
+static void scan_cell(const OMesh* m, int cell, double xp, double yp, double zp, int* best, double* bd2) {
+    for (int k = m->gh_off[cell]; k < m->gh_off[cell + 1]; ++k) {
+        int n = m->gh_ids[k];
+        double xn = m->xyz[3 * (int64_t)n], yn = m->xyz[3 * (int64_t)n + 1], zn = m->xyz[3 * (int64_t)n + 2];
+        double d2 = (xn - xp) * (xn - xp) + (yn - yp) * (yn - yp) + (zn - zp) * (zn - zp);
+        if (d2 < *bd2) { *bd2 = d2; *best = n; }
+    }
+}
+
+static void scan_row_range(const OMesh* m, int cj2, int lo, int hi, double xp, double yp, double zp, int* best, double* bd2) {
+    for (int k = m->gh_off[cj2 * m->nx + lo]; k < m->gh_off[cj2 * m->nx + hi + 1]; ++k) {
+        int n = m->gh_ids[k];
+        double xn = m->xyz[3 * (int64_t)n], yn = m->xyz[3 * (int64_t)n + 1], zn = m->xyz[3 * (int64_t)n + 2];
+        double d2 = (xn - xp) * (xn - xp) + (yn - yp) * (yn - yp) + (zn - zp) * (zn - zp);
+        if (d2 < *bd2) { *bd2 = d2; *best = n; }
+    }
+}
+
+/* mesh.py:1235-1303 */
+static int nearest_3x3(const OMesh* m, double lon_p, double lat_p) {
+    int ci, cj;
+    cell_of(m, lon_p, lat_p, &ci, &cj);
+    double xp, yp, zp, cl;
+    qxyz(lon_p, lat_p, &xp, &yp, &zp, &cl);
+    int best = -1;
+    double bd2 = 1e30;
+    for (int dj = -1; dj <= 1; ++dj) {
+        int cj2 = cj + dj;
+        if (cj2 < 0 || cj2 >= m->ny) continue;
+        for (int di = -1; di <= 1; ++di) {
+            int ci2 = ci + di;
+            if (ci2 < 0) ci2 = m->wrap ? ci2 + m->nx : -1;
+            else if (ci2 >= m->nx) ci2 = m->wrap ? ci2 - m->nx : -1;
+            if (ci2 < 0) continue;
+            scan_cell(m, cj2 * m->nx + ci2, xp, yp, zp, &best, &bd2);
+        }
+    }
+    return best;
+}
+
+/* mesh.py:1306-1328 */
+static void cap_extents(double lon_p, double lat_p, double lon_n, double lat_n, double* th, double* ext) {
+    double lat_pr = lat_p * DEG2RAD, lat_nr = lat_n * DEG2RAD;
+    double cosd = sin(lat_pr) * sin(lat_nr) + cos(lat_pr) * cos(lat_nr) * cos((lon_p - lon_n) * DEG2RAD);
+    if (cosd > 1.0) cosd = 1.0;
+    if (cosd < -1.0) cosd = -1.0;
+    double theta = acos(cosd);
+    if (theta <= 0.0) { *th = 0.0; *ext = 0.0; return; }
+    *th = theta * RAD2DEG;
+    if (fabs(lat_p) + *th >= 90.0) { *ext = 1.0e30; return; }
+    double r = sin(theta) / cos(lat_pr);
+    if (r >= 1.0) { *ext = 1.0e30; return; }
+    *ext = asin(r) * RAD2DEG;
+}
+
+/* mesh.py:1475-1549 */
+static int provable_rect(const OMesh* m, double lon_p, double lat_p, int node, int rx, int ry) {
+    double th, ext;
+    cap_extents(lon_p, lat_p, m->lon[node], m->lat[node], &th, &ext);
+    if (th <= 0.0) return 0;
+    double dlon = fold_dlon(m, lon_p);
+    double lon_q = m->lon_min + dlon;
+    int ci_raw = (int)floor(dlon / m->cell);
+    int cj_raw = (int)floor((lat_p - m->lat_min) / m->cell);
+    double INF = 1.0e30;
+    int cj = cj_raw;
+    if (cj < 0) cj = 0;
+    if (cj > m->ny - 1) cj = m->ny - 1;
+    double cov_dn = cj - ry >= 0 ? lat_p - (m->lat_min + (cj - ry) * m->cell) : INF;
+    double cov_up = cj + ry <= m->ny - 1 ? (m->lat_min + (cj + ry + 1) * m->cell) - lat_p : INF;
+    int code = 0;
+    if (th > cov_dn || th > cov_up) code |= 1;
+    if (m->wrap) {
+        if (2 * rx + 1 >= m->nx) return code;
+        if (ext >= INF) return code | 4;
+        double w_last = 360.0 - (m->nx - 1) * m->cell;
+        int ci = imod(ci_raw, m->nx);
+        double left = m->lon_min + (ci - rx) * m->cell;
+        if (ci - rx < 0) left += m->cell - w_last;
+        double right = m->lon_min + (ci + rx + 1) * m->cell;
+        if (ci + rx >= m->nx - 1) right -= m->cell - w_last;
+        if (ext > lon_q - left || ext > right - lon_q) code |= 2;
+        return code;
+    }
+    int ci = ci_raw;
+    if (ci < 0) ci = 0;
+    if (ci > m->nx - 1) ci = m->nx - 1;
+    double cov_l = ci - rx >= 0 ? lon_q - (m->lon_min + (ci - rx) * m->cell) : INF;
+    double cov_r = ci + rx <= m->nx - 1 ? (m->lon_min + (ci + rx + 1) * m->cell) - lon_q : INF;
+    if (cov_l >= INF && cov_r >= INF) return code;
+    if (ext >= INF) return code | 4;
+    if (ext > cov_l || ext > cov_r) code |= 2;
+    double n_lo = m->lon_min + m->cell, n_hi = m->lon_min + (m->nx - 1) * m->cell;
+    double shifts[2] = {-360.0, 360.0};
+    for (int s = 0; s < 2; ++s) {
+        double a = lon_q - ext + shifts[s], b = lon_q + ext + shifts[s];
+        if (b >= n_lo && a <= n_hi) return code | 4;
+    }
+    return code;
+}
+
+/* mesh.py:1331-1442 */
+static int nearest_widened(const OMesh* m, double lon_p, double lat_p) {
+    int best = nearest_3x3(m, lon_p, lat_p);
+    if (best >= 0) return best;
+    int ci, cj;
+    cell_of(m, lon_p, lat_p, &ci, &cj);
+    double xp, yp, zp, cl;
+    qxyz(lon_p, lat_p, &xp, &yp, &zp, &cl);
+    double bd2 = 1e30;
+    int max_ring = m->nx > m->ny ? m->nx : m->ny;
+    int found = -1;
+    for (int r = 2; r <= max_ring; ++r) {
+        for (int dj = -r; dj <= r; ++dj) {
+            int cj2 = cj + dj;
+            if (cj2 < 0 || cj2 >= m->ny) continue;
+            int step = (dj == -r || dj == r) ? 1 : 2 * r;
+            for (int di = -r; di <= r; di += step) {
+                int ci2 = ci + di;
+                if (m->wrap) ci2 = imod(ci2, m->nx);
+                else if (ci2 < 0 || ci2 >= m->nx) continue;
+                scan_cell(m, cj2 * m->nx + ci2, xp, yp, zp, &best, &bd2);
+            }
+        }
+        if (best >= 0) {
+            if (found < 0) found = r;
+            else if (r > found) break;
+        }
+    }
+    return best;
+}
+
+static void scan_row_window(const OMesh* m, int cj2, int ci, int rx, double xp, double yp, double zp, int* best, double* bd2) {
+    if (m->wrap && 2 * rx + 1 >= m->nx) { scan_row_range(m, cj2, 0, m->nx - 1, xp, yp, zp, best, bd2); return; }
+    int lo = ci - rx, hi = ci + rx;
+    if (m->wrap) {
+        if (lo < 0) { scan_row_range(m, cj2, lo + m->nx, m->nx - 1, xp, yp, zp, best, bd2); lo = 0; }
+        else if (hi > m->nx - 1) { scan_row_range(m, cj2, 0, hi - m->nx, xp, yp, zp, best, bd2); hi = m->nx - 1; }
+    } else {
+        if (lo < 0) lo = 0;
+        if (hi > m->nx - 1) hi = m->nx - 1;
+    }
+    scan_row_range(m, cj2, lo, hi, xp, yp, zp, best, bd2);
+}
+
+/* mesh.py:1611-1859 */
+static int nearest_exact(const OMesh* m, double lon_p, double lat_p) {
+    double far = m->far_rows * m->cell;
+    if (lat_p < m->lat_min - far || lat_p > m->lat_min + m->ny * m->cell + far)
+        return nearest_widened(m, lon_p, lat_p);
+    int best = nearest_3x3(m, lon_p, lat_p);
+    int code = 0;
+    if (best >= 0) {
+        code = provable_rect(m, lon_p, lat_p, best, 1, 1);
+        if (code == 0) return best;
+        double th, ext;
+        cap_extents(lon_p, lat_p, m->lon[best], m->lat[best], &th, &ext);
+        if (th > far) return best;
+    }
+    int ci, cj;
+    cell_of(m, lon_p, lat_p, &ci, &cj);
+    double xp, yp, zp, cos_lat_p;
+    qxyz(lon_p, lat_p, &xp, &yp, &zp, &cos_lat_p);
+    double best_d2 = 1.0e30;
+    if (best >= 0) {
+        double xn = m->xyz[3 * (int64_t)best], yn = m->xyz[3 * (int64_t)best + 1], zn = m->xyz[3 * (int64_t)best + 2];
+        best_d2 = (xn - xp) * (xn - xp) + (yn - yp) * (yn - yp) + (zn - zp) * (zn - zp);
+    }
+    int rx = 1, ry = 1;
+    int short_row = 360.0 * cos_lat_p <= 32 * m->cell;
+    int rx_max;
+    if (m->wrap) { rx_max = m->nx / 2; if (rx_max < 1) rx_max = 1; }
+    else rx_max = ci > m->nx - 1 - ci ? ci : m->nx - 1 - ci;
+    int ry_max = cj > m->ny - 1 - cj ? cj : m->ny - 1 - cj;
+    double abs_lat = lat_p >= 0.0 ? lat_p : -lat_p;
+    double dlon_q = fold_dlon(m, lon_p);
+    double INF = 1.0e30;
+    for (;;) {
+        if (best >= 0 && code == 0) {
+            code = provable_rect(m, lon_p, lat_p, best, rx, ry);
+            if (code == 0) return best;
+        }
+        if (best < 0 || 2.0 * asin(0.5 * sqrt(best_d2)) * RAD2DEG > far) {
+            int cols_full = m->wrap ? (2 * rx + 1 >= m->nx) : (ci - rx <= 0 && ci + rx >= m->nx - 1);
+            double clear = ry >= ry_max ? INF : ry * m->cell;
+            if (!cols_full) {
+                double lat_edge = abs_lat + (ry + 1) * m->cell;
+                double clear_lon;
+                if (lat_edge >= 90.0) clear_lon = 0.0;
+                else {
+                    double dl = rx * m->cell;
+                    if (!m->wrap) {
+                        double x = dlon_q > 0.0 ? dlon_q : 0.0;
+                        double w = m->nx * m->cell;
+                        if (x > w) x = w;
+                        double near_edge = x < w - x ? x : w - x;
+                        double dl_cut = 360.0 - w + near_edge;
+                        if (dl_cut < dl) dl = dl_cut;
+                    }
+                    if (dl > 180.0) dl = 180.0;
+                    clear_lon = asin(sin(dl * DEG2RAD) * cos(lat_edge * DEG2RAD)) * RAD2DEG;
+                }
+                if (clear_lon < clear) clear = clear_lon;
+            }
+            if (clear >= far) {
+                if (best >= 0) return best;
+                return nearest_widened(m, lon_p, lat_p);
+            }
+        }
+        int gx, gy, ax;
+        if (best >= 0) { gx = (code & 2) != 0; gy = (code & 1) != 0; ax = (code & 4) != 0; code = 0; }
+        else if (short_row) { gx = 0; gy = 1; ax = 1; }
+        else { gx = 1; gy = 1; ax = 0; }
+        if (rx >= rx_max) { gx = 0; ax = 0; }
+        if (ry >= ry_max) gy = 0;
+        if (!(gx || gy || ax)) {
+            if (best >= 0) return best;
+            return nearest_widened(m, lon_p, lat_p);
+        }
+        int rx_new = ax ? rx_max : (gx ? rx + 1 : rx);
+        int ry_new = gy ? ry + 1 : ry;
+        int j_lo = cj - ry > 0 ? cj - ry : 0;
+        int j_hi = cj + ry < m->ny - 1 ? cj + ry : m->ny - 1;
+        if (rx_new > rx) {
+            if (m->wrap && 2 * rx_new + 1 >= m->nx && rx_new - rx > 1) {
+                for (int cj2 = j_lo; cj2 <= j_hi; ++cj2) {
+                    int lo = imod(ci + rx + 1, m->nx), hi = imod(ci - rx - 1, m->nx);
+                    if (lo <= hi) scan_row_range(m, cj2, lo, hi, xp, yp, zp, &best, &best_d2);
+                    else {
+                        scan_row_range(m, cj2, lo, m->nx - 1, xp, yp, zp, &best, &best_d2);
+                        scan_row_range(m, cj2, 0, hi, xp, yp, zp, &best, &best_d2);
+                    }
+                }
+            } else if (!m->wrap && rx_new - rx > 1) {
+                for (int cj2 = j_lo; cj2 <= j_hi; ++cj2) {
+                    if (ci - rx - 1 >= 0) {
+                        int lo = ci - rx_new > 0 ? ci - rx_new : 0;
+                        scan_row_range(m, cj2, lo, ci - rx - 1, xp, yp, zp, &best, &best_d2);
+                    }
+                    if (ci + rx + 1 <= m->nx - 1) {
+                        int hi = ci + rx_new < m->nx - 1 ? ci + rx_new : m->nx - 1;
+                        scan_row_range(m, cj2, ci + rx + 1, hi, xp, yp, zp, &best, &best_d2);
+                    }
+                }
+            } else {
+                for (int r = rx + 1; r <= rx_new; ++r) {
+                    if (m->wrap) {
+                        int cl2 = imod(ci - r, m->nx), cr2 = imod(ci + r, m->nx);
+                        int two = 2 * r + 1 <= m->nx;
+                        for (int cj2 = j_lo; cj2 <= j_hi; ++cj2) {
+                            scan_cell(m, cj2 * m->nx + cl2, xp, yp, zp, &best, &best_d2);
+                            if (two) scan_cell(m, cj2 * m->nx + cr2, xp, yp, zp, &best, &best_d2);
+                        }
+                    } else {
+                        int cs[2] = {ci - r, ci + r};
+                        for (int s = 0; s < 2; ++s) {
+                            if (cs[s] < 0 || cs[s] > m->nx - 1) continue;
+                            for (int cj2 = j_lo; cj2 <= j_hi; ++cj2)
+                                scan_cell(m, cj2 * m->nx + cs[s], xp, yp, zp, &best, &best_d2);
+                        }
+                    }
+                }
+            }
+        }
+        for (int r = ry + 1; r <= ry_new; ++r) {
+            int rows[2] = {cj - r, cj + r};
+            for (int s = 0; s < 2; ++s) {
+                if (rows[s] < 0 || rows[s] > m->ny - 1) continue;
+                scan_row_window(m, rows[s], ci, rx_new, xp, yp, zp, &best, &best_d2);
+            }
+        }
+        rx = rx_new;
+        ry = ry_new;
+    }
+}
+
+/* integrators.py:1470-1487 */
+static int anchor(const OMesh* m, double lon_p, double lat_p) {
+    return m->exact ? nearest_exact(m, lon_p, lat_p) : nearest_widened(m, lon_p, lat_p);
+}
+
+/* mesh.py:2054-2073 */
+static void bary_tri(double px, double py, const double* tx, const double* ty, double* w) {
+    double ax = tx[0], ay = ty[0], bx = tx[1], by = ty[1], cx = tx[2], cy = ty[2];
+    double denom = (by - cy) * (ax - cx) + (cx - bx) * (ay - cy);
+    if (fabs(denom) < AREA_TOL) { w[0] = w[1] = w[2] = -1.0; return; }
+    w[0] = ((by - cy) * (px - cx) + (cx - bx) * (py - cy)) / denom;
+    w[1] = ((cy - ay) * (px - cx) + (ax - cx) * (py - cy)) / denom;
+    w[2] = 1.0 - w[0] - w[1];
+}
+
+/* mesh.py:2076-2116 */
+static void wachspress(double px, double py, const double* x, const double* y, double* out) {
+    double A[4], Cc[4], s = 0.0;
+    for (int k = 0; k < 4; ++k) {
+        int i1 = (k + 1) % 4, im = (k + 3) % 4;
+        A[k] = (x[k] - px) * (y[i1] - py) - (x[i1] - px) * (y[k] - py);
+        Cc[k] = (x[k] - x[im]) * (y[i1] - y[im]) - (x[i1] - x[im]) * (y[k] - y[im]);
+    }
+    for (int k = 0; k < 4; ++k) { out[k] = Cc[k] * A[(k + 1) % 4] * A[(k + 2) % 4]; s += out[k]; }
+    for (int k = 0; k < 4; ++k) out[k] = out[k] / s;
+}
+
+/* mesh.py:2119-2136 */
+static void polygon_weights(double px, double py, const double* x, const double* y, int nv, double* w) {
+    if (nv == 3) {
+        double t[3];
+        bary_tri(px, py, x, y, t);
+        w[0] = t[0]; w[1] = t[1]; w[2] = t[2];
+        return;
+    }
+    wachspress(px, py, x, y, w);
+}
+
+/* mesh.py:2210-2263 + :2006-2051 + :2139-2168 */
+static int element_contains(const OMesh* m, int c, double lon_p, double lat_p) {
+    const int32_t* nodes = m->en + (int64_t)c * m->max_v;
+    int mask[4] = {0, 0, 0, 0};
+    for (int k = 0; k < m->max_v; ++k) mask[k] = nodes[k] >= 0;
+    if (m->max_v == 4 && nodes[3] == nodes[0] && nodes[0] >= 0) mask[3] = 0;
+    double ln[4], la[4];
+    int n = 0;
+    for (int k = 0; k < m->max_v; ++k)
+        if (mask[k]) { ln[n] = m->lon[nodes[k]]; la[n] = m->lat[nodes[k]]; ++n; }
+    if (n < 3) return 0;
+    double ref = ln[0], dmax = -1e300, dmin = 1e300, lmax = -1e300, lmin = 1e300;
+    for (int k = 0; k < n; ++k) {
+        double d = wrap180(ln[k] - ref);
+        if (d > dmax) dmax = d;
+        if (d < dmin) dmin = d;
+        if (la[k] > lmax) lmax = la[k];
+        if (la[k] < lmin) lmin = la[k];
+    }
+    double dp = wrap180(lon_p - ref);
+    if (dp > dmax || dp < dmin) return 0;
+    if (lat_p > lmax || lat_p < lmin) return 0;
+    double lo_min = ln[0], lo_max = ln[0];
+    for (int k = 0; k < n; ++k) { if (ln[k] < lo_min) lo_min = ln[k]; if (ln[k] > lo_max) lo_max = ln[k]; }
+    double lon0;
+    if (lo_max - lo_min > 180.0) {
+        double ds = 0.0;
+        for (int k = 0; k < n; ++k) ds += wrap180(ln[k] - ln[0]);
+        lon0 = ln[0] + ds / n;
+    } else {
+        double s = 0.0;
+        for (int k = 0; k < n; ++k) s += ln[k];
+        lon0 = s / n;
+    }
+    double s = 0.0;
+    for (int k = 0; k < n; ++k) s += la[k];
+    double lat0 = s / n;
+    double cl = cos(lat0 * DEG2RAD);
+    double x[4], y[4];
+    for (int k = 0; k < n; ++k) {
+        x[k] = wrap180(ln[k] - lon0) * DEG2RAD * R_STD * cl;
+        y[k] = (la[k] - lat0) * DEG2RAD * R_STD;
+    }
+    double px = wrap180(lon_p - lon0) * DEG2RAD * R_STD * cl;
+    double py = (lat_p - lat0) * DEG2RAD * R_STD;
+    double w[3];
+    if (n == 3) {
+        bary_tri(px, py, x, y, w);
+        return w[0] >= BARY_EPS && w[1] >= BARY_EPS && w[2] >= BARY_EPS;
+    }
+    for (int i = 1; i < n - 1; ++i) {
+        double tx[3] = {x[0], x[i], x[i + 1]}, ty[3] = {y[0], y[i], y[i + 1]};
+        bary_tri(px, py, tx, ty, w);
+        if (w[0] >= BARY_EPS && w[1] >= BARY_EPS && w[2] >= BARY_EPS) return 1;
+    }
+    return 0;
+}
+
+/* mesh.py:2392-2470 */
+static int contain_local(const OMesh* m, double lon_p, double lat_p, int nn) {
+    int cnt = m->n2e_cnt[nn];
+    if (cnt == 0) return -1;
+    const int32_t* row = m->n2e + (int64_t)nn * m->max_conn;
+    for (int k = 0; k < cnt; ++k) {
+        int c = row[k];
+        if (c < 0) continue;
+        if (element_contains(m, c, lon_p, lat_p)) return c;
+    }
+    for (int k = 0; k < cnt; ++k) {
+        int e = row[k];
+        if (e < 0) continue;
+        for (int j = 0; j < m->max_v; ++j) {
+            int v = m->en[(int64_t)e * m->max_v + j];
+            if (v < 0 || v == nn) continue;
+            int cv = m->n2e_cnt[v];
+            const int32_t* rv = m->n2e + (int64_t)v * m->max_conn;
+            for (int kk = 0; kk < cv; ++kk) {
+                int c = rv[kk];
+                if (c < 0) continue;
+                int touches = 0;
+                for (int jj = 0; jj < m->max_v; ++jj)
+                    if (m->en[(int64_t)c * m->max_v + jj] == nn) { touches = 1; break; }
+                if (touches) continue;
+                if (element_contains(m, c, lon_p, lat_p)) return c;
+            }
+        }
+    }
+    return -1;
+}
+
+/* mesh.py:1973-2003 */
+static double seam_lon0(const double* ln, int n) {
+    double first = ln[0], lmin = first, lmax = first, s = 0.0;
+    for (int v = 0; v < n; ++v) { s += ln[v]; if (ln[v] < lmin) lmin = ln[v]; if (ln[v] > lmax) lmax = ln[v]; }
+    if (lmax - lmin > 180.0) {
+        double d = 0.0;
+        for (int v = 0; v < n; ++v) d += wrap180(ln[v] - first);
+        return first + d / n;
+    }
+    return s / n;
+}
+
+/* interpolate.py:1404-1436, vertical.py:1042-1061 */
+static double tblend(double a, double b, double t, double alpha0, double alpha) {
+    if (alpha < 1e-12) {
+        if (alpha0 == 0.0) return a;
+        return (1.0 - alpha0) * a + alpha0 * b;
+    }
+    if (alpha > 1.0 - 1e-12) return t;
+    if (alpha0 == 0.0) return (1.0 - alpha) * a + alpha * t;
+    double a0 = (1.0 - alpha0) * a + alpha0 * b;
+    return (1.0 - alpha) * a0 + alpha * t;
+}
+
+/* interpolate.py:1340-1529 (row 0: 2-D; row = layer: 3-D) */
+static int interp_uv(const OMesh* m, const OField* f, double xp, double yp, int nn, double td, int row,
+                     double alpha, double* U, double* V) {
+    *U = 0.0; *V = 0.0;
+    int elem = contain_local(m, xp, yp, nn);
+    if (elem < 0) return 0;
+    int verts[4], nv = 0;
+    for (int k = 0; k < m->max_v; ++k) {
+        int nd = m->en[(int64_t)elem * m->max_v + k];
+        if (nd < 0) continue;
+        if (nv > 0 && nd == verts[0]) continue;
+        verts[nv++] = nd;
+    }
+    if (nv < 3) return 0;
+    double R = m->r_earth;
+    double lon_ref = m->lon[verts[0]], dsum = 0.0, lat0 = 0.0;
+    for (int k = 0; k < nv; ++k) { dsum += wrap180(m->lon[verts[k]] - lon_ref); lat0 += m->lat[verts[k]]; }
+    double lon0 = lon_ref + dsum / nv;
+    lat0 /= nv;
+    double cosl = cos(lat0 * DEG2RAD);
+    double vx[4], vy[4];
+    for (int k = 0; k < nv; ++k) {
+        vx[k] = wrap180(m->lon[verts[k]] - lon0) * DEG2RAD * R * cosl;
+        vy[k] = (m->lat[verts[k]] - lat0) * DEG2RAD * R;
+    }
+    double px = wrap180(xp - lon0) * DEG2RAD * R * cosl;
+    double py = (yp - lat0) * DEG2RAD * R;
+    double w[4];
+    polygon_weights(px, py, vx, vy, nv, w);
+    if (w[0] == -1.0) return 0;
+    double Us = 0.0, Vs = 0.0;
+    for (int k = 0; k < nv; ++k) {
+        int64_t idx = (int64_t)row * f->n + verts[k];
+        double un = tblend(fld(f->ua, f->f32, idx), fld(f->ub, f->f32, idx), fld(f->ut, f->f32, idx), f->alpha0, alpha);
+        double vn = tblend(fld(f->va, f->f32, idx), fld(f->vb, f->f32, idx), fld(f->vt, f->f32, idx), f->alpha0, alpha);
+        Us += w[k] * un;
+        Vs += w[k] * vn;
+    }
+    *U = td * Us;
+    *V = td * Vs;
+    return 1;
+}
+
+/* vertical.py:39-91 */
+static int find_layer(const OMesh* m, double z, double bottom) {
+    int K = m->K;
+    const double* zl = m->zlev;
+    if (K < 2) return 0;
+    if (z <= zl[0]) return 0;
+    int max_layer = K - 2;
+    for (int k = 0; k < K - 1; ++k)
+        if (zl[k + 1] > bottom) { max_layer = k - 1 > 0 ? k - 1 : 0; break; }
+    if (z >= bottom || z >= zl[max_layer + 1]) return max_layer;
+    for (int k = 0; k <= max_layer; ++k)
+        if (z < zl[k + 1]) return k;
+    return max_layer;
+}
+
+static double wat(const OField* f, int k, int node, double alpha) {
+    int64_t idx = (int64_t)k * f->n + node;
+    return tblend(fld(f->wa, f->f32, idx), fld(f->wb, f->f32, idx), fld(f->wt, f->f32, idx), f->alpha0, alpha);
+}
+
+/* vertical.py:1064-1098 */
+static double w_linear(const OMesh* m, const OField* f, double alpha, double z, int node, double td) {
+    int K = m->K;
+    const double* zl = m->zlev;
+    if (K < 2) return td * wat(f, 0, node, alpha);
+    if (z <= zl[0]) return td * wat(f, 0, node, alpha);
+    if (z >= zl[K - 1]) return td * wat(f, K - 1, node, alpha);
+    int k = K - 2;
+    for (int j = 0; j < K - 1; ++j)
+        if (z < zl[j + 1]) { k = j; break; }
+    double dz = zl[k + 1] - zl[k];
+    if (dz < 1e-12) return td * wat(f, k, node, alpha);
+    double a = (z - zl[k]) / dz;
+    double lo = wat(f, k, node, alpha), hi = wat(f, k + 1, node, alpha);
+    return td * ((1.0 - a) * lo + a * hi);
+}
+
+static double pymin(double a, double b) { return b < a ? b : a; }
+
+/* vertical.py:744-881 */
+static double w_bary(const OMesh* m, const OField* f, double alpha, double xp, double yp, double z, int node, double td) {
+    int cnt = m->n2e_cnt[node];
+    if (cnt == 0) return w_linear(m, f, alpha, pymin(z, m->depth[node]), node, td);
+    for (int k = 0; k < cnt; ++k) {
+        int e = m->n2e[(int64_t)node * m->max_conn + k];
+        if (e < 0) continue;
+        int verts[4], nv = 0;
+        for (int v = 0; v < m->max_v; ++v) {
+            int nd = m->en[(int64_t)e * m->max_v + v];
+            if (nd < 0) continue;
+            if (nv > 0 && nd == verts[0]) continue;
+            verts[nv++] = nd;
+        }
+        if (nv < 3) continue;
+        double ln[4];
+        for (int v = 0; v < nv; ++v) ln[v] = m->lon[verts[v]];
+        double lon0 = seam_lon0(ln, nv), lat0 = 0.0;
+        for (int v = 0; v < nv; ++v) lat0 += m->lat[verts[v]];
+        lat0 /= nv;
+        double cl = cos(lat0 * DEG2RAD), R = 6371000.0;
+        double vx[4], vy[4];
+        for (int v = 0; v < nv; ++v) {
+            vx[v] = wrap180(m->lon[verts[v]] - lon0) * DEG2RAD * R * cl;
+            vy[v] = (m->lat[verts[v]] - lat0) * DEG2RAD * R;
+        }
+        double px = wrap180(xp - lon0) * DEG2RAD * R * cl;
+        double py = (yp - lat0) * DEG2RAD * R;
+        for (int t = 0; t < nv - 2; ++t) {
+            int i1 = t + 1, i2 = t + 2;
+            double ax = vx[0], ay = vy[0], bx = vx[i1], by = vy[i1], cx = vx[i2], cy = vy[i2];
+            double denom = (by - cy) * (ax - cx) + (cx - bx) * (ay - cy);
+            if (fabs(denom) < 1e-14) continue;
+            double w1 = ((by - cy) * (px - cx) + (cx - bx) * (py - cy)) / denom;
+            double w2 = ((cy - ay) * (px - cx) + (ax - cx) * (py - cy)) / denom;
+            double w3 = 1.0 - w1 - w2;
+            if (w1 >= -1e-6 && w2 >= -1e-6 && w3 >= -1e-6) {
+                if (nv == 4) {
+                    double wts[4], acc = 0.0;
+                    polygon_weights(px, py, vx, vy, 4, wts);
+                    for (int vi = 0; vi < 4; ++vi)
+                        acc += wts[vi] * w_linear(m, f, alpha, pymin(z, m->depth[verts[vi]]), verts[vi], td);
+                    return acc;
+                }
+                int n0 = verts[0], n1 = verts[i1], n2 = verts[i2];
+                double a0 = w_linear(m, f, alpha, pymin(z, m->depth[n0]), n0, td);
+                double a1 = w_linear(m, f, alpha, pymin(z, m->depth[n1]), n1, td);
+                double a2 = w_linear(m, f, alpha, pymin(z, m->depth[n2]), n2, td);
+                return w1 * a0 + w2 * a1 + w3 * a2;
+            }
+        }
+    }
+    return w_linear(m, f, alpha, pymin(z, m->depth[node]), node, td);
+}
+
+/* diffusion.py:180-249 */
+static uint64_t splitmix64(uint64_t x) {
+    x = x + 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+uint64_t orc_key_hash(uint64_t k0, uint64_t k1, uint64_t k2, uint64_t k3, uint64_t k4) {
+    uint64_t h = k0;
+    h = splitmix64(h ^ k1);
+    h = splitmix64(h ^ k2);
+    h = splitmix64(h ^ k3);
+    h = splitmix64(h ^ k4);
+    return h;
+}
+
+void orc_normal_pair(uint64_t seed, uint64_t real_id, uint64_t pid, uint64_t step, uint64_t comp, double* g) {
+    uint64_t h = orc_key_hash(seed, real_id, pid, step, comp);
+    double inv = 1.0 / 4294967296.0, half = 0.5 * inv;
+    double u1 = (double)((h >> 32) & 0xFFFFFFFFull) * inv + half;
+    double u2 = (double)(h & 0xFFFFFFFFull) * inv + half;
+    double two_pi = 2.0 * 3.141592653589793;
+    double r = sqrt(-2.0 * log(u1));
+    g[0] = r * cos(two_pi * u2);
+    g[1] = r * sin(two_pi * u2);
+}
+
+/* diffusion.py:538-575 */
+static void sphere_displace(double lon, double lat, double dx, double dy, double* lon2, double* lat2) {
+    double dist = sqrt(dx * dx + dy * dy);
+    if (dist == 0.0) { *lon2 = lon; *lat2 = lat; return; }
+    double rm = SLM / DEG2RAD;
+    double lam = lon * DEG2RAD, phi = lat * DEG2RAD;
+    double cl = cos(lam), sl = sin(lam), cp = cos(phi), sp = sin(phi);
+    double delta = dist / rm;
+    double c = cos(delta), s = sin(delta) / dist;
+    double tx = -sl * dx - sp * cl * dy;
+    double ty = cl * dx - sp * sl * dy;
+    double tz = cp * dy;
+    double x2 = cp * cl * c + tx * s, y2 = cp * sl * c + ty * s, z2 = sp * c + tz * s;
+    if (z2 > 1.0) z2 = 1.0;
+    else if (z2 < -1.0) z2 = -1.0;
+    *lat2 = asin(z2) / DEG2RAD;
+    *lon2 = wrap180(atan2(y2, x2) / DEG2RAD);
+}
+
+typedef struct {
+    int scheme, dims, w_code, kick;
+    double dt, td, ak[4], kh_x, kh_y;
+    uint64_t seed, real_id, step_i, pid_offset;
+} OStep;
+
+static double z0_of(double lat) {
+    double z0 = cos(lat * DEG2RAD) * SLM;
+    return z0 < 1.0 ? 1.0 : z0;
+}
+static double clat(double x) { return x > 90.0 ? 90.0 : (x < -90.0 ? -90.0 : x); }
+
+/* integrators.py:673-818 for one surviving particle */
+static void kick(const OMesh* m, const OStep* s, int64_t pid, double pre_lon, double pre_lat, double pre_z, int pre_nn,
+                 double* lon, double* lat, double* z, int* status, int* nn, int8_t* fr, int is3d) {
+    double g[2];
+    orc_normal_pair(s->seed, s->real_id, (uint64_t)pid + s->pid_offset, s->step_i, 0, g);
+    double adt = s->dt >= 0.0 ? s->dt : -s->dt;
+    double sq = sqrt(adt), sx = sqrt(2.0 * s->kh_x), sy = sqrt(2.0 * s->kh_y);
+    double dx = sx * sq * g[0], dy = sy * sq * g[1];
+    if (s->kh_x != s->kh_y) {
+        double la = *lat;
+        if (la < -89.9) la = -89.9;
+        if (la > 89.9) la = 89.9;
+        dy = dy + (s->kh_x - s->kh_y) * tan(la * DEG2RAD) / (SLM / DEG2RAD) * adt;
+    }
+    double lk, lak;
+    sphere_displace(*lon, *lat, dx, dy, &lk, &lak);
+    int nk = anchor(m, lk, lak);
+    if (contain_local(m, lk, lak, nk) < 0) {
+        *status = OUTSIDE; *lon = pre_lon; *lat = pre_lat; *z = pre_z; *nn = pre_nn; *fr = 2;
+        return;
+    }
+    *lon = lk; *lat = lak; *nn = nk;
+    if (is3d) {
+        double zv = *z;
+        if (zv < m->zlev[0]) zv = m->zlev[0];
+        if (zv > m->depth[nk]) zv = m->depth[nk];
+        *z = zv;
+    }
+}
+
+/* integrators.py:2521-2816 (2-D RK2/RK4 fused), the unfused Euler's per-particle
+ * arithmetic (integrators.py:4997-5147), :3647-3856 (3-D RK2 fused). */
+static void step_one(const OMesh* m, const OField* f, const OStep* s, int64_t i, double* lon, double* lat, double* z,
+                     int* status, int* nn, int8_t* fr, double* U, double* V, double* W, const int64_t* pid) {
+    if (status[i] != ALIVE) {
+        U[i] = 0.0; V[i] = 0.0;
+        if (W) W[i] = 0.0;
+        return;
+    }
+    double lon0 = lon[i], lat0 = lat[i], zp = z ? z[i] : 0.0, dt = s->dt, td = s->td;
+    int pre_nn = nn[i], st = ALIVE, nno;
+    int8_t frr = fr[i];
+    double ln = lon0, lt = lat0, zn = zp;
+    int node_i = anchor(m, lon0, lat0);
+    nno = node_i;
+    int ok = 1;
+    if (s->dims == 2) {
+        double U1, V1;
+        int ok1 = interp_uv(m, f, lon0, lat0, node_i, td, 0, s->ak[0], &U1, &V1);
+        U[i] = U1; V[i] = V1;
+        if (!ok1) { ok = 0; }
+        else if (s->scheme == 0) {
+            ln = wrap180(lon0 + dt * U1 / z0_of(lat0));
+            lt = clat(lat0 + dt * V1 / SLM);
+        } else if (s->scheme == 1) {
+            double lm = wrap180(lon0 + 0.5 * dt * U1 / z0_of(lat0));
+            double tm = clat(lat0 + 0.5 * dt * V1 / SLM);
+            int nm = anchor(m, lm, tm);
+            double U2, V2;
+            if (!interp_uv(m, f, lm, tm, nm, td, 0, s->ak[1], &U2, &V2)) ok = 0;
+            else { ln = wrap180(lon0 + dt * U2 / z0_of(tm)); lt = clat(lat0 + dt * V2 / SLM); }
+        } else {
+            double dl1 = dt * U1 / z0_of(lat0), dt1 = dt * V1 / SLM;
+            double l2 = wrap180(lon0 + 0.5 * dl1), t2 = clat(lat0 + 0.5 * dt1);
+            double U2, V2, U3, V3, U4, V4;
+            if (!interp_uv(m, f, l2, t2, anchor(m, l2, t2), td, 0, s->ak[1], &U2, &V2)) ok = 0;
+            else {
+                double dl2 = dt * U2 / z0_of(t2), dt2 = dt * V2 / SLM;
+                double l3 = wrap180(lon0 + 0.5 * dl2), t3 = clat(lat0 + 0.5 * dt2);
+                if (!interp_uv(m, f, l3, t3, anchor(m, l3, t3), td, 0, s->ak[2], &U3, &V3)) ok = 0;
+                else {
+                    double dl3 = dt * U3 / z0_of(t3), dt3 = dt * V3 / SLM;
+                    double l4 = wrap180(lon0 + dl3), t4 = clat(lat0 + dt3);
+                    if (!interp_uv(m, f, l4, t4, anchor(m, l4, t4), td, 0, s->ak[3], &U4, &V4)) ok = 0;
+                    else {
+                        double dl4 = dt * U4 / z0_of(t4), dt4 = dt * V4 / SLM;
+                        double dl = (dl1 + 2.0 * dl2 + 2.0 * dl3 + dl4) / 6.0;
+                        double dd = (dt1 + 2.0 * dt2 + 2.0 * dt3 + dt4) / 6.0;
+                        ln = wrap180(lon0 + dl);
+                        lt = clat(lat0 + dd);
+                    }
+                }
+            }
+        }
+        if (!ok) { st = OUTSIDE; frr = 1; ln = lon0; lt = lat0; }
+        else {
+            int nw = anchor(m, ln, lt);
+            if (contain_local(m, ln, lt, nw) < 0) { st = OUTSIDE; frr = 2; ln = lon0; lt = lat0; }
+            else nno = nw;
+        }
+    } else {
+        int l1 = find_layer(m, zp, m->depth[node_i]);
+        double U1, V1;
+        int ok1 = interp_uv(m, f, lon0, lat0, node_i, td, l1, s->ak[0], &U1, &V1);
+        double W1 = s->w_code == 0 ? w_linear(m, f, s->ak[0], zp, node_i, td)
+                                   : w_bary(m, f, s->ak[0], lon0, lat0, zp, node_i, td);
+        U[i] = U1; V[i] = V1; W[i] = W1;
+        if (!ok1) { st = OUTSIDE; frr = 1; }
+        else {
+            double lm = wrap180(lon0 + 0.5 * dt * U1 / z0_of(lat0));
+            double tm = clat(lat0 + 0.5 * dt * V1 / SLM);
+            double zm = zp + W1 * 0.5 * dt;
+            int nm = anchor(m, lm, tm);
+            int l2 = find_layer(m, zm, m->depth[nm]);
+            double U2, V2;
+            if (!interp_uv(m, f, lm, tm, nm, td, l2, s->ak[1], &U2, &V2)) { st = OUTSIDE; frr = 1; }
+            else {
+                double W2 = s->w_code == 0 ? w_linear(m, f, s->ak[1], zm, nm, td)
+                                           : w_bary(m, f, s->ak[1], lm, tm, zm, nm, td);
+                double a = wrap180(lon0 + dt * U2 / z0_of(tm));
+                double b = clat(lat0 + dt * V2 / SLM);
+                double c = zp + W2 * dt;
+                int nw = anchor(m, a, b);
+                if (contain_local(m, a, b, nw) < 0) { st = OUTSIDE; frr = 2; }
+                else {
+                    if (c < m->zlev[0]) c = m->zlev[0];
+                    if (c > m->depth[nw]) c = m->depth[nw];
+                    ln = a; lt = b; zn = c; nno = nw;
+                }
+            }
+        }
+    }
+    if (s->kick && st == ALIVE)
+        kick(m, s, pid ? pid[i] : i, lon0, lat0, zp, pre_nn, &ln, &lt, &zn, &st, &nno, &frr, s->dims == 3);
+    lon[i] = ln; lat[i] = lt;
+    if (z) z[i] = zn;
+    status[i] = st; nn[i] = nno; fr[i] = frr;
+}
+
+
+/* ---- a small dynamic parallel-for over particles (pthreads) ---------- */
+
+typedef void (*orc_body)(void* ctx, int64_t i);
+typedef struct {
+    orc_body fn;
+    void* ctx;
+    int64_t n, chunk;
+    int64_t next;
+    pthread_mutex_t mu;
+} orc_pool;
+
+static int g_threads = 0;
+
+int orc_set_threads(int n) { g_threads = n; return 0; }
+
+int orc_get_threads(void) {
+    if (g_threads > 0) return g_threads;
+    long n = sysconf(_SC_NPROCESSORS_ONLN);
+    return n > 0 ? (int)n : 1;
+}
+
+static void* orc_worker(void* arg) {
+    orc_pool* p = (orc_pool*)arg;
+    for (;;) {
+        pthread_mutex_lock(&p->mu);
+        int64_t s = p->next;
+        p->next += p->chunk;
+        pthread_mutex_unlock(&p->mu);
+        if (s >= p->n) break;
+        int64_t e = s + p->chunk < p->n ? s + p->chunk : p->n;
+        for (int64_t i = s; i < e; ++i) p->fn(p->ctx, i);
+    }
+    return NULL;
+}
+
+static void par_for(int64_t n, orc_body fn, void* ctx) {
+    int nt = orc_get_threads();
+    if (nt > 256) nt = 256;
+    orc_pool p;
+    p.fn = fn; p.ctx = ctx; p.n = n; p.chunk = 256; p.next = 0;
+    pthread_mutex_init(&p.mu, NULL);
+    if (nt <= 1 || n < 1024) {
+        orc_worker(&p);
+    } else {
+        pthread_t th[256];
+        for (int t = 0; t < nt; ++t) pthread_create(&th[t], NULL, orc_worker, &p);
+        for (int t = 0; t < nt; ++t) pthread_join(th[t], NULL);
+    }
+    pthread_mutex_destroy(&p.mu);
+}
+
+/* ---- exported entry points (ctypes) ---------------------------------- */
+
+typedef struct {
+    int64_t N, E;
+    int max_v, max_conn;
+    const double *lon, *lat, *depth, *xyz, *zlev;
+    const int32_t *en, *n2e, *n2e_cnt, *gh_off, *gh_ids;
+    double cell, lon_min, lat_min, r_earth;
+    int nx, ny, wrap, far_rows, exact, K;
+} orc_mesh;
+
+typedef struct {
+    const void *ua, *va, *wa, *ub, *vb, *wb, *ut, *vt, *wt;
+    int f32;
+    double alpha0;
+    int64_t n;
+} orc_field;
+
+typedef struct {
+    int scheme, dims, w_code, kick;
+    double dt, td, ak[4], kh_x, kh_y;
+    uint64_t seed, real_id, step_i, pid_offset;
+} orc_step_args;
+
+typedef struct {
+    const OMesh* m; const OField* f; const OStep* s;
+    double *lon, *lat, *z; int *status, *nn; int8_t* fr; double *U, *V, *W; const int64_t* pid;
+} StepCtx;
+
+static void step_body(void* ctx, int64_t i) {
+    StepCtx* c = (StepCtx*)ctx;
+    step_one(c->m, c->f, c->s, i, c->lon, c->lat, c->z, c->status, c->nn, c->fr, c->U, c->V, c->W, c->pid);
+}
+
+typedef struct { const OMesh* m; const double *lon, *lat; const int* nn; int* out; } QCtx;
+static void near_body(void* ctx, int64_t i) { QCtx* c = (QCtx*)ctx; c->out[i] = anchor(c->m, c->lon[i], c->lat[i]); }
+static void cont_body(void* ctx, int64_t i) { QCtx* c = (QCtx*)ctx; c->out[i] = contain_local(c->m, c->lon[i], c->lat[i], c->nn[i]); }
+
+int orc_step(const orc_mesh* mm, const orc_field* ff, const orc_step_args* ss, int64_t P, double* lon, double* lat,
+             double* z, int* status, int* nn, int8_t* fr, double* U, double* V, double* W, const int64_t* pid,
+             const int* release_step, int64_t global_step) {
+    const OMesh* m = (const OMesh*)mm;
+    const OField* f = (const OField*)ff;
+    const OStep* s = (const OStep*)ss;
+    if (release_step && global_step >= 0)
+        for (int64_t i = 0; i < P; ++i)
+            if (status[i] == NOT_RELEASED && global_step >= release_step[i]) status[i] = ALIVE;
+    StepCtx c = {m, f, s, lon, lat, z, status, nn, fr, U, V, W, pid};
+    par_for(P, step_body, &c);
+    return 0;
+}
+
+int orc_find_nearest(const orc_mesh* mm, int64_t P, const double* lon, const double* lat, int* out) {
+    const OMesh* m = (const OMesh*)mm;
+    QCtx c = {m, lon, lat, NULL, out};
+    par_for(P, near_body, &c);
+    return 0;
+}
+
+int orc_contain(const orc_mesh* mm, int64_t P, const double* lon, const double* lat, const int* nn, int* out) {
+    const OMesh* m = (const OMesh*)mm;
+    QCtx c = {m, lon, lat, nn, out};
+    par_for(P, cont_body, &c);
+    return 0;
+}
+
+int orc_normals(int64_t P, uint64_t seed, uint64_t real_id, uint64_t step, uint64_t pid_offset, double* g) {
+    for (int64_t i = 0; i < P; ++i) orc_normal_pair(seed, real_id, (uint64_t)i + pid_offset, step, 0, g + 2 * i);
+    return 0;
+}
+
+int orc_node_xyz(int64_t n, const double* lon, const double* lat, double* out) {
+    for (int64_t i = 0; i < n; ++i) {
+        double cl;
+        qxyz(lon[i], lat[i], out + 3 * i, out + 3 * i + 1, out + 3 * i + 2, &cl);
+    }
+    return 0;
+}

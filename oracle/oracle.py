@@ -1,0 +1,204 @@
+"""TEST INFRASTRUCTURE, NOT THE PRODUCT: ctypes driver of the CPU oracle
+(``oracle/kelp_oracle.c``), a C restatement of KELP's step path.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
+leg use this module, and only as the checker / the timed CPU baseline.  The
+functions mirror the reference's step API over its own array layout:
+``step(state, vel, mesh, dt, time_dir, scheme, ...)`` returns new arrays like
+KELP's ``rk2_step`` (``src/kelp/numerics/integrators.py:5611``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+
+
+class OMesh(C.Structure):
+    _fields_ = [("N", C.c_int64), ("E", C.c_int64), ("max_v", C.c_int), ("max_conn", C.c_int),
+                ("lon", C.c_void_p), ("lat", C.c_void_p), ("depth", C.c_void_p), ("xyz", C.c_void_p),
+                ("zlev", C.c_void_p), ("en", C.c_void_p), ("n2e", C.c_void_p), ("n2e_cnt", C.c_void_p),
+                ("gh_off", C.c_void_p), ("gh_ids", C.c_void_p),
+                ("cell", C.c_double), ("lon_min", C.c_double), ("lat_min", C.c_double), ("r_earth", C.c_double),
+                ("nx", C.c_int), ("ny", C.c_int), ("wrap", C.c_int), ("far_rows", C.c_int),
+                ("exact", C.c_int), ("K", C.c_int)]
+
+
+class OField(C.Structure):
+    _fields_ = [("ua", C.c_void_p), ("va", C.c_void_p), ("wa", C.c_void_p),
+                ("ub", C.c_void_p), ("vb", C.c_void_p), ("wb", C.c_void_p),
+                ("ut", C.c_void_p), ("vt", C.c_void_p), ("wt", C.c_void_p),
+                ("f32", C.c_int), ("alpha0", C.c_double), ("n", C.c_int64)]
+
+
+class OStep(C.Structure):
+    _fields_ = [("scheme", C.c_int), ("dims", C.c_int), ("w_code", C.c_int), ("kick", C.c_int),
+                ("dt", C.c_double), ("td", C.c_double), ("ak", C.c_double * 4),
+                ("kh_x", C.c_double), ("kh_y", C.c_double),
+                ("seed", C.c_uint64), ("real_id", C.c_uint64), ("step_i", C.c_uint64),
+                ("pid_offset", C.c_uint64)]
+
+
+_lib = None
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        vp, i64 = C.c_void_p, C.c_int64
+        L.orc_step.argtypes = [C.POINTER(OMesh), C.POINTER(OField), C.POINTER(OStep), i64,
+                               vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, i64]
+        L.orc_find_nearest.argtypes = [C.POINTER(OMesh), i64, vp, vp, vp]
+        L.orc_contain.argtypes = [C.POINTER(OMesh), i64, vp, vp, vp, vp]
+        L.orc_normals.argtypes = [i64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, vp]
+        L.orc_node_xyz.argtypes = [i64, vp, vp, vp]
+        L.orc_normal_pair.argtypes = [C.c_uint64] * 5 + [vp]
+        L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_get_threads.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def set_threads(n: int) -> None:
+    lib().orc_set_threads(int(n))
+
+
+def threads() -> int:
+    return int(lib().orc_get_threads())
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+class MeshView:
+    """The oracle's view of a mesh (keeps the converted arrays alive)."""
+
+    def __init__(self, mesh):
+        c = lambda a, t: np.ascontiguousarray(a, dtype=t)
+        self.lon = c(mesh.nodes_lon, np.float64)
+        self.lat = c(mesh.nodes_lat, np.float64)
+        self.depth = c(mesh.depth, np.float64)
+        self.xyz = c(mesh._node_xyz, np.float64)
+        self.en = c(mesh.elem_nodes, np.int32)
+        self.n2e = c(mesh.node_to_elems, np.int32)
+        self.cnt = c(mesh.node_to_elems_count, np.int32)
+        self.off = c(mesh._gh_offsets, np.int32)
+        self.ids = c(mesh._gh_node_ids, np.int32)
+        sig = np.asarray(getattr(mesh, "sigma", np.zeros(0)))
+        self.zl = c(np.abs(sig), np.float64) if sig.size else None
+        s = OMesh()
+        s.N, s.E = self.lon.size, self.en.shape[0]
+        s.max_v, s.max_conn = self.en.shape[1], self.n2e.shape[1]
+        s.lon, s.lat, s.depth, s.xyz = _p(self.lon), _p(self.lat), _p(self.depth), _p(self.xyz)
+        s.zlev = _p(self.zl)
+        s.en, s.n2e, s.n2e_cnt, s.gh_off, s.gh_ids = _p(self.en), _p(self.n2e), _p(self.cnt), _p(self.off), _p(self.ids)
+        s.cell, s.lon_min, s.lat_min = float(mesh._gh_cell_size), float(mesh._gh_lon_min), float(mesh._gh_lat_min)
+        s.r_earth = float(getattr(mesh, "r_earth", 6371000.0))
+        s.nx, s.ny, s.wrap, s.far_rows = int(mesh._gh_nx), int(mesh._gh_ny), int(bool(mesh._gh_wrap_lon)), int(mesh._gh_far_rows)
+        s.exact = int(bool((mesh.metadata or {}).get("exact_nearest", False)))
+        s.K = 0 if self.zl is None else int(self.zl.size)
+        self.s = s
+
+
+def _field_arrays(f, dtype):
+    u = np.ascontiguousarray(f.u, dtype=dtype)
+    v = np.ascontiguousarray(f.v, dtype=dtype)
+    w = None if getattr(f, "w", None) is None else np.ascontiguousarray(f.w, dtype=dtype)
+    return u, v, w
+
+
+def step(state, vel, mesh, dt, time_dir, scheme: str, *, vel_next=None, dt_to_next=None, w_interp="nearest",
+         diffusion=None, pid=None, release_step=None, global_step=-1, view=None):
+    """One step of every particle; returns a dict of new arrays
+    (lon, lat, z, status, nearest_node, failure_reason, u, v, w)."""
+    view = view or MeshView(mesh)
+    vel_a = getattr(vel, "vel_a", vel)
+    vel_b = getattr(vel, "vel_b", vel_next if vel_next is not None else vel_a)
+    alpha0 = float(getattr(vel, "alpha", 0.0))
+    target = vel_next if vel_next is not None else vel_a
+    flds = [vel_a, vel_b, target]
+    all32 = all(np.asarray(f.u).dtype == np.float32 and np.asarray(f.v).dtype == np.float32
+                and (f.w is None or np.asarray(f.w).dtype == np.float32) for f in flds)
+    dtype = np.float32 if all32 else np.float64
+    arrs = [_field_arrays(f, dtype) for f in flds]
+    of = OField()
+    (of.ua, of.va, of.wa), (of.ub, of.vb, of.wb), (of.ut, of.vt, of.wt) = [tuple(_p(x) for x in a) for a in arrs]
+    of.f32 = 1 if all32 else 0
+    of.alpha0 = alpha0
+    of.n = view.lon.size
+    is3d = arrs[0][2] is not None
+    os_ = OStep()
+    os_.scheme = {"euler": 0, "rk2": 1, "rk4": 2}[scheme]
+    os_.dims = 3 if is3d else 2
+    os_.w_code = 0 if w_interp == "nearest" else 1
+    cc = {"euler": (0.0,), "rk2": (0.0, 0.5), "rk4": (0.0, 0.5, 0.5, 1.0)}[scheme]
+    if vel_next is not None and scheme != "euler":
+        for k, c in enumerate(cc):
+            os_.ak[k] = float(c) * float(dt) / float(dt_to_next)
+    os_.dt, os_.td = float(dt), float(time_dir)
+    if diffusion is not None and not (float(diffusion.kh_x) == 0.0 and float(diffusion.kh_y) == 0.0):
+        os_.kick = 1
+        os_.kh_x, os_.kh_y = float(diffusion.kh_x), float(diffusion.kh_y)
+        os_.seed, os_.real_id, os_.step_i = int(diffusion.seed), int(diffusion.real_id), int(diffusion.step_i)
+        os_.pid_offset = int(getattr(diffusion, "pid_offset", 0))
+    P = state.lon.shape[0]
+    out = {"lon": np.array(state.lon, dtype=np.float64), "lat": np.array(state.lat, dtype=np.float64),
+           "z": np.array(state.z, dtype=np.float64), "status": np.array(state.status, dtype=np.int32),
+           "nearest_node": np.array(state.nearest_node, dtype=np.int32),
+           "failure_reason": (np.zeros(P, np.int8) if state.failure_reason is None
+                              else np.array(state.failure_reason, dtype=np.int8)),
+           "u": np.zeros(P), "v": np.zeros(P), "w": np.zeros(P)}
+    pid_a = None if pid is None else np.ascontiguousarray(pid, dtype=np.int64)
+    rs = None if release_step is None else np.ascontiguousarray(release_step, dtype=np.int32)
+    lib().orc_step(C.byref(view.s), C.byref(of), C.byref(os_), P,
+                   _p(out["lon"]), _p(out["lat"]), _p(out["z"]), _p(out["status"]), _p(out["nearest_node"]),
+                   _p(out["failure_reason"]), _p(out["u"]), _p(out["v"]), _p(out["w"]), _p(pid_a), _p(rs),
+                   int(global_step))
+    return out
+
+
+def find_nearest(mesh, lon, lat, view=None) -> np.ndarray:
+    view = view or MeshView(mesh)
+    lon = np.ascontiguousarray(lon, dtype=np.float64)
+    lat = np.ascontiguousarray(lat, dtype=np.float64)
+    out = np.empty(lon.size, np.int32)
+    lib().orc_find_nearest(C.byref(view.s), lon.size, _p(lon), _p(lat), _p(out))
+    return out
+
+
+def contain(mesh, lon, lat, nn, view=None) -> np.ndarray:
+    view = view or MeshView(mesh)
+    lon = np.ascontiguousarray(lon, dtype=np.float64)
+    lat = np.ascontiguousarray(lat, dtype=np.float64)
+    nn = np.ascontiguousarray(nn, dtype=np.int32)
+    out = np.empty(lon.size, np.int32)
+    lib().orc_contain(C.byref(view.s), lon.size, _p(lon), _p(lat), _p(nn), _p(out))
+    return out
+
+
+def normals(P, seed, real_id, step_i, pid_offset=0) -> np.ndarray:
+    g = np.empty((P, 2))
+    lib().orc_normals(P, seed, real_id, step_i, pid_offset, _p(g))
+    return g
+
+
+def node_xyz(lon, lat) -> np.ndarray:
+    lon = np.ascontiguousarray(lon, dtype=np.float64)
+    lat = np.ascontiguousarray(lat, dtype=np.float64)
+    out = np.empty((lon.size, 3))
+    lib().orc_node_xyz(lon.size, _p(lon), _p(lat), _p(out))
+    return out

@@ -1,0 +1,224 @@
+"""Generate the golden fixtures of tests/golden/ by running the REFERENCE.
+
+This script imports KELP itself (its ``src`` tree, path given by
+``KELP_REFERENCE_SRC``) and runs its own Numba step functions
+(``kelp.numerics.integrators.rk2_step`` / ``rk4_step`` / ``euler_step``), its
+``find_nearest_nodes`` and its counter RNG on small seeded synthetic inputs.
+The inputs (mesh arrays, the reference-built grid hash and unit-sphere node
+table, snapshots, particles) and the reference's outputs are written to
+``tests/golden/*.npz``.  The fixtures pin the CPU oracle and, through it, the
+CUDA kernels; nothing at test time imports the reference.
+
+    KELP_REFERENCE_SRC=<kelp checkout>/src python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.environ.get("KELP_REFERENCE_SRC", "/root/reference/src"))
+
+os.environ.setdefault("NUMBA_NUM_THREADS", "8")
+
+from kelp.core.io import LazyLerpField as RLazy, VelocityField as RVel  # noqa: E402
+from kelp.core.mesh import (Mesh as RMesh, build_node_to_elems as r_n2e, build_search,  # noqa: E402
+                            find_nearest_nodes, set_exact_nearest, set_grid_hash_cell)
+from kelp.core.particles import ParticleState as RState, ParticleStatus  # noqa: E402
+from kelp.numerics import integrators as RI  # noqa: E402
+from kelp.numerics.diffusion import DiffusionStepArgs as RDiff, _normal_pair  # noqa: E402
+
+from kelp_b200 import synthetic as S  # noqa: E402  (input generators only)
+
+
+def ref_mesh(m, cell=0.0, sigma=None):
+    en = np.ascontiguousarray(m.elem_nodes, dtype=np.int32)
+    n2e, cnt = r_n2e(m.n_nodes, en)
+    rm = RMesh(name="golden", nodes_lon=np.array(m.nodes_lon), nodes_lat=np.array(m.nodes_lat),
+               depth=np.array(m.depth), elem_nodes=en,
+               elem_center_lon=np.array(m.elem_center_lon), elem_center_lat=np.array(m.elem_center_lat),
+               node_to_elems=n2e, node_to_elems_count=cnt,
+               sigma=np.zeros(0) if sigma is None else np.asarray(sigma, dtype=np.float64))
+    build_search(rm)
+    if cell > 0:
+        set_grid_hash_cell(rm, cell)
+    set_exact_nearest(rm, True)
+    return rm
+
+
+def mesh_record(rm):
+    return {"nodes_lon": rm.nodes_lon, "nodes_lat": rm.nodes_lat, "depth": rm.depth,
+            "elem_nodes": rm.elem_nodes, "node_to_elems": rm.node_to_elems,
+            "node_to_elems_count": rm.node_to_elems_count, "sigma": rm.sigma,
+            "gh_offsets": rm._gh_offsets, "gh_node_ids": rm._gh_node_ids, "node_xyz": rm._node_xyz,
+            "gh_geom": np.array([rm._gh_cell_size, rm._gh_lon_min, rm._gh_lat_min, rm._gh_nx, rm._gh_ny,
+                                 int(rm._gh_wrap_lon), rm._gh_far_rows, rm.r_earth], dtype=np.float64)}
+
+
+def ref_fields(snaps):
+    return [RVel(u=s.u, v=s.v, w=s.w, eta=np.zeros(s.u.shape[-1]), uv_layout="node",
+                 uv_vertical="layer") for s in snaps]
+
+
+def payload(fields, t, T):
+    """_build_vel_payload (tracking.py:3136-3206), forward, snapshots T apart."""
+    ia = int(np.floor(t / T + 1e-9))
+    ta = ia * T
+    a, b = fields[ia], fields[ia + 1]
+    alpha = (t - ta) / T
+    vel = a if abs(alpha) < 1e-12 else (b if abs(alpha - 1.0) < 1e-12 else RLazy(a, b, alpha))
+    return vel, b, (ta + T) - t, ia, alpha
+
+
+def run_case(rm, fields, lon, lat, z, status, scheme, dt, T, n_steps, *, time_dir=1.0, w_interp="nearest",
+             kh=None, seed=7, real_id=0, pid_offset=0, record=(1,)):
+    fn = {"rk2": RI.rk2_step, "rk4": RI.rk4_step, "euler": RI.euler_step}[scheme]
+    P = lon.size
+    st = RState(lon=lon.copy(), lat=lat.copy(), z=z.copy(), status=status.copy(),
+                nearest_node=np.full(P, -1, np.int32), failure_reason=np.zeros(P, np.int8))
+    out = {}
+    sched = []
+    for k in range(n_steps):
+        t = k * dt
+        vel, vnext, dtn, ia, alpha = payload(fields, t, T)
+        kw = dict(uv_interp="barycentric", w_interp=w_interp, vel_next=vnext, dt_to_next=dtn)
+        if kh is not None:
+            kw["diffusion"] = RDiff(scheme="uniform", kh_x=kh[0], kh_y=kh[1], seed=seed, real_id=real_id,
+                                    step_i=k, pid_offset=pid_offset)
+        sched.append([ia, alpha, dtn])
+        st = fn(st, vel, rm, dt, time_dir, **kw)
+        if (k + 1) in record or k + 1 == n_steps:
+            tag = f"s{k + 1}"
+            for name in ("lon", "lat", "z", "status", "nearest_node", "failure_reason", "u", "v"):
+                out[f"{tag}_{name}"] = np.asarray(getattr(st, name))
+            if st.w is not None:
+                out[f"{tag}_w"] = np.asarray(st.w)
+    out["schedule"] = np.array(sched, dtype=np.float64)
+    out["params"] = np.array([dt, T, n_steps, time_dir, -1 if kh is None else kh[0], -1 if kh is None else kh[1],
+                              seed, real_id, pid_offset], dtype=np.float64)
+    return out
+
+
+def particles(m, P, seed, z=False, n_off=0, n_dead=0):
+    lon, lat, zz = S.release_uniform(m, P, seed=seed, depth_uniform=z)
+    status = np.full(P, int(ParticleStatus.ALIVE), np.int32)
+    rng = np.random.default_rng(seed + 100)
+    if n_off:
+        idx = rng.choice(P, n_off, replace=False)
+        lat[idx] = rng.uniform(-89, 89, n_off)          # many land up on land / outside
+        lon[idx] = rng.uniform(-180, 180, n_off)
+    if n_dead:
+        idx = rng.choice(P, n_dead, replace=False)
+        status[idx[: n_dead // 2]] = int(ParticleStatus.OUTSIDE)
+        status[idx[n_dead // 2:]] = int(ParticleStatus.NOT_RELEASED)
+    return lon, lat, zz, status
+
+
+def save(name, mesh_rec, snaps, cases, parts):
+    d = {}
+    for k, v in mesh_rec.items():
+        d[f"mesh_{k}"] = v
+    for i, s in enumerate(snaps):
+        d[f"snap{i}_u"] = s.u
+        d[f"snap{i}_v"] = s.v
+        if s.w is not None:
+            d[f"snap{i}_w"] = s.w
+    for k, v in parts.items():
+        d[f"p_{k}"] = v
+    for cname, c in cases.items():
+        for k, v in c.items():
+            d[f"{cname}__{k}"] = v
+    path = os.path.join(HERE, f"{name}.npz")
+    np.savez_compressed(path, **d)
+    print(name, os.path.getsize(path) // 1024, "KB", sorted(cases))
+
+
+def main():
+    T = 86400.0
+    # --- global band (seam wrap), jitter, land mask, triangles --------------
+    m = S.lattice_mesh(3.0, 72.0, jitter=0.2, land_frac=0.3)
+    rm = ref_mesh(m)
+    snaps = S.gyre_snapshots(m, 4, amp=1.5)
+    rf = ref_fields(snaps)
+    lon, lat, z, status = particles(m, 1500, 11, n_off=60, n_dead=40)
+    cases = {}
+    cases["rk2"] = run_case(rm, rf, lon, lat, z, status, "rk2", 21600.0, T, 12)
+    cases["rk4"] = run_case(rm, rf, lon, lat, z, status, "rk4", 21600.0, T, 12)
+    cases["euler"] = run_case(rm, rf, lon, lat, z, status, "euler", 21600.0, T, 12)
+    cases["rk2_bwd"] = run_case(rm, rf, lon, lat, z, status, "rk2", 21600.0, T, 12, time_dir=-1.0)
+    cases["rk2_kick"] = run_case(rm, rf, lon, lat, z, status, "rk2", 21600.0, T, 12, kh=(5.0e4, 5.0e4),
+                                 seed=7, real_id=3, pid_offset=1000)
+    cases["rk4_kick_aniso"] = run_case(rm, rf, lon, lat, z, status, "rk4", 21600.0, T, 8, kh=(8.0e4, 2.0e4),
+                                       seed=11, real_id=0)
+    cases["rk2_dt4800"] = run_case(rm, rf, lon, lat, z, status, "rk2", 4800.0, T, 20)
+    nn_q = find_nearest_nodes(rm, lon, lat)
+    save("golden_band", mesh_record(rm), snaps, cases,
+         {"lon": lon, "lat": lat, "z": z, "status": status, "nearest_exact": nn_q})
+
+    # --- regional mixed tri/quad mesh (no wrap), float64 fields -------------
+    m = S.lattice_mesh(1.0, 15.0, lon_min=-20.0, lon_max=20.0, jitter=0.15, land_frac=0.2, quad_frac=0.3)
+    rm = ref_mesh(m)
+    snaps = S.gyre_snapshots(m, 4, amp=2.0, dtype=np.float64)
+    rf = ref_fields(snaps)
+    lon, lat, z, status = particles(m, 1200, 12, n_dead=20)
+    cases = {"rk2": run_case(rm, rf, lon, lat, z, status, "rk2", 10800.0, T, 16),
+             "rk4": run_case(rm, rf, lon, lat, z, status, "rk4", 10800.0, T, 16),
+             "euler": run_case(rm, rf, lon, lat, z, status, "euler", 10800.0, T, 16),
+             "rk2_kick": run_case(rm, rf, lon, lat, z, status, "rk2", 10800.0, T, 16, kh=(2.0e4, 2.0e4))}
+    q_lon = np.random.default_rng(5).uniform(-60, 60, 3000)
+    q_lat = np.random.default_rng(6).uniform(-60, 60, 3000)
+    save("golden_quad", mesh_record(rm), snaps, cases,
+         {"lon": lon, "lat": lat, "z": z, "status": status, "q_lon": q_lon, "q_lat": q_lat,
+          "q_nearest": find_nearest_nodes(rm, q_lon, q_lat)})
+
+    # --- polar cap: anisotropic cells force the widened exact search --------
+    m = S.lattice_mesh(2.0, 88.0, jitter=0.1, land_frac=0.0, cell_size=0.5)
+    rm = ref_mesh(m, cell=0.5)
+    q_lon = np.random.default_rng(7).uniform(-180, 180, 4000)
+    q_lat = np.concatenate([np.random.default_rng(8).uniform(70, 89.9, 2000),
+                            np.random.default_rng(9).uniform(-89.9, 89.9, 2000)])
+    snaps = S.gyre_snapshots(m, 3, amp=1.0)
+    rf = ref_fields(snaps)
+    lon = np.random.default_rng(10).uniform(-180, 180, 800)
+    lat = np.random.default_rng(11).uniform(60, 87.5, 800)
+    z = np.zeros(800)
+    status = np.full(800, 1, np.int32)
+    cases = {"rk2": run_case(rm, rf, lon, lat, z, status, "rk2", 21600.0, T, 6)}
+    save("golden_polar", mesh_record(rm), snaps, cases,
+         {"lon": lon, "lat": lat, "z": z, "status": status, "q_lon": q_lon, "q_lat": q_lat,
+          "q_nearest": find_nearest_nodes(rm, q_lon, q_lat)})
+
+    # --- 3-D z-level band: layer u/v, W nearest / barycentric, kick ---------
+    zl = S.stretched_levels(12, 5.0, 4000.0)
+    m = S.lattice_mesh(3.0, 60.0, jitter=0.2, land_frac=0.25,
+                       depth=lambda lo, la: S.smooth_bathymetry(lo, la, 30.0, 4000.0), sigma=zl)
+    rm = ref_mesh(m, sigma=zl)
+    snaps = S.gyre_snapshots(m, 4, amp=1.5, z_levels=zl, decay=800.0, w_scale=2e-3)
+    rf = ref_fields(snaps)
+    lon, lat, z, status = particles(m, 1200, 13, z=True, n_dead=20)
+    cases = {"rk2_wnear": run_case(rm, rf, lon, lat, z, status, "rk2", 21600.0, T, 12, w_interp="nearest"),
+             "rk2_wbary": run_case(rm, rf, lon, lat, z, status, "rk2", 21600.0, T, 12, w_interp="barycentric"),
+             "rk2_wbary_kick": run_case(rm, rf, lon, lat, z, status, "rk2", 21600.0, T, 12,
+                                        w_interp="barycentric", kh=(3.0e4, 3.0e4), seed=5)}
+    save("golden_3d", mesh_record(rm), snaps, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
+
+    # --- counter RNG: normal pairs of the reference for a key grid ----------
+    keys = []
+    vals = []
+    rng = np.random.default_rng(0)
+    for _ in range(4000):
+        k = (int(rng.integers(0, 2**63)), int(rng.integers(0, 64)), int(rng.integers(0, 2**40)),
+             int(rng.integers(0, 100000)), int(rng.integers(0, 2)))
+        keys.append(k)
+        vals.append(_normal_pair(*(np.uint64(x) for x in k)))
+    np.savez_compressed(os.path.join(HERE, "golden_rng.npz"), keys=np.array(keys, dtype=np.uint64),
+                        normals=np.array(vals, dtype=np.float64))
+    print("golden_rng")
+
+
+if __name__ == "__main__":
+    main()

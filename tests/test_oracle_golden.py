@@ -1,0 +1,86 @@
+"""The CPU oracle against the reference's own outputs (golden fixtures).
+
+Pins ``oracle/kelp_oracle.c`` before it is trusted as the checker of the CUDA
+kernels.  Integer outputs (status, nearest node, failure reason) must match
+bit for bit.  Positions and velocities of the fused reference kernels (2-D
+RK2/RK4, 3-D RK2) match bit for bit too: both sides evaluate the same
+expressions with the C library's math and no contraction.  The unfused
+reference paths (Euler) evaluate their displacement metric with numpy's SIMD
+``cos``, so there the tolerance is 1e-12 degrees.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from kelp_b200.diffusion import DiffusionStepArgs
+
+CASES = [("golden_band", c) for c in ("rk2", "rk4", "euler", "rk2_bwd", "rk2_kick", "rk4_kick_aniso", "rk2_dt4800")]
+CASES += [("golden_quad", c) for c in ("rk2", "rk4", "euler", "rk2_kick")]
+CASES += [("golden_polar", "rk2")]
+CASES += [("golden_3d", c) for c in ("rk2_wnear", "rk2_wbary", "rk2_wbary_kick")]
+
+
+def replay_oracle(g, cname):
+    c = g.case(cname)
+    dt, T, n_steps, td, khx, khy, seed, real_id, pid_off = c["params"]
+    scheme = cname.split("_")[0]
+    w_interp = "barycentric" if "wbary" in cname else "nearest"
+    st = g.particles()
+    view = O.MeshView(g.mesh)
+    snaps = {}
+    for k in range(int(n_steps)):
+        vel, vnext, dtn = g.payload(c["schedule"][k], T)
+        diff = None
+        if khx >= 0:
+            diff = DiffusionStepArgs("uniform", khx, khy, int(seed), int(real_id), k, pid_offset=int(pid_off))
+        out = O.step(st, vel, g.mesh, dt, td, scheme, vel_next=vnext, dt_to_next=dtn, w_interp=w_interp,
+                     diffusion=diff, view=view)
+        st = st.replace(lon=out["lon"], lat=out["lat"], z=out["z"], status=out["status"],
+                        nearest_node=out["nearest_node"], failure_reason=out["failure_reason"],
+                        u=out["u"], v=out["v"], w=out["w"])
+        if f"s{k + 1}_lon" in c:
+            snaps[k + 1] = out
+    return c, snaps
+
+
+@pytest.mark.parametrize("fixture,cname", CASES)
+def test_oracle_matches_reference(golden, fixture, cname):
+    g = golden(fixture)
+    c, snaps = replay_oracle(g, cname)
+    exact_float = not cname.startswith("euler")
+    for k, out in snaps.items():
+        tag = f"s{k}_"
+        for name in ("status", "nearest_node", "failure_reason"):
+            np.testing.assert_array_equal(out[name], c[tag + name], err_msg=f"{cname} step {k} {name}")
+        for name in ("lon", "lat", "z", "u", "v", "w"):
+            if tag + name not in c:
+                continue
+            if exact_float:
+                np.testing.assert_array_equal(out[name], c[tag + name], err_msg=f"{cname} step {k} {name}")
+            else:
+                np.testing.assert_allclose(out[name], c[tag + name], rtol=0, atol=1e-12,
+                                           err_msg=f"{cname} step {k} {name}")
+
+
+@pytest.mark.parametrize("fixture", ["golden_quad", "golden_polar"])
+def test_oracle_exact_nearest(golden, fixture):
+    g = golden(fixture)
+    got = O.find_nearest(g.mesh, g.d["p_q_lon"], g.d["p_q_lat"])
+    np.testing.assert_array_equal(got, g.d["p_q_nearest"])
+
+
+def test_oracle_rng_normals():
+    import os
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden_rng.npz"))
+    keys, want = d["keys"], d["normals"]
+    got = np.empty_like(want)
+    for i, k in enumerate(keys):
+        g = np.empty(2)
+        O.lib().orc_normal_pair(*(int(x) for x in k), g.ctypes.data)
+        got[i] = g
+    np.testing.assert_array_equal(got, want)
+
+
+def test_oracle_node_xyz(golden):
+    g = golden("golden_band")
+    np.testing.assert_array_equal(O.node_xyz(g.mesh.nodes_lon, g.mesh.nodes_lat), g.mesh._node_xyz)
