@@ -1,0 +1,322 @@
+"""Benchmark of the B200 time-stepping path: particle-steps/s on one node.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c1]
+                    [--impl b200|reference]
+
+One step = one pass of the step kernel over every particle of the workload
+(inputs resident in HBM, L2 evicted between timed steps, CUDA events on the
+library's stream).  Under torchrun (N > 1) every rank runs its own shard of
+the same per-GPU size (weak scaling: particles are independent, nothing is
+exchanged); the time is the maximum over ranks.  Rank 0 prints one JSON line.
+
+``--impl reference`` times the reference algorithm's CPU implementation on
+this host's cores (the oracle port in oracle/, all host threads) on the same
+workload, metric and unit.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s on 1 B200, mixed vs FP64 form at ≤1 m p99 error; HBM GB/s vs peak"
+UNIT = "particle-steps/s"
+PUBLISHED = {}   # workload -> the reference's published figure for this exact metric
+
+
+def env_rank():
+    r = int(os.environ.get("RANK", "0"))
+    w = int(os.environ.get("WORLD_SIZE", "1"))
+    lr = int(os.environ.get("LOCAL_RANK", "0"))
+    return r, w, lr
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+
+    def __init__(self, device: int):
+        self.lines = []
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append((time.time(), line.strip()))
+
+    def mark(self):
+        return time.time()
+
+    def stop(self, t0, t1):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = [l for (t, l) in self.lines if t0 - 0.25 <= t <= t1 + 0.25] or [l for _, l in self.lines]
+        sm, mx, reasons = [], [], set()
+        for l in rows:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(self.NAMES, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(wl, seconds: float = 8.0):
+    """The oracle port on this host's cores over a bounded sample of the
+    workload (all its particles, as many steps as fit in ~``seconds``)."""
+    from oracle import oracle as O
+    from kelp_b200.particles import make_state
+    from kelp_b200.fields import LazyLerpField
+    view = O.MeshView(wl.mesh)
+    st = make_state(wl.lon, wl.lat, wl.z)
+    st = st.replace(failure_reason=np.zeros(wl.P, np.int8))
+    done, t_used, k = 0, 0.0, 0
+    while t_used < seconds and k < wl.n_steps_run:
+        ia, ib, alpha0, dtn = wl.bracket(k)
+        a, b = wl.snaps[ia], wl.snaps[ib]
+        vel = a if alpha0 == 0.0 else LazyLerpField(a, b, alpha0)
+        t0 = time.perf_counter()
+        out = O.step(st, vel, wl.mesh, wl.dt, 1.0, wl.scheme, vel_next=b, dt_to_next=dtn, w_interp=wl.w_interp,
+                     view=view)
+        t_used += time.perf_counter() - t0
+        st = st.replace(lon=out["lon"], lat=out["lat"], z=out["z"], status=out["status"],
+                        nearest_node=out["nearest_node"], failure_reason=out["failure_reason"])
+        done += wl.P
+        k += 1
+    return {"value": done / t_used, "unit": UNIT, "cores": O.threads(), "kind": "port",
+            "sample": f"{k} steps x {wl.P} particles of {wl.name} (oracle C port, {O.threads()} threads)"}
+
+
+def run_reference(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return 0
+    from kelp_b200 import workloads
+    wl = workloads.WORKLOADS[args.workload]()
+    from oracle import oracle as O
+    from kelp_b200.particles import make_state
+    from kelp_b200.fields import LazyLerpField
+    view = O.MeshView(wl.mesh)
+    st = make_state(wl.lon, wl.lat, wl.z)
+    st = st.replace(failure_reason=np.zeros(wl.P, np.int8))
+    times = []
+    for k in range(args.warmup + args.steps):
+        ia, ib, alpha0, dtn = wl.bracket(k)
+        a, b = wl.snaps[ia], wl.snaps[ib]
+        vel = a if alpha0 == 0.0 else LazyLerpField(a, b, alpha0)
+        t0 = time.perf_counter()
+        out = O.step(st, vel, wl.mesh, wl.dt, 1.0, wl.scheme, vel_next=b, dt_to_next=dtn, w_interp=wl.w_interp,
+                     view=view)
+        dt = time.perf_counter() - t0
+        st = st.replace(lon=out["lon"], lat=out["lat"], z=out["z"], status=out["status"],
+                        nearest_node=out["nearest_node"], failure_reason=out["failure_reason"])
+        if k >= args.warmup:
+            times.append(dt)
+    total = sum(times)
+    value = wl.P * args.steps / total
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": wl.name, **wl.description},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": O.threads(), "kind": "port",
+                             "sample": f"{args.steps} timed steps x {wl.P} particles (oracle C port)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def load_traffic(workload: str):
+    """Per-launch DRAM bytes of the step kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "traffic.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        f = line.split()
+        if len(f) >= 3 and f[0] == workload:
+            return float(f[2])
+    return None
+
+
+def run_b200(args):
+    rank, world, local = env_rank()
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+    from kelp_b200 import workloads, roofline
+    from kelp_b200 import integrators as KI
+    from kelp_b200.device import DeviceContext, set_default_device, default_context, pinned_empty
+    from kelp_b200.fields import LazyLerpField
+    from kelp_b200.particles import ParticleState
+
+    wl = workloads.WORKLOADS[args.workload]()
+    set_default_device(local)
+    ctx = default_context()
+    ctx.ensure_mesh(wl.mesh)
+    slots = ctx.slots_for(wl.snaps)
+    P = wl.P
+    pid = np.arange(P, dtype=np.int64) + rank * P
+    status0 = np.full(P, 1, np.int32)
+
+    def upload():
+        ctx.upload_particles(wl.lon, wl.lat, wl.z, status0, np.full(P, -1, np.int32), np.zeros(P, np.int8), pid)
+
+    upload()
+    for k in range(args.warmup):
+        ctx.step(wl.step_args(k, slots))
+    ctx.synchronize()
+    if ctx.device_errors():
+        raise RuntimeError("device-side iteration cap hit during warm-up")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        ctx.synchronize()
+
+    sampler = ClockSampler(local)
+    time.sleep(0.6)
+    barrier()
+    t_wall0 = time.time()
+    kernel_ms = []
+    for k in range(args.warmup, args.warmup + args.steps):
+        ctx.l2_flush()
+        ctx.record(0)
+        ctx.step(wl.step_args(k, slots))
+        ctx.record(1)
+        kernel_ms.append(ctx.elapsed_ms(0, 1))
+    barrier()
+    t_wall1 = time.time()
+    clocks = sampler.stop(t_wall0, t_wall1)
+    total_ms = float(sum(kernel_ms))
+    if dist is not None:
+        import torch
+        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    errs = ctx.device_errors()
+
+    # end to end through the public step API: host state in page-locked memory
+    st_h = {}
+    for name, dt_, src in (("lon", np.float64, wl.lon), ("lat", np.float64, wl.lat), ("z", np.float64, wl.z),
+                           ("status", np.int32, status0), ("nearest_node", np.int32, np.full(P, -1, np.int32)),
+                           ("failure_reason", np.int8, np.zeros(P, np.int8))):
+        a = pinned_empty((P,), dt_)
+        a[:] = src
+        st_h[name] = a
+    state = ParticleState(**st_h)
+    step_fn = KI.get_integrator(wl.scheme)
+    e2e_steps = max(1, min(args.steps, 50))
+    barrier()
+    ctx.record(2)
+    for k in range(e2e_steps):
+        ia, ib, alpha0, dtn = wl.bracket(k)
+        a, b = wl.snaps[ia], wl.snaps[ib]
+        vel = a if alpha0 == 0.0 else LazyLerpField(a, b, alpha0)
+        state = step_fn(state, vel, wl.mesh, wl.dt, 1.0, uv_interp="barycentric", w_interp=wl.w_interp,
+                        vel_next=b, dt_to_next=dtn)
+        for name in ("lon", "lat", "z", "status", "nearest_node", "failure_reason"):
+            st_h[name][:] = getattr(state, name)
+        state = ParticleState(**st_h)
+    ctx.record(3)
+    e2e_ms = ctx.elapsed_ms(2, 3)
+    if dist is not None:
+        import torch
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    h2d = P * (8 + 8 + 8 + 4 + 4 + 1)
+    d2h = P * (8 * 6 + 4 + 4 + 1)
+
+    line = None
+    if rank == 0:
+        fbytes = 4 if np.asarray(wl.snaps[0].u).dtype == np.float32 else 8
+        bpp = roofline.bytes_per_particle_step(wl.mesh, wl.scheme, wl.dims, fbytes, kick=wl.kh is not None,
+                                               w_code=0 if wl.w_interp == "nearest" else 1)
+        avg_launch_s = (sum(kernel_ms) / len(kernel_ms)) * 1e-3
+        achieved = bpp["total"] * P / avg_launch_s / 1e9
+        peak, kind = peaks()
+        traffic = load_traffic(wl.name)
+        value = world * P * args.steps / (total_ms * 1e-3)
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": (value / PUBLISHED[wl.name]) if wl.name in PUBLISHED else None,
+                "dtype": "f64", "data": "synthetic",
+                "config": {"workload": wl.name, **wl.description, "particles_per_gpu": P,
+                           "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}"},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "peak_kind": kind,
+                             "traffic": traffic, "algorithmic_bytes_per_particle_step": bpp["total"]},
+                "e2e": {"value": world * P * e2e_steps / (e2e_ms * 1e-3), "unit": UNIT,
+                        "h2d_bytes_per_step": h2d * world, "d2h_bytes_per_step": d2h * world,
+                        "steps": e2e_steps},
+                "gpu_launches": args.steps, "clocks": clocks, "device_errors": errs}
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(wl)
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=240)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--workload", default="c1")
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

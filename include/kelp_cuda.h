@@ -24,6 +24,7 @@
  *                         (src/kelp/core/particles.py:153)
  *   kc_node_xyz_fill   <- core.mesh._node_xyz_fill (src/kelp/core/mesh.py:712)
  *   kc_find_nearest    <- core.mesh.find_nearest_nodes (src/kelp/core/mesh.py:1896)
+ *   kc_rng_normals     <- numerics.diffusion._normal_pair (src/kelp/numerics/diffusion.py:233)
  */
 #ifndef KELP_CUDA_H
 #define KELP_CUDA_H
@@ -123,6 +124,13 @@ int kc_run(kc_ctx* ctx, const kc_step_args* steps, int n_steps);
 /* Batch exact nearest node of P query points (host arrays). */
 int kc_find_nearest(kc_ctx* ctx, long long P, const double* lon, const double* lat, int* out);
 
+/* Counter-RNG normal pairs of the diffusion kick, drawn on the device for
+ * particle ids pid_offset .. pid_offset + P - 1 (out: (P, 2)).  The kick
+ * kernel draws exactly these numbers; this entry point exposes them for
+ * checking (src/kelp/numerics/diffusion.py:233-249 _normal_pair). */
+int kc_rng_normals(kc_ctx* ctx, long long P, unsigned long long seed, unsigned long long real_id,
+                   unsigned long long step_i, unsigned long long pid_offset, double* out);
+
 /* Device error word (bitmask of iteration caps hit since the last call). */
 int kc_device_errors(kc_ctx* ctx, int* word);
 
@@ -130,6 +138,10 @@ int kc_device_errors(kc_ctx* ctx, int* word);
  * elapsed milliseconds between two recorded events. */
 int kc_event_record(kc_ctx* ctx, int slot);
 int kc_event_elapsed(kc_ctx* ctx, int slot_a, int slot_b, float* ms);
+
+/* Evict the L2 cache between timed steps: writes a library-owned buffer of
+ * `bytes` (>= the 126 MB L2) on the context's stream. */
+int kc_l2_flush(kc_ctx* ctx, long long bytes);
 
 /* Page-locked host buffers for the end-to-end path. */
 int kc_host_alloc(long long bytes, void** out);

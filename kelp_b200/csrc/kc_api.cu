@@ -60,6 +60,10 @@ struct kc_ctx {
     int* qout = nullptr;
     long long qcap = 0;
     cudaEvent_t ev[kEvents] = {};
+    // L2 eviction buffer of kc_l2_flush
+    char* flush = nullptr;
+    long long flush_cap = 0;
+    unsigned flush_val = 0;
 };
 
 namespace {
@@ -135,6 +139,16 @@ __global__ void __launch_bounds__(kBlock) k_nearest(kc::DMesh m, const double* q
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P) return;
     out[i] = kc::site_anchor(m, q[i], q[P + i]);
+}
+
+__global__ void __launch_bounds__(kBlock) k_normals(long long P, unsigned long long seed, unsigned long long real_id,
+                                                    unsigned long long step, unsigned long long pid0, double* out) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P) return;
+    double g1, g2;
+    kc::normal_pair(seed, real_id, (unsigned long long)i + pid0, step, 0ull, g1, g2);
+    out[2 * i] = g1;
+    out[2 * i + 1] = g2;
 }
 
 unsigned grid_for(long long n) { return (unsigned)((n + kBlock - 1) / kBlock); }
@@ -252,7 +266,7 @@ void kc_destroy(kc_ctx* c) {
     free_mesh(c);
     free_particles(c);
     for (auto& s : c->slots) { dfree(s.u); dfree(s.v); dfree(s.w); }
-    dfree(c->q); dfree(c->qout); dfree(c->d_err);
+    dfree(c->q); dfree(c->qout); dfree(c->d_err); dfree(c->flush);
     for (int k = 0; k < kEvents; ++k) if (c->ev[k]) cudaEventDestroy(c->ev[k]);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -481,6 +495,23 @@ int kc_find_nearest(kc_ctx* c, long long P, const double* lon, const double* lat
     return KC_OK;
 }
 
+int kc_rng_normals(kc_ctx* c, long long P, unsigned long long seed, unsigned long long real_id,
+                   unsigned long long step_i, unsigned long long pid_offset, double* out) {
+    if (!c) return KC_ERR_ARG;
+    if (P < 0 || (P > 0 && !out)) return fail(c, KC_ERR_ARG, "kc_rng_normals: arrays");
+    if (P == 0) return KC_OK;
+    KC_CUDA(c, cudaSetDevice(c->device));
+    double* d = nullptr;
+    KC_CUDA(c, cudaMallocAsync((void**)&d, (size_t)P * 16, c->stream));
+    k_normals<<<grid_for(P), kBlock, 0, c->stream>>>(P, seed, real_id, step_i, pid_offset, d);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, (size_t)P * 16, cudaMemcpyDeviceToHost, c->stream);
+    cudaFreeAsync(d, c->stream);
+    if (e != cudaSuccess) return fail(c, KC_ERR_CUDA, std::string("kc_rng_normals: ") + cudaGetErrorString(e));
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KC_OK;
+}
+
 int kc_device_errors(kc_ctx* c, int* word) {
     if (!c || !word) return KC_ERR_ARG;
     KC_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -499,6 +530,19 @@ int kc_event_elapsed(kc_ctx* c, int a, int b, float* ms) {
     if (!c || !ms || a < 0 || b < 0 || a >= kEvents || b >= kEvents) return KC_ERR_ARG;
     KC_CUDA(c, cudaEventSynchronize(c->ev[b]));
     KC_CUDA(c, cudaEventElapsedTime(ms, c->ev[a], c->ev[b]));
+    return KC_OK;
+}
+
+int kc_l2_flush(kc_ctx* c, long long bytes) {
+    if (!c || bytes <= 0) return KC_ERR_ARG;
+    KC_CUDA(c, cudaSetDevice(c->device));
+    if (bytes > c->flush_cap) {
+        KC_CUDA(c, cudaStreamSynchronize(c->stream));
+        dfree(c->flush);
+        KC_CUDA(c, cudaMalloc((void**)&c->flush, (size_t)bytes));
+        c->flush_cap = bytes;
+    }
+    KC_CUDA(c, cudaMemsetAsync(c->flush, (int)(++c->flush_val & 0xff), (size_t)bytes, c->stream));
     return KC_OK;
 }
 

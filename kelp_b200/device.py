@@ -216,10 +216,19 @@ class DeviceContext:
                   "kc_find_nearest")
         return out
 
+    def rng_normals(self, P, seed, real_id, step_i, pid_offset=0) -> np.ndarray:
+        out = np.empty((int(P), 2))
+        self._chk(N.lib().kc_rng_normals(self._ctx, int(P), int(seed), int(real_id), int(step_i), int(pid_offset),
+                                         N.ptr(out)), "kc_rng_normals")
+        return out
+
     def device_errors(self) -> int:
         w = C.c_int(0)
         self._chk(N.lib().kc_device_errors(self._ctx, C.byref(w)), "kc_device_errors")
         return int(w.value)
+
+    def l2_flush(self, nbytes: int = 256 << 20) -> None:
+        self._chk(N.lib().kc_l2_flush(self._ctx, int(nbytes)), "kc_l2_flush")
 
     def record(self, slot: int) -> None:
         self._chk(N.lib().kc_event_record(self._ctx, slot), "kc_event_record")
@@ -230,12 +239,40 @@ class DeviceContext:
         return float(ms.value)
 
 
+def pinned_empty(shape, dtype) -> np.ndarray:
+    """A numpy array in page-locked host memory (freed when the array dies)."""
+    dtype = np.dtype(dtype)
+    n = int(np.prod(shape)) * dtype.itemsize
+    p = C.c_void_p()
+    rc = N.lib().kc_host_alloc(max(n, 1), C.byref(p))
+    if rc:
+        raise N.KcError(rc, "kc_host_alloc")
+    buf = (C.c_char * max(n, 1)).from_address(p.value)
+    arr = np.frombuffer(buf, dtype=dtype, count=int(np.prod(shape))).reshape(shape)
+    import weakref
+    weakref.finalize(buf, N.lib().kc_host_free, p)
+    return arr
+
+
 _default: Optional[DeviceContext] = None
 
 
+_default_device = 0
+
+
+def set_default_device(device: int) -> None:
+    """Device of the process-wide context (one process per GPU: its local rank)."""
+    global _default_device, _default
+    if _default is not None and _default.device != device:
+        _default.close()
+        _default = None
+    _default_device = int(device)
+
+
 def default_context() -> DeviceContext:
-    """The process-wide context on CUDA device 0 (created on first use)."""
+    """The process-wide context (device 0 unless set_default_device was called),
+    created on first use."""
     global _default
     if _default is None:
-        _default = DeviceContext(0)
+        _default = DeviceContext(_default_device)
     return _default
