@@ -102,30 +102,52 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(wl, seconds: float = 8.0):
-    """The oracle port on this host's cores over a bounded sample of the
-    workload (all its particles, as many steps as fit in ~``seconds``)."""
+def _oracle_run(wl, n_particles: int, step_iter, view=None):
+    """Oracle steps over the first ``n_particles`` particles of the workload
+    (a uniform random sample: releases are seeded uniform); yields seconds."""
     from oracle import oracle as O
     from kelp_b200.particles import make_state
     from kelp_b200.fields import LazyLerpField
-    view = O.MeshView(wl.mesh)
-    st = make_state(wl.lon, wl.lat, wl.z)
-    st = st.replace(failure_reason=np.zeros(wl.P, np.int8))
-    done, t_used, k = 0, 0.0, 0
-    while t_used < seconds and k < wl.n_steps_run:
+    from kelp_b200.diffusion import DiffusionStepArgs
+    view = view or O.MeshView(wl.mesh)
+    n = min(n_particles, wl.P)
+    st = make_state(wl.lon[:n], wl.lat[:n], wl.z[:n])
+    st = st.replace(failure_reason=np.zeros(n, np.int8))
+    for k in step_iter:
         ia, ib, alpha0, dtn = wl.bracket(k)
         a, b = wl.snaps[ia], wl.snaps[ib]
         vel = a if alpha0 == 0.0 else LazyLerpField(a, b, alpha0)
+        diff = None if wl.kh is None else DiffusionStepArgs("uniform", wl.kh[0], wl.kh[1], wl.seed, 0, k)
         t0 = time.perf_counter()
         out = O.step(st, vel, wl.mesh, wl.dt, 1.0, wl.scheme, vel_next=b, dt_to_next=dtn, w_interp=wl.w_interp,
-                     view=view)
-        t_used += time.perf_counter() - t0
+                     diffusion=diff, view=view)
+        dt = time.perf_counter() - t0
         st = st.replace(lon=out["lon"], lat=out["lat"], z=out["z"], status=out["status"],
                         nearest_node=out["nearest_node"], failure_reason=out["failure_reason"])
-        done += wl.P
-        k += 1
+        yield k, n, dt
+
+
+def cpu_baseline(wl, seconds: float = 10.0, n_particles: int = 200_000):
+    """The oracle port on this host's cores over a bounded sample of the
+    workload: up to ``n_particles`` particles, as many steps as fit in
+    ~``seconds``."""
+    from oracle import oracle as O
+    done, t_used, steps, n = 0, 0.0, 0, 0
+
+    def it():
+        k = 0
+        while k < wl.n_steps_run:
+            yield k
+            k += 1
+
+    for k, n, dt in _oracle_run(wl, n_particles, it()):
+        t_used += dt
+        done += n
+        steps += 1
+        if t_used >= seconds:
+            break
     return {"value": done / t_used, "unit": UNIT, "cores": O.threads(), "kind": "port",
-            "sample": f"{k} steps x {wl.P} particles of {wl.name} (oracle C port, {O.threads()} threads)"}
+            "sample": f"{steps} steps x {n} particles of {wl.name} (oracle C port, {O.threads()} threads)"}
 
 
 def run_reference(args):
@@ -135,32 +157,19 @@ def run_reference(args):
     from kelp_b200 import workloads
     wl = workloads.WORKLOADS[args.workload]()
     from oracle import oracle as O
-    from kelp_b200.particles import make_state
-    from kelp_b200.fields import LazyLerpField
-    view = O.MeshView(wl.mesh)
-    st = make_state(wl.lon, wl.lat, wl.z)
-    st = st.replace(failure_reason=np.zeros(wl.P, np.int8))
-    times = []
-    for k in range(args.warmup + args.steps):
-        ia, ib, alpha0, dtn = wl.bracket(k)
-        a, b = wl.snaps[ia], wl.snaps[ib]
-        vel = a if alpha0 == 0.0 else LazyLerpField(a, b, alpha0)
-        t0 = time.perf_counter()
-        out = O.step(st, vel, wl.mesh, wl.dt, 1.0, wl.scheme, vel_next=b, dt_to_next=dtn, w_interp=wl.w_interp,
-                     view=view)
-        dt = time.perf_counter() - t0
-        st = st.replace(lon=out["lon"], lat=out["lat"], z=out["z"], status=out["status"],
-                        nearest_node=out["nearest_node"], failure_reason=out["failure_reason"])
-        if k >= args.warmup:
-            times.append(dt)
+    # each step a bounded sample of the workload: the whole --steps/--warmup
+    # run stays within a few minutes of CPU time
+    n_sample = min(wl.P, args.reference_particles)
+    times = [dt for k, n, dt in _oracle_run(wl, n_sample, range(args.warmup + args.steps)) if k >= args.warmup]
     total = sum(times)
-    value = wl.P * args.steps / total
+    value = n_sample * args.steps / total
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps * wl.P / n_sample,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": {"workload": wl.name, **wl.description},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": O.threads(), "kind": "port",
-                             "sample": f"{args.steps} timed steps x {wl.P} particles (oracle C port)"},
+                             "sample": f"{args.steps} timed steps x {n_sample} of {wl.P} particles "
+                                       f"(oracle C port, {O.threads()} threads)"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -248,15 +257,18 @@ def run_b200(args):
         st_h[name] = a
     state = ParticleState(**st_h)
     step_fn = KI.get_integrator(wl.scheme)
-    e2e_steps = max(1, min(args.steps, 50))
+    from kelp_b200.diffusion import DiffusionStepArgs
+    e2e_steps = max(1, min(args.steps, 20))
     barrier()
     ctx.record(2)
     for k in range(e2e_steps):
         ia, ib, alpha0, dtn = wl.bracket(k)
         a, b = wl.snaps[ia], wl.snaps[ib]
         vel = a if alpha0 == 0.0 else LazyLerpField(a, b, alpha0)
+        diff = None if wl.kh is None else DiffusionStepArgs("uniform", wl.kh[0], wl.kh[1], wl.seed, 0, k,
+                                                            pid_offset=rank * P)
         state = step_fn(state, vel, wl.mesh, wl.dt, 1.0, uv_interp="barycentric", w_interp=wl.w_interp,
-                        vel_next=b, dt_to_next=dtn)
+                        vel_next=b, dt_to_next=dtn, diffusion=diff)
         for name in ("lon", "lat", "z", "status", "nearest_node", "failure_reason"):
             st_h[name][:] = getattr(state, name)
         state = ParticleState(**st_h)
@@ -310,6 +322,8 @@ def main():
     ap.add_argument("--workload", default="c1")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--reference-particles", type=int, default=100_000,
+                    help="particles per step of the --impl reference sample")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -151,6 +151,54 @@ def gyre_snapshots(mesh, n_snap: int = 2, *, amp: float = 0.5, dtype=np.float32,
     return out
 
 
+def vortex_snapshots(mesh, n_snap: int = 2, *, n_vortex: int = 256, rms: float = 0.3, z_levels=None,
+                     decay: float = 1000.0, w_amp: float = 1e-5, dtype=np.float32, seed: int = 3):
+    """Eddying node-layout field: a sum of ``n_vortex`` Gaussian vortices
+    (centres uniform on the sphere, radii 30-300 km, random sign), scaled to
+    ``rms`` m/s over the nodes; successive snapshots drift the centres
+    westward by one radius.  3-D: u/v per layer decaying as exp(-z/decay), and
+    a small smooth w (``w_amp`` m/s) on the interfaces, zero at the surface."""
+    rng = np.random.default_rng(seed)
+    lon = np.asarray(mesh.nodes_lon)
+    lat = np.asarray(mesh.nodes_lat)
+    zc = rng.uniform(-1, 1, n_vortex)
+    clat = np.degrees(np.arcsin(zc))
+    clon = rng.uniform(-180, 180, n_vortex)
+    rad = rng.uniform(30e3, 300e3, n_vortex)
+    sgn = rng.choice([-1.0, 1.0], n_vortex)
+    R_E = 6371000.0
+    out = []
+    for s in range(n_snap):
+        u = np.zeros(lon.size)
+        v = np.zeros(lon.size)
+        for k in range(n_vortex):
+            band = 4.0 * np.degrees(rad[k] / R_E)
+            sel = np.flatnonzero(np.abs(lat - clat[k]) < band)
+            cl = clon[k] - s * np.degrees(rad[k] / R_E) / max(np.cos(np.radians(clat[k])), 0.05)
+            dx = (((lon[sel] - cl + 180.0) % 360.0) - 180.0) * DEG2RAD * R_E * np.cos(np.radians(clat[k]))
+            dy = (lat[sel] - clat[k]) * DEG2RAD * R_E
+            g = np.exp(-(dx * dx + dy * dy) / (2 * rad[k] ** 2))
+            # stream function sgn * exp(-r^2 / 2R^2): u = -dpsi/dy, v = dpsi/dx
+            u[sel] += sgn[k] * g * dy / rad[k]
+            v[sel] -= sgn[k] * g * dx / rad[k]
+        scale = rms / max(np.sqrt(np.mean(u * u + v * v)), 1e-30)
+        u *= scale
+        v *= scale
+        if z_levels is None:
+            out.append(VelocityField(u=u.astype(dtype), v=v.astype(dtype), eta=np.zeros(lon.size),
+                                     uv_layout="node"))
+            continue
+        zl = np.asarray(z_levels, dtype=np.float64)
+        zm = 0.5 * (zl[:-1] + zl[1:])
+        dec = np.exp(-zm / decay).astype(dtype)[:, None]
+        wpat = np.sin(3 * lon * DEG2RAD + 0.9 * s) * np.cos(4 * lat * DEG2RAD)
+        wz = (1.0 - np.exp(-zl / decay)).astype(dtype)[:, None]
+        out.append(VelocityField(u=dec * u.astype(dtype)[None, :], v=dec * v.astype(dtype)[None, :],
+                                 w=(w_amp * wz) * wpat.astype(dtype)[None, :], eta=np.zeros(lon.size),
+                                 uv_layout="node", uv_vertical="layer"))
+    return out
+
+
 def release_uniform(mesh, P: int, seed: int = 3, *, depth_uniform: bool = False):
     """``P`` positions uniform in area over the mesh's elements (lon, lat, z)."""
     rng = np.random.default_rng(seed)

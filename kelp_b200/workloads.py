@@ -86,4 +86,39 @@ def c1(P: int = 100_000, spacing: float = 0.5625) -> Workload:
                                  "dt_s": 3600, "steps_run": 240, "fields": "f32 node u,v, 2 snapshots 24 h"})
 
 
-WORKLOADS: dict = {"c1": c1}
+def c3(P: int = 6_000_000, nside: int = 512, n_levels: int = 69, n_snap: int = 2) -> Workload:
+    """HEALPix nside 512 dual mesh (3.1 M pixels, ~70 % wet from smooth noise),
+    69 z-level interfaces (5 m .. 6000 m stretched), u/v (68, N) and w (69, N)
+    float32 (~1.8 GB per snapshot) from 256 Gaussian vortices at 0.3 m/s rms,
+    snapshots 24 h apart cycled, 6 M particles uniform over the wet area and
+    in the column, RK2 dt 6 h, W barycentric, split uniform random walk
+    Kh = 10 m^2/s keyed to particle id and step (seed 0)."""
+    from . import healpix as H
+    npix = 12 * nside * nside
+    pix = np.arange(npix)
+    plon, plat = H.pix2lonlat(nside, pix)
+    noise = S._sphere_noise(plon, plat, seed=2)
+    wet = noise >= np.quantile(noise, 0.3)
+    zl = S.stretched_levels(n_levels, 5.0, 6000.0)
+    depth = S.smooth_bathymetry(plon, plat, 50.0, 6000.0)
+    m = H.dual_mesh(nside, wet, depth, sigma=zl)
+    snaps = S.vortex_snapshots(m, n_snap, z_levels=zl)
+    lon, lat, z = S.release_uniform(m, P, seed=3, depth_uniform=True)
+    return Workload("c3_healpix512_3d_rk2_kick", m, snaps, lon, lat, z, "rk2", 21600.0, 86400.0, 1460,
+                    dims=3, w_interp="barycentric", kh=(10.0, 10.0), seed=0,
+                    description={"mesh": f"HEALPix nside {nside} dual mesh, ~70% wet", "nodes": int(m.n_nodes),
+                                 "elements": int(m.n_elements), "levels": n_levels, "particles": P,
+                                 "scheme": "rk2", "dt_s": 21600, "steps_run": 1460,
+                                 "fields": "f32 node u,v (68,N), w (69,N), 256 Gaussian vortices 0.3 m/s rms",
+                                 "diffusion": "split uniform Kh=10 m^2/s", "w_interp": "barycentric"})
+
+
+def c3_small(P: int = 200_000) -> Workload:
+    """C3's kernel on a reduced HEALPix grid (nside 128) and particle count:
+    the profiling case (a few hundred MB on the device)."""
+    w = c3(P=P, nside=128, n_levels=69)
+    w.name = "c3small_healpix128_3d_rk2_kick"
+    return w
+
+
+WORKLOADS: dict = {"c1": c1, "c3": c3, "c3small": c3_small}

@@ -137,3 +137,33 @@ def test_cuda_vs_oracle_c1_like(scheme):
                         failure_reason=out["failure_reason"], u=out["u"], v=out["v"])
     want = {f"f_{k}": getattr(so, k) for k in ("lon", "lat", "status", "nearest_node", "failure_reason", "u", "v")}
     assert_close_state(st, want, "f_", f"c1-like {scheme}")
+
+
+def test_cuda_vs_oracle_healpix_3d_kick():
+    """A C3-shaped run on a reduced HEALPix dual mesh (nside 32: quads, the 8
+    valence-3 triangles and the pole cells), 69 levels, W barycentric, the split
+    uniform kick, 12 steps of 6 h: CUDA against the oracle."""
+    from oracle import oracle as O
+    from kelp_b200 import workloads as W
+    from kelp_b200.particles import make_state
+    from kelp_b200.fields import LazyLerpField
+    w = W.c3(P=20000, nside=32)
+    st = make_state(w.lon, w.lat, w.z).replace(failure_reason=np.zeros(w.P, np.int8))
+    so = st
+    view = O.MeshView(w.mesh)
+    for k in range(12):
+        ia, ib, alpha0, dtn = w.bracket(k)
+        a, b = w.snaps[ia], w.snaps[ib]
+        vel = a if alpha0 == 0.0 else LazyLerpField(a, b, alpha0)
+        diff = DiffusionStepArgs("uniform", 10.0, 10.0, 0, 0, k)
+        st = KI.rk2_step(st, vel, w.mesh, w.dt, 1.0, uv_interp="barycentric", w_interp="barycentric",
+                         vel_next=b, dt_to_next=dtn, diffusion=diff)
+        out = O.step(so, vel, w.mesh, w.dt, 1.0, "rk2", vel_next=b, dt_to_next=dtn, w_interp="barycentric",
+                     diffusion=diff, view=view)
+        so = so.replace(lon=out["lon"], lat=out["lat"], z=out["z"], status=out["status"],
+                        nearest_node=out["nearest_node"], failure_reason=out["failure_reason"],
+                        u=out["u"], v=out["v"], w=out["w"])
+    want = {f"f_{k}": getattr(so, k) for k in ("lon", "lat", "z", "status", "nearest_node", "failure_reason",
+                                               "u", "v", "w")}
+    assert_close_state(st, want, "f_", "healpix 3-D rk2 + kick")
+    assert (st.status == 1).sum() > 0.5 * w.P
