@@ -21,10 +21,10 @@ LIB = os.path.join(HERE, "libkelpcuda.so")
 
 CU_SOURCES = ["kc_api.cu"]
 CPP_SOURCES = ["kc_host.cpp"]
-HEADERS = ["kc_geom.cuh", "kc_interp.cuh", "kc_step.cuh"]
+HEADERS = ["kc_geom.cuh", "kc_interp.cuh", "kc_step.cuh", "kc_host.h"]
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-              "-fmad=false", "-Xcompiler", "-fPIC", "-Xptxas", "-v"]
+              "-fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off", "-Xptxas", "-v"]
 
 
 def _nvcc() -> str:

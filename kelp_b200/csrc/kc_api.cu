@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/kelp_cuda.h"
+#include "kc_host.h"
 #include "kc_step.cuh"
 
 namespace {
@@ -44,6 +45,9 @@ struct kc_ctx {
     double* d_xyz = nullptr;
     double* d_depth = nullptr;
     double* d_zlev = nullptr;
+    double2* d_nsc = nullptr;
+    double2* d_ecos = nullptr;
+    int* d_maxl = nullptr;
     int* d_err = nullptr;
     kc::DMesh dm{};
     // snapshot ring
@@ -120,7 +124,7 @@ __device__ __forceinline__ void activate(const kc::DState& st, const kc::DStep& 
 }
 
 template <typename T, int SCHEME>
-__global__ void __launch_bounds__(kBlock) k_step2d(kc::DMesh m, kc::DBlend<T> f, kc::DState st, kc::DStep s) {
+__global__ void __launch_bounds__(kBlock) k_step2d(const __grid_constant__ kc::DMesh m, const __grid_constant__ kc::DBlend<T> f, const __grid_constant__ kc::DState st, const __grid_constant__ kc::DStep s) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= st.P) return;
     activate(st, s, i);
@@ -128,17 +132,17 @@ __global__ void __launch_bounds__(kBlock) k_step2d(kc::DMesh m, kc::DBlend<T> f,
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kBlock) k_step3d_rk2(kc::DMesh m, kc::DBlend<T> f, kc::DState st, kc::DStep s) {
+__global__ void __launch_bounds__(kBlock) k_step3d_rk2(const __grid_constant__ kc::DMesh m, const __grid_constant__ kc::DBlend<T> f, const __grid_constant__ kc::DState st, const __grid_constant__ kc::DStep s) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= st.P) return;
     activate(st, s, i);
     kc::step3d_rk2_particle<T>(m, f, st, s, i);
 }
 
-__global__ void __launch_bounds__(kBlock) k_nearest(kc::DMesh m, const double* q, long long P, int* out) {
+__global__ void __launch_bounds__(kBlock) k_nearest(const __grid_constant__ kc::DMesh m, const double* q, long long P, int* out) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P) return;
-    out[i] = kc::site_anchor(m, q[i], q[P + i]);
+    out[i] = kc::site_anchor(m, kc::make_site(q[i], q[P + i]));
 }
 
 __global__ void __launch_bounds__(kBlock) k_normals(long long P, unsigned long long seed, unsigned long long real_id,
@@ -225,6 +229,7 @@ int upload(kc_ctx* c, T** dst, const void* src, size_t count) {
 void free_mesh(kc_ctx* c) {
     dfree(c->d_ll); dfree(c->d_en); dfree(c->d_n2e_off); dfree(c->d_n2e); dfree(c->d_gh_off);
     dfree(c->d_gh_tab); dfree(c->d_xyz); dfree(c->d_depth); dfree(c->d_zlev);
+    dfree(c->d_nsc); dfree(c->d_ecos); dfree(c->d_maxl);
     c->has_mesh = false;
 }
 
@@ -337,7 +342,15 @@ int kc_mesh_upload(kc_ctx* c, const kc_mesh_desc* d) {
         tab[k] = make_double4(d->node_xyz[3 * (long long)nd], d->node_xyz[3 * (long long)nd + 1],
                               d->node_xyz[3 * (long long)nd + 2], (double)nd);
     }
+    std::vector<double2> nsc((size_t)N), ecos((size_t)E);
+    std::vector<int> maxl(d->n_levels >= 2 ? (size_t)N : 0);
+    kc_host::mesh_tables(N, E, d->max_v, d->nodes_lat, d->elem_nodes, d->depth, d->z_levels, d->n_levels,
+                         reinterpret_cast<double*>(nsc.data()), reinterpret_cast<double*>(ecos.data()),
+                         maxl.empty() ? nullptr : maxl.data());
     int rc;
+    if ((rc = upload(c, &c->d_nsc, nsc.data(), nsc.size()))) return rc;
+    if ((rc = upload(c, &c->d_ecos, ecos.data(), ecos.size()))) return rc;
+    if (!maxl.empty() && (rc = upload(c, &c->d_maxl, maxl.data(), maxl.size()))) return rc;
     if ((rc = upload(c, &c->d_ll, ll.data(), ll.size()))) return rc;
     if ((rc = upload(c, &c->d_en, en.data(), en.size()))) return rc;
     if ((rc = upload(c, &c->d_n2e_off, off.data(), off.size()))) return rc;
@@ -352,6 +365,7 @@ int kc_mesh_upload(kc_ctx* c, const kc_mesh_desc* d) {
     m.ll = c->d_ll; m.en = c->d_en; m.n2e_off = c->d_n2e_off; m.n2e = c->d_n2e;
     m.gh_off = c->d_gh_off; m.gh_tab = c->d_gh_tab; m.xyz = c->d_xyz;
     m.depth = c->d_depth; m.zlev = c->d_zlev;
+    m.nsc = c->d_nsc; m.ecos = c->d_ecos; m.max_layer = c->d_maxl;
     m.cell = d->gh_cell_size; m.lon_min = d->gh_lon_min; m.lat_min = d->gh_lat_min; m.r_earth = d->r_earth;
     m.nx = d->gh_nx; m.ny = d->gh_ny; m.wrap = d->gh_wrap_lon ? 1 : 0; m.far_rows = d->gh_far_rows;
     m.K = d->n_levels; m.exact = d->exact_nearest ? 1 : 0;

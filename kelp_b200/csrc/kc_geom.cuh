@@ -7,6 +7,13 @@
 // compiled with -fmad=false: Numba emits no fused multiply-adds, so a
 // contracted a*b+c here would round differently and could flip an anchor or
 // a containment verdict.
+//
+// Trigonometric values that depend only on the mesh (sin/cos of a node's
+// latitude, cos of an element's mean latitude) come from tables evaluated on
+// the host with the C library -- the functions the reference's Numba code
+// calls -- so they carry the reference's exact values.  Values that depend on
+// a particle position are evaluated once per evaluation site with CUDA's
+// double-precision functions and shared by every consumer at that site.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -19,30 +26,52 @@ constexpr double SLM = 111120.0;                   // metres per degree of latit
 constexpr double R_STD = 6371000.0;                // standard Earth radius
 constexpr double BARY_EPS = -1e-6;                 // mesh.py:33
 constexpr double AREA_TOL = 1e-10;                 // mesh.py:32
-constexpr double INF30 = 1.0e30;
 constexpr int SHORT_ROW_CELLS = 32;                // mesh.py:1608
 constexpr int ALIVE = 1, BEACHED = 2, OUTSIDE = 3, NOT_RELEASED = 4;
 constexpr int FR_INTERP = 1, FR_OOB = 2;
 
 // device error word bits (read back by the host)
 constexpr int ERR_SEARCH_CAP = 1;   // exact-search growth loop hit its cap
-constexpr int ERR_RING_CAP = 2;     // widened ring search hit its cap
 
-// Resident mesh: node table, element table, node->element CSR, grid hash.
+// Resident mesh: node table, element table, node->element CSR, grid hash and
+// the host-evaluated trigonometric tables.
 struct DMesh {
     const double2* ll;        // (N) node lon, lat in degrees
+    const double2* nsc;       // (N) sin, cos of the node latitude (radians)
     const int4* en;           // (E) element nodes, -1 padded to 4
+    const double2* ecos;      // (E) cos(mean vertex latitude): x containment set, y compacted set
     const int* n2e_off;       // (N+1) CSR offsets of the node->element table
     const int* n2e;           // element ids, per node in the reference order
     const int* gh_off;        // (nx*ny+1) CSR offsets of the grid hash
     const double4* gh_tab;    // hash-ordered {x, y, z, node id} unit-sphere table
     const double* xyz;        // (N, 3) unit-sphere table by node id
     const double* depth;      // (N) bottom depth, positive down (3-D)
+    const int* max_layer;     // (N) deepest valid layer above the node's bottom (3-D)
     const double* zlev;       // (K) z-level interfaces, positive down (3-D)
     double cell, lon_min, lat_min, r_earth;
     int nx, ny, wrap, far_rows, K, exact;
     int* err;                 // device error word
 };
+
+// Trigonometry of one evaluation site (a query position).
+struct Site {
+    double lon, lat;
+    double xp, yp, zp;        // unit-sphere position
+    double sin_lat, cos_lat;  // of lat * DEG2RAD
+    double sin_lon, cos_lon;  // of lon * DEG2RAD
+};
+
+__device__ __forceinline__ Site make_site(double lon, double lat) {
+    Site s;
+    s.lon = lon;
+    s.lat = lat;
+    sincos(lat * DEG2RAD, &s.sin_lat, &s.cos_lat);
+    sincos(lon * DEG2RAD, &s.sin_lon, &s.cos_lon);
+    s.xp = s.cos_lat * s.cos_lon;
+    s.yp = s.cos_lat * s.sin_lon;
+    s.zp = s.sin_lat;
+    return s;
+}
 
 // Python float modulo for a positive divisor (CPython float_rem, Numba
 // real_divmod): the remainder carries the divisor's sign, zero is +0.
@@ -86,17 +115,6 @@ __device__ __forceinline__ void gh_cell_of(const DMesh& m, double lon_p, double 
     if (cj >= m.ny) cj = m.ny - 1;
 }
 
-// Query point on the unit sphere (mesh.py:1268-1273); also returns cos(lat).
-__device__ __forceinline__ void query_xyz(double lon_p, double lat_p, double& xp, double& yp, double& zp, double& cos_lat) {
-    double lat_r = lat_p * DEG2RAD;
-    double lon_r = lon_p * DEG2RAD;
-    double cl = cos(lat_r);
-    xp = cl * cos(lon_r);
-    yp = cl * sin(lon_r);
-    zp = sin(lat_r);
-    cos_lat = cl;
-}
-
 // Scan hash-table positions [s, e): strict '<' keeps the first node found
 // on a tie, which makes the CSR order part of the contract (mesh.py:1290-1301).
 __device__ __forceinline__ void scan_range(const double4* __restrict__ tab, int s, int e,
@@ -110,17 +128,17 @@ __device__ __forceinline__ void scan_range(const double4* __restrict__ tab, int 
     }
 }
 
-__device__ __forceinline__ void scan_cell(const DMesh& m, int cell, double xp, double yp, double zp, int& best, double& bd2) {
+__device__ __forceinline__ void scan_cell(const DMesh& m, int cell, double xp, double yp, double zp, int& best,
+                                          double& bd2) {
     scan_range(m.gh_tab, __ldg(&m.gh_off[cell]), __ldg(&m.gh_off[cell + 1]), xp, yp, zp, best, bd2);
 }
 
 // mesh.py:1235-1303 _grid_hash_nearest_3x3.  Adjacent columns of one row are
 // adjacent in the CSR, so an unclipped, unwrapped row is one contiguous slice
 // (same nodes, same order as three cell scans).
-__device__ __forceinline__ int nearest_3x3(const DMesh& m, double lon_p, double lat_p,
-                                           double xp, double yp, double zp, double& bd2_out) {
+__device__ __forceinline__ int nearest_3x3(const DMesh& m, const Site& q, double& bd2_out) {
     int ci, cj;
-    gh_cell_of(m, lon_p, lat_p, ci, cj);
+    gh_cell_of(m, q.lon, q.lat, ci, cj);
     int best = -1;
     double bd2 = 1e30;
     for (int dj = -1; dj <= 1; ++dj) {
@@ -128,14 +146,15 @@ __device__ __forceinline__ int nearest_3x3(const DMesh& m, double lon_p, double 
         if (cj2 < 0 || cj2 >= m.ny) continue;
         int row = cj2 * m.nx;
         if (ci >= 1 && ci + 1 < m.nx) {
-            scan_range(m.gh_tab, __ldg(&m.gh_off[row + ci - 1]), __ldg(&m.gh_off[row + ci + 2]), xp, yp, zp, best, bd2);
+            scan_range(m.gh_tab, __ldg(&m.gh_off[row + ci - 1]), __ldg(&m.gh_off[row + ci + 2]), q.xp, q.yp, q.zp,
+                       best, bd2);
         } else {
             for (int di = -1; di <= 1; ++di) {
                 int ci2 = ci + di;
                 if (ci2 < 0) ci2 = m.wrap ? ci2 + m.nx : -1;
                 else if (ci2 >= m.nx) ci2 = m.wrap ? ci2 - m.nx : -1;
                 if (ci2 < 0) continue;
-                scan_cell(m, row + ci2, xp, yp, zp, best, bd2);
+                scan_cell(m, row + ci2, q.xp, q.yp, q.zp, best, bd2);
             }
         }
     }
@@ -143,30 +162,30 @@ __device__ __forceinline__ int nearest_3x3(const DMesh& m, double lon_p, double 
     return best;
 }
 
-// mesh.py:1306-1328 _cap_extents -> (theta_deg, ext_lon_deg)
-__device__ __forceinline__ void cap_extents(double lon_p, double lat_p, double lon_n, double lat_n,
-                                            double& theta_deg, double& ext) {
-    double lat_pr = lat_p * DEG2RAD;
-    double lat_nr = lat_n * DEG2RAD;
-    double cosd = sin(lat_pr) * sin(lat_nr) + cos(lat_pr) * cos(lat_nr) * cos((lon_p - lon_n) * DEG2RAD);
+// mesh.py:1306-1328 _cap_extents -> (theta_deg, ext_lon_deg); the node's
+// sin/cos(latitude) from the host table, the query's from the site.
+__device__ __forceinline__ void cap_extents(const DMesh& m, const Site& q, int node, double& theta_deg, double& ext) {
+    double2 nl = __ldg(&m.ll[node]);
+    double2 sc = __ldg(&m.nsc[node]);
+    double cosd = q.sin_lat * sc.x + q.cos_lat * sc.y * cos((q.lon - nl.x) * DEG2RAD);
     if (cosd > 1.0) cosd = 1.0;
     if (cosd < -1.0) cosd = -1.0;
     double theta = acos(cosd);
     if (theta <= 0.0) { theta_deg = 0.0; ext = 0.0; return; }
     theta_deg = theta * RAD2DEG;
-    if (fabs(lat_p) + theta_deg >= 90.0) { ext = 1.0e30; return; }
-    double r = sin(theta) / cos(lat_pr);
+    if (fabs(q.lat) + theta_deg >= 90.0) { ext = 1.0e30; return; }
+    double r = sin(theta) / q.cos_lat;
     if (r >= 1.0) { ext = 1.0e30; return; }
     ext = asin(r) * RAD2DEG;
 }
 
-// mesh.py:1475-1549 _anchor_provable_rect: 0 when `node` is provably the
-// nearest for the (2rx+1) x (2ry+1) window, else a deficit bitmask.
-__device__ __noinline__ int anchor_provable_rect(const DMesh& m, double lon_p, double lat_p, int node, int rx, int ry) {
-    double2 nl = __ldg(&m.ll[node]);
-    double theta_deg, ext_lon;
-    cap_extents(lon_p, lat_p, nl.x, nl.y, theta_deg, ext_lon);
+// The coverage tests of mesh.py:1475-1549 _anchor_provable_rect for given
+// (theta_deg, ext_lon).  Every test is monotone in both, so upper bounds that
+// pass prove that the reference's own values pass.
+__device__ __forceinline__ int provable_code(const DMesh& m, const Site& q, int rx, int ry, double theta_deg,
+                                             double ext_lon) {
     if (theta_deg <= 0.0) return 0;
+    const double lon_p = q.lon, lat_p = q.lat;
     double dlon = gh_fold_dlon(m, lon_p);
     double lon_q = m.lon_min + dlon;
     int ci_raw = (int)floor(dlon / m.cell);
@@ -210,15 +229,39 @@ __device__ __noinline__ int anchor_provable_rect(const DMesh& m, double lon_p, d
     return code;
 }
 
+// mesh.py:1475-1549 _anchor_provable_rect with the reference's own extents.
+__device__ __noinline__ int anchor_provable_rect(const DMesh& m, const Site& q, int node, int rx, int ry) {
+    double theta_deg, ext_lon;
+    cap_extents(m, q, node, theta_deg, ext_lon);
+    return provable_code(m, q, rx, ry, theta_deg, ext_lon);
+}
+
+// Fast sufficient test of the 3x3 certificate.  Upper bounds of the cap's
+// angular radius -- from the scan's chord c: 2 asin(c/2) <= c (1 + c^2/16)
+// for c <= 1, plus 1e-7 rad for the rounding of the reference's acos form --
+// and of its longitude extent (sin t <= t; asin(r) <= r (1 + 0.2 r^2) for
+// r <= 0.5).  True only when the bounds pass every coverage test, so the
+// reference's certificate passes too; otherwise the caller evaluates it.
+__device__ __forceinline__ bool provable_fast(const DMesh& m, const Site& q, double bd2) {
+    double c = sqrt(bd2);
+    if (!(c <= 0.5)) return false;
+    double t = c * (1.0 + c * c * 0.0625) * (1.0 + 1e-12) + 1e-7;
+    double tdeg = t * RAD2DEG * (1.0 + 1e-12);
+    if (fabs(q.lat) + tdeg >= 89.0) return false;
+    double r = t / q.cos_lat * (1.0 + 1e-12);
+    if (!(r <= 0.5)) return false;
+    double edeg = r * (1.0 + 0.2 * r * r) * RAD2DEG * (1.0 + 1e-12);
+    return provable_code(m, q, 1, 1, tdeg, edeg) == 0;
+}
+
 // mesh.py:1331-1442 _grid_hash_nearest_widened: the 3x3 window, and on an
 // empty window a ring-by-ring scan that stops one ring after the first hit.
-__device__ __noinline__ int nearest_widened(const DMesh& m, double lon_p, double lat_p) {
-    double xp, yp, zp, cl, bd2;
-    query_xyz(lon_p, lat_p, xp, yp, zp, cl);
-    int best = nearest_3x3(m, lon_p, lat_p, xp, yp, zp, bd2);
+__device__ __noinline__ int nearest_widened(const DMesh& m, const Site& q) {
+    double bd2;
+    int best = nearest_3x3(m, q, bd2);
     if (best >= 0) return best;
     int ci, cj;
-    gh_cell_of(m, lon_p, lat_p, ci, cj);
+    gh_cell_of(m, q.lon, q.lat, ci, cj);
     bd2 = 1e30;
     int max_ring = m.nx > m.ny ? m.nx : m.ny;
     int found_ring = -1;
@@ -231,7 +274,7 @@ __device__ __noinline__ int nearest_widened(const DMesh& m, double lon_p, double
                 int ci2 = ci + di;
                 if (m.wrap) ci2 = imod(ci2, m.nx);
                 else if (ci2 < 0 || ci2 >= m.nx) continue;
-                scan_cell(m, cj2 * m.nx + ci2, xp, yp, zp, best, bd2);
+                scan_cell(m, cj2 * m.nx + ci2, q.xp, q.yp, q.zp, best, bd2);
             }
         }
         if (best >= 0) {
@@ -245,7 +288,8 @@ __device__ __noinline__ int nearest_widened(const DMesh& m, double lon_p, double
 // mesh.py:1552-1605 row slices
 __device__ __forceinline__ void scan_row_range(const DMesh& m, int cj2, int c_lo, int c_hi,
                                                double xp, double yp, double zp, int& best, double& bd2) {
-    scan_range(m.gh_tab, __ldg(&m.gh_off[cj2 * m.nx + c_lo]), __ldg(&m.gh_off[cj2 * m.nx + c_hi + 1]), xp, yp, zp, best, bd2);
+    scan_range(m.gh_tab, __ldg(&m.gh_off[cj2 * m.nx + c_lo]), __ldg(&m.gh_off[cj2 * m.nx + c_hi + 1]), xp, yp, zp,
+               best, bd2);
 }
 
 __device__ __forceinline__ void scan_row_window(const DMesh& m, int cj2, int ci, int rx,
@@ -267,43 +311,23 @@ __device__ __forceinline__ void scan_row_window(const DMesh& m, int cj2, int ci,
     scan_row_range(m, cj2, c_lo, c_hi, xp, yp, zp, best, bd2);
 }
 
-
-// mesh.py:1611-1859 _grid_hash_nearest_exact: the 3x3 window accepted when
-// the certificate proves it, else a rectangle grown by the certificate's
-// deficits until the best node is provable, every cell is scanned, or the
-// row budget `far_rows` says the query is outside every element.
-__device__ __noinline__ int nearest_exact_slow(const DMesh& m, double lon_p, double lat_p, int best, int code);
-
-__device__ __forceinline__ int nearest_exact(const DMesh& m, double lon_p, double lat_p,
-                                             double xp, double yp, double zp) {
+// The certificate-driven rectangle growth of mesh.py:1670-1859, entered when
+// the 3x3 hit is not provable (or the window is empty).
+__device__ __noinline__ int nearest_exact_slow(const DMesh& m, const Site& q, int best, int code) {
     const double far = (double)m.far_rows * m.cell;
-    if (lat_p < m.lat_min - far || lat_p > m.lat_min + (double)m.ny * m.cell + far)
-        return nearest_widened(m, lon_p, lat_p);
-    double bd2;
-    int best = nearest_3x3(m, lon_p, lat_p, xp, yp, zp, bd2);
-    int code = 0;
+    const double lat_p = q.lat;
     if (best >= 0) {
-        code = anchor_provable_rect(m, lon_p, lat_p, best, 1, 1);
-        if (code == 0) return best;
-    }
-    return nearest_exact_slow(m, lon_p, lat_p, best, code);
-}
-
-__device__ __noinline__ int nearest_exact_slow(const DMesh& m, double lon_p, double lat_p, int best, int code) {
-    const double far = (double)m.far_rows * m.cell;
-    if (best >= 0) {
-        double2 nl = __ldg(&m.ll[best]);
         double theta_deg, ext;
-        cap_extents(lon_p, lat_p, nl.x, nl.y, theta_deg, ext);
+        cap_extents(m, q, best, theta_deg, ext);
         if (theta_deg > far) return best;
     }
     int ci, cj;
-    gh_cell_of(m, lon_p, lat_p, ci, cj);
-    double xp, yp, zp, cos_lat_p;
-    query_xyz(lon_p, lat_p, xp, yp, zp, cos_lat_p);
+    gh_cell_of(m, q.lon, q.lat, ci, cj);
+    const double xp = q.xp, yp = q.yp, zp = q.zp, cos_lat_p = q.cos_lat;
     double best_d2 = 1.0e30;
     if (best >= 0) {
-        double xn = m.xyz[3 * (long long)best], yn = m.xyz[3 * (long long)best + 1], zn = m.xyz[3 * (long long)best + 2];
+        double xn = m.xyz[3 * (long long)best], yn = m.xyz[3 * (long long)best + 1];
+        double zn = m.xyz[3 * (long long)best + 2];
         double dx = xn - xp, dy = yn - yp, dz = zn - zp;
         best_d2 = dx * dx + dy * dy + dz * dz;
     }
@@ -318,13 +342,13 @@ __device__ __noinline__ int nearest_exact_slow(const DMesh& m, double lon_p, dou
     }
     int ry_max = cj > m.ny - 1 - cj ? cj : m.ny - 1 - cj;
     double abs_lat = lat_p >= 0.0 ? lat_p : -lat_p;
-    double dlon_q = gh_fold_dlon(m, lon_p);
+    double dlon_q = gh_fold_dlon(m, q.lon);
     const double INF = 1.0e30;
     // each pass grows rx or ry by at least one, or returns
     const int cap = 4 * (m.nx + m.ny) + 16;
     for (int it = 0; it < cap; ++it) {
         if (best >= 0 && code == 0) {
-            code = anchor_provable_rect(m, lon_p, lat_p, best, rx, ry);
+            code = anchor_provable_rect(m, q, best, rx, ry);
             if (code == 0) return best;
         }
         if (best < 0 || 2.0 * asin(0.5 * sqrt(best_d2)) * RAD2DEG > far) {
@@ -354,7 +378,7 @@ __device__ __noinline__ int nearest_exact_slow(const DMesh& m, double lon_p, dou
             }
             if (clear >= far) {
                 if (best >= 0) return best;
-                return nearest_widened(m, lon_p, lat_p);
+                return nearest_widened(m, q);
             }
         }
         bool grow_x, grow_y, all_x;
@@ -372,7 +396,7 @@ __device__ __noinline__ int nearest_exact_slow(const DMesh& m, double lon_p, dou
         if (ry >= ry_max) grow_y = false;
         if (!(grow_x || grow_y || all_x)) {
             if (best >= 0) return best;
-            return nearest_widened(m, lon_p, lat_p);
+            return nearest_widened(m, q);
         }
         int rx_new = all_x ? rx_max : (grow_x ? rx + 1 : rx);
         int ry_new = grow_y ? ry + 1 : ry;
@@ -436,12 +460,26 @@ __device__ __noinline__ int nearest_exact_slow(const DMesh& m, double lon_p, dou
     return best;
 }
 
+// mesh.py:1611-1859 _grid_hash_nearest_exact: the 3x3 window accepted when
+// the certificate proves it (fast bound first, the reference's own
+// certificate when the bound is inconclusive), else the rectangle growth.
+__device__ __noinline__ int nearest_exact(const DMesh& m, const Site& q) {
+    const double far = (double)m.far_rows * m.cell;
+    if (q.lat < m.lat_min - far || q.lat > m.lat_min + (double)m.ny * m.cell + far) return nearest_widened(m, q);
+    double bd2;
+    int best = nearest_3x3(m, q, bd2);
+    int code = 0;
+    if (best >= 0) {
+        if (provable_fast(m, q, bd2)) return best;
+        code = anchor_provable_rect(m, q, best, 1, 1);
+        if (code == 0) return best;
+    }
+    return nearest_exact_slow(m, q, best, code);
+}
+
 // The anchor of one evaluation site (integrators.py:1470-1487).
-__device__ __forceinline__ int site_anchor(const DMesh& m, double lon_p, double lat_p) {
-    if (!m.exact) return nearest_widened(m, lon_p, lat_p);
-    double xp, yp, zp, cl;
-    query_xyz(lon_p, lat_p, xp, yp, zp, cl);
-    return nearest_exact(m, lon_p, lat_p, xp, yp, zp);
+__device__ __forceinline__ int site_anchor(const DMesh& m, const Site& q) {
+    return m.exact ? nearest_exact(m, q) : nearest_widened(m, q);
 }
 
 // ---------------------------------------------------------------------------
@@ -484,95 +522,96 @@ __device__ __forceinline__ void wachspress_quad(double px, double py, const doub
     for (int k = 0; k < 4; ++k) out[k] = out[k] / s;
 }
 
-// mesh.py:2119-2136 _polygon_weights; returns false only for the degenerate
-// triangle sentinel (w[0] == -1.0 is what the callers test).
-__device__ __forceinline__ bool polygon_weights(double px, double py, const double* x, const double* y, int nv, double* w) {
-    if (nv == 3) {
-        bary_tri(px, py, x[0], y[0], x[1], y[1], x[2], y[2], w[0], w[1], w[2]);
-        return !(w[0] == -1.0);
-    }
-    wachspress_quad(px, py, x, y, w);
-    return !(w[0] == -1.0);
+// The vertices of an element in the containment (mask) convention of
+// mesh.py:2216-2236: drop -1 slots, and slot 3 when it repeats slot 0.
+struct Poly {
+    double ln[4], la[4];
+    int n;
+};
+
+__device__ __forceinline__ void put_vertex(Poly& p, int n, double2 a) {
+    if (n == 0) { p.ln[0] = a.x; p.la[0] = a.y; }
+    else if (n == 1) { p.ln[1] = a.x; p.la[1] = a.y; }
+    else if (n == 2) { p.ln[2] = a.x; p.la[2] = a.y; }
+    else { p.ln[3] = a.x; p.la[3] = a.y; }
+}
+
+__device__ __forceinline__ void load_poly_mask(const DMesh& m, int4 e, Poly& p) {
+    bool v3 = e.w >= 0 && !(e.w == e.x && e.x >= 0);
+    int n = 0;
+    if (e.x >= 0) put_vertex(p, n++, __ldg(&m.ll[e.x]));
+    if (e.y >= 0) put_vertex(p, n++, __ldg(&m.ll[e.y]));
+    if (e.z >= 0) put_vertex(p, n++, __ldg(&m.ll[e.z]));
+    if (v3) put_vertex(p, n++, __ldg(&m.ll[e.w]));
+    p.n = n;
 }
 
 // mesh.py:2210-2263 _element_contains with mesh.py:2006-2051
-// _project_to_local_xy and mesh.py:2139-2168 _polygon_contains_bool.
+// _project_to_local_xy and mesh.py:2139-2168 _polygon_contains_bool; the
+// cos of the mean vertex latitude comes from the host table.
 __device__ __forceinline__ bool element_contains(const DMesh& m, int c, double lon_p, double lat_p) {
     int4 e = __ldg(&m.en[c]);
-    int nodes[4] = {e.x, e.y, e.z, e.w};
-    bool mask[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) mask[k] = nodes[k] >= 0;
-    if (nodes[3] == nodes[0] && nodes[0] >= 0) mask[3] = false;
-    int n = 0;
-    double ln[4], la[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        if (mask[k]) {
-            double2 p = __ldg(&m.ll[nodes[k]]);
-            ln[n] = p.x;
-            la[n] = p.y;
-            ++n;
-        }
-    }
+    Poly p;
+    load_poly_mask(m, e, p);
+    const int n = p.n;
     if (n < 3) return false;
     // bbox prefilter in wrapped-delta space around the first valid vertex
-    double lon_ref = ln[0];
-    double dmin = 0.0, dmax = 0.0, lamin = la[0], lamax = la[0];
-    for (int k = 0; k < n; ++k) {
-        double d = wrap180(ln[k] - lon_ref);
-        if (k == 0) { dmin = d; dmax = d; }
-        else { if (d < dmin) dmin = d; if (d > dmax) dmax = d; }
-        if (la[k] > lamax) lamax = la[k];
-        if (la[k] < lamin) lamin = la[k];
+    // (the first vertex's own delta is wrap180(0) == 0)
+    const double lon_ref = p.ln[0];
+    const double d1 = wrap180(p.ln[1] - lon_ref), d2 = wrap180(p.ln[2] - lon_ref);
+    const double d3 = n == 4 ? wrap180(p.ln[3] - lon_ref) : 0.0;
+    double dmin = fmin(fmin(0.0, d1), d2), dmax = fmax(fmax(0.0, d1), d2);
+    double lamin = fmin(fmin(p.la[0], p.la[1]), p.la[2]), lamax = fmax(fmax(p.la[0], p.la[1]), p.la[2]);
+    if (n == 4) {
+        dmin = fmin(dmin, d3); dmax = fmax(dmax, d3);
+        lamin = fmin(lamin, p.la[3]); lamax = fmax(lamax, p.la[3]);
     }
-    double dlon_p = wrap180(lon_p - lon_ref);
+    const double dlon_p = wrap180(lon_p - lon_ref);
     if (dlon_p > dmax || dlon_p < dmin) return false;
     if (lat_p > lamax || lat_p < lamin) return false;
     // local projection: raw-mean origin unless the element spans > 180 deg
-    double lmin = ln[0], lmax = ln[0];
-    for (int k = 0; k < n; ++k) {
-        if (ln[k] < lmin) lmin = ln[k];
-        if (ln[k] > lmax) lmax = ln[k];
-    }
+    double lmin = fmin(fmin(p.ln[0], p.ln[1]), p.ln[2]), lmax = fmax(fmax(p.ln[0], p.ln[1]), p.ln[2]);
+    if (n == 4) { lmin = fmin(lmin, p.ln[3]); lmax = fmax(lmax, p.ln[3]); }
     double lon0;
     if (lmax - lmin > 180.0) {
-        double ref = ln[0], dsum = 0.0;
-        for (int k = 0; k < n; ++k) dsum += wrap180(ln[k] - ref);
-        lon0 = ref + dsum / (double)n;
+        double dsum = 0.0 + d1;        // 0 + wrap180(ln[0] - ln[0]) + d1 + d2 (+ d3)
+        dsum += d2;
+        if (n == 4) dsum += d3;
+        lon0 = lon_ref + dsum / (double)n;
     } else {
-        double s = 0.0;
-        for (int k = 0; k < n; ++k) s += ln[k];
+        double s = p.ln[0] + p.ln[1];
+        s += p.ln[2];
+        if (n == 4) s += p.ln[3];
         lon0 = s / (double)n;
     }
-    double s = 0.0;
-    for (int k = 0; k < n; ++k) s += la[k];
-    double lat0 = s / (double)n;
-    double cos_lat0 = cos(lat0 * DEG2RAD);
-    double x[4], y[4];
-    for (int k = 0; k < n; ++k) {
-        x[k] = wrap180(ln[k] - lon0) * DEG2RAD * R_STD * cos_lat0;
-        y[k] = (la[k] - lat0) * DEG2RAD * R_STD;
-    }
-    double px = wrap180(lon_p - lon0) * DEG2RAD * R_STD * cos_lat0;
-    double py = (lat_p - lat0) * DEG2RAD * R_STD;
+    double sl = p.la[0] + p.la[1];
+    sl += p.la[2];
+    if (n == 4) sl += p.la[3];
+    const double lat0 = sl / (double)n;
+    const double cos_lat0 = __ldg(&m.ecos[c]).x;
+    const double x0 = wrap180(p.ln[0] - lon0) * DEG2RAD * R_STD * cos_lat0;
+    const double x1 = wrap180(p.ln[1] - lon0) * DEG2RAD * R_STD * cos_lat0;
+    const double x2 = wrap180(p.ln[2] - lon0) * DEG2RAD * R_STD * cos_lat0;
+    const double y0 = (p.la[0] - lat0) * DEG2RAD * R_STD;
+    const double y1 = (p.la[1] - lat0) * DEG2RAD * R_STD;
+    const double y2 = (p.la[2] - lat0) * DEG2RAD * R_STD;
+    const double px = wrap180(lon_p - lon0) * DEG2RAD * R_STD * cos_lat0;
+    const double py = (lat_p - lat0) * DEG2RAD * R_STD;
     double w1, w2, w3;
-    if (n == 3) {
-        bary_tri(px, py, x[0], y[0], x[1], y[1], x[2], y[2], w1, w2, w3);
-        return w1 >= BARY_EPS && w2 >= BARY_EPS && w3 >= BARY_EPS;
-    }
-    for (int i = 1; i < n - 1; ++i) {
-        bary_tri(px, py, x[0], y[0], x[i], y[i], x[i + 1], y[i + 1], w1, w2, w3);
-        if (w1 >= BARY_EPS && w2 >= BARY_EPS && w3 >= BARY_EPS) return true;
-    }
-    return false;
+    bary_tri(px, py, x0, y0, x1, y1, x2, y2, w1, w2, w3);
+    if (w1 >= BARY_EPS && w2 >= BARY_EPS && w3 >= BARY_EPS) return true;
+    if (n == 3) return false;
+    const double x3 = wrap180(p.ln[3] - lon0) * DEG2RAD * R_STD * cos_lat0;
+    const double y3 = (p.la[3] - lat0) * DEG2RAD * R_STD;
+    bary_tri(px, py, x0, y0, x2, y2, x3, y3, w1, w2, w3);
+    return w1 >= BARY_EPS && w2 >= BARY_EPS && w3 >= BARY_EPS;
 }
 
 __device__ __noinline__ int contain_two_ring(const DMesh& m, double lon_p, double lat_p, int nn);
 
 // mesh.py:2392-2470 _find_containing_element_local: the 1-ring of the anchor,
 // then its 2-ring; -1 when no element contains the point.
-__device__ __forceinline__ int contain_local(const DMesh& m, double lon_p, double lat_p, int nn) {
+__device__ __noinline__ int contain_local(const DMesh& m, double lon_p, double lat_p, int nn) {
     int s = __ldg(&m.n2e_off[nn]), e = __ldg(&m.n2e_off[nn + 1]);
     if (e == s) return -1;
     for (int k = s; k < e; ++k) {

@@ -1,7 +1,7 @@
 // Device-side interpolation, time blending, vertical helpers, the counter RNG
 // and the great-circle diffusion kick of the KELP time-stepping path.  Same
 // floating-point operation order as the cited Numba functions (see the note
-// at the top of kc_geom.cuh on -fmad=false).
+// at the top of kc_geom.cuh on -fmad=false and the trigonometric tables).
 #pragma once
 #include "kc_geom.cuh"
 
@@ -35,87 +35,110 @@ __device__ __forceinline__ double tblend(double a, double b, double t, double al
     return (1.0 - alpha) * a0 + alpha * t;
 }
 
+// The compacted vertex ring of interpolate.py:1368-1377 (skip -1 slots and a
+// repeat of vertex 0), with coordinates.
+struct Ring {
+    int v[4];
+    double ln[4], la[4];
+    int n;
+};
+
+__device__ __forceinline__ void put_ring(Ring& r, int n, int nd, double2 a) {
+    if (n == 0) { r.v[0] = nd; r.ln[0] = a.x; r.la[0] = a.y; }
+    else if (n == 1) { r.v[1] = nd; r.ln[1] = a.x; r.la[1] = a.y; }
+    else if (n == 2) { r.v[2] = nd; r.ln[2] = a.x; r.la[2] = a.y; }
+    else { r.v[3] = nd; r.ln[3] = a.x; r.la[3] = a.y; }
+}
+
+__device__ __forceinline__ void load_ring(const DMesh& m, int4 e, Ring& r) {
+    int n = 0;
+    int first = -1;
+    if (e.x >= 0) { put_ring(r, n++, e.x, __ldg(&m.ll[e.x])); first = e.x; }
+    if (e.y >= 0 && !(n > 0 && e.y == first)) { put_ring(r, n++, e.y, __ldg(&m.ll[e.y])); if (first < 0) first = e.y; }
+    if (e.z >= 0 && !(n > 0 && e.z == first)) { put_ring(r, n++, e.z, __ldg(&m.ll[e.z])); if (first < 0) first = e.z; }
+    if (e.w >= 0 && !(n > 0 && e.w == first)) put_ring(r, n++, e.w, __ldg(&m.ll[e.w]));
+    if (n == 3) { r.v[3] = r.v[0]; r.ln[3] = r.ln[0]; r.la[3] = r.la[0]; }   // defined, never weighted
+    r.n = n;
+}
+
 // Vertex weights of the point in the containing element, projected around the
-// wrapped-delta centroid (interpolate.py:1376-1402).  Returns false for the
-// degenerate-triangle sentinel or an element with fewer than 3 vertices.
+// wrapped-delta centroid (interpolate.py:1376-1402) with radius R; false for
+// the degenerate-triangle sentinel or an element with fewer than 3 vertices.
 __device__ __forceinline__ bool bary_weights_core(const DMesh& m, int elem, double xp, double yp, double R,
-                                                  int* verts, double* w, int& nv) {
-    int4 e = __ldg(&m.en[elem]);
-    int raw[4] = {e.x, e.y, e.z, e.w};
-    nv = 0;
+                                                  Ring& r, double* w) {
+    load_ring(m, __ldg(&m.en[elem]), r);
+    const int nv = r.n;
+    if (nv < 3) return false;
+    const double lon_ref = r.ln[0];
+    double dsum = 0.0, lat0 = 0.0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        int nd = raw[k];
-        if (nd < 0) continue;
-        if (nv > 0 && nd == verts[0]) continue;
-        verts[nv++] = nd;
+        if (k < nv) {
+            dsum += wrap180(r.ln[k] - lon_ref);
+            lat0 += r.la[k];
+        }
     }
-    if (nv < 3) return false;
-    double ln[4], la[4];
-    for (int k = 0; k < nv; ++k) {
-        double2 p = __ldg(&m.ll[verts[k]]);
-        ln[k] = p.x;
-        la[k] = p.y;
-    }
-    double lon_ref = ln[0];
-    double dsum = 0.0, lat0 = 0.0;
-    for (int k = 0; k < nv; ++k) {
-        dsum += wrap180(ln[k] - lon_ref);
-        lat0 += la[k];
-    }
-    double lon0 = lon_ref + dsum / (double)nv;
+    const double lon0 = lon_ref + dsum / (double)nv;
     lat0 /= (double)nv;
-    double cosl = cos(lat0 * DEG2RAD);
+    const double cosl = __ldg(&m.ecos[elem]).y;
     double vx[4], vy[4];
-    for (int k = 0; k < nv; ++k) {
-        vx[k] = wrap180(ln[k] - lon0) * DEG2RAD * R * cosl;
-        vy[k] = (la[k] - lat0) * DEG2RAD * R;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        vx[k] = wrap180(r.ln[k] - lon0) * DEG2RAD * R * cosl;
+        vy[k] = (r.la[k] - lat0) * DEG2RAD * R;
     }
-    double px = wrap180(xp - lon0) * DEG2RAD * R * cosl;
-    double py = (yp - lat0) * DEG2RAD * R;
-    return polygon_weights(px, py, vx, vy, nv, w);
+    const double px = wrap180(xp - lon0) * DEG2RAD * R * cosl;
+    const double py = (yp - lat0) * DEG2RAD * R;
+    if (nv == 3) {
+        bary_tri(px, py, vx[0], vy[0], vx[1], vy[1], vx[2], vy[2], w[0], w[1], w[2]);
+        w[3] = 0.0;
+        return !(w[0] == -1.0);
+    }
+    wachspress_quad(px, py, vx, vy, w);
+    return !(w[0] == -1.0);
 }
 
 // interpolate.py:1340-1440 _interp_barycentric_core_tinterp (row = 0) and
 // interpolate.py:1443-1529 its 3-D twin (row = the particle's layer).
 template <typename T>
-__device__ __forceinline__ bool interp_uv_bary(const DMesh& m, const DBlend<T>& f, double xp, double yp, int nn,
-                                               double time_dir, int row, double alpha, double& U, double& V) {
+__device__ __noinline__ bool interp_uv_bary(const DMesh& m, const DBlend<T>& f, double xp, double yp, int nn,
+                                            double time_dir, int row, double alpha, double& U, double& V) {
     U = 0.0;
     V = 0.0;
     int elem = contain_local(m, xp, yp, nn);
     if (elem < 0) return false;
-    int verts[4];
+    Ring r;
     double w[4];
-    int nv;
-    if (!bary_weights_core(m, elem, xp, yp, m.r_earth, verts, w, nv)) return false;
+    if (!bary_weights_core(m, elem, xp, yp, m.r_earth, r, w)) return false;
     const long long base = (long long)row * f.n;
     const double alpha0 = f.alpha0;
     const double beta0 = 1.0 - alpha0;
     const double beta = 1.0 - alpha;
     double Us = 0.0, Vs = 0.0;
-    for (int k = 0; k < nv; ++k) {
-        long long idx = base + verts[k];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (k >= r.n) break;
+        long long idx = base + r.v[k];
         double un, vn;
         if (alpha < 1e-12) {
             if (alpha0 == 0.0) {
-                un = (double)f.a.u[idx];
-                vn = (double)f.a.v[idx];
+                un = (double)__ldg(&f.a.u[idx]);
+                vn = (double)__ldg(&f.a.v[idx]);
             } else {
-                un = beta0 * (double)f.a.u[idx] + alpha0 * (double)f.b.u[idx];
-                vn = beta0 * (double)f.a.v[idx] + alpha0 * (double)f.b.v[idx];
+                un = beta0 * (double)__ldg(&f.a.u[idx]) + alpha0 * (double)__ldg(&f.b.u[idx]);
+                vn = beta0 * (double)__ldg(&f.a.v[idx]) + alpha0 * (double)__ldg(&f.b.v[idx]);
             }
         } else if (alpha > 1.0 - 1e-12) {
-            un = (double)f.t.u[idx];
-            vn = (double)f.t.v[idx];
+            un = (double)__ldg(&f.t.u[idx]);
+            vn = (double)__ldg(&f.t.v[idx]);
         } else if (alpha0 == 0.0) {
-            un = beta * (double)f.a.u[idx] + alpha * (double)f.t.u[idx];
-            vn = beta * (double)f.a.v[idx] + alpha * (double)f.t.v[idx];
+            un = beta * (double)__ldg(&f.a.u[idx]) + alpha * (double)__ldg(&f.t.u[idx]);
+            vn = beta * (double)__ldg(&f.a.v[idx]) + alpha * (double)__ldg(&f.t.v[idx]);
         } else {
-            double ua0 = beta0 * (double)f.a.u[idx] + alpha0 * (double)f.b.u[idx];
-            double va0 = beta0 * (double)f.a.v[idx] + alpha0 * (double)f.b.v[idx];
-            un = beta * ua0 + alpha * (double)f.t.u[idx];
-            vn = beta * va0 + alpha * (double)f.t.v[idx];
+            double ua0 = beta0 * (double)__ldg(&f.a.u[idx]) + alpha0 * (double)__ldg(&f.b.u[idx]);
+            double va0 = beta0 * (double)__ldg(&f.a.v[idx]) + alpha0 * (double)__ldg(&f.b.v[idx]);
+            un = beta * ua0 + alpha * (double)__ldg(&f.t.u[idx]);
+            vn = beta * va0 + alpha * (double)__ldg(&f.t.v[idx]);
         }
         Us += w[k] * un;
         Vs += w[k] * vn;
@@ -125,23 +148,28 @@ __device__ __forceinline__ bool interp_uv_bary(const DMesh& m, const DBlend<T>& 
     return true;
 }
 
-// vertical.py:39-91 find_layer
-__device__ __forceinline__ int find_layer(const DMesh& m, double z, double bottom) {
-    const int K = m.K;
-    const double* zl = m.zlev;
-    if (K < 2) return 0;
-    if (z <= zl[0]) return 0;
-    int max_layer = K - 2;
-    for (int k = 0; k < K - 1; ++k) {
-        if (zl[k + 1] > bottom) {
-            max_layer = k - 1 > 0 ? k - 1 : 0;
-            break;
-        }
+// First k in [lo, hi] with z < zl[k + 1] (the caller guarantees one exists):
+// the linear scans of the reference as a binary search over the monotone
+// interface table (same index).
+__device__ __forceinline__ int first_above(const double* __restrict__ zl, int lo, int hi, double z) {
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (z < __ldg(&zl[mid + 1])) hi = mid;
+        else lo = mid + 1;
     }
-    if (z >= bottom || z >= zl[max_layer + 1]) return max_layer;
-    for (int k = 0; k <= max_layer; ++k)
-        if (z < zl[k + 1]) return k;
-    return max_layer;
+    return lo;
+}
+
+// vertical.py:39-91 find_layer; the deepest valid layer of the node (the
+// reference's first scan) comes from a host table.
+__device__ __forceinline__ int find_layer(const DMesh& m, double z, int node) {
+    const int K = m.K;
+    if (K < 2) return 0;
+    if (z <= __ldg(&m.zlev[0])) return 0;
+    const int max_layer = __ldg(&m.max_layer[node]);
+    const double bottom = __ldg(&m.depth[node]);
+    if (z >= bottom || z >= __ldg(&m.zlev[max_layer + 1])) return max_layer;
+    return first_above(m.zlev, 0, max_layer, z);
 }
 
 // vertical.py:1064-1098 _interp_w_linear_single_tinterp
@@ -153,119 +181,106 @@ __device__ __forceinline__ double w_linear(const DMesh& m, const DBlend<T>& f, d
     const long long n = f.n;
     auto at = [&](int k) {
         long long idx = (long long)k * n + node;
-        return tblend((double)f.a.w[idx], (double)f.b.w[idx], (double)f.t.w[idx], f.alpha0, alpha);
+        return tblend((double)__ldg(&f.a.w[idx]), (double)__ldg(&f.b.w[idx]), (double)__ldg(&f.t.w[idx]),
+                      f.alpha0, alpha);
     };
     if (K < 2) return time_dir * at(0);
-    if (z <= zl[0]) return time_dir * at(0);
-    if (z >= zl[K - 1]) return time_dir * at(K - 1);
-    int k = K - 2;
-    for (int j = 0; j < K - 1; ++j) {
-        if (z < zl[j + 1]) { k = j; break; }
-    }
-    double dz = zl[k + 1] - zl[k];
+    if (z <= __ldg(&zl[0])) return time_dir * at(0);
+    if (z >= __ldg(&zl[K - 1])) return time_dir * at(K - 1);
+    const int k = first_above(zl, 0, K - 2, z);
+    const double zk = __ldg(&zl[k]), zk1 = __ldg(&zl[k + 1]);
+    const double dz = zk1 - zk;
     if (dz < 1e-12) return time_dir * at(k);
-    double a = (z - zl[k]) / dz;
-    double w_lo = at(k);
-    double w_hi = at(k + 1);
+    const double a = (z - zk) / dz;
+    const double w_lo = at(k);
+    const double w_hi = at(k + 1);
     return time_dir * ((1.0 - a) * w_lo + a * w_hi);
 }
 
 // Python's min(a, b): the first argument unless the second is smaller.
 __device__ __forceinline__ double pymin(double a, double b) { return b < a ? b : a; }
 
-// mesh.py:1973-2003 _seam_safe_lon0
-__device__ __forceinline__ double seam_safe_lon0(const double* ln, int n) {
-    double first = ln[0], lmin = first, lmax = first, s = 0.0;
-    for (int v = 0; v < n; ++v) {
-        double x = ln[v];
-        s += x;
-        if (x < lmin) lmin = x;
-        if (x > lmax) lmax = x;
-    }
-    if (lmax - lmin > 180.0) {
-        double d = 0.0;
-        for (int v = 0; v < n; ++v) d += wrap180(ln[v] - first);
-        return first + d / (double)n;
-    }
-    return s / (double)n;
-}
-
 // vertical.py:744-881 _interp_w_bary_single_tinterp: the anchor's own fan
-// search (denominator tolerance 1e-14, R = 6371000), triangles blended
-// inline, quads through Wachspress, nearest-node fallback.
+// search (denominator tolerance 1e-14, R = 6371000, origin by
+// mesh.py:1973-2003 _seam_safe_lon0), triangles blended inline, quads through
+// Wachspress, nearest-node fallback.
 template <typename T>
 __device__ __noinline__ double w_bary(const DMesh& m, const DBlend<T>& f, double alpha, double xp, double yp,
                                       double z, int node, double time_dir) {
-    int s = m.n2e_off[node], e = m.n2e_off[node + 1];
-    if (e == s) {
-        double zc = pymin(z, m.depth[node]);
-        return w_linear(m, f, alpha, zc, node, time_dir);
-    }
+    int s = __ldg(&m.n2e_off[node]), e = __ldg(&m.n2e_off[node + 1]);
     for (int kk = s; kk < e; ++kk) {
-        int el = m.n2e[kk];
-        int4 en = m.en[el];
-        int raw[4] = {en.x, en.y, en.z, en.w};
-        int verts[4];
-        int nvv = 0;
-        for (int v = 0; v < 4; ++v) {
-            int nd = raw[v];
-            if (nd < 0) continue;
-            if (nvv > 0 && nd == verts[0]) continue;
-            verts[nvv++] = nd;
-        }
+        const int el = __ldg(&m.n2e[kk]);
+        Ring r;
+        load_ring(m, __ldg(&m.en[el]), r);
+        const int nvv = r.n;
         if (nvv < 3) continue;
-        double ln[4], la[4];
-        for (int v = 0; v < nvv; ++v) {
-            double2 p = m.ll[verts[v]];
-            ln[v] = p.x;
-            la[v] = p.y;
+        double lmin = fmin(fmin(r.ln[0], r.ln[1]), r.ln[2]), lmax = fmax(fmax(r.ln[0], r.ln[1]), r.ln[2]);
+        if (nvv == 4) { lmin = fmin(lmin, r.ln[3]); lmax = fmax(lmax, r.ln[3]); }
+        double lon0;
+        if (lmax - lmin > 180.0) {
+            double d = 0.0;
+#pragma unroll
+            for (int v = 0; v < 4; ++v)
+                if (v < nvv) d += wrap180(r.ln[v] - r.ln[0]);
+            lon0 = r.ln[0] + d / (double)nvv;
+        } else {
+            double sm = 0.0;
+#pragma unroll
+            for (int v = 0; v < 4; ++v)
+                if (v < nvv) sm += r.ln[v];
+            lon0 = sm / (double)nvv;
         }
-        double lon0 = seam_safe_lon0(ln, nvv);
         double lat0 = 0.0;
-        for (int v = 0; v < nvv; ++v) lat0 += la[v];
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+            if (v < nvv) lat0 += r.la[v];
         lat0 /= (double)nvv;
-        double cos_lat0 = cos(lat0 * DEG2RAD);
+        const double cos_lat0 = __ldg(&m.ecos[el]).y;
         const double R = 6371000.0;
         double vx[4], vy[4];
-        for (int v = 0; v < nvv; ++v) {
-            double dlon = wrap180(ln[v] - lon0);
-            double dlat = la[v] - lat0;
-            vx[v] = dlon * DEG2RAD * R * cos_lat0;
-            vy[v] = dlat * DEG2RAD * R;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            vx[v] = wrap180(r.ln[v] - lon0) * DEG2RAD * R * cos_lat0;
+            vy[v] = (r.la[v] - lat0) * DEG2RAD * R;
         }
-        double px = wrap180(xp - lon0) * DEG2RAD * R * cos_lat0;
-        double py = (yp - lat0) * DEG2RAD * R;
-        for (int t = 0; t < nvv - 2; ++t) {
-            int i1 = t + 1, i2 = t + 2;
-            double ax = vx[0], ay = vy[0], bx = vx[i1], by = vy[i1], cx = vx[i2], cy = vy[i2];
-            double denom = (by - cy) * (ax - cx) + (cx - bx) * (ay - cy);
+        const double px = wrap180(xp - lon0) * DEG2RAD * R * cos_lat0;
+        const double py = (yp - lat0) * DEG2RAD * R;
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+            if (t >= nvv - 2) break;
+            const int i1 = t + 1, i2 = t + 2;
+            const double ax = vx[0], ay = vy[0];
+            const double bx = t == 0 ? vx[1] : vx[2], by = t == 0 ? vy[1] : vy[2];
+            const double cx = t == 0 ? vx[2] : vx[3], cy = t == 0 ? vy[2] : vy[3];
+            const double denom = (by - cy) * (ax - cx) + (cx - bx) * (ay - cy);
             if (fabs(denom) < 1e-14) continue;
-            double w1 = ((by - cy) * (px - cx) + (cx - bx) * (py - cy)) / denom;
-            double w2 = ((cy - ay) * (px - cx) + (ax - cx) * (py - cy)) / denom;
-            double w3 = 1.0 - w1 - w2;
+            const double w1 = ((by - cy) * (px - cx) + (cx - bx) * (py - cy)) / denom;
+            const double w2 = ((cy - ay) * (px - cx) + (ax - cx) * (py - cy)) / denom;
+            const double w3 = 1.0 - w1 - w2;
             const double eps = -1e-6;
             if (w1 >= eps && w2 >= eps && w3 >= eps) {
                 if (nvv == 4) {
                     double wts[4];
-                    polygon_weights(px, py, vx, vy, 4, wts);
+                    wachspress_quad(px, py, vx, vy, wts);
                     double acc = 0.0;
+#pragma unroll
                     for (int vi = 0; vi < 4; ++vi) {
-                        int nvn = verts[vi];
-                        double z_nv = pymin(z, m.depth[nvn]);
-                        acc += wts[vi] * w_linear(m, f, alpha, z_nv, nvn, time_dir);
+                        const int nvn = r.v[vi];
+                        acc += wts[vi] * w_linear(m, f, alpha, pymin(z, __ldg(&m.depth[nvn])), nvn, time_dir);
                     }
                     return acc;
                 }
-                int n0 = verts[0], n1 = verts[i1], n2 = verts[i2];
-                double w_v0 = w_linear(m, f, alpha, pymin(z, m.depth[n0]), n0, time_dir);
-                double w_v1 = w_linear(m, f, alpha, pymin(z, m.depth[n1]), n1, time_dir);
-                double w_v2 = w_linear(m, f, alpha, pymin(z, m.depth[n2]), n2, time_dir);
+                const int n0 = r.v[0];
+                const int n1 = i1 == 1 ? r.v[1] : r.v[2];
+                const int n2 = i2 == 2 ? r.v[2] : r.v[3];
+                const double w_v0 = w_linear(m, f, alpha, pymin(z, __ldg(&m.depth[n0])), n0, time_dir);
+                const double w_v1 = w_linear(m, f, alpha, pymin(z, __ldg(&m.depth[n1])), n1, time_dir);
+                const double w_v2 = w_linear(m, f, alpha, pymin(z, __ldg(&m.depth[n2])), n2, time_dir);
                 return w1 * w_v0 + w2 * w_v1 + w3 * w_v2;
             }
         }
     }
-    double zc = pymin(z, m.depth[node]);
-    return w_linear(m, f, alpha, zc, node, time_dir);
+    return w_linear(m, f, alpha, pymin(z, __ldg(&m.depth[node])), node, time_dir);
 }
 
 // ---------------------------------------------------------------------------
@@ -306,16 +321,16 @@ __device__ __forceinline__ void normal_pair(uint64_t seed, uint64_t real_id, uin
 
 constexpr double R_METRIC = SLM / DEG2RAD;
 
-// diffusion.py:538-575 sphere_displace (exponential map of the tangent kick)
-__device__ __forceinline__ void sphere_displace(double lon, double lat, double dx, double dy,
-                                                double& lon2, double& lat2) {
+// diffusion.py:538-575 sphere_displace (exponential map of the tangent kick);
+// sin/cos of the start longitude and latitude come from its evaluation site.
+__device__ __forceinline__ void sphere_displace(const Site& q, double dx, double dy, double& lon2, double& lat2) {
     double dist = sqrt(dx * dx + dy * dy);
-    if (dist == 0.0) { lon2 = lon; lat2 = lat; return; }
-    double lam = lon * DEG2RAD, phi = lat * DEG2RAD;
-    double cl = cos(lam), sl = sin(lam), cp = cos(phi), sp = sin(phi);
+    if (dist == 0.0) { lon2 = q.lon; lat2 = q.lat; return; }
+    const double cl = q.cos_lon, sl = q.sin_lon, cp = q.cos_lat, sp = q.sin_lat;
     double delta = dist / R_METRIC;
-    double c = cos(delta);
-    double s = sin(delta) / dist;
+    double sdel, c;
+    sincos(delta, &sdel, &c);
+    double s = sdel / dist;
     double tx = -sl * dx - sp * cl * dy;
     double ty = cl * dx - sp * sl * dy;
     double tz = cp * dy;

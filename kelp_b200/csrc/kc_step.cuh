@@ -3,7 +3,9 @@
 // 3-D RK2 step (z-level layers, W nearest/barycentric, surface/bottom clamp),
 // and the split uniform-Kh random-walk kick applied to the particles that
 // survived the deterministic step.  One thread owns one particle for the whole
-// step, so every intermediate stays in registers.
+// step, so every intermediate stays in registers; the searches, containment
+// and interpolation are shared (non-inlined) device functions, which keeps
+// the kernel's code footprint small under divergence.
 #pragma once
 #include "kc_interp.cuh"
 
@@ -35,9 +37,10 @@ struct DStep {
     long long global_step;     // for delayed release activation (-1: none)
 };
 
-// displacement metric z0 = max(cos(lat) * 111120, 1) (integrators.py:2563-2565)
-__device__ __forceinline__ double metric_z0(double lat) {
-    double z0 = cos(lat * DEG2RAD) * SLM;
+// displacement metric z0 = max(cos(lat) * 111120, 1) (integrators.py:2563-2565),
+// cos(lat) from the site anchored at that latitude
+__device__ __forceinline__ double metric_z0(const Site& q) {
+    double z0 = q.cos_lat * SLM;
     if (z0 < 1.0) z0 = 1.0;
     return z0;
 }
@@ -49,15 +52,13 @@ __device__ __forceinline__ double clamp_lat(double lat) {
 }
 
 // integrators.py:673-818 _apply_split_diffusion_kick for one particle that is
-// ALIVE after the deterministic step: counter-RNG kick (diffusion.py:485-529,
-// :261-298), great-circle move, exact re-anchor and containment re-check,
-// revert to the pre-step state on leaving the domain; 3-D reclamp in the new
-// column.  Returns the new status.
-template <bool IS3D>
-__device__ __forceinline__ void apply_kick(const DMesh& m, const DStep& s, long long i, long long pid,
-                                           double pre_lon, double pre_lat, double pre_z, int pre_nn,
-                                           double& lon, double& lat, double& z, int& status, int& nn,
-                                           signed char& fr) {
+// ALIVE after the deterministic step (site qn = its position): counter-RNG
+// kick (diffusion.py:485-529, :261-298), great-circle move, exact re-anchor
+// and containment re-check, revert to the pre-step state on leaving the
+// domain; 3-D reclamp in the new column.
+__device__ __noinline__ void apply_kick(const DMesh& m, const DStep& s, long long pid, const Site& qn,
+                                        double pre_lon, double pre_lat, double pre_z, int pre_nn, bool is3d,
+                                        double& lon, double& lat, double& z, int& status, int& nn, signed char& fr) {
     double g1, g2;
     normal_pair(s.seed, s.real_id, (unsigned long long)pid + s.pid_offset, s.step_i, 0ull, g1, g2);
     double abs_dt = s.dt >= 0.0 ? s.dt : -s.dt;
@@ -74,10 +75,10 @@ __device__ __forceinline__ void apply_kick(const DMesh& m, const DStep& s, long 
         dy = dy + corr;
     }
     double lk, lak;
-    sphere_displace(lon, lat, dx, dy, lk, lak);
-    int nk = site_anchor(m, lk, lak);
-    bool in_dom = contain_local(m, lk, lak, nk) >= 0;
-    if (!in_dom) {
+    sphere_displace(qn, dx, dy, lk, lak);
+    Site qk = make_site(lk, lak);
+    int nk = site_anchor(m, qk);
+    if (contain_local(m, lk, lak, nk) < 0) {
         status = OUTSIDE;
         lon = pre_lon;
         lat = pre_lat;
@@ -89,7 +90,7 @@ __device__ __forceinline__ void apply_kick(const DMesh& m, const DStep& s, long 
     lon = lk;
     lat = lak;
     nn = nk;
-    if (IS3D) {
+    if (is3d) {
         double zv = z;
         if (zv < m.zlev[0]) zv = m.zlev[0];
         double bottom = m.depth[nk];
@@ -115,9 +116,10 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
     const double dt = s.dt, td = s.time_dir;
     double lon_new = lon0, lat_new = lat0;
     int nn_out = pre_nn;
-    signed char fr = st.fr ? st.fr[i] : 0;
+    signed char fr = st.fr[i];
     bool failed = false;
-    int node_i = site_anchor(m, lon0, lat0);
+    const Site q0 = make_site(lon0, lat0);
+    const int node_i = site_anchor(m, q0);
 
     double U1, V1;
     bool ok1 = interp_uv_bary<T>(m, f, lon0, lat0, node_i, td, 0, s.ak[0], U1, V1);
@@ -126,64 +128,49 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
     if (!ok1) {
         status = OUTSIDE; fr = FR_INTERP; nn_out = node_i; failed = true;
     } else if (SCHEME == 0) {
-        double z0 = metric_z0(lat0);
-        double ln = lon0 + dt * U1 / z0;
-        double lt = lat0 + dt * V1 / SLM;
-        ln = wrap180(ln);
-        lt = clamp_lat(lt);
-        lon_new = ln;
-        lat_new = lt;
+        lon_new = wrap180(lon0 + dt * U1 / metric_z0(q0));
+        lat_new = clamp_lat(lat0 + dt * V1 / SLM);
     } else if (SCHEME == 1) {
-        double z0 = metric_z0(lat0);
-        double lon_mid = lon0 + 0.5 * dt * U1 / z0;
-        double lat_mid = lat0 + 0.5 * dt * V1 / SLM;
-        lon_mid = wrap180(lon_mid);
-        lat_mid = clamp_lat(lat_mid);
-        int nn_mid = site_anchor(m, lon_mid, lat_mid);
+        double lon_mid = wrap180(lon0 + 0.5 * dt * U1 / metric_z0(q0));
+        double lat_mid = clamp_lat(lat0 + 0.5 * dt * V1 / SLM);
+        const Site qm = make_site(lon_mid, lat_mid);
+        int nn_mid = site_anchor(m, qm);
         double U2, V2;
-        bool ok2 = interp_uv_bary<T>(m, f, lon_mid, lat_mid, nn_mid, td, 0, s.ak[1], U2, V2);
-        if (!ok2) {
+        if (!interp_uv_bary<T>(m, f, lon_mid, lat_mid, nn_mid, td, 0, s.ak[1], U2, V2)) {
             status = OUTSIDE; fr = FR_INTERP; nn_out = node_i; failed = true;
         } else {
-            double z0m = metric_z0(lat_mid);
-            double ln = lon0 + dt * U2 / z0m;
-            double lt = lat0 + dt * V2 / SLM;
-            lon_new = wrap180(ln);
-            lat_new = clamp_lat(lt);
+            lon_new = wrap180(lon0 + dt * U2 / metric_z0(qm));
+            lat_new = clamp_lat(lat0 + dt * V2 / SLM);
         }
     } else {
-        double z0_1 = metric_z0(lat0);
-        double dlon1 = dt * U1 / z0_1;
+        double dlon1 = dt * U1 / metric_z0(q0);
         double dlat1 = dt * V1 / SLM;
         double lon2 = wrap180(lon0 + 0.5 * dlon1);
         double lat2 = clamp_lat(lat0 + 0.5 * dlat1);
-        int nn2 = site_anchor(m, lon2, lat2);
+        const Site q2 = make_site(lon2, lat2);
         double U2, V2;
-        if (!interp_uv_bary<T>(m, f, lon2, lat2, nn2, td, 0, s.ak[1], U2, V2)) {
+        if (!interp_uv_bary<T>(m, f, lon2, lat2, site_anchor(m, q2), td, 0, s.ak[1], U2, V2)) {
             status = OUTSIDE; fr = FR_INTERP; nn_out = node_i; failed = true;
         } else {
-            double z0_2 = metric_z0(lat2);
-            double dlon2 = dt * U2 / z0_2;
+            double dlon2 = dt * U2 / metric_z0(q2);
             double dlat2 = dt * V2 / SLM;
             double lon3 = wrap180(lon0 + 0.5 * dlon2);
             double lat3 = clamp_lat(lat0 + 0.5 * dlat2);
-            int nn3 = site_anchor(m, lon3, lat3);
+            const Site q3 = make_site(lon3, lat3);
             double U3, V3;
-            if (!interp_uv_bary<T>(m, f, lon3, lat3, nn3, td, 0, s.ak[2], U3, V3)) {
+            if (!interp_uv_bary<T>(m, f, lon3, lat3, site_anchor(m, q3), td, 0, s.ak[2], U3, V3)) {
                 status = OUTSIDE; fr = FR_INTERP; nn_out = node_i; failed = true;
             } else {
-                double z0_3 = metric_z0(lat3);
-                double dlon3 = dt * U3 / z0_3;
+                double dlon3 = dt * U3 / metric_z0(q3);
                 double dlat3 = dt * V3 / SLM;
                 double lon4 = wrap180(lon0 + dlon3);
                 double lat4 = clamp_lat(lat0 + dlat3);
-                int nn4 = site_anchor(m, lon4, lat4);
+                const Site q4 = make_site(lon4, lat4);
                 double U4, V4;
-                if (!interp_uv_bary<T>(m, f, lon4, lat4, nn4, td, 0, s.ak[3], U4, V4)) {
+                if (!interp_uv_bary<T>(m, f, lon4, lat4, site_anchor(m, q4), td, 0, s.ak[3], U4, V4)) {
                     status = OUTSIDE; fr = FR_INTERP; nn_out = node_i; failed = true;
                 } else {
-                    double z0_4 = metric_z0(lat4);
-                    double dlon4 = dt * U4 / z0_4;
+                    double dlon4 = dt * U4 / metric_z0(q4);
                     double dlat4 = dt * V4 / SLM;
                     double dlon = (dlon1 + 2.0 * dlon2 + 2.0 * dlon3 + dlon4) / 6.0;
                     double dlat = (dlat1 + 2.0 * dlat2 + 2.0 * dlat3 + dlat4) / 6.0;
@@ -194,30 +181,30 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
         }
     }
     if (!failed) {
-        int nn_new = site_anchor(m, lon_new, lat_new);
+        const Site qn = make_site(lon_new, lat_new);
+        int nn_new = site_anchor(m, qn);
         if (contain_local(m, lon_new, lat_new, nn_new) < 0) {
             status = OUTSIDE; fr = FR_OOB; nn_out = node_i;
             lon_new = lon0; lat_new = lat0;
         } else {
             status = ALIVE;
             nn_out = nn_new;
+            if (s.kick) {
+                double zz = 0.0;
+                long long pid = st.pid ? st.pid[i] : i;
+                apply_kick(m, s, pid, qn, lon0, lat0, 0.0, pre_nn, false, lon_new, lat_new, zz, status, nn_out, fr);
+            }
         }
     } else {
         lon_new = lon0;
         lat_new = lat0;
     }
-    if (s.kick && status == ALIVE) {
-        double zz = 0.0;
-        long long pid = st.pid ? st.pid[i] : i;
-        apply_kick<false>(m, s, i, pid, lon0, lat0, 0.0, pre_nn, lon_new, lat_new, zz, status, nn_out, fr);
-    }
     st.lon[i] = lon_new;
     st.lat[i] = lat_new;
     st.status[i] = status;
     st.nn[i] = nn_out;
-    if (st.fr) st.fr[i] = fr;
+    st.fr[i] = fr;
 }
-
 
 template <typename T>
 __device__ __forceinline__ double stage_w(const DMesh& m, const DBlend<T>& f, int w_code, double alpha,
@@ -244,54 +231,52 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
     const double dt = s.dt, td = s.time_dir;
     signed char fr = st.fr[i];
     double lon_new = lon0, lat_new = lat0, z_new = z0p;
-    int nn_out;
-    bool failed = true;
 
-    int node_i = site_anchor(m, lon0, lat0);
-    nn_out = node_i;
-    int layer1 = find_layer(m, z0p, m.depth[node_i]);
+    const Site q0 = make_site(lon0, lat0);
+    const int node_i = site_anchor(m, q0);
+    int nn_out = node_i;
+    const int layer1 = find_layer(m, z0p, node_i);
     double U1, V1;
-    bool ok1 = interp_uv_bary<T>(m, f, lon0, lat0, node_i, td, layer1, s.ak[0], U1, V1);
-    double W1 = stage_w<T>(m, f, s.w_code, s.ak[0], lon0, lat0, z0p, node_i, td);
+    const bool ok1 = interp_uv_bary<T>(m, f, lon0, lat0, node_i, td, layer1, s.ak[0], U1, V1);
+    const double W1 = stage_w<T>(m, f, s.w_code, s.ak[0], lon0, lat0, z0p, node_i, td);
     st.U[i] = U1;
     st.V[i] = V1;
     st.W[i] = W1;
     if (!ok1) {
         status = OUTSIDE; fr = FR_INTERP;
     } else {
-        double z0 = metric_z0(lat0);
-        double lon_mid = wrap180(lon0 + 0.5 * dt * U1 / z0);
-        double lat_mid = clamp_lat(lat0 + 0.5 * dt * V1 / SLM);
-        double z_mid = z0p + W1 * 0.5 * dt;
-        int nn_mid = site_anchor(m, lon_mid, lat_mid);
-        int layer2 = find_layer(m, z_mid, m.depth[nn_mid]);
+        const double lon_mid = wrap180(lon0 + 0.5 * dt * U1 / metric_z0(q0));
+        const double lat_mid = clamp_lat(lat0 + 0.5 * dt * V1 / SLM);
+        const double z_mid = z0p + W1 * 0.5 * dt;
+        const Site qm = make_site(lon_mid, lat_mid);
+        const int nn_mid = site_anchor(m, qm);
+        const int layer2 = find_layer(m, z_mid, nn_mid);
         double U2, V2;
         if (!interp_uv_bary<T>(m, f, lon_mid, lat_mid, nn_mid, td, layer2, s.ak[1], U2, V2)) {
             status = OUTSIDE; fr = FR_INTERP;
         } else {
-            double W2 = stage_w<T>(m, f, s.w_code, s.ak[1], lon_mid, lat_mid, z_mid, nn_mid, td);
-            double z0m = metric_z0(lat_mid);
-            double ln = wrap180(lon0 + dt * U2 / z0m);
-            double lt = clamp_lat(lat0 + dt * V2 / SLM);
+            const double W2 = stage_w<T>(m, f, s.w_code, s.ak[1], lon_mid, lat_mid, z_mid, nn_mid, td);
+            const double ln = wrap180(lon0 + dt * U2 / metric_z0(qm));
+            const double lt = clamp_lat(lat0 + dt * V2 / SLM);
             double zn = z0p + W2 * dt;
-            int nn_new = site_anchor(m, ln, lt);
+            const Site qn = make_site(ln, lt);
+            const int nn_new = site_anchor(m, qn);
             if (contain_local(m, ln, lt, nn_new) < 0) {
                 status = OUTSIDE; fr = FR_OOB;
             } else {
                 if (zn < m.zlev[0]) zn = m.zlev[0];
-                double bottom = m.depth[nn_new];
+                const double bottom = m.depth[nn_new];
                 if (zn > bottom) zn = bottom;
                 lon_new = ln; lat_new = lt; z_new = zn;
                 status = ALIVE;
                 nn_out = nn_new;
-                failed = false;
+                if (s.kick) {
+                    long long pid = st.pid ? st.pid[i] : i;
+                    apply_kick(m, s, pid, qn, lon0, lat0, z0p, pre_nn, true, lon_new, lat_new, z_new, status,
+                               nn_out, fr);
+                }
             }
         }
-    }
-    (void)failed;
-    if (s.kick && status == ALIVE) {
-        long long pid = st.pid ? st.pid[i] : i;
-        apply_kick<true>(m, s, i, pid, lon0, lat0, z0p, pre_nn, lon_new, lat_new, z_new, status, nn_out, fr);
     }
     st.lon[i] = lon_new;
     st.lat[i] = lat_new;
