@@ -121,6 +121,13 @@ int kc_particles_download(kc_ctx* ctx, long long P, double* lon, double* lat, do
 int kc_step(kc_ctx* ctx, const kc_step_args* args);
 int kc_run(kc_ctx* ctx, const kc_step_args* steps, int n_steps);
 
+/* Re-order the resident particles by grid-hash cell (particles that left the
+ * domain last) so that a warp's particles share hash windows and elements.
+ * Results do not depend on the order: every particle keeps its RNG key, and
+ * kc_particles_download returns the upload order.  No reference counterpart
+ * (the reference's utils/sort_seeds.py sorts seed files offline). */
+int kc_sort(kc_ctx* ctx);
+
 /* Batch exact nearest node of P query points (host arrays). */
 int kc_find_nearest(kc_ctx* ctx, long long P, const double* lon, const double* lat, int* out);
 

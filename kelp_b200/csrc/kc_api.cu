@@ -7,6 +7,7 @@
 #include <vector>
 #include <algorithm>
 #include <cuda_runtime.h>
+#include <cub/device/device_radix_sort.cuh>
 
 #include "../../include/kelp_cuda.h"
 #include "kc_host.h"
@@ -59,6 +60,16 @@ struct kc_ctx {
     signed char* fr = nullptr;
     long long* pid = nullptr;
     bool has_pid = false, has_rs = false;
+    // re-sort by grid-hash cell: upload slot of every resident particle, the
+    // spare buffer of the gathers, radix-sort keys / indices and CUB's storage
+    long long* orig = nullptr;
+    void* spare = nullptr;
+    bool sorted = false;
+    unsigned* skey[2] = {nullptr, nullptr};
+    int* sidx[2] = {nullptr, nullptr};
+    void* cub_tmp = nullptr;
+    size_t cub_bytes = 0;
+    long long sort_cap = 0;
     // query scratch of kc_find_nearest
     double* q = nullptr;
     int* qout = nullptr;
@@ -155,7 +166,74 @@ __global__ void __launch_bounds__(kBlock) k_normals(long long P, unsigned long l
     out[2 * i + 1] = g2;
 }
 
+__global__ void k_iota64(long long* out, long long P) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < P) out[i] = i;
+}
+
+// Sort key of the periodic re-sort: the grid-hash cell of the particle's
+// position (mesh.py:1210-1232); particles that left the domain go last.
+__global__ void __launch_bounds__(kBlock) k_sort_keys(const __grid_constant__ kc::DMesh m, const double* lon,
+                                                      const double* lat, const int* status, long long P,
+                                                      unsigned* key, int* idx) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P) return;
+    unsigned k = 0xFFFFFFFFu;
+    if (status[i] != kc::OUTSIDE) {
+        int ci, cj;
+        kc::gh_cell_of(m, lon[i], lat[i], ci, cj);
+        k = (unsigned)(cj * m.nx + ci);
+    }
+    key[i] = k;
+    idx[i] = (int)i;
+}
+
+template <typename T>
+__global__ void k_gather(const T* __restrict__ src, T* __restrict__ dst, const int* __restrict__ idx, long long P) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < P) dst[i] = src[idx[i]];
+}
+
+template <typename T>
+__global__ void k_scatter(const T* __restrict__ src, T* __restrict__ dst, const long long* __restrict__ to,
+                          long long P) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < P) dst[to[i]] = src[i];
+}
+
 unsigned grid_for(long long n) { return (unsigned)((n + kBlock - 1) / kBlock); }
+
+// Gather one per-particle array into the spare buffer by the sort's index and
+// swap the two buffers (all are sized 8 bytes per particle).
+int regather(kc_ctx* c, void** arr, int es, const int* idx) {
+    const long long P = c->P;
+    unsigned g = grid_for(P);
+    if (es == 8) k_gather<long long><<<g, kBlock, 0, c->stream>>>((const long long*)*arr, (long long*)c->spare, idx, P);
+    else if (es == 4) k_gather<int><<<g, kBlock, 0, c->stream>>>((const int*)*arr, (int*)c->spare, idx, P);
+    else k_gather<signed char><<<g, kBlock, 0, c->stream>>>((const signed char*)*arr, (signed char*)c->spare, idx, P);
+    KC_CUDA(c, cudaGetLastError());
+    std::swap(*arr, c->spare);
+    return KC_OK;
+}
+
+// Copy one per-particle array to the host in upload order (scattered back
+// through the upload slots after a re-sort).
+int fetch(kc_ctx* c, void* host, const void* dev, int es) {
+    if (!host) return KC_OK;
+    const long long P = c->P;
+    const void* src = dev;
+    if (c->sorted) {
+        unsigned g = grid_for(P);
+        if (es == 8) k_scatter<long long><<<g, kBlock, 0, c->stream>>>((const long long*)dev, (long long*)c->spare, c->orig, P);
+        else if (es == 4) k_scatter<int><<<g, kBlock, 0, c->stream>>>((const int*)dev, (int*)c->spare, c->orig, P);
+        else k_scatter<signed char><<<g, kBlock, 0, c->stream>>>((const signed char*)dev, (signed char*)c->spare, c->orig, P);
+        KC_CUDA(c, cudaGetLastError());
+        src = c->spare;
+    }
+    KC_CUDA(c, cudaMemcpyAsync(host, src, (size_t)P * es, cudaMemcpyDeviceToHost, c->stream));
+    if (c->sorted) KC_CUDA(c, cudaStreamSynchronize(c->stream));   // the spare buffer is reused next
+    return KC_OK;
+}
 
 template <typename T>
 int launch_step(kc_ctx* c, const kc_step_args* a) {
@@ -236,7 +314,10 @@ void free_mesh(kc_ctx* c) {
 void free_particles(kc_ctx* c) {
     dfree(c->lon); dfree(c->lat); dfree(c->z); dfree(c->U); dfree(c->V); dfree(c->W);
     dfree(c->status); dfree(c->nn); dfree(c->fr); dfree(c->pid); dfree(c->rs);
-    c->P = c->cap = 0;
+    dfree(c->orig); dfree(c->spare);
+    dfree(c->skey[0]); dfree(c->skey[1]); dfree(c->sidx[0]); dfree(c->sidx[1]); dfree(c->cub_tmp);
+    c->P = c->cap = c->sort_cap = 0;
+    c->sorted = false;
 }
 
 }  // namespace
@@ -416,19 +497,25 @@ int kc_particles_upload(kc_ctx* c, long long P, const double* lon, const double*
     if (P > c->cap) {
         KC_CUDA(c, cudaStreamSynchronize(c->stream));
         free_particles(c);
-        size_t n = (size_t)P;
-        KC_CUDA(c, cudaMalloc((void**)&c->lon, n * 8)); KC_CUDA(c, cudaMalloc((void**)&c->lat, n * 8));
-        KC_CUDA(c, cudaMalloc((void**)&c->z, n * 8)); KC_CUDA(c, cudaMalloc((void**)&c->U, n * 8));
-        KC_CUDA(c, cudaMalloc((void**)&c->V, n * 8)); KC_CUDA(c, cudaMalloc((void**)&c->W, n * 8));
-        KC_CUDA(c, cudaMalloc((void**)&c->status, n * 4)); KC_CUDA(c, cudaMalloc((void**)&c->nn, n * 4));
-        KC_CUDA(c, cudaMalloc((void**)&c->fr, n)); KC_CUDA(c, cudaMalloc((void**)&c->pid, n * 8));
-        KC_CUDA(c, cudaMalloc((void**)&c->rs, n * 4));
+        // every per-particle buffer holds 8 bytes per particle, so the re-sort
+        // can gather any array into the spare buffer and swap the pointers
+        size_t n = (size_t)P * 8;
+        KC_CUDA(c, cudaMalloc((void**)&c->lon, n)); KC_CUDA(c, cudaMalloc((void**)&c->lat, n));
+        KC_CUDA(c, cudaMalloc((void**)&c->z, n)); KC_CUDA(c, cudaMalloc((void**)&c->U, n));
+        KC_CUDA(c, cudaMalloc((void**)&c->V, n)); KC_CUDA(c, cudaMalloc((void**)&c->W, n));
+        KC_CUDA(c, cudaMalloc((void**)&c->status, n)); KC_CUDA(c, cudaMalloc((void**)&c->nn, n));
+        KC_CUDA(c, cudaMalloc((void**)&c->fr, n)); KC_CUDA(c, cudaMalloc((void**)&c->pid, n));
+        KC_CUDA(c, cudaMalloc((void**)&c->rs, n)); KC_CUDA(c, cudaMalloc((void**)&c->orig, n));
+        KC_CUDA(c, cudaMalloc((void**)&c->spare, n));
         c->cap = P;
     }
     c->P = P;
+    c->sorted = false;
     if (P == 0) return KC_OK;
     size_t n = (size_t)P;
     cudaStream_t s = c->stream;
+    k_iota64<<<grid_for(P), kBlock, 0, s>>>(c->orig, P);
+    KC_CUDA(c, cudaGetLastError());
     KC_CUDA(c, cudaMemcpyAsync(c->lon, lon, n * 8, cudaMemcpyHostToDevice, s));
     KC_CUDA(c, cudaMemcpyAsync(c->lat, lat, n * 8, cudaMemcpyHostToDevice, s));
     if (z) KC_CUDA(c, cudaMemcpyAsync(c->z, z, n * 8, cudaMemcpyHostToDevice, s));
@@ -453,18 +540,67 @@ int kc_particles_download(kc_ctx* c, long long P, double* lon, double* lat, doub
     if (P != c->P) return fail(c, KC_ERR_ARG, "kc_particles_download: P differs from the resident count");
     if (P == 0) return KC_OK;
     KC_CUDA(c, cudaSetDevice(c->device));
-    size_t n = (size_t)P;
+    int rc;
+    if ((rc = fetch(c, lon, c->lon, 8))) return rc;
+    if ((rc = fetch(c, lat, c->lat, 8))) return rc;
+    if ((rc = fetch(c, z, c->z, 8))) return rc;
+    if ((rc = fetch(c, status, c->status, 4))) return rc;
+    if ((rc = fetch(c, nn, c->nn, 4))) return rc;
+    if ((rc = fetch(c, fr, c->fr, 1))) return rc;
+    if ((rc = fetch(c, u, c->U, 8))) return rc;
+    if ((rc = fetch(c, v, c->V, 8))) return rc;
+    if ((rc = fetch(c, w, c->W, 8))) return rc;
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KC_OK;
+}
+
+int kc_sort(kc_ctx* c) {
+    if (!c) return KC_ERR_ARG;
+    if (!c->has_mesh) return fail(c, KC_ERR_STATE, "kc_sort: no mesh uploaded");
+    const long long P = c->P;
+    if (P <= 1) return KC_OK;
+    KC_CUDA(c, cudaSetDevice(c->device));
     cudaStream_t s = c->stream;
-    if (lon) KC_CUDA(c, cudaMemcpyAsync(lon, c->lon, n * 8, cudaMemcpyDeviceToHost, s));
-    if (lat) KC_CUDA(c, cudaMemcpyAsync(lat, c->lat, n * 8, cudaMemcpyDeviceToHost, s));
-    if (z) KC_CUDA(c, cudaMemcpyAsync(z, c->z, n * 8, cudaMemcpyDeviceToHost, s));
-    if (status) KC_CUDA(c, cudaMemcpyAsync(status, c->status, n * 4, cudaMemcpyDeviceToHost, s));
-    if (nn) KC_CUDA(c, cudaMemcpyAsync(nn, c->nn, n * 4, cudaMemcpyDeviceToHost, s));
-    if (fr) KC_CUDA(c, cudaMemcpyAsync(fr, c->fr, n, cudaMemcpyDeviceToHost, s));
-    if (u) KC_CUDA(c, cudaMemcpyAsync(u, c->U, n * 8, cudaMemcpyDeviceToHost, s));
-    if (v) KC_CUDA(c, cudaMemcpyAsync(v, c->V, n * 8, cudaMemcpyDeviceToHost, s));
-    if (w) KC_CUDA(c, cudaMemcpyAsync(w, c->W, n * 8, cudaMemcpyDeviceToHost, s));
-    KC_CUDA(c, cudaStreamSynchronize(s));
+    if (P > c->sort_cap) {
+        KC_CUDA(c, cudaStreamSynchronize(s));
+        dfree(c->skey[0]); dfree(c->skey[1]); dfree(c->sidx[0]); dfree(c->sidx[1]); dfree(c->cub_tmp);
+        for (int k = 0; k < 2; ++k) {
+            KC_CUDA(c, cudaMalloc((void**)&c->skey[k], (size_t)P * 4));
+            KC_CUDA(c, cudaMalloc((void**)&c->sidx[k], (size_t)P * 4));
+        }
+        size_t tmp = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, tmp, c->skey[0], c->skey[1], c->sidx[0], c->sidx[1], (int)P, 0, 32, s);
+        KC_CUDA(c, cudaMalloc(&c->cub_tmp, tmp));
+        c->cub_bytes = tmp;
+        c->sort_cap = P;
+    }
+    if (!c->has_pid) {   // the RNG key stays the slot index the particles were uploaded with
+        KC_CUDA(c, cudaMemcpyAsync(c->pid, c->orig, (size_t)P * 8, cudaMemcpyDeviceToDevice, s));
+        c->has_pid = true;
+    }
+    const long long ncell = (long long)c->dm.nx * c->dm.ny;
+    int bits = 1;
+    while (bits < 32 && (1ll << bits) <= ncell) ++bits;
+    k_sort_keys<<<grid_for(P), kBlock, 0, s>>>(c->dm, c->lon, c->lat, c->status, P, c->skey[0], c->sidx[0]);
+    KC_CUDA(c, cudaGetLastError());
+    size_t tmp = c->cub_bytes;
+    KC_CUDA(c, cub::DeviceRadixSort::SortPairs(c->cub_tmp, tmp, c->skey[0], c->skey[1], c->sidx[0], c->sidx[1],
+                                               (int)P, 0, bits, s));
+    const int* idx = c->sidx[1];
+    int rc;
+    if ((rc = regather(c, (void**)&c->lon, 8, idx))) return rc;
+    if ((rc = regather(c, (void**)&c->lat, 8, idx))) return rc;
+    if ((rc = regather(c, (void**)&c->z, 8, idx))) return rc;
+    if ((rc = regather(c, (void**)&c->U, 8, idx))) return rc;
+    if ((rc = regather(c, (void**)&c->V, 8, idx))) return rc;
+    if ((rc = regather(c, (void**)&c->W, 8, idx))) return rc;
+    if ((rc = regather(c, (void**)&c->pid, 8, idx))) return rc;
+    if ((rc = regather(c, (void**)&c->orig, 8, idx))) return rc;
+    if ((rc = regather(c, (void**)&c->status, 4, idx))) return rc;
+    if ((rc = regather(c, (void**)&c->nn, 4, idx))) return rc;
+    if ((rc = regather(c, (void**)&c->fr, 1, idx))) return rc;
+    if (c->has_rs && (rc = regather(c, (void**)&c->rs, 4, idx))) return rc;
+    c->sorted = true;
     return KC_OK;
 }
 

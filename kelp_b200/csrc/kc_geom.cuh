@@ -61,7 +61,7 @@ struct Site {
     double sin_lon, cos_lon;  // of lon * DEG2RAD
 };
 
-__device__ __forceinline__ Site make_site(double lon, double lat) {
+__device__ __noinline__ Site make_site(double lon, double lat) {
     Site s;
     s.lon = lon;
     s.lat = lat;
@@ -73,12 +73,29 @@ __device__ __forceinline__ Site make_site(double lon, double lat) {
     return s;
 }
 
-// Python float modulo for a positive divisor (CPython float_rem, Numba
-// real_divmod): the remainder carries the divisor's sign, zero is +0.
-__device__ __forceinline__ double pymod(double x, double m) {
-    double r = fmod(x, m);
+// fmod(x, 360) for |x| < 2^40 * 360 without the general remainder loop:
+// with n the integer part of |x| / 360 (corrected by one when the division
+// rounded across an integer), |x| - n * 360 is exact (n * 360 is exact, and
+// for n >= 1 Sterbenz's lemma applies: n*360/2 <= |x| <= 2 n*360), so the
+// result equals C fmod bit for bit; larger or non-finite x take fmod itself.
+__device__ __noinline__ double fmod360_slow(double x) { return fmod(x, 360.0); }
+
+__device__ __forceinline__ double fmod360(double x) {
+    double a = fabs(x);
+    if (!(a < 395824185999360.0)) return fmod360_slow(x);    // 2^40 * 360, and NaN
+    double n = trunc(a * (1.0 / 360.0));
+    double r = a - n * 360.0;
+    if (r < 0.0) r = a - (n - 1.0) * 360.0;
+    else if (r >= 360.0) r = a - (n + 1.0) * 360.0;
+    return copysign(r, x);
+}
+
+// Python float modulo by 360 (CPython float_rem, Numba real_divmod): the
+// remainder carries the divisor's sign, zero is +0.
+__device__ __forceinline__ double pymod360(double x) {
+    double r = fmod360(x);
     if (r != 0.0) {
-        if (r < 0.0) r += m;
+        if (r < 0.0) r += 360.0;
     } else {
         r = 0.0;
     }
@@ -86,7 +103,7 @@ __device__ __forceinline__ double pymod(double x, double m) {
 }
 
 // ((x + 180) % 360) - 180
-__device__ __forceinline__ double wrap180(double x) { return pymod(x + 180.0, 360.0) - 180.0; }
+__device__ __forceinline__ double wrap180(double x) { return pymod360(x + 180.0) - 180.0; }
 
 // Python integer modulo for a positive divisor.
 __device__ __forceinline__ int imod(int a, int n) {
@@ -96,7 +113,7 @@ __device__ __forceinline__ int imod(int a, int n) {
 
 // mesh.py:1192-1207 _gh_fold_dlon
 __device__ __forceinline__ double gh_fold_dlon(const DMesh& m, double lon_p) {
-    double dlon = pymod(lon_p - m.lon_min, 360.0);
+    double dlon = pymod360(lon_p - m.lon_min);
     if (!m.wrap) {
         double grid_span = (double)m.nx * m.cell;
         if (dlon > grid_span && (dlon - grid_span) > (360.0 - dlon)) dlon -= 360.0;

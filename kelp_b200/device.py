@@ -208,6 +208,10 @@ class DeviceContext:
         arr = (N.StepArgs * len(steps))(*steps)
         self._chk(N.lib().kc_run(self._ctx, arr, len(steps)), "kc_run")
 
+    def sort(self) -> None:
+        """Re-order the resident particles by grid-hash cell (kc_sort)."""
+        self._chk(N.lib().kc_sort(self._ctx), "kc_sort")
+
     def find_nearest(self, lon, lat) -> np.ndarray:
         lon = _c(lon, np.float64)
         lat = _c(lat, np.float64)

@@ -139,6 +139,48 @@ def test_cuda_vs_oracle_c1_like(scheme):
     assert_close_state(st, want, "f_", f"c1-like {scheme}")
 
 
+def test_resident_loop_with_resort_matches_oracle():
+    """The device-resident loop (kc_run over per-step arguments) with a
+    re-sort by hash cell every 3 steps returns, in upload order, exactly what
+    the oracle computes: the order of the particles does not change any
+    result (each keeps its RNG key)."""
+    from oracle import oracle as O
+    from kelp_b200 import workloads as W
+    from kelp_b200.device import DeviceContext
+    from kelp_b200.particles import make_state
+    from kelp_b200.fields import LazyLerpField
+    w = W.c3(P=15000, nside=32)
+    ctx = DeviceContext(0)
+    ctx.ensure_mesh(w.mesh)
+    slots = ctx.slots_for(w.snaps)
+    P = w.P
+    ctx.upload_particles(w.lon, w.lat, w.z, np.ones(P, np.int32), np.full(P, -1, np.int32), np.zeros(P, np.int8))
+    so = make_state(w.lon, w.lat, w.z).replace(failure_reason=np.zeros(P, np.int8))
+    view = O.MeshView(w.mesh)
+    for k in range(9):
+        if k % 3 == 0:
+            ctx.sort()
+        ctx.run([w.step_args(k, slots)])
+        ia, ib, alpha0, dtn = w.bracket(k)
+        a, b = w.snaps[ia], w.snaps[ib]
+        vel = a if alpha0 == 0.0 else LazyLerpField(a, b, alpha0)
+        out = O.step(so, vel, w.mesh, w.dt, 1.0, "rk2", vel_next=b, dt_to_next=dtn, w_interp="barycentric",
+                     diffusion=DiffusionStepArgs("uniform", 10.0, 10.0, 0, 0, k), view=view)
+        so = so.replace(lon=out["lon"], lat=out["lat"], z=out["z"], status=out["status"],
+                        nearest_node=out["nearest_node"], failure_reason=out["failure_reason"],
+                        u=out["u"], v=out["v"], w=out["w"])
+    got = ctx.download_particles()
+    assert ctx.device_errors() == 0
+    from kelp_b200.particles import ParticleState
+    st = ParticleState(lon=got["lon"], lat=got["lat"], z=got["z"], status=got["status"],
+                       nearest_node=got["nearest_node"], failure_reason=got["failure_reason"], u=got["u"],
+                       v=got["v"], w=got["w"])
+    want = {f"f_{k}": getattr(so, k) for k in ("lon", "lat", "z", "status", "nearest_node", "failure_reason",
+                                               "u", "v", "w")}
+    assert_close_state(st, want, "f_", "resident loop with re-sort")
+    ctx.close()
+
+
 def test_cuda_vs_oracle_healpix_3d_kick():
     """A C3-shaped run on a reduced HEALPix dual mesh (nside 32: quads, the 8
     valence-3 triangles and the pole cells), 69 levels, W barycentric, the split
