@@ -131,6 +131,18 @@ int kc_sort(kc_ctx* ctx);
 /* Batch exact nearest node of P query points (host arrays). */
 int kc_find_nearest(kc_ctx* ctx, long long P, const double* lon, const double* lat, int* out);
 
+/* The same batch nearest-node query, allocating nothing on the device.  For
+ * callers that must not call cudaMalloc: it synchronises the whole device, and
+ * it fails when the host application has already reserved the free device
+ * memory for its own pool.  Queries and results are staged in one fixed
+ * device array (1.25 MiB, held by every GPU that loads the library until the
+ * process exits), so at most 65536 points per call (more is rejected with
+ * KC_ERR_ARG).  The first call on a device looks the array's address up
+ * (make it before any stream capture).  All calls share the array: calls that
+ * overlap on the GPU (several contexts or threads at once) race.  Same results
+ * as kc_find_nearest.  No counterpart in the reference. */
+int kc_find_nearest_noalloc(kc_ctx* ctx, long long P, const double* lon, const double* lat, int* out);
+
 /* Counter-RNG normal pairs of the diffusion kick, drawn on the device for
  * particle ids pid_offset .. pid_offset + P - 1 (out: (P, 2)).  The kick
  * kernel draws exactly these numbers; this entry point exposes them for

@@ -21,7 +21,7 @@ KC_EULER, KC_RK2, KC_RK4 = 0, 1, 2
 #: every symbol include/kelp_cuda.h declares
 EXPORTS = ("kc_abi_version", "kc_node_xyz_fill", "kc_create", "kc_destroy", "kc_last_error",
            "kc_synchronize", "kc_mesh_upload", "kc_field_upload", "kc_particles_upload",
-           "kc_particles_download", "kc_step", "kc_run", "kc_sort", "kc_find_nearest", "kc_rng_normals", "kc_device_errors",
+           "kc_particles_download", "kc_step", "kc_run", "kc_sort", "kc_find_nearest", "kc_find_nearest_noalloc", "kc_rng_normals", "kc_device_errors",
            "kc_event_record", "kc_event_elapsed", "kc_l2_flush", "kc_host_alloc", "kc_host_free")
 
 
@@ -85,6 +85,7 @@ def lib():
         L.kc_run.argtypes = [vp, C.POINTER(StepArgs), i]
         L.kc_sort.argtypes = [vp]
         L.kc_find_nearest.argtypes = [vp, ll, vp, vp, vp]
+        L.kc_find_nearest_noalloc.argtypes = [vp, ll, vp, vp, vp]
         L.kc_rng_normals.argtypes = [vp, ll, C.c_ulonglong, C.c_ulonglong, C.c_ulonglong, C.c_ulonglong, vp]
         L.kc_device_errors.argtypes = [vp, C.POINTER(i)]
         L.kc_event_record.argtypes = [vp, i]

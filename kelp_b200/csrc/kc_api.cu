@@ -6,6 +6,7 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <mutex>
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
 
@@ -641,6 +642,80 @@ int kc_find_nearest(kc_ctx* c, long long P, const double* lon, const double* lat
     k_nearest<<<grid_for(P), kBlock, 0, c->stream>>>(c->dm, c->q, P, c->qout);
     KC_CUDA(c, cudaGetLastError());
     KC_CUDA(c, cudaMemcpyAsync(out, c->qout, (size_t)P * 4, cudaMemcpyDeviceToHost, c->stream));
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KC_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Nearest-node queries without any device allocation.
+//
+// kc_find_nearest grows a per-context staging buffer with cudaMalloc.  Some
+// callers cannot allow that: cudaMalloc synchronises the whole device (a stall
+// in a latency-bound loop that shares the GPU with other work), and it fails
+// outright when the host application has already handed all free device
+// memory to its own pool.  kc_find_nearest_noalloc stages the queries and
+// results in this fixed array instead, which every GPU that loads the library
+// holds until the process exits.  In host code `g_noalloc_scratch` names a
+// host-side stand-in, not a device address: the device address is looked up
+// once per device with cudaGetSymbolAddress and passed to the kernel.
+// ---------------------------------------------------------------------------
+
+constexpr long long kNoAllocMaxPoints = 65536;   // 64 Ki queries -> 1.25 MiB of device memory
+constexpr int kNoAllocMaxDevices = 64;
+
+// lon (P doubles), lat (P doubles) at byte P*8, results (P ints) at byte
+// kNoAllocMaxPoints*16
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocMaxPoints * 20];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// The device address of the scratch array on the current device (set up on the
+// first call per device; the device must be current).
+int noalloc_scratch(kc_ctx* c, unsigned char** out) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (c->device < 0 || c->device >= kNoAllocMaxDevices)
+        return fail(c, KC_ERR_ARG, "kc_find_nearest_noalloc: device index beyond the supported range");
+    if (!g_noalloc_addr[c->device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(c, KC_ERR_CUDA, std::string("kc_find_nearest_noalloc: cudaGetSymbolAddress: ") +
+                                            cudaGetErrorString(e));
+        g_noalloc_addr[c->device] = p;
+    }
+    *out = static_cast<unsigned char*>(g_noalloc_addr[c->device]);
+    return KC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int kc_find_nearest_noalloc(kc_ctx* c, long long P, const double* lon, const double* lat, int* out) {
+    if (!c) return KC_ERR_ARG;
+    if (!c->has_mesh) return fail(c, KC_ERR_STATE, "kc_find_nearest_noalloc: no mesh uploaded");
+    if (P < 0 || (P > 0 && (!lon || !lat || !out))) return fail(c, KC_ERR_ARG, "kc_find_nearest_noalloc: arrays");
+    if (P > kNoAllocMaxPoints)
+        return fail(c, KC_ERR_ARG, "kc_find_nearest_noalloc: " + std::to_string(P) +
+                                       " queries exceed the fixed scratch of " + std::to_string(kNoAllocMaxPoints) +
+                                       "; split the batch or use kc_find_nearest");
+    if (P == 0) return KC_OK;
+    KC_CUDA(c, cudaSetDevice(c->device));
+    unsigned char* base = nullptr;
+    int rc = noalloc_scratch(c, &base);
+    if (rc) return rc;
+    double* q = reinterpret_cast<double*>(base);
+    int* res = reinterpret_cast<int*>(base + kNoAllocMaxPoints * 16);
+    KC_CUDA(c, cudaMemcpyAsync(q, lon, (size_t)P * 8, cudaMemcpyHostToDevice, c->stream));
+    KC_CUDA(c, cudaMemcpyAsync(q + P, lat, (size_t)P * 8, cudaMemcpyHostToDevice, c->stream));
+    k_nearest<<<grid_for(P), kBlock, 0, c->stream>>>(c->dm, q, P, res);
+    KC_CUDA(c, cudaGetLastError());
+    KC_CUDA(c, cudaMemcpyAsync(out, res, (size_t)P * 4, cudaMemcpyDeviceToHost, c->stream));
     KC_CUDA(c, cudaStreamSynchronize(c->stream));
     return KC_OK;
 }
