@@ -151,6 +151,17 @@ __global__ void __launch_bounds__(kBlock) k_step3d_rk2(const __grid_constant__ k
     kc::step3d_rk2_particle<T>(m, f, st, s, i);
 }
 
+template <typename T, int SCHEME>
+__global__ void __launch_bounds__(kBlock) k_step3d_unfused(const __grid_constant__ kc::DMesh m,
+                                                           const __grid_constant__ kc::DBlend<T> f,
+                                                           const __grid_constant__ kc::DState st,
+                                                           const __grid_constant__ kc::DStep s) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= st.P) return;
+    activate(st, s, i);
+    kc::step3d_unfused_particle<T, SCHEME>(m, f, st, s, i);
+}
+
 __global__ void __launch_bounds__(kBlock) k_nearest(const __grid_constant__ kc::DMesh m, const double* q, long long P, int* out) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P) return;
@@ -253,7 +264,9 @@ int launch_step(kc_ctx* c, const kc_step_args* a) {
         else if (a->scheme == KC_RK2) k_step2d<T, 1><<<g, kBlock, 0, c->stream>>>(c->dm, f, st, s);
         else k_step2d<T, 2><<<g, kBlock, 0, c->stream>>>(c->dm, f, st, s);
     } else {
-        k_step3d_rk2<T><<<g, kBlock, 0, c->stream>>>(c->dm, f, st, s);
+        if (a->scheme == KC_RK2) k_step3d_rk2<T><<<g, kBlock, 0, c->stream>>>(c->dm, f, st, s);
+        else if (a->scheme == KC_RK4) k_step3d_unfused<T, 2><<<g, kBlock, 0, c->stream>>>(c->dm, f, st, s);
+        else k_step3d_unfused<T, 0><<<g, kBlock, 0, c->stream>>>(c->dm, f, st, s);
     }
     KC_CUDA(c, cudaGetLastError());
     return KC_OK;
@@ -265,8 +278,6 @@ int check_step(kc_ctx* c, const kc_step_args* a) {
     if (!(a->scheme == KC_EULER || a->scheme == KC_RK2 || a->scheme == KC_RK4))
         return fail(c, KC_ERR_ARG, "kc_step: unknown scheme");
     if (!(a->dims == 2 || a->dims == 3)) return fail(c, KC_ERR_ARG, "kc_step: dims must be 2 or 3");
-    if (a->dims == 3 && a->scheme != KC_RK2)
-        return fail(c, KC_ERR_ARG, "kc_step: the 3-D step supports rk2 only in this build");
     if (!(a->dt > 0.0)) return fail(c, KC_ERR_ARG, "kc_step: dt must be > 0");
     if (!(a->time_dir == 1.0 || a->time_dir == -1.0)) return fail(c, KC_ERR_ARG, "kc_step: time_dir must be +-1");
     if (a->w_code != 0 && a->w_code != 1) return fail(c, KC_ERR_ARG, "kc_step: w_code must be 0 or 1");

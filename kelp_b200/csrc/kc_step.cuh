@@ -213,6 +213,115 @@ __device__ __forceinline__ double stage_w(const DMesh& m, const DBlend<T>& f, in
     return w_bary<T>(m, f, alpha, xp, yp, z, node, td);
 }
 
+// One 3-D stage of the unfused paths: exact anchor at the stage position,
+// layer at the stage depth, u/v and W from the stage blend.
+template <typename T>
+__device__ __forceinline__ bool stage3d(const DMesh& m, const DBlend<T>& f, const DStep& s, int k, double lon,
+                                        double lat, double z, const Site& q, double& U, double& V, double& W) {
+    const int nn = site_anchor(m, q);
+    const int layer = find_layer(m, z, nn);
+    if (!interp_uv_bary<T>(m, f, lon, lat, nn, s.time_dir, layer, s.ak[k], U, V)) return false;
+    W = stage_w<T>(m, f, s.w_code, s.ak[k], lon, lat, z, nn, s.time_dir);
+    return true;
+}
+
+// 3-D Euler (integrators.py:4997-5147) and RK4 (:5760-6011): the reference's
+// unfused multi-pass paths restated per particle -- the batch exact anchor of
+// every stage position, the layer at the stage depth, the whole-field stage
+// lerps of _make_stage_vels (:1187-1237) reproduced per vertex, W at the stage
+// position; a failure reverts to the start with the start anchor.
+template <typename T, int SCHEME>
+__device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DBlend<T>& f, const DState& st,
+                                                        const DStep& s, long long i) {
+    int status = st.status[i];
+    if (status != ALIVE) {
+        st.U[i] = 0.0;
+        st.V[i] = 0.0;
+        st.W[i] = 0.0;
+        return;
+    }
+    const double lon0 = st.lon[i], lat0 = st.lat[i], z0p = st.z[i];
+    const int pre_nn = st.nn[i];
+    const double dt = s.dt, td = s.time_dir;
+    signed char fr = st.fr[i];
+    double lon_new = lon0, lat_new = lat0, z_new = z0p;
+
+    const Site q0 = make_site(lon0, lat0);
+    const int node_i = site_anchor(m, q0);
+    int nn_out = node_i;
+    const int layer1 = find_layer(m, z0p, node_i);
+    double U1, V1;
+    bool ok = interp_uv_bary<T>(m, f, lon0, lat0, node_i, td, layer1, s.ak[0], U1, V1);
+    const double W1 = stage_w<T>(m, f, s.w_code, s.ak[0], lon0, lat0, z0p, node_i, td);
+    st.U[i] = U1;
+    st.V[i] = V1;
+    st.W[i] = W1;
+    double a = lon0, b = lat0, c = z0p;
+    if (ok) {
+        if (SCHEME == 0) {
+            a = wrap180(lon0 + dt * U1 / metric_z0(q0));
+            b = clamp_lat(lat0 + dt * V1 / SLM);
+            c = z0p + W1 * dt;
+        } else {
+            const double dl1 = dt * U1 / metric_z0(q0), dd1 = dt * V1 / SLM, dz1 = dt * W1;
+            const double l2 = wrap180(lon0 + 0.5 * dl1), t2 = clamp_lat(lat0 + 0.5 * dd1), z2 = z0p + 0.5 * dz1;
+            const Site q2 = make_site(l2, t2);
+            double U2, V2, W2;
+            ok = stage3d<T>(m, f, s, 1, l2, t2, z2, q2, U2, V2, W2);
+            if (ok) {
+                const double dl2 = dt * U2 / metric_z0(q2), dd2 = dt * V2 / SLM, dz2 = dt * W2;
+                const double l3 = wrap180(lon0 + 0.5 * dl2), t3 = clamp_lat(lat0 + 0.5 * dd2), z3 = z0p + 0.5 * dz2;
+                const Site q3 = make_site(l3, t3);
+                double U3, V3, W3;
+                ok = stage3d<T>(m, f, s, 2, l3, t3, z3, q3, U3, V3, W3);
+                if (ok) {
+                    const double dl3 = dt * U3 / metric_z0(q3), dd3 = dt * V3 / SLM, dz3 = dt * W3;
+                    const double l4 = wrap180(lon0 + dl3), t4 = clamp_lat(lat0 + dd3), z4 = z0p + dz3;
+                    const Site q4 = make_site(l4, t4);
+                    double U4, V4, W4;
+                    ok = stage3d<T>(m, f, s, 3, l4, t4, z4, q4, U4, V4, W4);
+                    if (ok) {
+                        const double dl4 = dt * U4 / metric_z0(q4), dd4 = dt * V4 / SLM, dz4 = dt * W4;
+                        const double dl = (dl1 + 2.0 * dl2 + 2.0 * dl3 + dl4) / 6.0;
+                        const double dd = (dd1 + 2.0 * dd2 + 2.0 * dd3 + dd4) / 6.0;
+                        const double dz = (dz1 + 2.0 * dz2 + 2.0 * dz3 + dz4) / 6.0;
+                        a = wrap180(lon0 + dl);
+                        b = clamp_lat(lat0 + dd);
+                        c = z0p + dz;
+                    }
+                }
+            }
+        }
+    }
+    if (!ok) {
+        status = OUTSIDE; fr = FR_INTERP;
+    } else {
+        const Site qn = make_site(a, b);
+        const int nn_new = site_anchor(m, qn);
+        if (contain_local(m, a, b, nn_new) < 0) {
+            status = OUTSIDE; fr = FR_OOB;
+        } else {
+            if (c < m.zlev[0]) c = m.zlev[0];
+            const double bottom = m.depth[nn_new];
+            if (c > bottom) c = bottom;
+            lon_new = a; lat_new = b; z_new = c;
+            status = ALIVE;
+            nn_out = nn_new;
+            if (s.kick) {
+                long long pid = st.pid ? st.pid[i] : i;
+                apply_kick(m, s, pid, qn, lon0, lat0, z0p, pre_nn, true, lon_new, lat_new, z_new, status, nn_out,
+                           fr);
+            }
+        }
+    }
+    st.lon[i] = lon_new;
+    st.lat[i] = lat_new;
+    st.z[i] = z_new;
+    st.status[i] = status;
+    st.nn[i] = nn_out;
+    st.fr[i] = fr;
+}
+
 // integrators.py:3647-3856 _fused_rk2_step_3d_bary_tinterp (layer u/v,
 // z-level), with the exact stage-1 anchor of its runner (:4766-4770) and the
 // split kick epilogue.

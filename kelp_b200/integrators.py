@@ -126,15 +126,15 @@ def _run(state, vel, mesh, dt, time_dir, scheme, c_coeffs, kw, ctx=None) -> Part
             raise NotImplementedError("sigma meshes are not built on the CUDA backend")
         if getattr(vel, "uv_vertical", "layer") != "layer":
             raise NotImplementedError("depth-linear u/v placement is not built on the CUDA backend")
-        if scheme != N.KC_RK2:
-            raise NotImplementedError("3-D euler/rk4 are not built on the CUDA backend; rk2 is")
         w_interp = kw.get("w_interp", "leastsq")
         if w_interp not in ("nearest", "barycentric"):
             raise NotImplementedError(f"w_interp={w_interp!r} is not built on the CUDA backend")
         w_code = 0 if w_interp == "nearest" else 1
-        if hasattr(vel, "vel_a") and float(getattr(vel, "alpha", 1.0)) == 0.0:
+        if scheme == N.KC_RK2 and hasattr(vel, "vel_a") and float(getattr(vel, "alpha", 1.0)) == 0.0:
+            # integrators.py:5691-5692 routes this exotic payload to the
+            # unfused RK2, whose 0 * vel_b blend propagates non-finite values
             raise NotImplementedError("an endpoint LazyLerpField (alpha 0) takes the reference's unfused "
-                                      "path, which is not built on the CUDA backend")
+                                      "3-D RK2 path, which is not built on the CUDA backend")
     vel_a, vel_b, target, alpha0 = _fields(vel, vel_next)
     _check_node_fields(mesh, [vel_a, vel_b, target], is3d)
 

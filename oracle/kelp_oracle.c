@@ -811,6 +811,68 @@ static void step_one(const OMesh* m, const OField* f, const OStep* s, int64_t i,
             if (contain_local(m, ln, lt, nw) < 0) { st = OUTSIDE; frr = 2; ln = lon0; lt = lat0; }
             else nno = nw;
         }
+    } else if (s->scheme != 1) {
+        /* 3-D Euler (integrators.py:4997-5147) and RK4 (:5760-6011): the
+         * unfused multi-pass paths restated per particle -- batch exact anchor
+         * per stage, layer at the stage depth, stage fields blended per vertex
+         * (the whole-field lerps of _make_stage_vels, :1187-1237), W at the
+         * stage position, failure reverts to the start with the start anchor. */
+        int l1 = find_layer(m, zp, m->depth[node_i]);
+        double U1, V1;
+        int ok1 = interp_uv(m, f, lon0, lat0, node_i, td, l1, s->ak[0], &U1, &V1);
+        double W1 = s->w_code == 0 ? w_linear(m, f, s->ak[0], zp, node_i, td)
+                                   : w_bary(m, f, s->ak[0], lon0, lat0, zp, node_i, td);
+        U[i] = U1; V[i] = V1; W[i] = W1;
+        double a = lon0, b = lat0, c = zp;
+        if (!ok1) ok = 0;
+        else if (s->scheme == 0) {
+            a = wrap180(lon0 + dt * U1 / z0_of(lat0));
+            b = clat(lat0 + dt * V1 / SLM);
+            c = zp + W1 * dt;
+        } else {
+            double dl1 = dt * U1 / z0_of(lat0), dd1 = dt * V1 / SLM, dz1 = dt * W1;
+            double l2 = wrap180(lon0 + 0.5 * dl1), t2 = clat(lat0 + 0.5 * dd1), z2 = zp + 0.5 * dz1;
+            int n2 = anchor(m, l2, t2);
+            double U2, V2, U3, V3, U4, V4;
+            if (!interp_uv(m, f, l2, t2, n2, td, find_layer(m, z2, m->depth[n2]), s->ak[1], &U2, &V2)) ok = 0;
+            else {
+                double W2 = s->w_code == 0 ? w_linear(m, f, s->ak[1], z2, n2, td)
+                                           : w_bary(m, f, s->ak[1], l2, t2, z2, n2, td);
+                double dl2 = dt * U2 / z0_of(t2), dd2 = dt * V2 / SLM, dz2 = dt * W2;
+                double l3 = wrap180(lon0 + 0.5 * dl2), t3 = clat(lat0 + 0.5 * dd2), z3 = zp + 0.5 * dz2;
+                int n3 = anchor(m, l3, t3);
+                if (!interp_uv(m, f, l3, t3, n3, td, find_layer(m, z3, m->depth[n3]), s->ak[2], &U3, &V3)) ok = 0;
+                else {
+                    double W3 = s->w_code == 0 ? w_linear(m, f, s->ak[2], z3, n3, td)
+                                               : w_bary(m, f, s->ak[2], l3, t3, z3, n3, td);
+                    double dl3 = dt * U3 / z0_of(t3), dd3 = dt * V3 / SLM, dz3 = dt * W3;
+                    double l4 = wrap180(lon0 + dl3), t4 = clat(lat0 + dd3), z4 = zp + dz3;
+                    int n4 = anchor(m, l4, t4);
+                    if (!interp_uv(m, f, l4, t4, n4, td, find_layer(m, z4, m->depth[n4]), s->ak[3], &U4, &V4)) ok = 0;
+                    else {
+                        double W4 = s->w_code == 0 ? w_linear(m, f, s->ak[3], z4, n4, td)
+                                                   : w_bary(m, f, s->ak[3], l4, t4, z4, n4, td);
+                        double dl4 = dt * U4 / z0_of(t4), dd4 = dt * V4 / SLM, dz4 = dt * W4;
+                        double dl = (dl1 + 2.0 * dl2 + 2.0 * dl3 + dl4) / 6.0;
+                        double dd = (dd1 + 2.0 * dd2 + 2.0 * dd3 + dd4) / 6.0;
+                        double dz = (dz1 + 2.0 * dz2 + 2.0 * dz3 + dz4) / 6.0;
+                        a = wrap180(lon0 + dl);
+                        b = clat(lat0 + dd);
+                        c = zp + dz;
+                    }
+                }
+            }
+        }
+        if (!ok) { st = OUTSIDE; frr = 1; }
+        else {
+            int nw = anchor(m, a, b);
+            if (contain_local(m, a, b, nw) < 0) { st = OUTSIDE; frr = 2; }
+            else {
+                if (c < m->zlev[0]) c = m->zlev[0];
+                if (c > m->depth[nw]) c = m->depth[nw];
+                ln = a; lt = b; zn = c; nno = nw;
+            }
+        }
     } else {
         int l1 = find_layer(m, zp, m->depth[node_i]);
         double U1, V1;

@@ -203,7 +203,12 @@ def main():
     cases = {"rk2_wnear": run_case(rm, rf, lon, lat, z, status, "rk2", 21600.0, T, 12, w_interp="nearest"),
              "rk2_wbary": run_case(rm, rf, lon, lat, z, status, "rk2", 21600.0, T, 12, w_interp="barycentric"),
              "rk2_wbary_kick": run_case(rm, rf, lon, lat, z, status, "rk2", 21600.0, T, 12,
-                                        w_interp="barycentric", kh=(3.0e4, 3.0e4), seed=5)}
+                                        w_interp="barycentric", kh=(3.0e4, 3.0e4), seed=5),
+             # unfused reference paths: 3-D RK4 and 3-D Euler
+             "rk4_wnear": run_case(rm, rf, lon, lat, z, status, "rk4", 21600.0, T, 12, w_interp="nearest"),
+             "rk4_wbary_kick": run_case(rm, rf, lon, lat, z, status, "rk4", 21600.0, T, 12,
+                                        w_interp="barycentric", kh=(3.0e4, 1.0e4), seed=9),
+             "euler_wbary": run_case(rm, rf, lon, lat, z, status, "euler", 10800.0, T, 16, w_interp="barycentric")}
     save("golden_3d", mesh_record(rm), snaps, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
 
     # --- counter RNG: normal pairs of the reference for a key grid ----------

@@ -17,7 +17,7 @@ from kelp_b200.diffusion import DiffusionStepArgs
 CASES = [("golden_band", c) for c in ("rk2", "rk4", "euler", "rk2_bwd", "rk2_kick", "rk4_kick_aniso", "rk2_dt4800")]
 CASES += [("golden_quad", c) for c in ("rk2", "rk4", "euler", "rk2_kick")]
 CASES += [("golden_polar", "rk2")]
-CASES += [("golden_3d", c) for c in ("rk2_wnear", "rk2_wbary", "rk2_wbary_kick")]
+CASES += [("golden_3d", c) for c in ("rk2_wnear", "rk2_wbary", "rk2_wbary_kick", "rk4_wnear", "rk4_wbary_kick", "euler_wbary")]
 
 
 def replay_oracle(g, cname):
