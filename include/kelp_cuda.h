@@ -83,6 +83,7 @@ typedef struct kc_step_args {
     double dt;                   /* seconds, > 0 */
     double time_dir;             /* +1 forward, -1 backward */
     int w_code;                  /* 3-D W: 0 nearest, 1 barycentric */
+    int uv_vertical;             /* 3-D u/v: 0 layer (K-1 rows), 1 depth-linear (the table's M rows) */
     int kick;                    /* split uniform-Kh random walk on/off */
     double kh_x, kh_y;           /* m^2/s */
     unsigned long long seed, real_id, step_i, pid_offset;
@@ -100,6 +101,11 @@ int kc_last_error(const kc_ctx* ctx, char* buf, int buflen);
 int kc_synchronize(kc_ctx* ctx);
 
 int kc_mesh_upload(kc_ctx* ctx, const kc_mesh_desc* desc);
+
+/* The depth-linear data-point table of the mesh (uv_vertical "level" /
+ * "layer_linear"): M point depths p, and per node the last usable point and
+ * the bed depth (src/kelp/numerics/vertical_uv.py:181-278, :328). */
+int kc_depth_points_upload(kc_ctx* ctx, int M, const double* p, const int* last, const double* bed);
 
 /* One snapshot into ring slot `slot` (0..7): u, v (n_uv_rows, n_nodes) and
  * optional w (n_w_rows, n_nodes), all of element type `dtype`. */

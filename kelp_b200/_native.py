@@ -20,7 +20,7 @@ KC_EULER, KC_RK2, KC_RK4 = 0, 1, 2
 
 #: every symbol include/kelp_cuda.h declares
 EXPORTS = ("kc_abi_version", "kc_node_xyz_fill", "kc_create", "kc_destroy", "kc_last_error",
-           "kc_synchronize", "kc_mesh_upload", "kc_field_upload", "kc_particles_upload",
+           "kc_synchronize", "kc_mesh_upload", "kc_depth_points_upload", "kc_field_upload", "kc_particles_upload",
            "kc_particles_download", "kc_step", "kc_run", "kc_sort", "kc_find_nearest", "kc_find_nearest_noalloc", "kc_rng_normals", "kc_device_errors",
            "kc_event_record", "kc_event_elapsed", "kc_l2_flush", "kc_host_alloc", "kc_host_free")
 
@@ -51,7 +51,7 @@ class StepArgs(C.Structure):
                 ("slot_a", C.c_int), ("slot_b", C.c_int), ("slot_t", C.c_int),
                 ("alpha0", C.c_double), ("alpha_k", C.c_double * 4),
                 ("dt", C.c_double), ("time_dir", C.c_double),
-                ("w_code", C.c_int), ("kick", C.c_int),
+                ("w_code", C.c_int), ("uv_vertical", C.c_int), ("kick", C.c_int),
                 ("kh_x", C.c_double), ("kh_y", C.c_double),
                 ("seed", C.c_ulonglong), ("real_id", C.c_ulonglong),
                 ("step_i", C.c_ulonglong), ("pid_offset", C.c_ulonglong),
@@ -79,6 +79,7 @@ def lib():
         L.kc_synchronize.argtypes = [vp]
         L.kc_mesh_upload.argtypes = [vp, C.POINTER(MeshDesc)]
         L.kc_field_upload.argtypes = [vp, i, i, ll, i, vp, vp, i, vp]
+        L.kc_depth_points_upload.argtypes = [vp, i, vp, vp, vp]
         L.kc_particles_upload.argtypes = [vp, ll, vp, vp, vp, vp, vp, vp, vp, vp]
         L.kc_particles_download.argtypes = [vp, ll, vp, vp, vp, vp, vp, vp, vp, vp, vp]
         L.kc_step.argtypes = [vp, C.POINTER(StepArgs)]

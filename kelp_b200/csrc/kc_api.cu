@@ -50,6 +50,9 @@ struct kc_ctx {
     double2* d_nsc = nullptr;
     double2* d_ecos = nullptr;
     int* d_maxl = nullptr;
+    double* d_dl_p = nullptr;
+    int* d_dl_last = nullptr;
+    double* d_dl_bed = nullptr;
     int* d_err = nullptr;
     kc::DMesh dm{};
     // snapshot ring
@@ -121,7 +124,7 @@ kc::DStep step_of(const kc_step_args* a) {
     kc::DStep s;
     s.dt = a->dt; s.time_dir = a->time_dir;
     for (int k = 0; k < 4; ++k) s.ak[k] = a->alpha_k[k];
-    s.w_code = a->w_code; s.kick = a->kick;
+    s.w_code = a->w_code; s.kick = a->kick; s.uv_dl = a->uv_vertical;
     s.kh_x = a->kh_x; s.kh_y = a->kh_y;
     s.seed = a->seed; s.real_id = a->real_id; s.step_i = a->step_i; s.pid_offset = a->pid_offset;
     s.global_step = a->global_step;
@@ -294,8 +297,16 @@ int check_step(kc_ctx* c, const kc_step_args* a) {
         if (a->dims == 2 && s.uv_rows != 1) return fail(c, KC_ERR_ARG, "kc_step: 2-D step needs single-row u/v");
         if (a->dims == 3) {
             if (c->dm.K < 2) return fail(c, KC_ERR_STATE, "kc_step: 3-D step needs z-levels and depth");
-            if (s.uv_rows != c->dm.K - 1 || s.w_rows != c->dm.K)
-                return fail(c, KC_ERR_ARG, "kc_step: 3-D layer fields need u/v (K-1, N) and w (K, N)");
+            if (a->uv_vertical == 1) {
+                if (!c->d_dl_p) return fail(c, KC_ERR_STATE, "kc_step: depth-linear u/v needs kc_depth_points_upload");
+                if (s.uv_rows != c->dm.dl_M || s.w_rows != c->dm.K)
+                    return fail(c, KC_ERR_ARG, "kc_step: depth-linear fields need u/v (M, N) and w (K, N)");
+            } else if (a->uv_vertical == 0) {
+                if (s.uv_rows != c->dm.K - 1 || s.w_rows != c->dm.K)
+                    return fail(c, KC_ERR_ARG, "kc_step: 3-D layer fields need u/v (K-1, N) and w (K, N)");
+            } else {
+                return fail(c, KC_ERR_ARG, "kc_step: uv_vertical must be 0 (layer) or 1 (depth-linear)");
+            }
         }
     }
     if (c->P > 0 && !c->lon) return fail(c, KC_ERR_STATE, "kc_step: no particles uploaded");
@@ -320,6 +331,8 @@ void free_mesh(kc_ctx* c) {
     dfree(c->d_ll); dfree(c->d_en); dfree(c->d_n2e_off); dfree(c->d_n2e); dfree(c->d_gh_off);
     dfree(c->d_gh_tab); dfree(c->d_xyz); dfree(c->d_depth); dfree(c->d_zlev);
     dfree(c->d_nsc); dfree(c->d_ecos); dfree(c->d_maxl);
+    dfree(c->d_dl_p); dfree(c->d_dl_last); dfree(c->d_dl_bed);
+    c->dm.dl_p = nullptr; c->dm.dl_last = nullptr; c->dm.dl_bed = nullptr; c->dm.dl_M = 0;
     c->has_mesh = false;
 }
 
@@ -465,6 +478,29 @@ int kc_mesh_upload(kc_ctx* c, const kc_mesh_desc* d) {
     m.err = c->d_err;
     c->N = N; c->E = E;
     c->has_mesh = true;
+    return KC_OK;
+}
+
+int kc_depth_points_upload(kc_ctx* c, int M, const double* p, const int* last, const double* bed) {
+    if (!c) return KC_ERR_ARG;
+    if (!c->has_mesh) return fail(c, KC_ERR_STATE, "kc_depth_points_upload: no mesh uploaded");
+    if (M <= 0 || !p || !last || !bed) return fail(c, KC_ERR_ARG, "kc_depth_points_upload: empty table");
+    for (long long i = 0; i < c->N; ++i)
+        if (last[i] < 0 || last[i] >= M) return fail(c, KC_ERR_ARG, "kc_depth_points_upload: last out of range");
+    for (int k = 1; k < M; ++k)
+        if (!(p[k] >= p[k - 1])) return fail(c, KC_ERR_ARG, "kc_depth_points_upload: points not non-decreasing");
+    KC_CUDA(c, cudaSetDevice(c->device));
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    dfree(c->d_dl_p); dfree(c->d_dl_last); dfree(c->d_dl_bed);
+    int rc;
+    if ((rc = upload(c, &c->d_dl_p, p, (size_t)M))) return rc;
+    if ((rc = upload(c, &c->d_dl_last, last, (size_t)c->N))) return rc;
+    if ((rc = upload(c, &c->d_dl_bed, bed, (size_t)c->N))) return rc;
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->dm.dl_p = c->d_dl_p;
+    c->dm.dl_last = c->d_dl_last;
+    c->dm.dl_bed = c->d_dl_bed;
+    c->dm.dl_M = M;
     return KC_OK;
 }
 

@@ -48,8 +48,11 @@ struct DMesh {
     const double* depth;      // (N) bottom depth, positive down (3-D)
     const int* max_layer;     // (N) deepest valid layer above the node's bottom (3-D)
     const double* zlev;       // (K) z-level interfaces, positive down (3-D)
+    const double* dl_p;       // (M) depth-linear data points (uv_vertical level / layer_linear)
+    const int* dl_last;       // (N) last usable data point per node
+    const double* dl_bed;     // (N) bed depth per node for the wall test
     double cell, lon_min, lat_min, r_earth;
-    int nx, ny, wrap, far_rows, K, exact;
+    int nx, ny, wrap, far_rows, K, exact, dl_M;
     int* err;                 // device error word
 };
 

@@ -148,6 +148,150 @@ __device__ __noinline__ bool interp_uv_bary(const DMesh& m, const DBlend<T>& f, 
     return true;
 }
 
+// vertical_uv.py:457-523 uv_bracket: (k, alpha) of depth z among the data
+// points p[0..last_i]; alpha < 0 reads point k alone.
+__device__ __forceinline__ void uv_bracket(const double* __restrict__ p, int li, double z, int& k, double& alpha) {
+    if (li <= 0) { k = 0; alpha = -1.0; return; }
+    double zc = z;
+    const double p0 = __ldg(&p[0]), pl = __ldg(&p[li]);
+    if (zc > pl) zc = pl;
+    if (zc < p0) zc = p0;
+    if (zc <= p0) { k = 0; alpha = -1.0; return; }
+    if (zc >= pl) { k = li; alpha = -1.0; return; }
+    // first j in [0, li-1] with zc < p[j+1] (exists: zc < p[li])
+    int lo = 0, hi = li - 1;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (zc < __ldg(&p[mid + 1])) hi = mid;
+        else lo = mid + 1;
+    }
+    k = lo;
+    const double pk = __ldg(&p[k]);
+    const double dz = __ldg(&p[k + 1]) - pk;
+    if (dz < 1e-12) { alpha = -1.0; return; }
+    const double a = (zc - pk) / dz;
+    if (a <= 0.0) { alpha = -1.0; return; }
+    if (a >= 1.0) { k = k + 1; alpha = -1.0; return; }
+    alpha = a;
+}
+
+// The time blend of one stored (point, node) value (interpolate.py:1847-1876
+// _tinterp_point_uv).
+template <typename T>
+__device__ __forceinline__ void tinterp_point_uv(const DBlend<T>& f, int k, int nd, double alpha, double& u,
+                                                 double& v) {
+    const long long idx = (long long)k * f.n + nd;
+    const double alpha0 = f.alpha0;
+    if (alpha < 1e-12) {
+        if (alpha0 == 0.0) {
+            u = (double)__ldg(&f.a.u[idx]);
+            v = (double)__ldg(&f.a.v[idx]);
+            return;
+        }
+        const double beta0 = 1.0 - alpha0;
+        u = beta0 * (double)__ldg(&f.a.u[idx]) + alpha0 * (double)__ldg(&f.b.u[idx]);
+        v = beta0 * (double)__ldg(&f.a.v[idx]) + alpha0 * (double)__ldg(&f.b.v[idx]);
+        return;
+    }
+    if (alpha > 1.0 - 1e-12) {
+        u = (double)__ldg(&f.t.u[idx]);
+        v = (double)__ldg(&f.t.v[idx]);
+        return;
+    }
+    const double beta = 1.0 - alpha;
+    if (alpha0 == 0.0) {
+        u = beta * (double)__ldg(&f.a.u[idx]) + alpha * (double)__ldg(&f.t.u[idx]);
+        v = beta * (double)__ldg(&f.a.v[idx]) + alpha * (double)__ldg(&f.t.v[idx]);
+        return;
+    }
+    const double beta0 = 1.0 - alpha0;
+    const double ua0 = beta0 * (double)__ldg(&f.a.u[idx]) + alpha0 * (double)__ldg(&f.b.u[idx]);
+    const double va0 = beta0 * (double)__ldg(&f.a.v[idx]) + alpha0 * (double)__ldg(&f.b.v[idx]);
+    u = beta * ua0 + alpha * (double)__ldg(&f.t.u[idx]);
+    v = beta * va0 + alpha * (double)__ldg(&f.t.v[idx]);
+}
+
+// interpolate.py:1879-1971 _interp_barycentric_core_tinterp_dl with the wall
+// rule of :1664-1711 _dl_node_wall: the layer twin's geometry, each vertex
+// read linearly in depth between its bracketing data points (time first),
+// vertices dry at the depth left out.
+template <typename T>
+__device__ __noinline__ bool interp_uv_bary_dl(const DMesh& m, const DBlend<T>& f, double xp, double yp, int nn,
+                                               double z, double time_dir, double alpha, double& U, double& V) {
+    U = 0.0;
+    V = 0.0;
+    int elem = contain_local(m, xp, yp, nn);
+    if (elem < 0) return false;
+    Ring r;
+    double w[4];
+    if (!bary_weights_core(m, elem, xp, yp, m.r_earth, r, w)) return false;
+    const int nv = r.n;
+    double zq = z;
+    if (isnan(zq)) zq = INFINITY;   // dry wherever the bed is finite
+    bool wet[4];
+    int n_wet = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        wet[k] = k < nv && zq <= __ldg(&m.dl_bed[r.v[k]]);
+        n_wet += wet[k] ? 1 : 0;
+    }
+    if (n_wet == 0) {
+        int kd = 0;
+        for (int k = 1; k < nv; ++k)
+            if (__ldg(&m.dl_bed[r.v[k]]) > __ldg(&m.dl_bed[r.v[kd]])) kd = k;
+        const int nd = r.v[kd];
+        double un, vn;
+        tinterp_point_uv<T>(f, __ldg(&m.dl_last[nd]), nd, alpha, un, vn);
+        U = time_dir * un;
+        V = time_dir * vn;
+        return true;
+    }
+    double den = 1.0;
+    if (n_wet < nv) {
+        double wsum = 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (wet[k]) {
+                if (w[k] < 0.0) w[k] = 0.0;
+                wsum += w[k];
+            }
+        }
+        if (wsum < 1e-12) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (wet[k]) w[k] = 1.0;
+            den = (double)n_wet;
+        } else {
+            den = wsum;
+        }
+    }
+    double Us = 0.0, Vs = 0.0;
+    for (int k = 0; k < nv; ++k) {
+        const int nd = r.v[k];
+        if (n_wet < nv && !wet[k]) continue;
+        int kb;
+        double ab;
+        uv_bracket(m.dl_p, __ldg(&m.dl_last[nd]), zq, kb, ab);
+        double un, vn;
+        tinterp_point_uv<T>(f, kb, nd, alpha, un, vn);
+        if (!(ab < 0.0)) {
+            double un1, vn1;
+            tinterp_point_uv<T>(f, kb + 1, nd, alpha, un1, vn1);
+            un = (1.0 - ab) * un + ab * un1;
+            vn = (1.0 - ab) * vn + ab * vn1;
+        }
+        Us += w[k] * un;
+        Vs += w[k] * vn;
+    }
+    if (n_wet < nv) {
+        Us = Us / den;
+        Vs = Vs / den;
+    }
+    U = time_dir * Us;
+    V = time_dir * Vs;
+    return true;
+}
+
 // First k in [lo, hi] with z < zl[k + 1] (the caller guarantees one exists):
 // the linear scans of the reference as a binary search over the monotone
 // interface table (same index).

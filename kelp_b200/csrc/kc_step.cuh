@@ -31,6 +31,7 @@ struct DStep {
     double dt, time_dir;
     double ak[4];              // stage alphas c_k * dt / dt_to_next
     int w_code;                // 0 nearest, 1 barycentric (3-D)
+    int uv_dl;                 // 3-D u/v: 0 layer, 1 depth-linear (level / layer_linear)
     int kick;                  // split uniform-Kh kick on/off
     double kh_x, kh_y;
     unsigned long long seed, real_id, step_i, pid_offset;
@@ -213,14 +214,24 @@ __device__ __forceinline__ double stage_w(const DMesh& m, const DBlend<T>& f, in
     return w_bary<T>(m, f, alpha, xp, yp, z, node, td);
 }
 
+// u/v of one 3-D stage: the layer rule (the particle's layer at the anchor,
+// integrators.py:3668-3676) or the depth-linear rule at the stage depth
+// (:4071-4098).
+template <typename T>
+__device__ __forceinline__ bool stage_uv(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
+                                         double lat, int nn, double z, double alpha, double& U, double& V) {
+    if (s.uv_dl) return interp_uv_bary_dl<T>(m, f, lon, lat, nn, z, s.time_dir, alpha, U, V);
+    const int layer = find_layer(m, z, nn);
+    return interp_uv_bary<T>(m, f, lon, lat, nn, s.time_dir, layer, alpha, U, V);
+}
+
 // One 3-D stage of the unfused paths: exact anchor at the stage position,
-// layer at the stage depth, u/v and W from the stage blend.
+// u/v at the stage depth, W from the stage blend.
 template <typename T>
 __device__ __forceinline__ bool stage3d(const DMesh& m, const DBlend<T>& f, const DStep& s, int k, double lon,
                                         double lat, double z, const Site& q, double& U, double& V, double& W) {
     const int nn = site_anchor(m, q);
-    const int layer = find_layer(m, z, nn);
-    if (!interp_uv_bary<T>(m, f, lon, lat, nn, s.time_dir, layer, s.ak[k], U, V)) return false;
+    if (!stage_uv<T>(m, f, s, lon, lat, nn, z, s.ak[k], U, V)) return false;
     W = stage_w<T>(m, f, s.w_code, s.ak[k], lon, lat, z, nn, s.time_dir);
     return true;
 }
@@ -249,9 +260,8 @@ __device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DB
     const Site q0 = make_site(lon0, lat0);
     const int node_i = site_anchor(m, q0);
     int nn_out = node_i;
-    const int layer1 = find_layer(m, z0p, node_i);
     double U1, V1;
-    bool ok = interp_uv_bary<T>(m, f, lon0, lat0, node_i, td, layer1, s.ak[0], U1, V1);
+    bool ok = stage_uv<T>(m, f, s, lon0, lat0, node_i, z0p, s.ak[0], U1, V1);
     const double W1 = stage_w<T>(m, f, s.w_code, s.ak[0], lon0, lat0, z0p, node_i, td);
     st.U[i] = U1;
     st.V[i] = V1;
@@ -344,9 +354,8 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
     const Site q0 = make_site(lon0, lat0);
     const int node_i = site_anchor(m, q0);
     int nn_out = node_i;
-    const int layer1 = find_layer(m, z0p, node_i);
     double U1, V1;
-    const bool ok1 = interp_uv_bary<T>(m, f, lon0, lat0, node_i, td, layer1, s.ak[0], U1, V1);
+    const bool ok1 = stage_uv<T>(m, f, s, lon0, lat0, node_i, z0p, s.ak[0], U1, V1);
     const double W1 = stage_w<T>(m, f, s.w_code, s.ak[0], lon0, lat0, z0p, node_i, td);
     st.U[i] = U1;
     st.V[i] = V1;
@@ -359,9 +368,8 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
         const double z_mid = z0p + W1 * 0.5 * dt;
         const Site qm = make_site(lon_mid, lat_mid);
         const int nn_mid = site_anchor(m, qm);
-        const int layer2 = find_layer(m, z_mid, nn_mid);
         double U2, V2;
-        if (!interp_uv_bary<T>(m, f, lon_mid, lat_mid, nn_mid, td, layer2, s.ak[1], U2, V2)) {
+        if (!stage_uv<T>(m, f, s, lon_mid, lat_mid, nn_mid, z_mid, s.ak[1], U2, V2)) {
             status = OUTSIDE; fr = FR_INTERP;
         } else {
             const double W2 = stage_w<T>(m, f, s.w_code, s.ak[1], lon_mid, lat_mid, z_mid, nn_mid, td);

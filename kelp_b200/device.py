@@ -124,6 +124,25 @@ class DeviceContext:
         self._mesh_ref = mesh
         self._mesh_key = key
         self._slots.clear()
+        self._dl_key = None
+
+    def ensure_depth_points(self, mesh, placement: str) -> int:
+        """Upload the depth-linear data-point table of ``mesh`` for
+        ``placement`` (cached); returns its number of points M."""
+        self.ensure_mesh(mesh)
+        key = (self._mesh_key, placement, id(getattr(mesh, "depth", None)))
+        if getattr(self, "_dl_key", None) == key:
+            return self._dl_M
+        from .vertical_uv import depth_points
+        dp = depth_points(mesh, placement)
+        p = _c(dp.p, np.float64)
+        last = _c(dp.last, np.int32)
+        bed = _c(dp.bed, np.float64)
+        self._chk(N.lib().kc_depth_points_upload(self._ctx, int(p.size), N.ptr(p), N.ptr(last), N.ptr(bed)),
+                  "kc_depth_points_upload")
+        self._dl_key = key
+        self._dl_M = int(p.size)
+        return self._dl_M
 
     # -- snapshot ring --------------------------------------------------------
     def upload_field(self, field, slot: int, dtype=None) -> None:

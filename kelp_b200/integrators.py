@@ -77,7 +77,7 @@ def _fields(vel, vel_next):
     return vel_a, vel_b, target, alpha0
 
 
-def _check_node_fields(mesh, fields, is3d):
+def _check_node_fields(mesh, fields, is3d, placement="layer"):
     n = mesh.nodes_lon.shape[0]
     for f in fields:
         if getattr(f, "uv_layout", "element") != "node":
@@ -89,9 +89,13 @@ def _check_node_fields(mesh, fields, is3d):
         if is3d:
             zl = np.abs(np.asarray(mesh.sigma))
             w = np.asarray(f.w)
-            if w.shape != (zl.shape[0], n) or u.shape != (zl.shape[0] - 1, n):
-                raise ValueError(f"3-D layer fields need u/v ({zl.shape[0] - 1}, {n}) and w "
+            rows = {"layer": zl.shape[0] - 1, "level": zl.shape[0], "layer_linear": zl.shape[0] - 1}[placement]
+            if w.shape != (zl.shape[0], n) or u.shape != (rows, n):
+                raise ValueError(f"3-D {placement!r} fields need u/v ({rows}, {n}) and w "
                                  f"({zl.shape[0]}, {n}); got {u.shape} and {w.shape}")
+            if getattr(f, "uv_vertical", "layer") != placement:
+                raise ValueError("every field of one step needs the same uv_vertical placement "
+                                 "(integrators.py:4534-4553)")
 
 
 def _run(state, vel, mesh, dt, time_dir, scheme, c_coeffs, kw, ctx=None) -> ParticleState:
@@ -121,11 +125,13 @@ def _run(state, vel, mesh, dt, time_dir, scheme, c_coeffs, kw, ctx=None) -> Part
     _validate_time_aware(vel_next, dt_to_next, dt)
     is3d = _is_3d(vel)
     w_code = 0
+    placement = "layer"
     if is3d:
         if getattr(mesh, "vertical_coord", "zlevel") != "zlevel":
             raise NotImplementedError("sigma meshes are not built on the CUDA backend")
-        if getattr(vel, "uv_vertical", "layer") != "layer":
-            raise NotImplementedError("depth-linear u/v placement is not built on the CUDA backend")
+        placement = getattr(vel, "uv_vertical", "layer")
+        if placement not in ("layer", "level", "layer_linear"):
+            raise ValueError(f"unknown uv_vertical {placement!r}")
         w_interp = kw.get("w_interp", "leastsq")
         if w_interp not in ("nearest", "barycentric"):
             raise NotImplementedError(f"w_interp={w_interp!r} is not built on the CUDA backend")
@@ -136,10 +142,12 @@ def _run(state, vel, mesh, dt, time_dir, scheme, c_coeffs, kw, ctx=None) -> Part
             raise NotImplementedError("an endpoint LazyLerpField (alpha 0) takes the reference's unfused "
                                       "3-D RK2 path, which is not built on the CUDA backend")
     vel_a, vel_b, target, alpha0 = _fields(vel, vel_next)
-    _check_node_fields(mesh, [vel_a, vel_b, target], is3d)
+    _check_node_fields(mesh, [vel_a, vel_b, target], is3d, placement)
 
     ctx = ctx or default_context()
     ctx.ensure_mesh(mesh)
+    if is3d and placement != "layer":
+        ctx.ensure_depth_points(mesh, placement)
     sa, sb, st = ctx.slots_for([vel_a, vel_b, target])
     fr_in = state.failure_reason
     ctx.upload_particles(state.lon, state.lat, state.z, state.status, state.nearest_node,
@@ -155,6 +163,7 @@ def _run(state, vel, mesh, dt, time_dir, scheme, c_coeffs, kw, ctx=None) -> Part
     a.dt = float(dt)
     a.time_dir = float(time_dir)
     a.w_code = w_code
+    a.uv_vertical = 1 if placement != "layer" else 0
     if kick is not None:
         a.kick = 1
         a.kh_x, a.kh_y, a.seed, a.real_id, a.step_i, a.pid_offset = kick

@@ -124,11 +124,13 @@ def _gyre_uv(lon, lat, phase, amp):
 
 
 def gyre_snapshots(mesh, n_snap: int = 2, *, amp: float = 0.5, dtype=np.float32,
-                   z_levels=None, decay: float = 1000.0, w_scale: float = 1e-4):
+                   z_levels=None, decay: float = 1000.0, w_scale: float = 1e-4, placement: str = "layer"):
     """``n_snap`` node-layout snapshots, the phase advancing by 0.7 rad per
-    snapshot.  With ``z_levels`` (K interfaces): u/v (K-1, N) at the layer
-    mid-depths scaled by ``exp(-z / decay)``, and w (K, N) from continuity of
-    the divergent part (positive down, w = 0 at the surface)."""
+    snapshot.  With ``z_levels`` (K interfaces): u/v scaled by
+    ``exp(-z / decay)`` at the layer mid-depths ((K-1, N), placement
+    ``"layer"`` or ``"layer_linear"``) or on the levels ((K, N), placement
+    ``"level"``), and w (K, N) from continuity of the divergent part
+    (positive down, w = 0 at the surface)."""
     lon = np.asarray(mesh.nodes_lon)
     lat = np.asarray(mesh.nodes_lat)
     out = []
@@ -139,7 +141,7 @@ def gyre_snapshots(mesh, n_snap: int = 2, *, amp: float = 0.5, dtype=np.float32,
                                      uv_layout="node"))
             continue
         zl = np.asarray(z_levels, dtype=np.float64)
-        zm = 0.5 * (zl[:-1] + zl[1:])
+        zm = zl if placement == "level" else 0.5 * (zl[:-1] + zl[1:])
         dec = np.exp(-zm / decay)[:, None]
         div = np.sin(3 * lon * DEG2RAD + 0.7 * k) * np.cos(3 * lat * DEG2RAD)
         uu = (u[None, :] * dec).astype(dtype)
@@ -147,7 +149,7 @@ def gyre_snapshots(mesh, n_snap: int = 2, *, amp: float = 0.5, dtype=np.float32,
         # w(z) = -int_0^z div * f(z') dz', f = exp(-z/decay): closed form
         ww = (w_scale * div[None, :] * (1.0 - np.exp(-zl / decay))[:, None]).astype(dtype)
         out.append(VelocityField(u=uu, v=vv, w=ww, eta=np.zeros(lon.size), uv_layout="node",
-                                 uv_vertical="layer"))
+                                 uv_vertical=placement))
     return out
 
 

@@ -39,6 +39,9 @@ typedef struct {
     const int32_t *en, *n2e, *n2e_cnt, *gh_off, *gh_ids;
     double cell, lon_min, lat_min, r_earth;
     int nx, ny, wrap, far_rows, exact, K;
+    const double *dl_p, *dl_bed;      /* depth-linear table (vertical_uv.py:181-278) */
+    const int32_t* dl_last;
+    int dl_M;
 } OMesh;
 
 typedef struct {
@@ -713,7 +716,116 @@ typedef struct {
     int scheme, dims, w_code, kick;
     double dt, td, ak[4], kh_x, kh_y;
     uint64_t seed, real_id, step_i, pid_offset;
+    int uv_dl;
 } OStep;
+
+/* vertical_uv.py:457-523 uv_bracket */
+static void uv_bracket(const double* p, int li, double z, int* k, double* alpha) {
+    if (li <= 0) { *k = 0; *alpha = -1.0; return; }
+    double zc = z;
+    if (zc > p[li]) zc = p[li];
+    if (zc < p[0]) zc = p[0];
+    if (zc <= p[0]) { *k = 0; *alpha = -1.0; return; }
+    if (zc >= p[li]) { *k = li; *alpha = -1.0; return; }
+    int kk = li - 1;
+    for (int j = 0; j < li; ++j)
+        if (zc < p[j + 1]) { kk = j; break; }
+    double dz = p[kk + 1] - p[kk];
+    if (dz < 1e-12) { *k = kk; *alpha = -1.0; return; }
+    double a = (zc - p[kk]) / dz;
+    if (a <= 0.0) { *k = kk; *alpha = -1.0; return; }
+    if (a >= 1.0) { *k = kk + 1; *alpha = -1.0; return; }
+    *k = kk;
+    *alpha = a;
+}
+
+/* interpolate.py:1847-1876 _tinterp_point_uv */
+static void point_uv(const OField* f, int k, int nd, double alpha, double* u, double* v) {
+    int64_t idx = (int64_t)k * f->n + nd;
+    *u = tblend(fld(f->ua, f->f32, idx), fld(f->ub, f->f32, idx), fld(f->ut, f->f32, idx), f->alpha0, alpha);
+    *v = tblend(fld(f->va, f->f32, idx), fld(f->vb, f->f32, idx), fld(f->vt, f->f32, idx), f->alpha0, alpha);
+}
+
+/* interpolate.py:1879-1971 _interp_barycentric_core_tinterp_dl with
+ * :1664-1711 _dl_node_wall */
+static int interp_uv_dl(const OMesh* m, const OField* f, double xp, double yp, int nn, double z, double td,
+                        double alpha, double* U, double* V) {
+    *U = 0.0; *V = 0.0;
+    int elem = contain_local(m, xp, yp, nn);
+    if (elem < 0) return 0;
+    int verts[4], nv = 0;
+    for (int k = 0; k < m->max_v; ++k) {
+        int nd = m->en[(int64_t)elem * m->max_v + k];
+        if (nd < 0) continue;
+        if (nv > 0 && nd == verts[0]) continue;
+        verts[nv++] = nd;
+    }
+    if (nv < 3) return 0;
+    double R = m->r_earth;
+    double lon_ref = m->lon[verts[0]], dsum = 0.0, lat0 = 0.0;
+    for (int k = 0; k < nv; ++k) { dsum += wrap180(m->lon[verts[k]] - lon_ref); lat0 += m->lat[verts[k]]; }
+    double lon0 = lon_ref + dsum / nv;
+    lat0 /= nv;
+    double cosl = cos(lat0 * DEG2RAD);
+    double vx[4], vy[4];
+    for (int k = 0; k < nv; ++k) {
+        vx[k] = wrap180(m->lon[verts[k]] - lon0) * DEG2RAD * R * cosl;
+        vy[k] = (m->lat[verts[k]] - lat0) * DEG2RAD * R;
+    }
+    double px = wrap180(xp - lon0) * DEG2RAD * R * cosl;
+    double py = (yp - lat0) * DEG2RAD * R;
+    double w[4];
+    polygon_weights(px, py, vx, vy, nv, w);
+    if (w[0] == -1.0) return 0;
+    double zq = isnan(z) ? INFINITY : z;
+    int wet[4], n_wet = 0;
+    for (int k = 0; k < nv; ++k) { wet[k] = zq <= m->dl_bed[verts[k]]; n_wet += wet[k]; }
+    if (n_wet == 0) {
+        int kd = 0;
+        for (int k = 1; k < nv; ++k)
+            if (m->dl_bed[verts[k]] > m->dl_bed[verts[kd]]) kd = k;
+        double un, vn;
+        point_uv(f, m->dl_last[verts[kd]], verts[kd], alpha, &un, &vn);
+        *U = td * un; *V = td * vn;
+        return 1;
+    }
+    double den = 1.0;
+    if (n_wet < nv) {
+        double wsum = 0.0;
+        for (int k = 0; k < nv; ++k)
+            if (wet[k]) { if (w[k] < 0.0) w[k] = 0.0; wsum += w[k]; }
+        if (wsum < 1e-12) {
+            for (int k = 0; k < nv; ++k) if (wet[k]) w[k] = 1.0;
+            den = (double)n_wet;
+        } else den = wsum;
+    }
+    double Us = 0.0, Vs = 0.0;
+    for (int k = 0; k < nv; ++k) {
+        int nd = verts[k];
+        if (n_wet < nv && !wet[k]) continue;
+        int kb;
+        double ab, un, vn;
+        uv_bracket(m->dl_p, m->dl_last[nd], zq, &kb, &ab);
+        point_uv(f, kb, nd, alpha, &un, &vn);
+        if (!(ab < 0.0)) {
+            double un1, vn1;
+            point_uv(f, kb + 1, nd, alpha, &un1, &vn1);
+            un = (1.0 - ab) * un + ab * un1;
+            vn = (1.0 - ab) * vn + ab * vn1;
+        }
+        Us += w[k] * un; Vs += w[k] * vn;
+    }
+    if (n_wet < nv) { Us = Us / den; Vs = Vs / den; }
+    *U = td * Us; *V = td * Vs;
+    return 1;
+}
+
+/* u/v of a 3-D stage: the layer rule or the depth-linear rule */
+static int stage_uv(const OMesh* m, const OField* f, const OStep* s, double xp, double yp, int nn, double z,
+                    double alpha, double* U, double* V) {
+    if (s->uv_dl) return interp_uv_dl(m, f, xp, yp, nn, z, s->td, alpha, U, V);
+    return interp_uv(m, f, xp, yp, nn, s->td, find_layer(m, z, m->depth[nn]), alpha, U, V);
+}
 
 static double z0_of(double lat) {
     double z0 = cos(lat * DEG2RAD) * SLM;
@@ -817,9 +929,8 @@ static void step_one(const OMesh* m, const OField* f, const OStep* s, int64_t i,
          * per stage, layer at the stage depth, stage fields blended per vertex
          * (the whole-field lerps of _make_stage_vels, :1187-1237), W at the
          * stage position, failure reverts to the start with the start anchor. */
-        int l1 = find_layer(m, zp, m->depth[node_i]);
         double U1, V1;
-        int ok1 = interp_uv(m, f, lon0, lat0, node_i, td, l1, s->ak[0], &U1, &V1);
+        int ok1 = stage_uv(m, f, s, lon0, lat0, node_i, zp, s->ak[0], &U1, &V1);
         double W1 = s->w_code == 0 ? w_linear(m, f, s->ak[0], zp, node_i, td)
                                    : w_bary(m, f, s->ak[0], lon0, lat0, zp, node_i, td);
         U[i] = U1; V[i] = V1; W[i] = W1;
@@ -834,21 +945,21 @@ static void step_one(const OMesh* m, const OField* f, const OStep* s, int64_t i,
             double l2 = wrap180(lon0 + 0.5 * dl1), t2 = clat(lat0 + 0.5 * dd1), z2 = zp + 0.5 * dz1;
             int n2 = anchor(m, l2, t2);
             double U2, V2, U3, V3, U4, V4;
-            if (!interp_uv(m, f, l2, t2, n2, td, find_layer(m, z2, m->depth[n2]), s->ak[1], &U2, &V2)) ok = 0;
+            if (!stage_uv(m, f, s, l2, t2, n2, z2, s->ak[1], &U2, &V2)) ok = 0;
             else {
                 double W2 = s->w_code == 0 ? w_linear(m, f, s->ak[1], z2, n2, td)
                                            : w_bary(m, f, s->ak[1], l2, t2, z2, n2, td);
                 double dl2 = dt * U2 / z0_of(t2), dd2 = dt * V2 / SLM, dz2 = dt * W2;
                 double l3 = wrap180(lon0 + 0.5 * dl2), t3 = clat(lat0 + 0.5 * dd2), z3 = zp + 0.5 * dz2;
                 int n3 = anchor(m, l3, t3);
-                if (!interp_uv(m, f, l3, t3, n3, td, find_layer(m, z3, m->depth[n3]), s->ak[2], &U3, &V3)) ok = 0;
+                if (!stage_uv(m, f, s, l3, t3, n3, z3, s->ak[2], &U3, &V3)) ok = 0;
                 else {
                     double W3 = s->w_code == 0 ? w_linear(m, f, s->ak[2], z3, n3, td)
                                                : w_bary(m, f, s->ak[2], l3, t3, z3, n3, td);
                     double dl3 = dt * U3 / z0_of(t3), dd3 = dt * V3 / SLM, dz3 = dt * W3;
                     double l4 = wrap180(lon0 + dl3), t4 = clat(lat0 + dd3), z4 = zp + dz3;
                     int n4 = anchor(m, l4, t4);
-                    if (!interp_uv(m, f, l4, t4, n4, td, find_layer(m, z4, m->depth[n4]), s->ak[3], &U4, &V4)) ok = 0;
+                    if (!stage_uv(m, f, s, l4, t4, n4, z4, s->ak[3], &U4, &V4)) ok = 0;
                     else {
                         double W4 = s->w_code == 0 ? w_linear(m, f, s->ak[3], z4, n4, td)
                                                    : w_bary(m, f, s->ak[3], l4, t4, z4, n4, td);
@@ -874,9 +985,8 @@ static void step_one(const OMesh* m, const OField* f, const OStep* s, int64_t i,
             }
         }
     } else {
-        int l1 = find_layer(m, zp, m->depth[node_i]);
         double U1, V1;
-        int ok1 = interp_uv(m, f, lon0, lat0, node_i, td, l1, s->ak[0], &U1, &V1);
+        int ok1 = stage_uv(m, f, s, lon0, lat0, node_i, zp, s->ak[0], &U1, &V1);
         double W1 = s->w_code == 0 ? w_linear(m, f, s->ak[0], zp, node_i, td)
                                    : w_bary(m, f, s->ak[0], lon0, lat0, zp, node_i, td);
         U[i] = U1; V[i] = V1; W[i] = W1;
@@ -886,9 +996,8 @@ static void step_one(const OMesh* m, const OField* f, const OStep* s, int64_t i,
             double tm = clat(lat0 + 0.5 * dt * V1 / SLM);
             double zm = zp + W1 * 0.5 * dt;
             int nm = anchor(m, lm, tm);
-            int l2 = find_layer(m, zm, m->depth[nm]);
             double U2, V2;
-            if (!interp_uv(m, f, lm, tm, nm, td, l2, s->ak[1], &U2, &V2)) { st = OUTSIDE; frr = 1; }
+            if (!stage_uv(m, f, s, lm, tm, nm, zm, s->ak[1], &U2, &V2)) { st = OUTSIDE; frr = 1; }
             else {
                 double W2 = s->w_code == 0 ? w_linear(m, f, s->ak[1], zm, nm, td)
                                            : w_bary(m, f, s->ak[1], lm, tm, zm, nm, td);
@@ -973,6 +1082,9 @@ typedef struct {
     const int32_t *en, *n2e, *n2e_cnt, *gh_off, *gh_ids;
     double cell, lon_min, lat_min, r_earth;
     int nx, ny, wrap, far_rows, exact, K;
+    const double *dl_p, *dl_bed;
+    const int32_t* dl_last;
+    int dl_M;
 } orc_mesh;
 
 typedef struct {
@@ -986,6 +1098,7 @@ typedef struct {
     int scheme, dims, w_code, kick;
     double dt, td, ak[4], kh_x, kh_y;
     uint64_t seed, real_id, step_i, pid_offset;
+    int uv_dl;
 } orc_step_args;
 
 typedef struct {

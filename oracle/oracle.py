@@ -26,7 +26,8 @@ class OMesh(C.Structure):
                 ("gh_off", C.c_void_p), ("gh_ids", C.c_void_p),
                 ("cell", C.c_double), ("lon_min", C.c_double), ("lat_min", C.c_double), ("r_earth", C.c_double),
                 ("nx", C.c_int), ("ny", C.c_int), ("wrap", C.c_int), ("far_rows", C.c_int),
-                ("exact", C.c_int), ("K", C.c_int)]
+                ("exact", C.c_int), ("K", C.c_int),
+                ("dl_p", C.c_void_p), ("dl_bed", C.c_void_p), ("dl_last", C.c_void_p), ("dl_M", C.c_int)]
 
 
 class OField(C.Structure):
@@ -41,7 +42,7 @@ class OStep(C.Structure):
                 ("dt", C.c_double), ("td", C.c_double), ("ak", C.c_double * 4),
                 ("kh_x", C.c_double), ("kh_y", C.c_double),
                 ("seed", C.c_uint64), ("real_id", C.c_uint64), ("step_i", C.c_uint64),
-                ("pid_offset", C.c_uint64)]
+                ("pid_offset", C.c_uint64), ("uv_dl", C.c_int)]
 
 
 _lib = None
@@ -112,6 +113,32 @@ class MeshView:
         s.exact = int(bool((mesh.metadata or {}).get("exact_nearest", False)))
         s.K = 0 if self.zl is None else int(self.zl.size)
         self.s = s
+        self.mesh = mesh
+        self.placement = None
+
+    def use_placement(self, placement: str) -> None:
+        """Attach the depth-linear data-point table for ``placement``
+        (vertical_uv.py:181-278, node layout; z-level meshes)."""
+        if placement == self.placement:
+            return
+        z = np.abs(np.asarray(self.mesh.sigma, dtype=np.float64))
+        if placement == "level":
+            p, lower = z.copy(), z
+        else:
+            p, lower = 0.5 * (z[:-1] + z[1:]), z[1:]
+        d = np.asarray(self.mesh.depth, dtype=np.float64)
+        geo = np.searchsorted(lower, d, side="right").astype(np.int64) - 1
+        geo[np.isnan(d)] = 0
+        last = np.minimum(geo, p.size - 1)
+        decl = (getattr(self.mesh, "metadata", None) or {}).get("uv_data_last")
+        if decl is not None:
+            last = np.minimum(last, np.asarray(decl).astype(np.int64))
+        self.dl_p = np.ascontiguousarray(p)
+        self.dl_last = np.ascontiguousarray(np.maximum(last, 0), dtype=np.int32)
+        self.dl_bed = np.ascontiguousarray(d.copy())
+        self.s.dl_p, self.s.dl_bed, self.s.dl_last = _p(self.dl_p), _p(self.dl_bed), _p(self.dl_last)
+        self.s.dl_M = int(self.dl_p.size)
+        self.placement = placement
 
 
 def _field_arrays(f, dtype):
@@ -141,10 +168,14 @@ def step(state, vel, mesh, dt, time_dir, scheme: str, *, vel_next=None, dt_to_ne
     of.alpha0 = alpha0
     of.n = view.lon.size
     is3d = arrs[0][2] is not None
+    placement = getattr(vel_a, "uv_vertical", "layer")
+    if is3d and placement != "layer":
+        view.use_placement(placement)
     os_ = OStep()
     os_.scheme = {"euler": 0, "rk2": 1, "rk4": 2}[scheme]
     os_.dims = 3 if is3d else 2
     os_.w_code = 0 if w_interp == "nearest" else 1
+    os_.uv_dl = 1 if (is3d and placement != "layer") else 0
     cc = {"euler": (0.0,), "rk2": (0.0, 0.5), "rk4": (0.0, 0.5, 0.5, 1.0)}[scheme]
     if vel_next is not None and scheme != "euler":
         for k, c in enumerate(cc):

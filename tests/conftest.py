@@ -44,12 +44,14 @@ class Golden:
         m.metadata = {"exact_nearest": True}
         self.mesh = m
         from kelp_b200.fields import VelocityField
+        placement = {"golden_dl_lev": "level", "golden_dl_llin": "layer_linear"}.get(name, "layer")
         self.snaps = []
         i = 0
         while f"snap{i}_u" in self.d:
             w = self.d.get(f"snap{i}_w")
             self.snaps.append(VelocityField(u=self.d[f"snap{i}_u"], v=self.d[f"snap{i}_v"], w=w,
-                                            eta=np.zeros(self.d[f"snap{i}_u"].shape[-1]), uv_layout="node"))
+                                            eta=np.zeros(self.d[f"snap{i}_u"].shape[-1]), uv_layout="node",
+                                            uv_vertical=placement if w is not None else "layer"))
             i += 1
 
     def cases(self):

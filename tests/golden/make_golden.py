@@ -211,6 +211,25 @@ def main():
              "euler_wbary": run_case(rm, rf, lon, lat, z, status, "euler", 10800.0, T, 16, w_interp="barycentric")}
     save("golden_3d", mesh_record(rm), snaps, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
 
+    # --- depth-linear u/v (uv_vertical level / layer_linear) on the same mesh;
+    # a fifth of the particles start below their shallowest vertex (walls)
+    zdl = z.copy()
+    deep = np.random.default_rng(21).uniform(size=zdl.size) < 0.2
+    zdl[deep] *= 1.6
+    cases = {}
+    for placement, tag in (("level", "lev"), ("layer_linear", "llin")):
+        sn = S.gyre_snapshots(m, 4, amp=1.5, z_levels=zl, decay=800.0, w_scale=2e-3, placement=placement)
+        rfp = [RVel(u=s.u, v=s.v, w=s.w, eta=np.zeros(s.u.shape[-1]), uv_layout="node", uv_vertical=placement)
+               for s in sn]
+        cases[f"rk2_{tag}_wbary"] = run_case(rm, rfp, lon, lat, zdl, status, "rk2", 21600.0, T, 12,
+                                             w_interp="barycentric")
+        cases[f"rk4_{tag}_wnear_kick"] = run_case(rm, rfp, lon, lat, zdl, status, "rk4", 21600.0, T, 10,
+                                                  w_interp="nearest", kh=(2.0e4, 2.0e4), seed=4)
+        cases[f"euler_{tag}_wnear"] = run_case(rm, rfp, lon, lat, zdl, status, "euler", 10800.0, T, 8,
+                                               w_interp="nearest")
+        save(f"golden_dl_{tag}", mesh_record(rm), sn, {k: v for k, v in cases.items() if f"_{tag}_" in k},
+             {"lon": lon, "lat": lat, "z": zdl, "status": status})
+
     # --- counter RNG: normal pairs of the reference for a key grid ----------
     keys = []
     vals = []

@@ -18,6 +18,8 @@ CASES = [("golden_band", c) for c in ("rk2", "rk4", "euler", "rk2_bwd", "rk2_kic
 CASES += [("golden_quad", c) for c in ("rk2", "rk4", "euler", "rk2_kick")]
 CASES += [("golden_polar", "rk2")]
 CASES += [("golden_3d", c) for c in ("rk2_wnear", "rk2_wbary", "rk2_wbary_kick", "rk4_wnear", "rk4_wbary_kick", "euler_wbary")]
+CASES += [("golden_dl_lev", c) for c in ("rk2_lev_wbary", "rk4_lev_wnear_kick", "euler_lev_wnear")]
+CASES += [("golden_dl_llin", c) for c in ("rk2_llin_wbary", "rk4_llin_wnear_kick", "euler_llin_wnear")]
 
 
 def replay_oracle(g, cname):
