@@ -90,6 +90,18 @@ typedef struct kc_step_args {
     long long global_step;       /* delayed-release activation step, -1 for none */
 } kc_step_args;
 
+/* Beaching / resuspension of one step (src/kelp/tracking.py:199-364,
+ * src/kelp/numerics/beaching.py:95-181).  Criteria flags mirror
+ * beaching.criteria; resuspension: 0 never, 1 auto, 2 stochastic,
+ * 3 auto_or_stochastic.  p_beach = 1 - exp(-|dt| / t_beach) and
+ * p_resusp = 1 - exp(-|dt| / t_resuspend) are evaluated by the caller. */
+typedef struct kc_beach_args {
+    int use_depth, use_coastal, use_stochastic, on_failure;
+    int resuspension, min_wet_steps;
+    double depth_min, zone_depth, rewet_hysteresis, p_beach, p_resusp;
+    unsigned long long seed, real_id, step_i, pid_offset;
+} kc_beach_args;
+
 int kc_abi_version(void);
 
 /* Host routine: unit-sphere node table with the C library's cos/sin. */
@@ -121,6 +133,20 @@ int kc_particles_upload(kc_ctx* ctx, long long P, const double* lon, const doubl
 int kc_particles_download(kc_ctx* ctx, long long P, double* lon, double* lat, double* z,
                           int* status, int* nearest_node, signed char* failure_reason,
                           double* u, double* v, double* w);
+
+/* Coastal element flags (E bytes, 1 = owns a boundary edge;
+ * src/kelp/core/mesh.py:2764-2821 build_boundary_info). */
+int kc_coastal_upload(kc_ctx* ctx, const unsigned char* elem_is_coastal);
+
+/* Beaching state of the resident particles: the status each had when its
+ * last step began (NULL: the status the next kc_step records) and the
+ * consecutive-wet-step counters (NULL: zeros).  After this call every step
+ * records the entry status for the hook; kc_particles_upload clears it. */
+int kc_beach_state_upload(kc_ctx* ctx, const int* prev_status, const int* wet_streak);
+int kc_beach_state_download(kc_ctx* ctx, int* wet_streak);
+
+/* The beaching hook on the resident particles after a step. */
+int kc_beach(kc_ctx* ctx, const kc_beach_args* args);
 
 /* One step of every resident particle; kc_run: n_steps steps in order,
  * per-step arguments, no host round trip in between. */
@@ -156,7 +182,9 @@ int kc_find_nearest_noalloc(kc_ctx* ctx, long long P, const double* lon, const d
 int kc_rng_normals(kc_ctx* ctx, long long P, unsigned long long seed, unsigned long long real_id,
                    unsigned long long step_i, unsigned long long pid_offset, double* out);
 
-/* Device error word (bitmask of iteration caps hit since the last call). */
+/* Device error word since the last call: bit 0 an exact-search iteration cap
+ * was hit, bit 1 kc_beach met a nearest_node outside [-n_nodes, n_nodes) and
+ * left that particle unchanged. */
 int kc_device_errors(kc_ctx* ctx, int* word);
 
 /* Timing on the context's stream: record event `slot` (0..15), and the

@@ -21,8 +21,22 @@ KC_EULER, KC_RK2, KC_RK4 = 0, 1, 2
 #: every symbol include/kelp_cuda.h declares
 EXPORTS = ("kc_abi_version", "kc_node_xyz_fill", "kc_create", "kc_destroy", "kc_last_error",
            "kc_synchronize", "kc_mesh_upload", "kc_depth_points_upload", "kc_field_upload", "kc_particles_upload",
-           "kc_particles_download", "kc_step", "kc_run", "kc_sort", "kc_find_nearest", "kc_find_nearest_noalloc", "kc_rng_normals", "kc_device_errors",
+           "kc_particles_download", "kc_coastal_upload", "kc_beach_state_upload",
+           "kc_beach_state_download", "kc_beach", "kc_step", "kc_run", "kc_sort", "kc_find_nearest", "kc_find_nearest_noalloc", "kc_rng_normals", "kc_device_errors",
            "kc_event_record", "kc_event_elapsed", "kc_l2_flush", "kc_host_alloc", "kc_host_free")
+
+
+#: device error word bits (kc_device_errors)
+ERR_SEARCH_CAP, ERR_BAD_ANCHOR = 1, 2
+
+
+def describe_device_errors(word: int) -> str:
+    parts = []
+    if word & ERR_SEARCH_CAP:
+        parts.append("a device-side search iteration cap was hit")
+    if word & ERR_BAD_ANCHOR:
+        parts.append("a particle's nearest_node lies outside [-n_nodes, n_nodes)")
+    return "; ".join(parts) or f"device error word {word:#x}"
 
 
 class KcError(RuntimeError):
@@ -58,6 +72,15 @@ class StepArgs(C.Structure):
                 ("global_step", C.c_longlong)]
 
 
+class BeachArgs(C.Structure):
+    _fields_ = [("use_depth", C.c_int), ("use_coastal", C.c_int), ("use_stochastic", C.c_int),
+                ("on_failure", C.c_int), ("resuspension", C.c_int), ("min_wet_steps", C.c_int),
+                ("depth_min", C.c_double), ("zone_depth", C.c_double), ("rewet_hysteresis", C.c_double),
+                ("p_beach", C.c_double), ("p_resusp", C.c_double),
+                ("seed", C.c_ulonglong), ("real_id", C.c_ulonglong),
+                ("step_i", C.c_ulonglong), ("pid_offset", C.c_ulonglong)]
+
+
 _lib = None
 
 
@@ -82,6 +105,10 @@ def lib():
         L.kc_depth_points_upload.argtypes = [vp, i, vp, vp, vp]
         L.kc_particles_upload.argtypes = [vp, ll, vp, vp, vp, vp, vp, vp, vp, vp]
         L.kc_particles_download.argtypes = [vp, ll, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.kc_coastal_upload.argtypes = [vp, vp]
+        L.kc_beach_state_upload.argtypes = [vp, vp, vp]
+        L.kc_beach_state_download.argtypes = [vp, vp]
+        L.kc_beach.argtypes = [vp, C.POINTER(BeachArgs)]
         L.kc_step.argtypes = [vp, C.POINTER(StepArgs)]
         L.kc_run.argtypes = [vp, C.POINTER(StepArgs), i]
         L.kc_sort.argtypes = [vp]

@@ -12,7 +12,7 @@
 
 #include "../../include/kelp_cuda.h"
 #include "kc_host.h"
-#include "kc_step.cuh"
+#include "kc_beach.cuh"
 
 namespace {
 
@@ -68,6 +68,11 @@ struct kc_ctx {
     // spare buffer of the gathers, radix-sort keys / indices and CUB's storage
     long long* orig = nullptr;
     void* spare = nullptr;
+    // beaching: entry status of the last step, wet-step counters, coastal flags
+    int* prev = nullptr;
+    int* wet = nullptr;
+    bool has_beach = false;
+    unsigned char* d_coastal = nullptr;
     bool sorted = false;
     unsigned* skey[2] = {nullptr, nullptr};
     int* sidx[2] = {nullptr, nullptr};
@@ -116,6 +121,7 @@ kc::DState state_of(kc_ctx* c) {
     st.U = c->U; st.V = c->V; st.W = c->W; st.fr = c->fr;
     st.pid = c->has_pid ? c->pid : nullptr;
     st.release_step = c->has_rs ? c->rs : nullptr;
+    st.prev = c->has_beach ? c->prev : nullptr;
     st.P = c->P;
     return st;
 }
@@ -143,6 +149,7 @@ __global__ void __launch_bounds__(kBlock) k_step2d(const __grid_constant__ kc::D
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= st.P) return;
     activate(st, s, i);
+    if (st.prev) st.prev[i] = st.status[i];
     kc::step2d_particle<T, SCHEME>(m, f, st, s, i);
 }
 
@@ -151,6 +158,7 @@ __global__ void __launch_bounds__(kBlock) k_step3d_rk2(const __grid_constant__ k
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= st.P) return;
     activate(st, s, i);
+    if (st.prev) st.prev[i] = st.status[i];
     kc::step3d_rk2_particle<T>(m, f, st, s, i);
 }
 
@@ -162,6 +170,7 @@ __global__ void __launch_bounds__(kBlock) k_step3d_unfused(const __grid_constant
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= st.P) return;
     activate(st, s, i);
+    if (st.prev) st.prev[i] = st.status[i];
     kc::step3d_unfused_particle<T, SCHEME>(m, f, st, s, i);
 }
 
@@ -179,6 +188,14 @@ __global__ void __launch_bounds__(kBlock) k_normals(long long P, unsigned long l
     kc::normal_pair(seed, real_id, (unsigned long long)i + pid0, step, 0ull, g1, g2);
     out[2 * i] = g1;
     out[2 * i + 1] = g2;
+}
+
+__global__ void __launch_bounds__(kBlock) k_beach(const __grid_constant__ kc::DMesh m,
+                                                  const __grid_constant__ kc::DState st,
+                                                  const __grid_constant__ kc::DBeach b, long long N) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= st.P) return;
+    kc::beach_particle(m, st, b, N, i);
 }
 
 __global__ void k_iota64(long long* out, long long P) {
@@ -330,7 +347,7 @@ int upload(kc_ctx* c, T** dst, const void* src, size_t count) {
 void free_mesh(kc_ctx* c) {
     dfree(c->d_ll); dfree(c->d_en); dfree(c->d_n2e_off); dfree(c->d_n2e); dfree(c->d_gh_off);
     dfree(c->d_gh_tab); dfree(c->d_xyz); dfree(c->d_depth); dfree(c->d_zlev);
-    dfree(c->d_nsc); dfree(c->d_ecos); dfree(c->d_maxl);
+    dfree(c->d_nsc); dfree(c->d_ecos); dfree(c->d_maxl); dfree(c->d_coastal);
     dfree(c->d_dl_p); dfree(c->d_dl_last); dfree(c->d_dl_bed);
     c->dm.dl_p = nullptr; c->dm.dl_last = nullptr; c->dm.dl_bed = nullptr; c->dm.dl_M = 0;
     c->has_mesh = false;
@@ -339,7 +356,8 @@ void free_mesh(kc_ctx* c) {
 void free_particles(kc_ctx* c) {
     dfree(c->lon); dfree(c->lat); dfree(c->z); dfree(c->U); dfree(c->V); dfree(c->W);
     dfree(c->status); dfree(c->nn); dfree(c->fr); dfree(c->pid); dfree(c->rs);
-    dfree(c->orig); dfree(c->spare);
+    dfree(c->orig); dfree(c->spare); dfree(c->prev); dfree(c->wet);
+    c->has_beach = false;
     dfree(c->skey[0]); dfree(c->skey[1]); dfree(c->sidx[0]); dfree(c->sidx[1]); dfree(c->cub_tmp);
     c->P = c->cap = c->sort_cap = 0;
     c->sorted = false;
@@ -481,6 +499,75 @@ int kc_mesh_upload(kc_ctx* c, const kc_mesh_desc* d) {
     return KC_OK;
 }
 
+int kc_coastal_upload(kc_ctx* c, const unsigned char* flags) {
+    if (!c || !flags) return KC_ERR_ARG;
+    if (!c->has_mesh) return fail(c, KC_ERR_STATE, "kc_coastal_upload: no mesh uploaded");
+    KC_CUDA(c, cudaSetDevice(c->device));
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    dfree(c->d_coastal);
+    int rc = upload(c, &c->d_coastal, flags, (size_t)c->E);
+    if (rc) return rc;
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KC_OK;
+}
+
+int kc_beach_state_upload(kc_ctx* c, const int* prev_status, const int* wet_streak) {
+    if (!c) return KC_ERR_ARG;
+    if (c->P > 0 && !c->prev) return fail(c, KC_ERR_STATE, "kc_beach_state_upload: no particles uploaded");
+    KC_CUDA(c, cudaSetDevice(c->device));
+    if (c->sorted) return fail(c, KC_ERR_STATE, "kc_beach_state_upload: upload the beaching state before kc_sort");
+    const size_t n = (size_t)c->P * 4;
+    if (c->P > 0) {
+        if (prev_status) KC_CUDA(c, cudaMemcpyAsync(c->prev, prev_status, n, cudaMemcpyHostToDevice, c->stream));
+        else KC_CUDA(c, cudaMemcpyAsync(c->prev, c->status, n, cudaMemcpyDeviceToDevice, c->stream));
+        if (wet_streak) KC_CUDA(c, cudaMemcpyAsync(c->wet, wet_streak, n, cudaMemcpyHostToDevice, c->stream));
+        else KC_CUDA(c, cudaMemsetAsync(c->wet, 0, n, c->stream));
+    }
+    c->has_beach = true;
+    return KC_OK;
+}
+
+int kc_beach_state_download(kc_ctx* c, int* wet_streak) {
+    if (!c || !wet_streak) return KC_ERR_ARG;
+    if (!c->has_beach) return fail(c, KC_ERR_STATE, "kc_beach_state_download: no beaching state");
+    KC_CUDA(c, cudaSetDevice(c->device));
+    int rc = fetch(c, wet_streak, c->wet, 4);
+    if (rc) return rc;
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KC_OK;
+}
+
+int kc_beach(kc_ctx* c, const kc_beach_args* a) {
+    if (!c || !a) return KC_ERR_ARG;
+    if (!c->has_mesh) return fail(c, KC_ERR_STATE, "kc_beach: no mesh uploaded");
+    if (!c->has_beach) return fail(c, KC_ERR_STATE, "kc_beach: call kc_beach_state_upload first");
+    if (!c->d_depth) return fail(c, KC_ERR_STATE, "kc_beach: the mesh has no depth");
+    if (a->resuspension < 0 || a->resuspension > 3) return fail(c, KC_ERR_ARG, "kc_beach: resuspension code");
+    const bool need_topo = a->use_coastal || a->use_stochastic;
+    if (need_topo && !c->d_coastal) return fail(c, KC_ERR_STATE, "kc_beach: coastal flags not uploaded");
+    if (c->P == 0) return KC_OK;
+    KC_CUDA(c, cudaSetDevice(c->device));
+    kc::DBeach b;
+    b.use_depth = a->use_depth; b.use_coastal = a->use_coastal; b.use_stochastic = a->use_stochastic;
+    b.on_failure = a->on_failure; b.need_topo = need_topo ? 1 : 0; b.resuspension = a->resuspension;
+    b.min_wet_steps = a->min_wet_steps;
+    b.depth_min = a->depth_min; b.zone_depth = a->zone_depth;
+    b.rewet_level = a->depth_min + a->rewet_hysteresis;
+    b.p_beach = a->p_beach; b.p_resusp = a->p_resusp;
+    b.seed = a->seed; b.real_id = a->real_id; b.step_i = a->step_i; b.pid_offset = a->pid_offset;
+    b.coastal = need_topo ? c->d_coastal : nullptr;
+    b.prev = c->prev;
+    b.wet_streak = c->wet;
+    if (!c->has_pid) {   // the RNG key stays the slot index the particles were uploaded with
+        KC_CUDA(c, cudaMemcpyAsync(c->pid, c->orig, (size_t)c->P * 8, cudaMemcpyDeviceToDevice, c->stream));
+        c->has_pid = true;
+    }
+    kc::DState st = state_of(c);
+    k_beach<<<grid_for(c->P), kBlock, 0, c->stream>>>(c->dm, st, b, c->N);
+    KC_CUDA(c, cudaGetLastError());
+    return KC_OK;
+}
+
 int kc_depth_points_upload(kc_ctx* c, int M, const double* p, const int* last, const double* bed) {
     if (!c) return KC_ERR_ARG;
     if (!c->has_mesh) return fail(c, KC_ERR_STATE, "kc_depth_points_upload: no mesh uploaded");
@@ -555,10 +642,12 @@ int kc_particles_upload(kc_ctx* c, long long P, const double* lon, const double*
         KC_CUDA(c, cudaMalloc((void**)&c->fr, n)); KC_CUDA(c, cudaMalloc((void**)&c->pid, n));
         KC_CUDA(c, cudaMalloc((void**)&c->rs, n)); KC_CUDA(c, cudaMalloc((void**)&c->orig, n));
         KC_CUDA(c, cudaMalloc((void**)&c->spare, n));
+        KC_CUDA(c, cudaMalloc((void**)&c->prev, n)); KC_CUDA(c, cudaMalloc((void**)&c->wet, n));
         c->cap = P;
     }
     c->P = P;
     c->sorted = false;
+    c->has_beach = false;   // the beaching state belongs to the particles it was uploaded with
     if (P == 0) return KC_OK;
     size_t n = (size_t)P;
     cudaStream_t s = c->stream;
@@ -648,6 +737,10 @@ int kc_sort(kc_ctx* c) {
     if ((rc = regather(c, (void**)&c->nn, 4, idx))) return rc;
     if ((rc = regather(c, (void**)&c->fr, 1, idx))) return rc;
     if (c->has_rs && (rc = regather(c, (void**)&c->rs, 4, idx))) return rc;
+    if (c->has_beach) {
+        if ((rc = regather(c, (void**)&c->prev, 4, idx))) return rc;
+        if ((rc = regather(c, (void**)&c->wet, 4, idx))) return rc;
+    }
     c->sorted = true;
     return KC_OK;
 }

@@ -32,6 +32,7 @@ constexpr int FR_INTERP = 1, FR_OOB = 2;
 
 // device error word bits (read back by the host)
 constexpr int ERR_SEARCH_CAP = 1;   // exact-search growth loop hit its cap
+constexpr int ERR_BAD_ANCHOR = 2;   // a particle's nearest_node is outside [-N, N)
 
 // Resident mesh: node table, element table, node->element CSR, grid hash and
 // the host-evaluated trigonometric tables.

@@ -24,6 +24,7 @@ struct DState {
     signed char* fr;
     const long long* pid;      // stable particle id (RNG key), index when null
     const int* release_step;   // delayed release (null: all released)
+    int* prev;                 // status at the step's entry, for the beaching hook (null: not kept)
     long long P;
 };
 

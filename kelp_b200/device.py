@@ -125,6 +125,7 @@ class DeviceContext:
         self._mesh_key = key
         self._slots.clear()
         self._dl_key = None
+        self._coastal_key = None
 
     def ensure_depth_points(self, mesh, placement: str) -> int:
         """Upload the depth-linear data-point table of ``mesh`` for
@@ -218,6 +219,35 @@ class DeviceContext:
             N.ptr(out["nearest_node"]), N.ptr(out["failure_reason"]), N.ptr(out["u"]), N.ptr(out["v"]),
             N.ptr(out["w"])), "kc_particles_download")
         return out
+
+    # -- beaching ----------------------------------------------------------------
+    def ensure_coastal(self, mesh, flags) -> None:
+        """Upload the coastal element flags of the resident mesh (cached)."""
+        self.ensure_mesh(mesh)
+        key = (self._mesh_key, id(flags))
+        if getattr(self, "_coastal_key", None) == key:
+            return
+        f = np.ascontiguousarray(flags, dtype=np.uint8)
+        if f.shape != (np.asarray(mesh.elem_nodes).shape[0],):
+            raise ValueError("coastal flags must have one entry per element")
+        self._chk(N.lib().kc_coastal_upload(self._ctx, N.ptr(f)), "kc_coastal_upload")
+        self._coastal_key = key
+
+    def beach_state_upload(self, prev_status=None, wet_streak=None) -> None:
+        prev = None if prev_status is None else _c(prev_status, np.int32)
+        wet = None if wet_streak is None else _c(wet_streak, np.int32)
+        for a in (prev, wet):
+            if a is not None and a.shape != (self.P,):
+                raise ValueError("beaching state arrays must have one entry per particle")
+        self._chk(N.lib().kc_beach_state_upload(self._ctx, N.ptr(prev), N.ptr(wet)), "kc_beach_state_upload")
+
+    def beach_state_download(self) -> np.ndarray:
+        out = np.empty(self.P, np.int32)
+        self._chk(N.lib().kc_beach_state_download(self._ctx, N.ptr(out)), "kc_beach_state_download")
+        return out
+
+    def beach(self, args: N.BeachArgs) -> None:
+        self._chk(N.lib().kc_beach(self._ctx, C.byref(args)), "kc_beach")
 
     # -- work -------------------------------------------------------------------
     def step(self, args: N.StepArgs) -> None:

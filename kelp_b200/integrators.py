@@ -24,6 +24,7 @@ from .particles import ParticleState
 
 _RK2_C = (0.0, 0.5)
 _RK4_C = (0.0, 0.5, 0.5, 1.0)
+_SCHEMES = {"euler": (N.KC_EULER, (0.0,)), "rk2": (N.KC_RK2, _RK2_C), "rk4": (N.KC_RK4, _RK4_C)}
 
 
 def _is_3d(vel) -> bool:
@@ -98,24 +99,30 @@ def _check_node_fields(mesh, fields, is3d, placement="layer"):
                                  "(integrators.py:4534-4553)")
 
 
-def _run(state, vel, mesh, dt, time_dir, scheme, c_coeffs, kw, ctx=None) -> ParticleState:
+def _check_call(dt, time_dir, kw):
     if float(dt) <= 0:
         raise ValueError(f"dt must be > 0, got {dt!r}")
     if float(time_dir) not in (1.0, -1.0):
         raise ValueError(f"time_dir must be +1 or -1, got {time_dir!r}")
     if kw.get("uv_interp", "leastsq") == "nemo_cgrid":
         raise NotImplementedError("the NEMO C-grid step is not built on the CUDA backend")
-    diffusion = kw.get("diffusion", None)
-    kick = _kick_args(diffusion)
-    if not np.any(state.alive_mask):
-        return _zero_dead_velocity(state)
+    return _kick_args(kw.get("diffusion", None))
+
+
+def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=None):
+    """Validate one step's payload and make it resident on ``ctx`` (mesh,
+    depth-point table, snapshot slots); returns ``(StepArgs, is3d)``.  ``scheme``
+    is ``"euler"``, ``"rk2"`` or ``"rk4"``; ``ctx`` defaults to the default
+    device context, opened only after validation.  Raises ``NotImplementedError``
+    for combinations the CUDA backend does not build."""
+    code, c_coeffs = _SCHEMES[scheme]
     uv_interp = kw.get("uv_interp", "leastsq")
     if uv_interp != "barycentric":
         raise NotImplementedError(f"uv_interp={uv_interp!r} is not built on the CUDA backend; "
                                   "use 'barycentric' (node-layout velocities)")
     if kw.get("recon") is not None:
         raise NotImplementedError("PCHIP temporal reconstruction is not built on the CUDA backend")
-    if state.elem is not None:
+    if elem is not None:
         raise NotImplementedError("elem_search: walk (carried elements) is not built on the CUDA backend")
     if not (mesh.metadata or {}).get("exact_nearest", False):
         raise NotImplementedError("the CUDA backend anchors with the exact nearest-node search only "
@@ -136,7 +143,7 @@ def _run(state, vel, mesh, dt, time_dir, scheme, c_coeffs, kw, ctx=None) -> Part
         if w_interp not in ("nearest", "barycentric"):
             raise NotImplementedError(f"w_interp={w_interp!r} is not built on the CUDA backend")
         w_code = 0 if w_interp == "nearest" else 1
-        if scheme == N.KC_RK2 and hasattr(vel, "vel_a") and float(getattr(vel, "alpha", 1.0)) == 0.0:
+        if code == N.KC_RK2 and hasattr(vel, "vel_a") and float(getattr(vel, "alpha", 1.0)) == 0.0:
             # integrators.py:5691-5692 routes this exotic payload to the
             # unfused RK2, whose 0 * vel_b blend propagates non-finite values
             raise NotImplementedError("an endpoint LazyLerpField (alpha 0) takes the reference's unfused "
@@ -149,15 +156,12 @@ def _run(state, vel, mesh, dt, time_dir, scheme, c_coeffs, kw, ctx=None) -> Part
     if is3d and placement != "layer":
         ctx.ensure_depth_points(mesh, placement)
     sa, sb, st = ctx.slots_for([vel_a, vel_b, target])
-    fr_in = state.failure_reason
-    ctx.upload_particles(state.lon, state.lat, state.z, state.status, state.nearest_node,
-                         fr=fr_in)
     a = N.StepArgs()
-    a.scheme = scheme
+    a.scheme = code
     a.dims = 3 if is3d else 2
     a.slot_a, a.slot_b, a.slot_t = sa, sb, st
     a.alpha0 = alpha0
-    if vel_next is not None and scheme != N.KC_EULER:
+    if vel_next is not None and code != N.KC_EULER:
         for k, c in enumerate(c_coeffs):
             a.alpha_k[k] = float(c) * float(dt) / float(dt_to_next)
     a.dt = float(dt)
@@ -168,6 +172,18 @@ def _run(state, vel, mesh, dt, time_dir, scheme, c_coeffs, kw, ctx=None) -> Part
         a.kick = 1
         a.kh_x, a.kh_y, a.seed, a.real_id, a.step_i, a.pid_offset = kick
     a.global_step = -1
+    return a, is3d
+
+
+def _run(state, vel, mesh, dt, time_dir, scheme, kw, ctx=None) -> ParticleState:
+    kick = _check_call(dt, time_dir, kw)
+    if not np.any(state.alive_mask):
+        return _zero_dead_velocity(state)
+    a, is3d = prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx, kick=kick, elem=state.elem)
+    ctx = ctx or default_context()
+    fr_in = state.failure_reason
+    ctx.upload_particles(state.lon, state.lat, state.z, state.status, state.nearest_node,
+                         fr=fr_in)
     ctx.step(a)
     out = ctx.download_particles()
     if ctx.device_errors():
@@ -182,17 +198,17 @@ def _run(state, vel, mesh, dt, time_dir, scheme, c_coeffs, kw, ctx=None) -> Part
 
 def euler_step(state, vel, mesh, dt, time_dir, layer: int = 0, **kwargs) -> ParticleState:
     """Forward Euler (integrators.py:5150)."""
-    return _run(state, vel, mesh, dt, time_dir, N.KC_EULER, (0.0,), kwargs)
+    return _run(state, vel, mesh, dt, time_dir, "euler", kwargs)
 
 
 def rk2_step(state, vel, mesh, dt, time_dir, layer: int = 0, **kwargs) -> ParticleState:
     """RK2 midpoint (integrators.py:5611)."""
-    return _run(state, vel, mesh, dt, time_dir, N.KC_RK2, _RK2_C, kwargs)
+    return _run(state, vel, mesh, dt, time_dir, "rk2", kwargs)
 
 
 def rk4_step(state, vel, mesh, dt, time_dir, layer: int = 0, **kwargs) -> ParticleState:
     """Classical RK4 (integrators.py:6013)."""
-    return _run(state, vel, mesh, dt, time_dir, N.KC_RK4, _RK4_C, kwargs)
+    return _run(state, vel, mesh, dt, time_dir, "rk4", kwargs)
 
 
 def _rk45_unavailable(*a, **k):

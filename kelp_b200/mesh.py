@@ -237,6 +237,49 @@ def build_grid_hash(mesh, cell_size: float = 0.0) -> None:
     mesh._gh_far_rows = _gh_far_rows_for(mesh, cell_size)
 
 
+def build_boundary_info(mesh) -> None:
+    """Coastal element flags: an element owning an edge that no other element
+    shares (``mesh.py:2764-2821``).  Each element's edge ring runs over its
+    compacted valid vertices (the closing edge included), an undirected edge
+    counted once per element."""
+    if getattr(mesh, "_elem_is_coastal", None) is not None:
+        return
+    en = np.asarray(mesh.elem_nodes)
+    E, mv = en.shape
+    if E == 0:
+        mesh._elem_is_coastal = np.zeros(0, dtype=np.bool_)
+        return
+    mask = en >= 0
+    if mv == 4:
+        mask[:, 3] &= ~((en[:, 3] == en[:, 0]) & (en[:, 0] >= 0))
+    nv = mask.sum(axis=1)
+    # compact each row's valid vertices to the front, in order
+    order = np.argsort(~mask, axis=1, kind="stable")
+    verts = np.take_along_axis(en, order, axis=1).astype(np.int64)
+    rows = np.arange(E)
+    e_all, k_all = [], []
+    base = np.int64(mesh.nodes_lon.shape[0] + 1)
+    for j in range(mv):
+        ok = (nv >= 3) & (j < nv)
+        nxt = np.where(ok, (j + 1) % np.maximum(nv, 1), 0)
+        a = verts[rows, j]
+        b = verts[rows, nxt]
+        ok &= a != b
+        lo, hi = np.minimum(a, b), np.maximum(a, b)
+        e_all.append(rows[ok])
+        k_all.append(lo[ok] * base + hi[ok])
+    coastal = np.zeros(E, dtype=np.bool_)
+    if e_all:
+        e_cat = np.concatenate(e_all)
+        k_cat = np.concatenate(k_all)
+        if e_cat.size:
+            # an undirected edge counts once per element
+            pairs = np.unique(np.stack([k_cat, e_cat.astype(np.int64)], axis=1), axis=0)
+            _, inv, cnt = np.unique(pairs[:, 0], return_inverse=True, return_counts=True)
+            coastal[pairs[cnt[inv] == 1, 1]] = True
+    mesh._elem_is_coastal = coastal
+
+
 def build_search(mesh) -> None:
     """Build the grid hash (``mesh.py:237``)."""
     build_grid_hash(mesh)

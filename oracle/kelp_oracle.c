@@ -1143,6 +1143,78 @@ int orc_contain(const orc_mesh* mm, int64_t P, const double* lon, const double* 
     return 0;
 }
 
+/* tracking.py:199-364 _apply_beaching_hook with beaching.py:95-181
+ * evaluate_beaching, over all particles in index order (serial: the
+ * reference's stochastic loops are serial too). */
+typedef struct {
+    int use_depth, use_coastal, use_stochastic, on_failure;
+    int resuspension, min_wet_steps;
+    double depth_min, zone_depth, rewet_hysteresis, p_beach, p_resusp;
+    uint64_t seed, real_id, step_i, pid_offset;
+} orc_beach_args;
+
+static double u01(uint64_t seed, uint64_t real_id, uint64_t pid, uint64_t step, uint64_t comp) {
+    uint64_t h = orc_key_hash(seed, real_id, pid, step, comp);
+    return (double)(h >> 11) * (1.0 / 9007199254740992.0);
+}
+
+int orc_beach(const orc_mesh* mm, const orc_beach_args* a, const unsigned char* coastal, int64_t P,
+              const double* lon, const double* lat, int* status, const int* prev, int* nn, int8_t* fr,
+              int* wet) {
+    const OMesh* m = (const OMesh*)mm;
+    int need_topo = a->use_coastal || a->use_stochastic;
+    int any_beached = 0;
+    /* stale anchors of newly failed particles, containing elements, remap */
+    int* cont = (int*)malloc(sizeof(int) * (P > 0 ? P : 1));
+    for (int64_t i = 0; i < P; ++i) {
+        int newly = status[i] == OUTSIDE && prev[i] == ALIVE;
+        if (newly && nn[i] < 0) nn[i] = anchor(m, lon[i], lat[i]);
+        cont[i] = -1;
+        if (need_topo && (status[i] == ALIVE || status[i] == 2 || newly)) {
+            int a0 = nn[i] < 0 ? (int)(nn[i] + m->N) : nn[i];
+            cont[i] = contain_local(m, lon[i], lat[i], a0);
+        }
+        if (a->on_failure && newly) {
+            double hf = nn[i] >= 0 ? m->depth[nn[i]] : INFINITY;
+            int context = hf < a->zone_depth;
+            if (need_topo && cont[i] >= 0 && coastal[cont[i]]) context = 1;
+            if (context) { status[i] = 2; fr[i] = 0; }
+        }
+    }
+    for (int64_t i = 0; i < P; ++i) any_beached |= status[i] == 2;
+    double rewet_level = a->depth_min + a->rewet_hysteresis;
+    for (int64_t i = 0; i < P; ++i) {
+        int alive = status[i] == ALIVE, beached = status[i] == 2;
+        double h = nn[i] >= 0 ? m->depth[nn[i]] : INFINITY;
+        int cc = need_topo && cont[i] >= 0 && coastal[cont[i]];
+        uint64_t key = (uint64_t)i + a->pid_offset;
+        int to_beach = 0;
+        if (a->use_depth && h < a->depth_min) to_beach = 1;
+        if (a->use_coastal && cc) to_beach = 1;
+        if (a->use_stochastic && alive) {
+            int in_zone = h < a->zone_depth || cc;
+            if (in_zone && u01(a->seed, a->real_id, key, a->step_i, 10) < a->p_beach) to_beach = 1;
+        }
+        to_beach = to_beach && alive;
+        int ws = wet[i], to_release = 0;
+        if (a->resuspension != 0 && any_beached && beached) {
+            int rewet = h > rewet_level && nn[i] >= 0;
+            ws = rewet ? ws + 1 : 0;
+            if (a->resuspension == 1 || a->resuspension == 3) to_release = to_release || ws >= a->min_wet_steps;
+            if ((a->resuspension == 2 || a->resuspension == 3) && rewet &&
+                u01(a->seed, a->real_id, key, a->step_i, 11) < a->p_resusp)
+                to_release = 1;
+        }
+        if (to_release) ws = 0;
+        if (!beached) ws = 0;
+        if (to_beach) status[i] = 2;
+        if (to_release) { status[i] = ALIVE; fr[i] = 0; }
+        wet[i] = ws;
+    }
+    free(cont);
+    return 0;
+}
+
 int orc_normals(int64_t P, uint64_t seed, uint64_t real_id, uint64_t step, uint64_t pid_offset, double* g) {
     for (int64_t i = 0; i < P; ++i) orc_normal_pair(seed, real_id, (uint64_t)i + pid_offset, step, 0, g + 2 * i);
     return 0;

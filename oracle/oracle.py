@@ -67,6 +67,7 @@ def lib():
         L.orc_normals.argtypes = [i64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, vp]
         L.orc_node_xyz.argtypes = [i64, vp, vp, vp]
         L.orc_normal_pair.argtypes = [C.c_uint64] * 5 + [vp]
+        L.orc_beach.argtypes = [C.POINTER(OMesh), C.c_void_p, vp, i64, vp, vp, vp, vp, vp, vp, vp]
         L.orc_set_threads.argtypes = [C.c_int]
         L.orc_get_threads.restype = C.c_int
         _lib = L
@@ -200,6 +201,42 @@ def step(state, vel, mesh, dt, time_dir, scheme: str, *, vel_next=None, dt_to_ne
                    _p(out["failure_reason"]), _p(out["u"]), _p(out["v"]), _p(out["w"]), _p(pid_a), _p(rs),
                    int(global_step))
     return out
+
+
+class OBeach(C.Structure):
+    _fields_ = [("use_depth", C.c_int), ("use_coastal", C.c_int), ("use_stochastic", C.c_int),
+                ("on_failure", C.c_int), ("resuspension", C.c_int), ("min_wet_steps", C.c_int),
+                ("depth_min", C.c_double), ("zone_depth", C.c_double), ("rewet_hysteresis", C.c_double),
+                ("p_beach", C.c_double), ("p_resusp", C.c_double),
+                ("seed", C.c_uint64), ("real_id", C.c_uint64), ("step_i", C.c_uint64), ("pid_offset", C.c_uint64)]
+
+
+RESUSP = {"never": 0, "auto": 1, "stochastic": 2, "auto_or_stochastic": 3}
+
+
+def beach(state, prev_status, mesh, coastal, wet_streak, *, criteria, depth_min, zone_depth, t_beach,
+          resuspension, rewet_hysteresis, min_wet_steps, t_resuspend, seed, real_id, step_i, dt, pid_offset=0,
+          view=None):
+    """The beaching hook after one step; returns (state dict, wet_streak)."""
+    view = view or MeshView(mesh)
+    a = OBeach()
+    a.use_depth, a.use_coastal = int("depth" in criteria), int("coastal_element" in criteria)
+    a.use_stochastic, a.on_failure = int("stochastic" in criteria), int("on_failure" in criteria)
+    a.resuspension, a.min_wet_steps = RESUSP[resuspension], int(min_wet_steps)
+    a.depth_min, a.zone_depth, a.rewet_hysteresis = float(depth_min), float(zone_depth), float(rewet_hysteresis)
+    a.p_beach = float(1.0 - np.exp(-abs(dt) / t_beach)) if t_beach else 0.0
+    a.p_resusp = float(1.0 - np.exp(-abs(dt) / t_resuspend)) if t_resuspend else 0.0
+    a.seed, a.real_id, a.step_i, a.pid_offset = int(seed), int(real_id), int(step_i), int(pid_offset)
+    out = {"status": np.array(state.status, np.int32), "nearest_node": np.array(state.nearest_node, np.int32),
+           "failure_reason": np.array(state.failure_reason, np.int8)}
+    prev = np.ascontiguousarray(prev_status, np.int32)
+    ws = np.array(wet_streak, np.int32)
+    cst = np.ascontiguousarray(coastal, np.uint8)
+    lon = np.ascontiguousarray(state.lon, np.float64)
+    lat = np.ascontiguousarray(state.lat, np.float64)
+    lib().orc_beach(C.byref(view.s), C.byref(a), _p(cst), lon.size, _p(lon), _p(lat), _p(out["status"]),
+                    _p(prev), _p(out["nearest_node"]), _p(out["failure_reason"]), _p(ws))
+    return out, ws
 
 
 def find_nearest(mesh, lon, lat, view=None) -> np.ndarray:

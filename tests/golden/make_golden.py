@@ -31,6 +31,10 @@ from kelp.core.mesh import (Mesh as RMesh, build_node_to_elems as r_n2e, build_s
 from kelp.core.particles import ParticleState as RState, ParticleStatus  # noqa: E402
 from kelp.numerics import integrators as RI  # noqa: E402
 from kelp.numerics.diffusion import DiffusionStepArgs as RDiff, _normal_pair  # noqa: E402
+from kelp.core.config import BeachingConfig as RBeachCfg  # noqa: E402
+from kelp.core.mesh import build_boundary_info as r_boundary  # noqa: E402
+from kelp.numerics.beaching import BeachRunConfig as RBeachRun, _RESUSP_CODES  # noqa: E402
+from kelp.tracking import _apply_beaching_hook  # noqa: E402
 
 from kelp_b200 import synthetic as S  # noqa: E402  (input generators only)
 
@@ -101,6 +105,87 @@ def run_case(rm, fields, lon, lat, z, status, scheme, dt, T, n_steps, *, time_di
     out["params"] = np.array([dt, T, n_steps, time_dir, -1 if kh is None else kh[0], -1 if kh is None else kh[1],
                               seed, real_id, pid_offset], dtype=np.float64)
     return out
+
+
+def run_beach_case(rm, fields, lon, lat, z, status, dt, T, n_steps, beach, *, kh=(5.0e4, 5.0e4), seed=7,
+                   real_id=0, pid_offset=0, record=(1, 2, 4, 8, 12, 16)):
+    """RK2 + split kick steps, each followed by the reference's beaching hook
+    (tracking.py:2616-2672): prev_status is the status at the step's entry."""
+    P = lon.size
+    cfg = RBeachCfg(enabled=True, **beach)
+    crit = frozenset(cfg.criteria)
+    need_topo = bool({"coastal_element", "stochastic"} & crit)
+    coastal = None
+    if need_topo:
+        r_boundary(rm)
+        coastal = rm._elem_is_coastal
+    bseed = cfg.seed if cfg.seed is not None else seed
+    zone = cfg.zone_depth if cfg.zone_depth is not None else 2.0 * cfg.depth_min
+    run_cfg = RBeachRun(cfg=cfg, crit=crit, need_topo=need_topo, elem_coastal=coastal, seed=bseed, zone=zone,
+                        pid_offset=pid_offset)
+    st = RState(lon=lon.copy(), lat=lat.copy(), z=z.copy(), status=status.copy(),
+                nearest_node=np.full(P, -1, np.int32), failure_reason=np.zeros(P, np.int8))
+    wet = np.zeros(P, np.int32)
+    out = {}
+    sched = []
+    for k in range(n_steps):
+        t = k * dt
+        vel, vnext, dtn, ia, alpha = payload(fields, t, T)
+        kw = dict(uv_interp="barycentric", vel_next=vnext, dt_to_next=dtn)
+        if kh is not None:
+            kw["diffusion"] = RDiff(scheme="uniform", kh_x=kh[0], kh_y=kh[1], seed=seed, real_id=real_id,
+                                    step_i=k, pid_offset=pid_offset)
+        sched.append([ia, alpha, dtn])
+        prev = st.status
+        st = RI.rk2_step(st, vel, rm, dt, 1.0, **kw)
+        st, wet = _apply_beaching_hook(st, prev, rm, vel, run_cfg, wet, real_id, k, dt)
+        if (k + 1) in record or k + 1 == n_steps:
+            tag = f"s{k + 1}"
+            for name in ("lon", "lat", "status", "nearest_node", "failure_reason"):
+                out[f"{tag}_{name}"] = np.asarray(getattr(st, name))
+            out[f"{tag}_wet"] = np.asarray(wet)
+    out["schedule"] = np.array(sched, dtype=np.float64)
+    out["params"] = np.array([dt, T, n_steps, 1.0, -1 if kh is None else kh[0], -1 if kh is None else kh[1],
+                              seed, real_id, pid_offset], dtype=np.float64)
+    c = set(cfg.criteria)
+    out["beach"] = np.array([int("depth" in c), int("coastal_element" in c), int("stochastic" in c),
+                             int("on_failure" in c), _RESUSP_CODES[cfg.resuspension], cfg.min_wet_steps,
+                             cfg.depth_min, zone, cfg.rewet_hysteresis, cfg.t_beach or 0.0,
+                             cfg.t_resuspend or 0.0, bseed], dtype=np.float64)
+    n_beached = int((st.status == int(ParticleStatus.BEACHED)).sum())
+    print(f"  beach case: {n_beached} beached at the end, {int((wet > 0).sum())} wet streaks")
+    return out
+
+
+def beach_fixture():
+    """A regional coast with shallow shelves: particles strand, remap on
+    failure and resuspend under every criterion."""
+    T = 86400.0
+    m = S.lattice_mesh(1.0, 20.0, lon_min=-25.0, lon_max=25.0, jitter=0.15, land_frac=0.3, quad_frac=0.25,
+                       depth=lambda lo, la: S.smooth_bathymetry(lo, la, 0.0, 6.0, seed=8))
+    rm = ref_mesh(m)
+    snaps = S.gyre_snapshots(m, 4, amp=1.5, dtype=np.float64)
+    rf = ref_fields(snaps)
+    lon, lat, z, status = particles(m, 1500, 31, n_dead=20)
+    cases = {
+        "dco_auto": run_beach_case(rm, rf, lon, lat, z, status, 10800.0, T, 16,
+                                   dict(criteria=["depth", "coastal_element", "on_failure"], depth_min=1.0,
+                                        resuspension="auto", min_wet_steps=2, rewet_hysteresis=0.5)),
+        "sto_both": run_beach_case(rm, rf, lon, lat, z, status, 10800.0, T, 16,
+                                   dict(criteria=["stochastic", "on_failure"], depth_min=1.0, zone_depth=3.0,
+                                        t_beach=43200.0, resuspension="auto_or_stochastic", t_resuspend=21600.0,
+                                        min_wet_steps=3, seed=99),
+                                   real_id=2, pid_offset=500),
+        "cd_sresusp": run_beach_case(rm, rf, lon, lat, z, status, 10800.0, T, 16,
+                                     dict(criteria=["coastal_element", "depth"], depth_min=0.5,
+                                          resuspension="stochastic", t_resuspend=10800.0, rewet_hysteresis=0.2),
+                                     kh=(2.0e4, 2.0e4)),
+        "depth_never": run_beach_case(rm, rf, lon, lat, z, status, 10800.0, T, 12,
+                                      dict(criteria=["depth"], depth_min=2.0), kh=None),
+    }
+    r_boundary(rm)
+    save("golden_beach", mesh_record(rm), snaps, cases,
+         {"lon": lon, "lat": lat, "z": z, "status": status, "coastal": rm._elem_is_coastal.astype(np.uint8)})
 
 
 def particles(m, P, seed, z=False, n_off=0, n_dead=0):
@@ -245,4 +330,9 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    # no argument: every fixture; otherwise the named ones ("steps", "beach")
+    which = set(sys.argv[1:]) or {"steps", "beach"}
+    if "steps" in which:
+        main()
+    if "beach" in which:
+        beach_fixture()

@@ -86,3 +86,62 @@ def test_oracle_rng_normals():
 def test_oracle_node_xyz(golden):
     g = golden("golden_band")
     np.testing.assert_array_equal(O.node_xyz(g.mesh.nodes_lon, g.mesh.nodes_lat), g.mesh._node_xyz)
+
+
+BEACH_CASES = ("dco_auto", "sto_both", "cd_sresusp", "depth_never")
+_RESUSP_NAMES = {0: "never", 1: "auto", 2: "stochastic", 3: "auto_or_stochastic"}
+
+
+def beach_kwargs(c):
+    """The hook's parameters recorded with a beaching case."""
+    b = c["beach"]
+    crit = [n for n, on in zip(("depth", "coastal_element", "stochastic", "on_failure"), b[:4]) if on]
+    return dict(criteria=crit, resuspension=_RESUSP_NAMES[int(b[4])], min_wet_steps=int(b[5]),
+                depth_min=float(b[6]), zone_depth=float(b[7]), rewet_hysteresis=float(b[8]),
+                t_beach=float(b[9]), t_resuspend=float(b[10]), seed=int(b[11]))
+
+
+def replay_oracle_beach(g, cname):
+    """RK2 (+ kick) steps, each followed by the beaching hook, on the oracle."""
+    c = g.case(cname)
+    dt, T, n_steps, td, khx, khy, seed, real_id, pid_off = c["params"]
+    kw = beach_kwargs(c)
+    st = g.particles()
+    wet = np.zeros(st.n_particles, np.int32)
+    view = O.MeshView(g.mesh)
+    snaps = {}
+    for k in range(int(n_steps)):
+        vel, vnext, dtn = g.payload(c["schedule"][k], T)
+        diff = None
+        if khx >= 0:
+            diff = DiffusionStepArgs("uniform", khx, khy, int(seed), int(real_id), k, pid_offset=int(pid_off))
+        prev = st.status
+        out = O.step(st, vel, g.mesh, dt, td, "rk2", vel_next=vnext, dt_to_next=dtn, diffusion=diff, view=view)
+        st = st.replace(lon=out["lon"], lat=out["lat"], status=out["status"], nearest_node=out["nearest_node"],
+                        failure_reason=out["failure_reason"])
+        res, wet = O.beach(st, prev, g.mesh, g.d["p_coastal"], wet, real_id=int(real_id), step_i=k, dt=dt,
+                           pid_offset=int(pid_off), view=view, **kw)
+        st = st.replace(**res)
+        if f"s{k + 1}_status" in c:
+            snaps[k + 1] = {"lon": st.lon, "lat": st.lat, "status": st.status, "nearest_node": st.nearest_node,
+                            "failure_reason": st.failure_reason, "wet": wet}
+    return c, snaps
+
+
+@pytest.mark.parametrize("cname", BEACH_CASES)
+def test_oracle_beaching_matches_reference(golden, cname):
+    g = golden("golden_beach")
+    c, snaps = replay_oracle_beach(g, cname)
+    assert snaps
+    for k, out in snaps.items():
+        for name in ("status", "nearest_node", "failure_reason", "wet", "lon", "lat"):
+            np.testing.assert_array_equal(out[name], c[f"s{k}_{name}"], err_msg=f"{cname} step {k} {name}")
+
+
+def test_oracle_coastal_flags(golden):
+    from kelp_b200.mesh import build_boundary_info
+    g = golden("golden_beach")
+    import types
+    m = types.SimpleNamespace(elem_nodes=g.mesh.elem_nodes, nodes_lon=g.mesh.nodes_lon, _elem_is_coastal=None)
+    build_boundary_info(m)
+    np.testing.assert_array_equal(m._elem_is_coastal.astype(np.uint8), g.d["p_coastal"])
