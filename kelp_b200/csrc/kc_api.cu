@@ -18,7 +18,16 @@ namespace {
 
 constexpr int kSlots = 8;
 constexpr int kEvents = 16;
-constexpr int kBlock = 128;
+#ifndef KC_BLOCK
+#define KC_BLOCK 128   // threads per block of every kernel (a build option)
+#endif
+#ifndef KC_STEP_MIN_BLOCKS
+// resident blocks per SM the step kernels' register budget must allow: 8
+// blocks of 128 threads cap them at 64 registers (measured fastest on the
+// HEALPix 3-D step: the path is latency-bound, occupancy beats spills)
+#define KC_STEP_MIN_BLOCKS 8
+#endif
+constexpr int kBlock = KC_BLOCK;
 
 struct Slot {
     void* u = nullptr;
@@ -71,6 +80,9 @@ struct kc_ctx {
     // beaching: entry status of the last step, wet-step counters, coastal flags
     int* prev = nullptr;
     int* wet = nullptr;
+    // 1 where nn holds the exact anchor of the particle's current position
+    // (written by the step and beaching kernels; cleared by every upload)
+    unsigned char* nn_ok = nullptr;
     bool has_beach = false;
     unsigned char* d_coastal = nullptr;
     bool sorted = false;
@@ -122,6 +134,7 @@ kc::DState state_of(kc_ctx* c) {
     st.pid = c->has_pid ? c->pid : nullptr;
     st.release_step = c->has_rs ? c->rs : nullptr;
     st.prev = c->has_beach ? c->prev : nullptr;
+    st.nn_ok = c->nn_ok;
     st.P = c->P;
     return st;
 }
@@ -145,7 +158,7 @@ __device__ __forceinline__ void activate(const kc::DState& st, const kc::DStep& 
 }
 
 template <typename T, int SCHEME>
-__global__ void __launch_bounds__(kBlock) k_step2d(const __grid_constant__ kc::DMesh m, const __grid_constant__ kc::DBlend<T> f, const __grid_constant__ kc::DState st, const __grid_constant__ kc::DStep s) {
+__global__ void __launch_bounds__(kBlock, KC_STEP_MIN_BLOCKS) k_step2d(const __grid_constant__ kc::DMesh m, const __grid_constant__ kc::DBlend<T> f, const __grid_constant__ kc::DState st, const __grid_constant__ kc::DStep s) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= st.P) return;
     activate(st, s, i);
@@ -154,7 +167,7 @@ __global__ void __launch_bounds__(kBlock) k_step2d(const __grid_constant__ kc::D
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kBlock) k_step3d_rk2(const __grid_constant__ kc::DMesh m, const __grid_constant__ kc::DBlend<T> f, const __grid_constant__ kc::DState st, const __grid_constant__ kc::DStep s) {
+__global__ void __launch_bounds__(kBlock, KC_STEP_MIN_BLOCKS) k_step3d_rk2(const __grid_constant__ kc::DMesh m, const __grid_constant__ kc::DBlend<T> f, const __grid_constant__ kc::DState st, const __grid_constant__ kc::DStep s) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= st.P) return;
     activate(st, s, i);
@@ -163,7 +176,7 @@ __global__ void __launch_bounds__(kBlock) k_step3d_rk2(const __grid_constant__ k
 }
 
 template <typename T, int SCHEME>
-__global__ void __launch_bounds__(kBlock) k_step3d_unfused(const __grid_constant__ kc::DMesh m,
+__global__ void __launch_bounds__(kBlock, KC_STEP_MIN_BLOCKS) k_step3d_unfused(const __grid_constant__ kc::DMesh m,
                                                            const __grid_constant__ kc::DBlend<T> f,
                                                            const __grid_constant__ kc::DState st,
                                                            const __grid_constant__ kc::DStep s) {
@@ -356,7 +369,7 @@ void free_mesh(kc_ctx* c) {
 void free_particles(kc_ctx* c) {
     dfree(c->lon); dfree(c->lat); dfree(c->z); dfree(c->U); dfree(c->V); dfree(c->W);
     dfree(c->status); dfree(c->nn); dfree(c->fr); dfree(c->pid); dfree(c->rs);
-    dfree(c->orig); dfree(c->spare); dfree(c->prev); dfree(c->wet);
+    dfree(c->orig); dfree(c->spare); dfree(c->prev); dfree(c->wet); dfree(c->nn_ok);
     c->has_beach = false;
     dfree(c->skey[0]); dfree(c->skey[1]); dfree(c->sidx[0]); dfree(c->sidx[1]); dfree(c->cub_tmp);
     c->P = c->cap = c->sort_cap = 0;
@@ -643,6 +656,7 @@ int kc_particles_upload(kc_ctx* c, long long P, const double* lon, const double*
         KC_CUDA(c, cudaMalloc((void**)&c->rs, n)); KC_CUDA(c, cudaMalloc((void**)&c->orig, n));
         KC_CUDA(c, cudaMalloc((void**)&c->spare, n));
         KC_CUDA(c, cudaMalloc((void**)&c->prev, n)); KC_CUDA(c, cudaMalloc((void**)&c->wet, n));
+        KC_CUDA(c, cudaMalloc((void**)&c->nn_ok, n));
         c->cap = P;
     }
     c->P = P;
@@ -665,6 +679,7 @@ int kc_particles_upload(kc_ctx* c, long long P, const double* lon, const double*
     if (pid) KC_CUDA(c, cudaMemcpyAsync(c->pid, pid, n * 8, cudaMemcpyHostToDevice, s));
     c->has_rs = rs != nullptr;
     if (rs) KC_CUDA(c, cudaMemcpyAsync(c->rs, rs, n * 4, cudaMemcpyHostToDevice, s));
+    KC_CUDA(c, cudaMemsetAsync(c->nn_ok, 0, n, s));   // uploaded anchors are not trusted
     KC_CUDA(c, cudaMemsetAsync(c->U, 0, n * 8, s));
     KC_CUDA(c, cudaMemsetAsync(c->V, 0, n * 8, s));
     KC_CUDA(c, cudaMemsetAsync(c->W, 0, n * 8, s));
@@ -736,6 +751,7 @@ int kc_sort(kc_ctx* c) {
     if ((rc = regather(c, (void**)&c->status, 4, idx))) return rc;
     if ((rc = regather(c, (void**)&c->nn, 4, idx))) return rc;
     if ((rc = regather(c, (void**)&c->fr, 1, idx))) return rc;
+    if ((rc = regather(c, (void**)&c->nn_ok, 1, idx))) return rc;
     if (c->has_rs && (rc = regather(c, (void**)&c->rs, 4, idx))) return rc;
     if (c->has_beach) {
         if ((rc = regather(c, (void**)&c->prev, 4, idx))) return rc;

@@ -44,6 +44,7 @@ __device__ __forceinline__ void beach_particle(const DMesh& m, const DState& st,
     if (newly && nn < 0) {
         nn = site_anchor(m, make_site(st.lon[i], st.lat[i]));
         st.nn[i] = nn;
+        if (st.nn_ok) st.nn_ok[i] = 1;
     }
     const bool alive0 = status == ALIVE, beached0 = status == BEACHED;
     int contained = -1;

@@ -316,41 +316,108 @@ __device__ __forceinline__ int find_layer(const DMesh& m, double z, int node) {
     return first_above(m.zlev, 0, max_layer, z);
 }
 
+// Where depth z falls among the interfaces, as vertical.py:1064-1098
+// _interp_w_linear_single_tinterp decides it: one level read (k, a < 0) or
+// the linear blend of levels k and k + 1 with fraction a.  It depends on z
+// alone, so the vertices of one element share it unless their own depth
+// clamps z.
+struct WLoc {
+    int k;
+    double a;
+};
+
+__device__ __forceinline__ WLoc w_locate(const DMesh& m, double z) {
+    const int K = m.K;
+    const double* zl = m.zlev;
+    if (K < 2 || z <= __ldg(&zl[0])) return {0, -1.0};
+    if (z >= __ldg(&zl[K - 1])) return {K - 1, -1.0};
+    const int k = first_above(zl, 0, K - 2, z);
+    const double zk = __ldg(&zl[k]), zk1 = __ldg(&zl[k + 1]);
+    const double dz = zk1 - zk;
+    if (dz < 1e-12) return {k, -1.0};
+    return {k, (z - zk) / dz};
+}
+
+// The time-blended W of one node at a located depth (the value part of
+// vertical.py:1064-1098; tblend per level, :1042-1061).
+template <typename T>
+__device__ __forceinline__ double w_at(const DBlend<T>& f, double alpha, const WLoc& L, int node, double time_dir) {
+    const long long n = f.n;
+    auto at = [&](int k) {
+        const long long idx = (long long)k * n + node;
+        if (alpha < 1e-12) {
+            const double a = (double)__ldg(&f.a.w[idx]);
+            if (f.alpha0 == 0.0) return a;
+            return (1.0 - f.alpha0) * a + f.alpha0 * (double)__ldg(&f.b.w[idx]);
+        }
+        if (alpha > 1.0 - 1e-12) return (double)__ldg(&f.t.w[idx]);
+        return tblend((double)__ldg(&f.a.w[idx]), (double)__ldg(&f.b.w[idx]), (double)__ldg(&f.t.w[idx]),
+                      f.alpha0, alpha);
+    };
+    if (L.a < 0.0) return time_dir * at(L.k);
+    const double w_lo = at(L.k);
+    const double w_hi = at(L.k + 1);
+    return time_dir * ((1.0 - L.a) * w_lo + L.a * w_hi);
+}
+
 // vertical.py:1064-1098 _interp_w_linear_single_tinterp
 template <typename T>
 __device__ __forceinline__ double w_linear(const DMesh& m, const DBlend<T>& f, double alpha, double z, int node,
                                            double time_dir) {
-    const int K = m.K;
-    const double* zl = m.zlev;
-    const long long n = f.n;
-    auto at = [&](int k) {
-        long long idx = (long long)k * n + node;
-        return tblend((double)__ldg(&f.a.w[idx]), (double)__ldg(&f.b.w[idx]), (double)__ldg(&f.t.w[idx]),
-                      f.alpha0, alpha);
-    };
-    if (K < 2) return time_dir * at(0);
-    if (z <= __ldg(&zl[0])) return time_dir * at(0);
-    if (z >= __ldg(&zl[K - 1])) return time_dir * at(K - 1);
-    const int k = first_above(zl, 0, K - 2, z);
-    const double zk = __ldg(&zl[k]), zk1 = __ldg(&zl[k + 1]);
-    const double dz = zk1 - zk;
-    if (dz < 1e-12) return time_dir * at(k);
-    const double a = (z - zk) / dz;
-    const double w_lo = at(k);
-    const double w_hi = at(k + 1);
-    return time_dir * ((1.0 - a) * w_lo + a * w_hi);
+    return w_at(f, alpha, w_locate(m, z), node, time_dir);
 }
 
 // Python's min(a, b): the first argument unless the second is smaller.
 __device__ __forceinline__ double pymin(double a, double b) { return b < a ? b : a; }
 
+// W of a vertex at min(z, its depth), reusing the location of z when the
+// vertex's depth does not clamp it.
+template <typename T>
+__device__ __forceinline__ double w_vertex(const DMesh& m, const DBlend<T>& f, double alpha, double z,
+                                           const WLoc& Lz, int nd, double time_dir) {
+    const double zc = pymin(z, __ldg(&m.depth[nd]));
+    return w_at(f, alpha, zc == z ? Lz : w_locate(m, zc), nd, time_dir);
+}
+
+// True when no fan triangle of the ring can give the point three weights
+// >= -1e-6 in the projected test below, decided from longitude offsets
+// (wrapped around vertex 0) and latitudes alone.  In exact arithmetic a point
+// whose barycentric weights are all >= -eps lies within 2 eps times the
+// element's extent of its bounding box along each projected axis; the
+// projection scales each axis by a positive factor, so the test holds in
+// degrees.  The margin is 1e-5 of the extent (five times the bound) plus
+// 1e-9 degrees for rounding, and elements spanning 90 degrees or more of
+// longitude (pole cells) are never skipped.
+__device__ __forceinline__ bool w_ring_rejects(const Ring& r, int nvv, double xp, double yp) {
+    double dmin = 0.0, dmax = 0.0, lmin = r.la[0], lmax = r.la[0];
+#pragma unroll
+    for (int v = 1; v < 4; ++v) {
+        if (v < nvv) {
+            const double d = wrap180(r.ln[v] - r.ln[0]);
+            dmin = fmin(dmin, d);
+            dmax = fmax(dmax, d);
+            lmin = fmin(lmin, r.la[v]);
+            lmax = fmax(lmax, r.la[v]);
+        }
+    }
+    if (!(dmax - dmin < 90.0)) return false;
+    const double my = 1e-5 * (lmax - lmin) + 1e-9;
+    if (yp < lmin - my || yp > lmax + my) return true;
+    const double mx = 1e-5 * (dmax - dmin) + 1e-9;
+    const double dp = wrap180(xp - r.ln[0]);
+    return dp < dmin - mx || dp > dmax + mx;
+}
+
 // vertical.py:744-881 _interp_w_bary_single_tinterp: the anchor's own fan
 // search (denominator tolerance 1e-14, R = 6371000, origin by
 // mesh.py:1973-2003 _seam_safe_lon0), triangles blended inline, quads through
-// Wachspress, nearest-node fallback.
+// Wachspress, nearest-node fallback.  Elements the point provably lies
+// outside of (w_ring_rejects) skip the projected test, whose verdict for them
+// is "outside" anyway.
 template <typename T>
 __device__ __noinline__ double w_bary(const DMesh& m, const DBlend<T>& f, double alpha, double xp, double yp,
                                       double z, int node, double time_dir) {
+    const WLoc Lz = w_locate(m, z);
     int s = __ldg(&m.n2e_off[node]), e = __ldg(&m.n2e_off[node + 1]);
     for (int kk = s; kk < e; ++kk) {
         const int el = __ldg(&m.n2e[kk]);
@@ -358,6 +425,7 @@ __device__ __noinline__ double w_bary(const DMesh& m, const DBlend<T>& f, double
         load_ring(m, __ldg(&m.en[el]), r);
         const int nvv = r.n;
         if (nvv < 3) continue;
+        if (w_ring_rejects(r, nvv, xp, yp)) continue;
         double lmin = fmin(fmin(r.ln[0], r.ln[1]), r.ln[2]), lmax = fmax(fmax(r.ln[0], r.ln[1]), r.ln[2]);
         if (nvv == 4) { lmin = fmin(lmin, r.ln[3]); lmax = fmax(lmax, r.ln[3]); }
         double lon0;
@@ -408,23 +476,21 @@ __device__ __noinline__ double w_bary(const DMesh& m, const DBlend<T>& f, double
                     wachspress_quad(px, py, vx, vy, wts);
                     double acc = 0.0;
 #pragma unroll
-                    for (int vi = 0; vi < 4; ++vi) {
-                        const int nvn = r.v[vi];
-                        acc += wts[vi] * w_linear(m, f, alpha, pymin(z, __ldg(&m.depth[nvn])), nvn, time_dir);
-                    }
+                    for (int vi = 0; vi < 4; ++vi)
+                        acc += wts[vi] * w_vertex(m, f, alpha, z, Lz, r.v[vi], time_dir);
                     return acc;
                 }
                 const int n0 = r.v[0];
                 const int n1 = i1 == 1 ? r.v[1] : r.v[2];
                 const int n2 = i2 == 2 ? r.v[2] : r.v[3];
-                const double w_v0 = w_linear(m, f, alpha, pymin(z, __ldg(&m.depth[n0])), n0, time_dir);
-                const double w_v1 = w_linear(m, f, alpha, pymin(z, __ldg(&m.depth[n1])), n1, time_dir);
-                const double w_v2 = w_linear(m, f, alpha, pymin(z, __ldg(&m.depth[n2])), n2, time_dir);
+                const double w_v0 = w_vertex(m, f, alpha, z, Lz, n0, time_dir);
+                const double w_v1 = w_vertex(m, f, alpha, z, Lz, n1, time_dir);
+                const double w_v2 = w_vertex(m, f, alpha, z, Lz, n2, time_dir);
                 return w1 * w_v0 + w2 * w_v1 + w3 * w_v2;
             }
         }
     }
-    return w_linear(m, f, alpha, pymin(z, __ldg(&m.depth[node])), node, time_dir);
+    return w_vertex(m, f, alpha, z, Lz, node, time_dir);
 }
 
 // ---------------------------------------------------------------------------

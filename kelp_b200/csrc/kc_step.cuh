@@ -25,6 +25,7 @@ struct DState {
     const long long* pid;      // stable particle id (RNG key), index when null
     const int* release_step;   // delayed release (null: all released)
     int* prev;                 // status at the step's entry, for the beaching hook (null: not kept)
+    unsigned char* nn_ok;      // 1: nn is the exact anchor of the current position (null: never trusted)
     long long P;
 };
 
@@ -51,6 +52,24 @@ __device__ __forceinline__ double clamp_lat(double lat) {
     if (lat > 90.0) return 90.0;
     if (lat < -90.0) return -90.0;
     return lat;
+}
+
+// The anchor of the step's start position: the carried one when a kernel of
+// this library computed it for exactly this position (the reference searches
+// it afresh; the search is a pure function of the position, so the result is
+// the same), else the exact search.
+__device__ __forceinline__ int start_anchor(const DMesh& m, const DState& st, const Site& q0, int pre_nn,
+                                            long long i) {
+    if (st.nn_ok && st.nn_ok[i] && pre_nn >= 0) return pre_nn;
+    return site_anchor(m, q0);
+}
+
+// After a step: an ALIVE particle carries the anchor of its new position; a
+// failed one sits at its start position and carries the start anchor, except
+// after a reverted kick, which restores the carried anchor (trusted only when
+// it equals the start anchor).
+__device__ __forceinline__ void mark_anchor(const DState& st, long long i, int status, int nn_out, int node_i) {
+    if (st.nn_ok) st.nn_ok[i] = (status == ALIVE || nn_out == node_i) ? 1 : 0;
 }
 
 // integrators.py:673-818 _apply_split_diffusion_kick for one particle that is
@@ -121,7 +140,7 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
     signed char fr = st.fr[i];
     bool failed = false;
     const Site q0 = make_site(lon0, lat0);
-    const int node_i = site_anchor(m, q0);
+    const int node_i = start_anchor(m, st, q0, pre_nn, i);
 
     double U1, V1;
     bool ok1 = interp_uv_bary<T>(m, f, lon0, lat0, node_i, td, 0, s.ak[0], U1, V1);
@@ -206,6 +225,7 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
     st.status[i] = status;
     st.nn[i] = nn_out;
     st.fr[i] = fr;
+    mark_anchor(st, i, status, nn_out, node_i);
 }
 
 template <typename T>
@@ -259,7 +279,7 @@ __device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DB
     double lon_new = lon0, lat_new = lat0, z_new = z0p;
 
     const Site q0 = make_site(lon0, lat0);
-    const int node_i = site_anchor(m, q0);
+    const int node_i = start_anchor(m, st, q0, pre_nn, i);
     int nn_out = node_i;
     double U1, V1;
     bool ok = stage_uv<T>(m, f, s, lon0, lat0, node_i, z0p, s.ak[0], U1, V1);
@@ -331,6 +351,7 @@ __device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DB
     st.status[i] = status;
     st.nn[i] = nn_out;
     st.fr[i] = fr;
+    mark_anchor(st, i, status, nn_out, node_i);
 }
 
 // integrators.py:3647-3856 _fused_rk2_step_3d_bary_tinterp (layer u/v,
@@ -353,7 +374,7 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
     double lon_new = lon0, lat_new = lat0, z_new = z0p;
 
     const Site q0 = make_site(lon0, lat0);
-    const int node_i = site_anchor(m, q0);
+    const int node_i = start_anchor(m, st, q0, pre_nn, i);
     int nn_out = node_i;
     double U1, V1;
     const bool ok1 = stage_uv<T>(m, f, s, lon0, lat0, node_i, z0p, s.ak[0], U1, V1);
@@ -402,6 +423,7 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
     st.status[i] = status;
     st.nn[i] = nn_out;
     st.fr[i] = fr;
+    mark_anchor(st, i, status, nn_out, node_i);
 }
 
 }  // namespace kc
