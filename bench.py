@@ -1,12 +1,20 @@
 """Benchmark of the B200 time-stepping path: particle-steps/s on one node.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c1]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c3]
+                    [--form mixed] [--forms plain,mixed,mixed_f16]
                     [--impl b200|reference]
 
 One step = one pass of the step kernel over every particle of the workload
 (inputs resident in HBM, L2 evicted between timed steps, CUDA events on the
-library's stream).  Under torchrun (N > 1) every rank runs its own shard of
-the same per-GPU size (weak scaling: particles are independent, nothing is
+library's stream, the periodic re-sort inside the timed region).  Every form
+in --forms is timed the same way: "plain" (the reference's float64
+arithmetic), "mixed" (float32 interpolation, float64 positions and element
+decisions) and "mixed_f16" (the same on float16 snapshots with per-row
+scales); the headline value is --form's.  On one GPU the line also reports
+each form's great-circle separation from the plain form after 24 h (all
+particles) and after the configuration's horizon (a subset), and the oracle
+port's CPU throughput.  Under torchrun (N > 1) every rank runs its own shard
+of the same per-GPU size (weak scaling: particles are independent, nothing is
 exchanged); the time is the maximum over ranks.  Rank 0 prints one JSON line.
 
 ``--impl reference`` times the reference algorithm's CPU implementation on
@@ -31,7 +39,10 @@ sys.path.insert(0, ROOT)
 
 METRIC = "particle-steps/s on 1 B200, mixed vs FP64 form at ≤1 m p99 error; HBM GB/s vs peak"
 UNIT = "particle-steps/s"
-PUBLISHED = {}   # workload -> the reference's published figure for this exact metric
+# workload -> the reference's published figure for this exact metric: the fused
+# 3-D RK2 step on HEALPix nside 512, 69 levels, 6 M particles, 128 EPYC 7763
+# cores (manual/chapters/17-performance.tex:219-233)
+PUBLISHED = {"c3_healpix512_3d_rk2_kick": 10.4e6}
 
 
 def env_rank():
@@ -175,16 +186,75 @@ def run_reference(args):
     return 0
 
 
-def load_traffic(workload: str):
-    """Per-launch DRAM bytes of the step kernel from the committed ncu summary."""
+def load_traffic(workload: str, form: str = "plain"):
+    """Per-launch DRAM bytes of the step kernel from the committed ncu summary
+    (lines: workload form kernel bytes ...)."""
     p = os.path.join(ROOT, "profiles", "traffic.txt")
     if not os.path.exists(p):
         return None
     for line in open(p):
         f = line.split()
-        if len(f) >= 3 and f[0] == workload:
-            return float(f[2])
+        if len(f) >= 4 and f[0] == workload and f[1] == form:
+            return float(f[3])
     return None
+
+
+FORMS = {   # name -> (kernel form, snapshot storage)
+    "plain": ("plain", None),
+    "mixed": ("mixed", np.float32),
+    "mixed_f16": ("mixed", np.float16),
+}
+
+
+def _form_args(wl, k, slots, form):
+    from kelp_b200 import _native as N
+    code, store = FORMS[form]
+    key = "f16" if store is np.float16 else "f32"
+    return wl.step_args(k, slots[key], N.KC_MIXED if code == "mixed" else N.KC_PLAIN)
+
+
+def _upload(ctx, wl, idx=None, pid_base=0):
+    lon, lat, z = (wl.lon, wl.lat, wl.z) if idx is None else (wl.lon[idx], wl.lat[idx], wl.z[idx])
+    P = lon.size
+    ctx.upload_particles(lon, lat, z, np.full(P, 1, np.int32), np.full(P, -1, np.int32), np.zeros(P, np.int8),
+                         np.arange(P, dtype=np.int64) + pid_base)
+
+
+def _run_steps(ctx, wl, slots, form, k0, n, sort_every):
+    for j in range(n):
+        if sort_every > 0 and j % sort_every == 0:
+            ctx.sort()
+        ctx.step(_form_args(wl, k0 + j, slots, form))
+    ctx.synchronize()
+    return ctx.download_particles()
+
+
+def accuracy(ctx, wl, slots, forms, sort_every, n_sub):
+    """Separation of each non-plain form from the plain float64 form: after
+    24 h on every particle, and after the configuration's full horizon on a
+    uniform subset of n_sub particles; with the dispersion of each run."""
+    from kelp_b200 import accuracy as A
+    out = {}
+    h24 = max(1, int(round(86400.0 / wl.dt)))
+    ref = {}
+    _upload(ctx, wl)
+    ref["24h"] = _run_steps(ctx, wl, slots, "plain", 0, h24, sort_every)
+    idx = np.arange(min(n_sub, wl.P))
+    _upload(ctx, wl, idx)
+    ref["full"] = _run_steps(ctx, wl, slots, "plain", 0, wl.n_steps_run, sort_every)
+    for form in forms:
+        if form == "plain":
+            continue
+        _upload(ctx, wl)
+        t24 = _run_steps(ctx, wl, slots, form, 0, h24, sort_every)
+        _upload(ctx, wl, idx)
+        tfull = _run_steps(ctx, wl, slots, form, 0, wl.n_steps_run, sort_every)
+        out[form] = {"after_24h": {"steps": h24, "particles": wl.P, **A.separation_stats(ref["24h"], t24)},
+                     "after_horizon": {"steps": wl.n_steps_run, "particles": int(idx.size),
+                                       **A.separation_stats(ref["full"], tfull)},
+                     "dispersion_m2_horizon": {"plain": A.dispersion_m2(wl.lon[idx], wl.lat[idx], ref["full"]),
+                                               form: A.dispersion_m2(wl.lon[idx], wl.lat[idx], tfull)}}
+    return out
 
 
 def run_b200(args):
@@ -197,7 +267,7 @@ def run_b200(args):
         dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
     from kelp_b200 import workloads, roofline
     from kelp_b200 import integrators as KI
-    from kelp_b200.device import DeviceContext, set_default_device, default_context, pinned_empty
+    from kelp_b200.device import set_default_device, default_context, pinned_empty
     from kelp_b200.fields import LazyLerpField
     from kelp_b200.particles import ParticleState
 
@@ -205,22 +275,16 @@ def run_b200(args):
     set_default_device(local)
     ctx = default_context()
     ctx.ensure_mesh(wl.mesh)
-    slots = ctx.slots_for(wl.snaps)
+    if wl.dims == 3 and wl.uv_vertical != "layer":
+        ctx.ensure_depth_points(wl.mesh, wl.uv_vertical)
+    forms = [f.strip() for f in args.forms.split(",") if f.strip()]
+    if args.form not in forms:
+        forms.append(args.form)
+    slots = {"f32": ctx.slots_for(wl.snaps, np.float32)}
+    if any(FORMS[f][1] is np.float16 for f in forms):
+        slots["f16"] = ctx.slots_for(wl.snaps, np.float16)
     P = wl.P
-    pid = np.arange(P, dtype=np.int64) + rank * P
-    status0 = np.full(P, 1, np.int32)
-
-    def upload():
-        ctx.upload_particles(wl.lon, wl.lat, wl.z, status0, np.full(P, -1, np.int32), np.zeros(P, np.int8), pid)
-
-    upload()
-    for k in range(args.warmup):
-        if args.sort_every > 0 and k == 0:
-            ctx.sort()
-        ctx.step(wl.step_args(k, slots))
-    ctx.synchronize()
-    if ctx.device_errors():
-        raise RuntimeError("device-side iteration cap hit during warm-up")
+    pid_base = rank * P
 
     def barrier():
         if dist is not None:
@@ -229,39 +293,54 @@ def run_b200(args):
 
     sampler = ClockSampler(local)
     time.sleep(0.6)
-    barrier()
     t_wall0 = time.time()
-    kernel_ms = []
-    sort_ms = []
-    launches = 0
-    for j, k in enumerate(range(args.warmup, args.warmup + args.steps)):
-        ctx.l2_flush()
-        ctx.record(0)
-        if args.sort_every > 0 and j % args.sort_every == 0:
-            ctx.sort()
-            ctx.record(2)
-            launches += 15      # key kernel, 2-4 radix passes, one gather per array
-        ctx.step(wl.step_args(k, slots))
-        launches += 1
-        ctx.record(1)
-        kernel_ms.append(ctx.elapsed_ms(0, 1))
-        if args.sort_every > 0 and j % args.sort_every == 0:
-            sort_ms.append(ctx.elapsed_ms(0, 2))
-    barrier()
+    timed = {}
+    for form in forms:
+        _upload(ctx, wl, pid_base=pid_base)
+        for k in range(args.warmup):
+            if args.sort_every > 0 and k == 0:
+                ctx.sort()
+            ctx.step(_form_args(wl, k, slots, form))
+        ctx.synchronize()
+        if ctx.device_errors():
+            raise RuntimeError("device-side iteration cap hit during warm-up")
+        barrier()
+        step_ms, sort_ms, launches = [], [], 0
+        for j, k in enumerate(range(args.warmup, args.warmup + args.steps)):
+            ctx.l2_flush()
+            ctx.record(0)
+            if args.sort_every > 0 and j % args.sort_every == 0:
+                ctx.sort()
+                ctx.record(2)
+                launches += 15      # key kernel, radix passes, one gather per particle array
+            ctx.step(_form_args(wl, k, slots, form))
+            launches += 1
+            ctx.record(1)
+            step_ms.append(ctx.elapsed_ms(0, 1))
+            if args.sort_every > 0 and j % args.sort_every == 0:
+                sort_ms.append(ctx.elapsed_ms(0, 2))
+        barrier()
+        total = float(sum(step_ms))
+        if dist is not None:
+            import torch
+            t = torch.tensor([total], dtype=torch.float64, device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total = float(t.item())
+        timed[form] = {"total_ms": total, "kernel_ms": (sum(step_ms) - sum(sort_ms)) / len(step_ms),
+                       "sort_ms": float(sum(sort_ms)), "launches": launches, "errors": ctx.device_errors()}
     t_wall1 = time.time()
     clocks = sampler.stop(t_wall0, t_wall1)
-    total_ms = float(sum(kernel_ms))
-    if dist is not None:
-        import torch
-        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    errs = ctx.device_errors()
 
-    # end to end through the public step API: host state in page-locked memory
+    # end to end through the public step API, headline form: host state in
+    # page-locked memory copied in and out every step
+    code, store = FORMS[args.form]
+    api_kw = {"cuda_precision": code}
+    if store is np.float16:
+        api_kw["cuda_snapshots"] = "f16"
     st_h = {}
     for name, dt_, src in (("lon", np.float64, wl.lon), ("lat", np.float64, wl.lat), ("z", np.float64, wl.z),
-                           ("status", np.int32, status0), ("nearest_node", np.int32, np.full(P, -1, np.int32)),
+                           ("status", np.int32, np.full(P, 1, np.int32)),
+                           ("nearest_node", np.int32, np.full(P, -1, np.int32)),
                            ("failure_reason", np.int8, np.zeros(P, np.int8))):
         a = pinned_empty((P,), dt_)
         a[:] = src
@@ -277,9 +356,9 @@ def run_b200(args):
         a, b = wl.snaps[ia], wl.snaps[ib]
         vel = a if alpha0 == 0.0 else LazyLerpField(a, b, alpha0)
         diff = None if wl.kh is None else DiffusionStepArgs("uniform", wl.kh[0], wl.kh[1], wl.seed, 0, k,
-                                                            pid_offset=rank * P)
+                                                            pid_offset=pid_base)
         state = step_fn(state, vel, wl.mesh, wl.dt, 1.0, uv_interp="barycentric", w_interp=wl.w_interp,
-                        vel_next=b, dt_to_next=dtn, diffusion=diff)
+                        vel_next=b, dt_to_next=dtn, diffusion=diff, **api_kw)
         for name in ("lon", "lat", "z", "status", "nearest_node", "failure_reason"):
             st_h[name][:] = getattr(state, name)
         state = ParticleState(**st_h)
@@ -293,31 +372,45 @@ def run_b200(args):
     h2d = P * (8 + 8 + 8 + 4 + 4 + 1)
     d2h = P * (8 * 6 + 4 + 4 + 1)
 
-    line = None
+    acc = None
+    if world == 1 and not args.no_accuracy and len(forms) > 1:
+        acc = accuracy(ctx, wl, slots, forms, args.sort_every, args.accuracy_particles)
+
     if rank == 0:
-        fbytes = 4 if np.asarray(wl.snaps[0].u).dtype == np.float32 else 8
-        bpp = roofline.bytes_per_particle_step(wl.mesh, wl.scheme, wl.dims, fbytes, kick=wl.kh is not None,
-                                               w_code=0 if wl.w_interp == "nearest" else 1)
-        # the step kernel's own average duration (the re-sort timed apart)
-        avg_launch_s = (sum(kernel_ms) - sum(sort_ms)) / len(kernel_ms) * 1e-3
-        achieved = bpp["total"] * P / avg_launch_s / 1e9
         peak, kind = peaks()
-        traffic = load_traffic(wl.name)
-        value = world * P * args.steps / (total_ms * 1e-3)
+        per_form = {}
+        for form in forms:
+            fb = 2 if FORMS[form][1] is np.float16 else 4
+            bpp = roofline.bytes_per_particle_step(wl.mesh, wl.scheme, wl.dims, fb, kick=wl.kh is not None,
+                                                   w_code=0 if wl.w_interp == "nearest" else 1)
+            t = timed[form]
+            per_form[form] = {"value": world * P * args.steps / (t["total_ms"] * 1e-3),
+                              "ms_per_step": t["total_ms"] / args.steps, "kernel_ms": t["kernel_ms"],
+                              "achieved_gbs": bpp["total"] * P / (t["kernel_ms"] * 1e-3) / 1e9,
+                              "bytes_per_particle_step": bpp["total"], "device_errors": t["errors"]}
+        head = per_form[args.form]
+        traffic = load_traffic(wl.name, args.form)
+        value = head["value"]
+        dtype = "f64" if args.form == "plain" else ("f32 interp + f64 state, f16 snapshots"
+                                                    if FORMS[args.form][1] is np.float16 else
+                                                    "f32 interp + f64 state")
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": (value / PUBLISHED[wl.name]) if wl.name in PUBLISHED else None,
-                "dtype": "f64", "data": "synthetic",
-                "config": {"workload": wl.name, **wl.description, "particles_per_gpu": P,
+                "dtype": dtype, "data": "synthetic",
+                "config": {"workload": wl.name, "form": args.form, **wl.description, "particles_per_gpu": P,
                            "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}"},
-                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak, "peak_kind": kind,
-                             "traffic": traffic, "algorithmic_bytes_per_particle_step": bpp["total"]},
+                "roofline": {"bound": "hbm", "achieved": head["achieved_gbs"], "peak": peak, "unit": "GB/s",
+                             "frac": head["achieved_gbs"] / peak, "peak_kind": kind, "traffic": traffic,
+                             "algorithmic_bytes_per_particle_step": head["bytes_per_particle_step"]},
+                "forms": per_form,
                 "e2e": {"value": world * P * e2e_steps / (e2e_ms * 1e-3), "unit": UNIT,
                         "h2d_bytes_per_step": h2d * world, "d2h_bytes_per_step": d2h * world,
-                        "steps": e2e_steps},
-                "gpu_launches": launches, "clocks": clocks, "device_errors": errs,
-                "resort": {"every_steps": args.sort_every, "ms_total": float(sum(sort_ms))}}
+                        "steps": e2e_steps, "form": args.form},
+                "gpu_launches": timed[args.form]["launches"], "clocks": clocks,
+                "resort": {"every_steps": args.sort_every, "ms_total": timed[args.form]["sort_ms"]}}
+        if acc is not None:
+            line["accuracy_vs_plain"] = acc
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(wl)
         print(json.dumps(line), flush=True)
@@ -330,9 +423,14 @@ def run_b200(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=240)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--workload", default="c1")
+    ap.add_argument("--workload", default="c3", help="c1, c2, c3 (default: the published configuration) or c3small")
+    ap.add_argument("--form", default="mixed", choices=sorted(FORMS), help="the form the headline value reports")
+    ap.add_argument("--forms", default="plain,mixed,mixed_f16", help="forms timed beside it")
+    ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--accuracy-particles", type=int, default=200_000,
+                    help="particles of the full-horizon separation run")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sort-every", type=int, default=16, help="re-sort particles by hash cell every N steps")

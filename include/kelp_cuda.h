@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define KC_ABI_VERSION 1
+#define KC_ABI_VERSION 2
 
 #define KC_OK 0
 #define KC_ERR_ARG 1      /* invalid argument or combination */
@@ -44,6 +44,11 @@ extern "C" {
 /* field element types */
 #define KC_F32 0
 #define KC_F64 1
+#define KC_F16 2     /* float32 input stored as float16 with a power-of-two scale per row */
+
+/* numerical forms of kc_step */
+#define KC_PLAIN 0   /* float64 interpolation: the reference's arithmetic */
+#define KC_MIXED 1   /* float32 interpolation, float64 positions and element decisions */
 
 /* integration schemes */
 #define KC_EULER 0
@@ -88,6 +93,7 @@ typedef struct kc_step_args {
     double kh_x, kh_y;           /* m^2/s */
     unsigned long long seed, real_id, step_i, pid_offset;
     long long global_step;       /* delayed-release activation step, -1 for none */
+    int precision;               /* KC_PLAIN (snapshots F32/F64) or KC_MIXED (snapshots F32/F16) */
 } kc_step_args;
 
 /* Beaching / resuspension of one step (src/kelp/tracking.py:199-364,
@@ -120,7 +126,9 @@ int kc_mesh_upload(kc_ctx* ctx, const kc_mesh_desc* desc);
 int kc_depth_points_upload(kc_ctx* ctx, int M, const double* p, const int* last, const double* bed);
 
 /* One snapshot into ring slot `slot` (0..7): u, v (n_uv_rows, n_nodes) and
- * optional w (n_w_rows, n_nodes), all of element type `dtype`. */
+ * optional w (n_w_rows, n_nodes), all of element type `dtype` (KC_F32 or
+ * KC_F64); KC_F16 takes float32 arrays and stores them as float16, each row
+ * scaled by a power of two so that its largest magnitude is below 2^15. */
 int kc_field_upload(kc_ctx* ctx, int slot, int dtype, long long n_nodes, int n_uv_rows,
                     const void* u, const void* v, int n_w_rows, const void* w);
 

@@ -15,7 +15,9 @@ import numpy as np
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libkelpcuda.so")
 
 KC_OK, KC_ERR_ARG, KC_ERR_CUDA, KC_ERR_STATE, KC_ERR_DEVICE = 0, 1, 2, 3, 4
-KC_F32, KC_F64 = 0, 1
+KC_F32, KC_F64, KC_F16 = 0, 1, 2
+KC_PLAIN, KC_MIXED = 0, 1
+ABI_VERSION = 2
 KC_EULER, KC_RK2, KC_RK4 = 0, 1, 2
 
 #: every symbol include/kelp_cuda.h declares
@@ -69,7 +71,7 @@ class StepArgs(C.Structure):
                 ("kh_x", C.c_double), ("kh_y", C.c_double),
                 ("seed", C.c_ulonglong), ("real_id", C.c_ulonglong),
                 ("step_i", C.c_ulonglong), ("pid_offset", C.c_ulonglong),
-                ("global_step", C.c_longlong)]
+                ("global_step", C.c_longlong), ("precision", C.c_int)]
 
 
 class BeachArgs(C.Structure):

@@ -19,9 +19,10 @@ ROOT = os.path.dirname(HERE)
 BUILD = os.path.join(ROOT, "_build")
 LIB = os.path.join(HERE, "libkelpcuda.so")
 
-CU_SOURCES = ["kc_api.cu"]
+CU_SOURCES = ["kc_api.cu", "kc_mixed.cu"]
 CPP_SOURCES = ["kc_host.cpp"]
-HEADERS = ["kc_geom.cuh", "kc_interp.cuh", "kc_step.cuh", "kc_beach.cuh", "kc_host.h"]
+HEADERS = ["kc_geom.cuh", "kc_interp.cuh", "kc_step.cuh", "kc_beach.cuh", "kc_mixed.cuh", "kc_kernels.cuh",
+           "kc_host.h"]
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off", "-Xptxas", "-v"]
@@ -46,19 +47,22 @@ def build(verbose: bool = False, force: bool = False) -> str:
     nvcc = _nvcc()
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "kelp_cuda.h")]
     objs = []
-    for src in CU_SOURCES:
+    jobs = []
+    for src in CU_SOURCES:   # the translation units compile in parallel
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
         if force or _stale(o, [s] + hdrs):
             cmd = [nvcc, *NVCC_FLAGS, "-c", s, "-o", o]
-            r = subprocess.run(cmd, capture_output=True, text=True)
-            if r.returncode != 0:
-                raise RuntimeError(f"nvcc failed for {src}:\n{r.stderr}")
-            with open(os.path.join(BUILD, src + ".ptxas.txt"), "w") as fh:
-                fh.write(r.stderr)
-            if verbose:
-                print(r.stderr)
+            jobs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
         objs.append(o)
+    for src, p in jobs:
+        _, err = p.communicate()
+        if p.returncode != 0:
+            raise RuntimeError(f"nvcc failed for {src}:\n{err}")
+        with open(os.path.join(BUILD, src + ".ptxas.txt"), "w") as fh:
+            fh.write(err)
+        if verbose:
+            print(err)
     for src in CPP_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")

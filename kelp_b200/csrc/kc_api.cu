@@ -8,34 +8,30 @@
 #include <algorithm>
 #include <mutex>
 #include <cuda_runtime.h>
+#include <cuda_fp16.h>
 #include <cub/device/device_radix_sort.cuh>
 
 #include "../../include/kelp_cuda.h"
 #include "kc_host.h"
+#include "kc_kernels.cuh"
 #include "kc_beach.cuh"
 
 namespace {
 
 constexpr int kSlots = 8;
 constexpr int kEvents = 16;
-#ifndef KC_BLOCK
-#define KC_BLOCK 128   // threads per block of every kernel (a build option)
-#endif
-#ifndef KC_STEP_MIN_BLOCKS
-// resident blocks per SM the step kernels' register budget must allow: 8
-// blocks of 128 threads cap them at 64 registers (measured fastest on the
-// HEALPix 3-D step: the path is latency-bound, occupancy beats spills)
-#define KC_STEP_MIN_BLOCKS 8
-#endif
-constexpr int kBlock = KC_BLOCK;
+
 
 struct Slot {
     void* u = nullptr;
     void* v = nullptr;
     void* w = nullptr;
+    float* su = nullptr;   // per-row scales of half storage
+    float* sv = nullptr;
+    float* sw = nullptr;
     long long n = 0;
     int uv_rows = 0, w_rows = 0, dtype = -1;
-    size_t cap_uv = 0, cap_w = 0;
+    size_t cap_uv = 0, cap_w = 0, cap_su = 0, cap_sv = 0, cap_sw = 0;
 };
 
 }  // namespace
@@ -98,6 +94,9 @@ struct kc_ctx {
     cudaEvent_t ev[kEvents] = {};
     // L2 eviction buffer of kc_l2_flush
     char* flush = nullptr;
+    // float staging buffer of the half-precision snapshot conversion
+    float* stage = nullptr;
+    size_t stage_cap = 0;
     long long flush_cap = 0;
     unsigned flush_val = 0;
 };
@@ -124,7 +123,7 @@ void dfree(P*& p) {
 
 template <typename T>
 kc::DField<T> field_of(const Slot& s) {
-    return kc::DField<T>{(const T*)s.u, (const T*)s.v, (const T*)s.w};
+    return kc::DField<T>{(const T*)s.u, (const T*)s.v, (const T*)s.w, s.su, s.sv, s.sw};
 }
 
 kc::DState state_of(kc_ctx* c) {
@@ -150,43 +149,6 @@ kc::DStep step_of(const kc_step_args* a) {
     return s;
 }
 
-// delayed release (release.py:112-129): NOT_RELEASED -> ALIVE at its step
-__device__ __forceinline__ void activate(const kc::DState& st, const kc::DStep& s, long long i) {
-    if (st.release_step && s.global_step >= 0 && st.status[i] == kc::NOT_RELEASED &&
-        s.global_step >= (long long)st.release_step[i])
-        st.status[i] = kc::ALIVE;
-}
-
-template <typename T, int SCHEME>
-__global__ void __launch_bounds__(kBlock, KC_STEP_MIN_BLOCKS) k_step2d(const __grid_constant__ kc::DMesh m, const __grid_constant__ kc::DBlend<T> f, const __grid_constant__ kc::DState st, const __grid_constant__ kc::DStep s) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= st.P) return;
-    activate(st, s, i);
-    if (st.prev) st.prev[i] = st.status[i];
-    kc::step2d_particle<T, SCHEME>(m, f, st, s, i);
-}
-
-template <typename T>
-__global__ void __launch_bounds__(kBlock, KC_STEP_MIN_BLOCKS) k_step3d_rk2(const __grid_constant__ kc::DMesh m, const __grid_constant__ kc::DBlend<T> f, const __grid_constant__ kc::DState st, const __grid_constant__ kc::DStep s) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= st.P) return;
-    activate(st, s, i);
-    if (st.prev) st.prev[i] = st.status[i];
-    kc::step3d_rk2_particle<T>(m, f, st, s, i);
-}
-
-template <typename T, int SCHEME>
-__global__ void __launch_bounds__(kBlock, KC_STEP_MIN_BLOCKS) k_step3d_unfused(const __grid_constant__ kc::DMesh m,
-                                                           const __grid_constant__ kc::DBlend<T> f,
-                                                           const __grid_constant__ kc::DState st,
-                                                           const __grid_constant__ kc::DStep s) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= st.P) return;
-    activate(st, s, i);
-    if (st.prev) st.prev[i] = st.status[i];
-    kc::step3d_unfused_particle<T, SCHEME>(m, f, st, s, i);
-}
-
 __global__ void __launch_bounds__(kBlock) k_nearest(const __grid_constant__ kc::DMesh m, const double* q, long long P, int* out) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P) return;
@@ -209,6 +171,39 @@ __global__ void __launch_bounds__(kBlock) k_beach(const __grid_constant__ kc::DM
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= st.P) return;
     kc::beach_particle(m, st, b, N, i);
+}
+
+// Per-row power-of-two scale of a (rows, n) float array for half storage:
+// 2^(e - 15) with max|x| = m 2^e, m in [0.5, 1), so every scaled value is
+// below 2^15 in magnitude; 1 for an all-zero or non-finite row.
+__global__ void k_row_scale(const float* __restrict__ x, long long n, float* __restrict__ scale) {
+    const long long row = blockIdx.x;
+    float mx = 0.0f;
+    for (long long j = threadIdx.x; j < n; j += blockDim.x) mx = fmaxf(mx, fabsf(x[row * n + j]));
+    __shared__ float red[256];
+    red[threadIdx.x] = mx;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] = fmaxf(red[threadIdx.x], red[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const float m = red[0];
+        int e = 0;
+        float sc = 1.0f;
+        if (m > 0.0f && isfinite(m)) {
+            frexpf(m, &e);
+            sc = ldexpf(1.0f, e - 15);
+        }
+        scale[row] = sc;
+    }
+}
+
+__global__ void k_to_half(const float* __restrict__ x, long long n, long long total, const float* __restrict__ scale,
+                          __half* __restrict__ out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    out[i] = __float2half_rn(x[i] / scale[i / n]);
 }
 
 __global__ void k_iota64(long long* out, long long P) {
@@ -281,25 +276,40 @@ int fetch(kc_ctx* c, void* host, const void* dev, int es) {
 }
 
 template <typename T>
-int launch_step(kc_ctx* c, const kc_step_args* a) {
+kc::DBlend<T> blend_of(kc_ctx* c, const kc_step_args* a) {
     kc::DBlend<T> f;
     f.a = field_of<T>(c->slots[a->slot_a]);
     f.b = field_of<T>(c->slots[a->slot_b]);
     f.t = field_of<T>(c->slots[a->slot_t]);
     f.alpha0 = a->alpha0;
     f.n = c->N;
-    kc::DState st = state_of(c);
-    kc::DStep s = step_of(a);
+    return f;
+}
+
+}  // namespace
+
+// the mixed-form kernels (kc_mixed.cu)
+void kc_launch_mixed_f32(const kc::DMesh& m, const kc::DBlend<float>& f, const kc::DState& st, const kc::DStep& s,
+                         int dims, int scheme, cudaStream_t stream);
+void kc_launch_mixed_f16(const kc::DMesh& m, const kc::DBlend<__half>& f, const kc::DState& st,
+                         const kc::DStep& s, int dims, int scheme, cudaStream_t stream);
+
+namespace {
+
+int launch_step(kc_ctx* c, const kc_step_args* a) {
     if (c->P == 0) return KC_OK;
-    unsigned g = grid_for(c->P);
-    if (a->dims == 2) {
-        if (a->scheme == KC_EULER) k_step2d<T, 0><<<g, kBlock, 0, c->stream>>>(c->dm, f, st, s);
-        else if (a->scheme == KC_RK2) k_step2d<T, 1><<<g, kBlock, 0, c->stream>>>(c->dm, f, st, s);
-        else k_step2d<T, 2><<<g, kBlock, 0, c->stream>>>(c->dm, f, st, s);
+    const kc::DState st = state_of(c);
+    const kc::DStep s = step_of(a);
+    const int dtype = c->slots[a->slot_a].dtype;
+    if (a->precision == KC_MIXED) {
+        if (dtype == KC_F16) kc_launch_mixed_f16(c->dm, blend_of<__half>(c, a), st, s, a->dims, a->scheme, c->stream);
+        else kc_launch_mixed_f32(c->dm, blend_of<float>(c, a), st, s, a->dims, a->scheme, c->stream);
+    } else if (dtype == KC_F32) {
+        launch_step_kernel<float, kc::PlainForm<float>>(c->dm, blend_of<float>(c, a), st, s, a->dims, a->scheme,
+                                                         c->stream);
     } else {
-        if (a->scheme == KC_RK2) k_step3d_rk2<T><<<g, kBlock, 0, c->stream>>>(c->dm, f, st, s);
-        else if (a->scheme == KC_RK4) k_step3d_unfused<T, 2><<<g, kBlock, 0, c->stream>>>(c->dm, f, st, s);
-        else k_step3d_unfused<T, 0><<<g, kBlock, 0, c->stream>>>(c->dm, f, st, s);
+        launch_step_kernel<double, kc::PlainForm<double>>(c->dm, blend_of<double>(c, a), st, s, a->dims, a->scheme,
+                                                           c->stream);
     }
     KC_CUDA(c, cudaGetLastError());
     return KC_OK;
@@ -315,6 +325,8 @@ int check_step(kc_ctx* c, const kc_step_args* a) {
     if (!(a->time_dir == 1.0 || a->time_dir == -1.0)) return fail(c, KC_ERR_ARG, "kc_step: time_dir must be +-1");
     if (a->w_code != 0 && a->w_code != 1) return fail(c, KC_ERR_ARG, "kc_step: w_code must be 0 or 1");
     if (a->kick && !(a->kh_x >= 0.0 && a->kh_y >= 0.0)) return fail(c, KC_ERR_ARG, "kc_step: Kh must be >= 0");
+    if (a->precision != KC_PLAIN && a->precision != KC_MIXED)
+        return fail(c, KC_ERR_ARG, "kc_step: precision must be KC_PLAIN or KC_MIXED");
     int sl[3] = {a->slot_a, a->slot_b, a->slot_t};
     int dtype = -1;
     for (int k = 0; k < 3; ++k) {
@@ -324,6 +336,10 @@ int check_step(kc_ctx* c, const kc_step_args* a) {
         if (s.n != c->N) return fail(c, KC_ERR_ARG, "kc_step: snapshot node count differs from the mesh");
         if (dtype >= 0 && s.dtype != dtype) return fail(c, KC_ERR_ARG, "kc_step: snapshots of mixed element types");
         dtype = s.dtype;
+        if (a->precision == KC_PLAIN && dtype == KC_F16)
+            return fail(c, KC_ERR_ARG, "kc_step: the plain form reads float32 or float64 snapshots");
+        if (a->precision == KC_MIXED && dtype == KC_F64)
+            return fail(c, KC_ERR_ARG, "kc_step: the mixed form reads float32 or float16 snapshots");
         if (a->dims == 2 && s.uv_rows != 1) return fail(c, KC_ERR_ARG, "kc_step: 2-D step needs single-row u/v");
         if (a->dims == 3) {
             if (c->dm.K < 2) return fail(c, KC_ERR_STATE, "kc_step: 3-D step needs z-levels and depth");
@@ -346,8 +362,7 @@ int check_step(kc_ctx* c, const kc_step_args* a) {
 int do_step(kc_ctx* c, const kc_step_args* a) {
     int rc = check_step(c, a);
     if (rc) return rc;
-    if (c->slots[a->slot_a].dtype == KC_F32) return launch_step<float>(c, a);
-    return launch_step<double>(c, a);
+    return launch_step(c, a);
 }
 
 template <typename T>
@@ -407,8 +422,8 @@ void kc_destroy(kc_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     free_mesh(c);
     free_particles(c);
-    for (auto& s : c->slots) { dfree(s.u); dfree(s.v); dfree(s.w); }
-    dfree(c->q); dfree(c->qout); dfree(c->d_err); dfree(c->flush);
+    for (auto& s : c->slots) { dfree(s.u); dfree(s.v); dfree(s.w); dfree(s.su); dfree(s.sv); dfree(s.sw); }
+    dfree(c->q); dfree(c->qout); dfree(c->d_err); dfree(c->flush); dfree(c->stage);
     for (int k = 0; k < kEvents; ++k) if (c->ev[k]) cudaEventDestroy(c->ev[k]);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -604,16 +619,42 @@ int kc_depth_points_upload(kc_ctx* c, int M, const double* p, const int* last, c
     return KC_OK;
 }
 
+// One (rows, n) float array into half storage with per-row scales: staged
+// through a float device buffer, scaled and rounded on the device.
+static int upload_half(kc_ctx* c, const float* host, long long n, int rows, float** scale, size_t* scale_cap,
+                       __half* out) {
+    const size_t total = (size_t)n * rows;
+    if (c->stage_cap < total) {
+        KC_CUDA(c, cudaStreamSynchronize(c->stream));
+        dfree(c->stage);
+        KC_CUDA(c, cudaMalloc((void**)&c->stage, total * 4));
+        c->stage_cap = total;
+    }
+    if (*scale == nullptr || *scale_cap < (size_t)rows) {
+        dfree(*scale);
+        KC_CUDA(c, cudaMalloc((void**)scale, (size_t)rows * 4));
+        *scale_cap = rows;
+    }
+    KC_CUDA(c, cudaMemcpyAsync(c->stage, host, total * 4, cudaMemcpyHostToDevice, c->stream));
+    k_row_scale<<<rows, 256, 0, c->stream>>>(c->stage, n, *scale);
+    KC_CUDA(c, cudaGetLastError());
+    k_to_half<<<(unsigned)((total + 255) / 256), 256, 0, c->stream>>>(c->stage, n, (long long)total, *scale, out);
+    KC_CUDA(c, cudaGetLastError());
+    // the staging buffer is reused by the next array
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KC_OK;
+}
+
 int kc_field_upload(kc_ctx* c, int slot, int dtype, long long n_nodes, int n_uv_rows, const void* u,
                     const void* v, int n_w_rows, const void* w) {
     if (!c) return KC_ERR_ARG;
     if (slot < 0 || slot >= kSlots) return fail(c, KC_ERR_ARG, "kc_field_upload: slot out of range");
-    if (dtype != KC_F32 && dtype != KC_F64) return fail(c, KC_ERR_ARG, "kc_field_upload: dtype");
+    if (dtype != KC_F32 && dtype != KC_F64 && dtype != KC_F16) return fail(c, KC_ERR_ARG, "kc_field_upload: dtype");
     if (n_nodes <= 0 || n_uv_rows <= 0 || !u || !v) return fail(c, KC_ERR_ARG, "kc_field_upload: empty u/v");
     if (n_w_rows > 0 && !w) return fail(c, KC_ERR_ARG, "kc_field_upload: missing w");
     KC_CUDA(c, cudaSetDevice(c->device));
     Slot& s = c->slots[slot];
-    size_t es = dtype == KC_F32 ? 4 : 8;
+    size_t es = dtype == KC_F32 ? 4 : (dtype == KC_F16 ? 2 : 8);
     size_t nuv = (size_t)n_nodes * n_uv_rows * es;
     size_t nw = (size_t)n_nodes * (n_w_rows > 0 ? n_w_rows : 0) * es;
     KC_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -628,9 +669,16 @@ int kc_field_upload(kc_ctx* c, int slot, int dtype, long long n_nodes, int n_uv_
         KC_CUDA(c, cudaMalloc(&s.w, nw));
         s.cap_w = nw;
     }
-    KC_CUDA(c, cudaMemcpyAsync(s.u, u, nuv, cudaMemcpyHostToDevice, c->stream));
-    KC_CUDA(c, cudaMemcpyAsync(s.v, v, nuv, cudaMemcpyHostToDevice, c->stream));
-    if (nw) KC_CUDA(c, cudaMemcpyAsync(s.w, w, nw, cudaMemcpyHostToDevice, c->stream));
+    if (dtype == KC_F16) {
+        int rc;
+        if ((rc = upload_half(c, (const float*)u, n_nodes, n_uv_rows, &s.su, &s.cap_su, (__half*)s.u))) return rc;
+        if ((rc = upload_half(c, (const float*)v, n_nodes, n_uv_rows, &s.sv, &s.cap_sv, (__half*)s.v))) return rc;
+        if (nw && (rc = upload_half(c, (const float*)w, n_nodes, n_w_rows, &s.sw, &s.cap_sw, (__half*)s.w))) return rc;
+    } else {
+        KC_CUDA(c, cudaMemcpyAsync(s.u, u, nuv, cudaMemcpyHostToDevice, c->stream));
+        KC_CUDA(c, cudaMemcpyAsync(s.v, v, nuv, cudaMemcpyHostToDevice, c->stream));
+        if (nw) KC_CUDA(c, cudaMemcpyAsync(s.w, w, nw, cudaMemcpyHostToDevice, c->stream));
+    }
     s.n = n_nodes; s.uv_rows = n_uv_rows; s.w_rows = n_w_rows > 0 ? n_w_rows : 0; s.dtype = dtype;
     return KC_OK;
 }

@@ -65,7 +65,7 @@ struct Site {
     double sin_lon, cos_lon;  // of lon * DEG2RAD
 };
 
-__device__ __noinline__ Site make_site(double lon, double lat) {
+static __device__ __noinline__ Site make_site(double lon, double lat) {
     Site s;
     s.lon = lon;
     s.lat = lat;
@@ -82,7 +82,7 @@ __device__ __noinline__ Site make_site(double lon, double lat) {
 // rounded across an integer), |x| - n * 360 is exact (n * 360 is exact, and
 // for n >= 1 Sterbenz's lemma applies: n*360/2 <= |x| <= 2 n*360), so the
 // result equals C fmod bit for bit; larger or non-finite x take fmod itself.
-__device__ __noinline__ double fmod360_slow(double x) { return fmod(x, 360.0); }
+static __device__ __noinline__ double fmod360_slow(double x) { return fmod(x, 360.0); }
 
 __device__ __forceinline__ double fmod360(double x) {
     double a = fabs(x);
@@ -251,7 +251,7 @@ __device__ __forceinline__ int provable_code(const DMesh& m, const Site& q, int 
 }
 
 // mesh.py:1475-1549 _anchor_provable_rect with the reference's own extents.
-__device__ __noinline__ int anchor_provable_rect(const DMesh& m, const Site& q, int node, int rx, int ry) {
+static __device__ __noinline__ int anchor_provable_rect(const DMesh& m, const Site& q, int node, int rx, int ry) {
     double theta_deg, ext_lon;
     cap_extents(m, q, node, theta_deg, ext_lon);
     return provable_code(m, q, rx, ry, theta_deg, ext_lon);
@@ -277,7 +277,7 @@ __device__ __forceinline__ bool provable_fast(const DMesh& m, const Site& q, dou
 
 // mesh.py:1331-1442 _grid_hash_nearest_widened: the 3x3 window, and on an
 // empty window a ring-by-ring scan that stops one ring after the first hit.
-__device__ __noinline__ int nearest_widened(const DMesh& m, const Site& q) {
+static __device__ __noinline__ int nearest_widened(const DMesh& m, const Site& q) {
     double bd2;
     int best = nearest_3x3(m, q, bd2);
     if (best >= 0) return best;
@@ -334,7 +334,7 @@ __device__ __forceinline__ void scan_row_window(const DMesh& m, int cj2, int ci,
 
 // The certificate-driven rectangle growth of mesh.py:1670-1859, entered when
 // the 3x3 hit is not provable (or the window is empty).
-__device__ __noinline__ int nearest_exact_slow(const DMesh& m, const Site& q, int best, int code) {
+static __device__ __noinline__ int nearest_exact_slow(const DMesh& m, const Site& q, int best, int code) {
     const double far = (double)m.far_rows * m.cell;
     const double lat_p = q.lat;
     if (best >= 0) {
@@ -484,7 +484,7 @@ __device__ __noinline__ int nearest_exact_slow(const DMesh& m, const Site& q, in
 // mesh.py:1611-1859 _grid_hash_nearest_exact: the 3x3 window accepted when
 // the certificate proves it (fast bound first, the reference's own
 // certificate when the bound is inconclusive), else the rectangle growth.
-__device__ __noinline__ int nearest_exact(const DMesh& m, const Site& q) {
+static __device__ __noinline__ int nearest_exact(const DMesh& m, const Site& q) {
     const double far = (double)m.far_rows * m.cell;
     if (q.lat < m.lat_min - far || q.lat > m.lat_min + (double)m.ny * m.cell + far) return nearest_widened(m, q);
     double bd2;
@@ -567,15 +567,41 @@ __device__ __forceinline__ void load_poly_mask(const DMesh& m, int4 e, Poly& p) 
     p.n = n;
 }
 
+// Verdicts of element_contains_t for the barycentric W search of
+// vertical.py:744-881, which tests the same fan triangles in the same frame
+// but without the bounding-box prefilter and with a 1e-14 degenerate
+// tolerance: W_OUT when that search rejects the element too, W_UNSURE when
+// it might accept it (bbox-rejected within the tolerance band, a fan
+// triangle with |denominator| in [1e-14, 1e-10), or an element whose W
+// vertex ring differs from the containment vertex set).
+constexpr int W_OUT = 0, W_UNSURE = 2;
+
+__device__ __forceinline__ bool w_ring_matches_mask(const int4& e) {
+    // the W ring drops every later vertex equal to the first valid one, the
+    // mask only slot 3 repeating slot 0: they agree unless another slot
+    // repeats the first valid vertex
+    const int first = e.x >= 0 ? e.x : (e.y >= 0 ? e.y : e.z);
+    if (first < 0) return true;
+    if (e.x >= 0 && e.y == first) return false;
+    if ((e.x >= 0 || e.y >= 0) && e.z == first) return false;
+    if (e.x < 0 && e.w == first) return false;
+    if (e.x >= 0 && e.w == first && e.w != e.x) return false;
+    return true;
+}
+
 // mesh.py:2210-2263 _element_contains with mesh.py:2006-2051
 // _project_to_local_xy and mesh.py:2139-2168 _polygon_contains_bool; the
-// cos of the mean vertex latitude comes from the host table.
-__device__ __forceinline__ bool element_contains(const DMesh& m, int c, double lon_p, double lat_p) {
+// cos of the mean vertex latitude comes from the host table.  Returns 1 when
+// the element contains the point; otherwise 0, or with W_INFO the verdict
+// class of the W search (W_OUT / W_UNSURE).
+template <bool W_INFO>
+__device__ __forceinline__ int element_contains_t(const DMesh& m, int c, double lon_p, double lat_p) {
     int4 e = __ldg(&m.en[c]);
     Poly p;
     load_poly_mask(m, e, p);
     const int n = p.n;
-    if (n < 3) return false;
+    if (n < 3) return (W_INFO && !w_ring_matches_mask(e)) ? W_UNSURE : 0;
+    const int miss = (W_INFO && !w_ring_matches_mask(e)) ? W_UNSURE : 0;
     // bbox prefilter in wrapped-delta space around the first valid vertex
     // (the first vertex's own delta is wrap180(0) == 0)
     const double lon_ref = p.ln[0];
@@ -588,8 +614,15 @@ __device__ __forceinline__ bool element_contains(const DMesh& m, int c, double l
         lamin = fmin(lamin, p.la[3]); lamax = fmax(lamax, p.la[3]);
     }
     const double dlon_p = wrap180(lon_p - lon_ref);
-    if (dlon_p > dmax || dlon_p < dmin) return false;
-    if (lat_p > lamax || lat_p < lamin) return false;
+    if (dlon_p > dmax || dlon_p < dmin || lat_p > lamax || lat_p < lamin) {
+        if (!W_INFO) return 0;
+        // the W search has no bbox: it rejects the element for sure only
+        // beyond the margin of w_ring_rejects (same bound, same frame)
+        if (miss || !(dmax - dmin < 90.0)) return W_UNSURE;
+        const double my = 1e-5 * (lamax - lamin) + 1e-9, mx = 1e-5 * (dmax - dmin) + 1e-9;
+        if (lat_p < lamin - my || lat_p > lamax + my || dlon_p < dmin - mx || dlon_p > dmax + mx) return W_OUT;
+        return W_UNSURE;
+    }
     // local projection: raw-mean origin unless the element spans > 180 deg
     double lmin = fmin(fmin(p.ln[0], p.ln[1]), p.ln[2]), lmax = fmax(fmax(p.ln[0], p.ln[1]), p.ln[2]);
     if (n == 4) { lmin = fmin(lmin, p.ln[3]); lmax = fmax(lmax, p.ln[3]); }
@@ -619,20 +652,26 @@ __device__ __forceinline__ bool element_contains(const DMesh& m, int c, double l
     const double px = wrap180(lon_p - lon0) * DEG2RAD * R_STD * cos_lat0;
     const double py = (lat_p - lat0) * DEG2RAD * R_STD;
     double w1, w2, w3;
-    bary_tri(px, py, x0, y0, x1, y1, x2, y2, w1, w2, w3);
-    if (w1 >= BARY_EPS && w2 >= BARY_EPS && w3 >= BARY_EPS) return true;
-    if (n == 3) return false;
+    bool nondeg = bary_tri(px, py, x0, y0, x1, y1, x2, y2, w1, w2, w3);
+    if (w1 >= BARY_EPS && w2 >= BARY_EPS && w3 >= BARY_EPS) return 1;
+    int verdict = (W_INFO && !nondeg) ? W_UNSURE : miss;
+    if (n == 3) return verdict;
     const double x3 = wrap180(p.ln[3] - lon0) * DEG2RAD * R_STD * cos_lat0;
     const double y3 = (p.la[3] - lat0) * DEG2RAD * R_STD;
-    bary_tri(px, py, x0, y0, x2, y2, x3, y3, w1, w2, w3);
-    return w1 >= BARY_EPS && w2 >= BARY_EPS && w3 >= BARY_EPS;
+    nondeg = bary_tri(px, py, x0, y0, x2, y2, x3, y3, w1, w2, w3);
+    if (w1 >= BARY_EPS && w2 >= BARY_EPS && w3 >= BARY_EPS) return 1;
+    return (W_INFO && !nondeg) ? W_UNSURE : verdict;
 }
 
-__device__ __noinline__ int contain_two_ring(const DMesh& m, double lon_p, double lat_p, int nn);
+__device__ __forceinline__ bool element_contains(const DMesh& m, int c, double lon_p, double lat_p) {
+    return element_contains_t<false>(m, c, lon_p, lat_p) == 1;
+}
+
+static __device__ __noinline__ int contain_two_ring(const DMesh& m, double lon_p, double lat_p, int nn);
 
 // mesh.py:2392-2470 _find_containing_element_local: the 1-ring of the anchor,
 // then its 2-ring; -1 when no element contains the point.
-__device__ __noinline__ int contain_local(const DMesh& m, double lon_p, double lat_p, int nn) {
+static __device__ __noinline__ int contain_local(const DMesh& m, double lon_p, double lat_p, int nn) {
     int s = __ldg(&m.n2e_off[nn]), e = __ldg(&m.n2e_off[nn + 1]);
     if (e == s) return -1;
     for (int k = s; k < e; ++k) {
@@ -642,7 +681,7 @@ __device__ __noinline__ int contain_local(const DMesh& m, double lon_p, double l
     return contain_two_ring(m, lon_p, lat_p, nn);
 }
 
-__device__ __noinline__ int contain_two_ring(const DMesh& m, double lon_p, double lat_p, int nn) {
+static __device__ __noinline__ int contain_two_ring(const DMesh& m, double lon_p, double lat_p, int nn) {
     int s = m.n2e_off[nn], e = m.n2e_off[nn + 1];
     for (int k = s; k < e; ++k) {
         int el = m.n2e[k];
@@ -660,6 +699,28 @@ __device__ __noinline__ int contain_two_ring(const DMesh& m, double lon_p, doubl
         }
     }
     return -1;
+}
+
+// contain_local, plus what its 1-ring scan implies for the barycentric W
+// search of the same point and anchor (vertical.py:744-881): w_elem is the
+// element that search returns (-1: its nodal fallback) unless w_unsure, when
+// only running that search decides.
+static __device__ __noinline__ int contain_local_w(const DMesh& m, double lon_p, double lat_p, int nn, int& w_elem,
+                                                   bool& w_unsure) {
+    w_elem = -1;
+    w_unsure = false;
+    int s = __ldg(&m.n2e_off[nn]), e = __ldg(&m.n2e_off[nn + 1]);
+    if (e == s) return -1;
+    for (int k = s; k < e; ++k) {
+        const int c = __ldg(&m.n2e[k]);
+        const int v = element_contains_t<true>(m, c, lon_p, lat_p);
+        if (v == 1) {
+            w_elem = c;
+            return c;
+        }
+        if (v == W_UNSURE) w_unsure = true;
+    }
+    return contain_two_ring(m, lon_p, lat_p, nn);
 }
 
 }  // namespace kc

@@ -7,12 +7,17 @@
 
 namespace kc {
 
-// Snapshot views: u/v rows are (L, N) row-major, w rows (K, N).
+// Snapshot views: u/v rows are (L, N) row-major, w rows (K, N).  Half
+// precision storage carries one power-of-two scale per row (value =
+// stored * scale); the scale pointers are null for float and double.
 template <typename T>
 struct DField {
     const T* u;
     const T* v;
     const T* w;
+    const float* su;
+    const float* sv;
+    const float* sw;
 };
 
 template <typename T>
@@ -100,13 +105,12 @@ __device__ __forceinline__ bool bary_weights_core(const DMesh& m, int elem, doub
 
 // interpolate.py:1340-1440 _interp_barycentric_core_tinterp (row = 0) and
 // interpolate.py:1443-1529 its 3-D twin (row = the particle's layer).
+// The core given its containing element `elem` (>= 0).
 template <typename T>
-__device__ __noinline__ bool interp_uv_bary(const DMesh& m, const DBlend<T>& f, double xp, double yp, int nn,
-                                            double time_dir, int row, double alpha, double& U, double& V) {
+__device__ __noinline__ bool interp_uv_at(const DMesh& m, const DBlend<T>& f, int elem, double xp, double yp,
+                                          double time_dir, int row, double alpha, double& U, double& V) {
     U = 0.0;
     V = 0.0;
-    int elem = contain_local(m, xp, yp, nn);
-    if (elem < 0) return false;
     Ring r;
     double w[4];
     if (!bary_weights_core(m, elem, xp, yp, m.r_earth, r, w)) return false;
@@ -146,6 +150,18 @@ __device__ __noinline__ bool interp_uv_bary(const DMesh& m, const DBlend<T>& f, 
     U = time_dir * Us;
     V = time_dir * Vs;
     return true;
+}
+
+template <typename T>
+__device__ __forceinline__ bool interp_uv_bary(const DMesh& m, const DBlend<T>& f, double xp, double yp, int nn,
+                                               double time_dir, int row, double alpha, double& U, double& V) {
+    const int elem = contain_local(m, xp, yp, nn);
+    if (elem < 0) {
+        U = 0.0;
+        V = 0.0;
+        return false;
+    }
+    return interp_uv_at<T>(m, f, elem, xp, yp, time_dir, row, alpha, U, V);
 }
 
 // vertical_uv.py:457-523 uv_bracket: (k, alpha) of depth z among the data
@@ -216,12 +232,10 @@ __device__ __forceinline__ void tinterp_point_uv(const DBlend<T>& f, int k, int 
 // read linearly in depth between its bracketing data points (time first),
 // vertices dry at the depth left out.
 template <typename T>
-__device__ __noinline__ bool interp_uv_bary_dl(const DMesh& m, const DBlend<T>& f, double xp, double yp, int nn,
-                                               double z, double time_dir, double alpha, double& U, double& V) {
+__device__ __noinline__ bool interp_uv_dl_at(const DMesh& m, const DBlend<T>& f, int elem, double xp, double yp,
+                                             double z, double time_dir, double alpha, double& U, double& V) {
     U = 0.0;
     V = 0.0;
-    int elem = contain_local(m, xp, yp, nn);
-    if (elem < 0) return false;
     Ring r;
     double w[4];
     if (!bary_weights_core(m, elem, xp, yp, m.r_earth, r, w)) return false;
@@ -290,6 +304,18 @@ __device__ __noinline__ bool interp_uv_bary_dl(const DMesh& m, const DBlend<T>& 
     U = time_dir * Us;
     V = time_dir * Vs;
     return true;
+}
+
+template <typename T>
+__device__ __forceinline__ bool interp_uv_bary_dl(const DMesh& m, const DBlend<T>& f, double xp, double yp, int nn,
+                                                  double z, double time_dir, double alpha, double& U, double& V) {
+    const int elem = contain_local(m, xp, yp, nn);
+    if (elem < 0) {
+        U = 0.0;
+        V = 0.0;
+        return false;
+    }
+    return interp_uv_dl_at<T>(m, f, elem, xp, yp, z, time_dir, alpha, U, V);
 }
 
 // First k in [lo, hi] with z < zl[k + 1] (the caller guarantees one exists):
@@ -491,6 +517,117 @@ __device__ __noinline__ double w_bary(const DMesh& m, const DBlend<T>& f, double
         }
     }
     return w_vertex(m, f, alpha, z, Lz, node, time_dir);
+}
+
+// The barycentric W of vertical.py:744-881 when its search is known to stop
+// at element `el` (contain_local_w): that element's own frame and weights,
+// the first fan triangle for a triangle, Wachspress for a quad.
+template <typename T>
+__device__ __noinline__ double w_bary_at(const DMesh& m, const DBlend<T>& f, double alpha, double xp, double yp,
+                                         double z, int el, double time_dir) {
+    const WLoc Lz = w_locate(m, z);
+    Ring r;
+    load_ring(m, __ldg(&m.en[el]), r);
+    const int nvv = r.n;
+    double lmin = fmin(fmin(r.ln[0], r.ln[1]), r.ln[2]), lmax = fmax(fmax(r.ln[0], r.ln[1]), r.ln[2]);
+    if (nvv == 4) { lmin = fmin(lmin, r.ln[3]); lmax = fmax(lmax, r.ln[3]); }
+    double lon0;
+    if (lmax - lmin > 180.0) {
+        double d = 0.0;
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+            if (v < nvv) d += wrap180(r.ln[v] - r.ln[0]);
+        lon0 = r.ln[0] + d / (double)nvv;
+    } else {
+        double sm = 0.0;
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+            if (v < nvv) sm += r.ln[v];
+        lon0 = sm / (double)nvv;
+    }
+    double lat0 = 0.0;
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+        if (v < nvv) lat0 += r.la[v];
+    lat0 /= (double)nvv;
+    const double cos_lat0 = __ldg(&m.ecos[el]).y;
+    const double R = 6371000.0;
+    double vx[4], vy[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        vx[v] = wrap180(r.ln[v] - lon0) * DEG2RAD * R * cos_lat0;
+        vy[v] = (r.la[v] - lat0) * DEG2RAD * R;
+    }
+    const double px = wrap180(xp - lon0) * DEG2RAD * R * cos_lat0;
+    const double py = (yp - lat0) * DEG2RAD * R;
+    if (nvv == 4) {
+        double wts[4];
+        wachspress_quad(px, py, vx, vy, wts);
+        double acc = 0.0;
+#pragma unroll
+        for (int vi = 0; vi < 4; ++vi) acc += wts[vi] * w_vertex(m, f, alpha, z, Lz, r.v[vi], time_dir);
+        return acc;
+    }
+    const double ax = vx[0], ay = vy[0], bx = vx[1], by = vy[1], cx = vx[2], cy = vy[2];
+    const double denom = (by - cy) * (ax - cx) + (cx - bx) * (ay - cy);
+    const double w1 = ((by - cy) * (px - cx) + (cx - bx) * (py - cy)) / denom;
+    const double w2 = ((cy - ay) * (px - cx) + (ax - cx) * (py - cy)) / denom;
+    const double w3 = 1.0 - w1 - w2;
+    const double w_v0 = w_vertex(m, f, alpha, z, Lz, r.v[0], time_dir);
+    const double w_v1 = w_vertex(m, f, alpha, z, Lz, r.v[1], time_dir);
+    const double w_v2 = w_vertex(m, f, alpha, z, Lz, r.v[2], time_dir);
+    return w1 * w_v0 + w2 * w_v1 + w3 * w_v2;
+}
+
+// The element the barycentric W search of vertical.py:744-881 selects for
+// the point (the first 1-ring element of the anchor with a fan triangle whose
+// three weights are >= -1e-6), or -1 for its nodal fallback: w_bary's loop
+// without the values.
+static __device__ __noinline__ int w_search_elem(const DMesh& m, double xp, double yp, int node) {
+    int s = __ldg(&m.n2e_off[node]), e = __ldg(&m.n2e_off[node + 1]);
+    for (int kk = s; kk < e; ++kk) {
+        const int el = __ldg(&m.n2e[kk]);
+        Ring r;
+        load_ring(m, __ldg(&m.en[el]), r);
+        const int nvv = r.n;
+        if (nvv < 3) continue;
+        if (w_ring_rejects(r, nvv, xp, yp)) continue;
+        double lmin = fmin(fmin(r.ln[0], r.ln[1]), r.ln[2]), lmax = fmax(fmax(r.ln[0], r.ln[1]), r.ln[2]);
+        if (nvv == 4) { lmin = fmin(lmin, r.ln[3]); lmax = fmax(lmax, r.ln[3]); }
+        double lon0;
+        if (lmax - lmin > 180.0) {
+            double d = 0.0;
+            for (int v = 0; v < nvv; ++v) d += wrap180(r.ln[v] - r.ln[0]);
+            lon0 = r.ln[0] + d / (double)nvv;
+        } else {
+            double sm = 0.0;
+            for (int v = 0; v < nvv; ++v) sm += r.ln[v];
+            lon0 = sm / (double)nvv;
+        }
+        double lat0 = 0.0;
+        for (int v = 0; v < nvv; ++v) lat0 += r.la[v];
+        lat0 /= (double)nvv;
+        const double cos_lat0 = __ldg(&m.ecos[el]).y;
+        const double R = 6371000.0;
+        double vx[4], vy[4];
+        for (int v = 0; v < 4; ++v) {
+            vx[v] = wrap180(r.ln[v] - lon0) * DEG2RAD * R * cos_lat0;
+            vy[v] = (r.la[v] - lat0) * DEG2RAD * R;
+        }
+        const double px = wrap180(xp - lon0) * DEG2RAD * R * cos_lat0;
+        const double py = (yp - lat0) * DEG2RAD * R;
+        for (int t = 0; t < nvv - 2; ++t) {
+            const double ax = vx[0], ay = vy[0];
+            const double bx = vx[t + 1], by = vy[t + 1], cx = vx[t + 2], cy = vy[t + 2];
+            const double denom = (by - cy) * (ax - cx) + (cx - bx) * (ay - cy);
+            if (fabs(denom) < 1e-14) continue;
+            const double w1 = ((by - cy) * (px - cx) + (cx - bx) * (py - cy)) / denom;
+            const double w2 = ((cy - ay) * (px - cx) + (ax - cx) * (py - cy)) / denom;
+            const double w3 = 1.0 - w1 - w2;
+            if (w1 >= -1e-6 && w2 >= -1e-6 && w3 >= -1e-6) return el;
+        }
+    }
+    return -1;
 }
 
 // ---------------------------------------------------------------------------

@@ -77,7 +77,7 @@ __device__ __forceinline__ void mark_anchor(const DState& st, long long i, int s
 // kick (diffusion.py:485-529, :261-298), great-circle move, exact re-anchor
 // and containment re-check, revert to the pre-step state on leaving the
 // domain; 3-D reclamp in the new column.
-__device__ __noinline__ void apply_kick(const DMesh& m, const DStep& s, long long pid, const Site& qn,
+static __device__ __noinline__ void apply_kick(const DMesh& m, const DStep& s, long long pid, const Site& qn,
                                         double pre_lon, double pre_lat, double pre_z, int pre_nn, bool is3d,
                                         double& lon, double& lat, double& z, int& status, int& nn, signed char& fr) {
     double g1, g2;
@@ -123,7 +123,7 @@ __device__ __noinline__ void apply_kick(const DMesh& m, const DStep& s, long lon
 // integrators.py:2521-2638 (RK2), :2641-2816 (RK4); Euler follows the
 // per-particle arithmetic of the unfused path (integrators.py:4997-5147):
 // one stage at the start, move, re-anchor, domain check.
-template <typename T, int SCHEME>
+template <typename T, int SCHEME, typename Form>
 __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>& f, const DState& st,
                                                 const DStep& s, long long i) {
     int status = st.status[i];
@@ -143,7 +143,7 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
     const int node_i = start_anchor(m, st, q0, pre_nn, i);
 
     double U1, V1;
-    bool ok1 = interp_uv_bary<T>(m, f, lon0, lat0, node_i, td, 0, s.ak[0], U1, V1);
+    bool ok1 = Form::uv2(m, f, s, lon0, lat0, node_i, s.ak[0], U1, V1);
     st.U[i] = U1;
     st.V[i] = V1;
     if (!ok1) {
@@ -157,7 +157,7 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
         const Site qm = make_site(lon_mid, lat_mid);
         int nn_mid = site_anchor(m, qm);
         double U2, V2;
-        if (!interp_uv_bary<T>(m, f, lon_mid, lat_mid, nn_mid, td, 0, s.ak[1], U2, V2)) {
+        if (!Form::uv2(m, f, s, lon_mid, lat_mid, nn_mid, s.ak[1], U2, V2)) {
             status = OUTSIDE; fr = FR_INTERP; nn_out = node_i; failed = true;
         } else {
             lon_new = wrap180(lon0 + dt * U2 / metric_z0(qm));
@@ -170,7 +170,7 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
         double lat2 = clamp_lat(lat0 + 0.5 * dlat1);
         const Site q2 = make_site(lon2, lat2);
         double U2, V2;
-        if (!interp_uv_bary<T>(m, f, lon2, lat2, site_anchor(m, q2), td, 0, s.ak[1], U2, V2)) {
+        if (!Form::uv2(m, f, s, lon2, lat2, site_anchor(m, q2), s.ak[1], U2, V2)) {
             status = OUTSIDE; fr = FR_INTERP; nn_out = node_i; failed = true;
         } else {
             double dlon2 = dt * U2 / metric_z0(q2);
@@ -179,7 +179,7 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
             double lat3 = clamp_lat(lat0 + 0.5 * dlat2);
             const Site q3 = make_site(lon3, lat3);
             double U3, V3;
-            if (!interp_uv_bary<T>(m, f, lon3, lat3, site_anchor(m, q3), td, 0, s.ak[2], U3, V3)) {
+            if (!Form::uv2(m, f, s, lon3, lat3, site_anchor(m, q3), s.ak[2], U3, V3)) {
                 status = OUTSIDE; fr = FR_INTERP; nn_out = node_i; failed = true;
             } else {
                 double dlon3 = dt * U3 / metric_z0(q3);
@@ -188,7 +188,7 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
                 double lat4 = clamp_lat(lat0 + dlat3);
                 const Site q4 = make_site(lon4, lat4);
                 double U4, V4;
-                if (!interp_uv_bary<T>(m, f, lon4, lat4, site_anchor(m, q4), td, 0, s.ak[3], U4, V4)) {
+                if (!Form::uv2(m, f, s, lon4, lat4, site_anchor(m, q4), s.ak[3], U4, V4)) {
                     status = OUTSIDE; fr = FR_INTERP; nn_out = node_i; failed = true;
                 } else {
                     double dlon4 = dt * U4 / metric_z0(q4);
@@ -246,15 +246,48 @@ __device__ __forceinline__ bool stage_uv(const DMesh& m, const DBlend<T>& f, con
     return interp_uv_bary<T>(m, f, lon, lat, nn, s.time_dir, layer, alpha, U, V);
 }
 
+// The plain form: the reference's float64 interpolation, bit for bit.
+// uvw3 evaluates W even where u/v failed (the caller then discards it).
+template <typename T>
+struct PlainForm {
+    static __device__ __forceinline__ bool uv2(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
+                                               double lat, int nn, double alpha, double& U, double& V) {
+        return interp_uv_bary<T>(m, f, lon, lat, nn, s.time_dir, 0, alpha, U, V);
+    }
+    static __device__ __forceinline__ bool uvw3(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
+                                                double lat, int nn, double z, double alpha, double& U, double& V,
+                                                double& W) {
+        if (s.w_code == 0) {
+            const bool ok = stage_uv<T>(m, f, s, lon, lat, nn, z, alpha, U, V);
+            W = w_linear<T>(m, f, alpha, z, nn, s.time_dir);
+            return ok;
+        }
+        // W barycentric: one containment scan decides the u/v element and,
+        // almost always, the element the W search would stop at
+        int w_elem;
+        bool w_unsure;
+        const int elem = contain_local_w(m, lon, lat, nn, w_elem, w_unsure);
+        bool ok = false;
+        U = 0.0;
+        V = 0.0;
+        if (elem >= 0) {
+            ok = s.uv_dl ? interp_uv_dl_at<T>(m, f, elem, lon, lat, z, s.time_dir, alpha, U, V)
+                         : interp_uv_at<T>(m, f, elem, lon, lat, s.time_dir, find_layer(m, z, nn), alpha, U, V);
+        }
+        if (w_unsure) W = w_bary<T>(m, f, alpha, lon, lat, z, nn, s.time_dir);
+        else if (w_elem >= 0) W = w_bary_at<T>(m, f, alpha, lon, lat, z, w_elem, s.time_dir);
+        else W = w_vertex<T>(m, f, alpha, z, w_locate(m, z), nn, s.time_dir);
+        return ok;
+    }
+};
+
 // One 3-D stage of the unfused paths: exact anchor at the stage position,
 // u/v at the stage depth, W from the stage blend.
-template <typename T>
+template <typename T, typename Form>
 __device__ __forceinline__ bool stage3d(const DMesh& m, const DBlend<T>& f, const DStep& s, int k, double lon,
                                         double lat, double z, const Site& q, double& U, double& V, double& W) {
     const int nn = site_anchor(m, q);
-    if (!stage_uv<T>(m, f, s, lon, lat, nn, z, s.ak[k], U, V)) return false;
-    W = stage_w<T>(m, f, s.w_code, s.ak[k], lon, lat, z, nn, s.time_dir);
-    return true;
+    return Form::uvw3(m, f, s, lon, lat, nn, z, s.ak[k], U, V, W);
 }
 
 // 3-D Euler (integrators.py:4997-5147) and RK4 (:5760-6011): the reference's
@@ -262,7 +295,7 @@ __device__ __forceinline__ bool stage3d(const DMesh& m, const DBlend<T>& f, cons
 // every stage position, the layer at the stage depth, the whole-field stage
 // lerps of _make_stage_vels (:1187-1237) reproduced per vertex, W at the stage
 // position; a failure reverts to the start with the start anchor.
-template <typename T, int SCHEME>
+template <typename T, int SCHEME, typename Form>
 __device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DBlend<T>& f, const DState& st,
                                                         const DStep& s, long long i) {
     int status = st.status[i];
@@ -281,9 +314,8 @@ __device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DB
     const Site q0 = make_site(lon0, lat0);
     const int node_i = start_anchor(m, st, q0, pre_nn, i);
     int nn_out = node_i;
-    double U1, V1;
-    bool ok = stage_uv<T>(m, f, s, lon0, lat0, node_i, z0p, s.ak[0], U1, V1);
-    const double W1 = stage_w<T>(m, f, s.w_code, s.ak[0], lon0, lat0, z0p, node_i, td);
+    double U1, V1, W1;
+    bool ok = Form::uvw3(m, f, s, lon0, lat0, node_i, z0p, s.ak[0], U1, V1, W1);
     st.U[i] = U1;
     st.V[i] = V1;
     st.W[i] = W1;
@@ -298,19 +330,19 @@ __device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DB
             const double l2 = wrap180(lon0 + 0.5 * dl1), t2 = clamp_lat(lat0 + 0.5 * dd1), z2 = z0p + 0.5 * dz1;
             const Site q2 = make_site(l2, t2);
             double U2, V2, W2;
-            ok = stage3d<T>(m, f, s, 1, l2, t2, z2, q2, U2, V2, W2);
+            ok = stage3d<T, Form>(m, f, s, 1, l2, t2, z2, q2, U2, V2, W2);
             if (ok) {
                 const double dl2 = dt * U2 / metric_z0(q2), dd2 = dt * V2 / SLM, dz2 = dt * W2;
                 const double l3 = wrap180(lon0 + 0.5 * dl2), t3 = clamp_lat(lat0 + 0.5 * dd2), z3 = z0p + 0.5 * dz2;
                 const Site q3 = make_site(l3, t3);
                 double U3, V3, W3;
-                ok = stage3d<T>(m, f, s, 2, l3, t3, z3, q3, U3, V3, W3);
+                ok = stage3d<T, Form>(m, f, s, 2, l3, t3, z3, q3, U3, V3, W3);
                 if (ok) {
                     const double dl3 = dt * U3 / metric_z0(q3), dd3 = dt * V3 / SLM, dz3 = dt * W3;
                     const double l4 = wrap180(lon0 + dl3), t4 = clamp_lat(lat0 + dd3), z4 = z0p + dz3;
                     const Site q4 = make_site(l4, t4);
                     double U4, V4, W4;
-                    ok = stage3d<T>(m, f, s, 3, l4, t4, z4, q4, U4, V4, W4);
+                    ok = stage3d<T, Form>(m, f, s, 3, l4, t4, z4, q4, U4, V4, W4);
                     if (ok) {
                         const double dl4 = dt * U4 / metric_z0(q4), dd4 = dt * V4 / SLM, dz4 = dt * W4;
                         const double dl = (dl1 + 2.0 * dl2 + 2.0 * dl3 + dl4) / 6.0;
@@ -357,7 +389,7 @@ __device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DB
 // integrators.py:3647-3856 _fused_rk2_step_3d_bary_tinterp (layer u/v,
 // z-level), with the exact stage-1 anchor of its runner (:4766-4770) and the
 // split kick epilogue.
-template <typename T>
+template <typename T, typename Form>
 __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend<T>& f, const DState& st,
                                                     const DStep& s, long long i) {
     int status = st.status[i];
@@ -376,9 +408,8 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
     const Site q0 = make_site(lon0, lat0);
     const int node_i = start_anchor(m, st, q0, pre_nn, i);
     int nn_out = node_i;
-    double U1, V1;
-    const bool ok1 = stage_uv<T>(m, f, s, lon0, lat0, node_i, z0p, s.ak[0], U1, V1);
-    const double W1 = stage_w<T>(m, f, s.w_code, s.ak[0], lon0, lat0, z0p, node_i, td);
+    double U1, V1, W1;
+    const bool ok1 = Form::uvw3(m, f, s, lon0, lat0, node_i, z0p, s.ak[0], U1, V1, W1);
     st.U[i] = U1;
     st.V[i] = V1;
     st.W[i] = W1;
@@ -390,11 +421,10 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
         const double z_mid = z0p + W1 * 0.5 * dt;
         const Site qm = make_site(lon_mid, lat_mid);
         const int nn_mid = site_anchor(m, qm);
-        double U2, V2;
-        if (!stage_uv<T>(m, f, s, lon_mid, lat_mid, nn_mid, z_mid, s.ak[1], U2, V2)) {
+        double U2, V2, W2;
+        if (!Form::uvw3(m, f, s, lon_mid, lat_mid, nn_mid, z_mid, s.ak[1], U2, V2, W2)) {
             status = OUTSIDE; fr = FR_INTERP;
         } else {
-            const double W2 = stage_w<T>(m, f, s.w_code, s.ak[1], lon_mid, lat_mid, z_mid, nn_mid, td);
             const double ln = wrap180(lon0 + dt * U2 / metric_z0(qm));
             const double lt = clamp_lat(lat0 + dt * V2 / SLM);
             double zn = z0p + W2 * dt;

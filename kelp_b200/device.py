@@ -147,30 +147,36 @@ class DeviceContext:
 
     # -- snapshot ring --------------------------------------------------------
     def upload_field(self, field, slot: int, dtype=None) -> None:
+        """Upload one snapshot into ring slot ``slot``: float32 or float64
+        storage, or ``np.float16`` for half storage with per-row power-of-two
+        scales (converted on the device from float32)."""
         u = np.asarray(field.u)
         v = np.asarray(field.v)
         w = None if getattr(field, "w", None) is None else np.asarray(field.w)
         if dtype is None:
             dtype = np.float32 if (u.dtype == np.float32 and v.dtype == np.float32
                                    and (w is None or w.dtype == np.float32)) else np.float64
-        u = _c(u, dtype)
-        v = _c(v, dtype)
-        w = None if w is None else _c(w, dtype)
+        code = {np.dtype(np.float32): N.KC_F32, np.dtype(np.float64): N.KC_F64,
+                np.dtype(np.float16): N.KC_F16}[np.dtype(dtype)]
+        host = np.float32 if code == N.KC_F16 else dtype
+        u = _c(u, host)
+        v = _c(v, host)
+        w = None if w is None else _c(w, host)
         n = u.shape[-1]
         rows = 1 if u.ndim == 1 else u.shape[0]
         wrows = 0 if w is None else (1 if w.ndim == 1 else w.shape[0])
-        code = N.KC_F32 if dtype == np.float32 else N.KC_F64
         self._chk(N.lib().kc_field_upload(self._ctx, slot, code, n, rows, N.ptr(u), N.ptr(v), wrows, N.ptr(w)),
                   "kc_field_upload")
         self.synchronize()
 
-    def slots_for(self, fields) -> list:
+    def slots_for(self, fields, storage=None) -> list:
         """Ring slots holding ``fields`` (uploading the ones not resident).
         All fields of one step share one element type: float32 only when every
-        one of them is float32."""
+        one of them is float32, unless ``storage`` names it (``np.float16``:
+        half storage with per-row scales)."""
         all32 = all(np.asarray(f.u).dtype == np.float32 and np.asarray(f.v).dtype == np.float32
                     and (f.w is None or np.asarray(f.w).dtype == np.float32) for f in fields)
-        dtype = np.float32 if all32 else np.float64
+        dtype = np.dtype(storage) if storage is not None else np.dtype(np.float32 if all32 else np.float64)
         out = []
         pinned = set()
         for f in fields:

@@ -8,7 +8,11 @@ vel_next, dt_to_next, diffusion, ...) -> ParticleState``.  ``INTEGRATORS`` /
 module is a drop-in at the plugin point.
 
 Every supported combination runs as one CUDA kernel launch per step; there is
-no CPU path.  Combinations this build does not implement raise
+no CPU path.  Two backend keywords select the numerical form:
+``cuda_precision="plain"`` (default: the reference's float64 arithmetic) or
+``"mixed"`` (float32 interpolation, float64 positions and element decisions),
+and ``cuda_snapshots="f16"`` stores the snapshots as float16 with per-row
+scales (mixed form only).  Combinations this build does not implement raise
 ``NotImplementedError`` before any device work, naming what is missing.
 Argument errors raise ``ValueError`` in Python, as in the reference.
 """
@@ -150,12 +154,23 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
                                       "3-D RK2 path, which is not built on the CUDA backend")
     vel_a, vel_b, target, alpha0 = _fields(vel, vel_next)
     _check_node_fields(mesh, [vel_a, vel_b, target], is3d, placement)
+    form = kw.get("cuda_precision", "plain")
+    if form not in ("plain", "mixed"):
+        raise ValueError(f"cuda_precision must be 'plain' or 'mixed', got {form!r}")
+    storage = kw.get("cuda_snapshots", None)
+    if storage not in (None, "f32", "f16"):
+        raise ValueError(f"cuda_snapshots must be None, 'f32' or 'f16', got {storage!r}")
+    if storage == "f16" and form != "mixed":
+        raise ValueError("float16 snapshots are read by the mixed form only (cuda_precision='mixed')")
+    store = {None: None, "f32": np.float32, "f16": np.float16}[storage]
+    if form == "mixed" and store is None:
+        store = np.float32
 
     ctx = ctx or default_context()
     ctx.ensure_mesh(mesh)
     if is3d and placement != "layer":
         ctx.ensure_depth_points(mesh, placement)
-    sa, sb, st = ctx.slots_for([vel_a, vel_b, target])
+    sa, sb, st = ctx.slots_for([vel_a, vel_b, target], store)
     a = N.StepArgs()
     a.scheme = code
     a.dims = 3 if is3d else 2
@@ -172,6 +187,7 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
         a.kick = 1
         a.kh_x, a.kh_y, a.seed, a.real_id, a.step_i, a.pid_offset = kick
     a.global_step = -1
+    a.precision = N.KC_MIXED if form == "mixed" else N.KC_PLAIN
     return a, is3d
 
 

@@ -31,6 +31,7 @@ class Workload:
     w_interp: str = "nearest"
     kh: Optional[tuple] = None      # (kh_x, kh_y) of the split uniform kick
     seed: int = 0
+    uv_vertical: str = "layer"      # 3-D u/v placement: layer, level or layer_linear
     description: dict = field(default_factory=dict)
 
     @property
@@ -50,7 +51,7 @@ class Workload:
             alpha = 0.0
         return ia, (ia + 1) % n, alpha, (ta + self.interval) - tw
 
-    def step_args(self, k: int, slots) -> N.StepArgs:
+    def step_args(self, k: int, slots, precision: int = N.KC_PLAIN) -> N.StepArgs:
         ia, ib, alpha0, dtn = self.bracket(k)
         a = N.StepArgs()
         a.scheme = {"euler": N.KC_EULER, "rk2": N.KC_RK2, "rk4": N.KC_RK4}[self.scheme]
@@ -69,6 +70,8 @@ class Workload:
             a.kh_x, a.kh_y = self.kh
             a.seed, a.real_id, a.step_i, a.pid_offset = self.seed, 0, k, 0
         a.global_step = -1
+        a.uv_vertical = 0 if self.uv_vertical == "layer" else 1
+        a.precision = precision
         return a
 
 
@@ -84,6 +87,26 @@ def c1(P: int = 100_000, spacing: float = 0.5625) -> Workload:
                     description={"mesh": "jittered 0.5625 deg lattice, 30% land", "nodes": int(m.n_nodes),
                                  "elements": int(m.n_elements), "particles": P, "scheme": "rk2",
                                  "dt_s": 3600, "steps_run": 240, "fields": "f32 node u,v, 2 snapshots 24 h"})
+
+
+def c2(P: int = 1_000_000, spacing: float = 0.5625, n_levels: int = 47) -> Workload:
+    """3-D depth-linear on the C1 mesh: 47 z-level interfaces (5 m .. 6000 m
+    stretched), smooth bathymetry 50-6000 m, u/v/w float32 on nodes x levels
+    (uv_vertical level; w from the continuity of the gyre field), 4 snapshots
+    3.5 days apart cycled, 1 M particles uniform in the wet volume, RK4, dt
+    30 min, 480 steps, W nearest."""
+    zl = S.stretched_levels(n_levels, 5.0, 6000.0)
+    m = S.lattice_mesh(spacing, 80.0, jitter=0.2, land_frac=0.3,
+                       depth=lambda lo, la: S.smooth_bathymetry(lo, la, 50.0, 6000.0), sigma=zl)
+    snaps = S.gyre_snapshots(m, 4, amp=0.5, z_levels=zl, decay=1000.0, w_scale=1e-3, placement="level")
+    lon, lat, z = S.release_uniform(m, P, seed=3, depth_uniform=True)
+    return Workload("c2_fesom2_3d_dl_rk4", m, snaps, lon, lat, z, "rk4", 1800.0, 3.5 * 86400.0, 480,
+                    dims=3, w_interp="nearest", uv_vertical="level",
+                    description={"mesh": "jittered 0.5625 deg lattice, 30% land", "nodes": int(m.n_nodes),
+                                 "elements": int(m.n_elements), "levels": n_levels, "particles": P,
+                                 "scheme": "rk4", "dt_s": 1800, "steps_run": 480,
+                                 "fields": "f32 node u,v,w (47,N) depth-linear (level), 4 snapshots 3.5 d",
+                                 "w_interp": "nearest"})
 
 
 def c3(P: int = 6_000_000, nside: int = 512, n_levels: int = 69, n_snap: int = 2) -> Workload:
@@ -121,4 +144,4 @@ def c3_small(P: int = 200_000) -> Workload:
     return w
 
 
-WORKLOADS: dict = {"c1": c1, "c3": c3, "c3small": c3_small}
+WORKLOADS: dict = {"c1": c1, "c2": c2, "c3": c3, "c3small": c3_small}
