@@ -114,15 +114,16 @@ class ClockSampler:
 
 
 def _oracle_run(wl, n_particles: int, step_iter, view=None):
-    """Oracle steps over the first ``n_particles`` particles of the workload
-    (a uniform random sample: releases are seeded uniform); yields seconds."""
+    """Oracle steps over ``n_particles`` particles of the workload, evenly
+    strided through the seed order; yields seconds."""
     from oracle import oracle as O
     from kelp_b200.particles import make_state
     from kelp_b200.fields import LazyLerpField
     from kelp_b200.diffusion import DiffusionStepArgs
     view = view or O.MeshView(wl.mesh)
     n = min(n_particles, wl.P)
-    st = make_state(wl.lon[:n], wl.lat[:n], wl.z[:n])
+    idx = np.linspace(0, wl.P - 1, n).astype(np.int64)   # spread over the (sorted) seed order
+    st = make_state(wl.lon[idx], wl.lat[idx], wl.z[idx])
     st = st.replace(failure_reason=np.zeros(n, np.int8))
     for k in step_iter:
         ia, ib, alpha0, dtn = wl.bracket(k)
@@ -266,10 +267,7 @@ def run_b200(args):
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
     from kelp_b200 import workloads, roofline
-    from kelp_b200 import integrators as KI
     from kelp_b200.device import set_default_device, default_context, pinned_empty
-    from kelp_b200.fields import LazyLerpField
-    from kelp_b200.particles import ParticleState
 
     wl = workloads.WORKLOADS[args.workload]()
     set_default_device(local)
@@ -331,37 +329,36 @@ def run_b200(args):
     t_wall1 = time.time()
     clocks = sampler.stop(t_wall0, t_wall1)
 
-    # end to end through the public step API, headline form: host state in
-    # page-locked memory copied in and out every step
-    code, store = FORMS[args.form]
-    api_kw = {"cuda_precision": code}
-    if store is np.float16:
-        api_kw["cuda_snapshots"] = "f16"
-    st_h = {}
-    for name, dt_, src in (("lon", np.float64, wl.lon), ("lat", np.float64, wl.lat), ("z", np.float64, wl.z),
-                           ("status", np.int32, np.full(P, 1, np.int32)),
-                           ("nearest_node", np.int32, np.full(P, -1, np.int32)),
-                           ("failure_reason", np.int8, np.zeros(P, np.int8))):
-        a = pinned_empty((P,), dt_)
-        a[:] = src
-        st_h[name] = a
-    state = ParticleState(**st_h)
-    step_fn = KI.get_integrator(wl.scheme)
-    from kelp_b200.diffusion import DiffusionStepArgs
+    # end to end through the C-ABI host-buffer step (kc_step_host), headline
+    # form: every step uploads the state from page-locked host arrays, steps
+    # it and downloads the new state (positions, status, anchors, failure
+    # reasons, velocities), chunked so the copies overlap the step
+    names_in = {"lon": np.float64, "lat": np.float64, "z": np.float64, "status": np.int32,
+                "nearest_node": np.int32, "failure_reason": np.int8}
+    names_out = dict(names_in, u=np.float64, v=np.float64, w=np.float64)
+    bufs = []
+    for _ in range(2):
+        d = {name: pinned_empty((P,), dt_) for name, dt_ in names_out.items()}
+        bufs.append(d)
+    bufs[0]["lon"][:] = wl.lon
+    bufs[0]["lat"][:] = wl.lat
+    bufs[0]["z"][:] = wl.z
+    bufs[0]["status"][:] = 1
+    bufs[0]["nearest_node"][:] = -1
+    bufs[0]["failure_reason"][:] = 0
     e2e_steps = max(1, min(args.steps, 20))
+
+    def e2e_args(k):
+        a_ = _form_args(wl, k, slots, args.form)
+        a_.pid_offset = pid_base
+        return a_
+
+    ctx.step_host(e2e_args(0), {n: bufs[0][n] for n in names_in}, bufs[1])   # warm-up
     barrier()
     ctx.record(2)
     for k in range(e2e_steps):
-        ia, ib, alpha0, dtn = wl.bracket(k)
-        a, b = wl.snaps[ia], wl.snaps[ib]
-        vel = a if alpha0 == 0.0 else LazyLerpField(a, b, alpha0)
-        diff = None if wl.kh is None else DiffusionStepArgs("uniform", wl.kh[0], wl.kh[1], wl.seed, 0, k,
-                                                            pid_offset=pid_base)
-        state = step_fn(state, vel, wl.mesh, wl.dt, 1.0, uv_interp="barycentric", w_interp=wl.w_interp,
-                        vel_next=b, dt_to_next=dtn, diffusion=diff, **api_kw)
-        for name in ("lon", "lat", "z", "status", "nearest_node", "failure_reason"):
-            st_h[name][:] = getattr(state, name)
-        state = ParticleState(**st_h)
+        src, dst = bufs[k % 2], bufs[(k + 1) % 2]
+        ctx.step_host(e2e_args(k), {n: src[n] for n in names_in}, dst)
     ctx.record(3)
     e2e_ms = ctx.elapsed_ms(2, 3)
     if dist is not None:
@@ -406,7 +403,7 @@ def run_b200(args):
                 "forms": per_form,
                 "e2e": {"value": world * P * e2e_steps / (e2e_ms * 1e-3), "unit": UNIT,
                         "h2d_bytes_per_step": h2d * world, "d2h_bytes_per_step": d2h * world,
-                        "steps": e2e_steps, "form": args.form},
+                        "steps": e2e_steps, "form": args.form, "api": "kc_step_host, page-locked host arrays"},
                 "gpu_launches": timed[args.form]["launches"], "clocks": clocks,
                 "resort": {"every_steps": args.sort_every, "ms_total": timed[args.form]["sort_ms"]}}
         if acc is not None:

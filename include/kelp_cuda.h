@@ -156,6 +156,33 @@ int kc_beach_state_download(kc_ctx* ctx, int* wet_streak);
 /* The beaching hook on the resident particles after a step. */
 int kc_beach(kc_ctx* ctx, const kc_beach_args* args);
 
+/* Host particle arrays of kc_step_host (SoA, P entries each).  Input: lon,
+ * lat, status, nearest_node required; z and failure_reason may be NULL
+ * (zeros).  Output: lon, lat, status, nearest_node required; z,
+ * failure_reason, u, v, w may be NULL (not returned).  Input and output may
+ * be the same arrays. */
+typedef struct kc_host_particles {
+    double* lon;
+    double* lat;
+    double* z;
+    int* status;
+    int* nearest_node;
+    signed char* failure_reason;
+    double* u;
+    double* v;
+    double* w;
+} kc_host_particles;
+
+/* One step of P particles held in host memory, in the reference's per-step
+ * form (state in, new state out; tracking.py:2643-2655): the particles are
+ * cut into chunks of `chunk` (0: P/8, at most 64 chunks) whose upload,
+ * step and download run on three streams, so the copies of one chunk overlap
+ * the step of another.  Page-locked host arrays (kc_host_alloc) make the
+ * copies asynchronous.  RNG keys are pid_offset + the particle's index.  The
+ * particles stay resident afterwards, as after kc_particles_upload + kc_step. */
+int kc_step_host(kc_ctx* ctx, const kc_step_args* args, long long P, const kc_host_particles* in,
+                 const kc_host_particles* out, long long chunk);
+
 /* One step of every resident particle; kc_run: n_steps steps in order,
  * per-step arguments, no host round trip in between. */
 int kc_step(kc_ctx* ctx, const kc_step_args* args);

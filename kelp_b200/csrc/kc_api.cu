@@ -20,6 +20,7 @@ namespace {
 
 constexpr int kSlots = 8;
 constexpr int kEvents = 16;
+constexpr int kChunks = 64;   // most chunks of one host-buffer step
 
 
 struct Slot {
@@ -92,6 +93,9 @@ struct kc_ctx {
     int* qout = nullptr;
     long long qcap = 0;
     cudaEvent_t ev[kEvents] = {};
+    // the host-buffer step's copy streams and per-chunk events (created on first use)
+    cudaStream_t s_in = nullptr, s_out = nullptr;
+    cudaEvent_t ev_in[kChunks] = {}, ev_k[kChunks] = {}, ev_start = nullptr;
     // L2 eviction buffer of kc_l2_flush
     char* flush = nullptr;
     // float staging buffer of the half-precision snapshot conversion
@@ -296,10 +300,7 @@ void kc_launch_mixed_f16(const kc::DMesh& m, const kc::DBlend<__half>& f, const 
 
 namespace {
 
-int launch_step(kc_ctx* c, const kc_step_args* a) {
-    if (c->P == 0) return KC_OK;
-    const kc::DState st = state_of(c);
-    const kc::DStep s = step_of(a);
+int launch_step_on(kc_ctx* c, const kc_step_args* a, const kc::DState& st, const kc::DStep& s) {
     const int dtype = c->slots[a->slot_a].dtype;
     if (a->precision == KC_MIXED) {
         if (dtype == KC_F16) kc_launch_mixed_f16(c->dm, blend_of<__half>(c, a), st, s, a->dims, a->scheme, c->stream);
@@ -313,6 +314,11 @@ int launch_step(kc_ctx* c, const kc_step_args* a) {
     }
     KC_CUDA(c, cudaGetLastError());
     return KC_OK;
+}
+
+int launch_step(kc_ctx* c, const kc_step_args* a) {
+    if (c->P == 0) return KC_OK;
+    return launch_step_on(c, a, state_of(c), step_of(a));
 }
 
 int check_step(kc_ctx* c, const kc_step_args* a) {
@@ -425,6 +431,13 @@ void kc_destroy(kc_ctx* c) {
     for (auto& s : c->slots) { dfree(s.u); dfree(s.v); dfree(s.w); dfree(s.su); dfree(s.sv); dfree(s.sw); }
     dfree(c->q); dfree(c->qout); dfree(c->d_err); dfree(c->flush); dfree(c->stage);
     for (int k = 0; k < kEvents; ++k) if (c->ev[k]) cudaEventDestroy(c->ev[k]);
+    for (int k = 0; k < kChunks; ++k) {
+        if (c->ev_in[k]) cudaEventDestroy(c->ev_in[k]);
+        if (c->ev_k[k]) cudaEventDestroy(c->ev_k[k]);
+    }
+    if (c->ev_start) cudaEventDestroy(c->ev_start);
+    if (c->s_in) { cudaStreamSynchronize(c->s_in); cudaStreamDestroy(c->s_in); }
+    if (c->s_out) { cudaStreamSynchronize(c->s_out); cudaStreamDestroy(c->s_out); }
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -683,6 +696,27 @@ int kc_field_upload(kc_ctx* c, int slot, int dtype, long long n_nodes, int n_uv_
     return KC_OK;
 }
 
+// Device particle buffers for at least P particles.
+static int ensure_capacity(kc_ctx* c, long long P) {
+    if (P <= c->cap) return KC_OK;
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    free_particles(c);
+    // every per-particle buffer holds 8 bytes per particle, so the re-sort
+    // can gather any array into the spare buffer and swap the pointers
+    size_t n = (size_t)P * 8;
+    KC_CUDA(c, cudaMalloc((void**)&c->lon, n)); KC_CUDA(c, cudaMalloc((void**)&c->lat, n));
+    KC_CUDA(c, cudaMalloc((void**)&c->z, n)); KC_CUDA(c, cudaMalloc((void**)&c->U, n));
+    KC_CUDA(c, cudaMalloc((void**)&c->V, n)); KC_CUDA(c, cudaMalloc((void**)&c->W, n));
+    KC_CUDA(c, cudaMalloc((void**)&c->status, n)); KC_CUDA(c, cudaMalloc((void**)&c->nn, n));
+    KC_CUDA(c, cudaMalloc((void**)&c->fr, n)); KC_CUDA(c, cudaMalloc((void**)&c->pid, n));
+    KC_CUDA(c, cudaMalloc((void**)&c->rs, n)); KC_CUDA(c, cudaMalloc((void**)&c->orig, n));
+    KC_CUDA(c, cudaMalloc((void**)&c->spare, n));
+    KC_CUDA(c, cudaMalloc((void**)&c->prev, n)); KC_CUDA(c, cudaMalloc((void**)&c->wet, n));
+    KC_CUDA(c, cudaMalloc((void**)&c->nn_ok, n));
+    c->cap = P;
+    return KC_OK;
+}
+
 int kc_particles_upload(kc_ctx* c, long long P, const double* lon, const double* lat, const double* z,
                         const int* status, const int* nn, const signed char* fr, const long long* pid,
                         const int* rs) {
@@ -690,23 +724,8 @@ int kc_particles_upload(kc_ctx* c, long long P, const double* lon, const double*
     if (P < 0 || (P > 0 && (!lon || !lat || !status || !nn)))
         return fail(c, KC_ERR_ARG, "kc_particles_upload: missing array");
     KC_CUDA(c, cudaSetDevice(c->device));
-    if (P > c->cap) {
-        KC_CUDA(c, cudaStreamSynchronize(c->stream));
-        free_particles(c);
-        // every per-particle buffer holds 8 bytes per particle, so the re-sort
-        // can gather any array into the spare buffer and swap the pointers
-        size_t n = (size_t)P * 8;
-        KC_CUDA(c, cudaMalloc((void**)&c->lon, n)); KC_CUDA(c, cudaMalloc((void**)&c->lat, n));
-        KC_CUDA(c, cudaMalloc((void**)&c->z, n)); KC_CUDA(c, cudaMalloc((void**)&c->U, n));
-        KC_CUDA(c, cudaMalloc((void**)&c->V, n)); KC_CUDA(c, cudaMalloc((void**)&c->W, n));
-        KC_CUDA(c, cudaMalloc((void**)&c->status, n)); KC_CUDA(c, cudaMalloc((void**)&c->nn, n));
-        KC_CUDA(c, cudaMalloc((void**)&c->fr, n)); KC_CUDA(c, cudaMalloc((void**)&c->pid, n));
-        KC_CUDA(c, cudaMalloc((void**)&c->rs, n)); KC_CUDA(c, cudaMalloc((void**)&c->orig, n));
-        KC_CUDA(c, cudaMalloc((void**)&c->spare, n));
-        KC_CUDA(c, cudaMalloc((void**)&c->prev, n)); KC_CUDA(c, cudaMalloc((void**)&c->wet, n));
-        KC_CUDA(c, cudaMalloc((void**)&c->nn_ok, n));
-        c->cap = P;
-    }
+    int rc0 = ensure_capacity(c, P);
+    if (rc0) return rc0;
     c->P = P;
     c->sorted = false;
     c->has_beach = false;   // the beaching state belongs to the particles it was uploaded with
@@ -806,6 +825,92 @@ int kc_sort(kc_ctx* c) {
         if ((rc = regather(c, (void**)&c->wet, 4, idx))) return rc;
     }
     c->sorted = true;
+    return KC_OK;
+}
+
+int kc_step_host(kc_ctx* c, const kc_step_args* a, long long P, const kc_host_particles* in,
+                 const kc_host_particles* out, long long chunk) {
+    if (!c || !in || !out) return KC_ERR_ARG;
+    if (P < 0) return fail(c, KC_ERR_ARG, "kc_step_host: P < 0");
+    if (P > 0 && (!in->lon || !in->lat || !in->status || !in->nearest_node || !out->lon || !out->lat ||
+                  !out->status || !out->nearest_node))
+        return fail(c, KC_ERR_ARG, "kc_step_host: lon, lat, status and nearest_node are required in and out");
+    KC_CUDA(c, cudaSetDevice(c->device));
+    int rc = ensure_capacity(c, P);
+    if (rc) return rc;
+    c->P = P;
+    c->sorted = false;
+    c->has_pid = false;
+    c->has_rs = false;
+    c->has_beach = false;
+    if ((rc = check_step(c, a))) return rc;
+    if (P == 0) return KC_OK;
+    if (!c->s_in) {
+        KC_CUDA(c, cudaStreamCreateWithFlags(&c->s_in, cudaStreamNonBlocking));
+        KC_CUDA(c, cudaStreamCreateWithFlags(&c->s_out, cudaStreamNonBlocking));
+        for (int k = 0; k < kChunks; ++k) {
+            KC_CUDA(c, cudaEventCreateWithFlags(&c->ev_in[k], cudaEventDisableTiming));
+            KC_CUDA(c, cudaEventCreateWithFlags(&c->ev_k[k], cudaEventDisableTiming));
+        }
+        KC_CUDA(c, cudaEventCreateWithFlags(&c->ev_start, cudaEventDisableTiming));
+    }
+    // chunk: a multiple of the block size, at most kChunks chunks
+    long long ch = chunk > 0 ? chunk : (P + 7) / 8;
+    ch = std::max(ch, (P + kChunks - 1) / kChunks);
+    ch = std::max<long long>(kBlock, (ch + kBlock - 1) / kBlock * kBlock);
+    const int nch = (int)((P + ch - 1) / ch);
+    // the copies start after everything queued on the library's stream
+    KC_CUDA(c, cudaEventRecord(c->ev_start, c->stream));
+    KC_CUDA(c, cudaStreamWaitEvent(c->s_in, c->ev_start, 0));
+    const kc::DState full = state_of(c);
+    const kc::DStep s0 = step_of(a);
+    for (int k = 0; k < nch; ++k) {
+        const long long b = (long long)k * ch, n = std::min(ch, P - b);
+        cudaStream_t si = c->s_in;
+        KC_CUDA(c, cudaMemcpyAsync(c->lon + b, in->lon + b, n * 8, cudaMemcpyHostToDevice, si));
+        KC_CUDA(c, cudaMemcpyAsync(c->lat + b, in->lat + b, n * 8, cudaMemcpyHostToDevice, si));
+        if (in->z) KC_CUDA(c, cudaMemcpyAsync(c->z + b, in->z + b, n * 8, cudaMemcpyHostToDevice, si));
+        else KC_CUDA(c, cudaMemsetAsync(c->z + b, 0, n * 8, si));
+        KC_CUDA(c, cudaMemcpyAsync(c->status + b, in->status + b, n * 4, cudaMemcpyHostToDevice, si));
+        KC_CUDA(c, cudaMemcpyAsync(c->nn + b, in->nearest_node + b, n * 4, cudaMemcpyHostToDevice, si));
+        if (in->failure_reason)
+            KC_CUDA(c, cudaMemcpyAsync(c->fr + b, in->failure_reason + b, n, cudaMemcpyHostToDevice, si));
+        else KC_CUDA(c, cudaMemsetAsync(c->fr + b, 0, n, si));
+        KC_CUDA(c, cudaEventRecord(c->ev_in[k], si));
+        // the chunk's particles as a state of their own: RNG keys stay the
+        // global index (pid_offset + base + local index); carried anchors are
+        // not trusted (nn_ok null), as for any upload
+        kc::DState st = full;
+        st.lon += b; st.lat += b; st.z += b; st.status += b; st.nn += b;
+        st.U += b; st.V += b; st.W += b; st.fr += b;
+        st.pid = nullptr; st.release_step = nullptr; st.prev = nullptr; st.nn_ok = nullptr;
+        st.P = n;
+        kc::DStep sk = s0;
+        sk.pid_offset = s0.pid_offset + (unsigned long long)b;
+        KC_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_in[k], 0));
+        if ((rc = launch_step_on(c, a, st, sk))) return rc;
+        KC_CUDA(c, cudaEventRecord(c->ev_k[k], c->stream));
+    }
+    // downloads after every upload and step is queued: a copy into pageable
+    // memory returns only when done, and must not hold back the queueing
+    for (int k = 0; k < nch; ++k) {
+        const long long b = (long long)k * ch, n = std::min(ch, P - b);
+        cudaStream_t so = c->s_out;
+        KC_CUDA(c, cudaStreamWaitEvent(so, c->ev_k[k], 0));
+        KC_CUDA(c, cudaMemcpyAsync(out->lon + b, c->lon + b, n * 8, cudaMemcpyDeviceToHost, so));
+        KC_CUDA(c, cudaMemcpyAsync(out->lat + b, c->lat + b, n * 8, cudaMemcpyDeviceToHost, so));
+        if (out->z) KC_CUDA(c, cudaMemcpyAsync(out->z + b, c->z + b, n * 8, cudaMemcpyDeviceToHost, so));
+        KC_CUDA(c, cudaMemcpyAsync(out->status + b, c->status + b, n * 4, cudaMemcpyDeviceToHost, so));
+        KC_CUDA(c, cudaMemcpyAsync(out->nearest_node + b, c->nn + b, n * 4, cudaMemcpyDeviceToHost, so));
+        if (out->failure_reason)
+            KC_CUDA(c, cudaMemcpyAsync(out->failure_reason + b, c->fr + b, n, cudaMemcpyDeviceToHost, so));
+        if (out->u) KC_CUDA(c, cudaMemcpyAsync(out->u + b, c->U + b, n * 8, cudaMemcpyDeviceToHost, so));
+        if (out->v) KC_CUDA(c, cudaMemcpyAsync(out->v + b, c->V + b, n * 8, cudaMemcpyDeviceToHost, so));
+        if (out->w) KC_CUDA(c, cudaMemcpyAsync(out->w + b, c->W + b, n * 8, cudaMemcpyDeviceToHost, so));
+    }
+    KC_CUDA(c, cudaStreamSynchronize(c->s_out));
+    KC_CUDA(c, cudaMemsetAsync(c->nn_ok, 0, (size_t)P, c->stream));
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
     return KC_OK;
 }
 

@@ -259,6 +259,40 @@ class DeviceContext:
     def step(self, args: N.StepArgs) -> None:
         self._chk(N.lib().kc_step(self._ctx, C.byref(args)), "kc_step")
 
+    def step_host(self, args: N.StepArgs, inp: dict, out: dict, chunk: int = 0) -> None:
+        """One step of host-resident particles (kc_step_host): ``inp`` and
+        ``out`` map lon, lat, z, status, nearest_node, failure_reason (and in
+        ``out`` u, v, w) to C-contiguous arrays of the library's dtypes; absent
+        or None entries are not read / not written.  Page-locked arrays
+        (``pinned_empty``) let the copies overlap the step."""
+        types = {"lon": np.float64, "lat": np.float64, "z": np.float64, "status": np.int32,
+                 "nearest_node": np.int32, "failure_reason": np.int8, "u": np.float64, "v": np.float64,
+                 "w": np.float64}
+
+        def pack(d, names):
+            h = N.HostParticles()
+            P = None
+            for name in names:
+                a = d.get(name)
+                if a is None:
+                    continue
+                if a.dtype != types[name] or not a.flags.c_contiguous:
+                    raise ValueError(f"{name}: expected a C-contiguous {np.dtype(types[name])} array")
+                if P is None:
+                    P = a.shape[0]
+                elif a.shape[0] != P:
+                    raise ValueError("host particle arrays of different lengths")
+                setattr(h, name, a.ctypes.data)
+            return h, P
+
+        hi, P = pack(inp, ("lon", "lat", "z", "status", "nearest_node", "failure_reason"))
+        ho, P2 = pack(out, tuple(types))
+        if P is None or P2 != P:
+            raise ValueError("input and output particle counts differ")
+        self._chk(N.lib().kc_step_host(self._ctx, C.byref(args), P, C.byref(hi), C.byref(ho), int(chunk)),
+                  "kc_step_host")
+        self.P = P
+
     def run(self, steps) -> None:
         arr = (N.StepArgs * len(steps))(*steps)
         self._chk(N.lib().kc_run(self._ctx, arr, len(steps)), "kc_run")

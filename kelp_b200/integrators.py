@@ -198,17 +198,27 @@ def _run(state, vel, mesh, dt, time_dir, scheme, kw, ctx=None) -> ParticleState:
     a, is3d = prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx, kick=kick, elem=state.elem)
     ctx = ctx or default_context()
     fr_in = state.failure_reason
-    ctx.upload_particles(state.lon, state.lat, state.z, state.status, state.nearest_node,
-                         fr=fr_in)
-    ctx.step(a)
-    out = ctx.download_particles()
-    if ctx.device_errors():
-        raise N.KcError(N.KC_ERR_DEVICE, "a device-side search iteration cap was hit")
+    P = state.n_particles
+    inp = {"lon": np.ascontiguousarray(state.lon, dtype=np.float64),
+           "lat": np.ascontiguousarray(state.lat, dtype=np.float64),
+           "z": np.ascontiguousarray(state.z, dtype=np.float64) if is3d else None,
+           "status": np.ascontiguousarray(state.status, dtype=np.int32),
+           "nearest_node": np.ascontiguousarray(state.nearest_node, dtype=np.int32),
+           "failure_reason": None if fr_in is None else np.ascontiguousarray(fr_in, dtype=np.int8)}
+    out = {"lon": np.empty(P), "lat": np.empty(P), "z": np.empty(P) if is3d else None,
+           "status": np.empty(P, np.int32), "nearest_node": np.empty(P, np.int32),
+           "failure_reason": None if fr_in is None else np.empty(P, np.int8),
+           "u": np.empty(P), "v": np.empty(P), "w": np.empty(P) if is3d else None}
+    # one call: chunked upload, step and download overlapped on the device
+    ctx.step_host(a, inp, out)
+    err = ctx.device_errors()
+    if err:
+        raise N.KcError(N.KC_ERR_DEVICE, N.describe_device_errors(err))
     return state.replace(
         lon=out["lon"], lat=out["lat"], z=out["z"] if is3d else np.array(state.z, copy=True),
         status=out["status"], nearest_node=out["nearest_node"],
-        u=out["u"], v=out["v"], w=out["w"] if is3d else None,
-        failure_reason=None if fr_in is None else out["failure_reason"],
+        u=out["u"], v=out["v"], w=out["w"],
+        failure_reason=out["failure_reason"],
     )
 
 

@@ -230,3 +230,15 @@ def release_uniform(mesh, P: int, seed: int = 3, *, depth_uniform: bool = False)
         dep = np.asarray(mesh.depth)[t[pick]].min(1)
         z = rng.uniform(size=P) * dep
     return plon, plat, z
+
+
+def sort_seeds(lon, lat, z, cell: float = 1.0):
+    """Seed order for memory locality, as KELP's utils/sort_seeds.py prepares
+    seed files before a run: a stable sort by lon/lat cell (``cell`` degrees,
+    rows south to north) with the depth as the secondary key.  Returns the
+    permuted (lon, lat, z)."""
+    nx = int(np.ceil(360.0 / cell))
+    key = (np.floor((np.asarray(lat) + 90.0) / cell).astype(np.int64) * nx
+           + np.floor((np.asarray(lon) + 180.0) / cell).astype(np.int64) % nx)
+    order = np.lexsort((np.asarray(z), key))
+    return np.asarray(lon)[order], np.asarray(lat)[order], np.asarray(z)[order]

@@ -79,13 +79,14 @@ def c1(P: int = 100_000, spacing: float = 0.5625) -> Workload:
     """2-D FESOM2-style: jittered (+-20 %) lon/lat lattice with a 30 % land mask
     (~127 k wet nodes, ~250 k triangles), u/v float32 on nodes (solid-body
     rotation + double gyre, 0.5 m/s), 2 snapshots 24 h apart cycled, 100 k
-    particles uniform over the wet area, RK2, dt 1 h, 240 steps, no diffusion."""
+    particles uniform over the wet area, RK2, dt 1 h, 240 steps, no diffusion.
+    Every workload's seeds are sorted by 1-degree cell (sort_seeds)."""
     m = S.lattice_mesh(spacing, 80.0, jitter=0.2, land_frac=0.3)
     snaps = S.gyre_snapshots(m, 2, amp=0.5)
-    lon, lat, z = S.release_uniform(m, P, seed=3)
+    lon, lat, z = S.sort_seeds(*S.release_uniform(m, P, seed=3))
     return Workload("c1_fesom2_2d_rk2", m, snaps, lon, lat, z, "rk2", 3600.0, 86400.0, 240,
                     description={"mesh": "jittered 0.5625 deg lattice, 30% land", "nodes": int(m.n_nodes),
-                                 "elements": int(m.n_elements), "particles": P, "scheme": "rk2",
+                                 "elements": int(m.n_elements), "particles": P, "seeds": "sorted by 1-degree cell", "scheme": "rk2",
                                  "dt_s": 3600, "steps_run": 240, "fields": "f32 node u,v, 2 snapshots 24 h"})
 
 
@@ -99,11 +100,11 @@ def c2(P: int = 1_000_000, spacing: float = 0.5625, n_levels: int = 47) -> Workl
     m = S.lattice_mesh(spacing, 80.0, jitter=0.2, land_frac=0.3,
                        depth=lambda lo, la: S.smooth_bathymetry(lo, la, 50.0, 6000.0), sigma=zl)
     snaps = S.gyre_snapshots(m, 4, amp=0.5, z_levels=zl, decay=1000.0, w_scale=1e-3, placement="level")
-    lon, lat, z = S.release_uniform(m, P, seed=3, depth_uniform=True)
+    lon, lat, z = S.sort_seeds(*S.release_uniform(m, P, seed=3, depth_uniform=True))
     return Workload("c2_fesom2_3d_dl_rk4", m, snaps, lon, lat, z, "rk4", 1800.0, 3.5 * 86400.0, 480,
                     dims=3, w_interp="nearest", uv_vertical="level",
                     description={"mesh": "jittered 0.5625 deg lattice, 30% land", "nodes": int(m.n_nodes),
-                                 "elements": int(m.n_elements), "levels": n_levels, "particles": P,
+                                 "elements": int(m.n_elements), "levels": n_levels, "particles": P, "seeds": "sorted by 1-degree cell",
                                  "scheme": "rk4", "dt_s": 1800, "steps_run": 480,
                                  "fields": "f32 node u,v,w (47,N) depth-linear (level), 4 snapshots 3.5 d",
                                  "w_interp": "nearest"})
@@ -126,11 +127,11 @@ def c3(P: int = 6_000_000, nside: int = 512, n_levels: int = 69, n_snap: int = 2
     depth = S.smooth_bathymetry(plon, plat, 50.0, 6000.0)
     m = H.dual_mesh(nside, wet, depth, sigma=zl)
     snaps = S.vortex_snapshots(m, n_snap, z_levels=zl)
-    lon, lat, z = S.release_uniform(m, P, seed=3, depth_uniform=True)
+    lon, lat, z = S.sort_seeds(*S.release_uniform(m, P, seed=3, depth_uniform=True))
     return Workload("c3_healpix512_3d_rk2_kick", m, snaps, lon, lat, z, "rk2", 21600.0, 86400.0, 1460,
                     dims=3, w_interp="barycentric", kh=(10.0, 10.0), seed=0,
                     description={"mesh": f"HEALPix nside {nside} dual mesh, ~70% wet", "nodes": int(m.n_nodes),
-                                 "elements": int(m.n_elements), "levels": n_levels, "particles": P,
+                                 "elements": int(m.n_elements), "levels": n_levels, "particles": P, "seeds": "sorted by 1-degree cell",
                                  "scheme": "rk2", "dt_s": 21600, "steps_run": 1460,
                                  "fields": "f32 node u,v (68,N), w (69,N), 256 Gaussian vortices 0.3 m/s rms",
                                  "diffusion": "split uniform Kh=10 m^2/s", "w_interp": "barycentric"})
