@@ -142,6 +142,14 @@ int kc_particles_download(kc_ctx* ctx, long long P, double* lon, double* lat, do
                           int* status, int* nearest_node, signed char* failure_reason,
                           double* u, double* v, double* w);
 
+/* Per-particle realization ids of the resident particles (NULL: every
+ * particle takes kc_step_args.real_id again).  With them, the members of a
+ * diffusion ensemble (tracking.py runs one realization per call of
+ * run_single_realization, keyed by realization_id) share one particle array
+ * and one launch: each particle's kick and beaching draws use its own id.
+ * kc_particles_upload clears them; call before kc_sort. */
+int kc_particles_set_realization(kc_ctx* ctx, const int* real_id);
+
 /* Coastal element flags (E bytes, 1 = owns a boundary edge;
  * src/kelp/core/mesh.py:2764-2821 build_boundary_info). */
 int kc_coastal_upload(kc_ctx* ctx, const unsigned char* elem_is_coastal);
@@ -187,6 +195,24 @@ int kc_step_host(kc_ctx* ctx, const kc_step_args* args, long long P, const kc_ho
  * per-step arguments, no host round trip in between. */
 int kc_step(kc_ctx* ctx, const kc_step_args* args);
 int kc_run(kc_ctx* ctx, const kc_step_args* steps, int n_steps);
+
+/* One step of the resident particles [begin, begin + count) only, RNG keys
+ * unchanged (a cohort of a larger array).  No reference counterpart: the
+ * reference steps one cohort's state per call of its step function. */
+int kc_step_range(kc_ctx* ctx, const kc_step_args* args, long long begin, long long count);
+
+/* n_steps steps of every resident particle in ONE kernel launch: each thread
+ * carries its particles through all the steps (particles are independent),
+ * with the beaching hook after every step when beach != NULL (n_steps
+ * argument blocks; kc_beach_state_upload first).  Same results as n_steps
+ * kc_step (+ kc_beach) calls.  Every step must share dims, scheme, form and
+ * snapshot element type.  With use_graph the launch is captured once as a
+ * CUDA graph (argument upload + kernel) and replayed while n_steps, the
+ * particle count, the mesh and the form stay the same; the per-step arguments
+ * are read from a device buffer, so each replay runs the steps passed to it.
+ * No reference counterpart (the reference launches one parallel loop per
+ * step and per realization). */
+int kc_run_fused(kc_ctx* ctx, const kc_step_args* steps, int n_steps, const kc_beach_args* beach, int use_graph);
 
 /* Re-order the resident particles by grid-hash cell (particles that left the
  * domain last) so that a warp's particles share hash windows and elements.

@@ -24,7 +24,8 @@ KC_EULER, KC_RK2, KC_RK4 = 0, 1, 2
 EXPORTS = ("kc_abi_version", "kc_node_xyz_fill", "kc_create", "kc_destroy", "kc_last_error",
            "kc_synchronize", "kc_mesh_upload", "kc_depth_points_upload", "kc_field_upload", "kc_particles_upload",
            "kc_particles_download", "kc_coastal_upload", "kc_beach_state_upload",
-           "kc_beach_state_download", "kc_beach", "kc_step", "kc_step_host", "kc_run", "kc_sort", "kc_find_nearest", "kc_find_nearest_noalloc", "kc_rng_normals", "kc_device_errors",
+           "kc_beach_state_download", "kc_beach", "kc_step", "kc_step_host", "kc_step_range", "kc_run_fused",
+           "kc_particles_set_realization", "kc_run", "kc_sort", "kc_find_nearest", "kc_find_nearest_noalloc", "kc_rng_normals", "kc_device_errors",
            "kc_event_record", "kc_event_elapsed", "kc_l2_flush", "kc_host_alloc", "kc_host_free")
 
 
@@ -118,6 +119,9 @@ def lib():
         L.kc_beach_state_download.argtypes = [vp, vp]
         L.kc_beach.argtypes = [vp, C.POINTER(BeachArgs)]
         L.kc_step.argtypes = [vp, C.POINTER(StepArgs)]
+        L.kc_step_range.argtypes = [vp, C.POINTER(StepArgs), ll, ll]
+        L.kc_run_fused.argtypes = [vp, C.POINTER(StepArgs), i, C.c_void_p, i]
+        L.kc_particles_set_realization.argtypes = [vp, vp]
         L.kc_step_host.argtypes = [vp, C.POINTER(StepArgs), ll, C.POINTER(HostParticles), C.POINTER(HostParticles),
                                    ll]
         L.kc_run.argtypes = [vp, C.POINTER(StepArgs), i]

@@ -7,6 +7,7 @@
 #include <vector>
 #include <algorithm>
 #include <mutex>
+#include <type_traits>
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
 #include <cub/device/device_radix_sort.cuh>
@@ -69,7 +70,8 @@ struct kc_ctx {
     int *status = nullptr, *nn = nullptr, *rs = nullptr;
     signed char* fr = nullptr;
     long long* pid = nullptr;
-    bool has_pid = false, has_rs = false;
+    bool has_pid = false, has_rs = false, has_rid = false;
+    int* rid = nullptr;   // per-particle realization ids (ensemble members in one array)
     // re-sort by grid-hash cell: upload slot of every resident particle, the
     // spare buffer of the gathers, radix-sort keys / indices and CUB's storage
     long long* orig = nullptr;
@@ -98,6 +100,16 @@ struct kc_ctx {
     cudaEvent_t ev_in[kChunks] = {}, ev_k[kChunks] = {}, ev_start = nullptr;
     // L2 eviction buffer of kc_l2_flush
     char* flush = nullptr;
+    // fused multi-step launches: per-call argument block (page-locked staging
+    // and its device copy), the event after its upload, the cached graph
+    void* fused_host = nullptr;
+    void* fused_dev = nullptr;
+    size_t fused_cap = 0;
+    cudaEvent_t fused_ev = nullptr;
+    bool fused_ev_pending = false;
+    cudaGraphExec_t fused_exec = nullptr;
+    std::string fused_key;
+    unsigned long long mesh_gen = 0;
     // float staging buffer of the half-precision snapshot conversion
     float* stage = nullptr;
     size_t stage_cap = 0;
@@ -136,6 +148,7 @@ kc::DState state_of(kc_ctx* c) {
     st.U = c->U; st.V = c->V; st.W = c->W; st.fr = c->fr;
     st.pid = c->has_pid ? c->pid : nullptr;
     st.release_step = c->has_rs ? c->rs : nullptr;
+    st.rid = c->has_rid ? c->rid : nullptr;
     st.prev = c->has_beach ? c->prev : nullptr;
     st.nn_ok = c->nn_ok;
     st.P = c->P;
@@ -295,6 +308,10 @@ kc::DBlend<T> blend_of(kc_ctx* c, const kc_step_args* a) {
 // the mixed-form kernels (kc_mixed.cu)
 void kc_launch_mixed_f32(const kc::DMesh& m, const kc::DBlend<float>& f, const kc::DState& st, const kc::DStep& s,
                          int dims, int scheme, cudaStream_t stream);
+void kc_launch_multi_mixed_f32(const kc::DMesh& m, const MultiHead* head, const StepPack<float>* packs, long long P,
+                               int dims, int scheme, cudaStream_t stream);
+void kc_launch_multi_mixed_f16(const kc::DMesh& m, const MultiHead* head, const StepPack<__half>* packs, long long P,
+                               int dims, int scheme, cudaStream_t stream);
 void kc_launch_mixed_f16(const kc::DMesh& m, const kc::DBlend<__half>& f, const kc::DState& st,
                          const kc::DStep& s, int dims, int scheme, cudaStream_t stream);
 
@@ -389,7 +406,7 @@ void free_mesh(kc_ctx* c) {
 
 void free_particles(kc_ctx* c) {
     dfree(c->lon); dfree(c->lat); dfree(c->z); dfree(c->U); dfree(c->V); dfree(c->W);
-    dfree(c->status); dfree(c->nn); dfree(c->fr); dfree(c->pid); dfree(c->rs);
+    dfree(c->status); dfree(c->nn); dfree(c->fr); dfree(c->pid); dfree(c->rs); dfree(c->rid);
     dfree(c->orig); dfree(c->spare); dfree(c->prev); dfree(c->wet); dfree(c->nn_ok);
     c->has_beach = false;
     dfree(c->skey[0]); dfree(c->skey[1]); dfree(c->sidx[0]); dfree(c->sidx[1]); dfree(c->cub_tmp);
@@ -436,6 +453,10 @@ void kc_destroy(kc_ctx* c) {
         if (c->ev_k[k]) cudaEventDestroy(c->ev_k[k]);
     }
     if (c->ev_start) cudaEventDestroy(c->ev_start);
+    if (c->fused_exec) cudaGraphExecDestroy(c->fused_exec);
+    if (c->fused_ev) cudaEventDestroy(c->fused_ev);
+    if (c->fused_host) cudaFreeHost(c->fused_host);
+    dfree(c->fused_dev);
     if (c->s_in) { cudaStreamSynchronize(c->s_in); cudaStreamDestroy(c->s_in); }
     if (c->s_out) { cudaStreamSynchronize(c->s_out); cudaStreamDestroy(c->s_out); }
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -537,6 +558,7 @@ int kc_mesh_upload(kc_ctx* c, const kc_mesh_desc* d) {
     m.err = c->d_err;
     c->N = N; c->E = E;
     c->has_mesh = true;
+    ++c->mesh_gen;
     return KC_OK;
 }
 
@@ -549,6 +571,17 @@ int kc_coastal_upload(kc_ctx* c, const unsigned char* flags) {
     int rc = upload(c, &c->d_coastal, flags, (size_t)c->E);
     if (rc) return rc;
     KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KC_OK;
+}
+
+int kc_particles_set_realization(kc_ctx* c, const int* real_id) {
+    if (!c) return KC_ERR_ARG;
+    if (c->sorted) return fail(c, KC_ERR_STATE, "kc_particles_set_realization: set the realizations before kc_sort");
+    KC_CUDA(c, cudaSetDevice(c->device));
+    c->has_rid = false;
+    if (!real_id || c->P == 0) return KC_OK;
+    KC_CUDA(c, cudaMemcpyAsync(c->rid, real_id, (size_t)c->P * 4, cudaMemcpyHostToDevice, c->stream));
+    c->has_rid = true;
     return KC_OK;
 }
 
@@ -578,17 +611,15 @@ int kc_beach_state_download(kc_ctx* c, int* wet_streak) {
     return KC_OK;
 }
 
-int kc_beach(kc_ctx* c, const kc_beach_args* a) {
-    if (!c || !a) return KC_ERR_ARG;
+// Validate one hook call's arguments against the context and build the
+// device-side argument block.
+static int beach_of(kc_ctx* c, const kc_beach_args* a, kc::DBeach& b) {
     if (!c->has_mesh) return fail(c, KC_ERR_STATE, "kc_beach: no mesh uploaded");
     if (!c->has_beach) return fail(c, KC_ERR_STATE, "kc_beach: call kc_beach_state_upload first");
     if (!c->d_depth) return fail(c, KC_ERR_STATE, "kc_beach: the mesh has no depth");
     if (a->resuspension < 0 || a->resuspension > 3) return fail(c, KC_ERR_ARG, "kc_beach: resuspension code");
     const bool need_topo = a->use_coastal || a->use_stochastic;
     if (need_topo && !c->d_coastal) return fail(c, KC_ERR_STATE, "kc_beach: coastal flags not uploaded");
-    if (c->P == 0) return KC_OK;
-    KC_CUDA(c, cudaSetDevice(c->device));
-    kc::DBeach b;
     b.use_depth = a->use_depth; b.use_coastal = a->use_coastal; b.use_stochastic = a->use_stochastic;
     b.on_failure = a->on_failure; b.need_topo = need_topo ? 1 : 0; b.resuspension = a->resuspension;
     b.min_wet_steps = a->min_wet_steps;
@@ -599,10 +630,27 @@ int kc_beach(kc_ctx* c, const kc_beach_args* a) {
     b.coastal = need_topo ? c->d_coastal : nullptr;
     b.prev = c->prev;
     b.wet_streak = c->wet;
-    if (!c->has_pid) {   // the RNG key stays the slot index the particles were uploaded with
+    return KC_OK;
+}
+
+// The RNG key of every resident particle stays the slot index it was uploaded
+// with, whatever the order the re-sort leaves them in.
+static int pin_pid(kc_ctx* c) {
+    if (!c->has_pid && c->P > 0) {
         KC_CUDA(c, cudaMemcpyAsync(c->pid, c->orig, (size_t)c->P * 8, cudaMemcpyDeviceToDevice, c->stream));
         c->has_pid = true;
     }
+    return KC_OK;
+}
+
+int kc_beach(kc_ctx* c, const kc_beach_args* a) {
+    if (!c || !a) return KC_ERR_ARG;
+    kc::DBeach b;
+    int rc = beach_of(c, a, b);
+    if (rc) return rc;
+    if (c->P == 0) return KC_OK;
+    KC_CUDA(c, cudaSetDevice(c->device));
+    if ((rc = pin_pid(c))) return rc;
     kc::DState st = state_of(c);
     k_beach<<<grid_for(c->P), kBlock, 0, c->stream>>>(c->dm, st, b, c->N);
     KC_CUDA(c, cudaGetLastError());
@@ -710,6 +758,7 @@ static int ensure_capacity(kc_ctx* c, long long P) {
     KC_CUDA(c, cudaMalloc((void**)&c->status, n)); KC_CUDA(c, cudaMalloc((void**)&c->nn, n));
     KC_CUDA(c, cudaMalloc((void**)&c->fr, n)); KC_CUDA(c, cudaMalloc((void**)&c->pid, n));
     KC_CUDA(c, cudaMalloc((void**)&c->rs, n)); KC_CUDA(c, cudaMalloc((void**)&c->orig, n));
+    KC_CUDA(c, cudaMalloc((void**)&c->rid, n));
     KC_CUDA(c, cudaMalloc((void**)&c->spare, n));
     KC_CUDA(c, cudaMalloc((void**)&c->prev, n)); KC_CUDA(c, cudaMalloc((void**)&c->wet, n));
     KC_CUDA(c, cudaMalloc((void**)&c->nn_ok, n));
@@ -746,6 +795,7 @@ int kc_particles_upload(kc_ctx* c, long long P, const double* lon, const double*
     if (pid) KC_CUDA(c, cudaMemcpyAsync(c->pid, pid, n * 8, cudaMemcpyHostToDevice, s));
     c->has_rs = rs != nullptr;
     if (rs) KC_CUDA(c, cudaMemcpyAsync(c->rs, rs, n * 4, cudaMemcpyHostToDevice, s));
+    c->has_rid = false;
     KC_CUDA(c, cudaMemsetAsync(c->nn_ok, 0, n, s));   // uploaded anchors are not trusted
     KC_CUDA(c, cudaMemsetAsync(c->U, 0, n * 8, s));
     KC_CUDA(c, cudaMemsetAsync(c->V, 0, n * 8, s));
@@ -820,6 +870,7 @@ int kc_sort(kc_ctx* c) {
     if ((rc = regather(c, (void**)&c->fr, 1, idx))) return rc;
     if ((rc = regather(c, (void**)&c->nn_ok, 1, idx))) return rc;
     if (c->has_rs && (rc = regather(c, (void**)&c->rs, 4, idx))) return rc;
+    if (c->has_rid && (rc = regather(c, (void**)&c->rid, 4, idx))) return rc;
     if (c->has_beach) {
         if ((rc = regather(c, (void**)&c->prev, 4, idx))) return rc;
         if ((rc = regather(c, (void**)&c->wet, 4, idx))) return rc;
@@ -842,6 +893,7 @@ int kc_step_host(kc_ctx* c, const kc_step_args* a, long long P, const kc_host_pa
     c->sorted = false;
     c->has_pid = false;
     c->has_rs = false;
+    c->has_rid = false;
     c->has_beach = false;
     if ((rc = check_step(c, a))) return rc;
     if (P == 0) return KC_OK;
@@ -883,7 +935,7 @@ int kc_step_host(kc_ctx* c, const kc_step_args* a, long long P, const kc_host_pa
         kc::DState st = full;
         st.lon += b; st.lat += b; st.z += b; st.status += b; st.nn += b;
         st.U += b; st.V += b; st.W += b; st.fr += b;
-        st.pid = nullptr; st.release_step = nullptr; st.prev = nullptr; st.nn_ok = nullptr;
+        st.pid = nullptr; st.release_step = nullptr; st.prev = nullptr; st.nn_ok = nullptr; st.rid = nullptr;
         st.P = n;
         kc::DStep sk = s0;
         sk.pid_offset = s0.pid_offset + (unsigned long long)b;
@@ -912,6 +964,156 @@ int kc_step_host(kc_ctx* c, const kc_step_args* a, long long P, const kc_host_pa
     KC_CUDA(c, cudaMemsetAsync(c->nn_ok, 0, (size_t)P, c->stream));
     KC_CUDA(c, cudaStreamSynchronize(c->stream));
     return KC_OK;
+}
+
+// A particle state view of [begin, begin + count) of st.
+static kc::DState state_range(kc::DState st, long long begin, long long count) {
+    st.lon += begin; st.lat += begin; st.z += begin; st.status += begin; st.nn += begin;
+    st.U += begin; st.V += begin; st.W += begin; st.fr += begin;
+    if (st.pid) st.pid += begin;
+    if (st.rid) st.rid += begin;
+    if (st.release_step) st.release_step += begin;
+    if (st.prev) st.prev += begin;
+    if (st.nn_ok) st.nn_ok += begin;
+    st.P = count;
+    return st;
+}
+
+int kc_step_range(kc_ctx* c, const kc_step_args* a, long long begin, long long count) {
+    if (!c) return KC_ERR_ARG;
+    int rc = check_step(c, a);
+    if (rc) return rc;
+    if (begin < 0 || count < 0 || begin + count > c->P)
+        return fail(c, KC_ERR_ARG, "kc_step_range: range outside the resident particles");
+    if (count == 0) return KC_OK;
+    KC_CUDA(c, cudaSetDevice(c->device));
+    const kc::DState st = state_range(state_of(c), begin, count);
+    kc::DStep s = step_of(a);
+    if (!st.pid) s.pid_offset += (unsigned long long)begin;   // keys stay the global index
+    return launch_step_on(c, a, st, s);
+}
+
+extern "C++" {
+template <typename T>
+static void launch_multi(kc_ctx* c, int precision, int dtype, const MultiHead* dh, const void* dp, int dims,
+                         int scheme) {
+    if (precision == KC_MIXED) {
+        if (dtype == KC_F16)
+            kc_launch_multi_mixed_f16(c->dm, dh, (const StepPack<__half>*)dp, c->P, dims, scheme, c->stream);
+        else
+            kc_launch_multi_mixed_f32(c->dm, dh, (const StepPack<float>*)dp, c->P, dims, scheme, c->stream);
+    } else if constexpr (!std::is_same<T, __half>::value) {   // the plain form never reads half storage
+        launch_multi_kernel<T, kc::PlainForm<T>>(c->dm, dh, (const StepPack<T>*)dp, c->P, dims, scheme, c->stream);
+    }
+}
+
+template <typename T>
+static int run_fused_t(kc_ctx* c, const kc_step_args* steps, int n, const kc_beach_args* beach, int use_graph) {
+    const size_t head_bytes = (sizeof(MultiHead) + 255) / 256 * 256;
+    const size_t bytes = head_bytes + sizeof(StepPack<T>) * (size_t)n;
+    if (c->fused_ev_pending) {   // the previous call's upload has read the staging buffer
+        KC_CUDA(c, cudaEventSynchronize(c->fused_ev));
+        c->fused_ev_pending = false;
+    }
+    if (c->fused_cap < bytes) {
+        KC_CUDA(c, cudaStreamSynchronize(c->stream));
+        if (c->fused_exec) cudaGraphExecDestroy(c->fused_exec);
+        c->fused_exec = nullptr;
+        c->fused_key.clear();
+        if (c->fused_host) cudaFreeHost(c->fused_host);
+        c->fused_host = nullptr;
+        dfree(c->fused_dev);
+        c->fused_cap = 0;
+        KC_CUDA(c, cudaHostAlloc(&c->fused_host, bytes, cudaHostAllocDefault));
+        KC_CUDA(c, cudaMalloc(&c->fused_dev, bytes));
+        c->fused_cap = bytes;
+    }
+    if (!c->fused_ev) KC_CUDA(c, cudaEventCreateWithFlags(&c->fused_ev, cudaEventDisableTiming));
+    MultiHead* h = (MultiHead*)c->fused_host;
+    h->st = state_of(c);
+    h->N = c->N;
+    h->n_steps = n;
+    StepPack<T>* pk = (StepPack<T>*)((char*)c->fused_host + head_bytes);
+    for (int j = 0; j < n; ++j) {
+        std::memset((void*)&pk[j], 0, sizeof(StepPack<T>));
+        pk[j].f = blend_of<T>(c, &steps[j]);
+        pk[j].s = step_of(&steps[j]);
+        pk[j].beach = beach ? 1 : 0;
+        if (beach) {
+            int rc = beach_of(c, &beach[j], pk[j].b);
+            if (rc) return rc;
+        }
+    }
+    const MultiHead* dh = (const MultiHead*)c->fused_dev;
+    const void* dp = (const char*)c->fused_dev + head_bytes;
+    const int precision = steps[0].precision, dtype = c->slots[steps[0].slot_a].dtype;
+    const int dims = steps[0].dims, scheme = steps[0].scheme;
+    if (!use_graph) {
+        KC_CUDA(c, cudaMemcpyAsync(c->fused_dev, c->fused_host, bytes, cudaMemcpyHostToDevice, c->stream));
+        launch_multi<T>(c, precision, dtype, dh, dp, dims, scheme);
+        KC_CUDA(c, cudaGetLastError());
+    } else {
+        const std::string key = std::to_string(precision) + "/" + std::to_string(dtype) + "/" + std::to_string(dims) +
+                                "/" + std::to_string(scheme) + "/" + std::to_string(n) + "/" +
+                                std::to_string(bytes) + "/" + std::to_string(c->P) + "/" +
+                                std::to_string(c->mesh_gen) + "/" + std::to_string((size_t)c->fused_dev) + "/" +
+                                std::to_string((size_t)c->fused_host);
+        if (key != c->fused_key || !c->fused_exec) {
+            if (c->fused_exec) cudaGraphExecDestroy(c->fused_exec);
+            c->fused_exec = nullptr;
+            c->fused_key.clear();
+            // the graph: upload the argument block from the staging buffer,
+            // then the fused kernel; replays copy whatever the staging holds
+            cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) return fail(c, KC_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+            cudaError_t e1 = cudaMemcpyAsync(c->fused_dev, c->fused_host, bytes, cudaMemcpyHostToDevice, c->stream);
+            if (e1 == cudaSuccess) {
+                launch_multi<T>(c, precision, dtype, dh, dp, dims, scheme);
+                e1 = cudaGetLastError();
+            }
+            cudaGraph_t g = nullptr;
+            cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+            if (e1 != cudaSuccess || e2 != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                return fail(c, KC_ERR_CUDA, std::string("graph capture: ") +
+                                                cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+            }
+            e = cudaGraphInstantiate(&c->fused_exec, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                c->fused_exec = nullptr;
+                return fail(c, KC_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+            }
+            c->fused_key = key;
+        }
+        KC_CUDA(c, cudaGraphLaunch(c->fused_exec, c->stream));
+    }
+    KC_CUDA(c, cudaEventRecord(c->fused_ev, c->stream));
+    c->fused_ev_pending = true;
+    return KC_OK;
+}
+
+}  // extern "C++"
+
+int kc_run_fused(kc_ctx* c, const kc_step_args* steps, int n_steps, const kc_beach_args* beach, int use_graph) {
+    if (!c || !steps) return KC_ERR_ARG;
+    if (n_steps < 1 || n_steps > 1024) return fail(c, KC_ERR_ARG, "kc_run_fused: n_steps must be in 1..1024");
+    int rc;
+    for (int j = 0; j < n_steps; ++j) {
+        if ((rc = check_step(c, &steps[j]))) return rc;
+        const kc_step_args& a = steps[j];
+        const kc_step_args& a0 = steps[0];
+        if (a.dims != a0.dims || a.scheme != a0.scheme || a.precision != a0.precision ||
+            c->slots[a.slot_a].dtype != c->slots[a0.slot_a].dtype)
+            return fail(c, KC_ERR_ARG, "kc_run_fused: every step needs the same dims, scheme, form and snapshot type");
+    }
+    if (c->P == 0) return KC_OK;
+    KC_CUDA(c, cudaSetDevice(c->device));
+    if ((rc = pin_pid(c))) return rc;
+    const int dtype = c->slots[steps[0].slot_a].dtype;
+    if (dtype == KC_F64) return run_fused_t<double>(c, steps, n_steps, beach, use_graph);
+    if (dtype == KC_F16) return run_fused_t<__half>(c, steps, n_steps, beach, use_graph);
+    return run_fused_t<float>(c, steps, n_steps, beach, use_graph);
 }
 
 int kc_step(kc_ctx* c, const kc_step_args* a) {

@@ -57,6 +57,7 @@ __device__ __forceinline__ void beach_particle(const DMesh& m, const DState& st,
     const bool coastal_contact = contained >= 0 && b.coastal && b.coastal[contained];
     const long long pid = st.pid ? st.pid[i] : i;
     const unsigned long long key = (unsigned long long)pid + b.pid_offset;
+    const unsigned long long rid = st.rid ? (unsigned long long)st.rid[i] : b.real_id;
     // 1. on_failure context-gated remap (tracking.py:279-307)
     if (b.on_failure && newly) {
         bool context = h_raw < b.zone_depth;
@@ -74,7 +75,7 @@ __device__ __forceinline__ void beach_particle(const DMesh& m, const DState& st,
     if (b.use_stochastic && alive) {
         bool in_zone = h_raw < b.zone_depth;
         if (b.need_topo && b.coastal) in_zone = in_zone || coastal_contact;
-        if (in_zone && u01(b.seed, b.real_id, key, b.step_i, COMP_BEACH) < b.p_beach) to_beach = true;
+        if (in_zone && u01(b.seed, rid, key, b.step_i, COMP_BEACH) < b.p_beach) to_beach = true;
     }
     to_beach = to_beach && alive;
     // resuspension (beaching.py:142-178)
@@ -86,7 +87,7 @@ __device__ __forceinline__ void beach_particle(const DMesh& m, const DState& st,
         if (b.resuspension == RESUSP_AUTO || b.resuspension == RESUSP_BOTH)
             to_release = to_release || ws >= b.min_wet_steps;
         if ((b.resuspension == RESUSP_STOCH || b.resuspension == RESUSP_BOTH) && rewet &&
-            u01(b.seed, b.real_id, key, b.step_i, COMP_RESUSP) < b.p_resusp)
+            u01(b.seed, rid, key, b.step_i, COMP_RESUSP) < b.p_resusp)
             to_release = true;
     }
     if (to_release) ws = 0;

@@ -1,7 +1,7 @@
 // Launch shape and the step kernels of both numerical forms (one thread per
 // particle), shared by the translation units that instantiate them.
 #pragma once
-#include "kc_step.cuh"
+#include "kc_beach.cuh"
 
 #ifndef KC_BLOCK
 #define KC_BLOCK 128   // threads per block of every kernel (a build option)
@@ -65,5 +65,85 @@ void launch_step_kernel(const kc::DMesh& m, const kc::DBlend<T>& f, const kc::DS
         if (scheme == 1) k_step3d_rk2<T, Form><<<g, kBlock, 0, stream>>>(m, f, st, s);
         else if (scheme == 2) k_step3d_unfused<T, 2, Form><<<g, kBlock, 0, stream>>>(m, f, st, s);
         else k_step3d_unfused<T, 0, Form><<<g, kBlock, 0, stream>>>(m, f, st, s);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fused multi-step launch: each thread carries its particles through n steps
+// (particles are independent within and across steps), running the beaching
+// hook after a step where asked.  Everything that changes between calls is
+// read from device memory: the state view (kc_sort swaps its buffers) and,
+// per step, the snapshot blend, the step arguments and the beaching
+// arguments.  So one launch can be captured in a CUDA graph and replayed with
+// the next steps' arguments copied into the same device buffer.
+// ---------------------------------------------------------------------------
+
+template <typename T>
+struct StepPack {
+    kc::DBlend<T> f;
+    kc::DStep s;
+    kc::DBeach b;
+    int beach;   // run the beaching hook after this step
+};
+
+struct MultiHead {
+    kc::DState st;
+    long long N;   // mesh nodes (the beaching anchor wrap)
+    int n_steps;
+};
+
+template <typename T, int DIMS, int SCHEME, typename Form>
+__global__ void __launch_bounds__(kBlock, KC_STEP_MIN_BLOCKS) k_multi(const __grid_constant__ kc::DMesh m,
+                                                                     const MultiHead* __restrict__ head,
+                                                                     const StepPack<T>* __restrict__ packs) {
+    const kc::DState& st = head->st;
+    const long long P = st.P;
+    const long long N = head->N;
+    const int n = head->n_steps;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < P;
+         i += (long long)gridDim.x * blockDim.x) {
+        for (int j = 0; j < n; ++j) {
+            const StepPack<T>& pk = packs[j];
+            activate(st, pk.s, i);
+            if (st.prev) st.prev[i] = st.status[i];
+            if (DIMS == 2) kc::step2d_particle<T, SCHEME, Form>(m, pk.f, st, pk.s, i);
+            else if (SCHEME == 1) kc::step3d_rk2_particle<T, Form>(m, pk.f, st, pk.s, i);
+            else kc::step3d_unfused_particle<T, SCHEME, Form>(m, pk.f, st, pk.s, i);
+            if (pk.beach) kc::beach_particle(m, st, pk.b, N, i);
+        }
+    }
+}
+
+// Persistent grid: every SM's resident blocks, no more than the particles need.
+template <typename K>
+unsigned persistent_grid(K kernel, long long P) {
+    int dev = 0, sms = 1, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, 0);
+    if (per_sm < 1) per_sm = 1;
+    const long long need = (P + kBlock - 1) / kBlock;
+    const long long cap = (long long)sms * per_sm;
+    return (unsigned)(need < cap ? (need > 0 ? need : 1) : cap);
+}
+
+template <typename T, typename Form, int DIMS, int SCHEME>
+void launch_multi_one(const kc::DMesh& m, const MultiHead* head, const StepPack<T>* packs, long long P,
+                      cudaStream_t stream) {
+    auto kern = k_multi<T, DIMS, SCHEME, Form>;
+    kern<<<persistent_grid(kern, P), kBlock, 0, stream>>>(m, head, packs);
+}
+
+template <typename T, typename Form>
+void launch_multi_kernel(const kc::DMesh& m, const MultiHead* head, const StepPack<T>* packs, long long P, int dims,
+                         int scheme, cudaStream_t stream) {
+    if (dims == 2) {
+        if (scheme == 0) launch_multi_one<T, Form, 2, 0>(m, head, packs, P, stream);
+        else if (scheme == 1) launch_multi_one<T, Form, 2, 1>(m, head, packs, P, stream);
+        else launch_multi_one<T, Form, 2, 2>(m, head, packs, P, stream);
+    } else {
+        if (scheme == 1) launch_multi_one<T, Form, 3, 1>(m, head, packs, P, stream);
+        else if (scheme == 2) launch_multi_one<T, Form, 3, 2>(m, head, packs, P, stream);
+        else launch_multi_one<T, Form, 3, 0>(m, head, packs, P, stream);
     }
 }

@@ -23,6 +23,7 @@ struct DState {
     double* W;
     signed char* fr;
     const long long* pid;      // stable particle id (RNG key), index when null
+    const int* rid;            // per-particle realization (RNG key), the step's real_id when null
     const int* release_step;   // delayed release (null: all released)
     int* prev;                 // status at the step's entry, for the beaching hook (null: not kept)
     unsigned char* nn_ok;      // 1: nn is the exact anchor of the current position (null: never trusted)
@@ -72,16 +73,23 @@ __device__ __forceinline__ void mark_anchor(const DState& st, long long i, int s
     if (st.nn_ok) st.nn_ok[i] = (status == ALIVE || nn_out == node_i) ? 1 : 0;
 }
 
+// The realization key of particle i: its own when the particles carry one
+// (several ensemble members in one array), else the step's.
+__device__ __forceinline__ unsigned long long realization_of(const DState& st, const DStep& s, long long i) {
+    return st.rid ? (unsigned long long)st.rid[i] : s.real_id;
+}
+
 // integrators.py:673-818 _apply_split_diffusion_kick for one particle that is
 // ALIVE after the deterministic step (site qn = its position): counter-RNG
 // kick (diffusion.py:485-529, :261-298), great-circle move, exact re-anchor
 // and containment re-check, revert to the pre-step state on leaving the
 // domain; 3-D reclamp in the new column.
-static __device__ __noinline__ void apply_kick(const DMesh& m, const DStep& s, long long pid, const Site& qn,
+static __device__ __noinline__ void apply_kick(const DMesh& m, const DStep& s, long long pid, unsigned long long rid,
+                                        const Site& qn,
                                         double pre_lon, double pre_lat, double pre_z, int pre_nn, bool is3d,
                                         double& lon, double& lat, double& z, int& status, int& nn, signed char& fr) {
     double g1, g2;
-    normal_pair(s.seed, s.real_id, (unsigned long long)pid + s.pid_offset, s.step_i, 0ull, g1, g2);
+    normal_pair(s.seed, rid, (unsigned long long)pid + s.pid_offset, s.step_i, 0ull, g1, g2);
     double abs_dt = s.dt >= 0.0 ? s.dt : -s.dt;
     double sq = sqrt(abs_dt);
     double sx = sqrt(2.0 * s.kh_x);
@@ -213,7 +221,7 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
             if (s.kick) {
                 double zz = 0.0;
                 long long pid = st.pid ? st.pid[i] : i;
-                apply_kick(m, s, pid, qn, lon0, lat0, 0.0, pre_nn, false, lon_new, lat_new, zz, status, nn_out, fr);
+                apply_kick(m, s, pid, realization_of(st, s, i), qn, lon0, lat0, 0.0, pre_nn, false, lon_new, lat_new, zz, status, nn_out, fr);
             }
         }
     } else {
@@ -372,7 +380,7 @@ __device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DB
             nn_out = nn_new;
             if (s.kick) {
                 long long pid = st.pid ? st.pid[i] : i;
-                apply_kick(m, s, pid, qn, lon0, lat0, z0p, pre_nn, true, lon_new, lat_new, z_new, status, nn_out,
+                apply_kick(m, s, pid, realization_of(st, s, i), qn, lon0, lat0, z0p, pre_nn, true, lon_new, lat_new, z_new, status, nn_out,
                            fr);
             }
         }
@@ -441,7 +449,7 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
                 nn_out = nn_new;
                 if (s.kick) {
                     long long pid = st.pid ? st.pid[i] : i;
-                    apply_kick(m, s, pid, qn, lon0, lat0, z0p, pre_nn, true, lon_new, lat_new, z_new, status,
+                    apply_kick(m, s, pid, realization_of(st, s, i), qn, lon0, lat0, z0p, pre_nn, true, lon_new, lat_new, z_new, status,
                                nn_out, fr);
                 }
             }

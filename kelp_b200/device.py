@@ -293,6 +293,32 @@ class DeviceContext:
                   "kc_step_host")
         self.P = P
 
+    def set_realization(self, real_id=None) -> None:
+        """Per-particle realization ids of the resident particles (ensemble
+        members in one array); None returns to the step's real_id."""
+        rid = None if real_id is None else _c(real_id, np.int32)
+        if rid is not None and rid.shape != (self.P,):
+            raise ValueError("one realization id per resident particle")
+        self._chk(N.lib().kc_particles_set_realization(self._ctx, N.ptr(rid)), "kc_particles_set_realization")
+
+    def step_range(self, args: N.StepArgs, begin: int, count: int) -> None:
+        """One step of the resident particles [begin, begin + count)."""
+        self._chk(N.lib().kc_step_range(self._ctx, C.byref(args), int(begin), int(count)), "kc_step_range")
+
+    def run_fused(self, steps, beach=None, graph: bool = True) -> None:
+        """len(steps) steps in one kernel launch (kc_run_fused), the
+        beaching hook after each when ``beach`` (one argument block per step)
+        is given; ``graph`` replays a captured CUDA graph."""
+        n = len(steps)
+        arr = (N.StepArgs * n)(*steps)
+        barr = None
+        if beach is not None:
+            if len(beach) != n:
+                raise ValueError("one beaching argument block per step")
+            barr = (N.BeachArgs * n)(*beach)
+        self._chk(N.lib().kc_run_fused(self._ctx, arr, n, None if barr is None else C.cast(barr, C.c_void_p),
+                                       int(bool(graph))), "kc_run_fused")
+
     def run(self, steps) -> None:
         arr = (N.StepArgs * len(steps))(*steps)
         self._chk(N.lib().kc_run(self._ctx, arr, len(steps)), "kc_run")
