@@ -258,6 +258,118 @@ def accuracy(ctx, wl, slots, forms, sort_every, n_sub):
     return out
 
 
+def run_cohorts(args, wl, ctx, local):
+    """Batched cohorts (one GPU): every cohort x ensemble member in one slot
+    array, stepped by fused multi-step launches (autotuned block size, steps
+    per launch and re-sort interval) against one launch per cohort x member
+    per step (kc_step_range), the reference's way of running them."""
+    from kelp_b200 import autotune, roofline
+    from kelp_b200.device import pinned_empty
+    code, store = FORMS[args.form]
+    slots = {"f16" if store is np.float16 else "f32": ctx.slots_for(wl.snaps, store or np.float32)}
+    P = wl.P
+    t0 = wl.t0_step
+
+    def reset():
+        ctx.upload_particles(wl.lon, wl.lat, wl.z, np.full(P, 4, np.int32), np.full(P, -1, np.int32),
+                             np.zeros(P, np.int8), wl.pid, wl.release_step)
+        ctx.set_realization(wl.real_id)
+
+    def make_steps(k, n):
+        return [_form_args(wl, kk, slots, args.form) for kk in range(k, k + n)]
+
+    key = autotune.mesh_signature(wl.mesh, wl.dims, wl.scheme, args.form, P)
+    tuned = autotune.tune(ctx, key, reset, make_steps, t0, window=args.tune_window, steps_per_launch=(1, 12),
+                          sort_every=(12, 24))
+    spl, se = tuned["steps_per_launch"], tuned["sort_every"]
+    sampler = ClockSampler(local)
+    time.sleep(0.6)
+    t_wall0 = time.time()
+    # batched: fused launches over every slot
+    reset()
+    autotune.run_window(ctx, make_steps, t0, spl, spl, se)
+    ctx.synchronize()
+    if ctx.device_errors():
+        raise RuntimeError("device-side iteration cap hit during warm-up")
+    K = max(spl, (args.steps + spl - 1) // spl * spl)
+    ctx.record(0)
+    autotune.run_window(ctx, make_steps, t0 + spl, K, spl, se)
+    ctx.record(1)
+    batched_ms = ctx.elapsed_ms(0, 1)
+    batched_launches = K // spl + 15 * ((K + se - 1) // se)
+    errs = ctx.device_errors()
+    # one launch per cohort x member per step, no re-sort (the cohorts' slots
+    # must stay contiguous)
+    reset()
+    Kb = max(1, min(args.steps, 4))
+    for (b, cnt, r, c) in wl.cohorts:
+        ctx.step_range(make_steps(t0, 1)[0], b, cnt)
+    ctx.synchronize()
+    ctx.record(0)
+    for k in range(Kb):
+        a = make_steps(t0 + 1 + k, 1)[0]
+        for (b, cnt, r, c) in wl.cohorts:
+            ctx.step_range(a, b, cnt)
+    ctx.record(1)
+    per_cohort_ms = ctx.elapsed_ms(0, 1)
+    t_wall1 = time.time()
+    clocks = sampler.stop(t_wall0, t_wall1)
+
+    # end to end: page-locked host slots through kc_step_host every step
+    names = {"lon": np.float64, "lat": np.float64, "z": np.float64, "status": np.int32, "nearest_node": np.int32,
+             "failure_reason": np.int8, "u": np.float64, "v": np.float64, "w": np.float64}
+    # one set of arrays updated in place (kc_step_host allows it: a chunk is
+    # read before its new state is written back)
+    buf = {n: pinned_empty((P,), t) for n, t in names.items()}
+    for n, src in (("lon", wl.lon), ("lat", wl.lat), ("z", wl.z)):
+        buf[n][:] = src
+    buf["status"][:] = 4
+    buf["nearest_node"][:] = -1
+    buf["failure_reason"][:] = 0
+    ids = {"pid": pinned_empty((P,), np.int64), "real_id": pinned_empty((P,), np.int32),
+           "release_step": pinned_empty((P,), np.int32)}
+    ids["pid"][:] = wl.pid
+    ids["real_id"][:] = wl.real_id
+    ids["release_step"][:] = wl.release_step
+    ins = ("lon", "lat", "z", "status", "nearest_node", "failure_reason")
+    ctx.step_host(make_steps(t0, 1)[0], dict({n: buf[n] for n in ins}, **ids), buf)
+    e2e_steps = 3
+    ctx.record(2)
+    for k in range(e2e_steps):
+        ctx.step_host(make_steps(t0 + 1 + k, 1)[0], dict({n: buf[n] for n in ins}, **ids), buf)
+    ctx.record(3)
+    e2e_ms = ctx.elapsed_ms(2, 3)
+
+    peak, kind = peaks()
+    fb = 2 if store is np.float16 else 4
+    bpp = roofline.bytes_per_particle_step(wl.mesh, wl.scheme, wl.dims, fb, kick=True, w_code=1)
+    value = P * K / (batched_ms * 1e-3)
+    achieved = bpp["total"] * P * K / (batched_ms * 1e-3) / 1e9
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": spl,
+            "ms_per_step": batched_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if code == "plain" else "f32 interp + f64 state", "data": "synthetic",
+            "config": {"workload": wl.name, "form": args.form,
+                       **{k: v for k, v in wl.description.items() if k != "cohort_sizes"},
+                       "l2": "inputs larger than L2 (fields 1.1 GB, slots 7.6 GB); not flushed",
+                       "parallelism": "one GPU, all cohorts x members in one array"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": kind, "traffic": None,
+                         "algorithmic_bytes_per_particle_step": bpp["total"]},
+            "forms": {"batched_fused": {"value": value, "ms_per_step": batched_ms / K, "launches": batched_launches},
+                      "per_cohort_launches": {"value": P * Kb / (per_cohort_ms * 1e-3), "ms_per_step": per_cohort_ms / Kb,
+                                              "launches": Kb * len(wl.cohorts)}},
+            "autotune": {k: v for k, v in tuned.items() if k != "trials"},
+            "autotune_trials": tuned.get("trials"),
+            "e2e": {"value": P * e2e_steps / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": P * (33 + 16),
+                    "d2h_bytes_per_step": P * 57, "steps": e2e_steps, "form": args.form,
+                    "api": "kc_step_host, page-locked host arrays"},
+            "gpu_launches": batched_launches, "clocks": clocks, "device_errors": errs}
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(wl, n_particles=50_000)
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_b200(args):
     rank, world, local = env_rank()
     dist = None
@@ -273,6 +385,10 @@ def run_b200(args):
     set_default_device(local)
     ctx = default_context()
     ctx.ensure_mesh(wl.mesh)
+    if wl.cohorts is not None:
+        if world > 1:
+            raise SystemExit("the batched-cohort workload runs on one GPU")
+        return run_cohorts(args, wl, ctx, local)
     if wl.dims == 3 and wl.uv_vertical != "layer":
         ctx.ensure_depth_points(wl.mesh, wl.uv_vertical)
     forms = [f.strip() for f in args.forms.split(",") if f.strip()]
@@ -422,10 +538,12 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--workload", default="c3", help="c1, c2, c3 (default: the published configuration) or c3small")
+    ap.add_argument("--workload", default="c3",
+                    help="c1, c2, c3 (default: the published configuration), c4 (batched cohorts), c3small, c4small")
     ap.add_argument("--form", default="mixed", choices=sorted(FORMS), help="the form the headline value reports")
     ap.add_argument("--forms", default="plain,mixed,mixed_f16", help="forms timed beside it")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--tune-window", type=int, default=12, help="steps timed per autotuner candidate (c4)")
     ap.add_argument("--accuracy-particles", type=int, default=200_000,
                     help="particles of the full-horizon separation run")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])

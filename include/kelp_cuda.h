@@ -166,9 +166,11 @@ int kc_beach(kc_ctx* ctx, const kc_beach_args* args);
 
 /* Host particle arrays of kc_step_host (SoA, P entries each).  Input: lon,
  * lat, status, nearest_node required; z and failure_reason may be NULL
- * (zeros).  Output: lon, lat, status, nearest_node required; z,
- * failure_reason, u, v, w may be NULL (not returned).  Input and output may
- * be the same arrays. */
+ * (zeros); pid (RNG particle key; NULL: the index), real_id (per-particle
+ * realization; NULL: the step's) and release_step (delayed release, with
+ * kc_step_args.global_step; NULL: all released) are read only from the input.
+ * Output: lon, lat, status, nearest_node required; z, failure_reason, u, v, w
+ * may be NULL (not returned).  Input and output may be the same arrays. */
 typedef struct kc_host_particles {
     double* lon;
     double* lat;
@@ -179,6 +181,9 @@ typedef struct kc_host_particles {
     double* u;
     double* v;
     double* w;
+    long long* pid;
+    int* real_id;
+    int* release_step;
 } kc_host_particles;
 
 /* One step of P particles held in host memory, in the reference's per-step
@@ -213,6 +218,10 @@ int kc_step_range(kc_ctx* ctx, const kc_step_args* args, long long begin, long l
  * No reference counterpart (the reference launches one parallel loop per
  * step and per realization). */
 int kc_run_fused(kc_ctx* ctx, const kc_step_args* steps, int n_steps, const kc_beach_args* beach, int use_graph);
+
+/* Particles per block of kc_run_fused: 128 (default) or 256, both with a
+ * 64-register budget (the autotuner's choice; no reference counterpart). */
+int kc_set_fused_block(kc_ctx* ctx, int block);
 
 /* Re-order the resident particles by grid-hash cell (particles that left the
  * domain last) so that a warp's particles share hash windows and elements.

@@ -25,7 +25,7 @@ EXPORTS = ("kc_abi_version", "kc_node_xyz_fill", "kc_create", "kc_destroy", "kc_
            "kc_synchronize", "kc_mesh_upload", "kc_depth_points_upload", "kc_field_upload", "kc_particles_upload",
            "kc_particles_download", "kc_coastal_upload", "kc_beach_state_upload",
            "kc_beach_state_download", "kc_beach", "kc_step", "kc_step_host", "kc_step_range", "kc_run_fused",
-           "kc_particles_set_realization", "kc_run", "kc_sort", "kc_find_nearest", "kc_find_nearest_noalloc", "kc_rng_normals", "kc_device_errors",
+           "kc_particles_set_realization", "kc_set_fused_block", "kc_run", "kc_sort", "kc_find_nearest", "kc_find_nearest_noalloc", "kc_rng_normals", "kc_device_errors",
            "kc_event_record", "kc_event_elapsed", "kc_l2_flush", "kc_host_alloc", "kc_host_free")
 
 
@@ -87,7 +87,8 @@ class BeachArgs(C.Structure):
 class HostParticles(C.Structure):
     _fields_ = [("lon", C.c_void_p), ("lat", C.c_void_p), ("z", C.c_void_p), ("status", C.c_void_p),
                 ("nearest_node", C.c_void_p), ("failure_reason", C.c_void_p),
-                ("u", C.c_void_p), ("v", C.c_void_p), ("w", C.c_void_p)]
+                ("u", C.c_void_p), ("v", C.c_void_p), ("w", C.c_void_p),
+                ("pid", C.c_void_p), ("real_id", C.c_void_p), ("release_step", C.c_void_p)]
 
 
 _lib = None
@@ -122,6 +123,7 @@ def lib():
         L.kc_step_range.argtypes = [vp, C.POINTER(StepArgs), ll, ll]
         L.kc_run_fused.argtypes = [vp, C.POINTER(StepArgs), i, C.c_void_p, i]
         L.kc_particles_set_realization.argtypes = [vp, vp]
+        L.kc_set_fused_block.argtypes = [vp, i]
         L.kc_step_host.argtypes = [vp, C.POINTER(StepArgs), ll, C.POINTER(HostParticles), C.POINTER(HostParticles),
                                    ll]
         L.kc_run.argtypes = [vp, C.POINTER(StepArgs), i]

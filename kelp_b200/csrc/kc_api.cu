@@ -110,6 +110,7 @@ struct kc_ctx {
     cudaGraphExec_t fused_exec = nullptr;
     std::string fused_key;
     unsigned long long mesh_gen = 0;
+    int fused_block = 128;   // particles per block of the fused launch (kc_set_fused_block)
     // float staging buffer of the half-precision snapshot conversion
     float* stage = nullptr;
     size_t stage_cap = 0;
@@ -309,9 +310,9 @@ kc::DBlend<T> blend_of(kc_ctx* c, const kc_step_args* a) {
 void kc_launch_mixed_f32(const kc::DMesh& m, const kc::DBlend<float>& f, const kc::DState& st, const kc::DStep& s,
                          int dims, int scheme, cudaStream_t stream);
 void kc_launch_multi_mixed_f32(const kc::DMesh& m, const MultiHead* head, const StepPack<float>* packs, long long P,
-                               int dims, int scheme, cudaStream_t stream);
+                               int dims, int scheme, int block, cudaStream_t stream);
 void kc_launch_multi_mixed_f16(const kc::DMesh& m, const MultiHead* head, const StepPack<__half>* packs, long long P,
-                               int dims, int scheme, cudaStream_t stream);
+                               int dims, int scheme, int block, cudaStream_t stream);
 void kc_launch_mixed_f16(const kc::DMesh& m, const kc::DBlend<__half>& f, const kc::DState& st,
                          const kc::DStep& s, int dims, int scheme, cudaStream_t stream);
 
@@ -891,9 +892,9 @@ int kc_step_host(kc_ctx* c, const kc_step_args* a, long long P, const kc_host_pa
     if (rc) return rc;
     c->P = P;
     c->sorted = false;
-    c->has_pid = false;
-    c->has_rs = false;
-    c->has_rid = false;
+    c->has_pid = in->pid != nullptr;
+    c->has_rs = in->release_step != nullptr;
+    c->has_rid = in->real_id != nullptr;
     c->has_beach = false;
     if ((rc = check_step(c, a))) return rc;
     if (P == 0) return KC_OK;
@@ -928,6 +929,10 @@ int kc_step_host(kc_ctx* c, const kc_step_args* a, long long P, const kc_host_pa
         if (in->failure_reason)
             KC_CUDA(c, cudaMemcpyAsync(c->fr + b, in->failure_reason + b, n, cudaMemcpyHostToDevice, si));
         else KC_CUDA(c, cudaMemsetAsync(c->fr + b, 0, n, si));
+        if (in->pid) KC_CUDA(c, cudaMemcpyAsync(c->pid + b, in->pid + b, n * 8, cudaMemcpyHostToDevice, si));
+        if (in->real_id) KC_CUDA(c, cudaMemcpyAsync(c->rid + b, in->real_id + b, n * 4, cudaMemcpyHostToDevice, si));
+        if (in->release_step)
+            KC_CUDA(c, cudaMemcpyAsync(c->rs + b, in->release_step + b, n * 4, cudaMemcpyHostToDevice, si));
         KC_CUDA(c, cudaEventRecord(c->ev_in[k], si));
         // the chunk's particles as a state of their own: RNG keys stay the
         // global index (pid_offset + base + local index); carried anchors are
@@ -935,10 +940,13 @@ int kc_step_host(kc_ctx* c, const kc_step_args* a, long long P, const kc_host_pa
         kc::DState st = full;
         st.lon += b; st.lat += b; st.z += b; st.status += b; st.nn += b;
         st.U += b; st.V += b; st.W += b; st.fr += b;
-        st.pid = nullptr; st.release_step = nullptr; st.prev = nullptr; st.nn_ok = nullptr; st.rid = nullptr;
+        st.pid = in->pid ? c->pid + b : nullptr;
+        st.rid = in->real_id ? c->rid + b : nullptr;
+        st.release_step = in->release_step ? c->rs + b : nullptr;
+        st.prev = nullptr; st.nn_ok = nullptr;
         st.P = n;
         kc::DStep sk = s0;
-        sk.pid_offset = s0.pid_offset + (unsigned long long)b;
+        if (!in->pid) sk.pid_offset = s0.pid_offset + (unsigned long long)b;
         KC_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_in[k], 0));
         if ((rc = launch_step_on(c, a, st, sk))) return rc;
         KC_CUDA(c, cudaEventRecord(c->ev_k[k], c->stream));
@@ -999,11 +1007,14 @@ static void launch_multi(kc_ctx* c, int precision, int dtype, const MultiHead* d
                          int scheme) {
     if (precision == KC_MIXED) {
         if (dtype == KC_F16)
-            kc_launch_multi_mixed_f16(c->dm, dh, (const StepPack<__half>*)dp, c->P, dims, scheme, c->stream);
+            kc_launch_multi_mixed_f16(c->dm, dh, (const StepPack<__half>*)dp, c->P, dims, scheme, c->fused_block,
+                                      c->stream);
         else
-            kc_launch_multi_mixed_f32(c->dm, dh, (const StepPack<float>*)dp, c->P, dims, scheme, c->stream);
+            kc_launch_multi_mixed_f32(c->dm, dh, (const StepPack<float>*)dp, c->P, dims, scheme, c->fused_block,
+                                      c->stream);
     } else if constexpr (!std::is_same<T, __half>::value) {   // the plain form never reads half storage
-        launch_multi_kernel<T, kc::PlainForm<T>>(c->dm, dh, (const StepPack<T>*)dp, c->P, dims, scheme, c->stream);
+        launch_multi_kernel<T, kc::PlainForm<T>>(c->dm, dh, (const StepPack<T>*)dp, c->P, dims, scheme,
+                                                 c->fused_block, c->stream);
     }
 }
 
@@ -1056,7 +1067,8 @@ static int run_fused_t(kc_ctx* c, const kc_step_args* steps, int n, const kc_bea
         const std::string key = std::to_string(precision) + "/" + std::to_string(dtype) + "/" + std::to_string(dims) +
                                 "/" + std::to_string(scheme) + "/" + std::to_string(n) + "/" +
                                 std::to_string(bytes) + "/" + std::to_string(c->P) + "/" +
-                                std::to_string(c->mesh_gen) + "/" + std::to_string((size_t)c->fused_dev) + "/" +
+                                std::to_string(c->mesh_gen) + "/" + std::to_string(c->fused_block) + "/" +
+                                std::to_string((size_t)c->fused_dev) + "/" +
                                 std::to_string((size_t)c->fused_host);
         if (key != c->fused_key || !c->fused_exec) {
             if (c->fused_exec) cudaGraphExecDestroy(c->fused_exec);
@@ -1094,6 +1106,13 @@ static int run_fused_t(kc_ctx* c, const kc_step_args* steps, int n, const kc_bea
 }
 
 }  // extern "C++"
+
+int kc_set_fused_block(kc_ctx* c, int block) {
+    if (!c) return KC_ERR_ARG;
+    if (block != 128 && block != 256) return fail(c, KC_ERR_ARG, "kc_set_fused_block: 128 or 256");
+    c->fused_block = block;
+    return KC_OK;
+}
 
 int kc_run_fused(kc_ctx* c, const kc_step_args* steps, int n_steps, const kc_beach_args* beach, int use_graph) {
     if (!c || !steps) return KC_ERR_ARG;

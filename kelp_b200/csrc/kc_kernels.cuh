@@ -92,8 +92,10 @@ struct MultiHead {
     int n_steps;
 };
 
-template <typename T, int DIMS, int SCHEME, typename Form>
-__global__ void __launch_bounds__(kBlock, KC_STEP_MIN_BLOCKS) k_multi(const __grid_constant__ kc::DMesh m,
+// BLOCK threads per block, BLOCK * blocks-per-SM = 1024 threads: the same
+// 64-register budget at either block size.
+template <typename T, int DIMS, int SCHEME, typename Form, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_multi(const __grid_constant__ kc::DMesh m,
                                                                      const MultiHead* __restrict__ head,
                                                                      const StepPack<T>* __restrict__ packs) {
     const kc::DState& st = head->st;
@@ -116,34 +118,39 @@ __global__ void __launch_bounds__(kBlock, KC_STEP_MIN_BLOCKS) k_multi(const __gr
 
 // Persistent grid: every SM's resident blocks, no more than the particles need.
 template <typename K>
-unsigned persistent_grid(K kernel, long long P) {
+unsigned persistent_grid(K kernel, long long P, int block) {
     int dev = 0, sms = 1, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0);
     if (per_sm < 1) per_sm = 1;
-    const long long need = (P + kBlock - 1) / kBlock;
+    const long long need = (P + block - 1) / block;
     const long long cap = (long long)sms * per_sm;
     return (unsigned)(need < cap ? (need > 0 ? need : 1) : cap);
 }
 
 template <typename T, typename Form, int DIMS, int SCHEME>
-void launch_multi_one(const kc::DMesh& m, const MultiHead* head, const StepPack<T>* packs, long long P,
+void launch_multi_one(const kc::DMesh& m, const MultiHead* head, const StepPack<T>* packs, long long P, int block,
                       cudaStream_t stream) {
-    auto kern = k_multi<T, DIMS, SCHEME, Form>;
-    kern<<<persistent_grid(kern, P), kBlock, 0, stream>>>(m, head, packs);
+    if (block == 256) {
+        auto kern = k_multi<T, DIMS, SCHEME, Form, 256>;
+        kern<<<persistent_grid(kern, P, 256), 256, 0, stream>>>(m, head, packs);
+    } else {
+        auto kern = k_multi<T, DIMS, SCHEME, Form, 128>;
+        kern<<<persistent_grid(kern, P, 128), 128, 0, stream>>>(m, head, packs);
+    }
 }
 
 template <typename T, typename Form>
 void launch_multi_kernel(const kc::DMesh& m, const MultiHead* head, const StepPack<T>* packs, long long P, int dims,
-                         int scheme, cudaStream_t stream) {
+                         int scheme, int block, cudaStream_t stream) {
     if (dims == 2) {
-        if (scheme == 0) launch_multi_one<T, Form, 2, 0>(m, head, packs, P, stream);
-        else if (scheme == 1) launch_multi_one<T, Form, 2, 1>(m, head, packs, P, stream);
-        else launch_multi_one<T, Form, 2, 2>(m, head, packs, P, stream);
+        if (scheme == 0) launch_multi_one<T, Form, 2, 0>(m, head, packs, P, block, stream);
+        else if (scheme == 1) launch_multi_one<T, Form, 2, 1>(m, head, packs, P, block, stream);
+        else launch_multi_one<T, Form, 2, 2>(m, head, packs, P, block, stream);
     } else {
-        if (scheme == 1) launch_multi_one<T, Form, 3, 1>(m, head, packs, P, stream);
-        else if (scheme == 2) launch_multi_one<T, Form, 3, 2>(m, head, packs, P, stream);
-        else launch_multi_one<T, Form, 3, 0>(m, head, packs, P, stream);
+        if (scheme == 1) launch_multi_one<T, Form, 3, 1>(m, head, packs, P, block, stream);
+        else if (scheme == 2) launch_multi_one<T, Form, 3, 2>(m, head, packs, P, block, stream);
+        else launch_multi_one<T, Form, 3, 0>(m, head, packs, P, block, stream);
     }
 }

@@ -18,11 +18,11 @@ void kc_launch_mixed_f16(const kc::DMesh& m, const kc::DBlend<__half>& f, const 
 }
 
 void kc_launch_multi_mixed_f32(const kc::DMesh& m, const MultiHead* head, const StepPack<float>* packs, long long P,
-                               int dims, int scheme, cudaStream_t stream) {
-    launch_multi_kernel<float, kc::MixedForm<float>>(m, head, packs, P, dims, scheme, stream);
+                               int dims, int scheme, int block, cudaStream_t stream) {
+    launch_multi_kernel<float, kc::MixedForm<float>>(m, head, packs, P, dims, scheme, block, stream);
 }
 
 void kc_launch_multi_mixed_f16(const kc::DMesh& m, const MultiHead* head, const StepPack<__half>* packs, long long P,
-                               int dims, int scheme, cudaStream_t stream) {
-    launch_multi_kernel<__half, kc::MixedForm<__half>>(m, head, packs, P, dims, scheme, stream);
+                               int dims, int scheme, int block, cudaStream_t stream) {
+    launch_multi_kernel<__half, kc::MixedForm<__half>>(m, head, packs, P, dims, scheme, block, stream);
 }

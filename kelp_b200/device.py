@@ -267,7 +267,7 @@ class DeviceContext:
         (``pinned_empty``) let the copies overlap the step."""
         types = {"lon": np.float64, "lat": np.float64, "z": np.float64, "status": np.int32,
                  "nearest_node": np.int32, "failure_reason": np.int8, "u": np.float64, "v": np.float64,
-                 "w": np.float64}
+                 "w": np.float64, "pid": np.int64, "real_id": np.int32, "release_step": np.int32}
 
         def pack(d, names):
             h = N.HostParticles()
@@ -285,8 +285,9 @@ class DeviceContext:
                 setattr(h, name, a.ctypes.data)
             return h, P
 
-        hi, P = pack(inp, ("lon", "lat", "z", "status", "nearest_node", "failure_reason"))
-        ho, P2 = pack(out, tuple(types))
+        hi, P = pack(inp, ("lon", "lat", "z", "status", "nearest_node", "failure_reason", "pid", "real_id",
+                           "release_step"))
+        ho, P2 = pack(out, ("lon", "lat", "z", "status", "nearest_node", "failure_reason", "u", "v", "w"))
         if P is None or P2 != P:
             raise ValueError("input and output particle counts differ")
         self._chk(N.lib().kc_step_host(self._ctx, C.byref(args), P, C.byref(hi), C.byref(ho), int(chunk)),
@@ -318,6 +319,10 @@ class DeviceContext:
             barr = (N.BeachArgs * n)(*beach)
         self._chk(N.lib().kc_run_fused(self._ctx, arr, n, None if barr is None else C.cast(barr, C.c_void_p),
                                        int(bool(graph))), "kc_run_fused")
+
+    def set_fused_block(self, block: int) -> None:
+        """Particles per block of run_fused: 128 or 256."""
+        self._chk(N.lib().kc_set_fused_block(self._ctx, int(block)), "kc_set_fused_block")
 
     def run(self, steps) -> None:
         arr = (N.StepArgs * len(steps))(*steps)

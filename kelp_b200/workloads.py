@@ -32,6 +32,12 @@ class Workload:
     kh: Optional[tuple] = None      # (kh_x, kh_y) of the split uniform kick
     seed: int = 0
     uv_vertical: str = "layer"      # 3-D u/v placement: layer, level or layer_linear
+    # batched cohorts (one slot array for every cohort x ensemble member)
+    pid: Optional[np.ndarray] = None           # RNG particle key per slot: its index within its cohort
+    real_id: Optional[np.ndarray] = None       # realization (ensemble member) per slot
+    release_step: Optional[np.ndarray] = None  # global step of the slot's release
+    cohorts: Optional[list] = None             # (begin, count, member, cohort) blocks of the slot array
+    t0_step: int = 0                           # first global step of the timed window
     description: dict = field(default_factory=dict)
 
     @property
@@ -69,7 +75,7 @@ class Workload:
             a.kick = 1
             a.kh_x, a.kh_y = self.kh
             a.seed, a.real_id, a.step_i, a.pid_offset = self.seed, 0, k, 0
-        a.global_step = -1
+        a.global_step = -1 if self.release_step is None else k
         a.uv_vertical = 0 if self.uv_vertical == "layer" else 1
         a.precision = precision
         return a
@@ -137,6 +143,58 @@ def c3(P: int = 6_000_000, nside: int = 512, n_levels: int = 69, n_snap: int = 2
                                  "diffusion": "split uniform Kh=10 m^2/s", "w_interp": "barycentric"})
 
 
+def c4(n_cohorts: int = 64, members: int = 8, spacing: float = 0.2, n_levels: int = 47, seed: int = 4,
+       size_lo: int = 1000, size_hi: int = 500_000, release_days: float = 30.0) -> Workload:
+    """Batched cohorts: a ~1 M-node jittered lattice mesh (triangles plus 25 %
+    convex quads, 30 % land), 47 z-level interfaces, smooth bathymetry,
+    float32 u/v (46, N) and w (47, N) on nodes (layer placement, 2 daily
+    snapshots cycled); 64 release cohorts of log-uniform size 1 k - 500 k
+    particles (uniform over the wet volume, seeds sorted within each cohort),
+    released at uniform times over 30 days; 8 diffusion ensemble members each
+    (realization ids 0..7, Kh = 50 m^2/s); RK4, dt 1 h, W barycentric, 60-day
+    horizon.  Slots are member-major, then cohort: every (member, cohort) block
+    is contiguous.  The timed window starts at day 30, when every cohort is
+    released."""
+    zl = S.stretched_levels(n_levels, 5.0, 6000.0)
+    m = S.lattice_mesh(spacing, 80.0, jitter=0.2, land_frac=0.3, quad_frac=0.25,
+                       depth=lambda lo, la: S.smooth_bathymetry(lo, la, 50.0, 6000.0), sigma=zl)
+    snaps = S.gyre_snapshots(m, 2, amp=0.5, z_levels=zl, decay=1000.0, w_scale=1e-3)
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(size_lo), np.log(size_hi), n_cohorts)).astype(np.int64)
+    dt = 3600.0
+    rel = np.floor(rng.uniform(0.0, release_days * 86400.0, n_cohorts) / dt).astype(np.int32)
+    base = int(sizes.sum())
+    blon, blat, bz = S.release_uniform(m, base, seed=seed + 1, depth_uniform=True)
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    parts = [S.sort_seeds(blon[off[c]:off[c + 1]], blat[off[c]:off[c + 1]], bz[off[c]:off[c + 1]])
+             for c in range(n_cohorts)]
+    clon = np.concatenate([p[0] for p in parts])
+    clat = np.concatenate([p[1] for p in parts])
+    cz = np.concatenate([p[2] for p in parts])
+    cpid = np.concatenate([np.arange(s, dtype=np.int64) for s in sizes])
+    crel = np.repeat(rel, sizes)
+    lon = np.tile(clon, members)
+    lat = np.tile(clat, members)
+    z = np.tile(cz, members)
+    pid = np.tile(cpid, members)
+    rs = np.tile(crel, members)
+    rid = np.repeat(np.arange(members, dtype=np.int32), base)
+    cohorts = [(r * base + int(off[c]), int(sizes[c]), r, c) for r in range(members) for c in range(n_cohorts)]
+    P = lon.size
+    return Workload("c4_cohorts_3d_rk4_kick", m, snaps, lon, lat, z, "rk4", dt, 86400.0, 1440,
+                    dims=3, w_interp="barycentric", kh=(50.0, 50.0), seed=0,
+                    pid=pid, real_id=rid, release_step=rs, cohorts=cohorts, t0_step=int(release_days * 24),
+                    description={"mesh": f"jittered {spacing} deg lattice, 25% quads, 30% land",
+                                 "nodes": int(m.n_nodes), "elements": int(m.n_elements), "levels": n_levels,
+                                 "particles": P, "cohorts": n_cohorts, "members": members,
+                                 "cohort_sizes": [int(v) for v in sizes],
+                                 "seeds": "sorted by 1-degree cell within each cohort",
+                                 "release": f"uniform over {release_days:g} days", "scheme": "rk4", "dt_s": 3600,
+                                 "steps_run": 1440, "fields": "f32 node u,v (46,N), w (47,N), 2 daily snapshots",
+                                 "diffusion": "split uniform Kh=50 m^2/s, per-member realization ids",
+                                 "w_interp": "barycentric", "timed_from_step": int(release_days * 24)})
+
+
 def c3_small(P: int = 200_000) -> Workload:
     """C3's kernel on a reduced HEALPix grid (nside 128) and particle count:
     the profiling case (a few hundred MB on the device)."""
@@ -145,4 +203,12 @@ def c3_small(P: int = 200_000) -> Workload:
     return w
 
 
-WORKLOADS: dict = {"c1": c1, "c2": c2, "c3": c3, "c3small": c3_small}
+def c4_small() -> Workload:
+    """C4's structure at a test size: 8 cohorts of 500 - 5 000 particles on a
+    2-degree mesh, 3 members, releases over 2 days."""
+    w = c4(n_cohorts=8, members=3, spacing=2.0, size_lo=500, size_hi=5000, release_days=2.0)
+    w.name = "c4small_cohorts_3d_rk4_kick"
+    return w
+
+
+WORKLOADS: dict = {"c1": c1, "c2": c2, "c3": c3, "c3small": c3_small, "c4": c4, "c4small": c4_small}

@@ -133,3 +133,38 @@ def test_step_range_equals_step():
     with pytest.raises(N.KcError):
         ctx.step_range(a, P - 10, 20)
     ctx.close()
+
+
+def test_autotune_picks_a_candidate_and_results_do_not_depend_on_it(tmp_path, monkeypatch):
+    from kelp_b200 import autotune
+    from kelp_b200.device import DeviceContext
+    monkeypatch.setenv("KELP_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    w = _workload(8000)
+    P = w.P
+    ctx = DeviceContext(0)
+    ctx.ensure_mesh(w.mesh)
+    slots = ctx.slots_for(w.snaps)
+
+    def reset():
+        ctx.upload_particles(w.lon, w.lat, w.z, np.ones(P, np.int32), np.full(P, -1, np.int32),
+                             np.zeros(P, np.int8))
+
+    def make_steps(k, n):
+        return [w.step_args(kk, slots) for kk in range(k, k + n)]
+
+    key = autotune.mesh_signature(w.mesh, 3, "rk2", "plain", P)
+    t = autotune.tune(ctx, key, reset, make_steps, 0, window=4, blocks=(128, 256), steps_per_launch=(1, 2),
+                      sort_every=(2, 4))
+    assert t["block"] in (128, 256) and t["steps_per_launch"] in (1, 2) and t["sort_every"] in (2, 4)
+    assert len(t["trials"]) == 8 and not t["cached"]
+    again = autotune.tune(ctx, key, reset, make_steps, 0, window=4)
+    assert again["cached"] and again["block"] == t["block"]
+    outs = []
+    for blk, spl, se in ((128, 1, 2), (256, 2, 4)):
+        ctx.set_fused_block(blk)
+        reset()
+        autotune.run_window(ctx, make_steps, 0, 8, spl, se)
+        outs.append(ctx.download_particles())
+    for n in FIELDS:
+        np.testing.assert_array_equal(outs[0][n], outs[1][n], err_msg=n)
+    ctx.close()

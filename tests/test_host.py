@@ -116,3 +116,13 @@ def test_registry_mirrors_reference():
     from kelp_b200 import integrators as KI
     assert set(KI.INTEGRATORS) == {"euler", "rk2", "rk4", "rk45"}
     assert KI.get_integrator("RK2") is KI.rk2_step
+
+
+def test_autotune_cache_roundtrip(tmp_path, monkeypatch, golden):
+    from kelp_b200 import autotune
+    monkeypatch.setenv("KELP_B200_TUNE_CACHE", str(tmp_path / "t.json"))
+    g = golden("golden_quad")
+    key = autotune.mesh_signature(g.mesh, 2, "rk2", "plain", 1000)
+    assert key.startswith("N") and "-d2-rk2-plain-P512" in key
+    autotune._store({key: {"block": 256, "steps_per_launch": 6, "sort_every": 12}})
+    assert autotune._load()[key]["block"] == 256
