@@ -149,9 +149,11 @@ __device__ __noinline__ bool stage_f32(const DMesh& m, const DBlend<T>& f, const
     W = 0.0;
     const TBlendF tb = tblend_mode(f.alpha0, alpha);
     const float td = (float)s.time_dir;
-    int w_elem;
-    bool w_unsure;
-    const int elem = contain_local_w(m, xp, yp, nn, w_elem, w_unsure);
+    int w_elem = -1;
+    bool w_unsure = false;
+    // the W bookkeeping of the scan only where a barycentric W reads it
+    const int elem = (dims == 3 && s.w_code == 1) ? contain_local_w(m, xp, yp, nn, w_elem, w_unsure)
+                                                  : contain_local(m, xp, yp, nn);
     Ring r;
     float w[4];
     const bool ok = elem >= 0 && weights_f32(m, elem, xp, yp, r, w);
