@@ -134,6 +134,10 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
     vel_next = kw.get("vel_next", None)
     dt_to_next = kw.get("dt_to_next", None)
     _validate_time_aware(vel_next, dt_to_next, dt)
+    if scheme != "euler" and dt_to_next is not None and float(dt) > float(dt_to_next) + 1e-9:
+        # integrators.py:1046-1052: the RK stages would read past the bracket
+        raise ValueError(f"step endpoint past next snapshot: dt={float(dt):.6f}s > "
+                         f"dt_to_next={float(dt_to_next):.6f}s")
     is3d = _is_3d(vel)
     w_code = 0
     placement = "layer"

@@ -1,0 +1,504 @@
+"""The caller side of the step on the B200: a device-resident tracking loop.
+
+``Tracker.run`` follows the per-step order of KELP's
+``tracking.run_single_realization`` (``src/kelp/tracking.py:2384-2860``):
+delayed release (in the step kernel), the velocity payload of the step's time
+bracket, the step, the beaching hook, the clock, and a record every
+``output_freq`` global steps; only the records cross PCIe.  The mesh, the
+snapshots in use (a ring of device slots) and the particles stay resident;
+the particles are re-sorted by hash cell every ``sort_every`` steps (results do
+not depend on the order).  Several realizations that start together run as
+one array with per-particle realization ids (``run_realizations``), each with
+the draws of its own run.
+
+The time axis restates ``_resolve_time_bracket`` / ``_build_vel_payload``
+(``tracking.py:2910-3206``): brackets on the record times, ``stop`` or
+``cycle`` (period = span of the records + the last interval) when the records
+are exhausted, the on-snapshot shifts of forward and backward steps within the
+clock's roundoff band (``_snapshot_band``, ``:1667``).
+
+``run_tracking(config, ...)`` takes KELP's configuration schema (the
+``mode``, ``numerics`` (with ``diffusion`` and ``beaching``) and ``time``
+sections, as a dict or YAML file) with ``numerics.backend: cuda``.  KELP's
+readers (netCDF / zarr / healpy) are not part of this package: the mesh, the
+snapshot records and the seeds are passed in, or read from ``.npz`` files named
+in the ``data`` section (``mesh_npz``, ``velocity_npz``, ``seeds``).
+"""
+from __future__ import annotations
+
+import os
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _native as N
+from . import integrators as KI
+from .beaching import BeachingConfig, beach_args, make_run_config
+from .device import default_context
+from .fields import LazyLerpField, VelocityField
+from .particles import ParticleState, ParticleStatus, make_state
+
+# ---------------------------------------------------------------------------
+# time axis
+# ---------------------------------------------------------------------------
+
+
+def snapshot_band(dt: float) -> float:
+    """Seconds within which a step that reaches a record is on it
+    (tracking.py:1667-1679)."""
+    return 1e-5 * max(abs(float(dt)), 1.0)
+
+
+def _last_interval(ft) -> float:
+    return float(ft[-1] - ft[-2]) if len(ft) > 1 else 1.0
+
+
+def cycle_period(file_times) -> float:
+    """Period of ``on_exhausted: cycle``: the span of the records plus the
+    last interval (tracking.py:2910-2916)."""
+    ft = np.asarray(file_times, dtype=np.float64)
+    return float(ft[-1] - ft[0]) + _last_interval(ft)
+
+
+def wrap_time(t: float, file_times, on_exhausted: str) -> float:
+    ft = np.asarray(file_times, dtype=np.float64)
+    if on_exhausted != "cycle":
+        return float(t)
+    return float(ft[0] + ((t - ft[0]) % cycle_period(ft)))
+
+
+def resolve_time_bracket(t: float, file_times, on_exhausted: str = "stop", direction: int = 1,
+                         snap: float = 0.0):
+    """``(idx_a, idx_b, ta, tb, t_in_bracket)`` of the records around time
+    ``t``, or None past the records in ``stop`` mode (tracking.py:2947-3071).
+
+    A forward query within ``snap`` below a record starts the interval above
+    it; a backward query on (or within the band above) a record takes the
+    interval below it, its position at the top."""
+    ft = np.asarray(file_times, dtype=np.float64)
+    n = ft.size
+    cyc = on_exhausted == "cycle"
+    tw = wrap_time(t, ft, on_exhausted)
+    if not cyc and (tw < ft[0] - 1e-6 or tw > ft[-1] + 1e-6):
+        return None
+    ib = int(np.searchsorted(ft, tw, side="right"))
+    ia = ib - 1
+    if cyc:
+        ia, ib = ia % n, ib % n
+    else:
+        ia, ib = max(0, min(ia, n - 1)), max(0, min(ib, n - 1))
+    ta, tb = float(ft[ia]), float(ft[ib])
+    if cyc and tb <= ta:
+        tb = ta + _last_interval(ft)
+    if direction > 0 and snap > 0.0 and ia != ib and tb - tw <= snap:
+        s = ib
+        s_next = (s + 1) % n if cyc else min(s + 1, n - 1)
+        ta2, tb2 = float(ft[s]), float(ft[s_next])
+        if cyc and tb2 <= ta2:
+            tb2 = ta2 + _last_interval(ft)
+        return s, s_next, ta2, tb2, ta2
+    if direction < 0 and tw <= ta + max(1e-6, snap):
+        ib2 = ia
+        ia2 = (ia - 1) % n if cyc else ia - 1
+        if ia2 < 0 or ia2 == ib2:
+            return ib2, ib2, ta, ta, tw
+        ta2, tb2 = float(ft[ia2]), float(ft[ib2])
+        if tb2 <= ta2:
+            tb2 = ta2 + _last_interval(ft)
+        return ia2, ib2, ta2, tb2, tb2
+    return ia, ib, ta, tb, tw
+
+
+def vel_payload(bracket, fields: Sequence, direction: int = 1):
+    """``(vel, vel_next, dt_to_next)`` of a bracket (tracking.py:3136-3206):
+    the field at the query time (a snapshot, or a lazy pair with alpha), the
+    snapshot the step moves toward and the seconds to it; a degenerate bracket
+    gives the steady field."""
+    ia, ib, ta, tb, tw = bracket
+    a = fields[ia]
+    if ia == ib:
+        return a, None, None
+    b = fields[ib]
+    interval = tb - ta
+    alpha = (tw - ta) / interval if interval > 0 else 0.0
+    if abs(alpha) < 1e-12:
+        vel = a
+    elif abs(alpha - 1.0) < 1e-12:
+        vel = b
+    else:
+        vel = LazyLerpField(a, b, alpha)
+    if direction >= 0:
+        return vel, b, tb - tw
+    dt_prev = tw - ta
+    if dt_prev <= 1e-6:
+        return vel, None, None
+    return vel, a, dt_prev
+
+
+# ---------------------------------------------------------------------------
+# records
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class TrajectoryRecord:
+    """Snapshots of one realization at its record steps (tracking.py:50-80):
+    positions, velocity diagnostics, status and failure reason per record,
+    times in seconds on the forcing axis at the end of the recorded step."""
+    lons: List[np.ndarray] = field(default_factory=list)
+    lats: List[np.ndarray] = field(default_factory=list)
+    zs: List[np.ndarray] = field(default_factory=list)
+    times: List[float] = field(default_factory=list)
+    us: List[np.ndarray] = field(default_factory=list)
+    vs: List[np.ndarray] = field(default_factory=list)
+    ws: List[np.ndarray] = field(default_factory=list)
+    status: List[np.ndarray] = field(default_factory=list)
+    failure_reason: List[np.ndarray] = field(default_factory=list)
+    release_lon: Optional[np.ndarray] = None
+    release_lat: Optional[np.ndarray] = None
+    release_z: Optional[np.ndarray] = None
+    release_time: Optional[np.ndarray] = None
+
+    def append(self, s: dict, t: float, dims: int) -> None:
+        self.lons.append(s["lon"])
+        self.lats.append(s["lat"])
+        self.zs.append(s["z"])
+        self.times.append(float(t))
+        self.us.append(s["u"])
+        self.vs.append(s["v"])
+        if dims == 3:
+            self.ws.append(s["w"])
+        self.status.append(s["status"])
+        self.failure_reason.append(s["failure_reason"])
+
+    def as_arrays(self) -> dict:
+        """(n_records, P) arrays of every recorded quantity."""
+        out = {"time": np.asarray(self.times)}
+        for name in ("lons", "lats", "zs", "us", "vs", "ws", "status", "failure_reason"):
+            seq = getattr(self, name)
+            if seq:
+                out[name] = np.stack(seq)
+        return out
+
+
+# ---------------------------------------------------------------------------
+# the device-resident loop
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class RunResult:
+    records: List[TrajectoryRecord]
+    final: List[ParticleState]
+    wet_streak: List[Optional[np.ndarray]]
+    steps: int
+
+
+class Tracker:
+    """A tracking run whose mesh, snapshots and particles stay on the GPU.
+
+    ``fields`` are the snapshot records (``VelocityField``-like, node layout)
+    at ``file_times`` seconds; ``integrator`` is euler / rk2 / rk4;
+    ``diffusion`` a ``DiffusionConfig``-like object (``enabled``, ``scheme``
+    uniform, ``kh_zonal``, ``kh_meridional``, ``seed``) or None;
+    ``beaching`` a ``BeachingConfig`` or None.  ``precision`` and ``snapshots``
+    select the numerical form as for the step functions."""
+
+    def __init__(self, mesh, fields: Sequence, file_times, *, integrator: str = "rk2", dt: float,
+                 time_dir: float = 1.0, uv_interp: str = "barycentric", w_interp: str = "barycentric",
+                 diffusion=None, beaching: Optional[BeachingConfig] = None, on_exhausted: str = "stop",
+                 precision: str = "plain", snapshots: Optional[str] = None, sort_every: int = 16, ctx=None):
+        if integrator not in ("euler", "rk2", "rk4"):
+            raise NotImplementedError(f"integrator {integrator!r} is not built on the CUDA backend")
+        if on_exhausted not in ("stop", "cycle"):
+            raise ValueError(f"on_exhausted must be 'stop' or 'cycle', got {on_exhausted!r}")
+        if float(dt) <= 0:
+            raise ValueError(f"dt must be > 0, got {dt!r}")
+        if float(time_dir) not in (1.0, -1.0):
+            raise ValueError(f"time_dir must be +1 or -1, got {time_dir!r}")
+        self.mesh = mesh
+        self.fields = list(fields)
+        self.file_times = np.asarray(file_times, dtype=np.float64)
+        if self.file_times.size != len(self.fields) or self.file_times.size == 0:
+            raise ValueError("one record time per snapshot is required")
+        if np.any(np.diff(self.file_times) <= 0):
+            raise ValueError("record times must increase")
+        self.integrator = integrator
+        self.dt = float(dt)
+        self.direction = 1 if float(time_dir) > 0 else -1
+        self.kw = {"uv_interp": uv_interp, "w_interp": w_interp, "cuda_precision": precision}
+        if snapshots is not None:
+            self.kw["cuda_snapshots"] = snapshots
+        self.diffusion = diffusion if (diffusion is not None and getattr(diffusion, "enabled", True)) else None
+        if self.diffusion is not None:
+            if getattr(self.diffusion, "scheme", "uniform") != "uniform":
+                raise NotImplementedError("only the uniform-Kh split kick is built on the CUDA backend")
+            if getattr(self.diffusion, "composition", "split") != "split":
+                raise NotImplementedError("only the split kick composition is built on the CUDA backend")
+            if getattr(self.diffusion, "az_enabled", False):
+                raise NotImplementedError("the vertical Az kick is not built on the CUDA backend")
+        self.beaching = beaching if (beaching is not None and beaching.enabled) else None
+        self.on_exhausted = on_exhausted
+        self.sort_every = int(sort_every)
+        self.ctx = ctx or default_context()
+        self.dims = 3 if getattr(self.fields[0], "w", None) is not None else 2
+
+    def _kick(self, realization: int, step_i: int, particle_offset: int):
+        d = self.diffusion
+        if d is None:
+            return None
+        kx = float(getattr(d, "kh_zonal", getattr(d, "kh_x", 0.0)))
+        ky = float(getattr(d, "kh_meridional", getattr(d, "kh_y", 0.0)))
+        if kx == 0.0 and ky == 0.0:
+            return None
+        if kx < 0 or ky < 0:
+            raise ValueError("Kh must be >= 0")
+        return (kx, ky, int(d.seed), int(realization), int(step_i), int(particle_offset))
+
+    def run(self, init_state: ParticleState, n_steps: int, *, start_time: Optional[float] = None,
+            realization_id: int = 0, start_step_i: int = 0, output_freq: int = 1, particle_offset: int = 0,
+            release_step: Optional[np.ndarray] = None, start_wet_streak=None) -> RunResult:
+        """One realization; the result holds one record and final state."""
+        return self.run_realizations(init_state, n_steps, realizations=(realization_id,), start_time=start_time,
+                                     start_step_i=start_step_i, output_freq=output_freq,
+                                     particle_offset=particle_offset, release_step=release_step,
+                                     start_wet_streak=start_wet_streak)
+
+    def run_realizations(self, init_state: ParticleState, n_steps: int, *, realizations: Sequence[int] = (0,),
+                         start_time: Optional[float] = None, start_step_i: int = 0, output_freq: int = 1,
+                         particle_offset: int = 0, release_step: Optional[np.ndarray] = None,
+                         start_wet_streak=None) -> RunResult:
+        """Every realization of ``realizations`` from the same seeds and start
+        time, as one particle array (per-particle realization ids): one record
+        and final state per realization, each as its own run would give."""
+        ctx, mesh = self.ctx, self.mesh
+        R = len(realizations)
+        P = init_state.n_particles
+        ft = self.file_times
+        t0 = float(ft[0] if start_time is None else start_time)
+        band = snapshot_band(self.dt)
+        # resident particles: realization-major copies of the seeds
+        rep = (lambda a: np.concatenate([np.asarray(a)] * R)) if R > 1 else (lambda a: np.asarray(a))
+        fr0 = init_state.failure_reason if init_state.failure_reason is not None else np.zeros(P, np.int8)
+        rs = None
+        if release_step is not None:
+            rs = rep(np.asarray(release_step, dtype=np.int32))
+        elif init_state.release_step is not None:
+            rs = rep(np.asarray(init_state.release_step, dtype=np.int32))
+        ctx.ensure_mesh(mesh)
+        ctx.upload_particles(rep(init_state.lon), rep(init_state.lat), rep(init_state.z), rep(init_state.status),
+                             rep(init_state.nearest_node), rep(fr0), rep(np.arange(P, dtype=np.int64)), rs)
+        if R > 1:
+            ctx.set_realization(np.repeat(np.asarray(realizations, dtype=np.int32), P))
+        beach_cfg = None
+        if self.beaching is not None:
+            seed = int(getattr(self.diffusion, "seed", 0)) if self.diffusion is not None else 0
+            beach_cfg = make_run_config(self.beaching, mesh, diffusion_seed=seed, particle_offset=particle_offset)
+            if beach_cfg.need_topo:
+                ctx.ensure_coastal(mesh, beach_cfg.elem_coastal)
+            ws0 = None if start_wet_streak is None else rep(np.asarray(start_wet_streak, dtype=np.int32))
+            ctx.beach_state_upload(None, ws0)
+        records = [TrajectoryRecord() for _ in range(R)]
+        for r in range(R):
+            records[r].release_lon = np.array(init_state.lon, copy=True)
+            records[r].release_lat = np.array(init_state.lat, copy=True)
+            records[r].release_z = np.array(init_state.z, copy=True)
+        sim_time = t0
+        done = 0
+        for k in range(int(n_steps)):
+            g = start_step_i + k
+            bracket = resolve_time_bracket(sim_time, ft, self.on_exhausted, self.direction, band)
+            if bracket is None:
+                break
+            vel, vnext, dtn = vel_payload(bracket, self.fields, self.direction)
+            kw = dict(self.kw, vel_next=vnext, dt_to_next=dtn)
+            if self.sort_every > 0 and k % self.sort_every == 0:
+                ctx.sort()
+            # step 1 keys: the realization of each particle (its own when R > 1)
+            kick = self._kick(realizations[0], g, particle_offset)
+            a, _ = KI.prepare_step(vel, mesh, self.dt, float(self.direction), self.integrator, kw, ctx, kick=kick)
+            a.global_step = g
+            ctx.step(a)
+            if beach_cfg is not None:
+                ctx.beach(beach_args(beach_cfg, realizations[0], g, self.dt))
+            if dtn is not None and abs(self.dt - dtn) <= band:
+                sim_time = sim_time + dtn * self.direction   # the step ends on the record ahead
+            else:
+                sim_time = sim_time + self.dt * self.direction
+            done += 1
+            if (g + 1) % max(int(output_freq), 1) == 0:
+                s = ctx.download_particles()
+                t_rec = t0 + (g + 1 - start_step_i) * self.dt * self.direction
+                for r in range(R):
+                    sl = slice(r * P, (r + 1) * P)
+                    records[r].append({k2: v[sl] for k2, v in s.items()}, t_rec, self.dims)
+        err = ctx.device_errors()
+        if err:
+            raise N.KcError(N.KC_ERR_DEVICE, N.describe_device_errors(err))
+        s = ctx.download_particles()
+        ws = ctx.beach_state_download() if beach_cfg is not None else None
+        finals, wets = [], []
+        for r in range(R):
+            sl = slice(r * P, (r + 1) * P)
+            finals.append(init_state.replace(lon=s["lon"][sl], lat=s["lat"][sl], z=s["z"][sl],
+                                             status=s["status"][sl], nearest_node=s["nearest_node"][sl],
+                                             failure_reason=s["failure_reason"][sl], u=s["u"][sl], v=s["v"][sl],
+                                             w=s["w"][sl] if self.dims == 3 else None))
+            wets.append(None if ws is None else ws[sl])
+        return RunResult(records=records, final=finals, wet_streak=wets, steps=done)
+
+
+# ---------------------------------------------------------------------------
+# run_tracking: KELP's configuration schema, numerics.backend: cuda
+# ---------------------------------------------------------------------------
+
+
+def _section(cfg, name) -> dict:
+    v = cfg.get(name) if isinstance(cfg, dict) else getattr(cfg, name, None)
+    if v is None:
+        return {}
+    if isinstance(v, dict):
+        return v
+    return {k: getattr(v, k) for k in dir(v) if not k.startswith("_") and not callable(getattr(v, k))}
+
+
+class _Diffusion:
+    def __init__(self, d: dict):
+        self.enabled = bool(d.get("enabled", False))
+        self.scheme = d.get("scheme", "uniform")
+        self.kh_zonal = float(d.get("kh_zonal", 0.0))
+        self.kh_meridional = float(d.get("kh_meridional", 0.0))
+        self.seed = int(d.get("seed", 0))
+        self.composition = d.get("composition", "split")
+        self.az_enabled = bool(d.get("az_enabled", False))
+
+
+def load_config(path_or_dict):
+    """A configuration dict from a YAML path or a dict (KELP's schema)."""
+    if isinstance(path_or_dict, (str, os.PathLike)):
+        import yaml
+        with open(path_or_dict) as fh:
+            return yaml.safe_load(fh) or {}
+    return path_or_dict
+
+
+def load_mesh_npz(path: str):
+    """A mesh from an .npz of KELP Mesh arrays (nodes_lon, nodes_lat, depth,
+    elem_nodes and optionally z_levels): connectivity and the grid hash are
+    built here."""
+    from .mesh import make_mesh
+    d = np.load(path)
+    sigma = d["z_levels"] if "z_levels" in d else None
+    return make_mesh(os.path.basename(path), d["nodes_lon"], d["nodes_lat"], d["depth"], d["elem_nodes"],
+                     sigma=sigma)
+
+
+def load_velocity_npz(path: str):
+    """Snapshot records from an .npz with ``times`` (R,), ``u``, ``v`` (R, N) or
+    (R, L, N) and optionally ``w`` (R, K, N) and ``uv_vertical``."""
+    d = np.load(path)
+    times = d["times"]
+    placement = str(d["uv_vertical"]) if "uv_vertical" in d else "layer"
+    fields = []
+    for r in range(times.size):
+        u, v = d["u"][r], d["v"][r]
+        w = d["w"][r] if "w" in d else None
+        fields.append(VelocityField(u=u, v=v, w=w, eta=np.zeros(u.shape[-1]), uv_layout="node",
+                                    uv_vertical=placement if w is not None else "layer"))
+    return fields, times
+
+
+def load_seeds(path: str):
+    """KELP's seed text file (lon lat [depth] [release_sec] per line, '#'
+    comments) or an .npz with lon, lat[, z, release_sec]."""
+    if path.endswith(".npz"):
+        d = np.load(path)
+        return d["lon"], d["lat"], d.get("z"), d.get("release_sec")
+    rows = [l.split() for l in open(path) if l.strip() and not l.lstrip().startswith("#")]
+    a = np.asarray([[float(x) for x in r] for r in rows])
+    z = a[:, 2] if a.shape[1] > 2 else None
+    rel = a[:, 3] if a.shape[1] > 3 else None
+    return a[:, 0], a[:, 1], z, rel
+
+
+def run_tracking(config, *, mesh=None, fields=None, file_times=None, seeds=None, ctx=None) -> List[TrajectoryRecord]:
+    """Run every realization of a configuration on the GPU (tracking.py:3288).
+
+    ``config``: KELP's schema (dict or YAML path): ``mode`` (Fdrift3D,
+    time_dir), ``numerics`` (backend: cuda, integrator, dt, output_freq,
+    uv_interp, w_interp, temporal_interp, diffusion, beaching, and the
+    backend keywords cuda_precision / cuda_snapshots / sort_every), ``time``
+    (start_time_idx, n_steps, on_exhausted, num_runs, run_interval, n_pulses,
+    pulse_interval).  ``mesh``, ``fields`` + ``file_times`` and ``seeds``
+    ((lon, lat[, z[, release_sec]])) come from the arguments or from the
+    ``data`` section's ``mesh_npz``, ``velocity_npz`` and ``seeds`` paths.
+    Realizations that start together run as one particle array."""
+    cfg = load_config(config)
+    mode, num, tim, data = (_section(cfg, k) for k in ("mode", "numerics", "time", "data"))
+    backend = num.get("backend", "cuda")
+    if backend != "cuda":
+        raise ValueError(f"numerics.backend must be 'cuda' for this package, got {backend!r}")
+    if not num.get("temporal_interp", True):
+        raise NotImplementedError("the CUDA backend runs with temporal_interp: true")
+    if num.get("temporal_reconstruction", "linear") != "linear":
+        raise NotImplementedError("PCHIP temporal reconstruction is not built on the CUDA backend")
+    if num.get("periodic_lon") is not None or num.get("periodic_lat") is not None:
+        raise NotImplementedError("periodic windows are not built on the CUDA backend")
+    if mesh is None:
+        mesh = load_mesh_npz(data["mesh_npz"])
+    if fields is None:
+        fields, file_times = load_velocity_npz(data["velocity_npz"])
+    if seeds is None:
+        seeds = load_seeds(data["seeds"])
+    lon, lat = np.asarray(seeds[0], dtype=np.float64), np.asarray(seeds[1], dtype=np.float64)
+    z = None if len(seeds) < 3 or seeds[2] is None else np.asarray(seeds[2], dtype=np.float64)
+    rel_sec = None if len(seeds) < 4 or seeds[3] is None else np.asarray(seeds[3], dtype=np.float64)
+    dt = float(num["dt"])
+    ft = np.asarray(file_times, dtype=np.float64)
+    direction = 1.0 if float(mode.get("time_dir", 1.0)) > 0 else -1.0
+    # release pulses (TimeConfig n_pulses / pulse_interval) and per-seed release times
+    n_pulses = int(tim.get("n_pulses", 1))
+    pulse = float(tim.get("pulse_interval", 0.0))
+    if n_pulses > 1:
+        lon, lat = np.tile(lon, n_pulses), np.tile(lat, n_pulses)
+        z = None if z is None else np.tile(z, n_pulses)
+        base = np.zeros(lon.size) if rel_sec is None else np.tile(rel_sec, n_pulses)
+        rel_sec = base + np.repeat(np.arange(n_pulses) * pulse, lon.size // n_pulses)
+    state = make_state(lon, lat, z).replace(failure_reason=np.zeros(lon.size, np.int8))
+    release_step = None
+    if rel_sec is not None:
+        release_step = np.ceil(rel_sec / dt - 1e-9).astype(np.int32)
+        state = state.replace(status=np.where(release_step > 0, int(ParticleStatus.NOT_RELEASED),
+                                              int(ParticleStatus.ALIVE)).astype(np.int32))
+    diff = _Diffusion(num.get("diffusion") or {})
+    beach = num.get("beaching") or {}
+    beach_cfg = BeachingConfig(**beach) if beach else None
+    tracker = Tracker(mesh, fields, ft, integrator=num.get("integrator", "rk2"), dt=dt, time_dir=direction,
+                      uv_interp=num.get("uv_interp", "barycentric"), w_interp=num.get("w_interp", "barycentric"),
+                      diffusion=diff if diff.enabled else None, beaching=beach_cfg,
+                      on_exhausted=tim.get("on_exhausted", "stop"),
+                      precision=num.get("cuda_precision", "plain"), snapshots=num.get("cuda_snapshots"),
+                      sort_every=int(num.get("sort_every", 16)), ctx=ctx)
+    start_idx = int(tim.get("start_time_idx", 0))
+    n_steps = tim.get("n_steps")
+    if n_steps is None:
+        end_idx = tim.get("end_time_idx")
+        if end_idx is None:
+            raise ValueError("time.n_steps (or time.end_time_idx) is required")
+        n_steps = int(round((ft[int(end_idx)] - ft[start_idx]) / dt))
+    num_runs = int(tim.get("num_runs", 1))
+    run_interval = int(tim.get("run_interval", 0))
+    output_freq = int(num.get("output_freq", 1))
+    out: List[TrajectoryRecord] = []
+    if run_interval == 0:
+        res = tracker.run_realizations(state, int(n_steps), realizations=list(range(num_runs)),
+                                       start_time=float(ft[start_idx]), output_freq=output_freq,
+                                       release_step=release_step)
+        out.extend(res.records)
+    else:
+        for r in range(num_runs):
+            res = tracker.run(state, int(n_steps), start_time=float(ft[start_idx + r * run_interval]),
+                              realization_id=r, output_freq=output_freq, release_step=release_step)
+            out.extend(res.records)
+    return out

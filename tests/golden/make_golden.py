@@ -329,10 +329,33 @@ def main():
     print("golden_rng")
 
 
+def time_fixture():
+    """The reference's time-bracket resolution (tracking._resolve_time_bracket)
+    on a grid of query times, record axes, modes and directions."""
+    from kelp.tracking import _resolve_time_bracket, _snapshot_band
+    axes = {"uniform": np.arange(5) * 86400.0, "ragged": np.array([0.0, 3600.0, 90000.0, 100000.0, 180000.0])}
+    rows = []
+    for ai, (aname, ft) in enumerate(axes.items()):
+        qs = np.concatenate([ft, ft + 1e-7, ft - 1e-7, np.linspace(-1e5, ft[-1] + 3e5, 57),
+                             ft + 0.2, ft - 0.2])
+        for mi, mode in enumerate(("stop", "cycle")):
+            for d in (1, -1):
+                for snap in (0.0, _snapshot_band(3600.0)):
+                    for q in qs:
+                        b = _resolve_time_bracket(float(q), ft, ft.size, mode, d, cycle=None, snap=snap)
+                        out = [np.nan] * 5 if b is None else [float(x) for x in b]
+                        rows.append([ai, mi, d, snap, q] + out)
+    np.savez_compressed(os.path.join(HERE, "golden_time.npz"), rows=np.array(rows),
+                        axis_uniform=axes["uniform"], axis_ragged=axes["ragged"])
+    print("golden_time", len(rows))
+
+
 if __name__ == "__main__":
     # no argument: every fixture; otherwise the named ones ("steps", "beach")
-    which = set(sys.argv[1:]) or {"steps", "beach"}
+    which = set(sys.argv[1:]) or {"steps", "beach", "time"}
     if "steps" in which:
         main()
     if "beach" in which:
         beach_fixture()
+    if "time" in which:
+        time_fixture()

@@ -1,0 +1,120 @@
+"""The device-resident tracking loop (kelp_b200.tracking) against the
+reference's recorded run and against the per-call API.
+
+The beaching golden was recorded by running the reference's own step and
+beaching hook in the order of its tracking loop; the Tracker, which keeps the
+particles on the GPU, re-sorts them and carries their anchors between steps,
+must end where that run ends (integers bit-exact, positions within the step
+kernels' tolerance).  Several realizations in one array must equal separate
+runs bit for bit, and run_tracking with KELP's configuration schema must equal
+the Tracker it builds.
+"""
+import numpy as np
+import pytest
+
+from kelp_b200 import tracking as T
+from kelp_b200.beaching import BeachingConfig
+
+from test_oracle_golden import beach_kwargs
+
+pytestmark = pytest.mark.gpu
+
+POS_TOL_DEG = 1e-9 / 0.017453292519943295
+
+
+class Diff:
+    enabled = True
+    scheme = "uniform"
+    composition = "split"
+    az_enabled = False
+
+    def __init__(self, kh, seed):
+        self.kh_zonal = self.kh_meridional = kh
+        self.seed = seed
+
+
+def _tracker(g, c, sort_every=5):
+    kw = beach_kwargs(c)
+    dt, Tsnap, n_steps, td, khx, khy, seed, real_id, pid_off = c["params"]
+    cfg = BeachingConfig(enabled=True, criteria=kw["criteria"], depth_min=kw["depth_min"],
+                         zone_depth=kw["zone_depth"], t_beach=kw["t_beach"] or None,
+                         resuspension=kw["resuspension"], rewet_hysteresis=kw["rewet_hysteresis"],
+                         min_wet_steps=kw["min_wet_steps"], t_resuspend=kw["t_resuspend"] or None, seed=kw["seed"])
+    ft = np.arange(len(g.snaps)) * Tsnap
+    diff = Diff(khx, int(seed)) if khx >= 0 else None
+    return T.Tracker(g.mesh, g.snaps, ft, integrator="rk2", dt=dt, diffusion=diff, beaching=cfg,
+                     sort_every=sort_every), int(n_steps)
+
+
+def test_tracker_reproduces_the_reference_run(golden):
+    g = golden("golden_beach")
+    c = g.case("dco_auto")
+    tr, n = _tracker(g, c)
+    res = tr.run(g.particles(), n, output_freq=4)
+    fin = res.final[0]
+    for name in ("status", "nearest_node", "failure_reason"):
+        np.testing.assert_array_equal(getattr(fin, name), c[f"s{n}_{name}"], err_msg=name)
+    np.testing.assert_array_equal(res.wet_streak[0], c[f"s{n}_wet"])
+    for name in ("lon", "lat"):
+        np.testing.assert_allclose(getattr(fin, name), c[f"s{n}_{name}"], rtol=0, atol=POS_TOL_DEG, err_msg=name)
+    rec = res.records[0]
+    assert len(rec.times) == n // 4 and rec.times[-1] == n * c["params"][0]
+    # the record after step 8 is the reference's state after step 8
+    np.testing.assert_array_equal(rec.status[1], c["s8_status"])
+    np.testing.assert_allclose(rec.lons[1], c["s8_lon"], rtol=0, atol=POS_TOL_DEG)
+
+
+def test_realizations_in_one_array_equal_separate_runs(golden):
+    g = golden("golden_beach")
+    c = g.case("sto_both")
+    tr, n = _tracker(g, c)
+    st = g.particles()
+    together = tr.run_realizations(st, n, realizations=(0, 1, 2), output_freq=8)
+    for r in range(3):
+        alone = tr.run(st, n, realization_id=r, output_freq=8)
+        for name in ("lon", "lat", "status", "nearest_node", "failure_reason"):
+            np.testing.assert_array_equal(getattr(together.final[r], name), getattr(alone.final[0], name),
+                                          err_msg=f"realization {r} {name}")
+        np.testing.assert_array_equal(together.wet_streak[r], alone.wet_streak[0])
+        np.testing.assert_array_equal(np.stack(together.records[r].lons), np.stack(alone.records[0].lons))
+    # the members differ: their draws are their own
+    assert not np.array_equal(together.final[0].lon, together.final[1].lon)
+
+
+def test_run_tracking_config_equals_tracker(golden, tmp_path):
+    g = golden("golden_beach")
+    c = g.case("cd_sresusp")
+    dt, Tsnap, n_steps, td, khx, khy, seed, real_id, pid_off = c["params"]
+    kw = beach_kwargs(c)
+    m = g.mesh
+    np.savez(tmp_path / "mesh.npz", nodes_lon=m.nodes_lon, nodes_lat=m.nodes_lat, depth=m.depth,
+             elem_nodes=m.elem_nodes)
+    np.savez(tmp_path / "vel.npz", times=np.arange(len(g.snaps)) * Tsnap,
+             u=np.stack([np.asarray(s.u) for s in g.snaps]), v=np.stack([np.asarray(s.v) for s in g.snaps]))
+    st = g.particles()
+    np.savez(tmp_path / "seeds.npz", lon=st.lon, lat=st.lat)
+    cfg = {"mode": {"time_dir": 1.0},
+           "numerics": {"backend": "cuda", "integrator": "rk2", "dt": float(dt), "output_freq": 4,
+                        "uv_interp": "barycentric", "temporal_interp": True,
+                        "diffusion": {"enabled": True, "scheme": "uniform", "kh_zonal": float(khx),
+                                      "kh_meridional": float(khy), "seed": int(seed)},
+                        "beaching": {"enabled": True, "criteria": kw["criteria"], "depth_min": kw["depth_min"],
+                                     "resuspension": kw["resuspension"], "t_resuspend": kw["t_resuspend"],
+                                     "rewet_hysteresis": kw["rewet_hysteresis"]}},
+           "time": {"start_time_idx": 0, "n_steps": int(n_steps), "num_runs": 2},
+           "data": {"mesh_npz": str(tmp_path / "mesh.npz"), "velocity_npz": str(tmp_path / "vel.npz"),
+                    "seeds": str(tmp_path / "seeds.npz")}}
+    recs = T.run_tracking(cfg)
+    assert len(recs) == 2
+    # the same run through a Tracker on the golden's own mesh object
+    diff = Diff(khx, int(seed))
+    bcfg = BeachingConfig(enabled=True, criteria=kw["criteria"], depth_min=kw["depth_min"],
+                          resuspension=kw["resuspension"], t_resuspend=kw["t_resuspend"],
+                          rewet_hysteresis=kw["rewet_hysteresis"])
+    tr = T.Tracker(g.mesh, g.snaps, np.arange(len(g.snaps)) * Tsnap, integrator="rk2", dt=dt, diffusion=diff,
+                   beaching=bcfg)
+    alive = st.replace(status=np.ones(st.n_particles, np.int32))   # the seed file carries positions only
+    for r in range(2):
+        res = tr.run(alive, int(n_steps), realization_id=r, output_freq=4)
+        np.testing.assert_array_equal(np.stack(recs[r].status), np.stack(res.records[0].status))
+        np.testing.assert_array_equal(np.stack(recs[r].lons), np.stack(res.records[0].lons))
