@@ -90,3 +90,10 @@ class LazyLerpField:
     @property
     def eta(self):
         return self._blend("eta")
+
+    @property
+    def az(self):
+        """The blended vertical diffusivity, None unless both snapshots carry one."""
+        if getattr(self.vel_a, "az", None) is None or getattr(self.vel_b, "az", None) is None:
+            return None
+        return self._blend("az")

@@ -49,6 +49,7 @@ typedef struct {
     int f32;
     double alpha0;
     int64_t n;
+    const void *aza, *azb;   /* vertical diffusivity (K, N) of the bracket pair, or NULL */
 } OField;
 
 static double fld(const void* p, int f32, int64_t i) {
@@ -717,6 +718,8 @@ typedef struct {
     double dt, td, ak[4], kh_x, kh_y;
     uint64_t seed, real_id, step_i, pid_offset;
     int uv_dl;
+    int az_on, az_field;   /* vertical Az kick; Az from the snapshots' (K, N) az arrays */
+    double az_const;
 } OStep;
 
 /* vertical_uv.py:457-523 uv_bracket */
@@ -832,6 +835,84 @@ static double z0_of(double lat) {
     return z0 < 1.0 ? 1.0 : z0;
 }
 static double clat(double x) { return x > 90.0 ? 90.0 : (x < -90.0 ? -90.0 : x); }
+
+
+/* diffusion.py:333-352 reflect_depth: specular fold into [top, bot] */
+static double reflect_depth(double z, double top, double bot) {
+    double L = bot - top;
+    if (L <= 0.0) return top;
+    double y = pymod(z - top, 2.0 * L);   /* 2L > 0: the positive-divisor fold */
+    if (y < 0.0) y += 2.0 * L;
+    if (y > L) y = 2.0 * L - y;
+    return top + y;
+}
+
+/* the payload's Az at interface k of node (io.py:68-117 blend of the pair) */
+static double az_at(const OField* f, int k, int node) {
+    int64_t idx = (int64_t)k * f->n + node;
+    double a = fld(f->aza, f->f32, idx);
+    if (f->alpha0 == 0.0) return a;
+    double b = fld(f->azb, f->f32, idx);
+    return (1.0 - f->alpha0) * a + f->alpha0 * b;
+}
+
+/* diffusion.py:357-423 _az_interp_column + az_column_value_gradient */
+static void az_column(const OMesh* m, const OField* f, int node, double z, double node_bottom, double* az,
+                      double* g) {
+    int K = m->K;
+    const double* zl = m->zlev;
+    double top = zl[0];
+    double bot = node_bottom < zl[K - 1] ? node_bottom : zl[K - 1];
+    if (bot < top) bot = top;
+    double ze = z;
+    if (ze < top) ze = top;
+    if (ze > bot) ze = bot;
+    double val;
+    if (K < 2 || ze <= zl[0]) val = az_at(f, 0, node);
+    else if (ze >= zl[K - 1]) val = az_at(f, K - 1, node);
+    else {
+        val = az_at(f, K - 1, node);
+        for (int k = 0; k < K - 1; ++k)
+            if (ze <= zl[k + 1]) {
+                double dzl = zl[k + 1] - zl[k];
+                if (dzl <= 0.0) { val = az_at(f, k, node); break; }
+                double frac = (ze - zl[k]) / dzl;
+                val = (1.0 - frac) * az_at(f, k, node) + frac * az_at(f, k + 1, node);
+                break;
+            }
+    }
+    *az = val;
+    *g = 0.0;
+    if (K < 2) return;
+    int k = K - 2;
+    for (int kk = 0; kk < K - 1; ++kk)
+        if (ze <= zl[kk + 1]) { k = kk; break; }
+    double dz = zl[k + 1] - zl[k];
+    if (dz <= 0.0) return;
+    if (f->f32 && f->alpha0 == 0.0) {
+        /* an unblended float32 snapshot: the difference of two float32
+           values rounds in float32 before the float64 division */
+        float d = (float)az_at(f, k + 1, node) - (float)az_at(f, k, node);
+        *g = (double)d / dz;
+    } else {
+        *g = (az_at(f, k + 1, node) - az_at(f, k, node)) / dz;
+    }
+}
+
+/* integrators.py:842-938 _apply_split_az_kick with diffusion.py:302-330
+ * diffusion_az_step_meters and :426-455 _loop_az_kick_zlevel, one particle */
+static void az_kick(const OMesh* m, const OField* f, const OStep* s, int64_t pid, int nn, double* z) {
+    double az, g;
+    if (s->az_field) az_column(m, f, nn, *z, m->depth[nn], &az, &g);
+    else { az = s->az_const; g = 0.0; }
+    if (az < 0.0) { az = 0.0; g = 0.0; }
+    double xi[2];
+    orc_normal_pair(s->seed, s->real_id, (uint64_t)pid + s->pid_offset, s->step_i, 1, xi);
+    double sdt = s->td * s->dt;
+    double abs_dt = sdt >= 0.0 ? sdt : -sdt;
+    double dz = g * abs_dt + sqrt(2.0 * az * abs_dt) * xi[0];
+    *z = reflect_depth(*z + dz, m->zlev[0], m->depth[nn]);
+}
 
 /* integrators.py:673-818 for one surviving particle */
 static void kick(const OMesh* m, const OStep* s, int64_t pid, double pre_lon, double pre_lat, double pre_z, int pre_nn,
@@ -1016,6 +1097,7 @@ static void step_one(const OMesh* m, const OField* f, const OStep* s, int64_t i,
     }
     if (s->kick && st == ALIVE)
         kick(m, s, pid ? pid[i] : i, lon0, lat0, zp, pre_nn, &ln, &lt, &zn, &st, &nno, &frr, s->dims == 3);
+    if (s->az_on && st == ALIVE && s->dims == 3) az_kick(m, f, s, pid ? pid[i] : i, nno, &zn);
     lon[i] = ln; lat[i] = lt;
     if (z) z[i] = zn;
     status[i] = st; nn[i] = nno; fr[i] = frr;
@@ -1092,6 +1174,7 @@ typedef struct {
     int f32;
     double alpha0;
     int64_t n;
+    const void *aza, *azb;
 } orc_field;
 
 typedef struct {
@@ -1099,6 +1182,8 @@ typedef struct {
     double dt, td, ak[4], kh_x, kh_y;
     uint64_t seed, real_id, step_i, pid_offset;
     int uv_dl;
+    int az_on, az_field;
+    double az_const;
 } orc_step_args;
 
 typedef struct {

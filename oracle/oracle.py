@@ -34,7 +34,8 @@ class OField(C.Structure):
     _fields_ = [("ua", C.c_void_p), ("va", C.c_void_p), ("wa", C.c_void_p),
                 ("ub", C.c_void_p), ("vb", C.c_void_p), ("wb", C.c_void_p),
                 ("ut", C.c_void_p), ("vt", C.c_void_p), ("wt", C.c_void_p),
-                ("f32", C.c_int), ("alpha0", C.c_double), ("n", C.c_int64)]
+                ("f32", C.c_int), ("alpha0", C.c_double), ("n", C.c_int64),
+                ("aza", C.c_void_p), ("azb", C.c_void_p)]
 
 
 class OStep(C.Structure):
@@ -42,7 +43,8 @@ class OStep(C.Structure):
                 ("dt", C.c_double), ("td", C.c_double), ("ak", C.c_double * 4),
                 ("kh_x", C.c_double), ("kh_y", C.c_double),
                 ("seed", C.c_uint64), ("real_id", C.c_uint64), ("step_i", C.c_uint64),
-                ("pid_offset", C.c_uint64), ("uv_dl", C.c_int)]
+                ("pid_offset", C.c_uint64), ("uv_dl", C.c_int),
+                ("az_on", C.c_int), ("az_field", C.c_int), ("az_const", C.c_double)]
 
 
 _lib = None
@@ -160,7 +162,8 @@ def step(state, vel, mesh, dt, time_dir, scheme: str, *, vel_next=None, dt_to_ne
     target = vel_next if vel_next is not None else vel_a
     flds = [vel_a, vel_b, target]
     all32 = all(np.asarray(f.u).dtype == np.float32 and np.asarray(f.v).dtype == np.float32
-                and (f.w is None or np.asarray(f.w).dtype == np.float32) for f in flds)
+                and (f.w is None or np.asarray(f.w).dtype == np.float32)
+                and (getattr(f, "az", None) is None or np.asarray(f.az).dtype == np.float32) for f in flds)
     dtype = np.float32 if all32 else np.float64
     arrs = [_field_arrays(f, dtype) for f in flds]
     of = OField()
@@ -182,11 +185,30 @@ def step(state, vel, mesh, dt, time_dir, scheme: str, *, vel_next=None, dt_to_ne
         for k, c in enumerate(cc):
             os_.ak[k] = float(c) * float(dt) / float(dt_to_next)
     os_.dt, os_.td = float(dt), float(time_dir)
+    if diffusion is not None:
+        os_.seed, os_.real_id, os_.step_i = int(diffusion.seed), int(diffusion.real_id), int(diffusion.step_i)
+        os_.pid_offset = int(getattr(diffusion, "pid_offset", 0))
     if diffusion is not None and not (float(diffusion.kh_x) == 0.0 and float(diffusion.kh_y) == 0.0):
         os_.kick = 1
         os_.kh_x, os_.kh_y = float(diffusion.kh_x), float(diffusion.kh_y)
-        os_.seed, os_.real_id, os_.step_i = int(diffusion.seed), int(diffusion.real_id), int(diffusion.step_i)
-        os_.pid_offset = int(getattr(diffusion, "pid_offset", 0))
+    keep_az = []
+    if diffusion is not None and getattr(diffusion, "az_enabled", False):
+        # integrators.py:842-938: the payload's Az field, else the constant
+        az_a = getattr(vel_a, "az", None)
+        az_b = getattr(vel_b, "az", None) if hasattr(vel, "vel_a") else az_a
+        have = az_a is not None and az_b is not None
+        az_const = max(float(getattr(diffusion, "az_const", 0.0)), 0.0)
+        if not have and getattr(diffusion, "az_requires_field", False):
+            raise ValueError("diffusion.var_az is configured but the payload carries no az field")
+        if have or az_const != 0.0:
+            if not is3d:
+                raise ValueError("diffusion.az_enabled requires a 3-D run")
+            os_.az_on = 1
+            os_.az_const = az_const
+            if have:
+                os_.az_field = 1
+                keep_az = [np.ascontiguousarray(az_a, dtype=dtype), np.ascontiguousarray(az_b, dtype=dtype)]
+                of.aza, of.azb = _p(keep_az[0]), _p(keep_az[1])
     P = state.lon.shape[0]
     out = {"lon": np.array(state.lon, dtype=np.float64), "lat": np.array(state.lat, dtype=np.float64),
            "z": np.array(state.z, dtype=np.float64), "status": np.array(state.status, dtype=np.int32),

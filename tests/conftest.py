@@ -51,7 +51,8 @@ class Golden:
             w = self.d.get(f"snap{i}_w")
             self.snaps.append(VelocityField(u=self.d[f"snap{i}_u"], v=self.d[f"snap{i}_v"], w=w,
                                             eta=np.zeros(self.d[f"snap{i}_u"].shape[-1]), uv_layout="node",
-                                            uv_vertical=placement if w is not None else "layer"))
+                                            uv_vertical=placement if w is not None else "layer",
+                                            az=self.d.get(f"snap{i}_az")))
             i += 1
 
     def cases(self):

@@ -65,7 +65,7 @@ def mesh_record(rm):
 
 def ref_fields(snaps):
     return [RVel(u=s.u, v=s.v, w=s.w, eta=np.zeros(s.u.shape[-1]), uv_layout="node",
-                 uv_vertical="layer") for s in snaps]
+                 uv_vertical="layer", az=getattr(s, "az", None)) for s in snaps]
 
 
 def payload(fields, t, T):
@@ -79,7 +79,7 @@ def payload(fields, t, T):
 
 
 def run_case(rm, fields, lon, lat, z, status, scheme, dt, T, n_steps, *, time_dir=1.0, w_interp="nearest",
-             kh=None, seed=7, real_id=0, pid_offset=0, record=(1,)):
+             kh=None, seed=7, real_id=0, pid_offset=0, record=(1,), az=None):
     fn = {"rk2": RI.rk2_step, "rk4": RI.rk4_step, "euler": RI.euler_step}[scheme]
     P = lon.size
     st = RState(lon=lon.copy(), lat=lat.copy(), z=z.copy(), status=status.copy(),
@@ -92,7 +92,7 @@ def run_case(rm, fields, lon, lat, z, status, scheme, dt, T, n_steps, *, time_di
         kw = dict(uv_interp="barycentric", w_interp=w_interp, vel_next=vnext, dt_to_next=dtn)
         if kh is not None:
             kw["diffusion"] = RDiff(scheme="uniform", kh_x=kh[0], kh_y=kh[1], seed=seed, real_id=real_id,
-                                    step_i=k, pid_offset=pid_offset)
+                                    step_i=k, pid_offset=pid_offset, **(az or {}))
         sched.append([ia, alpha, dtn])
         st = fn(st, vel, rm, dt, time_dir, **kw)
         if (k + 1) in record or k + 1 == n_steps:
@@ -104,6 +104,8 @@ def run_case(rm, fields, lon, lat, z, status, scheme, dt, T, n_steps, *, time_di
     out["schedule"] = np.array(sched, dtype=np.float64)
     out["params"] = np.array([dt, T, n_steps, time_dir, -1 if kh is None else kh[0], -1 if kh is None else kh[1],
                               seed, real_id, pid_offset], dtype=np.float64)
+    if az:
+        out["az"] = np.array([float(az.get("az_const", 0.0)), float(az.get("az_requires_field", False))])
     return out
 
 
@@ -212,6 +214,8 @@ def save(name, mesh_rec, snaps, cases, parts):
         d[f"snap{i}_v"] = s.v
         if s.w is not None:
             d[f"snap{i}_w"] = s.w
+        if getattr(s, "az", None) is not None:
+            d[f"snap{i}_az"] = s.az
     for k, v in parts.items():
         d[f"p_{k}"] = v
     for cname, c in cases.items():
@@ -283,6 +287,9 @@ def main():
                        depth=lambda lo, la: S.smooth_bathymetry(lo, la, 30.0, 4000.0), sigma=zl)
     rm = ref_mesh(m, sigma=zl)
     snaps = S.gyre_snapshots(m, 4, amp=1.5, z_levels=zl, decay=800.0, w_scale=2e-3)
+    for k, sn in enumerate(snaps):   # a vertical diffusivity on the interfaces (K, N) for the Az kick
+        sn.az = ((1e-2 * (1.0 + 0.2 * k)) * np.exp(-np.asarray(zl)[:, None] / 300.0)
+                 * (1.0 + 0.5 * np.sin(np.radians(3.0 * np.asarray(m.nodes_lon))))[None, :] + 1e-4).astype(np.float32)
     rf = ref_fields(snaps)
     lon, lat, z, status = particles(m, 1200, 13, z=True, n_dead=20)
     cases = {"rk2_wnear": run_case(rm, rf, lon, lat, z, status, "rk2", 21600.0, T, 12, w_interp="nearest"),
@@ -293,7 +300,15 @@ def main():
              "rk4_wnear": run_case(rm, rf, lon, lat, z, status, "rk4", 21600.0, T, 12, w_interp="nearest"),
              "rk4_wbary_kick": run_case(rm, rf, lon, lat, z, status, "rk4", 21600.0, T, 12,
                                         w_interp="barycentric", kh=(3.0e4, 1.0e4), seed=9),
-             "euler_wbary": run_case(rm, rf, lon, lat, z, status, "euler", 10800.0, T, 16, w_interp="barycentric")}
+             "euler_wbary": run_case(rm, rf, lon, lat, z, status, "euler", 10800.0, T, 16, w_interp="barycentric"),
+             # the vertical Az kick: the snapshots' Az field with the split
+             # horizontal kick, and a constant Az alone (Kh = 0)
+             "rk2_wbary_kick_azf": run_case(rm, rf, lon, lat, z, status, "rk2", 21600.0, T, 12,
+                                            w_interp="barycentric", kh=(3.0e4, 3.0e4), seed=6,
+                                            az=dict(az_enabled=True, az_requires_field=True)),
+             "rk4_wnear_azf_nokh": run_case(rm, rf, lon, lat, z, status, "rk4", 21600.0, T, 10,
+                                            w_interp="nearest", kh=(0.0, 0.0), seed=8,
+                                            az=dict(az_enabled=True, az_const=5e-3))}
     save("golden_3d", mesh_record(rm), snaps, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
 
     # --- depth-linear u/v (uv_vertical level / layer_linear) on the same mesh;
@@ -312,6 +327,10 @@ def main():
                                                   w_interp="nearest", kh=(2.0e4, 2.0e4), seed=4)
         cases[f"euler_{tag}_wnear"] = run_case(rm, rfp, lon, lat, zdl, status, "euler", 10800.0, T, 8,
                                                w_interp="nearest")
+        if tag == "lev":   # snapshots without Az: the constant source
+            cases["rk2_lev_wbary_azc"] = run_case(rm, rfp, lon, lat, zdl, status, "rk2", 21600.0, T, 10,
+                                                  w_interp="barycentric", kh=(2.0e4, 2.0e4), seed=3,
+                                                  az=dict(az_enabled=True, az_const=2e-3))
         save(f"golden_dl_{tag}", mesh_record(rm), sn, {k: v for k, v in cases.items() if f"_{tag}_" in k},
              {"lon": lon, "lat": lat, "z": zdl, "status": status})
 

@@ -17,9 +17,21 @@ from kelp_b200.diffusion import DiffusionStepArgs
 CASES = [("golden_band", c) for c in ("rk2", "rk4", "euler", "rk2_bwd", "rk2_kick", "rk4_kick_aniso", "rk2_dt4800")]
 CASES += [("golden_quad", c) for c in ("rk2", "rk4", "euler", "rk2_kick")]
 CASES += [("golden_polar", "rk2")]
-CASES += [("golden_3d", c) for c in ("rk2_wnear", "rk2_wbary", "rk2_wbary_kick", "rk4_wnear", "rk4_wbary_kick", "euler_wbary")]
-CASES += [("golden_dl_lev", c) for c in ("rk2_lev_wbary", "rk4_lev_wnear_kick", "euler_lev_wnear")]
+CASES += [("golden_3d", c) for c in ("rk2_wnear", "rk2_wbary", "rk2_wbary_kick", "rk4_wnear", "rk4_wbary_kick", "euler_wbary",
+                                     "rk2_wbary_kick_azf", "rk4_wnear_azf_nokh")]
+CASES += [("golden_dl_lev", c) for c in ("rk2_lev_wbary", "rk4_lev_wnear_kick", "euler_lev_wnear", "rk2_lev_wbary_azc")]
 CASES += [("golden_dl_llin", c) for c in ("rk2_llin_wbary", "rk4_llin_wnear_kick", "euler_llin_wnear")]
+
+
+def diffusion_args(c, k):
+    """The recorded case's DiffusionStepArgs of step k (None without diffusion)."""
+    dt, T, n_steps, td, khx, khy, seed, real_id, pid_off = c["params"]
+    if khx < 0:
+        return None
+    az = {}
+    if "az" in c:
+        az = dict(az_enabled=True, az_const=float(c["az"][0]), az_requires_field=bool(c["az"][1]))
+    return DiffusionStepArgs("uniform", khx, khy, int(seed), int(real_id), k, pid_offset=int(pid_off), **az)
 
 
 def replay_oracle(g, cname):
@@ -32,9 +44,7 @@ def replay_oracle(g, cname):
     snaps = {}
     for k in range(int(n_steps)):
         vel, vnext, dtn = g.payload(c["schedule"][k], T)
-        diff = None
-        if khx >= 0:
-            diff = DiffusionStepArgs("uniform", khx, khy, int(seed), int(real_id), k, pid_offset=int(pid_off))
+        diff = diffusion_args(c, k)
         out = O.step(st, vel, g.mesh, dt, td, scheme, vel_next=vnext, dt_to_next=dtn, w_interp=w_interp,
                      diffusion=diff, view=view)
         st = st.replace(lon=out["lon"], lat=out["lat"], z=out["z"], status=out["status"],
