@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define KC_ABI_VERSION 2
+#define KC_ABI_VERSION 3
 
 #define KC_OK 0
 #define KC_ERR_ARG 1      /* invalid argument or combination */
@@ -94,6 +94,9 @@ typedef struct kc_step_args {
     unsigned long long seed, real_id, step_i, pid_offset;
     long long global_step;       /* delayed-release activation step, -1 for none */
     int precision;               /* KC_PLAIN (snapshots F32/F64) or KC_MIXED (snapshots F32/F16) */
+    int az_kick;                 /* vertical Az kick after the step (3-D; diffusion.az_enabled) */
+    int az_field;                /* Az from the bracket slots' az rows (kc_field_upload_az), else az_const */
+    double az_const;             /* m^2/s, >= 0 */
 } kc_step_args;
 
 /* Beaching / resuspension of one step (src/kelp/tracking.py:199-364,
@@ -131,6 +134,12 @@ int kc_depth_points_upload(kc_ctx* ctx, int M, const double* p, const int* last,
  * scaled by a power of two so that its largest magnitude is below 2^15. */
 int kc_field_upload(kc_ctx* ctx, int slot, int dtype, long long n_nodes, int n_uv_rows,
                     const void* u, const void* v, int n_w_rows, const void* w);
+
+/* The vertical diffusivity of the snapshot in ring slot `slot`: n_rows (= the
+ * mesh's interfaces K) x n_nodes values of the slot's element type (float32
+ * or float64; io.py VelocityField.az).  Uploading a new snapshot into the
+ * slot drops it. */
+int kc_field_upload_az(kc_ctx* ctx, int slot, int dtype, long long n_nodes, int n_rows, const void* az);
 
 /* Particle state.  Optional pointers may be NULL (z: zeros, fr: zeros,
  * pid: the index, release_step: all released). */

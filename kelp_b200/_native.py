@@ -17,12 +17,12 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libkelpcuda
 KC_OK, KC_ERR_ARG, KC_ERR_CUDA, KC_ERR_STATE, KC_ERR_DEVICE = 0, 1, 2, 3, 4
 KC_F32, KC_F64, KC_F16 = 0, 1, 2
 KC_PLAIN, KC_MIXED = 0, 1
-ABI_VERSION = 2
+ABI_VERSION = 3
 KC_EULER, KC_RK2, KC_RK4 = 0, 1, 2
 
 #: every symbol include/kelp_cuda.h declares
 EXPORTS = ("kc_abi_version", "kc_node_xyz_fill", "kc_create", "kc_destroy", "kc_last_error",
-           "kc_synchronize", "kc_mesh_upload", "kc_depth_points_upload", "kc_field_upload", "kc_particles_upload",
+           "kc_synchronize", "kc_mesh_upload", "kc_depth_points_upload", "kc_field_upload", "kc_particles_upload", "kc_field_upload_az",
            "kc_particles_download", "kc_coastal_upload", "kc_beach_state_upload",
            "kc_beach_state_download", "kc_beach", "kc_step", "kc_step_host", "kc_step_range", "kc_run_fused",
            "kc_particles_set_realization", "kc_set_fused_block", "kc_run", "kc_sort", "kc_find_nearest", "kc_find_nearest_noalloc", "kc_rng_normals", "kc_device_errors",
@@ -72,7 +72,8 @@ class StepArgs(C.Structure):
                 ("kh_x", C.c_double), ("kh_y", C.c_double),
                 ("seed", C.c_ulonglong), ("real_id", C.c_ulonglong),
                 ("step_i", C.c_ulonglong), ("pid_offset", C.c_ulonglong),
-                ("global_step", C.c_longlong), ("precision", C.c_int)]
+                ("global_step", C.c_longlong), ("precision", C.c_int),
+                ("az_kick", C.c_int), ("az_field", C.c_int), ("az_const", C.c_double)]
 
 
 class BeachArgs(C.Structure):
@@ -113,6 +114,7 @@ def lib():
         L.kc_mesh_upload.argtypes = [vp, C.POINTER(MeshDesc)]
         L.kc_field_upload.argtypes = [vp, i, i, ll, i, vp, vp, i, vp]
         L.kc_depth_points_upload.argtypes = [vp, i, vp, vp, vp]
+        L.kc_field_upload_az.argtypes = [vp, i, i, ll, i, vp]
         L.kc_particles_upload.argtypes = [vp, ll, vp, vp, vp, vp, vp, vp, vp, vp]
         L.kc_particles_download.argtypes = [vp, ll, vp, vp, vp, vp, vp, vp, vp, vp, vp]
         L.kc_coastal_upload.argtypes = [vp, vp]

@@ -28,6 +28,9 @@ struct Slot {
     void* u = nullptr;
     void* v = nullptr;
     void* w = nullptr;
+    void* az = nullptr;    // vertical diffusivity rows (K, N), same element type as u
+    int az_rows = 0;
+    size_t cap_az = 0;
     float* su = nullptr;   // per-row scales of half storage
     float* sv = nullptr;
     float* sw = nullptr;
@@ -140,7 +143,8 @@ void dfree(P*& p) {
 
 template <typename T>
 kc::DField<T> field_of(const Slot& s) {
-    return kc::DField<T>{(const T*)s.u, (const T*)s.v, (const T*)s.w, s.su, s.sv, s.sw};
+    return kc::DField<T>{(const T*)s.u, (const T*)s.v, (const T*)s.w, s.su, s.sv, s.sw,
+                         s.az_rows > 0 ? (const T*)s.az : nullptr};
 }
 
 kc::DState state_of(kc_ctx* c) {
@@ -164,6 +168,7 @@ kc::DStep step_of(const kc_step_args* a) {
     s.kh_x = a->kh_x; s.kh_y = a->kh_y;
     s.seed = a->seed; s.real_id = a->real_id; s.step_i = a->step_i; s.pid_offset = a->pid_offset;
     s.global_step = a->global_step;
+    s.az_on = a->az_kick; s.az_field = a->az_field; s.az_const = a->az_const;
     return s;
 }
 
@@ -351,6 +356,18 @@ int check_step(kc_ctx* c, const kc_step_args* a) {
     if (a->kick && !(a->kh_x >= 0.0 && a->kh_y >= 0.0)) return fail(c, KC_ERR_ARG, "kc_step: Kh must be >= 0");
     if (a->precision != KC_PLAIN && a->precision != KC_MIXED)
         return fail(c, KC_ERR_ARG, "kc_step: precision must be KC_PLAIN or KC_MIXED");
+    if (a->az_kick) {
+        if (a->dims != 3) return fail(c, KC_ERR_ARG, "kc_step: the Az kick needs a 3-D step");
+        if (!(a->az_const >= 0.0)) return fail(c, KC_ERR_ARG, "kc_step: az_const must be >= 0");
+        if (a->az_field) {
+            const int need[2] = {a->slot_a, a->alpha0 != 0.0 ? a->slot_b : a->slot_a};
+            for (int k = 0; k < 2; ++k) {
+                if (need[k] < 0 || need[k] >= kSlots) return fail(c, KC_ERR_ARG, "kc_step: slot out of range");
+                if (c->slots[need[k]].az_rows != c->dm.K)
+                    return fail(c, KC_ERR_STATE, "kc_step: the Az field needs (K, N) az rows in the bracket slots");
+            }
+        }
+    }
     int sl[3] = {a->slot_a, a->slot_b, a->slot_t};
     int dtype = -1;
     for (int k = 0; k < 3; ++k) {
@@ -446,7 +463,9 @@ void kc_destroy(kc_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     free_mesh(c);
     free_particles(c);
-    for (auto& s : c->slots) { dfree(s.u); dfree(s.v); dfree(s.w); dfree(s.su); dfree(s.sv); dfree(s.sw); }
+    for (auto& s : c->slots) {
+        dfree(s.u); dfree(s.v); dfree(s.w); dfree(s.su); dfree(s.sv); dfree(s.sw); dfree(s.az);
+    }
     dfree(c->q); dfree(c->qout); dfree(c->d_err); dfree(c->flush); dfree(c->stage);
     for (int k = 0; k < kEvents; ++k) if (c->ev[k]) cudaEventDestroy(c->ev[k]);
     for (int k = 0; k < kChunks; ++k) {
@@ -742,6 +761,7 @@ int kc_field_upload(kc_ctx* c, int slot, int dtype, long long n_nodes, int n_uv_
         if (nw) KC_CUDA(c, cudaMemcpyAsync(s.w, w, nw, cudaMemcpyHostToDevice, c->stream));
     }
     s.n = n_nodes; s.uv_rows = n_uv_rows; s.w_rows = n_w_rows > 0 ? n_w_rows : 0; s.dtype = dtype;
+    s.az_rows = 0;   // a new snapshot carries no Az until kc_field_upload_az
     return KC_OK;
 }
 
@@ -764,6 +784,27 @@ static int ensure_capacity(kc_ctx* c, long long P) {
     KC_CUDA(c, cudaMalloc((void**)&c->prev, n)); KC_CUDA(c, cudaMalloc((void**)&c->wet, n));
     KC_CUDA(c, cudaMalloc((void**)&c->nn_ok, n));
     c->cap = P;
+    return KC_OK;
+}
+
+int kc_field_upload_az(kc_ctx* c, int slot, int dtype, long long n_nodes, int n_rows, const void* az) {
+    if (!c) return KC_ERR_ARG;
+    if (slot < 0 || slot >= kSlots) return fail(c, KC_ERR_ARG, "kc_field_upload_az: slot out of range");
+    Slot& s = c->slots[slot];
+    if (s.dtype < 0) return fail(c, KC_ERR_STATE, "kc_field_upload_az: upload the snapshot first");
+    if (dtype != s.dtype || dtype == KC_F16)
+        return fail(c, KC_ERR_ARG, "kc_field_upload_az: Az takes the snapshot's element type, float32 or float64");
+    if (n_nodes != s.n || n_rows <= 0 || !az) return fail(c, KC_ERR_ARG, "kc_field_upload_az: shape");
+    KC_CUDA(c, cudaSetDevice(c->device));
+    const size_t bytes = (size_t)n_nodes * n_rows * (dtype == KC_F32 ? 4 : 8);
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (s.cap_az < bytes) {
+        dfree(s.az);
+        KC_CUDA(c, cudaMalloc(&s.az, bytes));
+        s.cap_az = bytes;
+    }
+    KC_CUDA(c, cudaMemcpyAsync(s.az, az, bytes, cudaMemcpyHostToDevice, c->stream));
+    s.az_rows = n_rows;
     return KC_OK;
 }
 

@@ -18,6 +18,7 @@ struct DField {
     const float* su;
     const float* sv;
     const float* sw;
+    const T* az;     // vertical diffusivity (K, N) on the interfaces, or null
 };
 
 template <typename T>

@@ -7,6 +7,7 @@
 // and interpolation are shared (non-inlined) device functions, which keeps
 // the kernel's code footprint small under divergence.
 #pragma once
+#include <type_traits>
 #include "kc_interp.cuh"
 
 namespace kc {
@@ -39,6 +40,8 @@ struct DStep {
     double kh_x, kh_y;
     unsigned long long seed, real_id, step_i, pid_offset;
     long long global_step;     // for delayed release activation (-1: none)
+    int az_on, az_field;       // vertical Az kick; Az from the snapshots' (K, N) az rows
+    double az_const;
 };
 
 // displacement metric z0 = max(cos(lat) * 111120, 1) (integrators.py:2563-2565),
@@ -126,6 +129,103 @@ static __device__ __noinline__ void apply_kick(const DMesh& m, const DStep& s, l
         if (zv > bottom) zv = bottom;
         z = zv;
     }
+}
+
+// diffusion.py:333-352 reflect_depth: specular fold into [top, bot] (Python's
+// float % for the positive divisor 2L).
+__device__ __forceinline__ double reflect_depth(double z, double top, double bot) {
+    const double L = bot - top;
+    if (L <= 0.0) return top;
+    const double L2 = 2.0 * L;
+    double y = fmod(z - top, L2);
+    if (y != 0.0) {
+        if (y < 0.0) y += L2;
+    } else {
+        y = 0.0;
+    }
+    if (y < 0.0) y += L2;
+    if (y > L) y = L2 - y;
+    return top + y;
+}
+
+// The payload's Az at interface k of node: the step-start field, a single
+// snapshot or the pair blended at alpha0 (io.py:68-117).
+template <typename T>
+__device__ __forceinline__ double az_at(const DBlend<T>& f, int k, int node) {
+    const long long idx = (long long)k * f.n + node;
+    const double a = (double)__ldg(&f.a.az[idx]);
+    if (f.alpha0 == 0.0) return a;
+    const double b = (double)__ldg(&f.b.az[idx]);
+    return (1.0 - f.alpha0) * a + f.alpha0 * b;
+}
+
+// integrators.py:842-938 _apply_split_az_kick for one particle ALIVE after
+// the deterministic step and the horizontal kick: Az and dAz/dz on the
+// anchor's column (diffusion.py:357-423, the evaluation depth clamped to the
+// wet column, the slope of the segment holding it), or the constant; the
+// Euler-Maruyama increment with the Ito drift, both on |dt| (:302-330), the
+// vertical counter-RNG component; reflective bounds [z_levels[0],
+// depth[anchor]] (:426-455).
+template <typename T>
+__device__ __noinline__ void apply_az(const DMesh& m, const DBlend<T>& f, const DStep& s, long long pid,
+                                      unsigned long long rid, int nn, double& z) {
+    double az = s.az_const, g = 0.0;
+    const double bottom = __ldg(&m.depth[nn]);
+    if (s.az_field) {
+        const int K = m.K;
+        const double* zl = m.zlev;
+        const double top = __ldg(&zl[0]);
+        double bot = bottom < __ldg(&zl[K - 1]) ? bottom : __ldg(&zl[K - 1]);
+        if (bot < top) bot = top;
+        double ze = z;
+        if (ze < top) ze = top;
+        if (ze > bot) ze = bot;
+        // first segment k with ze <= zl[k + 1] (K - 2 when none)
+        int k = K - 2;
+        if (K >= 2) {
+            int lo = 0, hi = K - 2;
+            if (!(ze <= __ldg(&zl[K - 1]))) lo = hi;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (ze <= __ldg(&zl[mid + 1])) hi = mid;
+                else lo = mid + 1;
+            }
+            k = lo;
+        }
+        if (K < 2 || ze <= __ldg(&zl[0])) az = az_at(f, 0, nn);
+        else if (ze >= __ldg(&zl[K - 1])) az = az_at(f, K - 1, nn);
+        else {
+            const double dzl = __ldg(&zl[k + 1]) - __ldg(&zl[k]);
+            if (dzl <= 0.0) az = az_at(f, k, nn);
+            else {
+                const double frac = (ze - __ldg(&zl[k])) / dzl;
+                az = (1.0 - frac) * az_at(f, k, nn) + frac * az_at(f, k + 1, nn);
+            }
+        }
+        if (K >= 2) {
+            const double dz = __ldg(&zl[k + 1]) - __ldg(&zl[k]);
+            if (dz > 0.0) {
+                if (std::is_same<T, float>::value && f.alpha0 == 0.0) {
+                    // an unblended float32 snapshot: the difference of two
+                    // float32 values rounds in float32 (numpy promotion)
+                    const float d = (float)az_at(f, k + 1, nn) - (float)az_at(f, k, nn);
+                    g = (double)d / dz;
+                } else {
+                    g = (az_at(f, k + 1, nn) - az_at(f, k, nn)) / dz;
+                }
+            }
+        }
+    }
+    if (az < 0.0) {
+        az = 0.0;
+        g = 0.0;
+    }
+    double xi, unused;
+    normal_pair(s.seed, rid, (unsigned long long)pid + s.pid_offset, s.step_i, 1ull, xi, unused);
+    const double sdt = s.time_dir * s.dt;
+    const double abs_dt = sdt >= 0.0 ? sdt : -sdt;
+    const double dz = g * abs_dt + sqrt(2.0 * az * abs_dt) * xi;
+    z = reflect_depth(z + dz, __ldg(&m.zlev[0]), bottom);
 }
 
 // integrators.py:2521-2638 (RK2), :2641-2816 (RK4); Euler follows the
@@ -383,6 +483,8 @@ __device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DB
                 apply_kick(m, s, pid, realization_of(st, s, i), qn, lon0, lat0, z0p, pre_nn, true, lon_new, lat_new, z_new, status, nn_out,
                            fr);
             }
+            if (s.az_on && status == ALIVE)
+                apply_az<T>(m, f, s, st.pid ? st.pid[i] : i, realization_of(st, s, i), nn_out, z_new);
         }
     }
     st.lon[i] = lon_new;
@@ -452,6 +554,8 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
                     apply_kick(m, s, pid, realization_of(st, s, i), qn, lon0, lat0, z0p, pre_nn, true, lon_new, lat_new, z_new, status,
                                nn_out, fr);
                 }
+                if (s.az_on && status == ALIVE)
+                    apply_az<T>(m, f, s, st.pid ? st.pid[i] : i, realization_of(st, s, i), nn_out, z_new);
             }
         }
     }

@@ -167,6 +167,11 @@ class DeviceContext:
         wrows = 0 if w is None else (1 if w.ndim == 1 else w.shape[0])
         self._chk(N.lib().kc_field_upload(self._ctx, slot, code, n, rows, N.ptr(u), N.ptr(v), wrows, N.ptr(w)),
                   "kc_field_upload")
+        az = getattr(field, "az", None)
+        if az is not None and code != N.KC_F16:
+            az = _c(np.asarray(az), host)
+            self._chk(N.lib().kc_field_upload_az(self._ctx, slot, code, n, 1 if az.ndim == 1 else az.shape[0],
+                                                 N.ptr(az)), "kc_field_upload_az")
         self.synchronize()
 
     def slots_for(self, fields, storage=None) -> list:
@@ -175,7 +180,8 @@ class DeviceContext:
         one of them is float32, unless ``storage`` names it (``np.float16``:
         half storage with per-row scales)."""
         all32 = all(np.asarray(f.u).dtype == np.float32 and np.asarray(f.v).dtype == np.float32
-                    and (f.w is None or np.asarray(f.w).dtype == np.float32) for f in fields)
+                    and (f.w is None or np.asarray(f.w).dtype == np.float32)
+                    and (getattr(f, "az", None) is None or np.asarray(f.az).dtype == np.float32) for f in fields)
         dtype = np.dtype(storage) if storage is not None else np.dtype(np.float32 if all32 else np.float64)
         out = []
         pinned = set()

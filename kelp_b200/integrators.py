@@ -62,8 +62,6 @@ def _kick_args(diffusion) -> Optional[tuple]:
     if diffusion.composition not in ("split",):
         raise NotImplementedError(f"diffusion.composition={diffusion.composition!r} is not built on the "
                                   "CUDA backend")
-    if getattr(diffusion, "az_enabled", False):
-        raise NotImplementedError("the vertical Az kick is not built on the CUDA backend")
     if float(diffusion.kh_x) == 0.0 and float(diffusion.kh_y) == 0.0:
         return None
     if float(diffusion.kh_x) < 0 or float(diffusion.kh_y) < 0:
@@ -103,14 +101,38 @@ def _check_node_fields(mesh, fields, is3d, placement="layer"):
                                  "(integrators.py:4534-4553)")
 
 
+def _az_args(diffusion, vel, is3d, mesh):
+    """(use_field, az_const) of the vertical Az kick, or None when it does
+    not apply (integrators.py:842-907): the payload's Az field when it carries
+    one, else the constant; a zero source skips the kick."""
+    if diffusion is None or not getattr(diffusion, "az_enabled", False):
+        return None
+    az_field = getattr(vel, "az", None)
+    az_const = max(float(getattr(diffusion, "az_const", 0.0)), 0.0)
+    if az_field is None and getattr(diffusion, "az_requires_field", False):
+        raise ValueError("diffusion.var_az is configured but the velocity payload carries no az field")
+    if az_field is None and az_const == 0.0:
+        return None
+    if not is3d:
+        raise ValueError("diffusion.az_enabled requires a 3-D run (Fdrift3D)")
+    if getattr(mesh, "vertical_coord", "zlevel") == "sigma":
+        raise NotImplementedError("the Az kick on sigma meshes is not built on the CUDA backend")
+    return (az_field is not None, az_const)
+
+
 def _check_call(dt, time_dir, kw):
     if float(dt) <= 0:
         raise ValueError(f"dt must be > 0, got {dt!r}")
     if float(time_dir) not in (1.0, -1.0):
         raise ValueError(f"time_dir must be +1 or -1, got {time_dir!r}")
+    diffusion = kw.get("diffusion", None)
+    if (diffusion is not None and getattr(diffusion, "az_enabled", False)
+            and getattr(diffusion, "scheme", "uniform") in ("em", "m1")):
+        # integrators.py:824-839: checked before anything else
+        raise ValueError("diffusion.az_enabled composes with scheme='uniform' only")
     if kw.get("uv_interp", "leastsq") == "nemo_cgrid":
         raise NotImplementedError("the NEMO C-grid step is not built on the CUDA backend")
-    return _kick_args(kw.get("diffusion", None))
+    return _kick_args(diffusion)
 
 
 def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=None):
@@ -192,6 +214,15 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
         a.kh_x, a.kh_y, a.seed, a.real_id, a.step_i, a.pid_offset = kick
     a.global_step = -1
     a.precision = N.KC_MIXED if form == "mixed" else N.KC_PLAIN
+    az = _az_args(kw.get("diffusion", None), vel, is3d, mesh)
+    if az is not None:
+        if az[0] and store is np.float16:
+            raise NotImplementedError("the Az field with float16 snapshots is not built on the CUDA backend")
+        a.az_kick, a.az_field, a.az_const = 1, int(az[0]), float(az[1])
+        d = kw["diffusion"]
+        if kick is None:   # the Az draws use the step's keys even without a horizontal kick
+            a.seed, a.real_id, a.step_i = int(d.seed), int(d.real_id), int(d.step_i)
+            a.pid_offset = int(getattr(d, "pid_offset", 0))
     return a, is3d
 
 

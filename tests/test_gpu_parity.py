@@ -13,6 +13,8 @@ import pytest
 from kelp_b200 import integrators as KI
 from kelp_b200.diffusion import DiffusionStepArgs
 
+from test_oracle_golden import diffusion_args
+
 pytestmark = pytest.mark.gpu
 
 POS_TOL_DEG = 1e-9 / 0.017453292519943295
@@ -22,8 +24,9 @@ VEL_TOL = 1e-9
 CASES = [("golden_band", c) for c in ("rk2", "rk4", "euler", "rk2_bwd", "rk2_kick", "rk4_kick_aniso", "rk2_dt4800")]
 CASES += [("golden_quad", c) for c in ("rk2", "rk4", "euler", "rk2_kick")]
 CASES += [("golden_polar", "rk2")]
-CASES += [("golden_3d", c) for c in ("rk2_wnear", "rk2_wbary", "rk2_wbary_kick", "rk4_wnear", "rk4_wbary_kick", "euler_wbary")]
-CASES += [("golden_dl_lev", c) for c in ("rk2_lev_wbary", "rk4_lev_wnear_kick", "euler_lev_wnear")]
+CASES += [("golden_3d", c) for c in ("rk2_wnear", "rk2_wbary", "rk2_wbary_kick", "rk4_wnear", "rk4_wbary_kick", "euler_wbary",
+                                     "rk2_wbary_kick_azf", "rk4_wnear_azf_nokh")]
+CASES += [("golden_dl_lev", c) for c in ("rk2_lev_wbary", "rk4_lev_wnear_kick", "euler_lev_wnear", "rk2_lev_wbary_azc")]
 CASES += [("golden_dl_llin", c) for c in ("rk2_llin_wbary", "rk4_llin_wnear_kick", "euler_llin_wnear")]
 
 
@@ -37,9 +40,7 @@ def replay_cuda(g, cname):
     snaps = {}
     for k in range(int(n_steps)):
         vel, vnext, dtn = g.payload(c["schedule"][k], T)
-        diff = None
-        if khx >= 0:
-            diff = DiffusionStepArgs("uniform", khx, khy, int(seed), int(real_id), k, pid_offset=int(pid_off))
+        diff = diffusion_args(c, k)
         st = fn(st, vel, g.mesh, dt, td, uv_interp="barycentric", w_interp=w_interp, vel_next=vnext,
                 dt_to_next=dtn, diffusion=diff)
         if f"s{k + 1}_lon" in c:
