@@ -280,6 +280,67 @@ def build_boundary_info(mesh) -> None:
     mesh._elem_is_coastal = coastal
 
 
+def build_elem_neighbors(mesh) -> np.ndarray:
+    """Element adjacency across shared edges (``mesh.py:2824-2910``): slot k of
+    row e holds the element sharing edge (v_k, v_{k+1}) of e's compacted
+    vertex ring (-1 pads and repeats of the first vertex dropped), -1 on a
+    boundary edge or an unused slot.  An edge of more than two elements (a
+    non-manifold mesh) raises.  Cached as ``mesh._elem_neighbors``."""
+    cached = getattr(mesh, "_elem_neighbors", None)
+    if cached is not None:
+        return cached
+    en = np.asarray(mesh.elem_nodes)
+    E, mv = en.shape
+    out = np.full((E, mv), -1, dtype=np.int32)
+    if E == 0:
+        mesh._elem_neighbors = out
+        return out
+    # compacted ring: keep a slot unless it is -1 or repeats the first valid vertex
+    first = np.full(E, -1, dtype=np.int64)
+    keep = np.zeros((E, mv), dtype=bool)
+    for j in range(mv):
+        v = en[:, j].astype(np.int64)
+        ok = v >= 0
+        ok &= ~((first >= 0) & (v == first))
+        keep[:, j] = ok
+        first = np.where((first < 0) & ok, v, first)
+    nv = keep.sum(axis=1)
+    order = np.argsort(~keep, axis=1, kind="stable")
+    verts = np.take_along_axis(en, order, axis=1).astype(np.int64)
+    rows = np.arange(E)
+    base = np.int64(np.asarray(mesh.nodes_lon).shape[0] + 1)
+    e_all, k_all, key_all = [], [], []
+    for k in range(mv):
+        ok = (nv >= 3) & (k < nv)
+        nxt = np.where(ok, (k + 1) % np.maximum(nv, 1), 0)
+        a = verts[rows, k]
+        b = verts[rows, nxt]
+        ok &= a != b
+        e_all.append(rows[ok])
+        k_all.append(np.full(int(ok.sum()), k, dtype=np.int64))
+        key_all.append(np.minimum(a, b)[ok] * base + np.maximum(a, b)[ok])
+    e_cat = np.concatenate(e_all)
+    k_cat = np.concatenate(k_all)
+    key = np.concatenate(key_all)
+    if key.size:
+        # a ring repeating an edge keeps its first slot (per-element dedup)
+        o = np.lexsort((k_cat, e_cat, key))
+        key, e_cat, k_cat = key[o], e_cat[o], k_cat[o]
+        dup = np.r_[False, (key[1:] == key[:-1]) & (e_cat[1:] == e_cat[:-1])]
+        key, e_cat, k_cat = key[~dup], e_cat[~dup], k_cat[~dup]
+        starts = np.flatnonzero(np.r_[True, key[1:] != key[:-1]])
+        counts = np.diff(np.r_[starts, key.size])
+        if (counts > 2).any():
+            s0 = starts[counts > 2][0]
+            raise ValueError(f"non-manifold mesh: edge key {int(key[s0])} is shared by {int(counts[counts > 2][0])} "
+                             "elements")
+        pairs = starts[counts == 2]
+        out[e_cat[pairs], k_cat[pairs]] = e_cat[pairs + 1]
+        out[e_cat[pairs + 1], k_cat[pairs + 1]] = e_cat[pairs]
+    mesh._elem_neighbors = out
+    return out
+
+
 def build_search(mesh) -> None:
     """Build the grid hash (``mesh.py:237``)."""
     build_grid_hash(mesh)

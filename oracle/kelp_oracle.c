@@ -42,6 +42,7 @@ typedef struct {
     const double *dl_p, *dl_bed;      /* depth-linear table (vertical_uv.py:181-278) */
     const int32_t* dl_last;
     int dl_M;
+    const int32_t* enb;   /* (E, max_v) edge neighbours of the compacted ring (walk), or NULL */
 } OMesh;
 
 typedef struct {
@@ -530,10 +531,15 @@ static double tblend(double a, double b, double t, double alpha0, double alpha) 
 }
 
 /* interpolate.py:1340-1529 (row 0: 2-D; row = layer: 3-D) */
+/* The walk's pre-validated containing element for the next interpolation of
+ * this thread (-1: search from the anchor), as interpolate.py:1246-1270
+ * takes elem_hint. */
+static _Thread_local int t_elem_hint = -1;
+
 static int interp_uv(const OMesh* m, const OField* f, double xp, double yp, int nn, double td, int row,
                      double alpha, double* U, double* V) {
     *U = 0.0; *V = 0.0;
-    int elem = contain_local(m, xp, yp, nn);
+    int elem = t_elem_hint >= 0 ? t_elem_hint : contain_local(m, xp, yp, nn);
     if (elem < 0) return 0;
     int verts[4], nv = 0;
     for (int k = 0; k < m->max_v; ++k) {
@@ -754,7 +760,7 @@ static void point_uv(const OField* f, int k, int nd, double alpha, double* u, do
 static int interp_uv_dl(const OMesh* m, const OField* f, double xp, double yp, int nn, double z, double td,
                         double alpha, double* U, double* V) {
     *U = 0.0; *V = 0.0;
-    int elem = contain_local(m, xp, yp, nn);
+    int elem = t_elem_hint >= 0 ? t_elem_hint : contain_local(m, xp, yp, nn);
     if (elem < 0) return 0;
     int verts[4], nv = 0;
     for (int k = 0; k < m->max_v; ++k) {
@@ -946,23 +952,120 @@ static void kick(const OMesh* m, const OStep* s, int64_t pid, double pre_lon, do
 
 /* integrators.py:2521-2816 (2-D RK2/RK4 fused), the unfused Euler's per-particle
  * arithmetic (integrators.py:4997-5147), :3647-3856 (3-D RK2 fused). */
+/* mesh.py:2488-2590 _walk_containing_element: from element e, cross the
+ * edge of the most negative normalized signed-area coordinate until all are
+ * >= -1e-6 (a near-edge accept below 1e-2 is verified with the exact local
+ * predicate), at most 256 crossings; -1 for every non-contained outcome. */
+static int edge_walk(const OMesh* m, double lon_p, double lat_p, int e) {
+    if (e < 0 || e >= m->E || !m->enb) return -1;
+    int prev = -1;
+    for (int it = 0; it < 256; ++it) {
+        int verts[4], nv = 0;
+        for (int k = 0; k < m->max_v; ++k) {
+            int nd = m->en[(int64_t)e * m->max_v + k];
+            if (nd < 0) continue;
+            if (nv > 0 && nd == verts[0]) continue;
+            verts[nv++] = nd;
+        }
+        if (nv < 3) return -1;
+        double ln[4], la[4];
+        for (int k = 0; k < nv; ++k) { ln[k] = m->lon[verts[k]]; la[k] = m->lat[verts[k]]; }
+        /* mesh.py:2006-2051 _project_to_local_xy */
+        double lmin = ln[0], lmax = ln[0];
+        for (int k = 0; k < nv; ++k) { if (ln[k] < lmin) lmin = ln[k]; if (ln[k] > lmax) lmax = ln[k]; }
+        double lon0;
+        if (lmax - lmin > 180.0) {
+            double ds = 0.0;
+            for (int k = 0; k < nv; ++k) ds += wrap180(ln[k] - ln[0]);
+            lon0 = ln[0] + ds / nv;
+        } else {
+            double sm = 0.0;
+            for (int k = 0; k < nv; ++k) sm += ln[k];
+            lon0 = sm / nv;
+        }
+        double sl = 0.0;
+        for (int k = 0; k < nv; ++k) sl += la[k];
+        double lat0 = sl / nv;
+        double cl = cos(lat0 * DEG2RAD);
+        double x[4], y[4];
+        for (int k = 0; k < nv; ++k) {
+            x[k] = wrap180(ln[k] - lon0) * DEG2RAD * R_STD * cl;
+            y[k] = (la[k] - lat0) * DEG2RAD * R_STD;
+        }
+        double px = wrap180(lon_p - lon0) * DEG2RAD * R_STD * cl;
+        double py = (lat_p - lat0) * DEG2RAD * R_STD;
+        double S = 0.0;
+        for (int k = 0; k < nv; ++k) {
+            int j = (k + 1) % nv;
+            S += x[k] * y[j] - x[j] * y[k];
+        }
+        double absS = fabs(S);
+        if (absS < AREA_TOL) return -1;
+        double sgn = S > 0.0 ? 1.0 : -1.0;
+        double worst = 1.0e100;
+        int worst_k = -1;
+        for (int k = 0; k < nv; ++k) {
+            int j = (k + 1) % nv;
+            double A = (x[j] - x[k]) * (py - y[k]) - (px - x[k]) * (y[j] - y[k]);
+            double w = A * sgn / absS;
+            if (w < worst) { worst = w; worst_k = k; }
+        }
+        if (worst >= -1e-6) {
+            if (worst >= 1e-2) return e;
+            return element_contains(m, e, lon_p, lat_p) ? e : -1;
+        }
+        int nb = m->enb[(int64_t)e * m->max_v + worst_k];
+        if (nb < 0 || nb == prev) return -1;
+        prev = e;
+        e = nb;
+    }
+    return -1;
+}
+
+/* mesh.py:2593-2712 find_containing_elements_walk for one point: the walk
+ * from the carried element, else the local scan around the widened anchor,
+ * else around the exact anchor nn (the exactness heal); -1 outside. */
+static int walk_locate(const OMesh* m, double lon_p, double lat_p, int start, int nn) {
+    if (start >= 0) {
+        int e = edge_walk(m, lon_p, lat_p, start);
+        if (e >= 0) return e;
+    }
+    int nw = nearest_widened(m, lon_p, lat_p);
+    int e = contain_local(m, lon_p, lat_p, nw);
+    if (e >= 0) return e;
+    return contain_local(m, lon_p, lat_p, nn);
+}
+
+/* Walk mode (elem_search: walk, elem != NULL): each stage's containing
+ * element is walked from the previous stage's (the step's start from the
+ * carried one) and handed to the interpolation as its element hint; the
+ * end-of-step walk gives the domain verdict and the new carried element;
+ * a failed step keeps the start element (integrators.py:5019-5147,
+ * :5415-5608, :5792-6011). */
+#define STAGE(e, call) (t_elem_hint = (e), _r = (call), t_elem_hint = -1, _r)
+
 static void step_one(const OMesh* m, const OField* f, const OStep* s, int64_t i, double* lon, double* lat, double* z,
-                     int* status, int* nn, int8_t* fr, double* U, double* V, double* W, const int64_t* pid) {
+                     int* status, int* nn, int8_t* fr, double* U, double* V, double* W, const int64_t* pid,
+                     int32_t* elem) {
     if (status[i] != ALIVE) {
         U[i] = 0.0; V[i] = 0.0;
         if (W) W[i] = 0.0;
         return;
     }
     double lon0 = lon[i], lat0 = lat[i], zp = z ? z[i] : 0.0, dt = s->dt, td = s->td;
-    int pre_nn = nn[i], st = ALIVE, nno;
+    int pre_nn = nn[i], st = ALIVE, nno, _r;
     int8_t frr = fr[i];
     double ln = lon0, lt = lat0, zn = zp;
     int node_i = anchor(m, lon0, lat0);
     nno = node_i;
+    const int walk = elem != NULL;
+    const int e1 = walk ? walk_locate(m, lon0, lat0, elem[i], node_i) : -1;
+    int e_last = e1, e_out = e1;
+#define LOC(x, y, from, n) (walk ? walk_locate(m, (x), (y), (from), (n)) : -1)
     int ok = 1;
     if (s->dims == 2) {
         double U1, V1;
-        int ok1 = interp_uv(m, f, lon0, lat0, node_i, td, 0, s->ak[0], &U1, &V1);
+        int ok1 = STAGE(e1, interp_uv(m, f, lon0, lat0, node_i, td, 0, s->ak[0], &U1, &V1));
         U[i] = U1; V[i] = V1;
         if (!ok1) { ok = 0; }
         else if (s->scheme == 0) {
@@ -972,22 +1075,28 @@ static void step_one(const OMesh* m, const OField* f, const OStep* s, int64_t i,
             double lm = wrap180(lon0 + 0.5 * dt * U1 / z0_of(lat0));
             double tm = clat(lat0 + 0.5 * dt * V1 / SLM);
             int nm = anchor(m, lm, tm);
+            int em = LOC(lm, tm, e1, nm);
+            e_last = em;
             double U2, V2;
-            if (!interp_uv(m, f, lm, tm, nm, td, 0, s->ak[1], &U2, &V2)) ok = 0;
+            if (!STAGE(em, interp_uv(m, f, lm, tm, nm, td, 0, s->ak[1], &U2, &V2))) ok = 0;
             else { ln = wrap180(lon0 + dt * U2 / z0_of(tm)); lt = clat(lat0 + dt * V2 / SLM); }
         } else {
             double dl1 = dt * U1 / z0_of(lat0), dt1 = dt * V1 / SLM;
             double l2 = wrap180(lon0 + 0.5 * dl1), t2 = clat(lat0 + 0.5 * dt1);
             double U2, V2, U3, V3, U4, V4;
-            if (!interp_uv(m, f, l2, t2, anchor(m, l2, t2), td, 0, s->ak[1], &U2, &V2)) ok = 0;
+            int n2 = anchor(m, l2, t2), e2 = LOC(l2, t2, e1, n2);
+            if (!STAGE(e2, interp_uv(m, f, l2, t2, n2, td, 0, s->ak[1], &U2, &V2))) ok = 0;
             else {
                 double dl2 = dt * U2 / z0_of(t2), dt2 = dt * V2 / SLM;
                 double l3 = wrap180(lon0 + 0.5 * dl2), t3 = clat(lat0 + 0.5 * dt2);
-                if (!interp_uv(m, f, l3, t3, anchor(m, l3, t3), td, 0, s->ak[2], &U3, &V3)) ok = 0;
+                int n3 = anchor(m, l3, t3), e3 = LOC(l3, t3, e2, n3);
+                if (!STAGE(e3, interp_uv(m, f, l3, t3, n3, td, 0, s->ak[2], &U3, &V3))) ok = 0;
                 else {
                     double dl3 = dt * U3 / z0_of(t3), dt3 = dt * V3 / SLM;
                     double l4 = wrap180(lon0 + dl3), t4 = clat(lat0 + dt3);
-                    if (!interp_uv(m, f, l4, t4, anchor(m, l4, t4), td, 0, s->ak[3], &U4, &V4)) ok = 0;
+                    int n4 = anchor(m, l4, t4), e4 = LOC(l4, t4, e3, n4);
+                    e_last = e4;
+                    if (!STAGE(e4, interp_uv(m, f, l4, t4, n4, td, 0, s->ak[3], &U4, &V4))) ok = 0;
                     else {
                         double dl4 = dt * U4 / z0_of(t4), dt4 = dt * V4 / SLM;
                         double dl = (dl1 + 2.0 * dl2 + 2.0 * dl3 + dl4) / 6.0;
@@ -1001,8 +1110,9 @@ static void step_one(const OMesh* m, const OField* f, const OStep* s, int64_t i,
         if (!ok) { st = OUTSIDE; frr = 1; ln = lon0; lt = lat0; }
         else {
             int nw = anchor(m, ln, lt);
-            if (contain_local(m, ln, lt, nw) < 0) { st = OUTSIDE; frr = 2; ln = lon0; lt = lat0; }
-            else nno = nw;
+            int ein = walk ? walk_locate(m, ln, lt, e_last, nw) : contain_local(m, ln, lt, nw);
+            if (ein < 0) { st = OUTSIDE; frr = 2; ln = lon0; lt = lat0; }
+            else { nno = nw; e_out = ein; }
         }
     } else if (s->scheme != 1) {
         /* 3-D Euler (integrators.py:4997-5147) and RK4 (:5760-6011): the
@@ -1011,7 +1121,7 @@ static void step_one(const OMesh* m, const OField* f, const OStep* s, int64_t i,
          * (the whole-field lerps of _make_stage_vels, :1187-1237), W at the
          * stage position, failure reverts to the start with the start anchor. */
         double U1, V1;
-        int ok1 = stage_uv(m, f, s, lon0, lat0, node_i, zp, s->ak[0], &U1, &V1);
+        int ok1 = STAGE(e1, stage_uv(m, f, s, lon0, lat0, node_i, zp, s->ak[0], &U1, &V1));
         double W1 = s->w_code == 0 ? w_linear(m, f, s->ak[0], zp, node_i, td)
                                    : w_bary(m, f, s->ak[0], lon0, lat0, zp, node_i, td);
         U[i] = U1; V[i] = V1; W[i] = W1;
@@ -1024,23 +1134,24 @@ static void step_one(const OMesh* m, const OField* f, const OStep* s, int64_t i,
         } else {
             double dl1 = dt * U1 / z0_of(lat0), dd1 = dt * V1 / SLM, dz1 = dt * W1;
             double l2 = wrap180(lon0 + 0.5 * dl1), t2 = clat(lat0 + 0.5 * dd1), z2 = zp + 0.5 * dz1;
-            int n2 = anchor(m, l2, t2);
+            int n2 = anchor(m, l2, t2), e2 = LOC(l2, t2, e1, n2);
             double U2, V2, U3, V3, U4, V4;
-            if (!stage_uv(m, f, s, l2, t2, n2, z2, s->ak[1], &U2, &V2)) ok = 0;
+            if (!STAGE(e2, stage_uv(m, f, s, l2, t2, n2, z2, s->ak[1], &U2, &V2))) ok = 0;
             else {
                 double W2 = s->w_code == 0 ? w_linear(m, f, s->ak[1], z2, n2, td)
                                            : w_bary(m, f, s->ak[1], l2, t2, z2, n2, td);
                 double dl2 = dt * U2 / z0_of(t2), dd2 = dt * V2 / SLM, dz2 = dt * W2;
                 double l3 = wrap180(lon0 + 0.5 * dl2), t3 = clat(lat0 + 0.5 * dd2), z3 = zp + 0.5 * dz2;
-                int n3 = anchor(m, l3, t3);
-                if (!stage_uv(m, f, s, l3, t3, n3, z3, s->ak[2], &U3, &V3)) ok = 0;
+                int n3 = anchor(m, l3, t3), e3 = LOC(l3, t3, e2, n3);
+                if (!STAGE(e3, stage_uv(m, f, s, l3, t3, n3, z3, s->ak[2], &U3, &V3))) ok = 0;
                 else {
                     double W3 = s->w_code == 0 ? w_linear(m, f, s->ak[2], z3, n3, td)
                                                : w_bary(m, f, s->ak[2], l3, t3, z3, n3, td);
                     double dl3 = dt * U3 / z0_of(t3), dd3 = dt * V3 / SLM, dz3 = dt * W3;
                     double l4 = wrap180(lon0 + dl3), t4 = clat(lat0 + dd3), z4 = zp + dz3;
-                    int n4 = anchor(m, l4, t4);
-                    if (!stage_uv(m, f, s, l4, t4, n4, z4, s->ak[3], &U4, &V4)) ok = 0;
+                    int n4 = anchor(m, l4, t4), e4 = LOC(l4, t4, e3, n4);
+                    e_last = e4;
+                    if (!STAGE(e4, stage_uv(m, f, s, l4, t4, n4, z4, s->ak[3], &U4, &V4))) ok = 0;
                     else {
                         double W4 = s->w_code == 0 ? w_linear(m, f, s->ak[3], z4, n4, td)
                                                    : w_bary(m, f, s->ak[3], l4, t4, z4, n4, td);
@@ -1058,16 +1169,17 @@ static void step_one(const OMesh* m, const OField* f, const OStep* s, int64_t i,
         if (!ok) { st = OUTSIDE; frr = 1; }
         else {
             int nw = anchor(m, a, b);
-            if (contain_local(m, a, b, nw) < 0) { st = OUTSIDE; frr = 2; }
+            int ein = walk ? walk_locate(m, a, b, e_last, nw) : contain_local(m, a, b, nw);
+            if (ein < 0) { st = OUTSIDE; frr = 2; }
             else {
                 if (c < m->zlev[0]) c = m->zlev[0];
                 if (c > m->depth[nw]) c = m->depth[nw];
-                ln = a; lt = b; zn = c; nno = nw;
+                ln = a; lt = b; zn = c; nno = nw; e_out = ein;
             }
         }
     } else {
         double U1, V1;
-        int ok1 = stage_uv(m, f, s, lon0, lat0, node_i, zp, s->ak[0], &U1, &V1);
+        int ok1 = STAGE(e1, stage_uv(m, f, s, lon0, lat0, node_i, zp, s->ak[0], &U1, &V1));
         double W1 = s->w_code == 0 ? w_linear(m, f, s->ak[0], zp, node_i, td)
                                    : w_bary(m, f, s->ak[0], lon0, lat0, zp, node_i, td);
         U[i] = U1; V[i] = V1; W[i] = W1;
@@ -1077,8 +1189,10 @@ static void step_one(const OMesh* m, const OField* f, const OStep* s, int64_t i,
             double tm = clat(lat0 + 0.5 * dt * V1 / SLM);
             double zm = zp + W1 * 0.5 * dt;
             int nm = anchor(m, lm, tm);
+            int em = LOC(lm, tm, e1, nm);
+            e_last = em;
             double U2, V2;
-            if (!stage_uv(m, f, s, lm, tm, nm, zm, s->ak[1], &U2, &V2)) { st = OUTSIDE; frr = 1; }
+            if (!STAGE(em, stage_uv(m, f, s, lm, tm, nm, zm, s->ak[1], &U2, &V2))) { st = OUTSIDE; frr = 1; }
             else {
                 double W2 = s->w_code == 0 ? w_linear(m, f, s->ak[1], zm, nm, td)
                                            : w_bary(m, f, s->ak[1], lm, tm, zm, nm, td);
@@ -1086,23 +1200,33 @@ static void step_one(const OMesh* m, const OField* f, const OStep* s, int64_t i,
                 double b = clat(lat0 + dt * V2 / SLM);
                 double c = zp + W2 * dt;
                 int nw = anchor(m, a, b);
-                if (contain_local(m, a, b, nw) < 0) { st = OUTSIDE; frr = 2; }
+                int ein = walk ? walk_locate(m, a, b, e_last, nw) : contain_local(m, a, b, nw);
+                if (ein < 0) { st = OUTSIDE; frr = 2; }
                 else {
                     if (c < m->zlev[0]) c = m->zlev[0];
                     if (c > m->depth[nw]) c = m->depth[nw];
-                    ln = a; lt = b; zn = c; nno = nw;
+                    ln = a; lt = b; zn = c; nno = nw; e_out = ein;
                 }
             }
         }
     }
+#undef LOC
     if (s->kick && st == ALIVE)
         kick(m, s, pid ? pid[i] : i, lon0, lat0, zp, pre_nn, &ln, &lt, &zn, &st, &nno, &frr, s->dims == 3);
     if (s->az_on && st == ALIVE && s->dims == 3) az_kick(m, f, s, pid ? pid[i] : i, nno, &zn);
     lon[i] = ln; lat[i] = lt;
     if (z) z[i] = zn;
     status[i] = st; nn[i] = nno; fr[i] = frr;
+    if (walk) elem[i] = e_out;
 }
 
+
+/* mesh.py:2593-2712 for a batch: the walk from start[i] (-1: none) */
+typedef struct { const OMesh* m; const double *lon, *lat; const int* start; const int* nn; int* out; } WCtx;
+static void walk_body(void* ctx, int64_t i) {
+    WCtx* c = (WCtx*)ctx;
+    c->out[i] = walk_locate(c->m, c->lon[i], c->lat[i], c->start[i], c->nn[i]);
+}
 
 /* ---- a small dynamic parallel-for over particles (pthreads) ---------- */
 
@@ -1167,6 +1291,7 @@ typedef struct {
     const double *dl_p, *dl_bed;
     const int32_t* dl_last;
     int dl_M;
+    const int32_t* enb;
 } orc_mesh;
 
 typedef struct {
@@ -1189,11 +1314,13 @@ typedef struct {
 typedef struct {
     const OMesh* m; const OField* f; const OStep* s;
     double *lon, *lat, *z; int *status, *nn; int8_t* fr; double *U, *V, *W; const int64_t* pid;
+    int32_t* elem;
 } StepCtx;
 
 static void step_body(void* ctx, int64_t i) {
     StepCtx* c = (StepCtx*)ctx;
-    step_one(c->m, c->f, c->s, i, c->lon, c->lat, c->z, c->status, c->nn, c->fr, c->U, c->V, c->W, c->pid);
+    step_one(c->m, c->f, c->s, i, c->lon, c->lat, c->z, c->status, c->nn, c->fr, c->U, c->V, c->W, c->pid,
+             c->elem);
 }
 
 typedef struct { const OMesh* m; const double *lon, *lat; const int* nn; int* out; } QCtx;
@@ -1202,15 +1329,22 @@ static void cont_body(void* ctx, int64_t i) { QCtx* c = (QCtx*)ctx; c->out[i] = 
 
 int orc_step(const orc_mesh* mm, const orc_field* ff, const orc_step_args* ss, int64_t P, double* lon, double* lat,
              double* z, int* status, int* nn, int8_t* fr, double* U, double* V, double* W, const int64_t* pid,
-             const int* release_step, int64_t global_step) {
+             const int* release_step, int64_t global_step, int32_t* elem) {
     const OMesh* m = (const OMesh*)mm;
     const OField* f = (const OField*)ff;
     const OStep* s = (const OStep*)ss;
     if (release_step && global_step >= 0)
         for (int64_t i = 0; i < P; ++i)
             if (status[i] == NOT_RELEASED && global_step >= release_step[i]) status[i] = ALIVE;
-    StepCtx c = {m, f, s, lon, lat, z, status, nn, fr, U, V, W, pid};
+    StepCtx c = {m, f, s, lon, lat, z, status, nn, fr, U, V, W, pid, elem};
     par_for(P, step_body, &c);
+    return 0;
+}
+
+int orc_walk(const orc_mesh* mm, int64_t P, const double* lon, const double* lat, const int* start, const int* nn,
+             int* out) {
+    WCtx c = {(const OMesh*)mm, lon, lat, start, nn, out};
+    par_for(P, walk_body, &c);
     return 0;
 }
 

@@ -27,7 +27,8 @@ class OMesh(C.Structure):
                 ("cell", C.c_double), ("lon_min", C.c_double), ("lat_min", C.c_double), ("r_earth", C.c_double),
                 ("nx", C.c_int), ("ny", C.c_int), ("wrap", C.c_int), ("far_rows", C.c_int),
                 ("exact", C.c_int), ("K", C.c_int),
-                ("dl_p", C.c_void_p), ("dl_bed", C.c_void_p), ("dl_last", C.c_void_p), ("dl_M", C.c_int)]
+                ("dl_p", C.c_void_p), ("dl_bed", C.c_void_p), ("dl_last", C.c_void_p), ("dl_M", C.c_int),
+                ("enb", C.c_void_p)]
 
 
 class OField(C.Structure):
@@ -63,7 +64,8 @@ def lib():
         L = C.CDLL(LIB)
         vp, i64 = C.c_void_p, C.c_int64
         L.orc_step.argtypes = [C.POINTER(OMesh), C.POINTER(OField), C.POINTER(OStep), i64,
-                               vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, i64]
+                               vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, i64, vp]
+        L.orc_walk.argtypes = [C.POINTER(OMesh), i64, vp, vp, vp, vp, vp]
         L.orc_find_nearest.argtypes = [C.POINTER(OMesh), i64, vp, vp, vp]
         L.orc_contain.argtypes = [C.POINTER(OMesh), i64, vp, vp, vp, vp]
         L.orc_normals.argtypes = [i64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, vp]
@@ -115,6 +117,9 @@ class MeshView:
         s.nx, s.ny, s.wrap, s.far_rows = int(mesh._gh_nx), int(mesh._gh_ny), int(bool(mesh._gh_wrap_lon)), int(mesh._gh_far_rows)
         s.exact = int(bool((mesh.metadata or {}).get("exact_nearest", False)))
         s.K = 0 if self.zl is None else int(self.zl.size)
+        enb = getattr(mesh, "_elem_neighbors", None)
+        self.enb = None if enb is None else c(enb, np.int32)
+        s.enb = _p(self.enb)
         self.s = s
         self.mesh = mesh
         self.placement = None
@@ -154,7 +159,9 @@ def _field_arrays(f, dtype):
 def step(state, vel, mesh, dt, time_dir, scheme: str, *, vel_next=None, dt_to_next=None, w_interp="nearest",
          diffusion=None, pid=None, release_step=None, global_step=-1, view=None):
     """One step of every particle; returns a dict of new arrays
-    (lon, lat, z, status, nearest_node, failure_reason, u, v, w)."""
+    (lon, lat, z, status, nearest_node, failure_reason, u, v, w, and elem
+    when the state carries elements: elem_search walk, the mesh's
+    ``_elem_neighbors`` table required)."""
     view = view or MeshView(mesh)
     vel_a = getattr(vel, "vel_a", vel)
     vel_b = getattr(vel, "vel_b", vel_next if vel_next is not None else vel_a)
@@ -218,10 +225,15 @@ def step(state, vel, mesh, dt, time_dir, scheme: str, *, vel_next=None, dt_to_ne
            "u": np.zeros(P), "v": np.zeros(P), "w": np.zeros(P)}
     pid_a = None if pid is None else np.ascontiguousarray(pid, dtype=np.int64)
     rs = None if release_step is None else np.ascontiguousarray(release_step, dtype=np.int32)
+    elem = getattr(state, "elem", None)
+    if elem is not None:
+        if view.enb is None:
+            raise ValueError("walk mode needs mesh._elem_neighbors (build_elem_neighbors)")
+        out["elem"] = np.array(elem, dtype=np.int32)
     lib().orc_step(C.byref(view.s), C.byref(of), C.byref(os_), P,
                    _p(out["lon"]), _p(out["lat"]), _p(out["z"]), _p(out["status"]), _p(out["nearest_node"]),
                    _p(out["failure_reason"]), _p(out["u"]), _p(out["v"]), _p(out["w"]), _p(pid_a), _p(rs),
-                   int(global_step))
+                   int(global_step), _p(out.get("elem")))
     return out
 
 
@@ -259,6 +271,19 @@ def beach(state, prev_status, mesh, coastal, wet_streak, *, criteria, depth_min,
     lib().orc_beach(C.byref(view.s), C.byref(a), _p(cst), lon.size, _p(lon), _p(lat), _p(out["status"]),
                     _p(prev), _p(out["nearest_node"]), _p(out["failure_reason"]), _p(ws))
     return out, ws
+
+
+def walk(mesh, lon, lat, start, nn, view=None) -> np.ndarray:
+    """find_containing_elements_walk (mesh.py:2631-2712): containing element
+    of every point, walked from ``start``, with the global fallbacks."""
+    view = view or MeshView(mesh)
+    lon = np.ascontiguousarray(lon, dtype=np.float64)
+    lat = np.ascontiguousarray(lat, dtype=np.float64)
+    st = np.ascontiguousarray(start, dtype=np.int32)
+    nn = np.ascontiguousarray(nn, dtype=np.int32)
+    out = np.empty(lon.size, np.int32)
+    lib().orc_walk(C.byref(view.s), lon.size, _p(lon), _p(lat), _p(st), _p(nn), _p(out))
+    return out
 
 
 def find_nearest(mesh, lon, lat, view=None) -> np.ndarray:

@@ -42,6 +42,7 @@ class Golden:
         m.r_earth = float(g[7])
         m.vertical_coord = "zlevel"
         m.metadata = {"exact_nearest": True}
+        m._elem_neighbors = self.d.get("mesh_elem_neighbors")
         self.mesh = m
         from kelp_b200.fields import VelocityField
         placement = {"golden_dl_lev": "level", "golden_dl_llin": "layer_linear"}.get(name, "layer")

@@ -27,7 +27,7 @@ os.environ.setdefault("NUMBA_NUM_THREADS", "8")
 
 from kelp.core.io import LazyLerpField as RLazy, VelocityField as RVel  # noqa: E402
 from kelp.core.mesh import (Mesh as RMesh, build_node_to_elems as r_n2e, build_search,  # noqa: E402
-                            find_nearest_nodes, set_exact_nearest, set_grid_hash_cell)
+                            find_containing_elements, find_nearest_nodes, set_exact_nearest, set_grid_hash_cell)
 from kelp.core.particles import ParticleState as RState, ParticleStatus  # noqa: E402
 from kelp.numerics import integrators as RI  # noqa: E402
 from kelp.numerics.diffusion import DiffusionStepArgs as RDiff, _normal_pair  # noqa: E402
@@ -55,7 +55,8 @@ def ref_mesh(m, cell=0.0, sigma=None):
 
 
 def mesh_record(rm):
-    return {"nodes_lon": rm.nodes_lon, "nodes_lat": rm.nodes_lat, "depth": rm.depth,
+    extra = {} if rm._elem_neighbors is None else {"elem_neighbors": rm._elem_neighbors}
+    return {**extra,"nodes_lon": rm.nodes_lon, "nodes_lat": rm.nodes_lat, "depth": rm.depth,
             "elem_nodes": rm.elem_nodes, "node_to_elems": rm.node_to_elems,
             "node_to_elems_count": rm.node_to_elems_count, "sigma": rm.sigma,
             "gh_offsets": rm._gh_offsets, "gh_node_ids": rm._gh_node_ids, "node_xyz": rm._node_xyz,
@@ -79,12 +80,18 @@ def payload(fields, t, T):
 
 
 def run_case(rm, fields, lon, lat, z, status, scheme, dt, T, n_steps, *, time_dir=1.0, w_interp="nearest",
-             kh=None, seed=7, real_id=0, pid_offset=0, record=(1,), az=None):
+             kh=None, seed=7, real_id=0, pid_offset=0, record=(1,), az=None, walk=False):
     fn = {"rk2": RI.rk2_step, "rk4": RI.rk4_step, "euler": RI.euler_step}[scheme]
     P = lon.size
     st = RState(lon=lon.copy(), lat=lat.copy(), z=z.copy(), status=status.copy(),
                 nearest_node=np.full(P, -1, np.int32), failure_reason=np.zeros(P, np.int8))
     out = {}
+    if walk:
+        # elem_search: walk seeds the carried elements with one global
+        # search (tracking.py:2243-2250)
+        el0, _ = find_containing_elements(rm, st.lon, st.lat, find_nearest_nodes(rm, st.lon, st.lat))
+        st = st.replace(elem=el0.astype(np.int32))
+        out["elem0"] = np.asarray(st.elem).copy()
     sched = []
     for k in range(n_steps):
         t = k * dt
@@ -101,6 +108,8 @@ def run_case(rm, fields, lon, lat, z, status, scheme, dt, T, n_steps, *, time_di
                 out[f"{tag}_{name}"] = np.asarray(getattr(st, name))
             if st.w is not None:
                 out[f"{tag}_w"] = np.asarray(st.w)
+            if st.elem is not None:
+                out[f"{tag}_elem"] = np.asarray(st.elem)
     out["schedule"] = np.array(sched, dtype=np.float64)
     out["params"] = np.array([dt, T, n_steps, time_dir, -1 if kh is None else kh[0], -1 if kh is None else kh[1],
                               seed, real_id, pid_offset], dtype=np.float64)
@@ -244,6 +253,11 @@ def main():
     cases["rk4_kick_aniso"] = run_case(rm, rf, lon, lat, z, status, "rk4", 21600.0, T, 8, kh=(8.0e4, 2.0e4),
                                        seed=11, real_id=0)
     cases["rk2_dt4800"] = run_case(rm, rf, lon, lat, z, status, "rk2", 4800.0, T, 20)
+    # elem_search: walk (carried elements, edge walk with global fallbacks)
+    cases["rk2_walk"] = run_case(rm, rf, lon, lat, z, status, "rk2", 21600.0, T, 12, walk=True, record=(1, 6))
+    cases["rk4_walk_kick"] = run_case(rm, rf, lon, lat, z, status, "rk4", 21600.0, T, 8, kh=(5.0e4, 5.0e4),
+                                      seed=3, walk=True)
+    cases["euler_walk"] = run_case(rm, rf, lon, lat, z, status, "euler", 10800.0, T, 12, walk=True)
     nn_q = find_nearest_nodes(rm, lon, lat)
     save("golden_band", mesh_record(rm), snaps, cases,
          {"lon": lon, "lat": lat, "z": z, "status": status, "nearest_exact": nn_q})
@@ -308,7 +322,11 @@ def main():
                                             az=dict(az_enabled=True, az_requires_field=True)),
              "rk4_wnear_azf_nokh": run_case(rm, rf, lon, lat, z, status, "rk4", 21600.0, T, 10,
                                             w_interp="nearest", kh=(0.0, 0.0), seed=8,
-                                            az=dict(az_enabled=True, az_const=5e-3))}
+                                            az=dict(az_enabled=True, az_const=5e-3)),
+             "rk2_wbary_walk": run_case(rm, rf, lon, lat, z, status, "rk2", 21600.0, T, 12,
+                                        w_interp="barycentric", walk=True),
+             "rk4_wnear_walk_kick": run_case(rm, rf, lon, lat, z, status, "rk4", 21600.0, T, 10,
+                                             w_interp="nearest", kh=(3.0e4, 3.0e4), seed=2, walk=True)}
     save("golden_3d", mesh_record(rm), snaps, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
 
     # --- depth-linear u/v (uv_vertical level / layer_linear) on the same mesh;

@@ -14,11 +14,13 @@ import pytest
 from oracle import oracle as O
 from kelp_b200.diffusion import DiffusionStepArgs
 
-CASES = [("golden_band", c) for c in ("rk2", "rk4", "euler", "rk2_bwd", "rk2_kick", "rk4_kick_aniso", "rk2_dt4800")]
+CASES = [("golden_band", c) for c in ("rk2", "rk4", "euler", "rk2_bwd", "rk2_kick", "rk4_kick_aniso", "rk2_dt4800",
+                                      "rk2_walk", "rk4_walk_kick", "euler_walk")]
 CASES += [("golden_quad", c) for c in ("rk2", "rk4", "euler", "rk2_kick")]
 CASES += [("golden_polar", "rk2")]
 CASES += [("golden_3d", c) for c in ("rk2_wnear", "rk2_wbary", "rk2_wbary_kick", "rk4_wnear", "rk4_wbary_kick", "euler_wbary",
-                                     "rk2_wbary_kick_azf", "rk4_wnear_azf_nokh")]
+                                     "rk2_wbary_kick_azf", "rk4_wnear_azf_nokh", "rk2_wbary_walk",
+                                     "rk4_wnear_walk_kick")]
 CASES += [("golden_dl_lev", c) for c in ("rk2_lev_wbary", "rk4_lev_wnear_kick", "euler_lev_wnear", "rk2_lev_wbary_azc")]
 CASES += [("golden_dl_llin", c) for c in ("rk2_llin_wbary", "rk4_llin_wnear_kick", "euler_llin_wnear")]
 
@@ -40,6 +42,8 @@ def replay_oracle(g, cname):
     scheme = cname.split("_")[0]
     w_interp = "barycentric" if "wbary" in cname else "nearest"
     st = g.particles()
+    if "elem0" in c:   # elem_search: walk
+        st = st.replace(elem=c["elem0"].copy())
     view = O.MeshView(g.mesh)
     snaps = {}
     for k in range(int(n_steps)):
@@ -49,7 +53,7 @@ def replay_oracle(g, cname):
                      diffusion=diff, view=view)
         st = st.replace(lon=out["lon"], lat=out["lat"], z=out["z"], status=out["status"],
                         nearest_node=out["nearest_node"], failure_reason=out["failure_reason"],
-                        u=out["u"], v=out["v"], w=out["w"])
+                        u=out["u"], v=out["v"], w=out["w"], elem=out.get("elem"))
         if f"s{k + 1}_lon" in c:
             snaps[k + 1] = out
     return c, snaps
@@ -62,8 +66,9 @@ def test_oracle_matches_reference(golden, fixture, cname):
     exact_float = not cname.startswith("euler")
     for k, out in snaps.items():
         tag = f"s{k}_"
-        for name in ("status", "nearest_node", "failure_reason"):
-            np.testing.assert_array_equal(out[name], c[tag + name], err_msg=f"{cname} step {k} {name}")
+        for name in ("status", "nearest_node", "failure_reason", "elem"):
+            if tag + name in c:
+                np.testing.assert_array_equal(out[name], c[tag + name], err_msg=f"{cname} step {k} {name}")
         for name in ("lon", "lat", "z", "u", "v", "w"):
             if tag + name not in c:
                 continue
@@ -155,3 +160,12 @@ def test_oracle_coastal_flags(golden):
     m = types.SimpleNamespace(elem_nodes=g.mesh.elem_nodes, nodes_lon=g.mesh.nodes_lon, _elem_is_coastal=None)
     build_boundary_info(m)
     np.testing.assert_array_equal(m._elem_is_coastal.astype(np.uint8), g.d["p_coastal"])
+
+
+@pytest.mark.parametrize("fixture", ["golden_band", "golden_3d"])
+def test_elem_neighbors_match_reference(golden, fixture):
+    import types
+    from kelp_b200.mesh import build_elem_neighbors
+    g = golden(fixture)
+    m = types.SimpleNamespace(elem_nodes=g.mesh.elem_nodes, nodes_lon=g.mesh.nodes_lon, _elem_neighbors=None)
+    np.testing.assert_array_equal(build_elem_neighbors(m), g.d["mesh_elem_neighbors"])
