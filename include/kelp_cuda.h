@@ -24,6 +24,10 @@
  *                         (src/kelp/core/particles.py:153)
  *   kc_node_xyz_fill   <- core.mesh._node_xyz_fill (src/kelp/core/mesh.py:712)
  *   kc_find_nearest    <- core.mesh.find_nearest_nodes (src/kelp/core/mesh.py:1896)
+ *   kc_find_elements   <- core.mesh.find_containing_elements (src/kelp/core/mesh.py:2286)
+ *   kc_find_elements_walk <- core.mesh.find_containing_elements_walk
+ *                         (src/kelp/core/mesh.py:2631-2712)
+ *   kc_elem_neighbors_upload <- core.mesh.build_elem_neighbors (src/kelp/core/mesh.py:2824)
  *   kc_rng_normals     <- numerics.diffusion._normal_pair (src/kelp/numerics/diffusion.py:233)
  */
 #ifndef KELP_CUDA_H
@@ -33,7 +37,7 @@
 extern "C" {
 #endif
 
-#define KC_ABI_VERSION 3
+#define KC_ABI_VERSION 4
 
 #define KC_OK 0
 #define KC_ERR_ARG 1      /* invalid argument or combination */
@@ -159,6 +163,31 @@ int kc_particles_download(kc_ctx* ctx, long long P, double* lon, double* lat, do
  * kc_particles_upload clears them; call before kc_sort. */
 int kc_particles_set_realization(kc_ctx* ctx, const int* real_id);
 
+/* Edge-neighbour table of the mesh (E x max_v int32, -1 on boundary edges;
+ * entry k is the element across the edge from compacted-ring vertex k to the
+ * next; src/kelp/core/mesh.py:2824-2908 build_elem_neighbors).  Needed by the
+ * edge walk (elem_search: walk). */
+int kc_elem_neighbors_upload(kc_ctx* ctx, int max_v, const int* elem_neighbors);
+
+/* Carried containing elements of the resident particles (P int32, -1 = no
+ * guess) for elem_search "walk" (integrators.py:5019-5147, :5415-5608,
+ * :5792-6011): each step walks every stage's containing element from the
+ * previous stage's, hands it to the interpolation, and ends with the walked
+ * element of the new position (the start element after a failed step).
+ * NULL returns to the local search.  kc_particles_upload clears them; call
+ * before kc_sort.  kc_particles_get_elem reads them back in upload order. */
+int kc_particles_set_elem(kc_ctx* ctx, const int* elem);
+int kc_particles_get_elem(kc_ctx* ctx, long long P, int* elem);
+
+/* Containing element of each point by the local 1-ring / 2-ring scan around
+ * the anchor nn[i] (NULL: the exact nearest node of the point); -1 outside. */
+int kc_find_elements(kc_ctx* ctx, long long P, const double* lon, const double* lat, const int* nn, int* out);
+
+/* Containing element of each point, walked from start[i] (-1: no guess),
+ * with the widened-anchor and exact-anchor fallbacks; -1 outside. */
+int kc_find_elements_walk(kc_ctx* ctx, long long P, const double* lon, const double* lat, const int* start,
+                          int* out);
+
 /* Coastal element flags (E bytes, 1 = owns a boundary edge;
  * src/kelp/core/mesh.py:2764-2821 build_boundary_info). */
 int kc_coastal_upload(kc_ctx* ctx, const unsigned char* elem_is_coastal);
@@ -178,8 +207,10 @@ int kc_beach(kc_ctx* ctx, const kc_beach_args* args);
  * (zeros); pid (RNG particle key; NULL: the index), real_id (per-particle
  * realization; NULL: the step's) and release_step (delayed release, with
  * kc_step_args.global_step; NULL: all released) are read only from the input.
- * Output: lon, lat, status, nearest_node required; z, failure_reason, u, v, w
- * may be NULL (not returned).  Input and output may be the same arrays. */
+ * elem: the carried containing elements (walk mode, as kc_particles_set_elem;
+ * NULL: local search), read from the input and written to the output.
+ * Output: lon, lat, status, nearest_node required; z, failure_reason, u, v, w,
+ * elem may be NULL (not returned).  Input and output may be the same arrays. */
 typedef struct kc_host_particles {
     double* lon;
     double* lat;
@@ -193,6 +224,7 @@ typedef struct kc_host_particles {
     long long* pid;
     int* real_id;
     int* release_step;
+    int* elem;
 } kc_host_particles;
 
 /* One step of P particles held in host memory, in the reference's per-step

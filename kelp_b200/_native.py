@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libkelpcuda
 KC_OK, KC_ERR_ARG, KC_ERR_CUDA, KC_ERR_STATE, KC_ERR_DEVICE = 0, 1, 2, 3, 4
 KC_F32, KC_F64, KC_F16 = 0, 1, 2
 KC_PLAIN, KC_MIXED = 0, 1
-ABI_VERSION = 3
+ABI_VERSION = 4
 KC_EULER, KC_RK2, KC_RK4 = 0, 1, 2
 
 #: every symbol include/kelp_cuda.h declares
@@ -25,7 +25,8 @@ EXPORTS = ("kc_abi_version", "kc_node_xyz_fill", "kc_create", "kc_destroy", "kc_
            "kc_synchronize", "kc_mesh_upload", "kc_depth_points_upload", "kc_field_upload", "kc_particles_upload", "kc_field_upload_az",
            "kc_particles_download", "kc_coastal_upload", "kc_beach_state_upload",
            "kc_beach_state_download", "kc_beach", "kc_step", "kc_step_host", "kc_step_range", "kc_run_fused",
-           "kc_particles_set_realization", "kc_set_fused_block", "kc_run", "kc_sort", "kc_find_nearest", "kc_find_nearest_noalloc", "kc_rng_normals", "kc_device_errors",
+           "kc_particles_set_realization", "kc_elem_neighbors_upload", "kc_particles_set_elem",
+           "kc_particles_get_elem", "kc_find_elements_walk", "kc_find_elements", "kc_set_fused_block", "kc_run", "kc_sort", "kc_find_nearest", "kc_find_nearest_noalloc", "kc_rng_normals", "kc_device_errors",
            "kc_event_record", "kc_event_elapsed", "kc_l2_flush", "kc_host_alloc", "kc_host_free")
 
 
@@ -89,7 +90,8 @@ class HostParticles(C.Structure):
     _fields_ = [("lon", C.c_void_p), ("lat", C.c_void_p), ("z", C.c_void_p), ("status", C.c_void_p),
                 ("nearest_node", C.c_void_p), ("failure_reason", C.c_void_p),
                 ("u", C.c_void_p), ("v", C.c_void_p), ("w", C.c_void_p),
-                ("pid", C.c_void_p), ("real_id", C.c_void_p), ("release_step", C.c_void_p)]
+                ("pid", C.c_void_p), ("real_id", C.c_void_p), ("release_step", C.c_void_p),
+                ("elem", C.c_void_p)]
 
 
 _lib = None
@@ -125,6 +127,11 @@ def lib():
         L.kc_step_range.argtypes = [vp, C.POINTER(StepArgs), ll, ll]
         L.kc_run_fused.argtypes = [vp, C.POINTER(StepArgs), i, C.c_void_p, i]
         L.kc_particles_set_realization.argtypes = [vp, vp]
+        L.kc_elem_neighbors_upload.argtypes = [vp, i, vp]
+        L.kc_particles_set_elem.argtypes = [vp, vp]
+        L.kc_particles_get_elem.argtypes = [vp, ll, vp]
+        L.kc_find_elements_walk.argtypes = [vp, ll, vp, vp, vp, vp]
+        L.kc_find_elements.argtypes = [vp, ll, vp, vp, vp, vp]
         L.kc_set_fused_block.argtypes = [vp, i]
         L.kc_step_host.argtypes = [vp, C.POINTER(StepArgs), ll, C.POINTER(HostParticles), C.POINTER(HostParticles),
                                    ll]

@@ -63,6 +63,8 @@ struct kc_ctx {
     double* d_dl_p = nullptr;
     int* d_dl_last = nullptr;
     double* d_dl_bed = nullptr;
+    int4* d_enb = nullptr;   // edge neighbours of the compacted rings (kc_elem_neighbors_upload)
+    int max_v = 0;
     int* d_err = nullptr;
     kc::DMesh dm{};
     // snapshot ring
@@ -73,8 +75,9 @@ struct kc_ctx {
     int *status = nullptr, *nn = nullptr, *rs = nullptr;
     signed char* fr = nullptr;
     long long* pid = nullptr;
-    bool has_pid = false, has_rs = false, has_rid = false;
+    bool has_pid = false, has_rs = false, has_rid = false, has_elem = false;
     int* rid = nullptr;   // per-particle realization ids (ensemble members in one array)
+    int* elem = nullptr;  // carried containing elements (elem_search walk)
     // re-sort by grid-hash cell: upload slot of every resident particle, the
     // spare buffer of the gathers, radix-sort keys / indices and CUB's storage
     long long* orig = nullptr;
@@ -156,6 +159,7 @@ kc::DState state_of(kc_ctx* c) {
     st.rid = c->has_rid ? c->rid : nullptr;
     st.prev = c->has_beach ? c->prev : nullptr;
     st.nn_ok = c->nn_ok;
+    st.elem = c->has_elem ? c->elem : nullptr;
     st.P = c->P;
     return st;
 }
@@ -176,6 +180,30 @@ __global__ void __launch_bounds__(kBlock) k_nearest(const __grid_constant__ kc::
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P) return;
     out[i] = kc::site_anchor(m, kc::make_site(q[i], q[P + i]));
+}
+
+// mesh.py:2631-2712 find_containing_elements_walk: the walk from start[i]
+// with its fallbacks; the exact anchor of the heal is searched here.  out may
+// alias start (each thread reads its own entry first).
+__global__ void __launch_bounds__(kBlock) k_walk(const __grid_constant__ kc::DMesh m, const double* q, long long P,
+                                                 const int* start, int* out) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P) return;
+    const double lon = q[i], lat = q[P + i];
+    const int s = start[i];
+    const int nn = kc::site_anchor(m, kc::make_site(lon, lat));
+    out[i] = kc::walk_locate(m, lon, lat, s, nn);
+}
+
+// mesh.py:2286-2324 find_containing_elements: the local 1-ring / 2-ring scan
+// around nn[i] (null: the exact anchor of the point); -1 outside.
+__global__ void __launch_bounds__(kBlock) k_contain(const __grid_constant__ kc::DMesh m, const double* q, long long P,
+                                                    const int* nn, int* out) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P) return;
+    const double lon = q[i], lat = q[P + i];
+    const int a = nn ? nn[i] : kc::site_anchor(m, kc::make_site(lon, lat));
+    out[i] = kc::contain_local(m, lon, lat, a);
 }
 
 __global__ void __launch_bounds__(kBlock) k_normals(long long P, unsigned long long seed, unsigned long long real_id,
@@ -417,14 +445,16 @@ void free_mesh(kc_ctx* c) {
     dfree(c->d_ll); dfree(c->d_en); dfree(c->d_n2e_off); dfree(c->d_n2e); dfree(c->d_gh_off);
     dfree(c->d_gh_tab); dfree(c->d_xyz); dfree(c->d_depth); dfree(c->d_zlev);
     dfree(c->d_nsc); dfree(c->d_ecos); dfree(c->d_maxl); dfree(c->d_coastal);
-    dfree(c->d_dl_p); dfree(c->d_dl_last); dfree(c->d_dl_bed);
+    dfree(c->d_dl_p); dfree(c->d_dl_last); dfree(c->d_dl_bed); dfree(c->d_enb);
     c->dm.dl_p = nullptr; c->dm.dl_last = nullptr; c->dm.dl_bed = nullptr; c->dm.dl_M = 0;
+    c->dm.enb = nullptr;
     c->has_mesh = false;
 }
 
 void free_particles(kc_ctx* c) {
     dfree(c->lon); dfree(c->lat); dfree(c->z); dfree(c->U); dfree(c->V); dfree(c->W);
-    dfree(c->status); dfree(c->nn); dfree(c->fr); dfree(c->pid); dfree(c->rs); dfree(c->rid);
+    dfree(c->status); dfree(c->nn); dfree(c->fr); dfree(c->pid); dfree(c->rs); dfree(c->rid); dfree(c->elem);
+    c->has_elem = false;
     dfree(c->orig); dfree(c->spare); dfree(c->prev); dfree(c->wet); dfree(c->nn_ok);
     c->has_beach = false;
     dfree(c->skey[0]); dfree(c->skey[1]); dfree(c->sidx[0]); dfree(c->sidx[1]); dfree(c->cub_tmp);
@@ -576,6 +606,8 @@ int kc_mesh_upload(kc_ctx* c, const kc_mesh_desc* d) {
     m.nx = d->gh_nx; m.ny = d->gh_ny; m.wrap = d->gh_wrap_lon ? 1 : 0; m.far_rows = d->gh_far_rows;
     m.K = d->n_levels; m.exact = d->exact_nearest ? 1 : 0;
     m.err = c->d_err;
+    m.E = E;
+    c->max_v = d->max_v;
     c->N = N; c->E = E;
     c->has_mesh = true;
     ++c->mesh_gen;
@@ -589,6 +621,54 @@ int kc_coastal_upload(kc_ctx* c, const unsigned char* flags) {
     KC_CUDA(c, cudaStreamSynchronize(c->stream));
     dfree(c->d_coastal);
     int rc = upload(c, &c->d_coastal, flags, (size_t)c->E);
+    if (rc) return rc;
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KC_OK;
+}
+
+int kc_elem_neighbors_upload(kc_ctx* c, int max_v, const int* enb) {
+    if (!c || !enb) return KC_ERR_ARG;
+    if (!c->has_mesh) return fail(c, KC_ERR_STATE, "kc_elem_neighbors_upload: no mesh uploaded");
+    if (max_v != c->max_v) return fail(c, KC_ERR_ARG, "kc_elem_neighbors_upload: max_v differs from the mesh's");
+    const long long E = c->E;
+    std::vector<int4> t((size_t)E);
+    for (long long e = 0; e < E; ++e) {
+        const int* r = enb + e * max_v;
+        for (int k = 0; k < max_v; ++k)
+            if (r[k] < -1 || r[k] >= E) return fail(c, KC_ERR_ARG, "kc_elem_neighbors_upload: index out of range");
+        t[e] = make_int4(r[0], r[1], r[2], max_v == 4 ? r[3] : -1);
+    }
+    KC_CUDA(c, cudaSetDevice(c->device));
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    dfree(c->d_enb);
+    c->dm.enb = nullptr;
+    int rc = upload(c, &c->d_enb, t.data(), t.size());
+    if (rc) return rc;
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->dm.enb = c->d_enb;
+    ++c->mesh_gen;
+    return KC_OK;
+}
+
+int kc_particles_set_elem(kc_ctx* c, const int* elem) {
+    if (!c) return KC_ERR_ARG;
+    if (c->sorted) return fail(c, KC_ERR_STATE, "kc_particles_set_elem: set the elements before kc_sort");
+    if (elem && !c->dm.enb) return fail(c, KC_ERR_STATE, "kc_particles_set_elem: upload the element neighbours first");
+    KC_CUDA(c, cudaSetDevice(c->device));
+    c->has_elem = false;
+    if (!elem) return KC_OK;
+    if (c->P > 0) KC_CUDA(c, cudaMemcpyAsync(c->elem, elem, (size_t)c->P * 4, cudaMemcpyHostToDevice, c->stream));
+    c->has_elem = true;
+    return KC_OK;
+}
+
+int kc_particles_get_elem(kc_ctx* c, long long P, int* elem) {
+    if (!c || !elem) return KC_ERR_ARG;
+    if (!c->has_elem) return fail(c, KC_ERR_STATE, "kc_particles_get_elem: no carried elements (kc_particles_set_elem)");
+    if (P != c->P) return fail(c, KC_ERR_ARG, "kc_particles_get_elem: P differs from the resident count");
+    if (P == 0) return KC_OK;
+    KC_CUDA(c, cudaSetDevice(c->device));
+    int rc = fetch(c, elem, c->elem, 4);
     if (rc) return rc;
     KC_CUDA(c, cudaStreamSynchronize(c->stream));
     return KC_OK;
@@ -780,6 +860,7 @@ static int ensure_capacity(kc_ctx* c, long long P) {
     KC_CUDA(c, cudaMalloc((void**)&c->fr, n)); KC_CUDA(c, cudaMalloc((void**)&c->pid, n));
     KC_CUDA(c, cudaMalloc((void**)&c->rs, n)); KC_CUDA(c, cudaMalloc((void**)&c->orig, n));
     KC_CUDA(c, cudaMalloc((void**)&c->rid, n));
+    KC_CUDA(c, cudaMalloc((void**)&c->elem, n));
     KC_CUDA(c, cudaMalloc((void**)&c->spare, n));
     KC_CUDA(c, cudaMalloc((void**)&c->prev, n)); KC_CUDA(c, cudaMalloc((void**)&c->wet, n));
     KC_CUDA(c, cudaMalloc((void**)&c->nn_ok, n));
@@ -838,6 +919,7 @@ int kc_particles_upload(kc_ctx* c, long long P, const double* lon, const double*
     c->has_rs = rs != nullptr;
     if (rs) KC_CUDA(c, cudaMemcpyAsync(c->rs, rs, n * 4, cudaMemcpyHostToDevice, s));
     c->has_rid = false;
+    c->has_elem = false;
     KC_CUDA(c, cudaMemsetAsync(c->nn_ok, 0, n, s));   // uploaded anchors are not trusted
     KC_CUDA(c, cudaMemsetAsync(c->U, 0, n * 8, s));
     KC_CUDA(c, cudaMemsetAsync(c->V, 0, n * 8, s));
@@ -913,6 +995,7 @@ int kc_sort(kc_ctx* c) {
     if ((rc = regather(c, (void**)&c->nn_ok, 1, idx))) return rc;
     if (c->has_rs && (rc = regather(c, (void**)&c->rs, 4, idx))) return rc;
     if (c->has_rid && (rc = regather(c, (void**)&c->rid, 4, idx))) return rc;
+    if (c->has_elem && (rc = regather(c, (void**)&c->elem, 4, idx))) return rc;
     if (c->has_beach) {
         if ((rc = regather(c, (void**)&c->prev, 4, idx))) return rc;
         if ((rc = regather(c, (void**)&c->wet, 4, idx))) return rc;
@@ -928,6 +1011,8 @@ int kc_step_host(kc_ctx* c, const kc_step_args* a, long long P, const kc_host_pa
     if (P > 0 && (!in->lon || !in->lat || !in->status || !in->nearest_node || !out->lon || !out->lat ||
                   !out->status || !out->nearest_node))
         return fail(c, KC_ERR_ARG, "kc_step_host: lon, lat, status and nearest_node are required in and out");
+    if (out->elem && !in->elem) return fail(c, KC_ERR_ARG, "kc_step_host: out.elem needs in.elem (walk mode)");
+    if (in->elem && !c->dm.enb) return fail(c, KC_ERR_STATE, "kc_step_host: upload the element neighbours first");
     KC_CUDA(c, cudaSetDevice(c->device));
     int rc = ensure_capacity(c, P);
     if (rc) return rc;
@@ -936,6 +1021,7 @@ int kc_step_host(kc_ctx* c, const kc_step_args* a, long long P, const kc_host_pa
     c->has_pid = in->pid != nullptr;
     c->has_rs = in->release_step != nullptr;
     c->has_rid = in->real_id != nullptr;
+    c->has_elem = in->elem != nullptr;
     c->has_beach = false;
     if ((rc = check_step(c, a))) return rc;
     if (P == 0) return KC_OK;
@@ -974,6 +1060,7 @@ int kc_step_host(kc_ctx* c, const kc_step_args* a, long long P, const kc_host_pa
         if (in->real_id) KC_CUDA(c, cudaMemcpyAsync(c->rid + b, in->real_id + b, n * 4, cudaMemcpyHostToDevice, si));
         if (in->release_step)
             KC_CUDA(c, cudaMemcpyAsync(c->rs + b, in->release_step + b, n * 4, cudaMemcpyHostToDevice, si));
+        if (in->elem) KC_CUDA(c, cudaMemcpyAsync(c->elem + b, in->elem + b, n * 4, cudaMemcpyHostToDevice, si));
         KC_CUDA(c, cudaEventRecord(c->ev_in[k], si));
         // the chunk's particles as a state of their own: RNG keys stay the
         // global index (pid_offset + base + local index); carried anchors are
@@ -984,6 +1071,7 @@ int kc_step_host(kc_ctx* c, const kc_step_args* a, long long P, const kc_host_pa
         st.pid = in->pid ? c->pid + b : nullptr;
         st.rid = in->real_id ? c->rid + b : nullptr;
         st.release_step = in->release_step ? c->rs + b : nullptr;
+        st.elem = in->elem ? c->elem + b : nullptr;
         st.prev = nullptr; st.nn_ok = nullptr;
         st.P = n;
         kc::DStep sk = s0;
@@ -1008,6 +1096,7 @@ int kc_step_host(kc_ctx* c, const kc_step_args* a, long long P, const kc_host_pa
         if (out->u) KC_CUDA(c, cudaMemcpyAsync(out->u + b, c->U + b, n * 8, cudaMemcpyDeviceToHost, so));
         if (out->v) KC_CUDA(c, cudaMemcpyAsync(out->v + b, c->V + b, n * 8, cudaMemcpyDeviceToHost, so));
         if (out->w) KC_CUDA(c, cudaMemcpyAsync(out->w + b, c->W + b, n * 8, cudaMemcpyDeviceToHost, so));
+        if (out->elem) KC_CUDA(c, cudaMemcpyAsync(out->elem + b, c->elem + b, n * 4, cudaMemcpyDeviceToHost, so));
     }
     KC_CUDA(c, cudaStreamSynchronize(c->s_out));
     KC_CUDA(c, cudaMemsetAsync(c->nn_ok, 0, (size_t)P, c->stream));
@@ -1024,6 +1113,7 @@ static kc::DState state_range(kc::DState st, long long begin, long long count) {
     if (st.release_step) st.release_step += begin;
     if (st.prev) st.prev += begin;
     if (st.nn_ok) st.nn_ok += begin;
+    if (st.elem) st.elem += begin;
     st.P = count;
     return st;
 }
@@ -1167,6 +1257,8 @@ int kc_run_fused(kc_ctx* c, const kc_step_args* steps, int n_steps, const kc_bea
             c->slots[a.slot_a].dtype != c->slots[a0.slot_a].dtype)
             return fail(c, KC_ERR_ARG, "kc_run_fused: every step needs the same dims, scheme, form and snapshot type");
     }
+    if (c->has_elem)
+        return fail(c, KC_ERR_STATE, "kc_run_fused: carried walk elements step through kc_step / kc_run");
     if (c->P == 0) return KC_OK;
     KC_CUDA(c, cudaSetDevice(c->device));
     if ((rc = pin_pid(c))) return rc;
@@ -1211,6 +1303,57 @@ int kc_find_nearest(kc_ctx* c, long long P, const double* lon, const double* lat
     KC_CUDA(c, cudaMemcpyAsync(c->q, lon, (size_t)P * 8, cudaMemcpyHostToDevice, c->stream));
     KC_CUDA(c, cudaMemcpyAsync(c->q + P, lat, (size_t)P * 8, cudaMemcpyHostToDevice, c->stream));
     k_nearest<<<grid_for(P), kBlock, 0, c->stream>>>(c->dm, c->q, P, c->qout);
+    KC_CUDA(c, cudaGetLastError());
+    KC_CUDA(c, cudaMemcpyAsync(out, c->qout, (size_t)P * 4, cudaMemcpyDeviceToHost, c->stream));
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KC_OK;
+}
+
+int kc_find_elements(kc_ctx* c, long long P, const double* lon, const double* lat, const int* nn, int* out) {
+    if (!c) return KC_ERR_ARG;
+    if (!c->has_mesh) return fail(c, KC_ERR_STATE, "kc_find_elements: no mesh uploaded");
+    if (P < 0 || (P > 0 && (!lon || !lat || !out))) return fail(c, KC_ERR_ARG, "kc_find_elements: arrays");
+    if (nn)
+        for (long long i = 0; i < P; ++i)
+            if (nn[i] < 0 || nn[i] >= c->N) return fail(c, KC_ERR_ARG, "kc_find_elements: anchor out of range");
+    if (P == 0) return KC_OK;
+    KC_CUDA(c, cudaSetDevice(c->device));
+    if (P > c->qcap) {
+        KC_CUDA(c, cudaStreamSynchronize(c->stream));
+        dfree(c->q); dfree(c->qout);
+        KC_CUDA(c, cudaMalloc((void**)&c->q, (size_t)P * 16));
+        KC_CUDA(c, cudaMalloc((void**)&c->qout, (size_t)P * 4));
+        c->qcap = P;
+    }
+    KC_CUDA(c, cudaMemcpyAsync(c->q, lon, (size_t)P * 8, cudaMemcpyHostToDevice, c->stream));
+    KC_CUDA(c, cudaMemcpyAsync(c->q + P, lat, (size_t)P * 8, cudaMemcpyHostToDevice, c->stream));
+    if (nn) KC_CUDA(c, cudaMemcpyAsync(c->qout, nn, (size_t)P * 4, cudaMemcpyHostToDevice, c->stream));
+    k_contain<<<grid_for(P), kBlock, 0, c->stream>>>(c->dm, c->q, P, nn ? c->qout : nullptr, c->qout);
+    KC_CUDA(c, cudaGetLastError());
+    KC_CUDA(c, cudaMemcpyAsync(out, c->qout, (size_t)P * 4, cudaMemcpyDeviceToHost, c->stream));
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KC_OK;
+}
+
+int kc_find_elements_walk(kc_ctx* c, long long P, const double* lon, const double* lat, const int* start, int* out) {
+    if (!c) return KC_ERR_ARG;
+    if (!c->has_mesh) return fail(c, KC_ERR_STATE, "kc_find_elements_walk: no mesh uploaded");
+    if (!c->dm.enb) return fail(c, KC_ERR_STATE, "kc_find_elements_walk: upload the element neighbours first");
+    if (P < 0 || (P > 0 && (!lon || !lat || !start || !out)))
+        return fail(c, KC_ERR_ARG, "kc_find_elements_walk: arrays");
+    if (P == 0) return KC_OK;
+    KC_CUDA(c, cudaSetDevice(c->device));
+    if (P > c->qcap) {
+        KC_CUDA(c, cudaStreamSynchronize(c->stream));
+        dfree(c->q); dfree(c->qout);
+        KC_CUDA(c, cudaMalloc((void**)&c->q, (size_t)P * 16));
+        KC_CUDA(c, cudaMalloc((void**)&c->qout, (size_t)P * 4));
+        c->qcap = P;
+    }
+    KC_CUDA(c, cudaMemcpyAsync(c->q, lon, (size_t)P * 8, cudaMemcpyHostToDevice, c->stream));
+    KC_CUDA(c, cudaMemcpyAsync(c->q + P, lat, (size_t)P * 8, cudaMemcpyHostToDevice, c->stream));
+    KC_CUDA(c, cudaMemcpyAsync(c->qout, start, (size_t)P * 4, cudaMemcpyHostToDevice, c->stream));
+    k_walk<<<grid_for(P), kBlock, 0, c->stream>>>(c->dm, c->q, P, c->qout, c->qout);
     KC_CUDA(c, cudaGetLastError());
     KC_CUDA(c, cudaMemcpyAsync(out, c->qout, (size_t)P * 4, cudaMemcpyDeviceToHost, c->stream));
     KC_CUDA(c, cudaStreamSynchronize(c->stream));

@@ -52,6 +52,8 @@ struct DMesh {
     const double* dl_p;       // (M) depth-linear data points (uv_vertical level / layer_linear)
     const int* dl_last;       // (N) last usable data point per node
     const double* dl_bed;     // (N) bed depth per node for the wall test
+    const int4* enb;          // (E) edge neighbours of the compacted ring (edge walk), or null
+    long long E;
     double cell, lon_min, lat_min, r_earth;
     int nx, ny, wrap, far_rows, K, exact, dl_M;
     int* err;                 // device error word
@@ -499,8 +501,12 @@ static __device__ __noinline__ int nearest_exact(const DMesh& m, const Site& q) 
 }
 
 // The anchor of one evaluation site (integrators.py:1470-1487).
+// A finite position always has a nearest node; a non-finite one (a NaN
+// velocity upstream) gets node 0, so every table read stays in bounds while
+// its containment test fails.
 __device__ __forceinline__ int site_anchor(const DMesh& m, const Site& q) {
-    return m.exact ? nearest_exact(m, q) : nearest_widened(m, q);
+    const int r = m.exact ? nearest_exact(m, q) : nearest_widened(m, q);
+    return r >= 0 ? r : 0;
 }
 
 // ---------------------------------------------------------------------------

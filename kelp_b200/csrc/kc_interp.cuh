@@ -155,8 +155,9 @@ __device__ __noinline__ bool interp_uv_at(const DMesh& m, const DBlend<T>& f, in
 
 template <typename T>
 __device__ __forceinline__ bool interp_uv_bary(const DMesh& m, const DBlend<T>& f, double xp, double yp, int nn,
-                                               double time_dir, int row, double alpha, double& U, double& V) {
-    const int elem = contain_local(m, xp, yp, nn);
+                                               int hint, double time_dir, int row, double alpha, double& U,
+                                               double& V) {
+    const int elem = hint >= 0 ? hint : contain_local(m, xp, yp, nn);
     if (elem < 0) {
         U = 0.0;
         V = 0.0;
@@ -309,8 +310,9 @@ __device__ __noinline__ bool interp_uv_dl_at(const DMesh& m, const DBlend<T>& f,
 
 template <typename T>
 __device__ __forceinline__ bool interp_uv_bary_dl(const DMesh& m, const DBlend<T>& f, double xp, double yp, int nn,
-                                                  double z, double time_dir, double alpha, double& U, double& V) {
-    const int elem = contain_local(m, xp, yp, nn);
+                                                  int hint, double z, double time_dir, double alpha, double& U,
+                                                  double& V) {
+    const int elem = hint >= 0 ? hint : contain_local(m, xp, yp, nn);
     if (elem < 0) {
         U = 0.0;
         V = 0.0;
@@ -629,6 +631,100 @@ static __device__ __noinline__ int w_search_elem(const DMesh& m, double xp, doub
         }
     }
     return -1;
+}
+
+// mesh.py:2488-2590 _walk_containing_element: from element e, cross the edge
+// of the most negative normalized signed-area coordinate (projection of
+// mesh.py:2006-2051 in the element's own frame) until every coordinate is
+// >= -1e-6; an accept within the 1e-2 band is verified with the exact local
+// predicate; at most 256 crossings; -1 for every non-contained outcome.
+static __device__ __noinline__ int edge_walk(const DMesh& m, double lon_p, double lat_p, int e) {
+    if (e < 0 || (long long)e >= m.E || !m.enb) return -1;
+    int prev = -1;
+    for (int it = 0; it < 256; ++it) {
+        Ring r;
+        load_ring(m, __ldg(&m.en[e]), r);
+        const int nv = r.n;
+        if (nv < 3) return -1;
+        double lmin = r.ln[0], lmax = r.ln[0];
+#pragma unroll
+        for (int k = 1; k < 4; ++k)
+            if (k < nv) { lmin = fmin(lmin, r.ln[k]); lmax = fmax(lmax, r.ln[k]); }
+        double lon0;
+        if (lmax - lmin > 180.0) {
+            double ds = 0.0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (k < nv) ds += wrap180(r.ln[k] - r.ln[0]);
+            lon0 = r.ln[0] + ds / (double)nv;
+        } else {
+            double sm = 0.0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (k < nv) sm += r.ln[k];
+            lon0 = sm / (double)nv;
+        }
+        double sl = 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (k < nv) sl += r.la[k];
+        const double lat0 = sl / (double)nv;
+        const double cl = __ldg(&m.ecos[e]).y;   // cos(mean ring latitude), the host C library's
+        double x[4], y[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            x[k] = wrap180(r.ln[k] - lon0) * DEG2RAD * R_STD * cl;
+            y[k] = (r.la[k] - lat0) * DEG2RAD * R_STD;
+        }
+        const double px = wrap180(lon_p - lon0) * DEG2RAD * R_STD * cl;
+        const double py = (lat_p - lat0) * DEG2RAD * R_STD;
+        double S = 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (k < nv) {
+                const int j = k + 1 < nv ? k + 1 : 0;
+                S += x[k] * y[j] - x[j] * y[k];
+            }
+        }
+        const double absS = fabs(S);
+        if (absS < AREA_TOL) return -1;
+        const double sgn = S > 0.0 ? 1.0 : -1.0;
+        double worst = 1.0e100;
+        int worst_k = -1;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (k < nv) {
+                const int j = k + 1 < nv ? k + 1 : 0;
+                const double A = (x[j] - x[k]) * (py - y[k]) - (px - x[k]) * (y[j] - y[k]);
+                const double w = A * sgn / absS;
+                if (w < worst) { worst = w; worst_k = k; }
+            }
+        }
+        if (worst >= -1e-6) {
+            if (worst >= 1e-2) return e;
+            return element_contains(m, e, lon_p, lat_p) ? e : -1;
+        }
+        const int4 nb4 = __ldg(&m.enb[e]);
+        const int nb = worst_k == 0 ? nb4.x : (worst_k == 1 ? nb4.y : (worst_k == 2 ? nb4.z : nb4.w));
+        if (nb < 0 || nb == prev) return -1;
+        prev = e;
+        e = nb;
+    }
+    return -1;
+}
+
+// mesh.py:2593-2712 find_containing_elements_walk for one point: the walk
+// from the carried element, else the local scan around the widened anchor,
+// else around the exact anchor nn (the exactness heal); -1 outside.
+static __device__ __noinline__ int walk_locate(const DMesh& m, double lon_p, double lat_p, int start, int nn) {
+    if (start >= 0) {
+        const int e = edge_walk(m, lon_p, lat_p, start);
+        if (e >= 0) return e;
+    }
+    const int nw = nearest_widened(m, make_site(lon_p, lat_p));
+    const int e = nw >= 0 ? contain_local(m, lon_p, lat_p, nw) : -1;
+    if (e >= 0) return e;
+    return contain_local(m, lon_p, lat_p, nn);
 }
 
 // ---------------------------------------------------------------------------

@@ -21,25 +21,25 @@ __device__ __forceinline__ void activate(const kc::DState& st, const kc::DStep& 
         st.status[i] = kc::ALIVE;
 }
 
-template <typename T, int SCHEME, typename Form>
+template <typename T, int SCHEME, typename Form, bool WALK>
 __global__ void __launch_bounds__(kBlock, KC_STEP_MIN_BLOCKS) k_step2d(const __grid_constant__ kc::DMesh m, const __grid_constant__ kc::DBlend<T> f, const __grid_constant__ kc::DState st, const __grid_constant__ kc::DStep s) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= st.P) return;
     activate(st, s, i);
     if (st.prev) st.prev[i] = st.status[i];
-    kc::step2d_particle<T, SCHEME, Form>(m, f, st, s, i);
+    kc::step2d_particle<T, SCHEME, Form, WALK>(m, f, st, s, i);
 }
 
-template <typename T, typename Form>
+template <typename T, typename Form, bool WALK>
 __global__ void __launch_bounds__(kBlock, KC_STEP_MIN_BLOCKS) k_step3d_rk2(const __grid_constant__ kc::DMesh m, const __grid_constant__ kc::DBlend<T> f, const __grid_constant__ kc::DState st, const __grid_constant__ kc::DStep s) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= st.P) return;
     activate(st, s, i);
     if (st.prev) st.prev[i] = st.status[i];
-    kc::step3d_rk2_particle<T, Form>(m, f, st, s, i);
+    kc::step3d_rk2_particle<T, Form, WALK>(m, f, st, s, i);
 }
 
-template <typename T, int SCHEME, typename Form>
+template <typename T, int SCHEME, typename Form, bool WALK>
 __global__ void __launch_bounds__(kBlock, KC_STEP_MIN_BLOCKS) k_step3d_unfused(const __grid_constant__ kc::DMesh m,
                                                            const __grid_constant__ kc::DBlend<T> f,
                                                            const __grid_constant__ kc::DState st,
@@ -48,24 +48,32 @@ __global__ void __launch_bounds__(kBlock, KC_STEP_MIN_BLOCKS) k_step3d_unfused(c
     if (i >= st.P) return;
     activate(st, s, i);
     if (st.prev) st.prev[i] = st.status[i];
-    kc::step3d_unfused_particle<T, SCHEME, Form>(m, f, st, s, i);
+    kc::step3d_unfused_particle<T, SCHEME, Form, WALK>(m, f, st, s, i);
 }
 
 
-// Launch one step of every particle: dims 2 / 3, scheme 0 Euler, 1 RK2, 2 RK4.
+// Launch one step of every particle: dims 2 / 3, scheme 0 Euler, 1 RK2, 2 RK4;
+// the walk-mode instantiations when the state carries elements.
+template <typename T, typename Form, bool WALK>
+void launch_step_kernel_t(const kc::DMesh& m, const kc::DBlend<T>& f, const kc::DState& st, const kc::DStep& s,
+                          int dims, int scheme, cudaStream_t stream) {
+    const unsigned g = (unsigned)((st.P + kBlock - 1) / kBlock);
+    if (dims == 2) {
+        if (scheme == 0) k_step2d<T, 0, Form, WALK><<<g, kBlock, 0, stream>>>(m, f, st, s);
+        else if (scheme == 1) k_step2d<T, 1, Form, WALK><<<g, kBlock, 0, stream>>>(m, f, st, s);
+        else k_step2d<T, 2, Form, WALK><<<g, kBlock, 0, stream>>>(m, f, st, s);
+    } else {
+        if (scheme == 1) k_step3d_rk2<T, Form, WALK><<<g, kBlock, 0, stream>>>(m, f, st, s);
+        else if (scheme == 2) k_step3d_unfused<T, 2, Form, WALK><<<g, kBlock, 0, stream>>>(m, f, st, s);
+        else k_step3d_unfused<T, 0, Form, WALK><<<g, kBlock, 0, stream>>>(m, f, st, s);
+    }
+}
+
 template <typename T, typename Form>
 void launch_step_kernel(const kc::DMesh& m, const kc::DBlend<T>& f, const kc::DState& st, const kc::DStep& s,
                         int dims, int scheme, cudaStream_t stream) {
-    const unsigned g = (unsigned)((st.P + kBlock - 1) / kBlock);
-    if (dims == 2) {
-        if (scheme == 0) k_step2d<T, 0, Form><<<g, kBlock, 0, stream>>>(m, f, st, s);
-        else if (scheme == 1) k_step2d<T, 1, Form><<<g, kBlock, 0, stream>>>(m, f, st, s);
-        else k_step2d<T, 2, Form><<<g, kBlock, 0, stream>>>(m, f, st, s);
-    } else {
-        if (scheme == 1) k_step3d_rk2<T, Form><<<g, kBlock, 0, stream>>>(m, f, st, s);
-        else if (scheme == 2) k_step3d_unfused<T, 2, Form><<<g, kBlock, 0, stream>>>(m, f, st, s);
-        else k_step3d_unfused<T, 0, Form><<<g, kBlock, 0, stream>>>(m, f, st, s);
-    }
+    if (st.elem) launch_step_kernel_t<T, Form, true>(m, f, st, s, dims, scheme, stream);
+    else launch_step_kernel_t<T, Form, false>(m, f, st, s, dims, scheme, stream);
 }
 
 // ---------------------------------------------------------------------------
@@ -75,7 +83,9 @@ void launch_step_kernel(const kc::DMesh& m, const kc::DBlend<T>& f, const kc::DS
 // read from device memory: the state view (kc_sort swaps its buffers) and,
 // per step, the snapshot blend, the step arguments and the beaching
 // arguments.  So one launch can be captured in a CUDA graph and replayed with
-// the next steps' arguments copied into the same device buffer.
+// the next steps' arguments copied into the same device buffer.  Local
+// element search only: a state that carries walk elements steps through the
+// per-step kernels.
 // ---------------------------------------------------------------------------
 
 template <typename T>

@@ -28,6 +28,7 @@ struct DState {
     const int* release_step;   // delayed release (null: all released)
     int* prev;                 // status at the step's entry, for the beaching hook (null: not kept)
     unsigned char* nn_ok;      // 1: nn is the exact anchor of the current position (null: never trusted)
+    int* elem;                 // carried containing element (elem_search walk), null: the local scan
     long long P;
 };
 
@@ -80,6 +81,24 @@ __device__ __forceinline__ void mark_anchor(const DState& st, long long i, int s
 // (several ensemble members in one array), else the step's.
 __device__ __forceinline__ unsigned long long realization_of(const DState& st, const DStep& s, long long i) {
     return st.rid ? (unsigned long long)st.rid[i] : s.real_id;
+}
+
+// Walk mode (elem_search: walk, integrators.py:5019-5147, :5415-5608,
+// :5792-6011): the containing element of a stage position walked from the
+// previous stage's, handed to the interpolation in place of its local scan;
+// -1 (no hint) in local mode.
+template <bool WALK>
+__device__ __forceinline__ int stage_elem(const DMesh& m, double lon, double lat, int from, int nn) {
+    if constexpr (WALK) return walk_locate(m, lon, lat, from, nn);
+    else return -1;
+}
+
+// The end-of-step containment: the walk from the last stage's element, or the
+// local scan around the exact anchor of the new position.
+template <bool WALK>
+__device__ __forceinline__ int end_elem(const DMesh& m, double lon, double lat, int from, int nn) {
+    if constexpr (WALK) return walk_locate(m, lon, lat, from, nn);
+    else return contain_local(m, lon, lat, nn);
 }
 
 // integrators.py:673-818 _apply_split_diffusion_kick for one particle that is
@@ -231,7 +250,7 @@ __device__ __noinline__ void apply_az(const DMesh& m, const DBlend<T>& f, const 
 // integrators.py:2521-2638 (RK2), :2641-2816 (RK4); Euler follows the
 // per-particle arithmetic of the unfused path (integrators.py:4997-5147):
 // one stage at the start, move, re-anchor, domain check.
-template <typename T, int SCHEME, typename Form>
+template <typename T, int SCHEME, typename Form, bool WALK = false>
 __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>& f, const DState& st,
                                                 const DStep& s, long long i) {
     int status = st.status[i];
@@ -249,9 +268,11 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
     bool failed = false;
     const Site q0 = make_site(lon0, lat0);
     const int node_i = start_anchor(m, st, q0, pre_nn, i);
+    const int e1 = stage_elem<WALK>(m, lon0, lat0, WALK ? st.elem[i] : -1, node_i);
+    int e_last = e1, e_out = e1;
 
     double U1, V1;
-    bool ok1 = Form::uv2(m, f, s, lon0, lat0, node_i, s.ak[0], U1, V1);
+    bool ok1 = Form::uv2(m, f, s, lon0, lat0, node_i, e1, s.ak[0], U1, V1);
     st.U[i] = U1;
     st.V[i] = V1;
     if (!ok1) {
@@ -264,8 +285,9 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
         double lat_mid = clamp_lat(lat0 + 0.5 * dt * V1 / SLM);
         const Site qm = make_site(lon_mid, lat_mid);
         int nn_mid = site_anchor(m, qm);
+        e_last = stage_elem<WALK>(m, lon_mid, lat_mid, e1, nn_mid);
         double U2, V2;
-        if (!Form::uv2(m, f, s, lon_mid, lat_mid, nn_mid, s.ak[1], U2, V2)) {
+        if (!Form::uv2(m, f, s, lon_mid, lat_mid, nn_mid, e_last, s.ak[1], U2, V2)) {
             status = OUTSIDE; fr = FR_INTERP; nn_out = node_i; failed = true;
         } else {
             lon_new = wrap180(lon0 + dt * U2 / metric_z0(qm));
@@ -277,8 +299,10 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
         double lon2 = wrap180(lon0 + 0.5 * dlon1);
         double lat2 = clamp_lat(lat0 + 0.5 * dlat1);
         const Site q2 = make_site(lon2, lat2);
+        const int n2 = site_anchor(m, q2);
+        const int e2 = stage_elem<WALK>(m, lon2, lat2, e1, n2);
         double U2, V2;
-        if (!Form::uv2(m, f, s, lon2, lat2, site_anchor(m, q2), s.ak[1], U2, V2)) {
+        if (!Form::uv2(m, f, s, lon2, lat2, n2, e2, s.ak[1], U2, V2)) {
             status = OUTSIDE; fr = FR_INTERP; nn_out = node_i; failed = true;
         } else {
             double dlon2 = dt * U2 / metric_z0(q2);
@@ -286,8 +310,10 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
             double lon3 = wrap180(lon0 + 0.5 * dlon2);
             double lat3 = clamp_lat(lat0 + 0.5 * dlat2);
             const Site q3 = make_site(lon3, lat3);
+            const int n3 = site_anchor(m, q3);
+            const int e3 = stage_elem<WALK>(m, lon3, lat3, e2, n3);
             double U3, V3;
-            if (!Form::uv2(m, f, s, lon3, lat3, site_anchor(m, q3), s.ak[2], U3, V3)) {
+            if (!Form::uv2(m, f, s, lon3, lat3, n3, e3, s.ak[2], U3, V3)) {
                 status = OUTSIDE; fr = FR_INTERP; nn_out = node_i; failed = true;
             } else {
                 double dlon3 = dt * U3 / metric_z0(q3);
@@ -295,8 +321,10 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
                 double lon4 = wrap180(lon0 + dlon3);
                 double lat4 = clamp_lat(lat0 + dlat3);
                 const Site q4 = make_site(lon4, lat4);
+                const int n4 = site_anchor(m, q4);
+                e_last = stage_elem<WALK>(m, lon4, lat4, e3, n4);
                 double U4, V4;
-                if (!Form::uv2(m, f, s, lon4, lat4, site_anchor(m, q4), s.ak[3], U4, V4)) {
+                if (!Form::uv2(m, f, s, lon4, lat4, n4, e_last, s.ak[3], U4, V4)) {
                     status = OUTSIDE; fr = FR_INTERP; nn_out = node_i; failed = true;
                 } else {
                     double dlon4 = dt * U4 / metric_z0(q4);
@@ -312,12 +340,14 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
     if (!failed) {
         const Site qn = make_site(lon_new, lat_new);
         int nn_new = site_anchor(m, qn);
-        if (contain_local(m, lon_new, lat_new, nn_new) < 0) {
+        const int ein = end_elem<WALK>(m, lon_new, lat_new, e_last, nn_new);
+        if (ein < 0) {
             status = OUTSIDE; fr = FR_OOB; nn_out = node_i;
             lon_new = lon0; lat_new = lat0;
         } else {
             status = ALIVE;
             nn_out = nn_new;
+            e_out = ein;
             if (s.kick) {
                 double zz = 0.0;
                 long long pid = st.pid ? st.pid[i] : i;
@@ -333,6 +363,7 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
     st.status[i] = status;
     st.nn[i] = nn_out;
     st.fr[i] = fr;
+    if constexpr (WALK) st.elem[i] = e_out;
     mark_anchor(st, i, status, nn_out, node_i);
 }
 
@@ -348,26 +379,34 @@ __device__ __forceinline__ double stage_w(const DMesh& m, const DBlend<T>& f, in
 // (:4071-4098).
 template <typename T>
 __device__ __forceinline__ bool stage_uv(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
-                                         double lat, int nn, double z, double alpha, double& U, double& V) {
-    if (s.uv_dl) return interp_uv_bary_dl<T>(m, f, lon, lat, nn, z, s.time_dir, alpha, U, V);
+                                         double lat, int nn, int hint, double z, double alpha, double& U,
+                                         double& V) {
+    if (s.uv_dl) return interp_uv_bary_dl<T>(m, f, lon, lat, nn, hint, z, s.time_dir, alpha, U, V);
     const int layer = find_layer(m, z, nn);
-    return interp_uv_bary<T>(m, f, lon, lat, nn, s.time_dir, layer, alpha, U, V);
+    return interp_uv_bary<T>(m, f, lon, lat, nn, hint, s.time_dir, layer, alpha, U, V);
 }
 
 // The plain form: the reference's float64 interpolation, bit for bit.
 // uvw3 evaluates W even where u/v failed (the caller then discards it).
+// hint >= 0 is the stage's containing element from the edge walk, which
+// replaces the u/v element search; the barycentric W keeps its own search.
 template <typename T>
 struct PlainForm {
     static __device__ __forceinline__ bool uv2(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
-                                               double lat, int nn, double alpha, double& U, double& V) {
-        return interp_uv_bary<T>(m, f, lon, lat, nn, s.time_dir, 0, alpha, U, V);
+                                               double lat, int nn, int hint, double alpha, double& U, double& V) {
+        return interp_uv_bary<T>(m, f, lon, lat, nn, hint, s.time_dir, 0, alpha, U, V);
     }
     static __device__ __forceinline__ bool uvw3(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
-                                                double lat, int nn, double z, double alpha, double& U, double& V,
-                                                double& W) {
+                                                double lat, int nn, int hint, double z, double alpha, double& U,
+                                                double& V, double& W) {
         if (s.w_code == 0) {
-            const bool ok = stage_uv<T>(m, f, s, lon, lat, nn, z, alpha, U, V);
+            const bool ok = stage_uv<T>(m, f, s, lon, lat, nn, hint, z, alpha, U, V);
             W = w_linear<T>(m, f, alpha, z, nn, s.time_dir);
+            return ok;
+        }
+        if (hint >= 0) {
+            const bool ok = stage_uv<T>(m, f, s, lon, lat, nn, hint, z, alpha, U, V);
+            W = w_bary<T>(m, f, alpha, lon, lat, z, nn, s.time_dir);
             return ok;
         }
         // W barycentric: one containment scan decides the u/v element and,
@@ -391,11 +430,13 @@ struct PlainForm {
 
 // One 3-D stage of the unfused paths: exact anchor at the stage position,
 // u/v at the stage depth, W from the stage blend.
-template <typename T, typename Form>
+template <typename T, typename Form, bool WALK>
 __device__ __forceinline__ bool stage3d(const DMesh& m, const DBlend<T>& f, const DStep& s, int k, double lon,
-                                        double lat, double z, const Site& q, double& U, double& V, double& W) {
+                                        double lat, double z, const Site& q, int from, int& e, double& U,
+                                        double& V, double& W) {
     const int nn = site_anchor(m, q);
-    return Form::uvw3(m, f, s, lon, lat, nn, z, s.ak[k], U, V, W);
+    e = stage_elem<WALK>(m, lon, lat, from, nn);
+    return Form::uvw3(m, f, s, lon, lat, nn, e, z, s.ak[k], U, V, W);
 }
 
 // 3-D Euler (integrators.py:4997-5147) and RK4 (:5760-6011): the reference's
@@ -403,7 +444,7 @@ __device__ __forceinline__ bool stage3d(const DMesh& m, const DBlend<T>& f, cons
 // every stage position, the layer at the stage depth, the whole-field stage
 // lerps of _make_stage_vels (:1187-1237) reproduced per vertex, W at the stage
 // position; a failure reverts to the start with the start anchor.
-template <typename T, int SCHEME, typename Form>
+template <typename T, int SCHEME, typename Form, bool WALK = false>
 __device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DBlend<T>& f, const DState& st,
                                                         const DStep& s, long long i) {
     int status = st.status[i];
@@ -422,8 +463,10 @@ __device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DB
     const Site q0 = make_site(lon0, lat0);
     const int node_i = start_anchor(m, st, q0, pre_nn, i);
     int nn_out = node_i;
+    const int e1 = stage_elem<WALK>(m, lon0, lat0, WALK ? st.elem[i] : -1, node_i);
+    int e_last = e1, e_out = e1;
     double U1, V1, W1;
-    bool ok = Form::uvw3(m, f, s, lon0, lat0, node_i, z0p, s.ak[0], U1, V1, W1);
+    bool ok = Form::uvw3(m, f, s, lon0, lat0, node_i, e1, z0p, s.ak[0], U1, V1, W1);
     st.U[i] = U1;
     st.V[i] = V1;
     st.W[i] = W1;
@@ -438,19 +481,20 @@ __device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DB
             const double l2 = wrap180(lon0 + 0.5 * dl1), t2 = clamp_lat(lat0 + 0.5 * dd1), z2 = z0p + 0.5 * dz1;
             const Site q2 = make_site(l2, t2);
             double U2, V2, W2;
-            ok = stage3d<T, Form>(m, f, s, 1, l2, t2, z2, q2, U2, V2, W2);
+            int e2, e3;
+            ok = stage3d<T, Form, WALK>(m, f, s, 1, l2, t2, z2, q2, e1, e2, U2, V2, W2);
             if (ok) {
                 const double dl2 = dt * U2 / metric_z0(q2), dd2 = dt * V2 / SLM, dz2 = dt * W2;
                 const double l3 = wrap180(lon0 + 0.5 * dl2), t3 = clamp_lat(lat0 + 0.5 * dd2), z3 = z0p + 0.5 * dz2;
                 const Site q3 = make_site(l3, t3);
                 double U3, V3, W3;
-                ok = stage3d<T, Form>(m, f, s, 2, l3, t3, z3, q3, U3, V3, W3);
+                ok = stage3d<T, Form, WALK>(m, f, s, 2, l3, t3, z3, q3, e2, e3, U3, V3, W3);
                 if (ok) {
                     const double dl3 = dt * U3 / metric_z0(q3), dd3 = dt * V3 / SLM, dz3 = dt * W3;
                     const double l4 = wrap180(lon0 + dl3), t4 = clamp_lat(lat0 + dd3), z4 = z0p + dz3;
                     const Site q4 = make_site(l4, t4);
                     double U4, V4, W4;
-                    ok = stage3d<T, Form>(m, f, s, 3, l4, t4, z4, q4, U4, V4, W4);
+                    ok = stage3d<T, Form, WALK>(m, f, s, 3, l4, t4, z4, q4, e3, e_last, U4, V4, W4);
                     if (ok) {
                         const double dl4 = dt * U4 / metric_z0(q4), dd4 = dt * V4 / SLM, dz4 = dt * W4;
                         const double dl = (dl1 + 2.0 * dl2 + 2.0 * dl3 + dl4) / 6.0;
@@ -469,7 +513,8 @@ __device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DB
     } else {
         const Site qn = make_site(a, b);
         const int nn_new = site_anchor(m, qn);
-        if (contain_local(m, a, b, nn_new) < 0) {
+        const int ein = end_elem<WALK>(m, a, b, e_last, nn_new);
+        if (ein < 0) {
             status = OUTSIDE; fr = FR_OOB;
         } else {
             if (c < m.zlev[0]) c = m.zlev[0];
@@ -478,6 +523,7 @@ __device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DB
             lon_new = a; lat_new = b; z_new = c;
             status = ALIVE;
             nn_out = nn_new;
+            e_out = ein;
             if (s.kick) {
                 long long pid = st.pid ? st.pid[i] : i;
                 apply_kick(m, s, pid, realization_of(st, s, i), qn, lon0, lat0, z0p, pre_nn, true, lon_new, lat_new, z_new, status, nn_out,
@@ -493,13 +539,14 @@ __device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DB
     st.status[i] = status;
     st.nn[i] = nn_out;
     st.fr[i] = fr;
+    if constexpr (WALK) st.elem[i] = e_out;
     mark_anchor(st, i, status, nn_out, node_i);
 }
 
 // integrators.py:3647-3856 _fused_rk2_step_3d_bary_tinterp (layer u/v,
 // z-level), with the exact stage-1 anchor of its runner (:4766-4770) and the
 // split kick epilogue.
-template <typename T, typename Form>
+template <typename T, typename Form, bool WALK = false>
 __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend<T>& f, const DState& st,
                                                     const DStep& s, long long i) {
     int status = st.status[i];
@@ -518,8 +565,10 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
     const Site q0 = make_site(lon0, lat0);
     const int node_i = start_anchor(m, st, q0, pre_nn, i);
     int nn_out = node_i;
+    const int e1 = stage_elem<WALK>(m, lon0, lat0, WALK ? st.elem[i] : -1, node_i);
+    int e_out = e1;
     double U1, V1, W1;
-    const bool ok1 = Form::uvw3(m, f, s, lon0, lat0, node_i, z0p, s.ak[0], U1, V1, W1);
+    const bool ok1 = Form::uvw3(m, f, s, lon0, lat0, node_i, e1, z0p, s.ak[0], U1, V1, W1);
     st.U[i] = U1;
     st.V[i] = V1;
     st.W[i] = W1;
@@ -531,8 +580,9 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
         const double z_mid = z0p + W1 * 0.5 * dt;
         const Site qm = make_site(lon_mid, lat_mid);
         const int nn_mid = site_anchor(m, qm);
+        const int em = stage_elem<WALK>(m, lon_mid, lat_mid, e1, nn_mid);
         double U2, V2, W2;
-        if (!Form::uvw3(m, f, s, lon_mid, lat_mid, nn_mid, z_mid, s.ak[1], U2, V2, W2)) {
+        if (!Form::uvw3(m, f, s, lon_mid, lat_mid, nn_mid, em, z_mid, s.ak[1], U2, V2, W2)) {
             status = OUTSIDE; fr = FR_INTERP;
         } else {
             const double ln = wrap180(lon0 + dt * U2 / metric_z0(qm));
@@ -540,7 +590,8 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
             double zn = z0p + W2 * dt;
             const Site qn = make_site(ln, lt);
             const int nn_new = site_anchor(m, qn);
-            if (contain_local(m, ln, lt, nn_new) < 0) {
+            const int ein = end_elem<WALK>(m, ln, lt, em, nn_new);
+            if (ein < 0) {
                 status = OUTSIDE; fr = FR_OOB;
             } else {
                 if (zn < m.zlev[0]) zn = m.zlev[0];
@@ -549,6 +600,7 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
                 lon_new = ln; lat_new = lt; z_new = zn;
                 status = ALIVE;
                 nn_out = nn_new;
+                e_out = ein;
                 if (s.kick) {
                     long long pid = st.pid ? st.pid[i] : i;
                     apply_kick(m, s, pid, realization_of(st, s, i), qn, lon0, lat0, z0p, pre_nn, true, lon_new, lat_new, z_new, status,
@@ -565,6 +617,7 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
     st.status[i] = status;
     st.nn[i] = nn_out;
     st.fr[i] = fr;
+    if constexpr (WALK) st.elem[i] = e_out;
     mark_anchor(st, i, status, nn_out, node_i);
 }
 

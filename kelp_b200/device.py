@@ -126,6 +126,19 @@ class DeviceContext:
         self._slots.clear()
         self._dl_key = None
         self._coastal_key = None
+        self._enb_key = None
+
+    def ensure_elem_neighbors(self, mesh) -> None:
+        """Upload the edge-neighbour table of the resident mesh (built by
+        mesh.build_elem_neighbors on first use; cached)."""
+        from .mesh import build_elem_neighbors
+        self.ensure_mesh(mesh)
+        if getattr(self, "_enb_key", None) == self._mesh_key:
+            return
+        enb = np.ascontiguousarray(build_elem_neighbors(mesh), dtype=np.int32)
+        self._chk(N.lib().kc_elem_neighbors_upload(self._ctx, int(enb.shape[1]), N.ptr(enb)),
+                  "kc_elem_neighbors_upload")
+        self._enb_key = self._mesh_key
 
     def ensure_depth_points(self, mesh, placement: str) -> int:
         """Upload the depth-linear data-point table of ``mesh`` for
@@ -273,7 +286,8 @@ class DeviceContext:
         (``pinned_empty``) let the copies overlap the step."""
         types = {"lon": np.float64, "lat": np.float64, "z": np.float64, "status": np.int32,
                  "nearest_node": np.int32, "failure_reason": np.int8, "u": np.float64, "v": np.float64,
-                 "w": np.float64, "pid": np.int64, "real_id": np.int32, "release_step": np.int32}
+                 "w": np.float64, "pid": np.int64, "real_id": np.int32, "release_step": np.int32,
+                 "elem": np.int32}
 
         def pack(d, names):
             h = N.HostParticles()
@@ -292,8 +306,9 @@ class DeviceContext:
             return h, P
 
         hi, P = pack(inp, ("lon", "lat", "z", "status", "nearest_node", "failure_reason", "pid", "real_id",
-                           "release_step"))
-        ho, P2 = pack(out, ("lon", "lat", "z", "status", "nearest_node", "failure_reason", "u", "v", "w"))
+                           "release_step", "elem"))
+        ho, P2 = pack(out, ("lon", "lat", "z", "status", "nearest_node", "failure_reason", "u", "v", "w",
+                            "elem"))
         if P is None or P2 != P:
             raise ValueError("input and output particle counts differ")
         self._chk(N.lib().kc_step_host(self._ctx, C.byref(args), P, C.byref(hi), C.byref(ho), int(chunk)),
@@ -307,6 +322,46 @@ class DeviceContext:
         if rid is not None and rid.shape != (self.P,):
             raise ValueError("one realization id per resident particle")
         self._chk(N.lib().kc_particles_set_realization(self._ctx, N.ptr(rid)), "kc_particles_set_realization")
+
+    def set_elem(self, elem=None) -> None:
+        """Carried containing elements of the resident particles (elem_search
+        walk; -1 = no guess); None returns to the local search.  Needs the
+        neighbour table (ensure_elem_neighbors)."""
+        e = None if elem is None else _c(elem, np.int32)
+        if e is not None and e.shape != (self.P,):
+            raise ValueError("one carried element per resident particle")
+        self._chk(N.lib().kc_particles_set_elem(self._ctx, N.ptr(e)), "kc_particles_set_elem")
+
+    def get_elem(self) -> np.ndarray:
+        out = np.empty(self.P, np.int32)
+        self._chk(N.lib().kc_particles_get_elem(self._ctx, self.P, N.ptr(out)), "kc_particles_get_elem")
+        return out
+
+    def find_elements(self, lon, lat, nn=None) -> np.ndarray:
+        """mesh.find_containing_elements on the device: the 1-ring / 2-ring
+        scan around nn (None: the exact nearest node); -1 outside."""
+        lon = _c(lon, np.float64)
+        lat = _c(lat, np.float64)
+        a = None if nn is None else _c(nn, np.int32)
+        if lon.shape != lat.shape or (a is not None and a.shape != lon.shape):
+            raise ValueError("lon, lat and nn must have the same length")
+        out = np.empty(lon.shape[0], np.int32)
+        self._chk(N.lib().kc_find_elements(self._ctx, lon.shape[0], N.ptr(lon), N.ptr(lat), N.ptr(a), N.ptr(out)),
+                  "kc_find_elements")
+        return out
+
+    def find_elements_walk(self, lon, lat, start) -> np.ndarray:
+        """mesh.find_containing_elements_walk on the device: the containing
+        element of each point walked from start (-1: no guess); -1 outside."""
+        lon = _c(lon, np.float64)
+        lat = _c(lat, np.float64)
+        st = _c(start, np.int32)
+        if not (lon.shape == lat.shape == st.shape):
+            raise ValueError("lon, lat and start must have the same length")
+        out = np.empty(lon.shape[0], np.int32)
+        self._chk(N.lib().kc_find_elements_walk(self._ctx, lon.shape[0], N.ptr(lon), N.ptr(lat), N.ptr(st),
+                                                N.ptr(out)), "kc_find_elements_walk")
+        return out
 
     def step_range(self, args: N.StepArgs, begin: int, count: int) -> None:
         """One step of the resident particles [begin, begin + count)."""

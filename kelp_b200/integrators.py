@@ -148,8 +148,6 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
                                   "use 'barycentric' (node-layout velocities)")
     if kw.get("recon") is not None:
         raise NotImplementedError("PCHIP temporal reconstruction is not built on the CUDA backend")
-    if elem is not None:
-        raise NotImplementedError("elem_search: walk (carried elements) is not built on the CUDA backend")
     if not (mesh.metadata or {}).get("exact_nearest", False):
         raise NotImplementedError("the CUDA backend anchors with the exact nearest-node search only "
                                   "(mesh.exact_nearest: true, the configuration default)")
@@ -194,6 +192,8 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
 
     ctx = ctx or default_context()
     ctx.ensure_mesh(mesh)
+    if elem is not None:   # elem_search: walk -- the edge walk reads the neighbour table
+        ctx.ensure_elem_neighbors(mesh)
     if is3d and placement != "layer":
         ctx.ensure_depth_points(mesh, placement)
     sa, sb, st = ctx.slots_for([vel_a, vel_b, target], store)
@@ -244,17 +244,24 @@ def _run(state, vel, mesh, dt, time_dir, scheme, kw, ctx=None) -> ParticleState:
            "status": np.empty(P, np.int32), "nearest_node": np.empty(P, np.int32),
            "failure_reason": None if fr_in is None else np.empty(P, np.int8),
            "u": np.empty(P), "v": np.empty(P), "w": np.empty(P) if is3d else None}
+    walk = state.elem is not None
+    if walk:   # elem_search: walk (integrators.py:5415-5416): carried elements in and out
+        inp["elem"] = np.ascontiguousarray(state.elem, dtype=np.int32)
+        out["elem"] = np.empty(P, np.int32)
     # one call: chunked upload, step and download overlapped on the device
     ctx.step_host(a, inp, out)
     err = ctx.device_errors()
     if err:
         raise N.KcError(N.KC_ERR_DEVICE, N.describe_device_errors(err))
-    return state.replace(
+    new = state.replace(
         lon=out["lon"], lat=out["lat"], z=out["z"] if is3d else np.array(state.z, copy=True),
         status=out["status"], nearest_node=out["nearest_node"],
         u=out["u"], v=out["v"], w=out["w"],
         failure_reason=out["failure_reason"],
     )
+    if walk:
+        new = new.replace(elem=out["elem"])
+    return new
 
 
 def euler_step(state, vel, mesh, dt, time_dir, layer: int = 0, **kwargs) -> ParticleState:

@@ -203,12 +203,16 @@ class Tracker:
     ``diffusion`` a ``DiffusionConfig``-like object (``enabled``, ``scheme``
     uniform, ``kh_zonal``, ``kh_meridional``, ``seed``) or None;
     ``beaching`` a ``BeachingConfig`` or None.  ``precision`` and ``snapshots``
-    select the numerical form as for the step functions."""
+    select the numerical form as for the step functions.  ``elem_search``
+    "walk" carries each particle's containing element from step to step
+    (tracking.py:2236-2253: seeded once at the start by the local search
+    around the exact anchor unless the initial state carries them)."""
 
     def __init__(self, mesh, fields: Sequence, file_times, *, integrator: str = "rk2", dt: float,
                  time_dir: float = 1.0, uv_interp: str = "barycentric", w_interp: str = "barycentric",
                  diffusion=None, beaching: Optional[BeachingConfig] = None, on_exhausted: str = "stop",
-                 precision: str = "plain", snapshots: Optional[str] = None, sort_every: int = 16, ctx=None):
+                 precision: str = "plain", snapshots: Optional[str] = None, sort_every: int = 16,
+                 elem_search: str = "local", ctx=None):
         if integrator not in ("euler", "rk2", "rk4"):
             raise NotImplementedError(f"integrator {integrator!r} is not built on the CUDA backend")
         if on_exhausted not in ("stop", "cycle"):
@@ -217,6 +221,9 @@ class Tracker:
             raise ValueError(f"dt must be > 0, got {dt!r}")
         if float(time_dir) not in (1.0, -1.0):
             raise ValueError(f"time_dir must be +1 or -1, got {time_dir!r}")
+        if elem_search not in ("local", "walk"):
+            raise ValueError(f"elem_search must be 'local' or 'walk', got {elem_search!r}")
+        self.walk = elem_search == "walk"
         self.mesh = mesh
         self.fields = list(fields)
         self.file_times = np.asarray(file_times, dtype=np.float64)
@@ -291,6 +298,12 @@ class Tracker:
                              rep(init_state.nearest_node), rep(fr0), rep(np.arange(P, dtype=np.int64)), rs)
         if R > 1:
             ctx.set_realization(np.repeat(np.asarray(realizations, dtype=np.int32), P))
+        if self.walk:
+            ctx.ensure_elem_neighbors(mesh)
+            e0 = init_state.elem
+            if e0 is None:   # one local search around the exact anchor at the start
+                e0 = ctx.find_elements(init_state.lon, init_state.lat)
+            ctx.set_elem(rep(np.asarray(e0, dtype=np.int32)))
         beach_cfg = None
         if self.beaching is not None:
             seed = int(getattr(self.diffusion, "seed", 0)) if self.diffusion is not None else 0
@@ -338,13 +351,15 @@ class Tracker:
             raise N.KcError(N.KC_ERR_DEVICE, N.describe_device_errors(err))
         s = ctx.download_particles()
         ws = ctx.beach_state_download() if beach_cfg is not None else None
+        el = ctx.get_elem() if self.walk else None
         finals, wets = [], []
         for r in range(R):
             sl = slice(r * P, (r + 1) * P)
             finals.append(init_state.replace(lon=s["lon"][sl], lat=s["lat"][sl], z=s["z"][sl],
                                              status=s["status"][sl], nearest_node=s["nearest_node"][sl],
                                              failure_reason=s["failure_reason"][sl], u=s["u"][sl], v=s["v"][sl],
-                                             w=s["w"][sl] if self.dims == 3 else None))
+                                             w=s["w"][sl] if self.dims == 3 else None,
+                                             elem=None if el is None else el[sl]))
             wets.append(None if ws is None else ws[sl])
         return RunResult(records=records, final=finals, wet_streak=wets, steps=done)
 
@@ -479,7 +494,8 @@ def run_tracking(config, *, mesh=None, fields=None, file_times=None, seeds=None,
                       diffusion=diff if diff.enabled else None, beaching=beach_cfg,
                       on_exhausted=tim.get("on_exhausted", "stop"),
                       precision=num.get("cuda_precision", "plain"), snapshots=num.get("cuda_snapshots"),
-                      sort_every=int(num.get("sort_every", 16)), ctx=ctx)
+                      sort_every=int(num.get("sort_every", 16)),
+                      elem_search=num.get("elem_search", "local"), ctx=ctx)
     start_idx = int(tim.get("start_time_idx", 0))
     n_steps = tim.get("n_steps")
     if n_steps is None:

@@ -28,6 +28,10 @@ CASES += [("golden_3d", c) for c in ("rk2_wnear", "rk2_wbary", "rk2_wbary_kick",
                                      "rk2_wbary_kick_azf", "rk4_wnear_azf_nokh")]
 CASES += [("golden_dl_lev", c) for c in ("rk2_lev_wbary", "rk4_lev_wnear_kick", "euler_lev_wnear", "rk2_lev_wbary_azc")]
 CASES += [("golden_dl_llin", c) for c in ("rk2_llin_wbary", "rk4_llin_wnear_kick", "euler_llin_wnear")]
+# elem_search: walk (carried elements in and out of every step)
+WALK_CASES = [("golden_band", c) for c in ("rk2_walk", "rk4_walk_kick", "euler_walk")]
+WALK_CASES += [("golden_3d", c) for c in ("rk2_wbary_walk", "rk4_wnear_walk_kick")]
+CASES += WALK_CASES
 
 
 def replay_cuda(g, cname):
@@ -37,6 +41,8 @@ def replay_cuda(g, cname):
     fn = KI.get_integrator(scheme)
     w_interp = "barycentric" if "wbary" in cname else "nearest"
     st = g.particles()
+    if "elem0" in c:   # elem_search: walk
+        st = st.replace(elem=c["elem0"].copy())
     snaps = {}
     for k in range(int(n_steps)):
         vel, vnext, dtn = g.payload(c["schedule"][k], T)
@@ -49,7 +55,9 @@ def replay_cuda(g, cname):
 
 
 def assert_close_state(st, c, tag, where):
-    for name in ("status", "nearest_node", "failure_reason"):
+    for name in ("status", "nearest_node", "failure_reason", "elem"):
+        if tag + name not in c:
+            continue
         got = np.asarray(getattr(st, name))
         bad = np.flatnonzero(got != c[tag + name])
         assert bad.size == 0, f"{where} {name}: {bad.size} mismatches, first at {bad[:5]}"
@@ -212,3 +220,57 @@ def test_cuda_vs_oracle_healpix_3d_kick():
                                                "u", "v", "w")}
     assert_close_state(st, want, "f_", "healpix 3-D rk2 + kick")
     assert (st.status == 1).sum() > 0.5 * w.P
+
+
+@pytest.mark.parametrize("fixture", ["golden_band", "golden_3d"])
+def test_cuda_walk_batch_matches_oracle(golden, fixture):
+    """find_containing_elements_walk on the device against the oracle: from
+    the true element, from a distant start (walks many edges or gives up and
+    falls back), and with no start; points inside, outside and on the mesh
+    boundary."""
+    from oracle import oracle as O
+    from kelp_b200.device import default_context
+    g = golden(fixture)
+    m = g.mesh
+    rng = np.random.default_rng(11)
+    lon0, lat0 = np.asarray(m.nodes_lon), np.asarray(m.nodes_lat)
+    n = 4000
+    lon = rng.uniform(lon0.min() - 1.0, lon0.max() + 1.0, n)
+    lat = rng.uniform(lat0.min() - 1.0, lat0.max() + 1.0, n)
+    E = np.asarray(m.elem_nodes).shape[0]
+    ctx = default_context()
+    ctx.ensure_elem_neighbors(m)
+    nn = O.find_nearest(m, lon, lat)
+    truth = O.contain(m, lon, lat, nn)
+    np.testing.assert_array_equal(ctx.find_elements(lon, lat), truth)
+    np.testing.assert_array_equal(ctx.find_elements(lon, lat, nn), truth)
+    for start in (truth, rng.integers(0, E, n).astype(np.int32), np.full(n, -1, np.int32),
+                  np.where(rng.random(n) < 0.5, E + 5, -7).astype(np.int32)):
+        want = O.walk(m, lon, lat, start, nn)
+        got = ctx.find_elements_walk(lon, lat, start)
+        np.testing.assert_array_equal(got, want)
+
+
+def test_cuda_walk_resident_sort_and_elem_roundtrip(golden):
+    """Carried elements through the resident path: set, re-sort, step, read
+    back in upload order; equal to the host-buffer step of the same state."""
+    from kelp_b200.device import default_context
+    g = golden("golden_band")
+    c = g.case("rk2_walk")
+    dt, T, n_steps, td, *_ = c["params"]
+    st = g.particles().replace(elem=c["elem0"].copy())
+    vel, vnext, dtn = g.payload(c["schedule"][0], T)
+    ref = KI.rk2_step(st, vel, g.mesh, dt, td, uv_interp="barycentric", vel_next=vnext, dt_to_next=dtn)
+    ctx = default_context()
+    a, _ = KI.prepare_step(vel, g.mesh, dt, td, "rk2", dict(uv_interp="barycentric", vel_next=vnext,
+                                                           dt_to_next=dtn), ctx, elem=st.elem)
+    ctx.upload_particles(st.lon, st.lat, st.z, st.status, st.nearest_node, st.failure_reason)
+    ctx.set_elem(st.elem)
+    np.testing.assert_array_equal(ctx.get_elem(), st.elem)
+    ctx.sort()
+    ctx.step(a)
+    out = ctx.download_particles()
+    np.testing.assert_array_equal(ctx.get_elem(), ref.elem)
+    np.testing.assert_array_equal(out["status"], ref.status)
+    np.testing.assert_array_equal(out["lon"], ref.lon)
+    np.testing.assert_array_equal(out["lat"], ref.lat)

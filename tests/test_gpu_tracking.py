@@ -118,3 +118,30 @@ def test_run_tracking_config_equals_tracker(golden, tmp_path):
         res = tr.run(alive, int(n_steps), realization_id=r, output_freq=4)
         np.testing.assert_array_equal(np.stack(recs[r].status), np.stack(res.records[0].status))
         np.testing.assert_array_equal(np.stack(recs[r].lons), np.stack(res.records[0].lons))
+
+
+def test_tracker_walk_equals_per_call_walk(golden):
+    """elem_search "walk" in the resident loop (seeded by the local search at
+    the start, carried through re-sorts) equals stepping the same state
+    through the per-call rk2_step with state.elem."""
+    from kelp_b200 import integrators as KI
+    g = golden("golden_band")
+    c = g.case("rk2_walk")
+    dt, Tsnap, n_steps, td, *_ = c["params"]
+    ft = np.arange(len(g.snaps)) * Tsnap
+    n = 6
+    tr = T.Tracker(g.mesh, g.snaps, ft, integrator="rk2", dt=dt, sort_every=2, elem_search="walk")
+    st0 = g.particles()
+    res = tr.run(st0, n)
+    fin = res.final[0]
+    # the start seed: the local search around the exact anchor (tracking.py:2243-2249)
+    np.testing.assert_array_equal(tr.ctx.find_elements(st0.lon, st0.lat), c["elem0"])
+    st = st0.replace(elem=c["elem0"].copy())
+    t = float(ft[0])
+    for k in range(n):
+        br = T.resolve_time_bracket(t, ft, "stop", 1, T.snapshot_band(dt))
+        vel, vnext, dtn = T.vel_payload(br, g.snaps, 1)
+        st = KI.rk2_step(st, vel, g.mesh, dt, 1.0, uv_interp="barycentric", vel_next=vnext, dt_to_next=dtn)
+        t += dtn if (dtn is not None and abs(dt - dtn) <= T.snapshot_band(dt)) else dt
+    for name in ("status", "nearest_node", "failure_reason", "elem", "lon", "lat"):
+        np.testing.assert_array_equal(getattr(fin, name), getattr(st, name), err_msg=name)
