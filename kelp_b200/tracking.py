@@ -36,6 +36,7 @@ from . import _native as N
 from . import integrators as KI
 from .beaching import BeachingConfig, beach_args, make_run_config
 from .device import default_context
+from .diffusion import DiffusionStepArgs
 from .fields import LazyLerpField, VelocityField
 from .particles import ParticleState, ParticleStatus, make_state
 
@@ -243,25 +244,26 @@ class Tracker:
                 raise NotImplementedError("only the uniform-Kh split kick is built on the CUDA backend")
             if getattr(self.diffusion, "composition", "split") != "split":
                 raise NotImplementedError("only the split kick composition is built on the CUDA backend")
-            if getattr(self.diffusion, "az_enabled", False):
-                raise NotImplementedError("the vertical Az kick is not built on the CUDA backend")
         self.beaching = beaching if (beaching is not None and beaching.enabled) else None
         self.on_exhausted = on_exhausted
         self.sort_every = int(sort_every)
         self.ctx = ctx or default_context()
         self.dims = 3 if getattr(self.fields[0], "w", None) is not None else 2
 
-    def _kick(self, realization: int, step_i: int, particle_offset: int):
+    def _diffusion_args(self, realization: int, step_i: int, particle_offset: int):
+        """The step's DiffusionStepArgs as tracking.py:2595-2611 builds them
+        (None when diffusion is off): Kh, the draws' keys, the Az switch and
+        source."""
         d = self.diffusion
         if d is None:
             return None
-        kx = float(getattr(d, "kh_zonal", getattr(d, "kh_x", 0.0)))
-        ky = float(getattr(d, "kh_meridional", getattr(d, "kh_y", 0.0)))
-        if kx == 0.0 and ky == 0.0:
-            return None
-        if kx < 0 or ky < 0:
-            raise ValueError("Kh must be >= 0")
-        return (kx, ky, int(d.seed), int(realization), int(step_i), int(particle_offset))
+        return DiffusionStepArgs(
+            scheme="uniform", kh_x=float(getattr(d, "kh_zonal", getattr(d, "kh_x", 0.0))),
+            kh_y=float(getattr(d, "kh_meridional", getattr(d, "kh_y", 0.0))), seed=int(d.seed),
+            real_id=int(realization), step_i=int(step_i),
+            az_enabled=bool(getattr(d, "az_enabled", False)), az_const=float(getattr(d, "az_const", 0.0)),
+            az_requires_field=bool(getattr(d, "var_az", None)) or bool(getattr(d, "az_requires_field", False)),
+            pid_offset=int(particle_offset))
 
     def run(self, init_state: ParticleState, n_steps: int, *, start_time: Optional[float] = None,
             realization_id: int = 0, start_step_i: int = 0, output_freq: int = 1, particle_offset: int = 0,
@@ -328,8 +330,10 @@ class Tracker:
             kw = dict(self.kw, vel_next=vnext, dt_to_next=dtn)
             if self.sort_every > 0 and k % self.sort_every == 0:
                 ctx.sort()
-            # step 1 keys: the realization of each particle (its own when R > 1)
-            kick = self._kick(realizations[0], g, particle_offset)
+            # the draws' keys: the realization of each particle (its own when R > 1)
+            diff = self._diffusion_args(realizations[0], g, particle_offset)
+            kw["diffusion"] = diff
+            kick = KI._kick_args(diff)
             a, _ = KI.prepare_step(vel, mesh, self.dt, float(self.direction), self.integrator, kw, ctx, kick=kick)
             a.global_step = g
             ctx.step(a)
@@ -387,6 +391,8 @@ class _Diffusion:
         self.seed = int(d.get("seed", 0))
         self.composition = d.get("composition", "split")
         self.az_enabled = bool(d.get("az_enabled", False))
+        self.az_const = float(d.get("az_const", 0.0))
+        self.var_az = d.get("var_az")
 
 
 def load_config(path_or_dict):
@@ -411,7 +417,8 @@ def load_mesh_npz(path: str):
 
 def load_velocity_npz(path: str):
     """Snapshot records from an .npz with ``times`` (R,), ``u``, ``v`` (R, N) or
-    (R, L, N) and optionally ``w`` (R, K, N) and ``uv_vertical``."""
+    (R, L, N) and optionally ``w`` (R, K, N), ``az`` (R, K, N) and
+    ``uv_vertical``."""
     d = np.load(path)
     times = d["times"]
     placement = str(d["uv_vertical"]) if "uv_vertical" in d else "layer"
@@ -419,8 +426,9 @@ def load_velocity_npz(path: str):
     for r in range(times.size):
         u, v = d["u"][r], d["v"][r]
         w = d["w"][r] if "w" in d else None
+        az = d["az"][r] if "az" in d else None
         fields.append(VelocityField(u=u, v=v, w=w, eta=np.zeros(u.shape[-1]), uv_layout="node",
-                                    uv_vertical=placement if w is not None else "layer"))
+                                    uv_vertical=placement if w is not None else "layer", az=az))
     return fields, times
 
 

@@ -145,3 +145,34 @@ def test_tracker_walk_equals_per_call_walk(golden):
         t += dtn if (dtn is not None and abs(dt - dtn) <= T.snapshot_band(dt)) else dt
     for name in ("status", "nearest_node", "failure_reason", "elem", "lon", "lat"):
         np.testing.assert_array_equal(getattr(fin, name), getattr(st, name), err_msg=name)
+
+
+def test_tracker_az_kick_equals_per_call(golden):
+    """The vertical Az kick (field Az from the snapshots) inside the resident
+    loop equals the per-call rk2_step with the DiffusionStepArgs the reference's
+    loop builds (tracking.py:2595-2611)."""
+    from kelp_b200 import integrators as KI
+    from kelp_b200.diffusion import DiffusionStepArgs
+    g = golden("golden_3d")
+    c = g.case("rk2_wbary_kick_azf")
+    dt, Tsnap, n_steps, td, khx, khy, seed, real_id, pid_off = c["params"]
+    ft = np.arange(len(g.snaps)) * Tsnap
+    n = 5
+    d = Diff(khx, int(seed))
+    d.az_enabled, d.az_const, d.var_az = True, 0.0, "az"
+    tr = T.Tracker(g.mesh, g.snaps, ft, integrator="rk2", dt=dt, w_interp="barycentric", diffusion=d,
+                   sort_every=2)
+    st0 = g.particles()
+    fin = tr.run(st0, n, realization_id=3).final[0]
+    st = st0
+    t = float(ft[0])
+    band = T.snapshot_band(dt)
+    for k in range(n):
+        vel, vnext, dtn = T.vel_payload(T.resolve_time_bracket(t, ft, "stop", 1, band), g.snaps, 1)
+        diff = DiffusionStepArgs("uniform", khx, khy, int(seed), 3, k, az_enabled=True, az_requires_field=True)
+        st = KI.rk2_step(st, vel, g.mesh, dt, 1.0, uv_interp="barycentric", w_interp="barycentric",
+                         vel_next=vnext, dt_to_next=dtn, diffusion=diff)
+        t += dtn if (dtn is not None and abs(dt - dtn) <= band) else dt
+    for name in ("status", "nearest_node", "failure_reason", "lon", "lat", "z"):
+        np.testing.assert_array_equal(getattr(fin, name), getattr(st, name), err_msg=name)
+    assert np.any(fin.z != st0.z)
