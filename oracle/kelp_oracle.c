@@ -43,6 +43,8 @@ typedef struct {
     const int32_t* dl_last;
     int dl_M;
     const int32_t* enb;   /* (E, max_v) edge neighbours of the compacted ring (walk), or NULL */
+    const double* sigma;  /* (K) sigma interfaces, 1 surface -> 0 bed (vertical_coord "sigma"), or NULL */
+    int sig;
 } OMesh;
 
 typedef struct {
@@ -51,6 +53,7 @@ typedef struct {
     double alpha0;
     int64_t n;
     const void *aza, *azb;   /* vertical diffusivity (K, N) of the bracket pair, or NULL */
+    const double *etaa, *etab, *etat;   /* free surface (N) of the pair and target (sigma meshes) */
 } OField;
 
 static double fld(const void* p, int f32, int64_t i) {
@@ -726,6 +729,8 @@ typedef struct {
     int uv_dl;
     int az_on, az_field;   /* vertical Az kick; Az from the snapshots' (K, N) az arrays */
     double az_const;
+    double Dmin, z0b_min;  /* sigma column floor and bed clearance */
+    double alpha_end;      /* blend fraction of the end-of-step surface (sigma) */
 } OStep;
 
 /* vertical_uv.py:457-523 uv_bracket */
@@ -1044,12 +1049,296 @@ static int walk_locate(const OMesh* m, double lon_p, double lat_p, int start, in
  * :5415-5608, :5792-6011). */
 #define STAGE(e, call) (t_elem_hint = (e), _r = (call), t_elem_hint = -1, _r)
 
+/* ---- sigma meshes (vertical_coord "sigma"; vertical_sigma.py,
+ * integrators.py:1322-1440): the step integrates s = z / H_p, H_p the
+ * column height max(depth + eta, Dmin) interpolated at the particle like W. */
+
+/* the stage's free surface at a node: the payload's eta blended like u/v
+ * (io.py:68-117 _blend in float64, the stage lerps of _make_stage_vels) */
+static double eta_at(const OField* f, int node, double alpha) {
+    return tblend(f->etaa[node], f->etab[node], f->etat[node], f->alpha0, alpha);
+}
+
+/* vertical_sigma.py:472-478 _col_H */
+static double col_H(const OMesh* m, const OField* f, const OStep* s, int node, double alpha) {
+    double H = m->depth[node] + eta_at(f, node, alpha);
+    if (H < s->Dmin) H = s->Dmin;
+    return H;
+}
+
+/* vertical_sigma.py:565-632 _bary_locate: the W search's element among the
+ * anchor's elements and its vertex weights (tris: the fan triangle's, quads:
+ * Wachspress); returns the vertex count, 0 when none contains the point. */
+static int bary_locate(const OMesh* m, double xp, double yp, int node, int* verts, double* wts) {
+    int cnt = m->n2e_cnt[node];
+    for (int k = 0; k < cnt; ++k) {
+        int e = m->n2e[(int64_t)node * m->max_conn + k];
+        if (e < 0) continue;
+        int nv = 0;
+        for (int v = 0; v < m->max_v; ++v) {
+            int nd = m->en[(int64_t)e * m->max_v + v];
+            if (nd < 0) continue;
+            if (nv > 0 && nd == verts[0]) continue;
+            verts[nv++] = nd;
+        }
+        if (nv < 3) continue;
+        double ln[4];
+        for (int v = 0; v < nv; ++v) ln[v] = m->lon[verts[v]];
+        double lon0 = seam_lon0(ln, nv), lat0 = 0.0;
+        for (int v = 0; v < nv; ++v) lat0 += m->lat[verts[v]];
+        lat0 /= nv;
+        double cl = cos(lat0 * DEG2RAD), R = 6371000.0;
+        double vx[4], vy[4];
+        for (int v = 0; v < nv; ++v) {
+            vx[v] = wrap180(m->lon[verts[v]] - lon0) * DEG2RAD * R * cl;
+            vy[v] = (m->lat[verts[v]] - lat0) * DEG2RAD * R;
+        }
+        double px = wrap180(xp - lon0) * DEG2RAD * R * cl;
+        double py = (yp - lat0) * DEG2RAD * R;
+        for (int t = 0; t < nv - 2; ++t) {
+            double ax = vx[0], ay = vy[0], bx = vx[t + 1], by = vy[t + 1], cx = vx[t + 2], cy = vy[t + 2];
+            double denom = (by - cy) * (ax - cx) + (cx - bx) * (ay - cy);
+            if (fabs(denom) < 1e-14) continue;
+            double w1 = ((by - cy) * (px - cx) + (cx - bx) * (py - cy)) / denom;
+            double w2 = ((cy - ay) * (px - cx) + (ax - cx) * (py - cy)) / denom;
+            double w3 = 1.0 - w1 - w2;
+            if (w1 >= -1e-6 && w2 >= -1e-6 && w3 >= -1e-6) {
+                for (int v = 0; v < 4; ++v) wts[v] = 0.0;
+                if (nv == 4) polygon_weights(px, py, vx, vy, 4, wts);
+                else { wts[0] = w1; wts[t + 1] = w2; wts[t + 2] = w3; }
+                return nv;
+            }
+        }
+    }
+    return 0;
+}
+
+/* vertical_sigma.py:1034-1060 the particle's column height, interpolated
+ * with the W method (nearest: the anchor's column; barycentric: :636-652) */
+static double sigma_H(const OMesh* m, const OField* f, const OStep* s, double alpha, double xp, double yp, int node) {
+    if (s->w_code == 0) return col_H(m, f, s, node, alpha);
+    int verts[4];
+    double wts[4];
+    int nv = bary_locate(m, xp, yp, node, verts, wts);
+    if (nv == 0) return col_H(m, f, s, node, alpha);
+    double H = 0.0;
+    for (int v = 0; v < nv; ++v) H += wts[v] * col_H(m, f, s, verts[v], alpha);
+    return H;
+}
+
+/* vertical_sigma.py:297-334 _interp_w_sigma_linear_single on the stage's w */
+static double w_sig_linear(const OMesh* m, const OField* f, double alpha, double z, int node, double H, double td) {
+    int K = m->K;
+    const double* sg = m->sigma;
+    if (K < 2) return td * wat(f, 0, node, alpha);
+    double z_top = (1.0 - sg[0]) * H, z_bot = (1.0 - sg[K - 1]) * H;
+    if (z <= z_top) return td * wat(f, 0, node, alpha);
+    if (z >= z_bot) return td * wat(f, K - 1, node, alpha);
+    int k = K - 2;
+    for (int j = 0; j < K - 1; ++j)
+        if (z < (1.0 - sg[j + 1]) * H) { k = j; break; }
+    double zk = (1.0 - sg[k]) * H, zk1 = (1.0 - sg[k + 1]) * H;
+    double dz = zk1 - zk;
+    if (dz < 1e-12) return td * wat(f, k, node, alpha);
+    double a = (z - zk) / dz;
+    double wv = (1.0 - a) * wat(f, k, node, alpha) + a * wat(f, k + 1, node, alpha);
+    return td * wv;
+}
+
+/* vertical_sigma.py:481-489 _sigma_frac */
+static double sigma_frac(double z, double H) {
+    double fr = z / H;
+    if (fr < 0.0) fr = 0.0;
+    else if (fr > 1.0) fr = 1.0;
+    return fr;
+}
+
+/* W on a sigma mesh (vertical_sigma.py:971-1031): nearest = the anchor's
+ * column (:337-360); barycentric = every vertex column at the particle's
+ * sigma (:766-816), the own column at min(z, H) outside every element */
+static double w_sig(const OMesh* m, const OField* f, const OStep* s, double alpha, double xp, double yp, double z,
+                    int node) {
+    if (s->w_code == 0) return w_sig_linear(m, f, alpha, z, node, col_H(m, f, s, node, alpha), s->td);
+    int verts[4];
+    double wts[4];
+    int nv = bary_locate(m, xp, yp, node, verts, wts);
+    if (nv == 0) {
+        double H = col_H(m, f, s, node, alpha);
+        double zc = z < H ? z : H;
+        return w_sig_linear(m, f, alpha, zc, node, H, s->td);
+    }
+    double Hp = 0.0;
+    for (int v = 0; v < nv; ++v) Hp += wts[v] * col_H(m, f, s, verts[v], alpha);
+    double fr = sigma_frac(z, Hp);
+    double acc = 0.0;
+    for (int v = 0; v < nv; ++v) {
+        double Hv = col_H(m, f, s, verts[v], alpha);
+        acc += wts[v] * w_sig_linear(m, f, alpha, fr * Hv, verts[v], Hv, s->td);
+    }
+    return acc;
+}
+
+/* vertical_sigma.py:73-109 find_layer_sigma in the particle's column
+ * (floored at Dmin, :135-144) */
+static int find_layer_sig(const OMesh* m, double z, double H, double Dmin) {
+    if (H < Dmin) H = Dmin;
+    int K = m->K;
+    const double* sg = m->sigma;
+    if (K < 2) return 0;
+    if (z <= (1.0 - sg[0]) * H) return 0;
+    if (z >= (1.0 - sg[K - 1]) * H) return K - 2;
+    for (int k = 0; k < K - 1; ++k)
+        if (z < (1.0 - sg[k + 1]) * H) return k;
+    return K - 2;
+}
+
+/* vertical_sigma.py:236-255 the clamp in the particle's column */
+static double clamp_sig(double z, double H, const OStep* s) {
+    if (H < s->Dmin) H = s->Dmin;
+    if (z < 0.0) z = 0.0;
+    double bottom = H - s->z0b_min;
+    if (bottom < 0.0) bottom = 0.0;
+    if (z > bottom) z = bottom;
+    return z;
+}
+
+/* integrators.py:1351-1376 _sigma_frac_for_uv (a NaN stays NaN) */
+static double sfrac_uv(double z, double H) {
+    double fr = z / H;
+    if (fr < 0.0) fr = 0.0;
+    if (fr > 1.0) fr = 1.0;
+    return fr;
+}
+
+/* u/v of a sigma stage: the layer in the particle's column, or the
+ * depth-linear rule read in s (vertical_uv.py:196-211) */
+static int sig_stage_uv(const OMesh* m, const OField* f, const OStep* s, double xp, double yp, int nn, double z,
+                        double H, double alpha, double* U, double* V) {
+    if (s->uv_dl) return interp_uv_dl(m, f, xp, yp, nn, sfrac_uv(z, H), s->td, alpha, U, V);
+    return interp_uv(m, f, xp, yp, nn, s->td, find_layer_sig(m, z, H, s->Dmin), alpha, U, V);
+}
+
+/* One particle of the sigma step: integrators.py:4997-5147 (Euler),
+ * :5380-5608 (RK2, unfused), :5760-6011 (RK4, unfused), sigma branches;
+ * the split kick keeps s = z / H_p into the kicked column (:783-803). */
+static void step_sigma(const OMesh* m, const OField* f, const OStep* s, int64_t i, double* lon, double* lat,
+                       double* z, int* status, int* nn, int8_t* fr, double* U, double* V, double* W,
+                       const int64_t* pid, int32_t* elem) {
+    double lon0 = lon[i], lat0 = lat[i], zp = z[i], dt = s->dt;
+    int pre_nn = nn[i], st = ALIVE, nno, _r;
+    int8_t frr = fr[i];
+    double ln = lon0, lt = lat0, zn = zp;
+    int node_i = anchor(m, lon0, lat0);
+    nno = node_i;
+    const int walk = elem != NULL;
+    const int e1 = walk ? walk_locate(m, lon0, lat0, elem[i], node_i) : -1;
+    int e_last = e1, e_out = e1;
+#define LOC(x, y, from, n) (walk ? walk_locate(m, (x), (y), (from), (n)) : -1)
+    double H1 = sigma_H(m, f, s, s->ak[0], lon0, lat0, node_i);
+    double U1, V1;
+    int ok = STAGE(e1, sig_stage_uv(m, f, s, lon0, lat0, node_i, zp, H1, s->ak[0], &U1, &V1));
+    double W1 = w_sig(m, f, s, s->ak[0], lon0, lat0, zp, node_i);
+    U[i] = U1; V[i] = V1; W[i] = W1;
+    double a = lon0, b = lat0, s_new = 0.0;
+    if (ok) {
+        if (s->scheme == 0) {
+            a = wrap180(lon0 + dt * U1 / z0_of(lat0));
+            b = clat(lat0 + dt * V1 / SLM);
+            s_new = (zp + W1 * dt) / H1;
+        } else if (s->scheme == 1) {
+            double lm = wrap180(lon0 + 0.5 * dt * U1 / z0_of(lat0));
+            double tm = clat(lat0 + 0.5 * dt * V1 / SLM);
+            double s_mid = (zp + W1 * 0.5 * dt) / H1;
+            int nm = anchor(m, lm, tm);
+            int em = LOC(lm, tm, e1, nm);
+            e_last = em;
+            double H2 = sigma_H(m, f, s, s->ak[1], lm, tm, nm);
+            double zm = s_mid * H2;
+            double U2, V2;
+            if (!STAGE(em, sig_stage_uv(m, f, s, lm, tm, nm, zm, H2, s->ak[1], &U2, &V2))) ok = 0;
+            else {
+                double W2 = w_sig(m, f, s, s->ak[1], lm, tm, zm, nm);
+                a = wrap180(lon0 + dt * U2 / z0_of(tm));
+                b = clat(lat0 + dt * V2 / SLM);
+                s_new = zp / H1 + dt * W2 / H2;
+            }
+        } else {
+            double dl1 = dt * U1 / z0_of(lat0), dd1 = dt * V1 / SLM;
+            double s0 = zp / H1, f1 = W1 / H1;
+            double l2 = wrap180(lon0 + 0.5 * dl1), t2 = clat(lat0 + 0.5 * dd1);
+            int n2 = anchor(m, l2, t2), e2 = LOC(l2, t2, e1, n2);
+            double H2 = sigma_H(m, f, s, s->ak[1], l2, t2, n2);
+            double z2 = (s0 + 0.5 * dt * f1) * H2;
+            double U2, V2, U3, V3, U4, V4;
+            if (!STAGE(e2, sig_stage_uv(m, f, s, l2, t2, n2, z2, H2, s->ak[1], &U2, &V2))) ok = 0;
+            else {
+                double W2 = w_sig(m, f, s, s->ak[1], l2, t2, z2, n2);
+                double dl2 = dt * U2 / z0_of(t2), dd2 = dt * V2 / SLM, f2 = W2 / H2;
+                double l3 = wrap180(lon0 + 0.5 * dl2), t3 = clat(lat0 + 0.5 * dd2);
+                int n3 = anchor(m, l3, t3), e3 = LOC(l3, t3, e2, n3);
+                double H3 = sigma_H(m, f, s, s->ak[2], l3, t3, n3);
+                double z3 = (s0 + 0.5 * dt * f2) * H3;
+                if (!STAGE(e3, sig_stage_uv(m, f, s, l3, t3, n3, z3, H3, s->ak[2], &U3, &V3))) ok = 0;
+                else {
+                    double W3 = w_sig(m, f, s, s->ak[2], l3, t3, z3, n3);
+                    double dl3 = dt * U3 / z0_of(t3), dd3 = dt * V3 / SLM, f3 = W3 / H3;
+                    double l4 = wrap180(lon0 + dl3), t4 = clat(lat0 + dd3);
+                    int n4 = anchor(m, l4, t4), e4 = LOC(l4, t4, e3, n4);
+                    e_last = e4;
+                    double H4 = sigma_H(m, f, s, s->ak[3], l4, t4, n4);
+                    double z4 = (s0 + dt * f3) * H4;
+                    if (!STAGE(e4, sig_stage_uv(m, f, s, l4, t4, n4, z4, H4, s->ak[3], &U4, &V4))) ok = 0;
+                    else {
+                        double W4 = w_sig(m, f, s, s->ak[3], l4, t4, z4, n4);
+                        double dl4 = dt * U4 / z0_of(t4), dd4 = dt * V4 / SLM, f4 = W4 / H4;
+                        double dl = (dl1 + 2.0 * dl2 + 2.0 * dl3 + dl4) / 6.0;
+                        double dd = (dd1 + 2.0 * dd2 + 2.0 * dd3 + dd4) / 6.0;
+                        a = wrap180(lon0 + dl);
+                        b = clat(lat0 + dd);
+                        s_new = s0 + dt * (f1 + 2.0 * f2 + 2.0 * f3 + f4) / 6.0;
+                    }
+                }
+            }
+        }
+    }
+    if (!ok) { st = OUTSIDE; frr = 1; }
+    else {
+        int nw = anchor(m, a, b);
+        int ein = walk ? walk_locate(m, a, b, e_last, nw) : contain_local(m, a, b, nw);
+        if (ein < 0) { st = OUTSIDE; frr = 2; }
+        else {
+            double He = sigma_H(m, f, s, s->alpha_end, a, b, nw);
+            ln = a; lt = b; nno = nw; e_out = ein;
+            zn = clamp_sig(s_new * He, He, s);
+        }
+    }
+#undef LOC
+    if (s->kick && st == ALIVE) {
+        double plon = ln, plat = lt;
+        int pnn = nno;
+        kick(m, s, pid ? pid[i] : i, lon0, lat0, zp, pre_nn, &ln, &lt, &zn, &st, &nno, &frr, 0);
+        if (st == ALIVE) {
+            double Hpost = sigma_H(m, f, s, s->alpha_end, plon, plat, pnn);
+            double Hk = sigma_H(m, f, s, s->alpha_end, ln, lt, nno);
+            zn = clamp_sig(zn / Hpost * Hk, Hk, s);
+        }
+    }
+    lon[i] = ln; lat[i] = lt; z[i] = zn;
+    status[i] = st; nn[i] = nno; fr[i] = frr;
+    if (walk) elem[i] = e_out;
+}
+
+
 static void step_one(const OMesh* m, const OField* f, const OStep* s, int64_t i, double* lon, double* lat, double* z,
                      int* status, int* nn, int8_t* fr, double* U, double* V, double* W, const int64_t* pid,
                      int32_t* elem) {
     if (status[i] != ALIVE) {
         U[i] = 0.0; V[i] = 0.0;
         if (W) W[i] = 0.0;
+        return;
+    }
+    if (m->sig && s->dims == 3) {
+        step_sigma(m, f, s, i, lon, lat, z, status, nn, fr, U, V, W, pid, elem);
         return;
     }
     double lon0 = lon[i], lat0 = lat[i], zp = z ? z[i] : 0.0, dt = s->dt, td = s->td;
@@ -1292,6 +1581,8 @@ typedef struct {
     const int32_t* dl_last;
     int dl_M;
     const int32_t* enb;
+    const double* sigma;
+    int sig;
 } orc_mesh;
 
 typedef struct {
@@ -1300,6 +1591,7 @@ typedef struct {
     double alpha0;
     int64_t n;
     const void *aza, *azb;
+    const double *etaa, *etab, *etat;
 } orc_field;
 
 typedef struct {
@@ -1309,6 +1601,7 @@ typedef struct {
     int uv_dl;
     int az_on, az_field;
     double az_const;
+    double Dmin, z0b_min, alpha_end;
 } orc_step_args;
 
 typedef struct {

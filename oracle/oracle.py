@@ -28,7 +28,7 @@ class OMesh(C.Structure):
                 ("nx", C.c_int), ("ny", C.c_int), ("wrap", C.c_int), ("far_rows", C.c_int),
                 ("exact", C.c_int), ("K", C.c_int),
                 ("dl_p", C.c_void_p), ("dl_bed", C.c_void_p), ("dl_last", C.c_void_p), ("dl_M", C.c_int),
-                ("enb", C.c_void_p)]
+                ("enb", C.c_void_p), ("sigma", C.c_void_p), ("sig", C.c_int)]
 
 
 class OField(C.Structure):
@@ -36,7 +36,8 @@ class OField(C.Structure):
                 ("ub", C.c_void_p), ("vb", C.c_void_p), ("wb", C.c_void_p),
                 ("ut", C.c_void_p), ("vt", C.c_void_p), ("wt", C.c_void_p),
                 ("f32", C.c_int), ("alpha0", C.c_double), ("n", C.c_int64),
-                ("aza", C.c_void_p), ("azb", C.c_void_p)]
+                ("aza", C.c_void_p), ("azb", C.c_void_p),
+                ("etaa", C.c_void_p), ("etab", C.c_void_p), ("etat", C.c_void_p)]
 
 
 class OStep(C.Structure):
@@ -45,7 +46,8 @@ class OStep(C.Structure):
                 ("kh_x", C.c_double), ("kh_y", C.c_double),
                 ("seed", C.c_uint64), ("real_id", C.c_uint64), ("step_i", C.c_uint64),
                 ("pid_offset", C.c_uint64), ("uv_dl", C.c_int),
-                ("az_on", C.c_int), ("az_field", C.c_int), ("az_const", C.c_double)]
+                ("az_on", C.c_int), ("az_field", C.c_int), ("az_const", C.c_double),
+                ("Dmin", C.c_double), ("z0b_min", C.c_double), ("alpha_end", C.c_double)]
 
 
 _lib = None
@@ -105,7 +107,9 @@ class MeshView:
         self.off = c(mesh._gh_offsets, np.int32)
         self.ids = c(mesh._gh_node_ids, np.int32)
         sig = np.asarray(getattr(mesh, "sigma", np.zeros(0)))
-        self.zl = c(np.abs(sig), np.float64) if sig.size else None
+        self.is_sigma = getattr(mesh, "vertical_coord", "zlevel") == "sigma"
+        self.sig = c(sig, np.float64) if (self.is_sigma and sig.size) else None
+        self.zl = c(np.abs(sig), np.float64) if (sig.size and not self.is_sigma) else None
         s = OMesh()
         s.N, s.E = self.lon.size, self.en.shape[0]
         s.max_v, s.max_conn = self.en.shape[1], self.n2e.shape[1]
@@ -117,6 +121,8 @@ class MeshView:
         s.nx, s.ny, s.wrap, s.far_rows = int(mesh._gh_nx), int(mesh._gh_ny), int(bool(mesh._gh_wrap_lon)), int(mesh._gh_far_rows)
         s.exact = int(bool((mesh.metadata or {}).get("exact_nearest", False)))
         s.K = 0 if self.zl is None else int(self.zl.size)
+        if self.sig is not None:   # sigma interfaces, 1 at the surface to 0 at the bed
+            s.sigma, s.sig, s.K = _p(self.sig), 1, int(self.sig.size)
         enb = getattr(mesh, "_elem_neighbors", None)
         self.enb = None if enb is None else c(enb, np.int32)
         s.enb = _p(self.enb)
@@ -128,6 +134,17 @@ class MeshView:
         """Attach the depth-linear data-point table for ``placement``
         (vertical_uv.py:181-278, node layout; z-level meshes)."""
         if placement == self.placement:
+            return
+        if self.is_sigma:
+            # sigma meshes (layer_linear only): layer centres in s, every
+            # column reads every layer, wet everywhere (vertical_uv.py:196-211)
+            sg = np.asarray(self.mesh.sigma, dtype=np.float64)
+            self.dl_p = np.ascontiguousarray(1.0 - 0.5 * (sg[:-1] + sg[1:]))
+            self.dl_last = np.full(self.lon.size, self.dl_p.size - 1, np.int32)
+            self.dl_bed = np.full(self.lon.size, np.inf)
+            self.s.dl_p, self.s.dl_bed, self.s.dl_last = _p(self.dl_p), _p(self.dl_bed), _p(self.dl_last)
+            self.s.dl_M = int(self.dl_p.size)
+            self.placement = placement
             return
         z = np.abs(np.asarray(self.mesh.sigma, dtype=np.float64))
         if placement == "level":
@@ -157,7 +174,7 @@ def _field_arrays(f, dtype):
 
 
 def step(state, vel, mesh, dt, time_dir, scheme: str, *, vel_next=None, dt_to_next=None, w_interp="nearest",
-         diffusion=None, pid=None, release_step=None, global_step=-1, view=None):
+         diffusion=None, pid=None, release_step=None, global_step=-1, view=None, Dmin=0.5, z0b_min=0.1):
     """One step of every particle; returns a dict of new arrays
     (lon, lat, z, status, nearest_node, failure_reason, u, v, w, and elem
     when the state carries elements: elem_search walk, the mesh's
@@ -178,6 +195,9 @@ def step(state, vel, mesh, dt, time_dir, scheme: str, *, vel_next=None, dt_to_ne
     of.f32 = 1 if all32 else 0
     of.alpha0 = alpha0
     of.n = view.lon.size
+    etas = [np.ascontiguousarray(getattr(f, "eta", None) if getattr(f, "eta", None) is not None
+                                 else np.zeros(view.lon.size), dtype=np.float64) for f in flds]
+    of.etaa, of.etab, of.etat = (_p(e) for e in etas)
     is3d = arrs[0][2] is not None
     placement = getattr(vel_a, "uv_vertical", "layer")
     if is3d and placement != "layer":
@@ -192,6 +212,9 @@ def step(state, vel, mesh, dt, time_dir, scheme: str, *, vel_next=None, dt_to_ne
         for k, c in enumerate(cc):
             os_.ak[k] = float(c) * float(dt) / float(dt_to_next)
     os_.dt, os_.td = float(dt), float(time_dir)
+    os_.Dmin, os_.z0b_min = float(Dmin), float(z0b_min)
+    if vel_next is not None:   # the end-of-step surface (integrators.py:1400-1420 _sigma_end_eta)
+        os_.alpha_end = float(dt) / float(dt_to_next)
     if diffusion is not None:
         os_.seed, os_.real_id, os_.step_i = int(diffusion.seed), int(diffusion.real_id), int(diffusion.step_i)
         os_.pid_offset = int(getattr(diffusion, "pid_offset", 0))

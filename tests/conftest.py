@@ -40,18 +40,21 @@ class Golden:
         m._gh_cell_size, m._gh_lon_min, m._gh_lat_min = float(g[0]), float(g[1]), float(g[2])
         m._gh_nx, m._gh_ny, m._gh_wrap_lon, m._gh_far_rows = int(g[3]), int(g[4]), bool(g[5]), int(g[6])
         m.r_earth = float(g[7])
-        m.vertical_coord = "zlevel"
+        m.vertical_coord = str(self.d["mesh_vertical_coord"]) if "mesh_vertical_coord" in self.d else "zlevel"
         m.metadata = {"exact_nearest": True}
         m._elem_neighbors = self.d.get("mesh_elem_neighbors")
         self.mesh = m
         from kelp_b200.fields import VelocityField
-        placement = {"golden_dl_lev": "level", "golden_dl_llin": "layer_linear"}.get(name, "layer")
+        placement = {"golden_dl_lev": "level", "golden_dl_llin": "layer_linear",
+                     "golden_sigma_llin": "layer_linear"}.get(name, "layer")
         self.snaps = []
         i = 0
         while f"snap{i}_u" in self.d:
             w = self.d.get(f"snap{i}_w")
+            eta = self.d.get(f"snap{i}_eta")
             self.snaps.append(VelocityField(u=self.d[f"snap{i}_u"], v=self.d[f"snap{i}_v"], w=w,
-                                            eta=np.zeros(self.d[f"snap{i}_u"].shape[-1]), uv_layout="node",
+                                            eta=np.zeros(self.d[f"snap{i}_u"].shape[-1]) if eta is None else eta,
+                                            uv_layout="node",
                                             uv_vertical=placement if w is not None else "layer",
                                             az=self.d.get(f"snap{i}_az")))
             i += 1
@@ -71,9 +74,12 @@ class Golden:
                              failure_reason=np.zeros(P, np.int8))
 
     def payload(self, sched_row, T):
-        """(vel, vel_next, dt_to_next) of one recorded step."""
+        """(vel, vel_next, dt_to_next) of one recorded step (a steady step,
+        recorded with dt_to_next -1, reads the first record alone)."""
         from kelp_b200.fields import LazyLerpField
         ia, alpha, dtn = int(sched_row[0]), float(sched_row[1]), float(sched_row[2])
+        if dtn < 0:
+            return self.snaps[ia], None, None
         a, b = self.snaps[ia], self.snaps[ia + 1]
         if abs(alpha) < 1e-12:
             vel = a

@@ -56,6 +56,8 @@ def ref_mesh(m, cell=0.0, sigma=None):
 
 def mesh_record(rm):
     extra = {} if rm._elem_neighbors is None else {"elem_neighbors": rm._elem_neighbors}
+    if rm.vertical_coord != "zlevel":
+        extra["vertical_coord"] = np.array(rm.vertical_coord)
     return {**extra,"nodes_lon": rm.nodes_lon, "nodes_lat": rm.nodes_lat, "depth": rm.depth,
             "elem_nodes": rm.elem_nodes, "node_to_elems": rm.node_to_elems,
             "node_to_elems_count": rm.node_to_elems_count, "sigma": rm.sigma,
@@ -64,9 +66,9 @@ def mesh_record(rm):
                                  int(rm._gh_wrap_lon), rm._gh_far_rows, rm.r_earth], dtype=np.float64)}
 
 
-def ref_fields(snaps):
-    return [RVel(u=s.u, v=s.v, w=s.w, eta=np.zeros(s.u.shape[-1]), uv_layout="node",
-                 uv_vertical="layer", az=getattr(s, "az", None)) for s in snaps]
+def ref_fields(snaps, placement="layer"):
+    return [RVel(u=s.u, v=s.v, w=s.w, eta=np.asarray(s.eta), uv_layout="node",
+                 uv_vertical=placement, az=getattr(s, "az", None)) for s in snaps]
 
 
 def payload(fields, t, T):
@@ -80,7 +82,7 @@ def payload(fields, t, T):
 
 
 def run_case(rm, fields, lon, lat, z, status, scheme, dt, T, n_steps, *, time_dir=1.0, w_interp="nearest",
-             kh=None, seed=7, real_id=0, pid_offset=0, record=(1,), az=None, walk=False):
+             kh=None, seed=7, real_id=0, pid_offset=0, record=(1,), az=None, walk=False, steady=False):
     fn = {"rk2": RI.rk2_step, "rk4": RI.rk4_step, "euler": RI.euler_step}[scheme]
     P = lon.size
     st = RState(lon=lon.copy(), lat=lat.copy(), z=z.copy(), status=status.copy(),
@@ -96,7 +98,10 @@ def run_case(rm, fields, lon, lat, z, status, scheme, dt, T, n_steps, *, time_di
     for k in range(n_steps):
         t = k * dt
         vel, vnext, dtn, ia, alpha = payload(fields, t, T)
-        kw = dict(uv_interp="barycentric", w_interp=w_interp, vel_next=vnext, dt_to_next=dtn)
+        if steady:   # no time-aware payload: every stage reads the first record
+            vel, vnext, dtn, ia, alpha = fields[0], None, -1.0, 0, 0.0
+        kw = dict(uv_interp="barycentric", w_interp=w_interp, vel_next=vnext,
+                  dt_to_next=None if steady else dtn)
         if kh is not None:
             kw["diffusion"] = RDiff(scheme="uniform", kh_x=kh[0], kh_y=kh[1], seed=seed, real_id=real_id,
                                     step_i=k, pid_offset=pid_offset, **(az or {}))
@@ -225,6 +230,8 @@ def save(name, mesh_rec, snaps, cases, parts):
             d[f"snap{i}_w"] = s.w
         if getattr(s, "az", None) is not None:
             d[f"snap{i}_az"] = s.az
+        if np.any(np.asarray(s.eta) != 0):
+            d[f"snap{i}_eta"] = s.eta
     for k, v in parts.items():
         d[f"p_{k}"] = v
     for cname, c in cases.items():
@@ -366,6 +373,57 @@ def main():
     print("golden_rng")
 
 
+def sigma_fixture():
+    """FESOM-C-style sigma meshes (mesh.vertical_coord "sigma"): a regional
+    mixed tri/quad shelf, 0.2-120 m deep, 11 sigma interfaces, a free surface
+    eta that changes from record to record (some columns fall below Dmin),
+    layer and layer_linear u/v, the dia-sigma W on the interfaces."""
+    T = 21600.0
+    sig = np.array([1.0, 0.95, 0.88, 0.8, 0.7, 0.58, 0.45, 0.32, 0.2, 0.1, 0.0])
+    m = S.lattice_mesh(1.0, 15.0, lon_min=-20.0, lon_max=20.0, jitter=0.15, land_frac=0.2, quad_frac=0.3,
+                       depth=lambda lo, la: S.smooth_bathymetry(lo, la, 0.2, 120.0), sigma=sig)
+    rm = ref_mesh(m, sigma=sig)
+    rm.vertical_coord = "sigma"
+    lon_n, lat_n = np.radians(np.asarray(m.nodes_lon)), np.radians(np.asarray(m.nodes_lat))
+    pseudo = (1.0 - sig) * 100.0   # depth scale of the synthetic vertical structure
+    lon, lat, z, status = particles(m, 1200, 31, z=True, n_dead=20)
+    for placement, tag in (("layer", "sigma"), ("layer_linear", "sigma_llin")):
+        snaps = S.gyre_snapshots(m, 6, amp=1.0, z_levels=pseudo, decay=60.0, w_scale=4e-4, placement=placement)
+        for k, sn in enumerate(snaps):
+            sn.eta = (0.6 * np.sin(2.0 * lon_n + 0.9 * k) * np.cos(3.0 * lat_n) - 0.15).astype(np.float32)
+        rf = ref_fields(snaps, placement)
+        if placement == "layer":
+            cases = {"rk2_wnear": run_case(rm, rf, lon, lat, z, status, "rk2", 3600.0, T, 12, w_interp="nearest"),
+                     "rk2_wbary": run_case(rm, rf, lon, lat, z, status, "rk2", 3600.0, T, 12,
+                                           w_interp="barycentric"),
+                     "rk4_wbary": run_case(rm, rf, lon, lat, z, status, "rk4", 3600.0, T, 12,
+                                           w_interp="barycentric"),
+                     "euler_wbary": run_case(rm, rf, lon, lat, z, status, "euler", 1800.0, T, 16,
+                                             w_interp="barycentric"),
+                     "euler_wnear": run_case(rm, rf, lon, lat, z, status, "euler", 1800.0, T, 16,
+                                             w_interp="nearest"),
+                     "rk2_wbary_kick": run_case(rm, rf, lon, lat, z, status, "rk2", 3600.0, T, 12,
+                                                w_interp="barycentric", kh=(20.0, 20.0), seed=5),
+                     "rk4_wnear_kick": run_case(rm, rf, lon, lat, z, status, "rk4", 3600.0, T, 10,
+                                                w_interp="nearest", kh=(30.0, 10.0), seed=9),
+                     "rk2_wnear_bwd": run_case(rm, rf, lon, lat, z, status, "rk2", 3600.0, T, 12,
+                                               w_interp="nearest", time_dir=-1.0),
+                     "rk2_wbary_steady": run_case(rm, rf, lon, lat, z, status, "rk2", 3600.0, T, 8,
+                                                  w_interp="barycentric", steady=True),
+                     "rk4_wnear_steady": run_case(rm, rf, lon, lat, z, status, "rk4", 3600.0, T, 8,
+                                                  w_interp="nearest", steady=True),
+                     "rk2_wbary_walk": run_case(rm, rf, lon, lat, z, status, "rk2", 3600.0, T, 12,
+                                                w_interp="barycentric", walk=True)}
+        else:
+            cases = {"rk2_llin_wbary": run_case(rm, rf, lon, lat, z, status, "rk2", 3600.0, T, 12,
+                                                w_interp="barycentric"),
+                     "rk4_llin_wnear_kick": run_case(rm, rf, lon, lat, z, status, "rk4", 3600.0, T, 10,
+                                                     w_interp="nearest", kh=(20.0, 20.0), seed=4),
+                     "euler_llin_wnear": run_case(rm, rf, lon, lat, z, status, "euler", 1800.0, T, 12,
+                                                  w_interp="nearest")}
+        save(f"golden_{tag}", mesh_record(rm), snaps, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
+
+
 def time_fixture():
     """The reference's time-bracket resolution (tracking._resolve_time_bracket)
     on a grid of query times, record axes, modes and directions."""
@@ -389,10 +447,12 @@ def time_fixture():
 
 if __name__ == "__main__":
     # no argument: every fixture; otherwise the named ones ("steps", "beach")
-    which = set(sys.argv[1:]) or {"steps", "beach", "time"}
+    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma"}
     if "steps" in which:
         main()
     if "beach" in which:
         beach_fixture()
     if "time" in which:
         time_fixture()
+    if "sigma" in which:
+        sigma_fixture()

@@ -23,6 +23,12 @@ CASES += [("golden_3d", c) for c in ("rk2_wnear", "rk2_wbary", "rk2_wbary_kick",
                                      "rk4_wnear_walk_kick")]
 CASES += [("golden_dl_lev", c) for c in ("rk2_lev_wbary", "rk4_lev_wnear_kick", "euler_lev_wnear", "rk2_lev_wbary_azc")]
 CASES += [("golden_dl_llin", c) for c in ("rk2_llin_wbary", "rk4_llin_wnear_kick", "euler_llin_wnear")]
+# sigma meshes (mesh.vertical_coord "sigma", free surface eta, s = z / H_p)
+SIGMA_CASES = [("golden_sigma", c) for c in ("rk2_wnear", "rk2_wbary", "rk4_wbary", "euler_wbary", "euler_wnear",
+                                             "rk2_wbary_kick", "rk4_wnear_kick", "rk2_wnear_bwd",
+                                             "rk2_wbary_steady", "rk4_wnear_steady", "rk2_wbary_walk")]
+SIGMA_CASES += [("golden_sigma_llin", c) for c in ("rk2_llin_wbary", "rk4_llin_wnear_kick", "euler_llin_wnear")]
+CASES += SIGMA_CASES
 
 
 def diffusion_args(c, k):
