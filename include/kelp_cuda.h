@@ -28,6 +28,8 @@
  *   kc_find_elements_walk <- core.mesh.find_containing_elements_walk
  *                         (src/kelp/core/mesh.py:2631-2712)
  *   kc_elem_neighbors_upload <- core.mesh.build_elem_neighbors (src/kelp/core/mesh.py:2824)
+ *   kc_sigma_upload    <- core.mesh.Mesh.sigma with vertical_coord "sigma" (src/kelp/core/mesh.py:63-91)
+ *   kc_field_upload_eta <- core.io.VelocityField.eta (src/kelp/core/io.py:180)
  *   kc_rng_normals     <- numerics.diffusion._normal_pair (src/kelp/numerics/diffusion.py:233)
  */
 #ifndef KELP_CUDA_H
@@ -37,7 +39,7 @@
 extern "C" {
 #endif
 
-#define KC_ABI_VERSION 4
+#define KC_ABI_VERSION 5
 
 #define KC_OK 0
 #define KC_ERR_ARG 1      /* invalid argument or combination */
@@ -101,6 +103,10 @@ typedef struct kc_step_args {
     int az_kick;                 /* vertical Az kick after the step (3-D; diffusion.az_enabled) */
     int az_field;                /* Az from the bracket slots' az rows (kc_field_upload_az), else az_const */
     double az_const;             /* m^2/s, >= 0 */
+    double Dmin;                 /* sigma meshes: column floor (m, > 0; the reference's default 0.5) */
+    double z0b_min;              /* sigma meshes: clearance above the bed (m, >= 0; default 0.1) */
+    double alpha_end;            /* sigma meshes: blend fraction of the end-of-step surface,
+                                    dt / dt_to_next (0 without a next snapshot) */
 } kc_step_args;
 
 /* Beaching / resuspension of one step (src/kelp/tracking.py:199-364,
@@ -162,6 +168,18 @@ int kc_particles_download(kc_ctx* ctx, long long P, double* lon, double* lat, do
  * and one launch: each particle's kick and beaching draws use its own id.
  * kc_particles_upload clears them; call before kc_sort. */
 int kc_particles_set_realization(kc_ctx* ctx, const int* real_id);
+
+/* A sigma mesh (FESOM-C; mesh.vertical_coord "sigma"): its K interfaces,
+ * 1 at the surface to 0 at the bed, on a mesh uploaded with depth and
+ * without z-levels.  3-D steps then integrate s = z / H_p in the particle's
+ * column H_p = max(depth + eta, Dmin) (integrators.py:1322-1440, the sigma
+ * branches of :4997-6011), in the plain form, and need every snapshot's
+ * surface (kc_field_upload_eta). */
+int kc_sigma_upload(kc_ctx* ctx, int K, const double* sigma);
+
+/* The free surface eta (n_nodes float64) of the snapshot in ring slot
+ * `slot`; uploading a new snapshot into the slot drops it. */
+int kc_field_upload_eta(kc_ctx* ctx, int slot, long long n_nodes, const double* eta);
 
 /* Edge-neighbour table of the mesh (E x max_v int32, -1 on boundary edges;
  * entry k is the element across the edge from compacted-ring vertex k to the

@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libkelpcuda
 KC_OK, KC_ERR_ARG, KC_ERR_CUDA, KC_ERR_STATE, KC_ERR_DEVICE = 0, 1, 2, 3, 4
 KC_F32, KC_F64, KC_F16 = 0, 1, 2
 KC_PLAIN, KC_MIXED = 0, 1
-ABI_VERSION = 4
+ABI_VERSION = 5
 KC_EULER, KC_RK2, KC_RK4 = 0, 1, 2
 
 #: every symbol include/kelp_cuda.h declares
@@ -26,7 +26,8 @@ EXPORTS = ("kc_abi_version", "kc_node_xyz_fill", "kc_create", "kc_destroy", "kc_
            "kc_particles_download", "kc_coastal_upload", "kc_beach_state_upload",
            "kc_beach_state_download", "kc_beach", "kc_step", "kc_step_host", "kc_step_range", "kc_run_fused",
            "kc_particles_set_realization", "kc_elem_neighbors_upload", "kc_particles_set_elem",
-           "kc_particles_get_elem", "kc_find_elements_walk", "kc_find_elements", "kc_set_fused_block", "kc_run", "kc_sort", "kc_find_nearest", "kc_find_nearest_noalloc", "kc_rng_normals", "kc_device_errors",
+           "kc_particles_get_elem", "kc_find_elements_walk", "kc_find_elements", "kc_sigma_upload", "kc_field_upload_eta",
+           "kc_set_fused_block", "kc_run", "kc_sort", "kc_find_nearest", "kc_find_nearest_noalloc", "kc_rng_normals", "kc_device_errors",
            "kc_event_record", "kc_event_elapsed", "kc_l2_flush", "kc_host_alloc", "kc_host_free")
 
 
@@ -74,7 +75,8 @@ class StepArgs(C.Structure):
                 ("seed", C.c_ulonglong), ("real_id", C.c_ulonglong),
                 ("step_i", C.c_ulonglong), ("pid_offset", C.c_ulonglong),
                 ("global_step", C.c_longlong), ("precision", C.c_int),
-                ("az_kick", C.c_int), ("az_field", C.c_int), ("az_const", C.c_double)]
+                ("az_kick", C.c_int), ("az_field", C.c_int), ("az_const", C.c_double),
+                ("Dmin", C.c_double), ("z0b_min", C.c_double), ("alpha_end", C.c_double)]
 
 
 class BeachArgs(C.Structure):
@@ -132,6 +134,8 @@ def lib():
         L.kc_particles_get_elem.argtypes = [vp, ll, vp]
         L.kc_find_elements_walk.argtypes = [vp, ll, vp, vp, vp, vp]
         L.kc_find_elements.argtypes = [vp, ll, vp, vp, vp, vp]
+        L.kc_sigma_upload.argtypes = [vp, i, vp]
+        L.kc_field_upload_eta.argtypes = [vp, i, ll, vp]
         L.kc_set_fused_block.argtypes = [vp, i]
         L.kc_step_host.argtypes = [vp, C.POINTER(StepArgs), ll, C.POINTER(HostParticles), C.POINTER(HostParticles),
                                    ll]

@@ -31,6 +31,9 @@ struct Slot {
     void* az = nullptr;    // vertical diffusivity rows (K, N), same element type as u
     int az_rows = 0;
     size_t cap_az = 0;
+    double* eta = nullptr; // free surface (N), float64 (sigma meshes)
+    bool has_eta = false;
+    long long cap_eta = 0;
     float* su = nullptr;   // per-row scales of half storage
     float* sv = nullptr;
     float* sw = nullptr;
@@ -64,6 +67,7 @@ struct kc_ctx {
     int* d_dl_last = nullptr;
     double* d_dl_bed = nullptr;
     int4* d_enb = nullptr;   // edge neighbours of the compacted rings (kc_elem_neighbors_upload)
+    double* d_sigma = nullptr;   // sigma interfaces (kc_sigma_upload)
     int max_v = 0;
     int* d_err = nullptr;
     kc::DMesh dm{};
@@ -147,7 +151,7 @@ void dfree(P*& p) {
 template <typename T>
 kc::DField<T> field_of(const Slot& s) {
     return kc::DField<T>{(const T*)s.u, (const T*)s.v, (const T*)s.w, s.su, s.sv, s.sw,
-                         s.az_rows > 0 ? (const T*)s.az : nullptr};
+                         s.az_rows > 0 ? (const T*)s.az : nullptr, s.has_eta ? s.eta : nullptr};
 }
 
 kc::DState state_of(kc_ctx* c) {
@@ -173,6 +177,7 @@ kc::DStep step_of(const kc_step_args* a) {
     s.seed = a->seed; s.real_id = a->real_id; s.step_i = a->step_i; s.pid_offset = a->pid_offset;
     s.global_step = a->global_step;
     s.az_on = a->az_kick; s.az_field = a->az_field; s.az_const = a->az_const;
+    s.Dmin = a->Dmin; s.z0b_min = a->z0b_min; s.alpha_end = a->alpha_end;
     return s;
 }
 
@@ -353,7 +358,10 @@ namespace {
 
 int launch_step_on(kc_ctx* c, const kc_step_args* a, const kc::DState& st, const kc::DStep& s) {
     const int dtype = c->slots[a->slot_a].dtype;
-    if (a->precision == KC_MIXED) {
+    if (c->dm.sig && a->dims == 3) {   // sigma meshes: the plain form's s = z / H_p step
+        if (dtype == KC_F32) launch_sigma_kernel<float>(c->dm, blend_of<float>(c, a), st, s, a->scheme, c->stream);
+        else launch_sigma_kernel<double>(c->dm, blend_of<double>(c, a), st, s, a->scheme, c->stream);
+    } else if (a->precision == KC_MIXED) {
         if (dtype == KC_F16) kc_launch_mixed_f16(c->dm, blend_of<__half>(c, a), st, s, a->dims, a->scheme, c->stream);
         else kc_launch_mixed_f32(c->dm, blend_of<float>(c, a), st, s, a->dims, a->scheme, c->stream);
     } else if (dtype == KC_F32) {
@@ -384,6 +392,18 @@ int check_step(kc_ctx* c, const kc_step_args* a) {
     if (a->kick && !(a->kh_x >= 0.0 && a->kh_y >= 0.0)) return fail(c, KC_ERR_ARG, "kc_step: Kh must be >= 0");
     if (a->precision != KC_PLAIN && a->precision != KC_MIXED)
         return fail(c, KC_ERR_ARG, "kc_step: precision must be KC_PLAIN or KC_MIXED");
+    if (c->dm.sig && a->dims == 3) {
+        if (a->precision != KC_PLAIN) return fail(c, KC_ERR_ARG, "kc_step: sigma meshes step in the plain form");
+        if (a->az_kick) return fail(c, KC_ERR_ARG, "kc_step: the Az kick on sigma meshes is not built");
+        if (!(a->Dmin > 0.0) || !(a->z0b_min >= 0.0))
+            return fail(c, KC_ERR_ARG, "kc_step: sigma steps need Dmin > 0 and z0b_min >= 0");
+        if (!(a->alpha_end >= 0.0 && a->alpha_end <= 1.0 + 1e-9))
+            return fail(c, KC_ERR_ARG, "kc_step: alpha_end must be in [0, 1]");
+        const int sl3[3] = {a->slot_a, a->slot_b, a->slot_t};
+        for (int k = 0; k < 3; ++k)
+            if (sl3[k] < 0 || sl3[k] >= kSlots || !c->slots[sl3[k]].has_eta)
+                return fail(c, KC_ERR_STATE, "kc_step: sigma steps need eta in every snapshot slot (kc_field_upload_eta)");
+    }
     if (a->az_kick) {
         if (a->dims != 3) return fail(c, KC_ERR_ARG, "kc_step: the Az kick needs a 3-D step");
         if (!(a->az_const >= 0.0)) return fail(c, KC_ERR_ARG, "kc_step: az_const must be >= 0");
@@ -445,9 +465,10 @@ void free_mesh(kc_ctx* c) {
     dfree(c->d_ll); dfree(c->d_en); dfree(c->d_n2e_off); dfree(c->d_n2e); dfree(c->d_gh_off);
     dfree(c->d_gh_tab); dfree(c->d_xyz); dfree(c->d_depth); dfree(c->d_zlev);
     dfree(c->d_nsc); dfree(c->d_ecos); dfree(c->d_maxl); dfree(c->d_coastal);
-    dfree(c->d_dl_p); dfree(c->d_dl_last); dfree(c->d_dl_bed); dfree(c->d_enb);
+    dfree(c->d_dl_p); dfree(c->d_dl_last); dfree(c->d_dl_bed); dfree(c->d_enb); dfree(c->d_sigma);
     c->dm.dl_p = nullptr; c->dm.dl_last = nullptr; c->dm.dl_bed = nullptr; c->dm.dl_M = 0;
     c->dm.enb = nullptr;
+    c->dm.sigma = nullptr; c->dm.sig = 0;
     c->has_mesh = false;
 }
 
@@ -494,7 +515,7 @@ void kc_destroy(kc_ctx* c) {
     free_mesh(c);
     free_particles(c);
     for (auto& s : c->slots) {
-        dfree(s.u); dfree(s.v); dfree(s.w); dfree(s.su); dfree(s.sv); dfree(s.sw); dfree(s.az);
+        dfree(s.u); dfree(s.v); dfree(s.w); dfree(s.su); dfree(s.sv); dfree(s.sw); dfree(s.az); dfree(s.eta);
     }
     dfree(c->q); dfree(c->qout); dfree(c->d_err); dfree(c->flush); dfree(c->stage);
     for (int k = 0; k < kEvents; ++k) if (c->ev[k]) cudaEventDestroy(c->ev[k]);
@@ -623,6 +644,29 @@ int kc_coastal_upload(kc_ctx* c, const unsigned char* flags) {
     int rc = upload(c, &c->d_coastal, flags, (size_t)c->E);
     if (rc) return rc;
     KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KC_OK;
+}
+
+int kc_sigma_upload(kc_ctx* c, int K, const double* sigma) {
+    if (!c) return KC_ERR_ARG;
+    if (!c->has_mesh) return fail(c, KC_ERR_STATE, "kc_sigma_upload: no mesh uploaded");
+    if (!c->d_depth) return fail(c, KC_ERR_STATE, "kc_sigma_upload: the mesh has no depth");
+    if (c->dm.zlev) return fail(c, KC_ERR_STATE, "kc_sigma_upload: the mesh was uploaded with z-levels");
+    if (K < 2 || !sigma) return fail(c, KC_ERR_ARG, "kc_sigma_upload: at least 2 interfaces");
+    for (int k = 0; k < K; ++k)
+        if (!(sigma[k] >= -1e9 && sigma[k] <= 1e9)) return fail(c, KC_ERR_ARG, "kc_sigma_upload: non-finite interface");
+    KC_CUDA(c, cudaSetDevice(c->device));
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    dfree(c->d_sigma);
+    c->dm.sigma = nullptr;
+    c->dm.sig = 0;
+    int rc = upload(c, &c->d_sigma, sigma, (size_t)K);
+    if (rc) return rc;
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->dm.sigma = c->d_sigma;
+    c->dm.sig = 1;
+    c->dm.K = K;
+    ++c->mesh_gen;
     return KC_OK;
 }
 
@@ -842,6 +886,7 @@ int kc_field_upload(kc_ctx* c, int slot, int dtype, long long n_nodes, int n_uv_
     }
     s.n = n_nodes; s.uv_rows = n_uv_rows; s.w_rows = n_w_rows > 0 ? n_w_rows : 0; s.dtype = dtype;
     s.az_rows = 0;   // a new snapshot carries no Az until kc_field_upload_az
+    s.has_eta = false;   // nor a surface until kc_field_upload_eta
     return KC_OK;
 }
 
@@ -886,6 +931,24 @@ int kc_field_upload_az(kc_ctx* c, int slot, int dtype, long long n_nodes, int n_
     }
     KC_CUDA(c, cudaMemcpyAsync(s.az, az, bytes, cudaMemcpyHostToDevice, c->stream));
     s.az_rows = n_rows;
+    return KC_OK;
+}
+
+int kc_field_upload_eta(kc_ctx* c, int slot, long long n_nodes, const double* eta) {
+    if (!c) return KC_ERR_ARG;
+    if (slot < 0 || slot >= kSlots) return fail(c, KC_ERR_ARG, "kc_field_upload_eta: slot out of range");
+    Slot& s = c->slots[slot];
+    if (s.dtype < 0) return fail(c, KC_ERR_STATE, "kc_field_upload_eta: upload the snapshot first");
+    if (n_nodes != s.n || !eta) return fail(c, KC_ERR_ARG, "kc_field_upload_eta: shape");
+    KC_CUDA(c, cudaSetDevice(c->device));
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (s.cap_eta < n_nodes) {
+        dfree(s.eta);
+        KC_CUDA(c, cudaMalloc((void**)&s.eta, (size_t)n_nodes * 8));
+        s.cap_eta = n_nodes;
+    }
+    KC_CUDA(c, cudaMemcpyAsync(s.eta, eta, (size_t)n_nodes * 8, cudaMemcpyHostToDevice, c->stream));
+    s.has_eta = true;
     return KC_OK;
 }
 
@@ -1259,6 +1322,8 @@ int kc_run_fused(kc_ctx* c, const kc_step_args* steps, int n_steps, const kc_bea
     }
     if (c->has_elem)
         return fail(c, KC_ERR_STATE, "kc_run_fused: carried walk elements step through kc_step / kc_run");
+    if (c->dm.sig && steps[0].dims == 3)
+        return fail(c, KC_ERR_STATE, "kc_run_fused: sigma meshes step through kc_step / kc_run");
     if (c->P == 0) return KC_OK;
     KC_CUDA(c, cudaSetDevice(c->device));
     if ((rc = pin_pid(c))) return rc;

@@ -53,6 +53,8 @@ struct DMesh {
     const int* dl_last;       // (N) last usable data point per node
     const double* dl_bed;     // (N) bed depth per node for the wall test
     const int4* enb;          // (E) edge neighbours of the compacted ring (edge walk), or null
+    const double* sigma;      // (K) sigma interfaces, 1 surface -> 0 bed (sigma meshes), or null
+    int sig;                  // 1: sigma mesh (K counts its interfaces, zlev is null)
     long long E;
     double cell, lon_min, lat_min, r_earth;
     int nx, ny, wrap, far_rows, K, exact, dl_M;

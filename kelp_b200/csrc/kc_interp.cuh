@@ -19,6 +19,7 @@ struct DField {
     const float* sv;
     const float* sw;
     const T* az;     // vertical diffusivity (K, N) on the interfaces, or null
+    const double* eta;   // free surface (N) (sigma meshes), or null
 };
 
 template <typename T>

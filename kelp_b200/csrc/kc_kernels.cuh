@@ -2,6 +2,7 @@
 // particle), shared by the translation units that instantiate them.
 #pragma once
 #include "kc_beach.cuh"
+#include "kc_sigma.cuh"
 
 #ifndef KC_BLOCK
 #define KC_BLOCK 128   // threads per block of every kernel (a build option)
@@ -51,6 +52,34 @@ __global__ void __launch_bounds__(kBlock, KC_STEP_MIN_BLOCKS) k_step3d_unfused(c
     kc::step3d_unfused_particle<T, SCHEME, Form, WALK>(m, f, st, s, i);
 }
 
+
+template <typename T, int SCHEME, bool WALK>
+__global__ void __launch_bounds__(kBlock, KC_STEP_MIN_BLOCKS) k_step3d_sigma(const __grid_constant__ kc::DMesh m,
+                                                                         const __grid_constant__ kc::DBlend<T> f,
+                                                                         const __grid_constant__ kc::DState st,
+                                                                         const __grid_constant__ kc::DStep s) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= st.P) return;
+    activate(st, s, i);
+    if (st.prev) st.prev[i] = st.status[i];
+    kc::step3d_sigma_particle<T, SCHEME, WALK>(m, f, st, s, i);
+}
+
+// The 3-D step of a sigma mesh (plain form): scheme 0 Euler, 1 RK2, 2 RK4.
+template <typename T>
+void launch_sigma_kernel(const kc::DMesh& m, const kc::DBlend<T>& f, const kc::DState& st, const kc::DStep& s,
+                         int scheme, cudaStream_t stream) {
+    const unsigned g = (unsigned)((st.P + kBlock - 1) / kBlock);
+    if (st.elem) {
+        if (scheme == 0) k_step3d_sigma<T, 0, true><<<g, kBlock, 0, stream>>>(m, f, st, s);
+        else if (scheme == 1) k_step3d_sigma<T, 1, true><<<g, kBlock, 0, stream>>>(m, f, st, s);
+        else k_step3d_sigma<T, 2, true><<<g, kBlock, 0, stream>>>(m, f, st, s);
+    } else {
+        if (scheme == 0) k_step3d_sigma<T, 0, false><<<g, kBlock, 0, stream>>>(m, f, st, s);
+        else if (scheme == 1) k_step3d_sigma<T, 1, false><<<g, kBlock, 0, stream>>>(m, f, st, s);
+        else k_step3d_sigma<T, 2, false><<<g, kBlock, 0, stream>>>(m, f, st, s);
+    }
+}
 
 // Launch one step of every particle: dims 2 / 3, scheme 0 Euler, 1 RK2, 2 RK4;
 // the walk-mode instantiations when the state carries elements.

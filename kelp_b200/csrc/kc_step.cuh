@@ -43,6 +43,8 @@ struct DStep {
     long long global_step;     // for delayed release activation (-1: none)
     int az_on, az_field;       // vertical Az kick; Az from the snapshots' (K, N) az rows
     double az_const;
+    double Dmin, z0b_min;      // sigma column floor and bed clearance
+    double alpha_end;          // blend fraction of the end-of-step surface (sigma)
 };
 
 // displacement metric z0 = max(cos(lat) * 111120, 1) (integrators.py:2563-2565),

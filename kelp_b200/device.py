@@ -121,6 +121,10 @@ class DeviceContext:
         keep: list = []
         d = mesh_desc(mesh, keep)
         self._chk(N.lib().kc_mesh_upload(self._ctx, C.byref(d)), "kc_mesh_upload")
+        self._sigma = getattr(mesh, "vertical_coord", "zlevel") == "sigma"
+        if self._sigma:
+            sg = _c(mesh.sigma, np.float64)
+            self._chk(N.lib().kc_sigma_upload(self._ctx, int(sg.size), N.ptr(sg)), "kc_sigma_upload")
         self._mesh_ref = mesh
         self._mesh_key = key
         self._slots.clear()
@@ -180,6 +184,13 @@ class DeviceContext:
         wrows = 0 if w is None else (1 if w.ndim == 1 else w.shape[0])
         self._chk(N.lib().kc_field_upload(self._ctx, slot, code, n, rows, N.ptr(u), N.ptr(v), wrows, N.ptr(w)),
                   "kc_field_upload")
+        if getattr(self, "_sigma", False) and w is not None:
+            # the free surface of the sigma step's column heights (float64)
+            eta = getattr(field, "eta", None)
+            eta = np.zeros(n) if eta is None else _c(np.asarray(eta), np.float64)
+            if eta.shape != (n,):
+                raise ValueError(f"eta of shape {eta.shape} does not match the mesh's {n} nodes")
+            self._chk(N.lib().kc_field_upload_eta(self._ctx, slot, n, N.ptr(eta)), "kc_field_upload_eta")
         az = getattr(field, "az", None)
         if az is not None and code != N.KC_F16:
             az = _c(np.asarray(az), host)

@@ -162,11 +162,23 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
     w_code = 0
     placement = "layer"
     if is3d:
-        if getattr(mesh, "vertical_coord", "zlevel") != "zlevel":
-            raise NotImplementedError("sigma meshes are not built on the CUDA backend")
+        coord = getattr(mesh, "vertical_coord", "zlevel")
+        if coord not in ("zlevel", "sigma"):
+            raise ValueError(f"unknown mesh.vertical_coord {coord!r}")
         placement = getattr(vel, "uv_vertical", "layer")
         if placement not in ("layer", "level", "layer_linear"):
             raise ValueError(f"unknown uv_vertical {placement!r}")
+        if coord == "sigma":
+            if placement == "level":
+                raise ValueError("uv_vertical 'level' on a sigma mesh: depth-linear u/v there is 'layer_linear' "
+                                 "only (vertical_uv.py:196-211)")
+            if kw.get("cuda_precision", "plain") != "plain":
+                raise NotImplementedError("sigma meshes step in the plain form (cuda_precision='plain')")
+            if kw.get("sigma_eta_start") is not None or kw.get("sigma_eta_end") is not None:
+                raise NotImplementedError("sigma_eta_start / sigma_eta_end (the tracking layer's surfaces) are "
+                                          "not built on the CUDA backend")
+            if float(kw.get("Dmin", 0.5)) <= 0.0:
+                raise ValueError("Dmin must be > 0")
         w_interp = kw.get("w_interp", "leastsq")
         if w_interp not in ("nearest", "barycentric"):
             raise NotImplementedError(f"w_interp={w_interp!r} is not built on the CUDA backend")
@@ -214,6 +226,11 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
         a.kh_x, a.kh_y, a.seed, a.real_id, a.step_i, a.pid_offset = kick
     a.global_step = -1
     a.precision = N.KC_MIXED if form == "mixed" else N.KC_PLAIN
+    # sigma meshes: the column floor, the bed clearance and the end-of-step
+    # surface's blend (integrators.py:1400-1420 _sigma_end_eta)
+    a.Dmin = float(kw.get("Dmin", 0.5))
+    a.z0b_min = float(kw.get("z0b_min", 0.1))
+    a.alpha_end = float(dt) / float(dt_to_next) if vel_next is not None else 0.0
     az = _az_args(kw.get("diffusion", None), vel, is3d, mesh)
     if az is not None:
         if az[0] and store is np.float16:

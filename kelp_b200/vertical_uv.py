@@ -1,4 +1,4 @@
-"""The depth-linear u/v data-point table (node layout, z-level meshes).
+"""The depth-linear u/v data-point table (node layout).
 
 Mirrors KELP's ``src/kelp/numerics/vertical_uv.py:181-278``
 (``_build_depth_points``) and ``depth_points`` (``:328``): for placement
@@ -6,8 +6,10 @@ Mirrors KELP's ``src/kelp/numerics/vertical_uv.py:181-278``
 layer centres; ``last[i]`` is the deepest point of node ``i`` whose lower
 bound lies at or above the node's bed (capped by the reader's optional
 declaration ``mesh.metadata["uv_data_last"]``); ``bed`` is the node depth.
-The CUDA kernels read the table for fields whose ``uv_vertical`` is
-``"level"`` or ``"layer_linear"``.
+On a sigma mesh (``"layer_linear"`` only) the points are the layer centres in
+the sigma fraction s = z / H, every node reads every layer and is wet at every
+s (``bed`` = +inf).  The CUDA kernels read the table for fields whose
+``uv_vertical`` is ``"level"`` or ``"layer_linear"``.
 """
 from __future__ import annotations
 
@@ -27,8 +29,17 @@ class DepthPoints(NamedTuple):
 def depth_points(mesh, placement: str) -> DepthPoints:
     if placement not in PLACEMENTS:
         raise ValueError(f"depth_points: placement must be one of {PLACEMENTS}, got {placement!r}")
-    if getattr(mesh, "vertical_coord", "zlevel") != "zlevel":
-        raise NotImplementedError("depth-linear u/v on sigma meshes is not built on the CUDA backend")
+    if getattr(mesh, "vertical_coord", "zlevel") == "sigma":
+        # vertical_uv.py:196-211: interfaces at s_k = 1 - sigma_k
+        if placement != "layer_linear":
+            raise ValueError(f"depth-linear u/v ({placement!r}) on a sigma mesh: only 'layer_linear' is defined")
+        sg = np.asarray(mesh.sigma, dtype=np.float64)
+        if sg.ndim != 1 or sg.size < 2:
+            raise ValueError(f"depth-linear u/v ({placement!r}) needs a 3-D sigma mesh with >= 2 interfaces "
+                             f"in mesh.sigma, got shape {sg.shape}")
+        p = 1.0 - 0.5 * (sg[:-1] + sg[1:])
+        n = np.asarray(mesh.nodes_lon).shape[0]
+        return DepthPoints(p=p, last=np.full(n, p.size - 1, np.int32), bed=np.full(n, np.inf))
     z = np.abs(np.asarray(mesh.sigma, dtype=np.float64))
     need = 1 if placement == "level" else 2
     if z.ndim != 1 or z.size < need:

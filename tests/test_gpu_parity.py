@@ -13,7 +13,7 @@ import pytest
 from kelp_b200 import integrators as KI
 from kelp_b200.diffusion import DiffusionStepArgs
 
-from test_oracle_golden import diffusion_args
+from test_oracle_golden import SIGMA_CASES, diffusion_args
 
 pytestmark = pytest.mark.gpu
 
@@ -32,6 +32,7 @@ CASES += [("golden_dl_llin", c) for c in ("rk2_llin_wbary", "rk4_llin_wnear_kick
 WALK_CASES = [("golden_band", c) for c in ("rk2_walk", "rk4_walk_kick", "euler_walk")]
 WALK_CASES += [("golden_3d", c) for c in ("rk2_wbary_walk", "rk4_wnear_walk_kick")]
 CASES += WALK_CASES
+CASES += SIGMA_CASES
 
 
 def replay_cuda(g, cname):
