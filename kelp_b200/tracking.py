@@ -225,6 +225,12 @@ class Tracker:
         if elem_search not in ("local", "walk"):
             raise ValueError(f"elem_search must be 'local' or 'walk', got {elem_search!r}")
         self.walk = elem_search == "walk"
+        if getattr(mesh, "vertical_coord", "zlevel") == "sigma":
+            # the reference's loop hands every sigma step the surfaces at its
+            # start and end times from one function of time
+            # (tracking.py:2562-2596, _eta_at_time :3097-3133)
+            raise NotImplementedError("sigma meshes in the resident loop need the tracking layer's start/end "
+                                      "surfaces, which are not built; step them through the step functions")
         self.mesh = mesh
         self.fields = list(fields)
         self.file_times = np.asarray(file_times, dtype=np.float64)
