@@ -45,6 +45,15 @@ typedef struct {
     const int32_t* enb;   /* (E, max_v) edge neighbours of the compacted ring (walk), or NULL */
     const double* sigma;  /* (K) sigma interfaces, 1 surface -> 0 bed (vertical_coord "sigma"), or NULL */
     int sig;
+    int cg;                        /* 1: a NEMO C-grid mesh (readers/nemo/_mesh.py build_nemo_cgrid_mesh) */
+    const int32_t* cg_corners;     /* (E, 4) F-point corners SW, SE, NE, NW */
+    const int64_t* cg_ji;          /* (E, 2) T-cell (j, i) */
+    const int32_t* cg_nlev;        /* (E) wet levels (0: the dry ring) */
+    const int32_t* cg_nlev_r;      /* (ny*nx) wet levels per column */
+    int cg_nx, cg_K, cg_shrunk, cg_has_e;
+    int64_t cg_nynx;
+    const double *cg_e2u, *cg_e1v, *cg_area, *cg_zw, *cg_e3b, *cg_e3u, *cg_e3v;
+    const int32_t *cg_kbu, *cg_kbv;
 } OMesh;
 
 typedef struct {
@@ -1041,6 +1050,239 @@ static int walk_locate(const OMesh* m, double lon_p, double lat_p, int start, in
     return contain_local(m, lon_p, lat_p, nn);
 }
 
+/* ---- NEMO C-grid meshes (numerics/nemo_cgrid.py) ------------------- */
+
+/* the stage's face value at flat raster index idx (the rasters of the
+ * payload blended like every field, io.py:68-117) */
+static double cg_val(const void* a, const void* b, const void* t, const OField* f, int64_t idx, double alpha) {
+    return tblend(fld(a, f->f32, idx), fld(b, f->f32, idx), fld(t, f->f32, idx), f->alpha0, alpha);
+}
+
+/* nemo_cgrid.py:75-81 _nemo_cgrid_e3face */
+static double cg_e3face(const OMesh* m, const int32_t* kb, const double* e3, int64_t fi, int k) {
+    if (k == kb[fi]) return e3[fi];
+    return m->cg_zw[k + 1] - m->cg_zw[k];
+}
+
+static double pmax(double a, double b) { return b > a ? b : a; }   /* Python max(a, b) */
+static double pmin2(double a, double b) { return b < a ? b : a; }  /* Python min(a, b) */
+
+/* nemo_cgrid.py:84-222 _interp_nemo_cgrid_core: the cell (hint >= 0, else
+ * the local search around nn), the closed-form bilinear inverse, the face
+ * fluxes (model widths, or each edge's plane length), the logical velocity
+ * linear along its own axis; 3-D: zp is the fractional level s, W = ds/dt. */
+static int cgrid_core(const OMesh* m, const OField* f, double alpha, double xp, double yp, double zp, int nn, int hint,
+                      double td, int three_d, double* U, double* V, double* W) {
+    *U = 0.0; *V = 0.0; *W = 0.0;
+    int e = hint;
+    if (e < 0) {
+        e = contain_local(m, xp, yp, nn);
+        if (e < 0) return 0;
+    }
+    if (m->cg_nlev[e] <= 0) return 1;
+    const int64_t nx = m->cg_nx;
+    const int64_t c = m->cg_ji[2 * (int64_t)e] * nx + m->cg_ji[2 * (int64_t)e + 1];
+    int kz = 0;
+    int64_t nynx = 0;
+    double fW = 1.0, fE = 1.0, fS = 1.0, fN = 1.0, e3c = 1.0;
+    if (three_d) {
+        nynx = m->cg_nynx;
+        if (zp >= m->cg_nlev[e]) return 1;
+        kz = (int)floor(zp);
+        if (kz < 0) kz = 0;
+        if (kz > m->cg_K - 1) kz = m->cg_K - 1;
+        e3c = m->cg_zw[kz + 1] - m->cg_zw[kz];
+        if (kz == m->cg_nlev[e] - 1) e3c = m->cg_e3b[c];
+        fW = cg_e3face(m, m->cg_kbu, m->cg_e3u, c - 1, kz) / e3c;
+        fE = cg_e3face(m, m->cg_kbu, m->cg_e3u, c, kz) / e3c;
+        fS = cg_e3face(m, m->cg_kbv, m->cg_e3v, c - nx, kz) / e3c;
+        fN = cg_e3face(m, m->cg_kbv, m->cg_e3v, c, kz) / e3c;
+    }
+    const int64_t ko = (int64_t)kz * nynx;
+    double uW = cg_val(f->ua, f->ub, f->ut, f, ko + c - 1, alpha);
+    double uE = cg_val(f->ua, f->ub, f->ut, f, ko + c, alpha);
+    double vS = cg_val(f->va, f->vb, f->vt, f, ko + c - nx, alpha);
+    double vN = cg_val(f->va, f->vb, f->vt, f, ko + c, alpha);
+    const double M = SLM;
+    double cosl = cos(yp * DEG2RAD);
+    double px[4], py[4];
+    for (int k = 0; k < 4; ++k) {
+        int nd = m->cg_corners[4 * (int64_t)e + k];
+        px[k] = wrap180(m->lon[nd] - xp) * cosl * M;
+        py[k] = (m->lat[nd] - yp) * M;
+    }
+    double a0 = px[0], a1 = px[1] - px[0], a2 = px[3] - px[0], a3 = px[0] - px[1] + px[2] - px[3];
+    double b0 = py[0], b1 = py[1] - py[0], b2 = py[3] - py[0], b3 = py[0] - py[1] + py[2] - py[3];
+    double scale = pmax(pmax(pmax(pmax(fabs(a1), fabs(a2)), fabs(b1)), fabs(b2)), 1e-30);
+    double aa = a3 * b2 - a2 * b3;
+    double bb = a3 * b0 - a0 * b3 + a1 * b2 - a2 * b1;
+    double cc = a1 * b0 - a0 * b1;
+    double eta;
+    if (fabs(aa) < 1e-12 * scale * scale) {
+        if (fabs(bb) < 1e-300) return 0;
+        eta = -cc / bb;
+    } else {
+        double disc = bb * bb - 4.0 * aa * cc;
+        if (disc < 0.0) disc = 0.0;
+        double sq = sqrt(disc);
+        double r1 = (-bb + sq) / (2.0 * aa);
+        double r2 = (-bb - sq) / (2.0 * aa);
+        double d1 = pmax(pmax(0.0, -r1), r1 - 1.0);
+        double d2 = pmax(pmax(0.0, -r2), r2 - 1.0);
+        eta = d1 <= d2 ? r1 : r2;
+    }
+    eta = pmin2(pmax(eta, 0.0), 1.0);
+    double den = a1 + a3 * eta, den2 = b1 + b3 * eta;
+    double xi;
+    if (fabs(den) >= fabs(den2)) xi = (0.0 - a0 - a2 * eta) / den;
+    else xi = (0.0 - b0 - b2 * eta) / den2;
+    xi = pmin2(pmax(xi, 0.0), 1.0);
+    double U0, U1, V0, V1;
+    if (m->cg_has_e) {
+        U0 = fW * uW * m->cg_e2u[c - 1]; U1 = fE * uE * m->cg_e2u[c];
+        V0 = fS * vS * m->cg_e1v[c - nx]; V1 = fN * vN * m->cg_e1v[c];
+    } else {
+        double L[4];
+        for (int k = 0; k < 4; ++k) {
+            int na = m->cg_corners[4 * (int64_t)e + k], nb = m->cg_corners[4 * (int64_t)e + (k + 1) % 4];
+            double dl = wrap180(m->lon[nb] - m->lon[na]);
+            double cm = cos(0.5 * (m->lat[na] + m->lat[nb]) * DEG2RAD);
+            L[k] = hypot(dl * cm * M, (m->lat[nb] - m->lat[na]) * M);
+        }
+        U0 = fW * uW * L[3]; U1 = fE * uE * L[1]; V0 = fS * vS * L[0]; V1 = fN * vN * L[2];
+    }
+    double dxdxi = (1.0 - eta) * a1 + eta * (px[2] - px[3]);
+    double dydxi = (1.0 - eta) * b1 + eta * (py[2] - py[3]);
+    double dxdeta = (1.0 - xi) * a2 + xi * (px[2] - px[1]);
+    double dydeta = (1.0 - xi) * b2 + xi * (py[2] - py[1]);
+    double det = dxdxi * dydeta - dxdeta * dydxi;
+    double adet = fabs(det);
+    if (adet < 1e-12 * scale * scale) return 0;
+    double dxi = ((1.0 - xi) * U0 + xi * U1) / adet;
+    double deta = ((1.0 - eta) * V0 + eta * V1) / adet;
+    double Uv = dxdxi * dxi + dxdeta * deta;
+    double Vv = dydxi * dxi + dydeta * deta;
+    double Wv = 0.0;
+    if (three_d) {
+        double zeta = pmin2(pmax(zp - kz, 0.0), 1.0);
+        Wv = ((1.0 - zeta) * cg_val(f->wa, f->wb, f->wt, f, ko + c, alpha)
+              + zeta * cg_val(f->wa, f->wb, f->wt, f, ko + nynx + c, alpha)) * m->cg_area[c] / (adet * e3c);
+    }
+    *U = td * Uv; *V = td * Vv; *W = td * Wv;
+    return 1;
+}
+
+/* nemo_cgrid.py:391-402 _cell_thickness */
+static void cg_cell(const OMesh* m, int e, int ok, int k, int* kout, double* e3) {
+    int64_t c = ok ? m->cg_ji[2 * (int64_t)e] * m->cg_nx + m->cg_ji[2 * (int64_t)e + 1] : 0;
+    int nl = m->cg_nlev_r[c];
+    if (k < 0) k = 0;
+    if (k > m->cg_K - 1) k = m->cg_K - 1;
+    *kout = k;
+    *e3 = (k == nl - 1 && m->cg_shrunk) ? m->cg_e3b[c] : m->cg_zw[k + 1] - m->cg_zw[k];
+}
+
+/* nemo_cgrid.py:405-413 _level_coord, z -> s and s -> z */
+static double cg_z2s(const OMesh* m, int e, int ok, double z) {
+    int k = 0;
+    if (isnan(z)) k = m->cg_K;
+    else while (k < m->cg_K + 1 && m->cg_zw[k] <= z) ++k;
+    double e3;
+    cg_cell(m, e, ok, k - 1, &k, &e3);
+    return k + (z - m->cg_zw[k]) / e3;
+}
+static double cg_s2z(const OMesh* m, int e, int ok, double s) {
+    int k;
+    double e3;
+    cg_cell(m, e, ok, (int)floor(s), &k, &e3);
+    return m->cg_zw[k] + (s - k) * e3;
+}
+
+/* nemo_cgrid.py:416-512 nemo_cgrid3d_step for one particle: Euler / RK2
+ * (midpoint) / RK4 in the fractional level s = k + zeta of the start cell,
+ * stage n at x0 + a_n k_{n-1}, the weighted sum of the stage increments,
+ * s clamped at the surface, the end cell's domain check and s -> z; a
+ * particle that is not alive only gets the nearest node of its position. */
+static void step_cgrid3d(const OMesh* m, const OField* f, const OStep* s, int64_t i, double* lon, double* lat,
+                         double* z, int* status, int* nn, int8_t* fr, double* U, double* V, double* W) {
+    static const double A[3][4] = {{0.0}, {0.0, 0.5}, {0.0, 0.5, 0.5, 1.0}};
+    static const double B[3][4] = {{1.0}, {0.0, 1.0}, {1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6}};
+    const int ns = s->scheme == 0 ? 1 : (s->scheme == 1 ? 2 : 4);
+    double lon0 = lon[i], lat0 = lat[i], z0 = z[i], dt = s->dt;
+    int nn0 = anchor(m, lon0, lat0);
+    if (status[i] != ALIVE) {
+        U[i] = 0.0; V[i] = 0.0; W[i] = 0.0;
+        nn[i] = nn0;
+        return;
+    }
+    int e0 = contain_local(m, lon0, lat0, nn0);
+    int ok0 = e0 >= 0;
+    double s0 = cg_z2s(m, e0, ok0, z0);
+    double ks[4][3], first[3] = {0.0, 0.0, 0.0};
+    int ok = 1;
+    for (int n = 0; n < ns; ++n) {
+        double ln = lon0, lt = lat0, sn = s0;
+        if (n) {
+            ln = wrap180(lon0 + A[s->scheme][n] * ks[n - 1][0]);
+            lt = clat(lat0 + A[s->scheme][n] * ks[n - 1][1]);
+            sn = s0 + A[s->scheme][n] * ks[n - 1][2];
+        }
+        double Un = 0.0, Vn = 0.0, Wn = 0.0;
+        if (ok) {
+            int nnn = n ? anchor(m, ln, lt) : nn0;
+            int okn = cgrid_core(m, f, s->ak[n], ln, lt, sn, nnn, n ? -1 : (ok0 ? e0 : -1), s->td, 1, &Un, &Vn, &Wn);
+            ok = ok && okn;
+        }
+        if (n == 0) { first[0] = Un; first[1] = Vn; first[2] = Wn; }
+        ks[n][0] = dt * Un / z0_of(lt);
+        ks[n][1] = dt * Vn / SLM;
+        ks[n][2] = dt * Wn;
+    }
+    double d[3];
+    for (int c = 0; c < 3; ++c) {
+        d[c] = 0.0;
+        for (int n = 0; n < ns; ++n) d[c] += B[s->scheme][n] * ks[n][c];
+    }
+    double ln = lon0, lt = lat0, sv = s0;
+    if (ok) {
+        ln = wrap180(lon0 + d[0]);
+        lt = clat(lat0 + d[1]);
+        sv = s0 + d[2];
+        if (!(sv >= 0.0)) sv = isnan(sv) ? sv : 0.0;
+    }
+    int nne = anchor(m, ln, lt);
+    int e1 = contain_local(m, ln, lt, nne);
+    int in_dom = e1 >= 0;
+    int failed = !ok || !in_dom;
+    double zn = z0;
+    int st = ALIVE;
+    int8_t frr = fr[i];
+    if (failed) {
+        ln = lon0; lt = lat0; sv = s0; nne = nn0; st = OUTSIDE;
+        frr = !ok ? 1 : 2;
+    } else if (!(sv == s0 && e1 == e0)) {
+        zn = cg_s2z(m, e1, in_dom, sv);
+    }
+    int kk;
+    double e3;
+    cg_cell(m, e0, ok0, (int)floor(s0), &kk, &e3);
+    U[i] = first[0]; V[i] = first[1]; W[i] = first[2] * e3;
+    lon[i] = ln; lat[i] = lt; z[i] = zn;
+    status[i] = st; nn[i] = nne; fr[i] = frr;
+}
+
+/* u/v of a 2-D stage: the C-grid core on the surface faces
+ * (nemo_cgrid.py:355-388 interp_nemo_cgrid), else the barycentric core */
+static int uv2(const OMesh* m, const OField* f, double xp, double yp, int nn, double td, double alpha, double* U,
+               double* V) {
+    if (m->cg) {
+        double Wd;
+        int h = t_elem_hint;
+        return cgrid_core(m, f, alpha, xp, yp, 0.0, nn, h, td, 0, U, V, &Wd);
+    }
+    return interp_uv(m, f, xp, yp, nn, td, 0, alpha, U, V);
+}
+
 /* Walk mode (elem_search: walk, elem != NULL): each stage's containing
  * element is walked from the previous stage's (the step's start from the
  * carried one) and handed to the interpolation as its element hint; the
@@ -1332,6 +1574,10 @@ static void step_sigma(const OMesh* m, const OField* f, const OStep* s, int64_t 
 static void step_one(const OMesh* m, const OField* f, const OStep* s, int64_t i, double* lon, double* lat, double* z,
                      int* status, int* nn, int8_t* fr, double* U, double* V, double* W, const int64_t* pid,
                      int32_t* elem) {
+    if (m->cg && s->dims == 3) {
+        step_cgrid3d(m, f, s, i, lon, lat, z, status, nn, fr, U, V, W);
+        return;
+    }
     if (status[i] != ALIVE) {
         U[i] = 0.0; V[i] = 0.0;
         if (W) W[i] = 0.0;
@@ -1354,7 +1600,7 @@ static void step_one(const OMesh* m, const OField* f, const OStep* s, int64_t i,
     int ok = 1;
     if (s->dims == 2) {
         double U1, V1;
-        int ok1 = STAGE(e1, interp_uv(m, f, lon0, lat0, node_i, td, 0, s->ak[0], &U1, &V1));
+        int ok1 = STAGE(e1, uv2(m, f, lon0, lat0, node_i, td, s->ak[0], &U1, &V1));
         U[i] = U1; V[i] = V1;
         if (!ok1) { ok = 0; }
         else if (s->scheme == 0) {
@@ -1367,25 +1613,25 @@ static void step_one(const OMesh* m, const OField* f, const OStep* s, int64_t i,
             int em = LOC(lm, tm, e1, nm);
             e_last = em;
             double U2, V2;
-            if (!STAGE(em, interp_uv(m, f, lm, tm, nm, td, 0, s->ak[1], &U2, &V2))) ok = 0;
+            if (!STAGE(em, uv2(m, f, lm, tm, nm, td, s->ak[1], &U2, &V2))) ok = 0;
             else { ln = wrap180(lon0 + dt * U2 / z0_of(tm)); lt = clat(lat0 + dt * V2 / SLM); }
         } else {
             double dl1 = dt * U1 / z0_of(lat0), dt1 = dt * V1 / SLM;
             double l2 = wrap180(lon0 + 0.5 * dl1), t2 = clat(lat0 + 0.5 * dt1);
             double U2, V2, U3, V3, U4, V4;
             int n2 = anchor(m, l2, t2), e2 = LOC(l2, t2, e1, n2);
-            if (!STAGE(e2, interp_uv(m, f, l2, t2, n2, td, 0, s->ak[1], &U2, &V2))) ok = 0;
+            if (!STAGE(e2, uv2(m, f, l2, t2, n2, td, s->ak[1], &U2, &V2))) ok = 0;
             else {
                 double dl2 = dt * U2 / z0_of(t2), dt2 = dt * V2 / SLM;
                 double l3 = wrap180(lon0 + 0.5 * dl2), t3 = clat(lat0 + 0.5 * dt2);
                 int n3 = anchor(m, l3, t3), e3 = LOC(l3, t3, e2, n3);
-                if (!STAGE(e3, interp_uv(m, f, l3, t3, n3, td, 0, s->ak[2], &U3, &V3))) ok = 0;
+                if (!STAGE(e3, uv2(m, f, l3, t3, n3, td, s->ak[2], &U3, &V3))) ok = 0;
                 else {
                     double dl3 = dt * U3 / z0_of(t3), dt3 = dt * V3 / SLM;
                     double l4 = wrap180(lon0 + dl3), t4 = clat(lat0 + dt3);
                     int n4 = anchor(m, l4, t4), e4 = LOC(l4, t4, e3, n4);
                     e_last = e4;
-                    if (!STAGE(e4, interp_uv(m, f, l4, t4, n4, td, 0, s->ak[3], &U4, &V4))) ok = 0;
+                    if (!STAGE(e4, uv2(m, f, l4, t4, n4, td, s->ak[3], &U4, &V4))) ok = 0;
                     else {
                         double dl4 = dt * U4 / z0_of(t4), dt4 = dt * V4 / SLM;
                         double dl = (dl1 + 2.0 * dl2 + 2.0 * dl3 + dl4) / 6.0;
@@ -1583,6 +1829,15 @@ typedef struct {
     const int32_t* enb;
     const double* sigma;
     int sig;
+    int cg;                        /* 1: a NEMO C-grid mesh (readers/nemo/_mesh.py build_nemo_cgrid_mesh) */
+    const int32_t* cg_corners;     /* (E, 4) F-point corners SW, SE, NE, NW */
+    const int64_t* cg_ji;          /* (E, 2) T-cell (j, i) */
+    const int32_t* cg_nlev;        /* (E) wet levels (0: the dry ring) */
+    const int32_t* cg_nlev_r;      /* (ny*nx) wet levels per column */
+    int cg_nx, cg_K, cg_shrunk, cg_has_e;
+    int64_t cg_nynx;
+    const double *cg_e2u, *cg_e1v, *cg_area, *cg_zw, *cg_e3b, *cg_e3u, *cg_e3v;
+    const int32_t *cg_kbu, *cg_kbv;
 } orc_mesh;
 
 typedef struct {

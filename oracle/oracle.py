@@ -28,7 +28,13 @@ class OMesh(C.Structure):
                 ("nx", C.c_int), ("ny", C.c_int), ("wrap", C.c_int), ("far_rows", C.c_int),
                 ("exact", C.c_int), ("K", C.c_int),
                 ("dl_p", C.c_void_p), ("dl_bed", C.c_void_p), ("dl_last", C.c_void_p), ("dl_M", C.c_int),
-                ("enb", C.c_void_p), ("sigma", C.c_void_p), ("sig", C.c_int)]
+                ("enb", C.c_void_p), ("sigma", C.c_void_p), ("sig", C.c_int),
+                ("cg", C.c_int), ("cg_corners", C.c_void_p), ("cg_ji", C.c_void_p), ("cg_nlev", C.c_void_p),
+                ("cg_nlev_r", C.c_void_p), ("cg_nx", C.c_int), ("cg_K", C.c_int), ("cg_shrunk", C.c_int),
+                ("cg_has_e", C.c_int), ("cg_nynx", C.c_int64),
+                ("cg_e2u", C.c_void_p), ("cg_e1v", C.c_void_p), ("cg_area", C.c_void_p), ("cg_zw", C.c_void_p),
+                ("cg_e3b", C.c_void_p), ("cg_e3u", C.c_void_p), ("cg_e3v", C.c_void_p),
+                ("cg_kbu", C.c_void_p), ("cg_kbv", C.c_void_p)]
 
 
 class OField(C.Structure):
@@ -123,6 +129,22 @@ class MeshView:
         s.K = 0 if self.zl is None else int(self.zl.size)
         if self.sig is not None:   # sigma interfaces, 1 at the surface to 0 at the bed
             s.sigma, s.sig, s.K = _p(self.sig), 1, int(self.sig.size)
+        if getattr(mesh, "_nemo_cgrid", False):   # NEMO C-grid: the builder's tables
+            g = lambda name, t: c(getattr(mesh, "_nemo_cgrid_" + name), t)
+            self.cg = {"corners": g("corners", np.int32), "ji": g("elem_ji", np.int64),
+                       "nlev": g("nlev", np.int32), "nlev_r": c(np.asarray(mesh._nemo_cgrid_nlev_raster).reshape(-1),
+                                                                 np.int32),
+                       "e2u": g("e2u", np.float64), "e1v": g("e1v", np.float64), "area": g("area", np.float64),
+                       "zw": g("zw", np.float64), "e3b": g("e3b", np.float64), "e3u": g("e3u", np.float64),
+                       "e3v": g("e3v", np.float64), "kbu": g("kbu", np.int32), "kbv": g("kbv", np.int32)}
+            ny, nx = (int(x) for x in mesh._structured_shape)
+            s.cg, s.cg_nx, s.cg_nynx = 1, nx, ny * nx
+            s.cg_K = max(int(self.cg["zw"].size) - 1, 0)
+            s.cg_shrunk = int(getattr(mesh, "_nemo_cgrid_partial", "shrunk") == "shrunk")
+            s.cg_has_e = int(self.cg["e2u"].size > 0)
+            for k, v in self.cg.items():
+                setattr(s, "cg_" + k, _p(v) if v.size else None)
+            s.zlev, s.K = None, 0   # the C-grid step measures depth on its own interfaces
         enb = getattr(mesh, "_elem_neighbors", None)
         self.enb = None if enb is None else c(enb, np.int32)
         s.enb = _p(self.enb)

@@ -43,6 +43,13 @@ class Golden:
         m.vertical_coord = str(self.d["mesh_vertical_coord"]) if "mesh_vertical_coord" in self.d else "zlevel"
         m.metadata = {"exact_nearest": True}
         m._elem_neighbors = self.d.get("mesh_elem_neighbors")
+        if "mesh_cgrid_corners" in self.d:   # a NEMO C-grid mesh (build_nemo_cgrid_mesh)
+            m._nemo_cgrid = True
+            for k in ("corners", "elem_ji", "nlev", "nlev_raster", "zw", "area", "e3b", "kbu", "e3u", "kbv", "e3v",
+                      "e2u", "e1v"):
+                setattr(m, "_nemo_cgrid_" + k, self.d["mesh_cgrid_" + k])
+            m._structured_shape = tuple(int(x) for x in self.d["mesh_cgrid_shape"])
+            m._nemo_cgrid_partial = str(self.d["mesh_cgrid_partial"])
         self.mesh = m
         from kelp_b200.fields import VelocityField
         placement = {"golden_dl_lev": "level", "golden_dl_llin": "layer_linear",
@@ -54,7 +61,7 @@ class Golden:
             eta = self.d.get(f"snap{i}_eta")
             self.snaps.append(VelocityField(u=self.d[f"snap{i}_u"], v=self.d[f"snap{i}_v"], w=w,
                                             eta=np.zeros(self.d[f"snap{i}_u"].shape[-1]) if eta is None else eta,
-                                            uv_layout="node",
+                                            uv_layout="nemo_cgrid" if "mesh_cgrid_corners" in self.d else "node",
                                             uv_vertical=placement if w is not None else "layer",
                                             az=self.d.get(f"snap{i}_az")))
             i += 1

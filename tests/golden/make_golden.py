@@ -82,7 +82,8 @@ def payload(fields, t, T):
 
 
 def run_case(rm, fields, lon, lat, z, status, scheme, dt, T, n_steps, *, time_dir=1.0, w_interp="nearest",
-             kh=None, seed=7, real_id=0, pid_offset=0, record=(1,), az=None, walk=False, steady=False):
+             kh=None, seed=7, real_id=0, pid_offset=0, record=(1,), az=None, walk=False, steady=False,
+             uv_interp="barycentric"):
     fn = {"rk2": RI.rk2_step, "rk4": RI.rk4_step, "euler": RI.euler_step}[scheme]
     P = lon.size
     st = RState(lon=lon.copy(), lat=lat.copy(), z=z.copy(), status=status.copy(),
@@ -100,7 +101,7 @@ def run_case(rm, fields, lon, lat, z, status, scheme, dt, T, n_steps, *, time_di
         vel, vnext, dtn, ia, alpha = payload(fields, t, T)
         if steady:   # no time-aware payload: every stage reads the first record
             vel, vnext, dtn, ia, alpha = fields[0], None, -1.0, 0, 0.0
-        kw = dict(uv_interp="barycentric", w_interp=w_interp, vel_next=vnext,
+        kw = dict(uv_interp=uv_interp, w_interp=w_interp, vel_next=vnext,
                   dt_to_next=None if steady else dtn)
         if kh is not None:
             kw["diffusion"] = RDiff(scheme="uniform", kh_x=kh[0], kh_y=kh[1], seed=seed, real_id=real_id,
@@ -424,6 +425,107 @@ def sigma_fixture():
         save(f"golden_{tag}", mesh_record(rm), snaps, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
 
 
+CGRID_KEYS = ("corners", "elem_ji", "nlev", "nlev_raster", "zw", "area", "e3b", "kbu", "e3u", "kbv", "e3v",
+              "e2u", "e1v")
+
+
+def cgrid_fixture():
+    """NEMO C-grid meshes built by the reference's own builder
+    (readers/nemo/_mesh.py build_nemo_cgrid_mesh, imported without the
+    reader package, which needs xarray): a regional curvilinear raster with
+    islands, model face widths, and in 3-D z-levels with partial bottom cells
+    and partial u faces; face-raster u/v (and interface w) records."""
+    import types
+    src = os.environ.get("KELP_REFERENCE_SRC", "/root/reference/src")
+    for name in ("kelp.readers", "kelp.readers.nemo"):
+        if name not in sys.modules:
+            pkg = types.ModuleType(name)
+            pkg.__path__ = [os.path.join(src, *name.split("."))]
+            sys.modules[name] = pkg
+    from kelp.readers.nemo._mesh import build_nemo_cgrid_mesh
+    T = 86400.0
+    ny, nx = 36, 48
+    jj, ii = np.mgrid[0:ny, 0:nx].astype(np.float64)
+    glamf = -10.0 + 0.5 * ii + 0.06 * np.sin(0.2 * jj)
+    gphif = 30.0 + 0.4 * jj + 0.04 * np.cos(0.15 * ii)
+    # T-point geometry (cell centres) for the masks and metrics
+    glat_t = gphif - 0.2
+    noise = (np.sin(0.31 * ii + 0.7) * np.cos(0.27 * jj - 0.4) + 0.6 * np.sin(0.13 * ii * jj / 9.0 + 1.1))
+    wet = noise > -0.55
+    wet[:, :2] = False
+    wet[:2, :] = False
+    e1t = 0.5 * 111120.0 * np.cos(np.radians(glat_t))
+    e2t = np.full((ny, nx), 0.4 * 111120.0)
+    e2u = e2t * (1.0 + 0.01 * np.sin(0.3 * jj))
+    e1v = 0.5 * 111120.0 * np.cos(np.radians(gphif))
+    zw = np.concatenate([[0.0], np.cumsum(10.0 * 1.35 ** np.arange(12))])   # 13 interfaces
+    K = zw.size - 1
+    depth = 60.0 + (zw[-1] - 80.0) * 0.5 * (1.0 + np.sin(0.11 * ii + 0.3) * np.cos(0.09 * jj))
+    nlev = np.where(wet, np.clip(np.searchsorted(zw, depth, side="left"), 1, K), 0).astype(np.int32)
+    lay = np.diff(zw)
+    bot_ref = lay[np.maximum(nlev - 1, 0)]
+    e3b = np.where(nlev > 0, np.clip(depth - zw[np.maximum(nlev - 1, 0)], 0.3 * bot_ref, bot_ref), 0.0)
+    e3u0 = np.broadcast_to(lay[:, None, None], (K, ny, nx)).copy()
+    for j in range(ny):
+        for i in range(nx - 1):
+            kb = min(nlev[j, i], nlev[j, i + 1]) - 1
+            if kb >= 0:
+                e3u0[kb, j, i] = min(e3b[j, i] if nlev[j, i] - 1 == kb else lay[kb],
+                                     e3b[j, i + 1] if nlev[j, i + 1] - 1 == kb else lay[kb])
+    area = e1t * e2t
+    rng = np.random.default_rng(41)
+    m3 = build_nemo_cgrid_mesh(glamf, gphif, wet, e2u=e2u, e1v=e1v, nlev2d=nlev, zw=zw, area=area, e3b=e3b,
+                               e3u0=e3u0, name="cgrid3d")
+    set_exact_nearest(m3, True)
+    m2 = build_nemo_cgrid_mesh(glamf, gphif, wet, name="cgrid2d")
+    set_exact_nearest(m2, True)
+
+    def fields(three_d, n_snap=4):
+        out = []
+        lev = np.arange(K)[:, None, None]
+        for k in range(n_snap):
+            ph = 0.8 * k
+            u = 0.4 * np.sin(0.25 * jj + ph) * np.cos(0.18 * ii) + 0.1
+            v = 0.3 * np.cos(0.2 * ii - ph) * np.sin(0.15 * jj) - 0.05
+            if not three_d:
+                uu = np.where(wet, u, 0.0).astype(np.float32).reshape(-1)
+                vv = np.where(wet, v, 0.0).astype(np.float32).reshape(-1)
+                out.append(RVel(u=uu, v=vv, w=None, eta=np.zeros(ny * nx), uv_layout="nemo_cgrid"))
+                continue
+            dec = np.exp(-zw[:-1] / 600.0)[:, None, None]
+            uu = (u[None] * dec * (lev < nlev[None])).astype(np.float32).reshape(K, -1)
+            vv = (v[None] * dec * (lev < nlev[None])).astype(np.float32).reshape(K, -1)
+            ww = (2e-4 * np.sin(0.3 * ii + 0.2 * jj + ph)[None] * np.sin(np.pi * zw / zw[-1])[:, None, None]
+                  ).astype(np.float32).reshape(K + 1, -1)
+            out.append(RVel(u=uu, v=vv, w=ww, eta=np.zeros(ny * nx), uv_layout="nemo_cgrid"))
+        return out
+
+    P = 1500
+    lon = rng.uniform(glamf.min(), glamf.max(), P)
+    lat = rng.uniform(gphif.min(), gphif.max(), P)
+    z = rng.uniform(0.0, 1800.0, P)
+    status = np.full(P, int(ParticleStatus.ALIVE), np.int32)
+    status[rng.choice(P, 30, replace=False)] = int(ParticleStatus.OUTSIDE)
+    for rm, tag, three_d in ((m2, "cgrid2d", False), (m3, "cgrid3d", True)):
+        rf = fields(three_d)
+        run = dict(uv_interp="nemo_cgrid")
+        cases = {"rk2": run_case(rm, rf, lon, lat, z, status, "rk2", 7200.0, T, 12, **run),
+                 "rk4": run_case(rm, rf, lon, lat, z, status, "rk4", 7200.0, T, 12, **run),
+                 "euler": run_case(rm, rf, lon, lat, z, status, "euler", 3600.0, T, 12, **run),
+                 "rk2_bwd": run_case(rm, rf, lon, lat, z, status, "rk2", 7200.0, T, 12, time_dir=-1.0, **run),
+                 "rk4_steady": run_case(rm, rf, lon, lat, z, status, "rk4", 7200.0, T, 8, steady=True, **run)}
+        if not three_d:
+            cases["rk2_kick"] = run_case(rm, rf, lon, lat, z, status, "rk2", 7200.0, T, 12, kh=(50.0, 50.0),
+                                         seed=13, **run)
+            cases["rk2_walk"] = run_case(rm, rf, lon, lat, z, status, "rk2", 7200.0, T, 12, walk=True, **run)
+        rec = mesh_record(rm)
+        for k in CGRID_KEYS:
+            rec["cgrid_" + k] = np.asarray(getattr(rm, "_nemo_cgrid_" + k))
+        rec["cgrid_shape"] = np.array(rm._structured_shape)
+        rec["cgrid_partial"] = np.array(rm._nemo_cgrid_partial)
+        save(f"golden_{tag}", rec, rf, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
+
+
 def time_fixture():
     """The reference's time-bracket resolution (tracking._resolve_time_bracket)
     on a grid of query times, record axes, modes and directions."""
@@ -447,7 +549,7 @@ def time_fixture():
 
 if __name__ == "__main__":
     # no argument: every fixture; otherwise the named ones ("steps", "beach")
-    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma"}
+    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid"}
     if "steps" in which:
         main()
     if "beach" in which:
@@ -456,3 +558,5 @@ if __name__ == "__main__":
         time_fixture()
     if "sigma" in which:
         sigma_fixture()
+    if "cgrid" in which:
+        cgrid_fixture()

@@ -29,6 +29,10 @@ SIGMA_CASES = [("golden_sigma", c) for c in ("rk2_wnear", "rk2_wbary", "rk4_wbar
                                              "rk2_wbary_steady", "rk4_wnear_steady", "rk2_wbary_walk")]
 SIGMA_CASES += [("golden_sigma_llin", c) for c in ("rk2_llin_wbary", "rk4_llin_wnear_kick", "euler_llin_wnear")]
 CASES += SIGMA_CASES
+# NEMO C-grid meshes (uv_interp nemo_cgrid): the 2-D unfused steps and the 3-D fractional-level step
+CGRID_CASES = [("golden_cgrid2d", c) for c in ("rk2", "rk4", "euler", "rk2_bwd", "rk4_steady", "rk2_kick", "rk2_walk")]
+CGRID_CASES += [("golden_cgrid3d", c) for c in ("rk2", "rk4", "euler", "rk2_bwd", "rk4_steady")]
+CASES += CGRID_CASES
 
 
 def diffusion_args(c, k):
