@@ -29,6 +29,9 @@
  *                         (src/kelp/core/mesh.py:2631-2712)
  *   kc_elem_neighbors_upload <- core.mesh.build_elem_neighbors (src/kelp/core/mesh.py:2824)
  *   kc_sigma_upload    <- core.mesh.Mesh.sigma with vertical_coord "sigma" (src/kelp/core/mesh.py:63-91)
+ *   kc_cgrid_upload    <- the C-grid tables of readers.nemo._mesh.build_nemo_cgrid_mesh
+ *                         (src/kelp/readers/nemo/_mesh.py:16-264), read by
+ *                         numerics.nemo_cgrid (src/kelp/numerics/nemo_cgrid.py:84-512)
  *   kc_field_upload_eta <- core.io.VelocityField.eta (src/kelp/core/io.py:180)
  *   kc_rng_normals     <- numerics.diffusion._normal_pair (src/kelp/numerics/diffusion.py:233)
  */
@@ -39,7 +42,7 @@
 extern "C" {
 #endif
 
-#define KC_ABI_VERSION 5
+#define KC_ABI_VERSION 6
 
 #define KC_OK 0
 #define KC_ERR_ARG 1      /* invalid argument or combination */
@@ -180,6 +183,36 @@ int kc_sigma_upload(kc_ctx* ctx, int K, const double* sigma);
 /* The free surface eta (n_nodes float64) of the snapshot in ring slot
  * `slot`; uploading a new snapshot into the slot drops it. */
 int kc_field_upload_eta(kc_ctx* ctx, int slot, long long n_nodes, const double* eta);
+
+/* The NEMO C-grid tables of a mesh built by build_nemo_cgrid_mesh (nodes =
+ * F-points, elements = T-cells with a ring of dry cells), uploaded after
+ * kc_mesh_upload.  Steps on such a mesh read face-raster snapshots
+ * (kc_field_upload with n_nodes = ny * nx: u, v one row in 2-D, K rows in
+ * 3-D, w K + 1 rows) through the exact C-grid interpolation
+ * (numerics/nemo_cgrid.py:84-222): 2-D steps as the reference's unfused
+ * Euler / RK2 / RK4 with uv_interp "nemo_cgrid", 3-D steps as
+ * nemo_cgrid3d_step (:416-512, fractional level coordinate, no diffusion).
+ * Plain form only. */
+typedef struct kc_cgrid_desc {
+    int ny, nx;                  /* T / F raster shape (mesh._structured_shape) */
+    int K;                       /* levels (zw has K + 1 interfaces); 0 for a 2-D mesh */
+    int partial_shrunk;          /* mesh._nemo_cgrid_partial: 1 "shrunk", 0 "porous" */
+    const int* corners;          /* (E, 4) node ids SW, SE, NE, NW (_nemo_cgrid_corners) */
+    const long long* elem_ji;    /* (E, 2) T-cell (j, i), j, i >= 1 (_nemo_cgrid_elem_ji) */
+    const int* nlev;             /* (E) wet levels, 0 for the dry ring (_nemo_cgrid_nlev) */
+    const int* nlev_raster;      /* (ny * nx) wet levels per column */
+    const double* e2u;           /* (ny * nx) model u-face widths, or NULL (plane edge lengths) */
+    const double* e1v;           /* (ny * nx) model v-face widths, or NULL */
+    const double* area;          /* 3-D: (ny * nx) T-cell areas */
+    const double* zw;            /* 3-D: (K + 1) interfaces, positive down */
+    const double* e3b;           /* 3-D: (ny * nx) bottom wet cell thickness */
+    const int* kbu;              /* 3-D: (ny * nx) partial level of each u face, -1 none */
+    const double* e3u;           /* 3-D: (ny * nx) its thickness */
+    const int* kbv;              /* 3-D: (ny * nx) partial level of each v face, -1 none */
+    const double* e3v;           /* 3-D: (ny * nx) its thickness */
+} kc_cgrid_desc;
+
+int kc_cgrid_upload(kc_ctx* ctx, const kc_cgrid_desc* desc);
 
 /* Edge-neighbour table of the mesh (E x max_v int32, -1 on boundary edges;
  * entry k is the element across the edge from compacted-ring vertex k to the

@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libkelpcuda
 KC_OK, KC_ERR_ARG, KC_ERR_CUDA, KC_ERR_STATE, KC_ERR_DEVICE = 0, 1, 2, 3, 4
 KC_F32, KC_F64, KC_F16 = 0, 1, 2
 KC_PLAIN, KC_MIXED = 0, 1
-ABI_VERSION = 5
+ABI_VERSION = 6
 KC_EULER, KC_RK2, KC_RK4 = 0, 1, 2
 
 #: every symbol include/kelp_cuda.h declares
@@ -26,7 +26,7 @@ EXPORTS = ("kc_abi_version", "kc_node_xyz_fill", "kc_create", "kc_destroy", "kc_
            "kc_particles_download", "kc_coastal_upload", "kc_beach_state_upload",
            "kc_beach_state_download", "kc_beach", "kc_step", "kc_step_host", "kc_step_range", "kc_run_fused",
            "kc_particles_set_realization", "kc_elem_neighbors_upload", "kc_particles_set_elem",
-           "kc_particles_get_elem", "kc_find_elements_walk", "kc_find_elements", "kc_sigma_upload", "kc_field_upload_eta",
+           "kc_particles_get_elem", "kc_find_elements_walk", "kc_find_elements", "kc_sigma_upload", "kc_field_upload_eta", "kc_cgrid_upload",
            "kc_set_fused_block", "kc_run", "kc_sort", "kc_find_nearest", "kc_find_nearest_noalloc", "kc_rng_normals", "kc_device_errors",
            "kc_event_record", "kc_event_elapsed", "kc_l2_flush", "kc_host_alloc", "kc_host_free")
 
@@ -88,6 +88,14 @@ class BeachArgs(C.Structure):
                 ("step_i", C.c_ulonglong), ("pid_offset", C.c_ulonglong)]
 
 
+class CgridDesc(C.Structure):
+    _fields_ = [("ny", C.c_int), ("nx", C.c_int), ("K", C.c_int), ("partial_shrunk", C.c_int),
+                ("corners", C.c_void_p), ("elem_ji", C.c_void_p), ("nlev", C.c_void_p), ("nlev_raster", C.c_void_p),
+                ("e2u", C.c_void_p), ("e1v", C.c_void_p), ("area", C.c_void_p), ("zw", C.c_void_p),
+                ("e3b", C.c_void_p), ("kbu", C.c_void_p), ("e3u", C.c_void_p), ("kbv", C.c_void_p),
+                ("e3v", C.c_void_p)]
+
+
 class HostParticles(C.Structure):
     _fields_ = [("lon", C.c_void_p), ("lat", C.c_void_p), ("z", C.c_void_p), ("status", C.c_void_p),
                 ("nearest_node", C.c_void_p), ("failure_reason", C.c_void_p),
@@ -136,6 +144,7 @@ def lib():
         L.kc_find_elements.argtypes = [vp, ll, vp, vp, vp, vp]
         L.kc_sigma_upload.argtypes = [vp, i, vp]
         L.kc_field_upload_eta.argtypes = [vp, i, ll, vp]
+        L.kc_cgrid_upload.argtypes = [vp, C.POINTER(CgridDesc)]
         L.kc_set_fused_block.argtypes = [vp, i]
         L.kc_step_host.argtypes = [vp, C.POINTER(StepArgs), ll, C.POINTER(HostParticles), C.POINTER(HostParticles),
                                    ll]

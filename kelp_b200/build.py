@@ -22,6 +22,7 @@ LIB = os.path.join(HERE, "libkelpcuda.so")
 CU_SOURCES = ["kc_api.cu", "kc_mixed.cu"]
 CPP_SOURCES = ["kc_host.cpp"]
 HEADERS = ["kc_geom.cuh", "kc_interp.cuh", "kc_step.cuh", "kc_beach.cuh", "kc_mixed.cuh", "kc_kernels.cuh", "kc_sigma.cuh",
+           "kc_cgrid.cuh",
            "kc_host.h"]
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",

@@ -68,6 +68,15 @@ struct kc_ctx {
     double* d_dl_bed = nullptr;
     int4* d_enb = nullptr;   // edge neighbours of the compacted rings (kc_elem_neighbors_upload)
     double* d_sigma = nullptr;   // sigma interfaces (kc_sigma_upload)
+    // NEMO C-grid tables (kc_cgrid_upload)
+    int4* d_cg_corners = nullptr;
+    int* d_cg_cell = nullptr;
+    int* d_cg_nlev = nullptr;
+    int* d_cg_nlev_r = nullptr;
+    double4* d_cg_L = nullptr;
+    double *d_cg_e2u = nullptr, *d_cg_e1v = nullptr, *d_cg_area = nullptr, *d_cg_zw = nullptr, *d_cg_e3b = nullptr;
+    double *d_cg_e3u = nullptr, *d_cg_e3v = nullptr;
+    int *d_cg_kbu = nullptr, *d_cg_kbv = nullptr;
     int max_v = 0;
     int* d_err = nullptr;
     kc::DMesh dm{};
@@ -358,7 +367,10 @@ namespace {
 
 int launch_step_on(kc_ctx* c, const kc_step_args* a, const kc::DState& st, const kc::DStep& s) {
     const int dtype = c->slots[a->slot_a].dtype;
-    if (c->dm.sig && a->dims == 3) {   // sigma meshes: the plain form's s = z / H_p step
+    if (c->dm.cg.on) {   // NEMO C-grid meshes: the exact C-grid steps (plain form)
+        if (dtype == KC_F32) launch_cgrid_kernel<float>(c->dm, blend_of<float>(c, a), st, s, a->dims, a->scheme, c->stream);
+        else launch_cgrid_kernel<double>(c->dm, blend_of<double>(c, a), st, s, a->dims, a->scheme, c->stream);
+    } else if (c->dm.sig && a->dims == 3) {   // sigma meshes: the plain form's s = z / H_p step
         if (dtype == KC_F32) launch_sigma_kernel<float>(c->dm, blend_of<float>(c, a), st, s, a->scheme, c->stream);
         else launch_sigma_kernel<double>(c->dm, blend_of<double>(c, a), st, s, a->scheme, c->stream);
     } else if (a->precision == KC_MIXED) {
@@ -392,6 +404,27 @@ int check_step(kc_ctx* c, const kc_step_args* a) {
     if (a->kick && !(a->kh_x >= 0.0 && a->kh_y >= 0.0)) return fail(c, KC_ERR_ARG, "kc_step: Kh must be >= 0");
     if (a->precision != KC_PLAIN && a->precision != KC_MIXED)
         return fail(c, KC_ERR_ARG, "kc_step: precision must be KC_PLAIN or KC_MIXED");
+    if (c->dm.cg.on) {
+        if (a->precision != KC_PLAIN) return fail(c, KC_ERR_ARG, "kc_step: C-grid meshes step in the plain form");
+        if (a->az_kick) return fail(c, KC_ERR_ARG, "kc_step: the Az kick on C-grid meshes is not built");
+        if (a->dims == 3 && (a->kick || c->dm.cg.K < 1))
+            return fail(c, KC_ERR_ARG, "kc_step: the 3-D C-grid step needs a 3-D C-grid mesh and takes no kick");
+        const long long nynx = c->dm.cg.nynx;
+        const int sl3[3] = {a->slot_a, a->slot_b, a->slot_t};
+        for (int k = 0; k < 3; ++k) {
+            if (sl3[k] < 0 || sl3[k] >= kSlots) return fail(c, KC_ERR_ARG, "kc_step: slot out of range");
+            const Slot& s = c->slots[sl3[k]];
+            if (s.dtype < 0) return fail(c, KC_ERR_STATE, "kc_step: snapshot slot " + std::to_string(sl3[k]) + " is empty");
+            if (s.dtype == KC_F16) return fail(c, KC_ERR_ARG, "kc_step: C-grid steps read float32 or float64 rasters");
+            if (s.n != nynx) return fail(c, KC_ERR_ARG, "kc_step: C-grid snapshots are ny * nx face rasters");
+            if (a->dims == 2 && s.uv_rows != 1 && s.uv_rows != c->dm.cg.K)
+                return fail(c, KC_ERR_ARG, "kc_step: 2-D C-grid u/v need one row (or K, the surface read)");
+            if (a->dims == 3 && (s.uv_rows != c->dm.cg.K || s.w_rows != c->dm.cg.K + 1))
+                return fail(c, KC_ERR_ARG, "kc_step: 3-D C-grid fields need u/v (K, ny*nx) and w (K+1, ny*nx)");
+        }
+        if (c->P > 0 && !c->lon) return fail(c, KC_ERR_STATE, "kc_step: no particles uploaded");
+        return KC_OK;
+    }
     if (c->dm.sig && a->dims == 3) {
         if (a->precision != KC_PLAIN) return fail(c, KC_ERR_ARG, "kc_step: sigma meshes step in the plain form");
         if (a->az_kick) return fail(c, KC_ERR_ARG, "kc_step: the Az kick on sigma meshes is not built");
@@ -466,6 +499,10 @@ void free_mesh(kc_ctx* c) {
     dfree(c->d_gh_tab); dfree(c->d_xyz); dfree(c->d_depth); dfree(c->d_zlev);
     dfree(c->d_nsc); dfree(c->d_ecos); dfree(c->d_maxl); dfree(c->d_coastal);
     dfree(c->d_dl_p); dfree(c->d_dl_last); dfree(c->d_dl_bed); dfree(c->d_enb); dfree(c->d_sigma);
+    dfree(c->d_cg_corners); dfree(c->d_cg_cell); dfree(c->d_cg_nlev); dfree(c->d_cg_nlev_r); dfree(c->d_cg_L);
+    dfree(c->d_cg_e2u); dfree(c->d_cg_e1v); dfree(c->d_cg_area); dfree(c->d_cg_zw); dfree(c->d_cg_e3b);
+    dfree(c->d_cg_e3u); dfree(c->d_cg_e3v); dfree(c->d_cg_kbu); dfree(c->d_cg_kbv);
+    c->dm.cg = kc::DCgrid{};
     c->dm.dl_p = nullptr; c->dm.dl_last = nullptr; c->dm.dl_bed = nullptr; c->dm.dl_M = 0;
     c->dm.enb = nullptr;
     c->dm.sigma = nullptr; c->dm.sig = 0;
@@ -647,6 +684,86 @@ int kc_coastal_upload(kc_ctx* c, const unsigned char* flags) {
     return KC_OK;
 }
 
+int kc_cgrid_upload(kc_ctx* c, const kc_cgrid_desc* d) {
+    if (!c || !d) return KC_ERR_ARG;
+    if (!c->has_mesh) return fail(c, KC_ERR_STATE, "kc_cgrid_upload: no mesh uploaded");
+    const long long E = c->E, N = c->N;
+    if (d->ny < 2 || d->nx < 2 || d->K < 0) return fail(c, KC_ERR_ARG, "kc_cgrid_upload: raster shape");
+    if (!d->corners || !d->elem_ji || !d->nlev || !d->nlev_raster)
+        return fail(c, KC_ERR_ARG, "kc_cgrid_upload: missing cell tables");
+    if ((d->e2u == nullptr) != (d->e1v == nullptr)) return fail(c, KC_ERR_ARG, "kc_cgrid_upload: e2u and e1v go together");
+    if (d->K > 0 && (!d->area || !d->zw || !d->e3b || !d->kbu || !d->e3u || !d->kbv || !d->e3v))
+        return fail(c, KC_ERR_ARG, "kc_cgrid_upload: a 3-D mesh needs area, zw, e3b and the face partial levels");
+    const long long nynx = (long long)d->ny * d->nx;
+    std::vector<int4> cr((size_t)E);
+    std::vector<int> cell((size_t)E);
+    for (long long e = 0; e < E; ++e) {
+        const int* q = d->corners + 4 * e;
+        for (int k = 0; k < 4; ++k)
+            if (q[k] < 0 || q[k] >= N) return fail(c, KC_ERR_ARG, "kc_cgrid_upload: corner out of range");
+        const long long j = d->elem_ji[2 * e], i = d->elem_ji[2 * e + 1];
+        if (j < 1 || j >= d->ny || i < 1 || i >= d->nx) return fail(c, KC_ERR_ARG, "kc_cgrid_upload: cell (j, i) out of range");
+        if (d->nlev[e] < 0 || (d->K > 0 && d->nlev[e] > d->K))
+            return fail(c, KC_ERR_ARG, "kc_cgrid_upload: wet levels out of range");
+        cr[e] = make_int4(q[0], q[1], q[2], q[3]);
+        cell[e] = (int)(j * d->nx + i);
+    }
+    for (long long k = 0; k < nynx; ++k)
+        if (d->nlev_raster[k] < 0 || (d->K > 0 && d->nlev_raster[k] > d->K))
+            return fail(c, KC_ERR_ARG, "kc_cgrid_upload: raster wet levels out of range");
+    if (d->K > 0) {
+        for (long long k = 0; k < nynx; ++k)
+            if (d->kbu[k] < -1 || d->kbu[k] >= d->K || d->kbv[k] < -1 || d->kbv[k] >= d->K)
+                return fail(c, KC_ERR_ARG, "kc_cgrid_upload: face partial level out of range");
+        for (int k = 0; k < d->K; ++k)
+            if (!(d->zw[k + 1] > d->zw[k])) return fail(c, KC_ERR_ARG, "kc_cgrid_upload: zw must increase");
+    }
+    std::vector<double> L;
+    if (!d->e2u) {
+        std::vector<double2> ll((size_t)N);
+        std::vector<double> lon((size_t)N), lat((size_t)N);
+        KC_CUDA(c, cudaSetDevice(c->device));
+        KC_CUDA(c, cudaMemcpy(ll.data(), c->d_ll, (size_t)N * 16, cudaMemcpyDeviceToHost));
+        for (long long n = 0; n < N; ++n) { lon[n] = ll[n].x; lat[n] = ll[n].y; }
+        L.resize((size_t)E * 4);
+        kc_host::cgrid_edge_lengths(E, d->corners, lon.data(), lat.data(), L.data());
+    }
+    KC_CUDA(c, cudaSetDevice(c->device));
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    dfree(c->d_cg_corners); dfree(c->d_cg_cell); dfree(c->d_cg_nlev); dfree(c->d_cg_nlev_r); dfree(c->d_cg_L);
+    dfree(c->d_cg_e2u); dfree(c->d_cg_e1v); dfree(c->d_cg_area); dfree(c->d_cg_zw); dfree(c->d_cg_e3b);
+    dfree(c->d_cg_e3u); dfree(c->d_cg_e3v); dfree(c->d_cg_kbu); dfree(c->d_cg_kbv);
+    c->dm.cg = kc::DCgrid{};
+    int rc;
+    if ((rc = upload(c, &c->d_cg_corners, cr.data(), cr.size()))) return rc;
+    if ((rc = upload(c, &c->d_cg_cell, cell.data(), cell.size()))) return rc;
+    if ((rc = upload(c, &c->d_cg_nlev, d->nlev, (size_t)E))) return rc;
+    if ((rc = upload(c, &c->d_cg_nlev_r, d->nlev_raster, (size_t)nynx))) return rc;
+    if (!L.empty() && (rc = upload(c, &c->d_cg_L, L.data(), (size_t)E))) return rc;
+    if (d->e2u) {
+        if ((rc = upload(c, &c->d_cg_e2u, d->e2u, (size_t)nynx))) return rc;
+        if ((rc = upload(c, &c->d_cg_e1v, d->e1v, (size_t)nynx))) return rc;
+    }
+    if (d->K > 0) {
+        if ((rc = upload(c, &c->d_cg_area, d->area, (size_t)nynx))) return rc;
+        if ((rc = upload(c, &c->d_cg_zw, d->zw, (size_t)d->K + 1))) return rc;
+        if ((rc = upload(c, &c->d_cg_e3b, d->e3b, (size_t)nynx))) return rc;
+        if ((rc = upload(c, &c->d_cg_kbu, d->kbu, (size_t)nynx))) return rc;
+        if ((rc = upload(c, &c->d_cg_e3u, d->e3u, (size_t)nynx))) return rc;
+        if ((rc = upload(c, &c->d_cg_kbv, d->kbv, (size_t)nynx))) return rc;
+        if ((rc = upload(c, &c->d_cg_e3v, d->e3v, (size_t)nynx))) return rc;
+    }
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    kc::DCgrid& g = c->dm.cg;
+    g.corners = c->d_cg_corners; g.cell = c->d_cg_cell; g.nlev = c->d_cg_nlev; g.nlev_r = c->d_cg_nlev_r;
+    g.L = c->d_cg_L; g.e2u = c->d_cg_e2u; g.e1v = c->d_cg_e1v; g.area = c->d_cg_area; g.zw = c->d_cg_zw;
+    g.e3b = c->d_cg_e3b; g.kbu = c->d_cg_kbu; g.e3u = c->d_cg_e3u; g.kbv = c->d_cg_kbv; g.e3v = c->d_cg_e3v;
+    g.nynx = nynx; g.nx = d->nx; g.K = d->K; g.shrunk = d->partial_shrunk ? 1 : 0; g.has_e = d->e2u ? 1 : 0;
+    g.on = 1;
+    ++c->mesh_gen;
+    return KC_OK;
+}
+
 int kc_sigma_upload(kc_ctx* c, int K, const double* sigma) {
     if (!c) return KC_ERR_ARG;
     if (!c->has_mesh) return fail(c, KC_ERR_STATE, "kc_sigma_upload: no mesh uploaded");
@@ -759,6 +876,7 @@ int kc_beach_state_download(kc_ctx* c, int* wet_streak) {
 // device-side argument block.
 static int beach_of(kc_ctx* c, const kc_beach_args* a, kc::DBeach& b) {
     if (!c->has_mesh) return fail(c, KC_ERR_STATE, "kc_beach: no mesh uploaded");
+    if (c->dm.cg.on) return fail(c, KC_ERR_ARG, "kc_beach: the reference runs no beaching on C-grid meshes");
     if (!c->has_beach) return fail(c, KC_ERR_STATE, "kc_beach: call kc_beach_state_upload first");
     if (!c->d_depth) return fail(c, KC_ERR_STATE, "kc_beach: the mesh has no depth");
     if (a->resuspension < 0 || a->resuspension > 3) return fail(c, KC_ERR_ARG, "kc_beach: resuspension code");
@@ -1324,6 +1442,7 @@ int kc_run_fused(kc_ctx* c, const kc_step_args* steps, int n_steps, const kc_bea
         return fail(c, KC_ERR_STATE, "kc_run_fused: carried walk elements step through kc_step / kc_run");
     if (c->dm.sig && steps[0].dims == 3)
         return fail(c, KC_ERR_STATE, "kc_run_fused: sigma meshes step through kc_step / kc_run");
+    if (c->dm.cg.on) return fail(c, KC_ERR_STATE, "kc_run_fused: C-grid meshes step through kc_step / kc_run");
     if (c->P == 0) return KC_OK;
     KC_CUDA(c, cudaSetDevice(c->device));
     if ((rc = pin_pid(c))) return rc;

@@ -34,6 +34,27 @@ constexpr int FR_INTERP = 1, FR_OOB = 2;
 constexpr int ERR_SEARCH_CAP = 1;   // exact-search growth loop hit its cap
 constexpr int ERR_BAD_ANCHOR = 2;   // a particle's nearest_node is outside [-N, N)
 
+// The NEMO C-grid tables of a mesh built by readers/nemo/_mesh.py
+// build_nemo_cgrid_mesh (nodes = F-points, elements = T-cells), or on = 0.
+struct DCgrid {
+    const int4* corners;      // (E) F-point corners SW, SE, NE, NW
+    const int* cell;          // (E) flat T index j * nx + i (j, i >= 1)
+    const int* nlev;          // (E) wet levels, 0 for the dry ring
+    const int* nlev_r;        // (ny * nx) wet levels per column
+    const double4* L;         // (E) plane edge lengths S, E, N, W (host C library) when has_e is 0
+    const double* e2u;        // (ny * nx) model u-face widths (has_e)
+    const double* e1v;        // (ny * nx) model v-face widths (has_e)
+    const double* area;       // (ny * nx) T-cell areas (3-D)
+    const double* zw;         // (K + 1) reference interfaces (3-D)
+    const double* e3b;        // (ny * nx) bottom wet cell thickness (3-D)
+    const int* kbu;           // (ny * nx) partial level of each u face, -1 none (3-D)
+    const double* e3u;
+    const int* kbv;
+    const double* e3v;
+    long long nynx;
+    int nx, K, shrunk, has_e, on;
+};
+
 // Resident mesh: node table, element table, node->element CSR, grid hash and
 // the host-evaluated trigonometric tables.
 struct DMesh {
@@ -55,6 +76,7 @@ struct DMesh {
     const int4* enb;          // (E) edge neighbours of the compacted ring (edge walk), or null
     const double* sigma;      // (K) sigma interfaces, 1 surface -> 0 bed (sigma meshes), or null
     int sig;                  // 1: sigma mesh (K counts its interfaces, zlev is null)
+    DCgrid cg;                // NEMO C-grid tables (cg.on)
     long long E;
     double cell, lon_min, lat_min, r_earth;
     int nx, ny, wrap, far_rows, K, exact, dl_M;

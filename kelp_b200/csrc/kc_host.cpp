@@ -66,6 +66,25 @@ void mesh_tables(long long N, long long E, int max_v, const double* lat, const i
     }
 }
 
+void cgrid_edge_lengths(long long E, const int* corners, const double* lon, const double* lat, double* out) {
+    const double deg2rad = 0.017453292519943295, M = 111120.0;
+    for (long long e = 0; e < E; ++e) {
+        for (int k = 0; k < 4; ++k) {
+            const int na = corners[4 * e + k], nb = corners[4 * e + (k + 1) % 4];
+            // ((dlon + 180) % 360) - 180 with Python's float remainder
+            double r = std::fmod(lon[nb] - lon[na] + 180.0, 360.0);
+            if (r != 0.0) {
+                if (r < 0.0) r += 360.0;
+            } else {
+                r = 0.0;
+            }
+            const double dl = r - 180.0;
+            const double cm = std::cos(0.5 * (lat[na] + lat[nb]) * deg2rad);
+            out[4 * e + k] = std::hypot(dl * cm * M, (lat[nb] - lat[na]) * M);
+        }
+    }
+}
+
 }  // namespace kc_host
 
 extern "C" int kc_node_xyz_fill(const double* lon, const double* lat, long long n, double* out) {

@@ -3,6 +3,7 @@
 #pragma once
 #include "kc_beach.cuh"
 #include "kc_sigma.cuh"
+#include "kc_cgrid.cuh"
 
 #ifndef KC_BLOCK
 #define KC_BLOCK 128   // threads per block of every kernel (a build option)
@@ -78,6 +79,41 @@ void launch_sigma_kernel(const kc::DMesh& m, const kc::DBlend<T>& f, const kc::D
         if (scheme == 0) k_step3d_sigma<T, 0, false><<<g, kBlock, 0, stream>>>(m, f, st, s);
         else if (scheme == 1) k_step3d_sigma<T, 1, false><<<g, kBlock, 0, stream>>>(m, f, st, s);
         else k_step3d_sigma<T, 2, false><<<g, kBlock, 0, stream>>>(m, f, st, s);
+    }
+}
+
+template <typename T, int SCHEME>
+__global__ void __launch_bounds__(kBlock, KC_STEP_MIN_BLOCKS) k_step3d_cgrid(const __grid_constant__ kc::DMesh m,
+                                                                         const __grid_constant__ kc::DBlend<T> f,
+                                                                         const __grid_constant__ kc::DState st,
+                                                                         const __grid_constant__ kc::DStep s) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= st.P) return;
+    activate(st, s, i);
+    if (st.prev) st.prev[i] = st.status[i];
+    kc::step3d_cgrid_particle<T, SCHEME>(m, f, st, s, i);
+}
+
+// One step on a NEMO C-grid mesh (plain form): the 2-D steps read the
+// surface faces through CgridForm (edge walk when the state carries
+// elements); the 3-D step is the fractional-level one (elements untouched).
+template <typename T>
+void launch_cgrid_kernel(const kc::DMesh& m, const kc::DBlend<T>& f, const kc::DState& st, const kc::DStep& s,
+                         int dims, int scheme, cudaStream_t stream) {
+    const unsigned g = (unsigned)((st.P + kBlock - 1) / kBlock);
+    using F = kc::CgridForm<T>;
+    if (dims == 3) {
+        if (scheme == 0) k_step3d_cgrid<T, 0><<<g, kBlock, 0, stream>>>(m, f, st, s);
+        else if (scheme == 1) k_step3d_cgrid<T, 1><<<g, kBlock, 0, stream>>>(m, f, st, s);
+        else k_step3d_cgrid<T, 2><<<g, kBlock, 0, stream>>>(m, f, st, s);
+    } else if (st.elem) {
+        if (scheme == 0) k_step2d<T, 0, F, true><<<g, kBlock, 0, stream>>>(m, f, st, s);
+        else if (scheme == 1) k_step2d<T, 1, F, true><<<g, kBlock, 0, stream>>>(m, f, st, s);
+        else k_step2d<T, 2, F, true><<<g, kBlock, 0, stream>>>(m, f, st, s);
+    } else {
+        if (scheme == 0) k_step2d<T, 0, F, false><<<g, kBlock, 0, stream>>>(m, f, st, s);
+        else if (scheme == 1) k_step2d<T, 1, F, false><<<g, kBlock, 0, stream>>>(m, f, st, s);
+        else k_step2d<T, 2, F, false><<<g, kBlock, 0, stream>>>(m, f, st, s);
     }
 }
 

@@ -121,7 +121,10 @@ class DeviceContext:
         keep: list = []
         d = mesh_desc(mesh, keep)
         self._chk(N.lib().kc_mesh_upload(self._ctx, C.byref(d)), "kc_mesh_upload")
-        self._sigma = getattr(mesh, "vertical_coord", "zlevel") == "sigma"
+        self._cg_nynx = None
+        if getattr(mesh, "_nemo_cgrid", False):
+            self._upload_cgrid(mesh)
+        self._sigma = getattr(mesh, "vertical_coord", "zlevel") == "sigma" and not getattr(mesh, "_nemo_cgrid", False)
         if self._sigma:
             sg = _c(mesh.sigma, np.float64)
             self._chk(N.lib().kc_sigma_upload(self._ctx, int(sg.size), N.ptr(sg)), "kc_sigma_upload")
@@ -131,6 +134,28 @@ class DeviceContext:
         self._dl_key = None
         self._coastal_key = None
         self._enb_key = None
+
+    def _upload_cgrid(self, mesh) -> None:
+        """The NEMO C-grid tables of a build_nemo_cgrid_mesh mesh (kc_cgrid_upload)."""
+        g = lambda name, t: _c(np.asarray(getattr(mesh, "_nemo_cgrid_" + name)).reshape(-1), t)
+        ny, nx = (int(x) for x in mesh._structured_shape)
+        zw = g("zw", np.float64)
+        K = max(int(zw.size) - 1, 0)
+        keep = {"corners": g("corners", np.int32), "ji": g("elem_ji", np.int64), "nlev": g("nlev", np.int32),
+                "nlev_r": g("nlev_raster", np.int32), "e2u": g("e2u", np.float64), "e1v": g("e1v", np.float64),
+                "area": g("area", np.float64), "zw": zw, "e3b": g("e3b", np.float64), "kbu": g("kbu", np.int32),
+                "e3u": g("e3u", np.float64), "kbv": g("kbv", np.int32), "e3v": g("e3v", np.float64)}
+        d = N.CgridDesc()
+        d.ny, d.nx, d.K = ny, nx, K
+        d.partial_shrunk = int(getattr(mesh, "_nemo_cgrid_partial", "shrunk") == "shrunk")
+        d.corners, d.elem_ji, d.nlev, d.nlev_raster = (N.ptr(keep[k]) for k in ("corners", "ji", "nlev", "nlev_r"))
+        if keep["e2u"].size:
+            d.e2u, d.e1v = N.ptr(keep["e2u"]), N.ptr(keep["e1v"])
+        if K > 0:
+            d.area, d.zw, d.e3b = N.ptr(keep["area"]), N.ptr(zw), N.ptr(keep["e3b"])
+            d.kbu, d.e3u, d.kbv, d.e3v = (N.ptr(keep[k]) for k in ("kbu", "e3u", "kbv", "e3v"))
+        self._chk(N.lib().kc_cgrid_upload(self._ctx, C.byref(d)), "kc_cgrid_upload")
+        self._cg_nynx = ny * nx
 
     def ensure_elem_neighbors(self, mesh) -> None:
         """Upload the edge-neighbour table of the resident mesh (built by
@@ -170,6 +195,12 @@ class DeviceContext:
         u = np.asarray(field.u)
         v = np.asarray(field.v)
         w = None if getattr(field, "w", None) is None else np.asarray(field.w)
+        if getattr(field, "uv_layout", None) == "nemo_cgrid" and getattr(self, "_cg_nynx", None):
+            # face rasters: one row per level of ny * nx values
+            nynx = self._cg_nynx
+            u = u.reshape(-1, nynx) if u.ndim > 1 or u.size != nynx else u
+            v = v.reshape(-1, nynx) if v.ndim > 1 or v.size != nynx else v
+            w = None if w is None else w.reshape(-1, nynx)
         if dtype is None:
             dtype = np.float32 if (u.dtype == np.float32 and v.dtype == np.float32
                                    and (w is None or w.dtype == np.float32)) else np.float64

@@ -120,7 +120,7 @@ def _az_args(diffusion, vel, is3d, mesh):
     return (az_field is not None, az_const)
 
 
-def _check_call(dt, time_dir, kw):
+def _check_call(dt, time_dir, kw, vel=None):
     if float(dt) <= 0:
         raise ValueError(f"dt must be > 0, got {dt!r}")
     if float(time_dir) not in (1.0, -1.0):
@@ -130,9 +130,58 @@ def _check_call(dt, time_dir, kw):
             and getattr(diffusion, "scheme", "uniform") in ("em", "m1")):
         # integrators.py:824-839: checked before anything else
         raise ValueError("diffusion.az_enabled composes with scheme='uniform' only")
-    if kw.get("uv_interp", "leastsq") == "nemo_cgrid":
-        raise NotImplementedError("the NEMO C-grid step is not built on the CUDA backend")
+    if kw.get("uv_interp", "leastsq") == "nemo_cgrid" and vel is not None and _is_3d(vel):
+        # nemo_cgrid.py:457-461: the 3-D C-grid step takes neither
+        if diffusion is not None or kw.get("recon") is not None:
+            raise NotImplementedError("the 3-D C-grid step supports neither diffusion nor temporal "
+                                      "(PCHIP) reconstruction")
     return _kick_args(diffusion)
+
+
+def _prepare_cgrid(vel, mesh, dt, time_dir, scheme, kw, ctx, kick):
+    """prepare_step for uv_interp "nemo_cgrid" on a build_nemo_cgrid_mesh mesh:
+    face-raster snapshots; 2-D steps read the surface faces
+    (nemo_cgrid.py:355-388), 3-D steps are nemo_cgrid3d_step (:416-512)."""
+    code, c_coeffs = _SCHEMES[scheme]
+    if not getattr(mesh, "_nemo_cgrid", False):
+        raise ValueError("uv_interp 'nemo_cgrid' needs a C-grid mesh (NEMO reader with mesh.nemo_grid: cgrid)")
+    if kw.get("recon") is not None:
+        raise NotImplementedError("PCHIP temporal reconstruction is not built on the CUDA backend")
+    if not (mesh.metadata or {}).get("exact_nearest", False):
+        raise NotImplementedError("the CUDA backend anchors with the exact nearest-node search only "
+                                  "(mesh.exact_nearest: true, the configuration default)")
+    if kw.get("cuda_precision", "plain") != "plain" or kw.get("cuda_snapshots") not in (None, "f32"):
+        raise NotImplementedError("C-grid meshes step in the plain form with float32 or float64 rasters")
+    vel_next = kw.get("vel_next", None)
+    dt_to_next = kw.get("dt_to_next", None)
+    _validate_time_aware(vel_next, dt_to_next, dt)
+    vel_a, vel_b, target, alpha0 = _fields(vel, vel_next)
+    for f in (vel_a, vel_b, target):
+        if getattr(f, "uv_layout", "element") != "nemo_cgrid":
+            raise ValueError(f"uv_interp 'nemo_cgrid' needs uv_layout='nemo_cgrid', got {f.uv_layout!r}")
+    is3d = _is_3d(vel)
+    ctx = ctx or default_context()
+    ctx.ensure_mesh(mesh)
+    sa, sb, st = ctx.slots_for([vel_a, vel_b, target], np.float32 if kw.get("cuda_snapshots") == "f32" else None)
+    a = N.StepArgs()
+    a.scheme = code
+    a.dims = 3 if is3d else 2
+    a.slot_a, a.slot_b, a.slot_t = sa, sb, st
+    a.alpha0 = alpha0
+    if vel_next is not None:
+        # _make_stage_vels at the stage fractions (the C-grid 3-D step's
+        # Butcher nodes are the same (0, .5, .5, 1) / (0, .5) / (0,))
+        for k, c in enumerate(c_coeffs):
+            a.alpha_k[k] = float(c) * float(dt) / float(dt_to_next)
+    a.dt = float(dt)
+    a.time_dir = float(time_dir)
+    if kick is not None:
+        a.kick = 1
+        a.kh_x, a.kh_y, a.seed, a.real_id, a.step_i, a.pid_offset = kick
+    a.global_step = -1
+    a.precision = N.KC_PLAIN
+    a.Dmin, a.z0b_min = 0.5, 0.1
+    return a, is3d
 
 
 def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=None):
@@ -143,6 +192,12 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
     for combinations the CUDA backend does not build."""
     code, c_coeffs = _SCHEMES[scheme]
     uv_interp = kw.get("uv_interp", "leastsq")
+    if uv_interp == "nemo_cgrid":
+        if elem is not None and _is_3d(vel):
+            elem = None   # the 3-D C-grid step neither reads nor updates carried elements
+        if elem is not None:
+            (ctx or default_context()).ensure_elem_neighbors(mesh)
+        return _prepare_cgrid(vel, mesh, dt, time_dir, scheme, kw, ctx, kick)
     if uv_interp != "barycentric":
         raise NotImplementedError(f"uv_interp={uv_interp!r} is not built on the CUDA backend; "
                                   "use 'barycentric' (node-layout velocities)")
@@ -244,7 +299,7 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
 
 
 def _run(state, vel, mesh, dt, time_dir, scheme, kw, ctx=None) -> ParticleState:
-    kick = _check_call(dt, time_dir, kw)
+    kick = _check_call(dt, time_dir, kw, vel)
     if not np.any(state.alive_mask):
         return _zero_dead_velocity(state)
     a, is3d = prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx, kick=kick, elem=state.elem)
@@ -261,8 +316,10 @@ def _run(state, vel, mesh, dt, time_dir, scheme, kw, ctx=None) -> ParticleState:
            "status": np.empty(P, np.int32), "nearest_node": np.empty(P, np.int32),
            "failure_reason": None if fr_in is None else np.empty(P, np.int8),
            "u": np.empty(P), "v": np.empty(P), "w": np.empty(P) if is3d else None}
-    walk = state.elem is not None
-    if walk:   # elem_search: walk (integrators.py:5415-5416): carried elements in and out
+    # elem_search: walk (integrators.py:5415-5416): carried elements in and
+    # out (the 3-D C-grid step leaves them untouched, nemo_cgrid.py:416-512)
+    walk = state.elem is not None and not (kw.get("uv_interp") == "nemo_cgrid" and is3d)
+    if walk:
         inp["elem"] = np.ascontiguousarray(state.elem, dtype=np.int32)
         out["elem"] = np.empty(P, np.int32)
     # one call: chunked upload, step and download overlapped on the device

@@ -13,7 +13,7 @@ import pytest
 from kelp_b200 import integrators as KI
 from kelp_b200.diffusion import DiffusionStepArgs
 
-from test_oracle_golden import SIGMA_CASES, diffusion_args
+from test_oracle_golden import CGRID_CASES, SIGMA_CASES, diffusion_args
 
 pytestmark = pytest.mark.gpu
 
@@ -33,6 +33,7 @@ WALK_CASES = [("golden_band", c) for c in ("rk2_walk", "rk4_walk_kick", "euler_w
 WALK_CASES += [("golden_3d", c) for c in ("rk2_wbary_walk", "rk4_wnear_walk_kick")]
 CASES += WALK_CASES
 CASES += SIGMA_CASES
+CASES += CGRID_CASES
 
 
 def replay_cuda(g, cname):
@@ -48,7 +49,8 @@ def replay_cuda(g, cname):
     for k in range(int(n_steps)):
         vel, vnext, dtn = g.payload(c["schedule"][k], T)
         diff = diffusion_args(c, k)
-        st = fn(st, vel, g.mesh, dt, td, uv_interp="barycentric", w_interp=w_interp, vel_next=vnext,
+        uv = "nemo_cgrid" if getattr(g.mesh, "_nemo_cgrid", False) else "barycentric"
+        st = fn(st, vel, g.mesh, dt, td, uv_interp=uv, w_interp=w_interp, vel_next=vnext,
                 dt_to_next=dtn, diffusion=diff)
         if f"s{k + 1}_lon" in c:
             snaps[k + 1] = st
