@@ -63,6 +63,10 @@ typedef struct {
     int64_t n;
     const void *aza, *azb;   /* vertical diffusivity (K, N) of the bracket pair, or NULL */
     const double *etaa, *etab, *etat;   /* free surface (N) of the pair and target (sigma meshes) */
+    int pchip;                          /* 1: a, b, t, d are a PCHIP stencil at times pt; alphas are times */
+    const void *ud, *vd, *wd;
+    const double* etad;
+    double pt[4];
 } OField;
 
 static double fld(const void* p, int f32, int64_t i) {
@@ -542,6 +546,35 @@ static double tblend(double a, double b, double t, double alpha0, double alpha) 
     return (1.0 - alpha) * a0 + alpha * t;
 }
 
+/* temporal_reconstruct.py:167-180 _fc_slope_scalar */
+static double fc_slope(double dp, double dn, double hp, double hn) {
+    if (dp * dn > 0.0) {
+        double w1 = 2.0 * hn + hp, w2 = hn + 2.0 * hp;
+        return (w1 + w2) / (w1 / dp + w2 / dn);
+    }
+    return 0.0;
+}
+
+/* temporal_reconstruct.py:183-215 _pchip_value_scalar: the monotone cubic
+ * at tq in [t1, t2] */
+static double pchip4(double f0, double f1, double f2, double f3, const double* t, double tq) {
+    double h0 = t[1] - t[0], h1 = t[2] - t[1], h2 = t[3] - t[2];
+    double d0 = (f1 - f0) / h0, d1 = (f2 - f1) / h1, d2 = (f3 - f2) / h2;
+    double m1 = fc_slope(d0, d1, h0, h1), m2 = fc_slope(d1, d2, h1, h2);
+    double s = (tq - t[1]) / h1, s2 = s * s, s3 = s2 * s;
+    double h00 = 2.0 * s3 - 3.0 * s2 + 1.0, h10 = s3 - 2.0 * s2 + s, h01 = -2.0 * s3 + 3.0 * s2, h11 = s3 - s2;
+    return h00 * f1 + h10 * h1 * m1 + h01 * f2 + h11 * h1 * m2;
+}
+
+/* the stage value of one field entry: the linear bracket blend, or the
+ * PCHIP stencil at time `alpha` (make_stage_vels_recon) */
+static double blend4(const OField* f, const void* a, const void* b, const void* t, const void* d, int64_t idx,
+                     double alpha) {
+    if (f->pchip) return pchip4(fld(a, f->f32, idx), fld(b, f->f32, idx), fld(t, f->f32, idx), fld(d, f->f32, idx),
+                                f->pt, alpha);
+    return tblend(fld(a, f->f32, idx), fld(b, f->f32, idx), fld(t, f->f32, idx), f->alpha0, alpha);
+}
+
 /* interpolate.py:1340-1529 (row 0: 2-D; row = layer: 3-D) */
 /* The walk's pre-validated containing element for the next interpolation of
  * this thread (-1: search from the anchor), as interpolate.py:1246-1270
@@ -580,8 +613,8 @@ static int interp_uv(const OMesh* m, const OField* f, double xp, double yp, int 
     double Us = 0.0, Vs = 0.0;
     for (int k = 0; k < nv; ++k) {
         int64_t idx = (int64_t)row * f->n + verts[k];
-        double un = tblend(fld(f->ua, f->f32, idx), fld(f->ub, f->f32, idx), fld(f->ut, f->f32, idx), f->alpha0, alpha);
-        double vn = tblend(fld(f->va, f->f32, idx), fld(f->vb, f->f32, idx), fld(f->vt, f->f32, idx), f->alpha0, alpha);
+        double un = blend4(f, f->ua, f->ub, f->ut, f->ud, idx, alpha);
+        double vn = blend4(f, f->va, f->vb, f->vt, f->vd, idx, alpha);
         Us += w[k] * un;
         Vs += w[k] * vn;
     }
@@ -607,7 +640,7 @@ static int find_layer(const OMesh* m, double z, double bottom) {
 
 static double wat(const OField* f, int k, int node, double alpha) {
     int64_t idx = (int64_t)k * f->n + node;
-    return tblend(fld(f->wa, f->f32, idx), fld(f->wb, f->f32, idx), fld(f->wt, f->f32, idx), f->alpha0, alpha);
+    return blend4(f, f->wa, f->wb, f->wt, f->wd, idx, alpha);
 }
 
 /* vertical.py:1064-1098 */
@@ -765,8 +798,8 @@ static void uv_bracket(const double* p, int li, double z, int* k, double* alpha)
 /* interpolate.py:1847-1876 _tinterp_point_uv */
 static void point_uv(const OField* f, int k, int nd, double alpha, double* u, double* v) {
     int64_t idx = (int64_t)k * f->n + nd;
-    *u = tblend(fld(f->ua, f->f32, idx), fld(f->ub, f->f32, idx), fld(f->ut, f->f32, idx), f->alpha0, alpha);
-    *v = tblend(fld(f->va, f->f32, idx), fld(f->vb, f->f32, idx), fld(f->vt, f->f32, idx), f->alpha0, alpha);
+    *u = blend4(f, f->ua, f->ub, f->ut, f->ud, idx, alpha);
+    *v = blend4(f, f->va, f->vb, f->vt, f->vd, idx, alpha);
 }
 
 /* interpolate.py:1879-1971 _interp_barycentric_core_tinterp_dl with
@@ -1298,6 +1331,7 @@ static int uv2(const OMesh* m, const OField* f, double xp, double yp, int nn, do
 /* the stage's free surface at a node: the payload's eta blended like u/v
  * (io.py:68-117 _blend in float64, the stage lerps of _make_stage_vels) */
 static double eta_at(const OField* f, int node, double alpha) {
+    if (f->pchip) return pchip4(f->etaa[node], f->etab[node], f->etat[node], f->etad[node], f->pt, alpha);
     return tblend(f->etaa[node], f->etab[node], f->etat[node], f->alpha0, alpha);
 }
 
@@ -1847,6 +1881,10 @@ typedef struct {
     int64_t n;
     const void *aza, *azb;
     const double *etaa, *etab, *etat;
+    int pchip;
+    const void *ud, *vd, *wd;
+    const double* etad;
+    double pt[4];
 } orc_field;
 
 typedef struct {

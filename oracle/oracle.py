@@ -43,7 +43,9 @@ class OField(C.Structure):
                 ("ut", C.c_void_p), ("vt", C.c_void_p), ("wt", C.c_void_p),
                 ("f32", C.c_int), ("alpha0", C.c_double), ("n", C.c_int64),
                 ("aza", C.c_void_p), ("azb", C.c_void_p),
-                ("etaa", C.c_void_p), ("etab", C.c_void_p), ("etat", C.c_void_p)]
+                ("etaa", C.c_void_p), ("etab", C.c_void_p), ("etat", C.c_void_p),
+                ("pchip", C.c_int), ("ud", C.c_void_p), ("vd", C.c_void_p), ("wd", C.c_void_p),
+                ("etad", C.c_void_p), ("pt", C.c_double * 4)]
 
 
 class OStep(C.Structure):
@@ -196,30 +198,43 @@ def _field_arrays(f, dtype):
 
 
 def step(state, vel, mesh, dt, time_dir, scheme: str, *, vel_next=None, dt_to_next=None, w_interp="nearest",
-         diffusion=None, pid=None, release_step=None, global_step=-1, view=None, Dmin=0.5, z0b_min=0.1):
+         diffusion=None, pid=None, release_step=None, global_step=-1, view=None, Dmin=0.5, z0b_min=0.1,
+         recon=None):
     """One step of every particle; returns a dict of new arrays
     (lon, lat, z, status, nearest_node, failure_reason, u, v, w, and elem
     when the state carries elements: elem_search walk, the mesh's
-    ``_elem_neighbors`` table required)."""
+    ``_elem_neighbors`` table required).  ``recon`` = (4 snapshots, their
+    times, the step's time, direction) reconstructs the RK stages by PCHIP
+    (temporal_reconstruct.py:298-325; Euler ignores it)."""
     view = view or MeshView(mesh)
     vel_a = getattr(vel, "vel_a", vel)
     vel_b = getattr(vel, "vel_b", vel_next if vel_next is not None else vel_a)
     alpha0 = float(getattr(vel, "alpha", 0.0))
     target = vel_next if vel_next is not None else vel_a
     flds = [vel_a, vel_b, target]
+    use_recon = recon is not None and scheme != "euler"
+    if use_recon:
+        flds = list(recon[0])
     all32 = all(np.asarray(f.u).dtype == np.float32 and np.asarray(f.v).dtype == np.float32
                 and (f.w is None or np.asarray(f.w).dtype == np.float32)
                 and (getattr(f, "az", None) is None or np.asarray(f.az).dtype == np.float32) for f in flds)
     dtype = np.float32 if all32 else np.float64
     arrs = [_field_arrays(f, dtype) for f in flds]
     of = OField()
-    (of.ua, of.va, of.wa), (of.ub, of.vb, of.wb), (of.ut, of.vt, of.wt) = [tuple(_p(x) for x in a) for a in arrs]
+    (of.ua, of.va, of.wa), (of.ub, of.vb, of.wb), (of.ut, of.vt, of.wt) = [tuple(_p(x) for x in a) for a in arrs[:3]]
+    if use_recon:
+        of.pchip = 1
+        of.ud, of.vd, of.wd = (_p(x) for x in arrs[3])
+        for k in range(4):
+            of.pt[k] = float(recon[1][k])
     of.f32 = 1 if all32 else 0
     of.alpha0 = alpha0
     of.n = view.lon.size
     etas = [np.ascontiguousarray(getattr(f, "eta", None) if getattr(f, "eta", None) is not None
                                  else np.zeros(view.lon.size), dtype=np.float64) for f in flds]
-    of.etaa, of.etab, of.etat = (_p(e) for e in etas)
+    of.etaa, of.etab, of.etat = (_p(e) for e in etas[:3])
+    if use_recon:
+        of.etad = _p(etas[3])
     is3d = arrs[0][2] is not None
     placement = getattr(vel_a, "uv_vertical", "layer")
     if is3d and placement != "layer":
@@ -230,12 +245,18 @@ def step(state, vel, mesh, dt, time_dir, scheme: str, *, vel_next=None, dt_to_ne
     os_.w_code = 0 if w_interp == "nearest" else 1
     os_.uv_dl = 1 if (is3d and placement != "layer") else 0
     cc = {"euler": (0.0,), "rk2": (0.0, 0.5), "rk4": (0.0, 0.5, 0.5, 1.0)}[scheme]
-    if vel_next is not None and scheme != "euler":
+    if use_recon:   # the stage times sim_time + time_dir * c * dt
+        q, d = float(recon[2]), float(recon[3])
+        for k, c in enumerate(cc):
+            os_.ak[k] = q + d * c * float(dt)
+    elif vel_next is not None and scheme != "euler":
         for k, c in enumerate(cc):
             os_.ak[k] = float(c) * float(dt) / float(dt_to_next)
     os_.dt, os_.td = float(dt), float(time_dir)
     os_.Dmin, os_.z0b_min = float(Dmin), float(z0b_min)
-    if vel_next is not None:   # the end-of-step surface (integrators.py:1400-1420 _sigma_end_eta)
+    if use_recon:   # the end-of-step surface: the reconstruction at c = 1 (integrators.py:1369-1391)
+        os_.alpha_end = float(recon[2]) + float(recon[3]) * 1.0 * float(dt)
+    elif vel_next is not None:   # the end-of-step surface (integrators.py:1400-1420 _sigma_end_eta)
         os_.alpha_end = float(dt) / float(dt_to_next)
     if diffusion is not None:
         os_.seed, os_.real_id, os_.step_i = int(diffusion.seed), int(diffusion.real_id), int(diffusion.step_i)

@@ -83,7 +83,7 @@ def payload(fields, t, T):
 
 def run_case(rm, fields, lon, lat, z, status, scheme, dt, T, n_steps, *, time_dir=1.0, w_interp="nearest",
              kh=None, seed=7, real_id=0, pid_offset=0, record=(1,), az=None, walk=False, steady=False,
-             uv_interp="barycentric"):
+             uv_interp="barycentric", pchip=False, t0=0.0):
     fn = {"rk2": RI.rk2_step, "rk4": RI.rk4_step, "euler": RI.euler_step}[scheme]
     P = lon.size
     st = RState(lon=lon.copy(), lat=lat.copy(), z=z.copy(), status=status.copy(),
@@ -97,7 +97,7 @@ def run_case(rm, fields, lon, lat, z, status, scheme, dt, T, n_steps, *, time_di
         out["elem0"] = np.asarray(st.elem).copy()
     sched = []
     for k in range(n_steps):
-        t = k * dt
+        t = t0 + k * dt
         vel, vnext, dtn, ia, alpha = payload(fields, t, T)
         if steady:   # no time-aware payload: every stage reads the first record
             vel, vnext, dtn, ia, alpha = fields[0], None, -1.0, 0, 0.0
@@ -106,7 +106,13 @@ def run_case(rm, fields, lon, lat, z, status, scheme, dt, T, n_steps, *, time_di
         if kh is not None:
             kw["diffusion"] = RDiff(scheme="uniform", kh_x=kh[0], kh_y=kh[1], seed=seed, real_id=real_id,
                                     step_i=k, pid_offset=pid_offset, **(az or {}))
-        sched.append([ia, alpha, dtn])
+        has_recon = 0
+        if pchip and scheme != "euler" and abs(alpha) >= 1e-12 and 1 <= ia and ia + 2 < len(fields):
+            # tracking._resolve_recon_stencil: (ia-1, ia, ia+1, ia+2) around the bracket
+            idx = (ia - 1, ia, ia + 1, ia + 2)
+            kw["recon"] = ([fields[i] for i in idx], [float(i * T) for i in idx], t, float(time_dir))
+            has_recon = 1
+        sched.append([ia, alpha, dtn, has_recon, t])
         st = fn(st, vel, rm, dt, time_dir, **kw)
         if (k + 1) in record or k + 1 == n_steps:
             tag = f"s{k + 1}"
@@ -526,6 +532,61 @@ def cgrid_fixture():
         save(f"golden_{tag}", rec, rf, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
 
 
+def pchip_fixture():
+    """Monotone-cubic (PCHIP) temporal reconstruction over a 4-snapshot
+    stencil (numerics/temporal_reconstruct.py; the tracking layer's bundle,
+    tracking.py:2415-2436): 2-D band, 3-D z-level (the fused RK2 PCHIP
+    kernel and the unfused RK4), a sigma mesh.  Steps start one record in, so
+    the stencil exists; the last interval falls back to the linear blend."""
+    T = 86400.0
+    m = S.lattice_mesh(3.0, 72.0, jitter=0.2, land_frac=0.3)
+    rm = ref_mesh(m)
+    snaps = S.gyre_snapshots(m, 6, amp=1.5)
+    for k, sn in enumerate(snaps):   # an uneven record sequence: the cubic differs from the lerp
+        sn.u = (sn.u * (1.0 + 0.6 * np.sin(1.3 * k))).astype(np.float32)
+        sn.v = (sn.v * (1.0 - 0.4 * np.cos(0.9 * k))).astype(np.float32)
+    rf = ref_fields(snaps)
+    lon, lat, z, status = particles(m, 1200, 51, n_off=40, n_dead=20)
+    cases = {"rk2": run_case(rm, rf, lon, lat, z, status, "rk2", 21600.0, T, 14, pchip=True, t0=T),
+             "rk4_kick": run_case(rm, rf, lon, lat, z, status, "rk4", 21600.0, T, 14, pchip=True, t0=T,
+                                  kh=(5.0e4, 5.0e4), seed=21)}
+    save("golden_pchip2d", mesh_record(rm), snaps, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
+
+    zl = S.stretched_levels(12, 5.0, 4000.0)
+    m = S.lattice_mesh(3.0, 60.0, jitter=0.2, land_frac=0.25,
+                       depth=lambda lo, la: S.smooth_bathymetry(lo, la, 30.0, 4000.0), sigma=zl)
+    rm = ref_mesh(m, sigma=zl)
+    snaps = S.gyre_snapshots(m, 6, amp=1.5, z_levels=zl, decay=800.0, w_scale=2e-3)
+    for k, sn in enumerate(snaps):
+        f = 1.0 + 0.5 * np.sin(1.1 * k)
+        sn.u, sn.v, sn.w = ((x * f).astype(np.float32) for x in (sn.u, sn.v, sn.w))
+    rf = ref_fields(snaps)
+    lon, lat, z, status = particles(m, 1200, 52, z=True, n_dead=20)
+    cases = {"rk2_wbary": run_case(rm, rf, lon, lat, z, status, "rk2", 21600.0, T, 14, w_interp="barycentric",
+                                   pchip=True, t0=T),
+             "rk4_wnear": run_case(rm, rf, lon, lat, z, status, "rk4", 21600.0, T, 14, w_interp="nearest",
+                                   pchip=True, t0=T)}
+    save("golden_pchip3d", mesh_record(rm), snaps, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
+
+    sig = np.array([1.0, 0.95, 0.88, 0.8, 0.7, 0.58, 0.45, 0.32, 0.2, 0.1, 0.0])
+    m = S.lattice_mesh(1.0, 15.0, lon_min=-20.0, lon_max=20.0, jitter=0.15, land_frac=0.2, quad_frac=0.3,
+                       depth=lambda lo, la: S.smooth_bathymetry(lo, la, 0.2, 120.0), sigma=sig)
+    rm = ref_mesh(m, sigma=sig)
+    rm.vertical_coord = "sigma"
+    lon_n, lat_n = np.radians(np.asarray(m.nodes_lon)), np.radians(np.asarray(m.nodes_lat))
+    Ts = 21600.0
+    snaps = S.gyre_snapshots(m, 6, amp=1.0, z_levels=(1.0 - sig) * 100.0, decay=60.0, w_scale=4e-4)
+    for k, sn in enumerate(snaps):
+        sn.eta = (0.6 * np.sin(2.0 * lon_n + 0.9 * k) * np.cos(3.0 * lat_n) - 0.15).astype(np.float32)
+    rf = ref_fields(snaps)
+    lon, lat, z, status = particles(m, 1000, 53, z=True, n_dead=20)
+    cases = {"rk4_wbary": run_case(rm, rf, lon, lat, z, status, "rk4", 3600.0, Ts, 16, w_interp="barycentric",
+                                   pchip=True, t0=Ts),
+             "rk2_wnear": run_case(rm, rf, lon, lat, z, status, "rk2", 3600.0, Ts, 16, w_interp="nearest",
+                                   pchip=True, t0=Ts)}
+    save("golden_pchip_sigma", mesh_record(rm), snaps, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
+
+
 def time_fixture():
     """The reference's time-bracket resolution (tracking._resolve_time_bracket)
     on a grid of query times, record axes, modes and directions."""
@@ -549,7 +610,7 @@ def time_fixture():
 
 if __name__ == "__main__":
     # no argument: every fixture; otherwise the named ones ("steps", "beach")
-    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid"}
+    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip"}
     if "steps" in which:
         main()
     if "beach" in which:
@@ -560,3 +621,5 @@ if __name__ == "__main__":
         sigma_fixture()
     if "cgrid" in which:
         cgrid_fixture()
+    if "pchip" in which:
+        pchip_fixture()

@@ -33,6 +33,22 @@ CASES += SIGMA_CASES
 CGRID_CASES = [("golden_cgrid2d", c) for c in ("rk2", "rk4", "euler", "rk2_bwd", "rk4_steady", "rk2_kick", "rk2_walk")]
 CGRID_CASES += [("golden_cgrid3d", c) for c in ("rk2", "rk4", "euler", "rk2_bwd", "rk4_steady")]
 CASES += CGRID_CASES
+# PCHIP temporal reconstruction (4-snapshot stencil; the last interval falls back to linear)
+PCHIP_CASES = [("golden_pchip2d", c) for c in ("rk2", "rk4_kick")]
+PCHIP_CASES += [("golden_pchip3d", c) for c in ("rk2_wbary", "rk4_wnear")]
+PCHIP_CASES += [("golden_pchip_sigma", c) for c in ("rk4_wbary", "rk2_wnear")]
+CASES += PCHIP_CASES
+
+
+def recon_of(g, c, k):
+    """The recorded step's PCHIP bundle (tracking.py:2415-2436), or None."""
+    row = c["schedule"][k]
+    if row.shape[0] < 5 or row[3] != 1:
+        return None
+    T, td = float(c["params"][1]), float(c["params"][3])
+    ia = int(row[0])
+    idx = (ia - 1, ia, ia + 1, ia + 2)
+    return ([g.snaps[i] for i in idx], [float(i * T) for i in idx], float(row[4]), td)
 
 
 def diffusion_args(c, k):
@@ -60,7 +76,7 @@ def replay_oracle(g, cname):
         vel, vnext, dtn = g.payload(c["schedule"][k], T)
         diff = diffusion_args(c, k)
         out = O.step(st, vel, g.mesh, dt, td, scheme, vel_next=vnext, dt_to_next=dtn, w_interp=w_interp,
-                     diffusion=diff, view=view)
+                     diffusion=diff, view=view, recon=recon_of(g, c, k))
         st = st.replace(lon=out["lon"], lat=out["lat"], z=out["z"], status=out["status"],
                         nearest_node=out["nearest_node"], failure_reason=out["failure_reason"],
                         u=out["u"], v=out["v"], w=out["w"], elem=out.get("elem"))
