@@ -42,7 +42,7 @@
 extern "C" {
 #endif
 
-#define KC_ABI_VERSION 6
+#define KC_ABI_VERSION 7
 
 #define KC_OK 0
 #define KC_ERR_ARG 1      /* invalid argument or combination */
@@ -110,6 +110,12 @@ typedef struct kc_step_args {
     double z0b_min;              /* sigma meshes: clearance above the bed (m, >= 0; default 0.1) */
     double alpha_end;            /* sigma meshes: blend fraction of the end-of-step surface,
                                     dt / dt_to_next (0 without a next snapshot) */
+    int pchip;                   /* 1: monotone-cubic (PCHIP) stages from the 4-record stencil
+                                    slot_a, slot_b, slot_t, slot_d at times pchip_t
+                                    (temporal_reconstruct.py:183-325); alpha_k are then the stage
+                                    times and alpha_end the end time; plain form, no Az */
+    int slot_d;
+    double pchip_t[4];
 } kc_step_args;
 
 /* Beaching / resuspension of one step (src/kelp/tracking.py:199-364,

@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libkelpcuda
 KC_OK, KC_ERR_ARG, KC_ERR_CUDA, KC_ERR_STATE, KC_ERR_DEVICE = 0, 1, 2, 3, 4
 KC_F32, KC_F64, KC_F16 = 0, 1, 2
 KC_PLAIN, KC_MIXED = 0, 1
-ABI_VERSION = 6
+ABI_VERSION = 7
 KC_EULER, KC_RK2, KC_RK4 = 0, 1, 2
 
 #: every symbol include/kelp_cuda.h declares
@@ -76,7 +76,8 @@ class StepArgs(C.Structure):
                 ("step_i", C.c_ulonglong), ("pid_offset", C.c_ulonglong),
                 ("global_step", C.c_longlong), ("precision", C.c_int),
                 ("az_kick", C.c_int), ("az_field", C.c_int), ("az_const", C.c_double),
-                ("Dmin", C.c_double), ("z0b_min", C.c_double), ("alpha_end", C.c_double)]
+                ("Dmin", C.c_double), ("z0b_min", C.c_double), ("alpha_end", C.c_double),
+                ("pchip", C.c_int), ("slot_d", C.c_int), ("pchip_t", C.c_double * 4)]
 
 
 class BeachArgs(C.Structure):

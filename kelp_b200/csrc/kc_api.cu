@@ -348,6 +348,9 @@ kc::DBlend<T> blend_of(kc_ctx* c, const kc_step_args* a) {
     f.t = field_of<T>(c->slots[a->slot_t]);
     f.alpha0 = a->alpha0;
     f.n = c->N;
+    f.pchip = a->pchip ? 1 : 0;
+    f.d = a->pchip ? field_of<T>(c->slots[a->slot_d]) : kc::DField<T>{};
+    for (int k = 0; k < 4; ++k) f.pt[k] = a->pchip ? a->pchip_t[k] : 0.0;
     return f;
 }
 
@@ -404,6 +407,21 @@ int check_step(kc_ctx* c, const kc_step_args* a) {
     if (a->kick && !(a->kh_x >= 0.0 && a->kh_y >= 0.0)) return fail(c, KC_ERR_ARG, "kc_step: Kh must be >= 0");
     if (a->precision != KC_PLAIN && a->precision != KC_MIXED)
         return fail(c, KC_ERR_ARG, "kc_step: precision must be KC_PLAIN or KC_MIXED");
+    if (a->pchip) {
+        if (a->precision != KC_PLAIN) return fail(c, KC_ERR_ARG, "kc_step: PCHIP stages run in the plain form");
+        if (a->az_kick) return fail(c, KC_ERR_ARG, "kc_step: the Az kick with PCHIP stages is not built");
+        if (c->dm.cg.on) return fail(c, KC_ERR_ARG, "kc_step: PCHIP stages on C-grid meshes are not built");
+        if (a->slot_d < 0 || a->slot_d >= kSlots) return fail(c, KC_ERR_ARG, "kc_step: slot out of range");
+        const Slot& d = c->slots[a->slot_d];
+        const Slot& s0 = c->slots[a->slot_a];
+        if (d.dtype < 0 || d.dtype != s0.dtype || d.n != s0.n || d.uv_rows != s0.uv_rows || d.w_rows != s0.w_rows)
+            return fail(c, KC_ERR_ARG, "kc_step: the fourth PCHIP record differs from the first in shape or type");
+        if (c->dm.sig && a->dims == 3 && !d.has_eta)
+            return fail(c, KC_ERR_STATE, "kc_step: sigma steps need eta in every snapshot slot (kc_field_upload_eta)");
+        const double* t = a->pchip_t;
+        if (!(t[0] < t[1] && t[1] < t[2] && t[2] < t[3]))
+            return fail(c, KC_ERR_ARG, "kc_step: PCHIP times must increase strictly");
+    }
     if (c->dm.cg.on) {
         if (a->precision != KC_PLAIN) return fail(c, KC_ERR_ARG, "kc_step: C-grid meshes step in the plain form");
         if (a->az_kick) return fail(c, KC_ERR_ARG, "kc_step: the Az kick on C-grid meshes is not built");
@@ -430,7 +448,7 @@ int check_step(kc_ctx* c, const kc_step_args* a) {
         if (a->az_kick) return fail(c, KC_ERR_ARG, "kc_step: the Az kick on sigma meshes is not built");
         if (!(a->Dmin > 0.0) || !(a->z0b_min >= 0.0))
             return fail(c, KC_ERR_ARG, "kc_step: sigma steps need Dmin > 0 and z0b_min >= 0");
-        if (!(a->alpha_end >= 0.0 && a->alpha_end <= 1.0 + 1e-9))
+        if (!a->pchip && !(a->alpha_end >= 0.0 && a->alpha_end <= 1.0 + 1e-9))
             return fail(c, KC_ERR_ARG, "kc_step: alpha_end must be in [0, 1]");
         const int sl3[3] = {a->slot_a, a->slot_b, a->slot_t};
         for (int k = 0; k < 3; ++k)

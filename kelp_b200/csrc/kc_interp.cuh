@@ -27,7 +27,42 @@ struct DBlend {
     DField<T> a, b, t;   // bracket pair and stage target
     double alpha0;       // bracket fraction of the step's start time
     long long n;         // row stride (nodes)
+    // PCHIP reconstruction (pchip = 1): a, b, t, d are the four-record
+    // stencil at times pt, and every stage "alpha" is the stage's time
+    DField<T> d;
+    double pt[4];
+    int pchip;
 };
+
+// temporal_reconstruct.py:167-180 _fc_slope_scalar: Fritsch-Carlson interior
+// slope, the weighted harmonic mean of the secants, 0 where they change sign
+__device__ __forceinline__ double fc_slope(double dp, double dn, double hp, double hn) {
+    if (dp * dn > 0.0) {
+        const double w1 = 2.0 * hn + hp, w2 = hn + 2.0 * hp;
+        return (w1 + w2) / (w1 / dp + w2 / dn);
+    }
+    return 0.0;
+}
+
+// temporal_reconstruct.py:183-215 _pchip_value_scalar: the monotone cubic
+// Hermite value at tq in the central interval [pt1, pt2]
+__device__ __forceinline__ double pchip4(double f0, double f1, double f2, double f3, const double* t, double tq) {
+    const double h0 = t[1] - t[0], h1 = t[2] - t[1], h2 = t[3] - t[2];
+    const double d0 = (f1 - f0) / h0, d1 = (f2 - f1) / h1, d2 = (f3 - f2) / h2;
+    const double m1 = fc_slope(d0, d1, h0, h1), m2 = fc_slope(d1, d2, h1, h2);
+    const double s = (tq - t[1]) / h1, s2 = s * s, s3 = s2 * s;
+    const double h00 = 2.0 * s3 - 3.0 * s2 + 1.0, h10 = s3 - 2.0 * s2 + s;
+    const double h01 = -2.0 * s3 + 3.0 * s2, h11 = s3 - s2;
+    return h00 * f1 + h10 * h1 * m1 + h01 * f2 + h11 * h1 * m2;
+}
+
+// The PCHIP stage value of entry idx of one field (pointers of the stencil)
+template <typename T>
+__device__ __forceinline__ double pchip_at(const T* p0, const T* p1, const T* p2, const T* p3, long long idx,
+                                          const double* t, double tq) {
+    return pchip4((double)__ldg(&p0[idx]), (double)__ldg(&p1[idx]), (double)__ldg(&p2[idx]), (double)__ldg(&p3[idx]),
+                  t, tq);
+}
 
 // Nested two-level time blend with the reference's endpoint shortcuts
 // (interpolate.py:1404-1436, vertical.py:1042-1061 _tblend_scalar).
@@ -126,7 +161,10 @@ __device__ __noinline__ bool interp_uv_at(const DMesh& m, const DBlend<T>& f, in
         if (k >= r.n) break;
         long long idx = base + r.v[k];
         double un, vn;
-        if (alpha < 1e-12) {
+        if (f.pchip) {
+            un = pchip_at(f.a.u, f.b.u, f.t.u, f.d.u, idx, f.pt, alpha);
+            vn = pchip_at(f.a.v, f.b.v, f.t.v, f.d.v, idx, f.pt, alpha);
+        } else if (alpha < 1e-12) {
             if (alpha0 == 0.0) {
                 un = (double)__ldg(&f.a.u[idx]);
                 vn = (double)__ldg(&f.a.v[idx]);
@@ -201,6 +239,11 @@ __device__ __forceinline__ void tinterp_point_uv(const DBlend<T>& f, int k, int 
                                                  double& v) {
     const long long idx = (long long)k * f.n + nd;
     const double alpha0 = f.alpha0;
+    if (f.pchip) {
+        u = pchip_at(f.a.u, f.b.u, f.t.u, f.d.u, idx, f.pt, alpha);
+        v = pchip_at(f.a.v, f.b.v, f.t.v, f.d.v, idx, f.pt, alpha);
+        return;
+    }
     if (alpha < 1e-12) {
         if (alpha0 == 0.0) {
             u = (double)__ldg(&f.a.u[idx]);
@@ -375,6 +418,7 @@ __device__ __forceinline__ double w_at(const DBlend<T>& f, double alpha, const W
     const long long n = f.n;
     auto at = [&](int k) {
         const long long idx = (long long)k * n + node;
+        if (f.pchip) return pchip_at(f.a.w, f.b.w, f.t.w, f.d.w, idx, f.pt, alpha);
         if (alpha < 1e-12) {
             const double a = (double)__ldg(&f.a.w[idx]);
             if (f.alpha0 == 0.0) return a;

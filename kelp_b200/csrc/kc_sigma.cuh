@@ -16,6 +16,9 @@ namespace kc {
 // u/v (io.py:68-117 _blend in float64; the stage lerps of _make_stage_vels).
 template <typename T>
 __device__ __forceinline__ double eta_at(const DBlend<T>& f, int node, double alpha) {
+    if (f.pchip)
+        return pchip4(__ldg(&f.a.eta[node]), __ldg(&f.b.eta[node]), __ldg(&f.t.eta[node]), __ldg(&f.d.eta[node]), f.pt,
+                      alpha);
     if (alpha < 1e-12) {
         const double a = __ldg(&f.a.eta[node]);
         if (f.alpha0 == 0.0) return a;

@@ -120,6 +120,34 @@ def _az_args(diffusion, vel, is3d, mesh):
     return (az_field is not None, az_const)
 
 
+def _check_recon(recon, dt, time_dir, c_coeffs):
+    """The PCHIP bundle (snapshots, times, sim_time, direction) validated as
+    reconstruct_pchip and the fused PCHIP runners do
+    (temporal_reconstruct.py:218-245, integrators.py:3444-3505); returns it
+    with float times."""
+    try:
+        snaps4, times4, q_time, direction = recon
+    except (TypeError, ValueError):
+        raise ValueError("recon must be (snapshots, times, sim_time, direction)") from None
+    if len(snaps4) != 4 or len(times4) != 4:
+        raise ValueError("reconstruct_pchip needs exactly 4 snapshots/times")
+    t = [float(x) for x in times4]
+    if not all(np.isfinite(x) for x in t):
+        raise ValueError(f"reconstruct_pchip: non-finite times {times4}")
+    if not (t[0] < t[1] < t[2] < t[3]):
+        raise ValueError(f"reconstruct_pchip: times must be strictly increasing, got {times4}")
+    d = float(direction)
+    if d != float(time_dir):
+        raise ValueError(f"recon direction {direction} disagrees with time_dir {time_dir}")
+    q = float(q_time)
+    tol = 1e-9 * (t[2] - t[1])
+    for c in c_coeffs:
+        tq = q + d * c * float(dt)
+        if not (t[1] - tol <= tq <= t[2] + tol):
+            raise ValueError(f"reconstruct_pchip: t_query={tq} outside the central interval [{t[1]}, {t[2]}]")
+    return list(snaps4), t, q, d
+
+
 def _check_call(dt, time_dir, kw, vel=None):
     if float(dt) <= 0:
         raise ValueError(f"dt must be > 0, got {dt!r}")
@@ -201,8 +229,11 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
     if uv_interp != "barycentric":
         raise NotImplementedError(f"uv_interp={uv_interp!r} is not built on the CUDA backend; "
                                   "use 'barycentric' (node-layout velocities)")
-    if kw.get("recon") is not None:
-        raise NotImplementedError("PCHIP temporal reconstruction is not built on the CUDA backend")
+    # PCHIP: the RK stages are reconstructed from the tracking layer's
+    # 4-record stencil; Euler evaluates the payload itself and ignores it
+    recon = kw.get("recon") if scheme != "euler" else None
+    if recon is not None:
+        recon = _check_recon(recon, dt, time_dir, c_coeffs)
     if not (mesh.metadata or {}).get("exact_nearest", False):
         raise NotImplementedError("the CUDA backend anchors with the exact nearest-node search only "
                                   "(mesh.exact_nearest: true, the configuration default)")
@@ -244,8 +275,11 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
             raise NotImplementedError("an endpoint LazyLerpField (alpha 0) takes the reference's unfused "
                                       "3-D RK2 path, which is not built on the CUDA backend")
     vel_a, vel_b, target, alpha0 = _fields(vel, vel_next)
-    _check_node_fields(mesh, [vel_a, vel_b, target], is3d, placement)
+    _check_node_fields(mesh, [vel_a, vel_b, target] + (list(recon[0]) if recon is not None else []), is3d,
+                       placement)
     form = kw.get("cuda_precision", "plain")
+    if recon is not None and form != "plain":
+        raise NotImplementedError("PCHIP reconstruction runs in the plain form (cuda_precision='plain')")
     if form not in ("plain", "mixed"):
         raise ValueError(f"cuda_precision must be 'plain' or 'mixed', got {form!r}")
     storage = kw.get("cuda_snapshots", None)
@@ -263,15 +297,26 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
         ctx.ensure_elem_neighbors(mesh)
     if is3d and placement != "layer":
         ctx.ensure_depth_points(mesh, placement)
-    sa, sb, st = ctx.slots_for([vel_a, vel_b, target], store)
     a = N.StepArgs()
+    if recon is None:
+        sa, sb, st = ctx.slots_for([vel_a, vel_b, target], store)
+        a.slot_a, a.slot_b, a.slot_t = sa, sb, st
+        a.alpha0 = alpha0
+        if vel_next is not None and code != N.KC_EULER:
+            for k, c in enumerate(c_coeffs):
+                a.alpha_k[k] = float(c) * float(dt) / float(dt_to_next)
+    else:
+        # the stencil in four slots; each stage "alpha" is its time
+        # sim_time + time_dir * c * dt (temporal_reconstruct.py:298-325)
+        snaps4, times4, q_time, direction = recon
+        a.slot_a, a.slot_b, a.slot_t, a.slot_d = ctx.slots_for(list(snaps4), store)
+        a.pchip = 1
+        for k in range(4):
+            a.pchip_t[k] = times4[k]
+        for k, c in enumerate(c_coeffs):
+            a.alpha_k[k] = q_time + direction * c * float(dt)
     a.scheme = code
     a.dims = 3 if is3d else 2
-    a.slot_a, a.slot_b, a.slot_t = sa, sb, st
-    a.alpha0 = alpha0
-    if vel_next is not None and code != N.KC_EULER:
-        for k, c in enumerate(c_coeffs):
-            a.alpha_k[k] = float(c) * float(dt) / float(dt_to_next)
     a.dt = float(dt)
     a.time_dir = float(time_dir)
     a.w_code = w_code
@@ -286,7 +331,11 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
     a.Dmin = float(kw.get("Dmin", 0.5))
     a.z0b_min = float(kw.get("z0b_min", 0.1))
     a.alpha_end = float(dt) / float(dt_to_next) if vel_next is not None else 0.0
+    if recon is not None:   # the end-of-step surface: the reconstruction at c = 1 (integrators.py:1369-1391)
+        a.alpha_end = recon[2] + recon[3] * 1.0 * float(dt)
     az = _az_args(kw.get("diffusion", None), vel, is3d, mesh)
+    if az is not None and recon is not None:
+        raise NotImplementedError("the Az kick with PCHIP reconstruction is not built on the CUDA backend")
     if az is not None:
         if az[0] and store is np.float16:
             raise NotImplementedError("the Az field with float16 snapshots is not built on the CUDA backend")

@@ -13,7 +13,7 @@ import pytest
 from kelp_b200 import integrators as KI
 from kelp_b200.diffusion import DiffusionStepArgs
 
-from test_oracle_golden import CGRID_CASES, SIGMA_CASES, diffusion_args
+from test_oracle_golden import CGRID_CASES, PCHIP_CASES, SIGMA_CASES, diffusion_args, recon_of
 
 pytestmark = pytest.mark.gpu
 
@@ -34,6 +34,7 @@ WALK_CASES += [("golden_3d", c) for c in ("rk2_wbary_walk", "rk4_wnear_walk_kick
 CASES += WALK_CASES
 CASES += SIGMA_CASES
 CASES += CGRID_CASES
+CASES += PCHIP_CASES
 
 
 def replay_cuda(g, cname):
@@ -50,8 +51,10 @@ def replay_cuda(g, cname):
         vel, vnext, dtn = g.payload(c["schedule"][k], T)
         diff = diffusion_args(c, k)
         uv = "nemo_cgrid" if getattr(g.mesh, "_nemo_cgrid", False) else "barycentric"
+        rc = recon_of(g, c, k)
+        extra = {} if rc is None else {"recon": rc}
         st = fn(st, vel, g.mesh, dt, td, uv_interp=uv, w_interp=w_interp, vel_next=vnext,
-                dt_to_next=dtn, diffusion=diff)
+                dt_to_next=dtn, diffusion=diff, **extra)
         if f"s{k + 1}_lon" in c:
             snaps[k + 1] = st
     return c, snaps

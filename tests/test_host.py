@@ -21,7 +21,7 @@ def test_library_exports_every_declared_symbol():
     missing = [s for s in declared if not hasattr(L, s)]
     assert not missing, missing
     assert declared == set(N.EXPORTS)
-    assert L.kc_abi_version() == N.ABI_VERSION == 6
+    assert L.kc_abi_version() == N.ABI_VERSION == 7
 
 
 def test_node_xyz_host_routine_matches_reference_table(golden):
@@ -86,8 +86,20 @@ def test_unsupported_paths_raise_before_device_work(golden):
     with pytest.raises(NotImplementedError):
         KI.rk2_step(st, sn[0], g.mesh, 3600.0, 1.0, **kw,
                     diffusion=DiffusionStepArgs("em", 1.0, 1.0, 0, 0, 0, composition="split_rk"))
-    with pytest.raises(NotImplementedError):
+    # malformed PCHIP bundles are refused as reconstruct_pchip refuses them
+    with pytest.raises(ValueError):
         KI.rk2_step(st, sn[0], g.mesh, 3600.0, 1.0, **kw, recon=object())
+    with pytest.raises(ValueError):   # times not increasing
+        KI.rk2_step(st, sn[0], g.mesh, 3600.0, 1.0, **kw, recon=(sn[:4], [0.0, 2.0, 1.0, 3.0], 0.5, 1.0))
+    with pytest.raises(ValueError):   # a stage outside the central interval
+        KI.rk2_step(st, sn[0], g.mesh, 3600.0, 1.0, **kw,
+                    recon=(sn[:4], [0.0, 86400.0, 172800.0, 259200.0], 172000.0, 1.0))
+    with pytest.raises(ValueError):   # direction against time_dir
+        KI.rk2_step(st, sn[0], g.mesh, 3600.0, 1.0, **kw,
+                    recon=(sn[:4], [0.0, 86400.0, 172800.0, 259200.0], 90000.0, -1.0))
+    with pytest.raises(NotImplementedError):   # PCHIP runs in the plain form
+        KI.rk2_step(st, sn[0], g.mesh, 3600.0, 1.0, **kw, cuda_precision="mixed",
+                    recon=(sn[:4], [0.0, 86400.0, 172800.0, 259200.0], 90000.0, 1.0))
     with pytest.raises(NotImplementedError):
         KI.get_integrator("rk45")(st, sn[0], g.mesh, 3600.0, 1.0)
     with pytest.raises(ValueError):
