@@ -14,6 +14,13 @@ figure), computed from the mesh's own statistics:
   per vertical row read;
 * W (3-D) per stage: nearest -- 2 interfaces x 2 snapshots x field bytes;
   barycentric -- vertices x (8 B depth + 2 interfaces x 2 snapshots x bytes).
+
+On a NEMO C-grid mesh a stage reads one cell instead: its corner ids (16 B),
+raster index and wet levels (8 B), the four corner lon/lat (64 B), the four
+faces of the bracket pair (4 x 2 x field bytes) and their widths (32 B); in
+3-D also two interfaces of w (2 x 2 x field bytes), the cell's area, bottom
+thickness and interfaces (32 B) and the four faces' partial levels (48 B); the
+step converts depth to level and back in the start and end cells (2 x 28 B).
 """
 from __future__ import annotations
 
@@ -38,6 +45,14 @@ def bytes_per_particle_step(mesh, scheme: str, dims: int, field_bytes: int, *, k
     state = 65 if dims == 2 else 89
     site = 4 + 4 * s["valence"] + 4 * s["max_v"] + 16 * s["nv"]
     n_sites = SITES[scheme] + (1 if kick else 0)
+    if getattr(mesh, "_nemo_cgrid", False):
+        stage = 16 + 8 + 64 + 4 * 2 * field_bytes + 32
+        if dims == 3:
+            stage += 2 * 2 * field_bytes + 32 + 48
+            state += 2 * 28
+        total = state + n_sites * site + STAGES[scheme] * stage
+        return {"total": float(total), "state": state, "site": site, "n_sites": n_sites, "stage": stage,
+                "n_stages": STAGES[scheme], **s}
     stage = s["nv"] * 2 * 2 * field_bytes
     w = 0.0
     if dims == 3:

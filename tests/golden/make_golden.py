@@ -529,6 +529,11 @@ def cgrid_fixture():
             rec["cgrid_" + k] = np.asarray(getattr(rm, "_nemo_cgrid_" + k))
         rec["cgrid_shape"] = np.array(rm._structured_shape)
         rec["cgrid_partial"] = np.array(rm._nemo_cgrid_partial)
+        # the builder's inputs, for checking a restated builder against the reference's
+        rec.update({"cgin_glamf": glamf, "cgin_gphif": gphif, "cgin_wet": wet})
+        if three_d:
+            rec.update({"cgin_e2u": e2u, "cgin_e1v": e1v, "cgin_nlev": nlev, "cgin_zw": zw, "cgin_area": area,
+                        "cgin_e3b": e3b, "cgin_e3u0": e3u0})
         save(f"golden_{tag}", rec, rf, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
 
 

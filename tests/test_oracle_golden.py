@@ -195,3 +195,26 @@ def test_elem_neighbors_match_reference(golden, fixture):
     g = golden(fixture)
     m = types.SimpleNamespace(elem_nodes=g.mesh.elem_nodes, nodes_lon=g.mesh.nodes_lon, _elem_neighbors=None)
     np.testing.assert_array_equal(build_elem_neighbors(m), g.d["mesh_elem_neighbors"])
+
+
+@pytest.mark.parametrize("fixture", ["golden_cgrid2d", "golden_cgrid3d"])
+def test_cgrid_mesh_builder_matches_reference(golden, fixture):
+    """kelp_b200.nemo.build_cgrid_mesh on the recorded raster equals the
+    reference's own build_nemo_cgrid_mesh: nodes, cells, ring, tables, grid hash."""
+    from kelp_b200.nemo import build_cgrid_mesh
+    g = golden(fixture)
+    d = g.d
+    kw = {}
+    if "mesh_cgin_zw" in d:
+        kw = dict(e2u=d["mesh_cgin_e2u"], e1v=d["mesh_cgin_e1v"], nlev2d=d["mesh_cgin_nlev"],
+                  zw=d["mesh_cgin_zw"], area=d["mesh_cgin_area"], e3b=d["mesh_cgin_e3b"],
+                  e3u0=d["mesh_cgin_e3u0"])
+    m = build_cgrid_mesh(d["mesh_cgin_glamf"], d["mesh_cgin_gphif"], d["mesh_cgin_wet"], **kw)
+    for k in ("nodes_lon", "nodes_lat", "depth", "elem_nodes", "node_to_elems", "node_to_elems_count"):
+        np.testing.assert_array_equal(np.asarray(getattr(m, k)), d[f"mesh_{k}"], err_msg=k)
+    np.testing.assert_array_equal(m._gh_offsets, d["mesh_gh_offsets"])
+    np.testing.assert_array_equal(m._gh_node_ids, d["mesh_gh_node_ids"])
+    for k in ("corners", "elem_ji", "nlev", "nlev_raster", "zw", "area", "e3b", "kbu", "e3u", "kbv", "e3v",
+              "e2u", "e1v"):
+        np.testing.assert_array_equal(np.asarray(getattr(m, "_nemo_cgrid_" + k)).reshape(-1),
+                                      d["mesh_cgrid_" + k].reshape(-1), err_msg=k)
