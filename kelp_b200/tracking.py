@@ -111,6 +111,31 @@ def resolve_time_bracket(t: float, file_times, on_exhausted: str = "stop", direc
     return ia, ib, ta, tb, tw
 
 
+def resolve_recon_stencil(bracket, n_records: int):
+    """tracking.py:3075-3094 _resolve_recon_stencil: the 4-record PCHIP
+    stencil ``((idx_a - 1, idx_a, idx_b, idx_b + 1), t_in_bracket)`` of a
+    bracket, or None at the first / last interval, on a record, or across a
+    cycle seam (the step then blends linearly)."""
+    ia, ib = int(bracket[0]), int(bracket[1])
+    if ib != ia + 1:
+        return None
+    if ia - 1 < 0 or ib + 1 >= n_records:
+        return None
+    return (ia - 1, ia, ib, ib + 1), float(bracket[4])
+
+
+def step_end_on_record(sim_time: float, pos: float, dt_to_next: float, direction: int, file_times,
+                       on_exhausted: str) -> float:
+    """tracking.py:2930-2944 _step_end_on_record: the clock after a step that
+    ends on the record ahead (``pos`` is the step's start in the bracket's
+    frame; under ``cycle`` the offset is taken modulo the period)."""
+    delta = pos - wrap_time(sim_time, file_times, on_exhausted)
+    if on_exhausted == "cycle":
+        period = cycle_period(file_times)
+        delta -= period * np.round(delta / period)
+    return sim_time + delta + dt_to_next * direction
+
+
 def vel_payload(bracket, fields: Sequence, direction: int = 1):
     """``(vel, vel_next, dt_to_next)`` of a bracket (tracking.py:3136-3206):
     the field at the query time (a snapshot, or a lazy pair with alpha), the
@@ -207,13 +232,15 @@ class Tracker:
     select the numerical form as for the step functions.  ``elem_search``
     "walk" carries each particle's containing element from step to step
     (tracking.py:2236-2253: seeded once at the start by the local search
-    around the exact anchor unless the initial state carries them)."""
+    around the exact anchor unless the initial state carries them).
+    ``temporal_reconstruction`` "pchip" hands the RK stages the 4-record
+    monotone-cubic stencil wherever one exists (tracking.py:2415-2436)."""
 
     def __init__(self, mesh, fields: Sequence, file_times, *, integrator: str = "rk2", dt: float,
                  time_dir: float = 1.0, uv_interp: str = "barycentric", w_interp: str = "barycentric",
                  diffusion=None, beaching: Optional[BeachingConfig] = None, on_exhausted: str = "stop",
                  precision: str = "plain", snapshots: Optional[str] = None, sort_every: int = 16,
-                 elem_search: str = "local", ctx=None):
+                 elem_search: str = "local", temporal_reconstruction: str = "linear", ctx=None):
         if integrator not in ("euler", "rk2", "rk4"):
             raise NotImplementedError(f"integrator {integrator!r} is not built on the CUDA backend")
         if on_exhausted not in ("stop", "cycle"):
@@ -224,6 +251,9 @@ class Tracker:
             raise ValueError(f"time_dir must be +1 or -1, got {time_dir!r}")
         if elem_search not in ("local", "walk"):
             raise ValueError(f"elem_search must be 'local' or 'walk', got {elem_search!r}")
+        if temporal_reconstruction not in ("linear", "pchip"):
+            raise ValueError(f"temporal_reconstruction must be 'linear' or 'pchip', got {temporal_reconstruction!r}")
+        self.pchip = temporal_reconstruction == "pchip"
         self.walk = elem_search == "walk"
         if getattr(mesh, "vertical_coord", "zlevel") == "sigma":
             # the reference's loop hands every sigma step the surfaces at its
@@ -327,28 +357,47 @@ class Tracker:
             records[r].release_z = np.array(init_state.z, copy=True)
         sim_time = t0
         done = 0
+        multistage = self.integrator in ("rk2", "rk4")
         for k in range(int(n_steps)):
             g = start_step_i + k
             bracket = resolve_time_bracket(sim_time, ft, self.on_exhausted, self.direction, band)
             if bracket is None:
                 break
+            stencil = resolve_recon_stencil(bracket, ft.size) if (self.pchip and multistage) else None
             vel, vnext, dtn = vel_payload(bracket, self.fields, self.direction)
+            recon = None
+            if stencil is not None:
+                idx4, q_time = stencil
+                recon = ([self.fields[i] for i in idx4], [float(ft[i]) for i in idx4], q_time,
+                         float(self.direction))
+            # tracking.py:2524-2560: a multistage step that reaches the record
+            # ahead within the band ends ON it (its length is the distance,
+            # the clock is set to the record); a step longer than the bracket
+            # falls back to steady velocity
+            step_len = self.dt
+            sim_time_end = None
+            if multistage and dtn is not None and abs(self.dt - dtn) <= band:
+                step_len = dtn
+                sim_time_end = step_end_on_record(sim_time, bracket[4], dtn, self.direction, ft, self.on_exhausted)
+            elif dtn is not None and dtn < self.dt <= dtn + band:
+                dtn = self.dt
+            if dtn is not None and step_len > dtn:
+                vnext, dtn, recon = None, None, None
             kw = dict(self.kw, vel_next=vnext, dt_to_next=dtn)
+            if recon is not None:
+                kw["recon"] = recon
             if self.sort_every > 0 and k % self.sort_every == 0:
                 ctx.sort()
             # the draws' keys: the realization of each particle (its own when R > 1)
             diff = self._diffusion_args(realizations[0], g, particle_offset)
             kw["diffusion"] = diff
             kick = KI._kick_args(diff)
-            a, _ = KI.prepare_step(vel, mesh, self.dt, float(self.direction), self.integrator, kw, ctx, kick=kick)
+            a, _ = KI.prepare_step(vel, mesh, step_len, float(self.direction), self.integrator, kw, ctx, kick=kick)
             a.global_step = g
             ctx.step(a)
             if beach_cfg is not None:
                 ctx.beach(beach_args(beach_cfg, realizations[0], g, self.dt))
-            if dtn is not None and abs(self.dt - dtn) <= band:
-                sim_time = sim_time + dtn * self.direction   # the step ends on the record ahead
-            else:
-                sim_time = sim_time + self.dt * self.direction
+            sim_time = sim_time_end if sim_time_end is not None else sim_time + self.dt * self.direction
             done += 1
             if (g + 1) % max(int(output_freq), 1) == 0:
                 s = ctx.download_particles()
@@ -470,8 +519,6 @@ def run_tracking(config, *, mesh=None, fields=None, file_times=None, seeds=None,
         raise ValueError(f"numerics.backend must be 'cuda' for this package, got {backend!r}")
     if not num.get("temporal_interp", True):
         raise NotImplementedError("the CUDA backend runs with temporal_interp: true")
-    if num.get("temporal_reconstruction", "linear") != "linear":
-        raise NotImplementedError("PCHIP temporal reconstruction is not built on the CUDA backend")
     if num.get("periodic_lon") is not None or num.get("periodic_lat") is not None:
         raise NotImplementedError("periodic windows are not built on the CUDA backend")
     if mesh is None:
@@ -509,7 +556,8 @@ def run_tracking(config, *, mesh=None, fields=None, file_times=None, seeds=None,
                       on_exhausted=tim.get("on_exhausted", "stop"),
                       precision=num.get("cuda_precision", "plain"), snapshots=num.get("cuda_snapshots"),
                       sort_every=int(num.get("sort_every", 16)),
-                      elem_search=num.get("elem_search", "local"), ctx=ctx)
+                      elem_search=num.get("elem_search", "local"),
+                      temporal_reconstruction=num.get("temporal_reconstruction", "linear"), ctx=ctx)
     start_idx = int(tim.get("start_time_idx", 0))
     n_steps = tim.get("n_steps")
     if n_steps is None:

@@ -611,6 +611,29 @@ def time_fixture():
     np.savez_compressed(os.path.join(HERE, "golden_time.npz"), rows=np.array(rows),
                         axis_uniform=axes["uniform"], axis_ragged=axes["ragged"])
     print("golden_time", len(rows))
+    # the PCHIP stencil of every bracket (tracking._resolve_recon_stencil) and
+    # the clock after a step that ends on the record ahead
+    # (tracking._step_end_on_record), for clocks one pass either side in cycle mode
+    from kelp.tracking import _resolve_recon_stencil, _step_end_on_record, _cycle_period
+    crow = []
+    for row in rows:
+        ai, mi, d, snap, q = row[:5]
+        if np.isnan(row[5]):
+            continue
+        ft = list(axes.values())[int(ai)]
+        mode = ("stop", "cycle")[int(mi)]
+        b = (int(row[5]), int(row[6]), row[7], row[8], row[9])
+        st = _resolve_recon_stencil(b, ft.size)
+        idx = [-1] * 4 if st is None else list(st[0])
+        target = b[3] if d > 0 else b[2]
+        dtn = abs(target - b[4])
+        shifts = (0.0,) if mode == "stop" else (0.0, _cycle_period(ft, ft.size, None), -_cycle_period(ft, ft.size, None))
+        for sh in shifts:
+            end = _step_end_on_record(q + sh, b[4], dtn, int(d), ft, ft.size, mode, None)
+            crow.append([ai, mi, d, q + sh] + list(b) + idx + [dtn, end])
+    np.savez_compressed(os.path.join(HERE, "golden_clock.npz"), rows=np.array(crow, dtype=np.float64),
+                        axis_uniform=axes["uniform"], axis_ragged=axes["ragged"])
+    print("golden_clock", len(crow))
 
 
 if __name__ == "__main__":

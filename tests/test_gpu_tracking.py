@@ -176,3 +176,38 @@ def test_tracker_az_kick_equals_per_call(golden):
     for name in ("status", "nearest_node", "failure_reason", "lon", "lat", "z"):
         np.testing.assert_array_equal(getattr(fin, name), getattr(st, name), err_msg=name)
     assert np.any(fin.z != st0.z)
+
+
+def test_tracker_pchip_equals_per_call(golden):
+    """temporal_reconstruction "pchip" in the resident loop: the RK stages take
+    the 4-record stencil where one exists (linear at the first and last
+    interval), bit-identical to the per-call rk4_step with the same bundles."""
+    from kelp_b200 import integrators as KI
+    g = golden("golden_pchip2d")
+    dt = 21600.0
+    ft = np.arange(len(g.snaps)) * 86400.0
+    n = 18
+    tr = T.Tracker(g.mesh, g.snaps, ft, integrator="rk4", dt=dt, sort_every=3, temporal_reconstruction="pchip")
+    st0 = g.particles()
+    fin = tr.run(st0, n).final[0]
+    st = st0
+    t = float(ft[0])
+    band = T.snapshot_band(dt)
+    used = 0
+    for k in range(n):
+        br = T.resolve_time_bracket(t, ft, "stop", 1, band)
+        vel, vnext, dtn = T.vel_payload(br, g.snaps, 1)
+        sten = T.resolve_recon_stencil(br, ft.size)
+        kw = {}
+        if sten is not None:
+            kw["recon"] = ([g.snaps[i] for i in sten[0]], [float(ft[i]) for i in sten[0]], sten[1], 1.0)
+            used += 1
+        step_len, t_end = dt, None
+        if dtn is not None and abs(dt - dtn) <= band:
+            step_len, t_end = dtn, T.step_end_on_record(t, br[4], dtn, 1, ft, "stop")
+        st = KI.rk4_step(st, vel, g.mesh, step_len, 1.0, uv_interp="barycentric", vel_next=vnext,
+                         dt_to_next=dtn, **kw)
+        t = t_end if t_end is not None else t + dt
+    assert 0 < used < n
+    for name in ("status", "nearest_node", "failure_reason", "lon", "lat"):
+        np.testing.assert_array_equal(getattr(fin, name), getattr(st, name), err_msg=name)

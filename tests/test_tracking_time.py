@@ -45,3 +45,27 @@ def test_payload_directions():
     assert vnext is fields[0] and dtn == 25.0
     vel, vnext, dtn = vel_payload(resolve_time_bracket(200.0, ft), fields, 1)
     assert vel is fields[2] and vnext is None and dtn is None
+
+
+def test_recon_stencil_and_record_clock_match_reference():
+    """The PCHIP stencil of each bracket (tracking._resolve_recon_stencil) and
+    the clock after a step that ends on the record ahead
+    (tracking._step_end_on_record), including clocks a cycle period away."""
+    from kelp_b200.tracking import resolve_recon_stencil, step_end_on_record
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden_clock.npz"))
+    axes = [d["axis_uniform"], d["axis_ragged"]]
+    modes = ["stop", "cycle"]
+    n_stencil = 0
+    for row in d["rows"]:
+        ai, mi, direction, t = int(row[0]), int(row[1]), int(row[2]), float(row[3])
+        b = (int(row[4]), int(row[5]), row[6], row[7], row[8])
+        st = resolve_recon_stencil(b, axes[ai].size)
+        want = [int(x) for x in row[9:13]]
+        if want[0] < 0:
+            assert st is None, row
+        else:
+            n_stencil += 1
+            assert list(st[0]) == want and st[1] == b[4], row
+        end = step_end_on_record(t, b[4], float(row[13]), direction, axes[ai], modes[mi])
+        assert end == float(row[14]), (row, end)
+    assert n_stencil > 0
