@@ -275,6 +275,13 @@ class DeviceContext:
                   "kc_particles_upload")
         self.P = P
 
+    def download_status(self) -> np.ndarray:
+        """The statuses of the resident particles (upload order)."""
+        out = np.empty(self.P, np.int32)
+        self._chk(N.lib().kc_particles_download(self._ctx, self.P, None, None, None, N.ptr(out), None, None, None,
+                                                None, None), "kc_particles_download")
+        return out
+
     def download_particles(self) -> dict:
         P = self.P
         out = {"lon": np.empty(P), "lat": np.empty(P), "z": np.empty(P),

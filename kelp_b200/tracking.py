@@ -136,6 +136,27 @@ def step_end_on_record(sim_time: float, pos: float, dt_to_next: float, direction
     return sim_time + delta + dt_to_next * direction
 
 
+def record_view(s: dict, prev_status: np.ndarray, direction: int) -> dict:
+    """The recorded values of one observation (output format 2): dormant
+    (NOT_RELEASED) rows get NaN positions and velocities
+    (core/release.py:132-167), a velocity exists only where the particle was
+    ALIVE through the whole step (:170-201), and a backward run records the
+    flow velocity (tracking.py:2770-2776)."""
+    out = dict(s)
+    dormant = s["status"] == int(ParticleStatus.NOT_RELEASED)
+    if np.any(dormant):
+        for k in ("lon", "lat", "z", "u", "v", "w"):
+            if out.get(k) is not None:
+                out[k] = np.where(dormant, np.nan, np.asarray(out[k], dtype=np.float64))
+    alive = int(ParticleStatus.ALIVE)
+    bad = (s["status"] != alive) | (np.asarray(prev_status) != alive)
+    for k in ("u", "v", "w"):
+        if out.get(k) is not None:
+            v = np.where(bad, np.nan, np.asarray(out[k], dtype=np.float64))
+            out[k] = -v if direction < 0 else v
+    return out
+
+
 def vel_payload(bracket, fields: Sequence, direction: int = 1):
     """``(vel, vel_next, dt_to_next)`` of a bracket (tracking.py:3136-3206):
     the field at the query time (a snapshot, or a lazy pair with alpha), the
@@ -303,22 +324,30 @@ class Tracker:
 
     def run(self, init_state: ParticleState, n_steps: int, *, start_time: Optional[float] = None,
             realization_id: int = 0, start_step_i: int = 0, output_freq: int = 1, particle_offset: int = 0,
-            release_step: Optional[np.ndarray] = None, start_wet_streak=None) -> RunResult:
-        """One realization; the result holds one record and final state."""
+            release_step: Optional[np.ndarray] = None, start_wet_streak=None, writer=None,
+            checkpoint_freq: int = 0) -> RunResult:
+        """One realization; the result holds one record and final state.
+        ``writer`` (kelp_b200.writers.TrajectoryWriter) receives every
+        record and, every ``checkpoint_freq`` global steps, a restart
+        checkpoint (tracking.py:2778-2792); resume with the checkpoint's
+        state, ``start_step_i = step_i + 1`` and the wet streaks."""
         return self.run_realizations(init_state, n_steps, realizations=(realization_id,), start_time=start_time,
                                      start_step_i=start_step_i, output_freq=output_freq,
                                      particle_offset=particle_offset, release_step=release_step,
-                                     start_wet_streak=start_wet_streak)
+                                     start_wet_streak=start_wet_streak, writer=writer,
+                                     checkpoint_freq=checkpoint_freq)
 
     def run_realizations(self, init_state: ParticleState, n_steps: int, *, realizations: Sequence[int] = (0,),
                          start_time: Optional[float] = None, start_step_i: int = 0, output_freq: int = 1,
                          particle_offset: int = 0, release_step: Optional[np.ndarray] = None,
-                         start_wet_streak=None) -> RunResult:
+                         start_wet_streak=None, writer=None, checkpoint_freq: int = 0) -> RunResult:
         """Every realization of ``realizations`` from the same seeds and start
         time, as one particle array (per-particle realization ids): one record
         and final state per realization, each as its own run would give."""
         ctx, mesh = self.ctx, self.mesh
         R = len(realizations)
+        if writer is not None and R != 1:
+            raise ValueError("a trajectory writer holds one realization: run them one by one")
         P = init_state.n_particles
         ft = self.file_times
         t0 = float(ft[0] if start_time is None else start_time)
@@ -386,6 +415,11 @@ class Tracker:
             kw = dict(self.kw, vel_next=vnext, dt_to_next=dtn)
             if recon is not None:
                 kw["recon"] = recon
+            recording = (g + 1) % max(int(output_freq), 1) == 0
+            if recording:   # the status after the release activation and before the step
+                prev = ctx.download_status()
+                if rs is not None:
+                    prev[(prev == int(ParticleStatus.NOT_RELEASED)) & (rs <= g)] = int(ParticleStatus.ALIVE)
             if self.sort_every > 0 and k % self.sort_every == 0:
                 ctx.sort()
             # the draws' keys: the realization of each particle (its own when R > 1)
@@ -399,12 +433,29 @@ class Tracker:
                 ctx.beach(beach_args(beach_cfg, realizations[0], g, self.dt))
             sim_time = sim_time_end if sim_time_end is not None else sim_time + self.dt * self.direction
             done += 1
-            if (g + 1) % max(int(output_freq), 1) == 0:
+            s = None
+            if recording:
                 s = ctx.download_particles()
                 t_rec = t0 + (g + 1 - start_step_i) * self.dt * self.direction
+                view = record_view(s, prev, self.direction)
                 for r in range(R):
                     sl = slice(r * P, (r + 1) * P)
-                    records[r].append({k2: v[sl] for k2, v in s.items()}, t_rec, self.dims)
+                    records[r].append({k2: (None if v is None else v[sl]) for k2, v in view.items()}, t_rec,
+                                      self.dims)
+                if writer is not None:
+                    writer.append(ParticleState(lon=view["lon"], lat=view["lat"], z=view["z"],
+                                                status=view["status"], nearest_node=view["nearest_node"],
+                                                u=view["u"], v=view["v"], w=view["w"] if self.dims == 3 else None,
+                                                failure_reason=view["failure_reason"]), t_rec)
+            if writer is not None and checkpoint_freq > 0 and (g + 1) % checkpoint_freq == 0:
+                s = s if s is not None else ctx.download_particles()
+                ck = init_state.replace(lon=s["lon"], lat=s["lat"], z=s["z"], status=s["status"],
+                                        nearest_node=s["nearest_node"], failure_reason=s["failure_reason"],
+                                        elem=ctx.get_elem() if self.walk else None)
+                writer.write_checkpoint(ck, g, int(bracket[0]),
+                                        wet_streak=ctx.beach_state_download() if beach_cfg is not None else None,
+                                        release_step=rs, particle_offset=particle_offset,
+                                        uv_vertical=getattr(self.fields[0], "uv_vertical", "layer"))
         err = ctx.device_errors()
         if err:
             raise N.KcError(N.KC_ERR_DEVICE, N.describe_device_errors(err))
