@@ -91,6 +91,8 @@ struct kc_ctx {
     bool has_pid = false, has_rs = false, has_rid = false, has_elem = false;
     int* rid = nullptr;   // per-particle realization ids (ensemble members in one array)
     int* elem = nullptr;  // carried containing elements (elem_search walk)
+    int* el = nullptr;    // carried local containment scans (valid where nn_ok bit 1)
+    int* wel = nullptr;
     // re-sort by grid-hash cell: upload slot of every resident particle, the
     // spare buffer of the gathers, radix-sort keys / indices and CUB's storage
     long long* orig = nullptr;
@@ -173,6 +175,8 @@ kc::DState state_of(kc_ctx* c) {
     st.prev = c->has_beach ? c->prev : nullptr;
     st.nn_ok = c->nn_ok;
     st.elem = c->has_elem ? c->elem : nullptr;
+    st.el = c->el;
+    st.wel = c->wel;
     st.P = c->P;
     return st;
 }
@@ -530,6 +534,7 @@ void free_mesh(kc_ctx* c) {
 void free_particles(kc_ctx* c) {
     dfree(c->lon); dfree(c->lat); dfree(c->z); dfree(c->U); dfree(c->V); dfree(c->W);
     dfree(c->status); dfree(c->nn); dfree(c->fr); dfree(c->pid); dfree(c->rs); dfree(c->rid); dfree(c->elem);
+    dfree(c->el); dfree(c->wel);
     c->has_elem = false;
     dfree(c->orig); dfree(c->spare); dfree(c->prev); dfree(c->wet); dfree(c->nn_ok);
     c->has_beach = false;
@@ -1042,6 +1047,8 @@ static int ensure_capacity(kc_ctx* c, long long P) {
     KC_CUDA(c, cudaMalloc((void**)&c->rs, n)); KC_CUDA(c, cudaMalloc((void**)&c->orig, n));
     KC_CUDA(c, cudaMalloc((void**)&c->rid, n));
     KC_CUDA(c, cudaMalloc((void**)&c->elem, n));
+    KC_CUDA(c, cudaMalloc((void**)&c->el, n));
+    KC_CUDA(c, cudaMalloc((void**)&c->wel, n));
     KC_CUDA(c, cudaMalloc((void**)&c->spare, n));
     KC_CUDA(c, cudaMalloc((void**)&c->prev, n)); KC_CUDA(c, cudaMalloc((void**)&c->wet, n));
     KC_CUDA(c, cudaMalloc((void**)&c->nn_ok, n));
@@ -1192,6 +1199,8 @@ int kc_sort(kc_ctx* c) {
     if ((rc = regather(c, (void**)&c->nn, 4, idx))) return rc;
     if ((rc = regather(c, (void**)&c->fr, 1, idx))) return rc;
     if ((rc = regather(c, (void**)&c->nn_ok, 1, idx))) return rc;
+    if ((rc = regather(c, (void**)&c->el, 4, idx))) return rc;
+    if ((rc = regather(c, (void**)&c->wel, 4, idx))) return rc;
     if (c->has_rs && (rc = regather(c, (void**)&c->rs, 4, idx))) return rc;
     if (c->has_rid && (rc = regather(c, (void**)&c->rid, 4, idx))) return rc;
     if (c->has_elem && (rc = regather(c, (void**)&c->elem, 4, idx))) return rc;
@@ -1271,7 +1280,7 @@ int kc_step_host(kc_ctx* c, const kc_step_args* a, long long P, const kc_host_pa
         st.rid = in->real_id ? c->rid + b : nullptr;
         st.release_step = in->release_step ? c->rs + b : nullptr;
         st.elem = in->elem ? c->elem + b : nullptr;
-        st.prev = nullptr; st.nn_ok = nullptr;
+        st.prev = nullptr; st.nn_ok = nullptr; st.el = nullptr; st.wel = nullptr;
         st.P = n;
         kc::DStep sk = s0;
         if (!in->pid) sk.pid_offset = s0.pid_offset + (unsigned long long)b;
@@ -1313,6 +1322,8 @@ static kc::DState state_range(kc::DState st, long long begin, long long count) {
     if (st.prev) st.prev += begin;
     if (st.nn_ok) st.nn_ok += begin;
     if (st.elem) st.elem += begin;
+    if (st.el) st.el += begin;
+    if (st.wel) st.wel += begin;
     st.P = count;
     return st;
 }

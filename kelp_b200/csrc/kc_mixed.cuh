@@ -142,8 +142,8 @@ __device__ __forceinline__ float w_node_f32(const DMesh& m, const DBlend<T>& f, 
 // dims 2 reads u/v row 0 and no W.
 template <typename T>
 __device__ __noinline__ bool stage_f32(const DMesh& m, const DBlend<T>& f, const DStep& s, int dims, double xp,
-                                       double yp, int nn, int hint, double z, double alpha, double& U, double& V,
-                                       double& W) {
+                                       double yp, int nn, int hint, int whint, double z, double alpha, double& U,
+                                       double& V, double& W) {
     U = 0.0;
     V = 0.0;
     W = 0.0;
@@ -151,12 +151,18 @@ __device__ __noinline__ bool stage_f32(const DMesh& m, const DBlend<T>& f, const
     const float td = (float)s.time_dir;
     int w_elem = -1;
     bool w_unsure = false;
-    // the W bookkeeping of the scan only where a barycentric W reads it; an
-    // edge-walk element (hint) replaces the scan, and the W search then runs
+    // the W bookkeeping of the scan only where a barycentric W reads it; a
+    // carried scan (hint, whint >= -2) replaces it, an edge-walk element
+    // (hint, whint -3) replaces the u/v scan and the W search then runs
     int elem;
     if (hint >= 0) {
         elem = hint;
-        w_unsure = true;
+        if (whint >= -2) {
+            w_elem = whint >= 0 ? whint : -1;
+            w_unsure = whint == -2;
+        } else {
+            w_unsure = true;
+        }
     } else {
         elem = (dims == 3 && s.w_code == 1) ? contain_local_w(m, xp, yp, nn, w_elem, w_unsure)
                                             : contain_local(m, xp, yp, nn);
@@ -269,12 +275,12 @@ struct MixedForm {
     static __device__ __forceinline__ bool uv2(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
                                                double lat, int nn, int hint, double alpha, double& U, double& V) {
         double W;
-        return stage_f32<T>(m, f, s, 2, lon, lat, nn, hint, 0.0, alpha, U, V, W);
+        return stage_f32<T>(m, f, s, 2, lon, lat, nn, hint, -3, 0.0, alpha, U, V, W);
     }
     static __device__ __forceinline__ bool uvw3(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
-                                                double lat, int nn, int hint, double z, double alpha, double& U,
-                                                double& V, double& W) {
-        return stage_f32<T>(m, f, s, 3, lon, lat, nn, hint, z, alpha, U, V, W);
+                                                double lat, int nn, int hint, int whint, double z, double alpha,
+                                                double& U, double& V, double& W) {
+        return stage_f32<T>(m, f, s, 3, lon, lat, nn, hint, whint, z, alpha, U, V, W);
     }
 };
 

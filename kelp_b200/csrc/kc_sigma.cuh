@@ -322,8 +322,9 @@ __device__ __forceinline__ void step3d_sigma_particle(const DMesh& m, const DBle
             z_new = clamp_sig(s_new * ce.H, ce.H, s);
             if (s.kick) {
                 const long long pid = st.pid ? st.pid[i] : i;
+                int kel, kwel;
                 apply_kick(m, s, pid, realization_of(st, s, i), qn, lon0, lat0, z0p, pre_nn, false, lon_new, lat_new,
-                           z_new, status, nn_out, fr);
+                           z_new, status, nn_out, fr, false, kel, kwel);
                 if (status == ALIVE) {
                     const double H_post = ce.H;
                     sigma_site<T>(m, f, s, s.alpha_end, lon_new, lat_new, nn_out, ce);

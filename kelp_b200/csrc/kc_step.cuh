@@ -27,8 +27,12 @@ struct DState {
     const int* rid;            // per-particle realization (RNG key), the step's real_id when null
     const int* release_step;   // delayed release (null: all released)
     int* prev;                 // status at the step's entry, for the beaching hook (null: not kept)
-    unsigned char* nn_ok;      // 1: nn is the exact anchor of the current position (null: never trusted)
+    unsigned char* nn_ok;      // bit 0: nn is the exact anchor of the current position; bit 1: el / wel hold
+                               // its local containment scan (null: never trusted)
     int* elem;                 // carried containing element (elem_search walk), null: the local scan
+    int* el;                   // the local scan's element at the current position and anchor
+    int* wel;                  // what that scan implies for the barycentric W search: its element (>= 0),
+                               // its nodal fallback (-1), undecided (-2), not evaluated (-3)
     long long P;
 };
 
@@ -67,7 +71,7 @@ __device__ __forceinline__ double clamp_lat(double lat) {
 // the same), else the exact search.
 __device__ __forceinline__ int start_anchor(const DMesh& m, const DState& st, const Site& q0, int pre_nn,
                                             long long i) {
-    if (st.nn_ok && st.nn_ok[i] && pre_nn >= 0) return pre_nn;
+    if (st.nn_ok && (st.nn_ok[i] & 1) && pre_nn >= 0) return pre_nn;
     return site_anchor(m, q0);
 }
 
@@ -77,6 +81,43 @@ __device__ __forceinline__ int start_anchor(const DMesh& m, const DState& st, co
 // it equals the start anchor).
 __device__ __forceinline__ void mark_anchor(const DState& st, long long i, int status, int nn_out, int node_i) {
     if (st.nn_ok) st.nn_ok[i] = (status == ALIVE || nn_out == node_i) ? 1 : 0;
+}
+
+// The containment scan of a step's start (position and anchor unchanged
+// since the last step of this library computed it): the scan is a pure
+// function of the two, so stage 1 reuses the end-of-step scan instead of
+// repeating it.  eh = -1 / wh = -3 when nothing is carried.
+__device__ __forceinline__ void carried_scan(const DState& st, long long i, int& eh, int& wh) {
+    eh = -1;
+    wh = -3;
+    if (st.el && st.nn_ok && (st.nn_ok[i] & 2)) {
+        eh = st.el[i];
+        wh = st.wel[i];
+    }
+}
+
+// After mark_anchor: keep the scan of the particle's final position (el >= 0).
+__device__ __forceinline__ void mark_scan(const DState& st, long long i, int status, int el, int wel) {
+    if (st.el && st.nn_ok && status == ALIVE && el >= 0) {
+        st.el[i] = el;
+        st.wel[i] = wel;
+        st.nn_ok[i] |= 2;
+    }
+}
+
+// The end-of-step containment in local mode: the scan at the new position and
+// its exact anchor, with the barycentric W search's information when the
+// step reads W that way (wel, for the next step's first stage).
+__device__ __forceinline__ int end_scan(const DMesh& m, bool want_w, double lon, double lat, int nn, int& wel) {
+    if (want_w) {
+        int we;
+        bool wu;
+        const int e = contain_local_w(m, lon, lat, nn, we, wu);
+        wel = wu ? -2 : we;
+        return e;
+    }
+    wel = -3;
+    return contain_local(m, lon, lat, nn);
 }
 
 // The realization key of particle i: its own when the particles carry one
@@ -111,7 +152,8 @@ __device__ __forceinline__ int end_elem(const DMesh& m, double lon, double lat, 
 static __device__ __noinline__ void apply_kick(const DMesh& m, const DStep& s, long long pid, unsigned long long rid,
                                         const Site& qn,
                                         double pre_lon, double pre_lat, double pre_z, int pre_nn, bool is3d,
-                                        double& lon, double& lat, double& z, int& status, int& nn, signed char& fr) {
+                                        double& lon, double& lat, double& z, int& status, int& nn, signed char& fr,
+                                        bool want_w, int& kel, int& kwel) {
     double g1, g2;
     normal_pair(s.seed, rid, (unsigned long long)pid + s.pid_offset, s.step_i, 0ull, g1, g2);
     double abs_dt = s.dt >= 0.0 ? s.dt : -s.dt;
@@ -131,7 +173,8 @@ static __device__ __noinline__ void apply_kick(const DMesh& m, const DStep& s, l
     sphere_displace(qn, dx, dy, lk, lak);
     Site qk = make_site(lk, lak);
     int nk = site_anchor(m, qk);
-    if (contain_local(m, lk, lak, nk) < 0) {
+    kel = end_scan(m, want_w, lk, lak, nk, kwel);
+    if (kel < 0) {
         status = OUTSIDE;
         lon = pre_lon;
         lat = pre_lat;
@@ -272,9 +315,12 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
     const int node_i = start_anchor(m, st, q0, pre_nn, i);
     const int e1 = stage_elem<WALK>(m, lon0, lat0, WALK ? st.elem[i] : -1, node_i);
     int e_last = e1, e_out = e1;
+    int eh = e1, wh = -3;
+    if constexpr (!WALK) carried_scan(st, i, eh, wh);
+    int sc_el = -1, sc_wel = -3;   // the scan of the final position
 
     double U1, V1;
-    bool ok1 = Form::uv2(m, f, s, lon0, lat0, node_i, e1, s.ak[0], U1, V1);
+    bool ok1 = Form::uv2(m, f, s, lon0, lat0, node_i, eh, s.ak[0], U1, V1);
     st.U[i] = U1;
     st.V[i] = V1;
     if (!ok1) {
@@ -342,7 +388,10 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
     if (!failed) {
         const Site qn = make_site(lon_new, lat_new);
         int nn_new = site_anchor(m, qn);
-        const int ein = end_elem<WALK>(m, lon_new, lat_new, e_last, nn_new);
+        int ein;
+        if constexpr (WALK) ein = walk_locate(m, lon_new, lat_new, e_last, nn_new);
+        else ein = end_scan(m, false, lon_new, lat_new, nn_new, sc_wel);
+        sc_el = ein;
         if (ein < 0) {
             status = OUTSIDE; fr = FR_OOB; nn_out = node_i;
             lon_new = lon0; lat_new = lat0;
@@ -353,7 +402,8 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
             if (s.kick) {
                 double zz = 0.0;
                 long long pid = st.pid ? st.pid[i] : i;
-                apply_kick(m, s, pid, realization_of(st, s, i), qn, lon0, lat0, 0.0, pre_nn, false, lon_new, lat_new, zz, status, nn_out, fr);
+                apply_kick(m, s, pid, realization_of(st, s, i), qn, lon0, lat0, 0.0, pre_nn, false, lon_new, lat_new,
+                           zz, status, nn_out, fr, false, sc_el, sc_wel);
             }
         }
     } else {
@@ -367,6 +417,7 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
     st.fr[i] = fr;
     if constexpr (WALK) st.elem[i] = e_out;
     mark_anchor(st, i, status, nn_out, node_i);
+    if constexpr (!WALK) mark_scan(st, i, status, sc_el, sc_wel);
 }
 
 template <typename T>
@@ -399,23 +450,28 @@ struct PlainForm {
         return interp_uv_bary<T>(m, f, lon, lat, nn, hint, s.time_dir, 0, alpha, U, V);
     }
     static __device__ __forceinline__ bool uvw3(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
-                                                double lat, int nn, int hint, double z, double alpha, double& U,
-                                                double& V, double& W) {
+                                                double lat, int nn, int hint, int whint, double z, double alpha,
+                                                double& U, double& V, double& W) {
         if (s.w_code == 0) {
             const bool ok = stage_uv<T>(m, f, s, lon, lat, nn, hint, z, alpha, U, V);
             W = w_linear<T>(m, f, alpha, z, nn, s.time_dir);
             return ok;
         }
-        if (hint >= 0) {
-            const bool ok = stage_uv<T>(m, f, s, lon, lat, nn, hint, z, alpha, U, V);
-            W = w_bary<T>(m, f, alpha, lon, lat, z, nn, s.time_dir);
-            return ok;
-        }
         // W barycentric: one containment scan decides the u/v element and,
-        // almost always, the element the W search would stop at
-        int w_elem;
-        bool w_unsure;
-        const int elem = contain_local_w(m, lon, lat, nn, w_elem, w_unsure);
+        // almost always, the element the W search would stop at (a carried
+        // scan, whint >= -2, gives both; a walk element, whint -3, leaves the
+        // W search to run)
+        int w_elem = -1;
+        bool w_unsure = true;
+        int elem = hint;
+        if (hint >= 0) {
+            if (whint >= -2) {
+                w_elem = whint >= 0 ? whint : -1;
+                w_unsure = whint == -2;
+            }
+        } else {
+            elem = contain_local_w(m, lon, lat, nn, w_elem, w_unsure);
+        }
         bool ok = false;
         U = 0.0;
         V = 0.0;
@@ -438,7 +494,7 @@ __device__ __forceinline__ bool stage3d(const DMesh& m, const DBlend<T>& f, cons
                                         double& V, double& W) {
     const int nn = site_anchor(m, q);
     e = stage_elem<WALK>(m, lon, lat, from, nn);
-    return Form::uvw3(m, f, s, lon, lat, nn, e, z, s.ak[k], U, V, W);
+    return Form::uvw3(m, f, s, lon, lat, nn, e, -3, z, s.ak[k], U, V, W);
 }
 
 // 3-D Euler (integrators.py:4997-5147) and RK4 (:5760-6011): the reference's
@@ -467,8 +523,11 @@ __device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DB
     int nn_out = node_i;
     const int e1 = stage_elem<WALK>(m, lon0, lat0, WALK ? st.elem[i] : -1, node_i);
     int e_last = e1, e_out = e1;
+    int eh = e1, wh = -3;
+    if constexpr (!WALK) carried_scan(st, i, eh, wh);
+    int sc_el = -1, sc_wel = -3;
     double U1, V1, W1;
-    bool ok = Form::uvw3(m, f, s, lon0, lat0, node_i, e1, z0p, s.ak[0], U1, V1, W1);
+    bool ok = Form::uvw3(m, f, s, lon0, lat0, node_i, eh, wh, z0p, s.ak[0], U1, V1, W1);
     st.U[i] = U1;
     st.V[i] = V1;
     st.W[i] = W1;
@@ -515,7 +574,10 @@ __device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DB
     } else {
         const Site qn = make_site(a, b);
         const int nn_new = site_anchor(m, qn);
-        const int ein = end_elem<WALK>(m, a, b, e_last, nn_new);
+        int ein;
+        if constexpr (WALK) ein = walk_locate(m, a, b, e_last, nn_new);
+        else ein = end_scan(m, s.w_code == 1, a, b, nn_new, sc_wel);
+        sc_el = ein;
         if (ein < 0) {
             status = OUTSIDE; fr = FR_OOB;
         } else {
@@ -528,8 +590,8 @@ __device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DB
             e_out = ein;
             if (s.kick) {
                 long long pid = st.pid ? st.pid[i] : i;
-                apply_kick(m, s, pid, realization_of(st, s, i), qn, lon0, lat0, z0p, pre_nn, true, lon_new, lat_new, z_new, status, nn_out,
-                           fr);
+                apply_kick(m, s, pid, realization_of(st, s, i), qn, lon0, lat0, z0p, pre_nn, true, lon_new, lat_new, z_new,
+                           status, nn_out, fr, s.w_code == 1, sc_el, sc_wel);
             }
             if (s.az_on && status == ALIVE)
                 apply_az<T>(m, f, s, st.pid ? st.pid[i] : i, realization_of(st, s, i), nn_out, z_new);
@@ -543,6 +605,7 @@ __device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DB
     st.fr[i] = fr;
     if constexpr (WALK) st.elem[i] = e_out;
     mark_anchor(st, i, status, nn_out, node_i);
+    if constexpr (!WALK) mark_scan(st, i, status, sc_el, sc_wel);
 }
 
 // integrators.py:3647-3856 _fused_rk2_step_3d_bary_tinterp (layer u/v,
@@ -569,8 +632,11 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
     int nn_out = node_i;
     const int e1 = stage_elem<WALK>(m, lon0, lat0, WALK ? st.elem[i] : -1, node_i);
     int e_out = e1;
+    int eh = e1, wh = -3;
+    if constexpr (!WALK) carried_scan(st, i, eh, wh);
+    int sc_el = -1, sc_wel = -3;
     double U1, V1, W1;
-    const bool ok1 = Form::uvw3(m, f, s, lon0, lat0, node_i, e1, z0p, s.ak[0], U1, V1, W1);
+    const bool ok1 = Form::uvw3(m, f, s, lon0, lat0, node_i, eh, wh, z0p, s.ak[0], U1, V1, W1);
     st.U[i] = U1;
     st.V[i] = V1;
     st.W[i] = W1;
@@ -584,7 +650,7 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
         const int nn_mid = site_anchor(m, qm);
         const int em = stage_elem<WALK>(m, lon_mid, lat_mid, e1, nn_mid);
         double U2, V2, W2;
-        if (!Form::uvw3(m, f, s, lon_mid, lat_mid, nn_mid, em, z_mid, s.ak[1], U2, V2, W2)) {
+        if (!Form::uvw3(m, f, s, lon_mid, lat_mid, nn_mid, em, -3, z_mid, s.ak[1], U2, V2, W2)) {
             status = OUTSIDE; fr = FR_INTERP;
         } else {
             const double ln = wrap180(lon0 + dt * U2 / metric_z0(qm));
@@ -592,7 +658,10 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
             double zn = z0p + W2 * dt;
             const Site qn = make_site(ln, lt);
             const int nn_new = site_anchor(m, qn);
-            const int ein = end_elem<WALK>(m, ln, lt, em, nn_new);
+            int ein;
+            if constexpr (WALK) ein = walk_locate(m, ln, lt, em, nn_new);
+            else ein = end_scan(m, s.w_code == 1, ln, lt, nn_new, sc_wel);
+            sc_el = ein;
             if (ein < 0) {
                 status = OUTSIDE; fr = FR_OOB;
             } else {
@@ -605,8 +674,8 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
                 e_out = ein;
                 if (s.kick) {
                     long long pid = st.pid ? st.pid[i] : i;
-                    apply_kick(m, s, pid, realization_of(st, s, i), qn, lon0, lat0, z0p, pre_nn, true, lon_new, lat_new, z_new, status,
-                               nn_out, fr);
+                    apply_kick(m, s, pid, realization_of(st, s, i), qn, lon0, lat0, z0p, pre_nn, true, lon_new, lat_new,
+                               z_new, status, nn_out, fr, s.w_code == 1, sc_el, sc_wel);
                 }
                 if (s.az_on && status == ALIVE)
                     apply_az<T>(m, f, s, st.pid ? st.pid[i] : i, realization_of(st, s, i), nn_out, z_new);
@@ -621,6 +690,7 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
     st.fr[i] = fr;
     if constexpr (WALK) st.elem[i] = e_out;
     mark_anchor(st, i, status, nn_out, node_i);
+    if constexpr (!WALK) mark_scan(st, i, status, sc_el, sc_wel);
 }
 
 }  // namespace kc
