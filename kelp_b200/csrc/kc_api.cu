@@ -2,6 +2,8 @@
 // context, resident mesh / snapshot ring / particle state, the step kernels'
 // launchers and the batch nearest-node query.
 #include <cstdio>
+#include <climits>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -57,6 +59,8 @@ struct kc_ctx {
     int* d_n2e = nullptr;
     int* d_gh_off = nullptr;
     double4* d_gh_tab = nullptr;
+    int* d_pw_off = nullptr;         // pruned windows of the nearest-node scan
+    int* d_pw_pos = nullptr;
     double* d_xyz = nullptr;
     double* d_depth = nullptr;
     double* d_zlev = nullptr;
@@ -278,6 +282,151 @@ __global__ void k_to_half(const float* __restrict__ x, long long n, long long to
 __global__ void k_iota64(long long* out, long long P) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < P) out[i] = i;
+}
+
+// ---- pruned windows of the 3x3 nearest-node scan --------------------------
+//
+// For each grid-hash cell, the nodes of its 3x3 window (mesh.py:1235-1303
+// order) that can be the window's first minimum for some query landing in the
+// cell.  A node n is dropped when, on each of kPwSub x kPwSub sub-rectangles
+// of the cell (grown by kPwPad degrees for the rounding of the cell index),
+// one window node m is closer to every point by more than kPwDelta in squared
+// chord: |q-n|^2 - |q-m|^2 = |n|^2 - |m|^2 + 2 q.(m-n) > kPwDelta, with the
+// minimum of q.(m-n) over the sub-rectangle bounded from below by
+// rect_min_dot.  kPwDelta covers the rounding of the scan's own float64
+// distances (|q|, |n|, |m| within 1e-15 of 1), so every dropped node is
+// strictly farther than the kept winner in the scan's own arithmetic and the
+// first minimum and its distance are unchanged.
+constexpr int kPwCap = 256;          // window positions held per cell; a larger window is kept whole
+constexpr int kPwSub = 4;            // sub-rectangles per cell side
+constexpr double kPwPad = 1e-9;      // degrees added around the cell
+constexpr double kPwDelta = 1e-12;   // required margin in squared chord
+
+// min over the sphere points q(l, p) of [l0, l1] x [p0, p1] (spans < pi,
+// p within [-pi/2, pi/2]) of q . v.  For fixed p, vx cos l + vy sin l is a
+// sinusoid with at most one critical point on the span, a minimum exactly when
+// its derivative goes from negative to positive; cos p >= 0 then leaves
+// g cos p + vz sin p, reduced the same way.
+__device__ double rect_min_dot(double vx, double vy, double vz, const double* cl, const double* sl,
+                               const double* cp, const double* sp) {
+    double g = fmin(vx * cl[0] + vy * sl[0], vx * cl[1] + vy * sl[1]);
+    if (-vx * sl[0] + vy * cl[0] < 0.0 && -vx * sl[1] + vy * cl[1] > 0.0) g = -sqrt(vx * vx + vy * vy);
+    double h = fmin(g * cp[0] + vz * sp[0], g * cp[1] + vz * sp[1]);
+    if (-g * sp[0] + vz * cp[0] < 0.0 && -g * sp[1] + vz * cp[1] > 0.0) h = -sqrt(g * g + vz * vz);
+    return h;
+}
+
+// One thread per cell.  counts[cell] = kept positions rounded up to a
+// multiple of 4 (pass 1, pos == null); pass 2 writes them at off[cell], the
+// tail of the last group repeating its first entry.
+__global__ void __launch_bounds__(kBlock) k_prune_windows(const __grid_constant__ kc::DMesh m, int* counts,
+                                                          const int* off, int* pos_out) {
+    const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= (long long)m.nx * m.ny) return;
+    const int ci = (int)(cell % m.nx), cj = (int)(cell / m.nx);
+    int pos[kPwCap];
+    unsigned keep[kPwCap / 32];
+    int n = 0;
+    bool whole = false;
+    for (int dj = -1; dj <= 1; ++dj) {           // the window in nearest_3x3's order
+        const int cj2 = cj + dj;
+        if (cj2 < 0 || cj2 >= m.ny) continue;
+        for (int di = -1; di <= 1; ++di) {
+            int ci2 = ci + di;
+            if (ci2 < 0) ci2 = m.wrap ? ci2 + m.nx : -1;
+            else if (ci2 >= m.nx) ci2 = m.wrap ? ci2 - m.nx : -1;
+            if (ci2 < 0) continue;
+            const int c2 = cj2 * m.nx + ci2;
+            for (int k = m.gh_off[c2]; k < m.gh_off[c2 + 1]; ++k) {
+                if (n < kPwCap) pos[n] = k;
+                else whole = true;
+                ++n;
+            }
+        }
+    }
+    const double lo0 = m.lon_min + (double)ci * m.cell - kPwPad, lo1 = m.lon_min + (double)(ci + 1) * m.cell + kPwPad;
+    const double la0 = m.lat_min + (double)cj * m.cell - kPwPad, la1 = m.lat_min + (double)(cj + 1) * m.cell + kPwPad;
+    if (!(m.cell < 90.0) || la0 < -90.0 || la1 > 90.0) whole = true;
+    for (int w = 0; w < kPwCap / 32; ++w) keep[w] = whole ? 0xFFFFFFFFu : 0u;
+    if (!whole && n > 1) {
+        const double wl = (lo1 - lo0) / kPwSub, wp = (la1 - la0) / kPwSub;
+        for (int b = 0; b < kPwSub && !whole; ++b) {
+            double cp[2], sp[2];
+            const double p0 = la0 + b * wp, p1 = (b + 1 == kPwSub) ? la1 : la0 + (b + 1) * wp;
+            sincos(p0 * kc::DEG2RAD, &sp[0], &cp[0]);
+            sincos(p1 * kc::DEG2RAD, &sp[1], &cp[1]);
+            const double pc = 0.5 * (p0 + p1);
+            for (int a = 0; a < kPwSub && !whole; ++a) {
+                double cl[2], sl[2];
+                const double l0 = lo0 + a * wl, l1 = (a + 1 == kPwSub) ? lo1 : lo0 + (a + 1) * wl;
+                sincos(l0 * kc::DEG2RAD, &sl[0], &cl[0]);
+                sincos(l1 * kc::DEG2RAD, &sl[1], &cl[1]);
+                double sa, ca, so, co;
+                sincos(pc * kc::DEG2RAD, &sa, &ca);
+                sincos(0.5 * (l0 + l1) * kc::DEG2RAD, &so, &co);
+                const double qx = ca * co, qy = ca * so, qz = sa;
+                int m1 = -1, m2 = -1;              // the two window nodes nearest the centre
+                double d1 = 1e300, d2 = 1e300;
+                for (int j = 0; j < n; ++j) {
+                    const double4 t = m.gh_tab[pos[j]];
+                    const double dx = t.x - qx, dy = t.y - qy, dz = t.z - qz;
+                    const double d = dx * dx + dy * dy + dz * dz;
+                    if (d < d1) { d2 = d1; m2 = m1; d1 = d; m1 = j; }
+                    else if (d < d2) { d2 = d; m2 = j; }
+                }
+                if (m1 < 0) { whole = true; break; }   // non-finite table entries: keep the window
+                const double4 t1 = m.gh_tab[pos[m1]];
+                const double n1 = t1.x * t1.x + t1.y * t1.y + t1.z * t1.z;
+                double4 t2 = t1;
+                double n2 = n1;
+                if (m2 >= 0) { t2 = m.gh_tab[pos[m2]]; n2 = t2.x * t2.x + t2.y * t2.y + t2.z * t2.z; }
+                keep[m1 >> 5] |= 1u << (m1 & 31);
+                for (int j = 0; j < n; ++j) {
+                    if (keep[j >> 5] & (1u << (j & 31))) continue;
+                    const double4 t = m.gh_tab[pos[j]];
+                    const double nn = t.x * t.x + t.y * t.y + t.z * t.z;
+                    bool dom = (nn - n1) + 2.0 * rect_min_dot(t1.x - t.x, t1.y - t.y, t1.z - t.z, cl, sl, cp, sp) >
+                               kPwDelta;
+                    if (!dom && m2 >= 0 && m2 != j)
+                        dom = (nn - n2) + 2.0 * rect_min_dot(t2.x - t.x, t2.y - t.y, t2.z - t.z, cl, sl, cp, sp) >
+                              kPwDelta;
+                    if (!dom) keep[j >> 5] |= 1u << (j & 31);
+                }
+            }
+        }
+    } else if (n <= 1) {
+        whole = true;
+    }
+    if (!pos_out) {
+        int cnt = n;
+        if (!whole) {
+            cnt = 0;
+            for (int w = 0; w < kPwCap / 32; ++w) cnt += __popc(keep[w]);
+        }
+        counts[cell] = (cnt + 3) & ~3;
+        return;
+    }
+    int* out = pos_out + off[cell];
+    int t = 0;
+    if (whole) {                                 // the window as it stands, enumerated again
+        for (int dj = -1; dj <= 1; ++dj) {
+            const int cj2 = cj + dj;
+            if (cj2 < 0 || cj2 >= m.ny) continue;
+            for (int di = -1; di <= 1; ++di) {
+                int ci2 = ci + di;
+                if (ci2 < 0) ci2 = m.wrap ? ci2 + m.nx : -1;
+                else if (ci2 >= m.nx) ci2 = m.wrap ? ci2 - m.nx : -1;
+                if (ci2 < 0) continue;
+                const int c2 = cj2 * m.nx + ci2;
+                for (int k = m.gh_off[c2]; k < m.gh_off[c2 + 1]; ++k) out[t++] = k;
+            }
+        }
+    } else {
+        for (int j = 0; j < n; ++j)
+            if (keep[j >> 5] & (1u << (j & 31))) out[t++] = pos[j];
+    }
+    const int end = off[cell + 1] - off[cell];
+    for (int u = t; u < end; ++u) out[u] = out[t & ~3];
 }
 
 // Sort key of the periodic re-sort: the grid-hash cell of the particle's
@@ -518,7 +667,7 @@ int upload(kc_ctx* c, T** dst, const void* src, size_t count) {
 
 void free_mesh(kc_ctx* c) {
     dfree(c->d_ll); dfree(c->d_en); dfree(c->d_n2e_off); dfree(c->d_n2e); dfree(c->d_gh_off);
-    dfree(c->d_gh_tab); dfree(c->d_xyz); dfree(c->d_depth); dfree(c->d_zlev);
+    dfree(c->d_gh_tab); dfree(c->d_pw_off); dfree(c->d_pw_pos); dfree(c->d_xyz); dfree(c->d_depth); dfree(c->d_zlev);
     dfree(c->d_nsc); dfree(c->d_ecos); dfree(c->d_maxl); dfree(c->d_coastal);
     dfree(c->d_dl_p); dfree(c->d_dl_last); dfree(c->d_dl_bed); dfree(c->d_enb); dfree(c->d_sigma);
     dfree(c->d_cg_corners); dfree(c->d_cg_cell); dfree(c->d_cg_nlev); dfree(c->d_cg_nlev_r); dfree(c->d_cg_L);
@@ -527,6 +676,7 @@ void free_mesh(kc_ctx* c) {
     c->dm.cg = kc::DCgrid{};
     c->dm.dl_p = nullptr; c->dm.dl_last = nullptr; c->dm.dl_bed = nullptr; c->dm.dl_M = 0;
     c->dm.enb = nullptr;
+    c->dm.pw_off = nullptr; c->dm.pw_pos = nullptr;
     c->dm.sigma = nullptr; c->dm.sig = 0;
     c->has_mesh = false;
 }
@@ -603,6 +753,43 @@ int kc_last_error(const kc_ctx* c, char* buf, int buflen) {
 int kc_synchronize(kc_ctx* c) {
     if (!c) return KC_ERR_ARG;
     KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KC_OK;
+}
+
+// The pruned windows of the uploaded grid hash (k_prune_windows): counts,
+// offsets on the host, positions.  KELP_B200_PRUNED_WINDOWS=0 in the
+// environment keeps the whole-window scan.
+int build_pruned_windows(kc_ctx* c) {
+    const char* env = getenv("KELP_B200_PRUNED_WINDOWS");
+    if (env && env[0] == '0') return KC_OK;
+    kc::DMesh& m = c->dm;
+    const long long ncell = (long long)m.nx * m.ny;
+    int* d_cnt = nullptr;
+    KC_CUDA(c, cudaMalloc((void**)&d_cnt, (size_t)ncell * sizeof(int)));
+    k_prune_windows<<<grid_for(ncell), kBlock, 0, c->stream>>>(m, d_cnt, nullptr, nullptr);
+    std::vector<int> cnt((size_t)ncell);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(cnt.data(), d_cnt, (size_t)ncell * sizeof(int), cudaMemcpyDeviceToHost,
+                                              c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(d_cnt);
+    KC_CUDA(c, e);
+    std::vector<int> off((size_t)ncell + 1);
+    long long total = 0;
+    for (long long k = 0; k < ncell; ++k) {
+        off[k] = (int)total;
+        total += cnt[k];
+        if (total > (long long)INT_MAX - 4) return KC_OK;   // too large to index: whole windows
+    }
+    off[ncell] = (int)total;
+    int rc;
+    if ((rc = upload(c, &c->d_pw_off, off.data(), off.size()))) return rc;
+    KC_CUDA(c, cudaMalloc((void**)&c->d_pw_pos, (size_t)std::max<long long>(total, 4) * sizeof(int)));
+    k_prune_windows<<<grid_for(ncell), kBlock, 0, c->stream>>>(m, nullptr, c->d_pw_off, c->d_pw_pos);
+    KC_CUDA(c, cudaGetLastError());
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    m.pw_off = c->d_pw_off;
+    m.pw_pos = c->d_pw_pos;
     return KC_OK;
 }
 
@@ -690,6 +877,7 @@ int kc_mesh_upload(kc_ctx* c, const kc_mesh_desc* d) {
     m.E = E;
     c->max_v = d->max_v;
     c->N = N; c->E = E;
+    if ((rc = build_pruned_windows(c))) return rc;
     c->has_mesh = true;
     ++c->mesh_gen;
     return KC_OK;

@@ -66,6 +66,8 @@ struct DMesh {
     const int* n2e;           // element ids, per node in the reference order
     const int* gh_off;        // (nx*ny+1) CSR offsets of the grid hash
     const double4* gh_tab;    // hash-ordered {x, y, z, node id} unit-sphere table
+    const int* pw_off;        // (nx*ny+1) pruned windows: CSR offsets (multiples of 4), or null
+    const int* pw_pos;        // gh_tab positions of each cell's pruned window, in window scan order
     const double* xyz;        // (N, 3) unit-sphere table by node id
     const double* depth;      // (N) bottom depth, positive down (3-D)
     const int* max_layer;     // (N) deepest valid layer above the node's bottom (3-D)
@@ -183,11 +185,37 @@ __device__ __forceinline__ void scan_cell(const DMesh& m, int cell, double xp, d
 // mesh.py:1235-1303 _grid_hash_nearest_3x3.  Adjacent columns of one row are
 // adjacent in the CSR, so an unclipped, unwrapped row is one contiguous slice
 // (same nodes, same order as three cell scans).
+//
+// A query whose cell needs no clamping scans the cell's pruned window instead
+// (built by k_prune_windows at mesh upload): the window's nodes in the same
+// scan order minus those that another window node is provably closer to at
+// every point of the cell, so the first minimum and its distance are the
+// window's own.  Groups of four positions; a list's tail repeats its group's
+// first entry, which can never win a strict '<' a second time.
 __device__ __forceinline__ int nearest_3x3(const DMesh& m, const Site& q, double& bd2_out) {
-    int ci, cj;
-    gh_cell_of(m, q.lon, q.lat, ci, cj);
     int best = -1;
     double bd2 = 1e30;
+    if (m.pw_off) {
+        const double dlon = gh_fold_dlon(m, q.lon), dlat = q.lat - m.lat_min;
+        if (dlon >= 0.0 && dlat >= 0.0) {
+            const int ti = (int)(dlon / m.cell), tj = (int)(dlat / m.cell);
+            if (ti < m.nx && tj < m.ny) {
+                const int cell = tj * m.nx + ti;
+                const int s = __ldg(&m.pw_off[cell]), e = __ldg(&m.pw_off[cell + 1]);
+                for (int k = s; k < e; k += 4) {
+                    const int4 p = __ldg(reinterpret_cast<const int4*>(m.pw_pos + k));
+                    scan_range(m.gh_tab, p.x, p.x + 1, q.xp, q.yp, q.zp, best, bd2);
+                    scan_range(m.gh_tab, p.y, p.y + 1, q.xp, q.yp, q.zp, best, bd2);
+                    scan_range(m.gh_tab, p.z, p.z + 1, q.xp, q.yp, q.zp, best, bd2);
+                    scan_range(m.gh_tab, p.w, p.w + 1, q.xp, q.yp, q.zp, best, bd2);
+                }
+                bd2_out = bd2;
+                return best;
+            }
+        }
+    }
+    int ci, cj;
+    gh_cell_of(m, q.lon, q.lat, ci, cj);
     for (int dj = -1; dj <= 1; ++dj) {
         int cj2 = cj + dj;
         if (cj2 < 0 || cj2 >= m.ny) continue;
