@@ -134,8 +134,13 @@ __device__ __forceinline__ double pymod360(double x) {
     return r;
 }
 
-// ((x + 180) % 360) - 180
-__device__ __forceinline__ double wrap180(double x) { return pymod360(x + 180.0) - 180.0; }
+// ((x + 180) % 360) - 180.  For 0 <= x + 180 < 360 the remainder is x + 180
+// itself, so the common case is the two roundings alone.
+__device__ __forceinline__ double wrap180(double x) {
+    const double y = x + 180.0;
+    if (y >= 0.0 && y < 360.0) return y - 180.0;
+    return pymod360(y) - 180.0;
+}
 
 // Python integer modulo for a positive divisor.
 __device__ __forceinline__ int imod(int a, int n) {
@@ -581,6 +586,33 @@ __device__ __forceinline__ bool bary_tri(double px, double py, double ax, double
     return true;
 }
 
+// The containment verdict of bary_tri (all three weights >= BARY_EPS)
+// without its divisions where the numerators decide it.  With s the sign of
+// the denominator, a_k = s num_k and d = |denom|, the exact weights are
+// a_k / d (a_3 = d - a_1 - a_2).  All a_k >= 0 (a_3 within its rounding)
+// puts every rounded weight above -1e-15 > BARY_EPS: inside.  One a_k below
+// -1.1e-6 d by more than its rounding puts that rounded weight below
+// BARY_EPS: outside.  Only the band between runs the division itself.  (a3
+// is within 4.4e-16 (d + |a1| + |a2|) of d - a1 - a2, and the rounded w3
+// within 6.6e-16 (d + |a1| + |a2|) / d of the exact third weight.)
+__device__ __forceinline__ bool bary_tri_inside(double px, double py, double ax, double ay, double bx, double by,
+                                                double cx, double cy, bool& nondeg) {
+    const double denom = (by - cy) * (ax - cx) + (cx - bx) * (ay - cy);
+    if (fabs(denom) < AREA_TOL) { nondeg = false; return -1.0 >= BARY_EPS; }
+    nondeg = true;
+    const double n1 = (by - cy) * (px - cx) + (cx - bx) * (py - cy);
+    const double n2 = (cy - ay) * (px - cx) + (ax - cx) * (py - cy);
+    const double d = fabs(denom);
+    const double a1 = denom > 0.0 ? n1 : -n1, a2 = denom > 0.0 ? n2 : -n2;
+    const double a3 = (d - a1) - a2;
+    const double r3 = 2e-15 * (d + fabs(a1) + fabs(a2));   // above the rounding of a3 plus that of w3
+    if (a1 >= 0.0 && a2 >= 0.0 && a3 >= r3) return true;
+    const double lim = 1.1e-6 * d;
+    if (a1 < -lim || a2 < -lim || a3 < -lim - r3) return false;
+    const double w1 = n1 / denom, w2 = n2 / denom, w3 = 1.0 - w1 - w2;
+    return w1 >= BARY_EPS && w2 >= BARY_EPS && w3 >= BARY_EPS;
+}
+
 // mesh.py:2076-2116 _wachspress_weights_quad (product form)
 __device__ __forceinline__ void wachspress_quad(double px, double py, const double* x, const double* y, double* out) {
     double A[4], C[4];
@@ -709,15 +741,13 @@ __device__ __forceinline__ int element_contains_t(const DMesh& m, int c, double 
     const double y2 = (p.la[2] - lat0) * DEG2RAD * R_STD;
     const double px = wrap180(lon_p - lon0) * DEG2RAD * R_STD * cos_lat0;
     const double py = (lat_p - lat0) * DEG2RAD * R_STD;
-    double w1, w2, w3;
-    bool nondeg = bary_tri(px, py, x0, y0, x1, y1, x2, y2, w1, w2, w3);
-    if (w1 >= BARY_EPS && w2 >= BARY_EPS && w3 >= BARY_EPS) return 1;
+    bool nondeg;
+    if (bary_tri_inside(px, py, x0, y0, x1, y1, x2, y2, nondeg)) return 1;
     int verdict = (W_INFO && !nondeg) ? W_UNSURE : miss;
     if (n == 3) return verdict;
     const double x3 = wrap180(p.ln[3] - lon0) * DEG2RAD * R_STD * cos_lat0;
     const double y3 = (p.la[3] - lat0) * DEG2RAD * R_STD;
-    nondeg = bary_tri(px, py, x0, y0, x2, y2, x3, y3, w1, w2, w3);
-    if (w1 >= BARY_EPS && w2 >= BARY_EPS && w3 >= BARY_EPS) return 1;
+    if (bary_tri_inside(px, py, x0, y0, x2, y2, x3, y3, nondeg)) return 1;
     return (W_INFO && !nondeg) ? W_UNSURE : verdict;
 }
 
