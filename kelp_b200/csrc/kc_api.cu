@@ -60,7 +60,7 @@ struct kc_ctx {
     int* d_gh_off = nullptr;
     double4* d_gh_tab = nullptr;
     int* d_pw_off = nullptr;         // pruned windows of the nearest-node scan
-    int* d_pw_pos = nullptr;
+    double4* d_pw_tab = nullptr;
     double* d_xyz = nullptr;
     double* d_depth = nullptr;
     double* d_zlev = nullptr;
@@ -316,11 +316,10 @@ __device__ double rect_min_dot(double vx, double vy, double vz, const double* cl
     return h;
 }
 
-// One thread per cell.  counts[cell] = kept positions rounded up to a
-// multiple of 4 (pass 1, pos == null); pass 2 writes them at off[cell], the
-// tail of the last group repeating its first entry.
+// One thread per cell.  counts[cell] = the kept records (pass 1,
+// tab_out == null); pass 2 copies them to off[cell] in window order.
 __global__ void __launch_bounds__(kBlock) k_prune_windows(const __grid_constant__ kc::DMesh m, int* counts,
-                                                          const int* off, int* pos_out) {
+                                                          const int* off, double4* tab_out) {
     const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (cell >= (long long)m.nx * m.ny) return;
     const int ci = (int)(cell % m.nx), cj = (int)(cell / m.nx);
@@ -397,16 +396,16 @@ __global__ void __launch_bounds__(kBlock) k_prune_windows(const __grid_constant_
     } else if (n <= 1) {
         whole = true;
     }
-    if (!pos_out) {
+    if (!tab_out) {
         int cnt = n;
         if (!whole) {
             cnt = 0;
             for (int w = 0; w < kPwCap / 32; ++w) cnt += __popc(keep[w]);
         }
-        counts[cell] = (cnt + 3) & ~3;
+        counts[cell] = cnt;
         return;
     }
-    int* out = pos_out + off[cell];
+    double4* out = tab_out + off[cell];
     int t = 0;
     if (whole) {                                 // the window as it stands, enumerated again
         for (int dj = -1; dj <= 1; ++dj) {
@@ -418,15 +417,13 @@ __global__ void __launch_bounds__(kBlock) k_prune_windows(const __grid_constant_
                 else if (ci2 >= m.nx) ci2 = m.wrap ? ci2 - m.nx : -1;
                 if (ci2 < 0) continue;
                 const int c2 = cj2 * m.nx + ci2;
-                for (int k = m.gh_off[c2]; k < m.gh_off[c2 + 1]; ++k) out[t++] = k;
+                for (int k = m.gh_off[c2]; k < m.gh_off[c2 + 1]; ++k) out[t++] = m.gh_tab[k];
             }
         }
     } else {
         for (int j = 0; j < n; ++j)
-            if (keep[j >> 5] & (1u << (j & 31))) out[t++] = pos[j];
+            if (keep[j >> 5] & (1u << (j & 31))) out[t++] = m.gh_tab[pos[j]];
     }
-    const int end = off[cell + 1] - off[cell];
-    for (int u = t; u < end; ++u) out[u] = out[t & ~3];
 }
 
 // Sort key of the periodic re-sort: the grid-hash cell of the particle's
@@ -667,7 +664,7 @@ int upload(kc_ctx* c, T** dst, const void* src, size_t count) {
 
 void free_mesh(kc_ctx* c) {
     dfree(c->d_ll); dfree(c->d_en); dfree(c->d_n2e_off); dfree(c->d_n2e); dfree(c->d_gh_off);
-    dfree(c->d_gh_tab); dfree(c->d_pw_off); dfree(c->d_pw_pos); dfree(c->d_xyz); dfree(c->d_depth); dfree(c->d_zlev);
+    dfree(c->d_gh_tab); dfree(c->d_pw_off); dfree(c->d_pw_tab); dfree(c->d_xyz); dfree(c->d_depth); dfree(c->d_zlev);
     dfree(c->d_nsc); dfree(c->d_ecos); dfree(c->d_maxl); dfree(c->d_coastal);
     dfree(c->d_dl_p); dfree(c->d_dl_last); dfree(c->d_dl_bed); dfree(c->d_enb); dfree(c->d_sigma);
     dfree(c->d_cg_corners); dfree(c->d_cg_cell); dfree(c->d_cg_nlev); dfree(c->d_cg_nlev_r); dfree(c->d_cg_L);
@@ -676,7 +673,7 @@ void free_mesh(kc_ctx* c) {
     c->dm.cg = kc::DCgrid{};
     c->dm.dl_p = nullptr; c->dm.dl_last = nullptr; c->dm.dl_bed = nullptr; c->dm.dl_M = 0;
     c->dm.enb = nullptr;
-    c->dm.pw_off = nullptr; c->dm.pw_pos = nullptr;
+    c->dm.pw_off = nullptr; c->dm.pw_tab = nullptr;
     c->dm.sigma = nullptr; c->dm.sig = 0;
     c->has_mesh = false;
 }
@@ -779,17 +776,17 @@ int build_pruned_windows(kc_ctx* c) {
     for (long long k = 0; k < ncell; ++k) {
         off[k] = (int)total;
         total += cnt[k];
-        if (total > (long long)INT_MAX - 4) return KC_OK;   // too large to index: whole windows
+        if (total > (long long)INT_MAX) return KC_OK;   // too large to index: whole windows
     }
     off[ncell] = (int)total;
     int rc;
     if ((rc = upload(c, &c->d_pw_off, off.data(), off.size()))) return rc;
-    KC_CUDA(c, cudaMalloc((void**)&c->d_pw_pos, (size_t)std::max<long long>(total, 4) * sizeof(int)));
-    k_prune_windows<<<grid_for(ncell), kBlock, 0, c->stream>>>(m, nullptr, c->d_pw_off, c->d_pw_pos);
+    KC_CUDA(c, cudaMalloc((void**)&c->d_pw_tab, (size_t)std::max<long long>(total, 1) * sizeof(double4)));
+    k_prune_windows<<<grid_for(ncell), kBlock, 0, c->stream>>>(m, nullptr, c->d_pw_off, c->d_pw_tab);
     KC_CUDA(c, cudaGetLastError());
     KC_CUDA(c, cudaStreamSynchronize(c->stream));
     m.pw_off = c->d_pw_off;
-    m.pw_pos = c->d_pw_pos;
+    m.pw_tab = c->d_pw_tab;
     return KC_OK;
 }
 

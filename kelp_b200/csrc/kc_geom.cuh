@@ -66,8 +66,8 @@ struct DMesh {
     const int* n2e;           // element ids, per node in the reference order
     const int* gh_off;        // (nx*ny+1) CSR offsets of the grid hash
     const double4* gh_tab;    // hash-ordered {x, y, z, node id} unit-sphere table
-    const int* pw_off;        // (nx*ny+1) pruned windows: CSR offsets (multiples of 4), or null
-    const int* pw_pos;        // gh_tab positions of each cell's pruned window, in window scan order
+    const int* pw_off;        // (nx*ny+1) pruned windows: CSR offsets, or null
+    const double4* pw_tab;    // each cell's pruned window: gh_tab records in window scan order
     const double* xyz;        // (N, 3) unit-sphere table by node id
     const double* depth;      // (N) bottom depth, positive down (3-D)
     const int* max_layer;     // (N) deepest valid layer above the node's bottom (3-D)
@@ -192,11 +192,10 @@ __device__ __forceinline__ void scan_cell(const DMesh& m, int cell, double xp, d
 // (same nodes, same order as three cell scans).
 //
 // A query whose cell needs no clamping scans the cell's pruned window instead
-// (built by k_prune_windows at mesh upload): the window's nodes in the same
+// (built by k_prune_windows at mesh upload): the window's records in the same
 // scan order minus those that another window node is provably closer to at
 // every point of the cell, so the first minimum and its distance are the
-// window's own.  Groups of four positions; a list's tail repeats its group's
-// first entry, which can never win a strict '<' a second time.
+// window's own.  The records are copies, one contiguous slice per cell.
 __device__ __forceinline__ int nearest_3x3(const DMesh& m, const Site& q, double& bd2_out) {
     int best = -1;
     double bd2 = 1e30;
@@ -206,14 +205,8 @@ __device__ __forceinline__ int nearest_3x3(const DMesh& m, const Site& q, double
             const int ti = (int)(dlon / m.cell), tj = (int)(dlat / m.cell);
             if (ti < m.nx && tj < m.ny) {
                 const int cell = tj * m.nx + ti;
-                const int s = __ldg(&m.pw_off[cell]), e = __ldg(&m.pw_off[cell + 1]);
-                for (int k = s; k < e; k += 4) {
-                    const int4 p = __ldg(reinterpret_cast<const int4*>(m.pw_pos + k));
-                    scan_range(m.gh_tab, p.x, p.x + 1, q.xp, q.yp, q.zp, best, bd2);
-                    scan_range(m.gh_tab, p.y, p.y + 1, q.xp, q.yp, q.zp, best, bd2);
-                    scan_range(m.gh_tab, p.z, p.z + 1, q.xp, q.yp, q.zp, best, bd2);
-                    scan_range(m.gh_tab, p.w, p.w + 1, q.xp, q.yp, q.zp, best, bd2);
-                }
+                scan_range(m.pw_tab, __ldg(&m.pw_off[cell]), __ldg(&m.pw_off[cell + 1]), q.xp, q.yp, q.zp, best,
+                           bd2);
                 bd2_out = bd2;
                 return best;
             }
