@@ -28,6 +28,8 @@
  *   kc_find_elements_walk <- core.mesh.find_containing_elements_walk
  *                         (src/kelp/core/mesh.py:2631-2712)
  *   kc_elem_neighbors_upload <- core.mesh.build_elem_neighbors (src/kelp/core/mesh.py:2824)
+ *   kc_elem_centers_upload <- the mesh's elem_center_lon / elem_center_lat, read by
+ *                         numerics.interpolate._interp_leastsq_core (interpolate.py:52)
  *   kc_sigma_upload    <- core.mesh.Mesh.sigma with vertical_coord "sigma" (src/kelp/core/mesh.py:63-91)
  *   kc_cgrid_upload    <- the C-grid tables of readers.nemo._mesh.build_nemo_cgrid_mesh
  *                         (src/kelp/readers/nemo/_mesh.py:16-264), read by
@@ -42,7 +44,7 @@
 extern "C" {
 #endif
 
-#define KC_ABI_VERSION 7
+#define KC_ABI_VERSION 8
 
 #define KC_OK 0
 #define KC_ERR_ARG 1      /* invalid argument or combination */
@@ -116,6 +118,9 @@ typedef struct kc_step_args {
                                     times and alpha_end the end time; plain form, no Az */
     int slot_d;
     double pchip_t[4];
+    int uv_lsq;                  /* 1: 2-D u/v on element centres by least squares (uv_interp "leastsq",
+                                    src/kelp/numerics/interpolate.py:52-354): snapshots hold one row of E
+                                    element values; needs kc_elem_centers_upload; plain form */
 } kc_step_args;
 
 /* Beaching / resuspension of one step (src/kelp/tracking.py:199-364,
@@ -225,6 +230,11 @@ int kc_cgrid_upload(kc_ctx* ctx, const kc_cgrid_desc* desc);
  * next; src/kelp/core/mesh.py:2824-2908 build_elem_neighbors).  Needed by the
  * edge walk (elem_search: walk). */
 int kc_elem_neighbors_upload(kc_ctx* ctx, int max_v, const int* elem_neighbors);
+
+/* Element centres of the mesh (E lon, E lat in degrees: mesh.elem_center_lon /
+ * elem_center_lat, src/kelp/core/mesh.py), read by the element-centre
+ * least-squares u/v of kc_step_args.uv_lsq (interpolate.py:52-354). */
+int kc_elem_centers_upload(kc_ctx* ctx, const double* lon, const double* lat);
 
 /* Carried containing elements of the resident particles (P int32, -1 = no
  * guess) for elem_search "walk" (integrators.py:5019-5147, :5415-5608,

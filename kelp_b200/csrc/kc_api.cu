@@ -71,6 +71,7 @@ struct kc_ctx {
     int* d_dl_last = nullptr;
     double* d_dl_bed = nullptr;
     int4* d_enb = nullptr;   // edge neighbours of the compacted rings (kc_elem_neighbors_upload)
+    double2* d_ec = nullptr;  // element centres (kc_elem_centers_upload)
     double* d_sigma = nullptr;   // sigma interfaces (kc_sigma_upload)
     // NEMO C-grid tables (kc_cgrid_upload)
     int4* d_cg_corners = nullptr;
@@ -497,7 +498,7 @@ kc::DBlend<T> blend_of(kc_ctx* c, const kc_step_args* a) {
     f.b = field_of<T>(c->slots[a->slot_b]);
     f.t = field_of<T>(c->slots[a->slot_t]);
     f.alpha0 = a->alpha0;
-    f.n = c->N;
+    f.n = a->uv_lsq ? c->E : c->N;
     f.pchip = a->pchip ? 1 : 0;
     f.d = a->pchip ? field_of<T>(c->slots[a->slot_d]) : kc::DField<T>{};
     for (int k = 0; k < 4; ++k) f.pt[k] = a->pchip ? a->pchip_t[k] : 0.0;
@@ -523,6 +524,9 @@ int launch_step_on(kc_ctx* c, const kc_step_args* a, const kc::DState& st, const
     if (c->dm.cg.on) {   // NEMO C-grid meshes: the exact C-grid steps (plain form)
         if (dtype == KC_F32) launch_cgrid_kernel<float>(c->dm, blend_of<float>(c, a), st, s, a->dims, a->scheme, c->stream);
         else launch_cgrid_kernel<double>(c->dm, blend_of<double>(c, a), st, s, a->dims, a->scheme, c->stream);
+    } else if (a->uv_lsq) {   // element-layout u/v: 2-D least squares (plain form)
+        if (dtype == KC_F32) launch_lsq_kernel<float>(c->dm, blend_of<float>(c, a), st, s, a->scheme, c->stream);
+        else launch_lsq_kernel<double>(c->dm, blend_of<double>(c, a), st, s, a->scheme, c->stream);
     } else if (c->dm.sig && a->dims == 3) {   // sigma meshes: the plain form's s = z / H_p step
         if (dtype == KC_F32) launch_sigma_kernel<float>(c->dm, blend_of<float>(c, a), st, s, a->scheme, c->stream);
         else launch_sigma_kernel<double>(c->dm, blend_of<double>(c, a), st, s, a->scheme, c->stream);
@@ -557,6 +561,14 @@ int check_step(kc_ctx* c, const kc_step_args* a) {
     if (a->kick && !(a->kh_x >= 0.0 && a->kh_y >= 0.0)) return fail(c, KC_ERR_ARG, "kc_step: Kh must be >= 0");
     if (a->precision != KC_PLAIN && a->precision != KC_MIXED)
         return fail(c, KC_ERR_ARG, "kc_step: precision must be KC_PLAIN or KC_MIXED");
+    if (a->uv_lsq) {
+        if (a->uv_lsq != 1) return fail(c, KC_ERR_ARG, "kc_step: uv_lsq must be 0 or 1");
+        if (a->dims != 2) return fail(c, KC_ERR_ARG, "kc_step: least-squares u/v is built for 2-D steps");
+        if (a->precision != KC_PLAIN) return fail(c, KC_ERR_ARG, "kc_step: least-squares u/v runs in the plain form");
+        if (c->dm.cg.on) return fail(c, KC_ERR_ARG, "kc_step: C-grid meshes read face velocities, not element centres");
+        if (!c->dm.ec) return fail(c, KC_ERR_STATE, "kc_step: least-squares u/v needs kc_elem_centers_upload");
+        if (c->has_elem) return fail(c, KC_ERR_ARG, "kc_step: least-squares u/v reads no element (no walk)");
+    }
     if (a->pchip) {
         if (a->precision != KC_PLAIN) return fail(c, KC_ERR_ARG, "kc_step: PCHIP stages run in the plain form");
         if (a->az_kick) return fail(c, KC_ERR_ARG, "kc_step: the Az kick with PCHIP stages is not built");
@@ -623,7 +635,9 @@ int check_step(kc_ctx* c, const kc_step_args* a) {
         if (sl[k] < 0 || sl[k] >= kSlots) return fail(c, KC_ERR_ARG, "kc_step: slot out of range");
         const Slot& s = c->slots[sl[k]];
         if (s.dtype < 0) return fail(c, KC_ERR_STATE, "kc_step: snapshot slot " + std::to_string(sl[k]) + " is empty");
-        if (s.n != c->N) return fail(c, KC_ERR_ARG, "kc_step: snapshot node count differs from the mesh");
+        if (s.n != (a->uv_lsq ? c->E : c->N))
+            return fail(c, KC_ERR_ARG, a->uv_lsq ? "kc_step: least-squares u/v snapshots hold one value per element"
+                                                 : "kc_step: snapshot node count differs from the mesh");
         if (dtype >= 0 && s.dtype != dtype) return fail(c, KC_ERR_ARG, "kc_step: snapshots of mixed element types");
         dtype = s.dtype;
         if (a->precision == KC_PLAIN && dtype == KC_F16)
@@ -673,6 +687,8 @@ void free_mesh(kc_ctx* c) {
     c->dm.cg = kc::DCgrid{};
     c->dm.dl_p = nullptr; c->dm.dl_last = nullptr; c->dm.dl_bed = nullptr; c->dm.dl_M = 0;
     c->dm.enb = nullptr;
+    dfree(c->d_ec);
+    c->dm.ec = nullptr;
     c->dm.pw_off = nullptr; c->dm.pw_tab = nullptr;
     c->dm.sigma = nullptr; c->dm.sig = 0;
     c->has_mesh = false;
@@ -1015,6 +1031,24 @@ int kc_elem_neighbors_upload(kc_ctx* c, int max_v, const int* enb) {
     if (rc) return rc;
     KC_CUDA(c, cudaStreamSynchronize(c->stream));
     c->dm.enb = c->d_enb;
+    ++c->mesh_gen;
+    return KC_OK;
+}
+
+int kc_elem_centers_upload(kc_ctx* c, const double* lon, const double* lat) {
+    if (!c || !lon || !lat) return KC_ERR_ARG;
+    if (!c->has_mesh) return fail(c, KC_ERR_STATE, "kc_elem_centers_upload: no mesh uploaded");
+    const long long E = c->E;
+    std::vector<double2> t((size_t)E);
+    for (long long e = 0; e < E; ++e) t[e] = make_double2(lon[e], lat[e]);
+    KC_CUDA(c, cudaSetDevice(c->device));
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    dfree(c->d_ec);
+    c->dm.ec = nullptr;
+    int rc = upload(c, &c->d_ec, t.data(), t.size());
+    if (rc) return rc;
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->dm.ec = c->d_ec;
     ++c->mesh_gen;
     return KC_OK;
 }
@@ -1657,6 +1691,7 @@ int kc_run_fused(kc_ctx* c, const kc_step_args* steps, int n_steps, const kc_bea
     if (c->dm.sig && steps[0].dims == 3)
         return fail(c, KC_ERR_STATE, "kc_run_fused: sigma meshes step through kc_step / kc_run");
     if (c->dm.cg.on) return fail(c, KC_ERR_STATE, "kc_run_fused: C-grid meshes step through kc_step / kc_run");
+    if (steps[0].uv_lsq) return fail(c, KC_ERR_STATE, "kc_run_fused: least-squares u/v steps through kc_step / kc_run");
     if (c->P == 0) return KC_OK;
     KC_CUDA(c, cudaSetDevice(c->device));
     if ((rc = pin_pid(c))) return rc;

@@ -68,6 +68,7 @@ struct DMesh {
     const double4* gh_tab;    // hash-ordered {x, y, z, node id} unit-sphere table
     const int* pw_off;        // (nx*ny+1) pruned windows: CSR offsets, or null
     const double4* pw_tab;    // each cell's pruned window: gh_tab records in window scan order
+    const double2* ec;        // (E) element centre lon, lat (element-layout u/v), or null
     const double* xyz;        // (N, 3) unit-sphere table by node id
     const double* depth;      // (N) bottom depth, positive down (3-D)
     const int* max_layer;     // (N) deepest valid layer above the node's bottom (3-D)

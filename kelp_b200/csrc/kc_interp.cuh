@@ -773,6 +773,73 @@ static __device__ __noinline__ int walk_locate(const DMesh& m, double lon_p, dou
 }
 
 // ---------------------------------------------------------------------------
+// Element-centre least squares (uv_interp "leastsq", element-layout u/v)
+// ---------------------------------------------------------------------------
+
+// interpolate.py:207-354 _interp_leastsq_core_tinterp (the steady core,
+// :52-205, is its alpha0 = alpha = 0 case): a plane through the time-blended
+// element-centre velocities of the anchor's element ring, in metres centred
+// on the particle, solved by Cramer's rule; its value at the particle.  The
+// sums run in the ring's order; a centre more than 180 degrees of raw
+// longitude away is moved by one turn.  false (and 0, 0) for an empty ring or
+// a normal matrix the scale-relative guard calls singular.  PCHIP stencils
+// take the four-record value per element (the _pchip4 twin, :355-474).
+template <typename T>
+__device__ __forceinline__ bool interp_uv_lsq(const DMesh& m, const DBlend<T>& f, double xp, double yp, int nn,
+                                              double time_dir, double alpha, double& U, double& V) {
+    U = 0.0;
+    V = 0.0;
+    const int s0 = __ldg(&m.n2e_off[nn]), s1 = __ldg(&m.n2e_off[nn + 1]);
+    if (s1 <= s0) return false;
+    const double z0 = cos(yp * DEG2RAD) * SLM;
+    const double xp_m = xp * z0;
+    const double yp_m = yp * SLM;
+    double a11 = 0.0, a12 = 0.0, a13 = 0.0, a22 = 0.0, a23 = 0.0, a33 = 0.0;
+    double fU = 0.0, f1U = 0.0, f2U = 0.0, fV = 0.0, f1V = 0.0, f2V = 0.0;
+    for (int k = s0; k < s1; ++k) {
+        const int e = __ldg(&m.n2e[k]);
+        const double2 c = __ldg(&m.ec[e]);
+        double ex = c.x * z0 - xp_m;
+        const double dlon_raw = c.x - xp;
+        if (dlon_raw > 180.0) ex -= 360.0 * z0;
+        else if (dlon_raw < -180.0) ex += 360.0 * z0;
+        const double ey = c.y * SLM - yp_m;
+        double uv, vv;
+        if (f.pchip) {
+            uv = pchip_at(f.a.u, f.b.u, f.t.u, f.d.u, e, f.pt, alpha);
+            vv = pchip_at(f.a.v, f.b.v, f.t.v, f.d.v, e, f.pt, alpha);
+        } else {
+            uv = tblend((double)__ldg(&f.a.u[e]), (double)__ldg(&f.b.u[e]), (double)__ldg(&f.t.u[e]), f.alpha0, alpha);
+            vv = tblend((double)__ldg(&f.a.v[e]), (double)__ldg(&f.b.v[e]), (double)__ldg(&f.t.v[e]), f.alpha0, alpha);
+        }
+        const double uu = time_dir * uv, vw = time_dir * vv;
+        a11 = a11 + 1.0;
+        a12 = a12 + ex;
+        a13 = a13 + ey;
+        a22 = a22 + ex * ex;
+        a23 = a23 + ex * ey;
+        a33 = a33 + ey * ey;
+        fU = fU + uu;
+        f1U = f1U + uu * ex;
+        f2U = f2U + uu * ey;
+        fV = fV + vw;
+        f1V = f1V + vw * ex;
+        f2V = f2V + vw * ey;
+    }
+    const double a21 = a12, a31 = a13, a32 = a23;
+    const double det = a11 * a22 * a33 + a12 * a23 * a31 + a13 * a21 * a32 - a13 * a22 * a31 - a12 * a21 * a33 -
+                       a11 * a23 * a32;
+    if (fabs(det) < 1e-30 || fabs(det) < 1e-12 * fabs(a11 * a22 * a33)) return false;
+    const double inv = 1.0 / fabs(det);
+    const double b11 = a22 * a33 - a23 * a32;
+    const double b12 = a13 * a32 - a12 * a33;
+    const double b13 = a12 * a23 - a13 * a22;
+    U = (b11 * fU + b12 * f1U + b13 * f2U) * inv;
+    V = (b11 * fV + b12 * f1V + b13 * f2V) * inv;
+    return true;
+}
+
+// ---------------------------------------------------------------------------
 // Counter RNG (diffusion.py:180-249): a keyed SplitMix64 chain over
 // (seed, realization, particle, step, component), split into two open-(0,1)
 // uniforms, Box-Muller to a normal pair.

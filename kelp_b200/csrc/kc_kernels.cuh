@@ -141,6 +141,16 @@ void launch_step_kernel(const kc::DMesh& m, const kc::DBlend<T>& f, const kc::DS
     else launch_step_kernel_t<T, Form, false>(m, f, st, s, dims, scheme, stream);
 }
 
+// 2-D steps with element-centre least-squares u/v (LsqForm), local search
+template <typename T>
+void launch_lsq_kernel(const kc::DMesh& m, const kc::DBlend<T>& f, const kc::DState& st, const kc::DStep& s,
+                       int scheme, cudaStream_t stream) {
+    const unsigned g = (unsigned)((st.P + kBlock - 1) / kBlock);
+    if (scheme == 0) k_step2d<T, 0, kc::LsqForm<T>, false><<<g, kBlock, 0, stream>>>(m, f, st, s);
+    else if (scheme == 1) k_step2d<T, 1, kc::LsqForm<T>, false><<<g, kBlock, 0, stream>>>(m, f, st, s);
+    else k_step2d<T, 2, kc::LsqForm<T>, false><<<g, kBlock, 0, stream>>>(m, f, st, s);
+}
+
 // ---------------------------------------------------------------------------
 // Fused multi-step launch: each thread carries its particles through n steps
 // (particles are independent within and across steps), running the beaching

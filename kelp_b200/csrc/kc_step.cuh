@@ -443,6 +443,18 @@ __device__ __forceinline__ bool stage_uv(const DMesh& m, const DBlend<T>& f, con
 // uvw3 evaluates W even where u/v failed (the caller then discards it).
 // hint >= 0 is the stage's containing element from the edge walk, which
 // replaces the u/v element search; the barycentric W keeps its own search.
+// Element-layout u/v by element-centre least squares (the 2-D fused
+// kernels of integrators.py:1490-2520 and their PCHIP twins :2820-3100):
+// the stage reads the anchor's element ring, no containment; plain float64
+// arithmetic, 2-D only.
+template <typename T>
+struct LsqForm {
+    static __device__ __forceinline__ bool uv2(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
+                                               double lat, int nn, int hint, double alpha, double& U, double& V) {
+        return interp_uv_lsq<T>(m, f, lon, lat, nn, s.time_dir, alpha, U, V);
+    }
+};
+
 template <typename T>
 struct PlainForm {
     static __device__ __forceinline__ bool uv2(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,

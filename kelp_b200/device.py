@@ -169,6 +169,20 @@ class DeviceContext:
                   "kc_elem_neighbors_upload")
         self._enb_key = self._mesh_key
 
+    def ensure_elem_centers(self, mesh) -> None:
+        """Upload the element centres of the resident mesh (the least-squares
+        u/v's stencil points; cached)."""
+        self.ensure_mesh(mesh)
+        if getattr(self, "_ec_key", None) == self._mesh_key:
+            return
+        lon = _c(mesh.elem_center_lon, np.float64)
+        lat = _c(mesh.elem_center_lat, np.float64)
+        E = np.asarray(mesh.elem_nodes).shape[0]
+        if lon.shape != (E,) or lat.shape != (E,):
+            raise ValueError(f"elem_center_lon/lat must hold the mesh's {E} elements, got {lon.shape}, {lat.shape}")
+        self._chk(N.lib().kc_elem_centers_upload(self._ctx, N.ptr(lon), N.ptr(lat)), "kc_elem_centers_upload")
+        self._ec_key = self._mesh_key
+
     def ensure_depth_points(self, mesh, placement: str) -> int:
         """Upload the depth-linear data-point table of ``mesh`` for
         ``placement`` (cached); returns its number of points M."""

@@ -101,6 +101,19 @@ def _check_node_fields(mesh, fields, is3d, placement="layer"):
                                  "(integrators.py:4534-4553)")
 
 
+def _check_element_fields(mesh, fields):
+    """2-D element-layout u/v for the least-squares stages: one value per
+    element (io.py:180 VelocityField, uv_layout 'element')."""
+    E = np.asarray(mesh.elem_nodes).shape[0]
+    for f in fields:
+        if getattr(f, "uv_layout", "element") != "element":
+            raise ValueError("uv_interp 'leastsq' reads element-centre velocities (uv_layout='element'), "
+                             f"got uv_layout={getattr(f, 'uv_layout', None)!r}")
+        u = np.asarray(f.u)
+        if u.shape != (E,) or np.asarray(f.v).shape != u.shape:
+            raise ValueError(f"2-D element-layout u/v need shape ({E},), got {u.shape}")
+
+
 def _az_args(diffusion, vel, is3d, mesh):
     """(use_field, az_const) of the vertical Az kick, or None when it does
     not apply (integrators.py:842-907): the payload's Az field when it carries
@@ -226,9 +239,19 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
         if elem is not None:
             (ctx or default_context()).ensure_elem_neighbors(mesh)
         return _prepare_cgrid(vel, mesh, dt, time_dir, scheme, kw, ctx, kick)
-    if uv_interp != "barycentric":
+    lsq = uv_interp == "leastsq"
+    if uv_interp not in ("barycentric", "leastsq"):
         raise NotImplementedError(f"uv_interp={uv_interp!r} is not built on the CUDA backend; "
-                                  "use 'barycentric' (node-layout velocities)")
+                                  "use 'barycentric' (node-layout velocities) or 'leastsq' (2-D element layout)")
+    if lsq:
+        if _is_3d(vel):
+            raise NotImplementedError("uv_interp 'leastsq' is built for 2-D steps on the CUDA backend "
+                                      "(the 3-D element-layout kernels are not)")
+        if elem is not None:
+            raise NotImplementedError("uv_interp 'leastsq' reads no containing element: elem_search 'walk' "
+                                      "does not apply to it on the CUDA backend")
+        if kw.get("cuda_precision", "plain") != "plain":
+            raise NotImplementedError("uv_interp 'leastsq' runs in the plain form (cuda_precision='plain')")
     # PCHIP: the RK stages are reconstructed from the tracking layer's
     # 4-record stencil; Euler evaluates the payload itself and ignores it
     recon = kw.get("recon") if scheme != "euler" else None
@@ -275,8 +298,11 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
             raise NotImplementedError("an endpoint LazyLerpField (alpha 0) takes the reference's unfused "
                                       "3-D RK2 path, which is not built on the CUDA backend")
     vel_a, vel_b, target, alpha0 = _fields(vel, vel_next)
-    _check_node_fields(mesh, [vel_a, vel_b, target] + (list(recon[0]) if recon is not None else []), is3d,
-                       placement)
+    if lsq:
+        _check_element_fields(mesh, [vel_a, vel_b, target] + (list(recon[0]) if recon is not None else []))
+    else:
+        _check_node_fields(mesh, [vel_a, vel_b, target] + (list(recon[0]) if recon is not None else []), is3d,
+                           placement)
     form = kw.get("cuda_precision", "plain")
     if recon is not None and form != "plain":
         raise NotImplementedError("PCHIP reconstruction runs in the plain form (cuda_precision='plain')")
@@ -297,7 +323,10 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
         ctx.ensure_elem_neighbors(mesh)
     if is3d and placement != "layer":
         ctx.ensure_depth_points(mesh, placement)
+    if lsq:
+        ctx.ensure_elem_centers(mesh)
     a = N.StepArgs()
+    a.uv_lsq = 1 if lsq else 0
     if recon is None:
         sa, sb, st = ctx.slots_for([vel_a, vel_b, target], store)
         a.slot_a, a.slot_b, a.slot_t = sa, sb, st

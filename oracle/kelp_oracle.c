@@ -54,6 +54,7 @@ typedef struct {
     int64_t cg_nynx;
     const double *cg_e2u, *cg_e1v, *cg_area, *cg_zw, *cg_e3b, *cg_e3u, *cg_e3v;
     const int32_t *cg_kbu, *cg_kbv;
+    const double *ec_lon, *ec_lat;   /* (E) element centres (least-squares u/v), or NULL */
 } OMesh;
 
 typedef struct {
@@ -67,6 +68,7 @@ typedef struct {
     const void *ud, *vd, *wd;
     const double* etad;
     double pt[4];
+    int lsq;                            /* 1: 2-D u/v on element centres by least squares (n = E) */
 } OField;
 
 static double fld(const void* p, int f32, int64_t i) {
@@ -1304,10 +1306,50 @@ static void step_cgrid3d(const OMesh* m, const OField* f, const OStep* s, int64_
     status[i] = st; nn[i] = nne; fr[i] = frr;
 }
 
+/* interpolate.py:207-354 _interp_leastsq_core_tinterp (steady: :52-205;
+ * PCHIP: :355-474): the plane a0 + a1 x + a2 y fitted through the anchor's
+ * element-centre velocities (metres, centred on the particle, the seam gate
+ * on the raw longitude difference), Cramer's rule, its value a0 at the
+ * particle; 0 for an empty ring or a singular normal matrix. */
+static int interp_lsq(const OMesh* m, const OField* f, double xp, double yp, int nn, double td, double alpha,
+                      double* U, double* V) {
+    *U = 0.0; *V = 0.0;
+    int count = m->n2e_cnt[nn];
+    if (count < 1) return 0;
+    double z0 = cos(yp * DEG2RAD) * SLM;
+    double xp_m = xp * z0, yp_m = yp * SLM;
+    double s11 = 0, s12 = 0, s13 = 0, s22 = 0, s23 = 0, s33 = 0, fu = 0, fu1 = 0, fu2 = 0, fv = 0, fv1 = 0, fv2 = 0;
+    for (int k = 0; k < count; ++k) {
+        int e = m->n2e[(int64_t)nn * m->max_conn + k];
+        double ex = m->ec_lon[e] * z0 - xp_m;
+        double raw = m->ec_lon[e] - xp;
+        if (raw > 180.0) ex -= 360.0 * z0;
+        else if (raw < -180.0) ex += 360.0 * z0;
+        double ey = m->ec_lat[e] * SLM - yp_m;
+        double uu = td * blend4(f, f->ua, f->ub, f->ut, f->ud, e, alpha);
+        double vv = td * blend4(f, f->va, f->vb, f->vt, f->vd, e, alpha);
+        s11 = s11 + 1.0; s12 = s12 + ex; s13 = s13 + ey;
+        s22 = s22 + ex * ex; s23 = s23 + ex * ey; s33 = s33 + ey * ey;
+        fu = fu + uu; fu1 = fu1 + uu * ex; fu2 = fu2 + uu * ey;
+        fv = fv + vv; fv1 = fv1 + vv * ex; fv2 = fv2 + vv * ey;
+    }
+    double s21 = s12, s31 = s13, s32 = s23;
+    double det = s11 * s22 * s33 + s12 * s23 * s31 + s13 * s21 * s32 - s13 * s22 * s31 - s12 * s21 * s33 -
+                 s11 * s23 * s32;
+    if (fabs(det) < 1e-30 || fabs(det) < 1e-12 * fabs(s11 * s22 * s33)) return 0;
+    double inv = 1.0 / fabs(det);
+    double c11 = s22 * s33 - s23 * s32, c12 = s13 * s32 - s12 * s33, c13 = s12 * s23 - s13 * s22;
+    *U = (c11 * fu + c12 * fu1 + c13 * fu2) * inv;
+    *V = (c11 * fv + c12 * fv1 + c13 * fv2) * inv;
+    return 1;
+}
+
 /* u/v of a 2-D stage: the C-grid core on the surface faces
- * (nemo_cgrid.py:355-388 interp_nemo_cgrid), else the barycentric core */
+ * (nemo_cgrid.py:355-388 interp_nemo_cgrid), the element-centre least
+ * squares, else the barycentric core */
 static int uv2(const OMesh* m, const OField* f, double xp, double yp, int nn, double td, double alpha, double* U,
                double* V) {
+    if (f->lsq) return interp_lsq(m, f, xp, yp, nn, td, alpha, U, V);
     if (m->cg) {
         double Wd;
         int h = t_elem_hint;
@@ -1872,6 +1914,7 @@ typedef struct {
     int64_t cg_nynx;
     const double *cg_e2u, *cg_e1v, *cg_area, *cg_zw, *cg_e3b, *cg_e3u, *cg_e3v;
     const int32_t *cg_kbu, *cg_kbv;
+    const double *ec_lon, *ec_lat;
 } orc_mesh;
 
 typedef struct {
@@ -1885,6 +1928,7 @@ typedef struct {
     const void *ud, *vd, *wd;
     const double* etad;
     double pt[4];
+    int lsq;
 } orc_field;
 
 typedef struct {

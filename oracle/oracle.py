@@ -34,7 +34,7 @@ class OMesh(C.Structure):
                 ("cg_has_e", C.c_int), ("cg_nynx", C.c_int64),
                 ("cg_e2u", C.c_void_p), ("cg_e1v", C.c_void_p), ("cg_area", C.c_void_p), ("cg_zw", C.c_void_p),
                 ("cg_e3b", C.c_void_p), ("cg_e3u", C.c_void_p), ("cg_e3v", C.c_void_p),
-                ("cg_kbu", C.c_void_p), ("cg_kbv", C.c_void_p)]
+                ("cg_kbu", C.c_void_p), ("cg_kbv", C.c_void_p), ("ec_lon", C.c_void_p), ("ec_lat", C.c_void_p)]
 
 
 class OField(C.Structure):
@@ -45,7 +45,7 @@ class OField(C.Structure):
                 ("aza", C.c_void_p), ("azb", C.c_void_p),
                 ("etaa", C.c_void_p), ("etab", C.c_void_p), ("etat", C.c_void_p),
                 ("pchip", C.c_int), ("ud", C.c_void_p), ("vd", C.c_void_p), ("wd", C.c_void_p),
-                ("etad", C.c_void_p), ("pt", C.c_double * 4)]
+                ("etad", C.c_void_p), ("pt", C.c_double * 4), ("lsq", C.c_int)]
 
 
 class OStep(C.Structure):
@@ -150,6 +150,10 @@ class MeshView:
         enb = getattr(mesh, "_elem_neighbors", None)
         self.enb = None if enb is None else c(enb, np.int32)
         s.enb = _p(self.enb)
+        ecl = getattr(mesh, "elem_center_lon", None)
+        self.ec_lon = None if ecl is None else c(ecl, np.float64)
+        self.ec_lat = None if ecl is None else c(mesh.elem_center_lat, np.float64)
+        s.ec_lon, s.ec_lat = _p(self.ec_lon), _p(self.ec_lat)
         self.s = s
         self.mesh = mesh
         self.placement = None
@@ -199,7 +203,7 @@ def _field_arrays(f, dtype):
 
 def step(state, vel, mesh, dt, time_dir, scheme: str, *, vel_next=None, dt_to_next=None, w_interp="nearest",
          diffusion=None, pid=None, release_step=None, global_step=-1, view=None, Dmin=0.5, z0b_min=0.1,
-         recon=None):
+         recon=None, uv_interp="barycentric"):
     """One step of every particle; returns a dict of new arrays
     (lon, lat, z, status, nearest_node, failure_reason, u, v, w, and elem
     when the state carries elements: elem_search walk, the mesh's
@@ -230,6 +234,13 @@ def step(state, vel, mesh, dt, time_dir, scheme: str, *, vel_next=None, dt_to_ne
     of.f32 = 1 if all32 else 0
     of.alpha0 = alpha0
     of.n = view.lon.size
+    if uv_interp == "leastsq":   # 2-D element-centre u/v (interpolate.py:52-354)
+        if view.ec_lon is None:
+            raise ValueError("uv_interp 'leastsq' needs the mesh's element centres")
+        of.lsq = 1
+        of.n = view.ec_lon.size
+    elif uv_interp != "barycentric":
+        raise ValueError(f"uv_interp {uv_interp!r}: the oracle restates 'barycentric' and 'leastsq'")
     etas = [np.ascontiguousarray(getattr(f, "eta", None) if getattr(f, "eta", None) is not None
                                  else np.zeros(view.lon.size), dtype=np.float64) for f in flds]
     of.etaa, of.etab, of.etat = (_p(e) for e in etas[:3])

@@ -43,6 +43,10 @@ class Golden:
         m.vertical_coord = str(self.d["mesh_vertical_coord"]) if "mesh_vertical_coord" in self.d else "zlevel"
         m.metadata = {"exact_nearest": True}
         m._elem_neighbors = self.d.get("mesh_elem_neighbors")
+        if "mesh_elem_center_lon" in self.d:   # element centres (least-squares u/v)
+            m.elem_center_lon = self.d["mesh_elem_center_lon"]
+            m.elem_center_lat = self.d["mesh_elem_center_lat"]
+        self.uv_element = "mesh_uv_element" in self.d
         if "mesh_cgrid_corners" in self.d:   # a NEMO C-grid mesh (build_nemo_cgrid_mesh)
             m._nemo_cgrid = True
             for k in ("corners", "elem_ji", "nlev", "nlev_raster", "zw", "area", "e3b", "kbu", "e3u", "kbv", "e3v",
@@ -61,7 +65,8 @@ class Golden:
             eta = self.d.get(f"snap{i}_eta")
             self.snaps.append(VelocityField(u=self.d[f"snap{i}_u"], v=self.d[f"snap{i}_v"], w=w,
                                             eta=np.zeros(self.d[f"snap{i}_u"].shape[-1]) if eta is None else eta,
-                                            uv_layout="nemo_cgrid" if "mesh_cgrid_corners" in self.d else "node",
+                                            uv_layout=("nemo_cgrid" if "mesh_cgrid_corners" in self.d else
+                                                       "element" if self.uv_element else "node"),
                                             uv_vertical=placement if w is not None else "layer",
                                             az=self.d.get(f"snap{i}_az")))
             i += 1

@@ -636,9 +636,53 @@ def time_fixture():
     print("golden_clock", len(crow))
 
 
+def lsq_fixture():
+    """Element-layout u/v with the element-centre least squares
+    (uv_interp "leastsq", interpolate.py:52-474): the seam-wrapping band and
+    the regional tri/quad mesh, element velocities the mean of the vertex
+    gyre values; steady, time-aware, backward, kicked and PCHIP runs."""
+    T = 86400.0
+
+    def elem_fields(m, snaps):
+        en = np.asarray(m.elem_nodes)
+        valid = en >= 0
+        out = []
+        for sn in snaps:
+            u, v = np.asarray(sn.u), np.asarray(sn.v)
+            ue = np.where(valid, u[np.maximum(en, 0)], 0.0).sum(1) / valid.sum(1)
+            ve = np.where(valid, v[np.maximum(en, 0)], 0.0).sum(1) / valid.sum(1)
+            out.append(RVel(u=ue.astype(u.dtype), v=ve.astype(v.dtype), w=None, eta=np.zeros(m.n_nodes),
+                            uv_layout="element"))
+        return out
+
+    for name, m, P, dt, dtype in (
+            ("golden_lsq_band", S.lattice_mesh(3.0, 72.0, jitter=0.2, land_frac=0.3), 1500, 21600.0, np.float32),
+            ("golden_lsq_quad", S.lattice_mesh(1.0, 15.0, lon_min=-20.0, lon_max=20.0, jitter=0.15, land_frac=0.2,
+                                               quad_frac=0.3), 1200, 10800.0, np.float64)):
+        rm = ref_mesh(m)
+        rf = elem_fields(m, S.gyre_snapshots(m, 5, amp=1.5, dtype=dtype))
+        lon, lat, z, status = particles(m, P, 21, n_off=40, n_dead=30)
+        cases = {"rk2": run_case(rm, rf, lon, lat, z, status, "rk2", dt, T, 12, uv_interp="leastsq"),
+                 "rk4": run_case(rm, rf, lon, lat, z, status, "rk4", dt, T, 12, uv_interp="leastsq"),
+                 "euler": run_case(rm, rf, lon, lat, z, status, "euler", dt, T, 12, uv_interp="leastsq"),
+                 "rk2_bwd": run_case(rm, rf, lon, lat, z, status, "rk2", dt, T, 12, time_dir=-1.0,
+                                     uv_interp="leastsq"),
+                 "rk2_kick": run_case(rm, rf, lon, lat, z, status, "rk2", dt, T, 12, kh=(5.0e4, 5.0e4), seed=5,
+                                      uv_interp="leastsq"),
+                 "rk4_steady": run_case(rm, rf, lon, lat, z, status, "rk4", dt, T, 8, steady=True,
+                                        uv_interp="leastsq"),
+                 "rk2_pchip": run_case(rm, rf, lon, lat, z, status, "rk2", dt, T, 12, uv_interp="leastsq",
+                                       pchip=True, t0=T)}
+        rec = mesh_record(rm)
+        rec.update(elem_center_lon=rm.elem_center_lon, elem_center_lat=rm.elem_center_lat, uv_element=np.array(1))
+        save(name, rec, rf, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
+
+
 if __name__ == "__main__":
     # no argument: every fixture; otherwise the named ones ("steps", "beach")
-    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip"}
+    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq"}
+    if "lsq" in which:
+        lsq_fixture()
     if "steps" in which:
         main()
     if "beach" in which:

@@ -13,7 +13,7 @@ import pytest
 from kelp_b200 import integrators as KI
 from kelp_b200.diffusion import DiffusionStepArgs
 
-from test_oracle_golden import CGRID_CASES, PCHIP_CASES, SIGMA_CASES, diffusion_args, recon_of
+from test_oracle_golden import CGRID_CASES, LSQ_CASES, PCHIP_CASES, SIGMA_CASES, diffusion_args, recon_of, uv_interp_of
 
 pytestmark = pytest.mark.gpu
 
@@ -34,6 +34,7 @@ WALK_CASES += [("golden_3d", c) for c in ("rk2_wbary_walk", "rk4_wnear_walk_kick
 CASES += WALK_CASES
 CASES += SIGMA_CASES
 CASES += CGRID_CASES
+CASES += LSQ_CASES
 CASES += PCHIP_CASES
 
 
@@ -50,7 +51,7 @@ def replay_cuda(g, cname):
     for k in range(int(n_steps)):
         vel, vnext, dtn = g.payload(c["schedule"][k], T)
         diff = diffusion_args(c, k)
-        uv = "nemo_cgrid" if getattr(g.mesh, "_nemo_cgrid", False) else "barycentric"
+        uv = uv_interp_of(g)
         rc = recon_of(g, c, k)
         extra = {} if rc is None else {"recon": rc}
         st = fn(st, vel, g.mesh, dt, td, uv_interp=uv, w_interp=w_interp, vel_next=vnext,

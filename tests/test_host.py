@@ -21,7 +21,7 @@ def test_library_exports_every_declared_symbol():
     missing = [s for s in declared if not hasattr(L, s)]
     assert not missing, missing
     assert declared == set(N.EXPORTS)
-    assert L.kc_abi_version() == N.ABI_VERSION == 7
+    assert L.kc_abi_version() == N.ABI_VERSION == 8
 
 
 def test_node_xyz_host_routine_matches_reference_table(golden):
@@ -81,8 +81,10 @@ def test_unsupported_paths_raise_before_device_work(golden):
     from kelp_b200.diffusion import DiffusionStepArgs
     g, st, sn = _tiny(golden)
     kw = dict(uv_interp="barycentric", vel_next=sn[1], dt_to_next=86400.0)
-    with pytest.raises(NotImplementedError):
+    with pytest.raises(ValueError):   # least squares reads element-layout u/v; these are on nodes
         KI.rk2_step(st, sn[0], g.mesh, 3600.0, 1.0, **{**kw, "uv_interp": "leastsq"})
+    with pytest.raises(NotImplementedError):
+        KI.rk2_step(st, sn[0], g.mesh, 3600.0, 1.0, **{**kw, "uv_interp": "edge_leastsq"})
     with pytest.raises(NotImplementedError):
         KI.rk2_step(st, sn[0], g.mesh, 3600.0, 1.0, **kw,
                     diffusion=DiffusionStepArgs("em", 1.0, 1.0, 0, 0, 0, composition="split_rk"))

@@ -38,6 +38,17 @@ PCHIP_CASES = [("golden_pchip2d", c) for c in ("rk2", "rk4_kick")]
 PCHIP_CASES += [("golden_pchip3d", c) for c in ("rk2_wbary", "rk4_wnear")]
 PCHIP_CASES += [("golden_pchip_sigma", c) for c in ("rk4_wbary", "rk2_wnear")]
 CASES += PCHIP_CASES
+# element-layout u/v by element-centre least squares (uv_interp leastsq, 2-D)
+LSQ_CASES = [(f, c) for f in ("golden_lsq_band", "golden_lsq_quad")
+             for c in ("rk2", "rk4", "euler", "rk2_bwd", "rk2_kick", "rk4_steady", "rk2_pchip")]
+CASES += LSQ_CASES
+
+
+def uv_interp_of(g):
+    """The recorded fixture's u/v interpolator."""
+    if getattr(g.mesh, "_nemo_cgrid", False):
+        return "nemo_cgrid"
+    return "leastsq" if g.uv_element else "barycentric"
 
 
 def recon_of(g, c, k):
@@ -76,7 +87,8 @@ def replay_oracle(g, cname):
         vel, vnext, dtn = g.payload(c["schedule"][k], T)
         diff = diffusion_args(c, k)
         out = O.step(st, vel, g.mesh, dt, td, scheme, vel_next=vnext, dt_to_next=dtn, w_interp=w_interp,
-                     diffusion=diff, view=view, recon=recon_of(g, c, k))
+                     diffusion=diff, view=view, recon=recon_of(g, c, k),
+                     uv_interp="leastsq" if g.uv_element else "barycentric")
         st = st.replace(lon=out["lon"], lat=out["lat"], z=out["z"], status=out["status"],
                         nearest_node=out["nearest_node"], failure_reason=out["failure_reason"],
                         u=out["u"], v=out["v"], w=out["w"], elem=out.get("elem"))
