@@ -28,6 +28,8 @@
  *   kc_find_elements_walk <- core.mesh.find_containing_elements_walk
  *                         (src/kelp/core/mesh.py:2631-2712)
  *   kc_elem_neighbors_upload <- core.mesh.build_elem_neighbors (src/kelp/core/mesh.py:2824)
+ *   kc_field_upload_async <- the snapshot upload of tracking.run_single_realization, overlapped
+ *                         with the steps (tracking.py:2947, the next bracket's records)
  *   kc_elem_centers_upload <- the mesh's elem_center_lon / elem_center_lat, read by
  *                         numerics.interpolate._interp_leastsq_core (interpolate.py:52)
  *   kc_sigma_upload    <- core.mesh.Mesh.sigma with vertical_coord "sigma" (src/kelp/core/mesh.py:63-91)
@@ -44,7 +46,7 @@
 extern "C" {
 #endif
 
-#define KC_ABI_VERSION 8
+#define KC_ABI_VERSION 9
 
 #define KC_OK 0
 #define KC_ERR_ARG 1      /* invalid argument or combination */
@@ -158,6 +160,18 @@ int kc_depth_points_upload(kc_ctx* ctx, int M, const double* p, const int* last,
  * scaled by a power of two so that its largest magnitude is below 2^15. */
 int kc_field_upload(kc_ctx* ctx, int slot, int dtype, long long n_nodes, int n_uv_rows,
                     const void* u, const void* v, int n_w_rows, const void* w);
+
+/* kc_field_upload without waiting: the copies run on the library's copy
+ * stream, after the last launch that read the slot, while steps already
+ * launched keep running; a later step that reads the slot waits for them on
+ * the device.  float32 / float64 u, v, w only (no eta or Az rows).  The host
+ * arrays must stay unchanged until the copy is done (the next kc_synchronize,
+ * or a step that reads the slot has finished); page-locked arrays
+ * (kc_host_alloc) make the copy fully asynchronous, pageable ones are staged
+ * before the call returns.  The prefetch of the tracking loop's next record
+ * (tracking.py:2947 _resolve_time_bracket decides which). */
+int kc_field_upload_async(kc_ctx* ctx, int slot, int dtype, long long n_nodes, int n_uv_rows, const void* u,
+                          const void* v, int n_w_rows, const void* w);
 
 /* The vertical diffusivity of the snapshot in ring slot `slot`: n_rows (= the
  * mesh's interfaces K) x n_nodes values of the slot's element type (float32

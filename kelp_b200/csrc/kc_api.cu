@@ -42,6 +42,10 @@ struct Slot {
     long long n = 0;
     int uv_rows = 0, w_rows = 0, dtype = -1;
     size_t cap_uv = 0, cap_w = 0, cap_su = 0, cap_sv = 0, cap_sw = 0;
+    // kc_field_upload_async: the copy's completion on the copy stream, and
+    // the last launch on the library's stream that read the slot
+    cudaEvent_t ready = nullptr, used = nullptr;
+    bool pending = false, has_used = false;
 };
 
 }  // namespace
@@ -49,6 +53,7 @@ struct Slot {
 struct kc_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;   // kc_field_upload_async (created on first use)
     std::string err;
     // mesh
     bool has_mesh = false;
@@ -519,7 +524,42 @@ void kc_launch_mixed_f16(const kc::DMesh& m, const kc::DBlend<__half>& f, const 
 
 namespace {
 
+// Slots of one step, and the ordering against kc_field_upload_async: the
+// library's stream waits for a pending copy into a slot it reads, and
+// records the slot's last read for the next copy into it to wait on.
+int step_slots(const kc_step_args* a, int* sl) {
+    sl[0] = a->slot_a; sl[1] = a->slot_b; sl[2] = a->slot_t;
+    if (a->pchip) { sl[3] = a->slot_d; return 4; }
+    return 3;
+}
+
+int wait_slots(kc_ctx* c, const int* sl, int n) {
+    for (int k = 0; k < n; ++k) {
+        Slot& s = c->slots[sl[k]];
+        if (s.pending) {
+            KC_CUDA(c, cudaStreamWaitEvent(c->stream, s.ready, 0));
+            s.pending = false;
+        }
+    }
+    return KC_OK;
+}
+
+int mark_slots_used(kc_ctx* c, const int* sl, int n) {
+    if (!c->copy_stream) return KC_OK;
+    for (int k = 0; k < n; ++k) {
+        Slot& s = c->slots[sl[k]];
+        if (!s.used) KC_CUDA(c, cudaEventCreateWithFlags(&s.used, cudaEventDisableTiming));
+        KC_CUDA(c, cudaEventRecord(s.used, c->stream));
+        s.has_used = true;
+    }
+    return KC_OK;
+}
+
 int launch_step_on(kc_ctx* c, const kc_step_args* a, const kc::DState& st, const kc::DStep& s) {
+    int sl[4];
+    const int nsl = step_slots(a, sl);
+    int rc0 = wait_slots(c, sl, nsl);
+    if (rc0) return rc0;
     const int dtype = c->slots[a->slot_a].dtype;
     if (c->dm.cg.on) {   // NEMO C-grid meshes: the exact C-grid steps (plain form)
         if (dtype == KC_F32) launch_cgrid_kernel<float>(c->dm, blend_of<float>(c, a), st, s, a->dims, a->scheme, c->stream);
@@ -541,7 +581,7 @@ int launch_step_on(kc_ctx* c, const kc_step_args* a, const kc::DState& st, const
                                                            c->stream);
     }
     KC_CUDA(c, cudaGetLastError());
-    return KC_OK;
+    return mark_slots_used(c, sl, nsl);
 }
 
 int launch_step(kc_ctx* c, const kc_step_args* a) {
@@ -737,9 +777,13 @@ void kc_destroy(kc_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     free_mesh(c);
     free_particles(c);
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
     for (auto& s : c->slots) {
         dfree(s.u); dfree(s.v); dfree(s.w); dfree(s.su); dfree(s.sv); dfree(s.sw); dfree(s.az); dfree(s.eta);
+        if (s.ready) cudaEventDestroy(s.ready);
+        if (s.used) cudaEventDestroy(s.used);
     }
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     dfree(c->q); dfree(c->qout); dfree(c->d_err); dfree(c->flush); dfree(c->stage);
     for (int k = 0; k < kEvents; ++k) if (c->ev[k]) cudaEventDestroy(c->ev[k]);
     for (int k = 0; k < kChunks; ++k) {
@@ -766,6 +810,7 @@ int kc_last_error(const kc_ctx* c, char* buf, int buflen) {
 int kc_synchronize(kc_ctx* c) {
     if (!c) return KC_ERR_ARG;
     KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (c->copy_stream) KC_CUDA(c, cudaStreamSynchronize(c->copy_stream));
     return KC_OK;
 }
 
@@ -1219,6 +1264,10 @@ int kc_field_upload(kc_ctx* c, int slot, int dtype, long long n_nodes, int n_uv_
     if (n_w_rows > 0 && !w) return fail(c, KC_ERR_ARG, "kc_field_upload: missing w");
     KC_CUDA(c, cudaSetDevice(c->device));
     Slot& s = c->slots[slot];
+    if (c->copy_stream) {   // an asynchronous copy may still be writing the slot
+        KC_CUDA(c, cudaStreamSynchronize(c->copy_stream));
+        s.pending = false;
+    }
     size_t es = dtype == KC_F32 ? 4 : (dtype == KC_F16 ? 2 : 8);
     size_t nuv = (size_t)n_nodes * n_uv_rows * es;
     size_t nw = (size_t)n_nodes * (n_w_rows > 0 ? n_w_rows : 0) * es;
@@ -1247,6 +1296,49 @@ int kc_field_upload(kc_ctx* c, int slot, int dtype, long long n_nodes, int n_uv_
     s.n = n_nodes; s.uv_rows = n_uv_rows; s.w_rows = n_w_rows > 0 ? n_w_rows : 0; s.dtype = dtype;
     s.az_rows = 0;   // a new snapshot carries no Az until kc_field_upload_az
     s.has_eta = false;   // nor a surface until kc_field_upload_eta
+    return KC_OK;
+}
+
+int kc_field_upload_async(kc_ctx* c, int slot, int dtype, long long n_nodes, int n_uv_rows, const void* u,
+                          const void* v, int n_w_rows, const void* w) {
+    if (!c) return KC_ERR_ARG;
+    if (slot < 0 || slot >= kSlots) return fail(c, KC_ERR_ARG, "kc_field_upload_async: slot out of range");
+    if (dtype != KC_F32 && dtype != KC_F64)
+        return fail(c, KC_ERR_ARG, "kc_field_upload_async: float32 or float64 (float16 storage converts synchronously)");
+    if (n_nodes <= 0 || n_uv_rows <= 0 || !u || !v) return fail(c, KC_ERR_ARG, "kc_field_upload_async: empty u/v");
+    if (n_w_rows > 0 && !w) return fail(c, KC_ERR_ARG, "kc_field_upload_async: missing w");
+    KC_CUDA(c, cudaSetDevice(c->device));
+    if (!c->copy_stream) KC_CUDA(c, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    Slot& s = c->slots[slot];
+    const size_t es = dtype == KC_F32 ? 4 : 8;
+    const size_t nuv = (size_t)n_nodes * n_uv_rows * es;
+    const size_t nw = (size_t)n_nodes * (n_w_rows > 0 ? n_w_rows : 0) * es;
+    if (s.cap_uv < nuv || s.cap_w < nw) {   // growing the slot: let every use of it finish first
+        KC_CUDA(c, cudaStreamSynchronize(c->stream));
+        KC_CUDA(c, cudaStreamSynchronize(c->copy_stream));
+        s.pending = false;
+        if (s.cap_uv < nuv) {
+            dfree(s.u); dfree(s.v);
+            KC_CUDA(c, cudaMalloc(&s.u, nuv));
+            KC_CUDA(c, cudaMalloc(&s.v, nuv));
+            s.cap_uv = nuv;
+        }
+        if (s.cap_w < nw) {
+            dfree(s.w);
+            KC_CUDA(c, cudaMalloc(&s.w, nw));
+            s.cap_w = nw;
+        }
+    }
+    if (s.has_used) KC_CUDA(c, cudaStreamWaitEvent(c->copy_stream, s.used, 0));
+    KC_CUDA(c, cudaMemcpyAsync(s.u, u, nuv, cudaMemcpyHostToDevice, c->copy_stream));
+    KC_CUDA(c, cudaMemcpyAsync(s.v, v, nuv, cudaMemcpyHostToDevice, c->copy_stream));
+    if (nw) KC_CUDA(c, cudaMemcpyAsync(s.w, w, nw, cudaMemcpyHostToDevice, c->copy_stream));
+    if (!s.ready) KC_CUDA(c, cudaEventCreateWithFlags(&s.ready, cudaEventDisableTiming));
+    KC_CUDA(c, cudaEventRecord(s.ready, c->copy_stream));
+    s.pending = true;
+    s.n = n_nodes; s.uv_rows = n_uv_rows; s.w_rows = n_w_rows > 0 ? n_w_rows : 0; s.dtype = dtype;
+    s.az_rows = 0;
+    s.has_eta = false;
     return KC_OK;
 }
 
@@ -1600,6 +1692,12 @@ static int run_fused_t(kc_ctx* c, const kc_step_args* steps, int n, const kc_bea
         c->fused_cap = bytes;
     }
     if (!c->fused_ev) KC_CUDA(c, cudaEventCreateWithFlags(&c->fused_ev, cudaEventDisableTiming));
+    for (int j = 0; j < n; ++j) {   // pending asynchronous snapshot copies, waited on before any capture
+        int sl[4];
+        const int nsl = step_slots(&steps[j], sl);
+        int rc = wait_slots(c, sl, nsl);
+        if (rc) return rc;
+    }
     MultiHead* h = (MultiHead*)c->fused_host;
     h->st = state_of(c);
     h->N = c->N;
@@ -1662,6 +1760,12 @@ static int run_fused_t(kc_ctx* c, const kc_step_args* steps, int n, const kc_bea
     }
     KC_CUDA(c, cudaEventRecord(c->fused_ev, c->stream));
     c->fused_ev_pending = true;
+    for (int j = 0; j < n; ++j) {
+        int sl[4];
+        const int nsl = step_slots(&steps[j], sl);
+        int rc = mark_slots_used(c, sl, nsl);
+        if (rc) return rc;
+    }
     return KC_OK;
 }
 

@@ -111,6 +111,7 @@ class DeviceContext:
 
     def synchronize(self):
         self._chk(N.lib().kc_synchronize(self._ctx), "kc_synchronize")
+        self._inflight = []
 
     # -- mesh ---------------------------------------------------------------
     def ensure_mesh(self, mesh) -> None:
@@ -243,15 +244,59 @@ class DeviceContext:
                                                  N.ptr(az)), "kc_field_upload_az")
         self.synchronize()
 
+    def prefetch(self, fields, storage=None, busy=()) -> int:
+        """Start uploading the ``fields`` a coming step will read into free
+        ring slots (or the least recently used ones outside ``busy`` and the
+        last step's), without waiting: kc_field_upload_async, ordered after
+        the launches that read those slots.  float16 storage, eta and Az rows
+        upload at the step instead.  Returns the number of uploads started."""
+        dtype = self._slot_dtype(fields, storage)
+        if dtype == np.dtype(np.float16) or getattr(self, "_sigma", False):
+            return 0
+        keep = set(busy) | set(getattr(self, "_last_slots", ()))
+        started = 0
+        for f in fields:
+            key = (id(f), dtype)
+            if key in self._slots or getattr(f, "az", None) is not None:
+                keep.update(s for k, (s, _) in self._slots.items() if k == key)
+                continue
+            if getattr(f, "uv_layout", None) == "nemo_cgrid":
+                return started
+            used = {s for s, _ in self._slots.values()}
+            free = [s for s in range(N_SLOTS) if s not in used and s not in keep]
+            if free:
+                slot = free[0]
+            else:
+                victims = [k for k, (s, _) in self._slots.items() if s not in keep]
+                if not victims:
+                    return started
+                slot = self._slots.pop(victims[0])[0]
+            u = _c(np.asarray(f.u), dtype)
+            v = _c(np.asarray(f.v), dtype)
+            w = None if getattr(f, "w", None) is None else _c(np.asarray(f.w), dtype)
+            code = N.KC_F32 if dtype == np.dtype(np.float32) else N.KC_F64
+            rows = 1 if u.ndim == 1 else u.shape[0]
+            wrows = 0 if w is None else (1 if w.ndim == 1 else w.shape[0])
+            self._chk(N.lib().kc_field_upload_async(self._ctx, slot, code, u.shape[-1], rows, N.ptr(u), N.ptr(v),
+                                                    wrows, N.ptr(w)), "kc_field_upload_async")
+            self._inflight = getattr(self, "_inflight", []) + [(u, v, w)]   # alive until the copies are done
+            self._slots[key] = (slot, f)
+            keep.add(slot)
+            started += 1
+        return started
+
+    def _slot_dtype(self, fields, storage):
+        all32 = all(np.asarray(f.u).dtype == np.float32 and np.asarray(f.v).dtype == np.float32
+                    and (f.w is None or np.asarray(f.w).dtype == np.float32)
+                    and (getattr(f, "az", None) is None or np.asarray(f.az).dtype == np.float32) for f in fields)
+        return np.dtype(storage) if storage is not None else np.dtype(np.float32 if all32 else np.float64)
+
     def slots_for(self, fields, storage=None) -> list:
         """Ring slots holding ``fields`` (uploading the ones not resident).
         All fields of one step share one element type: float32 only when every
         one of them is float32, unless ``storage`` names it (``np.float16``:
         half storage with per-row scales)."""
-        all32 = all(np.asarray(f.u).dtype == np.float32 and np.asarray(f.v).dtype == np.float32
-                    and (f.w is None or np.asarray(f.w).dtype == np.float32)
-                    and (getattr(f, "az", None) is None or np.asarray(f.az).dtype == np.float32) for f in fields)
-        dtype = np.dtype(storage) if storage is not None else np.dtype(np.float32 if all32 else np.float64)
+        dtype = self._slot_dtype(fields, storage)
         out = []
         pinned = set()
         for f in fields:
@@ -271,6 +316,7 @@ class DeviceContext:
                 self._slots[key] = (slot, f)
             pinned.add(slot)
             out.append(slot)
+        self._last_slots = tuple(out)
         return out
 
     # -- particles ------------------------------------------------------------

@@ -225,6 +225,16 @@ def _prepare_cgrid(vel, mesh, dt, time_dir, scheme, kw, ctx, kick):
     return a, is3d
 
 
+def snapshot_storage(kw):
+    """The snapshot slots' element type of a step's keyword set: float32 or
+    float16 when named (cuda_snapshots), float32 for the mixed form, else
+    None (the payload's own: float32 only when every array is)."""
+    store = {None: None, "f32": np.float32, "f16": np.float16}.get(kw.get("cuda_snapshots", None))
+    if kw.get("cuda_precision", "plain") == "mixed" and store is None:
+        store = np.float32
+    return store
+
+
 def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=None):
     """Validate one step's payload and make it resident on ``ctx`` (mesh,
     depth-point table, snapshot slots); returns ``(StepArgs, is3d)``.  ``scheme``

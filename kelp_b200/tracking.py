@@ -255,13 +255,17 @@ class Tracker:
     (tracking.py:2236-2253: seeded once at the start by the local search
     around the exact anchor unless the initial state carries them).
     ``temporal_reconstruction`` "pchip" hands the RK stages the 4-record
-    monotone-cubic stencil wherever one exists (tracking.py:2415-2436)."""
+    monotone-cubic stencil wherever one exists (tracking.py:2415-2436).
+    ``prefetch`` starts uploading the records of the next few steps as soon
+    as a step is launched (kc_field_upload_async), so an upload runs beside
+    the steps before the record is needed instead of in front of it."""
 
     def __init__(self, mesh, fields: Sequence, file_times, *, integrator: str = "rk2", dt: float,
                  time_dir: float = 1.0, uv_interp: str = "barycentric", w_interp: str = "barycentric",
                  diffusion=None, beaching: Optional[BeachingConfig] = None, on_exhausted: str = "stop",
                  precision: str = "plain", snapshots: Optional[str] = None, sort_every: int = 16,
-                 elem_search: str = "local", temporal_reconstruction: str = "linear", ctx=None):
+                 elem_search: str = "local", temporal_reconstruction: str = "linear", prefetch: bool = True,
+                 ctx=None):
         if integrator not in ("euler", "rk2", "rk4"):
             raise NotImplementedError(f"integrator {integrator!r} is not built on the CUDA backend")
         if on_exhausted not in ("stop", "cycle"):
@@ -275,6 +279,8 @@ class Tracker:
         if temporal_reconstruction not in ("linear", "pchip"):
             raise ValueError(f"temporal_reconstruction must be 'linear' or 'pchip', got {temporal_reconstruction!r}")
         self.pchip = temporal_reconstruction == "pchip"
+        self.prefetch = bool(prefetch)
+        self.prefetch_steps = 4   # steps ahead whose records are uploaded early (at most 4 records)
         self.walk = elem_search == "walk"
         if getattr(mesh, "vertical_coord", "zlevel") == "sigma":
             # the reference's loop hands every sigma step the surfaces at its
@@ -432,6 +438,20 @@ class Tracker:
             if beach_cfg is not None:
                 ctx.beach(beach_args(beach_cfg, realizations[0], g, self.dt))
             sim_time = sim_time_end if sim_time_end is not None else sim_time + self.dt * self.direction
+            if self.prefetch and k + 1 < int(n_steps):
+                # the records of the next few steps upload while this one runs
+                need, seen = [], set()
+                for j in range(min(self.prefetch_steps, int(n_steps) - k - 1)):
+                    nb = resolve_time_bracket(sim_time + j * self.dt * self.direction, ft, self.on_exhausted,
+                                              self.direction, band)
+                    if nb is None:
+                        break
+                    nst = resolve_recon_stencil(nb, ft.size) if (self.pchip and multistage) else None
+                    for i in (nst[0] if nst is not None else (nb[0], nb[1])):
+                        if i not in seen and len(seen) < 4:
+                            seen.add(i)
+                            need.append(self.fields[i])
+                ctx.prefetch(need, KI.snapshot_storage(self.kw))
             done += 1
             s = None
             if recording:

@@ -242,3 +242,36 @@ def test_checkpoint_restart_is_bit_identical(golden, tmp_path):
     np.testing.assert_array_equal(traj["lon"], np.stack(full.records[0].lons[: half // 2]))
     dead = traj["status"] != 1
     assert np.all(np.isnan(traj["vel_u"][dead]))
+
+
+@pytest.mark.parametrize("recon", ["linear", "pchip"])
+def test_prefetched_records_give_the_same_run(golden, recon):
+    """The next step's records uploaded beside the running step
+    (kc_field_upload_async, through the ring's eviction with more records
+    than slots) give the run of uploads made before each step, bit for bit."""
+    from kelp_b200.fields import VelocityField
+    from kelp_b200.device import DeviceContext
+    g = golden("golden_band")
+    recs = [VelocityField(u=np.asarray(s.u) * (1.0 + 0.1 * k), v=np.asarray(s.v) * (1.0 - 0.05 * k), w=None,
+                          eta=np.zeros(np.asarray(s.u).shape[-1]), uv_layout="node")
+            for k in range(3) for s in g.snaps]           # 12 records, more than the 8 ring slots
+    ft = np.arange(len(recs)) * 86400.0
+    diff = Diff(5.0e4, 9)
+    out = {}
+    for pf in (False, True):
+        ctx = DeviceContext(0)
+        try:
+            tr = T.Tracker(g.mesh, recs, ft, integrator="rk4", dt=21600.0, diffusion=diff, sort_every=5,
+                           temporal_reconstruction=recon, prefetch=pf, ctx=ctx)
+            res = tr.run(g.particles(), 40, output_freq=4)
+            out[pf] = (res.final[0], res.records[0])
+        finally:
+            ctx.close()
+    (fa, ra), (fb, rb) = out[False], out[True]
+    for name in ("status", "nearest_node", "failure_reason", "lon", "lat", "u", "v"):
+        np.testing.assert_array_equal(getattr(fa, name), getattr(fb, name), err_msg=name)
+    assert len(ra.times) == len(rb.times) == 10
+    np.testing.assert_array_equal(ra.times, rb.times)
+    for name in ("lons", "lats", "us", "vs", "status", "failure_reason"):
+        for a, b in zip(getattr(ra, name), getattr(rb, name)):
+            np.testing.assert_array_equal(a, b, err_msg=name)
