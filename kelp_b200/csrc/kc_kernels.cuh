@@ -14,6 +14,12 @@
 // HEALPix 3-D step: the path is latency-bound, occupancy beats spills)
 #define KC_STEP_MIN_BLOCKS 8
 #endif
+#ifndef KC_RK2_3D_MIN_BLOCKS
+// the fused 3-D RK2 step (the HEALPix benchmark's kernel): 10 blocks of 128
+// cap it at 48 registers, measured 2 % faster there than 64 (and 40
+// registers no faster)
+#define KC_RK2_3D_MIN_BLOCKS 10
+#endif
 constexpr int kBlock = KC_BLOCK;
 
 // delayed release (release.py:112-129): NOT_RELEASED -> ALIVE at its step
@@ -33,7 +39,7 @@ __global__ void __launch_bounds__(kBlock, KC_STEP_MIN_BLOCKS) k_step2d(const __g
 }
 
 template <typename T, typename Form, bool WALK>
-__global__ void __launch_bounds__(kBlock, KC_STEP_MIN_BLOCKS) k_step3d_rk2(const __grid_constant__ kc::DMesh m, const __grid_constant__ kc::DBlend<T> f, const __grid_constant__ kc::DState st, const __grid_constant__ kc::DStep s) {
+__global__ void __launch_bounds__(kBlock, KC_RK2_3D_MIN_BLOCKS) k_step3d_rk2(const __grid_constant__ kc::DMesh m, const __grid_constant__ kc::DBlend<T> f, const __grid_constant__ kc::DState st, const __grid_constant__ kc::DStep s) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= st.P) return;
     activate(st, s, i);
