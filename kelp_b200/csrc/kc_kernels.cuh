@@ -20,6 +20,11 @@
 // registers no faster)
 #define KC_RK2_3D_MIN_BLOCKS 10
 #endif
+#ifndef KC_UNFUSED_3D_MIN_BLOCKS
+// the 3-D RK4 / Euler step likewise (depth-linear RK4 benchmark: 3-5 % faster
+// at 48 registers; the 2-D and C-grid steps measured slower there)
+#define KC_UNFUSED_3D_MIN_BLOCKS 10
+#endif
 constexpr int kBlock = KC_BLOCK;
 
 // delayed release (release.py:112-129): NOT_RELEASED -> ALIVE at its step
@@ -48,7 +53,7 @@ __global__ void __launch_bounds__(kBlock, KC_RK2_3D_MIN_BLOCKS) k_step3d_rk2(con
 }
 
 template <typename T, int SCHEME, typename Form, bool WALK>
-__global__ void __launch_bounds__(kBlock, KC_STEP_MIN_BLOCKS) k_step3d_unfused(const __grid_constant__ kc::DMesh m,
+__global__ void __launch_bounds__(kBlock, KC_UNFUSED_3D_MIN_BLOCKS) k_step3d_unfused(const __grid_constant__ kc::DMesh m,
                                                            const __grid_constant__ kc::DBlend<T> f,
                                                            const __grid_constant__ kc::DState st,
                                                            const __grid_constant__ kc::DStep s) {
