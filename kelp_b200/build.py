@@ -19,11 +19,12 @@ ROOT = os.path.dirname(HERE)
 BUILD = os.path.join(ROOT, "_build")
 LIB = os.path.join(HERE, "libkelpcuda.so")
 
-CU_SOURCES = ["kc_api.cu", "kc_mixed.cu"]
+CU_SOURCES = ["kc_api.cu", "kc_plain_f64.cu", "kc_plain_f32.cu", "kc_mixed_f32.cu", "kc_mixed_f16.cu",
+              "kc_cgrid_f64.cu", "kc_cgrid_f32.cu", "kc_sigma.cu"]
 CPP_SOURCES = ["kc_host.cpp"]
 HEADERS = ["kc_geom.cuh", "kc_interp.cuh", "kc_step.cuh", "kc_beach.cuh", "kc_mixed.cuh", "kc_kernels.cuh", "kc_sigma.cuh",
            "kc_cgrid.cuh",
-           "kc_host.h"]
+           "kc_launch.h", "kc_host.h"]
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off", "-Xptxas", "-v"]

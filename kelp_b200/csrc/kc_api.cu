@@ -16,7 +16,7 @@
 
 #include "../../include/kelp_cuda.h"
 #include "kc_host.h"
-#include "kc_kernels.cuh"
+#include "kc_launch.h"
 #include "kc_beach.cuh"
 
 namespace {
@@ -512,16 +512,6 @@ kc::DBlend<T> blend_of(kc_ctx* c, const kc_step_args* a) {
 
 }  // namespace
 
-// the mixed-form kernels (kc_mixed.cu)
-void kc_launch_mixed_f32(const kc::DMesh& m, const kc::DBlend<float>& f, const kc::DState& st, const kc::DStep& s,
-                         int dims, int scheme, cudaStream_t stream);
-void kc_launch_multi_mixed_f32(const kc::DMesh& m, const MultiHead* head, const StepPack<float>* packs, long long P,
-                               int dims, int scheme, int block, cudaStream_t stream);
-void kc_launch_multi_mixed_f16(const kc::DMesh& m, const MultiHead* head, const StepPack<__half>* packs, long long P,
-                               int dims, int scheme, int block, cudaStream_t stream);
-void kc_launch_mixed_f16(const kc::DMesh& m, const kc::DBlend<__half>& f, const kc::DState& st,
-                         const kc::DStep& s, int dims, int scheme, cudaStream_t stream);
-
 namespace {
 
 // Slots of one step, and the ordering against kc_field_upload_async: the
@@ -562,23 +552,21 @@ int launch_step_on(kc_ctx* c, const kc_step_args* a, const kc::DState& st, const
     if (rc0) return rc0;
     const int dtype = c->slots[a->slot_a].dtype;
     if (c->dm.cg.on) {   // NEMO C-grid meshes: the exact C-grid steps (plain form)
-        if (dtype == KC_F32) launch_cgrid_kernel<float>(c->dm, blend_of<float>(c, a), st, s, a->dims, a->scheme, c->stream);
-        else launch_cgrid_kernel<double>(c->dm, blend_of<double>(c, a), st, s, a->dims, a->scheme, c->stream);
+        if (dtype == KC_F32) kc_launch_cgrid_f32(c->dm, blend_of<float>(c, a), st, s, a->dims, a->scheme, c->stream);
+        else kc_launch_cgrid_f64(c->dm, blend_of<double>(c, a), st, s, a->dims, a->scheme, c->stream);
     } else if (a->uv_lsq) {   // element-layout u/v: 2-D least squares (plain form)
-        if (dtype == KC_F32) launch_lsq_kernel<float>(c->dm, blend_of<float>(c, a), st, s, a->scheme, c->stream);
-        else launch_lsq_kernel<double>(c->dm, blend_of<double>(c, a), st, s, a->scheme, c->stream);
+        if (dtype == KC_F32) kc_launch_lsq_f32(c->dm, blend_of<float>(c, a), st, s, a->scheme, c->stream);
+        else kc_launch_lsq_f64(c->dm, blend_of<double>(c, a), st, s, a->scheme, c->stream);
     } else if (c->dm.sig && a->dims == 3) {   // sigma meshes: the plain form's s = z / H_p step
-        if (dtype == KC_F32) launch_sigma_kernel<float>(c->dm, blend_of<float>(c, a), st, s, a->scheme, c->stream);
-        else launch_sigma_kernel<double>(c->dm, blend_of<double>(c, a), st, s, a->scheme, c->stream);
+        if (dtype == KC_F32) kc_launch_sigma_f32(c->dm, blend_of<float>(c, a), st, s, a->scheme, c->stream);
+        else kc_launch_sigma_f64(c->dm, blend_of<double>(c, a), st, s, a->scheme, c->stream);
     } else if (a->precision == KC_MIXED) {
         if (dtype == KC_F16) kc_launch_mixed_f16(c->dm, blend_of<__half>(c, a), st, s, a->dims, a->scheme, c->stream);
         else kc_launch_mixed_f32(c->dm, blend_of<float>(c, a), st, s, a->dims, a->scheme, c->stream);
     } else if (dtype == KC_F32) {
-        launch_step_kernel<float, kc::PlainForm<float>>(c->dm, blend_of<float>(c, a), st, s, a->dims, a->scheme,
-                                                         c->stream);
+        kc_launch_plain_f32(c->dm, blend_of<float>(c, a), st, s, a->dims, a->scheme, c->stream);
     } else {
-        launch_step_kernel<double, kc::PlainForm<double>>(c->dm, blend_of<double>(c, a), st, s, a->dims, a->scheme,
-                                                           c->stream);
+        kc_launch_plain_f64(c->dm, blend_of<double>(c, a), st, s, a->dims, a->scheme, c->stream);
     }
     KC_CUDA(c, cudaGetLastError());
     return mark_slots_used(c, sl, nsl);
@@ -1664,9 +1652,12 @@ static void launch_multi(kc_ctx* c, int precision, int dtype, const MultiHead* d
         else
             kc_launch_multi_mixed_f32(c->dm, dh, (const StepPack<float>*)dp, c->P, dims, scheme, c->fused_block,
                                       c->stream);
-    } else if constexpr (!std::is_same<T, __half>::value) {   // the plain form never reads half storage
-        launch_multi_kernel<T, kc::PlainForm<T>>(c->dm, dh, (const StepPack<T>*)dp, c->P, dims, scheme,
-                                                 c->fused_block, c->stream);
+    } else if constexpr (std::is_same<T, double>::value) {   // the plain form never reads half storage
+        kc_launch_multi_plain_f64(c->dm, dh, (const StepPack<double>*)dp, c->P, dims, scheme, c->fused_block,
+                                  c->stream);
+    } else if constexpr (std::is_same<T, float>::value) {
+        kc_launch_multi_plain_f32(c->dm, dh, (const StepPack<float>*)dp, c->P, dims, scheme, c->fused_block,
+                                  c->stream);
     }
 }
 
