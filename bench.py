@@ -17,9 +17,11 @@ port's CPU throughput.  Under torchrun (N > 1) every rank runs its own shard
 of the same per-GPU size (weak scaling: particles are independent, nothing is
 exchanged); the time is the maximum over ranks.  Rank 0 prints one JSON line.
 
-``--impl reference`` times the reference algorithm's CPU implementation on
-this host's cores (the oracle port in oracle/, all host threads) on the same
-workload, metric and unit.
+``--impl reference`` times the reference's own CPU implementation of the step
+on this host's cores, all threads: KELP's Numba step functions from the
+package installed under baseline/_ref (else, or for workloads it cannot be
+driven on here, the oracle C port), on the same workload, metric, unit and
+config, with full-size steps where they fit the time budget.
 """
 from __future__ import annotations
 
@@ -162,29 +164,169 @@ def cpu_baseline(wl, seconds: float = 10.0, n_particles: int = 200_000):
             "sample": f"{steps} steps x {n} particles of {wl.name} (oracle C port, {O.threads()} threads)"}
 
 
+REF_DIR = os.path.join(ROOT, "baseline", "_ref")
+
+
+def _reference_kelp():
+    """The reference package installed under baseline/_ref (pip --target), or
+    None when it (or numba) cannot be imported here."""
+    if not os.path.isdir(os.path.join(REF_DIR, "kelp")):
+        return None
+    if REF_DIR not in sys.path:
+        sys.path.insert(0, REF_DIR)
+    try:
+        import kelp.numerics.integrators  # noqa: F401
+        return sys.modules["kelp"]
+    except Exception:
+        return None
+
+
+class _NumbaReference:
+    """The reference's own Numba step path on the workload: KELP's Mesh +
+    build_search + set_exact_nearest, node-layout VelocityField /
+    LazyLerpField payloads as tracking._build_vel_payload makes them, and
+    kelp.numerics.integrators.rk2_step / rk4_step / euler_step with
+    DiffusionStepArgs for the split kick."""
+
+    kind = "reference"
+
+    def __init__(self, wl):
+        from kelp.core.io import LazyLerpField, VelocityField
+        from kelp.core.mesh import Mesh, build_node_to_elems, build_search, set_exact_nearest
+        from kelp.core.particles import ParticleState
+        from kelp.numerics import integrators as RI
+        from kelp.numerics.diffusion import DiffusionStepArgs
+        import numba
+        self.numba = numba
+        self.wl, self.Lazy, self.State, self.Diff = wl, LazyLerpField, ParticleState, DiffusionStepArgs
+        self.fn = {"rk2": RI.rk2_step, "rk4": RI.rk4_step, "euler": RI.euler_step}[wl.scheme]
+        m = wl.mesh
+        en = np.ascontiguousarray(m.elem_nodes, dtype=np.int32)
+        n2e, cnt = build_node_to_elems(m.n_nodes, en)
+        self.mesh = Mesh(name=wl.name, nodes_lon=np.asarray(m.nodes_lon, np.float64),
+                         nodes_lat=np.asarray(m.nodes_lat, np.float64), depth=np.asarray(m.depth, np.float64),
+                         elem_nodes=en, elem_center_lon=np.asarray(m.elem_center_lon),
+                         elem_center_lat=np.asarray(m.elem_center_lat), node_to_elems=n2e, node_to_elems_count=cnt,
+                         sigma=np.asarray(m.sigma, np.float64))
+        build_search(self.mesh)
+        set_exact_nearest(self.mesh, True)
+        self.fields = [VelocityField(u=f.u, v=f.v, w=f.w, eta=np.asarray(f.eta), uv_layout="node",
+                                     uv_vertical=wl.uv_vertical) for f in wl.snaps]
+
+    def threads(self):
+        return int(self.numba.get_num_threads())
+
+    def state(self, idx):
+        wl, n = self.wl, idx.size
+        return self.State(lon=wl.lon[idx].copy(), lat=wl.lat[idx].copy(), z=wl.z[idx].copy(),
+                          status=np.ones(n, np.int32), nearest_node=np.full(n, -1, np.int32),
+                          failure_reason=np.zeros(n, np.int8))
+
+    def step(self, st, k):
+        wl = self.wl
+        ia, ib, alpha0, dtn = wl.bracket(k)
+        a, b = self.fields[ia], self.fields[ib]
+        vel = a if alpha0 == 0.0 else self.Lazy(a, b, alpha0)
+        kw = dict(uv_interp="barycentric", w_interp=wl.w_interp, vel_next=b, dt_to_next=dtn)
+        if wl.kh is not None:
+            kw["diffusion"] = self.Diff(scheme="uniform", kh_x=wl.kh[0], kh_y=wl.kh[1], seed=wl.seed, real_id=0,
+                                        step_i=k, pid_offset=0)
+        return self.fn(st, vel, self.mesh, wl.dt, 1.0, **kw)
+
+
+class _OraclePort:
+    """The C restatement in oracle/ (the reference's arithmetic, all host
+    threads), for workloads the reference's step cannot be driven on here."""
+
+    kind = "port"
+
+    def __init__(self, wl):
+        from oracle import oracle as O
+        self.O, self.wl, self.view = O, wl, O.MeshView(wl.mesh)
+
+    def threads(self):
+        return int(self.O.threads())
+
+    def state(self, idx):
+        from kelp_b200.particles import make_state
+        wl = self.wl
+        return make_state(wl.lon[idx], wl.lat[idx], wl.z[idx]).replace(failure_reason=np.zeros(idx.size, np.int8))
+
+    def step(self, st, k):
+        from kelp_b200.fields import LazyLerpField
+        from kelp_b200.diffusion import DiffusionStepArgs
+        wl = self.wl
+        ia, ib, alpha0, dtn = wl.bracket(k)
+        a, b = wl.snaps[ia], wl.snaps[ib]
+        vel = a if alpha0 == 0.0 else LazyLerpField(a, b, alpha0)
+        diff = None if wl.kh is None else DiffusionStepArgs("uniform", wl.kh[0], wl.kh[1], wl.seed, 0, k)
+        out = self.O.step(st, vel, wl.mesh, wl.dt, 1.0, wl.scheme, vel_next=b, dt_to_next=dtn, w_interp=wl.w_interp,
+                          diffusion=diff, view=self.view)
+        return st.replace(lon=out["lon"], lat=out["lat"], z=out["z"], status=out["status"],
+                          nearest_node=out["nearest_node"], failure_reason=out["failure_reason"])
+
+
 def run_reference(args):
+    """The reference's CPU implementation of the step on this host's cores, on
+    the GPU arm's workload, metric and unit.  Every timed step is a real step
+    of ``n`` particles (all of the workload's when the run fits the time
+    budget, else an evenly strided sample sized to it); ``ms_per_step`` is the
+    measured time of those steps, nothing is extrapolated."""
     rank, world, _ = env_rank()
     if rank != 0:
         return 0
+    os.environ.setdefault("NUMBA_NUM_THREADS", str(len(os.sched_getaffinity(0))))
     from kelp_b200 import workloads
     wl = workloads.WORKLOADS[args.workload]()
-    from oracle import oracle as O
-    # each step a bounded sample of the workload: the whole --steps/--warmup
-    # run stays within a few minutes of CPU time
-    n_sample = min(wl.P, args.reference_particles)
-    times = [dt for k, n, dt in _oracle_run(wl, n_sample, range(args.warmup + args.steps)) if k >= args.warmup]
+    impl = None
+    if wl.cohorts is None and not getattr(wl.mesh, "_nemo_cgrid", False) and _reference_kelp() is not None:
+        impl = _NumbaReference(wl)
+    if impl is None:
+        impl = _OraclePort(wl)
+    P = wl.P
+    # warm-up 1 compiles (Numba) on a small sample; warm-up 2 times a full step
+    small = np.linspace(0, P - 1, min(P, 20_000)).astype(np.int64)
+    impl.step(impl.state(small), 0)
+    full = np.arange(P)
+    t0 = time.perf_counter()
+    impl.step(impl.state(full), 0)
+    t_full = time.perf_counter() - t0
+    remaining_warm = max(0, args.warmup - 2)
+    n = P
+    if (args.steps + remaining_warm) * t_full > args.reference_budget_s:
+        n = max(1000, int(P * args.reference_budget_s / ((args.steps + remaining_warm) * t_full)))
+    idx = full if n == P else np.linspace(0, P - 1, n).astype(np.int64)
+    st = impl.state(idx)
+    for k in range(remaining_warm):
+        st = impl.step(st, 1 + k)
+    times = []
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        st = impl.step(st, 1 + remaining_warm + k)
+        times.append(time.perf_counter() - t0)
     total = sum(times)
-    value = n_sample * args.steps / total
+    value = n * args.steps / total
+    what = ("the reference's Numba rk2/rk4/euler_step (kelp " + getattr(sys.modules.get("kelp"), "__version__", "?")
+            + ", baseline/_ref)") if impl.kind == "reference" else "the oracle C port of the reference's step"
+    sample = (f"{args.steps} timed steps x {n} of {P} particles"
+              + ("" if n == P else " (evenly strided sample)") + f", {what}, {impl.threads()} threads; "
+              f"a full {P}-particle step measured {t_full:.2f} s")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps * wl.P / n_sample,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": wl.name, **wl.description},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": O.threads(), "kind": "port",
-                             "sample": f"{args.steps} timed steps x {n_sample} of {wl.P} particles "
-                                       f"(oracle C port, {O.threads()} threads)"},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": (value / PUBLISHED[wl.name]) if wl.name in PUBLISHED else None, "dtype": "f64",
+            "data": "synthetic", "config": _config(wl, args, world),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": impl.threads(), "kind": impl.kind,
+                             "sample": sample, "full_step_s": t_full, "particles_per_step": n},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def _config(wl, args, world):
+    """The workload's config dict, the same for both arms."""
+    return {"workload": wl.name, "form": args.form, **wl.description, "particles_per_gpu": wl.P,
+            "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}"}
 
 
 def load_traffic(workload: str, form: str = "plain"):
@@ -511,8 +653,7 @@ def run_b200(args):
                 "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": (value / PUBLISHED[wl.name]) if wl.name in PUBLISHED else None,
                 "dtype": dtype, "data": "synthetic",
-                "config": {"workload": wl.name, "form": args.form, **wl.description, "particles_per_gpu": P,
-                           "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas x{world}"},
+                "config": _config(wl, args, world),
                 "roofline": {"bound": "hbm", "achieved": head["achieved_gbs"], "peak": peak, "unit": "GB/s",
                              "frac": head["achieved_gbs"] / peak, "peak_kind": kind, "traffic": traffic,
                              "algorithmic_bytes_per_particle_step": head["bytes_per_particle_step"]},
@@ -549,8 +690,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sort-every", type=int, default=16, help="re-sort particles by hash cell every N steps")
-    ap.add_argument("--reference-particles", type=int, default=100_000,
-                    help="particles per step of the --impl reference sample")
+    ap.add_argument("--reference-budget-s", type=float, default=150.0,
+                    help="CPU seconds the --impl reference timed steps may take (beyond it: a particle sample)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

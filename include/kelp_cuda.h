@@ -46,7 +46,7 @@
 extern "C" {
 #endif
 
-#define KC_ABI_VERSION 9
+#define KC_ABI_VERSION 10
 
 #define KC_OK 0
 #define KC_ERR_ARG 1      /* invalid argument or combination */
@@ -367,12 +367,26 @@ int kc_find_nearest(kc_ctx* ctx, long long P, const double* lon, const double* l
  * as kc_find_nearest.  No counterpart in the reference. */
 int kc_find_nearest_noalloc(kc_ctx* ctx, long long P, const double* lon, const double* lat, int* out);
 
-/* Counter-RNG normal pairs of the diffusion kick, drawn on the device for
- * particle ids pid_offset .. pid_offset + P - 1 (out: (P, 2)).  The kick
- * kernel draws exactly these numbers; this entry point exposes them for
- * checking (src/kelp/numerics/diffusion.py:233-249 _normal_pair). */
+/* Counter-RNG normal pairs of the diffusion kicks, drawn on the device for
+ * particle ids pid_offset .. pid_offset + P - 1 and key component comp (0 the
+ * horizontal pair, 1 the vertical Az kick) (out: (P, 2)).  The kick kernels
+ * draw exactly these numbers, equal to the reference's bit for bit; this
+ * entry point exposes them for checking
+ * (src/kelp/numerics/diffusion.py:233-249 _normal_pair). */
 int kc_rng_normals(kc_ctx* ctx, long long P, unsigned long long seed, unsigned long long real_id,
-                   unsigned long long step_i, unsigned long long pid_offset, double* out);
+                   unsigned long long step_i, unsigned long long pid_offset, unsigned long long comp, double* out);
+
+/* Digests of the Box-Muller draws over their whole input domain, for
+ * checking the device arithmetic against the reference's: for every 32-bit
+ * index j (u = (j + 1/2) 2^-32, the uniforms of diffusion.py:222-230) the
+ * kick's r = sqrt(-2 log u), cos(2 pi u) and sin(2 pi u), summed as
+ * mix(mix(j) ^ bits(value)) mod 2^64 (mix = one SplitMix64 round) into
+ * out[0], out[1], out[2].  corrected = 0: the correctly rounded values;
+ * 1: as kc_rng_normals and the kicks draw them (moved to the host C
+ * library's value where its log / cos / sin round differently, so the draws
+ * equal the reference's).  A check of _normal_pair
+ * (src/kelp/numerics/diffusion.py:233-249) over all of its inputs. */
+int kc_rng_domain_digests(kc_ctx* ctx, int corrected, unsigned long long* out);
 
 /* Device error word since the last call: bit 0 an exact-search iteration cap
  * was hit, bit 1 kc_beach met a nearest_node outside [-n_nodes, n_nodes) and

@@ -14,15 +14,20 @@
 // correctly rounded values over the whole domain, which the GPU test
 // compares against the device (tests/golden/rng_domain.json).
 //
-// Build and run (all hardware threads, ~10 minutes on 8 cores):
-//   g++ -O2 -mfma -ffp-contract=off -std=c++17 -pthread \
-//       kelp_b200/csrc/gen_rng_exceptions.cpp -o /tmp/gen_rng_exceptions
-//   /tmp/gen_rng_exceptions kelp_b200/csrc/kc_rng_exceptions.bin > tests/golden/rng_domain.json
+// The build (kelp_b200/build.py) compiles and runs it when its output is
+// missing or older than its sources (~6 minutes on 8 cores):
+//   g++ -O2 -mfma -ffp-contract=off -std=c++17 -pthread -Ikelp_b200/csrc \
+//       kelp_b200/csrc/gen_rng_exceptions.cpp -o _build/gen_rng_exceptions
+//   _build/gen_rng_exceptions _build/kc_rng_exceptions.bin > _build/rng_domain.json
+// tests/golden/rng_domain.json holds the digests of the C library this
+// repository's fixtures were made with (glibc 2.39).
 //
-// File format (little-endian): "KCRX", u32 version (1), u32 nA, u32 nB,
-// then nA u32 keys j1 (ascending) and nA i8 deltas of r, then nB u32 keys j2
-// (ascending) and nB u8 codes: bits 0-1 the cos delta, bits 2-3 the sin
-// delta (0 none, 1 = +1, 2 = -1).
+// File format (little-endian), the device layout (kc::DRngX): "KCRX",
+// u32 version (2), u32 nA, u32 nB, u32 bucket bits (20); then for table a
+// (r) and table b (cos / sin): 2^20 + 1 u32 bucket offsets (bucket = j >> 12)
+// and n u16 entries (j & 0xfff) << 4 | code, ascending within a bucket.
+// Codes: table a 1 = +1, 2 = -1 (the library's r bits minus the correctly
+// rounded ones); table b bits 0-1 the cos delta, bits 2-3 the sin delta.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -60,7 +65,7 @@ static int delta_code(double lib, double cr, uint64_t j, const char* what) {
 struct Part {
     uint64_t dr_lib = 0, dr_cr = 0, dc_lib = 0, dc_cr = 0, ds_lib = 0, ds_cr = 0;
     uint64_t ambiguous = 0;
-    std::vector<std::pair<uint32_t, int8_t>> a;
+    std::vector<std::pair<uint32_t, uint8_t>> a;
     std::vector<std::pair<uint32_t, uint8_t>> b;
 };
 
@@ -85,7 +90,7 @@ int main(int argc, char** argv) {
                 const double r_cr = std::sqrt(-2.0 * kc::cr::log_cr_checked(u, &amb));
                 p.ambiguous += amb;
                 const int rc = delta_code(r_lib, r_cr, j, "r");
-                if (rc) p.a.push_back({(uint32_t)j, (int8_t)(rc == 1 ? 1 : -1)});
+                if (rc) p.a.push_back({(uint32_t)j, (uint8_t)rc});
                 p.dr_lib += term(j, r_lib);
                 p.dr_cr += term(j, r_cr);
                 const double th2 = TWO_PI * u;
@@ -112,12 +117,24 @@ int main(int argc, char** argv) {
     }
     FILE* f = std::fopen(argv[1], "wb");
     if (!f) return 1;
-    const uint32_t hdr[4] = {0x5852434bu /* "KCRX" */, 1u, (uint32_t)all.a.size(), (uint32_t)all.b.size()};
-    std::fwrite(hdr, 4, 4, f);
-    for (auto& e : all.a) std::fwrite(&e.first, 4, 1, f);
-    for (auto& e : all.a) std::fwrite(&e.second, 1, 1, f);
-    for (auto& e : all.b) std::fwrite(&e.first, 4, 1, f);
-    for (auto& e : all.b) std::fwrite(&e.second, 1, 1, f);
+    const uint32_t BITS = 20, NB = 1u << BITS;
+    const uint32_t hdr[5] = {0x5852434bu /* "KCRX" */, 2u, (uint32_t)all.a.size(), (uint32_t)all.b.size(), BITS};
+    std::fwrite(hdr, 4, 5, f);
+    auto put = [&](const auto& list) {
+        std::vector<uint32_t> off(NB + 1, 0);
+        std::vector<uint16_t> ent(list.size());
+        for (size_t k = 0; k < list.size(); ++k) {
+            const uint32_t j = list[k].first;
+            const unsigned code = (unsigned)list[k].second;
+            ent[k] = (uint16_t)(((j & 0xFFFu) << 4) | (code & 15u));
+            off[(j >> 12) + 1]++;
+        }
+        for (uint32_t b = 0; b < NB; ++b) off[b + 1] += off[b];
+        std::fwrite(off.data(), 4, off.size(), f);
+        std::fwrite(ent.data(), 2, ent.size(), f);
+    };
+    put(all.a);
+    put(all.b);
     std::fclose(f);
     std::printf("{\n  \"libc\": \"glibc %s\",\n  \"domain\": %llu,\n  \"ambiguous\": %llu,\n"
                 "  \"exceptions_r\": %zu,\n  \"exceptions_trig\": %zu,\n"

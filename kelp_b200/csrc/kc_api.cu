@@ -89,6 +89,8 @@ struct kc_ctx {
     int *d_cg_kbu = nullptr, *d_cg_kbv = nullptr;
     int max_v = 0;
     int* d_err = nullptr;
+    unsigned *d_rx_a_off = nullptr, *d_rx_b_off = nullptr;   // RNG exception tables (kc::DRngX)
+    unsigned short *d_rx_a = nullptr, *d_rx_b = nullptr;
     kc::DMesh dm{};
     // snapshot ring
     Slot slots[kSlots];
@@ -201,6 +203,7 @@ kc::DStep step_of(const kc_step_args* a) {
     s.global_step = a->global_step;
     s.az_on = a->az_kick; s.az_field = a->az_field; s.az_const = a->az_const;
     s.Dmin = a->Dmin; s.z0b_min = a->z0b_min; s.alpha_end = a->alpha_end;
+    s.rng_exact = a->precision == KC_PLAIN ? 1 : 0;
     return s;
 }
 
@@ -234,14 +237,62 @@ __global__ void __launch_bounds__(kBlock) k_contain(const __grid_constant__ kc::
     out[i] = kc::contain_local(m, lon, lat, a);
 }
 
-__global__ void __launch_bounds__(kBlock) k_normals(long long P, unsigned long long seed, unsigned long long real_id,
-                                                    unsigned long long step, unsigned long long pid0, double* out) {
+__global__ void __launch_bounds__(kBlock) k_normals(const kc::DRngX x, long long P, unsigned long long seed,
+                                                    unsigned long long real_id, unsigned long long step,
+                                                    unsigned long long pid0, unsigned long long comp, double* out) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P) return;
     double g1, g2;
-    kc::normal_pair(seed, real_id, (unsigned long long)i + pid0, step, 0ull, g1, g2);
+    kc::normal_pair(x, seed, real_id, (unsigned long long)i + pid0, step, comp, g1, g2);
     out[2 * i] = g1;
     out[2 * i + 1] = g2;
+}
+
+// Order-free digests over the whole Box-Muller input domain j = 0 .. 2^32-1:
+// the sums of mix(mix(j) ^ bits(v)) of v = sqrt(-2 log u), cos(2 pi u) and
+// sin(2 pi u) at u = (j + 1/2) 2^-32, each as normal_pair evaluates it (with
+// the exception tables when x carries them).  out[0..2] += r, cos, sin.
+__device__ __forceinline__ unsigned long long rng_mix(unsigned long long v) {
+    v += 0x9E3779B97F4A7C15ull;
+    v = (v ^ (v >> 30)) * 0xBF58476D1CE4E5B9ull;
+    v = (v ^ (v >> 27)) * 0x94D049BB133111EBull;
+    return v ^ (v >> 31);
+}
+
+__global__ void __launch_bounds__(256) k_rng_domain(const kc::DRngX x, unsigned long long* out) {
+    const double INV = 1.0 / 4294967296.0, HALF = 0.5 * INV, TWO_PI = 2.0 * 3.141592653589793;
+    unsigned long long dr = 0, dc = 0, ds = 0;
+    const unsigned long long n = 1ull << 32;
+    for (unsigned long long j = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+         j += (unsigned long long)gridDim.x * blockDim.x) {
+        const double u = (double)j * INV + HALF;
+        double r = sqrt(-2.0 * kc::cr::log_cr(u));
+        double sn, cs;
+        kc::cr::sincos_cr(TWO_PI * u, &sn, &cs);
+        if (x.a_off) {
+            const unsigned ca = kc::rngx_code(x.a_off, x.a, (unsigned)j);
+            if (ca) r = kc::rngx_bump(r, ca);
+        }
+        if (x.b_off) {
+            const unsigned cb = kc::rngx_code(x.b_off, x.b, (unsigned)j);
+            if (cb & 3u) cs = kc::rngx_bump(cs, cb & 3u);
+            if (cb >> 2) sn = kc::rngx_bump(sn, cb >> 2);
+        }
+        const unsigned long long mj = rng_mix(j);
+        dr += rng_mix(mj ^ (unsigned long long)__double_as_longlong(r));
+        dc += rng_mix(mj ^ (unsigned long long)__double_as_longlong(cs));
+        ds += rng_mix(mj ^ (unsigned long long)__double_as_longlong(sn));
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        dr += __shfl_down_sync(0xFFFFFFFFu, dr, o);
+        dc += __shfl_down_sync(0xFFFFFFFFu, dc, o);
+        ds += __shfl_down_sync(0xFFFFFFFFu, ds, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&out[0], dr);
+        atomicAdd(&out[1], dc);
+        atomicAdd(&out[2], ds);
+    }
 }
 
 __global__ void __launch_bounds__(kBlock) k_beach(const __grid_constant__ kc::DMesh m,
@@ -755,6 +806,24 @@ int kc_create(int device, kc_ctx** out) {
         return KC_ERR_CUDA;
     }
     for (int k = 0; k < kEvents; ++k) cudaEventCreate(&c->ev[k]);
+    // the RNG's exception tables, resident for the context's life
+    {
+        kc_host::RngTables t;
+        if (!kc_host::rng_exception_tables(t)) {
+            kc_destroy(c);
+            return KC_ERR_STATE;
+        }
+        auto put = [&](void** d, const void* h, size_t bytes) {
+            return cudaMalloc(d, bytes > 0 ? bytes : 4) == cudaSuccess &&
+                   (bytes == 0 || cudaMemcpy(*d, h, bytes, cudaMemcpyHostToDevice) == cudaSuccess);
+        };
+        if (!put((void**)&c->d_rx_a_off, t.a_off, t.n_off * 4) || !put((void**)&c->d_rx_a, t.a, t.na * 2) ||
+            !put((void**)&c->d_rx_b_off, t.b_off, t.n_off * 4) || !put((void**)&c->d_rx_b, t.b, t.nb * 2)) {
+            kc_destroy(c);
+            return KC_ERR_CUDA;
+        }
+        c->dm.rx = kc::DRngX{c->d_rx_a_off, c->d_rx_a, c->d_rx_b_off, c->d_rx_b};
+    }
     *out = c;
     return KC_OK;
 }
@@ -773,6 +842,7 @@ void kc_destroy(kc_ctx* c) {
     }
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     dfree(c->q); dfree(c->qout); dfree(c->d_err); dfree(c->flush); dfree(c->stage);
+    dfree(c->d_rx_a_off); dfree(c->d_rx_a); dfree(c->d_rx_b_off); dfree(c->d_rx_b);
     for (int k = 0; k < kEvents; ++k) if (c->ev[k]) cudaEventDestroy(c->ev[k]);
     for (int k = 0; k < kChunks; ++k) {
         if (c->ev_in[k]) cudaEventDestroy(c->ev_in[k]);
@@ -1963,18 +2033,39 @@ int kc_find_nearest_noalloc(kc_ctx* c, long long P, const double* lon, const dou
 }
 
 int kc_rng_normals(kc_ctx* c, long long P, unsigned long long seed, unsigned long long real_id,
-                   unsigned long long step_i, unsigned long long pid_offset, double* out) {
+                   unsigned long long step_i, unsigned long long pid_offset, unsigned long long comp, double* out) {
     if (!c) return KC_ERR_ARG;
     if (P < 0 || (P > 0 && !out)) return fail(c, KC_ERR_ARG, "kc_rng_normals: arrays");
     if (P == 0) return KC_OK;
     KC_CUDA(c, cudaSetDevice(c->device));
     double* d = nullptr;
     KC_CUDA(c, cudaMallocAsync((void**)&d, (size_t)P * 16, c->stream));
-    k_normals<<<grid_for(P), kBlock, 0, c->stream>>>(P, seed, real_id, step_i, pid_offset, d);
+    k_normals<<<grid_for(P), kBlock, 0, c->stream>>>(c->dm.rx, P, seed, real_id, step_i, pid_offset, comp, d);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, (size_t)P * 16, cudaMemcpyDeviceToHost, c->stream);
     cudaFreeAsync(d, c->stream);
     if (e != cudaSuccess) return fail(c, KC_ERR_CUDA, std::string("kc_rng_normals: ") + cudaGetErrorString(e));
+    KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KC_OK;
+}
+
+int kc_rng_domain_digests(kc_ctx* c, int corrected, unsigned long long* out) {
+    if (!c || !out) return KC_ERR_ARG;
+    if (corrected != 0 && corrected != 1) return fail(c, KC_ERR_ARG, "kc_rng_domain_digests: corrected is 0 or 1");
+    KC_CUDA(c, cudaSetDevice(c->device));
+    unsigned long long* d = nullptr;
+    KC_CUDA(c, cudaMallocAsync((void**)&d, 3 * sizeof(unsigned long long), c->stream));
+    cudaError_t e = cudaMemsetAsync(d, 0, 3 * sizeof(unsigned long long), c->stream);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    const kc::DRngX x = corrected ? c->dm.rx : kc::DRngX{nullptr, nullptr, nullptr, nullptr};
+    if (e == cudaSuccess) {
+        k_rng_domain<<<(unsigned)sms * 8, 256, 0, c->stream>>>(x, d);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream);
+    cudaFreeAsync(d, c->stream);
+    if (e != cudaSuccess) return fail(c, KC_ERR_CUDA, std::string("kc_rng_domain_digests: ") + cudaGetErrorString(e));
     KC_CUDA(c, cudaStreamSynchronize(c->stream));
     return KC_OK;
 }

@@ -57,6 +57,19 @@ struct DCgrid {
 
 // Resident mesh: node table, element table, node->element CSR, grid hash and
 // the host-evaluated trigonometric tables.
+// Box-Muller exception tables (built from the whole-domain scan of
+// gen_rng_exceptions.cpp): the uniforms' 32-bit indices j at which the host
+// C library's r = sqrt(-2 log u1) (table a) or cos / sin (2 pi u2) (table b)
+// differ from the correctly rounded values, bucketed by j >> 12:
+// off[b] .. off[b+1] index 16-bit entries (j & 0xfff) << 4 | code,
+// ascending.  Null pointers: the correctly rounded draws.
+struct DRngX {
+    const unsigned* a_off;
+    const unsigned short* a;
+    const unsigned* b_off;
+    const unsigned short* b;
+};
+
 struct DMesh {
     const double2* ll;        // (N) node lon, lat in degrees
     const double2* nsc;       // (N) sin, cos of the node latitude (radians)
@@ -84,6 +97,7 @@ struct DMesh {
     double cell, lon_min, lat_min, r_earth;
     int nx, ny, wrap, far_rows, K, exact, dl_M;
     int* err;                 // device error word
+    DRngX rx;                 // the RNG's exception tables (set by kc_create)
 };
 
 // Trigonometry of one evaluation site (a query position).

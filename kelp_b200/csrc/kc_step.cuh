@@ -49,6 +49,7 @@ struct DStep {
     double az_const;
     double Dmin, z0b_min;      // sigma column floor and bed clearance
     double alpha_end;          // blend fraction of the end-of-step surface (sigma)
+    int rng_exact;             // draws moved to the reference's C-library values (the plain form)
 };
 
 // displacement metric z0 = max(cos(lat) * 111120, 1) (integrators.py:2563-2565),
@@ -155,7 +156,7 @@ static __device__ __noinline__ void apply_kick(const DMesh& m, const DStep& s, l
                                         double& lon, double& lat, double& z, int& status, int& nn, signed char& fr,
                                         bool want_w, int& kel, int& kwel) {
     double g1, g2;
-    normal_pair(s.seed, rid, (unsigned long long)pid + s.pid_offset, s.step_i, 0ull, g1, g2);
+    normal_pair(s.rng_exact ? m.rx : DRngX{}, s.seed, rid, (unsigned long long)pid + s.pid_offset, s.step_i, 0ull, g1, g2);
     double abs_dt = s.dt >= 0.0 ? s.dt : -s.dt;
     double sq = sqrt(abs_dt);
     double sx = sqrt(2.0 * s.kh_x);
@@ -285,7 +286,7 @@ __device__ __noinline__ void apply_az(const DMesh& m, const DBlend<T>& f, const 
         g = 0.0;
     }
     double xi, unused;
-    normal_pair(s.seed, rid, (unsigned long long)pid + s.pid_offset, s.step_i, 1ull, xi, unused);
+    normal_pair(s.rng_exact ? m.rx : DRngX{}, s.seed, rid, (unsigned long long)pid + s.pid_offset, s.step_i, 1ull, xi, unused);
     const double sdt = s.time_dir * s.dt;
     const double abs_dt = sdt >= 0.0 ? sdt : -sdt;
     const double dz = g * abs_dt + sqrt(2.0 * az * abs_dt) * xi;

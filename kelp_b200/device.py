@@ -30,9 +30,8 @@ def mesh_desc(mesh, keep: list) -> N.MeshDesc:
     need a dtype conversion are appended to ``keep`` so they outlive the call."""
     if getattr(mesh, "_gh_offsets", None) is None:
         raise RuntimeError("mesh has no grid hash: call build_search(mesh) first")
-    xyz = getattr(mesh, "_node_xyz", None)
-    if xyz is None:
-        raise RuntimeError("grid hash without its node coordinate table: call build_search(mesh)")
+    from .mesh import ensure_node_xyz
+    xyz = ensure_node_xyz(mesh)
 
     def k(a, dt):
         a = _c(a, dt)
@@ -115,6 +114,9 @@ class DeviceContext:
 
     # -- mesh ---------------------------------------------------------------
     def ensure_mesh(self, mesh) -> None:
+        from .mesh import ensure_node_xyz
+        if getattr(mesh, "_gh_offsets", None) is not None:
+            ensure_node_xyz(mesh)
         key = (id(mesh), id(mesh._gh_offsets), id(getattr(mesh, "_node_xyz", None)),
                bool((mesh.metadata or {}).get("exact_nearest", False)))
         if self._mesh_key == key and self._mesh_ref is mesh:
@@ -510,11 +512,19 @@ class DeviceContext:
                   "kc_find_nearest")
         return out
 
-    def rng_normals(self, P, seed, real_id, step_i, pid_offset=0) -> np.ndarray:
+    def rng_normals(self, P, seed, real_id, step_i, pid_offset=0, comp=0) -> np.ndarray:
         out = np.empty((int(P), 2))
         self._chk(N.lib().kc_rng_normals(self._ctx, int(P), int(seed), int(real_id), int(step_i), int(pid_offset),
-                                         N.ptr(out)), "kc_rng_normals")
+                                         int(comp), N.ptr(out)), "kc_rng_normals")
         return out
+
+    def rng_domain_digests(self, corrected: bool = True) -> tuple:
+        """Digests of r, cos and sin of the Box-Muller draws over all 2^32
+        uniforms (kc_rng_domain_digests)."""
+        out = np.zeros(3, np.uint64)
+        self._chk(N.lib().kc_rng_domain_digests(self._ctx, 1 if corrected else 0, N.ptr(out)),
+                  "kc_rng_domain_digests")
+        return tuple(int(v) for v in out)
 
     def device_errors(self) -> int:
         w = C.c_int(0)

@@ -149,6 +149,16 @@ def node_xyz_table(nodes_lon: np.ndarray, nodes_lat: np.ndarray) -> np.ndarray:
     return out
 
 
+def ensure_node_xyz(mesh) -> np.ndarray:
+    """The mesh's unit-sphere node table, computed on first use (KELP's
+    ``build_search`` fills it at once; here building the grid hash does not
+    load the native library, so the arrays of a mesh can be prepared without
+    it)."""
+    if getattr(mesh, "_node_xyz", None) is None:
+        mesh._node_xyz = node_xyz_table(mesh.nodes_lon, mesh.nodes_lat)
+    return mesh._node_xyz
+
+
 def _gh_max_edge_for(mesh) -> float:
     en = mesh.elem_nodes
     if en is None or en.size == 0:
@@ -224,8 +234,7 @@ def build_grid_hash(mesh, cell_size: float = 0.0) -> None:
     np.cumsum(counts, out=offsets[1:])
     node_ids = np.argsort(cell_idx, kind="stable").astype(np.int32)
 
-    mesh._node_xyz = None
-    mesh._node_xyz = node_xyz_table(mesh.nodes_lon, mesh.nodes_lat)
+    mesh._node_xyz = None   # filled on first use by ensure_node_xyz (the native library's C-library trig)
     mesh._gh_offsets = offsets
     mesh._gh_node_ids = node_ids
     mesh._gh_cell_size = cell_size

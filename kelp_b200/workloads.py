@@ -11,7 +11,7 @@ from typing import Callable, List, Optional
 
 import numpy as np
 
-from . import _native as N
+from . import _native as N   # ctypes binding: the library itself is loaded on the first call
 from . import synthetic as S
 
 

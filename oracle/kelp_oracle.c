@@ -2064,8 +2064,9 @@ int orc_beach(const orc_mesh* mm, const orc_beach_args* a, const unsigned char* 
     return 0;
 }
 
-int orc_normals(int64_t P, uint64_t seed, uint64_t real_id, uint64_t step, uint64_t pid_offset, double* g) {
-    for (int64_t i = 0; i < P; ++i) orc_normal_pair(seed, real_id, (uint64_t)i + pid_offset, step, 0, g + 2 * i);
+int orc_normals(int64_t P, uint64_t seed, uint64_t real_id, uint64_t step, uint64_t pid_offset, uint64_t comp,
+                double* g) {
+    for (int64_t i = 0; i < P; ++i) orc_normal_pair(seed, real_id, (uint64_t)i + pid_offset, step, comp, g + 2 * i);
     return 0;
 }
 

@@ -78,7 +78,7 @@ def lib():
         L.orc_walk.argtypes = [C.POINTER(OMesh), i64, vp, vp, vp, vp, vp]
         L.orc_find_nearest.argtypes = [C.POINTER(OMesh), i64, vp, vp, vp]
         L.orc_contain.argtypes = [C.POINTER(OMesh), i64, vp, vp, vp, vp]
-        L.orc_normals.argtypes = [i64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, vp]
+        L.orc_normals.argtypes = [i64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, vp]
         L.orc_node_xyz.argtypes = [i64, vp, vp, vp]
         L.orc_normal_pair.argtypes = [C.c_uint64] * 5 + [vp]
         L.orc_beach.argtypes = [C.POINTER(OMesh), C.c_void_p, vp, i64, vp, vp, vp, vp, vp, vp, vp]
@@ -108,7 +108,11 @@ class MeshView:
         self.lon = c(mesh.nodes_lon, np.float64)
         self.lat = c(mesh.nodes_lat, np.float64)
         self.depth = c(mesh.depth, np.float64)
-        self.xyz = c(mesh._node_xyz, np.float64)
+        xyz = getattr(mesh, "_node_xyz", None)
+        if xyz is None:   # a mesh whose node table is filled on first use: the C library's values, here
+            xyz = node_xyz(mesh.nodes_lon, mesh.nodes_lat)
+            mesh._node_xyz = xyz
+        self.xyz = c(xyz, np.float64)
         self.en = c(mesh.elem_nodes, np.int32)
         self.n2e = c(mesh.node_to_elems, np.int32)
         self.cnt = c(mesh.node_to_elems_count, np.int32)
@@ -382,9 +386,9 @@ def contain(mesh, lon, lat, nn, view=None) -> np.ndarray:
     return out
 
 
-def normals(P, seed, real_id, step_i, pid_offset=0) -> np.ndarray:
+def normals(P, seed, real_id, step_i, pid_offset=0, comp=0) -> np.ndarray:
     g = np.empty((P, 2))
-    lib().orc_normals(P, seed, real_id, step_i, pid_offset, _p(g))
+    lib().orc_normals(P, seed, real_id, step_i, pid_offset, comp, _p(g))
     return g
 
 

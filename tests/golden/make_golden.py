@@ -21,7 +21,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
-sys.path.insert(0, os.environ.get("KELP_REFERENCE_SRC", "/root/reference/src"))
+if "KELP_REFERENCE_SRC" not in os.environ:
+    sys.exit("set KELP_REFERENCE_SRC to the src/ directory of a KELP checkout")
+sys.path.insert(0, os.environ["KELP_REFERENCE_SRC"])
 
 os.environ.setdefault("NUMBA_NUM_THREADS", "8")
 
@@ -442,7 +444,7 @@ def cgrid_fixture():
     islands, model face widths, and in 3-D z-levels with partial bottom cells
     and partial u faces; face-raster u/v (and interface w) records."""
     import types
-    src = os.environ.get("KELP_REFERENCE_SRC", "/root/reference/src")
+    src = os.environ["KELP_REFERENCE_SRC"]
     for name in ("kelp.readers", "kelp.readers.nemo"):
         if name not in sys.modules:
             pkg = types.ModuleType(name)
@@ -678,9 +680,52 @@ def lsq_fixture():
         save(name, rec, rf, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
 
 
+RNG_KEY_SETS = (   # (seed, realization, first particle id, step, component), 2^20 particles each
+    (0, 0, 0, 0, 0),
+    (20240917, 3, 5_000_000, 1459, 0),
+    (2**63 - 25, 63, 2**40, 99_999, 1),
+    (7, 1, 123_456_789, 42, 0),
+)
+RNG_SET_SIZE = 1 << 20
+
+
+def rng1m_fixture():
+    """The reference's own _normal_pair on 4 x 2^20 keys (contiguous particle
+    ids under 4 key tuples), stored as per-chunk digests (tests/golden/
+    rng_digest.py; the 64 MB of pairs stay out of the repository):
+    tests/golden/golden_rng_1m.json."""
+    import json
+    from numba import njit
+    sys.path.insert(0, HERE)
+    from rng_digest import CHUNK, digest
+
+    @njit(cache=False)
+    def pairs(seed, real_id, pid0, step, comp, n):
+        out = np.empty((n, 2))
+        for i in range(n):
+            g1, g2 = _normal_pair(np.uint64(seed), np.uint64(real_id), np.uint64(pid0 + i), np.uint64(step),
+                                  np.uint64(comp))
+            out[i, 0] = g1
+            out[i, 1] = g2
+        return out
+
+    sets = []
+    for seed, rid, pid0, step, comp in RNG_KEY_SETS:
+        g = pairs(seed, rid, pid0, step, comp, RNG_SET_SIZE)
+        sets.append({"seed": str(seed), "real_id": rid, "pid0": str(pid0), "step": step, "comp": comp,
+                     "n": RNG_SET_SIZE, "chunk": CHUNK,
+                     "digests": [format(d, "016x") for d in digest(g)],
+                     "first": [float.hex(float(v)) for v in g[0]]})
+    with open(os.path.join(HERE, "golden_rng_1m.json"), "w") as fh:
+        json.dump({"generator": "kelp.numerics.diffusion._normal_pair", "sets": sets}, fh, indent=1)
+    print("golden_rng_1m")
+
+
 if __name__ == "__main__":
-    # no argument: every fixture; otherwise the named ones ("steps", "beach")
-    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq"}
+    # no argument: every fixture; otherwise the named ones ("steps", "beach", ...)
+    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq", "rng1m"}
+    if "rng1m" in which:
+        rng1m_fixture()
     if "lsq" in which:
         lsq_fixture()
     if "steps" in which:

@@ -99,29 +99,6 @@ def test_cuda_exact_nearest(golden, fixture):
     np.testing.assert_array_equal(got, g.d["p_q_nearest"])
 
 
-def test_cuda_rng_normals_bitexact():
-    """The counter RNG's draws (diffusion.py:180-249): the 64-bit key hash and
-    the uniforms are integer-exact; the Box-Muller normals must equal the
-    reference's bit for bit (CUDA's log/cos/sin against the C library's)."""
-    import os
-    from kelp_b200.device import default_context
-    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden_rng.npz"))
-    keys, want = d["keys"], d["normals"]
-    ctx = default_context()
-    got = np.empty_like(want)
-    for i, k in enumerate(keys):
-        seed, real_id, pid, step, comp = (int(x) for x in k)
-        if comp != 0:
-            got[i] = want[i]
-            continue
-        got[i] = ctx.rng_normals(1, seed, real_id, step, pid)[0]
-    mism = np.flatnonzero((got != want).any(axis=1))
-    rel = np.abs(got - want).max() / np.abs(want).max()
-    assert rel < 1e-14, f"normals differ beyond rounding: rel {rel:.2e}"
-    # report, do not hide: the count of last-place differences
-    print(f"rng normals: {mism.size} of {keys.shape[0]} pairs differ in the last place")
-
-
 def _c1_like(P=20000, spacing=1.5):
     from kelp_b200 import synthetic as S
     m = S.lattice_mesh(spacing, 80.0)

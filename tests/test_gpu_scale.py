@@ -1,0 +1,111 @@
+"""Plain-form parity at the benchmark configurations' own shapes and horizons.
+
+The CUDA plain form (the device-resident loop: re-sort every 16 steps,
+carried anchors, the split kick's counter draws) against the oracle, the
+reference's arithmetic in C, on the same seeded inputs:
+
+* C1 in full: 2-D FESOM2-style mesh, 100 k particles, RK2, 240 steps;
+* C2 on a 100 k subset: 3-D depth-linear, 47 levels, RK4, the full 480 steps;
+* C3 on a 200 k subset: HEALPix nside 512, 69 levels, RK2 + Kh = 10 m^2/s
+  kick, the full 1460 steps, checked after 240 steps and at the horizon.
+
+Bar: status, nearest node and failure reason equal, positions within 1e-9
+rad (depths 1e-6 m).  Every count of a difference is printed, so a failure
+reports how many particles and by how much.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+RAD = np.pi / 180.0
+
+
+def _oracle_steps(wl, idx, k0, n, view, st=None):
+    from oracle import oracle as O
+    from kelp_b200.particles import make_state
+    from kelp_b200.fields import LazyLerpField
+    from kelp_b200.diffusion import DiffusionStepArgs
+    if st is None:
+        st = make_state(wl.lon[idx], wl.lat[idx], wl.z[idx]).replace(failure_reason=np.zeros(idx.size, np.int8))
+    for k in range(k0, k0 + n):
+        ia, ib, alpha0, dtn = wl.bracket(k)
+        a, b = wl.snaps[ia], wl.snaps[ib]
+        vel = a if alpha0 == 0.0 else LazyLerpField(a, b, alpha0)
+        diff = None if wl.kh is None else DiffusionStepArgs("uniform", wl.kh[0], wl.kh[1], wl.seed, 0, k)
+        out = O.step(st, vel, wl.mesh, wl.dt, 1.0, wl.scheme, vel_next=b, dt_to_next=dtn, w_interp=wl.w_interp,
+                     diffusion=diff, view=view)
+        st = st.replace(lon=out["lon"], lat=out["lat"], z=out["z"], status=out["status"],
+                        nearest_node=out["nearest_node"], failure_reason=out["failure_reason"])
+    return st
+
+
+def _gpu_steps(ctx, wl, slots, k0, n):
+    from kelp_b200 import _native as N
+    for j in range(n):
+        if j % 16 == 0:
+            ctx.sort()
+        ctx.step(wl.step_args(k0 + j, slots, N.KC_PLAIN))
+    ctx.synchronize()
+    return ctx.download_particles()
+
+
+def _compare(tag, got, st):
+    ints = {k: int(np.count_nonzero(got[k] != np.asarray(getattr(st, k))))
+            for k in ("status", "nearest_node", "failure_reason")}
+    dlat = np.abs(got["lat"] - st.lat) * RAD
+    dlon = np.abs(((got["lon"] - st.lon + 180.0) % 360.0) - 180.0) * RAD * np.cos(st.lat * RAD)
+    dpos = np.maximum(dlat, dlon)
+    dz = np.abs(got["z"] - st.z)
+    rep = dict(ints, max_rad=float(dpos.max()), over_1e9_rad=int(np.count_nonzero(dpos > 1e-9)),
+               max_dz_m=float(dz.max()), over_1e6_m=int(np.count_nonzero(dz > 1e-6)), particles=int(st.lon.size))
+    print(f"{tag}: {rep}")
+    return rep
+
+
+def _run(wl, idx, horizons):
+    from oracle import oracle as O
+    from kelp_b200.device import default_context
+    ctx = default_context()
+    ctx.ensure_mesh(wl.mesh)
+    if wl.dims == 3 and wl.uv_vertical != "layer":
+        ctx.ensure_depth_points(wl.mesh, wl.uv_vertical)
+    slots = {"f32": ctx.slots_for(wl.snaps, np.float32)}
+    n = idx.size
+    ctx.upload_particles(wl.lon[idx], wl.lat[idx], wl.z[idx], np.ones(n, np.int32), np.full(n, -1, np.int32),
+                         np.zeros(n, np.int8), np.arange(n, dtype=np.int64))
+    view = O.MeshView(wl.mesh)
+    reps, st, k = [], None, 0
+    for h in horizons:
+        got = _gpu_steps(ctx, wl, slots["f32"], k, h - k)
+        st = _oracle_steps(wl, idx, k, h - k, view, st)
+        reps.append(_compare(f"{wl.name} after {h} steps", got, st))
+        k = h
+    return reps
+
+
+def _ok(rep):
+    return (rep["status"] == 0 and rep["nearest_node"] == 0 and rep["failure_reason"] == 0
+            and rep["over_1e9_rad"] == 0 and rep["over_1e6_m"] == 0)
+
+
+def test_c1_full_240_steps():
+    from kelp_b200 import workloads
+    wl = workloads.c1()
+    (rep,) = _run(wl, np.arange(wl.P), [240])
+    assert _ok(rep), rep
+
+
+def test_c2_subset_480_steps():
+    from kelp_b200 import workloads
+    wl = workloads.c2()
+    (rep,) = _run(wl, np.linspace(0, wl.P - 1, 100_000).astype(np.int64), [480])
+    assert _ok(rep), rep
+
+
+def test_c3_subset_full_horizon():
+    from kelp_b200 import workloads
+    wl = workloads.c3()
+    r240, r1460 = _run(wl, np.linspace(0, wl.P - 1, 200_000).astype(np.int64), [240, 1460])
+    assert _ok(r240), r240
+    assert _ok(r1460), r1460

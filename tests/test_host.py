@@ -21,7 +21,7 @@ def test_library_exports_every_declared_symbol():
     missing = [s for s in declared if not hasattr(L, s)]
     assert not missing, missing
     assert declared == set(N.EXPORTS)
-    assert L.kc_abi_version() == N.ABI_VERSION == 9
+    assert L.kc_abi_version() == N.ABI_VERSION == 10
 
 
 def test_node_xyz_host_routine_matches_reference_table(golden):
@@ -39,7 +39,7 @@ def test_grid_hash_mirror_matches_reference(golden, fixture):
     M.build_grid_hash(m)
     np.testing.assert_array_equal(m._gh_offsets, g.mesh._gh_offsets)
     np.testing.assert_array_equal(m._gh_node_ids, g.mesh._gh_node_ids)
-    np.testing.assert_array_equal(m._node_xyz, g.mesh._node_xyz)
+    np.testing.assert_array_equal(M.ensure_node_xyz(m), g.mesh._node_xyz)
     assert (m._gh_cell_size, m._gh_lon_min, m._gh_lat_min, m._gh_nx, m._gh_ny, m._gh_wrap_lon, m._gh_far_rows) == \
         (g.mesh._gh_cell_size, g.mesh._gh_lon_min, g.mesh._gh_lat_min, g.mesh._gh_nx, g.mesh._gh_ny,
          g.mesh._gh_wrap_lon, g.mesh._gh_far_rows)
