@@ -11,7 +11,9 @@ Tables:
   * ln 2 in three parts (the first with 42 significant bits, so e * part is
     exact for any double exponent e);
   * pi/2 in three 53-bit parts (Cody-Waite reduction);
-  * the Taylor coefficients (-1)^k / (2k+1)! and (-1)^k / (2k)!.
+  * the Taylor coefficients (-1)^k / (2k+1)! and (-1)^k / (2k)!;
+  * sin(j/64) and cos(j/64), j = 0..51, as double-double records (the fast
+    path of sin / cos).
 """
 from __future__ import annotations
 
@@ -76,6 +78,19 @@ def main() -> None:
     lines += arr("KC_CR_LOG_INV", inv)
     lines += arr("KC_CR_LOG_NLC_HI", nlh)
     lines += arr("KC_CR_LOG_NLC_LO", nll)
+
+    # sin / cos fast path: sin(j/64), cos(j/64), j = 0..51 (|r| <= pi/4 + eps)
+    tsh, tsl, tch, tcl = [], [], [], []
+    for j in range(52):
+        a = mp.mpf(j) / 64
+        h, l = dd(mp.sin(a))
+        tsh.append(h)
+        tsl.append(l)
+        h, l = dd(mp.cos(a))
+        tch.append(h)
+        tcl.append(l)
+    # interleaved per j: sin hi, sin lo, cos hi, cos lo (one 32-byte record)
+    lines += arr("KC_CR_TAB_SC", [v for j in range(52) for v in (tsh[j], tsl[j], tch[j], tcl[j])])
 
     ln2 = mp.log(2)
     ln2_1 = trunc_bits(ln2, 42)

@@ -10,7 +10,9 @@
 // cos and sin and the correctly rounded ones (kc_crmath.cuh), and records
 // each j where they differ as (j, bit delta) -- the library value's bit
 // pattern minus the correctly rounded one's, +-1 (anything else aborts).
-// It also prints order-independent digests of the library's and the
+// It also checks that the fast paths of log_cr / sincos_cr return the
+// double-double paths' results (fast_path_differs must be 0) and prints
+// order-independent digests of the library's and the
 // correctly rounded values over the whole domain, which the GPU test
 // compares against the device (tests/golden/rng_domain.json).
 //
@@ -64,7 +66,7 @@ static int delta_code(double lib, double cr, uint64_t j, const char* what) {
 
 struct Part {
     uint64_t dr_lib = 0, dr_cr = 0, dc_lib = 0, dc_cr = 0, ds_lib = 0, ds_cr = 0;
-    uint64_t ambiguous = 0;
+    uint64_t ambiguous = 0, fast_differs = 0;
     std::vector<std::pair<uint32_t, uint8_t>> a;
     std::vector<std::pair<uint32_t, uint8_t>> b;
 };
@@ -87,8 +89,10 @@ int main(int argc, char** argv) {
                 const double u = (double)j * INV + HALF;
                 bool amb = false;
                 const double r_lib = std::sqrt(-2.0 * std::log(u));
-                const double r_cr = std::sqrt(-2.0 * kc::cr::log_cr_checked(u, &amb));
+                const double l_cr = kc::cr::log_cr_checked(u, &amb);
                 p.ambiguous += amb;
+                p.fast_differs += bits_of(kc::cr::log_cr(u)) != bits_of(l_cr);
+                const double r_cr = std::sqrt(-2.0 * l_cr);
                 const int rc = delta_code(r_lib, r_cr, j, "r");
                 if (rc) p.a.push_back({(uint32_t)j, (uint8_t)rc});
                 p.dr_lib += term(j, r_lib);
@@ -97,6 +101,9 @@ int main(int argc, char** argv) {
                 double s_cr, c_cr;
                 kc::cr::sincos_cr_checked(th2, &s_cr, &c_cr, &amb);
                 p.ambiguous += amb;
+                double s_f, c_f;
+                kc::cr::sincos_cr(th2, &s_f, &c_f);
+                p.fast_differs += (bits_of(s_f) != bits_of(s_cr)) + (bits_of(c_f) != bits_of(c_cr));
                 const double s_lib = std::sin(th2), c_lib = std::cos(th2);
                 const int cc = delta_code(c_lib, c_cr, j, "cos"), sc = delta_code(s_lib, s_cr, j, "sin");
                 if (cc || sc) p.b.push_back({(uint32_t)j, (uint8_t)(cc | (sc << 2))});
@@ -112,6 +119,7 @@ int main(int argc, char** argv) {
     for (auto& p : parts) {   // parts cover ascending ranges: concatenation keeps keys sorted
         all.dr_lib += p.dr_lib; all.dr_cr += p.dr_cr; all.dc_lib += p.dc_lib; all.dc_cr += p.dc_cr;
         all.ds_lib += p.ds_lib; all.ds_cr += p.ds_cr; all.ambiguous += p.ambiguous;
+        all.fast_differs += p.fast_differs;
         all.a.insert(all.a.end(), p.a.begin(), p.a.end());
         all.b.insert(all.b.end(), p.b.begin(), p.b.end());
     }
@@ -137,11 +145,12 @@ int main(int argc, char** argv) {
     put(all.b);
     std::fclose(f);
     std::printf("{\n  \"libc\": \"glibc %s\",\n  \"domain\": %llu,\n  \"ambiguous\": %llu,\n"
-                "  \"exceptions_r\": %zu,\n  \"exceptions_trig\": %zu,\n"
+                "  \"fast_path_differs\": %llu,\n  \"exceptions_r\": %zu,\n  \"exceptions_trig\": %zu,\n"
                 "  \"digest_r_lib\": \"%016llx\",\n  \"digest_r_cr\": \"%016llx\",\n"
                 "  \"digest_cos_lib\": \"%016llx\",\n  \"digest_cos_cr\": \"%016llx\",\n"
                 "  \"digest_sin_lib\": \"%016llx\",\n  \"digest_sin_cr\": \"%016llx\"\n}\n",
-                gnu_get_libc_version(), (unsigned long long)n, (unsigned long long)all.ambiguous, all.a.size(),
+                gnu_get_libc_version(), (unsigned long long)n, (unsigned long long)all.ambiguous,
+                (unsigned long long)all.fast_differs, all.a.size(),
                 all.b.size(), (unsigned long long)all.dr_lib, (unsigned long long)all.dr_cr,
                 (unsigned long long)all.dc_lib, (unsigned long long)all.dc_cr, (unsigned long long)all.ds_lib,
                 (unsigned long long)all.ds_cr);

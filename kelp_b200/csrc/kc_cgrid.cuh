@@ -80,7 +80,7 @@ static __device__ __noinline__ bool cgrid_core(const DMesh& m, const DBlend<T>& 
     const double vS = cg_val(f.a.v, f.b.v, f.t.v, f.alpha0, alpha, ko + c - nx);
     const double vN = cg_val(f.a.v, f.b.v, f.t.v, f.alpha0, alpha, ko + c);
     const double M = SLM;
-    const double cosl = cos(yp * DEG2RAD);
+    const double cosl = cr::cos_cr(yp * DEG2RAD);
     const int4 cr = __ldg(&g.corners[e]);
     double px[4], py[4];
 #pragma unroll
@@ -239,7 +239,7 @@ __device__ __forceinline__ void step3d_cgrid_particle(const DMesh& m, const DBle
             first_v = Vn;
             first_w = Wn;
         }
-        double z0n = cos(lt * DEG2RAD) * SLM;
+        double z0n = cr::cos_cr(lt * DEG2RAD) * SLM;
         if (z0n < 1.0) z0n = 1.0;
         k0 = dt * Un / z0n;
         k1 = dt * Vn / SLM;

@@ -15,6 +15,27 @@
 // a particle position are evaluated once per evaluation site with CUDA's
 // double-precision functions and shared by every consumer at that site.
 #pragma once
+#include "kc_crmath.cuh"
+
+// Inlining of the shared helpers of the step kernels (build options, -D):
+// __noinline__ keeps a kernel's code footprint small under divergence;
+// __forceinline__ lets the register allocator see across the call, without
+// the saves and restores of the call boundary.
+#ifndef KC_INL_SITE
+#define KC_INL_SITE __noinline__          // make_site
+#endif
+#ifndef KC_INL_NEAREST
+#define KC_INL_NEAREST __noinline__       // nearest_exact
+#endif
+#ifndef KC_INL_CONTAIN
+#define KC_INL_CONTAIN __noinline__       // contain_local, contain_local_w, w_search_elem
+#endif
+#ifndef KC_INL_STAGE
+#define KC_INL_STAGE __noinline__         // stage_f32 (mixed form), interp_uv_at, w_bary_at (plain form)
+#endif
+#ifndef KC_INL_KICK
+#define KC_INL_KICK __noinline__          // apply_kick
+#endif
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -108,12 +129,12 @@ struct Site {
     double sin_lon, cos_lon;  // of lon * DEG2RAD
 };
 
-static __device__ __noinline__ Site make_site(double lon, double lat) {
+static __device__ KC_INL_SITE Site make_site(double lon, double lat) {
     Site s;
     s.lon = lon;
     s.lat = lat;
-    sincos(lat * DEG2RAD, &s.sin_lat, &s.cos_lat);
-    sincos(lon * DEG2RAD, &s.sin_lon, &s.cos_lon);
+    cr::sincos_cr(lat * DEG2RAD, &s.sin_lat, &s.cos_lat);   // correctly rounded: the C library's values but
+    cr::sincos_cr(lon * DEG2RAD, &s.sin_lon, &s.cos_lon);   // where it misrounds (kc_crmath.cuh)
     s.xp = s.cos_lat * s.cos_lon;
     s.yp = s.cos_lat * s.sin_lon;
     s.zp = s.sin_lat;
@@ -551,7 +572,7 @@ static __device__ __noinline__ int nearest_exact_slow(const DMesh& m, const Site
 // mesh.py:1611-1859 _grid_hash_nearest_exact: the 3x3 window accepted when
 // the certificate proves it (fast bound first, the reference's own
 // certificate when the bound is inconclusive), else the rectangle growth.
-static __device__ __noinline__ int nearest_exact(const DMesh& m, const Site& q) {
+static __device__ KC_INL_NEAREST int nearest_exact(const DMesh& m, const Site& q) {
     const double far = (double)m.far_rows * m.cell;
     if (q.lat < m.lat_min - far || q.lat > m.lat_min + (double)m.ny * m.cell + far) return nearest_widened(m, q);
     double bd2;
@@ -767,7 +788,7 @@ static __device__ __noinline__ int contain_two_ring(const DMesh& m, double lon_p
 
 // mesh.py:2392-2470 _find_containing_element_local: the 1-ring of the anchor,
 // then its 2-ring; -1 when no element contains the point.
-static __device__ __noinline__ int contain_local(const DMesh& m, double lon_p, double lat_p, int nn) {
+static __device__ KC_INL_CONTAIN int contain_local(const DMesh& m, double lon_p, double lat_p, int nn) {
     int s = __ldg(&m.n2e_off[nn]), e = __ldg(&m.n2e_off[nn + 1]);
     if (e == s) return -1;
     for (int k = s; k < e; ++k) {
@@ -801,7 +822,7 @@ static __device__ __noinline__ int contain_two_ring(const DMesh& m, double lon_p
 // search of the same point and anchor (vertical.py:744-881): w_elem is the
 // element that search returns (-1: its nodal fallback) unless w_unsure, when
 // only running that search decides.
-static __device__ __noinline__ int contain_local_w(const DMesh& m, double lon_p, double lat_p, int nn, int& w_elem,
+static __device__ KC_INL_CONTAIN int contain_local_w(const DMesh& m, double lon_p, double lat_p, int nn, int& w_elem,
                                                    bool& w_unsure) {
     w_elem = -1;
     w_unsure = false;

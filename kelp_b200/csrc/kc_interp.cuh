@@ -145,7 +145,7 @@ __device__ __forceinline__ bool bary_weights_core(const DMesh& m, int elem, doub
 // interpolate.py:1443-1529 its 3-D twin (row = the particle's layer).
 // The core given its containing element `elem` (>= 0).
 template <typename T>
-__device__ __noinline__ bool interp_uv_at(const DMesh& m, const DBlend<T>& f, int elem, double xp, double yp,
+__device__ KC_INL_STAGE bool interp_uv_at(const DMesh& m, const DBlend<T>& f, int elem, double xp, double yp,
                                           double time_dir, int row, double alpha, double& U, double& V) {
     U = 0.0;
     V = 0.0;
@@ -572,7 +572,7 @@ __device__ __noinline__ double w_bary(const DMesh& m, const DBlend<T>& f, double
 // at element `el` (contain_local_w): that element's own frame and weights,
 // the first fan triangle for a triangle, Wachspress for a quad.
 template <typename T>
-__device__ __noinline__ double w_bary_at(const DMesh& m, const DBlend<T>& f, double alpha, double xp, double yp,
+__device__ KC_INL_STAGE double w_bary_at(const DMesh& m, const DBlend<T>& f, double alpha, double xp, double yp,
                                          double z, int el, double time_dir) {
     const WLoc Lz = w_locate(m, z);
     Ring r;
@@ -632,7 +632,7 @@ __device__ __noinline__ double w_bary_at(const DMesh& m, const DBlend<T>& f, dou
 // the point (the first 1-ring element of the anchor with a fan triangle whose
 // three weights are >= -1e-6), or -1 for its nodal fallback: w_bary's loop
 // without the values.
-static __device__ __noinline__ int w_search_elem(const DMesh& m, double xp, double yp, int node) {
+static __device__ KC_INL_CONTAIN int w_search_elem(const DMesh& m, double xp, double yp, int node) {
     int s = __ldg(&m.n2e_off[node]), e = __ldg(&m.n2e_off[node + 1]);
     for (int kk = s; kk < e; ++kk) {
         const int el = __ldg(&m.n2e[kk]);
@@ -792,7 +792,7 @@ __device__ __forceinline__ bool interp_uv_lsq(const DMesh& m, const DBlend<T>& f
     V = 0.0;
     const int s0 = __ldg(&m.n2e_off[nn]), s1 = __ldg(&m.n2e_off[nn + 1]);
     if (s1 <= s0) return false;
-    const double z0 = cos(yp * DEG2RAD) * SLM;
+    const double z0 = cr::cos_cr(yp * DEG2RAD) * SLM;
     const double xp_m = xp * z0;
     const double yp_m = yp * SLM;
     double a11 = 0.0, a12 = 0.0, a13 = 0.0, a22 = 0.0, a23 = 0.0, a33 = 0.0;
@@ -916,7 +916,7 @@ __device__ __forceinline__ void sphere_displace(const Site& q, double dx, double
     const double cl = q.cos_lon, sl = q.sin_lon, cp = q.cos_lat, sp = q.sin_lat;
     double delta = dist / R_METRIC;
     double sdel, c;
-    sincos(delta, &sdel, &c);
+    cr::sincos_cr(delta, &sdel, &c);
     double s = sdel / dist;
     double tx = -sl * dx - sp * cl * dy;
     double ty = cl * dx - sp * sl * dy;

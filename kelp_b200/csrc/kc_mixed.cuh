@@ -141,7 +141,7 @@ __device__ __forceinline__ float w_node_f32(const DMesh& m, const DBlend<T>& f, 
 // containment and the vertical decisions in float64, values in float32.
 // dims 2 reads u/v row 0 and no W.
 template <typename T>
-__device__ __noinline__ bool stage_f32(const DMesh& m, const DBlend<T>& f, const DStep& s, int dims, double xp,
+__device__ KC_INL_STAGE bool stage_f32(const DMesh& m, const DBlend<T>& f, const DStep& s, int dims, double xp,
                                        double yp, int nn, int hint, int whint, double z, double alpha, double& U,
                                        double& V, double& W) {
     U = 0.0;

@@ -150,7 +150,7 @@ __device__ __forceinline__ int end_elem(const DMesh& m, double lon, double lat, 
 // kick (diffusion.py:485-529, :261-298), great-circle move, exact re-anchor
 // and containment re-check, revert to the pre-step state on leaving the
 // domain; 3-D reclamp in the new column.
-static __device__ __noinline__ void apply_kick(const DMesh& m, const DStep& s, long long pid, unsigned long long rid,
+static __device__ KC_INL_KICK void apply_kick(const DMesh& m, const DStep& s, long long pid, unsigned long long rid,
                                         const Site& qn,
                                         double pre_lon, double pre_lat, double pre_z, int pre_nn, bool is3d,
                                         double& lon, double& lat, double& z, int& status, int& nn, signed char& fr,
