@@ -203,7 +203,6 @@ kc::DStep step_of(const kc_step_args* a) {
     s.global_step = a->global_step;
     s.az_on = a->az_kick; s.az_field = a->az_field; s.az_const = a->az_const;
     s.Dmin = a->Dmin; s.z0b_min = a->z0b_min; s.alpha_end = a->alpha_end;
-    s.rng_exact = a->precision == KC_PLAIN ? 1 : 0;
     return s;
 }
 
@@ -243,7 +242,7 @@ __global__ void __launch_bounds__(kBlock) k_normals(const kc::DRngX x, long long
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P) return;
     double g1, g2;
-    kc::normal_pair(x, seed, real_id, (unsigned long long)i + pid0, step, comp, g1, g2);
+    kc::normal_pair<true>(x, seed, real_id, (unsigned long long)i + pid0, step, comp, g1, g2);
     out[2 * i] = g1;
     out[2 * i + 1] = g2;
 }

@@ -155,6 +155,8 @@ static __device__ __noinline__ bool cgrid_core(const DMesh& m, const DBlend<T>& 
 // interp_nemo_cgrid: the surface faces), for step2d_particle.
 template <typename T>
 struct CgridForm {
+    static constexpr bool kExact = true;
+    static __device__ __forceinline__ Site site(double lon, double lat) { return make_site(lon, lat); }
     static __device__ __forceinline__ bool uv2(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
                                                double lat, int nn, int hint, double alpha, double& U, double& V) {
         double W;

@@ -214,16 +214,25 @@ KC_CR_HD DD log_fast(double x) {
     return fast_two_sum(s3.hi, lo);
 }
 
+// The double-double second steps, out of line on the device: they run for a
+// few arguments in a thousand, and one copy keeps the callers' code small.
+#if defined(__CUDACC__)
+#define KC_CR_SLOW static __host__ __device__ __noinline__
+#else
+#define KC_CR_SLOW static inline
+#endif
+KC_CR_SLOW double log_slow(double x) { return log_dd(x).hi; }
+
 // Correctly rounded log(x) for positive normal x (the RNG's uniforms are in
 // [2^-33, 1)); other arguments take the library log.  The fast path decides
-// all but ~0.2 % of arguments; the rest take the double-double path.
+// all but ~0.02 % of arguments; the rest take the double-double path.
 KC_CR_HD double log_cr(double x) {
     const uint64_t ix = bits_of(x);
     const unsigned ex = (unsigned)((ix >> 52) & 0x7ff);
     if ((ix >> 63) || ex == 0 || ex == 0x7ff) return log(x);
     const DD v = log_fast(x);
     if (!round_ambiguous(v, 0x1p-63)) return v.hi;
-    return log_dd(x).hi;
+    return log_slow(x);
 }
 
 KC_CR_HD double log_cr_checked(double x, bool* ambiguous) {
@@ -325,6 +334,13 @@ KC_CR_HD void sincos_fast(double x, DD& s, DD& c) {
     else if (qd == 3) { s = DD{-cr.hi, -cr.lo}; c = sr; }
 }
 
+KC_CR_SLOW void sincos_slow(double x, double* sn, double* cs) {
+    DD s, c;
+    sincos_dd(x, s, c);
+    *sn = s.hi;
+    *cs = c.hi;
+}
+
 // Correctly rounded sin(x), cos(x) for |x| < 2^20 (the RNG's angles are in
 // (0, 2 pi)); larger or non-finite arguments take the library functions.
 // The fast path decides all but ~0.4 % of arguments; the rest take the
@@ -337,7 +353,10 @@ KC_CR_HD void sincos_cr(double x, double* sn, double* cs) {
     }
     DD s, c;
     sincos_fast(x, s, c);
-    if (round_ambiguous(s, 0x1p-63) || round_ambiguous(c, 0x1p-63)) sincos_dd(x, s, c);
+    if (round_ambiguous(s, 0x1p-63) || round_ambiguous(c, 0x1p-63)) {
+        sincos_slow(x, sn, cs);
+        return;
+    }
     *sn = s.hi;
     *cs = c.hi;
 }

@@ -141,6 +141,20 @@ static __device__ KC_INL_SITE Site make_site(double lon, double lat) {
     return s;
 }
 
+// The same site with CUDA's sincos (within 2 ulp): the mixed form's sites,
+// where last-place agreement with the C library is not the contract.
+static __device__ KC_INL_SITE Site make_site_fast(double lon, double lat) {
+    Site s;
+    s.lon = lon;
+    s.lat = lat;
+    sincos(lat * DEG2RAD, &s.sin_lat, &s.cos_lat);
+    sincos(lon * DEG2RAD, &s.sin_lon, &s.cos_lon);
+    s.xp = s.cos_lat * s.cos_lon;
+    s.yp = s.cos_lat * s.sin_lon;
+    s.zp = s.sin_lat;
+    return s;
+}
+
 // fmod(x, 360) for |x| < 2^40 * 360 without the general remainder loop:
 // with n the integer part of |x| / 360 (corrected by one when the division
 // rounded across an integer), |x| - n * 360 is exact (n * 360 is exact, and
@@ -715,22 +729,42 @@ __device__ __forceinline__ bool w_ring_matches_mask(const int4& e) {
 // class of the W search (W_OUT / W_UNSURE).
 template <bool W_INFO>
 __device__ __forceinline__ int element_contains_t(const DMesh& m, int c, double lon_p, double lat_p) {
-    int4 e = __ldg(&m.en[c]);
-    Poly p;
-    load_poly_mask(m, e, p);
-    const int n = p.n;
+    const int4 e = __ldg(&m.en[c]);
+    // the mask's vertex slots in order (-1 slots dropped, slot 3 dropped when
+    // it repeats slot 0)
+    const bool v3 = e.w >= 0 && !(e.w == e.x && e.x >= 0);
+    int id0 = -1, id1 = -1, id2 = -1, id3 = -1;   // scalars: no dynamically indexed array
+    int n = 0;
+    auto push = [&](int v) {
+        if (n == 0) id0 = v;
+        else if (n == 1) id1 = v;
+        else if (n == 2) id2 = v;
+        else id3 = v;
+        ++n;
+    };
+    if (e.x >= 0) push(e.x);
+    if (e.y >= 0) push(e.y);
+    if (e.z >= 0) push(e.z);
+    if (v3) push(e.w);
     if (n < 3) return (W_INFO && !w_ring_matches_mask(e)) ? W_UNSURE : 0;
+    auto vid = [&](int k) { return k == 1 ? id1 : (k == 2 ? id2 : id3); };
     const int miss = (W_INFO && !w_ring_matches_mask(e)) ? W_UNSURE : 0;
     // bbox prefilter in wrapped-delta space around the first valid vertex
-    // (the first vertex's own delta is wrap180(0) == 0)
-    const double lon_ref = p.ln[0];
-    const double d1 = wrap180(p.ln[1] - lon_ref), d2 = wrap180(p.ln[2] - lon_ref);
-    const double d3 = n == 4 ? wrap180(p.ln[3] - lon_ref) : 0.0;
-    double dmin = fmin(fmin(0.0, d1), d2), dmax = fmax(fmax(0.0, d1), d2);
-    double lamin = fmin(fmin(p.la[0], p.la[1]), p.la[2]), lamax = fmax(fmax(p.la[0], p.la[1]), p.la[2]);
-    if (n == 4) {
-        dmin = fmin(dmin, d3); dmax = fmax(dmax, d3);
-        lamin = fmin(lamin, p.la[3]); lamax = fmax(lamax, p.la[3]);
+    // (the first vertex's own delta is wrap180(0) == 0): running bounds only,
+    // in the reference's order, so most rejected elements hold few registers
+    const double2 a0 = __ldg(&m.ll[id0]);
+    const double lon_ref = a0.x;
+    double dmin = 0.0, dmax = 0.0, lamin = a0.y, lamax = a0.y;
+#pragma unroll
+    for (int k = 1; k < 4; ++k) {
+        if (k < n) {
+            const double2 a = __ldg(&m.ll[vid(k)]);
+            const double d = wrap180(a.x - lon_ref);
+            dmin = fmin(dmin, d);
+            dmax = fmax(dmax, d);
+            lamin = fmin(lamin, a.y);
+            lamax = fmax(lamax, a.y);
+        }
     }
     const double dlon_p = wrap180(lon_p - lon_ref);
     if (dlon_p > dmax || dlon_p < dmin || lat_p > lamax || lat_p < lamin) {
@@ -742,7 +776,19 @@ __device__ __forceinline__ int element_contains_t(const DMesh& m, int c, double 
         if (lat_p < lamin - my || lat_p > lamax + my || dlon_p < dmin - mx || dlon_p > dmax + mx) return W_OUT;
         return W_UNSURE;
     }
-    // local projection: raw-mean origin unless the element spans > 180 deg
+    // inside the box: the vertices again (cached), the local projection with
+    // the raw-mean origin unless the element spans > 180 deg
+    Poly p;
+    p.ln[0] = a0.x;
+    p.la[0] = a0.y;
+#pragma unroll
+    for (int k = 1; k < 4; ++k) {
+        const double2 a = __ldg(&m.ll[k < n ? vid(k) : id0]);
+        p.ln[k] = a.x;
+        p.la[k] = a.y;
+    }
+    const double d1 = wrap180(p.ln[1] - lon_ref), d2 = wrap180(p.ln[2] - lon_ref);
+    const double d3 = n == 4 ? wrap180(p.ln[3] - lon_ref) : 0.0;
     double lmin = fmin(fmin(p.ln[0], p.ln[1]), p.ln[2]), lmax = fmax(fmax(p.ln[0], p.ln[1]), p.ln[2]);
     if (n == 4) { lmin = fmin(lmin, p.ln[3]); lmax = fmax(lmax, p.ln[3]); }
     double lon0;

@@ -881,12 +881,26 @@ __device__ __forceinline__ double rngx_bump(double v, unsigned code) {
     return __longlong_as_double(code == 1u ? b + 1 : b - 1);
 }
 
-// The draw of the reference (diffusion.py:222-249): log, cos and sin are
-// correctly rounded (kc_crmath.cuh), then moved to the host C library's
-// value at the inputs listed in the exception tables, so the pair equals
-// the reference's bit for bit for every key.
+// The draw of the reference (diffusion.py:222-249).  EXACT (the plain
+// form): log, cos and sin correctly rounded (kc_crmath.cuh), then moved to
+// the host C library's value at the inputs listed in the exception tables x,
+// so the pair equals the reference's bit for bit for every key.  Otherwise
+// (the mixed form) CUDA's log and sincos.
+template <bool EXACT>
 __device__ __forceinline__ void normal_pair(const DRngX& x, uint64_t seed, uint64_t real_id, uint64_t pid,
                                             uint64_t step, uint64_t comp, double& g1, double& g2) {
+    if constexpr (!EXACT) {
+        const uint64_t h = key_hash(seed, real_id, pid, step, comp);
+        const double INV = 1.0 / 4294967296.0;
+        const double u1 = (double)(h >> 32) * INV + 0.5 * INV;
+        const double u2 = (double)(h & 0xFFFFFFFFull) * INV + 0.5 * INV;
+        const double r = sqrt(-2.0 * log(u1));
+        double sn, cs;
+        sincos(2.0 * 3.141592653589793 * u2, &sn, &cs);
+        g1 = r * cs;
+        g2 = r * sn;
+        return;
+    }
     uint64_t h = key_hash(seed, real_id, pid, step, comp);
     const double INV = 1.0 / 4294967296.0;
     const double HALF = 0.5 * INV;
@@ -910,13 +924,15 @@ constexpr double R_METRIC = SLM / DEG2RAD;
 
 // diffusion.py:538-575 sphere_displace (exponential map of the tangent kick);
 // sin/cos of the start longitude and latitude come from its evaluation site.
+template <bool EXACT>
 __device__ __forceinline__ void sphere_displace(const Site& q, double dx, double dy, double& lon2, double& lat2) {
     double dist = sqrt(dx * dx + dy * dy);
     if (dist == 0.0) { lon2 = q.lon; lat2 = q.lat; return; }
     const double cl = q.cos_lon, sl = q.sin_lon, cp = q.cos_lat, sp = q.sin_lat;
     double delta = dist / R_METRIC;
     double sdel, c;
-    cr::sincos_cr(delta, &sdel, &c);
+    if constexpr (EXACT) cr::sincos_cr(delta, &sdel, &c);
+    else sincos(delta, &sdel, &c);
     double s = sdel / dist;
     double tx = -sl * dx - sp * cl * dy;
     double ty = cl * dx - sp * sl * dy;

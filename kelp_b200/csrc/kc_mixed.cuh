@@ -81,22 +81,44 @@ __device__ __forceinline__ float blend_w(const DBlend<T>& f, const TBlendF& tb, 
     return blend_val<T>(tb, f.a.w, f.a.sw, f.b.w, f.b.sw, f.t.w, f.t.sw, row, f.n, node);
 }
 
-// Vertex weights of the point in element `elem` (its compacted ring), in
-// float32 in the frame of the ring's first vertex.
-__device__ __forceinline__ bool weights_f32(const DMesh& m, int elem, double xp, double yp, Ring& r, float* w) {
-    load_ring(m, __ldg(&m.en[elem]), r);
-    const int nv = r.n;
-    if (nv < 3) return false;
+// Vertex weights of the point in element `elem` (its compacted ring, as
+// load_ring compacts it), in float32 in the frame of the ring's first vertex:
+// v[0..n-1] the vertex ids, w[0..n-1] their weights (w[3] = 0 for a
+// triangle).  Only the float offsets stay live, never the double
+// coordinates, and every array index is a compile-time constant.
+__device__ __forceinline__ bool weights_f32(const DMesh& m, int elem, double xp, double yp, int* v, float* w,
+                                            int& nv) {
+    const int4 e = __ldg(&m.en[elem]);
+    int n = 0, first = -1;
+    v[0] = v[1] = v[2] = v[3] = -1;
+    auto push = [&](int id) {
+        if (n == 0) v[0] = id;
+        else if (n == 1) v[1] = id;
+        else if (n == 2) v[2] = id;
+        else v[3] = id;
+        ++n;
+    };
+    if (e.x >= 0) { push(e.x); first = e.x; }
+    if (e.y >= 0 && !(n > 0 && e.y == first)) { push(e.y); if (first < 0) first = e.y; }
+    if (e.z >= 0 && !(n > 0 && e.z == first)) { push(e.z); if (first < 0) first = e.z; }
+    if (e.w >= 0 && !(n > 0 && e.w == first)) push(e.w);
+    nv = n;
+    if (n < 3) return false;
+    if (n == 3) v[3] = v[0];
     const float cl = (float)__ldg(&m.ecos[elem]).y;
+    const double2 a0 = __ldg(&m.ll[v[0]]);
     float x[4], y[4];
+    x[0] = 0.0f;
+    y[0] = 0.0f;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        x[k] = (float)wrap180(r.ln[k] - r.ln[0]) * cl;
-        y[k] = (float)(r.la[k] - r.la[0]);
+    for (int k = 1; k < 4; ++k) {
+        const double2 a = __ldg(&m.ll[v[k]]);
+        x[k] = (float)wrap180(a.x - a0.x) * cl;
+        y[k] = (float)(a.y - a0.y);
     }
-    const float px = (float)wrap180(xp - r.ln[0]) * cl;
-    const float py = (float)(yp - r.la[0]);
-    if (nv == 3) {
+    const float px = (float)wrap180(xp - a0.x) * cl;
+    const float py = (float)(yp - a0.y);
+    if (n == 3) {
         const float denom = (y[1] - y[2]) * (x[0] - x[2]) + (x[2] - x[1]) * (y[0] - y[2]);
         if (!(fabsf(denom) > 0.0f)) return false;
         w[0] = ((y[1] - y[2]) * (px - x[2]) + (x[2] - x[1]) * (py - y[2])) / denom;
@@ -167,9 +189,9 @@ __device__ KC_INL_STAGE bool stage_f32(const DMesh& m, const DBlend<T>& f, const
         elem = (dims == 3 && s.w_code == 1) ? contain_local_w(m, xp, yp, nn, w_elem, w_unsure)
                                             : contain_local(m, xp, yp, nn);
     }
-    Ring r;
+    int rv[4], rn = 0;
     float w[4];
-    const bool ok = elem >= 0 && weights_f32(m, elem, xp, yp, r, w);
+    const bool ok = elem >= 0 && weights_f32(m, elem, xp, yp, rv, w, rn);
     if (dims == 3) {
         const WLoc Lz = w_locate(m, z);
         float Wf;
@@ -178,17 +200,22 @@ __device__ KC_INL_STAGE bool stage_f32(const DMesh& m, const DBlend<T>& f, const
             // decides it; the containment scan usually already has)
             if (w_unsure) w_elem = w_search_elem(m, xp, yp, nn);
             if (w_elem >= 0) {
-                Ring rw;
-                float ww[4];
-                const bool same = ok && w_elem == elem;
-                const bool okw = same || weights_f32(m, w_elem, xp, yp, rw, ww);
-                const Ring& rr = same ? r : rw;
-                const float* wk = same ? w : ww;
                 Wf = 0.0f;
-                if (okw)
-                    for (int k = 0; k < rr.n; ++k) Wf += wk[k] * w_node_f32<T>(m, f, tb, z, Lz, rr.v[k], true);
-                else
-                    Wf = w_node_f32<T>(m, f, tb, z, Lz, nn, true);
+                if (ok && w_elem == elem) {   // the u/v weights
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        if (k < rn) Wf += w[k] * w_node_f32<T>(m, f, tb, z, Lz, rv[k], true);
+                } else {
+                    int wv[4], wn = 0;
+                    float ww[4];
+                    if (weights_f32(m, w_elem, xp, yp, wv, ww, wn)) {
+#pragma unroll
+                        for (int k = 0; k < 4; ++k)
+                            if (k < wn) Wf += ww[k] * w_node_f32<T>(m, f, tb, z, Lz, wv[k], true);
+                    } else {
+                        Wf = w_node_f32<T>(m, f, tb, z, Lz, nn, true);
+                    }
+                }
             } else {
                 Wf = w_node_f32<T>(m, f, tb, z, Lz, nn, true);   // its nodal fallback, z clamped
             }
@@ -207,21 +234,25 @@ __device__ KC_INL_STAGE bool stage_f32(const DMesh& m, const DBlend<T>& f, const
         int n_wet = 0;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            wet[k] = k < r.n && zq <= __ldg(&m.dl_bed[r.v[k]]);
+            wet[k] = k < rn && zq <= __ldg(&m.dl_bed[rv[k]]);
             n_wet += wet[k] ? 1 : 0;
         }
         if (n_wet == 0) {
-            int kd = 0;
-            for (int k = 1; k < r.n; ++k)
-                if (__ldg(&m.dl_bed[r.v[k]]) > __ldg(&m.dl_bed[r.v[kd]])) kd = k;
-            const int nd = r.v[kd];
+            int nd = rv[0];
+            double bd = __ldg(&m.dl_bed[rv[0]]);
+#pragma unroll
+            for (int k = 1; k < 4; ++k)
+                if (k < rn) {
+                    const double b = __ldg(&m.dl_bed[rv[k]]);
+                    if (b > bd) { bd = b; nd = rv[k]; }
+                }
             const int row = __ldg(&m.dl_last[nd]);
             U = (double)(td * blend_u<T>(f, tb, row, nd));
             V = (double)(td * blend_v<T>(f, tb, row, nd));
             return true;
         }
         float den = 1.0f;
-        if (n_wet < r.n) {
+        if (n_wet < rn) {
             float wsum = 0.0f;
 #pragma unroll
             for (int k = 0; k < 4; ++k)
@@ -238,9 +269,10 @@ __device__ KC_INL_STAGE bool stage_f32(const DMesh& m, const DBlend<T>& f, const
                 den = wsum;
             }
         }
-        for (int k = 0; k < r.n; ++k) {
-            if (n_wet < r.n && !wet[k]) continue;
-            const int nd = r.v[k];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (k >= rn || (n_wet < rn && !wet[k])) continue;
+            const int nd = rv[k];
             int kb;
             double ab;
             uv_bracket(m.dl_p, __ldg(&m.dl_last[nd]), zq, kb, ab);
@@ -253,16 +285,18 @@ __device__ KC_INL_STAGE bool stage_f32(const DMesh& m, const DBlend<T>& f, const
             Us += w[k] * un;
             Vs += w[k] * vn;
         }
-        if (n_wet < r.n) {
+        if (n_wet < rn) {
             Us /= den;
             Vs /= den;
         }
     } else {
         const int row = dims == 3 ? find_layer(m, z, nn) : 0;
-        for (int k = 0; k < r.n; ++k) {
-            Us += w[k] * blend_u<T>(f, tb, row, r.v[k]);
-            Vs += w[k] * blend_v<T>(f, tb, row, r.v[k]);
-        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (k < rn) {
+                Us += w[k] * blend_u<T>(f, tb, row, rv[k]);
+                Vs += w[k] * blend_v<T>(f, tb, row, rv[k]);
+            }
     }
     U = (double)(td * Us);
     V = (double)(td * Vs);
@@ -272,6 +306,8 @@ __device__ KC_INL_STAGE bool stage_f32(const DMesh& m, const DBlend<T>& f, const
 // The mixed form as a step-body policy (see PlainForm in kc_step.cuh).
 template <typename T>
 struct MixedForm {
+    static constexpr bool kExact = false;   // CUDA's sincos for sites and draws
+    static __device__ __forceinline__ Site site(double lon, double lat) { return make_site_fast(lon, lat); }
     static __device__ __forceinline__ bool uv2(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
                                                double lat, int nn, int hint, double alpha, double& U, double& V) {
         double W;

@@ -323,7 +323,7 @@ __device__ __forceinline__ void step3d_sigma_particle(const DMesh& m, const DBle
             if (s.kick) {
                 const long long pid = st.pid ? st.pid[i] : i;
                 int kel, kwel;
-                apply_kick(m, s, pid, realization_of(st, s, i), qn, lon0, lat0, z0p, pre_nn, false, lon_new, lat_new,
+                apply_kick<true>(m, s, pid, realization_of(st, s, i), qn, lon0, lat0, z0p, pre_nn, false, lon_new, lat_new,
                            z_new, status, nn_out, fr, false, kel, kwel);
                 if (status == ALIVE) {
                     const double H_post = ce.H;

@@ -49,7 +49,6 @@ struct DStep {
     double az_const;
     double Dmin, z0b_min;      // sigma column floor and bed clearance
     double alpha_end;          // blend fraction of the end-of-step surface (sigma)
-    int rng_exact;             // draws moved to the reference's C-library values (the plain form)
 };
 
 // displacement metric z0 = max(cos(lat) * 111120, 1) (integrators.py:2563-2565),
@@ -150,13 +149,14 @@ __device__ __forceinline__ int end_elem(const DMesh& m, double lon, double lat, 
 // kick (diffusion.py:485-529, :261-298), great-circle move, exact re-anchor
 // and containment re-check, revert to the pre-step state on leaving the
 // domain; 3-D reclamp in the new column.
+template <bool EXACT>
 static __device__ KC_INL_KICK void apply_kick(const DMesh& m, const DStep& s, long long pid, unsigned long long rid,
                                         const Site& qn,
                                         double pre_lon, double pre_lat, double pre_z, int pre_nn, bool is3d,
                                         double& lon, double& lat, double& z, int& status, int& nn, signed char& fr,
                                         bool want_w, int& kel, int& kwel) {
     double g1, g2;
-    normal_pair(s.rng_exact ? m.rx : DRngX{}, s.seed, rid, (unsigned long long)pid + s.pid_offset, s.step_i, 0ull, g1, g2);
+    normal_pair<EXACT>(m.rx, s.seed, rid, (unsigned long long)pid + s.pid_offset, s.step_i, 0ull, g1, g2);
     double abs_dt = s.dt >= 0.0 ? s.dt : -s.dt;
     double sq = sqrt(abs_dt);
     double sx = sqrt(2.0 * s.kh_x);
@@ -171,8 +171,8 @@ static __device__ KC_INL_KICK void apply_kick(const DMesh& m, const DStep& s, lo
         dy = dy + corr;
     }
     double lk, lak;
-    sphere_displace(qn, dx, dy, lk, lak);
-    Site qk = make_site(lk, lak);
+    sphere_displace<EXACT>(qn, dx, dy, lk, lak);
+    Site qk = EXACT ? make_site(lk, lak) : make_site_fast(lk, lak);
     int nk = site_anchor(m, qk);
     kel = end_scan(m, want_w, lk, lak, nk, kwel);
     if (kel < 0) {
@@ -231,7 +231,7 @@ __device__ __forceinline__ double az_at(const DBlend<T>& f, int k, int node) {
 // Euler-Maruyama increment with the Ito drift, both on |dt| (:302-330), the
 // vertical counter-RNG component; reflective bounds [z_levels[0],
 // depth[anchor]] (:426-455).
-template <typename T>
+template <typename T, bool EXACT>
 __device__ __noinline__ void apply_az(const DMesh& m, const DBlend<T>& f, const DStep& s, long long pid,
                                       unsigned long long rid, int nn, double& z) {
     double az = s.az_const, g = 0.0;
@@ -286,7 +286,7 @@ __device__ __noinline__ void apply_az(const DMesh& m, const DBlend<T>& f, const 
         g = 0.0;
     }
     double xi, unused;
-    normal_pair(s.rng_exact ? m.rx : DRngX{}, s.seed, rid, (unsigned long long)pid + s.pid_offset, s.step_i, 1ull, xi, unused);
+    normal_pair<EXACT>(m.rx, s.seed, rid, (unsigned long long)pid + s.pid_offset, s.step_i, 1ull, xi, unused);
     const double sdt = s.time_dir * s.dt;
     const double abs_dt = sdt >= 0.0 ? sdt : -sdt;
     const double dz = g * abs_dt + sqrt(2.0 * az * abs_dt) * xi;
@@ -312,7 +312,7 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
     int nn_out = pre_nn;
     signed char fr = st.fr[i];
     bool failed = false;
-    const Site q0 = make_site(lon0, lat0);
+    const Site q0 = Form::site(lon0, lat0);
     const int node_i = start_anchor(m, st, q0, pre_nn, i);
     const int e1 = stage_elem<WALK>(m, lon0, lat0, WALK ? st.elem[i] : -1, node_i);
     int e_last = e1, e_out = e1;
@@ -332,7 +332,7 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
     } else if (SCHEME == 1) {
         double lon_mid = wrap180(lon0 + 0.5 * dt * U1 / metric_z0(q0));
         double lat_mid = clamp_lat(lat0 + 0.5 * dt * V1 / SLM);
-        const Site qm = make_site(lon_mid, lat_mid);
+        const Site qm = Form::site(lon_mid, lat_mid);
         int nn_mid = site_anchor(m, qm);
         e_last = stage_elem<WALK>(m, lon_mid, lat_mid, e1, nn_mid);
         double U2, V2;
@@ -347,7 +347,7 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
         double dlat1 = dt * V1 / SLM;
         double lon2 = wrap180(lon0 + 0.5 * dlon1);
         double lat2 = clamp_lat(lat0 + 0.5 * dlat1);
-        const Site q2 = make_site(lon2, lat2);
+        const Site q2 = Form::site(lon2, lat2);
         const int n2 = site_anchor(m, q2);
         const int e2 = stage_elem<WALK>(m, lon2, lat2, e1, n2);
         double U2, V2;
@@ -358,7 +358,7 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
             double dlat2 = dt * V2 / SLM;
             double lon3 = wrap180(lon0 + 0.5 * dlon2);
             double lat3 = clamp_lat(lat0 + 0.5 * dlat2);
-            const Site q3 = make_site(lon3, lat3);
+            const Site q3 = Form::site(lon3, lat3);
             const int n3 = site_anchor(m, q3);
             const int e3 = stage_elem<WALK>(m, lon3, lat3, e2, n3);
             double U3, V3;
@@ -369,7 +369,7 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
                 double dlat3 = dt * V3 / SLM;
                 double lon4 = wrap180(lon0 + dlon3);
                 double lat4 = clamp_lat(lat0 + dlat3);
-                const Site q4 = make_site(lon4, lat4);
+                const Site q4 = Form::site(lon4, lat4);
                 const int n4 = site_anchor(m, q4);
                 e_last = stage_elem<WALK>(m, lon4, lat4, e3, n4);
                 double U4, V4;
@@ -387,7 +387,7 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
         }
     }
     if (!failed) {
-        const Site qn = make_site(lon_new, lat_new);
+        const Site qn = Form::site(lon_new, lat_new);
         int nn_new = site_anchor(m, qn);
         int ein;
         if constexpr (WALK) ein = walk_locate(m, lon_new, lat_new, e_last, nn_new);
@@ -403,7 +403,7 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
             if (s.kick) {
                 double zz = 0.0;
                 long long pid = st.pid ? st.pid[i] : i;
-                apply_kick(m, s, pid, realization_of(st, s, i), qn, lon0, lat0, 0.0, pre_nn, false, lon_new, lat_new,
+                apply_kick<Form::kExact>(m, s, pid, realization_of(st, s, i), qn, lon0, lat0, 0.0, pre_nn, false, lon_new, lat_new,
                            zz, status, nn_out, fr, false, sc_el, sc_wel);
             }
         }
@@ -450,6 +450,8 @@ __device__ __forceinline__ bool stage_uv(const DMesh& m, const DBlend<T>& f, con
 // arithmetic, 2-D only.
 template <typename T>
 struct LsqForm {
+    static constexpr bool kExact = true;
+    static __device__ __forceinline__ Site site(double lon, double lat) { return make_site(lon, lat); }
     static __device__ __forceinline__ bool uv2(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
                                                double lat, int nn, int hint, double alpha, double& U, double& V) {
         return interp_uv_lsq<T>(m, f, lon, lat, nn, s.time_dir, alpha, U, V);
@@ -458,6 +460,8 @@ struct LsqForm {
 
 template <typename T>
 struct PlainForm {
+    static constexpr bool kExact = true;   // correctly rounded sites and draws, the reference's draws
+    static __device__ __forceinline__ Site site(double lon, double lat) { return make_site(lon, lat); }
     static __device__ __forceinline__ bool uv2(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
                                                double lat, int nn, int hint, double alpha, double& U, double& V) {
         return interp_uv_bary<T>(m, f, lon, lat, nn, hint, s.time_dir, 0, alpha, U, V);
@@ -531,7 +535,7 @@ __device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DB
     signed char fr = st.fr[i];
     double lon_new = lon0, lat_new = lat0, z_new = z0p;
 
-    const Site q0 = make_site(lon0, lat0);
+    const Site q0 = Form::site(lon0, lat0);
     const int node_i = start_anchor(m, st, q0, pre_nn, i);
     int nn_out = node_i;
     const int e1 = stage_elem<WALK>(m, lon0, lat0, WALK ? st.elem[i] : -1, node_i);
@@ -553,20 +557,20 @@ __device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DB
         } else {
             const double dl1 = dt * U1 / metric_z0(q0), dd1 = dt * V1 / SLM, dz1 = dt * W1;
             const double l2 = wrap180(lon0 + 0.5 * dl1), t2 = clamp_lat(lat0 + 0.5 * dd1), z2 = z0p + 0.5 * dz1;
-            const Site q2 = make_site(l2, t2);
+            const Site q2 = Form::site(l2, t2);
             double U2, V2, W2;
             int e2, e3;
             ok = stage3d<T, Form, WALK>(m, f, s, 1, l2, t2, z2, q2, e1, e2, U2, V2, W2);
             if (ok) {
                 const double dl2 = dt * U2 / metric_z0(q2), dd2 = dt * V2 / SLM, dz2 = dt * W2;
                 const double l3 = wrap180(lon0 + 0.5 * dl2), t3 = clamp_lat(lat0 + 0.5 * dd2), z3 = z0p + 0.5 * dz2;
-                const Site q3 = make_site(l3, t3);
+                const Site q3 = Form::site(l3, t3);
                 double U3, V3, W3;
                 ok = stage3d<T, Form, WALK>(m, f, s, 2, l3, t3, z3, q3, e2, e3, U3, V3, W3);
                 if (ok) {
                     const double dl3 = dt * U3 / metric_z0(q3), dd3 = dt * V3 / SLM, dz3 = dt * W3;
                     const double l4 = wrap180(lon0 + dl3), t4 = clamp_lat(lat0 + dd3), z4 = z0p + dz3;
-                    const Site q4 = make_site(l4, t4);
+                    const Site q4 = Form::site(l4, t4);
                     double U4, V4, W4;
                     ok = stage3d<T, Form, WALK>(m, f, s, 3, l4, t4, z4, q4, e3, e_last, U4, V4, W4);
                     if (ok) {
@@ -585,7 +589,7 @@ __device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DB
     if (!ok) {
         status = OUTSIDE; fr = FR_INTERP;
     } else {
-        const Site qn = make_site(a, b);
+        const Site qn = Form::site(a, b);
         const int nn_new = site_anchor(m, qn);
         int ein;
         if constexpr (WALK) ein = walk_locate(m, a, b, e_last, nn_new);
@@ -603,11 +607,11 @@ __device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DB
             e_out = ein;
             if (s.kick) {
                 long long pid = st.pid ? st.pid[i] : i;
-                apply_kick(m, s, pid, realization_of(st, s, i), qn, lon0, lat0, z0p, pre_nn, true, lon_new, lat_new, z_new,
+                apply_kick<Form::kExact>(m, s, pid, realization_of(st, s, i), qn, lon0, lat0, z0p, pre_nn, true, lon_new, lat_new, z_new,
                            status, nn_out, fr, s.w_code == 1, sc_el, sc_wel);
             }
             if (s.az_on && status == ALIVE)
-                apply_az<T>(m, f, s, st.pid ? st.pid[i] : i, realization_of(st, s, i), nn_out, z_new);
+                apply_az<T, Form::kExact>(m, f, s, st.pid ? st.pid[i] : i, realization_of(st, s, i), nn_out, z_new);
         }
     }
     st.lon[i] = lon_new;
@@ -640,7 +644,7 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
     signed char fr = st.fr[i];
     double lon_new = lon0, lat_new = lat0, z_new = z0p;
 
-    const Site q0 = make_site(lon0, lat0);
+    const Site q0 = Form::site(lon0, lat0);
     const int node_i = start_anchor(m, st, q0, pre_nn, i);
     int nn_out = node_i;
     const int e1 = stage_elem<WALK>(m, lon0, lat0, WALK ? st.elem[i] : -1, node_i);
@@ -659,7 +663,7 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
         const double lon_mid = wrap180(lon0 + 0.5 * dt * U1 / metric_z0(q0));
         const double lat_mid = clamp_lat(lat0 + 0.5 * dt * V1 / SLM);
         const double z_mid = z0p + W1 * 0.5 * dt;
-        const Site qm = make_site(lon_mid, lat_mid);
+        const Site qm = Form::site(lon_mid, lat_mid);
         const int nn_mid = site_anchor(m, qm);
         const int em = stage_elem<WALK>(m, lon_mid, lat_mid, e1, nn_mid);
         double U2, V2, W2;
@@ -669,7 +673,7 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
             const double ln = wrap180(lon0 + dt * U2 / metric_z0(qm));
             const double lt = clamp_lat(lat0 + dt * V2 / SLM);
             double zn = z0p + W2 * dt;
-            const Site qn = make_site(ln, lt);
+            const Site qn = Form::site(ln, lt);
             const int nn_new = site_anchor(m, qn);
             int ein;
             if constexpr (WALK) ein = walk_locate(m, ln, lt, em, nn_new);
@@ -687,11 +691,11 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
                 e_out = ein;
                 if (s.kick) {
                     long long pid = st.pid ? st.pid[i] : i;
-                    apply_kick(m, s, pid, realization_of(st, s, i), qn, lon0, lat0, z0p, pre_nn, true, lon_new, lat_new,
+                    apply_kick<Form::kExact>(m, s, pid, realization_of(st, s, i), qn, lon0, lat0, z0p, pre_nn, true, lon_new, lat_new,
                                z_new, status, nn_out, fr, s.w_code == 1, sc_el, sc_wel);
                 }
                 if (s.az_on && status == ALIVE)
-                    apply_az<T>(m, f, s, st.pid ? st.pid[i] : i, realization_of(st, s, i), nn_out, z_new);
+                    apply_az<T, Form::kExact>(m, f, s, st.pid ? st.pid[i] : i, realization_of(st, s, i), nn_out, z_new);
             }
         }
     }
