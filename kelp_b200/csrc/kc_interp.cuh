@@ -104,21 +104,51 @@ __device__ __forceinline__ void load_ring(const DMesh& m, int4 e, Ring& r) {
     r.n = n;
 }
 
+// The compacted ring as vertex ids only (load_ring's order and dedupe; slot
+// 3 repeats slot 0 for a triangle): the coordinates are read where they are
+// used, so no double-precision vertex array stays live across the loops.
+struct RingId {
+    int v[4];
+    int n;
+};
+
+__device__ __forceinline__ void ring_ids(int4 e, RingId& r) {
+    int n = 0, first = -1;
+    r.v[0] = r.v[1] = r.v[2] = r.v[3] = -1;
+    auto push = [&](int id) {
+        if (n == 0) r.v[0] = id;
+        else if (n == 1) r.v[1] = id;
+        else if (n == 2) r.v[2] = id;
+        else r.v[3] = id;
+        ++n;
+    };
+    if (e.x >= 0) { push(e.x); first = e.x; }
+    if (e.y >= 0 && !(n > 0 && e.y == first)) { push(e.y); if (first < 0) first = e.y; }
+    if (e.z >= 0 && !(n > 0 && e.z == first)) { push(e.z); if (first < 0) first = e.z; }
+    if (e.w >= 0 && !(n > 0 && e.w == first)) push(e.w);
+    if (n == 3) r.v[3] = r.v[0];
+    r.n = n;
+}
+
 // Vertex weights of the point in the containing element, projected around the
 // wrapped-delta centroid (interpolate.py:1376-1402) with radius R; false for
 // the degenerate-triangle sentinel or an element with fewer than 3 vertices.
+// Two passes over the vertices (sums, then the projection), each operation
+// in the reference's order.
 __device__ __forceinline__ bool bary_weights_core(const DMesh& m, int elem, double xp, double yp, double R,
-                                                  Ring& r, double* w) {
-    load_ring(m, __ldg(&m.en[elem]), r);
+                                                  RingId& r, double* w) {
+    ring_ids(__ldg(&m.en[elem]), r);
     const int nv = r.n;
     if (nv < 3) return false;
-    const double lon_ref = r.ln[0];
-    double dsum = 0.0, lat0 = 0.0;
+    const double2 a0 = __ldg(&m.ll[r.v[0]]);
+    const double lon_ref = a0.x;
+    double dsum = 0.0 + wrap180(a0.x - lon_ref), lat0 = 0.0 + a0.y;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 1; k < 4; ++k) {
         if (k < nv) {
-            dsum += wrap180(r.ln[k] - lon_ref);
-            lat0 += r.la[k];
+            const double2 a = __ldg(&m.ll[r.v[k]]);
+            dsum += wrap180(a.x - lon_ref);
+            lat0 += a.y;
         }
     }
     const double lon0 = lon_ref + dsum / (double)nv;
@@ -127,8 +157,9 @@ __device__ __forceinline__ bool bary_weights_core(const DMesh& m, int elem, doub
     double vx[4], vy[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        vx[k] = wrap180(r.ln[k] - lon0) * DEG2RAD * R * cosl;
-        vy[k] = (r.la[k] - lat0) * DEG2RAD * R;
+        const double2 a = __ldg(&m.ll[r.v[k]]);
+        vx[k] = wrap180(a.x - lon0) * DEG2RAD * R * cosl;
+        vy[k] = (a.y - lat0) * DEG2RAD * R;
     }
     const double px = wrap180(xp - lon0) * DEG2RAD * R * cosl;
     const double py = (yp - lat0) * DEG2RAD * R;
@@ -149,7 +180,7 @@ __device__ KC_INL_STAGE bool interp_uv_at(const DMesh& m, const DBlend<T>& f, in
                                           double time_dir, int row, double alpha, double& U, double& V) {
     U = 0.0;
     V = 0.0;
-    Ring r;
+    RingId r;
     double w[4];
     if (!bary_weights_core(m, elem, xp, yp, m.r_earth, r, w)) return false;
     const long long base = (long long)row * f.n;
@@ -283,7 +314,7 @@ __device__ __noinline__ bool interp_uv_dl_at(const DMesh& m, const DBlend<T>& f,
                                              double z, double time_dir, double alpha, double& U, double& V) {
     U = 0.0;
     V = 0.0;
-    Ring r;
+    RingId r;
     double w[4];
     if (!bary_weights_core(m, elem, xp, yp, m.r_earth, r, w)) return false;
     const int nv = r.n;
@@ -575,37 +606,32 @@ template <typename T>
 __device__ KC_INL_STAGE double w_bary_at(const DMesh& m, const DBlend<T>& f, double alpha, double xp, double yp,
                                          double z, int el, double time_dir) {
     const WLoc Lz = w_locate(m, z);
-    Ring r;
-    load_ring(m, __ldg(&m.en[el]), r);
+    RingId r;
+    ring_ids(__ldg(&m.en[el]), r);
     const int nvv = r.n;
-    double lmin = fmin(fmin(r.ln[0], r.ln[1]), r.ln[2]), lmax = fmax(fmax(r.ln[0], r.ln[1]), r.ln[2]);
-    if (nvv == 4) { lmin = fmin(lmin, r.ln[3]); lmax = fmax(lmax, r.ln[3]); }
-    double lon0;
-    if (lmax - lmin > 180.0) {
-        double d = 0.0;
+    // pass 1: the running extent and sums in the reference's order
+    const double2 a0 = __ldg(&m.ll[r.v[0]]);
+    double lmin = a0.x, lmax = a0.x, d = 0.0 + wrap180(a0.x - a0.x), sm = 0.0 + a0.x, lat0 = 0.0 + a0.y;
 #pragma unroll
-        for (int v = 0; v < 4; ++v)
-            if (v < nvv) d += wrap180(r.ln[v] - r.ln[0]);
-        lon0 = r.ln[0] + d / (double)nvv;
-    } else {
-        double sm = 0.0;
-#pragma unroll
-        for (int v = 0; v < 4; ++v)
-            if (v < nvv) sm += r.ln[v];
-        lon0 = sm / (double)nvv;
+    for (int v = 1; v < 4; ++v) {
+        if (v < nvv) {
+            const double2 a = __ldg(&m.ll[r.v[v]]);
+            if (v < 3 || nvv == 4) { lmin = fmin(lmin, a.x); lmax = fmax(lmax, a.x); }
+            d += wrap180(a.x - a0.x);
+            sm += a.x;
+            lat0 += a.y;
+        }
     }
-    double lat0 = 0.0;
-#pragma unroll
-    for (int v = 0; v < 4; ++v)
-        if (v < nvv) lat0 += r.la[v];
+    const double lon0 = lmax - lmin > 180.0 ? a0.x + d / (double)nvv : sm / (double)nvv;
     lat0 /= (double)nvv;
     const double cos_lat0 = __ldg(&m.ecos[el]).y;
     const double R = 6371000.0;
     double vx[4], vy[4];
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
-        vx[v] = wrap180(r.ln[v] - lon0) * DEG2RAD * R * cos_lat0;
-        vy[v] = (r.la[v] - lat0) * DEG2RAD * R;
+        const double2 a = __ldg(&m.ll[r.v[v]]);
+        vx[v] = wrap180(a.x - lon0) * DEG2RAD * R * cos_lat0;
+        vy[v] = (a.y - lat0) * DEG2RAD * R;
     }
     const double px = wrap180(xp - lon0) * DEG2RAD * R * cos_lat0;
     const double py = (yp - lat0) * DEG2RAD * R;

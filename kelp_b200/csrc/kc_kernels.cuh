@@ -188,10 +188,17 @@ struct MultiHead {
     int n_steps;
 };
 
-// BLOCK threads per block, BLOCK * blocks-per-SM = 1024 threads: the same
-// 64-register budget at either block size.
+// BLOCK threads per block; the resident threads per SM those bounds ask for
+// are the per-step kernels' (1024 for 2-D: 64 registers; 128 x
+// KC_RK2_3D_MIN_BLOCKS / KC_UNFUSED_3D_MIN_BLOCKS for 3-D), so a fused
+// launch gets the same register budget at either block size.
+template <int DIMS, int SCHEME>
+constexpr int multi_threads_per_sm() {
+    return DIMS == 2 ? 1024 : 128 * (SCHEME == 1 ? KC_RK2_3D_MIN_BLOCKS : KC_UNFUSED_3D_MIN_BLOCKS);
+}
+
 template <typename T, int DIMS, int SCHEME, typename Form, int BLOCK>
-__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_multi(const __grid_constant__ kc::DMesh m,
+__global__ void __launch_bounds__(BLOCK, multi_threads_per_sm<DIMS, SCHEME>() / BLOCK) k_multi(const __grid_constant__ kc::DMesh m,
                                                                      const MultiHead* __restrict__ head,
                                                                      const StepPack<T>* __restrict__ packs) {
     const kc::DState& st = head->st;
