@@ -156,7 +156,7 @@ static __device__ __noinline__ bool cgrid_core(const DMesh& m, const DBlend<T>& 
 template <typename T>
 struct CgridForm {
     static constexpr bool kExact = true;
-    static __device__ __forceinline__ Site site(double lon, double lat) { return make_site(lon, lat); }
+    static __device__ __forceinline__ Site site(double lon, double lat) { return make_site_fast(lon, lat); }
     static __device__ __forceinline__ bool uv2(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
                                                double lat, int nn, int hint, double alpha, double& U, double& V) {
         double W;
@@ -203,7 +203,7 @@ __device__ __forceinline__ void step3d_cgrid_particle(const DMesh& m, const DBle
                                                       const DStep& s, long long i) {
     constexpr int NS = SCHEME == 0 ? 1 : (SCHEME == 1 ? 2 : 4);
     const double lon0 = st.lon[i], lat0 = st.lat[i], z0 = st.z[i];
-    const Site q0 = make_site(lon0, lat0);
+    const Site q0 = make_site_fast(lon0, lat0);   // the anchor search only: positions use cos_cr below
     const int nn0 = start_anchor(m, st, q0, st.nn[i], i);
     if (st.status[i] != ALIVE) {
         st.U[i] = 0.0;
@@ -233,7 +233,7 @@ __device__ __forceinline__ void step3d_cgrid_particle(const DMesh& m, const DBle
         }
         double Un = 0.0, Vn = 0.0, Wn = 0.0;
         if (ok) {
-            const int nnn = n ? site_anchor(m, make_site(ln, lt)) : nn0;
+            const int nnn = n ? site_anchor(m, make_site_fast(ln, lt)) : nn0;
             ok = cgrid_core<T>(m, f, s.ak[n], ln, lt, sn, nnn, n ? -1 : (ok0 ? e0 : -1), s.time_dir, true, Un, Vn, Wn);
         }
         if (n == 0) {
@@ -258,7 +258,7 @@ __device__ __forceinline__ void step3d_cgrid_particle(const DMesh& m, const DBle
         sv = s0 + d2;
         if (sv < 0.0) sv = 0.0;
     }
-    int nne = site_anchor(m, make_site(ln, lt));
+    int nne = site_anchor(m, make_site_fast(ln, lt));
     const int e1 = contain_local(m, ln, lt, nne);
     const bool in_dom = e1 >= 0;
     double zn = z0;

@@ -53,6 +53,15 @@ struct DStep {
 
 // displacement metric z0 = max(cos(lat) * 111120, 1) (integrators.py:2563-2565),
 // cos(lat) from the site anchored at that latitude
+// EXACT (the plain forms): cos(lat) correctly rounded, as the site of the
+// anchor search may carry CUDA's value.
+template <bool EXACT>
+__device__ __forceinline__ double metric_z0f(const Site& q) {
+    double z0 = (EXACT ? cr::cos_cr(q.lat * DEG2RAD) : q.cos_lat) * SLM;
+    if (z0 < 1.0) z0 = 1.0;
+    return z0;
+}
+
 __device__ __forceinline__ double metric_z0(const Site& q) {
     double z0 = q.cos_lat * SLM;
     if (z0 < 1.0) z0 = 1.0;
@@ -171,8 +180,9 @@ static __device__ KC_INL_KICK void apply_kick(const DMesh& m, const DStep& s, lo
         dy = dy + corr;
     }
     double lk, lak;
-    sphere_displace<EXACT>(qn, dx, dy, lk, lak);
-    Site qk = EXACT ? make_site(lk, lak) : make_site_fast(lk, lak);
+    if constexpr (EXACT) sphere_displace<true>(make_site(qn.lon, qn.lat), dx, dy, lk, lak);   // correctly rounded trig
+    else sphere_displace<false>(qn, dx, dy, lk, lak);
+    Site qk = make_site_fast(lk, lak);   // the anchor search of the kicked position only
     int nk = site_anchor(m, qk);
     kel = end_scan(m, want_w, lk, lak, nk, kwel);
     if (kel < 0) {
@@ -327,10 +337,10 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
     if (!ok1) {
         status = OUTSIDE; fr = FR_INTERP; nn_out = node_i; failed = true;
     } else if (SCHEME == 0) {
-        lon_new = wrap180(lon0 + dt * U1 / metric_z0(q0));
+        lon_new = wrap180(lon0 + dt * U1 / metric_z0f<Form::kExact>(q0));
         lat_new = clamp_lat(lat0 + dt * V1 / SLM);
     } else if (SCHEME == 1) {
-        double lon_mid = wrap180(lon0 + 0.5 * dt * U1 / metric_z0(q0));
+        double lon_mid = wrap180(lon0 + 0.5 * dt * U1 / metric_z0f<Form::kExact>(q0));
         double lat_mid = clamp_lat(lat0 + 0.5 * dt * V1 / SLM);
         const Site qm = Form::site(lon_mid, lat_mid);
         int nn_mid = site_anchor(m, qm);
@@ -339,11 +349,11 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
         if (!Form::uv2(m, f, s, lon_mid, lat_mid, nn_mid, e_last, s.ak[1], U2, V2)) {
             status = OUTSIDE; fr = FR_INTERP; nn_out = node_i; failed = true;
         } else {
-            lon_new = wrap180(lon0 + dt * U2 / metric_z0(qm));
+            lon_new = wrap180(lon0 + dt * U2 / metric_z0f<Form::kExact>(qm));
             lat_new = clamp_lat(lat0 + dt * V2 / SLM);
         }
     } else {
-        double dlon1 = dt * U1 / metric_z0(q0);
+        double dlon1 = dt * U1 / metric_z0f<Form::kExact>(q0);
         double dlat1 = dt * V1 / SLM;
         double lon2 = wrap180(lon0 + 0.5 * dlon1);
         double lat2 = clamp_lat(lat0 + 0.5 * dlat1);
@@ -354,7 +364,7 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
         if (!Form::uv2(m, f, s, lon2, lat2, n2, e2, s.ak[1], U2, V2)) {
             status = OUTSIDE; fr = FR_INTERP; nn_out = node_i; failed = true;
         } else {
-            double dlon2 = dt * U2 / metric_z0(q2);
+            double dlon2 = dt * U2 / metric_z0f<Form::kExact>(q2);
             double dlat2 = dt * V2 / SLM;
             double lon3 = wrap180(lon0 + 0.5 * dlon2);
             double lat3 = clamp_lat(lat0 + 0.5 * dlat2);
@@ -365,7 +375,7 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
             if (!Form::uv2(m, f, s, lon3, lat3, n3, e3, s.ak[2], U3, V3)) {
                 status = OUTSIDE; fr = FR_INTERP; nn_out = node_i; failed = true;
             } else {
-                double dlon3 = dt * U3 / metric_z0(q3);
+                double dlon3 = dt * U3 / metric_z0f<Form::kExact>(q3);
                 double dlat3 = dt * V3 / SLM;
                 double lon4 = wrap180(lon0 + dlon3);
                 double lat4 = clamp_lat(lat0 + dlat3);
@@ -376,7 +386,7 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
                 if (!Form::uv2(m, f, s, lon4, lat4, n4, e_last, s.ak[3], U4, V4)) {
                     status = OUTSIDE; fr = FR_INTERP; nn_out = node_i; failed = true;
                 } else {
-                    double dlon4 = dt * U4 / metric_z0(q4);
+                    double dlon4 = dt * U4 / metric_z0f<Form::kExact>(q4);
                     double dlat4 = dt * V4 / SLM;
                     double dlon = (dlon1 + 2.0 * dlon2 + 2.0 * dlon3 + dlon4) / 6.0;
                     double dlat = (dlat1 + 2.0 * dlat2 + 2.0 * dlat3 + dlat4) / 6.0;
@@ -451,7 +461,7 @@ __device__ __forceinline__ bool stage_uv(const DMesh& m, const DBlend<T>& f, con
 template <typename T>
 struct LsqForm {
     static constexpr bool kExact = true;
-    static __device__ __forceinline__ Site site(double lon, double lat) { return make_site(lon, lat); }
+    static __device__ __forceinline__ Site site(double lon, double lat) { return make_site_fast(lon, lat); }
     static __device__ __forceinline__ bool uv2(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
                                                double lat, int nn, int hint, double alpha, double& U, double& V) {
         return interp_uv_lsq<T>(m, f, lon, lat, nn, s.time_dir, alpha, U, V);
@@ -459,9 +469,13 @@ struct LsqForm {
 };
 
 template <typename T>
+// kExact: the displacement metric, the kick's move and the draws take the
+// correctly rounded trigonometry (the reference's values but where the C
+// library misrounds) and the table-corrected draws; sites carry CUDA's
+// sincos, as they only feed the anchor search.
 struct PlainForm {
-    static constexpr bool kExact = true;   // correctly rounded sites and draws, the reference's draws
-    static __device__ __forceinline__ Site site(double lon, double lat) { return make_site(lon, lat); }
+    static constexpr bool kExact = true;
+    static __device__ __forceinline__ Site site(double lon, double lat) { return make_site_fast(lon, lat); }
     static __device__ __forceinline__ bool uv2(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
                                                double lat, int nn, int hint, double alpha, double& U, double& V) {
         return interp_uv_bary<T>(m, f, lon, lat, nn, hint, s.time_dir, 0, alpha, U, V);
@@ -551,30 +565,30 @@ __device__ __forceinline__ void step3d_unfused_particle(const DMesh& m, const DB
     double a = lon0, b = lat0, c = z0p;
     if (ok) {
         if (SCHEME == 0) {
-            a = wrap180(lon0 + dt * U1 / metric_z0(q0));
+            a = wrap180(lon0 + dt * U1 / metric_z0f<Form::kExact>(q0));
             b = clamp_lat(lat0 + dt * V1 / SLM);
             c = z0p + W1 * dt;
         } else {
-            const double dl1 = dt * U1 / metric_z0(q0), dd1 = dt * V1 / SLM, dz1 = dt * W1;
+            const double dl1 = dt * U1 / metric_z0f<Form::kExact>(q0), dd1 = dt * V1 / SLM, dz1 = dt * W1;
             const double l2 = wrap180(lon0 + 0.5 * dl1), t2 = clamp_lat(lat0 + 0.5 * dd1), z2 = z0p + 0.5 * dz1;
             const Site q2 = Form::site(l2, t2);
             double U2, V2, W2;
             int e2, e3;
             ok = stage3d<T, Form, WALK>(m, f, s, 1, l2, t2, z2, q2, e1, e2, U2, V2, W2);
             if (ok) {
-                const double dl2 = dt * U2 / metric_z0(q2), dd2 = dt * V2 / SLM, dz2 = dt * W2;
+                const double dl2 = dt * U2 / metric_z0f<Form::kExact>(q2), dd2 = dt * V2 / SLM, dz2 = dt * W2;
                 const double l3 = wrap180(lon0 + 0.5 * dl2), t3 = clamp_lat(lat0 + 0.5 * dd2), z3 = z0p + 0.5 * dz2;
                 const Site q3 = Form::site(l3, t3);
                 double U3, V3, W3;
                 ok = stage3d<T, Form, WALK>(m, f, s, 2, l3, t3, z3, q3, e2, e3, U3, V3, W3);
                 if (ok) {
-                    const double dl3 = dt * U3 / metric_z0(q3), dd3 = dt * V3 / SLM, dz3 = dt * W3;
+                    const double dl3 = dt * U3 / metric_z0f<Form::kExact>(q3), dd3 = dt * V3 / SLM, dz3 = dt * W3;
                     const double l4 = wrap180(lon0 + dl3), t4 = clamp_lat(lat0 + dd3), z4 = z0p + dz3;
                     const Site q4 = Form::site(l4, t4);
                     double U4, V4, W4;
                     ok = stage3d<T, Form, WALK>(m, f, s, 3, l4, t4, z4, q4, e3, e_last, U4, V4, W4);
                     if (ok) {
-                        const double dl4 = dt * U4 / metric_z0(q4), dd4 = dt * V4 / SLM, dz4 = dt * W4;
+                        const double dl4 = dt * U4 / metric_z0f<Form::kExact>(q4), dd4 = dt * V4 / SLM, dz4 = dt * W4;
                         const double dl = (dl1 + 2.0 * dl2 + 2.0 * dl3 + dl4) / 6.0;
                         const double dd = (dd1 + 2.0 * dd2 + 2.0 * dd3 + dd4) / 6.0;
                         const double dz = (dz1 + 2.0 * dz2 + 2.0 * dz3 + dz4) / 6.0;
@@ -660,7 +674,7 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
     if (!ok1) {
         status = OUTSIDE; fr = FR_INTERP;
     } else {
-        const double lon_mid = wrap180(lon0 + 0.5 * dt * U1 / metric_z0(q0));
+        const double lon_mid = wrap180(lon0 + 0.5 * dt * U1 / metric_z0f<Form::kExact>(q0));
         const double lat_mid = clamp_lat(lat0 + 0.5 * dt * V1 / SLM);
         const double z_mid = z0p + W1 * 0.5 * dt;
         const Site qm = Form::site(lon_mid, lat_mid);
@@ -670,7 +684,7 @@ __device__ __forceinline__ void step3d_rk2_particle(const DMesh& m, const DBlend
         if (!Form::uvw3(m, f, s, lon_mid, lat_mid, nn_mid, em, -3, z_mid, s.ak[1], U2, V2, W2)) {
             status = OUTSIDE; fr = FR_INTERP;
         } else {
-            const double ln = wrap180(lon0 + dt * U2 / metric_z0(qm));
+            const double ln = wrap180(lon0 + dt * U2 / metric_z0f<Form::kExact>(qm));
             const double lt = clamp_lat(lat0 + dt * V2 / SLM);
             double zn = z0p + W2 * dt;
             const Site qn = Form::site(ln, lt);
