@@ -367,6 +367,26 @@ KC_CR_HD double cos_cr(double x) {
     return cs;
 }
 
+// Out-of-line entry points for the step kernels: the double-double
+// temporaries of the correctly rounded paths then live in the callee instead
+// of raising the register pressure of a large kernel body.
+#ifndef KC_CR_OUTLINE
+#define KC_CR_OUTLINE 1
+#endif
+#if defined(__CUDACC__)
+#if KC_CR_OUTLINE
+#define KC_CR_K __device__ __noinline__ static
+#else
+#define KC_CR_K __device__ __forceinline__ static
+#endif
+KC_CR_K double cos_cr_k(double x) { return cos_cr(x); }
+KC_CR_K double2 sincos_cr_k(double x) {
+    double2 r;
+    sincos_cr(x, &r.x, &r.y);
+    return r;
+}
+#endif
+
 KC_CR_HD void sincos_cr_checked(double x, double* sn, double* cs, bool* ambiguous) {
     DD s, c;
     sincos_dd(x, s, c);

@@ -957,8 +957,13 @@ __device__ __forceinline__ void sphere_displace(const Site& q, double dx, double
     const double cl = q.cos_lon, sl = q.sin_lon, cp = q.cos_lat, sp = q.sin_lat;
     double delta = dist / R_METRIC;
     double sdel, c;
-    if constexpr (EXACT) cr::sincos_cr(delta, &sdel, &c);
-    else sincos(delta, &sdel, &c);
+    if constexpr (EXACT) {
+        const double2 sc = cr::sincos_cr_k(delta);
+        sdel = sc.x;
+        c = sc.y;
+    } else {
+        sincos(delta, &sdel, &c);
+    }
     double s = sdel / dist;
     double tx = -sl * dx - sp * cl * dy;
     double ty = cl * dx - sp * sl * dy;

@@ -57,7 +57,7 @@ struct DStep {
 // anchor search may carry CUDA's value.
 template <bool EXACT>
 __device__ __forceinline__ double metric_z0f(const Site& q) {
-    double z0 = (EXACT ? cr::cos_cr(q.lat * DEG2RAD) : q.cos_lat) * SLM;
+    double z0 = (EXACT ? cr::cos_cr_k(q.lat * DEG2RAD) : q.cos_lat) * SLM;
     if (z0 < 1.0) z0 = 1.0;
     return z0;
 }
