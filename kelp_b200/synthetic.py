@@ -242,3 +242,74 @@ def sort_seeds(lon, lat, z, cell: float = 1.0):
            + np.floor((np.asarray(lon) + 180.0) / cell).astype(np.int64) % nx)
     order = np.lexsort((np.asarray(z), key))
     return np.asarray(lon)[order], np.asarray(lat)[order], np.asarray(z)[order]
+
+
+def tripolar_grid(ny: int, nx: int, *, fold: str = "T", cap_lat: float = 20.0, pole_lat: float = 65.0,
+                  pole_lon: float = 73.0, south_lat: float = -78.0):
+    """An ORCA-like tripolar raster in canonical form: ``(layout, glamf,
+    gphif, glamt, gphit)``.  East-west periodic with one halo column each
+    side (nx - 2 columns, 360 / (nx - 2) degrees apart) and a north fold
+    pivoting on T or F points with one halo row.  South of ``cap_lat`` the
+    rows are latitude circles, uniformly spaced from ``south_lat``; north of
+    it a bipolar cap: in polar stereographic coordinates (the cap boundary
+    the unit circle) a column runs straight from its boundary point to that
+    point's projection on the segment between the two grid poles (at
+    ``pole_lat``, ``pole_lon`` and ``pole_lon + 180``), which is the fold
+    line; a column and its mirror image about the poles' meridian plane meet
+    there.  The fold copies are set from their canonical points."""
+    from .nemo import CgridLayout, to_canonical
+    lay = CgridLayout((ny, nx), periodic=True, fold=fold)
+    c0, w, J = lay.first_col, lay.width, lay.fold_row
+    step = 360.0 / w
+    fold_r = J + (0.5 if fold == "F" else 0.0)             # the fold line's row coordinate
+    axis = np.radians(pole_lon - (0.5 * step if fold == "F" else 0.0))
+    t_cap = np.tan(np.radians(90.0 - cap_lat) / 2.0)
+    a = np.tan(np.radians(90.0 - pole_lat) / 2.0) / t_cap
+    r_cap = round(fold_r * (cap_lat - south_lat) / (cap_lat - south_lat + (90.0 - cap_lat)))
+
+    def points(oy, ox):
+        r, i = np.meshgrid(np.arange(ny) + 0.5 * oy, np.arange(nx) + 0.5 * ox, indexing="ij")
+        lam = np.radians(pole_lon + (i - c0) * step)
+        lon = np.degrees(lam)
+        lat = south_lat + (cap_lat - south_lat) * r / r_cap
+        cap = r > r_cap
+        s = (r[cap] - r_cap) / (fold_r - r_cap)
+        proj = a * np.cos(lam[cap] - axis)
+        px = (1.0 - s) * np.cos(lam[cap]) + s * proj * np.cos(axis)
+        py = (1.0 - s) * np.sin(lam[cap]) + s * proj * np.sin(axis)
+        rho = np.hypot(px, py)
+        lon[cap] = np.degrees(np.arctan2(py, px))
+        lat[cap] = 90.0 - np.degrees(2.0 * np.arctan(rho * t_cap))
+        return ((lon + 180.0) % 360.0) - 180.0, lat
+
+    flon, flat = points(1, 1)
+    tlon, tlat = points(0, 0)
+    return (lay, to_canonical(flon, lay, "F"), to_canonical(flat, lay, "F"), to_canonical(tlon, lay, "T"),
+            to_canonical(tlat, lay, "T"))
+
+
+def cgrid_stream_flow(glamf, gphif, amp: float = 5e5):
+    """Face velocities of a smooth non-divergent flow on a C-grid raster, from
+    a streamfunction psi (m^2/s) sampled at the F-points: the east-face (u)
+    transport psi(F(j,i)) - psi(F(j-1,i)) over the face's great-circle length
+    e2u, the north-face (v) transport psi(F(j,i-1)) - psi(F(j,i)) over e1v;
+    every cell's net transport is zero.  psi is a smooth function of the
+    unit-sphere position, so halo and fold copies agree.  Returns
+    (u, v, e2u, e1v) rasters (the first row / column: the raster's own
+    neighbours, edge-clamped)."""
+    la, lo = np.radians(gphif), np.radians(glamf)
+    x, y, z = np.cos(la) * np.cos(lo), np.cos(la) * np.sin(lo), np.sin(la)
+    psi = amp * (0.6 * x * y + 0.5 * np.sin(2.0 * z + 0.3) * x + 0.4 * np.cos(3.0 * y) * z + 0.3 * z * z)
+
+    def arc(j0, i0, j1, i1):
+        dot = x[j0, i0] * x[j1, i1] + y[j0, i0] * y[j1, i1] + z[j0, i0] * z[j1, i1]
+        return 6371000.0 * np.arccos(np.clip(dot, -1.0, 1.0))
+
+    ny, nx = glamf.shape
+    jj, ii = np.indices((ny, nx))
+    js, iw = np.maximum(jj - 1, 0), np.maximum(ii - 1, 0)
+    e2u = np.maximum(arc(js, ii, jj, ii), 1.0)
+    e1v = np.maximum(arc(jj, iw, jj, ii), 1.0)
+    u = (psi[jj, ii] - psi[js, ii]) / e2u
+    v = (psi[jj, iw] - psi[jj, ii]) / e1v
+    return u, v, e2u, e1v

@@ -212,68 +212,84 @@ def c4_small() -> Workload:
 
 
 def c5(P: int = 2_000_000, ny: int = 1021, nx: int = 1442, n_levels: int = 75, n_snap: int = 2) -> Workload:
-    """NEMO C-grid 3-D: a curvilinear 1442 x 1021 raster (F-points 0.1 x 0.08
-    deg with bent columns and rows; a regional raster -- the tripolar fold and
-    E-W halo are not built), ~30 % land from smooth noise, 75 z-levels
-    (1 m .. 5800 m stretched) with partial bottom cells over a smooth 200-5500
-    m bathymetry, model face widths and cell areas; face-raster u/v (75, ny*nx)
-    and w (76, ny*nx) float32, a mesoscale field of 0.5 m/s rms decaying with
-    depth, 2 five-day records cycled; 2 M particles uniform over the wet cells
-    and in their columns; the exact C-grid RK4 in the fractional level
+    """NEMO C-grid 3-D on a global tripolar ORCA-like raster of 1442 x 1021
+    (kelp_b200.synthetic.tripolar_grid: 1440 columns 0.25 deg apart plus the
+    two E-W halo columns, a T-pivot north fold with its halo row, the two grid
+    poles over land at 65 N, 73 E / 107 W), ~30 % land from smooth noise plus
+    the poles, the Antarctic rows and the fold pivots; 75 z-levels (1 m ..
+    5800 m stretched) with partial bottom cells over a smooth 200-5500 m
+    bathymetry; face-raster u/v (75, ny*nx) of a non-divergent flow from a
+    streamfunction sampled at the F-points (continuous through the seam and
+    the fold; 0.5 m/s rms at the surface, decaying with depth) and w (76,
+    ny*nx) float32, in canonical form (halo and fold copies from their
+    canonical points, vectors with the fold sign); model face widths and cell
+    areas; 2 five-day records cycled; 2 M particles uniform over the wet
+    cells and in their columns; the exact C-grid RK4 in the fractional level
     coordinate, dt 1 h, 720 steps (no diffusion, no beaching: the reference's
     3-D C-grid step takes neither)."""
     from .fields import VelocityField
-    from .nemo import build_cgrid_mesh
+    from .nemo import build_cgrid_mesh, to_canonical
     rng = np.random.default_rng(5)
-    jj, ii = np.mgrid[0:ny, 0:nx].astype(np.float64)
-    glamf = -100.0 + 0.1 * ii + 0.15 * np.sin(jj / 160.0)
-    gphif = -40.0 + 0.08 * jj + 0.1 * np.sin(ii / 200.0)
-    tlon, tlat = glamf - 0.05, gphif - 0.04
-    noise = S._sphere_noise(tlon.reshape(-1), tlat.reshape(-1), seed=6).reshape(ny, nx)
-    wet = noise >= np.quantile(noise, 0.3)
-    depth = S.smooth_bathymetry(tlon.reshape(-1), tlat.reshape(-1), 200.0, 5500.0).reshape(ny, nx)
+    lay, glamf, gphif, glamt, gphit = S.tripolar_grid(ny, nx, fold="T")
+    tl, tp = glamt.reshape(-1), gphit.reshape(-1)
+    noise = S._sphere_noise(tl, tp, seed=6).reshape(ny, nx)
+
+    def sep(lo, la):
+        r = np.radians
+        c = np.sin(r(gphit)) * np.sin(r(la)) + np.cos(r(gphit)) * np.cos(r(la)) * np.cos(r(glamt - lo))
+        return np.degrees(np.arccos(np.clip(c, -1.0, 1.0)))
+
+    wet = (noise >= np.quantile(noise, 0.3)) & (gphit > -76.0) & (sep(73.0, 65.0) > 6.0) & (sep(-107.0, 65.0) > 6.0)
+    wet = to_canonical(wet & ~lay.pivot_cells(), lay, "T") > 0.5
+    depth = S.smooth_bathymetry(tl, tp, 200.0, 5500.0).reshape(ny, nx)
     zw = S.stretched_levels(n_levels + 1, 1.0, 5800.0)
-    lay = np.diff(zw)
+    lay_d = np.diff(zw)
     nlev = np.where(wet, np.clip(np.searchsorted(zw, depth, side="left"), 1, n_levels), 0).astype(np.int32)
-    bot = lay[np.maximum(nlev - 1, 0)]
+    bot = lay_d[np.maximum(nlev - 1, 0)]
     e3b = np.where(nlev > 0, np.clip(depth - zw[np.maximum(nlev - 1, 0)], 0.1 * bot, bot), 0.0)
-    m_per_deg = 111120.0
-    e1t = 0.1 * m_per_deg * np.cos(np.radians(tlat))
-    e2t = np.full((ny, nx), 0.08 * m_per_deg)
-    e1v = 0.1 * m_per_deg * np.cos(np.radians(gphif))
-    mesh = build_cgrid_mesh(glamf, gphif, wet, e2u=e2t, e1v=e1v, nlev2d=nlev, zw=zw, area=e1t * e2t, e3b=e3b,
-                            name="c5_regional_cgrid")
+    nlev = to_canonical(nlev, lay, "T").astype(np.int32)
+    e3b = to_canonical(e3b, lay, "T")
+    u2, v2, e2u, e1v = S.cgrid_stream_flow(glamf, gphif, amp=1.0)
+    scale = 0.5 / np.sqrt(np.mean(np.concatenate([u2[wet] ** 2, v2[wet] ** 2])))
+    u2 = to_canonical(u2 * scale, lay, "U", vector=True).astype(np.float32)
+    v2 = to_canonical(v2 * scale, lay, "V", vector=True).astype(np.float32)
+    e2u = to_canonical(e2u, lay, "U")
+    e1v = to_canonical(e1v, lay, "V")
+    area = to_canonical(np.maximum(e2u * e1v, 1.0), lay, "T")
+    mesh = build_cgrid_mesh(glamf, gphif, wet, layout=lay, e2u=e2u, e1v=e1v, nlev2d=nlev, zw=zw, area=area,
+                            e3b=e3b, name="c5_tripolar_cgrid")
     K = n_levels
     zm = 0.5 * (zw[:-1] + zw[1:])
     dec = np.exp(-zm / 800.0).astype(np.float32)[:, None]
     lev = np.arange(K)[:, None]
+    wetk = lev < nlev.reshape(1, -1)
     snaps = []
     for k in range(n_snap):
-        ph = 1.3 * k
-        u2 = (0.5 * np.sin(jj / 23.0 + ph) * np.cos(ii / 31.0) + 0.2 * np.cos(ii / 17.0 - ph)).astype(np.float32)
-        v2 = (0.5 * np.cos(jj / 29.0 - ph) * np.sin(ii / 19.0) + 0.2 * np.sin(jj / 13.0 + ph)).astype(np.float32)
-        wetk = lev < nlev.reshape(1, -1)
-        u = np.where(wetk, u2.reshape(1, -1) * dec, np.float32(0.0))
-        v = np.where(wetk, v2.reshape(1, -1) * dec, np.float32(0.0))
-        wf = (1e-5 * np.sin(ii / 11.0 + jj / 7.0 + ph)).astype(np.float32).reshape(1, -1)
-        w = np.where(np.arange(K + 1)[:, None] < nlev.reshape(1, -1), wf * np.ones((K + 1, 1), np.float32),
+        ph = np.float32(1.0 + 0.3 * k)
+        u = np.where(wetk, u2.reshape(1, -1) * dec * ph, np.float32(0.0))
+        v = np.where(wetk, v2.reshape(1, -1) * dec * (np.float32(2.3) - ph), np.float32(0.0))
+        wt = to_canonical(1e-5 * np.sin(np.radians(4.0 * glamt + 60.0 * k)) * np.cos(np.radians(gphit)), lay, "T")
+        w = np.where(np.arange(K + 1)[:, None] < nlev.reshape(1, -1), wt.astype(np.float32).reshape(1, -1),
                      np.float32(0.0))
         snaps.append(VelocityField(u=u, v=v, w=w, eta=np.zeros(ny * nx), uv_layout="nemo_cgrid"))
-    # particles: uniform over the wet cells (bilinear in the cell's F corners), in the column
-    ej, ei = mesh._nemo_cgrid_elem_ji[: int((mesh._nemo_cgrid_nlev > 0).sum())].T
-    pick = rng.integers(0, ej.size, P)
-    j, i = ej[pick], ei[pick]
-    a, b = rng.random(P), rng.random(P)
-    corner = lambda g, dj, di: g[j + dj, i + di]
-    lon = ((1 - a) * (1 - b) * corner(glamf, -1, -1) + a * (1 - b) * corner(glamf, -1, 0)
-           + a * b * corner(glamf, 0, 0) + (1 - a) * b * corner(glamf, 0, -1))
-    lat = ((1 - a) * (1 - b) * corner(gphif, -1, -1) + a * (1 - b) * corner(gphif, -1, 0)
-           + a * b * corner(gphif, 0, 0) + (1 - a) * b * corner(gphif, 0, -1))
+    # particles: uniform over the wet cells (a random point of the cell's
+    # corner quad, on the sphere), uniform in the column
+    n_wet = int((mesh._nemo_cgrid_nlev > 0).sum())
+    pick = rng.integers(0, n_wet, P)
+    cn = mesh._nemo_cgrid_corners[pick]
+    la, lo = np.radians(mesh.nodes_lat[cn]), np.radians(mesh.nodes_lon[cn])
+    xyz = np.stack((np.cos(la) * np.cos(lo), np.cos(la) * np.sin(lo), np.sin(la)), axis=-1)
+    a, b = rng.random(P)[:, None], rng.random(P)[:, None]
+    pt = ((1 - a) * (1 - b) * xyz[:, 0] + a * (1 - b) * xyz[:, 1] + a * b * xyz[:, 2] + (1 - a) * b * xyz[:, 3])
+    lon = np.degrees(np.arctan2(pt[:, 1], pt[:, 0]))
+    lat = np.degrees(np.arcsin(pt[:, 2] / np.linalg.norm(pt, axis=1)))
+    j, i = mesh._nemo_cgrid_elem_ji[pick].T
     floor_ = zw[np.maximum(nlev[j, i] - 1, 0)] + e3b[j, i]
     z = rng.random(P) * 0.95 * floor_
     lon, lat, z = S.sort_seeds(lon, lat, z)
     return Workload("c5_nemo_cgrid_3d_rk4", mesh, snaps, lon, lat, z, "rk4", 3600.0, 5 * 86400.0, 720, dims=3,
-                    description={"mesh": f"regional curvilinear C-grid {nx}x{ny}, ~30% land, partial bottom cells",
+                    description={"mesh": f"tripolar ORCA-like C-grid {nx}x{ny} (T-pivot north fold, E-W halo), "
+                                         "~30% land, partial bottom cells",
                                  "nodes": int(mesh.n_nodes), "elements": int(mesh.n_elements), "levels": n_levels,
                                  "particles": P, "seeds": "sorted by 1-degree cell", "scheme": "rk4", "dt_s": 3600,
                                  "steps_run": 720, "uv_interp": "nemo_cgrid",
@@ -281,8 +297,9 @@ def c5(P: int = 2_000_000, ny: int = 1021, nx: int = 1442, n_levels: int = 75, n
 
 
 def c5_small(P: int = 200_000) -> Workload:
-    """C5's kernel on a 360 x 256 raster: the profiling case."""
-    w = c5(P=P, ny=256, nx=360)
+    """C5's construction on a 362 x 256 tripolar raster (1 degree): the
+    profiling and test case."""
+    w = c5(P=P, ny=256, nx=362)
     w.name = "c5small_nemo_cgrid_3d_rk4"
     return w
 

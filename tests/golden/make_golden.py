@@ -539,6 +539,110 @@ def cgrid_fixture():
         save(f"golden_{tag}", rec, rf, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
 
 
+def cgrid_tripolar_fixture():
+    """A global tripolar C-grid (T-pivot north fold, E-W halo columns; the
+    synthetic ORCA-like raster of kelp_b200.synthetic.tripolar_grid) through
+    the reference's own NemoCgridLayout, build_nemo_cgrid_mesh and
+    nemo_cgrid_to_canonical, and its C-grid steps (2-D RK2, 3-D RK4 with
+    partial bottom cells) of particles seeded next to the seam and the fold:
+    tests/golden/golden_cgrid_tripolar2d.npz / _tripolar3d.npz."""
+    import types
+    src = os.environ["KELP_REFERENCE_SRC"]
+    for name in ("kelp.readers", "kelp.readers.nemo"):
+        if name not in sys.modules:
+            pkg = types.ModuleType(name)
+            pkg.__path__ = [os.path.join(src, *name.split("."))]
+            sys.modules[name] = pkg
+    from kelp.readers.nemo._mesh import build_nemo_cgrid_mesh
+    from kelp.readers.nemo._layout import NemoCgridLayout, nemo_cgrid_to_canonical
+    T = 86400.0
+    ny, nx = 48, 66
+    lay, glamf, gphif, glamt, gphit = S.tripolar_grid(ny, nx, fold="T")
+    rlay = NemoCgridLayout((ny, nx), halo_cols=True, halo_row=True, periodic=True, fold="T")
+
+    def sep(lo1, la1, lo2, la2):
+        r = np.radians
+        c = np.sin(r(la1)) * np.sin(r(la2)) + np.cos(r(la1)) * np.cos(r(la2)) * np.cos(r(lo1 - lo2))
+        return np.degrees(np.arccos(np.clip(c, -1.0, 1.0)))
+
+    jj, ii = np.indices((ny, nx))
+    noise = np.sin(0.43 * ii + 0.2) * np.cos(0.37 * jj - 0.5) + 0.5 * np.sin(0.11 * ii * jj / 7.0)
+    wet = ((sep(glamt, gphit, 73.0, 65.0) > 14.0) & (sep(glamt, gphit, -107.0, 65.0) > 14.0) & (gphit > -70.0)
+           & (noise > -0.9))
+    wet = nemo_cgrid_to_canonical(wet.astype(np.float64), rlay, "T") > 0.5
+    zw = np.concatenate([[0.0], np.cumsum(10.0 * 1.35 ** np.arange(12))])
+    K = zw.size - 1
+    lay_d = np.diff(zw)
+    depth = 60.0 + (zw[-1] - 80.0) * 0.5 * (1.0 + np.sin(np.radians(3.0 * glamt)) * np.cos(np.radians(2.0 * gphit)))
+    nlev = np.where(wet, np.clip(np.searchsorted(zw, depth, side="left"), 1, K), 0).astype(np.int32)
+    bot_ref = lay_d[np.maximum(nlev - 1, 0)]
+    e3b = np.where(nlev > 0, np.clip(depth - zw[np.maximum(nlev - 1, 0)], 0.3 * bot_ref, bot_ref), 0.0)
+    nlev = nemo_cgrid_to_canonical(nlev.astype(np.float64), rlay, "T").astype(np.int32)
+    e3b = nemo_cgrid_to_canonical(e3b, rlay, "T")
+    u2, v2, e2u, e1v = S.cgrid_stream_flow(glamf, gphif, amp=3e7)
+    e2u = nemo_cgrid_to_canonical(e2u, rlay, "U")
+    e1v = nemo_cgrid_to_canonical(e1v, rlay, "V")
+    area = nemo_cgrid_to_canonical(np.maximum(e2u * e1v, 1.0), rlay, "T")
+    m3 = build_nemo_cgrid_mesh(glamf, gphif, wet, layout=rlay, e2u=e2u, e1v=e1v, nlev2d=nlev, zw=zw, area=area,
+                               e3b=e3b, name="tripolar3d")
+    set_exact_nearest(m3, True)
+    m2 = build_nemo_cgrid_mesh(glamf, gphif, wet, layout=rlay, name="tripolar2d")
+    set_exact_nearest(m2, True)
+
+    def fields(three_d, n_snap=3):
+        out = []
+        for k in range(n_snap):
+            ph = 1.0 + 0.25 * k
+            u = nemo_cgrid_to_canonical(u2 * ph, rlay, "U", vector=True)
+            v = nemo_cgrid_to_canonical(v2 * (2.0 - ph * 0.5), rlay, "V", vector=True)
+            if not three_d:
+                out.append(RVel(u=u.astype(np.float32).reshape(-1), v=v.astype(np.float32).reshape(-1), w=None,
+                                eta=np.zeros(ny * nx), uv_layout="nemo_cgrid"))
+                continue
+            lev = np.arange(K)[:, None, None]
+            dec = np.exp(-zw[:-1] / 400.0)[:, None, None]
+            uu = (u[None] * dec * (lev < nlev[None])).astype(np.float32).reshape(K, -1)
+            vv = (v[None] * dec * (lev < nlev[None])).astype(np.float32).reshape(K, -1)
+            wt = nemo_cgrid_to_canonical(3e-4 * np.sin(np.radians(5.0 * glamt + 40.0 * k)) * np.cos(np.radians(gphit)),
+                                         rlay, "T")
+            ww = (wt[None] * np.sin(np.pi * zw / zw[-1])[:, None, None]).astype(np.float32).reshape(K + 1, -1)
+            out.append(RVel(u=uu, v=vv, w=ww, eta=np.zeros(ny * nx), uv_layout="nemo_cgrid"))
+        return out
+
+    # particles: uniform over the wet cells, plus clusters across the seam
+    # (+-180) and along the fold line (the poles' meridian plane, high north)
+    rng = np.random.default_rng(77)
+    P = 1500
+    lon = np.concatenate([rng.uniform(-180, 180, 700), rng.uniform(176.0, 184.0, 400),
+                          np.where(rng.random(400) < 0.5, 73.0, -107.0) + rng.uniform(-30, 30, 400)])
+    lat = np.concatenate([rng.uniform(-60, 85, 700), rng.uniform(-50, 70, 400), rng.uniform(76.0, 89.0, 400)])
+    lon = ((lon + 180.0) % 360.0) - 180.0
+    z = rng.uniform(0.0, 1500.0, P)
+    status = np.full(P, int(ParticleStatus.ALIVE), np.int32)
+    for rm, tag, three_d in ((m2, "tripolar2d", False), (m3, "tripolar3d", True)):
+        rf = fields(three_d)
+        run = dict(uv_interp="nemo_cgrid")
+        if three_d:
+            cases = {"rk4": run_case(rm, rf, lon, lat, z, status, "rk4", 10800.0, T, 12, **run),
+                     "rk2": run_case(rm, rf, lon, lat, z, status, "rk2", 10800.0, T, 12, **run)}
+        else:
+            cases = {"rk2": run_case(rm, rf, lon, lat, z, status, "rk2", 10800.0, T, 12, **run),
+                     "rk4": run_case(rm, rf, lon, lat, z, status, "rk4", 10800.0, T, 12, **run)}
+        rec = mesh_record(rm)
+        for k in CGRID_KEYS:
+            rec["cgrid_" + k] = np.asarray(getattr(rm, "_nemo_cgrid_" + k))
+        rec["cgrid_shape"] = np.array(rm._structured_shape)
+        rec["cgrid_partial"] = np.array(rm._nemo_cgrid_partial)
+        rec.update({"cgin_glamf": glamf, "cgin_gphif": gphif, "cgin_wet": wet, "cgin_fold": np.array("T"),
+                    "cgin_raw_u": u2, "cgin_raw_v": v2,
+                    "cgin_canon_u": nemo_cgrid_to_canonical(u2, rlay, "U", vector=True),
+                    "cgin_canon_v": nemo_cgrid_to_canonical(v2, rlay, "V", vector=True)})
+        if three_d:
+            rec.update({"cgin_e2u": e2u, "cgin_e1v": e1v, "cgin_nlev": nlev, "cgin_zw": zw, "cgin_area": area,
+                        "cgin_e3b": e3b})
+        save(f"golden_cgrid_{tag}", rec, rf, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
+
+
 def pchip_fixture():
     """Monotone-cubic (PCHIP) temporal reconstruction over a 4-snapshot
     stencil (numerics/temporal_reconstruct.py; the tracking layer's bundle,
@@ -723,7 +827,7 @@ def rng1m_fixture():
 
 if __name__ == "__main__":
     # no argument: every fixture; otherwise the named ones ("steps", "beach", ...)
-    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq", "rng1m"}
+    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq", "rng1m", "tripolar"}
     if "rng1m" in which:
         rng1m_fixture()
     if "lsq" in which:
@@ -738,5 +842,7 @@ if __name__ == "__main__":
         sigma_fixture()
     if "cgrid" in which:
         cgrid_fixture()
+    if "tripolar" in which:
+        cgrid_tripolar_fixture()
     if "pchip" in which:
         pchip_fixture()

@@ -32,6 +32,8 @@ CASES += SIGMA_CASES
 # NEMO C-grid meshes (uv_interp nemo_cgrid): the 2-D unfused steps and the 3-D fractional-level step
 CGRID_CASES = [("golden_cgrid2d", c) for c in ("rk2", "rk4", "euler", "rk2_bwd", "rk4_steady", "rk2_kick", "rk2_walk")]
 CGRID_CASES += [("golden_cgrid3d", c) for c in ("rk2", "rk4", "euler", "rk2_bwd", "rk4_steady")]
+# a global tripolar raster (T-pivot north fold, E-W halo) built by the reference's own builder
+CGRID_CASES += [(f"golden_cgrid_tripolar{d}", c) for d in ("2d", "3d") for c in ("rk2", "rk4")]
 CASES += CGRID_CASES
 # PCHIP temporal reconstruction (4-snapshot stencil; the last interval falls back to linear)
 PCHIP_CASES = [("golden_pchip2d", c) for c in ("rk2", "rk4_kick")]
@@ -209,18 +211,23 @@ def test_elem_neighbors_match_reference(golden, fixture):
     np.testing.assert_array_equal(build_elem_neighbors(m), g.d["mesh_elem_neighbors"])
 
 
-@pytest.mark.parametrize("fixture", ["golden_cgrid2d", "golden_cgrid3d"])
+@pytest.mark.parametrize("fixture", ["golden_cgrid2d", "golden_cgrid3d", "golden_cgrid_tripolar2d",
+                                     "golden_cgrid_tripolar3d"])
 def test_cgrid_mesh_builder_matches_reference(golden, fixture):
     """kelp_b200.nemo.build_cgrid_mesh on the recorded raster equals the
-    reference's own build_nemo_cgrid_mesh: nodes, cells, ring, tables, grid hash."""
-    from kelp_b200.nemo import build_cgrid_mesh
+    reference's own build_nemo_cgrid_mesh: nodes, cells, ring, tables, grid
+    hash; on the tripolar raster through the seam and the fold."""
+    from kelp_b200.nemo import CgridLayout, build_cgrid_mesh
     g = golden(fixture)
     d = g.d
     kw = {}
     if "mesh_cgin_zw" in d:
         kw = dict(e2u=d["mesh_cgin_e2u"], e1v=d["mesh_cgin_e1v"], nlev2d=d["mesh_cgin_nlev"],
-                  zw=d["mesh_cgin_zw"], area=d["mesh_cgin_area"], e3b=d["mesh_cgin_e3b"],
-                  e3u0=d["mesh_cgin_e3u0"])
+                  zw=d["mesh_cgin_zw"], area=d["mesh_cgin_area"], e3b=d["mesh_cgin_e3b"])
+        if "mesh_cgin_e3u0" in d:
+            kw["e3u0"] = d["mesh_cgin_e3u0"]
+    if "mesh_cgin_fold" in d:
+        kw["layout"] = CgridLayout(d["mesh_cgin_glamf"].shape, periodic=True, fold=str(d["mesh_cgin_fold"]))
     m = build_cgrid_mesh(d["mesh_cgin_glamf"], d["mesh_cgin_gphif"], d["mesh_cgin_wet"], **kw)
     for k in ("nodes_lon", "nodes_lat", "depth", "elem_nodes", "node_to_elems", "node_to_elems_count"):
         np.testing.assert_array_equal(np.asarray(getattr(m, k)), d[f"mesh_{k}"], err_msg=k)
@@ -230,3 +237,14 @@ def test_cgrid_mesh_builder_matches_reference(golden, fixture):
               "e2u", "e1v"):
         np.testing.assert_array_equal(np.asarray(getattr(m, "_nemo_cgrid_" + k)).reshape(-1),
                                       d["mesh_cgrid_" + k].reshape(-1), err_msg=k)
+
+
+def test_tripolar_raster_canonical_form_matches_reference(golden):
+    """kelp_b200.nemo.to_canonical of face-velocity rasters equals the
+    reference's nemo_cgrid_to_canonical (halo columns, the fold's half turn,
+    the vector sign)."""
+    from kelp_b200.nemo import CgridLayout, to_canonical
+    d = golden("golden_cgrid_tripolar2d").d
+    lay = CgridLayout(d["mesh_cgin_glamf"].shape, periodic=True, fold=str(d["mesh_cgin_fold"]))
+    np.testing.assert_array_equal(to_canonical(d["mesh_cgin_raw_u"], lay, "U", vector=True), d["mesh_cgin_canon_u"])
+    np.testing.assert_array_equal(to_canonical(d["mesh_cgin_raw_v"], lay, "V", vector=True), d["mesh_cgin_canon_v"])
