@@ -34,9 +34,23 @@ class TrajectoryWriter:
         self._n_obs = 0
 
     def open(self) -> "TrajectoryWriter":
-        os.makedirs(os.path.join(self.path, "obs"), exist_ok=True)
+        """Open (or reopen) the store.  Reopening a store that holds a
+        checkpoint resumes numbering at the checkpoint's record count: records
+        written after the checkpoint (by a run that stopped before its next
+        one) are dropped, as the resumed run writes them again."""
+        obs_dir = os.path.join(self.path, "obs")
+        os.makedirs(obs_dir, exist_ok=True)
         self._write_json("attrs.json", {"n_particles": self.n_particles, **self.metadata})
-        self._n_obs = len([f for f in os.listdir(os.path.join(self.path, "obs")) if f.endswith(".npz")])
+        files = sorted(f for f in os.listdir(obs_dir) if f.endswith(".npz") and ".tmp" not in f)
+        kept = len(files)
+        rst = os.path.join(self.path, "restart.npz")
+        if os.path.exists(rst):
+            with np.load(rst) as d:
+                if "restart_n_obs" in d.files:
+                    kept = min(kept, int(d["restart_n_obs"]))
+        for f in files[kept:]:
+            os.remove(os.path.join(obs_dir, f))
+        self._n_obs = kept
         return self
 
     def __enter__(self):
@@ -96,7 +110,8 @@ class TrajectoryWriter:
                "restart_z": self._check(state.z, "z").astype(np.float64),
                "restart_status": self._check(state.status, "status").astype(np.int32),
                "restart_nearest_node": self._check(state.nearest_node, "nearest_node").astype(np.int32),
-               "restart_step_i": np.int64(step_i), "restart_file_idx": np.int64(file_idx)}
+               "restart_step_i": np.int64(step_i), "restart_file_idx": np.int64(file_idx),
+               "restart_n_obs": np.int64(self._n_obs)}   # the records that belong to this checkpoint
         optional = []
         for name, val, dt in (("failure_reason", state.failure_reason, np.int8),
                               ("release_step", release_step, np.int32),

@@ -54,3 +54,26 @@ def test_checkpoint_round_trip_and_replace(tmp_path):
     np.testing.assert_array_equal(r["wet_streak"], np.arange(P) + 1)
     assert r["release_step"] is None and r["state"].release_step is None
     assert not any(f.endswith(".tmp.npz") for f in os.listdir(path))
+
+
+def test_resume_after_a_crash_drops_the_records_past_the_checkpoint(tmp_path):
+    """A run checkpoints after 3 records, writes 2 more and stops; the resumed
+    run reopens the store: numbering continues at 3, the 2 records written
+    after the checkpoint are gone (the resumed run writes them again), so no
+    observation is duplicated."""
+    P = 5
+    path = str(tmp_path / "t")
+    w = TrajectoryWriter(path, P).open()
+    for k in range(3):
+        w.append(_state(P, k), 3600.0 * (k + 1))
+    w.write_checkpoint(_state(P, 2), step_i=3, file_idx=3)
+    for k in range(3, 5):
+        w.append(_state(P, k), 3600.0 * (k + 1))
+    assert w.n_obs == 5
+    w2 = TrajectoryWriter(path, P).open()   # the resumed run
+    assert w2.n_obs == 3
+    for k in range(3, 6):
+        w2.append(_state(P, 10 + k), 3600.0 * (k + 1))
+    tr = read_trajectory(path)
+    np.testing.assert_array_equal(tr["time"], 3600.0 * np.arange(1, 7))
+    np.testing.assert_array_equal(tr["lon"][3], _state(P, 13).lon)
