@@ -586,8 +586,10 @@ def run_b200(args):
     if wl.dims == 3 and wl.uv_vertical != "layer":
         ctx.ensure_depth_points(wl.mesh, wl.uv_vertical)
     forms = [f.strip() for f in args.forms.split(",") if f.strip()]
-    if getattr(wl.mesh, "_nemo_cgrid", False):   # C-grid meshes step in the plain form only
-        forms, args.form = ["plain"], "plain"
+    if getattr(wl.mesh, "_nemo_cgrid", False):   # C-grid meshes: no fused multi-step launch
+        forms = [f for f in forms if f not in BATCHED]
+        if args.form in ("auto", "mixed_batched"):
+            args.form = "mixed"
     if args.form == "auto":
         forms += [f for f in ("mixed", "mixed_batched") if f not in forms]
     elif args.form not in forms:

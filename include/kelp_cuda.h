@@ -46,7 +46,7 @@
 extern "C" {
 #endif
 
-#define KC_ABI_VERSION 10
+#define KC_ABI_VERSION 11
 
 #define KC_OK 0
 #define KC_ERR_ARG 1      /* invalid argument or combination */
@@ -375,6 +375,15 @@ int kc_find_nearest_noalloc(kc_ctx* ctx, long long P, const double* lon, const d
  * (src/kelp/numerics/diffusion.py:233-249 _normal_pair). */
 int kc_rng_normals(kc_ctx* ctx, long long P, unsigned long long seed, unsigned long long real_id,
                    unsigned long long step_i, unsigned long long pid_offset, unsigned long long comp, double* out);
+
+/* The grid hash of a mesh's nodes built on the device (the CSR of
+ * src/kelp/core/mesh.py:844-1001 build_grid_hash): each node's cell
+ * (cj * nx + ci, the quotient by cell_size truncated and clamped; lon in the
+ * branch the host chose, lon_min 0 when wrap), the node ids stable-sorted by
+ * cell into node_ids (n_nodes) and the CSR offsets (nx * ny + 1).  Equal to
+ * the host build bit for bit. */
+int kc_grid_hash_build(kc_ctx* ctx, long long n_nodes, const double* lon, const double* lat, double cell_size,
+                       double lon_min, double lat_min, int nx, int ny, int wrap, int* offsets, int* node_ids);
 
 /* Digests of the Box-Muller draws over their whole input domain, for
  * checking the device arithmetic against the reference's: for every 32-bit

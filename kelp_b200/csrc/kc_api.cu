@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include "../../include/kelp_cuda.h"
 #include "kc_host.h"
@@ -292,6 +293,28 @@ __global__ void __launch_bounds__(256) k_rng_domain(const kc::DRngX x, unsigned 
         atomicAdd(&out[1], dc);
         atomicAdd(&out[2], ds);
     }
+}
+
+// The grid hash's cell of every node (mesh.py:980-990 _gh_cell_index: the
+// quotient by the cell size truncated toward zero, then clamped), and the
+// per-cell node counts.
+__global__ void __launch_bounds__(kBlock) k_hash_cells(const double* lon, const double* lat, long long N, double cell,
+                                                       double lon_min, double lat_min, int nx, int ny, int wrap,
+                                                       unsigned* key, int* val, int* counts) {
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    int ci = wrap ? (int)(lon[n] / cell) : (int)((lon[n] - lon_min) / cell);
+    if (wrap) {
+        if (ci > nx - 1) ci = nx - 1;
+    } else {
+        ci = ci < 0 ? 0 : (ci > nx - 1 ? nx - 1 : ci);
+    }
+    int cj = (int)((lat[n] - lat_min) / cell);
+    cj = cj < 0 ? 0 : (cj > ny - 1 ? ny - 1 : cj);
+    const unsigned k = (unsigned)cj * (unsigned)nx + (unsigned)ci;
+    key[n] = k;
+    val[n] = (int)n;
+    atomicAdd(&counts[k], 1);
 }
 
 __global__ void __launch_bounds__(kBlock) k_beach(const __grid_constant__ kc::DMesh m,
@@ -601,7 +624,10 @@ int launch_step_on(kc_ctx* c, const kc_step_args* a, const kc::DState& st, const
     int rc0 = wait_slots(c, sl, nsl);
     if (rc0) return rc0;
     const int dtype = c->slots[a->slot_a].dtype;
-    if (c->dm.cg.on) {   // NEMO C-grid meshes: the exact C-grid steps (plain form)
+    if (c->dm.cg.on && a->precision == KC_MIXED) {   // the mixed form's 3-D C-grid step
+        if (dtype == KC_F16) kc_launch_cgrid_mixed_f16(c->dm, blend_of<__half>(c, a), st, s, a->scheme, c->stream);
+        else kc_launch_cgrid_mixed_f32(c->dm, blend_of<float>(c, a), st, s, a->scheme, c->stream);
+    } else if (c->dm.cg.on) {   // NEMO C-grid meshes: the exact C-grid steps (plain form)
         if (dtype == KC_F32) kc_launch_cgrid_f32(c->dm, blend_of<float>(c, a), st, s, a->dims, a->scheme, c->stream);
         else kc_launch_cgrid_f64(c->dm, blend_of<double>(c, a), st, s, a->dims, a->scheme, c->stream);
     } else if (a->uv_lsq) {   // element-layout u/v: 2-D least squares (plain form)
@@ -663,7 +689,8 @@ int check_step(kc_ctx* c, const kc_step_args* a) {
             return fail(c, KC_ERR_ARG, "kc_step: PCHIP times must increase strictly");
     }
     if (c->dm.cg.on) {
-        if (a->precision != KC_PLAIN) return fail(c, KC_ERR_ARG, "kc_step: C-grid meshes step in the plain form");
+        if (a->precision == KC_MIXED && a->dims != 3)
+            return fail(c, KC_ERR_ARG, "kc_step: the mixed form on C-grid meshes is the 3-D step");
         if (a->az_kick) return fail(c, KC_ERR_ARG, "kc_step: the Az kick on C-grid meshes is not built");
         if (a->dims == 3 && (a->kick || c->dm.cg.K < 1))
             return fail(c, KC_ERR_ARG, "kc_step: the 3-D C-grid step needs a 3-D C-grid mesh and takes no kick");
@@ -673,7 +700,10 @@ int check_step(kc_ctx* c, const kc_step_args* a) {
             if (sl3[k] < 0 || sl3[k] >= kSlots) return fail(c, KC_ERR_ARG, "kc_step: slot out of range");
             const Slot& s = c->slots[sl3[k]];
             if (s.dtype < 0) return fail(c, KC_ERR_STATE, "kc_step: snapshot slot " + std::to_string(sl3[k]) + " is empty");
-            if (s.dtype == KC_F16) return fail(c, KC_ERR_ARG, "kc_step: C-grid steps read float32 or float64 rasters");
+            if (a->precision == KC_PLAIN && s.dtype == KC_F16)
+                return fail(c, KC_ERR_ARG, "kc_step: the plain form reads float32 or float64 rasters");
+            if (a->precision == KC_MIXED && s.dtype == KC_F64)
+                return fail(c, KC_ERR_ARG, "kc_step: the mixed form reads float32 or float16 rasters");
             if (s.n != nynx) return fail(c, KC_ERR_ARG, "kc_step: C-grid snapshots are ny * nx face rasters");
             if (a->dims == 2 && s.uv_rows != 1 && s.uv_rows != c->dm.cg.K)
                 return fail(c, KC_ERR_ARG, "kc_step: 2-D C-grid u/v need one row (or K, the surface read)");
@@ -2045,6 +2075,56 @@ int kc_rng_normals(kc_ctx* c, long long P, unsigned long long seed, unsigned lon
     cudaFreeAsync(d, c->stream);
     if (e != cudaSuccess) return fail(c, KC_ERR_CUDA, std::string("kc_rng_normals: ") + cudaGetErrorString(e));
     KC_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KC_OK;
+}
+
+int kc_grid_hash_build(kc_ctx* c, long long n_nodes, const double* lon, const double* lat, double cell_size,
+                       double lon_min, double lat_min, int nx, int ny, int wrap, int* offsets, int* node_ids) {
+    if (!c) return KC_ERR_ARG;
+    if (n_nodes <= 0 || n_nodes > INT_MAX || !lon || !lat || !offsets || !node_ids)
+        return fail(c, KC_ERR_ARG, "kc_grid_hash_build: arrays");
+    if (!(cell_size > 0.0) || nx <= 0 || ny <= 0 || (long long)nx * ny > 2000000000LL)
+        return fail(c, KC_ERR_ARG, "kc_grid_hash_build: grid geometry");
+    KC_CUDA(c, cudaSetDevice(c->device));
+    const long long N = n_nodes, C = (long long)nx * ny;
+    cudaStream_t s = c->stream;
+    double *dlon = nullptr, *dlat = nullptr;
+    unsigned *k0 = nullptr, *k1 = nullptr;
+    int *v0 = nullptr, *v1 = nullptr, *cnt = nullptr, *off = nullptr;
+    void* tmp = nullptr;
+    size_t tsort = 0, tscan = 0;
+    cudaError_t e = cudaSuccess;
+    auto ok = [&](cudaError_t r) { if (e == cudaSuccess) e = r; return e == cudaSuccess; };
+    ok(cudaMallocAsync((void**)&dlon, N * 8, s));
+    ok(cudaMallocAsync((void**)&dlat, N * 8, s));
+    ok(cudaMallocAsync((void**)&k0, N * 4, s));
+    ok(cudaMallocAsync((void**)&k1, N * 4, s));
+    ok(cudaMallocAsync((void**)&v0, N * 4, s));
+    ok(cudaMallocAsync((void**)&v1, N * 4, s));
+    ok(cudaMallocAsync((void**)&cnt, (C + 1) * 4, s));
+    ok(cudaMallocAsync((void**)&off, (C + 1) * 4, s));
+    ok(cudaMemcpyAsync(dlon, lon, N * 8, cudaMemcpyHostToDevice, s));
+    ok(cudaMemcpyAsync(dlat, lat, N * 8, cudaMemcpyHostToDevice, s));
+    ok(cudaMemsetAsync(cnt, 0, (C + 1) * 4, s));
+    if (e == cudaSuccess) {
+        k_hash_cells<<<grid_for(N), kBlock, 0, s>>>(dlon, dlat, N, cell_size, lon_min, lat_min, nx, ny, wrap, k0, v0,
+                                                    cnt);
+        ok(cudaGetLastError());
+    }
+    // stable radix sort of the node ids by cell (the order of numpy's stable argsort)
+    int bits = 1;
+    while (bits < 32 && (1ull << bits) < (unsigned long long)C) ++bits;
+    ok(cub::DeviceRadixSort::SortPairs(nullptr, tsort, k0, k1, v0, v1, (int)N, 0, bits, s));
+    ok(cub::DeviceScan::ExclusiveSum(nullptr, tscan, cnt, off, (int)(C + 1), s));
+    ok(cudaMallocAsync(&tmp, std::max(tsort, tscan), s));
+    ok(cub::DeviceRadixSort::SortPairs(tmp, tsort, k0, k1, v0, v1, (int)N, 0, bits, s));
+    ok(cub::DeviceScan::ExclusiveSum(tmp, tscan, cnt, off, (int)(C + 1), s));   // offsets[C] = N
+    ok(cudaMemcpyAsync(node_ids, v1, N * 4, cudaMemcpyDeviceToHost, s));
+    ok(cudaMemcpyAsync(offsets, off, (C + 1) * 4, cudaMemcpyDeviceToHost, s));
+    for (void* p : {(void*)dlon, (void*)dlat, (void*)k0, (void*)k1, (void*)v0, (void*)v1, (void*)cnt, (void*)off, tmp})
+        if (p) cudaFreeAsync(p, s);
+    if (e != cudaSuccess) return fail(c, KC_ERR_CUDA, std::string("kc_grid_hash_build: ") + cudaGetErrorString(e));
+    KC_CUDA(c, cudaStreamSynchronize(s));
     return KC_OK;
 }
 

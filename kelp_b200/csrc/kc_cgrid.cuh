@@ -7,6 +7,7 @@
 // float64 operation order.
 #pragma once
 #include "kc_step.cuh"
+#include "kc_mixed.cuh"
 
 namespace kc {
 
@@ -41,7 +42,12 @@ __device__ __forceinline__ double pymax(double a, double b) { return b > a ? b :
 // fractional level s and W = ds/dt.  False outside the mesh or for a
 // degenerate cell; a dry-ring cell or a level at or below the floor reads
 // zero velocity.
-template <typename T>
+//
+// MIXED (the mixed form, 3-D): the six face / interface values are read
+// (float32, or float16 with per-level scales) and time-blended in float32,
+// and the fluxes formed in float32; the cell search, the bilinear inverse, the
+// metric terms and positions stay float64.
+template <typename T, bool MIXED = false>
 static __device__ __noinline__ bool cgrid_core(const DMesh& m, const DBlend<T>& f, double alpha, double xp, double yp,
                                                double zp, int nn, int hint, double td, bool three_d, double& U,
                                                double& V, double& W) {
@@ -75,10 +81,21 @@ static __device__ __noinline__ bool cgrid_core(const DMesh& m, const DBlend<T>& 
         fN = cg_e3face(g, g.kbv, g.e3v, c, kz) / e3c;
     }
     const long long ko = (long long)kz * nynx;
-    const double uW = cg_val(f.a.u, f.b.u, f.t.u, f.alpha0, alpha, ko + c - 1);
-    const double uE = cg_val(f.a.u, f.b.u, f.t.u, f.alpha0, alpha, ko + c);
-    const double vS = cg_val(f.a.v, f.b.v, f.t.v, f.alpha0, alpha, ko + c - nx);
-    const double vN = cg_val(f.a.v, f.b.v, f.t.v, f.alpha0, alpha, ko + c);
+    double uW, uE, vS, vN;
+    TBlendF tb;
+    if constexpr (MIXED) {
+        tb = tblend_mode(f.alpha0, alpha);
+        const long long rn = nynx > 0 ? nynx : 0;
+        uW = (double)blend_val<T>(tb, f.a.u, f.a.su, f.b.u, f.b.su, f.t.u, f.t.su, kz, rn, (int)(c - 1));
+        uE = (double)blend_val<T>(tb, f.a.u, f.a.su, f.b.u, f.b.su, f.t.u, f.t.su, kz, rn, (int)c);
+        vS = (double)blend_val<T>(tb, f.a.v, f.a.sv, f.b.v, f.b.sv, f.t.v, f.t.sv, kz, rn, (int)(c - nx));
+        vN = (double)blend_val<T>(tb, f.a.v, f.a.sv, f.b.v, f.b.sv, f.t.v, f.t.sv, kz, rn, (int)c);
+    } else {
+        uW = cg_val(f.a.u, f.b.u, f.t.u, f.alpha0, alpha, ko + c - 1);
+        uE = cg_val(f.a.u, f.b.u, f.t.u, f.alpha0, alpha, ko + c);
+        vS = cg_val(f.a.v, f.b.v, f.t.v, f.alpha0, alpha, ko + c - nx);
+        vN = cg_val(f.a.v, f.b.v, f.t.v, f.alpha0, alpha, ko + c);
+    }
     const double M = SLM;
     const double cosl = cr::cos_cr(yp * DEG2RAD);
     const int4 cr = __ldg(&g.corners[e]);
@@ -115,17 +132,29 @@ static __device__ __noinline__ bool cgrid_core(const DMesh& m, const DBlend<T>& 
     double xi = fabs(den) >= fabs(den2) ? (0.0 - a0 - a2 * eta) / den : (0.0 - b0 - b2 * eta) / den2;
     xi = pymin(pymax(xi, 0.0), 1.0);
     double U0, U1, V0, V1;
+    double lW, lE, lS, lN;
     if (g.has_e) {
-        U0 = fW * uW * __ldg(&g.e2u[c - 1]);
-        U1 = fE * uE * __ldg(&g.e2u[c]);
-        V0 = fS * vS * __ldg(&g.e1v[c - nx]);
-        V1 = fN * vN * __ldg(&g.e1v[c]);
+        lW = __ldg(&g.e2u[c - 1]);
+        lE = __ldg(&g.e2u[c]);
+        lS = __ldg(&g.e1v[c - nx]);
+        lN = __ldg(&g.e1v[c]);
     } else {   // edges S (c0-c1), E (c1-c2), N (c2-c3), W (c3-c0)
         const double4 L = g.L[e];
-        U0 = fW * uW * L.w;
-        U1 = fE * uE * L.y;
-        V0 = fS * vS * L.x;
-        V1 = fN * vN * L.z;
+        lW = L.w;
+        lE = L.y;
+        lS = L.x;
+        lN = L.z;
+    }
+    if constexpr (MIXED) {
+        U0 = (double)((float)fW * (float)uW * (float)lW);
+        U1 = (double)((float)fE * (float)uE * (float)lE);
+        V0 = (double)((float)fS * (float)vS * (float)lS);
+        V1 = (double)((float)fN * (float)vN * (float)lN);
+    } else {
+        U0 = fW * uW * lW;
+        U1 = fE * uE * lE;
+        V0 = fS * vS * lS;
+        V1 = fN * vN * lN;
     }
     const double dxdxi = (1.0 - eta) * a1 + eta * (px[2] - px[3]);
     const double dydxi = (1.0 - eta) * b1 + eta * (py[2] - py[3]);
@@ -141,9 +170,16 @@ static __device__ __noinline__ bool cgrid_core(const DMesh& m, const DBlend<T>& 
     double Wv = 0.0;
     if (three_d) {
         const double zeta = pymin(pymax(zp - kz, 0.0), 1.0);
-        Wv = ((1.0 - zeta) * cg_val(f.a.w, f.b.w, f.t.w, f.alpha0, alpha, ko + c) +
-              zeta * cg_val(f.a.w, f.b.w, f.t.w, f.alpha0, alpha, ko + nynx + c)) *
-             __ldg(&g.area[c]) / (adet * e3c);
+        if constexpr (MIXED) {
+            const float wl = blend_val<T>(tb, f.a.w, f.a.sw, f.b.w, f.b.sw, f.t.w, f.t.sw, kz, nynx, (int)c);
+            const float wu = blend_val<T>(tb, f.a.w, f.a.sw, f.b.w, f.b.sw, f.t.w, f.t.sw, kz + 1, nynx, (int)c);
+            const float zf = (float)zeta;
+            Wv = (double)((1.0f - zf) * wl + zf * wu) * __ldg(&g.area[c]) / (adet * e3c);
+        } else {
+            Wv = ((1.0 - zeta) * cg_val(f.a.w, f.b.w, f.t.w, f.alpha0, alpha, ko + c) +
+                  zeta * cg_val(f.a.w, f.b.w, f.t.w, f.alpha0, alpha, ko + nynx + c)) *
+                 __ldg(&g.area[c]) / (adet * e3c);
+        }
     }
     U = td * Uv;
     V = td * Vv;
@@ -198,7 +234,7 @@ __device__ __forceinline__ double cg_s2z(const DCgrid& g, int e, bool ok, double
 // the surface, the end cell's domain check and s -> z (an unchanged s in an
 // unchanged cell keeps z).  A particle that is not alive gets the nearest
 // node of its position and nothing else.
-template <typename T, int SCHEME>
+template <typename T, int SCHEME, bool MIXED = false>
 __device__ __forceinline__ void step3d_cgrid_particle(const DMesh& m, const DBlend<T>& f, const DState& st,
                                                       const DStep& s, long long i) {
     constexpr int NS = SCHEME == 0 ? 1 : (SCHEME == 1 ? 2 : 4);
@@ -234,7 +270,8 @@ __device__ __forceinline__ void step3d_cgrid_particle(const DMesh& m, const DBle
         double Un = 0.0, Vn = 0.0, Wn = 0.0;
         if (ok) {
             const int nnn = n ? site_anchor(m, make_site_fast(ln, lt)) : nn0;
-            ok = cgrid_core<T>(m, f, s.ak[n], ln, lt, sn, nnn, n ? -1 : (ok0 ? e0 : -1), s.time_dir, true, Un, Vn, Wn);
+            ok = cgrid_core<T, MIXED>(m, f, s.ak[n], ln, lt, sn, nnn, n ? -1 : (ok0 ? e0 : -1), s.time_dir, true,
+                                      Un, Vn, Wn);
         }
         if (n == 0) {
             first_u = Un;

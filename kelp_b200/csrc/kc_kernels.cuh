@@ -93,7 +93,7 @@ void launch_sigma_kernel(const kc::DMesh& m, const kc::DBlend<T>& f, const kc::D
     }
 }
 
-template <typename T, int SCHEME>
+template <typename T, int SCHEME, bool MIXED = false>
 __global__ void __launch_bounds__(kBlock, KC_STEP_MIN_BLOCKS) k_step3d_cgrid(const __grid_constant__ kc::DMesh m,
                                                                          const __grid_constant__ kc::DBlend<T> f,
                                                                          const __grid_constant__ kc::DState st,
@@ -102,7 +102,17 @@ __global__ void __launch_bounds__(kBlock, KC_STEP_MIN_BLOCKS) k_step3d_cgrid(con
     if (i >= st.P) return;
     activate(st, s, i);
     if (st.prev) st.prev[i] = st.status[i];
-    kc::step3d_cgrid_particle<T, SCHEME>(m, f, st, s, i);
+    kc::step3d_cgrid_particle<T, SCHEME, MIXED>(m, f, st, s, i);
+}
+
+// The 3-D C-grid step of the mixed form (float32 or scaled float16 rasters).
+template <typename T>
+void launch_cgrid_mixed_kernel(const kc::DMesh& m, const kc::DBlend<T>& f, const kc::DState& st, const kc::DStep& s,
+                               int scheme, cudaStream_t stream) {
+    const unsigned g = (unsigned)((st.P + kBlock - 1) / kBlock);
+    if (scheme == 0) k_step3d_cgrid<T, 0, true><<<g, kBlock, 0, stream>>>(m, f, st, s);
+    else if (scheme == 1) k_step3d_cgrid<T, 1, true><<<g, kBlock, 0, stream>>>(m, f, st, s);
+    else k_step3d_cgrid<T, 2, true><<<g, kBlock, 0, stream>>>(m, f, st, s);
 }
 
 // One step on a NEMO C-grid mesh (plain form): the 2-D steps read the

@@ -1,7 +1,7 @@
 // Launchers of the step kernels, one set per translation unit so the kernel
 // instantiations compile in parallel (kc_plain_f64.cu, kc_plain_f32.cu,
 // kc_mixed_f32.cu, kc_mixed_f16.cu, kc_cgrid_f64.cu, kc_cgrid_f32.cu,
-// kc_sigma.cu).  kc_api.cu calls them; the kernels are kc_kernels.cuh.
+// kc_cgrid_mixed.cu, kc_sigma.cu).  kc_api.cu calls them; the kernels are kc_kernels.cuh.
 #pragma once
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
@@ -33,6 +33,11 @@ void kc_launch_cgrid_f64(const kc::DMesh& m, const kc::DBlend<double>& f, const 
                          int dims, int scheme, cudaStream_t stream);
 void kc_launch_cgrid_f32(const kc::DMesh& m, const kc::DBlend<float>& f, const kc::DState& st, const kc::DStep& s,
                          int dims, int scheme, cudaStream_t stream);
+// the mixed form's 3-D C-grid step (kc_cgrid_mixed.cu)
+void kc_launch_cgrid_mixed_f32(const kc::DMesh& m, const kc::DBlend<float>& f, const kc::DState& st,
+                               const kc::DStep& s, int scheme, cudaStream_t stream);
+void kc_launch_cgrid_mixed_f16(const kc::DMesh& m, const kc::DBlend<__half>& f, const kc::DState& st,
+                               const kc::DStep& s, int scheme, cudaStream_t stream);
 void kc_launch_sigma_f64(const kc::DMesh& m, const kc::DBlend<double>& f, const kc::DState& st, const kc::DStep& s,
                          int scheme, cudaStream_t stream);
 void kc_launch_sigma_f32(const kc::DMesh& m, const kc::DBlend<float>& f, const kc::DState& st, const kc::DStep& s,

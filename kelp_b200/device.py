@@ -518,6 +518,18 @@ class DeviceContext:
                                          int(comp), N.ptr(out)), "kc_rng_normals")
         return out
 
+    def grid_hash(self, lon, lat, cell_size, lon_min, lat_min, nx, ny, wrap):
+        """(offsets, node_ids) of the grid hash built on the device
+        (kc_grid_hash_build); lon in the branch the host chose."""
+        lon = _c(lon, np.float64)
+        lat = _c(lat, np.float64)
+        off = np.empty(int(nx) * int(ny) + 1, np.int32)
+        ids = np.empty(lon.size, np.int32)
+        self._chk(N.lib().kc_grid_hash_build(self._ctx, lon.size, N.ptr(lon), N.ptr(lat), float(cell_size),
+                                             float(lon_min), float(lat_min), int(nx), int(ny), int(bool(wrap)),
+                                             N.ptr(off), N.ptr(ids)), "kc_grid_hash_build")
+        return off, ids
+
     def rng_domain_digests(self, corrected: bool = True) -> tuple:
         """Digests of r, cos and sin of the Box-Muller draws over all 2^32
         uniforms (kc_rng_domain_digests)."""

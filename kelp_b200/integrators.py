@@ -191,8 +191,15 @@ def _prepare_cgrid(vel, mesh, dt, time_dir, scheme, kw, ctx, kick):
     if not (mesh.metadata or {}).get("exact_nearest", False):
         raise NotImplementedError("the CUDA backend anchors with the exact nearest-node search only "
                                   "(mesh.exact_nearest: true, the configuration default)")
-    if kw.get("cuda_precision", "plain") != "plain" or kw.get("cuda_snapshots") not in (None, "f32"):
-        raise NotImplementedError("C-grid meshes step in the plain form with float32 or float64 rasters")
+    form = kw.get("cuda_precision", "plain")
+    if form not in ("plain", "mixed"):
+        raise ValueError(f"cuda_precision must be 'plain' or 'mixed', got {form!r}")
+    if kw.get("cuda_snapshots") not in (None, "f32", "f16"):
+        raise ValueError(f"cuda_snapshots must be None, 'f32' or 'f16', got {kw.get('cuda_snapshots')!r}")
+    if kw.get("cuda_snapshots") == "f16" and form != "mixed":
+        raise ValueError("float16 rasters are read by the mixed form only (cuda_precision='mixed')")
+    if form == "mixed" and not _is_3d(vel):
+        raise NotImplementedError("the mixed form on C-grid meshes is the 3-D step")
     vel_next = kw.get("vel_next", None)
     dt_to_next = kw.get("dt_to_next", None)
     _validate_time_aware(vel_next, dt_to_next, dt)
@@ -203,7 +210,7 @@ def _prepare_cgrid(vel, mesh, dt, time_dir, scheme, kw, ctx, kick):
     is3d = _is_3d(vel)
     ctx = ctx or default_context()
     ctx.ensure_mesh(mesh)
-    sa, sb, st = ctx.slots_for([vel_a, vel_b, target], np.float32 if kw.get("cuda_snapshots") == "f32" else None)
+    sa, sb, st = ctx.slots_for([vel_a, vel_b, target], snapshot_storage(kw))
     a = N.StepArgs()
     a.scheme = code
     a.dims = 3 if is3d else 2
@@ -220,7 +227,7 @@ def _prepare_cgrid(vel, mesh, dt, time_dir, scheme, kw, ctx, kick):
         a.kick = 1
         a.kh_x, a.kh_y, a.seed, a.real_id, a.step_i, a.pid_offset = kick
     a.global_step = -1
-    a.precision = N.KC_PLAIN
+    a.precision = N.KC_MIXED if form == "mixed" else N.KC_PLAIN
     a.Dmin, a.z0b_min = 0.5, 0.1
     return a, is3d
 

@@ -202,11 +202,14 @@ def _gh_far_rows_for(mesh, cell_size: float) -> int:
     return int(rows)
 
 
-def build_grid_hash(mesh, cell_size: float = 0.0) -> None:
+def build_grid_hash(mesh, cell_size: float = 0.0, ctx=None) -> None:
     """Uniform lon/lat CSR hash over the mesh nodes (``mesh.py:844-1001``).
 
     ``cell_size`` 0 takes ``metadata["grid_hash_cell"]`` when pinned, else the
-    reference's automatic size ``max(0.05, 2 sqrt(area / N))`` degrees."""
+    reference's automatic size ``max(0.05, 2 sqrt(area / N))`` degrees.  With
+    a device context ``ctx`` the cells, the stable sort and the offsets are
+    computed on the GPU (kc_grid_hash_build, equal bit for bit); the lon
+    branch and the grid geometry are host decisions either way."""
     lon, wrap = _gh_lon_branch(np.asarray(mesh.nodes_lon, dtype=np.float64))
     lon_span = lon.max() - lon.min()
     lat = np.asarray(mesh.nodes_lat, dtype=np.float64)
@@ -228,11 +231,14 @@ def build_grid_hash(mesh, cell_size: float = 0.0) -> None:
     if n_cells > _GRID_HASH_MAX_CELLS:
         raise ValueError(f"grid hash: cell size {cell_size:.6g} deg needs {n_cells} cells "
                          f"(> {_GRID_HASH_MAX_CELLS}); use a larger cell.")
-    cell_idx = _gh_cell_index(lon, lat, cell_size, lon_min, lat_min, nx, ny, wrap)
-    counts = np.bincount(cell_idx, minlength=n_cells).astype(np.int32)
-    offsets = np.zeros(n_cells + 1, dtype=np.int32)
-    np.cumsum(counts, out=offsets[1:])
-    node_ids = np.argsort(cell_idx, kind="stable").astype(np.int32)
+    if ctx is not None:
+        offsets, node_ids = ctx.grid_hash(lon, lat, cell_size, lon_min, lat_min, nx, ny, wrap)
+    else:
+        cell_idx = _gh_cell_index(lon, lat, cell_size, lon_min, lat_min, nx, ny, wrap)
+        counts = np.bincount(cell_idx, minlength=n_cells).astype(np.int32)
+        offsets = np.zeros(n_cells + 1, dtype=np.int32)
+        np.cumsum(counts, out=offsets[1:])
+        node_ids = np.argsort(cell_idx, kind="stable").astype(np.int32)
 
     mesh._node_xyz = None   # filled on first use by ensure_node_xyz (the native library's C-library trig)
     mesh._gh_offsets = offsets

@@ -825,11 +825,32 @@ def rng1m_fixture():
     print("golden_rng_1m")
 
 
+def reftypes_fixture():
+    """The attribute layout of the reference's own types (field names in
+    order, and the defaults of DiffusionStepArgs), for the drop-in test that
+    passes objects shaped exactly like KELP's to kelp_b200's step functions:
+    tests/golden/reference_types.json."""
+    import dataclasses
+    import json
+    from kelp.core.particles import ParticleState as RPS
+    out = {"Mesh": [f.name for f in dataclasses.fields(RMesh)],
+           "VelocityField": [f.name for f in dataclasses.fields(RVel)],
+           "ParticleState": [f.name for f in dataclasses.fields(RPS)],
+           "LazyLerpField": ["vel_a", "vel_b", "alpha"],
+           "DiffusionStepArgs": list(RDiff._fields),
+           "DiffusionStepArgs_defaults": {k: v for k, v in RDiff._field_defaults.items()}}
+    with open(os.path.join(HERE, "reference_types.json"), "w") as fh:
+        json.dump(out, fh, indent=1)
+    print("reference_types")
+
+
 if __name__ == "__main__":
     # no argument: every fixture; otherwise the named ones ("steps", "beach", ...)
-    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq", "rng1m", "tripolar"}
+    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq", "rng1m", "tripolar", "reftypes"}
     if "rng1m" in which:
         rng1m_fixture()
+    if "reftypes" in which:
+        reftypes_fixture()
     if "lsq" in which:
         lsq_fixture()
     if "steps" in which:

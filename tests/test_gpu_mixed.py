@@ -84,3 +84,31 @@ def test_plain_rejects_f16_and_mixed_rejects_f64(golden):
     out = KI.rk2_step(st, vel, g.mesh, 3600.0, 1.0, uv_interp="barycentric", vel_next=vnext, dt_to_next=dtn,
                       cuda_precision="mixed")
     assert np.isfinite(out.lon).all()
+
+
+@pytest.mark.parametrize("storage,bound_m", [("f32", 1.0), ("f16", 50.0)])
+def test_mixed_cgrid_tracks_plain(storage, bound_m):
+    """The mixed form's 3-D C-grid step (float32 values and fluxes on float32
+    or scaled float16 face rasters, float64 geometry) on the tripolar C5-shaped
+    workload against the plain form over 24 one-hour RK4 steps: p99
+    separation under 1 m on float32 rasters; float16 rasters within their
+    storage error (p99 under 50 m after a day)."""
+    from kelp_b200 import workloads as W
+    from kelp_b200.fields import LazyLerpField
+    from kelp_b200.particles import make_state
+    w = W.c5_small(P=20_000)
+    out = {}
+    for form, snaps in (("plain", None), ("mixed", storage)):
+        st = make_state(w.lon, w.lat, w.z).replace(failure_reason=np.zeros(w.P, np.int8))
+        for k in range(24):
+            ia, ib, a0, dtn = w.bracket(k)
+            a, b = w.snaps[ia], w.snaps[ib]
+            vel = a if a0 == 0.0 else LazyLerpField(a, b, a0)
+            st = KI.rk4_step(st, vel, w.mesh, w.dt, 1.0, uv_interp="nemo_cgrid", vel_next=b, dt_to_next=dtn,
+                             cuda_precision=form, cuda_snapshots=snaps)
+        out[form] = {"lon": st.lon, "lat": st.lat, "z": st.z, "status": st.status, "nearest_node": st.nearest_node}
+    s = A.separation_stats(out["plain"], out["mixed"])
+    print("cgrid mixed", storage, s)
+    assert s["compared"] > 10_000
+    assert s["status_mismatch"] <= 20
+    assert s["p99_m"] < bound_m, s
