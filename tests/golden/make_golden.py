@@ -827,10 +827,12 @@ def rng1m_fixture():
 
 def reftypes_fixture():
     """The attribute layout of the reference's own types (field names in
-    order, and the defaults of DiffusionStepArgs), for the drop-in test that
-    passes objects shaped exactly like KELP's to kelp_b200's step functions:
+    order, the read-only properties each class defines, and the defaults of
+    DiffusionStepArgs), for the drop-in test that passes objects shaped
+    exactly like KELP's to kelp_b200's step functions:
     tests/golden/reference_types.json."""
     import dataclasses
+    import inspect
     import json
     from kelp.core.particles import ParticleState as RPS
     out = {"Mesh": [f.name for f in dataclasses.fields(RMesh)],
@@ -838,7 +840,9 @@ def reftypes_fixture():
            "ParticleState": [f.name for f in dataclasses.fields(RPS)],
            "LazyLerpField": ["vel_a", "vel_b", "alpha"],
            "DiffusionStepArgs": list(RDiff._fields),
-           "DiffusionStepArgs_defaults": {k: v for k, v in RDiff._field_defaults.items()}}
+           "DiffusionStepArgs_defaults": {k: v for k, v in RDiff._field_defaults.items()},
+           "properties": {c.__name__: [n for n, v in inspect.getmembers(c) if isinstance(v, property)]
+                          for c in (RMesh, RVel, RPS)}}
     with open(os.path.join(HERE, "reference_types.json"), "w") as fh:
         json.dump(out, fh, indent=1)
     print("reference_types")

@@ -4,8 +4,9 @@
 the field lists of ``kelp.core.mesh.Mesh``, ``kelp.core.io.VelocityField``,
 ``kelp.core.particles.ParticleState``, ``kelp.core.io.LazyLerpField`` and
 ``kelp.numerics.diffusion.DiffusionStepArgs`` (a NamedTuple, with its
-defaults).  Here classes with those fields and nothing else (dataclasses with
-a ``replace``, a NamedTuple) carry a golden case's mesh, payload and
+defaults), and the read-only properties the classes define.  Here classes with
+those fields and properties and nothing else (dataclasses with a ``replace``,
+a NamedTuple) carry a golden case's mesh, payload and
 particles through ``kelp_b200.integrators.get_integrator`` -- the
 registry KELP's tracking loop calls -- and the result must be the reference's
 recorded one, returned as the caller's own state type.
@@ -24,10 +25,25 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 TYPES = json.load(open(os.path.join(HERE, "golden", "reference_types.json")))
 
 
+# What each recorded property returns in KELP (kelp/core/mesh.py:167-190,
+# kelp/core/particles.py:224-231); z_levels, the zlevel column boundaries,
+# is |sigma| on a zlevel mesh and an error on a sigma mesh.
+PROPERTIES = {
+    "n_nodes": lambda m: m.nodes_lon.shape[0],
+    "n_elements": lambda m: m.elem_nodes.shape[0],
+    "n_sigma": lambda m: m.sigma.shape[0],
+    "z_levels": lambda m: np.abs(m.sigma) if m.vertical_coord == "zlevel" else (_ for _ in ()).throw(
+        NotImplementedError("mesh.z_levels is only valid for z-level meshes")),
+    "n_particles": lambda s: s.lon.shape[0],
+    "alive_mask": lambda s: s.status == 1,
+}
+
+
 def _dataclass(name, fields):
-    cls = dataclasses.make_dataclass(name, [(f, object, dataclasses.field(default=None)) for f in fields],
-                                     namespace={"replace": lambda self, **kw: dataclasses.replace(self, **kw)})
-    return cls
+    ns = {"replace": lambda self, **kw: dataclasses.replace(self, **kw)}
+    ns.update({p: property(PROPERTIES[p]) for p in TYPES["properties"].get(name, [])})
+    return dataclasses.make_dataclass(name, [(f, object, dataclasses.field(default=None)) for f in fields],
+                                      namespace=ns)
 
 
 Mesh = _dataclass("Mesh", TYPES["Mesh"])
