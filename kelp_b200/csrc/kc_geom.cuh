@@ -98,6 +98,7 @@ struct DMesh {
     const double2* ecos;      // (E) cos(mean vertex latitude): x containment set, y compacted set
     const int* n2e_off;       // (N+1) CSR offsets of the node->element table
     const int* n2e;           // element ids, per node in the reference order
+    const float4* ebox;       // (E) containment prefilter boxes (elem_box), or null
     const int* gh_off;        // (nx*ny+1) CSR offsets of the grid hash
     const double4* gh_tab;    // hash-ordered {x, y, z, node id} unit-sphere table
     const int* pw_off;        // (nx*ny+1) pruned windows: CSR offsets, or null
@@ -826,7 +827,81 @@ __device__ __forceinline__ int element_contains_t(const DMesh& m, int c, double 
     return (W_INFO && !nondeg) ? W_UNSURE : verdict;
 }
 
+// A box around each element that can only reject what the test above
+// rejects too.  {centre longitude, half width in longitude, lowest and
+// highest latitude}, in degrees, from the mask vertices: the half width and
+// the latitudes are widened by the W search's margin (1e-5 of the extent
+// plus 1e-9) and by kBoxSlack, then rounded outward to float.  A point
+// outside it is outside the reference's bounding box by more than that
+// margin, so element_contains_t returns 0 (W_OUT with W_INFO) for it.
+// Elements whose verdict the box cannot give -- fewer than three vertices,
+// a W ring unlike the mask, or an extent of 90 degrees or more -- get a
+// negative half width and are never rejected by it.
+constexpr double kBoxSlack = 1e-7;   // degrees, far above the double roundings of either test
+
+__device__ __forceinline__ float4 elem_box(const DMesh& m, int c) {
+    const float4 none = make_float4(0.0f, -1.0f, 0.0f, 0.0f);
+    const int4 e = m.en[c];
+    const bool v3 = e.w >= 0 && !(e.w == e.x && e.x >= 0);
+    const int n = (e.x >= 0) + (e.y >= 0) + (e.z >= 0) + (v3 ? 1 : 0);
+    if (n < 3 || !w_ring_matches_mask(e)) return none;
+    const int ids[4] = {e.x, e.y, e.z, v3 ? e.w : -1};
+    double lon_ref = 0.0, dmin = 0.0, dmax = 0.0, lamin = 0.0, lamax = 0.0;
+    bool first = true;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (ids[k] < 0) continue;
+        const double2 a = m.ll[ids[k]];
+        if (first) {
+            lon_ref = a.x; lamin = lamax = a.y; first = false;
+            continue;
+        }
+        const double d = wrap180(a.x - lon_ref);
+        dmin = fmin(dmin, d); dmax = fmax(dmax, d);
+        lamin = fmin(lamin, a.y); lamax = fmax(lamax, a.y);
+    }
+    if (!(dmax - dmin < 90.0)) return none;
+    const float cf = __double2float_rn(wrap180(lon_ref + 0.5 * (dmin + dmax)));
+    double hw = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (ids[k] < 0) continue;
+        hw = fmax(hw, fabs(wrap180(m.ll[ids[k]].x - (double)cf)));
+    }
+    const double mx = 1e-5 * (dmax - dmin) + 1e-9 + kBoxSlack, my = 1e-5 * (lamax - lamin) + 1e-9 + kBoxSlack;
+    return make_float4(cf, __double2float_ru(hw + mx), __double2float_rd(lamin - my), __double2float_ru(lamax + my));
+}
+
+__device__ __forceinline__ bool box_rejects(float4 b, double lon_p, double lat_p) {
+    if (b.y < 0.0f) return false;
+    double dl = lon_p - (double)b.x;
+    if (!(dl >= -180.0 && dl < 180.0)) dl -= 360.0 * floor((dl + 180.0) / 360.0);
+    return fabs(dl) > (double)b.y || lat_p < (double)b.z || lat_p > (double)b.w;
+}
+
+// Which of ring positions k0 .. k0+3 (below e) survive their boxes, as bits;
+// the element ids in c0..c3.  All four loads are issued before any test.
+__device__ __forceinline__ unsigned ring_pass4(const DMesh& m, int k0, int e, double lon_p, double lat_p, int& c0,
+                                               int& c1, int& c2, int& c3) {
+    c0 = __ldg(&m.n2e[k0]);
+    c1 = k0 + 1 < e ? __ldg(&m.n2e[k0 + 1]) : -1;
+    c2 = k0 + 2 < e ? __ldg(&m.n2e[k0 + 2]) : -1;
+    c3 = k0 + 3 < e ? __ldg(&m.n2e[k0 + 3]) : -1;
+    const float4 reject = make_float4(0.0f, 0.0f, 1.0f, -1.0f);
+    const float4 b0 = __ldg(&m.ebox[c0]);
+    const float4 b1 = c1 >= 0 ? __ldg(&m.ebox[c1]) : reject;
+    const float4 b2 = c2 >= 0 ? __ldg(&m.ebox[c2]) : reject;
+    const float4 b3 = c3 >= 0 ? __ldg(&m.ebox[c3]) : reject;
+    return (box_rejects(b0, lon_p, lat_p) ? 0u : 1u) | (box_rejects(b1, lon_p, lat_p) ? 0u : 2u) |
+           (box_rejects(b2, lon_p, lat_p) ? 0u : 4u) | (box_rejects(b3, lon_p, lat_p) ? 0u : 8u);
+}
+
+__device__ __forceinline__ int pick4(int j, int c0, int c1, int c2, int c3) {
+    return j == 0 ? c0 : (j == 1 ? c1 : (j == 2 ? c2 : c3));
+}
+
 __device__ __forceinline__ bool element_contains(const DMesh& m, int c, double lon_p, double lat_p) {
+    if (m.ebox && box_rejects(__ldg(&m.ebox[c]), lon_p, lat_p)) return false;
     return element_contains_t<false>(m, c, lon_p, lat_p) == 1;
 }
 
@@ -837,6 +912,19 @@ static __device__ __noinline__ int contain_two_ring(const DMesh& m, double lon_p
 static __device__ KC_INL_CONTAIN int contain_local(const DMesh& m, double lon_p, double lat_p, int nn) {
     int s = __ldg(&m.n2e_off[nn]), e = __ldg(&m.n2e_off[nn + 1]);
     if (e == s) return -1;
+    if (m.ebox) {
+        // the ring's boxes four at a time; the survivors in ring order
+        for (int k0 = s; k0 < e; k0 += 4) {
+            int c0, c1, c2, c3;
+            unsigned pass = ring_pass4(m, k0, e, lon_p, lat_p, c0, c1, c2, c3);
+            while (pass) {
+                const int c = pick4(__ffs(pass) - 1, c0, c1, c2, c3);
+                pass &= pass - 1;
+                if (element_contains_t<false>(m, c, lon_p, lat_p) == 1) return c;
+            }
+        }
+        return contain_two_ring(m, lon_p, lat_p, nn);
+    }
     for (int k = s; k < e; ++k) {
         int c = __ldg(&m.n2e[k]);
         if (element_contains(m, c, lon_p, lat_p)) return c;
@@ -874,6 +962,24 @@ static __device__ KC_INL_CONTAIN int contain_local_w(const DMesh& m, double lon_
     w_unsure = false;
     int s = __ldg(&m.n2e_off[nn]), e = __ldg(&m.n2e_off[nn + 1]);
     if (e == s) return -1;
+    if (m.ebox) {
+        // a box rejection is a W_OUT verdict (elem_box)
+        for (int k0 = s; k0 < e; k0 += 4) {
+            int c0, c1, c2, c3;
+            unsigned pass = ring_pass4(m, k0, e, lon_p, lat_p, c0, c1, c2, c3);
+            while (pass) {
+                const int c = pick4(__ffs(pass) - 1, c0, c1, c2, c3);
+                pass &= pass - 1;
+                const int v = element_contains_t<true>(m, c, lon_p, lat_p);
+                if (v == 1) {
+                    w_elem = c;
+                    return c;
+                }
+                if (v == W_UNSURE) w_unsure = true;
+            }
+        }
+        return contain_two_ring(m, lon_p, lat_p, nn);
+    }
     for (int k = s; k < e; ++k) {
         const int c = __ldg(&m.n2e[k]);
         const int v = element_contains_t<true>(m, c, lon_p, lat_p);
