@@ -31,7 +31,10 @@
 #define KC_INL_CONTAIN __noinline__       // contain_local, contain_local_w, w_search_elem
 #endif
 #ifndef KC_INL_STAGE
-#define KC_INL_STAGE __noinline__         // stage_f32 (mixed form), interp_uv_at, w_bary_at (plain form)
+#define KC_INL_STAGE __noinline__         // interp_uv_at, w_bary_at (plain form)
+#endif
+#ifndef KC_INL_MSTAGE
+#define KC_INL_MSTAGE __forceinline__     // stage_f32 (mixed form): inlined, 11 % faster on the 3-D RK2 step
 #endif
 #ifndef KC_INL_KICK
 #define KC_INL_KICK __noinline__          // apply_kick

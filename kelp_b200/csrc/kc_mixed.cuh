@@ -161,9 +161,11 @@ __device__ __forceinline__ float w_node_f32(const DMesh& m, const DBlend<T>& f, 
 
 // One 2-D or 3-D stage of the mixed form at (xp, yp, z) with anchor nn:
 // containment and the vertical decisions in float64, values in float32.
-// dims 2 reads u/v row 0 and no W.
-template <typename T>
-__device__ KC_INL_STAGE bool stage_f32(const DMesh& m, const DBlend<T>& f, const DStep& s, int dims, double xp,
+// DIMS 2 reads u/v row 0 and no W; DL: depth-linear u/v (uv_vertical level /
+// layer_linear).  One function per combination, so each keeps only its own
+// values live across its calls.
+template <typename T, int DIMS, bool DL>
+__device__ KC_INL_MSTAGE bool stage_f32(const DMesh& m, const DBlend<T>& f, const DStep& s, double xp,
                                        double yp, int nn, int hint, int whint, double z, double alpha, double& U,
                                        double& V, double& W) {
     U = 0.0;
@@ -186,13 +188,13 @@ __device__ KC_INL_STAGE bool stage_f32(const DMesh& m, const DBlend<T>& f, const
             w_unsure = true;
         }
     } else {
-        elem = (dims == 3 && s.w_code == 1) ? contain_local_w(m, xp, yp, nn, w_elem, w_unsure)
+        elem = (DIMS == 3 && s.w_code == 1) ? contain_local_w(m, xp, yp, nn, w_elem, w_unsure)
                                             : contain_local(m, xp, yp, nn);
     }
     int rv[4], rn = 0;
     float w[4];
     const bool ok = elem >= 0 && weights_f32(m, elem, xp, yp, rv, w, rn);
-    if (dims == 3) {
+    if constexpr (DIMS == 3) {
         const WLoc Lz = w_locate(m, z);
         float Wf;
         if (s.w_code == 1) {
@@ -226,7 +228,7 @@ __device__ KC_INL_STAGE bool stage_f32(const DMesh& m, const DBlend<T>& f, const
     }
     if (!ok) return false;
     float Us = 0.0f, Vs = 0.0f;
-    if (dims == 3 && s.uv_dl) {
+    if constexpr (DIMS == 3 && DL) {
         // depth-linear u/v with the wall rule (interpolate.py:1879-1971)
         double zq = z;
         if (isnan(zq)) zq = INFINITY;
@@ -290,7 +292,7 @@ __device__ KC_INL_STAGE bool stage_f32(const DMesh& m, const DBlend<T>& f, const
             Vs /= den;
         }
     } else {
-        const int row = dims == 3 ? find_layer(m, z, nn) : 0;
+        const int row = DIMS == 3 ? find_layer(m, z, nn) : 0;
 #pragma unroll
         for (int k = 0; k < 4; ++k)
             if (k < rn) {
@@ -311,12 +313,13 @@ struct MixedForm {
     static __device__ __forceinline__ bool uv2(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
                                                double lat, int nn, int hint, double alpha, double& U, double& V) {
         double W;
-        return stage_f32<T>(m, f, s, 2, lon, lat, nn, hint, -3, 0.0, alpha, U, V, W);
+        return stage_f32<T, 2, false>(m, f, s, lon, lat, nn, hint, -3, 0.0, alpha, U, V, W);
     }
     static __device__ __forceinline__ bool uvw3(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
                                                 double lat, int nn, int hint, int whint, double z, double alpha,
                                                 double& U, double& V, double& W) {
-        return stage_f32<T>(m, f, s, 3, lon, lat, nn, hint, whint, z, alpha, U, V, W);
+        return s.uv_dl ? stage_f32<T, 3, true>(m, f, s, lon, lat, nn, hint, whint, z, alpha, U, V, W)
+                       : stage_f32<T, 3, false>(m, f, s, lon, lat, nn, hint, whint, z, alpha, U, V, W);
     }
 };
 
