@@ -73,6 +73,7 @@ struct kc_ctx {
     double2* d_nsc = nullptr;
     double2* d_ecos = nullptr;
     float4* d_ebox = nullptr;        // containment prefilter boxes
+    double2* d_erec = nullptr;       // per-element mask vertex coordinates
     int* d_maxl = nullptr;
     double* d_dl_p = nullptr;
     int* d_dl_last = nullptr;
@@ -401,6 +402,11 @@ __device__ double rect_min_dot(double vx, double vy, double vz, const double* cl
 __global__ void __launch_bounds__(kBlock) k_elem_boxes(const __grid_constant__ kc::DMesh m, float4* out) {
     const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c < m.E) out[c] = kc::elem_box(m, (int)c);
+}
+
+__global__ void __launch_bounds__(kBlock) k_elem_records(const __grid_constant__ kc::DMesh m, double2* out) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < m.E) kc::elem_record(m, (int)c, out + 4 * c);
 }
 
 __global__ void __launch_bounds__(kBlock) k_prune_windows(const __grid_constant__ kc::DMesh m, int* counts,
@@ -793,8 +799,9 @@ int upload(kc_ctx* c, T** dst, const void* src, size_t count) {
 void free_mesh(kc_ctx* c) {
     dfree(c->d_ll); dfree(c->d_en); dfree(c->d_n2e_off); dfree(c->d_n2e); dfree(c->d_gh_off);
     dfree(c->d_gh_tab); dfree(c->d_pw_off); dfree(c->d_pw_tab); dfree(c->d_xyz); dfree(c->d_depth); dfree(c->d_zlev);
-    dfree(c->d_nsc); dfree(c->d_ecos); dfree(c->d_ebox); dfree(c->d_maxl); dfree(c->d_coastal);
+    dfree(c->d_nsc); dfree(c->d_ecos); dfree(c->d_ebox); dfree(c->d_erec); dfree(c->d_maxl); dfree(c->d_coastal);
     c->dm.ebox = nullptr;
+    c->dm.erec = nullptr;
     dfree(c->d_dl_p); dfree(c->d_dl_last); dfree(c->d_dl_bed); dfree(c->d_enb); dfree(c->d_sigma);
     dfree(c->d_cg_corners); dfree(c->d_cg_cell); dfree(c->d_cg_nlev); dfree(c->d_cg_nlev_r); dfree(c->d_cg_L);
     dfree(c->d_cg_e2u); dfree(c->d_cg_e1v); dfree(c->d_cg_area); dfree(c->d_cg_zw); dfree(c->d_cg_e3b);
@@ -908,19 +915,30 @@ int kc_synchronize(kc_ctx* c) {
     return KC_OK;
 }
 
-// The containment prefilter boxes of the uploaded elements (elem_box).
-// KELP_B200_ELEM_BOXES=0 in the environment leaves them out (every ring
-// element then goes through the full test).
+// The containment tables of the uploaded elements: the prefilter boxes
+// (elem_box) and the mask vertex records (elem_record).  In the environment,
+// KELP_B200_ELEM_BOXES=0 leaves out the boxes (every ring element then goes
+// through the full test) and KELP_B200_ELEM_RECORDS=0 the records (vertices
+// then read through the element's node ids).
 int build_elem_boxes(kc_ctx* c) {
     kc::DMesh& m = c->dm;
     m.ebox = nullptr;
+    m.erec = nullptr;
     const char* env = getenv("KELP_B200_ELEM_BOXES");
-    if (env && env[0] == '0') return KC_OK;
-    KC_CUDA(c, cudaMalloc((void**)&c->d_ebox, (size_t)c->E * sizeof(float4)));
-    k_elem_boxes<<<grid_for(c->E), kBlock, 0, c->stream>>>(m, c->d_ebox);
-    KC_CUDA(c, cudaGetLastError());
+    if (!(env && env[0] == '0')) {
+        KC_CUDA(c, cudaMalloc((void**)&c->d_ebox, (size_t)c->E * sizeof(float4)));
+        k_elem_boxes<<<grid_for(c->E), kBlock, 0, c->stream>>>(m, c->d_ebox);
+        KC_CUDA(c, cudaGetLastError());
+    }
+    env = getenv("KELP_B200_ELEM_RECORDS");
+    if (!(env && env[0] == '0')) {
+        KC_CUDA(c, cudaMalloc((void**)&c->d_erec, (size_t)c->E * 4 * sizeof(double2)));
+        k_elem_records<<<grid_for(c->E), kBlock, 0, c->stream>>>(m, c->d_erec);
+        KC_CUDA(c, cudaGetLastError());
+    }
     KC_CUDA(c, cudaStreamSynchronize(c->stream));
     m.ebox = c->d_ebox;
+    m.erec = c->d_erec;
     return KC_OK;
 }
 

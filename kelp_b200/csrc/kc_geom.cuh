@@ -102,6 +102,7 @@ struct DMesh {
     const int* n2e_off;       // (N+1) CSR offsets of the node->element table
     const int* n2e;           // element ids, per node in the reference order
     const float4* ebox;       // (E) containment prefilter boxes (elem_box), or null
+    const double2* erec;      // (E, 4) mask vertex lon, lat per element (elem_record), or null
     const int* gh_off;        // (nx*ny+1) CSR offsets of the grid hash
     const double4* gh_tab;    // hash-ordered {x, y, z, node id} unit-sphere table
     const int* pw_off;        // (nx*ny+1) pruned windows: CSR offsets, or null
@@ -726,6 +727,68 @@ __device__ __forceinline__ bool w_ring_matches_mask(const int4& e) {
     return true;
 }
 
+// The verdict for a point outside the reference's bounding box (the running
+// bounds of the wrapped longitudes around the first vertex, dmin..dmax, and
+// of the latitudes): 0, or with W_INFO the class of the W search, which has no
+// bbox and rejects the element for sure only beyond the margin of
+// w_ring_rejects (same bound, same frame).
+template <bool W_INFO>
+__device__ __forceinline__ int outside_box_verdict(int miss, double dmin, double dmax, double lamin, double lamax,
+                                                   double dlon_p, double lat_p) {
+    if (!W_INFO) return 0;
+    if (miss || !(dmax - dmin < 90.0)) return W_UNSURE;
+    const double my = 1e-5 * (lamax - lamin) + 1e-9, mx = 1e-5 * (dmax - dmin) + 1e-9;
+    if (lat_p < lamin - my || lat_p > lamax + my || dlon_p < dmin - mx || dlon_p > dmax + mx) return W_OUT;
+    return W_UNSURE;
+}
+
+// Inside the box: the local projection with the raw-mean origin unless the
+// element spans > 180 deg, then the fan triangles.  p holds the n mask
+// vertices (slot 3 repeats slot 0 for a triangle).
+template <bool W_INFO>
+__device__ __forceinline__ int inside_box_verdict(const DMesh& m, int c, const Poly& p, int n, int miss, double lon_p,
+                                                  double lat_p) {
+    const double lon_ref = p.ln[0];
+    const double d1 = wrap180(p.ln[1] - lon_ref), d2 = wrap180(p.ln[2] - lon_ref);
+    const double d3 = n == 4 ? wrap180(p.ln[3] - lon_ref) : 0.0;
+    double lmin = fmin(fmin(p.ln[0], p.ln[1]), p.ln[2]), lmax = fmax(fmax(p.ln[0], p.ln[1]), p.ln[2]);
+    if (n == 4) { lmin = fmin(lmin, p.ln[3]); lmax = fmax(lmax, p.ln[3]); }
+    double lon0;
+    if (lmax - lmin > 180.0) {
+        double dsum = 0.0 + d1;        // 0 + wrap180(ln[0] - ln[0]) + d1 + d2 (+ d3)
+        dsum += d2;
+        if (n == 4) dsum += d3;
+        lon0 = lon_ref + dsum / (double)n;
+    } else {
+        double s = p.ln[0] + p.ln[1];
+        s += p.ln[2];
+        if (n == 4) s += p.ln[3];
+        lon0 = s / (double)n;
+    }
+    double sl = p.la[0] + p.la[1];
+    sl += p.la[2];
+    if (n == 4) sl += p.la[3];
+    const double lat0 = sl / (double)n;
+    const double cos_lat0 = __ldg(&m.ecos[c]).x;
+    const double x0 = wrap180(p.ln[0] - lon0) * DEG2RAD * R_STD * cos_lat0;
+    const double x1 = wrap180(p.ln[1] - lon0) * DEG2RAD * R_STD * cos_lat0;
+    const double x2 = wrap180(p.ln[2] - lon0) * DEG2RAD * R_STD * cos_lat0;
+    const double y0 = (p.la[0] - lat0) * DEG2RAD * R_STD;
+    const double y1 = (p.la[1] - lat0) * DEG2RAD * R_STD;
+    const double y2 = (p.la[2] - lat0) * DEG2RAD * R_STD;
+    const double px = wrap180(lon_p - lon0) * DEG2RAD * R_STD * cos_lat0;
+    const double py = (lat_p - lat0) * DEG2RAD * R_STD;
+    bool nondeg;
+    if (bary_tri_inside(px, py, x0, y0, x1, y1, x2, y2, nondeg)) return 1;
+    int verdict = (W_INFO && !nondeg) ? W_UNSURE : miss;
+    if (n == 3) return verdict;
+    const double x3 = wrap180(p.ln[3] - lon0) * DEG2RAD * R_STD * cos_lat0;
+    const double y3 = (p.la[3] - lat0) * DEG2RAD * R_STD;
+    if (bary_tri_inside(px, py, x0, y0, x2, y2, x3, y3, nondeg)) return 1;
+    return (W_INFO && !nondeg) ? W_UNSURE : verdict;
+}
+
+
 // mesh.py:2210-2263 _element_contains with mesh.py:2006-2051
 // _project_to_local_xy and mesh.py:2139-2168 _polygon_contains_bool; the
 // cos of the mean vertex latitude comes from the host table.  Returns 1 when
@@ -733,6 +796,35 @@ __device__ __forceinline__ bool w_ring_matches_mask(const int4& e) {
 // class of the W search (W_OUT / W_UNSURE).
 template <bool W_INFO>
 __device__ __forceinline__ int element_contains_t(const DMesh& m, int c, double lon_p, double lat_p) {
+    if (m.erec) {
+        // the element's own record of its mask vertices (elem_record): one
+        // read, no vertex-id indirection; the same values and arithmetic
+        const double2* r = m.erec + 4 * (long long)c;
+        const double2 r0 = __ldg(r), r1 = __ldg(r + 1), r2 = __ldg(r + 2), r3 = __ldg(r + 3);
+        if (!isnan(r0.x)) {
+            const int n = isnan(r3.x) ? 3 : 4;
+            Poly p;
+            p.ln[0] = r0.x; p.la[0] = r0.y;
+            p.ln[1] = r1.x; p.la[1] = r1.y;
+            p.ln[2] = r2.x; p.la[2] = r2.y;
+            p.ln[3] = n == 4 ? r3.x : r0.x; p.la[3] = n == 4 ? r3.y : r0.y;
+            double dmin = 0.0, dmax = 0.0, lamin = r0.y, lamax = r0.y;
+#pragma unroll
+            for (int k = 1; k < 4; ++k) {
+                if (k < n) {
+                    const double d = wrap180(p.ln[k] - p.ln[0]);
+                    dmin = fmin(dmin, d);
+                    dmax = fmax(dmax, d);
+                    lamin = fmin(lamin, p.la[k]);
+                    lamax = fmax(lamax, p.la[k]);
+                }
+            }
+            const double dlon_p = wrap180(lon_p - p.ln[0]);
+            if (dlon_p > dmax || dlon_p < dmin || lat_p > lamax || lat_p < lamin)
+                return outside_box_verdict<W_INFO>(0, dmin, dmax, lamin, lamax, dlon_p, lat_p);
+            return inside_box_verdict<W_INFO>(m, c, p, n, 0, lon_p, lat_p);
+        }
+    }
     const int4 e = __ldg(&m.en[c]);
     // the mask's vertex slots in order (-1 slots dropped, slot 3 dropped when
     // it repeats slot 0)
@@ -771,17 +863,9 @@ __device__ __forceinline__ int element_contains_t(const DMesh& m, int c, double 
         }
     }
     const double dlon_p = wrap180(lon_p - lon_ref);
-    if (dlon_p > dmax || dlon_p < dmin || lat_p > lamax || lat_p < lamin) {
-        if (!W_INFO) return 0;
-        // the W search has no bbox: it rejects the element for sure only
-        // beyond the margin of w_ring_rejects (same bound, same frame)
-        if (miss || !(dmax - dmin < 90.0)) return W_UNSURE;
-        const double my = 1e-5 * (lamax - lamin) + 1e-9, mx = 1e-5 * (dmax - dmin) + 1e-9;
-        if (lat_p < lamin - my || lat_p > lamax + my || dlon_p < dmin - mx || dlon_p > dmax + mx) return W_OUT;
-        return W_UNSURE;
-    }
-    // inside the box: the vertices again (cached), the local projection with
-    // the raw-mean origin unless the element spans > 180 deg
+    if (dlon_p > dmax || dlon_p < dmin || lat_p > lamax || lat_p < lamin)
+        return outside_box_verdict<W_INFO>(miss, dmin, dmax, lamin, lamax, dlon_p, lat_p);
+    // inside the box: the vertices again (cached)
     Poly p;
     p.ln[0] = a0.x;
     p.la[0] = a0.y;
@@ -791,43 +875,7 @@ __device__ __forceinline__ int element_contains_t(const DMesh& m, int c, double 
         p.ln[k] = a.x;
         p.la[k] = a.y;
     }
-    const double d1 = wrap180(p.ln[1] - lon_ref), d2 = wrap180(p.ln[2] - lon_ref);
-    const double d3 = n == 4 ? wrap180(p.ln[3] - lon_ref) : 0.0;
-    double lmin = fmin(fmin(p.ln[0], p.ln[1]), p.ln[2]), lmax = fmax(fmax(p.ln[0], p.ln[1]), p.ln[2]);
-    if (n == 4) { lmin = fmin(lmin, p.ln[3]); lmax = fmax(lmax, p.ln[3]); }
-    double lon0;
-    if (lmax - lmin > 180.0) {
-        double dsum = 0.0 + d1;        // 0 + wrap180(ln[0] - ln[0]) + d1 + d2 (+ d3)
-        dsum += d2;
-        if (n == 4) dsum += d3;
-        lon0 = lon_ref + dsum / (double)n;
-    } else {
-        double s = p.ln[0] + p.ln[1];
-        s += p.ln[2];
-        if (n == 4) s += p.ln[3];
-        lon0 = s / (double)n;
-    }
-    double sl = p.la[0] + p.la[1];
-    sl += p.la[2];
-    if (n == 4) sl += p.la[3];
-    const double lat0 = sl / (double)n;
-    const double cos_lat0 = __ldg(&m.ecos[c]).x;
-    const double x0 = wrap180(p.ln[0] - lon0) * DEG2RAD * R_STD * cos_lat0;
-    const double x1 = wrap180(p.ln[1] - lon0) * DEG2RAD * R_STD * cos_lat0;
-    const double x2 = wrap180(p.ln[2] - lon0) * DEG2RAD * R_STD * cos_lat0;
-    const double y0 = (p.la[0] - lat0) * DEG2RAD * R_STD;
-    const double y1 = (p.la[1] - lat0) * DEG2RAD * R_STD;
-    const double y2 = (p.la[2] - lat0) * DEG2RAD * R_STD;
-    const double px = wrap180(lon_p - lon0) * DEG2RAD * R_STD * cos_lat0;
-    const double py = (lat_p - lat0) * DEG2RAD * R_STD;
-    bool nondeg;
-    if (bary_tri_inside(px, py, x0, y0, x1, y1, x2, y2, nondeg)) return 1;
-    int verdict = (W_INFO && !nondeg) ? W_UNSURE : miss;
-    if (n == 3) return verdict;
-    const double x3 = wrap180(p.ln[3] - lon0) * DEG2RAD * R_STD * cos_lat0;
-    const double y3 = (p.la[3] - lat0) * DEG2RAD * R_STD;
-    if (bary_tri_inside(px, py, x0, y0, x2, y2, x3, y3, nondeg)) return 1;
-    return (W_INFO && !nondeg) ? W_UNSURE : verdict;
+    return inside_box_verdict<W_INFO>(m, c, p, n, miss, lon_p, lat_p);
 }
 
 // A box around each element that can only reject what the test above
@@ -873,6 +921,25 @@ __device__ __forceinline__ float4 elem_box(const DMesh& m, int c) {
     }
     const double mx = 1e-5 * (dmax - dmin) + 1e-9 + kBoxSlack, my = 1e-5 * (lamax - lamin) + 1e-9 + kBoxSlack;
     return make_float4(cf, __double2float_ru(hw + mx), __double2float_rd(lamin - my), __double2float_ru(lamax + my));
+}
+
+// The mask vertices of element c in the containment convention (-1 slots
+// dropped, slot 3 dropped when it repeats slot 0), as element_contains_t
+// reads them: lon, lat of each; slot 3 NaN for a triangle.  An element that
+// needs its vertex ids for the verdict (fewer than three vertices, or a W
+// ring unlike the mask) gets NaN in slot 0 and is tested from the ids.
+__device__ __forceinline__ void elem_record(const DMesh& m, int c, double2* out) {
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    const int4 e = m.en[c];
+    const bool v3 = e.w >= 0 && !(e.w == e.x && e.x >= 0);
+    const int n = (e.x >= 0) + (e.y >= 0) + (e.z >= 0) + (v3 ? 1 : 0);
+    out[0] = out[1] = out[2] = out[3] = make_double2(nan, nan);
+    if (n < 3 || !w_ring_matches_mask(e)) return;
+    const int ids[4] = {e.x, e.y, e.z, v3 ? e.w : -1};
+    int k = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        if (ids[j] >= 0) out[k++] = m.ll[ids[j]];
 }
 
 __device__ __forceinline__ bool box_rejects(float4 b, double lon_p, double lat_p) {

@@ -1,10 +1,12 @@
-"""The containment prefilter boxes change no result.
+"""The containment tables change no result.
 
 Each element's box (elem_box in kc_geom.cuh) may only reject a point that the
-full element test rejects too, with the barycentric W search's own verdict.
-So with and without the box table (KELP_B200_ELEM_BOXES=0 at mesh upload
-leaves it out) every containment, every step and every state array must be
-bit-identical:
+full element test rejects too, with the barycentric W search's own verdict;
+each element's record (elem_record) holds the very vertex coordinates the
+test would read through the node ids.  So with both tables, with neither and
+with the boxes alone (KELP_B200_ELEM_BOXES=0 / KELP_B200_ELEM_RECORDS=0 at
+mesh upload leave them out) every containment, every step and every state
+array must be bit-identical:
 
 * kc_find_elements on points that sit on the tolerance band: each element's
   vertices and edge midpoints nudged by +-1e-9 .. 1e-5 degrees, plus uniform
@@ -18,9 +20,14 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _ctx(monkeypatch, boxes, mesh):
+CONFIGS = {"both": ("1", "1"), "neither": ("0", "0"), "boxes only": ("1", "0")}
+
+
+def _ctx(monkeypatch, config, mesh):
     from kelp_b200.device import DeviceContext
-    monkeypatch.setenv("KELP_B200_ELEM_BOXES", "1" if boxes else "0")
+    boxes, records = CONFIGS[config]
+    monkeypatch.setenv("KELP_B200_ELEM_BOXES", boxes)
+    monkeypatch.setenv("KELP_B200_ELEM_RECORDS", records)
     ctx = DeviceContext(0)
     ctx.ensure_mesh(mesh)
     return ctx
@@ -51,15 +58,15 @@ def test_find_elements_same_with_and_without_boxes(monkeypatch, wname):
     wl = W.WORKLOADS[wname]()
     qlon, qlat = _band_points(wl.mesh, np.random.default_rng(7))
     out = {}
-    for boxes in (True, False):
-        ctx = _ctx(monkeypatch, boxes, wl.mesh)
+    for config in CONFIGS:
+        ctx = _ctx(monkeypatch, config, wl.mesh)
         try:
-            out[boxes] = ctx.find_elements(qlon, qlat)
+            out[config] = ctx.find_elements(qlon, qlat)
         finally:
             ctx.close()
-    diff = int(np.count_nonzero(out[True] != out[False]))
-    print(f"{wname}: {qlon.size} points, {int(np.count_nonzero(out[True] >= 0))} inside, {diff} differ")
-    assert diff == 0
+    diff = {c: int(np.count_nonzero(out[c] != out["both"])) for c in CONFIGS}
+    print(f"{wname}: {qlon.size} points, {int(np.count_nonzero(out['both'] >= 0))} inside, differ {diff}")
+    assert all(v == 0 for v in diff.values())
 
 
 def _steps(ctx, wl, form, n, idx):
@@ -95,12 +102,13 @@ def test_steps_same_with_and_without_boxes(monkeypatch, wname, form):
     wl = W.WORKLOADS[wname]()
     idx = np.random.default_rng(3).choice(wl.P, size=min(wl.P, 100_000), replace=False)
     out = {}
-    for boxes in (True, False):
-        ctx = _ctx(monkeypatch, boxes, wl.mesh)
+    for config in CONFIGS:
+        ctx = _ctx(monkeypatch, config, wl.mesh)
         try:
-            out[boxes] = _steps(ctx, wl, form, 48, idx)
+            out[config] = _steps(ctx, wl, form, 48, idx)
         finally:
             ctx.close()
-    rep = {k: _ndiff(out[True][k], out[False][k]) for k in out[True] if out[True][k] is not None}
+    ref = out["both"]
+    rep = {c: {k: _ndiff(ref[k], out[c][k]) for k in ref if ref[k] is not None} for c in CONFIGS if c != "both"}
     print(f"{wname} {form}: {rep}")
-    assert all(v == 0 for v in rep.values()), rep
+    assert all(v == 0 for r in rep.values() for v in r.values()), rep
