@@ -38,6 +38,7 @@
  *                         numerics.nemo_cgrid (src/kelp/numerics/nemo_cgrid.py:84-512)
  *   kc_field_upload_eta <- core.io.VelocityField.eta (src/kelp/core/io.py:180)
  *   kc_rng_normals     <- numerics.diffusion._normal_pair (src/kelp/numerics/diffusion.py:233)
+ *   kc_sample_field    <- numerics.sampling.sample_field (src/kelp/numerics/sampling.py:727)
  */
 #ifndef KELP_CUDA_H
 #define KELP_CUDA_H
@@ -46,7 +47,7 @@
 extern "C" {
 #endif
 
-#define KC_ABI_VERSION 11
+#define KC_ABI_VERSION 12
 
 #define KC_OK 0
 #define KC_ERR_ARG 1      /* invalid argument or combination */
@@ -354,6 +355,22 @@ int kc_sort(kc_ctx* ctx);
 
 /* Batch exact nearest node of P query points (host arrays). */
 int kc_find_nearest(kc_ctx* ctx, long long P, const double* lon, const double* lat, int* out);
+
+/* Sample a node scalar field at P points (host arrays), the rules of
+ * numerics.sampling.sample_field (src/kelp/numerics/sampling.py:727-933):
+ * values (N) when rows == 0, or a z-level mid-layer field (rows, N) with its
+ * mid-layer depths z_mids (rows, positive down) and the points' depths z (P);
+ * nearest (P) the anchors (NULL: the exact nearest node, as the reference
+ * finds it), a negative anchor giving NaN; alive (P, nonzero = alive) or NULL
+ * (all alive); method 0 nearest, 1 leastsq, 2 barycentric, 3 idw.  out (P)
+ * receives the samples, NaN for dead or anchorless points.  The field is
+ * float64, as the reference reads it; interface fields (K, N) and sigma
+ * meshes are not covered (the host raises before calling).  KC_ERR_ARG for
+ * a method outside 0..3, an anchor >= N or a mid-layer field without its
+ * depths or the mesh depth. */
+int kc_sample_field(kc_ctx* ctx, const double* values, int rows, const double* z_mids, long long P,
+                    const double* lon, const double* lat, const double* z, const int* nearest,
+                    const unsigned char* alive, int method, double* out);
 
 /* The same batch nearest-node query, allocating nothing on the device.  For
  * callers that must not call cudaMalloc: it synchronises the whole device, and

@@ -27,7 +27,7 @@ CU_SOURCES = ["kc_api.cu", "kc_plain_f64.cu", "kc_plain_f32.cu", "kc_mixed_f32.c
 CPP_SOURCES = ["kc_host.cpp", "kc_rngx.cpp"]
 RNGX = os.path.join(BUILD, "kc_rng_exceptions.bin")
 HEADERS = ["kc_geom.cuh", "kc_interp.cuh", "kc_step.cuh", "kc_beach.cuh", "kc_mixed.cuh", "kc_kernels.cuh", "kc_sigma.cuh",
-           "kc_cgrid.cuh",
+           "kc_cgrid.cuh", "kc_sample.cuh",
            "kc_launch.h", "kc_host.h", "kc_crmath.cuh", "kc_crmath_tables.h"]
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",

@@ -19,6 +19,7 @@
 #include "kc_host.h"
 #include "kc_launch.h"
 #include "kc_beach.cuh"
+#include "kc_sample.cuh"
 
 namespace {
 
@@ -207,6 +208,21 @@ kc::DStep step_of(const kc_step_args* a) {
     s.az_on = a->az_kick; s.az_field = a->az_field; s.az_const = a->az_const;
     s.Dmin = a->Dmin; s.z0b_min = a->z0b_min; s.alpha_end = a->alpha_end;
     return s;
+}
+
+// sampling.py:383-429 / :487-541: one particle per thread; dead particles
+// and negative anchors give NaN.
+__global__ void __launch_bounds__(kBlock) k_sample(const __grid_constant__ kc::DMesh m, const kc::DSample S,
+                                                   const double* q, const double* z, const int* nn,
+                                                   const unsigned char* alive, long long P, int method, double* out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P) return;
+    const int a = nn[i];
+    if ((alive && !alive[i]) || a < 0) {
+        out[i] = __longlong_as_double(0x7ff8000000000000LL);
+        return;
+    }
+    out[i] = kc::sample_point(m, S, q[i], q[P + i], z ? z[i] : 0.0, a, method);
 }
 
 __global__ void __launch_bounds__(kBlock) k_nearest(const __grid_constant__ kc::DMesh m, const double* q, long long P, int* out) {
@@ -1976,6 +1992,74 @@ int kc_find_nearest(kc_ctx* c, long long P, const double* lon, const double* lat
     KC_CUDA(c, cudaMemcpyAsync(out, c->qout, (size_t)P * 4, cudaMemcpyDeviceToHost, c->stream));
     KC_CUDA(c, cudaStreamSynchronize(c->stream));
     return KC_OK;
+}
+
+// One scratch allocation for a sampling call (values, depths, query,
+// anchors, mask, results), freed before kc_sample_field returns.
+static int sample_run(kc_ctx* c, char* buf, const double* values, size_t nvals, int rows, const double* z_mids,
+                      long long P, const double* lon, const double* lat, const double* z, const int* nearest,
+                      const unsigned char* alive, int method, double* out) {
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    double* d_vals = (double*)buf;
+    double* d_zm = (double*)(buf + al(nvals * 8));
+    double* d_q = (double*)((char*)d_zm + al((size_t)rows * 8));
+    double* d_z = (double*)((char*)d_q + al((size_t)P * 16));
+    double* d_out = (double*)((char*)d_z + al((size_t)P * 8));
+    int* d_nn = (int*)((char*)d_out + al((size_t)P * 8));
+    unsigned char* d_al = (unsigned char*)((char*)d_nn + al((size_t)P * 4));
+    cudaStream_t st = c->stream;
+    KC_CUDA(c, cudaMemcpyAsync(d_vals, values, nvals * 8, cudaMemcpyHostToDevice, st));
+    if (rows > 0) {
+        KC_CUDA(c, cudaMemcpyAsync(d_zm, z_mids, (size_t)rows * 8, cudaMemcpyHostToDevice, st));
+        KC_CUDA(c, cudaMemcpyAsync(d_z, z, (size_t)P * 8, cudaMemcpyHostToDevice, st));
+    }
+    KC_CUDA(c, cudaMemcpyAsync(d_q, lon, (size_t)P * 8, cudaMemcpyHostToDevice, st));
+    KC_CUDA(c, cudaMemcpyAsync(d_q + P, lat, (size_t)P * 8, cudaMemcpyHostToDevice, st));
+    if (alive) KC_CUDA(c, cudaMemcpyAsync(d_al, alive, (size_t)P, cudaMemcpyHostToDevice, st));
+    if (nearest) {
+        KC_CUDA(c, cudaMemcpyAsync(d_nn, nearest, (size_t)P * 4, cudaMemcpyHostToDevice, st));
+    } else {
+        k_nearest<<<grid_for(P), kBlock, 0, st>>>(c->dm, d_q, P, d_nn);
+        KC_CUDA(c, cudaGetLastError());
+    }
+    kc::DSample S;
+    S.values = d_vals;
+    S.zm = rows > 0 ? d_zm : nullptr;
+    S.n = c->N;
+    S.rows = rows;
+    k_sample<<<grid_for(P), kBlock, 0, st>>>(c->dm, S, d_q, rows > 0 ? d_z : nullptr, d_nn, alive ? d_al : nullptr, P,
+                                           method, d_out);
+    KC_CUDA(c, cudaGetLastError());
+    KC_CUDA(c, cudaMemcpyAsync(out, d_out, (size_t)P * 8, cudaMemcpyDeviceToHost, st));
+    KC_CUDA(c, cudaStreamSynchronize(st));
+    return KC_OK;
+}
+
+int kc_sample_field(kc_ctx* c, const double* values, int rows, const double* z_mids, long long P, const double* lon,
+                    const double* lat, const double* z, const int* nearest, const unsigned char* alive, int method,
+                    double* out) {
+    if (!c) return KC_ERR_ARG;
+    if (!c->has_mesh) return fail(c, KC_ERR_STATE, "kc_sample_field: no mesh uploaded");
+    if (method < 0 || method > 3) return fail(c, KC_ERR_ARG, "kc_sample_field: method must be 0..3");
+    if (rows < 0 || !values || P < 0 || (P > 0 && (!lon || !lat || !out)))
+        return fail(c, KC_ERR_ARG, "kc_sample_field: arrays");
+    if (rows > 0 && (!z_mids || (P > 0 && !z) || !c->d_depth))
+        return fail(c, KC_ERR_ARG, "kc_sample_field: a mid-layer field needs z_mids, the depths and the mesh depth");
+    if (nearest)
+        for (long long i = 0; i < P; ++i)
+            if (nearest[i] >= c->N) return fail(c, KC_ERR_ARG, "kc_sample_field: nearest node out of range");
+    if (P == 0) return KC_OK;
+    KC_CUDA(c, cudaSetDevice(c->device));
+    const size_t nvals = (size_t)(rows > 0 ? rows : 1) * (size_t)c->N;
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t total = al(nvals * 8) + al((size_t)rows * 8) + al((size_t)P * 16) + 2 * al((size_t)P * 8) +
+                         al((size_t)P * 4) + al((size_t)P);
+    char* buf = nullptr;
+    KC_CUDA(c, cudaMalloc((void**)&buf, total));
+    const int rc = sample_run(c, buf, values, nvals, rows, z_mids, P, lon, lat, z, nearest, alive, method, out);
+    cudaStreamSynchronize(c->stream);
+    cudaFree(buf);
+    return rc;
 }
 
 int kc_find_elements(kc_ctx* c, long long P, const double* lon, const double* lat, const int* nn, int* out) {

@@ -448,6 +448,25 @@ class DeviceContext:
         self._chk(N.lib().kc_particles_get_elem(self._ctx, self.P, N.ptr(out)), "kc_particles_get_elem")
         return out
 
+    def sample_field(self, values, lon, lat, z=None, z_mids=None, nearest=None, alive=None,
+                     method: int = 1) -> np.ndarray:
+        """kc_sample_field: a node field (N,) or a mid-layer field (rows, N)
+        with its mid-layer depths, sampled at the points (NaN for dead or
+        anchorless ones)."""
+        values = _c(values, np.float64)
+        lon = _c(lon, np.float64)
+        lat = _c(lat, np.float64)
+        rows = values.shape[0] if values.ndim == 2 else 0
+        zz = _c(z, np.float64) if rows else None
+        zm = _c(z_mids, np.float64) if rows else None
+        nn = None if nearest is None else _c(nearest, np.int32)
+        al = None if alive is None else _c(np.asarray(alive).astype(np.uint8), np.uint8)
+        out = np.empty(lon.shape[0], np.float64)
+        self._chk(N.lib().kc_sample_field(self._ctx, N.ptr(values), rows, N.ptr(zm), lon.shape[0], N.ptr(lon),
+                                          N.ptr(lat), N.ptr(zz), N.ptr(nn), N.ptr(al), int(method), N.ptr(out)),
+                  "kc_sample_field")
+        return out
+
     def find_elements(self, lon, lat, nn=None) -> np.ndarray:
         """mesh.find_containing_elements on the device: the 1-ring / 2-ring
         scan around nn (None: the exact nearest node); -1 outside."""

@@ -2077,3 +2077,206 @@ int orc_node_xyz(int64_t n, const double* lon, const double* lat, double* out) {
     }
     return 0;
 }
+
+/* ------------------------------------------------------------------------
+ * Scalar field sampling at particle positions (numerics/sampling.py).
+ * ------------------------------------------------------------------------ */
+#define S_NEAREST 0
+#define S_LEASTSQ 1
+#define S_BARYCENTRIC 2
+#define S_IDW 3
+#define MAX_NEIGH 64   /* vertical.py:443 _MAX_NEIGHBOURS */
+
+/* vertical.py:447-485 _collect_neighbour_nodes: the centre, then each
+ * element's vertex slots in order, first occurrence only, at most 64. */
+static int neigh_ring(const OMesh* m, int nn, int32_t* buf) {
+    int count = 1;
+    buf[0] = nn;
+    int ne = m->n2e_cnt[nn];
+    for (int k = 0; k < ne; ++k) {
+        int e = m->n2e[(int64_t)nn * m->max_conn + k];
+        if (e < 0) continue;
+        for (int v = 0; v < m->max_v; ++v) {
+            int nd = m->en[(int64_t)e * m->max_v + v];
+            if (nd < 0) continue;
+            int found = 0;
+            for (int j = 0; j < count; ++j)
+                if (buf[j] == nd) { found = 1; break; }
+            if (!found && count < MAX_NEIGH) buf[count++] = nd;
+        }
+    }
+    return count;
+}
+
+/* sampling.py:82-380 _combine_horizontal */
+static double combine_horizontal(const OMesh* m, const double* vals, const int32_t* buf, int cnt, double lon_p,
+                                 double lat_p, int nn, int method) {
+    double fallback = vals[0];
+    if (method == S_NEAREST) return fallback;
+    if (method == S_IDW) {
+        double z0 = cos(lat_p * DEG2RAD) * SLM;
+        if (z0 < 1.0) z0 = 1.0;
+        double sw = 0.0, swv = 0.0;
+        for (int i = 0; i < cnt; ++i) {
+            int nd = buf[i];
+            double dx = wrap180(m->lon[nd] - lon_p) * z0;
+            double dy = (m->lat[nd] - lat_p) * SLM;
+            double d2 = dx * dx + dy * dy;
+            if (d2 < 1e-12) return vals[i];
+            if (!isfinite(vals[i])) continue;
+            double w = 1.0 / d2;
+            sw += w;
+            swv += w * vals[i];
+        }
+        if (sw < 1e-30) return fallback;
+        return swv / sw;
+    }
+    if (method == S_BARYCENTRIC) {
+        int ne = m->n2e_cnt[nn];
+        for (int k = 0; k < ne; ++k) {
+            int e = m->n2e[(int64_t)nn * m->max_conn + k];
+            if (e < 0) continue;
+            int verts[4], nv = 0;
+            for (int v = 0; v < m->max_v; ++v) {
+                int nd = m->en[(int64_t)e * m->max_v + v];
+                if (nd < 0) continue;
+                if (nv > 0 && nd == verts[0]) continue;
+                verts[nv++] = nd;
+            }
+            if (nv < 3) continue;
+            double ln[4], vx[4], vy[4];
+            for (int v = 0; v < nv; ++v) ln[v] = m->lon[verts[v]];
+            double lon0 = seam_lon0(ln, nv);
+            double lat0 = 0.0;
+            for (int v = 0; v < nv; ++v) lat0 += m->lat[verts[v]];
+            lat0 /= nv;
+            double cl = cos(lat0 * DEG2RAD);
+            for (int v = 0; v < nv; ++v) {
+                vx[v] = wrap180(m->lon[verts[v]] - lon0) * DEG2RAD * R_STD * cl;
+                vy[v] = (m->lat[verts[v]] - lat0) * DEG2RAD * R_STD;
+            }
+            double px = wrap180(lon_p - lon0) * DEG2RAD * R_STD * cl;
+            double py = (lat_p - lat0) * DEG2RAD * R_STD;
+            for (int t = 0; t < nv - 2; ++t) {
+                double ax = vx[0], ay = vy[0], bx = vx[t + 1], by = vy[t + 1], cx = vx[t + 2], cy = vy[t + 2];
+                double denom = (by - cy) * (ax - cx) + (cx - bx) * (ay - cy);
+                if (fabs(denom) < 1e-14) continue;
+                double w1 = ((by - cy) * (px - cx) + (cx - bx) * (py - cy)) / denom;
+                double w2 = ((cy - ay) * (px - cx) + (ax - cx) * (py - cy)) / denom;
+                double w3 = 1.0 - w1 - w2;
+                if (!(w1 >= -1e-6 && w2 >= -1e-6 && w3 >= -1e-6)) continue;
+                if (nv == 4) {
+                    double wts[4], acc = 0.0;
+                    polygon_weights(px, py, vx, vy, 4, wts);
+                    for (int vi = 0; vi < 4; ++vi) {
+                        double vv = vals[0];
+                        int fnd = 0;
+                        for (int j = 0; j < cnt; ++j)
+                            if (buf[j] == verts[vi]) { vv = vals[j]; fnd = 1; break; }
+                        if (!fnd || !isfinite(vv)) return fallback;
+                        acc += wts[vi] * vv;
+                    }
+                    return acc;
+                }
+                int n0 = verts[0], n1 = verts[t + 1], n2 = verts[t + 2];
+                double v0 = vals[0], v1 = vals[0], v2 = vals[0];
+                int f0 = 0, f1 = 0, f2 = 0;
+                for (int j = 0; j < cnt; ++j) {
+                    if (buf[j] == n0) { v0 = vals[j]; f0 = 1; }
+                    if (buf[j] == n1) { v1 = vals[j]; f1 = 1; }
+                    if (buf[j] == n2) { v2 = vals[j]; f2 = 1; }
+                }
+                if (!(f0 && f1 && f2)) return fallback;
+                if (!(isfinite(v0) && isfinite(v1) && isfinite(v2))) return fallback;
+                return w1 * v0 + w2 * v1 + w3 * v2;
+            }
+        }
+        return fallback;
+    }
+    if (method == S_LEASTSQ) {
+        if (cnt < 3) return fallback;
+        double z0 = cos(lat_p * DEG2RAD) * SLM;
+        if (z0 < 1.0) z0 = 1.0;
+        double a11 = 0.0, a12 = 0.0, a13 = 0.0, a22 = 0.0, a23 = 0.0, a33 = 0.0, f0 = 0.0, f1 = 0.0, f2 = 0.0;
+        int nfin = 0;
+        for (int i = 0; i < cnt; ++i) {
+            int nd = buf[i];
+            double val = vals[i];
+            if (!isfinite(val)) continue;
+            nfin++;
+            double ex = wrap180(m->lon[nd] - lon_p) * z0;
+            double ey = (m->lat[nd] - lat_p) * SLM;
+            a11 += 1.0; a12 += ex; a13 += ey;
+            a22 += ex * ex; a23 += ex * ey; a33 += ey * ey;
+            f0 += val; f1 += val * ex; f2 += val * ey;
+        }
+        if (nfin < 3) return fallback;
+        double a21 = a12, a31 = a13, a32 = a23;
+        double det = a11 * a22 * a33 + a12 * a23 * a31 + a13 * a21 * a32 - a13 * a22 * a31 - a12 * a21 * a33 -
+                     a11 * a23 * a32;
+        if (fabs(det) < 1e-12 || fabs(det) < 1e-12 * fabs(a11 * a22 * a33)) return fallback;
+        double inv = 1.0 / fabs(det);
+        double b11 = a22 * a33 - a23 * a32, b12 = a13 * a32 - a12 * a33, b13 = a12 * a23 - a13 * a22;
+        return (b11 * f0 + b12 * f1 + b13 * f2) * inv;
+    }
+    return fallback;
+}
+
+/* sampling.py:432-484 _interp_mid_linear_single on a (K1, N) field */
+static double mid_linear(const double* field, int64_t N, const double* zm, int K1, double z, int node) {
+    if (K1 == 0) return 0.0;
+    if (K1 == 1) return field[node];
+    if (z <= zm[0]) return field[node];
+    if (z >= zm[K1 - 1]) return field[(int64_t)(K1 - 1) * N + node];
+    for (int k = 0; k < K1 - 1; ++k) {
+        if (z < zm[k + 1]) {
+            double dz = zm[k + 1] - zm[k];
+            if (dz < 1e-12) return field[(int64_t)k * N + node];
+            double a = (z - zm[k]) / dz;
+            return (1.0 - a) * field[(int64_t)k * N + node] + a * field[(int64_t)(k + 1) * N + node];
+        }
+    }
+    return field[(int64_t)(K1 - 1) * N + node];
+}
+
+typedef struct {
+    const OMesh* m;
+    const double* values;
+    int rows;                  /* 0: a 2-D (N,) field; K1 >= 1: a (K1, N) mid-layer field */
+    const double* zm;          /* (K1) mid-layer depths */
+    const double *lon, *lat, *z;
+    const int* nearest;
+    const unsigned char* alive;
+    int method;
+    double* out;
+} SCtx;
+
+/* sampling.py:383-429 _loop_sample_2d and :487-541 _loop_sample_mid_3d, one particle */
+static void sample_body(void* ctx, int64_t i) {
+    SCtx* c = (SCtx*)ctx;
+    const OMesh* m = c->m;
+    if ((c->alive && !c->alive[i]) || c->nearest[i] < 0) { c->out[i] = NAN; return; }
+    int nn = c->nearest[i];
+    int32_t buf[MAX_NEIGH];
+    double vals[MAX_NEIGH];
+    int cnt = neigh_ring(m, nn, buf);
+    for (int k = 0; k < cnt; ++k) {
+        int nd = buf[k];
+        if (c->rows == 0) {
+            vals[k] = c->values[nd];
+        } else {
+            double zp = c->z[i];
+            double ze = zp < m->depth[nd] ? zp : m->depth[nd];
+            vals[k] = mid_linear(c->values, m->N, c->zm, c->rows, ze, nd);
+        }
+    }
+    c->out[i] = combine_horizontal(m, vals, buf, cnt, c->lon[i], c->lat[i], nn, c->method);
+}
+
+int orc_sample(const orc_mesh* mm, const double* values, int rows, const double* zm, int64_t P, const double* lon,
+               const double* lat, const double* z, const int* nearest, const unsigned char* alive, int method,
+               double* out) {
+    SCtx c = {(const OMesh*)mm, values, rows, zm, lon, lat, z, nearest, alive, method, out};
+    par_for(P, sample_body, &c);
+    return 0;
+}

@@ -80,6 +80,7 @@ def lib():
         L.orc_contain.argtypes = [C.POINTER(OMesh), i64, vp, vp, vp, vp]
         L.orc_normals.argtypes = [i64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, vp]
         L.orc_node_xyz.argtypes = [i64, vp, vp, vp]
+        L.orc_sample.argtypes = [C.POINTER(OMesh), vp, C.c_int, vp, i64, vp, vp, vp, vp, vp, C.c_int, vp]
         L.orc_normal_pair.argtypes = [C.c_uint64] * 5 + [vp]
         L.orc_beach.argtypes = [C.POINTER(OMesh), C.c_void_p, vp, i64, vp, vp, vp, vp, vp, vp, vp]
         L.orc_set_threads.argtypes = [C.c_int]
@@ -397,4 +398,31 @@ def node_xyz(lon, lat) -> np.ndarray:
     lat = np.ascontiguousarray(lat, dtype=np.float64)
     out = np.empty((lon.size, 3))
     lib().orc_node_xyz(lon.size, _p(lon), _p(lat), _p(out))
+    return out
+
+
+SAMPLE_METHODS = {"nearest": 0, "leastsq": 1, "barycentric": 2, "idw": 3}
+
+
+def sample_field(values, mesh, lon, lat, z=None, *, nearest=None, alive=None, method="leastsq", view=None):
+    """sampling.py:727 sample_field for a node field of shape (N,) or a
+    z-level mid-layer field (K-1, N): the oracle's restatement."""
+    view = view or MeshView(mesh)
+    values = np.ascontiguousarray(values, dtype=np.float64)
+    lon = np.ascontiguousarray(lon, dtype=np.float64)
+    lat = np.ascontiguousarray(lat, dtype=np.float64)
+    P = lon.size
+    if nearest is None:
+        nearest = find_nearest(mesh, lon, lat, view)
+    nearest = np.ascontiguousarray(nearest, dtype=np.int32)
+    al = None if alive is None else np.ascontiguousarray(alive, dtype=np.uint8)
+    rows, zm, zz = 0, None, None
+    if values.ndim == 2:
+        zl = np.abs(np.asarray(mesh.sigma, dtype=np.float64))
+        zm = np.ascontiguousarray(0.5 * (zl[:-1] + zl[1:]))
+        rows = values.shape[0]
+        zz = np.ascontiguousarray(z, dtype=np.float64)
+    out = np.empty(P)
+    lib().orc_sample(C.byref(view.s), _p(values), rows, _p(zm), P, _p(lon), _p(lat), _p(zz), _p(nearest), _p(al),
+                     SAMPLE_METHODS[method], _p(out))
     return out

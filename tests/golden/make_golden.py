@@ -793,6 +793,57 @@ RNG_KEY_SETS = (   # (seed, realization, first particle id, step, component), 2^
 RNG_SET_SIZE = 1 << 20
 
 
+def sample_fixture():
+    """sampling.py:727 sample_field, the reference's own outputs: 2-D node
+    fields on a seam-wrapping triangle band and on a regional tri/quad mesh,
+    and a z-level mid-layer (K-1, N) field on a 3-D band, with every method;
+    fill NaNs in the fields (isolated nodes, and the levels below each node's
+    bottom), query points on nodes (the coincident-node rule), dead particles
+    and nearest = -1.  tests/golden/golden_sample_*.npz."""
+    from kelp.numerics.sampling import sample_field as r_sample
+    methods = ("nearest", "leastsq", "barycentric", "idw")
+    zl = S.stretched_levels(12, 5.0, 4000.0)
+    meshes = {
+        "band": (S.lattice_mesh(3.0, 72.0, jitter=0.2, land_frac=0.3), None),
+        "quad": (S.lattice_mesh(1.0, 15.0, lon_min=-20.0, lon_max=20.0, jitter=0.15, land_frac=0.2,
+                                quad_frac=0.3), None),
+        "3d": (S.lattice_mesh(3.0, 60.0, jitter=0.2, land_frac=0.25,
+                              depth=lambda lo, la: S.smooth_bathymetry(lo, la, 30.0, 4000.0), sigma=zl), zl),
+    }
+    for name, (m, sig) in meshes.items():
+        rm = ref_mesh(m, sigma=sig)
+        rng = np.random.default_rng({"band": 1, "quad": 2, "3d": 3}[name])
+        lo, la = np.asarray(m.nodes_lon), np.asarray(m.nodes_lat)
+        N = lo.size
+        v2 = 10.0 + 5.0 * np.sin(np.radians(2.0 * lo)) * np.cos(np.radians(3.0 * la)) + 0.01 * la
+        v2[rng.choice(N, N // 30, replace=False)] = np.nan
+        P = 1500
+        lon, lat, z, _ = particles(m, P, 21 + len(name), z=sig is not None)
+        on = rng.choice(P, 60, replace=False)                       # exactly on nodes
+        pick = rng.choice(N, 60, replace=False)
+        lon[on], lat[on] = lo[pick], la[pick]
+        alive = np.ones(P, bool)
+        alive[rng.choice(P, 40, replace=False)] = False
+        nearest = find_nearest_nodes(rm, lon, lat).astype(np.int32)
+        nearest[rng.choice(P, 20, replace=False)] = -1
+        d = {f"mesh_{k}": v for k, v in mesh_record(rm).items()}
+        d.update(lon=lon, lat=lat, alive=alive, nearest=nearest, v2=v2)
+        for meth in methods:
+            d[f"o2_{meth}"] = r_sample(v2, rm, lon, lat, nearest=nearest, alive=alive, method=meth)
+        if sig is not None:
+            zmid = 0.5 * (np.abs(zl)[:-1] + np.abs(zl)[1:])
+            v3 = (4.0 + 20.0 * np.exp(-zmid[:, None] / 700.0)
+                  * (1.0 + 0.3 * np.sin(np.radians(3.0 * lo)))[None, :])
+            v3[zmid[:, None] > np.asarray(m.depth)[None, :]] = np.nan     # fill below the bottom
+            v3[rng.integers(0, zmid.size, 50), rng.choice(N, 50, replace=False)] = np.nan
+            d.update(z=z, v3=v3)
+            for meth in methods:
+                d[f"o3_{meth}"] = r_sample(v3, rm, lon, lat, z, nearest=nearest, alive=alive, method=meth)
+        path = os.path.join(HERE, f"golden_sample_{name}.npz")
+        np.savez_compressed(path, **d)
+        print(f"golden_sample_{name}", os.path.getsize(path) // 1024, "KB")
+
+
 def rng1m_fixture():
     """The reference's own _normal_pair on 4 x 2^20 keys (contiguous particle
     ids under 4 key tuples), stored as per-chunk digests (tests/golden/
@@ -850,11 +901,13 @@ def reftypes_fixture():
 
 if __name__ == "__main__":
     # no argument: every fixture; otherwise the named ones ("steps", "beach", ...)
-    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq", "rng1m", "tripolar", "reftypes"}
+    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq", "rng1m", "tripolar", "reftypes", "sample"}
     if "rng1m" in which:
         rng1m_fixture()
     if "reftypes" in which:
         reftypes_fixture()
+    if "sample" in which:
+        sample_fixture()
     if "lsq" in which:
         lsq_fixture()
     if "steps" in which:
