@@ -33,9 +33,6 @@
 #ifndef KC_INL_STAGE
 #define KC_INL_STAGE __noinline__         // interp_uv_at, w_bary_at (plain form)
 #endif
-#ifndef KC_INL_MSTAGE
-#define KC_INL_MSTAGE __forceinline__     // stage_f32 (mixed form): inlined, 11 % faster on the 3-D RK2 step
-#endif
 #ifndef KC_INL_KICK
 #define KC_INL_KICK __noinline__          // apply_kick
 #endif

@@ -150,8 +150,8 @@ void launch_step_kernel_t(const kc::DMesh& m, const kc::DBlend<T>& f, const kc::
         else k_step2d<T, 2, Form, WALK><<<g, kBlock, 0, stream>>>(m, f, st, s);
     } else {
         if (scheme == 1) k_step3d_rk2<T, Form, WALK><<<g, kBlock, 0, stream>>>(m, f, st, s);
-        else if (scheme == 2) k_step3d_unfused<T, 2, Form, WALK><<<g, kBlock, 0, stream>>>(m, f, st, s);
-        else k_step3d_unfused<T, 0, Form, WALK><<<g, kBlock, 0, stream>>>(m, f, st, s);
+        else if (scheme == 2) k_step3d_unfused<T, 2, typename kc::UnfusedFormOf<Form>::type, WALK><<<g, kBlock, 0, stream>>>(m, f, st, s);
+        else k_step3d_unfused<T, 0, typename kc::UnfusedFormOf<Form>::type, WALK><<<g, kBlock, 0, stream>>>(m, f, st, s);
     }
 }
 
@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(BLOCK, multi_threads_per_sm<DIMS, SCHEME>() / 
             if (st.prev) st.prev[i] = st.status[i];
             if (DIMS == 2) kc::step2d_particle<T, SCHEME, Form>(m, pk.f, st, pk.s, i);
             else if (SCHEME == 1) kc::step3d_rk2_particle<T, Form>(m, pk.f, st, pk.s, i);
-            else kc::step3d_unfused_particle<T, SCHEME, Form>(m, pk.f, st, pk.s, i);
+            else kc::step3d_unfused_particle<T, SCHEME, typename kc::UnfusedFormOf<Form>::type>(m, pk.f, st, pk.s, i);
             if (pk.beach) kc::beach_particle(m, st, pk.b, N, i);
         }
     }

@@ -165,7 +165,7 @@ __device__ __forceinline__ float w_node_f32(const DMesh& m, const DBlend<T>& f, 
 // layer_linear).  One function per combination, so each keeps only its own
 // values live across its calls.
 template <typename T, int DIMS, bool DL>
-__device__ KC_INL_MSTAGE bool stage_f32(const DMesh& m, const DBlend<T>& f, const DStep& s, double xp,
+__device__ __forceinline__ bool stage_f32(const DMesh& m, const DBlend<T>& f, const DStep& s, double xp,
                                        double yp, int nn, int hint, int whint, double z, double alpha, double& U,
                                        double& V, double& W) {
     U = 0.0;
@@ -305,22 +305,45 @@ __device__ KC_INL_MSTAGE bool stage_f32(const DMesh& m, const DBlend<T>& f, cons
     return true;
 }
 
-// The mixed form as a step-body policy (see PlainForm in kc_step.cuh).
-template <typename T>
+// The same stage behind a call boundary: the unfused 3-D RK4 / Euler step
+// evaluates four stages, and four inlined copies of both vertical variants
+// (eight in all) cost more in instruction fetch than the calls.
+template <typename T, int DIMS, bool DL>
+__device__ __noinline__ bool stage_f32_call(const DMesh& m, const DBlend<T>& f, const DStep& s, double xp, double yp,
+                                            int nn, int hint, int whint, double z, double alpha, double& U,
+                                            double& V, double& W) {
+    return stage_f32<T, DIMS, DL>(m, f, s, xp, yp, nn, hint, whint, z, alpha, U, V, W);
+}
+
+// The mixed form as a step-body policy (see PlainForm in kc_step.cuh).  INL:
+// the stage inlined into the kernel (the fused 3-D RK2 and the 2-D steps,
+// measured 11 % faster on the 3-D RK2 step) or called (the unfused 3-D
+// steps, UnfusedFormOf).
+template <typename T, bool INL = true>
 struct MixedForm {
     static constexpr bool kExact = false;   // CUDA's sincos for sites and draws
     static __device__ __forceinline__ Site site(double lon, double lat) { return make_site_fast(lon, lat); }
     static __device__ __forceinline__ bool uv2(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
                                                double lat, int nn, int hint, double alpha, double& U, double& V) {
         double W;
-        return stage_f32<T, 2, false>(m, f, s, lon, lat, nn, hint, -3, 0.0, alpha, U, V, W);
+        if constexpr (INL) return stage_f32<T, 2, false>(m, f, s, lon, lat, nn, hint, -3, 0.0, alpha, U, V, W);
+        else return stage_f32_call<T, 2, false>(m, f, s, lon, lat, nn, hint, -3, 0.0, alpha, U, V, W);
     }
     static __device__ __forceinline__ bool uvw3(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
                                                 double lat, int nn, int hint, int whint, double z, double alpha,
                                                 double& U, double& V, double& W) {
-        return s.uv_dl ? stage_f32<T, 3, true>(m, f, s, lon, lat, nn, hint, whint, z, alpha, U, V, W)
-                       : stage_f32<T, 3, false>(m, f, s, lon, lat, nn, hint, whint, z, alpha, U, V, W);
+        if constexpr (INL)
+            return s.uv_dl ? stage_f32<T, 3, true>(m, f, s, lon, lat, nn, hint, whint, z, alpha, U, V, W)
+                           : stage_f32<T, 3, false>(m, f, s, lon, lat, nn, hint, whint, z, alpha, U, V, W);
+        else
+            return s.uv_dl ? stage_f32_call<T, 3, true>(m, f, s, lon, lat, nn, hint, whint, z, alpha, U, V, W)
+                           : stage_f32_call<T, 3, false>(m, f, s, lon, lat, nn, hint, whint, z, alpha, U, V, W);
     }
+};
+
+template <typename T>
+struct UnfusedFormOf<MixedForm<T, true>> {
+    using type = MixedForm<T, false>;
 };
 
 }  // namespace kc

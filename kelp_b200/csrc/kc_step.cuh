@@ -458,6 +458,13 @@ __device__ __forceinline__ bool stage_uv(const DMesh& m, const DBlend<T>& f, con
 // kernels of integrators.py:1490-2520 and their PCHIP twins :2820-3100):
 // the stage reads the anchor's element ring, no containment; plain float64
 // arithmetic, 2-D only.
+// The form an unfused 3-D step (four stages) runs with: the form itself,
+// unless a form says otherwise (MixedForm: its stage behind a call).
+template <typename Form>
+struct UnfusedFormOf {
+    using type = Form;
+};
+
 template <typename T>
 struct LsqForm {
     static constexpr bool kExact = true;
