@@ -39,6 +39,8 @@
  *   kc_field_upload_eta <- core.io.VelocityField.eta (src/kelp/core/io.py:180)
  *   kc_rng_normals     <- numerics.diffusion._normal_pair (src/kelp/numerics/diffusion.py:233)
  *   kc_sample_field    <- numerics.sampling.sample_field (src/kelp/numerics/sampling.py:727)
+ *   kc_beach_surface   <- the vel.eta / vel.scalars[dry_mask_var] reads of tracking._apply_beaching_hook
+ *                         (src/kelp/tracking.py:236-327)
  */
 #ifndef KELP_CUDA_H
 #define KELP_CUDA_H
@@ -47,7 +49,7 @@
 extern "C" {
 #endif
 
-#define KC_ABI_VERSION 12
+#define KC_ABI_VERSION 13
 
 #define KC_OK 0
 #define KC_ERR_ARG 1      /* invalid argument or combination */
@@ -283,6 +285,16 @@ int kc_beach_state_download(kc_ctx* ctx, int* wet_streak);
 
 /* The beaching hook on the resident particles after a step. */
 int kc_beach(kc_ctx* ctx, const kc_beach_args* args);
+
+/* The payload's node surfaces for the beaching hook, tracking.py:236-327 and
+ * beaching.py:95-181: eta (N) the free surface added to the anchor's depth
+ * (beaching.use_eta), dry_mask (N) the dry-mask variable's surface layer
+ * (beaching.dry_mask_var; a node above 0.5 is dry for the depth criterion
+ * and never wet for resuspension).  Each is copied and used by the following
+ * kc_beach calls until set again; NULL turns it off.  The host blends them
+ * as the payload does ((1 - alpha) a + alpha b).  kc_run_fused refuses a
+ * beaching hook while a surface is set (it changes every step). */
+int kc_beach_surface(kc_ctx* ctx, const double* eta, const double* dry_mask);
 
 /* Host particle arrays of kc_step_host (SoA, P entries each).  Input: lon,
  * lat, status, nearest_node required; z and failure_reason may be NULL

@@ -11,8 +11,11 @@ stochastic resuspension.  One kernel launch (``kc_beach``) per hook call; the
 stochastic draws use the same counter hash as the diffusion kick with
 components 10 and 11, keyed by the particle's original index.
 
-Not built: the sea-surface-height column (``use_eta``) and the dry-mask
-variable (``dry_mask_var``) raise ``NotImplementedError``.
+With ``use_eta`` the payload's free surface is added to the anchor's depth,
+and with ``dry_mask_var`` the payload's scalar of that name (its surface
+layer) marks dry nodes: both node arrays are formed on the host as the
+payload forms them and handed to the kernel per hook call
+(``kc_beach_surface``).
 """
 from __future__ import annotations
 
@@ -105,10 +108,6 @@ def beach_args(run_cfg: BeachRunConfig, real_id: int, step_i: int, dt: float) ->
     1 - exp(-|dt| / t) with the host's exp, as the reference evaluates them
     (beaching.py:135, :170)."""
     cfg = run_cfg.cfg
-    if cfg.use_eta:
-        raise NotImplementedError("beaching.use_eta (the eta column height) is not built on the CUDA backend")
-    if cfg.dry_mask_var:
-        raise NotImplementedError("beaching.dry_mask_var is not built on the CUDA backend")
     crit = run_cfg.crit
     a = N.BeachArgs()
     a.use_depth = int("depth" in crit)
@@ -131,6 +130,38 @@ def beach_args(run_cfg: BeachRunConfig, real_id: int, step_i: int, dt: float) ->
     return a
 
 
+def _payload_node(vel, get):
+    """A node array of the step's payload as the reference reads it: a
+    LazyLerpField's is (1 - alpha) a + alpha b of its pair, in the arrays'
+    own dtype (io.py:68-117, :499-513)."""
+    if all(hasattr(vel, k) for k in ("vel_a", "vel_b", "alpha")):
+        a, b = get(vel.vel_a), get(vel.vel_b)
+        if a is None or b is None:
+            return None
+        return (1.0 - float(vel.alpha)) * np.asarray(a) + float(vel.alpha) * np.asarray(b)
+    return get(vel)
+
+
+def payload_surfaces(vel, cfg: BeachingConfig):
+    """(eta, dry_mask) node arrays the hook reads from the payload
+    (tracking.py:236-327): eta when ``use_eta``, the surface layer of the
+    ``dry_mask_var`` scalar when the payload carries it; None otherwise."""
+    eta = dry = None
+    if cfg.use_eta:
+        eta = _payload_node(vel, lambda v: getattr(v, "eta", None))
+        if eta is None:
+            raise ValueError("beaching.use_eta needs the payload's eta")
+    if cfg.dry_mask_var:
+        def surface(v):
+            x = (getattr(v, "scalars", None) or {}).get(cfg.dry_mask_var)
+            if x is None:
+                return None
+            x = np.asarray(x)
+            return x[0] if x.ndim > 1 else x
+        dry = _payload_node(vel, surface)
+    return eta, dry
+
+
 def apply_beaching_hook(state: ParticleState, prev_status, mesh, vel, run_cfg: BeachRunConfig, wet_streak,
                         real_id: int, step_i: int, dt: float, ctx=None):
     """Beaching + resuspension of a post-step state (tracking.py:199-364).
@@ -148,6 +179,7 @@ def apply_beaching_hook(state: ParticleState, prev_status, mesh, vel, run_cfg: B
     ctx.upload_particles(state.lon, state.lat, state.z, state.status, state.nearest_node,
                          fr=state.failure_reason)
     ctx.beach_state_upload(prev_status, wet)
+    ctx.beach_surface(*payload_surfaces(vel, run_cfg.cfg))
     ctx.beach(a)
     out = ctx.download_particles()
     ws = ctx.beach_state_download()

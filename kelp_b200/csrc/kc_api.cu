@@ -74,6 +74,9 @@ struct kc_ctx {
     double2* d_nsc = nullptr;
     double2* d_ecos = nullptr;
     float4* d_ebox = nullptr;        // containment prefilter boxes
+    double* d_beach_eta = nullptr;   // (N) beaching surfaces set by kc_beach_surface
+    double* d_beach_dry = nullptr;
+    bool beach_eta_on = false, beach_dry_on = false;
     double2* d_erec = nullptr;       // per-element mask vertex coordinates
     int* d_maxl = nullptr;
     double* d_dl_p = nullptr;
@@ -818,6 +821,8 @@ void free_mesh(kc_ctx* c) {
     dfree(c->d_nsc); dfree(c->d_ecos); dfree(c->d_ebox); dfree(c->d_erec); dfree(c->d_maxl); dfree(c->d_coastal);
     c->dm.ebox = nullptr;
     c->dm.erec = nullptr;
+    dfree(c->d_beach_eta); dfree(c->d_beach_dry);
+    c->beach_eta_on = c->beach_dry_on = false;
     dfree(c->d_dl_p); dfree(c->d_dl_last); dfree(c->d_dl_bed); dfree(c->d_enb); dfree(c->d_sigma);
     dfree(c->d_cg_corners); dfree(c->d_cg_cell); dfree(c->d_cg_nlev); dfree(c->d_cg_nlev_r); dfree(c->d_cg_L);
     dfree(c->d_cg_e2u); dfree(c->d_cg_e1v); dfree(c->d_cg_area); dfree(c->d_cg_zw); dfree(c->d_cg_e3b);
@@ -1322,6 +1327,8 @@ static int beach_of(kc_ctx* c, const kc_beach_args* a, kc::DBeach& b) {
     b.p_beach = a->p_beach; b.p_resusp = a->p_resusp;
     b.seed = a->seed; b.real_id = a->real_id; b.step_i = a->step_i; b.pid_offset = a->pid_offset;
     b.coastal = need_topo ? c->d_coastal : nullptr;
+    b.eta = c->beach_eta_on ? c->d_beach_eta : nullptr;
+    b.dry = c->beach_dry_on ? c->d_beach_dry : nullptr;
     b.prev = c->prev;
     b.wet_streak = c->wet;
     return KC_OK;
@@ -1348,6 +1355,25 @@ int kc_beach(kc_ctx* c, const kc_beach_args* a) {
     kc::DState st = state_of(c);
     k_beach<<<grid_for(c->P), kBlock, 0, c->stream>>>(c->dm, st, b, c->N);
     KC_CUDA(c, cudaGetLastError());
+    return KC_OK;
+}
+
+int kc_beach_surface(kc_ctx* c, const double* eta, const double* dry_mask) {
+    if (!c) return KC_ERR_ARG;
+    if (!c->has_mesh) return fail(c, KC_ERR_STATE, "kc_beach_surface: no mesh uploaded");
+    KC_CUDA(c, cudaSetDevice(c->device));
+    const size_t bytes = (size_t)c->N * 8;
+    if (eta) {
+        if (!c->d_beach_eta) KC_CUDA(c, cudaMalloc((void**)&c->d_beach_eta, bytes));
+        KC_CUDA(c, cudaMemcpyAsync(c->d_beach_eta, eta, bytes, cudaMemcpyHostToDevice, c->stream));
+    }
+    if (dry_mask) {
+        if (!c->d_beach_dry) KC_CUDA(c, cudaMalloc((void**)&c->d_beach_dry, bytes));
+        KC_CUDA(c, cudaMemcpyAsync(c->d_beach_dry, dry_mask, bytes, cudaMemcpyHostToDevice, c->stream));
+    }
+    if (eta || dry_mask) KC_CUDA(c, cudaStreamSynchronize(c->stream));   // the caller may free its arrays
+    c->beach_eta_on = eta != nullptr;
+    c->beach_dry_on = dry_mask != nullptr;
     return KC_OK;
 }
 
@@ -1857,6 +1883,8 @@ static int run_fused_t(kc_ctx* c, const kc_step_args* steps, int n, const kc_bea
         pk[j].s = step_of(&steps[j]);
         pk[j].beach = beach ? 1 : 0;
         if (beach) {
+            if (c->beach_eta_on || c->beach_dry_on)   // one surface per call cannot follow several steps
+                return fail(c, KC_ERR_ARG, "kc_run_fused: beaching surfaces are per step; use kc_step + kc_beach");
             int rc = beach_of(c, &beach[j], pk[j].b);
             if (rc) return rc;
         }

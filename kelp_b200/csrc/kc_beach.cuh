@@ -17,6 +17,8 @@ struct DBeach {
     double p_beach, p_resusp;                    // 1 - exp(-|dt| / t), evaluated by the host
     unsigned long long seed, real_id, step_i, pid_offset;
     const unsigned char* coastal;                // (E) coastal element flags, null without topology
+    const double* eta;                           // (N) the payload's free surface (use_eta), or null
+    const double* dry;                           // (N) the payload's dry mask (dry_mask_var), or null
     const int* prev;                             // (P) status at the step's entry
     int* wet_streak;                             // (P) consecutive wet steps of a beached particle
 };
@@ -53,7 +55,15 @@ __device__ __forceinline__ void beach_particle(const DMesh& m, const DState& st,
         const int a = nn < 0 ? (int)(nn + N) : nn;
         contained = contain_local(m, st.lon[i], st.lat[i], a);
     }
-    const double h_raw = nn >= 0 ? m.depth[nn] : INFINITY;
+    // the unclamped column height, with the free surface when use_eta
+    // (beaching.py:112-117, tracking.py:290-297); a node the dry mask marks
+    // (> 0.5) is dry for the depth criterion and never wet (:124-129, :151-159)
+    double h_raw = INFINITY;
+    if (nn >= 0) {
+        h_raw = m.depth[nn];
+        if (b.eta) h_raw = h_raw + b.eta[nn];
+    }
+    const bool masked = b.dry && nn >= 0 && b.dry[nn] > 0.5;
     const bool coastal_contact = contained >= 0 && b.coastal && b.coastal[contained];
     const long long pid = st.pid ? st.pid[i] : i;
     const unsigned long long key = (unsigned long long)pid + b.pid_offset;
@@ -70,7 +80,7 @@ __device__ __forceinline__ void beach_particle(const DMesh& m, const DState& st,
     // 2. criteria (beaching.py:118-140)
     const bool alive = status == ALIVE, beached = status == BEACHED;
     bool to_beach = false;
-    if (b.use_depth) to_beach = to_beach || (h_raw < b.depth_min);
+    if (b.use_depth) to_beach = to_beach || (h_raw < b.depth_min) || masked;
     if (b.use_coastal) to_beach = to_beach || coastal_contact;
     if (b.use_stochastic && alive) {
         bool in_zone = h_raw < b.zone_depth;
@@ -82,7 +92,7 @@ __device__ __forceinline__ void beach_particle(const DMesh& m, const DState& st,
     int ws = b.wet_streak[i];
     bool to_release = false;
     if (b.resuspension != RESUSP_NEVER && beached) {
-        const bool rewet = h_raw > b.rewet_level && nn >= 0;
+        const bool rewet = h_raw > b.rewet_level && nn >= 0 && !masked;
         ws = rewet ? ws + 1 : 0;
         if (b.resuspension == RESUSP_AUTO || b.resuspension == RESUSP_BOTH)
             to_release = to_release || ws >= b.min_wet_steps;

@@ -382,6 +382,17 @@ class DeviceContext:
         self._chk(N.lib().kc_beach_state_download(self._ctx, N.ptr(out)), "kc_beach_state_download")
         return out
 
+    def beach_surface(self, eta=None, dry_mask=None) -> None:
+        """kc_beach_surface: the node free surface and dry mask the next
+        beaching calls read (None: off)."""
+        e = None if eta is None else _c(eta, np.float64)
+        d = None if dry_mask is None else _c(dry_mask, np.float64)
+        n = None if self._mesh_ref is None else int(np.asarray(self._mesh_ref.nodes_lon).shape[0])
+        for a in (e, d):
+            if a is not None and (n is None or a.shape != (n,)):
+                raise ValueError("beaching surfaces are node arrays (N,) of the uploaded mesh")
+        self._chk(N.lib().kc_beach_surface(self._ctx, N.ptr(e), N.ptr(d)), "kc_beach_surface")
+
     def beach(self, args: N.BeachArgs) -> None:
         self._chk(N.lib().kc_beach(self._ctx, C.byref(args)), "kc_beach")
 

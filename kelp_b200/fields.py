@@ -42,6 +42,12 @@ class VelocityField:
             raise ValueError(f"u/v shape mismatch {self.u.shape} vs {self.v.shape}")
 
 
+def _lerp(a, b, alpha: float) -> np.ndarray:
+    """(1 - alpha) a + alpha b in the arrays' own dtype, the expression of
+    io.py:68-117 _blend (a float32 pair blends in float32, as numpy does)."""
+    return (1.0 - alpha) * np.asarray(a) + alpha * np.asarray(b)
+
+
 class LazyLerpField:
     """``(vel_a, vel_b, alpha)``: the field at a time between two snapshots.
 
@@ -70,8 +76,7 @@ class LazyLerpField:
         a, b = getattr(self.vel_a, name), getattr(self.vel_b, name)
         if a is None or b is None:
             return None
-        beta = 1.0 - self.alpha
-        return beta * np.asarray(a, dtype=np.float64) + self.alpha * np.asarray(b, dtype=np.float64)
+        return _lerp(a, b, self.alpha)
 
     @property
     def u(self):
@@ -90,6 +95,17 @@ class LazyLerpField:
     @property
     def eta(self):
         return self._blend("eta")
+
+    @property
+    def scalars(self):
+        """The snapshots' node scalars blended key by key (io.py:499-513),
+        None unless both carry them."""
+        sa, sb = getattr(self.vel_a, "scalars", None), getattr(self.vel_b, "scalars", None)
+        if sa is None or sb is None:
+            return None
+        if set(sa) != set(sb):
+            raise ValueError(f"LazyLerpField: scalars key mismatch {sorted(sa)} vs {sorted(sb)}")
+        return {k: _lerp(sa[k], sb[k], self.alpha) for k in sa}
 
     @property
     def az(self):

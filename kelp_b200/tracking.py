@@ -34,7 +34,7 @@ import numpy as np
 
 from . import _native as N
 from . import integrators as KI
-from .beaching import BeachingConfig, beach_args, make_run_config
+from .beaching import BeachingConfig, beach_args, make_run_config, payload_surfaces
 from .device import default_context
 from .diffusion import DiffusionStepArgs
 from .fields import LazyLerpField, VelocityField
@@ -378,13 +378,16 @@ class Tracker:
                 e0 = ctx.find_elements(init_state.lon, init_state.lat)
             ctx.set_elem(rep(np.asarray(e0, dtype=np.int32)))
         beach_cfg = None
+        surfaces = False
         if self.beaching is not None:
+            surfaces = bool(self.beaching.use_eta or self.beaching.dry_mask_var)
             seed = int(getattr(self.diffusion, "seed", 0)) if self.diffusion is not None else 0
             beach_cfg = make_run_config(self.beaching, mesh, diffusion_seed=seed, particle_offset=particle_offset)
             if beach_cfg.need_topo:
                 ctx.ensure_coastal(mesh, beach_cfg.elem_coastal)
             ws0 = None if start_wet_streak is None else rep(np.asarray(start_wet_streak, dtype=np.int32))
             ctx.beach_state_upload(None, ws0)
+            ctx.beach_surface(None, None)
         records = [TrajectoryRecord() for _ in range(R)]
         for r in range(R):
             records[r].release_lon = np.array(init_state.lon, copy=True)
@@ -436,6 +439,8 @@ class Tracker:
             a.global_step = g
             ctx.step(a)
             if beach_cfg is not None:
+                if surfaces:
+                    ctx.beach_surface(*payload_surfaces(vel, beach_cfg.cfg))
                 ctx.beach(beach_args(beach_cfg, realizations[0], g, self.dt))
             sim_time = sim_time_end if sim_time_end is not None else sim_time + self.dt * self.direction
             if self.prefetch and k + 1 < int(n_steps):

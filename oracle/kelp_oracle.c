@@ -2007,9 +2007,11 @@ static double u01(uint64_t seed, uint64_t real_id, uint64_t pid, uint64_t step, 
     return (double)(h >> 11) * (1.0 / 9007199254740992.0);
 }
 
+/* eta (N): the payload's free surface when use_eta, else NULL; dry (N): the
+ * dry-mask variable's surface layer, else NULL (tracking.py:236-327). */
 int orc_beach(const orc_mesh* mm, const orc_beach_args* a, const unsigned char* coastal, int64_t P,
               const double* lon, const double* lat, int* status, const int* prev, int* nn, int8_t* fr,
-              int* wet) {
+              int* wet, const double* eta, const double* dry) {
     const OMesh* m = (const OMesh*)mm;
     int need_topo = a->use_coastal || a->use_stochastic;
     int any_beached = 0;
@@ -2024,7 +2026,8 @@ int orc_beach(const orc_mesh* mm, const orc_beach_args* a, const unsigned char* 
             cont[i] = contain_local(m, lon[i], lat[i], a0);
         }
         if (a->on_failure && newly) {
-            double hf = nn[i] >= 0 ? m->depth[nn[i]] : INFINITY;
+            double hf = INFINITY;
+            if (nn[i] >= 0) { hf = m->depth[nn[i]]; if (eta) hf = hf + eta[nn[i]]; }
             int context = hf < a->zone_depth;
             if (need_topo && cont[i] >= 0 && coastal[cont[i]]) context = 1;
             if (context) { status[i] = 2; fr[i] = 0; }
@@ -2034,11 +2037,13 @@ int orc_beach(const orc_mesh* mm, const orc_beach_args* a, const unsigned char* 
     double rewet_level = a->depth_min + a->rewet_hysteresis;
     for (int64_t i = 0; i < P; ++i) {
         int alive = status[i] == ALIVE, beached = status[i] == 2;
-        double h = nn[i] >= 0 ? m->depth[nn[i]] : INFINITY;
+        double h = INFINITY;
+        if (nn[i] >= 0) { h = m->depth[nn[i]]; if (eta) h = h + eta[nn[i]]; }
+        int masked = dry && nn[i] >= 0 && dry[nn[i]] > 0.5;
         int cc = need_topo && cont[i] >= 0 && coastal[cont[i]];
         uint64_t key = (uint64_t)i + a->pid_offset;
         int to_beach = 0;
-        if (a->use_depth && h < a->depth_min) to_beach = 1;
+        if (a->use_depth && (h < a->depth_min || masked)) to_beach = 1;
         if (a->use_coastal && cc) to_beach = 1;
         if (a->use_stochastic && alive) {
             int in_zone = h < a->zone_depth || cc;
@@ -2047,7 +2052,7 @@ int orc_beach(const orc_mesh* mm, const orc_beach_args* a, const unsigned char* 
         to_beach = to_beach && alive;
         int ws = wet[i], to_release = 0;
         if (a->resuspension != 0 && any_beached && beached) {
-            int rewet = h > rewet_level && nn[i] >= 0;
+            int rewet = h > rewet_level && nn[i] >= 0 && !masked;
             ws = rewet ? ws + 1 : 0;
             if (a->resuspension == 1 || a->resuspension == 3) to_release = to_release || ws >= a->min_wet_steps;
             if ((a->resuspension == 2 || a->resuspension == 3) && rewet &&

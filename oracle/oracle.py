@@ -82,7 +82,7 @@ def lib():
         L.orc_node_xyz.argtypes = [i64, vp, vp, vp]
         L.orc_sample.argtypes = [C.POINTER(OMesh), vp, C.c_int, vp, i64, vp, vp, vp, vp, vp, C.c_int, vp]
         L.orc_normal_pair.argtypes = [C.c_uint64] * 5 + [vp]
-        L.orc_beach.argtypes = [C.POINTER(OMesh), C.c_void_p, vp, i64, vp, vp, vp, vp, vp, vp, vp]
+        L.orc_beach.argtypes = [C.POINTER(OMesh), C.c_void_p, vp, i64, vp, vp, vp, vp, vp, vp, vp, vp, vp]
         L.orc_set_threads.argtypes = [C.c_int]
         L.orc_get_threads.restype = C.c_int
         _lib = L
@@ -332,7 +332,7 @@ RESUSP = {"never": 0, "auto": 1, "stochastic": 2, "auto_or_stochastic": 3}
 
 def beach(state, prev_status, mesh, coastal, wet_streak, *, criteria, depth_min, zone_depth, t_beach,
           resuspension, rewet_hysteresis, min_wet_steps, t_resuspend, seed, real_id, step_i, dt, pid_offset=0,
-          view=None):
+          view=None, eta=None, dry_mask=None):
     """The beaching hook after one step; returns (state dict, wet_streak)."""
     view = view or MeshView(mesh)
     a = OBeach()
@@ -350,8 +350,10 @@ def beach(state, prev_status, mesh, coastal, wet_streak, *, criteria, depth_min,
     cst = np.ascontiguousarray(coastal, np.uint8)
     lon = np.ascontiguousarray(state.lon, np.float64)
     lat = np.ascontiguousarray(state.lat, np.float64)
+    e = None if eta is None else np.ascontiguousarray(eta, np.float64)
+    d = None if dry_mask is None else np.ascontiguousarray(dry_mask, np.float64)
     lib().orc_beach(C.byref(view.s), C.byref(a), _p(cst), lon.size, _p(lon), _p(lat), _p(out["status"]),
-                    _p(prev), _p(out["nearest_node"]), _p(out["failure_reason"]), _p(ws))
+                    _p(prev), _p(out["nearest_node"]), _p(out["failure_reason"]), _p(ws), _p(e), _p(d))
     return out, ws
 
 

@@ -68,7 +68,9 @@ class Golden:
                                             uv_layout=("nemo_cgrid" if "mesh_cgrid_corners" in self.d else
                                                        "element" if self.uv_element else "node"),
                                             uv_vertical=placement if w is not None else "layer",
-                                            az=self.d.get(f"snap{i}_az")))
+                                            az=self.d.get(f"snap{i}_az"),
+                                            scalars={k[len(f"snap{i}_scalar_"):]: self.d[k] for k in self.d
+                                                     if k.startswith(f"snap{i}_scalar_")} or None))
             i += 1
 
     def cases(self):

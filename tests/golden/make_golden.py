@@ -70,7 +70,8 @@ def mesh_record(rm):
 
 def ref_fields(snaps, placement="layer"):
     return [RVel(u=s.u, v=s.v, w=s.w, eta=np.asarray(s.eta), uv_layout="node",
-                 uv_vertical=placement, az=getattr(s, "az", None)) for s in snaps]
+                 uv_vertical=placement, az=getattr(s, "az", None), scalars=getattr(s, "scalars", None))
+            for s in snaps]
 
 
 def payload(fields, t, T):
@@ -176,7 +177,8 @@ def run_beach_case(rm, fields, lon, lat, z, status, dt, T, n_steps, beach, *, kh
     out["beach"] = np.array([int("depth" in c), int("coastal_element" in c), int("stochastic" in c),
                              int("on_failure" in c), _RESUSP_CODES[cfg.resuspension], cfg.min_wet_steps,
                              cfg.depth_min, zone, cfg.rewet_hysteresis, cfg.t_beach or 0.0,
-                             cfg.t_resuspend or 0.0, bseed], dtype=np.float64)
+                             cfg.t_resuspend or 0.0, bseed, int(bool(cfg.use_eta)),
+                             int(bool(cfg.dry_mask_var))], dtype=np.float64)
     n_beached = int((st.status == int(ParticleStatus.BEACHED)).sum())
     print(f"  beach case: {n_beached} beached at the end, {int((wet > 0).sum())} wet streaks")
     return out
@@ -190,6 +192,13 @@ def beach_fixture():
                        depth=lambda lo, la: S.smooth_bathymetry(lo, la, 0.0, 6.0, seed=8))
     rm = ref_mesh(m)
     snaps = S.gyre_snapshots(m, 4, amp=1.5, dtype=np.float64)
+    # a free surface that floods and drains the shelves (use_eta) and a dry
+    # mask scalar (dry_mask_var), both moving between the daily records
+    lo, la = np.asarray(m.nodes_lon), np.asarray(m.nodes_lat)
+    for i, sn in enumerate(snaps):
+        sn.eta = 1.2 * np.sin(np.radians(9.0 * lo + 40.0 * i)) * np.cos(np.radians(7.0 * la - 25.0 * i))
+        dry = ((np.asarray(m.depth) + sn.eta) < 0.9) | (np.sin(np.radians(23.0 * lo + 31.0 * la + 50.0 * i)) > 0.93)
+        sn.scalars = {"dry": dry.astype(np.float64)}
     rf = ref_fields(snaps)
     lon, lat, z, status = particles(m, 1500, 31, n_dead=20)
     cases = {
@@ -207,6 +216,16 @@ def beach_fixture():
                                      kh=(2.0e4, 2.0e4)),
         "depth_never": run_beach_case(rm, rf, lon, lat, z, status, 10800.0, T, 12,
                                       dict(criteria=["depth"], depth_min=2.0), kh=None),
+        "eta_dry_auto": run_beach_case(rm, rf, lon, lat, z, status, 10800.0, T, 16,
+                                       dict(criteria=["depth", "on_failure"], depth_min=1.0, use_eta=True,
+                                            dry_mask_var="dry", resuspension="auto", min_wet_steps=2,
+                                            rewet_hysteresis=0.3)),
+        "eta_sto_both": run_beach_case(rm, rf, lon, lat, z, status, 10800.0, T, 16,
+                                       dict(criteria=["stochastic", "depth"], depth_min=0.8, zone_depth=3.0,
+                                            t_beach=43200.0, use_eta=True, dry_mask_var="dry",
+                                            resuspension="auto_or_stochastic", t_resuspend=21600.0,
+                                            min_wet_steps=2, seed=5),
+                                       real_id=1, pid_offset=300),
     }
     r_boundary(rm)
     save("golden_beach", mesh_record(rm), snaps, cases,
@@ -241,6 +260,8 @@ def save(name, mesh_rec, snaps, cases, parts):
             d[f"snap{i}_az"] = s.az
         if np.any(np.asarray(s.eta) != 0):
             d[f"snap{i}_eta"] = s.eta
+        for k, v in (getattr(s, "scalars", None) or {}).items():
+            d[f"snap{i}_scalar_{k}"] = v
     for k, v in parts.items():
         d[f"p_{k}"] = v
     for cname, c in cases.items():

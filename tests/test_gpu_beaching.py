@@ -7,6 +7,8 @@ device's trig differs from the C library's in the last bits).  Two routes:
 the public per-call API (``integrators.rk2_step`` +
 ``beaching.apply_beaching_hook``, host arrays in and out every step) and the
 device-resident loop (``kc_step`` + ``kc_beach`` with periodic re-sorts).
+Two of the cases read the payload's free surface (``use_eta``) and dry mask
+(``dry_mask_var``), which move between the records.
 """
 import numpy as np
 import pytest
@@ -29,7 +31,7 @@ def _run_cfg(g, c):
                             zone_depth=kw["zone_depth"], t_beach=kw["t_beach"] or None,
                             resuspension=kw["resuspension"], rewet_hysteresis=kw["rewet_hysteresis"],
                             min_wet_steps=kw["min_wet_steps"], t_resuspend=kw["t_resuspend"] or None,
-                            seed=kw["seed"])
+                            seed=kw["seed"], use_eta=kw["use_eta"], dry_mask_var=kw["dry_mask_var"])
     return KB.make_run_config(cfg, g.mesh, diffusion_seed=int(seed), particle_offset=int(pid_off))
 
 
@@ -92,6 +94,7 @@ def test_cuda_beaching_resident_loop(golden, cname):
             kick = (khx, khy, int(seed), int(real_id), k, int(pid_off))
         a, _ = KI.prepare_step(vel, g.mesh, dt, td, "rk2", kw, ctx, kick=kick)
         ctx.step(a)
+        ctx.beach_surface(*KB.payload_surfaces(vel, run_cfg.cfg))
         ctx.beach(KB.beach_args(run_cfg, int(real_id), k, dt))
         if f"s{k + 1}_status" in c:
             out = ctx.download_particles()

@@ -168,3 +168,24 @@ def test_autotune_picks_a_candidate_and_results_do_not_depend_on_it(tmp_path, mo
     for n in FIELDS:
         np.testing.assert_array_equal(outs[0][n], outs[1][n], err_msg=n)
     ctx.close()
+
+
+def test_fused_refuses_per_step_beaching_surfaces():
+    """A beaching surface (kc_beach_surface) belongs to one step: a fused
+    launch over several steps refuses the hook while one is set, and runs
+    again once it is cleared."""
+    from kelp_b200.device import DeviceContext
+    w = _workload(4000)
+    ctx = DeviceContext(0)
+    ctx.ensure_mesh(w.mesh)
+    slots = ctx.slots_for(w.snaps)
+    args = [w.step_args(k, slots) for k in range(4)]
+    _start(ctx, w, True)
+    ctx.beach_surface(np.zeros(np.asarray(w.mesh.nodes_lon).size))
+    with pytest.raises(N.KcError, match="per step"):
+        ctx.run_fused(args, beach=[_beach_args(k) for k in range(4)])
+    ctx.beach_surface(None, None)
+    ctx.run_fused(args, beach=[_beach_args(k) for k in range(4)])
+    ctx.synchronize()
+    assert ctx.device_errors() == 0
+    ctx.close()

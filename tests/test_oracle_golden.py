@@ -143,7 +143,7 @@ def test_oracle_node_xyz(golden):
     np.testing.assert_array_equal(O.node_xyz(g.mesh.nodes_lon, g.mesh.nodes_lat), g.mesh._node_xyz)
 
 
-BEACH_CASES = ("dco_auto", "sto_both", "cd_sresusp", "depth_never")
+BEACH_CASES = ("dco_auto", "sto_both", "cd_sresusp", "depth_never", "eta_dry_auto", "eta_sto_both")
 _RESUSP_NAMES = {0: "never", 1: "auto", 2: "stochastic", 3: "auto_or_stochastic"}
 
 
@@ -153,7 +153,15 @@ def beach_kwargs(c):
     crit = [n for n, on in zip(("depth", "coastal_element", "stochastic", "on_failure"), b[:4]) if on]
     return dict(criteria=crit, resuspension=_RESUSP_NAMES[int(b[4])], min_wet_steps=int(b[5]),
                 depth_min=float(b[6]), zone_depth=float(b[7]), rewet_hysteresis=float(b[8]),
-                t_beach=float(b[9]), t_resuspend=float(b[10]), seed=int(b[11]))
+                t_beach=float(b[9]), t_resuspend=float(b[10]), seed=int(b[11]),
+                use_eta=bool(b[12]) if b.size > 12 else False,
+                dry_mask_var="dry" if b.size > 13 and b[13] else None)
+
+
+def beach_surfaces(vel, kw):
+    """The payload's eta and dry mask the hook reads (tracking.py:236-327)."""
+    from kelp_b200.beaching import BeachingConfig, payload_surfaces
+    return payload_surfaces(vel, BeachingConfig(use_eta=kw["use_eta"], dry_mask_var=kw["dry_mask_var"]))
 
 
 def replay_oracle_beach(g, cname):
@@ -174,8 +182,10 @@ def replay_oracle_beach(g, cname):
         out = O.step(st, vel, g.mesh, dt, td, "rk2", vel_next=vnext, dt_to_next=dtn, diffusion=diff, view=view)
         st = st.replace(lon=out["lon"], lat=out["lat"], status=out["status"], nearest_node=out["nearest_node"],
                         failure_reason=out["failure_reason"])
+        eta, dry = beach_surfaces(vel, kw)
+        okw = {k: v for k, v in kw.items() if k not in ("use_eta", "dry_mask_var")}
         res, wet = O.beach(st, prev, g.mesh, g.d["p_coastal"], wet, real_id=int(real_id), step_i=k, dt=dt,
-                           pid_offset=int(pid_off), view=view, **kw)
+                           pid_offset=int(pid_off), view=view, eta=eta, dry_mask=dry, **okw)
         st = st.replace(**res)
         if f"s{k + 1}_status" in c:
             snaps[k + 1] = {"lon": st.lon, "lat": st.lat, "status": st.status, "nearest_node": st.nearest_node,
