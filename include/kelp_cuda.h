@@ -40,6 +40,8 @@
  *   kc_rng_normals     <- numerics.diffusion._normal_pair (src/kelp/numerics/diffusion.py:233)
  *   kc_sample_field    <- numerics.sampling.sample_field (src/kelp/numerics/sampling.py:727)
  *   kc_beach_surface   <- the vel.eta / vel.scalars[dry_mask_var] reads of tracking._apply_beaching_hook
+ *   kc_grid_cell_stats <- core.mesh._gh_sample_stats, the per-sample kernel of the occupancy cell rule
+ *                         choose_grid_hash_cell (src/kelp/core/mesh.py:384-461, :464-616)
  *                         (src/kelp/tracking.py:236-327)
  */
 #ifndef KELP_CUDA_H
@@ -49,7 +51,7 @@
 extern "C" {
 #endif
 
-#define KC_ABI_VERSION 13
+#define KC_ABI_VERSION 14
 
 #define KC_OK 0
 #define KC_ERR_ARG 1      /* invalid argument or combination */
@@ -413,6 +415,25 @@ int kc_rng_normals(kc_ctx* ctx, long long P, unsigned long long seed, unsigned l
  * the host build bit for bit. */
 int kc_grid_hash_build(kc_ctx* ctx, long long n_nodes, const double* lon, const double* lat, double cell_size,
                        double lon_min, double lat_min, int nx, int ny, int wrap, int* offsets, int* node_ids);
+
+/* One candidate cell of the grid-hash occupancy rule at P sample points
+ * (host arrays; src/kelp/core/mesh.py:384-461 _gh_sample_stats, run by
+ * choose_grid_hash_cell :464-616 for each cell of its ladder).  The node
+ * counts of the candidate grid (cell_size, lon_min, lat_min, nx, ny, wrap:
+ * the geometry the host derived for it; lon_branch (n_nodes) the node
+ * longitudes in the branch the host chose, the resident mesh's latitudes)
+ * and their 2-D prefix table are built on the device.  For every sample:
+ * nn (P) its exact nearest node on the resident mesh's own grid hash
+ * (-1 only on an empty grid; the other outputs are then 0), occ the nodes
+ * in its candidate 3x3 window, approx 1 where that node lies outside the
+ * window, unprov 1 where the 3x3 certificate does not prove it (an empty
+ * window, an outside node, or a failed coverage test), and cost the exact
+ * search's scan-cost proxy (nodes scanned + cells visited + 20 per
+ * certificate evaluation).  KC_ERR_ARG when n_nodes is not the resident
+ * mesh's or the grid has more than 2e9 cells. */
+int kc_grid_cell_stats(kc_ctx* ctx, long long n_nodes, const double* lon_branch, double cell_size, double lon_min,
+                       double lat_min, int nx, int ny, int wrap, long long P, const double* lon, const double* lat,
+                       int* nn, int* occ, double* cost, signed char* unprov, signed char* approx);
 
 /* Digests of the Box-Muller draws over their whole input domain, for
  * checking the device arithmetic against the reference's: for every 32-bit

@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libkelpcuda
 KC_OK, KC_ERR_ARG, KC_ERR_CUDA, KC_ERR_STATE, KC_ERR_DEVICE = 0, 1, 2, 3, 4
 KC_F32, KC_F64, KC_F16 = 0, 1, 2
 KC_PLAIN, KC_MIXED = 0, 1
-ABI_VERSION = 13
+ABI_VERSION = 14
 KC_EULER, KC_RK2, KC_RK4 = 0, 1, 2
 
 #: every symbol include/kelp_cuda.h declares
@@ -27,7 +27,7 @@ EXPORTS = ("kc_abi_version", "kc_node_xyz_fill", "kc_create", "kc_destroy", "kc_
            "kc_beach_state_download", "kc_beach", "kc_step", "kc_step_host", "kc_step_range", "kc_run_fused",
            "kc_particles_set_realization", "kc_elem_neighbors_upload", "kc_elem_centers_upload", "kc_field_upload_async", "kc_particles_set_elem",
            "kc_particles_get_elem", "kc_find_elements_walk", "kc_find_elements", "kc_sigma_upload", "kc_field_upload_eta", "kc_cgrid_upload",
-           "kc_set_fused_block", "kc_run", "kc_sort", "kc_find_nearest", "kc_find_nearest_noalloc", "kc_rng_normals", "kc_rng_domain_digests", "kc_grid_hash_build", "kc_sample_field", "kc_beach_surface",
+           "kc_set_fused_block", "kc_run", "kc_sort", "kc_find_nearest", "kc_find_nearest_noalloc", "kc_rng_normals", "kc_rng_domain_digests", "kc_grid_hash_build", "kc_grid_cell_stats", "kc_sample_field", "kc_beach_surface",
            "kc_device_errors",
            "kc_event_record", "kc_event_elapsed", "kc_l2_flush", "kc_host_alloc", "kc_host_free")
 
@@ -163,6 +163,8 @@ def lib():
                                      C.c_ulonglong, vp]
         L.kc_rng_domain_digests.argtypes = [vp, i, vp]
         L.kc_grid_hash_build.argtypes = [vp, ll, vp, vp, C.c_double, C.c_double, C.c_double, i, i, i, vp, vp]
+        L.kc_grid_cell_stats.argtypes = [vp, ll, vp, C.c_double, C.c_double, C.c_double, i, i, i, ll, vp, vp, vp, vp,
+                                         vp, vp, vp]
         L.kc_device_errors.argtypes = [vp, C.POINTER(i)]
         L.kc_event_record.argtypes = [vp, i]
         L.kc_event_elapsed.argtypes = [vp, i, i, C.POINTER(C.c_float)]

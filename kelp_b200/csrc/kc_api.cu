@@ -14,6 +14,7 @@
 #include <cuda_fp16.h>
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
+#include <cub/block/block_scan.cuh>
 
 #include "../../include/kelp_cuda.h"
 #include "kc_host.h"
@@ -336,6 +337,151 @@ __global__ void __launch_bounds__(kBlock) k_hash_cells(const double* lon, const 
     key[n] = k;
     val[n] = (int)n;
     atomicAdd(&counts[k], 1);
+}
+
+// ---------------------------------------------------------------------------
+// The occupancy rule's per-sample statistics of one candidate cell
+// (mesh.py:384-461 _gh_sample_stats).  cum is the (ny + 1) x (nx + 1) 2-D
+// prefix table of the candidate grid's node counts: cum[j][i] = nodes in rows
+// < j and columns < i.
+// ---------------------------------------------------------------------------
+
+// The candidate cell of every node (the cell rule of k_hash_cells), counted
+// into cum[cj + 1][ci + 1] before the prefix passes.
+__global__ void __launch_bounds__(kBlock) k_cell_counts(const double* lon, const double2* ll, long long N, double cell,
+                                                        double lon_min, double lat_min, int nx, int ny, int wrap,
+                                                        int* cum) {
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    int ci = wrap ? (int)(lon[n] / cell) : (int)((lon[n] - lon_min) / cell);
+    if (wrap) {
+        if (ci > nx - 1) ci = nx - 1;
+    } else {
+        ci = ci < 0 ? 0 : (ci > nx - 1 ? nx - 1 : ci);
+    }
+    int cj = (int)((ll[n].y - lat_min) / cell);
+    cj = cj < 0 ? 0 : (cj > ny - 1 ? ny - 1 : cj);
+    atomicAdd(&cum[(long long)(cj + 1) * (nx + 1) + ci + 1], 1);
+}
+
+// Running sums along each row j = 1..ny of cum (one block per row, the row
+// scanned in tiles of the block with a carry between them).
+constexpr int kScanBlock = 256;
+__global__ void __launch_bounds__(kScanBlock) k_prefix_rows(int* cum, int nx) {
+    using Scan = cub::BlockScan<int, kScanBlock>;
+    __shared__ typename Scan::TempStorage tmp;
+    __shared__ int carry;
+    int* row = cum + (long long)(blockIdx.x + 1) * (nx + 1);
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 1; base <= nx; base += kScanBlock) {
+        const int i = base + (int)threadIdx.x;
+        const int v = i <= nx ? row[i] : 0;
+        int incl, total;
+        Scan(tmp).InclusiveSum(v, incl, total);
+        if (i <= nx) row[i] = incl + carry;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += total;
+        __syncthreads();
+    }
+}
+
+// Running sums down each column i = 1..nx (adjacent threads read adjacent
+// columns of a row).
+__global__ void __launch_bounds__(kBlock) k_prefix_cols(int* cum, int nx, int ny) {
+    const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x) + 1;
+    if (i > nx) return;
+    int acc = 0;
+    for (int j = 1; j <= ny; ++j) {
+        const long long k = (long long)j * (nx + 1) + i;
+        acc += cum[k];
+        cum[k] = acc;
+    }
+}
+
+// mesh.py:353-380 _gh_rect_sum: the nodes of the cells ci-rx..ci+rx x
+// cj-ry..cj+ry, rows clipped, columns wrapped on a cyclic grid (one or two
+// slices) and clipped otherwise.
+__device__ __forceinline__ int rect_nodes(const int* cum, int nx, int ny, int wrap, int ci, int cj, int rx, int ry) {
+    const long long W = nx + 1;
+    const int j0 = cj - ry < 0 ? 0 : cj - ry;
+    const int j1 = cj + ry + 1 > ny ? ny : cj + ry + 1;
+    auto span = [&](int a, int b) {   // columns [a, b) of rows [j0, j1)
+        return (cum[j1 * W + b] - cum[j0 * W + b]) - (cum[j1 * W + a] - cum[j0 * W + a]);
+    };
+    if (wrap && 2 * rx + 1 >= nx) return span(0, nx);
+    int i0 = ci - rx, i1 = ci + rx + 1;
+    if (wrap) {
+        if (i0 < 0) return span(0, i1) + span(i0 + nx, nx);
+        if (i1 > nx) return span(i0, nx) + span(0, i1 - nx);
+    } else {
+        if (i0 < 0) i0 = 0;
+        if (i1 > nx) i1 = nx;
+    }
+    return span(i0, i1);
+}
+
+// Per sample: its exact nearest node on the resident hash (mr), then the 3x3
+// occupancy, the outside-window flag, the certificate's verdict and the
+// scan-cost proxy on the candidate grid (mc: the resident mesh's node tables
+// with the candidate geometry).  Cost weights: a cell visit 1, a certificate
+// evaluation 20 (mesh.py:348-349).
+__global__ void __launch_bounds__(kBlock) k_cell_stats(const __grid_constant__ kc::DMesh mr,
+                                                       const __grid_constant__ kc::DMesh mc, const int* cum,
+                                                       const double* q, long long P, int* nn_out, int* occ_out,
+                                                       double* cost_out, signed char* unprov_out,
+                                                       signed char* approx_out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P) return;
+    const double lon = q[i], lat = q[P + i];
+    const kc::Site s = kc::make_site(lon, lat);
+    const int n = kc::nearest_exact(mr, s);
+    nn_out[i] = n;
+    if (n < 0) {
+        occ_out[i] = 0; cost_out[i] = 0.0; unprov_out[i] = 0; approx_out[i] = 0;
+        return;
+    }
+    int ci, cj, cin, cjn;
+    kc::gh_cell_of(mc, lon, lat, ci, cj);
+    const int occ = rect_nodes(cum, mc.nx, mc.ny, mc.wrap, ci, cj, 1, 1);
+    occ_out[i] = occ;
+    const double2 nl = __ldg(&mc.ll[n]);
+    kc::gh_cell_of(mc, nl.x, nl.y, cin, cjn);
+    int di = abs(cin - ci);
+    if (mc.wrap && mc.nx - di < di) di = mc.nx - di;
+    const int dj = abs(cjn - cj);
+    const int approx = (di > 1 || dj > 1) ? 1 : 0;
+    approx_out[i] = (signed char)approx;
+    double theta, ext;
+    kc::cap_extents(mc, s, n, theta, ext);
+    const bool provable = occ > 0 && !approx && kc::provable_code(mc, s, 1, 1, theta, ext) == 0;
+    if (provable) {
+        cost_out[i] = (double)occ + 9.0 + 20.0;
+        unprov_out[i] = 0;
+        return;
+    }
+    int ry = (int)ceil(theta / mc.cell);
+    if (ry < 1) ry = 1;
+    if (ry > mc.ny) ry = mc.ny;
+    int rx;
+    if (ext >= 1.0e29) {
+        rx = mc.nx;
+    } else {
+        rx = (int)ceil(ext / mc.cell);
+        if (rx < 1) rx = 1;
+    }
+    long long cells, iters;
+    if (rx * 2LL + 1 >= mc.nx) {
+        rx = mc.nx;
+        cells = 9 + 2LL * ry;
+        iters = ry;
+    } else {
+        cells = 9 + (long long)rx * (2LL * ry + 1) + 2LL * ry;
+        iters = rx > ry ? rx : ry;
+    }
+    cost_out[i] = ((double)rect_nodes(cum, mc.nx, mc.ny, mc.wrap, ci, cj, rx, ry) + (double)cells) +
+                  (double)(iters + 1) * 20.0;
+    unprov_out[i] = 1;
 }
 
 __global__ void __launch_bounds__(kBlock) k_beach(const __grid_constant__ kc::DMesh m,
@@ -2278,6 +2424,67 @@ int kc_grid_hash_build(kc_ctx* c, long long n_nodes, const double* lon, const do
     for (void* p : {(void*)dlon, (void*)dlat, (void*)k0, (void*)k1, (void*)v0, (void*)v1, (void*)cnt, (void*)off, tmp})
         if (p) cudaFreeAsync(p, s);
     if (e != cudaSuccess) return fail(c, KC_ERR_CUDA, std::string("kc_grid_hash_build: ") + cudaGetErrorString(e));
+    KC_CUDA(c, cudaStreamSynchronize(s));
+    return KC_OK;
+}
+
+int kc_grid_cell_stats(kc_ctx* c, long long n_nodes, const double* lon_branch, double cell_size, double lon_min,
+                       double lat_min, int nx, int ny, int wrap, long long P, const double* lon, const double* lat,
+                       int* nn, int* occ, double* cost, signed char* unprov, signed char* approx) {
+    if (!c) return KC_ERR_ARG;
+    if (!c->has_mesh) return fail(c, KC_ERR_STATE, "kc_grid_cell_stats: no mesh uploaded");
+    if (n_nodes != c->N || !lon_branch) return fail(c, KC_ERR_ARG, "kc_grid_cell_stats: node longitudes");
+    if (!(cell_size > 0.0) || nx <= 0 || ny <= 0 || (long long)nx * ny > 2000000000LL)
+        return fail(c, KC_ERR_ARG, "kc_grid_cell_stats: grid geometry");
+    if (P < 0 || (P > 0 && (!lon || !lat || !nn || !occ || !cost || !unprov || !approx)))
+        return fail(c, KC_ERR_ARG, "kc_grid_cell_stats: sample arrays");
+    if (P == 0) return KC_OK;
+    KC_CUDA(c, cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    const long long N = n_nodes, T = (long long)(nx + 1) * (ny + 1);
+    double *dlon = nullptr, *dq = nullptr, *dcost = nullptr;
+    int *cum = nullptr, *dnn = nullptr, *docc = nullptr;
+    signed char *dun = nullptr, *dap = nullptr;
+    cudaError_t e = cudaSuccess;
+    auto ok = [&](cudaError_t r) { if (e == cudaSuccess) e = r; return e == cudaSuccess; };
+    ok(cudaMallocAsync((void**)&dlon, N * 8, s));
+    ok(cudaMallocAsync((void**)&cum, T * 4, s));
+    ok(cudaMallocAsync((void**)&dq, P * 16, s));
+    ok(cudaMallocAsync((void**)&dnn, P * 4, s));
+    ok(cudaMallocAsync((void**)&docc, P * 4, s));
+    ok(cudaMallocAsync((void**)&dcost, P * 8, s));
+    ok(cudaMallocAsync((void**)&dun, P, s));
+    ok(cudaMallocAsync((void**)&dap, P, s));
+    ok(cudaMemcpyAsync(dlon, lon_branch, N * 8, cudaMemcpyHostToDevice, s));
+    ok(cudaMemcpyAsync(dq, lon, P * 8, cudaMemcpyHostToDevice, s));
+    ok(cudaMemcpyAsync(dq + P, lat, P * 8, cudaMemcpyHostToDevice, s));
+    ok(cudaMemsetAsync(cum, 0, T * 4, s));
+    if (e == cudaSuccess) {
+        k_cell_counts<<<grid_for(N), kBlock, 0, s>>>(dlon, c->dm.ll, N, cell_size, lon_min, lat_min, nx, ny, wrap, cum);
+        ok(cudaGetLastError());
+    }
+    if (e == cudaSuccess) {
+        k_prefix_rows<<<(unsigned)ny, kScanBlock, 0, s>>>(cum, nx);
+        ok(cudaGetLastError());
+    }
+    if (e == cudaSuccess) {
+        k_prefix_cols<<<grid_for(nx), kBlock, 0, s>>>(cum, nx, ny);
+        ok(cudaGetLastError());
+    }
+    if (e == cudaSuccess) {
+        kc::DMesh mr = c->dm, mc = c->dm;
+        mc.cell = cell_size; mc.lon_min = lon_min; mc.lat_min = lat_min; mc.nx = nx; mc.ny = ny; mc.wrap = wrap ? 1 : 0;
+        k_cell_stats<<<grid_for(P), kBlock, 0, s>>>(mr, mc, cum, dq, P, dnn, docc, dcost, dun, dap);
+        ok(cudaGetLastError());
+    }
+    ok(cudaMemcpyAsync(nn, dnn, P * 4, cudaMemcpyDeviceToHost, s));
+    ok(cudaMemcpyAsync(occ, docc, P * 4, cudaMemcpyDeviceToHost, s));
+    ok(cudaMemcpyAsync(cost, dcost, P * 8, cudaMemcpyDeviceToHost, s));
+    ok(cudaMemcpyAsync(unprov, dun, P, cudaMemcpyDeviceToHost, s));
+    ok(cudaMemcpyAsync(approx, dap, P, cudaMemcpyDeviceToHost, s));
+    for (void* p : {(void*)dlon, (void*)cum, (void*)dq, (void*)dnn, (void*)docc, (void*)dcost, (void*)dun, (void*)dap})
+        if (p) cudaFreeAsync(p, s);
+    if (e != cudaSuccess) return fail(c, KC_ERR_CUDA, std::string("kc_grid_cell_stats: ") + cudaGetErrorString(e));
     KC_CUDA(c, cudaStreamSynchronize(s));
     return KC_OK;
 }

@@ -560,6 +560,24 @@ class DeviceContext:
                                              N.ptr(off), N.ptr(ids)), "kc_grid_hash_build")
         return off, ids
 
+    def grid_cell_stats(self, lon_branch, cell_size, lon_min, lat_min, nx, ny, wrap, lon, lat):
+        """Per-sample statistics of one candidate grid-hash cell on the
+        resident mesh (kc_grid_cell_stats): (nn, occ, cost, unprov, approx)."""
+        lb = _c(lon_branch, np.float64)
+        lon = _c(lon, np.float64)
+        lat = _c(lat, np.float64)
+        P = lon.size
+        nn = np.empty(P, np.int32)
+        occ = np.empty(P, np.int32)
+        cost = np.empty(P, np.float64)
+        unprov = np.empty(P, np.int8)
+        approx = np.empty(P, np.int8)
+        self._chk(N.lib().kc_grid_cell_stats(self._ctx, lb.size, N.ptr(lb), float(cell_size), float(lon_min),
+                                             float(lat_min), int(nx), int(ny), int(bool(wrap)), P, N.ptr(lon),
+                                             N.ptr(lat), N.ptr(nn), N.ptr(occ), N.ptr(cost), N.ptr(unprov),
+                                             N.ptr(approx)), "kc_grid_cell_stats")
+        return nn, occ, cost, unprov, approx
+
     def rng_domain_digests(self, corrected: bool = True) -> tuple:
         """Digests of r, cos and sin of the Box-Muller draws over all 2^32
         uniforms (kc_rng_domain_digests)."""

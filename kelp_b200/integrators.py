@@ -80,6 +80,16 @@ def _fields(vel, vel_next):
     return vel_a, vel_b, target, alpha0
 
 
+def _materialized(vel):
+    """A LazyLerpField as the plain field its own blend makes of it (every
+    array the payload carries, blended by the payload itself), for the paths
+    where the reference steps the materialised field."""
+    from .fields import VelocityField
+    return VelocityField(u=np.asarray(vel.u), v=np.asarray(vel.v), eta=np.asarray(vel.eta), w=vel.w,
+                         uv_layout=vel.uv_layout, uv_vertical=getattr(vel, "uv_vertical", "layer"),
+                         az=getattr(vel, "az", None), scalars=getattr(vel, "scalars", None))
+
+
 def _check_node_fields(mesh, fields, is3d, placement="layer"):
     n = mesh.nodes_lon.shape[0]
     for f in fields:
@@ -310,10 +320,11 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
             raise NotImplementedError(f"w_interp={w_interp!r} is not built on the CUDA backend")
         w_code = 0 if w_interp == "nearest" else 1
         if code == N.KC_RK2 and hasattr(vel, "vel_a") and float(getattr(vel, "alpha", 1.0)) == 0.0:
-            # integrators.py:5691-5692 routes this exotic payload to the
-            # unfused RK2, whose 0 * vel_b blend propagates non-finite values
-            raise NotImplementedError("an endpoint LazyLerpField (alpha 0) takes the reference's unfused "
-                                      "3-D RK2 path, which is not built on the CUDA backend")
+            # integrators.py:5691-5692 routes an endpoint LazyLerpField to the
+            # unfused RK2 (:5380-5608): its stage fields are the payload
+            # materialised, 1.0 a + 0.0 b, and its stage arithmetic is the
+            # fused RK2's, so the fused kernel steps the materialised field
+            vel = _materialized(vel)
     vel_a, vel_b, target, alpha0 = _fields(vel, vel_next)
     if lsq:
         _check_element_fields(mesh, [vel_a, vel_b, target] + (list(recon[0]) if recon is not None else []))

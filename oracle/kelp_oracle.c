@@ -1985,6 +1985,80 @@ int orc_find_nearest(const orc_mesh* mm, int64_t P, const double* lon, const dou
     return 0;
 }
 
+/* mesh.py:353-380 _gh_rect_sum over the (ny+1) x (nx+1) prefix table cum */
+static int64_t rect_sum(const int32_t* cum, int nx, int ny, int wrap, int ci, int cj, int rx, int ry) {
+    int64_t W = nx + 1;
+    int j0 = cj - ry < 0 ? 0 : cj - ry;
+    int j1 = cj + ry + 1 > ny ? ny : cj + ry + 1;
+#define CUM(j, i) ((int64_t)cum[(int64_t)(j) * W + (i)])
+    if (wrap && 2 * rx + 1 >= nx) return CUM(j1, nx) - CUM(j0, nx);
+    int i0 = ci - rx, i1 = ci + rx + 1;
+    if (wrap) {
+        if (i0 < 0)
+            return (CUM(j1, i1) - CUM(j0, i1)) + (CUM(j1, nx) - CUM(j0, nx)) - (CUM(j1, i0 + nx) - CUM(j0, i0 + nx));
+        if (i1 > nx)
+            return (CUM(j1, nx) - CUM(j0, nx)) - (CUM(j1, i0) - CUM(j0, i0)) + (CUM(j1, i1 - nx) - CUM(j0, i1 - nx));
+    } else {
+        if (i0 < 0) i0 = 0;
+        if (i1 > nx) i1 = nx;
+    }
+    return (CUM(j1, i1) - CUM(j0, i1)) - (CUM(j1, i0) - CUM(j0, i0));
+#undef CUM
+}
+
+/* mesh.py:384-461 _gh_sample_stats for one candidate grid (cell, lon_min,
+ * lat_min, nx, ny, wrap over the mesh's nodes; cum its prefix table) at P
+ * samples with their nearest nodes nn.  Serial: a test-size checker. */
+int orc_cell_stats(const orc_mesh* mm, const int32_t* cum, double cell, double lon_min, double lat_min, int nx,
+                   int ny, int wrap, int64_t P, const double* lon, const double* lat, const int32_t* nn,
+                   int64_t* occ_out, double* cost_out, int8_t* unprov_out, int8_t* approx_out) {
+    OMesh g = *(const OMesh*)mm;
+    g.cell = cell; g.lon_min = lon_min; g.lat_min = lat_min; g.nx = nx; g.ny = ny; g.wrap = wrap;
+    for (int64_t i = 0; i < P; ++i) {
+        int ci, cj, cin, cjn;
+        cell_of(&g, lon[i], lat[i], &ci, &cj);
+        int64_t occ = rect_sum(cum, nx, ny, wrap, ci, cj, 1, 1);
+        occ_out[i] = occ;
+        cell_of(&g, g.lon[nn[i]], g.lat[nn[i]], &cin, &cjn);
+        int di = cin - ci < 0 ? ci - cin : cin - ci;
+        if (wrap && nx - di < di) di = nx - di;
+        int dj = cjn - cj < 0 ? cj - cjn : cjn - cj;
+        approx_out[i] = (di > 1 || dj > 1) ? 1 : 0;
+        double theta, ext;
+        cap_extents(lon[i], lat[i], g.lon[nn[i]], g.lat[nn[i]], &theta, &ext);
+        int provable = occ > 0 && approx_out[i] == 0;
+        if (provable) provable = provable_rect(&g, lon[i], lat[i], nn[i], 1, 1) == 0;
+        if (provable) {
+            cost_out[i] = (double)occ + 9.0 * 1.0 + 20.0;
+            unprov_out[i] = 0;
+            continue;
+        }
+        int ry = (int)ceil(theta / cell);
+        if (ry < 1) ry = 1;
+        if (ry > ny) ry = ny;
+        int rx;
+        if (ext >= 1.0e29) {
+            rx = nx;
+        } else {
+            rx = (int)ceil(ext / cell);
+            if (rx < 1) rx = 1;
+        }
+        int64_t cells, iters;
+        if (rx * 2 + 1 >= nx) {
+            rx = nx;
+            cells = 9 + 2 * (int64_t)ry;
+            iters = ry;
+        } else {
+            cells = 9 + (int64_t)rx * (2 * (int64_t)ry + 1) + 2 * (int64_t)ry;
+            iters = rx > ry ? rx : ry;
+        }
+        cost_out[i] = ((double)rect_sum(cum, nx, ny, wrap, ci, cj, rx, ry) + (double)cells * 1.0) +
+                      (double)(iters + 1) * 20.0;
+        unprov_out[i] = 1;
+    }
+    return 0;
+}
+
 int orc_contain(const orc_mesh* mm, int64_t P, const double* lon, const double* lat, const int* nn, int* out) {
     const OMesh* m = (const OMesh*)mm;
     QCtx c = {m, lon, lat, nn, out};

@@ -78,6 +78,8 @@ def lib():
         L.orc_walk.argtypes = [C.POINTER(OMesh), i64, vp, vp, vp, vp, vp]
         L.orc_find_nearest.argtypes = [C.POINTER(OMesh), i64, vp, vp, vp]
         L.orc_contain.argtypes = [C.POINTER(OMesh), i64, vp, vp, vp, vp]
+        L.orc_cell_stats.argtypes = [C.POINTER(OMesh), vp, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
+                                     C.c_int, i64, vp, vp, vp, vp, vp, vp, vp]
         L.orc_normals.argtypes = [i64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, vp]
         L.orc_node_xyz.argtypes = [i64, vp, vp, vp]
         L.orc_sample.argtypes = [C.POINTER(OMesh), vp, C.c_int, vp, i64, vp, vp, vp, vp, vp, C.c_int, vp]
@@ -377,6 +379,25 @@ def find_nearest(mesh, lon, lat, view=None) -> np.ndarray:
     out = np.empty(lon.size, np.int32)
     lib().orc_find_nearest(C.byref(view.s), lon.size, _p(lon), _p(lat), _p(out))
     return out
+
+
+def cell_stats(mesh, cum, cell, lon_min, lat_min, nx, ny, wrap, lon, lat, nn, view=None):
+    """mesh.py:384-461 _gh_sample_stats of one candidate grid: (occ, cost,
+    unprov, approx) of every sample, cum the candidate's (ny+1, nx+1) prefix
+    table of node counts."""
+    view = view or MeshView(mesh)
+    cum = np.ascontiguousarray(cum, dtype=np.int32)
+    lon = np.ascontiguousarray(lon, dtype=np.float64)
+    lat = np.ascontiguousarray(lat, dtype=np.float64)
+    nn = np.ascontiguousarray(nn, dtype=np.int32)
+    P = lon.size
+    occ = np.empty(P, np.int64)
+    cost = np.empty(P, np.float64)
+    unprov = np.empty(P, np.int8)
+    approx = np.empty(P, np.int8)
+    lib().orc_cell_stats(C.byref(view.s), _p(cum), float(cell), float(lon_min), float(lat_min), int(nx), int(ny),
+                         int(bool(wrap)), P, _p(lon), _p(lat), _p(nn), _p(occ), _p(cost), _p(unprov), _p(approx))
+    return occ, cost, unprov, approx
 
 
 def contain(mesh, lon, lat, nn, view=None) -> np.ndarray:

@@ -865,6 +865,117 @@ def sample_fixture():
         print(f"golden_sample_{name}", os.path.getsize(path) // 1024, "KB")
 
 
+def lazy0_fixture():
+    """integrators.py:5691-5692 -> :5380-5608: a 3-D RK2 step whose payload is
+    an endpoint LazyLerpField (alpha 0) takes the reference's unfused RK2,
+    which materialises the payload as 1.0 a + 0.0 b.  On the 3-D z-level
+    mesh of golden_3d, each step's payload is LazyLerpField(record ia,
+    record ia + 1, 0.0) with record ia + 1 as vel_next: W barycentric, and W
+    nearest with the split kick.  (With a non-finite b the reference's
+    unfused step raises inside find_nearest_nodes once a NaN position
+    reaches it, so only finite records are recorded.)
+    tests/golden/golden_lazy0.npz."""
+    T = 86400.0
+    zl = S.stretched_levels(12, 5.0, 4000.0)
+    m = S.lattice_mesh(3.0, 60.0, jitter=0.2, land_frac=0.25,
+                       depth=lambda lo, la: S.smooth_bathymetry(lo, la, 30.0, 4000.0), sigma=zl)
+    rm = ref_mesh(m, sigma=zl)
+    snaps = S.gyre_snapshots(m, 4, amp=1.5, z_levels=zl, decay=800.0, w_scale=2e-3)
+    rf = ref_fields(snaps)
+    lon, lat, z, status = particles(m, 1200, 43, z=True, n_dead=20)
+
+    def run(w_interp, kh, n_steps=10, dt=21600.0, seed=5):
+        P = lon.size
+        st = RState(lon=lon.copy(), lat=lat.copy(), z=z.copy(), status=status.copy(),
+                    nearest_node=np.full(P, -1, np.int32), failure_reason=np.zeros(P, np.int8))
+        out = {}
+        for k in range(n_steps):
+            t = k * dt
+            ia = int(np.floor(t / T + 1e-9))
+            kw = dict(uv_interp="barycentric", w_interp=w_interp, vel_next=rf[ia + 1], dt_to_next=(ia + 1) * T - t)
+            if kh is not None:
+                kw["diffusion"] = RDiff(scheme="uniform", kh_x=kh, kh_y=kh, seed=seed, real_id=0, step_i=k)
+            st = RI.rk2_step(st, RLazy(rf[ia], rf[ia + 1], 0.0), rm, dt, 1.0, **kw)
+        for name in ("lon", "lat", "z", "status", "nearest_node", "failure_reason", "u", "v", "w"):
+            out[f"s{n_steps}_{name}"] = np.asarray(getattr(st, name))
+        out["params"] = np.array([dt, T, n_steps, 1.0, -1 if kh is None else kh, -1 if kh is None else kh, seed],
+                                 dtype=np.float64)
+        return out
+
+    cases = {"rk2_wbary": run("barycentric", None), "rk2_wnear_kick": run("nearest", 3.0e4)}
+    save("golden_lazy0", mesh_record(rm), snaps, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
+    for c, o in cases.items():
+        print(c, "statuses", np.bincount(o["s10_status"]), "failure reasons", np.bincount(o["s10_failure_reason"]))
+
+
+def cellrule_fixture():
+    """mesh.py:464-616 choose_grid_hash_cell, the reference's own reports in
+    both modes, and its per-sample kernel _gh_sample_stats (:384-461) at a few
+    candidates of the ladder: a seam-wrapping global band, a regional mesh
+    whose node density varies by two orders of magnitude (a sinh-stretched
+    lattice: exact mode leaves the reader's cell there), and a near-polar
+    mesh whose caps reach the pole.  The band and the polar mesh are sampled
+    (sample < E: the seeded draw), the stretched mesh uses every element
+    centre.
+    tests/golden/golden_cellrule_*.npz."""
+    import json
+    from kelp.core import mesh as RM
+    from kelp_b200.mesh import make_mesh
+
+    def stretched():
+        b = S.lattice_mesh(0.5, 20.0, lon_min=-30.0, lon_max=30.0, jitter=0.2, land_frac=0.1)
+        lon = 30.0 * np.sinh(np.asarray(b.nodes_lon) / 5.0) / np.sinh(6.0)
+        lat = 20.0 * np.sinh(np.asarray(b.nodes_lat) / 4.0) / np.sinh(5.0)
+        return make_mesh("stretched", lon, lat, np.asarray(b.depth), np.asarray(b.elem_nodes))
+
+    meshes = {"band": (S.lattice_mesh(2.0, 75.0, jitter=0.25, land_frac=0.3), 5000),
+              "stretched": (stretched(), 200_000),
+              "polar": (S.lattice_mesh(1.5, 88.5, jitter=0.3, land_frac=0.2), 20_000)}
+    for name, (m, sample) in meshes.items():
+        rm = ref_mesh(m)
+        reps = {mode: RM.choose_grid_hash_cell(rm, exact=(mode == "exact"), sample=sample)[1]
+                for mode in ("exact", "approx")}
+        d = {f"mesh_{k}": v for k, v in mesh_record(rm).items()}
+        d["mesh_elem_center_lon"] = np.asarray(rm.elem_center_lon)
+        d["mesh_elem_center_lat"] = np.asarray(rm.elem_center_lat)
+        d["sample"] = np.array(sample)
+        for mode, rep in reps.items():
+            d[f"report_{mode}"] = np.array(json.dumps(rep))
+        # per-sample statistics of three candidates (the chooser's sample, all finite here)
+        E = rm.n_elements
+        pick = np.sort(np.random.default_rng(0).choice(E, sample, replace=False)) if E > sample else np.arange(E)
+        qlon = np.ascontiguousarray(rm.elem_center_lon[pick], dtype=np.float64)
+        qlat = np.ascontiguousarray(rm.elem_center_lat[pick], dtype=np.float64)
+        nn = np.empty(qlon.size, dtype=np.int32)
+        RM._grid_hash_nearest_batch(qlon.size, qlon, qlat, rm._gh_offsets, rm._gh_node_ids, rm._gh_cell_size,
+                                    rm._gh_lon_min, rm._gh_lat_min, rm._gh_nx, rm._gh_ny, rm._gh_wrap_lon,
+                                    rm.nodes_lon, rm.nodes_lat, RM._require_node_xyz(rm), nn, True,
+                                    int(rm._gh_far_rows))
+        d.update(qlon=qlon, qlat=qlat, nn=nn)
+        lon_b, wrap = RM._gh_lon_branch(rm.nodes_lon)
+        for k in (0, 2, 5):
+            cell = float(rm._gh_cell_size) / (np.sqrt(2.0) ** k)
+            lon_min, lat_min, nx, ny = RM._gh_grid_geometry(lon_b, rm.nodes_lat, cell, wrap)
+            idx = RM._gh_cell_index(lon_b, rm.nodes_lat, cell, lon_min, lat_min, nx, ny, wrap)
+            counts = np.bincount(idx, minlength=nx * ny).reshape(ny, nx)
+            cum = np.zeros((ny + 1, nx + 1), dtype=np.int32)
+            np.cumsum(counts, axis=0, dtype=np.int32, out=cum[1:, 1:])
+            np.cumsum(cum[1:, 1:], axis=1, dtype=np.int32, out=cum[1:, 1:])
+            occ = np.empty(qlon.size, np.int64)
+            cost = np.empty(qlon.size, np.float64)
+            unprov = np.empty(qlon.size, np.int8)
+            approx = np.empty(qlon.size, np.int8)
+            RM._gh_sample_stats(qlon, qlat, nn, np.ascontiguousarray(rm.nodes_lon), np.ascontiguousarray(rm.nodes_lat),
+                                cum, cell, float(lon_min), float(lat_min), int(nx), int(ny), bool(wrap),
+                                occ, cost, unprov, approx)
+            d[f"k{k}_geom"] = np.array([cell, lon_min, lat_min, nx, ny, int(wrap)], dtype=np.float64)
+            d.update({f"k{k}_occ": occ, f"k{k}_cost": cost, f"k{k}_unprov": unprov, f"k{k}_approx": approx})
+        path = os.path.join(HERE, f"golden_cellrule_{name}.npz")
+        np.savez_compressed(path, **d)
+        print(f"golden_cellrule_{name}", os.path.getsize(path) // 1024, "KB",
+              {m_: (r["chosen"], r["legacy"], len(r["candidates"])) for m_, r in reps.items()})
+
+
 def rng1m_fixture():
     """The reference's own _normal_pair on 4 x 2^20 keys (contiguous particle
     ids under 4 key tuples), stored as per-chunk digests (tests/golden/
@@ -922,13 +1033,17 @@ def reftypes_fixture():
 
 if __name__ == "__main__":
     # no argument: every fixture; otherwise the named ones ("steps", "beach", ...)
-    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq", "rng1m", "tripolar", "reftypes", "sample"}
+    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq", "rng1m", "tripolar", "reftypes", "sample", "cellrule", "lazy0"}
     if "rng1m" in which:
         rng1m_fixture()
     if "reftypes" in which:
         reftypes_fixture()
     if "sample" in which:
         sample_fixture()
+    if "cellrule" in which:
+        cellrule_fixture()
+    if "lazy0" in which:
+        lazy0_fixture()
     if "lsq" in which:
         lsq_fixture()
     if "steps" in which:

@@ -21,7 +21,7 @@ def test_library_exports_every_declared_symbol():
     missing = [s for s in declared if not hasattr(L, s)]
     assert not missing, missing
     assert declared == set(N.EXPORTS)
-    assert L.kc_abi_version() == N.ABI_VERSION == 13
+    assert L.kc_abi_version() == N.ABI_VERSION == 14
 
 
 def test_node_xyz_host_routine_matches_reference_table(golden):
