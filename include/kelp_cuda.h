@@ -40,6 +40,9 @@
  *   kc_rng_normals     <- numerics.diffusion._normal_pair (src/kelp/numerics/diffusion.py:233)
  *   kc_sample_field    <- numerics.sampling.sample_field (src/kelp/numerics/sampling.py:727)
  *   kc_beach_surface   <- the vel.eta / vel.scalars[dry_mask_var] reads of tracking._apply_beaching_hook
+ *   kc_sigma_surfaces  <- the sigma_eta_start / sigma_eta_end arguments of the step functions
+ *                         (src/kelp/numerics/integrators.py:1358-1441; tracking.py:2562-2596)
+ *   kc_sigma_surface_slots <- tracking._eta_at_time (src/kelp/tracking.py:3097-3133) on resident records
  *   kc_grid_cell_stats <- core.mesh._gh_sample_stats, the per-sample kernel of the occupancy cell rule
  *                         choose_grid_hash_cell (src/kelp/core/mesh.py:384-461, :464-616)
  *                         (src/kelp/tracking.py:236-327)
@@ -297,6 +300,28 @@ int kc_beach(kc_ctx* ctx, const kc_beach_args* args);
  * as the payload does ((1 - alpha) a + alpha b).  kc_run_fused refuses a
  * beaching hook while a surface is set (it changes every step). */
 int kc_beach_surface(kc_ctx* ctx, const double* eta, const double* dry_mask);
+
+/* The tracking layer's free surfaces for the following sigma-mesh steps
+ * (sigma_eta_start / sigma_eta_end of integrators.rk2_step / rk4_step /
+ * euler_step, src/kelp/numerics/integrators.py:1358-1441, supplied by
+ * tracking.run_single_realization, src/kelp/tracking.py:2562-2596):
+ * eta_start (N) the surface at the step's start, eta_end (N) at its end, NULL
+ * for the payload's own; steady 1 for a step without a next snapshot or a
+ * PCHIP stencil (its stage surfaces then blend from the start towards the
+ * end surface), else 0.  Copied; used by every sigma step until set again.
+ * KC_ERR_STATE unless the resident mesh is a sigma mesh. */
+int kc_sigma_surfaces(kc_ctx* ctx, const double* eta_start, const double* eta_end, int steady);
+
+/* One of those surfaces (which 0: the step's start, 1: its end) evaluated on
+ * the device from resident snapshot slots, as tracking._eta_at_time does
+ * (src/kelp/tracking.py:3097-3133): kind 1 the eta of slots[0]; 2 the blend
+ * (1 - alpha) eta(slots[0]) + alpha eta(slots[1]); 3 the monotone-cubic
+ * value at time q of the four-record stencil slots[0..3] at times t[0..3]
+ * (temporal_reconstruct.py:87-153); 0 turns that surface off (the payload's
+ * own).  Ordered on the context's stream after pending uploads into those
+ * slots.  steady as kc_sigma_surfaces. */
+int kc_sigma_surface_slots(kc_ctx* ctx, int which, int kind, const int* slots, double alpha, const double* t,
+                           double q, int steady);
 
 /* Host particle arrays of kc_step_host (SoA, P entries each).  Input: lon,
  * lat, status, nearest_node required; z and failure_reason may be NULL

@@ -75,6 +75,9 @@ struct kc_ctx {
     double2* d_nsc = nullptr;
     double2* d_ecos = nullptr;
     float4* d_ebox = nullptr;        // containment prefilter boxes
+    double* d_sig_eta_s = nullptr;   // (N) the tracking layer's sigma surfaces set by kc_sigma_surfaces
+    double* d_sig_eta_e = nullptr;
+    bool sig_s_on = false, sig_e_on = false, sig_steady = false;
     double* d_beach_eta = nullptr;   // (N) beaching surfaces set by kc_beach_surface
     double* d_beach_dry = nullptr;
     bool beach_eta_on = false, beach_dry_on = false;
@@ -211,6 +214,7 @@ kc::DStep step_of(const kc_step_args* a) {
     s.global_step = a->global_step;
     s.az_on = a->az_kick; s.az_field = a->az_field; s.az_const = a->az_const;
     s.Dmin = a->Dmin; s.z0b_min = a->z0b_min; s.alpha_end = a->alpha_end;
+    s.eta_s = nullptr; s.eta_e = nullptr; s.sig_steady = 0;
     return s;
 }
 
@@ -337,6 +341,26 @@ __global__ void __launch_bounds__(kBlock) k_hash_cells(const double* lon, const 
     key[n] = k;
     val[n] = (int)n;
     atomicAdd(&counts[k], 1);
+}
+
+// One of the tracking layer's sigma surfaces from resident records, as
+// tracking.py:3097-3133 _eta_at_time evaluates it: kind 1 a record's own eta,
+// 2 the linear blend of two records (io.py:68-117 _blend), 3 the
+// monotone-cubic value of a four-record stencil at time q
+// (temporal_reconstruct.py:87-153 _pchip_blend4).
+__global__ void __launch_bounds__(kBlock) k_surface(long long N, int kind, const double* e0, const double* e1,
+                                                   const double* e2, const double* e3, double alpha, double t0,
+                                                   double t1, double t2, double t3, double q, double* out) {
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    if (kind == 1) {
+        out[n] = e0[n];
+    } else if (kind == 2) {
+        out[n] = (1.0 - alpha) * e0[n] + alpha * e1[n];
+    } else {
+        const double t[4] = {t0, t1, t2, t3};
+        out[n] = kc::pchip4(e0[n], e1[n], e2[n], e3[n], t, q);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -811,8 +835,12 @@ int launch_step_on(kc_ctx* c, const kc_step_args* a, const kc::DState& st, const
         if (dtype == KC_F32) kc_launch_lsq_f32(c->dm, blend_of<float>(c, a), st, s, a->scheme, c->stream);
         else kc_launch_lsq_f64(c->dm, blend_of<double>(c, a), st, s, a->scheme, c->stream);
     } else if (c->dm.sig && a->dims == 3) {   // sigma meshes: the plain form's s = z / H_p step
-        if (dtype == KC_F32) kc_launch_sigma_f32(c->dm, blend_of<float>(c, a), st, s, a->scheme, c->stream);
-        else kc_launch_sigma_f64(c->dm, blend_of<double>(c, a), st, s, a->scheme, c->stream);
+        kc::DStep ss = s;
+        ss.eta_s = c->sig_s_on ? c->d_sig_eta_s : nullptr;
+        ss.eta_e = c->sig_e_on ? c->d_sig_eta_e : nullptr;
+        ss.sig_steady = c->sig_steady ? 1 : 0;
+        if (dtype == KC_F32) kc_launch_sigma_f32(c->dm, blend_of<float>(c, a), st, ss, a->scheme, c->stream);
+        else kc_launch_sigma_f64(c->dm, blend_of<double>(c, a), st, ss, a->scheme, c->stream);
     } else if (a->precision == KC_MIXED) {
         if (dtype == KC_F16) kc_launch_mixed_f16(c->dm, blend_of<__half>(c, a), st, s, a->dims, a->scheme, c->stream);
         else kc_launch_mixed_f32(c->dm, blend_of<float>(c, a), st, s, a->dims, a->scheme, c->stream);
@@ -968,7 +996,9 @@ void free_mesh(kc_ctx* c) {
     c->dm.ebox = nullptr;
     c->dm.erec = nullptr;
     dfree(c->d_beach_eta); dfree(c->d_beach_dry);
+    dfree(c->d_sig_eta_s); dfree(c->d_sig_eta_e);
     c->beach_eta_on = c->beach_dry_on = false;
+    c->sig_s_on = c->sig_e_on = c->sig_steady = false;
     dfree(c->d_dl_p); dfree(c->d_dl_last); dfree(c->d_dl_bed); dfree(c->d_enb); dfree(c->d_sigma);
     dfree(c->d_cg_corners); dfree(c->d_cg_cell); dfree(c->d_cg_nlev); dfree(c->d_cg_nlev_r); dfree(c->d_cg_L);
     dfree(c->d_cg_e2u); dfree(c->d_cg_e1v); dfree(c->d_cg_area); dfree(c->d_cg_zw); dfree(c->d_cg_e3b);
@@ -1520,6 +1550,68 @@ int kc_beach_surface(kc_ctx* c, const double* eta, const double* dry_mask) {
     if (eta || dry_mask) KC_CUDA(c, cudaStreamSynchronize(c->stream));   // the caller may free its arrays
     c->beach_eta_on = eta != nullptr;
     c->beach_dry_on = dry_mask != nullptr;
+    return KC_OK;
+}
+
+int kc_sigma_surfaces(kc_ctx* c, const double* eta_start, const double* eta_end, int steady) {
+    if (!c) return KC_ERR_ARG;
+    if (!c->has_mesh) return fail(c, KC_ERR_STATE, "kc_sigma_surfaces: no mesh uploaded");
+    if (!c->dm.sig) return fail(c, KC_ERR_STATE, "kc_sigma_surfaces: the resident mesh is not a sigma mesh");
+    if (steady != 0 && steady != 1) return fail(c, KC_ERR_ARG, "kc_sigma_surfaces: steady is 0 or 1");
+    KC_CUDA(c, cudaSetDevice(c->device));
+    const size_t bytes = (size_t)c->N * 8;
+    if (eta_start) {
+        if (!c->d_sig_eta_s) KC_CUDA(c, cudaMalloc((void**)&c->d_sig_eta_s, bytes));
+        KC_CUDA(c, cudaMemcpyAsync(c->d_sig_eta_s, eta_start, bytes, cudaMemcpyHostToDevice, c->stream));
+    }
+    if (eta_end) {
+        if (!c->d_sig_eta_e) KC_CUDA(c, cudaMalloc((void**)&c->d_sig_eta_e, bytes));
+        KC_CUDA(c, cudaMemcpyAsync(c->d_sig_eta_e, eta_end, bytes, cudaMemcpyHostToDevice, c->stream));
+    }
+    if (eta_start || eta_end) KC_CUDA(c, cudaStreamSynchronize(c->stream));   // the caller may free its arrays
+    c->sig_s_on = eta_start != nullptr;
+    c->sig_e_on = eta_end != nullptr;
+    c->sig_steady = steady != 0;
+    return KC_OK;
+}
+
+int kc_sigma_surface_slots(kc_ctx* c, int which, int kind, const int* slots, double alpha, const double* t, double q,
+                           int steady) {
+    if (!c) return KC_ERR_ARG;
+    if (!c->has_mesh) return fail(c, KC_ERR_STATE, "kc_sigma_surface_slots: no mesh uploaded");
+    if (!c->dm.sig) return fail(c, KC_ERR_STATE, "kc_sigma_surface_slots: the resident mesh is not a sigma mesh");
+    if ((which != 0 && which != 1) || kind < 0 || kind > 3 || (steady != 0 && steady != 1))
+        return fail(c, KC_ERR_ARG, "kc_sigma_surface_slots: which 0 / 1, kind 0..3, steady 0 / 1");
+    c->sig_steady = steady != 0;
+    bool& on = which == 0 ? c->sig_s_on : c->sig_e_on;
+    if (kind == 0) {
+        on = false;
+        return KC_OK;
+    }
+    const int n_rec = kind == 1 ? 1 : (kind == 2 ? 2 : 4);
+    if (!slots || (kind == 3 && !t)) return fail(c, KC_ERR_ARG, "kc_sigma_surface_slots: slots / times");
+    const double* e[4] = {nullptr, nullptr, nullptr, nullptr};
+    for (int k = 0; k < n_rec; ++k) {
+        if (slots[k] < 0 || slots[k] >= kSlots) return fail(c, KC_ERR_ARG, "kc_sigma_surface_slots: slot");
+        const Slot& sl = c->slots[slots[k]];
+        if (!sl.has_eta || sl.n != c->N)
+            return fail(c, KC_ERR_STATE, "kc_sigma_surface_slots: a slot without this mesh's surface");
+        e[k] = sl.eta;
+    }
+    if (kind == 3 && !(t[0] < t[1] && t[1] < t[2] && t[2] < t[3]))
+        return fail(c, KC_ERR_ARG, "kc_sigma_surface_slots: stencil times must increase");
+    KC_CUDA(c, cudaSetDevice(c->device));
+    double*& buf = which == 0 ? c->d_sig_eta_s : c->d_sig_eta_e;
+    if (!buf) KC_CUDA(c, cudaMalloc((void**)&buf, (size_t)c->N * 8));
+    int rc = wait_slots(c, slots, n_rec);
+    if (rc) return rc;
+    k_surface<<<grid_for(c->N), kBlock, 0, c->stream>>>(c->N, kind, e[0], e[1], e[2], e[3], alpha,
+                                                        kind == 3 ? t[0] : 0.0, kind == 3 ? t[1] : 0.0,
+                                                        kind == 3 ? t[2] : 0.0, kind == 3 ? t[3] : 0.0, q, buf);
+    KC_CUDA(c, cudaGetLastError());
+    rc = mark_slots_used(c, slots, n_rec);
+    if (rc) return rc;
+    on = true;
     return KC_OK;
 }
 

@@ -28,11 +28,30 @@ __device__ __forceinline__ double eta_at(const DBlend<T>& f, int node, double al
     return tblend(__ldg(&f.a.eta[node]), __ldg(&f.b.eta[node]), __ldg(&f.t.eta[node]), f.alpha0, alpha);
 }
 
+// The free surface at a node at one instant of the step (integrators.py:
+// 1358-1441, the sigma branches :5031-5079, :5424-5436, :5797-5815): slot 0
+// the start, 1..3 the RK stages (c = 0.5, 0.5, 1 for RK4; 0.5 for RK2), 4 the
+// end of the step (also the column of the split kick).  The tracking layer's
+// surfaces replace the payload's own where it supplies them (s.eta_s at the
+// start, s.eta_e at the end); a steady step (no next snapshot, no PCHIP)
+// blends its stages from the start towards the end surface as
+// _eta_blend does ((1 - c) a + c b), a time-aware step reads each stage
+// field's own surface.
+template <typename T>
+__device__ __forceinline__ double eta_src(const DBlend<T>& f, const DStep& s, int node, int slot) {
+    if (slot != 0 && !s.sig_steady && !(slot == 4 && s.eta_e))
+        return eta_at(f, node, slot == 4 ? s.alpha_end : s.ak[slot]);
+    const double e0 = s.eta_s ? __ldg(&s.eta_s[node]) : eta_at(f, node, s.ak[0]);
+    if (slot == 0) return e0;
+    const double e1 = s.eta_e ? __ldg(&s.eta_e[node]) : e0;
+    if (slot == 4 || slot == 3) return e1;
+    return (1.0 - 0.5) * e0 + 0.5 * e1;
+}
+
 // vertical_sigma.py:472-478 _col_H
 template <typename T>
-__device__ __forceinline__ double col_H(const DMesh& m, const DBlend<T>& f, const DStep& s, int node,
-                                        double alpha) {
-    double H = __ldg(&m.depth[node]) + eta_at(f, node, alpha);
+__device__ __forceinline__ double col_H(const DMesh& m, const DBlend<T>& f, const DStep& s, int node, int slot) {
+    double H = __ldg(&m.depth[node]) + eta_src(f, s, node, slot);
     if (H < s.Dmin) H = s.Dmin;
     return H;
 }
@@ -54,7 +73,7 @@ struct SigSite {
 // >= -1e-6, frame of mesh.py:1973-2003); its weights are the accepting
 // triangle's for a triangle and Wachspress for a quad.
 template <typename T>
-static __device__ __noinline__ void sigma_site(const DMesh& m, const DBlend<T>& f, const DStep& s, double alpha,
+static __device__ __noinline__ void sigma_site(const DMesh& m, const DBlend<T>& f, const DStep& s, int slot,
                                                double xp, double yp, int node, SigSite& q) {
     q.nv = 0;
     if (s.w_code == 1) {
@@ -101,7 +120,7 @@ static __device__ __noinline__ void sigma_site(const DMesh& m, const DBlend<T>& 
             double H = 0.0;
             for (int v = 0; v < nvv; ++v) {
                 q.v[v] = r.v[v];
-                q.Hv[v] = col_H(m, f, s, r.v[v], alpha);
+                q.Hv[v] = col_H(m, f, s, r.v[v], slot);
                 H += q.w[v] * q.Hv[v];
             }
             q.nv = nvv;
@@ -109,7 +128,7 @@ static __device__ __noinline__ void sigma_site(const DMesh& m, const DBlend<T>& 
             return;
         }
     }
-    q.H = col_H(m, f, s, node, alpha);
+    q.H = col_H(m, f, s, node, slot);
 }
 
 // vertical_sigma.py:297-334: the interface bracket of depth z in a column of
@@ -227,7 +246,7 @@ __device__ __forceinline__ void step3d_sigma_particle(const DMesh& m, const DBle
     int e_last = e1, e_out = e1;
 
     SigSite c1;
-    sigma_site<T>(m, f, s, s.ak[0], lon0, lat0, node_i, c1);
+    sigma_site<T>(m, f, s, 0, lon0, lat0, node_i, c1);
     double U1, V1, W1;
     bool ok = sig_stage<T>(m, f, s, lon0, lat0, node_i, e1, z0p, s.ak[0], c1, U1, V1, W1);
     st.U[i] = U1;
@@ -247,7 +266,7 @@ __device__ __forceinline__ void step3d_sigma_particle(const DMesh& m, const DBle
             const int nm = site_anchor(m, qm);
             e_last = stage_elem<WALK>(m, lm, tm, e1, nm);
             SigSite c2;
-            sigma_site<T>(m, f, s, s.ak[1], lm, tm, nm, c2);
+            sigma_site<T>(m, f, s, 1, lm, tm, nm, c2);
             const double zm = s_mid * c2.H;
             double U2, V2, W2;
             if (!sig_stage<T>(m, f, s, lm, tm, nm, e_last, zm, s.ak[1], c2, U2, V2, W2)) {
@@ -265,7 +284,7 @@ __device__ __forceinline__ void step3d_sigma_particle(const DMesh& m, const DBle
             const int n2 = site_anchor(m, q2);
             const int e2 = stage_elem<WALK>(m, l2, t2, e1, n2);
             SigSite c;
-            sigma_site<T>(m, f, s, s.ak[1], l2, t2, n2, c);
+            sigma_site<T>(m, f, s, 1, l2, t2, n2, c);
             double U2, V2, W2;
             if (!sig_stage<T>(m, f, s, l2, t2, n2, e2, (s0 + 0.5 * dt * f1) * c.H, s.ak[1], c, U2, V2, W2)) {
                 ok = false;
@@ -275,7 +294,7 @@ __device__ __forceinline__ void step3d_sigma_particle(const DMesh& m, const DBle
                 const Site q3 = make_site(l3, t3);
                 const int n3 = site_anchor(m, q3);
                 const int e3 = stage_elem<WALK>(m, l3, t3, e2, n3);
-                sigma_site<T>(m, f, s, s.ak[2], l3, t3, n3, c);
+                sigma_site<T>(m, f, s, 2, l3, t3, n3, c);
                 double U3, V3, W3;
                 if (!sig_stage<T>(m, f, s, l3, t3, n3, e3, (s0 + 0.5 * dt * f2) * c.H, s.ak[2], c, U3, V3, W3)) {
                     ok = false;
@@ -285,7 +304,7 @@ __device__ __forceinline__ void step3d_sigma_particle(const DMesh& m, const DBle
                     const Site q4 = make_site(l4, t4);
                     const int n4 = site_anchor(m, q4);
                     e_last = stage_elem<WALK>(m, l4, t4, e3, n4);
-                    sigma_site<T>(m, f, s, s.ak[3], l4, t4, n4, c);
+                    sigma_site<T>(m, f, s, 3, l4, t4, n4, c);
                     double U4, V4, W4;
                     if (!sig_stage<T>(m, f, s, l4, t4, n4, e_last, (s0 + dt * f3) * c.H, s.ak[3], c, U4, V4, W4)) {
                         ok = false;
@@ -313,7 +332,7 @@ __device__ __forceinline__ void step3d_sigma_particle(const DMesh& m, const DBle
             fr = FR_OOB;
         } else {
             SigSite ce;
-            sigma_site<T>(m, f, s, s.alpha_end, a, b, nn_new, ce);
+            sigma_site<T>(m, f, s, 4, a, b, nn_new, ce);
             lon_new = a;
             lat_new = b;
             nn_out = nn_new;
@@ -327,7 +346,7 @@ __device__ __forceinline__ void step3d_sigma_particle(const DMesh& m, const DBle
                            z_new, status, nn_out, fr, false, kel, kwel);
                 if (status == ALIVE) {
                     const double H_post = ce.H;
-                    sigma_site<T>(m, f, s, s.alpha_end, lon_new, lat_new, nn_out, ce);
+                    sigma_site<T>(m, f, s, 4, lon_new, lat_new, nn_out, ce);
                     z_new = clamp_sig(z_new / H_post * ce.H, ce.H, s);
                 }
             }

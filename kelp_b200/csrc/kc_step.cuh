@@ -49,6 +49,9 @@ struct DStep {
     double az_const;
     double Dmin, z0b_min;      // sigma column floor and bed clearance
     double alpha_end;          // blend fraction of the end-of-step surface (sigma)
+    const double* eta_s;       // sigma: the tracking layer's surface at the step's start (N), or null
+    const double* eta_e;       // sigma: the tracking layer's surface at the step's end (N), or null
+    int sig_steady;            // sigma: a steady step (stage surfaces blend from start to end)
 };
 
 // displacement metric z0 = max(cos(lat) * 111120, 1) (integrators.py:2563-2565),

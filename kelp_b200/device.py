@@ -393,6 +393,29 @@ class DeviceContext:
                 raise ValueError("beaching surfaces are node arrays (N,) of the uploaded mesh")
         self._chk(N.lib().kc_beach_surface(self._ctx, N.ptr(e), N.ptr(d)), "kc_beach_surface")
 
+    def sigma_surfaces(self, eta_start=None, eta_end=None, steady: bool = False) -> None:
+        """The tracking layer's surfaces at the start and end of the following
+        sigma steps (kc_sigma_surfaces); None: the payload's own."""
+        es = None if eta_start is None else _c(eta_start, np.float64)
+        ee = None if eta_end is None else _c(eta_end, np.float64)
+        n = None if self._mesh_ref is None else int(np.asarray(self._mesh_ref.nodes_lon).shape[0])
+        for a in (es, ee):
+            if a is not None and (n is None or a.shape != (n,)):
+                raise ValueError("sigma surfaces are node arrays (N,) of the uploaded mesh")
+        self._chk(N.lib().kc_sigma_surfaces(self._ctx, N.ptr(es), N.ptr(ee), int(bool(steady))),
+                  "kc_sigma_surfaces")
+
+    def sigma_surface_records(self, which: int, kind: int, slots=(), alpha: float = 0.0, times=None,
+                              q: float = 0.0, steady: bool = False) -> None:
+        """One tracking-layer surface (which 0 start, 1 end) evaluated on the
+        device from resident slots (kc_sigma_surface_slots): kind 0 off,
+        1 a record, 2 a linear blend at alpha, 3 PCHIP at time q."""
+        sl = np.zeros(4, np.int32)
+        sl[:len(slots)] = np.asarray(slots, dtype=np.int32)
+        t = None if times is None else np.ascontiguousarray(times, dtype=np.float64)
+        self._chk(N.lib().kc_sigma_surface_slots(self._ctx, int(which), int(kind), N.ptr(sl), float(alpha), N.ptr(t),
+                                                 float(q), int(bool(steady))), "kc_sigma_surface_slots")
+
     def beach(self, args: N.BeachArgs) -> None:
         self._chk(N.lib().kc_beach(self._ctx, C.byref(args)), "kc_beach")
 

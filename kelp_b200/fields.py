@@ -43,9 +43,10 @@ class VelocityField:
 
 
 def _lerp(a, b, alpha: float) -> np.ndarray:
-    """(1 - alpha) a + alpha b in the arrays' own dtype, the expression of
-    io.py:68-117 _blend (a float32 pair blends in float32, as numpy does)."""
-    return (1.0 - alpha) * np.asarray(a) + alpha * np.asarray(b)
+    """(1 - alpha) a + alpha b in float64, the expression of io.py:68-117
+    _blend (float32 snapshots are widened first, so they blend in float64 as
+    the reference's do, io.py:110-117)."""
+    return (1.0 - alpha) * np.asarray(a, dtype=np.float64) + alpha * np.asarray(b, dtype=np.float64)
 
 
 class LazyLerpField:

@@ -80,6 +80,11 @@ def _fields(vel, vel_next):
     return vel_a, vel_b, target, alpha0
 
 
+def _sigma_mesh(mesh) -> bool:
+    """A sigma mesh stepped by the s = z / H_p kernels (not a NEMO C-grid)."""
+    return getattr(mesh, "vertical_coord", "zlevel") == "sigma" and not getattr(mesh, "_nemo_cgrid", False)
+
+
 def _materialized(vel):
     """A LazyLerpField as the plain field its own blend makes of it (every
     array the payload carries, blended by the payload itself), for the paths
@@ -310,9 +315,12 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
                                  "only (vertical_uv.py:196-211)")
             if kw.get("cuda_precision", "plain") != "plain":
                 raise NotImplementedError("sigma meshes step in the plain form (cuda_precision='plain')")
-            if kw.get("sigma_eta_start") is not None or kw.get("sigma_eta_end") is not None:
-                raise NotImplementedError("sigma_eta_start / sigma_eta_end (the tracking layer's surfaces) are "
-                                          "not built on the CUDA backend")
+            own = np.shape(vel.eta)
+            for key in ("sigma_eta_start", "sigma_eta_end"):
+                given = kw.get(key)
+                if given is not None and np.shape(given) != own:   # integrators.py:1413-1424 _sigma_given
+                    raise ValueError(f"sigma step: supplied surface has shape {np.shape(given)}, "
+                                     f"the velocity field's eta {own}")
             if float(kw.get("Dmin", 0.5)) <= 0.0:
                 raise ValueError("Dmin must be > 0")
         w_interp = kw.get("w_interp", "leastsq")
@@ -428,6 +436,11 @@ def _run(state, vel, mesh, dt, time_dir, scheme, kw, ctx=None) -> ParticleState:
     if walk:
         inp["elem"] = np.ascontiguousarray(state.elem, dtype=np.int32)
         out["elem"] = np.empty(P, np.int32)
+    if is3d and _sigma_mesh(mesh):
+        # the tracking layer's surfaces of this step (integrators.py:1381-1441),
+        # or the payload's own; a steady step blends its stage surfaces
+        steady = kw.get("recon") is None and (kw.get("vel_next") is None or not (kw.get("dt_to_next") or 0) > 0)
+        ctx.sigma_surfaces(kw.get("sigma_eta_start"), kw.get("sigma_eta_end"), steady)
     # one call: chunked upload, step and download overlapped on the device
     ctx.step_host(a, inp, out)
     err = ctx.device_errors()

@@ -282,12 +282,10 @@ class Tracker:
         self.prefetch = bool(prefetch)
         self.prefetch_steps = 4   # steps ahead whose records are uploaded early (at most 4 records)
         self.walk = elem_search == "walk"
-        if getattr(mesh, "vertical_coord", "zlevel") == "sigma":
-            # the reference's loop hands every sigma step the surfaces at its
-            # start and end times from one function of time
-            # (tracking.py:2562-2596, _eta_at_time :3097-3133)
-            raise NotImplementedError("sigma meshes in the resident loop need the tracking layer's start/end "
-                                      "surfaces, which are not built; step them through the step functions")
+        # sigma meshes: every step gets the surfaces at its start and end times
+        # from one function of time (tracking.py:2562-2596), evaluated on the
+        # device from the resident records (_surface)
+        self.sigma = KI._sigma_mesh(mesh)
         self.mesh = mesh
         self.fields = list(fields)
         self.file_times = np.asarray(file_times, dtype=np.float64)
@@ -312,6 +310,37 @@ class Tracker:
         self.sort_every = int(sort_every)
         self.ctx = ctx or default_context()
         self.dims = 3 if getattr(self.fields[0], "w", None) is not None else 2
+
+    def _surface(self, which: int, t: float, multistage: bool, steady: bool, band: float) -> None:
+        """The sigma surface at time ``t`` as tracking.py:3097-3133
+        _eta_at_time defines it -- a record itself on a record, the PCHIP
+        stencil's value where PCHIP is on for a multistage step and a stencil
+        exists, else the linear blend of the bracket -- computed on the device
+        from the resident records into the start (which 0) or end (1)
+        surface of the next step; outside the data the step keeps the
+        payload's own surface."""
+        ctx, ft = self.ctx, self.file_times
+        b = resolve_time_bracket(t, ft, self.on_exhausted, self.direction, band)
+        if b is None:
+            ctx.sigma_surface_records(which, 0, steady=steady)
+            return
+        ia, ib, ta, tb, tw = b
+        interval = tb - ta
+        alpha = (tw - ta) / interval if interval > 0 else 0.0
+        times, q = None, 0.0
+        if ia == ib or abs(alpha) < 1e-12:
+            recs, kind = [ia], 1
+        elif abs(alpha - 1.0) < 1e-12:
+            recs, kind = [ib], 1
+        else:
+            stencil = resolve_recon_stencil(b, ft.size) if (self.pchip and multistage) else None
+            if stencil is not None:
+                recs, kind = list(stencil[0]), 3
+                times, q = [float(ft[i]) for i in recs], float(stencil[1])
+            else:
+                recs, kind = [ia, ib], 2
+        slots = ctx.slots_for([self.fields[i] for i in recs], KI.snapshot_storage(self.kw))
+        ctx.sigma_surface_records(which, kind, slots, alpha, times, q, steady)
 
     def _diffusion_args(self, realization: int, step_i: int, particle_offset: int):
         """The step's DiffusionStepArgs as tracking.py:2595-2611 builds them
@@ -435,6 +464,11 @@ class Tracker:
             diff = self._diffusion_args(realizations[0], g, particle_offset)
             kw["diffusion"] = diff
             kick = KI._kick_args(diff)
+            if self.sigma and self.dims == 3:
+                steady = recon is None and vnext is None
+                t_end = sim_time_end if sim_time_end is not None else sim_time + self.dt * self.direction
+                self._surface(0, sim_time, multistage, steady, band)
+                self._surface(1, t_end, multistage, steady, band)
             a, _ = KI.prepare_step(vel, mesh, step_len, float(self.direction), self.integrator, kw, ctx, kick=kick)
             a.global_step = g
             ctx.step(a)

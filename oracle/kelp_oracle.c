@@ -775,6 +775,9 @@ typedef struct {
     double az_const;
     double Dmin, z0b_min;  /* sigma column floor and bed clearance */
     double alpha_end;      /* blend fraction of the end-of-step surface (sigma) */
+    const double* eta_s;   /* sigma: the tracking layer's surface at the step's start (N), or NULL */
+    const double* eta_e;   /* sigma: the tracking layer's surface at the step's end (N), or NULL */
+    int sig_steady;        /* sigma: a steady step (stage surfaces blend from start to end) */
 } OStep;
 
 /* vertical_uv.py:457-523 uv_bracket */
@@ -1377,9 +1380,26 @@ static double eta_at(const OField* f, int node, double alpha) {
     return tblend(f->etaa[node], f->etab[node], f->etat[node], f->alpha0, alpha);
 }
 
+/* The surface at one instant of the step (integrators.py:1358-1441 and the
+ * sigma branches :5031-5079, :5424-5436, :5797-5815): slot 0 the start, 1..3
+ * the RK stages (c = 0.5, 0.5, 1), 4 the end; the tracking layer's surfaces
+ * (eta_s, eta_e) where given, a steady step's stages blended from the start
+ * to the end surface by _eta_blend, else the stage field's own. */
+static double stage_alpha(const OStep* s, int slot) { return slot == 4 ? s->alpha_end : s->ak[slot]; }
+
+static double eta_slot(const OField* f, const OStep* s, int node, int slot) {
+    double e0 = s->eta_s ? s->eta_s[node] : eta_at(f, node, s->ak[0]);
+    if (slot == 0) return e0;
+    if (slot == 4 && s->eta_e) return s->eta_e[node];
+    if (!s->sig_steady) return eta_at(f, node, stage_alpha(s, slot));
+    double e1 = s->eta_e ? s->eta_e[node] : e0;
+    if (slot == 3 || slot == 4) return e1;
+    return (1.0 - 0.5) * e0 + 0.5 * e1;
+}
+
 /* vertical_sigma.py:472-478 _col_H */
-static double col_H(const OMesh* m, const OField* f, const OStep* s, int node, double alpha) {
-    double H = m->depth[node] + eta_at(f, node, alpha);
+static double col_H(const OMesh* m, const OField* f, const OStep* s, int node, int slot) {
+    double H = m->depth[node] + eta_slot(f, s, node, slot);
     if (H < s->Dmin) H = s->Dmin;
     return H;
 }
@@ -1433,14 +1453,14 @@ static int bary_locate(const OMesh* m, double xp, double yp, int node, int* vert
 
 /* vertical_sigma.py:1034-1060 the particle's column height, interpolated
  * with the W method (nearest: the anchor's column; barycentric: :636-652) */
-static double sigma_H(const OMesh* m, const OField* f, const OStep* s, double alpha, double xp, double yp, int node) {
-    if (s->w_code == 0) return col_H(m, f, s, node, alpha);
+static double sigma_H(const OMesh* m, const OField* f, const OStep* s, int slot, double xp, double yp, int node) {
+    if (s->w_code == 0) return col_H(m, f, s, node, slot);
     int verts[4];
     double wts[4];
     int nv = bary_locate(m, xp, yp, node, verts, wts);
-    if (nv == 0) return col_H(m, f, s, node, alpha);
+    if (nv == 0) return col_H(m, f, s, node, slot);
     double H = 0.0;
-    for (int v = 0; v < nv; ++v) H += wts[v] * col_H(m, f, s, verts[v], alpha);
+    for (int v = 0; v < nv; ++v) H += wts[v] * col_H(m, f, s, verts[v], slot);
     return H;
 }
 
@@ -1474,23 +1494,24 @@ static double sigma_frac(double z, double H) {
 /* W on a sigma mesh (vertical_sigma.py:971-1031): nearest = the anchor's
  * column (:337-360); barycentric = every vertex column at the particle's
  * sigma (:766-816), the own column at min(z, H) outside every element */
-static double w_sig(const OMesh* m, const OField* f, const OStep* s, double alpha, double xp, double yp, double z,
+static double w_sig(const OMesh* m, const OField* f, const OStep* s, int slot, double xp, double yp, double z,
                     int node) {
-    if (s->w_code == 0) return w_sig_linear(m, f, alpha, z, node, col_H(m, f, s, node, alpha), s->td);
+    double alpha = stage_alpha(s, slot);
+    if (s->w_code == 0) return w_sig_linear(m, f, alpha, z, node, col_H(m, f, s, node, slot), s->td);
     int verts[4];
     double wts[4];
     int nv = bary_locate(m, xp, yp, node, verts, wts);
     if (nv == 0) {
-        double H = col_H(m, f, s, node, alpha);
+        double H = col_H(m, f, s, node, slot);
         double zc = z < H ? z : H;
         return w_sig_linear(m, f, alpha, zc, node, H, s->td);
     }
     double Hp = 0.0;
-    for (int v = 0; v < nv; ++v) Hp += wts[v] * col_H(m, f, s, verts[v], alpha);
+    for (int v = 0; v < nv; ++v) Hp += wts[v] * col_H(m, f, s, verts[v], slot);
     double fr = sigma_frac(z, Hp);
     double acc = 0.0;
     for (int v = 0; v < nv; ++v) {
-        double Hv = col_H(m, f, s, verts[v], alpha);
+        double Hv = col_H(m, f, s, verts[v], slot);
         acc += wts[v] * w_sig_linear(m, f, alpha, fr * Hv, verts[v], Hv, s->td);
     }
     return acc;
@@ -1552,10 +1573,10 @@ static void step_sigma(const OMesh* m, const OField* f, const OStep* s, int64_t 
     const int e1 = walk ? walk_locate(m, lon0, lat0, elem[i], node_i) : -1;
     int e_last = e1, e_out = e1;
 #define LOC(x, y, from, n) (walk ? walk_locate(m, (x), (y), (from), (n)) : -1)
-    double H1 = sigma_H(m, f, s, s->ak[0], lon0, lat0, node_i);
+    double H1 = sigma_H(m, f, s, 0, lon0, lat0, node_i);
     double U1, V1;
     int ok = STAGE(e1, sig_stage_uv(m, f, s, lon0, lat0, node_i, zp, H1, s->ak[0], &U1, &V1));
-    double W1 = w_sig(m, f, s, s->ak[0], lon0, lat0, zp, node_i);
+    double W1 = w_sig(m, f, s, 0, lon0, lat0, zp, node_i);
     U[i] = U1; V[i] = V1; W[i] = W1;
     double a = lon0, b = lat0, s_new = 0.0;
     if (ok) {
@@ -1570,12 +1591,12 @@ static void step_sigma(const OMesh* m, const OField* f, const OStep* s, int64_t 
             int nm = anchor(m, lm, tm);
             int em = LOC(lm, tm, e1, nm);
             e_last = em;
-            double H2 = sigma_H(m, f, s, s->ak[1], lm, tm, nm);
+            double H2 = sigma_H(m, f, s, 1, lm, tm, nm);
             double zm = s_mid * H2;
             double U2, V2;
             if (!STAGE(em, sig_stage_uv(m, f, s, lm, tm, nm, zm, H2, s->ak[1], &U2, &V2))) ok = 0;
             else {
-                double W2 = w_sig(m, f, s, s->ak[1], lm, tm, zm, nm);
+                double W2 = w_sig(m, f, s, 1, lm, tm, zm, nm);
                 a = wrap180(lon0 + dt * U2 / z0_of(tm));
                 b = clat(lat0 + dt * V2 / SLM);
                 s_new = zp / H1 + dt * W2 / H2;
@@ -1585,29 +1606,29 @@ static void step_sigma(const OMesh* m, const OField* f, const OStep* s, int64_t 
             double s0 = zp / H1, f1 = W1 / H1;
             double l2 = wrap180(lon0 + 0.5 * dl1), t2 = clat(lat0 + 0.5 * dd1);
             int n2 = anchor(m, l2, t2), e2 = LOC(l2, t2, e1, n2);
-            double H2 = sigma_H(m, f, s, s->ak[1], l2, t2, n2);
+            double H2 = sigma_H(m, f, s, 1, l2, t2, n2);
             double z2 = (s0 + 0.5 * dt * f1) * H2;
             double U2, V2, U3, V3, U4, V4;
             if (!STAGE(e2, sig_stage_uv(m, f, s, l2, t2, n2, z2, H2, s->ak[1], &U2, &V2))) ok = 0;
             else {
-                double W2 = w_sig(m, f, s, s->ak[1], l2, t2, z2, n2);
+                double W2 = w_sig(m, f, s, 1, l2, t2, z2, n2);
                 double dl2 = dt * U2 / z0_of(t2), dd2 = dt * V2 / SLM, f2 = W2 / H2;
                 double l3 = wrap180(lon0 + 0.5 * dl2), t3 = clat(lat0 + 0.5 * dd2);
                 int n3 = anchor(m, l3, t3), e3 = LOC(l3, t3, e2, n3);
-                double H3 = sigma_H(m, f, s, s->ak[2], l3, t3, n3);
+                double H3 = sigma_H(m, f, s, 2, l3, t3, n3);
                 double z3 = (s0 + 0.5 * dt * f2) * H3;
                 if (!STAGE(e3, sig_stage_uv(m, f, s, l3, t3, n3, z3, H3, s->ak[2], &U3, &V3))) ok = 0;
                 else {
-                    double W3 = w_sig(m, f, s, s->ak[2], l3, t3, z3, n3);
+                    double W3 = w_sig(m, f, s, 2, l3, t3, z3, n3);
                     double dl3 = dt * U3 / z0_of(t3), dd3 = dt * V3 / SLM, f3 = W3 / H3;
                     double l4 = wrap180(lon0 + dl3), t4 = clat(lat0 + dd3);
                     int n4 = anchor(m, l4, t4), e4 = LOC(l4, t4, e3, n4);
                     e_last = e4;
-                    double H4 = sigma_H(m, f, s, s->ak[3], l4, t4, n4);
+                    double H4 = sigma_H(m, f, s, 3, l4, t4, n4);
                     double z4 = (s0 + dt * f3) * H4;
                     if (!STAGE(e4, sig_stage_uv(m, f, s, l4, t4, n4, z4, H4, s->ak[3], &U4, &V4))) ok = 0;
                     else {
-                        double W4 = w_sig(m, f, s, s->ak[3], l4, t4, z4, n4);
+                        double W4 = w_sig(m, f, s, 3, l4, t4, z4, n4);
                         double dl4 = dt * U4 / z0_of(t4), dd4 = dt * V4 / SLM, f4 = W4 / H4;
                         double dl = (dl1 + 2.0 * dl2 + 2.0 * dl3 + dl4) / 6.0;
                         double dd = (dd1 + 2.0 * dd2 + 2.0 * dd3 + dd4) / 6.0;
@@ -1625,7 +1646,7 @@ static void step_sigma(const OMesh* m, const OField* f, const OStep* s, int64_t 
         int ein = walk ? walk_locate(m, a, b, e_last, nw) : contain_local(m, a, b, nw);
         if (ein < 0) { st = OUTSIDE; frr = 2; }
         else {
-            double He = sigma_H(m, f, s, s->alpha_end, a, b, nw);
+            double He = sigma_H(m, f, s, 4, a, b, nw);
             ln = a; lt = b; nno = nw; e_out = ein;
             zn = clamp_sig(s_new * He, He, s);
         }
@@ -1636,8 +1657,8 @@ static void step_sigma(const OMesh* m, const OField* f, const OStep* s, int64_t 
         int pnn = nno;
         kick(m, s, pid ? pid[i] : i, lon0, lat0, zp, pre_nn, &ln, &lt, &zn, &st, &nno, &frr, 0);
         if (st == ALIVE) {
-            double Hpost = sigma_H(m, f, s, s->alpha_end, plon, plat, pnn);
-            double Hk = sigma_H(m, f, s, s->alpha_end, ln, lt, nno);
+            double Hpost = sigma_H(m, f, s, 4, plon, plat, pnn);
+            double Hk = sigma_H(m, f, s, 4, ln, lt, nno);
             zn = clamp_sig(zn / Hpost * Hk, Hk, s);
         }
     }
@@ -1939,6 +1960,8 @@ typedef struct {
     int az_on, az_field;
     double az_const;
     double Dmin, z0b_min, alpha_end;
+    const double *eta_s, *eta_e;
+    int sig_steady;
 } orc_step_args;
 
 typedef struct {

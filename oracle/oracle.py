@@ -55,7 +55,8 @@ class OStep(C.Structure):
                 ("seed", C.c_uint64), ("real_id", C.c_uint64), ("step_i", C.c_uint64),
                 ("pid_offset", C.c_uint64), ("uv_dl", C.c_int),
                 ("az_on", C.c_int), ("az_field", C.c_int), ("az_const", C.c_double),
-                ("Dmin", C.c_double), ("z0b_min", C.c_double), ("alpha_end", C.c_double)]
+                ("Dmin", C.c_double), ("z0b_min", C.c_double), ("alpha_end", C.c_double),
+                ("eta_s", C.c_void_p), ("eta_e", C.c_void_p), ("sig_steady", C.c_int)]
 
 
 _lib = None
@@ -210,13 +211,15 @@ def _field_arrays(f, dtype):
 
 def step(state, vel, mesh, dt, time_dir, scheme: str, *, vel_next=None, dt_to_next=None, w_interp="nearest",
          diffusion=None, pid=None, release_step=None, global_step=-1, view=None, Dmin=0.5, z0b_min=0.1,
-         recon=None, uv_interp="barycentric"):
+         recon=None, uv_interp="barycentric", eta_start=None, eta_end=None):
     """One step of every particle; returns a dict of new arrays
     (lon, lat, z, status, nearest_node, failure_reason, u, v, w, and elem
     when the state carries elements: elem_search walk, the mesh's
     ``_elem_neighbors`` table required).  ``recon`` = (4 snapshots, their
     times, the step's time, direction) reconstructs the RK stages by PCHIP
-    (temporal_reconstruct.py:298-325; Euler ignores it)."""
+    (temporal_reconstruct.py:298-325; Euler ignores it).  ``eta_start`` /
+    ``eta_end``: the tracking layer's surfaces of a sigma step
+    (sigma_eta_start / sigma_eta_end), None for the payload's own."""
     view = view or MeshView(mesh)
     vel_a = getattr(vel, "vel_a", vel)
     vel_b = getattr(vel, "vel_b", vel_next if vel_next is not None else vel_a)
@@ -276,6 +279,10 @@ def step(state, vel, mesh, dt, time_dir, scheme: str, *, vel_next=None, dt_to_ne
         os_.alpha_end = float(recon[2]) + float(recon[3]) * 1.0 * float(dt)
     elif vel_next is not None:   # the end-of-step surface (integrators.py:1400-1420 _sigma_end_eta)
         os_.alpha_end = float(dt) / float(dt_to_next)
+    # the tracking layer's surfaces of a sigma step (integrators.py:1381-1441)
+    sig_keep = [None if e is None else np.ascontiguousarray(e, dtype=np.float64) for e in (eta_start, eta_end)]
+    os_.eta_s, os_.eta_e = (_p(e) for e in sig_keep)
+    os_.sig_steady = 1 if (not use_recon and vel_next is None) else 0
     if diffusion is not None:
         os_.seed, os_.real_id, os_.step_i = int(diffusion.seed), int(diffusion.real_id), int(diffusion.step_i)
         os_.pid_offset = int(getattr(diffusion, "pid_offset", 0))

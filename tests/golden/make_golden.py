@@ -86,7 +86,7 @@ def payload(fields, t, T):
 
 def run_case(rm, fields, lon, lat, z, status, scheme, dt, T, n_steps, *, time_dir=1.0, w_interp="nearest",
              kh=None, seed=7, real_id=0, pid_offset=0, record=(1,), az=None, walk=False, steady=False,
-             uv_interp="barycentric", pchip=False, t0=0.0):
+             uv_interp="barycentric", pchip=False, t0=0.0, surfaces=None):
     fn = {"rk2": RI.rk2_step, "rk4": RI.rk4_step, "euler": RI.euler_step}[scheme]
     P = lon.size
     st = RState(lon=lon.copy(), lat=lat.copy(), z=z.copy(), status=status.copy(),
@@ -116,6 +116,12 @@ def run_case(rm, fields, lon, lat, z, status, scheme, dt, T, n_steps, *, time_di
             kw["recon"] = ([fields[i] for i in idx], [float(i * T) for i in idx], t, float(time_dir))
             has_recon = 1
         sched.append([ia, alpha, dtn, has_recon, t])
+        if surfaces is not None:   # the tracking layer's sigma surfaces at the step's start and end
+            es, ee = surfaces(t, t + dt * time_dir)
+            for key, e in (("sigma_eta_start", es), ("sigma_eta_end", ee)):
+                if e is not None:
+                    kw[key] = e
+                    out.setdefault(key, []).append(e)
         st = fn(st, vel, rm, dt, time_dir, **kw)
         if (k + 1) in record or k + 1 == n_steps:
             tag = f"s{k + 1}"
@@ -125,6 +131,9 @@ def run_case(rm, fields, lon, lat, z, status, scheme, dt, T, n_steps, *, time_di
                 out[f"{tag}_w"] = np.asarray(st.w)
             if st.elem is not None:
                 out[f"{tag}_elem"] = np.asarray(st.elem)
+    for key in ("sigma_eta_start", "sigma_eta_end"):
+        if key in out:
+            out[key] = np.array(out[key])
     out["schedule"] = np.array(sched, dtype=np.float64)
     out["params"] = np.array([dt, T, n_steps, time_dir, -1 if kh is None else kh[0], -1 if kh is None else kh[1],
                               seed, real_id, pid_offset], dtype=np.float64)
@@ -452,6 +461,85 @@ def sigma_fixture():
                      "euler_llin_wnear": run_case(rm, rf, lon, lat, z, status, "euler", 1800.0, T, 12,
                                                   w_interp="nearest")}
         save(f"golden_{tag}", mesh_record(rm), snaps, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
+
+
+def sigma_surf_fixture():
+    """The tracking layer's surfaces on sigma steps (sigma_eta_start /
+    sigma_eta_end of the step functions, integrators.py:1358-1441, supplied
+    per step by tracking.py:2562-2596): on the sigma shelf of golden_sigma,
+    each step gets the surfaces of a smooth function of time (not the
+    payload's own) at its start and end -- time-aware RK2 / RK4 / Euler, steady
+    steps whose stages blend from the start to the end surface, the end
+    surface alone (the discrete mode), the start alone, and the split kick.
+    tests/golden/golden_sigma_surf.npz."""
+    T = 21600.0
+    sig = np.array([1.0, 0.95, 0.88, 0.8, 0.7, 0.58, 0.45, 0.32, 0.2, 0.1, 0.0])
+    m = S.lattice_mesh(1.0, 15.0, lon_min=-20.0, lon_max=20.0, jitter=0.15, land_frac=0.2, quad_frac=0.3,
+                       depth=lambda lo, la: S.smooth_bathymetry(lo, la, 0.2, 120.0), sigma=sig)
+    rm = ref_mesh(m, sigma=sig)
+    rm.vertical_coord = "sigma"
+    lon_n, lat_n = np.radians(np.asarray(m.nodes_lon)), np.radians(np.asarray(m.nodes_lat))
+    pseudo = (1.0 - sig) * 100.0
+    lon, lat, z, status = particles(m, 1200, 37, z=True, n_dead=20)
+    snaps = S.gyre_snapshots(m, 6, amp=1.0, z_levels=pseudo, decay=60.0, w_scale=4e-4, placement="layer")
+    for k, sn in enumerate(snaps):
+        sn.eta = (0.6 * np.sin(2.0 * lon_n + 0.9 * k) * np.cos(3.0 * lat_n) - 0.15).astype(np.float32)
+    rf = ref_fields(snaps)
+
+    def surf(t):
+        return 0.5 * np.sin(2.0 * lon_n + 2.0e-4 * t) * np.cos(3.0 * lat_n) - 0.1 + 0.3 * np.cos(lat_n + 1.0e-4 * t)
+
+    both = lambda t0, t1: (surf(t0), surf(t1))
+    cases = {"rk2_wbary_surf": run_case(rm, rf, lon, lat, z, status, "rk2", 3600.0, T, 10, w_interp="barycentric",
+                                        surfaces=both),
+             "rk4_wnear_surf": run_case(rm, rf, lon, lat, z, status, "rk4", 3600.0, T, 10, w_interp="nearest",
+                                        surfaces=both),
+             "euler_wbary_surf": run_case(rm, rf, lon, lat, z, status, "euler", 1800.0, T, 12,
+                                          w_interp="barycentric", surfaces=both),
+             "rk2_wbary_steady_surf": run_case(rm, rf, lon, lat, z, status, "rk2", 3600.0, T, 8,
+                                               w_interp="barycentric", steady=True, surfaces=both),
+             "rk4_wnear_steady_surf_kick": run_case(rm, rf, lon, lat, z, status, "rk4", 3600.0, T, 8,
+                                                    w_interp="nearest", steady=True, kh=(20.0, 20.0), seed=3,
+                                                    surfaces=both),
+             "rk4_wbary_steady_endonly": run_case(rm, rf, lon, lat, z, status, "rk4", 3600.0, T, 8,
+                                                  w_interp="barycentric", steady=True,
+                                                  surfaces=lambda t0, t1: (None, surf(t1))),
+             "rk2_wnear_startonly_kick": run_case(rm, rf, lon, lat, z, status, "rk2", 3600.0, T, 10,
+                                                  w_interp="nearest", kh=(30.0, 10.0), seed=8,
+                                                  surfaces=lambda t0, t1: (surf(t0), None))}
+    save("golden_sigma_surf", mesh_record(rm), snaps, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
+
+
+def eta_time_fixture():
+    """tracking.py:3097-3133 _eta_at_time, the surface a sigma step sees at
+    the start and end times of its step, on the records of golden_sigma_surf
+    (6 records 6 h apart): linear blends and the PCHIP stencil (multistage
+    steps with temporal_reconstruction pchip), every step start and end of a
+    forward run with dt = 1 h (and of a backward one), computed by the
+    reference with a record cache standing in for its reader.
+    tests/golden/golden_eta_time.npz."""
+    import types
+    from kelp.tracking import _eta_at_time, _snapshot_band
+    T = 21600.0
+    sig = np.array([1.0, 0.95, 0.88, 0.8, 0.7, 0.58, 0.45, 0.32, 0.2, 0.1, 0.0])
+    m = S.lattice_mesh(1.0, 15.0, lon_min=-20.0, lon_max=20.0, jitter=0.15, land_frac=0.2, quad_frac=0.3,
+                       depth=lambda lo, la: S.smooth_bathymetry(lo, la, 0.2, 120.0), sigma=sig)
+    lon_n, lat_n = np.radians(np.asarray(m.nodes_lon)), np.radians(np.asarray(m.nodes_lat))
+    etas = [(0.6 * np.sin(2.0 * lon_n + 0.9 * k) * np.cos(3.0 * lat_n) - 0.15).astype(np.float32) for k in range(6)]
+    ft = np.arange(6) * T
+    cache = types.SimpleNamespace(get=lambda i, *a, **k: types.SimpleNamespace(eta=etas[i]))
+    d = {"file_times": ft, "etas": np.array(etas)}
+    dt = 3600.0
+    for tag, direction, t0 in (("fwd", 1, 0.0), ("bwd", -1, ft[-1])):
+        times = t0 + direction * dt * np.arange(int(ft[-1] / dt) + 1)
+        d[f"{tag}_times"] = times
+        for pch in (False, True):
+            out = [_eta_at_time(float(t), ft, ft.size, "stop", direction, cache, None, None, None, "tinterp",
+                                None, None, pchip=pch, cycle=None, snap=_snapshot_band(dt)) for t in times]
+            d[f"{tag}_{'pchip' if pch else 'linear'}"] = np.array([np.full(lon_n.size, np.nan) if e is None
+                                                                   else np.asarray(e, dtype=np.float64) for e in out])
+    np.savez_compressed(os.path.join(HERE, "golden_eta_time.npz"), **d)
+    print("golden_eta_time", os.path.getsize(os.path.join(HERE, "golden_eta_time.npz")) // 1024, "KB")
 
 
 CGRID_KEYS = ("corners", "elem_ji", "nlev", "nlev_raster", "zw", "area", "e3b", "kbu", "e3u", "kbv", "e3v",
@@ -1033,7 +1121,7 @@ def reftypes_fixture():
 
 if __name__ == "__main__":
     # no argument: every fixture; otherwise the named ones ("steps", "beach", ...)
-    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq", "rng1m", "tripolar", "reftypes", "sample", "cellrule", "lazy0"}
+    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq", "rng1m", "tripolar", "reftypes", "sample", "cellrule", "lazy0", "sigma_surf", "eta_time"}
     if "rng1m" in which:
         rng1m_fixture()
     if "reftypes" in which:
@@ -1044,6 +1132,10 @@ if __name__ == "__main__":
         cellrule_fixture()
     if "lazy0" in which:
         lazy0_fixture()
+    if "sigma_surf" in which:
+        sigma_surf_fixture()
+    if "eta_time" in which:
+        eta_time_fixture()
     if "lsq" in which:
         lsq_fixture()
     if "steps" in which:

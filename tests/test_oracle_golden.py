@@ -28,6 +28,10 @@ SIGMA_CASES = [("golden_sigma", c) for c in ("rk2_wnear", "rk2_wbary", "rk4_wbar
                                              "rk2_wbary_kick", "rk4_wnear_kick", "rk2_wnear_bwd",
                                              "rk2_wbary_steady", "rk4_wnear_steady", "rk2_wbary_walk")]
 SIGMA_CASES += [("golden_sigma_llin", c) for c in ("rk2_llin_wbary", "rk4_llin_wnear_kick", "euler_llin_wnear")]
+# the tracking layer's surfaces supplied to sigma steps (sigma_eta_start / sigma_eta_end)
+SIGMA_CASES += [("golden_sigma_surf", c) for c in ("rk2_wbary_surf", "rk4_wnear_surf", "euler_wbary_surf",
+                                                  "rk2_wbary_steady_surf", "rk4_wnear_steady_surf_kick",
+                                                  "rk4_wbary_steady_endonly", "rk2_wnear_startonly_kick")]
 CASES += SIGMA_CASES
 # NEMO C-grid meshes (uv_interp nemo_cgrid): the 2-D unfused steps and the 3-D fractional-level step
 CGRID_CASES = [("golden_cgrid2d", c) for c in ("rk2", "rk4", "euler", "rk2_bwd", "rk4_steady", "rk2_kick", "rk2_walk")]
@@ -75,6 +79,11 @@ def diffusion_args(c, k):
     return DiffusionStepArgs("uniform", khx, khy, int(seed), int(real_id), k, pid_offset=int(pid_off), **az)
 
 
+def surfaces_of(c, k):
+    """The recorded step's sigma surfaces (start, end), None where not supplied."""
+    return tuple(c[key][k] if key in c else None for key in ("sigma_eta_start", "sigma_eta_end"))
+
+
 def replay_oracle(g, cname):
     c = g.case(cname)
     dt, T, n_steps, td, khx, khy, seed, real_id, pid_off = c["params"]
@@ -88,9 +97,10 @@ def replay_oracle(g, cname):
     for k in range(int(n_steps)):
         vel, vnext, dtn = g.payload(c["schedule"][k], T)
         diff = diffusion_args(c, k)
+        es, ee = surfaces_of(c, k)
         out = O.step(st, vel, g.mesh, dt, td, scheme, vel_next=vnext, dt_to_next=dtn, w_interp=w_interp,
                      diffusion=diff, view=view, recon=recon_of(g, c, k),
-                     uv_interp="leastsq" if g.uv_element else "barycentric")
+                     uv_interp="leastsq" if g.uv_element else "barycentric", eta_start=es, eta_end=ee)
         st = st.replace(lon=out["lon"], lat=out["lat"], z=out["z"], status=out["status"],
                         nearest_node=out["nearest_node"], failure_reason=out["failure_reason"],
                         u=out["u"], v=out["v"], w=out["w"], elem=out.get("elem"))
