@@ -866,7 +866,10 @@ int check_step(kc_ctx* c, const kc_step_args* a) {
     if (!(a->dims == 2 || a->dims == 3)) return fail(c, KC_ERR_ARG, "kc_step: dims must be 2 or 3");
     if (!(a->dt > 0.0)) return fail(c, KC_ERR_ARG, "kc_step: dt must be > 0");
     if (!(a->time_dir == 1.0 || a->time_dir == -1.0)) return fail(c, KC_ERR_ARG, "kc_step: time_dir must be +-1");
-    if (a->w_code != 0 && a->w_code != 1) return fail(c, KC_ERR_ARG, "kc_step: w_code must be 0 or 1");
+    if (a->w_code < 0 || a->w_code > 3) return fail(c, KC_ERR_ARG, "kc_step: w_code must be 0..3");
+    if (a->w_code >= 2 && (a->precision != KC_PLAIN || c->dm.sig || c->dm.cg.on))
+        return fail(c, KC_ERR_ARG, "kc_step: least-squares / inverse-distance W run in the plain form on z-level "
+                                   "meshes");
     if (a->kick && !(a->kh_x >= 0.0 && a->kh_y >= 0.0)) return fail(c, KC_ERR_ARG, "kc_step: Kh must be >= 0");
     if (a->precision != KC_PLAIN && a->precision != KC_MIXED)
         return fail(c, KC_ERR_ARG, "kc_step: precision must be KC_PLAIN or KC_MIXED");
@@ -920,7 +923,8 @@ int check_step(kc_ctx* c, const kc_step_args* a) {
     }
     if (c->dm.sig && a->dims == 3) {
         if (a->precision != KC_PLAIN) return fail(c, KC_ERR_ARG, "kc_step: sigma meshes step in the plain form");
-        if (a->az_kick) return fail(c, KC_ERR_ARG, "kc_step: the Az kick on sigma meshes is not built");
+        if (a->az_kick && a->az_field)
+            return fail(c, KC_ERR_ARG, "kc_step: sigma meshes take the constant Az source only");
         if (!(a->Dmin > 0.0) || !(a->z0b_min >= 0.0))
             return fail(c, KC_ERR_ARG, "kc_step: sigma steps need Dmin > 0 and z0b_min >= 0");
         if (!a->pchip && !(a->alpha_end >= 0.0 && a->alpha_end <= 1.0 + 1e-9))

@@ -443,6 +443,40 @@ __device__ __forceinline__ WLoc w_locate(const DMesh& m, double z) {
     return {k, (z - zk) / dz};
 }
 
+constexpr int kRingMax = 64;   // vertical.py:443 _MAX_NEIGHBOURS
+
+__device__ __forceinline__ int slot_of(const int4& e, int v) {
+    return v == 0 ? e.x : (v == 1 ? e.y : (v == 2 ? e.z : e.w));
+}
+
+// vertical.py:447-485 _collect_neighbour_nodes, visited in place: the
+// centre, then every vertex slot of the centre's elements in node->element
+// order, each node at its first occurrence only, at most kRingMax nodes.
+// f(node) returns false to stop; the return value counts the nodes visited.
+template <class F>
+__device__ __forceinline__ int for_ring(const DMesh& m, int nn, F&& f) {
+    if (!f(nn)) return 1;
+    int count = 1;
+    const int s = m.n2e_off[nn], e = m.n2e_off[nn + 1];
+    for (int k = s; k < e && count < kRingMax; ++k) {
+        const int4 ek = m.en[m.n2e[k]];
+        for (int v = 0; v < 4 && count < kRingMax; ++v) {
+            const int nd = slot_of(ek, v);
+            if (nd < 0 || nd == nn) continue;
+            bool dup = false;
+            for (int u = 0; u < v && !dup; ++u) dup = slot_of(ek, u) == nd;
+            for (int kk = s; kk < k && !dup; ++kk) {
+                const int4 ej = m.en[m.n2e[kk]];
+                dup = ej.x == nd || ej.y == nd || ej.z == nd || ej.w == nd;
+            }
+            if (dup) continue;
+            ++count;
+            if (!f(nd)) return count;
+        }
+    }
+    return count;
+}
+
 // The time-blended W of one node at a located depth (the value part of
 // vertical.py:1064-1098; tblend per level, :1042-1061).
 template <typename T>
@@ -483,6 +517,76 @@ __device__ __forceinline__ double w_vertex(const DMesh& m, const DBlend<T>& f, d
                                            const WLoc& Lz, int nd, double time_dir) {
     const double zc = pymin(z, __ldg(&m.depth[nd]));
     return w_at(f, alpha, zc == z ? Lz : w_locate(m, zc), nd, time_dir);
+}
+
+// W from the anchor's 1-ring of nodes (vertical.py:447-485 order), each
+// node's W at the particle's depth, or at its own bottom where the particle
+// is deeper (w_vertex): the least-squares plane through them evaluated at
+// the particle (vertical.py:493-601 _interp_w_leastsq_single; fewer than
+// three nodes or a singular system: the anchor's own W), or their
+// inverse-square-distance mean (:1148-1229 _interp_w_idw_single; a node
+// within 1 m is taken as is, no weight: the anchor's own W).  The cos of
+// the latitude is the correctly rounded one, the C library's value but
+// where the library misrounds.
+template <typename T>
+static __device__ __noinline__ double w_ring(const DMesh& m, const DBlend<T>& f, int w_code, double alpha,
+                                             double xp, double yp, double z, int node, double td) {
+    const WLoc Lz = w_locate(m, z);
+    double z0 = cr::cos_cr(yp * DEG2RAD) * SLM;
+    if (z0 < 1.0) z0 = 1.0;
+    if (w_code == 3) {
+        double sw = 0.0, swv = 0.0, hit_val = 0.0;
+        bool hit = false;
+        for_ring(m, node, [&](int nd) {
+            const double wv = w_vertex<T>(m, f, alpha, z, Lz, nd, td);
+            const double2 p = __ldg(&m.ll[nd]);
+            const double dx = wrap180(p.x - xp) * z0;
+            const double dy = (p.y - yp) * SLM;
+            const double d2 = dx * dx + dy * dy;
+            if (d2 < 1.0) {
+                hit = true;
+                hit_val = wv;
+                return false;
+            }
+            const double wt = 1.0 / d2;
+            sw += wt;
+            swv += wt * wv;
+            return true;
+        });
+        if (hit) return hit_val;
+        if (!(sw < 1e-30)) return swv / sw;
+        return w_vertex<T>(m, f, alpha, z, Lz, node, td);
+    }
+    double a11 = 0.0, a12 = 0.0, a13 = 0.0, a22 = 0.0, a23 = 0.0, a33 = 0.0, fw = 0.0, f1w = 0.0, f2w = 0.0;
+    const int cnt = for_ring(m, node, [&](int nd) {
+        const double wv = w_vertex<T>(m, f, alpha, z, Lz, nd, td);
+        const double2 p = __ldg(&m.ll[nd]);
+        const double ex = wrap180(p.x - xp) * z0;
+        const double ey = (p.y - yp) * SLM;
+        a11 += 1.0;
+        a12 += ex;
+        a13 += ey;
+        a22 += ex * ex;
+        a23 += ex * ey;
+        a33 += ey * ey;
+        fw += wv;
+        f1w += wv * ex;
+        f2w += wv * ey;
+        return true;
+    });
+    if (cnt >= 3) {
+        const double a21 = a12, a31 = a13, a32 = a23;
+        const double det = a11 * a22 * a33 + a12 * a23 * a31 + a13 * a21 * a32 - a13 * a22 * a31 - a12 * a21 * a33 -
+                           a11 * a23 * a32;
+        if (!(fabs(det) < 1e-30 || fabs(det) < 1e-12 * fabs(a11 * a22 * a33))) {
+            const double inv = 1.0 / fabs(det);
+            const double b11 = a22 * a33 - a23 * a32;
+            const double b12 = a13 * a32 - a12 * a33;
+            const double b13 = a12 * a23 - a13 * a22;
+            return (b11 * fw + b12 * f1w + b13 * f2w) * inv;
+        }
+    }
+    return w_vertex<T>(m, f, alpha, z, Lz, node, td);
 }
 
 // True when no fan triangle of the ring can give the point three weights

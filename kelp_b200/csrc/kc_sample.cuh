@@ -6,12 +6,11 @@
 // reference's order straight from the node->element table, and each rule
 // accumulates in that order, so the sums round as the reference's do.
 #pragma once
-#include "kc_geom.cuh"
+#include "kc_interp.cuh"
 
 namespace kc {
 
 constexpr int S_NEAREST = 0, S_LEASTSQ = 1, S_BARYCENTRIC = 2, S_IDW = 3;
-constexpr int kRingMax = 64;   // vertical.py:443 _MAX_NEIGHBOURS
 
 struct DSample {
     const double* values;   // (N) or (rows, N), float64
@@ -20,9 +19,6 @@ struct DSample {
     int rows;               // 0: a 2-D field; >= 1: a mid-layer field
 };
 
-__device__ __forceinline__ int slot_of(const int4& e, int v) {
-    return v == 0 ? e.x : (v == 1 ? e.y : (v == 2 ? e.z : e.w));
-}
 
 // sampling.py:432-484 _interp_mid_linear_single: linear between the
 // mid-layer values around z, clamped to the first / last layer.  The
@@ -55,34 +51,6 @@ __device__ __forceinline__ double node_value(const DMesh& m, const DSample& S, d
     if (S.rows == 0) return S.values[nd];
     const double bot = m.depth[nd];
     return mid_linear(S, z_p < bot ? z_p : bot, nd);
-}
-
-// vertical.py:447-485 _collect_neighbour_nodes, visited in place: the
-// centre, then every vertex slot of the centre's elements in node->element
-// order, each node at its first occurrence only, at most kRingMax nodes.
-// f(node) returns false to stop; the return value counts the nodes visited.
-template <class F>
-__device__ __forceinline__ int for_ring(const DMesh& m, int nn, F&& f) {
-    if (!f(nn)) return 1;
-    int count = 1;
-    const int s = m.n2e_off[nn], e = m.n2e_off[nn + 1];
-    for (int k = s; k < e && count < kRingMax; ++k) {
-        const int4 ek = m.en[m.n2e[k]];
-        for (int v = 0; v < 4 && count < kRingMax; ++v) {
-            const int nd = slot_of(ek, v);
-            if (nd < 0 || nd == nn) continue;
-            bool dup = false;
-            for (int u = 0; u < v && !dup; ++u) dup = slot_of(ek, u) == nd;
-            for (int kk = s; kk < k && !dup; ++kk) {
-                const int4 ej = m.en[m.n2e[kk]];
-                dup = ej.x == nd || ej.y == nd || ej.z == nd || ej.w == nd;
-            }
-            if (dup) continue;
-            ++count;
-            if (!f(nd)) return count;
-        }
-    }
-    return count;
 }
 
 // Whether node nd is among the ring's first kRingMax distinct nodes (the

@@ -350,6 +350,23 @@ __device__ __forceinline__ void step3d_sigma_particle(const DMesh& m, const DBle
                     z_new = clamp_sig(z_new / H_post * ce.H, ce.H, s);
                 }
             }
+            if (s.az_on && status == ALIVE) {
+                // integrators.py:917-930, diffusion.py:458-482 _loop_az_kick_sigma:
+                // the constant Az (no drift), folded into [0, max(H, Dmin) -
+                // z0b_min] of the end-of-step column at the particle
+                double H = ce.H;
+                if (H < s.Dmin) H = s.Dmin;
+                double bot = H - s.z0b_min;
+                if (bot < 0.0) bot = 0.0;
+                double xi, unused;
+                normal_pair<true>(m.rx, s.seed, realization_of(st, s, i),
+                                  (unsigned long long)(st.pid ? st.pid[i] : i) + s.pid_offset, s.step_i, 1ull, xi,
+                                  unused);
+                const double sdt = s.time_dir * s.dt;
+                const double abs_dt = sdt >= 0.0 ? sdt : -sdt;
+                const double dz = 0.0 * abs_dt + sqrt(2.0 * s.az_const * abs_dt) * xi;
+                z_new = reflect_depth(z_new + dz, 0.0, bot);
+            }
         }
     }
     st.lon[i] = lon_new;

@@ -39,7 +39,7 @@ struct DState {
 struct DStep {
     double dt, time_dir;
     double ak[4];              // stage alphas c_k * dt / dt_to_next
-    int w_code;                // 0 nearest, 1 barycentric (3-D)
+    int w_code;                // 3-D W: 0 nearest, 1 barycentric, 2 least squares, 3 inverse distance
     int uv_dl;                 // 3-D u/v: 0 layer, 1 depth-linear (level / layer_linear)
     int kick;                  // split uniform-Kh kick on/off
     double kh_x, kh_y;
@@ -434,13 +434,6 @@ __device__ __forceinline__ void step2d_particle(const DMesh& m, const DBlend<T>&
     if constexpr (!WALK) mark_scan(st, i, status, sc_el, sc_wel);
 }
 
-template <typename T>
-__device__ __forceinline__ double stage_w(const DMesh& m, const DBlend<T>& f, int w_code, double alpha,
-                                          double xp, double yp, double z, int node, double td) {
-    if (w_code == 0) return w_linear<T>(m, f, alpha, z, node, td);
-    return w_bary<T>(m, f, alpha, xp, yp, z, node, td);
-}
-
 // u/v of one 3-D stage: the layer rule (the particle's layer at the anchor,
 // integrators.py:3668-3676) or the depth-linear rule at the stage depth
 // (:4071-4098).
@@ -493,9 +486,10 @@ struct PlainForm {
     static __device__ __forceinline__ bool uvw3(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
                                                 double lat, int nn, int hint, int whint, double z, double alpha,
                                                 double& U, double& V, double& W) {
-        if (s.w_code == 0) {
+        if (s.w_code != 1) {   // W nearest (0), least squares (2), inverse distance (3)
             const bool ok = stage_uv<T>(m, f, s, lon, lat, nn, hint, z, alpha, U, V);
-            W = w_linear<T>(m, f, alpha, z, nn, s.time_dir);
+            W = s.w_code == 0 ? w_linear<T>(m, f, alpha, z, nn, s.time_dir)
+                              : w_ring<T>(m, f, s.w_code, alpha, lon, lat, z, nn, s.time_dir);
             return ok;
         }
         // W barycentric: one containment scan decides the u/v element and,

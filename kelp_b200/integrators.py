@@ -143,8 +143,10 @@ def _az_args(diffusion, vel, is3d, mesh):
         return None
     if not is3d:
         raise ValueError("diffusion.az_enabled requires a 3-D run (Fdrift3D)")
-    if getattr(mesh, "vertical_coord", "zlevel") == "sigma":
-        raise NotImplementedError("the Az kick on sigma meshes is not built on the CUDA backend")
+    if getattr(mesh, "vertical_coord", "zlevel") == "sigma" and az_field is not None:
+        # integrators.py:917-922: sigma meshes take the constant source only
+        raise ValueError("diffusion.var_az is not supported on sigma meshes (v1) — use the constant az_const "
+                         "source instead")
     return (az_field is not None, az_const)
 
 
@@ -324,9 +326,15 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
             if float(kw.get("Dmin", 0.5)) <= 0.0:
                 raise ValueError("Dmin must be > 0")
         w_interp = kw.get("w_interp", "leastsq")
-        if w_interp not in ("nearest", "barycentric"):
-            raise NotImplementedError(f"w_interp={w_interp!r} is not built on the CUDA backend")
-        w_code = 0 if w_interp == "nearest" else 1
+        codes = {"nearest": 0, "barycentric": 1, "leastsq": 2, "idw": 3}
+        if w_interp not in codes:
+            raise ValueError(f"unknown w_interp {w_interp!r}; expected one of {tuple(codes)}")
+        w_code = codes[w_interp]
+        if w_code >= 2 and coord == "sigma":
+            raise NotImplementedError(f"w_interp={w_interp!r} on sigma meshes is not built on the CUDA backend "
+                                      "(nearest and barycentric are)")
+        if w_code >= 2 and kw.get("cuda_precision", "plain") != "plain":
+            raise NotImplementedError(f"w_interp={w_interp!r} runs in the plain form (cuda_precision='plain')")
         if code == N.KC_RK2 and hasattr(vel, "vel_a") and float(getattr(vel, "alpha", 1.0)) == 0.0:
             # integrators.py:5691-5692 routes an endpoint LazyLerpField to the
             # unfused RK2 (:5380-5608): its stage fields are the payload

@@ -645,6 +645,29 @@ static double wat(const OField* f, int k, int node, double alpha) {
     return blend4(f, f->wa, f->wb, f->wt, f->wd, idx, alpha);
 }
 
+#define MAX_NEIGH 64   /* vertical.py:443 _MAX_NEIGHBOURS */
+
+/* vertical.py:447-485 _collect_neighbour_nodes: the centre, then each
+ * element's vertex slots in order, first occurrence only, at most 64. */
+static int neigh_ring(const OMesh* m, int nn, int32_t* buf) {
+    int count = 1;
+    buf[0] = nn;
+    int ne = m->n2e_cnt[nn];
+    for (int k = 0; k < ne; ++k) {
+        int e = m->n2e[(int64_t)nn * m->max_conn + k];
+        if (e < 0) continue;
+        for (int v = 0; v < m->max_v; ++v) {
+            int nd = m->en[(int64_t)e * m->max_v + v];
+            if (nd < 0) continue;
+            int found = 0;
+            for (int j = 0; j < count; ++j)
+                if (buf[j] == nd) { found = 1; break; }
+            if (!found && count < MAX_NEIGH) buf[count++] = nd;
+        }
+    }
+    return count;
+}
+
 /* vertical.py:1064-1098 */
 static double w_linear(const OMesh* m, const OField* f, double alpha, double z, int node, double td) {
     int K = m->K;
@@ -663,6 +686,52 @@ static double w_linear(const OMesh* m, const OField* f, double alpha, double z, 
 }
 
 static double pymin(double a, double b) { return b < a ? b : a; }
+
+/* vertical.py:493-601 _interp_w_leastsq_single (w_code 2) and :1148-1229
+ * _interp_w_idw_single (w_code 3) on the stage's W: the anchor's 1-ring of
+ * nodes, each node's W at min(z, its bottom) */
+static double w_ring(const OMesh* m, const OField* f, int w_code, double alpha, double xp, double yp, double z,
+                     int node, double td) {
+    int32_t buf[MAX_NEIGH];
+    int count = neigh_ring(m, node, buf);
+    double fallback = w_linear(m, f, alpha, pymin(z, m->depth[node]), node, td);
+    double z0 = cos(yp * DEG2RAD) * SLM;
+    if (z0 < 1.0) z0 = 1.0;
+    if (w_code == 3) {
+        double sw = 0.0, swv = 0.0;
+        for (int i = 0; i < count; ++i) {
+            int nd = buf[i];
+            double wv = w_linear(m, f, alpha, pymin(z, m->depth[nd]), nd, td);
+            double dx = wrap180(m->lon[nd] - xp) * z0;
+            double dy = (m->lat[nd] - yp) * SLM;
+            double d2 = dx * dx + dy * dy;
+            if (d2 < 1.0) return wv;
+            double wt = 1.0 / d2;
+            sw += wt;
+            swv += wt * wv;
+        }
+        if (sw < 1e-30) return fallback;
+        return swv / sw;
+    }
+    if (count < 3) return fallback;
+    double a11 = 0.0, a12 = 0.0, a13 = 0.0, a22 = 0.0, a23 = 0.0, a33 = 0.0, fw = 0.0, f1w = 0.0, f2w = 0.0;
+    for (int i = 0; i < count; ++i) {
+        int nd = buf[i];
+        double wv = w_linear(m, f, alpha, pymin(z, m->depth[nd]), nd, td);
+        double ex = wrap180(m->lon[nd] - xp) * z0;
+        double ey = (m->lat[nd] - yp) * SLM;
+        a11 += 1.0; a12 += ex; a13 += ey;
+        a22 += ex * ex; a23 += ex * ey; a33 += ey * ey;
+        fw += wv; f1w += wv * ex; f2w += wv * ey;
+    }
+    double a21 = a12, a31 = a13, a32 = a23;
+    double det = a11 * a22 * a33 + a12 * a23 * a31 + a13 * a21 * a32 - a13 * a22 * a31 - a12 * a21 * a33 -
+                 a11 * a23 * a32;
+    if (fabs(det) < 1e-30 || fabs(det) < 1e-12 * fabs(a11 * a22 * a33)) return fallback;
+    double inv = 1.0 / fabs(det);
+    double b11 = a22 * a33 - a23 * a32, b12 = a13 * a32 - a12 * a33, b13 = a12 * a23 - a13 * a22;
+    return (b11 * fw + b12 * f1w + b13 * f2w) * inv;
+}
 
 /* vertical.py:744-881 */
 static double w_bary(const OMesh* m, const OField* f, double alpha, double xp, double yp, double z, int node, double td) {
@@ -717,6 +786,14 @@ static double w_bary(const OMesh* m, const OField* f, double alpha, double xp, d
         }
     }
     return w_linear(m, f, alpha, pymin(z, m->depth[node]), node, td);
+}
+
+/* W of one stage by the step's method (integrators.py:1260-1288 _compute_w, z-level) */
+static double w_stage(const OMesh* m, const OField* f, int w_code, double alpha, double xp, double yp, double z,
+                      int node, double td) {
+    if (w_code == 0) return w_linear(m, f, alpha, z, node, td);
+    if (w_code == 1) return w_bary(m, f, alpha, xp, yp, z, node, td);
+    return w_ring(m, f, w_code, alpha, xp, yp, z, node, td);
 }
 
 /* diffusion.py:180-249 */
@@ -970,6 +1047,21 @@ static void az_kick(const OMesh* m, const OField* f, const OStep* s, int64_t pid
     double abs_dt = sdt >= 0.0 ? sdt : -sdt;
     double dz = g * abs_dt + sqrt(2.0 * az * abs_dt) * xi[0];
     *z = reflect_depth(*z + dz, m->zlev[0], m->depth[nn]);
+}
+
+/* integrators.py:917-930 with diffusion.py:458-482 _loop_az_kick_sigma, one
+ * particle: the constant Az, no drift, folded into [0, max(H, Dmin) - z0b_min]
+ * of its end-of-step column H */
+static void az_kick_sigma(const OStep* s, int64_t pid, double H, double* z) {
+    if (H < s->Dmin) H = s->Dmin;
+    double bot = H - s->z0b_min;
+    if (bot < 0.0) bot = 0.0;
+    double xi[2];
+    orc_normal_pair(s->seed, s->real_id, (uint64_t)pid + s->pid_offset, s->step_i, 1, xi);
+    double sdt = s->td * s->dt;
+    double abs_dt = sdt >= 0.0 ? sdt : -sdt;
+    double dz = 0.0 * abs_dt + sqrt(2.0 * s->az_const * abs_dt) * xi[0];
+    *z = reflect_depth(*z + dz, 0.0, bot);
 }
 
 /* integrators.py:673-818 for one surviving particle */
@@ -1662,6 +1754,7 @@ static void step_sigma(const OMesh* m, const OField* f, const OStep* s, int64_t 
             zn = clamp_sig(zn / Hpost * Hk, Hk, s);
         }
     }
+    if (s->az_on && st == ALIVE) az_kick_sigma(s, pid ? pid[i] : i, sigma_H(m, f, s, 4, ln, lt, nno), &zn);
     lon[i] = ln; lat[i] = lt; z[i] = zn;
     status[i] = st; nn[i] = nno; fr[i] = frr;
     if (walk) elem[i] = e_out;
@@ -1754,8 +1847,7 @@ static void step_one(const OMesh* m, const OField* f, const OStep* s, int64_t i,
          * stage position, failure reverts to the start with the start anchor. */
         double U1, V1;
         int ok1 = STAGE(e1, stage_uv(m, f, s, lon0, lat0, node_i, zp, s->ak[0], &U1, &V1));
-        double W1 = s->w_code == 0 ? w_linear(m, f, s->ak[0], zp, node_i, td)
-                                   : w_bary(m, f, s->ak[0], lon0, lat0, zp, node_i, td);
+        double W1 = w_stage(m, f, s->w_code, s->ak[0], lon0, lat0, zp, node_i, td);
         U[i] = U1; V[i] = V1; W[i] = W1;
         double a = lon0, b = lat0, c = zp;
         if (!ok1) ok = 0;
@@ -1770,23 +1862,20 @@ static void step_one(const OMesh* m, const OField* f, const OStep* s, int64_t i,
             double U2, V2, U3, V3, U4, V4;
             if (!STAGE(e2, stage_uv(m, f, s, l2, t2, n2, z2, s->ak[1], &U2, &V2))) ok = 0;
             else {
-                double W2 = s->w_code == 0 ? w_linear(m, f, s->ak[1], z2, n2, td)
-                                           : w_bary(m, f, s->ak[1], l2, t2, z2, n2, td);
+                double W2 = w_stage(m, f, s->w_code, s->ak[1], l2, t2, z2, n2, td);
                 double dl2 = dt * U2 / z0_of(t2), dd2 = dt * V2 / SLM, dz2 = dt * W2;
                 double l3 = wrap180(lon0 + 0.5 * dl2), t3 = clat(lat0 + 0.5 * dd2), z3 = zp + 0.5 * dz2;
                 int n3 = anchor(m, l3, t3), e3 = LOC(l3, t3, e2, n3);
                 if (!STAGE(e3, stage_uv(m, f, s, l3, t3, n3, z3, s->ak[2], &U3, &V3))) ok = 0;
                 else {
-                    double W3 = s->w_code == 0 ? w_linear(m, f, s->ak[2], z3, n3, td)
-                                               : w_bary(m, f, s->ak[2], l3, t3, z3, n3, td);
+                    double W3 = w_stage(m, f, s->w_code, s->ak[2], l3, t3, z3, n3, td);
                     double dl3 = dt * U3 / z0_of(t3), dd3 = dt * V3 / SLM, dz3 = dt * W3;
                     double l4 = wrap180(lon0 + dl3), t4 = clat(lat0 + dd3), z4 = zp + dz3;
                     int n4 = anchor(m, l4, t4), e4 = LOC(l4, t4, e3, n4);
                     e_last = e4;
                     if (!STAGE(e4, stage_uv(m, f, s, l4, t4, n4, z4, s->ak[3], &U4, &V4))) ok = 0;
                     else {
-                        double W4 = s->w_code == 0 ? w_linear(m, f, s->ak[3], z4, n4, td)
-                                                   : w_bary(m, f, s->ak[3], l4, t4, z4, n4, td);
+                        double W4 = w_stage(m, f, s->w_code, s->ak[3], l4, t4, z4, n4, td);
                         double dl4 = dt * U4 / z0_of(t4), dd4 = dt * V4 / SLM, dz4 = dt * W4;
                         double dl = (dl1 + 2.0 * dl2 + 2.0 * dl3 + dl4) / 6.0;
                         double dd = (dd1 + 2.0 * dd2 + 2.0 * dd3 + dd4) / 6.0;
@@ -1812,8 +1901,7 @@ static void step_one(const OMesh* m, const OField* f, const OStep* s, int64_t i,
     } else {
         double U1, V1;
         int ok1 = STAGE(e1, stage_uv(m, f, s, lon0, lat0, node_i, zp, s->ak[0], &U1, &V1));
-        double W1 = s->w_code == 0 ? w_linear(m, f, s->ak[0], zp, node_i, td)
-                                   : w_bary(m, f, s->ak[0], lon0, lat0, zp, node_i, td);
+        double W1 = w_stage(m, f, s->w_code, s->ak[0], lon0, lat0, zp, node_i, td);
         U[i] = U1; V[i] = V1; W[i] = W1;
         if (!ok1) { st = OUTSIDE; frr = 1; }
         else {
@@ -1826,8 +1914,7 @@ static void step_one(const OMesh* m, const OField* f, const OStep* s, int64_t i,
             double U2, V2;
             if (!STAGE(em, stage_uv(m, f, s, lm, tm, nm, zm, s->ak[1], &U2, &V2))) { st = OUTSIDE; frr = 1; }
             else {
-                double W2 = s->w_code == 0 ? w_linear(m, f, s->ak[1], zm, nm, td)
-                                           : w_bary(m, f, s->ak[1], lm, tm, zm, nm, td);
+                double W2 = w_stage(m, f, s->w_code, s->ak[1], lm, tm, zm, nm, td);
                 double a = wrap180(lon0 + dt * U2 / z0_of(tm));
                 double b = clat(lat0 + dt * V2 / SLM);
                 double c = zp + W2 * dt;
@@ -2187,29 +2274,6 @@ int orc_node_xyz(int64_t n, const double* lon, const double* lat, double* out) {
 #define S_LEASTSQ 1
 #define S_BARYCENTRIC 2
 #define S_IDW 3
-#define MAX_NEIGH 64   /* vertical.py:443 _MAX_NEIGHBOURS */
-
-/* vertical.py:447-485 _collect_neighbour_nodes: the centre, then each
- * element's vertex slots in order, first occurrence only, at most 64. */
-static int neigh_ring(const OMesh* m, int nn, int32_t* buf) {
-    int count = 1;
-    buf[0] = nn;
-    int ne = m->n2e_cnt[nn];
-    for (int k = 0; k < ne; ++k) {
-        int e = m->n2e[(int64_t)nn * m->max_conn + k];
-        if (e < 0) continue;
-        for (int v = 0; v < m->max_v; ++v) {
-            int nd = m->en[(int64_t)e * m->max_v + v];
-            if (nd < 0) continue;
-            int found = 0;
-            for (int j = 0; j < count; ++j)
-                if (buf[j] == nd) { found = 1; break; }
-            if (!found && count < MAX_NEIGH) buf[count++] = nd;
-        }
-    }
-    return count;
-}
-
 /* sampling.py:82-380 _combine_horizontal */
 static double combine_horizontal(const OMesh* m, const double* vals, const int32_t* buf, int cnt, double lon_p,
                                  double lat_p, int nn, int method) {

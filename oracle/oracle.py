@@ -263,7 +263,7 @@ def step(state, vel, mesh, dt, time_dir, scheme: str, *, vel_next=None, dt_to_ne
     os_ = OStep()
     os_.scheme = {"euler": 0, "rk2": 1, "rk4": 2}[scheme]
     os_.dims = 3 if is3d else 2
-    os_.w_code = 0 if w_interp == "nearest" else 1
+    os_.w_code = {"nearest": 0, "barycentric": 1, "leastsq": 2, "idw": 3}[w_interp]
     os_.uv_dl = 1 if (is3d and placement != "layer") else 0
     cc = {"euler": (0.0,), "rk2": (0.0, 0.5), "rk4": (0.0, 0.5, 0.5, 1.0)}[scheme]
     if use_recon:   # the stage times sim_time + time_dir * c * dt

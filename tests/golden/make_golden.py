@@ -510,6 +510,72 @@ def sigma_surf_fixture():
     save("golden_sigma_surf", mesh_record(rm), snaps, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
 
 
+def sigma_az_fixture():
+    """The vertical Az kick on sigma meshes (integrators.py:917-930,
+    diffusion.py:458-482 _loop_az_kick_sigma: the constant source, folded
+    into the particle's end-of-step column): on the sigma shelf of
+    golden_sigma_surf, Az alone and with the horizontal split kick, RK2 / RK4
+    / Euler, forward and backward, with and without the tracking layer's
+    surfaces.  tests/golden/golden_sigma_az.npz."""
+    T = 21600.0
+    sig = np.array([1.0, 0.95, 0.88, 0.8, 0.7, 0.58, 0.45, 0.32, 0.2, 0.1, 0.0])
+    m = S.lattice_mesh(1.0, 15.0, lon_min=-20.0, lon_max=20.0, jitter=0.15, land_frac=0.2, quad_frac=0.3,
+                       depth=lambda lo, la: S.smooth_bathymetry(lo, la, 0.2, 120.0), sigma=sig)
+    rm = ref_mesh(m, sigma=sig)
+    rm.vertical_coord = "sigma"
+    lon_n, lat_n = np.radians(np.asarray(m.nodes_lon)), np.radians(np.asarray(m.nodes_lat))
+    pseudo = (1.0 - sig) * 100.0
+    lon, lat, z, status = particles(m, 1200, 39, z=True, n_dead=20)
+    snaps = S.gyre_snapshots(m, 6, amp=1.0, z_levels=pseudo, decay=60.0, w_scale=4e-4, placement="layer")
+    for k, sn in enumerate(snaps):
+        sn.eta = (0.6 * np.sin(2.0 * lon_n + 0.9 * k) * np.cos(3.0 * lat_n) - 0.15).astype(np.float32)
+    rf = ref_fields(snaps)
+
+    def surf(t):
+        return 0.5 * np.sin(2.0 * lon_n + 2.0e-4 * t) * np.cos(3.0 * lat_n) - 0.1 + 0.3 * np.cos(lat_n + 1.0e-4 * t)
+
+    azc = dict(az_enabled=True, az_const=2e-3)
+    cases = {"rk2_wbary_azc": run_case(rm, rf, lon, lat, z, status, "rk2", 3600.0, T, 10, w_interp="barycentric",
+                                       kh=(0.0, 0.0), seed=4, az=azc),
+             "rk4_wnear_kick_azc": run_case(rm, rf, lon, lat, z, status, "rk4", 3600.0, T, 10, w_interp="nearest",
+                                            kh=(20.0, 20.0), seed=6, az=azc),
+             "euler_wbary_azc": run_case(rm, rf, lon, lat, z, status, "euler", 1800.0, T, 12,
+                                         w_interp="barycentric", kh=(0.0, 0.0), seed=2, az=azc),
+             "rk2_wnear_bwd_kick_azc": run_case(rm, rf, lon, lat, z, status, "rk2", 3600.0, T, 10,
+                                                w_interp="nearest", kh=(30.0, 10.0), seed=7, az=azc,
+                                                time_dir=-1.0),
+             "rk2_wbary_surf_kick_azc": run_case(rm, rf, lon, lat, z, status, "rk2", 3600.0, T, 10,
+                                                 w_interp="barycentric", kh=(20.0, 20.0), seed=9, az=azc,
+                                                 surfaces=lambda t0, t1: (surf(t0), surf(t1)))}
+    save("golden_sigma_az", mesh_record(rm), snaps, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
+
+
+def wring_fixture():
+    """W by least squares (the reference's default w_interp,
+    vertical.py:493-601) and by inverse distance (:1148-1229) on the 3-D
+    z-level mesh of golden_3d, through the reference's unfused steps: RK2,
+    RK4, Euler, the split kick, backward time, depth-linear u/v.
+    tests/golden/golden_wring.npz."""
+    T = 86400.0
+    zl = S.stretched_levels(12, 5.0, 4000.0)
+    m = S.lattice_mesh(3.0, 60.0, jitter=0.2, land_frac=0.25,
+                       depth=lambda lo, la: S.smooth_bathymetry(lo, la, 30.0, 4000.0), sigma=zl)
+    rm = ref_mesh(m, sigma=zl)
+    snaps = S.gyre_snapshots(m, 4, amp=1.5, z_levels=zl, decay=800.0, w_scale=2e-3)
+    rf = ref_fields(snaps)
+    lon, lat, z, status = particles(m, 1200, 47, z=True, n_dead=20)
+    cases = {"rk2_wlsq": run_case(rm, rf, lon, lat, z, status, "rk2", 21600.0, T, 10, w_interp="leastsq"),
+             "rk4_wlsq_kick": run_case(rm, rf, lon, lat, z, status, "rk4", 21600.0, T, 10, w_interp="leastsq",
+                                       kh=(3.0e4, 3.0e4), seed=5),
+             "euler_wlsq": run_case(rm, rf, lon, lat, z, status, "euler", 10800.0, T, 12, w_interp="leastsq"),
+             "rk2_wlsq_bwd": run_case(rm, rf, lon, lat, z, status, "rk2", 21600.0, T, 10, w_interp="leastsq",
+                                      time_dir=-1.0),
+             "rk2_widw": run_case(rm, rf, lon, lat, z, status, "rk2", 21600.0, T, 10, w_interp="idw"),
+             "rk4_widw_kick": run_case(rm, rf, lon, lat, z, status, "rk4", 21600.0, T, 10, w_interp="idw",
+                                       kh=(3.0e4, 1.0e4), seed=9)}
+    save("golden_wring", mesh_record(rm), snaps, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
+
+
 def eta_time_fixture():
     """tracking.py:3097-3133 _eta_at_time, the surface a sigma step sees at
     the start and end times of its step, on the records of golden_sigma_surf
@@ -1121,7 +1187,7 @@ def reftypes_fixture():
 
 if __name__ == "__main__":
     # no argument: every fixture; otherwise the named ones ("steps", "beach", ...)
-    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq", "rng1m", "tripolar", "reftypes", "sample", "cellrule", "lazy0", "sigma_surf", "eta_time"}
+    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq", "rng1m", "tripolar", "reftypes", "sample", "cellrule", "lazy0", "sigma_surf", "eta_time", "sigma_az", "wring"}
     if "rng1m" in which:
         rng1m_fixture()
     if "reftypes" in which:
@@ -1136,6 +1202,10 @@ if __name__ == "__main__":
         sigma_surf_fixture()
     if "eta_time" in which:
         eta_time_fixture()
+    if "sigma_az" in which:
+        sigma_az_fixture()
+    if "wring" in which:
+        wring_fixture()
     if "lsq" in which:
         lsq_fixture()
     if "steps" in which:

@@ -14,7 +14,7 @@ from kelp_b200 import integrators as KI
 from kelp_b200.diffusion import DiffusionStepArgs
 
 from test_oracle_golden import (CGRID_CASES, LSQ_CASES, PCHIP_CASES, SIGMA_CASES, diffusion_args, recon_of, surfaces_of,
-                                uv_interp_of)
+                                uv_interp_of, w_interp_of)
 
 pytestmark = pytest.mark.gpu
 
@@ -29,6 +29,8 @@ CASES += [("golden_3d", c) for c in ("rk2_wnear", "rk2_wbary", "rk2_wbary_kick",
                                      "rk2_wbary_kick_azf", "rk4_wnear_azf_nokh")]
 CASES += [("golden_dl_lev", c) for c in ("rk2_lev_wbary", "rk4_lev_wnear_kick", "euler_lev_wnear", "rk2_lev_wbary_azc")]
 CASES += [("golden_dl_llin", c) for c in ("rk2_llin_wbary", "rk4_llin_wnear_kick", "euler_llin_wnear")]
+CASES += [("golden_wring", c) for c in ("rk2_wlsq", "rk4_wlsq_kick", "euler_wlsq", "rk2_wlsq_bwd", "rk2_widw",
+                                        "rk4_widw_kick")]
 # elem_search: walk (carried elements in and out of every step)
 WALK_CASES = [("golden_band", c) for c in ("rk2_walk", "rk4_walk_kick", "euler_walk")]
 WALK_CASES += [("golden_3d", c) for c in ("rk2_wbary_walk", "rk4_wnear_walk_kick")]
@@ -44,7 +46,7 @@ def replay_cuda(g, cname):
     dt, T, n_steps, td, khx, khy, seed, real_id, pid_off = c["params"]
     scheme = cname.split("_")[0]
     fn = KI.get_integrator(scheme)
-    w_interp = "barycentric" if "wbary" in cname else "nearest"
+    w_interp = w_interp_of(cname)
     st = g.particles()
     if "elem0" in c:   # elem_search: walk
         st = st.replace(elem=c["elem0"].copy())

@@ -23,6 +23,9 @@ CASES += [("golden_3d", c) for c in ("rk2_wnear", "rk2_wbary", "rk2_wbary_kick",
                                      "rk4_wnear_walk_kick")]
 CASES += [("golden_dl_lev", c) for c in ("rk2_lev_wbary", "rk4_lev_wnear_kick", "euler_lev_wnear", "rk2_lev_wbary_azc")]
 CASES += [("golden_dl_llin", c) for c in ("rk2_llin_wbary", "rk4_llin_wnear_kick", "euler_llin_wnear")]
+# W by least squares and by inverse distance (unfused reference steps)
+CASES += [("golden_wring", c) for c in ("rk2_wlsq", "rk4_wlsq_kick", "euler_wlsq", "rk2_wlsq_bwd", "rk2_widw",
+                                        "rk4_widw_kick")]
 # sigma meshes (mesh.vertical_coord "sigma", free surface eta, s = z / H_p)
 SIGMA_CASES = [("golden_sigma", c) for c in ("rk2_wnear", "rk2_wbary", "rk4_wbary", "euler_wbary", "euler_wnear",
                                              "rk2_wbary_kick", "rk4_wnear_kick", "rk2_wnear_bwd",
@@ -32,6 +35,9 @@ SIGMA_CASES += [("golden_sigma_llin", c) for c in ("rk2_llin_wbary", "rk4_llin_w
 SIGMA_CASES += [("golden_sigma_surf", c) for c in ("rk2_wbary_surf", "rk4_wnear_surf", "euler_wbary_surf",
                                                   "rk2_wbary_steady_surf", "rk4_wnear_steady_surf_kick",
                                                   "rk4_wbary_steady_endonly", "rk2_wnear_startonly_kick")]
+# the vertical Az kick on sigma meshes (constant source, end-of-step column)
+SIGMA_CASES += [("golden_sigma_az", c) for c in ("rk2_wbary_azc", "rk4_wnear_kick_azc", "euler_wbary_azc",
+                                                "rk2_wnear_bwd_kick_azc", "rk2_wbary_surf_kick_azc")]
 CASES += SIGMA_CASES
 # NEMO C-grid meshes (uv_interp nemo_cgrid): the 2-D unfused steps and the 3-D fractional-level step
 CGRID_CASES = [("golden_cgrid2d", c) for c in ("rk2", "rk4", "euler", "rk2_bwd", "rk4_steady", "rk2_kick", "rk2_walk")]
@@ -48,6 +54,14 @@ CASES += PCHIP_CASES
 LSQ_CASES = [(f, c) for f in ("golden_lsq_band", "golden_lsq_quad")
              for c in ("rk2", "rk4", "euler", "rk2_bwd", "rk2_kick", "rk4_steady", "rk2_pchip")]
 CASES += LSQ_CASES
+
+
+def w_interp_of(cname):
+    """The recorded case's W method, from its name."""
+    for tag, method in (("wlsq", "leastsq"), ("widw", "idw"), ("wbary", "barycentric")):
+        if tag in cname:
+            return method
+    return "nearest"
 
 
 def uv_interp_of(g):
@@ -88,7 +102,7 @@ def replay_oracle(g, cname):
     c = g.case(cname)
     dt, T, n_steps, td, khx, khy, seed, real_id, pid_off = c["params"]
     scheme = cname.split("_")[0]
-    w_interp = "barycentric" if "wbary" in cname else "nearest"
+    w_interp = w_interp_of(cname)
     st = g.particles()
     if "elem0" in c:   # elem_search: walk
         st = st.replace(elem=c["elem0"].copy())
