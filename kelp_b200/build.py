@@ -23,7 +23,7 @@ BUILD = os.path.join(ROOT, "_build")
 LIB = os.path.join(HERE, "libkelpcuda.so")
 
 CU_SOURCES = ["kc_api.cu", "kc_plain_f64.cu", "kc_plain_f32.cu", "kc_mixed_f32.cu", "kc_mixed_f16.cu",
-              "kc_cgrid_f64.cu", "kc_cgrid_f32.cu", "kc_cgrid_mixed.cu", "kc_sigma.cu"]
+              "kc_cgrid_f64.cu", "kc_cgrid_f32.cu", "kc_cgrid_mixed.cu", "kc_sigma.cu", "kc_lsq.cu"]
 CPP_SOURCES = ["kc_host.cpp", "kc_rngx.cpp"]
 RNGX = os.path.join(BUILD, "kc_rng_exceptions.bin")
 HEADERS = ["kc_geom.cuh", "kc_interp.cuh", "kc_step.cuh", "kc_beach.cuh", "kc_mixed.cuh", "kc_kernels.cuh", "kc_sigma.cuh",

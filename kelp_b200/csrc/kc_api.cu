@@ -770,6 +770,13 @@ int fetch(kc_ctx* c, void* host, const void* dev, int es) {
     return KC_OK;
 }
 
+// Row stride of a step's snapshot slots: nodes; element-centre u/v in 2-D:
+// elements; 3-D element-centre u/v (K-1, E) with node w (K, N): max(E, N).
+long long lsq_stride(const kc_ctx* c, const kc_step_args* a) {
+    if (!a->uv_lsq) return c->N;
+    return a->dims == 3 ? std::max(c->E, c->N) : c->E;
+}
+
 template <typename T>
 kc::DBlend<T> blend_of(kc_ctx* c, const kc_step_args* a) {
     kc::DBlend<T> f;
@@ -777,7 +784,7 @@ kc::DBlend<T> blend_of(kc_ctx* c, const kc_step_args* a) {
     f.b = field_of<T>(c->slots[a->slot_b]);
     f.t = field_of<T>(c->slots[a->slot_t]);
     f.alpha0 = a->alpha0;
-    f.n = a->uv_lsq ? c->E : c->N;
+    f.n = lsq_stride(c, a);
     f.pchip = a->pchip ? 1 : 0;
     f.d = a->pchip ? field_of<T>(c->slots[a->slot_d]) : kc::DField<T>{};
     for (int k = 0; k < 4; ++k) f.pt[k] = a->pchip ? a->pchip_t[k] : 0.0;
@@ -832,8 +839,8 @@ int launch_step_on(kc_ctx* c, const kc_step_args* a, const kc::DState& st, const
         if (dtype == KC_F32) kc_launch_cgrid_f32(c->dm, blend_of<float>(c, a), st, s, a->dims, a->scheme, c->stream);
         else kc_launch_cgrid_f64(c->dm, blend_of<double>(c, a), st, s, a->dims, a->scheme, c->stream);
     } else if (a->uv_lsq) {   // element-layout u/v: 2-D least squares (plain form)
-        if (dtype == KC_F32) kc_launch_lsq_f32(c->dm, blend_of<float>(c, a), st, s, a->scheme, c->stream);
-        else kc_launch_lsq_f64(c->dm, blend_of<double>(c, a), st, s, a->scheme, c->stream);
+        if (dtype == KC_F32) kc_launch_lsq_f32(c->dm, blend_of<float>(c, a), st, s, a->dims, a->scheme, c->stream);
+        else kc_launch_lsq_f64(c->dm, blend_of<double>(c, a), st, s, a->dims, a->scheme, c->stream);
     } else if (c->dm.sig && a->dims == 3) {   // sigma meshes: the plain form's s = z / H_p step
         kc::DStep ss = s;
         ss.eta_s = c->sig_s_on ? c->d_sig_eta_s : nullptr;
@@ -875,7 +882,8 @@ int check_step(kc_ctx* c, const kc_step_args* a) {
         return fail(c, KC_ERR_ARG, "kc_step: precision must be KC_PLAIN or KC_MIXED");
     if (a->uv_lsq) {
         if (a->uv_lsq != 1) return fail(c, KC_ERR_ARG, "kc_step: uv_lsq must be 0 or 1");
-        if (a->dims != 2) return fail(c, KC_ERR_ARG, "kc_step: least-squares u/v is built for 2-D steps");
+        if (a->dims == 3 && (a->uv_vertical != 0 || c->dm.sig))
+            return fail(c, KC_ERR_ARG, "kc_step: 3-D least-squares u/v is built for layer fields on z-level meshes");
         if (a->precision != KC_PLAIN) return fail(c, KC_ERR_ARG, "kc_step: least-squares u/v runs in the plain form");
         if (c->dm.cg.on) return fail(c, KC_ERR_ARG, "kc_step: C-grid meshes read face velocities, not element centres");
         if (!c->dm.ec) return fail(c, KC_ERR_STATE, "kc_step: least-squares u/v needs kc_elem_centers_upload");
@@ -952,8 +960,9 @@ int check_step(kc_ctx* c, const kc_step_args* a) {
         if (sl[k] < 0 || sl[k] >= kSlots) return fail(c, KC_ERR_ARG, "kc_step: slot out of range");
         const Slot& s = c->slots[sl[k]];
         if (s.dtype < 0) return fail(c, KC_ERR_STATE, "kc_step: snapshot slot " + std::to_string(sl[k]) + " is empty");
-        if (s.n != (a->uv_lsq ? c->E : c->N))
-            return fail(c, KC_ERR_ARG, a->uv_lsq ? "kc_step: least-squares u/v snapshots hold one value per element"
+        if (s.n != lsq_stride(c, a))
+            return fail(c, KC_ERR_ARG, a->uv_lsq ? "kc_step: least-squares u/v snapshots hold one value per element "
+                                                   "(3-D: u/v and w rows of stride max(E, N))"
                                                  : "kc_step: snapshot node count differs from the mesh");
         if (dtype >= 0 && s.dtype != dtype) return fail(c, KC_ERR_ARG, "kc_step: snapshots of mixed element types");
         dtype = s.dtype;

@@ -917,7 +917,7 @@ static __device__ __noinline__ int walk_locate(const DMesh& m, double lon_p, dou
 // take the four-record value per element (the _pchip4 twin, :355-474).
 template <typename T>
 __device__ __forceinline__ bool interp_uv_lsq(const DMesh& m, const DBlend<T>& f, double xp, double yp, int nn,
-                                              double time_dir, double alpha, double& U, double& V) {
+                                              double time_dir, double alpha, double& U, double& V, int row = 0) {
     U = 0.0;
     V = 0.0;
     const int s0 = __ldg(&m.n2e_off[nn]), s1 = __ldg(&m.n2e_off[nn + 1]);
@@ -935,13 +935,16 @@ __device__ __forceinline__ bool interp_uv_lsq(const DMesh& m, const DBlend<T>& f
         if (dlon_raw > 180.0) ex -= 360.0 * z0;
         else if (dlon_raw < -180.0) ex += 360.0 * z0;
         const double ey = c.y * SLM - yp_m;
+        const long long idx = (long long)row * f.n + e;   // row: the layer of a 3-D field
         double uv, vv;
         if (f.pchip) {
-            uv = pchip_at(f.a.u, f.b.u, f.t.u, f.d.u, e, f.pt, alpha);
-            vv = pchip_at(f.a.v, f.b.v, f.t.v, f.d.v, e, f.pt, alpha);
+            uv = pchip_at(f.a.u, f.b.u, f.t.u, f.d.u, idx, f.pt, alpha);
+            vv = pchip_at(f.a.v, f.b.v, f.t.v, f.d.v, idx, f.pt, alpha);
         } else {
-            uv = tblend((double)__ldg(&f.a.u[e]), (double)__ldg(&f.b.u[e]), (double)__ldg(&f.t.u[e]), f.alpha0, alpha);
-            vv = tblend((double)__ldg(&f.a.v[e]), (double)__ldg(&f.b.v[e]), (double)__ldg(&f.t.v[e]), f.alpha0, alpha);
+            uv = tblend((double)__ldg(&f.a.u[idx]), (double)__ldg(&f.b.u[idx]), (double)__ldg(&f.t.u[idx]), f.alpha0,
+                        alpha);
+            vv = tblend((double)__ldg(&f.a.v[idx]), (double)__ldg(&f.b.v[idx]), (double)__ldg(&f.t.v[idx]), f.alpha0,
+                        alpha);
         }
         const double uu = time_dir * uv, vw = time_dir * vv;
         a11 = a11 + 1.0;

@@ -43,6 +43,6 @@ void kc_launch_sigma_f64(const kc::DMesh& m, const kc::DBlend<double>& f, const 
 void kc_launch_sigma_f32(const kc::DMesh& m, const kc::DBlend<float>& f, const kc::DState& st, const kc::DStep& s,
                          int scheme, cudaStream_t stream);
 void kc_launch_lsq_f64(const kc::DMesh& m, const kc::DBlend<double>& f, const kc::DState& st, const kc::DStep& s,
-                       int scheme, cudaStream_t stream);
+                       int dims, int scheme, cudaStream_t stream);
 void kc_launch_lsq_f32(const kc::DMesh& m, const kc::DBlend<float>& f, const kc::DState& st, const kc::DStep& s,
-                       int scheme, cudaStream_t stream);
+                       int dims, int scheme, cudaStream_t stream);

@@ -1,5 +1,4 @@
-// The sigma-mesh 3-D steps and the element-centre least-squares 2-D steps
-// (plain form) on float64 and float32 snapshots.
+// The sigma-mesh 3-D steps (plain form) on float64 and float32 snapshots.
 #include "kc_launch.h"
 
 void kc_launch_sigma_f64(const kc::DMesh& m, const kc::DBlend<double>& f, const kc::DState& st, const kc::DStep& s,
@@ -10,14 +9,4 @@ void kc_launch_sigma_f64(const kc::DMesh& m, const kc::DBlend<double>& f, const 
 void kc_launch_sigma_f32(const kc::DMesh& m, const kc::DBlend<float>& f, const kc::DState& st, const kc::DStep& s,
                          int scheme, cudaStream_t stream) {
     launch_sigma_kernel<float>(m, f, st, s, scheme, stream);
-}
-
-void kc_launch_lsq_f64(const kc::DMesh& m, const kc::DBlend<double>& f, const kc::DState& st, const kc::DStep& s,
-                       int scheme, cudaStream_t stream) {
-    launch_lsq_kernel<double>(m, f, st, s, scheme, stream);
-}
-
-void kc_launch_lsq_f32(const kc::DMesh& m, const kc::DBlend<float>& f, const kc::DState& st, const kc::DStep& s,
-                       int scheme, cudaStream_t stream) {
-    launch_lsq_kernel<float>(m, f, st, s, scheme, stream);
 }

@@ -461,6 +461,10 @@ struct UnfusedFormOf {
     using type = Form;
 };
 
+// 3-D (interpolate.py:644-750 interp_leastsq with the per-particle layer of
+// _compute_layers): the same fit on the layer's row of element values, W of
+// the nodes by the step's W method.  A 3-D field's u/v (K-1, E) and w (K, N)
+// rows share one stride, max(E, N).
 template <typename T>
 struct LsqForm {
     static constexpr bool kExact = true;
@@ -468,6 +472,15 @@ struct LsqForm {
     static __device__ __forceinline__ bool uv2(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
                                                double lat, int nn, int hint, double alpha, double& U, double& V) {
         return interp_uv_lsq<T>(m, f, lon, lat, nn, s.time_dir, alpha, U, V);
+    }
+    static __device__ __forceinline__ bool uvw3(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
+                                                double lat, int nn, int hint, int whint, double z, double alpha,
+                                                double& U, double& V, double& W) {
+        const bool ok = interp_uv_lsq<T>(m, f, lon, lat, nn, s.time_dir, alpha, U, V, find_layer(m, z, nn));
+        if (s.w_code == 0) W = w_linear<T>(m, f, alpha, z, nn, s.time_dir);
+        else if (s.w_code == 1) W = w_bary<T>(m, f, alpha, lon, lat, z, nn, s.time_dir);
+        else W = w_ring<T>(m, f, s.w_code, alpha, lon, lat, z, nn, s.time_dir);
+        return ok;
     }
 };
 

@@ -24,6 +24,22 @@ def _c(a, dtype):
     return np.ascontiguousarray(a, dtype=dtype)
 
 
+def _pad_to(a, n):
+    """``a`` with its last axis zero-padded to ``n`` (unchanged when it is)."""
+    if a.shape[-1] == n:
+        return a
+    return np.ascontiguousarray(np.pad(a, [(0, 0)] * (a.ndim - 1) + [(0, n - a.shape[-1])]))
+
+
+def _shared_stride(u, v, w):
+    """3-D element-layout u/v (K-1, E) with node w (K, N): both padded to the
+    row stride max(E, N) the least-squares kernels read them with."""
+    if w is None or w.ndim != 2 or u.shape[-1] == w.shape[-1]:
+        return u, v, w
+    n = max(u.shape[-1], w.shape[-1])
+    return _pad_to(u, n), _pad_to(v, n), _pad_to(w, n)
+
+
 def mesh_desc(mesh, keep: list) -> N.MeshDesc:
     """Fill the C mesh descriptor from a mesh (duck-typed: a kelp_b200 Mesh or
     KELP's own ``kelp.core.mesh.Mesh`` after ``build_search``).  Arrays that
@@ -227,6 +243,7 @@ class DeviceContext:
         u = _c(u, host)
         v = _c(v, host)
         w = None if w is None else _c(w, host)
+        u, v, w = _shared_stride(u, v, w)
         n = u.shape[-1]
         rows = 1 if u.ndim == 1 else u.shape[0]
         wrows = 0 if w is None else (1 if w.ndim == 1 else w.shape[0])
@@ -241,7 +258,7 @@ class DeviceContext:
             self._chk(N.lib().kc_field_upload_eta(self._ctx, slot, n, N.ptr(eta)), "kc_field_upload_eta")
         az = getattr(field, "az", None)
         if az is not None and code != N.KC_F16:
-            az = _c(np.asarray(az), host)
+            az = _pad_to(_c(np.asarray(az), host), n)
             self._chk(N.lib().kc_field_upload_az(self._ctx, slot, code, n, 1 if az.ndim == 1 else az.shape[0],
                                                  N.ptr(az)), "kc_field_upload_az")
         self.synchronize()
@@ -276,6 +293,7 @@ class DeviceContext:
             u = _c(np.asarray(f.u), dtype)
             v = _c(np.asarray(f.v), dtype)
             w = None if getattr(f, "w", None) is None else _c(np.asarray(f.w), dtype)
+            u, v, w = _shared_stride(u, v, w)
             code = N.KC_F32 if dtype == np.dtype(np.float32) else N.KC_F64
             rows = 1 if u.ndim == 1 else u.shape[0]
             wrows = 0 if w is None else (1 if w.ndim == 1 else w.shape[0])

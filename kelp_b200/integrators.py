@@ -116,17 +116,26 @@ def _check_node_fields(mesh, fields, is3d, placement="layer"):
                                  "(integrators.py:4534-4553)")
 
 
-def _check_element_fields(mesh, fields):
-    """2-D element-layout u/v for the least-squares stages: one value per
-    element (io.py:180 VelocityField, uv_layout 'element')."""
+def _check_element_fields(mesh, fields, is3d=False):
+    """Element-layout u/v for the least-squares stages: one value per element
+    (io.py:180 VelocityField, uv_layout 'element'), per layer in 3-D with W on
+    the nodes' interfaces."""
     E = np.asarray(mesh.elem_nodes).shape[0]
+    n = np.asarray(mesh.nodes_lon).shape[0]
+    K = np.asarray(mesh.sigma).shape[0]
     for f in fields:
         if getattr(f, "uv_layout", "element") != "element":
             raise ValueError("uv_interp 'leastsq' reads element-centre velocities (uv_layout='element'), "
                              f"got uv_layout={getattr(f, 'uv_layout', None)!r}")
         u = np.asarray(f.u)
-        if u.shape != (E,) or np.asarray(f.v).shape != u.shape:
-            raise ValueError(f"2-D element-layout u/v need shape ({E},), got {u.shape}")
+        if not is3d:
+            if u.shape != (E,) or np.asarray(f.v).shape != u.shape:
+                raise ValueError(f"2-D element-layout u/v need shape ({E},), got {u.shape}")
+            continue
+        w = np.asarray(f.w)
+        if u.shape != (K - 1, E) or np.asarray(f.v).shape != u.shape or w.shape != (K, n):
+            raise ValueError(f"3-D element-layout fields need u/v ({K - 1}, {E}) and w ({K}, {n}); got {u.shape} "
+                             f"and {w.shape}")
 
 
 def _az_args(diffusion, vel, is3d, mesh):
@@ -278,9 +287,9 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
         raise NotImplementedError(f"uv_interp={uv_interp!r} is not built on the CUDA backend; "
                                   "use 'barycentric' (node-layout velocities) or 'leastsq' (2-D element layout)")
     if lsq:
-        if _is_3d(vel):
-            raise NotImplementedError("uv_interp 'leastsq' is built for 2-D steps on the CUDA backend "
-                                      "(the 3-D element-layout kernels are not)")
+        if _is_3d(vel) and (getattr(vel, "uv_vertical", "layer") != "layer" or _sigma_mesh(mesh)):
+            raise NotImplementedError("3-D uv_interp 'leastsq' is built for layer fields on z-level meshes on the "
+                                      "CUDA backend (depth-linear element fields and sigma meshes are not)")
         if elem is not None:
             raise NotImplementedError("uv_interp 'leastsq' reads no containing element: elem_search 'walk' "
                                       "does not apply to it on the CUDA backend")
@@ -343,7 +352,7 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
             vel = _materialized(vel)
     vel_a, vel_b, target, alpha0 = _fields(vel, vel_next)
     if lsq:
-        _check_element_fields(mesh, [vel_a, vel_b, target] + (list(recon[0]) if recon is not None else []))
+        _check_element_fields(mesh, [vel_a, vel_b, target] + (list(recon[0]) if recon is not None else []), is3d)
     else:
         _check_node_fields(mesh, [vel_a, vel_b, target] + (list(recon[0]) if recon is not None else []), is3d,
                            placement)

@@ -583,8 +583,12 @@ static double blend4(const OField* f, const void* a, const void* b, const void* 
  * takes elem_hint. */
 static _Thread_local int t_elem_hint = -1;
 
+static int interp_lsq(const OMesh* m, const OField* f, double xp, double yp, int nn, double td, int row,
+                      double alpha, double* U, double* V);
+
 static int interp_uv(const OMesh* m, const OField* f, double xp, double yp, int nn, double td, int row,
                      double alpha, double* U, double* V) {
+    if (f->lsq) return interp_lsq(m, f, xp, yp, nn, td, row, alpha, U, V);   /* element-layout u/v, row = layer */
     *U = 0.0; *V = 0.0;
     int elem = t_elem_hint >= 0 ? t_elem_hint : contain_local(m, xp, yp, nn);
     if (elem < 0) return 0;
@@ -1406,8 +1410,8 @@ static void step_cgrid3d(const OMesh* m, const OField* f, const OStep* s, int64_
  * element-centre velocities (metres, centred on the particle, the seam gate
  * on the raw longitude difference), Cramer's rule, its value a0 at the
  * particle; 0 for an empty ring or a singular normal matrix. */
-static int interp_lsq(const OMesh* m, const OField* f, double xp, double yp, int nn, double td, double alpha,
-                      double* U, double* V) {
+static int interp_lsq(const OMesh* m, const OField* f, double xp, double yp, int nn, double td, int row,
+                      double alpha, double* U, double* V) {
     *U = 0.0; *V = 0.0;
     int count = m->n2e_cnt[nn];
     if (count < 1) return 0;
@@ -1421,8 +1425,9 @@ static int interp_lsq(const OMesh* m, const OField* f, double xp, double yp, int
         if (raw > 180.0) ex -= 360.0 * z0;
         else if (raw < -180.0) ex += 360.0 * z0;
         double ey = m->ec_lat[e] * SLM - yp_m;
-        double uu = td * blend4(f, f->ua, f->ub, f->ut, f->ud, e, alpha);
-        double vv = td * blend4(f, f->va, f->vb, f->vt, f->vd, e, alpha);
+        int64_t idx = (int64_t)row * f->n + e;
+        double uu = td * blend4(f, f->ua, f->ub, f->ut, f->ud, idx, alpha);
+        double vv = td * blend4(f, f->va, f->vb, f->vt, f->vd, idx, alpha);
         s11 = s11 + 1.0; s12 = s12 + ex; s13 = s13 + ey;
         s22 = s22 + ex * ex; s23 = s23 + ex * ey; s33 = s33 + ey * ey;
         fu = fu + uu; fu1 = fu1 + uu * ex; fu2 = fu2 + uu * ey;
@@ -1444,7 +1449,7 @@ static int interp_lsq(const OMesh* m, const OField* f, double xp, double yp, int
  * squares, else the barycentric core */
 static int uv2(const OMesh* m, const OField* f, double xp, double yp, int nn, double td, double alpha, double* U,
                double* V) {
-    if (f->lsq) return interp_lsq(m, f, xp, yp, nn, td, alpha, U, V);
+    if (f->lsq) return interp_lsq(m, f, xp, yp, nn, td, 0, alpha, U, V);
     if (m->cg) {
         double Wd;
         int h = t_elem_hint;

@@ -244,11 +244,21 @@ def step(state, vel, mesh, dt, time_dir, scheme: str, *, vel_next=None, dt_to_ne
     of.f32 = 1 if all32 else 0
     of.alpha0 = alpha0
     of.n = view.lon.size
-    if uv_interp == "leastsq":   # 2-D element-centre u/v (interpolate.py:52-354)
+    if uv_interp == "leastsq":   # element-centre u/v (interpolate.py:52-354, 644-750)
         if view.ec_lon is None:
             raise ValueError("uv_interp 'leastsq' needs the mesh's element centres")
         of.lsq = 1
         of.n = view.ec_lon.size
+        if arrs[0][2] is not None:   # 3-D: u/v (K-1, E) and w (K, N) share the stride max(E, N)
+            S = max(view.ec_lon.size, view.lon.size)
+            pad = lambda x: None if x is None else np.ascontiguousarray(
+                np.pad(x, [(0, 0)] * (x.ndim - 1) + [(0, S - x.shape[-1])]))
+            arrs = [tuple(pad(x) for x in a) for a in arrs]
+            (of.ua, of.va, of.wa), (of.ub, of.vb, of.wb), (of.ut, of.vt, of.wt) = [tuple(_p(x) for x in a)
+                                                                                    for a in arrs[:3]]
+            if use_recon:
+                of.ud, of.vd, of.wd = (_p(x) for x in arrs[3])
+            of.n = S
     elif uv_interp != "barycentric":
         raise ValueError(f"uv_interp {uv_interp!r}: the oracle restates 'barycentric' and 'leastsq'")
     etas = [np.ascontiguousarray(getattr(f, "eta", None) if getattr(f, "eta", None) is not None
@@ -306,6 +316,9 @@ def step(state, vel, mesh, dt, time_dir, scheme: str, *, vel_next=None, dt_to_ne
             if have:
                 os_.az_field = 1
                 keep_az = [np.ascontiguousarray(az_a, dtype=dtype), np.ascontiguousarray(az_b, dtype=dtype)]
+                if of.lsq and of.n != view.lon.size:   # the shared stride of 3-D element-layout fields
+                    keep_az = [np.ascontiguousarray(np.pad(a, [(0, 0)] * (a.ndim - 1) + [(0, of.n - a.shape[-1])]))
+                               for a in keep_az]
                 of.aza, of.azb = _p(keep_az[0]), _p(keep_az[1])
     P = state.lon.shape[0]
     out = {"lon": np.array(state.lon, dtype=np.float64), "lat": np.array(state.lat, dtype=np.float64),

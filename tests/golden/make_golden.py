@@ -959,6 +959,44 @@ def lsq_fixture():
         save(name, rec, rf, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
 
 
+def lsq3d_fixture():
+    """3-D element-layout u/v with the element-centre least squares per layer
+    (uv_interp "leastsq", interpolate.py:644-750 with the layer of
+    integrators.py _compute_layers), node W, through the reference's unfused
+    3-D steps: the z-level mesh of golden_3d, element velocities the mean of
+    the vertex gyre values of each layer; W nearest / barycentric / least
+    squares, RK2 / RK4 / Euler, kick, backward, PCHIP.
+    tests/golden/golden_lsq3d.npz."""
+    T = 86400.0
+    zl = S.stretched_levels(12, 5.0, 4000.0)
+    m = S.lattice_mesh(3.0, 60.0, jitter=0.2, land_frac=0.25,
+                       depth=lambda lo, la: S.smooth_bathymetry(lo, la, 30.0, 4000.0), sigma=zl)
+    rm = ref_mesh(m, sigma=zl)
+    en = np.asarray(m.elem_nodes)
+    valid = en >= 0
+    rf = []
+    for sn in S.gyre_snapshots(m, 5, amp=1.5, z_levels=zl, decay=800.0, w_scale=2e-3):
+        u, v = np.asarray(sn.u), np.asarray(sn.v)
+        ue = np.where(valid[None], u[:, np.maximum(en, 0)], 0.0).sum(2) / valid.sum(1)[None]
+        ve = np.where(valid[None], v[:, np.maximum(en, 0)], 0.0).sum(2) / valid.sum(1)[None]
+        rf.append(RVel(u=ue.astype(u.dtype), v=ve.astype(v.dtype), w=np.asarray(sn.w), eta=np.zeros(m.n_nodes),
+                       uv_layout="element"))
+    lon, lat, z, status = particles(m, 1200, 53, z=True, n_dead=20)
+    cases = {"rk2_wbary": run_case(rm, rf, lon, lat, z, status, "rk2", 21600.0, T, 10, w_interp="barycentric",
+                                   uv_interp="leastsq"),
+             "rk4_wnear_kick": run_case(rm, rf, lon, lat, z, status, "rk4", 21600.0, T, 10, w_interp="nearest",
+                                        kh=(3.0e4, 3.0e4), seed=5, uv_interp="leastsq"),
+             "euler_wlsq": run_case(rm, rf, lon, lat, z, status, "euler", 10800.0, T, 12, w_interp="leastsq",
+                                    uv_interp="leastsq"),
+             "rk2_wlsq_bwd": run_case(rm, rf, lon, lat, z, status, "rk2", 21600.0, T, 10, w_interp="leastsq",
+                                      time_dir=-1.0, uv_interp="leastsq"),
+             "rk4_wbary_pchip": run_case(rm, rf, lon, lat, z, status, "rk4", 21600.0, T, 8, w_interp="barycentric",
+                                         uv_interp="leastsq", pchip=True, t0=T)}
+    rec = mesh_record(rm)
+    rec.update(elem_center_lon=rm.elem_center_lon, elem_center_lat=rm.elem_center_lat, uv_element=np.array(1))
+    save("golden_lsq3d", rec, rf, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
+
+
 RNG_KEY_SETS = (   # (seed, realization, first particle id, step, component), 2^20 particles each
     (0, 0, 0, 0, 0),
     (20240917, 3, 5_000_000, 1459, 0),
@@ -1187,7 +1225,7 @@ def reftypes_fixture():
 
 if __name__ == "__main__":
     # no argument: every fixture; otherwise the named ones ("steps", "beach", ...)
-    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq", "rng1m", "tripolar", "reftypes", "sample", "cellrule", "lazy0", "sigma_surf", "eta_time", "sigma_az", "wring"}
+    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq", "rng1m", "tripolar", "reftypes", "sample", "cellrule", "lazy0", "sigma_surf", "eta_time", "sigma_az", "wring", "lsq3d"}
     if "rng1m" in which:
         rng1m_fixture()
     if "reftypes" in which:
@@ -1206,6 +1244,8 @@ if __name__ == "__main__":
         sigma_az_fixture()
     if "wring" in which:
         wring_fixture()
+    if "lsq3d" in which:
+        lsq3d_fixture()
     if "lsq" in which:
         lsq_fixture()
     if "steps" in which:

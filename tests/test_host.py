@@ -140,3 +140,17 @@ def test_autotune_cache_roundtrip(tmp_path, monkeypatch, golden):
     assert key.startswith("N") and "-d2-rk2-plain-P512" in key
     autotune._store({key: {"block": 256, "steps_per_launch": 6, "sort_every": 12}})
     assert autotune._load()[key]["block"] == 256
+
+
+def test_shared_stride_of_3d_element_fields():
+    """3-D element-layout u/v (K-1, E) and node w (K, N) upload with one row
+    stride, max(E, N); node-layout fields pass through unchanged."""
+    from kelp_b200.device import _shared_stride
+    u, w = np.arange(30.0).reshape(3, 10), np.arange(24.0).reshape(4, 6)
+    u2, v2, w2 = _shared_stride(u, u + 1.0, w)
+    assert u2.shape == (3, 10) and v2.shape == (3, 10) and w2.shape == (4, 10)
+    assert np.array_equal(w2[:, :6], w) and not w2[:, 6:].any() and np.array_equal(u2, u)
+    u3, _, w3 = _shared_stride(np.ones((3, 4)), np.ones((3, 4)), np.ones((4, 9)))
+    assert u3.shape == (3, 9) and w3.shape == (4, 9)
+    n = np.ones((3, 5))
+    assert _shared_stride(n, n, np.ones((4, 5)))[0] is n

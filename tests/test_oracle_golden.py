@@ -54,6 +54,10 @@ CASES += PCHIP_CASES
 LSQ_CASES = [(f, c) for f in ("golden_lsq_band", "golden_lsq_quad")
              for c in ("rk2", "rk4", "euler", "rk2_bwd", "rk2_kick", "rk4_steady", "rk2_pchip")]
 CASES += LSQ_CASES
+# 3-D element-layout u/v by least squares per layer, node W (the unfused reference steps)
+LSQ_CASES += [("golden_lsq3d", c) for c in ("rk2_wbary", "rk4_wnear_kick", "euler_wlsq", "rk2_wlsq_bwd",
+                                            "rk4_wbary_pchip")]
+CASES += LSQ_CASES[-5:]
 
 
 def w_interp_of(cname):
