@@ -54,6 +54,25 @@ def env_rank():
     return r, w, lr
 
 
+def shard_pid_base(rank: int, particles_per_rank: int) -> int:
+    """The first global particle key of a rank's shard.  Ranks hold
+    consecutive key ranges, so N ranks of P particles draw exactly the random
+    numbers one run of N x P particles draws (the counter RNG is keyed by the
+    global particle index): weak scaling with no data-path exchange."""
+    return int(rank) * int(particles_per_rank)
+
+
+def max_over_ranks(value: float, dist, device) -> float:
+    """The maximum of a per-rank time over all ranks (the job's time); the
+    value itself on one process."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -550,12 +569,7 @@ def _time_batched(ctx, wl, slots, form, args, pid_base, barrier, dist, local):
     autotune.run_window(ctx, make_steps, args.warmup, K, spl, se)
     ctx.record(1)
     barrier()
-    total = ctx.elapsed_ms(0, 1)
-    if dist is not None:
-        import torch
-        t = torch.tensor([total], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total = float(t.item())
+    total = max_over_ranks(ctx.elapsed_ms(0, 1), dist, f"cuda:{local}")
     launches = (K + spl - 1) // spl + 15 * ((K + se - 1) // se)
     return {"total_ms": total, "kernel_ms": total / K, "sort_ms": 0.0, "launches": launches,
             "errors": ctx.device_errors(),
@@ -598,7 +612,7 @@ def run_b200(args):
     if any(FORMS[f][1] is np.float16 for f in forms):
         slots["f16"] = ctx.slots_for(wl.snaps, np.float16)
     P = wl.P
-    pid_base = rank * P
+    pid_base = shard_pid_base(rank, P)
 
     def barrier():
         if dist is not None:
@@ -637,12 +651,7 @@ def run_b200(args):
             if args.sort_every > 0 and j % args.sort_every == 0:
                 sort_ms.append(ctx.elapsed_ms(0, 2))
         barrier()
-        total = float(sum(step_ms))
-        if dist is not None:
-            import torch
-            t = torch.tensor([total], dtype=torch.float64, device=f"cuda:{local}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total = float(t.item())
+        total = max_over_ranks(float(sum(step_ms)), dist, f"cuda:{local}")
         timed[form] = {"total_ms": total, "kernel_ms": (sum(step_ms) - sum(sort_ms)) / len(step_ms),
                        "sort_ms": float(sum(sort_ms)), "launches": launches, "errors": ctx.device_errors()}
     t_wall1 = time.time()
@@ -681,12 +690,7 @@ def run_b200(args):
         src, dst = bufs[k % 2], bufs[(k + 1) % 2]
         ctx.step_host(e2e_args(k), {n: src[n] for n in names_in}, dst)
     ctx.record(3)
-    e2e_ms = ctx.elapsed_ms(2, 3)
-    if dist is not None:
-        import torch
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(ctx.elapsed_ms(2, 3), dist, f"cuda:{local}")
     h2d = P * (8 + 8 + 8 + 4 + 4 + 1)
     d2h = P * (8 * 6 + 4 + 4 + 1)
 
