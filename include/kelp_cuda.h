@@ -109,7 +109,8 @@ typedef struct kc_step_args {
     double dt;                   /* seconds, > 0 */
     double time_dir;             /* +1 forward, -1 backward */
     int w_code;                  /* 3-D W: 0 nearest, 1 barycentric, 2 least squares, 3 inverse distance
-                                    (2 and 3: plain form, z-level meshes; vertical.py:493-601, :1148-1229) */
+                                    (2 and 3: plain form; vertical.py:493-601, :1148-1229, and on sigma
+                                    meshes vertical_sigma.py:493-563, :656-905) */
     int uv_vertical;             /* 3-D u/v: 0 layer (K-1 rows), 1 depth-linear (the table's M rows) */
     int kick;                    /* split uniform-Kh random walk on/off */
     double kh_x, kh_y;           /* m^2/s */

@@ -874,9 +874,8 @@ int check_step(kc_ctx* c, const kc_step_args* a) {
     if (!(a->dt > 0.0)) return fail(c, KC_ERR_ARG, "kc_step: dt must be > 0");
     if (!(a->time_dir == 1.0 || a->time_dir == -1.0)) return fail(c, KC_ERR_ARG, "kc_step: time_dir must be +-1");
     if (a->w_code < 0 || a->w_code > 3) return fail(c, KC_ERR_ARG, "kc_step: w_code must be 0..3");
-    if (a->w_code >= 2 && (a->precision != KC_PLAIN || c->dm.sig || c->dm.cg.on))
-        return fail(c, KC_ERR_ARG, "kc_step: least-squares / inverse-distance W run in the plain form on z-level "
-                                   "meshes");
+    if (a->w_code >= 2 && (a->precision != KC_PLAIN || c->dm.cg.on))
+        return fail(c, KC_ERR_ARG, "kc_step: least-squares / inverse-distance W run in the plain form");
     if (a->kick && !(a->kh_x >= 0.0 && a->kh_y >= 0.0)) return fail(c, KC_ERR_ARG, "kc_step: Kh must be >= 0");
     if (a->precision != KC_PLAIN && a->precision != KC_MIXED)
         return fail(c, KC_ERR_ARG, "kc_step: precision must be KC_PLAIN or KC_MIXED");

@@ -56,6 +56,68 @@ __device__ __forceinline__ double col_H(const DMesh& m, const DBlend<T>& f, cons
     return H;
 }
 
+// The particle's column height from the anchor's 1-ring of node columns
+// (vertical.py:447-485 order), as the W methods interpolate it: the
+// least-squares plane (w_code 2, vertical_sigma.py:493-531 _H_leastsq_single,
+// floored at Dmin) or the inverse-distance mean (3, :534-563 _H_idw_single;
+// a node within 1 m gives its own column); the anchor's column where the
+// fit fails.
+template <typename T>
+static __device__ __noinline__ double H_ring(const DMesh& m, const DBlend<T>& f, const DStep& s, int slot, double xp,
+                                             double yp, int node) {
+    double z0 = cr::cos_cr(yp * DEG2RAD) * SLM;
+    if (z0 < 1.0) z0 = 1.0;
+    if (s.w_code == 3) {
+        double sw = 0.0, swh = 0.0, hit = 0.0;
+        bool is_hit = false;
+        for_ring(m, node, [&](int nd) {
+            const double h = col_H(m, f, s, nd, slot);
+            const double2 p = __ldg(&m.ll[nd]);
+            const double dx = wrap180(p.x - xp) * z0;
+            const double dy = (p.y - yp) * SLM;
+            const double d2 = dx * dx + dy * dy;
+            if (d2 < 1.0) {
+                is_hit = true;
+                hit = h;
+                return false;
+            }
+            sw += 1.0 / d2;
+            swh += h / d2;
+            return true;
+        });
+        if (is_hit) return hit;
+        if (sw < 1e-30) return col_H(m, f, s, node, slot);
+        return swh / sw;
+    }
+    double a11 = 0.0, a12 = 0.0, a13 = 0.0, a22 = 0.0, a23 = 0.0, a33 = 0.0, fw = 0.0, f1w = 0.0, f2w = 0.0;
+    const int cnt = for_ring(m, node, [&](int nd) {
+        const double h = col_H(m, f, s, nd, slot);
+        const double2 p = __ldg(&m.ll[nd]);
+        const double ex = wrap180(p.x - xp) * z0;
+        const double ey = (p.y - yp) * SLM;
+        a11 += 1.0;
+        a12 += ex;
+        a13 += ey;
+        a22 += ex * ex;
+        a23 += ex * ey;
+        a33 += ey * ey;
+        fw += h;
+        f1w += h * ex;
+        f2w += h * ey;
+        return true;
+    });
+    if (cnt < 3) return col_H(m, f, s, node, slot);
+    const double a21 = a12, a31 = a13, a32 = a23;
+    const double det = a11 * a22 * a33 + a12 * a23 * a31 + a13 * a21 * a32 - a13 * a22 * a31 - a12 * a21 * a33 -
+                       a11 * a23 * a32;
+    if (fabs(det) < 1e-30 || fabs(det) < 1e-12 * fabs(a11 * a22 * a33)) return col_H(m, f, s, node, slot);
+    const double inv = 1.0 / fabs(det);
+    const double b11 = a22 * a33 - a23 * a32, b12 = a13 * a32 - a12 * a33, b13 = a12 * a23 - a13 * a22;
+    double H = (b11 * fw + b12 * f1w + b13 * f2w) * inv;
+    if (H < s.Dmin) H = s.Dmin;
+    return H;
+}
+
 // One evaluation site of the sigma step: the W method's element and vertex
 // weights (vertical_sigma.py:565-632 _bary_locate, nv = 0 for the nearest
 // method or when no element of the anchor contains the point), the vertex
@@ -76,6 +138,10 @@ template <typename T>
 static __device__ __noinline__ void sigma_site(const DMesh& m, const DBlend<T>& f, const DStep& s, int slot,
                                                double xp, double yp, int node, SigSite& q) {
     q.nv = 0;
+    if (s.w_code >= 2) {
+        q.H = H_ring<T>(m, f, s, slot, xp, yp, node);
+        return;
+    }
     if (s.w_code == 1) {
         const int el = w_search_elem(m, xp, yp, node);
         if (el >= 0) {
@@ -160,9 +226,79 @@ __device__ __forceinline__ double sigma_frac(double z, double H) {
 // column at z (:337-360); barycentric = every vertex column at the
 // particle's sigma (:766-816), the own column at min(z, H) outside every
 // element.
+// W by the 1-ring (vertical_sigma.py:656-765 _interp_w_sigma_leastsq_single,
+// :820-905 _interp_w_sigma_idw_single): every node's column sampled at the
+// particle's sigma z / Hp (Hp the site's column by the same method), the
+// plane fit or the inverse-distance mean; the anchor's own column at
+// min(z, H) where the fit fails.
 template <typename T>
-__device__ __forceinline__ double w_sig(const DMesh& m, const DBlend<T>& f, const DStep& s, double alpha, double z,
-                                        int node, const SigSite& q) {
+static __device__ __noinline__ double w_sig_ring(const DMesh& m, const DBlend<T>& f, const DStep& s, int slot,
+                                                 double alpha, double xp, double yp, double z, int node, double Hp) {
+    const double td = s.time_dir;
+    auto own = [&]() {
+        const double H = col_H(m, f, s, node, slot);
+        return w_at(f, alpha, sig_locate(m, z < H ? z : H, H), node, td);
+    };
+    double z0 = cr::cos_cr(yp * DEG2RAD) * SLM;
+    if (z0 < 1.0) z0 = 1.0;
+    const double fr = sigma_frac(z, Hp);
+    if (s.w_code == 3) {
+        double sw = 0.0, swv = 0.0, hit = 0.0;
+        bool is_hit = false;
+        for_ring(m, node, [&](int nd) {
+            const double H = col_H(m, f, s, nd, slot);
+            const double wv = w_at(f, alpha, sig_locate(m, fr * H, H), nd, td);
+            const double2 p = __ldg(&m.ll[nd]);
+            const double dx = wrap180(p.x - xp) * z0;
+            const double dy = (p.y - yp) * SLM;
+            const double d2 = dx * dx + dy * dy;
+            if (d2 < 1.0) {
+                is_hit = true;
+                hit = wv;
+                return false;
+            }
+            const double wt = 1.0 / d2;
+            sw += wt;
+            swv += wt * wv;
+            return true;
+        });
+        if (is_hit) return hit;
+        if (sw < 1e-30) return own();
+        return swv / sw;
+    }
+    double a11 = 0.0, a12 = 0.0, a13 = 0.0, a22 = 0.0, a23 = 0.0, a33 = 0.0, fw = 0.0, f1w = 0.0, f2w = 0.0;
+    const int cnt = for_ring(m, node, [&](int nd) {
+        const double H = col_H(m, f, s, nd, slot);
+        const double wv = w_at(f, alpha, sig_locate(m, fr * H, H), nd, td);
+        const double2 p = __ldg(&m.ll[nd]);
+        const double ex = wrap180(p.x - xp) * z0;
+        const double ey = (p.y - yp) * SLM;
+        a11 += 1.0;
+        a12 += ex;
+        a13 += ey;
+        a22 += ex * ex;
+        a23 += ex * ey;
+        a33 += ey * ey;
+        fw += wv;
+        f1w += wv * ex;
+        f2w += wv * ey;
+        return true;
+    });
+    if (cnt < 3) return own();
+    const double a21 = a12, a31 = a13, a32 = a23;
+    const double det = a11 * a22 * a33 + a12 * a23 * a31 + a13 * a21 * a32 - a13 * a22 * a31 - a12 * a21 * a33 -
+                       a11 * a23 * a32;
+    if (fabs(det) < 1e-30 || fabs(det) < 1e-12 * fabs(a11 * a22 * a33)) return own();
+    const double inv = 1.0 / fabs(det);
+    const double b11 = a22 * a33 - a23 * a32, b12 = a13 * a32 - a12 * a33, b13 = a12 * a23 - a13 * a22;
+    return (b11 * fw + b12 * f1w + b13 * f2w) * inv;
+}
+
+template <typename T>
+__device__ __forceinline__ double w_sig(const DMesh& m, const DBlend<T>& f, const DStep& s, int slot, double xp,
+                                        double yp, double z, int node, const SigSite& q) {
+    const double alpha = slot == 4 ? s.alpha_end : s.ak[slot];
+    if (s.w_code >= 2) return w_sig_ring<T>(m, f, s, slot, alpha, xp, yp, z, node, q.H);
     if (q.nv == 0) {
         const double zc = (s.w_code == 0 || z < q.H) ? z : q.H;
         return w_at(f, alpha, sig_locate(m, zc, q.H), node, s.time_dir);
@@ -211,12 +347,13 @@ __device__ __forceinline__ double sfrac_uv(double z, double H) {
 // (vertical_uv.py:196-211); hint >= 0 is the edge walk's element.
 template <typename T>
 __device__ __forceinline__ bool sig_stage(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon, double lat,
-                                          int nn, int hint, double z, double alpha, const SigSite& q, double& U,
+                                          int nn, int hint, double z, int slot, const SigSite& q, double& U,
                                           double& V, double& W) {
+    const double alpha = s.ak[slot];
     bool ok;
     if (s.uv_dl) ok = interp_uv_bary_dl<T>(m, f, lon, lat, nn, hint, sfrac_uv(z, q.H), s.time_dir, alpha, U, V);
     else ok = interp_uv_bary<T>(m, f, lon, lat, nn, hint, s.time_dir, find_layer_sig(m, z, q.H, s.Dmin), alpha, U, V);
-    W = w_sig<T>(m, f, s, alpha, z, nn, q);
+    W = w_sig<T>(m, f, s, slot, lon, lat, z, nn, q);
     return ok;
 }
 
@@ -248,7 +385,7 @@ __device__ __forceinline__ void step3d_sigma_particle(const DMesh& m, const DBle
     SigSite c1;
     sigma_site<T>(m, f, s, 0, lon0, lat0, node_i, c1);
     double U1, V1, W1;
-    bool ok = sig_stage<T>(m, f, s, lon0, lat0, node_i, e1, z0p, s.ak[0], c1, U1, V1, W1);
+    bool ok = sig_stage<T>(m, f, s, lon0, lat0, node_i, e1, z0p, 0, c1, U1, V1, W1);
     st.U[i] = U1;
     st.V[i] = V1;
     st.W[i] = W1;
@@ -269,7 +406,7 @@ __device__ __forceinline__ void step3d_sigma_particle(const DMesh& m, const DBle
             sigma_site<T>(m, f, s, 1, lm, tm, nm, c2);
             const double zm = s_mid * c2.H;
             double U2, V2, W2;
-            if (!sig_stage<T>(m, f, s, lm, tm, nm, e_last, zm, s.ak[1], c2, U2, V2, W2)) {
+            if (!sig_stage<T>(m, f, s, lm, tm, nm, e_last, zm, 1, c2, U2, V2, W2)) {
                 ok = false;
             } else {
                 a = wrap180(lon0 + dt * U2 / metric_z0(qm));
@@ -286,7 +423,7 @@ __device__ __forceinline__ void step3d_sigma_particle(const DMesh& m, const DBle
             SigSite c;
             sigma_site<T>(m, f, s, 1, l2, t2, n2, c);
             double U2, V2, W2;
-            if (!sig_stage<T>(m, f, s, l2, t2, n2, e2, (s0 + 0.5 * dt * f1) * c.H, s.ak[1], c, U2, V2, W2)) {
+            if (!sig_stage<T>(m, f, s, l2, t2, n2, e2, (s0 + 0.5 * dt * f1) * c.H, 1, c, U2, V2, W2)) {
                 ok = false;
             } else {
                 const double dl2 = dt * U2 / metric_z0(q2), dd2 = dt * V2 / SLM, f2 = W2 / c.H;
@@ -296,7 +433,7 @@ __device__ __forceinline__ void step3d_sigma_particle(const DMesh& m, const DBle
                 const int e3 = stage_elem<WALK>(m, l3, t3, e2, n3);
                 sigma_site<T>(m, f, s, 2, l3, t3, n3, c);
                 double U3, V3, W3;
-                if (!sig_stage<T>(m, f, s, l3, t3, n3, e3, (s0 + 0.5 * dt * f2) * c.H, s.ak[2], c, U3, V3, W3)) {
+                if (!sig_stage<T>(m, f, s, l3, t3, n3, e3, (s0 + 0.5 * dt * f2) * c.H, 2, c, U3, V3, W3)) {
                     ok = false;
                 } else {
                     const double dl3 = dt * U3 / metric_z0(q3), dd3 = dt * V3 / SLM, f3 = W3 / c.H;
@@ -306,7 +443,7 @@ __device__ __forceinline__ void step3d_sigma_particle(const DMesh& m, const DBle
                     e_last = stage_elem<WALK>(m, l4, t4, e3, n4);
                     sigma_site<T>(m, f, s, 3, l4, t4, n4, c);
                     double U4, V4, W4;
-                    if (!sig_stage<T>(m, f, s, l4, t4, n4, e_last, (s0 + dt * f3) * c.H, s.ak[3], c, U4, V4, W4)) {
+                    if (!sig_stage<T>(m, f, s, l4, t4, n4, e_last, (s0 + dt * f3) * c.H, 3, c, U4, V4, W4)) {
                         ok = false;
                     } else {
                         const double dl4 = dt * U4 / metric_z0(q4), dd4 = dt * V4 / SLM, f4 = W4 / c.H;

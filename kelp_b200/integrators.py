@@ -339,9 +339,6 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
         if w_interp not in codes:
             raise ValueError(f"unknown w_interp {w_interp!r}; expected one of {tuple(codes)}")
         w_code = codes[w_interp]
-        if w_code >= 2 and coord == "sigma":
-            raise NotImplementedError(f"w_interp={w_interp!r} on sigma meshes is not built on the CUDA backend "
-                                      "(nearest and barycentric are)")
         if w_code >= 2 and kw.get("cuda_precision", "plain") != "plain":
             raise NotImplementedError(f"w_interp={w_interp!r} runs in the plain form (cuda_precision='plain')")
         if code == N.KC_RK2 and hasattr(vel, "vel_a") and float(getattr(vel, "alpha", 1.0)) == 0.0:

@@ -1550,7 +1550,47 @@ static int bary_locate(const OMesh* m, double xp, double yp, int node, int* vert
 
 /* vertical_sigma.py:1034-1060 the particle's column height, interpolated
  * with the W method (nearest: the anchor's column; barycentric: :636-652) */
+/* vertical_sigma.py:493-563 _H_leastsq_single (w_code 2) / _H_idw_single (3) */
+static double H_ring(const OMesh* m, const OField* f, const OStep* s, int slot, double xp, double yp, int node) {
+    int32_t buf[MAX_NEIGH];
+    int count = neigh_ring(m, node, buf);
+    double z0 = cos(yp * DEG2RAD) * SLM;
+    if (z0 < 1.0) z0 = 1.0;
+    if (s->w_code == 3) {
+        double sw = 0.0, swh = 0.0;
+        for (int i = 0; i < count; ++i) {
+            int nd = buf[i];
+            double h = col_H(m, f, s, nd, slot);
+            double dx = wrap180(m->lon[nd] - xp) * z0, dy = (m->lat[nd] - yp) * SLM;
+            double d2 = dx * dx + dy * dy;
+            if (d2 < 1.0) return h;
+            sw += 1.0 / d2;
+            swh += h / d2;
+        }
+        if (sw < 1e-30) return col_H(m, f, s, node, slot);
+        return swh / sw;
+    }
+    if (count < 3) return col_H(m, f, s, node, slot);
+    double a11 = 0, a12 = 0, a13 = 0, a22 = 0, a23 = 0, a33 = 0, fw = 0, f1w = 0, f2w = 0;
+    for (int i = 0; i < count; ++i) {
+        int nd = buf[i];
+        double h = col_H(m, f, s, nd, slot);
+        double ex = wrap180(m->lon[nd] - xp) * z0, ey = (m->lat[nd] - yp) * SLM;
+        a11 += 1.0; a12 += ex; a13 += ey; a22 += ex * ex; a23 += ex * ey; a33 += ey * ey;
+        fw += h; f1w += h * ex; f2w += h * ey;
+    }
+    double a21 = a12, a31 = a13, a32 = a23;
+    double det = a11 * a22 * a33 + a12 * a23 * a31 + a13 * a21 * a32 - a13 * a22 * a31 - a12 * a21 * a33 -
+                 a11 * a23 * a32;
+    if (fabs(det) < 1e-30 || fabs(det) < 1e-12 * fabs(a11 * a22 * a33)) return col_H(m, f, s, node, slot);
+    double inv = 1.0 / fabs(det);
+    double H = ((a22 * a33 - a23 * a32) * fw + (a13 * a32 - a12 * a33) * f1w + (a12 * a23 - a13 * a22) * f2w) * inv;
+    if (H < s->Dmin) H = s->Dmin;
+    return H;
+}
+
 static double sigma_H(const OMesh* m, const OField* f, const OStep* s, int slot, double xp, double yp, int node) {
+    if (s->w_code >= 2) return H_ring(m, f, s, slot, xp, yp, node);
     if (s->w_code == 0) return col_H(m, f, s, node, slot);
     int verts[4];
     double wts[4];
@@ -1591,9 +1631,48 @@ static double sigma_frac(double z, double H) {
 /* W on a sigma mesh (vertical_sigma.py:971-1031): nearest = the anchor's
  * column (:337-360); barycentric = every vertex column at the particle's
  * sigma (:766-816), the own column at min(z, H) outside every element */
+/* vertical_sigma.py:656-765 _interp_w_sigma_leastsq_single / :820-905
+ * _interp_w_sigma_idw_single: the 1-ring sampled at the particle's sigma */
+static double w_sig_ring(const OMesh* m, const OField* f, const OStep* s, int slot, double alpha, double xp, double yp,
+                         double z, int node) {
+    int32_t buf[MAX_NEIGH];
+    int count = neigh_ring(m, node, buf);
+    double Hn = col_H(m, f, s, node, slot);
+    double fallback = w_sig_linear(m, f, alpha, z < Hn ? z : Hn, node, Hn, s->td);
+    if (s->w_code == 2 && count < 3) return fallback;
+    double z0 = cos(yp * DEG2RAD) * SLM;
+    if (z0 < 1.0) z0 = 1.0;
+    double fr = sigma_frac(z, H_ring(m, f, s, slot, xp, yp, node));
+    double a11 = 0, a12 = 0, a13 = 0, a22 = 0, a23 = 0, a33 = 0, fw = 0, f1w = 0, f2w = 0, sw = 0, swv = 0;
+    for (int i = 0; i < count; ++i) {
+        int nd = buf[i];
+        double H = col_H(m, f, s, nd, slot);
+        double wv = w_sig_linear(m, f, alpha, fr * H, nd, H, s->td);
+        double dx = wrap180(m->lon[nd] - xp) * z0, dy = (m->lat[nd] - yp) * SLM;
+        if (s->w_code == 3) {
+            double d2 = dx * dx + dy * dy;
+            if (d2 < 1.0) return wv;
+            double wt = 1.0 / d2;
+            sw += wt;
+            swv += wt * wv;
+            continue;
+        }
+        a11 += 1.0; a12 += dx; a13 += dy; a22 += dx * dx; a23 += dx * dy; a33 += dy * dy;
+        fw += wv; f1w += wv * dx; f2w += wv * dy;
+    }
+    if (s->w_code == 3) return sw < 1e-30 ? fallback : swv / sw;
+    double a21 = a12, a31 = a13, a32 = a23;
+    double det = a11 * a22 * a33 + a12 * a23 * a31 + a13 * a21 * a32 - a13 * a22 * a31 - a12 * a21 * a33 -
+                 a11 * a23 * a32;
+    if (fabs(det) < 1e-30 || fabs(det) < 1e-12 * fabs(a11 * a22 * a33)) return fallback;
+    double inv = 1.0 / fabs(det);
+    return ((a22 * a33 - a23 * a32) * fw + (a13 * a32 - a12 * a33) * f1w + (a12 * a23 - a13 * a22) * f2w) * inv;
+}
+
 static double w_sig(const OMesh* m, const OField* f, const OStep* s, int slot, double xp, double yp, double z,
                     int node) {
     double alpha = stage_alpha(s, slot);
+    if (s->w_code >= 2) return w_sig_ring(m, f, s, slot, alpha, xp, yp, z, node);
     if (s->w_code == 0) return w_sig_linear(m, f, alpha, z, node, col_H(m, f, s, node, slot), s->td);
     int verts[4];
     double wts[4];

@@ -576,6 +576,40 @@ def wring_fixture():
     save("golden_wring", mesh_record(rm), snaps, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
 
 
+def sigma_wring_fixture():
+    """W (and the particle's column height) by least squares and by inverse
+    distance on sigma meshes (vertical_sigma.py:493-563, :656-905): on the
+    sigma shelf of golden_sigma_surf, RK2 / RK4 / Euler, the split kick,
+    backward time, the tracking layer's surfaces, depth-linear u/v.
+    tests/golden/golden_sigma_wring.npz."""
+    T = 21600.0
+    sig = np.array([1.0, 0.95, 0.88, 0.8, 0.7, 0.58, 0.45, 0.32, 0.2, 0.1, 0.0])
+    m = S.lattice_mesh(1.0, 15.0, lon_min=-20.0, lon_max=20.0, jitter=0.15, land_frac=0.2, quad_frac=0.3,
+                       depth=lambda lo, la: S.smooth_bathymetry(lo, la, 0.2, 120.0), sigma=sig)
+    rm = ref_mesh(m, sigma=sig)
+    rm.vertical_coord = "sigma"
+    lon_n, lat_n = np.radians(np.asarray(m.nodes_lon)), np.radians(np.asarray(m.nodes_lat))
+    pseudo = (1.0 - sig) * 100.0
+    lon, lat, z, status = particles(m, 1200, 59, z=True, n_dead=20)
+    snaps = S.gyre_snapshots(m, 6, amp=1.0, z_levels=pseudo, decay=60.0, w_scale=4e-4, placement="layer")
+    for k, sn in enumerate(snaps):
+        sn.eta = (0.6 * np.sin(2.0 * lon_n + 0.9 * k) * np.cos(3.0 * lat_n) - 0.15).astype(np.float32)
+    rf = ref_fields(snaps)
+
+    def surf(t):
+        return 0.5 * np.sin(2.0 * lon_n + 2.0e-4 * t) * np.cos(3.0 * lat_n) - 0.1 + 0.3 * np.cos(lat_n + 1.0e-4 * t)
+
+    cases = {"rk2_wlsq": run_case(rm, rf, lon, lat, z, status, "rk2", 3600.0, T, 10, w_interp="leastsq"),
+             "rk4_widw_kick": run_case(rm, rf, lon, lat, z, status, "rk4", 3600.0, T, 10, w_interp="idw",
+                                       kh=(20.0, 20.0), seed=3),
+             "euler_wlsq": run_case(rm, rf, lon, lat, z, status, "euler", 1800.0, T, 12, w_interp="leastsq"),
+             "rk2_widw_bwd": run_case(rm, rf, lon, lat, z, status, "rk2", 3600.0, T, 10, w_interp="idw",
+                                      time_dir=-1.0),
+             "rk4_wlsq_surf_kick": run_case(rm, rf, lon, lat, z, status, "rk4", 3600.0, T, 8, w_interp="leastsq",
+                                            kh=(30.0, 10.0), seed=6, surfaces=lambda t0, t1: (surf(t0), surf(t1)))}
+    save("golden_sigma_wring", mesh_record(rm), snaps, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
+
+
 def eta_time_fixture():
     """tracking.py:3097-3133 _eta_at_time, the surface a sigma step sees at
     the start and end times of its step, on the records of golden_sigma_surf
@@ -1225,7 +1259,7 @@ def reftypes_fixture():
 
 if __name__ == "__main__":
     # no argument: every fixture; otherwise the named ones ("steps", "beach", ...)
-    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq", "rng1m", "tripolar", "reftypes", "sample", "cellrule", "lazy0", "sigma_surf", "eta_time", "sigma_az", "wring", "lsq3d"}
+    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq", "rng1m", "tripolar", "reftypes", "sample", "cellrule", "lazy0", "sigma_surf", "eta_time", "sigma_az", "wring", "lsq3d", "sigma_wring"}
     if "rng1m" in which:
         rng1m_fixture()
     if "reftypes" in which:
@@ -1246,6 +1280,8 @@ if __name__ == "__main__":
         wring_fixture()
     if "lsq3d" in which:
         lsq3d_fixture()
+    if "sigma_wring" in which:
+        sigma_wring_fixture()
     if "lsq" in which:
         lsq_fixture()
     if "steps" in which:

@@ -35,6 +35,9 @@ SIGMA_CASES += [("golden_sigma_llin", c) for c in ("rk2_llin_wbary", "rk4_llin_w
 SIGMA_CASES += [("golden_sigma_surf", c) for c in ("rk2_wbary_surf", "rk4_wnear_surf", "euler_wbary_surf",
                                                   "rk2_wbary_steady_surf", "rk4_wnear_steady_surf_kick",
                                                   "rk4_wbary_steady_endonly", "rk2_wnear_startonly_kick")]
+# W and the particle's column by least squares / inverse distance on sigma meshes
+SIGMA_CASES += [("golden_sigma_wring", c) for c in ("rk2_wlsq", "rk4_widw_kick", "euler_wlsq", "rk2_widw_bwd",
+                                                   "rk4_wlsq_surf_kick")]
 # the vertical Az kick on sigma meshes (constant source, end-of-step column)
 SIGMA_CASES += [("golden_sigma_az", c) for c in ("rk2_wbary_azc", "rk4_wnear_kick_azc", "euler_wbary_azc",
                                                 "rk2_wnear_bwd_kick_azc", "rk2_wbary_surf_kick_azc")]
