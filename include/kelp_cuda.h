@@ -408,7 +408,9 @@ int kc_find_nearest(kc_ctx* ctx, long long P, const double* lon, const double* l
  * float64, as the reference reads it; interface fields (K, N) and sigma
  * meshes are not covered (the host raises before calling).  KC_ERR_ARG for
  * a method outside 0..3, an anchor >= N or a mid-layer field without its
- * depths or the mesh depth. */
+ * depths or the mesh depth.  z_mids NULL with rows == K: an interface field
+ * (K, N) on the mesh's z-levels, sampled by the W interpolation of the
+ * method as sampling.py:876-890 does (vertical.py:1330-1420). */
 int kc_sample_field(kc_ctx* ctx, const double* values, int rows, const double* z_mids, long long P,
                     const double* lon, const double* lat, const double* z, const int* nearest,
                     const unsigned char* alive, int method, double* out);

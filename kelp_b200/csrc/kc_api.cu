@@ -233,6 +233,27 @@ __global__ void __launch_bounds__(kBlock) k_sample(const __grid_constant__ kc::D
     out[i] = kc::sample_point(m, S, q[i], q[P + i], z ? z[i] : 0.0, a, method);
 }
 
+// sampling.py:876-890: an interface-shaped (K, N) field through the W
+// interpolation of the method (vertical.py:1330-1420 interp_w_spatial,
+// time_dir +1): nearest = the anchor's column, leastsq / idw = the 1-ring,
+// barycentric = the containing element's vertex columns.
+__global__ void __launch_bounds__(kBlock) k_sample_iface(const __grid_constant__ kc::DMesh m,
+                                                         const kc::DBlend<double> f, const double* q, const double* z,
+                                                         const int* nn, const unsigned char* alive, long long P,
+                                                         int method, double* out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P) return;
+    const int a = nn[i];
+    if ((alive && !alive[i]) || a < 0) {
+        out[i] = __longlong_as_double(0x7ff8000000000000LL);
+        return;
+    }
+    const double lon = q[i], lat = q[P + i], zp = z[i];
+    if (method == kc::S_NEAREST) out[i] = kc::w_linear<double>(m, f, 0.0, zp, a, 1.0);
+    else if (method == kc::S_BARYCENTRIC) out[i] = kc::w_bary<double>(m, f, 0.0, lon, lat, zp, a, 1.0);
+    else out[i] = kc::w_ring<double>(m, f, method == kc::S_LEASTSQ ? 2 : 3, 0.0, lon, lat, zp, a, 1.0);
+}
+
 __global__ void __launch_bounds__(kBlock) k_nearest(const __grid_constant__ kc::DMesh m, const double* q, long long P, int* out) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P) return;
@@ -2288,7 +2309,7 @@ static int sample_run(kc_ctx* c, char* buf, const double* values, size_t nvals, 
     cudaStream_t st = c->stream;
     KC_CUDA(c, cudaMemcpyAsync(d_vals, values, nvals * 8, cudaMemcpyHostToDevice, st));
     if (rows > 0) {
-        KC_CUDA(c, cudaMemcpyAsync(d_zm, z_mids, (size_t)rows * 8, cudaMemcpyHostToDevice, st));
+        if (z_mids) KC_CUDA(c, cudaMemcpyAsync(d_zm, z_mids, (size_t)rows * 8, cudaMemcpyHostToDevice, st));
         KC_CUDA(c, cudaMemcpyAsync(d_z, z, (size_t)P * 8, cudaMemcpyHostToDevice, st));
     }
     KC_CUDA(c, cudaMemcpyAsync(d_q, lon, (size_t)P * 8, cudaMemcpyHostToDevice, st));
@@ -2300,13 +2321,22 @@ static int sample_run(kc_ctx* c, char* buf, const double* values, size_t nvals, 
         k_nearest<<<grid_for(P), kBlock, 0, st>>>(c->dm, d_q, P, d_nn);
         KC_CUDA(c, cudaGetLastError());
     }
-    kc::DSample S;
-    S.values = d_vals;
-    S.zm = rows > 0 ? d_zm : nullptr;
-    S.n = c->N;
-    S.rows = rows;
-    k_sample<<<grid_for(P), kBlock, 0, st>>>(c->dm, S, d_q, rows > 0 ? d_z : nullptr, d_nn, alive ? d_al : nullptr, P,
-                                           method, d_out);
+    if (rows > 0 && !z_mids) {   // an interface field (K, N)
+        kc::DBlend<double> f{};
+        f.a.w = f.b.w = f.t.w = d_vals;
+        f.alpha0 = 0.0;
+        f.n = c->N;
+        k_sample_iface<<<grid_for(P), kBlock, 0, st>>>(c->dm, f, d_q, d_z, d_nn, alive ? d_al : nullptr, P, method,
+                                                       d_out);
+    } else {
+        kc::DSample S;
+        S.values = d_vals;
+        S.zm = rows > 0 ? d_zm : nullptr;
+        S.n = c->N;
+        S.rows = rows;
+        k_sample<<<grid_for(P), kBlock, 0, st>>>(c->dm, S, d_q, rows > 0 ? d_z : nullptr, d_nn,
+                                               alive ? d_al : nullptr, P, method, d_out);
+    }
     KC_CUDA(c, cudaGetLastError());
     KC_CUDA(c, cudaMemcpyAsync(out, d_out, (size_t)P * 8, cudaMemcpyDeviceToHost, st));
     KC_CUDA(c, cudaStreamSynchronize(st));
@@ -2321,8 +2351,11 @@ int kc_sample_field(kc_ctx* c, const double* values, int rows, const double* z_m
     if (method < 0 || method > 3) return fail(c, KC_ERR_ARG, "kc_sample_field: method must be 0..3");
     if (rows < 0 || !values || P < 0 || (P > 0 && (!lon || !lat || !out)))
         return fail(c, KC_ERR_ARG, "kc_sample_field: arrays");
-    if (rows > 0 && (!z_mids || (P > 0 && !z) || !c->d_depth))
-        return fail(c, KC_ERR_ARG, "kc_sample_field: a mid-layer field needs z_mids, the depths and the mesh depth");
+    if (rows > 0 && ((P > 0 && !z) || !c->d_depth))
+        return fail(c, KC_ERR_ARG, "kc_sample_field: a 3-D field needs the depths and the mesh depth");
+    if (rows > 0 && !z_mids && (rows != c->dm.K || c->dm.sig || !c->dm.zlev))
+        return fail(c, KC_ERR_ARG, "kc_sample_field: without z_mids the field is an interface field of the mesh's "
+                                   "K z-levels");
     if (nearest)
         for (long long i = 0; i < P; ++i)
             if (nearest[i] >= c->N) return fail(c, KC_ERR_ARG, "kc_sample_field: nearest node out of range");

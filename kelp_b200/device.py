@@ -510,7 +510,7 @@ class DeviceContext:
         lat = _c(lat, np.float64)
         rows = values.shape[0] if values.ndim == 2 else 0
         zz = _c(z, np.float64) if rows else None
-        zm = _c(z_mids, np.float64) if rows else None
+        zm = _c(z_mids, np.float64) if (rows and z_mids is not None) else None   # None: an interface field
         nn = None if nearest is None else _c(nearest, np.int32)
         al = None if alive is None else _c(np.asarray(alive).astype(np.uint8), np.uint8)
         out = np.empty(lon.shape[0], np.float64)

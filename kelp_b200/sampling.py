@@ -6,10 +6,11 @@ validation errors and results (NaN for dead or anchorless particles, the
 anchor's raw value as the fallback of every rule).  The work runs in the
 native library (``kc_sample_field``, one thread per particle).
 
-Covered: node fields ``(N,)`` and z-level mid-layer fields ``(K-1, N)``
-with the methods ``nearest``, ``leastsq``, ``barycentric`` and ``idw``.
-Not built: interface-shaped fields ``(K, N)`` (the reference hands them to its
-W interpolation) and sigma meshes; both raise ``NotImplementedError``.
+Covered: node fields ``(N,)``, z-level mid-layer fields ``(K-1, N)`` and
+interface fields ``(K, N)`` (through the W interpolation of the method, as
+the reference hands them over, sampling.py:876-890) with the methods
+``nearest``, ``leastsq``, ``barycentric`` and ``idw``.  Not built: sigma
+meshes (``NotImplementedError``).
 """
 from __future__ import annotations
 
@@ -51,12 +52,12 @@ def sample_field(values, mesh, lons, lats, zs=None, *, nearest=None, alive=None,
             raise NotImplementedError("sampling on sigma meshes is not built on the CUDA backend")
         zl = np.abs(np.asarray(mesh.sigma, dtype=np.float64))
         K = zl.size
-        if values.shape[0] == K:
-            raise NotImplementedError("interface-shaped (K, N) fields are not built on the CUDA backend")
-        if values.shape[0] != K - 1:
+        if values.shape[0] not in (K, K - 1):
             raise ValueError(f"3D z-level field shape[0]={values.shape[0]} does not match "
                              f"K={K} (interface) or K-1={K - 1} (mid-layer) from mesh.sigma")
-        z_mids = 0.5 * (zl[:-1] + zl[1:])
+        # an interface field (K, N) goes through the W interpolation
+        # (sampling.py:876-890): no mid-layer depths
+        z_mids = None if values.shape[0] == K else 0.5 * (zl[:-1] + zl[1:])
     elif values.ndim != 1:
         raise ValueError(f"values must be 1D (N,) or 2D (K, N) or (K-1, N), got shape {values.shape}")
     ctx = ctx or default_context()

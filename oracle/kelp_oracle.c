@@ -2507,6 +2507,17 @@ static void sample_body(void* ctx, int64_t i) {
     const OMesh* m = c->m;
     if ((c->alive && !c->alive[i]) || c->nearest[i] < 0) { c->out[i] = NAN; return; }
     int nn = c->nearest[i];
+    if (c->rows > 0 && !c->zm) {
+        /* sampling.py:876-890: an interface field (K, N) through the W
+         * interpolation of the method (vertical.py:1330-1420, time_dir +1) */
+        OField f;
+        memset(&f, 0, sizeof f);
+        f.wa = f.wb = f.wt = c->values;
+        f.n = m->N;
+        int wc = c->method == S_NEAREST ? 0 : c->method == S_BARYCENTRIC ? 1 : c->method == S_LEASTSQ ? 2 : 3;
+        c->out[i] = w_stage(m, &f, wc, 0.0, c->lon[i], c->lat[i], c->z[i], nn, 1.0);
+        return;
+    }
     int32_t buf[MAX_NEIGH];
     double vals[MAX_NEIGH];
     int cnt = neigh_ring(m, nn, buf);

@@ -448,8 +448,9 @@ SAMPLE_METHODS = {"nearest": 0, "leastsq": 1, "barycentric": 2, "idw": 3}
 
 
 def sample_field(values, mesh, lon, lat, z=None, *, nearest=None, alive=None, method="leastsq", view=None):
-    """sampling.py:727 sample_field for a node field of shape (N,) or a
-    z-level mid-layer field (K-1, N): the oracle's restatement."""
+    """sampling.py:727 sample_field for a node field of shape (N,), a
+    z-level mid-layer field (K-1, N) or an interface field (K, N): the
+    oracle's restatement."""
     view = view or MeshView(mesh)
     values = np.ascontiguousarray(values, dtype=np.float64)
     lon = np.ascontiguousarray(lon, dtype=np.float64)
@@ -462,8 +463,10 @@ def sample_field(values, mesh, lon, lat, z=None, *, nearest=None, alive=None, me
     rows, zm, zz = 0, None, None
     if values.ndim == 2:
         zl = np.abs(np.asarray(mesh.sigma, dtype=np.float64))
-        zm = np.ascontiguousarray(0.5 * (zl[:-1] + zl[1:]))
         rows = values.shape[0]
+        # a mid-layer field (K-1, N) has its mid-layer depths; an interface
+        # field (K, N) none (the W interpolation reads the z-levels)
+        zm = None if rows == zl.size else np.ascontiguousarray(0.5 * (zl[:-1] + zl[1:]))
         zz = np.ascontiguousarray(z, dtype=np.float64)
     out = np.empty(P)
     lib().orc_sample(C.byref(view.s), _p(values), rows, _p(zm), P, _p(lon), _p(lat), _p(zz), _p(nearest), _p(al),

@@ -1202,6 +1202,39 @@ def cellrule_fixture():
               {m_: (r["chosen"], r["legacy"], len(r["candidates"])) for m_, r in reps.items()})
 
 
+def sample_iface_fixture():
+    """sampling.py:876-890: an interface-shaped (K, N) node field on a
+    z-level mesh, which sample_field hands to the W interpolation of each
+    method (vertical.py:1330-1420, time_dir +1): the 3-D band of
+    golden_sample_3d, points at every depth (the surface, below the bottom),
+    dead particles and nearest = -1.  tests/golden/golden_sample_iface.npz."""
+    from kelp.numerics.sampling import sample_field as r_sample
+    zl = S.stretched_levels(12, 5.0, 4000.0)
+    m = S.lattice_mesh(3.0, 60.0, jitter=0.2, land_frac=0.25,
+                       depth=lambda lo, la: S.smooth_bathymetry(lo, la, 30.0, 4000.0), sigma=zl)
+    rm = ref_mesh(m, sigma=zl)
+    rng = np.random.default_rng(61)
+    lo = np.asarray(m.nodes_lon)
+    zi = np.abs(np.asarray(zl))
+    vk = (2.0 + 10.0 * np.exp(-zi[:, None] / 500.0) * (1.0 + 0.4 * np.cos(np.radians(2.0 * lo)))[None, :]
+          + 1e-3 * np.arange(lo.size)[None, :] / lo.size)
+    P = 1500
+    lon, lat, z, _ = particles(m, P, 67, z=True)
+    z[:40] = 0.0
+    z[40:80] = 1e4          # below every bottom
+    alive = np.ones(P, bool)
+    alive[rng.choice(P, 40, replace=False)] = False
+    nearest = find_nearest_nodes(rm, lon, lat).astype(np.int32)
+    nearest[rng.choice(P, 20, replace=False)] = -1
+    d = {f"mesh_{k}": v for k, v in mesh_record(rm).items()}
+    d.update(lon=lon, lat=lat, z=z, alive=alive, nearest=nearest, vk=vk)
+    for meth in ("nearest", "leastsq", "barycentric", "idw"):
+        d[f"ok_{meth}"] = r_sample(vk, rm, lon, lat, z, nearest=nearest, alive=alive, method=meth)
+    path = os.path.join(HERE, "golden_sample_iface.npz")
+    np.savez_compressed(path, **d)
+    print("golden_sample_iface", os.path.getsize(path) // 1024, "KB")
+
+
 def rng1m_fixture():
     """The reference's own _normal_pair on 4 x 2^20 keys (contiguous particle
     ids under 4 key tuples), stored as per-chunk digests (tests/golden/
@@ -1259,7 +1292,7 @@ def reftypes_fixture():
 
 if __name__ == "__main__":
     # no argument: every fixture; otherwise the named ones ("steps", "beach", ...)
-    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq", "rng1m", "tripolar", "reftypes", "sample", "cellrule", "lazy0", "sigma_surf", "eta_time", "sigma_az", "wring", "lsq3d", "sigma_wring"}
+    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq", "rng1m", "tripolar", "reftypes", "sample", "cellrule", "lazy0", "sigma_surf", "eta_time", "sigma_az", "wring", "lsq3d", "sigma_wring", "sample_iface"}
     if "rng1m" in which:
         rng1m_fixture()
     if "reftypes" in which:
@@ -1282,6 +1315,8 @@ if __name__ == "__main__":
         lsq3d_fixture()
     if "sigma_wring" in which:
         sigma_wring_fixture()
+    if "sample_iface" in which:
+        sample_iface_fixture()
     if "lsq" in which:
         lsq_fixture()
     if "steps" in which:

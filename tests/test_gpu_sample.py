@@ -80,3 +80,15 @@ def test_sample_at_scale_against_oracle():
         got3 = sample_field(v3, m, wl.lon, wl.lat, wl.z, method=method)
         _check(got3, O.sample_field(v3, m, wl.lon, wl.lat, wl.z, nearest=nn, method=method, view=view),
                f"c3small mid-layer {method}")
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_interface_field_matches_reference(golden, method):
+    """An interface-shaped (K, N) field through the W interpolation of the
+    method (sampling.py:876-890), against the reference's own outputs."""
+    from kelp_b200.sampling import sample_field
+    g = golden("golden_sample_iface")
+    d = g.d
+    got = sample_field(d["vk"], g.mesh, d["lon"], d["lat"], d["z"], nearest=d["nearest"], alive=d["alive"],
+                       method=method)
+    _check(got, d[f"ok_{method}"], f"interface {method}")

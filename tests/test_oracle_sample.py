@@ -54,7 +54,18 @@ def test_sample_field_host_validation(golden):
     with pytest.raises(ValueError, match="zs"):
         sample_field(d["v3"], g.mesh, d["lon"], d["lat"])
     K = np.asarray(g.mesh.sigma).size
-    with pytest.raises(NotImplementedError):
-        sample_field(np.zeros((K, d["v2"].size)), g.mesh, d["lon"], d["lat"], d["z"])
     with pytest.raises(ValueError, match="K-1"):
         sample_field(np.zeros((K + 3, d["v2"].size)), g.mesh, d["lon"], d["lat"], d["z"])
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_oracle_interface_field_matches_reference(golden, method):
+    """An interface-shaped (K, N) field: sample_field hands it to the W
+    interpolation of the method (sampling.py:876-890)."""
+    from oracle import oracle as O
+    g = golden("golden_sample_iface")
+    d = g.d
+    got = O.sample_field(d["vk"], g.mesh, d["lon"], d["lat"], d["z"], nearest=d["nearest"], alive=d["alive"],
+                         method=method)
+    assert _same(got, d[f"ok_{method}"]) == 0
+    assert np.isfinite(d[f"ok_{method}"][d["alive"] & (d["nearest"] >= 0)]).all()
