@@ -130,9 +130,13 @@ typedef struct kc_step_args {
                                     times and alpha_end the end time; plain form, no Az */
     int slot_d;
     double pchip_t[4];
-    int uv_lsq;                  /* 1: 2-D u/v on element centres by least squares (uv_interp "leastsq",
-                                    src/kelp/numerics/interpolate.py:52-354): snapshots hold one row of E
-                                    element values; needs kc_elem_centers_upload; plain form */
+    int uv_lsq;                  /* element-centre u/v: 1 the least-squares plane of the anchor's elements
+                                    (uv_interp "leastsq", src/kelp/numerics/interpolate.py:52-354, 644-750);
+                                    2 / 3 the edge-neighbour plane with freeslip / noslip ghost values
+                                    (uv_interp "edge_leastsq", interpolate.py:2588-2747; needs
+                                    kc_elem_neighbors_upload).  Snapshots hold one row of E element values
+                                    (3-D: u/v (K-1, E) and w (K, N) rows of stride max(E, N)); needs
+                                    kc_elem_centers_upload; plain form */
 } kc_step_args;
 
 /* Beaching / resuspension of one step (src/kelp/tracking.py:199-364,

@@ -215,6 +215,7 @@ kc::DStep step_of(const kc_step_args* a) {
     s.az_on = a->az_kick; s.az_field = a->az_field; s.az_const = a->az_const;
     s.Dmin = a->Dmin; s.z0b_min = a->z0b_min; s.alpha_end = a->alpha_end;
     s.eta_s = nullptr; s.eta_e = nullptr; s.sig_steady = 0;
+    s.edge_bc = a->uv_lsq >= 2 ? a->uv_lsq - 2 : -1;
     return s;
 }
 
@@ -901,7 +902,9 @@ int check_step(kc_ctx* c, const kc_step_args* a) {
     if (a->precision != KC_PLAIN && a->precision != KC_MIXED)
         return fail(c, KC_ERR_ARG, "kc_step: precision must be KC_PLAIN or KC_MIXED");
     if (a->uv_lsq) {
-        if (a->uv_lsq != 1) return fail(c, KC_ERR_ARG, "kc_step: uv_lsq must be 0 or 1");
+        if (a->uv_lsq < 1 || a->uv_lsq > 3) return fail(c, KC_ERR_ARG, "kc_step: uv_lsq must be 0..3");
+        if (a->uv_lsq >= 2 && !c->dm.enb)
+            return fail(c, KC_ERR_STATE, "kc_step: edge least-squares u/v needs kc_elem_neighbors_upload");
         if (a->dims == 3 && (a->uv_vertical != 0 || c->dm.sig))
             return fail(c, KC_ERR_ARG, "kc_step: 3-D least-squares u/v is built for layer fields on z-level meshes");
         if (a->precision != KC_PLAIN) return fail(c, KC_ERR_ARG, "kc_step: least-squares u/v runs in the plain form");

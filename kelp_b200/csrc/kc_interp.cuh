@@ -973,6 +973,106 @@ __device__ __forceinline__ bool interp_uv_lsq(const DMesh& m, const DBlend<T>& f
     return true;
 }
 
+// interpolate.py:2588-2747 _interp_edge_leastsq_core (row: the layer of a
+// 3-D field): the containing element (the local search around the anchor,
+// mesh.py:2392-2470), the plane through its centre velocity and its edge
+// neighbours' (build_elem_neighbors order); a boundary edge contributes the
+// centre mirrored across the edge with the mirrored velocity (bc 0,
+// freeslip: tangential kept, normal reversed) or the reversed one (bc 1,
+// noslip), a zero-length boundary edge nothing; particle-centred metric
+// coordinates with wrapped longitudes, Cramer's rule and the scale-relative
+// singular guard of the element-centre fit.
+template <typename T>
+static __device__ __noinline__ bool interp_uv_edge_lsq(const DMesh& m, const DBlend<T>& f, double xp, double yp,
+                                                       int nn, int bc, double time_dir, double alpha, int row,
+                                                       double& U, double& V) {
+    U = 0.0;
+    V = 0.0;
+    const int el = contain_local(m, xp, yp, nn);
+    if (el < 0) return false;
+    Ring r;
+    load_ring(m, __ldg(&m.en[el]), r);
+    const int nv = r.n;
+    if (nv < 3) return false;
+    const double z0 = cr::cos_cr(yp * DEG2RAD) * SLM;
+    auto val = [&](int e, double& uu, double& vv) {
+        const long long idx = (long long)row * f.n + e;
+        if (f.pchip) {
+            uu = pchip_at(f.a.u, f.b.u, f.t.u, f.d.u, idx, f.pt, alpha);
+            vv = pchip_at(f.a.v, f.b.v, f.t.v, f.d.v, idx, f.pt, alpha);
+        } else {
+            uu = tblend((double)__ldg(&f.a.u[idx]), (double)__ldg(&f.b.u[idx]), (double)__ldg(&f.t.u[idx]), f.alpha0,
+                        alpha);
+            vv = tblend((double)__ldg(&f.a.v[idx]), (double)__ldg(&f.b.v[idx]), (double)__ldg(&f.t.v[idx]), f.alpha0,
+                        alpha);
+        }
+    };
+    const double2 c = __ldg(&m.ec[el]);
+    const double cx = wrap180(c.x - xp) * z0;
+    const double cy = (c.y - yp) * SLM;
+    double uo, vo;
+    val(el, uo, vo);
+    const double u_own = time_dir * uo, v_own = time_dir * vo;
+    double a11 = 1.0, a12 = cx, a13 = cy, a22 = cx * cx, a23 = cx * cy, a33 = cy * cy;
+    double fU = u_own, f1U = u_own * cx, f2U = u_own * cy, fV = v_own, f1V = v_own * cx, f2V = v_own * cy;
+    const int4 nb4 = __ldg(&m.enb[el]);
+    for (int k = 0; k < nv; ++k) {
+        const int nb = slot_of(nb4, k);
+        double ex, ey, uu, vv;
+        if (nb >= 0) {
+            const double2 cn = __ldg(&m.ec[nb]);
+            ex = wrap180(cn.x - xp) * z0;
+            ey = (cn.y - yp) * SLM;
+            double un, vn;
+            val(nb, un, vn);
+            uu = time_dir * un;
+            vv = time_dir * vn;
+        } else {
+            const int k2 = k + 1 < nv ? k + 1 : 0;
+            const double dax = wrap180(r.ln[k] - xp) * z0, day = (r.la[k] - yp) * SLM;
+            const double dbx = wrap180(r.ln[k2] - xp) * z0, dby = (r.la[k2] - yp) * SLM;
+            const double tx = dbx - dax, ty = dby - day;
+            const double tt = tx * tx + ty * ty;
+            if (tt <= 0.0) continue;
+            const double proj = ((cx - dax) * tx + (cy - day) * ty) / tt;
+            const double fx = dax + proj * tx, fy = day + proj * ty;
+            ex = 2.0 * fx - cx;
+            ey = 2.0 * fy - cy;
+            if (bc == 1) {
+                uu = -u_own;
+                vv = -v_own;
+            } else {
+                const double ut = (u_own * tx + v_own * ty) / tt;
+                uu = 2.0 * ut * tx - u_own;
+                vv = 2.0 * ut * ty - v_own;
+            }
+        }
+        a11 = a11 + 1.0;
+        a12 = a12 + ex;
+        a13 = a13 + ey;
+        a22 = a22 + ex * ex;
+        a23 = a23 + ex * ey;
+        a33 = a33 + ey * ey;
+        fU = fU + uu;
+        f1U = f1U + uu * ex;
+        f2U = f2U + uu * ey;
+        fV = fV + vv;
+        f1V = f1V + vv * ex;
+        f2V = f2V + vv * ey;
+    }
+    const double a21 = a12, a31 = a13, a32 = a23;
+    const double det = a11 * a22 * a33 + a12 * a23 * a31 + a13 * a21 * a32 - a13 * a22 * a31 - a12 * a21 * a33 -
+                       a11 * a23 * a32;
+    if (fabs(det) < 1e-30 || fabs(det) < 1e-12 * fabs(a11 * a22 * a33)) return false;
+    const double inv = 1.0 / fabs(det);
+    const double b11 = a22 * a33 - a23 * a32;
+    const double b12 = a13 * a32 - a12 * a33;
+    const double b13 = a12 * a23 - a13 * a22;
+    U = (b11 * fU + b12 * f1U + b13 * f2U) * inv;
+    V = (b11 * fV + b12 * f1V + b13 * f2V) * inv;
+    return true;
+}
+
 // ---------------------------------------------------------------------------
 // Counter RNG (diffusion.py:180-249): a keyed SplitMix64 chain over
 // (seed, realization, particle, step, component), split into two open-(0,1)

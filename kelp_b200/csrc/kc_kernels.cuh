@@ -163,19 +163,19 @@ void launch_step_kernel(const kc::DMesh& m, const kc::DBlend<T>& f, const kc::DS
 }
 
 // 2-D steps with element-centre least-squares u/v (LsqForm), local search
-template <typename T>
+template <typename T, typename Form = kc::LsqForm<T>>
 void launch_lsq_kernel(const kc::DMesh& m, const kc::DBlend<T>& f, const kc::DState& st, const kc::DStep& s,
                        int dims, int scheme, cudaStream_t stream) {
     const unsigned g = (unsigned)((st.P + kBlock - 1) / kBlock);
     if (dims == 3) {   // the 3-D RK2 (arithmetic of the unfused RK2) and the unfused RK4 / Euler
-        if (scheme == 1) k_step3d_rk2<T, kc::LsqForm<T>, false><<<g, kBlock, 0, stream>>>(m, f, st, s);
-        else if (scheme == 2) k_step3d_unfused<T, 2, kc::LsqForm<T>, false><<<g, kBlock, 0, stream>>>(m, f, st, s);
-        else k_step3d_unfused<T, 0, kc::LsqForm<T>, false><<<g, kBlock, 0, stream>>>(m, f, st, s);
+        if (scheme == 1) k_step3d_rk2<T, Form, false><<<g, kBlock, 0, stream>>>(m, f, st, s);
+        else if (scheme == 2) k_step3d_unfused<T, 2, Form, false><<<g, kBlock, 0, stream>>>(m, f, st, s);
+        else k_step3d_unfused<T, 0, Form, false><<<g, kBlock, 0, stream>>>(m, f, st, s);
         return;
     }
-    if (scheme == 0) k_step2d<T, 0, kc::LsqForm<T>, false><<<g, kBlock, 0, stream>>>(m, f, st, s);
-    else if (scheme == 1) k_step2d<T, 1, kc::LsqForm<T>, false><<<g, kBlock, 0, stream>>>(m, f, st, s);
-    else k_step2d<T, 2, kc::LsqForm<T>, false><<<g, kBlock, 0, stream>>>(m, f, st, s);
+    if (scheme == 0) k_step2d<T, 0, Form, false><<<g, kBlock, 0, stream>>>(m, f, st, s);
+    else if (scheme == 1) k_step2d<T, 1, Form, false><<<g, kBlock, 0, stream>>>(m, f, st, s);
+    else k_step2d<T, 2, Form, false><<<g, kBlock, 0, stream>>>(m, f, st, s);
 }
 
 // ---------------------------------------------------------------------------

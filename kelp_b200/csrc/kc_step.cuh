@@ -49,6 +49,7 @@ struct DStep {
     double az_const;
     double Dmin, z0b_min;      // sigma column floor and bed clearance
     double alpha_end;          // blend fraction of the end-of-step surface (sigma)
+    int edge_bc;               // edge least-squares u/v: 0 freeslip, 1 noslip ghost values
     const double* eta_s;       // sigma: the tracking layer's surface at the step's start (N), or null
     const double* eta_e;       // sigma: the tracking layer's surface at the step's end (N), or null
     int sig_steady;            // sigma: a steady step (stage surfaces blend from start to end)
@@ -477,6 +478,29 @@ struct LsqForm {
                                                 double lat, int nn, int hint, int whint, double z, double alpha,
                                                 double& U, double& V, double& W) {
         const bool ok = interp_uv_lsq<T>(m, f, lon, lat, nn, s.time_dir, alpha, U, V, find_layer(m, z, nn));
+        if (s.w_code == 0) W = w_linear<T>(m, f, alpha, z, nn, s.time_dir);
+        else if (s.w_code == 1) W = w_bary<T>(m, f, alpha, lon, lat, z, nn, s.time_dir);
+        else W = w_ring<T>(m, f, s.w_code, alpha, lon, lat, z, nn, s.time_dir);
+        return ok;
+    }
+};
+
+// Element-centre u/v by the edge-neighbour least squares
+// (interpolate.py:2588-2747 _interp_edge_leastsq_core, uv_interp
+// "edge_leastsq"): 2-D and 3-D layer fields, node W by the step's W method.
+template <typename T>
+struct EdgeLsqForm {
+    static constexpr bool kExact = true;
+    static __device__ __forceinline__ Site site(double lon, double lat) { return make_site_fast(lon, lat); }
+    static __device__ __forceinline__ bool uv2(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
+                                               double lat, int nn, int hint, double alpha, double& U, double& V) {
+        return interp_uv_edge_lsq<T>(m, f, lon, lat, nn, s.edge_bc, s.time_dir, alpha, 0, U, V);
+    }
+    static __device__ __forceinline__ bool uvw3(const DMesh& m, const DBlend<T>& f, const DStep& s, double lon,
+                                                double lat, int nn, int hint, int whint, double z, double alpha,
+                                                double& U, double& V, double& W) {
+        const bool ok = interp_uv_edge_lsq<T>(m, f, lon, lat, nn, s.edge_bc, s.time_dir, alpha, find_layer(m, z, nn),
+                                              U, V);
         if (s.w_code == 0) W = w_linear<T>(m, f, alpha, z, nn, s.time_dir);
         else if (s.w_code == 1) W = w_bary<T>(m, f, alpha, lon, lat, z, nn, s.time_dir);
         else W = w_ring<T>(m, f, s.w_code, alpha, lon, lat, z, nn, s.time_dir);

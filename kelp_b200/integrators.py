@@ -282,17 +282,22 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
         if elem is not None:
             (ctx or default_context()).ensure_elem_neighbors(mesh)
         return _prepare_cgrid(vel, mesh, dt, time_dir, scheme, kw, ctx, kick)
-    lsq = uv_interp == "leastsq"
-    if uv_interp not in ("barycentric", "leastsq"):
-        raise NotImplementedError(f"uv_interp={uv_interp!r} is not built on the CUDA backend; "
-                                  "use 'barycentric' (node-layout velocities) or 'leastsq' (2-D element layout)")
+    lsq = uv_interp in ("leastsq", "edge_leastsq")
+    if uv_interp not in ("barycentric", "leastsq", "edge_leastsq"):
+        raise NotImplementedError(f"uv_interp={uv_interp!r} is not built on the CUDA backend; use 'barycentric' "
+                                  "(node-layout velocities), 'leastsq' or 'edge_leastsq' (element layout)")
+    edge_bc = None
+    if uv_interp == "edge_leastsq":   # interpolate.py:3374-3395: the lateral boundary rule of the ghost points
+        edge_bc = kw.get("edge_leastsq_bc", "freeslip")
+        if edge_bc not in ("freeslip", "noslip"):
+            raise ValueError(f"edge_leastsq_bc must be 'freeslip' or 'noslip', got {edge_bc!r}")
     if lsq:
         if _is_3d(vel) and (getattr(vel, "uv_vertical", "layer") != "layer" or _sigma_mesh(mesh)):
-            raise NotImplementedError("3-D uv_interp 'leastsq' is built for layer fields on z-level meshes on the "
-                                      "CUDA backend (depth-linear element fields and sigma meshes are not)")
+            raise NotImplementedError(f"3-D uv_interp {uv_interp!r} is built for layer fields on z-level meshes on "
+                                      "the CUDA backend (depth-linear element fields and sigma meshes are not)")
         if elem is not None:
-            raise NotImplementedError("uv_interp 'leastsq' reads no containing element: elem_search 'walk' "
-                                      "does not apply to it on the CUDA backend")
+            raise NotImplementedError(f"uv_interp {uv_interp!r} with elem_search 'walk' is not built on the "
+                                      "CUDA backend")
         if kw.get("cuda_precision", "plain") != "plain":
             raise NotImplementedError("uv_interp 'leastsq' runs in the plain form (cuda_precision='plain')")
     # PCHIP: the RK stages are reconstructed from the tracking layer's
@@ -375,8 +380,10 @@ def prepare_step(vel, mesh, dt, time_dir, scheme, kw, ctx=None, kick=None, elem=
         ctx.ensure_depth_points(mesh, placement)
     if lsq:
         ctx.ensure_elem_centers(mesh)
+    if edge_bc is not None:
+        ctx.ensure_elem_neighbors(mesh)
     a = N.StepArgs()
-    a.uv_lsq = 1 if lsq else 0
+    a.uv_lsq = 0 if not lsq else (1 if edge_bc is None else (2 if edge_bc == "freeslip" else 3))
     if recon is None:
         sa, sb, st = ctx.slots_for([vel_a, vel_b, target], store)
         a.slot_a, a.slot_b, a.slot_t = sa, sb, st

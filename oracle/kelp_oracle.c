@@ -585,9 +585,12 @@ static _Thread_local int t_elem_hint = -1;
 
 static int interp_lsq(const OMesh* m, const OField* f, double xp, double yp, int nn, double td, int row,
                       double alpha, double* U, double* V);
+static int interp_edge_lsq(const OMesh* m, const OField* f, double xp, double yp, int nn, double td, int row,
+                           double alpha, int bc, double* U, double* V);
 
 static int interp_uv(const OMesh* m, const OField* f, double xp, double yp, int nn, double td, int row,
                      double alpha, double* U, double* V) {
+    if (f->lsq >= 2) return interp_edge_lsq(m, f, xp, yp, nn, td, row, alpha, f->lsq - 2, U, V);
     if (f->lsq) return interp_lsq(m, f, xp, yp, nn, td, row, alpha, U, V);   /* element-layout u/v, row = layer */
     *U = 0.0; *V = 0.0;
     int elem = t_elem_hint >= 0 ? t_elem_hint : contain_local(m, xp, yp, nn);
@@ -1444,11 +1447,77 @@ static int interp_lsq(const OMesh* m, const OField* f, double xp, double yp, int
     return 1;
 }
 
+/* interpolate.py:2588-2747 _interp_edge_leastsq_core (bc 0 freeslip, 1
+ * noslip): the containing element, its centre and its edge neighbours'
+ * centres (boundary edges: the mirrored centre and ghost velocity) */
+static int interp_edge_lsq(const OMesh* m, const OField* f, double xp, double yp, int nn, double td, int row,
+                           double alpha, int bc, double* U, double* V) {
+    *U = 0.0; *V = 0.0;
+    int el = contain_local(m, xp, yp, nn);
+    if (el < 0) return 0;
+    int verts[4], nv = 0;
+    for (int k = 0; k < m->max_v; ++k) {
+        int nd = m->en[(int64_t)el * m->max_v + k];
+        if (nd < 0) continue;
+        if (nv > 0 && nd == verts[0]) continue;
+        verts[nv++] = nd;
+    }
+    if (nv < 3) return 0;
+    double z0 = cos(yp * DEG2RAD) * SLM;
+    double cx = wrap180(m->ec_lon[el] - xp) * z0, cy = (m->ec_lat[el] - yp) * SLM;
+    int64_t io = (int64_t)row * f->n + el;
+    double u_own = td * blend4(f, f->ua, f->ub, f->ut, f->ud, io, alpha);
+    double v_own = td * blend4(f, f->va, f->vb, f->vt, f->vd, io, alpha);
+    double a11 = 1.0, a12 = cx, a13 = cy, a22 = cx * cx, a23 = cx * cy, a33 = cy * cy;
+    double fu = u_own, fu1 = u_own * cx, fu2 = u_own * cy, fv = v_own, fv1 = v_own * cx, fv2 = v_own * cy;
+    for (int k = 0; k < nv; ++k) {
+        int nb = m->enb[(int64_t)el * m->max_v + k];
+        double ex, ey, uu, vv;
+        if (nb >= 0) {
+            ex = wrap180(m->ec_lon[nb] - xp) * z0;
+            ey = (m->ec_lat[nb] - yp) * SLM;
+            int64_t ib = (int64_t)row * f->n + nb;
+            uu = td * blend4(f, f->ua, f->ub, f->ut, f->ud, ib, alpha);
+            vv = td * blend4(f, f->va, f->vb, f->vt, f->vd, ib, alpha);
+        } else {
+            int na = verts[k], n2 = verts[(k + 1) % nv];
+            double dax = wrap180(m->lon[na] - xp) * z0, day = (m->lat[na] - yp) * SLM;
+            double dbx = wrap180(m->lon[n2] - xp) * z0, dby = (m->lat[n2] - yp) * SLM;
+            double tx = dbx - dax, ty = dby - day, tt = tx * tx + ty * ty;
+            if (tt <= 0.0) continue;
+            double proj = ((cx - dax) * tx + (cy - day) * ty) / tt;
+            double fx = dax + proj * tx, fy = day + proj * ty;
+            ex = 2.0 * fx - cx;
+            ey = 2.0 * fy - cy;
+            if (bc == 1) { uu = -u_own; vv = -v_own; }
+            else {
+                double ut = (u_own * tx + v_own * ty) / tt;
+                uu = 2.0 * ut * tx - u_own;
+                vv = 2.0 * ut * ty - v_own;
+            }
+        }
+        a11 = a11 + 1.0; a12 = a12 + ex; a13 = a13 + ey;
+        a22 = a22 + ex * ex; a23 = a23 + ex * ey; a33 = a33 + ey * ey;
+        fu = fu + uu; fu1 = fu1 + uu * ex; fu2 = fu2 + uu * ey;
+        fv = fv + vv; fv1 = fv1 + vv * ex; fv2 = fv2 + vv * ey;
+    }
+    double a21 = a12, a31 = a13, a32 = a23;
+    double det = a11 * a22 * a33 + a12 * a23 * a31 + a13 * a21 * a32 - a13 * a22 * a31 - a12 * a21 * a33 -
+                 a11 * a23 * a32;
+    if (fabs(det) < 1e-30 || fabs(det) < 1e-12 * fabs(a11 * a22 * a33)) return 0;
+    double inv = 1.0 / fabs(det);
+    double c11 = a22 * a33 - a23 * a32, c12 = a13 * a32 - a12 * a33, c13 = a12 * a23 - a13 * a22;
+    *U = (c11 * fu + c12 * fu1 + c13 * fu2) * inv;
+    *V = (c11 * fv + c12 * fv1 + c13 * fv2) * inv;
+    return 1;
+}
+
 /* u/v of a 2-D stage: the C-grid core on the surface faces
  * (nemo_cgrid.py:355-388 interp_nemo_cgrid), the element-centre least
  * squares, else the barycentric core */
 static int uv2(const OMesh* m, const OField* f, double xp, double yp, int nn, double td, double alpha, double* U,
                double* V) {
+    if (f->lsq >= 2) return interp_edge_lsq(m, f, xp, yp, nn, td, 0, alpha, f->lsq - 2, U, V);
     if (f->lsq) return interp_lsq(m, f, xp, yp, nn, td, 0, alpha, U, V);
     if (m->cg) {
         double Wd;

@@ -211,7 +211,7 @@ def _field_arrays(f, dtype):
 
 def step(state, vel, mesh, dt, time_dir, scheme: str, *, vel_next=None, dt_to_next=None, w_interp="nearest",
          diffusion=None, pid=None, release_step=None, global_step=-1, view=None, Dmin=0.5, z0b_min=0.1,
-         recon=None, uv_interp="barycentric", eta_start=None, eta_end=None):
+         recon=None, uv_interp="barycentric", eta_start=None, eta_end=None, edge_leastsq_bc="freeslip"):
     """One step of every particle; returns a dict of new arrays
     (lon, lat, z, status, nearest_node, failure_reason, u, v, w, and elem
     when the state carries elements: elem_search walk, the mesh's
@@ -244,10 +244,14 @@ def step(state, vel, mesh, dt, time_dir, scheme: str, *, vel_next=None, dt_to_ne
     of.f32 = 1 if all32 else 0
     of.alpha0 = alpha0
     of.n = view.lon.size
-    if uv_interp == "leastsq":   # element-centre u/v (interpolate.py:52-354, 644-750)
+    if uv_interp in ("leastsq", "edge_leastsq"):   # element-centre u/v (interpolate.py:52-354, 644-750, 2588-2747)
         if view.ec_lon is None:
-            raise ValueError("uv_interp 'leastsq' needs the mesh's element centres")
+            raise ValueError(f"uv_interp {uv_interp!r} needs the mesh's element centres")
         of.lsq = 1
+        if uv_interp == "edge_leastsq":
+            if view.enb is None:
+                raise ValueError("uv_interp 'edge_leastsq' needs the mesh's element neighbours")
+            of.lsq = 2 if edge_leastsq_bc == "freeslip" else 3
         of.n = view.ec_lon.size
         if arrs[0][2] is not None:   # 3-D: u/v (K-1, E) and w (K, N) share the stride max(E, N)
             S = max(view.ec_lon.size, view.lon.size)
@@ -260,7 +264,8 @@ def step(state, vel, mesh, dt, time_dir, scheme: str, *, vel_next=None, dt_to_ne
                 of.ud, of.vd, of.wd = (_p(x) for x in arrs[3])
             of.n = S
     elif uv_interp != "barycentric":
-        raise ValueError(f"uv_interp {uv_interp!r}: the oracle restates 'barycentric' and 'leastsq'")
+        raise ValueError(f"uv_interp {uv_interp!r}: the oracle restates 'barycentric', 'leastsq' and "
+                         "'edge_leastsq'")
     etas = [np.ascontiguousarray(getattr(f, "eta", None) if getattr(f, "eta", None) is not None
                                  else np.zeros(view.lon.size), dtype=np.float64) for f in flds]
     of.etaa, of.etab, of.etat = (_p(e) for e in etas[:3])

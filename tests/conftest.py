@@ -47,6 +47,7 @@ class Golden:
             m.elem_center_lon = self.d["mesh_elem_center_lon"]
             m.elem_center_lat = self.d["mesh_elem_center_lat"]
         self.uv_element = "mesh_uv_element" in self.d
+        self.uv_edge = "mesh_uv_edge" in self.d   # element-layout u/v by the edge-neighbour fit
         if "mesh_cgrid_corners" in self.d:   # a NEMO C-grid mesh (build_nemo_cgrid_mesh)
             m._nemo_cgrid = True
             for k in ("corners", "elem_ji", "nlev", "nlev_raster", "zw", "area", "e3b", "kbu", "e3u", "kbv", "e3v",

@@ -86,7 +86,7 @@ def payload(fields, t, T):
 
 def run_case(rm, fields, lon, lat, z, status, scheme, dt, T, n_steps, *, time_dir=1.0, w_interp="nearest",
              kh=None, seed=7, real_id=0, pid_offset=0, record=(1,), az=None, walk=False, steady=False,
-             uv_interp="barycentric", pchip=False, t0=0.0, surfaces=None):
+             uv_interp="barycentric", pchip=False, t0=0.0, surfaces=None, edge_bc=None):
     fn = {"rk2": RI.rk2_step, "rk4": RI.rk4_step, "euler": RI.euler_step}[scheme]
     P = lon.size
     st = RState(lon=lon.copy(), lat=lat.copy(), z=z.copy(), status=status.copy(),
@@ -106,6 +106,8 @@ def run_case(rm, fields, lon, lat, z, status, scheme, dt, T, n_steps, *, time_di
             vel, vnext, dtn, ia, alpha = fields[0], None, -1.0, 0, 0.0
         kw = dict(uv_interp=uv_interp, w_interp=w_interp, vel_next=vnext,
                   dt_to_next=None if steady else dtn)
+        if edge_bc is not None:
+            kw["edge_leastsq_bc"] = edge_bc
         if kh is not None:
             kw["diffusion"] = RDiff(scheme="uniform", kh_x=kh[0], kh_y=kh[1], seed=seed, real_id=real_id,
                                     step_i=k, pid_offset=pid_offset, **(az or {}))
@@ -1031,6 +1033,68 @@ def lsq3d_fixture():
     save("golden_lsq3d", rec, rf, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
 
 
+def edge_fixture():
+    """Element-layout u/v by the edge-neighbour least squares (uv_interp
+    "edge_leastsq", interpolate.py:2588-2747, 3210-3300): the plane through
+    the containing element's centre velocity and its edge neighbours', with
+    mirrored ghost points on boundary edges (freeslip or noslip), through the
+    reference's unfused steps: the seam-wrapping band and the regional
+    tri/quad mesh in 2-D, the z-level mesh of golden_3d in 3-D.
+    tests/golden/golden_edge_band.npz, golden_edge_quad.npz, golden_edge3d.npz."""
+    T = 86400.0
+
+    def elem_fields(m, snaps):
+        en = np.asarray(m.elem_nodes)
+        valid = en >= 0
+        out = []
+        for sn in snaps:
+            u, v = np.asarray(sn.u), np.asarray(sn.v)
+            if u.ndim == 1:
+                ue = np.where(valid, u[np.maximum(en, 0)], 0.0).sum(1) / valid.sum(1)
+                ve = np.where(valid, v[np.maximum(en, 0)], 0.0).sum(1) / valid.sum(1)
+            else:
+                ue = np.where(valid[None], u[:, np.maximum(en, 0)], 0.0).sum(2) / valid.sum(1)[None]
+                ve = np.where(valid[None], v[:, np.maximum(en, 0)], 0.0).sum(2) / valid.sum(1)[None]
+            out.append(RVel(u=ue.astype(u.dtype), v=ve.astype(v.dtype), w=None if sn.w is None else np.asarray(sn.w),
+                            eta=np.zeros(m.n_nodes), uv_layout="element"))
+        return out
+
+    def saved(name, rm, rf, cases, lon, lat, z, status):
+        rec = mesh_record(rm)
+        rec.update(elem_center_lon=rm.elem_center_lon, elem_center_lat=rm.elem_center_lat, uv_element=np.array(1),
+                   uv_edge=np.array(1))
+        save(name, rec, rf, cases, {"lon": lon, "lat": lat, "z": z, "status": status})
+
+    ui = "edge_leastsq"
+    for name, m, P, dt, dtype in (
+            ("golden_edge_band", S.lattice_mesh(3.0, 72.0, jitter=0.2, land_frac=0.3), 1500, 21600.0, np.float32),
+            ("golden_edge_quad", S.lattice_mesh(1.0, 15.0, lon_min=-20.0, lon_max=20.0, jitter=0.15, land_frac=0.2,
+                                                quad_frac=0.3), 1200, 10800.0, np.float64)):
+        rm = ref_mesh(m)
+        rf = elem_fields(m, S.gyre_snapshots(m, 5, amp=1.5, dtype=dtype))
+        lon, lat, z, status = particles(m, P, 71, n_off=40, n_dead=30)
+        cases = {"rk2": run_case(rm, rf, lon, lat, z, status, "rk2", dt, T, 12, uv_interp=ui),
+                 "rk4_noslip": run_case(rm, rf, lon, lat, z, status, "rk4", dt, T, 12, uv_interp=ui,
+                                        edge_bc="noslip"),
+                 "euler": run_case(rm, rf, lon, lat, z, status, "euler", dt, T, 12, uv_interp=ui),
+                 "rk2_kick_noslip": run_case(rm, rf, lon, lat, z, status, "rk2", dt, T, 12, kh=(5.0e4, 5.0e4),
+                                             seed=5, uv_interp=ui, edge_bc="noslip")}
+        saved(name, rm, rf, cases, lon, lat, z, status)
+    zl = S.stretched_levels(12, 5.0, 4000.0)
+    m = S.lattice_mesh(3.0, 60.0, jitter=0.2, land_frac=0.25,
+                       depth=lambda lo, la: S.smooth_bathymetry(lo, la, 30.0, 4000.0), sigma=zl)
+    rm = ref_mesh(m, sigma=zl)
+    rf = elem_fields(m, S.gyre_snapshots(m, 5, amp=1.5, z_levels=zl, decay=800.0, w_scale=2e-3))
+    lon, lat, z, status = particles(m, 1200, 73, z=True, n_dead=20)
+    cases = {"rk2_wbary": run_case(rm, rf, lon, lat, z, status, "rk2", 21600.0, T, 10, w_interp="barycentric",
+                                   uv_interp=ui),
+             "rk4_wlsq_noslip": run_case(rm, rf, lon, lat, z, status, "rk4", 21600.0, T, 10, w_interp="leastsq",
+                                         uv_interp=ui, edge_bc="noslip"),
+             "euler_wnear": run_case(rm, rf, lon, lat, z, status, "euler", 10800.0, T, 12, w_interp="nearest",
+                                     uv_interp=ui)}
+    saved("golden_edge3d", rm, rf, cases, lon, lat, z, status)
+
+
 RNG_KEY_SETS = (   # (seed, realization, first particle id, step, component), 2^20 particles each
     (0, 0, 0, 0, 0),
     (20240917, 3, 5_000_000, 1459, 0),
@@ -1292,7 +1356,7 @@ def reftypes_fixture():
 
 if __name__ == "__main__":
     # no argument: every fixture; otherwise the named ones ("steps", "beach", ...)
-    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq", "rng1m", "tripolar", "reftypes", "sample", "cellrule", "lazy0", "sigma_surf", "eta_time", "sigma_az", "wring", "lsq3d", "sigma_wring", "sample_iface"}
+    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq", "rng1m", "tripolar", "reftypes", "sample", "cellrule", "lazy0", "sigma_surf", "eta_time", "sigma_az", "wring", "lsq3d", "sigma_wring", "sample_iface", "edge"}
     if "rng1m" in which:
         rng1m_fixture()
     if "reftypes" in which:
@@ -1317,6 +1381,8 @@ if __name__ == "__main__":
         sigma_wring_fixture()
     if "sample_iface" in which:
         sample_iface_fixture()
+    if "edge" in which:
+        edge_fixture()
     if "lsq" in which:
         lsq_fixture()
     if "steps" in which:

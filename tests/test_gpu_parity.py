@@ -13,8 +13,8 @@ import pytest
 from kelp_b200 import integrators as KI
 from kelp_b200.diffusion import DiffusionStepArgs
 
-from test_oracle_golden import (CGRID_CASES, LSQ_CASES, PCHIP_CASES, SIGMA_CASES, diffusion_args, recon_of, surfaces_of,
-                                uv_interp_of, w_interp_of)
+from test_oracle_golden import (CGRID_CASES, EDGE_CASES, LSQ_CASES, PCHIP_CASES, SIGMA_CASES, diffusion_args, edge_kw,
+                                recon_of, surfaces_of, uv_interp_of, w_interp_of)
 
 pytestmark = pytest.mark.gpu
 
@@ -38,6 +38,7 @@ CASES += WALK_CASES
 CASES += SIGMA_CASES
 CASES += CGRID_CASES
 CASES += LSQ_CASES
+CASES += EDGE_CASES
 CASES += PCHIP_CASES
 
 
@@ -60,6 +61,7 @@ def replay_cuda(g, cname):
         for key, e in zip(("sigma_eta_start", "sigma_eta_end"), surfaces_of(c, k)):
             if e is not None:
                 extra[key] = e
+        extra.update(edge_kw(g, cname))
         st = fn(st, vel, g.mesh, dt, td, uv_interp=uv, w_interp=w_interp, vel_next=vnext,
                 dt_to_next=dtn, diffusion=diff, **extra)
         if f"s{k + 1}_lon" in c:

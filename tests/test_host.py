@@ -83,8 +83,12 @@ def test_unsupported_paths_raise_before_device_work(golden):
     kw = dict(uv_interp="barycentric", vel_next=sn[1], dt_to_next=86400.0)
     with pytest.raises(ValueError):   # least squares reads element-layout u/v; these are on nodes
         KI.rk2_step(st, sn[0], g.mesh, 3600.0, 1.0, **{**kw, "uv_interp": "leastsq"})
-    with pytest.raises(NotImplementedError):
+    with pytest.raises(ValueError):   # the edge-neighbour fit reads element-layout u/v too
         KI.rk2_step(st, sn[0], g.mesh, 3600.0, 1.0, **{**kw, "uv_interp": "edge_leastsq"})
+    with pytest.raises(ValueError, match="edge_leastsq_bc"):
+        KI.rk2_step(st, sn[0], g.mesh, 3600.0, 1.0, **{**kw, "uv_interp": "edge_leastsq", "edge_leastsq_bc": "slip"})
+    with pytest.raises(NotImplementedError):
+        KI.rk2_step(st, sn[0], g.mesh, 3600.0, 1.0, **{**kw, "uv_interp": "spline"})
     with pytest.raises(NotImplementedError):
         KI.rk2_step(st, sn[0], g.mesh, 3600.0, 1.0, **kw,
                     diffusion=DiffusionStepArgs("em", 1.0, 1.0, 0, 0, 0, composition="split_rk"))

@@ -61,6 +61,11 @@ CASES += LSQ_CASES
 LSQ_CASES += [("golden_lsq3d", c) for c in ("rk2_wbary", "rk4_wnear_kick", "euler_wlsq", "rk2_wlsq_bwd",
                                             "rk4_wbary_pchip")]
 CASES += LSQ_CASES[-5:]
+# element-layout u/v by the edge-neighbour least squares (freeslip / noslip ghosts)
+EDGE_CASES = [(f, c) for f in ("golden_edge_band", "golden_edge_quad")
+              for c in ("rk2", "rk4_noslip", "euler", "rk2_kick_noslip")]
+EDGE_CASES += [("golden_edge3d", c) for c in ("rk2_wbary", "rk4_wlsq_noslip", "euler_wnear")]
+CASES += EDGE_CASES
 
 
 def w_interp_of(cname):
@@ -75,7 +80,16 @@ def uv_interp_of(g):
     """The recorded fixture's u/v interpolator."""
     if getattr(g.mesh, "_nemo_cgrid", False):
         return "nemo_cgrid"
+    if getattr(g, "uv_edge", False):
+        return "edge_leastsq"
     return "leastsq" if g.uv_element else "barycentric"
+
+
+def edge_kw(g, cname):
+    """The edge_leastsq boundary rule of a recorded case (from its name)."""
+    if not getattr(g, "uv_edge", False):
+        return {}
+    return {"edge_leastsq_bc": "noslip" if "noslip" in cname else "freeslip"}
 
 
 def recon_of(g, c, k):
@@ -121,7 +135,8 @@ def replay_oracle(g, cname):
         es, ee = surfaces_of(c, k)
         out = O.step(st, vel, g.mesh, dt, td, scheme, vel_next=vnext, dt_to_next=dtn, w_interp=w_interp,
                      diffusion=diff, view=view, recon=recon_of(g, c, k),
-                     uv_interp="leastsq" if g.uv_element else "barycentric", eta_start=es, eta_end=ee)
+                     uv_interp={"nemo_cgrid": "barycentric"}.get(uv_interp_of(g), uv_interp_of(g)),
+                     eta_start=es, eta_end=ee, **edge_kw(g, cname))
         st = st.replace(lon=out["lon"], lat=out["lat"], z=out["z"], status=out["status"],
                         nearest_node=out["nearest_node"], failure_reason=out["failure_reason"],
                         u=out["u"], v=out["v"], w=out["w"], elem=out.get("elem"))
