@@ -39,6 +39,7 @@
  *   kc_field_upload_eta <- core.io.VelocityField.eta (src/kelp/core/io.py:180)
  *   kc_rng_normals     <- numerics.diffusion._normal_pair (src/kelp/numerics/diffusion.py:233)
  *   kc_sample_field    <- numerics.sampling.sample_field (src/kelp/numerics/sampling.py:727)
+ *   kc_sample_field_sigma <- its sigma-mesh branch _sample_sigma_3d (sampling.py:620-723)
  *   kc_beach_surface   <- the vel.eta / vel.scalars[dry_mask_var] reads of tracking._apply_beaching_hook
  *   kc_sigma_surfaces  <- the sigma_eta_start / sigma_eta_end arguments of the step functions
  *                         (src/kelp/numerics/integrators.py:1358-1441; tracking.py:2562-2596)
@@ -397,6 +398,17 @@ int kc_set_fused_block(kc_ctx* ctx, int block);
  * kc_particles_download returns the upload order.  No reference counterpart
  * (the reference's utils/sort_seeds.py sorts seed files offline). */
 int kc_sort(kc_ctx* ctx);
+
+/* Sampling on a sigma mesh (sampling.py:620-723 _sample_sigma_3d): values
+ * (rows, N) an interface field (rows == K, the sigma W interpolation of the
+ * method, vertical_sigma.py:971-1031) or a mid-layer field (rows == K-1, each
+ * node's column max(depth + eta, Dmin) with its mid-layer depths, z clamped to
+ * it, then the method's horizontal rule); eta (N) the free surface; the other
+ * arguments as kc_sample_field, methods 0 (nearest), 1 (leastsq) and 3 (idw).
+ * KC_ERR_STATE unless the mesh is a sigma mesh. */
+int kc_sample_field_sigma(kc_ctx* ctx, const double* values, int rows, const double* eta, double Dmin, long long P,
+                          const double* lon, const double* lat, const double* z, const int* nearest,
+                          const unsigned char* alive, int method, double* out);
 
 /* Batch exact nearest node of P query points (host arrays). */
 int kc_find_nearest(kc_ctx* ctx, long long P, const double* lon, const double* lat, int* out);

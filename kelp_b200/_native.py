@@ -27,7 +27,7 @@ EXPORTS = ("kc_abi_version", "kc_node_xyz_fill", "kc_create", "kc_destroy", "kc_
            "kc_beach_state_download", "kc_beach", "kc_step", "kc_step_host", "kc_step_range", "kc_run_fused",
            "kc_particles_set_realization", "kc_elem_neighbors_upload", "kc_elem_centers_upload", "kc_field_upload_async", "kc_particles_set_elem",
            "kc_particles_get_elem", "kc_find_elements_walk", "kc_find_elements", "kc_sigma_upload", "kc_field_upload_eta", "kc_cgrid_upload",
-           "kc_set_fused_block", "kc_run", "kc_sort", "kc_find_nearest", "kc_find_nearest_noalloc", "kc_rng_normals", "kc_rng_domain_digests", "kc_grid_hash_build", "kc_grid_cell_stats", "kc_sample_field", "kc_beach_surface", "kc_sigma_surfaces", "kc_sigma_surface_slots",
+           "kc_set_fused_block", "kc_run", "kc_sort", "kc_find_nearest", "kc_find_nearest_noalloc", "kc_rng_normals", "kc_rng_domain_digests", "kc_grid_hash_build", "kc_grid_cell_stats", "kc_sample_field", "kc_sample_field_sigma", "kc_beach_surface", "kc_sigma_surfaces", "kc_sigma_surface_slots",
            "kc_device_errors",
            "kc_event_record", "kc_event_elapsed", "kc_l2_flush", "kc_host_alloc", "kc_host_free")
 
@@ -160,6 +160,7 @@ def lib():
         L.kc_sigma_surfaces.argtypes = [vp, vp, vp, i]
         L.kc_sigma_surface_slots.argtypes = [vp, i, i, vp, C.c_double, vp, C.c_double, i]
         L.kc_sample_field.argtypes = [vp, vp, C.c_int, vp, ll, vp, vp, vp, vp, vp, C.c_int, vp]
+        L.kc_sample_field_sigma.argtypes = [vp, vp, C.c_int, vp, C.c_double, ll, vp, vp, vp, vp, vp, C.c_int, vp]
         L.kc_find_nearest_noalloc.argtypes = [vp, ll, vp, vp, vp]
         L.kc_rng_normals.argtypes = [vp, ll, C.c_ulonglong, C.c_ulonglong, C.c_ulonglong, C.c_ulonglong,
                                      C.c_ulonglong, vp]

@@ -21,6 +21,7 @@
 #include "kc_launch.h"
 #include "kc_beach.cuh"
 #include "kc_sample.cuh"
+#include "kc_sigma.cuh"
 
 namespace {
 
@@ -253,6 +254,28 @@ __global__ void __launch_bounds__(kBlock) k_sample_iface(const __grid_constant__
     if (method == kc::S_NEAREST) out[i] = kc::w_linear<double>(m, f, 0.0, zp, a, 1.0);
     else if (method == kc::S_BARYCENTRIC) out[i] = kc::w_bary<double>(m, f, 0.0, lon, lat, zp, a, 1.0);
     else out[i] = kc::w_ring<double>(m, f, method == kc::S_LEASTSQ ? 2 : 3, 0.0, lon, lat, zp, a, 1.0);
+}
+
+// sampling.py:659-689 on a sigma mesh: an interface field (K, N) through the
+// sigma W interpolation of the method (vertical_sigma.py:971-1031, the
+// columns max(depth + eta, Dmin)); mid-layer fields take k_sample with the
+// sigma columns in DSample.
+__global__ void __launch_bounds__(kBlock) k_sample_iface_sigma(const __grid_constant__ kc::DMesh m,
+                                                               const kc::DBlend<double> f,
+                                                               const __grid_constant__ kc::DStep s, const double* q,
+                                                               const double* z, const int* nn,
+                                                               const unsigned char* alive, long long P, double* out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P) return;
+    const int a = nn[i];
+    if ((alive && !alive[i]) || a < 0) {
+        out[i] = __longlong_as_double(0x7ff8000000000000LL);
+        return;
+    }
+    const double lon = q[i], lat = q[P + i];
+    kc::SigSite site;
+    kc::sigma_site<double>(m, f, s, 0, lon, lat, a, site);
+    out[i] = kc::w_sig<double>(m, f, s, 0, lon, lat, z[i], a, site);
 }
 
 __global__ void __launch_bounds__(kBlock) k_nearest(const __grid_constant__ kc::DMesh m, const double* q, long long P, int* out) {
@@ -2332,7 +2355,7 @@ static int sample_run(kc_ctx* c, char* buf, const double* values, size_t nvals, 
         k_sample_iface<<<grid_for(P), kBlock, 0, st>>>(c->dm, f, d_q, d_z, d_nn, alive ? d_al : nullptr, P, method,
                                                        d_out);
     } else {
-        kc::DSample S;
+        kc::DSample S{};
         S.values = d_vals;
         S.zm = rows > 0 ? d_zm : nullptr;
         S.n = c->N;
@@ -2374,6 +2397,82 @@ int kc_sample_field(kc_ctx* c, const double* values, int rows, const double* z_m
     cudaStreamSynchronize(c->stream);
     cudaFree(buf);
     return rc;
+}
+
+int kc_sample_field_sigma(kc_ctx* c, const double* values, int rows, const double* eta, double Dmin, long long P,
+                          const double* lon, const double* lat, const double* z, const int* nearest,
+                          const unsigned char* alive, int method, double* out) {
+    if (!c) return KC_ERR_ARG;
+    if (!c->has_mesh) return fail(c, KC_ERR_STATE, "kc_sample_field_sigma: no mesh uploaded");
+    if (!c->dm.sig || !c->d_sigma) return fail(c, KC_ERR_STATE, "kc_sample_field_sigma: the mesh is not a sigma mesh");
+    if (method < 0 || method > 3 || method == kc::S_BARYCENTRIC)
+        return fail(c, KC_ERR_ARG, "kc_sample_field_sigma: method must be 0 (nearest), 1 (leastsq) or 3 (idw)");
+    const int K = c->dm.K;
+    if ((rows != K && rows != K - 1) || K < 2 || !values || !eta || !(Dmin > 0.0) || P < 0 ||
+        (P > 0 && (!lon || !lat || !z || !out)))
+        return fail(c, KC_ERR_ARG, "kc_sample_field_sigma: a (K, N) or (K-1, N) field, eta, Dmin > 0, depths");
+    if (nearest)
+        for (long long i = 0; i < P; ++i)
+            if (nearest[i] >= c->N) return fail(c, KC_ERR_ARG, "kc_sample_field_sigma: nearest node out of range");
+    if (P == 0) return KC_OK;
+    KC_CUDA(c, cudaSetDevice(c->device));
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t nvals = (size_t)rows * (size_t)c->N;
+    const size_t total = al(nvals * 8) + al((size_t)c->N * 8) + al((size_t)P * 16) + 2 * al((size_t)P * 8) +
+                         al((size_t)P * 4) + al((size_t)P);
+    char* buf = nullptr;
+    KC_CUDA(c, cudaMalloc((void**)&buf, total));
+    double* d_vals = (double*)buf;
+    double* d_eta = (double*)(buf + al(nvals * 8));
+    double* d_q = (double*)((char*)d_eta + al((size_t)c->N * 8));
+    double* d_z = (double*)((char*)d_q + al((size_t)P * 16));
+    double* d_out = (double*)((char*)d_z + al((size_t)P * 8));
+    int* d_nn = (int*)((char*)d_out + al((size_t)P * 8));
+    unsigned char* d_al = (unsigned char*)((char*)d_nn + al((size_t)P * 4));
+    cudaStream_t st = c->stream;
+    cudaError_t e = cudaSuccess;
+    auto ok = [&](cudaError_t r) { if (e == cudaSuccess) e = r; return e == cudaSuccess; };
+    ok(cudaMemcpyAsync(d_vals, values, nvals * 8, cudaMemcpyHostToDevice, st));
+    ok(cudaMemcpyAsync(d_eta, eta, (size_t)c->N * 8, cudaMemcpyHostToDevice, st));
+    ok(cudaMemcpyAsync(d_q, lon, (size_t)P * 8, cudaMemcpyHostToDevice, st));
+    ok(cudaMemcpyAsync(d_q + P, lat, (size_t)P * 8, cudaMemcpyHostToDevice, st));
+    ok(cudaMemcpyAsync(d_z, z, (size_t)P * 8, cudaMemcpyHostToDevice, st));
+    if (alive) ok(cudaMemcpyAsync(d_al, alive, (size_t)P, cudaMemcpyHostToDevice, st));
+    if (nearest) {
+        ok(cudaMemcpyAsync(d_nn, nearest, (size_t)P * 4, cudaMemcpyHostToDevice, st));
+    } else if (e == cudaSuccess) {
+        k_nearest<<<grid_for(P), kBlock, 0, st>>>(c->dm, d_q, P, d_nn);
+        ok(cudaGetLastError());
+    }
+    if (e == cudaSuccess && rows == K) {
+        kc::DBlend<double> f{};
+        f.a.w = f.b.w = f.t.w = d_vals;
+        f.a.eta = f.b.eta = f.t.eta = d_eta;
+        f.alpha0 = 0.0;
+        f.n = c->N;
+        kc::DStep s{};
+        s.dt = 1.0; s.time_dir = 1.0; s.Dmin = Dmin;
+        s.w_code = method == kc::S_NEAREST ? 0 : method == kc::S_BARYCENTRIC ? 1 : method == kc::S_LEASTSQ ? 2 : 3;
+        s.edge_bc = -1;
+        k_sample_iface_sigma<<<grid_for(P), kBlock, 0, st>>>(c->dm, f, s, d_q, d_z, d_nn, alive ? d_al : nullptr, P,
+                                                             d_out);
+        ok(cudaGetLastError());
+    } else if (e == cudaSuccess) {
+        kc::DSample S{};
+        S.values = d_vals;
+        S.n = c->N;
+        S.rows = rows;
+        S.sig = c->d_sigma;
+        S.eta = d_eta;
+        S.Dmin = Dmin;
+        k_sample<<<grid_for(P), kBlock, 0, st>>>(c->dm, S, d_q, d_z, d_nn, alive ? d_al : nullptr, P, method, d_out);
+        ok(cudaGetLastError());
+    }
+    ok(cudaMemcpyAsync(out, d_out, (size_t)P * 8, cudaMemcpyDeviceToHost, st));
+    ok(cudaStreamSynchronize(st));
+    cudaFree(buf);
+    if (e != cudaSuccess) return fail(c, KC_ERR_CUDA, std::string("kc_sample_field_sigma: ") + cudaGetErrorString(e));
+    return KC_OK;
 }
 
 int kc_find_elements(kc_ctx* c, long long P, const double* lon, const double* lat, const int* nn, int* out) {

@@ -14,9 +14,12 @@ constexpr int S_NEAREST = 0, S_LEASTSQ = 1, S_BARYCENTRIC = 2, S_IDW = 3;
 
 struct DSample {
     const double* values;   // (N) or (rows, N), float64
-    const double* zm;       // (rows) mid-layer depths, positive down
+    const double* zm;       // (rows) mid-layer depths, positive down (z-level meshes)
     long long n;            // N
     int rows;               // 0: a 2-D field; >= 1: a mid-layer field
+    const double* sig;      // (rows + 1) sigma interfaces of a sigma mesh, else null
+    const double* eta;      // (N) the free surface of a sigma mesh's columns
+    double Dmin;            // the sigma columns' floor
 };
 
 
@@ -24,23 +27,26 @@ struct DSample {
 // mid-layer values around z, clamped to the first / last layer.  The
 // bracket is the first k with z < zm[k + 1] (a binary search finds the same
 // k in the non-decreasing zm; a NaN z takes the last layer, as the scan does).
-__device__ __forceinline__ double mid_linear(const DSample& S, double z, int node) {
+__device__ __forceinline__ double mid_linear(const DSample& S, double z, int node, double H = -1.0) {
     const int K1 = S.rows;
     const double* f = S.values;
-    const double* zm = S.zm;
+    // the mid-layer depths: the mesh's, or a sigma column's of height H
+    // (sampling.py:598-601: (1 - (s_m + s_m+1) / 2) H)
+    auto zm_at = [&](int k) { return S.sig ? (1.0 - 0.5 * (S.sig[k] + S.sig[k + 1])) * H : S.zm[k]; };
     if (K1 == 1) return f[node];
-    if (z <= zm[0]) return f[node];
-    if (z >= zm[K1 - 1] || isnan(z)) return f[(long long)(K1 - 1) * S.n + node];
+    if (z <= zm_at(0)) return f[node];
+    if (z >= zm_at(K1 - 1) || isnan(z)) return f[(long long)(K1 - 1) * S.n + node];
     int lo = 1, hi = K1 - 1;
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
-        if (z < zm[mid]) hi = mid;
+        if (z < zm_at(mid)) hi = mid;
         else lo = mid + 1;
     }
     const int k = lo - 1;
-    const double dz = zm[k + 1] - zm[k];
+    const double zk = zm_at(k), zk1 = zm_at(k + 1);
+    const double dz = zk1 - zk;
     if (dz < 1e-12) return f[(long long)k * S.n + node];
-    const double a = (z - zm[k]) / dz;
+    const double a = (z - zk) / dz;
     return (1.0 - a) * f[(long long)k * S.n + node] + a * f[(long long)(k + 1) * S.n + node];
 }
 
@@ -49,6 +55,11 @@ __device__ __forceinline__ double mid_linear(const DSample& S, double z, int nod
 // (sampling.py:528-531).
 __device__ __forceinline__ double node_value(const DMesh& m, const DSample& S, double z_p, int nd) {
     if (S.rows == 0) return S.values[nd];
+    if (S.sig) {   // sampling.py:586-605: the node's column max(depth + eta, Dmin), z clamped to it
+        double H = m.depth[nd] + S.eta[nd];
+        if (H < S.Dmin) H = S.Dmin;
+        return mid_linear(S, z_p < H ? z_p : H, nd, H);
+    }
     const double bot = m.depth[nd];
     return mid_linear(S, z_p < bot ? z_p : bot, nd);
 }

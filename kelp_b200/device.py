@@ -519,6 +519,23 @@ class DeviceContext:
                   "kc_sample_field")
         return out
 
+    def sample_field_sigma(self, values, lon, lat, z, eta, Dmin, nearest=None, alive=None,
+                           method: int = 1) -> np.ndarray:
+        """kc_sample_field_sigma: an interface (K, N) or mid-layer (K-1, N)
+        field on the resident sigma mesh with its free surface eta."""
+        values = _c(values, np.float64)
+        lon = _c(lon, np.float64)
+        lat = _c(lat, np.float64)
+        zz = _c(z, np.float64)
+        et = _c(eta, np.float64)
+        nn = None if nearest is None else _c(nearest, np.int32)
+        al = None if alive is None else _c(np.asarray(alive).astype(np.uint8), np.uint8)
+        out = np.empty(lon.shape[0], np.float64)
+        self._chk(N.lib().kc_sample_field_sigma(self._ctx, N.ptr(values), values.shape[0], N.ptr(et), float(Dmin),
+                                                lon.shape[0], N.ptr(lon), N.ptr(lat), N.ptr(zz), N.ptr(nn),
+                                                N.ptr(al), int(method), N.ptr(out)), "kc_sample_field_sigma")
+        return out
+
     def find_elements(self, lon, lat, nn=None) -> np.ndarray:
         """mesh.find_containing_elements on the device: the 1-ring / 2-ring
         scan around nn (None: the exact nearest node); -1 outside."""

@@ -9,8 +9,10 @@ native library (``kc_sample_field``, one thread per particle).
 Covered: node fields ``(N,)``, z-level mid-layer fields ``(K-1, N)`` and
 interface fields ``(K, N)`` (through the W interpolation of the method, as
 the reference hands them over, sampling.py:876-890) with the methods
-``nearest``, ``leastsq``, ``barycentric`` and ``idw``.  Not built: sigma
-meshes (``NotImplementedError``).
+``nearest``, ``leastsq``, ``barycentric`` and ``idw``, and on sigma meshes
+(sampling.py:620-723: the node columns max(depth + eta, Dmin)) with
+``nearest``, ``leastsq`` and ``idw``; barycentric sampling on sigma meshes
+raises ``NotImplementedError``.
 """
 from __future__ import annotations
 
@@ -28,11 +30,11 @@ def sample_field(values, mesh, lons, lats, zs=None, *, nearest=None, alive=None,
                  Dmin=0.5, ctx=None) -> np.ndarray:
     """Sample a node scalar field at particle positions (sampling.py:727).
 
-    values (N,) or (K-1, N) on a z-level mesh; lons, lats (P,) degrees;
-    zs (P,) positive-down metres, required for a 3-D field; nearest (P,)
-    anchors (None: the exact nearest node); alive (P,) mask (None: all
-    alive); method one of nearest / leastsq / barycentric / idw.  eta and
-    Dmin belong to the sigma-mesh form, which is not built.
+    values (N,), (K-1, N) or (K, N); lons, lats (P,) degrees; zs (P,)
+    positive-down metres, required for a 3-D field; nearest (P,) anchors
+    (None: the exact nearest node); alive (P,) mask (None: all alive);
+    method one of nearest / leastsq / barycentric / idw; on a sigma mesh
+    eta (N,) the free surface of the columns and Dmin their floor.
     """
     from .device import default_context
     if method not in METHOD_CODES:
@@ -48,8 +50,19 @@ def sample_field(values, mesh, lons, lats, zs=None, *, nearest=None, alive=None,
     if values.ndim == 2:
         if zs is None:
             raise ValueError("zs (particle depths) is required for 3D field sampling")
-        if getattr(mesh, "vertical_coord", "zlevel") == "sigma":
-            raise NotImplementedError("sampling on sigma meshes is not built on the CUDA backend")
+        if getattr(mesh, "vertical_coord", "zlevel") == "sigma":   # sampling.py:620-723 _sample_sigma_3d
+            if eta is None:
+                raise ValueError("eta (free-surface elevation) is required for sigma mesh sampling")
+            if method == "barycentric":
+                raise NotImplementedError("barycentric sampling on sigma meshes is not built on the CUDA backend "
+                                          "(nearest, leastsq and idw are)")
+            K = np.asarray(mesh.sigma).size
+            if values.shape[0] not in (K, K - 1):
+                raise ValueError(f"sigma 3D field shape[0]={values.shape[0]} does not match "
+                                 f"K={K} (interface) or K-1={K - 1} (mid-layer) from mesh.sigma")
+            ctx = ctx or default_context()
+            ctx.ensure_mesh(mesh)
+            return ctx.sample_field_sigma(values, lons, lats, zs, eta, Dmin, nearest, alive, METHOD_CODES[method])
         zl = np.abs(np.asarray(mesh.sigma, dtype=np.float64))
         K = zl.size
         if values.shape[0] not in (K, K - 1):

@@ -2610,3 +2610,49 @@ int orc_sample(const orc_mesh* mm, const double* values, int rows, const double*
     par_for(P, sample_body, &c);
     return 0;
 }
+
+/* sampling.py:620-723 _sample_sigma_3d and :545-617 _loop_sample_mid_sigma:
+ * an interface field (K, N) through the sigma W interpolation of the method,
+ * or a mid-layer field read in each ring node's column max(depth + eta,
+ * Dmin), z clamped to it, then the method's horizontal rule.  Serial: a
+ * test-size checker. */
+int orc_sample_sigma(const orc_mesh* mm, const double* values, int rows, const double* eta, double Dmin, int64_t P,
+                     const double* lon, const double* lat, const double* z, const int* nearest,
+                     const unsigned char* alive, int method, double* out) {
+    const OMesh* m = (const OMesh*)mm;
+    int K = m->K;
+    double zm_col[512];
+    if (rows >= 512) return 1;
+    for (int64_t i = 0; i < P; ++i) {
+        if ((alive && !alive[i]) || nearest[i] < 0) { out[i] = NAN; continue; }
+        int nn = nearest[i];
+        if (rows == K) {
+            OField f;
+            memset(&f, 0, sizeof f);
+            f.wa = f.wb = f.wt = values;
+            f.etaa = f.etab = f.etat = eta;
+            f.n = m->N;
+            OStep s;
+            memset(&s, 0, sizeof s);
+            s.w_code = method == S_NEAREST ? 0 : method == S_BARYCENTRIC ? 1 : method == S_LEASTSQ ? 2 : 3;
+            s.td = 1.0;
+            s.dt = 1.0;
+            s.Dmin = Dmin;
+            out[i] = w_sig(m, &f, &s, 0, lon[i], lat[i], z[i], nn);
+            continue;
+        }
+        int32_t buf[MAX_NEIGH];
+        double vals[MAX_NEIGH];
+        int cnt = neigh_ring(m, nn, buf);
+        for (int k = 0; k < cnt; ++k) {
+            int nd = buf[k];
+            double H = m->depth[nd] + eta[nd];
+            if (H < Dmin) H = Dmin;
+            double ze = z[i] < H ? z[i] : H;
+            for (int q = 0; q < rows; ++q) zm_col[q] = (1.0 - 0.5 * (m->sigma[q] + m->sigma[q + 1])) * H;
+            vals[k] = mid_linear(values, m->N, zm_col, rows, ze, nd);
+        }
+        out[i] = combine_horizontal(m, vals, buf, cnt, lon[i], lat[i], nn, method);
+    }
+    return 0;
+}

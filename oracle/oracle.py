@@ -79,6 +79,8 @@ def lib():
         L.orc_walk.argtypes = [C.POINTER(OMesh), i64, vp, vp, vp, vp, vp]
         L.orc_find_nearest.argtypes = [C.POINTER(OMesh), i64, vp, vp, vp]
         L.orc_contain.argtypes = [C.POINTER(OMesh), i64, vp, vp, vp, vp]
+        L.orc_sample_sigma.argtypes = [C.POINTER(OMesh), vp, C.c_int, vp, C.c_double, i64, vp, vp, vp, vp, vp,
+                                       C.c_int, vp]
         L.orc_cell_stats.argtypes = [C.POINTER(OMesh), vp, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
                                      C.c_int, i64, vp, vp, vp, vp, vp, vp, vp]
         L.orc_normals.argtypes = [i64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, vp]
@@ -452,7 +454,8 @@ def node_xyz(lon, lat) -> np.ndarray:
 SAMPLE_METHODS = {"nearest": 0, "leastsq": 1, "barycentric": 2, "idw": 3}
 
 
-def sample_field(values, mesh, lon, lat, z=None, *, nearest=None, alive=None, method="leastsq", view=None):
+def sample_field(values, mesh, lon, lat, z=None, *, nearest=None, alive=None, method="leastsq", view=None, eta=None,
+                 Dmin=0.5):
     """sampling.py:727 sample_field for a node field of shape (N,), a
     z-level mid-layer field (K-1, N) or an interface field (K, N): the
     oracle's restatement."""
@@ -466,6 +469,13 @@ def sample_field(values, mesh, lon, lat, z=None, *, nearest=None, alive=None, me
     nearest = np.ascontiguousarray(nearest, dtype=np.int32)
     al = None if alive is None else np.ascontiguousarray(alive, dtype=np.uint8)
     rows, zm, zz = 0, None, None
+    if values.ndim == 2 and getattr(mesh, "vertical_coord", "zlevel") == "sigma":   # sampling.py:620-723
+        out = np.empty(P)
+        et = np.ascontiguousarray(eta, dtype=np.float64)
+        zz = np.ascontiguousarray(z, dtype=np.float64)
+        lib().orc_sample_sigma(C.byref(view.s), _p(values), values.shape[0], _p(et), float(Dmin), P, _p(lon),
+                               _p(lat), _p(zz), _p(nearest), _p(al), SAMPLE_METHODS[method], _p(out))
+        return out
     if values.ndim == 2:
         zl = np.abs(np.asarray(mesh.sigma, dtype=np.float64))
         rows = values.shape[0]

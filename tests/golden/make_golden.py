@@ -1299,6 +1299,42 @@ def sample_iface_fixture():
     print("golden_sample_iface", os.path.getsize(path) // 1024, "KB")
 
 
+def sample_sigma_fixture():
+    """sampling.py:620-723 _sample_sigma_3d: an interface (K, N) and a
+    mid-layer (K-1, N) field on the sigma shelf of golden_sigma_surf with a
+    free surface eta, every method; points at the surface and below every
+    bottom, dead particles and nearest = -1.  tests/golden/golden_sample_sigma.npz."""
+    from kelp.numerics.sampling import sample_field as r_sample
+    sig = np.array([1.0, 0.95, 0.88, 0.8, 0.7, 0.58, 0.45, 0.32, 0.2, 0.1, 0.0])
+    m = S.lattice_mesh(1.0, 15.0, lon_min=-20.0, lon_max=20.0, jitter=0.15, land_frac=0.2, quad_frac=0.3,
+                       depth=lambda lo, la: S.smooth_bathymetry(lo, la, 0.2, 120.0), sigma=sig)
+    rm = ref_mesh(m, sigma=sig)
+    rm.vertical_coord = "sigma"
+    rng = np.random.default_rng(79)
+    lo, la = np.asarray(m.nodes_lon), np.asarray(m.nodes_lat)
+    eta = 0.6 * np.sin(np.radians(2.0 * lo) * 20.0) * np.cos(np.radians(3.0 * la) * 10.0) - 0.15
+    K = sig.size
+    vk = 3.0 + 2.0 * sig[:, None] + 0.5 * np.cos(np.radians(4.0 * lo))[None, :] + 1e-3 * np.arange(K)[:, None]
+    sm = 0.5 * (sig[:-1] + sig[1:])
+    vm = 10.0 + 4.0 * sm[:, None] * (1.0 + 0.3 * np.sin(np.radians(5.0 * la)))[None, :]
+    P = 1500
+    lon, lat, z, _ = particles(m, P, 83, z=True)
+    z[:40] = 0.0
+    z[40:80] = 500.0     # below every column
+    alive = np.ones(P, bool)
+    alive[rng.choice(P, 40, replace=False)] = False
+    nearest = find_nearest_nodes(rm, lon, lat).astype(np.int32)
+    nearest[rng.choice(P, 20, replace=False)] = -1
+    d = {f"mesh_{k}": v for k, v in mesh_record(rm).items()}
+    d.update(lon=lon, lat=lat, z=z, alive=alive, nearest=nearest, vk=vk, vm=vm, eta=eta)
+    for meth in ("nearest", "leastsq", "barycentric", "idw"):
+        d[f"ok_{meth}"] = r_sample(vk, rm, lon, lat, z, nearest=nearest, alive=alive, eta=eta, method=meth, Dmin=0.5)
+        d[f"om_{meth}"] = r_sample(vm, rm, lon, lat, z, nearest=nearest, alive=alive, eta=eta, method=meth, Dmin=0.5)
+    path = os.path.join(HERE, "golden_sample_sigma.npz")
+    np.savez_compressed(path, **d)
+    print("golden_sample_sigma", os.path.getsize(path) // 1024, "KB")
+
+
 def rng1m_fixture():
     """The reference's own _normal_pair on 4 x 2^20 keys (contiguous particle
     ids under 4 key tuples), stored as per-chunk digests (tests/golden/
@@ -1356,7 +1392,7 @@ def reftypes_fixture():
 
 if __name__ == "__main__":
     # no argument: every fixture; otherwise the named ones ("steps", "beach", ...)
-    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq", "rng1m", "tripolar", "reftypes", "sample", "cellrule", "lazy0", "sigma_surf", "eta_time", "sigma_az", "wring", "lsq3d", "sigma_wring", "sample_iface", "edge"}
+    which = set(sys.argv[1:]) or {"steps", "beach", "time", "sigma", "cgrid", "pchip", "lsq", "rng1m", "tripolar", "reftypes", "sample", "cellrule", "lazy0", "sigma_surf", "eta_time", "sigma_az", "wring", "lsq3d", "sigma_wring", "sample_iface", "edge", "sample_sigma"}
     if "rng1m" in which:
         rng1m_fixture()
     if "reftypes" in which:
@@ -1383,6 +1419,8 @@ if __name__ == "__main__":
         sample_iface_fixture()
     if "edge" in which:
         edge_fixture()
+    if "sample_sigma" in which:
+        sample_sigma_fixture()
     if "lsq" in which:
         lsq_fixture()
     if "steps" in which:

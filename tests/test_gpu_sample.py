@@ -92,3 +92,16 @@ def test_interface_field_matches_reference(golden, method):
     got = sample_field(d["vk"], g.mesh, d["lon"], d["lat"], d["z"], nearest=d["nearest"], alive=d["alive"],
                        method=method)
     _check(got, d[f"ok_{method}"], f"interface {method}")
+
+
+@pytest.mark.parametrize("method", ("nearest", "leastsq", "idw"))
+def test_sigma_fields_match_reference(golden, method):
+    """Sigma-mesh sampling (sampling.py:620-723) on the device: interface and
+    mid-layer fields with the free surface, against the reference's outputs."""
+    from kelp_b200.sampling import sample_field
+    g = golden("golden_sample_sigma")
+    d = g.d
+    for key, out in (("vk", "ok"), ("vm", "om")):
+        got = sample_field(d[key], g.mesh, d["lon"], d["lat"], d["z"], nearest=d["nearest"], alive=d["alive"],
+                           eta=d["eta"], method=method, Dmin=0.5)
+        _check(got, d[f"{out}_{method}"], f"sigma {key} {method}")

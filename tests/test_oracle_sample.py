@@ -69,3 +69,17 @@ def test_oracle_interface_field_matches_reference(golden, method):
                          method=method)
     assert _same(got, d[f"ok_{method}"]) == 0
     assert np.isfinite(d[f"ok_{method}"][d["alive"] & (d["nearest"] >= 0)]).all()
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_oracle_sigma_fields_match_reference(golden, method):
+    """Sigma-mesh sampling (sampling.py:620-723): an interface field through
+    the sigma W interpolation, a mid-layer field in the node columns
+    max(depth + eta, Dmin)."""
+    from oracle import oracle as O
+    g = golden("golden_sample_sigma")
+    d = g.d
+    for key, out in (("vk", "ok"), ("vm", "om")):
+        got = O.sample_field(d[key], g.mesh, d["lon"], d["lat"], d["z"], nearest=d["nearest"], alive=d["alive"],
+                             method=method, eta=d["eta"], Dmin=0.5)
+        assert _same(got, d[f"{out}_{method}"]) == 0, key
