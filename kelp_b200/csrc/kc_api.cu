@@ -2021,8 +2021,10 @@ int kc_step_host(kc_ctx* c, const kc_step_args* a, long long P, const kc_host_pa
         }
         KC_CUDA(c, cudaEventCreateWithFlags(&c->ev_start, cudaEventDisableTiming));
     }
-    // chunk: a multiple of the block size, at most kChunks chunks
-    long long ch = chunk > 0 ? chunk : (P + 7) / 8;
+    // chunk: a multiple of the block size, at most kChunks chunks; by default
+    // eight, but no smaller than 2^18 particles, so a small state is not cut
+    // into pieces whose copies and launches cost more than they overlap
+    long long ch = chunk > 0 ? chunk : std::max((P + 7) / 8, 1LL << 18);
     ch = std::max(ch, (P + kChunks - 1) / kChunks);
     ch = std::max<long long>(kBlock, (ch + kBlock - 1) / kBlock * kBlock);
     const int nch = (int)((P + ch - 1) / ch);
