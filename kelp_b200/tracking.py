@@ -515,6 +515,8 @@ class Tracker:
                                         wet_streak=ctx.beach_state_download() if beach_cfg is not None else None,
                                         release_step=rs, particle_offset=particle_offset,
                                         uv_vertical=getattr(self.fields[0], "uv_vertical", "layer"))
+        if self.sigma and self.dims == 3:   # later steps on this context take their own surfaces again
+            ctx.sigma_surfaces(None, None, False)
         err = ctx.device_errors()
         if err:
             raise N.KcError(N.KC_ERR_DEVICE, N.describe_device_errors(err))
